@@ -1,0 +1,226 @@
+/*
+ * nrrs.h -- C-ABI of the B200 (sm_100a) neural Russian-roulette-and-splitting step.
+ *
+ * One library (libnrrs_b200.so) exports the per-path-vertex NRRS hot path:
+ *   1. inference on a SoA wavefront queue: hash-grid + spherical-harmonics encoding,
+ *      StatNet MLP, glue, RRSNet MLP, activation, clamp           (nrrs_infer)
+ *   2. RRS normalisation and the stochastic kill/split decision,
+ *      compaction of survivors into the next-bounce queue         (nrrs_decide_emit)
+ *   3. both fused (nrrs_step) and batched over uneven depths      (nrrs_step_batched)
+ *   4. one training step of StatNet and RRSNet on a sample batch  (nrrs_train_step)
+ *
+ * Everything is asynchronous on the caller's CUDA stream (passed as void*; NULL = legacy
+ * default stream). Input and output buffers are device pointers owned by the caller. The
+ * context owns the weights, optimizer state and scratch. No entry point synchronises the
+ * stream except the ones documented as synchronous (nrrs_get_device_status, parameter
+ * copies to host, nrrs_save/nrrs_load).
+ *
+ * Reference interfaces replaced (paths inside banbao990/NRRS-Code):
+ *   NRRSNetwork class                    src/render/nrrs/net/network.h:22-214
+ *   NRRSPathTracer::generateRRSNumber    src/render/nrrs/integrator.cpp:1057-1483
+ *   NRRSPathTracer::trainStep            src/render/nrrs/integrator.cpp:2337-2657
+ *   calcSum2PassAsync<true>              src/render/common/commoncudautilshost.cpp:6-22
+ *   TidQueue::push / pushCheck           src/render/common/commonworkqueue.h:19-42
+ */
+#ifndef NRRS_B200_H
+#define NRRS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NRRS_ABI_VERSION 1
+
+/* ---- status codes (the reference has none: Log(Fatal) aborts, overflow only printf's) ---- */
+typedef enum {
+    NRRS_OK = 0,
+    NRRS_ERR_INVALID_ARG = -1,      /* bad pointer / size / config value                     */
+    NRRS_ERR_CAPACITY_OVERFLOW = -2,/* next queue too small; *next_size still holds the need */
+    NRRS_ERR_NAN = -3,              /* a NaN/Inf factor or loss was seen on the device       */
+    NRRS_ERR_TIMEOUT = -4,          /* a bounded device wait gave up                         */
+    NRRS_ERR_CUDA = -5,             /* a CUDA runtime call failed (see nrrs_last_error)      */
+    NRRS_ERR_NO_DEVICE = -6,        /* no sm_100 device / library built without kernels      */
+    NRRS_ERR_UNSUPPORTED = -7,      /* configuration outside what the kernels implement     */
+    NRRS_ERR_IO = -8                /* nrrs_save / nrrs_load file error                       */
+} nrrs_status;
+
+/* device status bits accumulated by the kernels (nrrs_get_device_status) */
+#define NRRS_DEV_OVERFLOW   0x1u    /* a queue write past capacity was dropped  */
+#define NRRS_DEV_NAN        0x2u    /* non-finite factor or loss                */
+#define NRRS_DEV_TIMEOUT    0x4u    /* look-back / barrier wait ran out         */
+#define NRRS_DEV_SATURATED  0x8u    /* a split count above 255 was clamped      */
+
+typedef enum {
+    NRRS_PREC_FP32 = 0,   /* plain path: FP32 table, FP32 SIMT MLP                         */
+    NRRS_PREC_FP16 = 1,   /* mixed: FP16 table, FP16 tcgen05 MLP, FP32 accumulate          */
+    NRRS_PREC_BF16 = 2    /* mixed: FP16 table, BF16 tcgen05 MLP, FP32 accumulate          */
+} nrrs_precision;
+
+typedef enum {
+    NRRS_FACTOR_ADRRS = 2,   /* step 2: mean(clamp(L,1e-4,1e4)*thp/(ref+0.01)) (integrator.cpp:1244-1254) */
+    NRRS_FACTOR_RRSNET = 3   /* step 3: activationSigma(RRSNet raw)              (integrator.cpp:1188-1243) */
+} nrrs_factor_source;
+
+/* Network, encoding, optimizer and loss hyper-parameters.
+ * Replaces the JSON config of common/configs/nrrs/nrrs/2net-simple.json + NRRSNetwork::reset
+ * (src/render/nrrs/net/network.cpp:443-576). Fill with nrrs_config_default(). */
+typedef struct {
+    /* multiresolution hash grid (Instant-NGP); level l has floor(base_resolution*scale^l) cells */
+    int32_t n_levels;              /* 16                                  */
+    int32_t n_features_per_level;  /* 2 (only 2 is implemented)           */
+    int32_t log2_hashmap_size;     /* 19                                  */
+    int32_t base_resolution;       /* 16                                  */
+    float per_level_scale;         /* 1.5                                 */
+    int32_t sh_degree;             /* 4 -> 16 coefficients (only 4)       */
+    /* networks: bias-free MLPs (a constant-1 input lane carries the bias, as in the reference) */
+    int32_t statnet_width;         /* 64 or 128                           */
+    int32_t statnet_hidden;        /* hidden layers: 2 or 3               */
+    int32_t rrsnet_width;          /* 64 or 128                           */
+    int32_t rrsnet_hidden;         /* 2 or 3                              */
+    int32_t precision;             /* nrrs_precision                      */
+    /* initialisation */
+    uint64_t seed;                 /* Xavier-uniform weights + table init */
+    float table_init_scale;        /* table ~ U(-s, s); 1e-4 as tcnn      */
+    /* Adam (FP32 master weights and moments) */
+    float lr, beta1, beta2, eps, l2_reg;
+    /* losses */
+    float stat_eps;                /* 0.01: StatNet target is log(L + stat_eps) */
+    float ref_eps;                 /* 0.01: pixel estimate offset (integrator.cpp:1249) */
+    float loss_clamp_max;          /* 10: per-sample relative contribution clamp (2net-simple.json clamp_max) */
+    float cost_offset;             /* 1: path cost of a vertex = cost_offset + q */
+    /* scene AABB for position normalisation (nrctrain.h:111-115); normalize_pos=0 feeds pos as-is */
+    int32_t normalize_pos;
+    float aabb_min[3], aabb_max[3];
+    /* capacities (NRRSNetwork::resize, network.cpp:351) */
+    uint32_t max_queue;            /* largest n for infer/decide        */
+    uint32_t max_train;            /* largest batch for nrrs_train_step */
+    int32_t step;                  /* setStep: 0..3 (network.cpp:578-589) */
+} nrrs_config;
+
+/* Input record of one path vertex, SoA (NRRSInferenceWorkItem, src/render/nrrs/workitem.h:9-15,
+ * extended with the fields of the synthetic benchmark record). vec3 fields are [n][3] float. */
+typedef struct {
+    const float* pos;              /* [n][3] world (normalize_pos=1) or normalised position */
+    const float* wi;               /* [n][3] unit incoming direction                         */
+    const float* normal;           /* [n][3] unit shading normal                             */
+    const float* roughness;        /* [n]                                                    */
+    const float* albedo;           /* [n][3]                                                 */
+    const float* thp;              /* [n][3] path throughput before RRS                      */
+    const uint32_t* depth;         /* [n] bounce depth                                       */
+    const float* ref_mean;         /* [n] mean of the pixel estimate (MyFilm, train.cu:54-58); NULL = 0.5 */
+    const uint32_t* scatter_index; /* [n] mScatterQueueIndex; NULL = identity                */
+} nrrs_vertex_soa;
+
+/* Decision parameters (NRRSPathTracer members, src/render/nrrs/integrator.h:265-275, 521-539). */
+typedef struct {
+    float clamp_min;               /* RRS_CLAMP_MIN  (kill threshold)              */
+    float clamp_max;               /* RRS_CLAMP_MAX  (split cap)                   */
+    float normalize_rate;          /* RRS_NORMALIZE_RATE (used when !use_ceil)     */
+    int32_t use_ceil;              /* mRRSNormalizeUseCeil                         */
+    int32_t scale_up;              /* !mDonnotNormalizeWhenLessThanOne             */
+    int32_t use_weight_window;     /* mUseWeightWindow (RRSWeightWindow, size 5)   */
+    float weight_window_size;      /* 5                                            */
+    int32_t factor_source;         /* nrrs_factor_source                           */
+} nrrs_decide_params;
+
+/* One segment of the batched launch: one depth's queue inside a concatenated SoA. */
+typedef struct {
+    uint32_t offset;               /* first vertex of this depth in the SoA        */
+    uint32_t count;                /* vertices of this depth                       */
+    uint32_t budget;               /* normalisation budget B (pixel count)         */
+    uint32_t n_specular;           /* specular vertices excluded from the budget   */
+    uint32_t queue_offset;         /* where this depth's next queue starts         */
+    uint32_t queue_capacity;       /* capacity of this depth's next queue          */
+} nrrs_segment;
+
+typedef struct nrrs_ctx nrrs_ctx;
+
+/* ---- lifetime ---- */
+void nrrs_config_default(nrrs_config* cfg);
+/* NRRSNetwork::NRRSNetwork + reset + resize (network.cpp:443-576, 351-441). */
+int nrrs_create(const nrrs_config* cfg, nrrs_ctx** out);
+void nrrs_destroy(nrrs_ctx* ctx);
+/* NRRSNetwork::setStep (network.cpp:578-589): 0/1 train StatNet only, 2 ADRRS factors, 3 RRSNet. */
+int nrrs_set_step(nrrs_ctx* ctx, int32_t step);
+const char* nrrs_last_error(const nrrs_ctx* ctx);
+const char* nrrs_status_string(int status);
+/* 1 when the library carries sm_100a kernels and a device is present. */
+int nrrs_device_available(void);
+void nrrs_decide_params_default(nrrs_decide_params* p);
+
+/* ---- inference: replaces prepareInferenceData + inference + "Gen RRS Number"
+ *      (network.cpp:297-349, integrator.cpp:1184-1298). Writes the 3 log-statistics
+ *      (may be NULL), the clamped factor rrs[n] and, when use_ceil, adds ceil(rrs) to the
+ *      context's exact 64-bit normalisation accumulator instead of rrs. ---- */
+int nrrs_infer(nrrs_ctx* ctx, const nrrs_vertex_soa* v, uint32_t n,
+               const nrrs_decide_params* p, float* stats, float* rrs, void* stream);
+
+/* ---- decision + emission on given factors: replaces calcSum2PassAsync<true> +
+ *      "Gen Tids" + TidQueue::push (integrator.cpp:1301-1460, commonworkqueue.h:19-25).
+ *      Sums rrs (or ceil(rrs)) exactly, forms nf = (budget - n_specular) / sum, scales,
+ *      draws s = int(r) + (rnd <= r - int(r)) and writes s copies of scatter_index[i] (or i)
+ *      to next_queue in vertex order. rrs_norm[stid] receives the normalised factor
+ *      (mScatterRayQueue->mRRS). split[i] receives s (may be NULL). n_specular_dev, when not
+ *      NULL, overrides n_specular from device memory. *next_size_dev receives the total;
+ *      writes at or past capacity are dropped and flagged. ---- */
+int nrrs_decide_emit(nrrs_ctx* ctx, const float* rrs, const float* rnd,
+                     const uint32_t* scatter_index, uint32_t n, uint32_t budget,
+                     uint32_t n_specular, const uint32_t* n_specular_dev,
+                     const nrrs_decide_params* p, float* rrs_norm, uint8_t* split,
+                     uint32_t* next_queue, uint32_t capacity, uint32_t* next_size_dev,
+                     void* stream);
+
+/* ---- fused: infer + decide + emit for one depth (generateRRSNumber<false,*>) ---- */
+int nrrs_step(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* rnd, uint32_t n,
+              uint32_t budget, uint32_t n_specular, const nrrs_decide_params* p,
+              float* stats, float* rrs, float* rrs_norm, uint8_t* split,
+              uint32_t* next_queue, uint32_t capacity, uint32_t* next_size_dev, void* stream);
+
+/* ---- batched uneven depths in one persistent launch sequence (graph-capturable).
+ *      segs is a HOST array of n_segs segments; next_size_dev[n_segs]. ---- */
+int nrrs_step_batched(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* rnd,
+                      const nrrs_segment* segs, int32_t n_segs, const nrrs_decide_params* p,
+                      float* stats, float* rrs, float* rrs_norm, uint8_t* split,
+                      uint32_t* next_queue, uint32_t* next_size_dev, void* stream);
+
+/* ---- training: replaces NRRSNetwork::train (network.cpp:196-295) with the two
+ *      tcnn training_step calls it makes. target is [n][3] radiance. loss_dev (may be
+ *      NULL) receives {statnet_loss, rrsnet_loss} as FP64 on the device. ---- */
+int nrrs_train_step(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* target,
+                    uint32_t n, double* loss_dev, void* stream);
+
+/* ---- parameters: FP32 master copy. Layout: [table | statnet W0..Wk | rrsnet V0..Vk],
+ *      each W row-major [out][in]. Pointers are HOST pointers (synchronous copies). ---- */
+uint64_t nrrs_param_count(const nrrs_ctx* ctx);
+int nrrs_param_layout(const nrrs_ctx* ctx, uint64_t* table_params, uint64_t* statnet_params,
+                      uint64_t* rrsnet_params);
+int nrrs_get_params(const nrrs_ctx* ctx, float* host_dst, uint64_t count);
+int nrrs_set_params(nrrs_ctx* ctx, const float* host_src, uint64_t count);
+/* gradients of the last nrrs_train_step (before the Adam update); host copy */
+int nrrs_get_grads(const nrrs_ctx* ctx, float* host_dst, uint64_t count);
+/* Adam step count and moments (host copies, count each) */
+int nrrs_get_adam_state(const nrrs_ctx* ctx, float* m, float* v, uint64_t count, uint64_t* t);
+/* level table: per level {offset (entries), entries, resolution, dense} as 4 uint32 */
+int nrrs_level_table(const nrrs_ctx* ctx, uint32_t* host_dst, int32_t max_levels);
+
+/* checkpoint: FP32 master weights, Adam m/v and step (loadWeights/saveWeights are stubs in
+ * the reference, network.cpp:157-194) */
+int nrrs_save(const nrrs_ctx* ctx, const char* path);
+int nrrs_load(nrrs_ctx* ctx, const char* path);
+
+/* ---- status: synchronises the stream, returns and clears the device status bits ---- */
+int nrrs_get_device_status(nrrs_ctx* ctx, uint32_t* flags, void* stream);
+
+/* ---- synthetic inputs (host, deterministic): mt19937_64 + explicit transforms. Buffers are
+ *      HOST arrays sized as in nrrs_vertex_soa; any may be NULL to skip. target [n][3]. ---- */
+void nrrs_synth_vertices(uint64_t seed, uint64_t first, uint64_t n, float* pos, float* wi,
+                         float* normal, float* roughness, float* albedo, float* thp,
+                         uint32_t* depth, float* rnd, float* ref_mean, float* target);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NRRS_B200_H */

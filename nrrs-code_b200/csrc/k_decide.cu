@@ -1,0 +1,233 @@
+// k_decide.cu -- RRS normalisation, kill/split decision and next-bounce queue emission.
+//
+// Replaces, in banbao990/NRRS-Code:
+//   calcSum2PassAsync<true>   src/render/common/commoncudautilshost.cpp:6-22
+//   SumTwoPassInterleaved...  src/render/common/commoncudautils.cu:144-181
+//   "Gen Tids" lambda         src/render/nrrs/integrator.cpp:1368-1460
+//   TidQueue::push(tid, cnt)  src/render/common/commonworkqueue.h:19-25 (+ pushCheck :34-42)
+//
+// The sum is exact: every term is a 64-bit fixed-point integer, so the order in which CTAs add
+// them does not change a bit (the reference's FP32 sum depends on the occupancy-chosen grid).
+// The emission is a single-pass prefix sum with decoupled look-back over 2048-vertex chunks:
+// chunks are taken in ticket order, so every predecessor of a waiting chunk has already
+// started and the wait ends; each wait is still bounded and reports NRRS_DEV_TIMEOUT.
+// The queue is in vertex order with the s copies of a vertex contiguous.
+#include "kernels.hpp"
+
+namespace nrrs {
+
+namespace {
+
+constexpr unsigned long long kFlagAgg = 1ull;
+constexpr unsigned long long kFlagIncl = 2ull;
+
+__device__ __forceinline__ unsigned long long pack_state(unsigned epoch, unsigned long long flag,
+                                                         unsigned value) {
+    return ((unsigned long long)(epoch & 0x3fffffffu) << 34) | (flag << 32) | value;
+}
+
+__device__ __forceinline__ unsigned long long load_state(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void store_state(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned sat_add(unsigned a, unsigned b) {
+    const unsigned s = a + b;
+    return s < a ? 0xffffffffu : s;
+}
+
+// s = int(r) + (rnd <= r - int(r)), with NaN -> 0 and a cap of 255 (flagged)
+__device__ __forceinline__ unsigned split_count(float r, float rnd, unsigned* flags) {
+    if (!(r == r)) { *flags |= NRRS_DEV_NAN; return 0; }
+    if (!(r < 256.0f)) { *flags |= NRRS_DEV_SATURATED; return 255; }
+    int s = (int)r;
+    const float frac = __fsub_rn(r, (float)s);
+    s += (rnd <= frac) ? 1 : 0;
+    if (s > 255) { *flags |= NRRS_DEV_SATURATED; s = 255; }
+    return (unsigned)s;
+}
+
+__global__ void __launch_bounds__(kDecThreads) k_decide(const __grid_constant__ DecideArgs a) {
+    __shared__ unsigned s_chunk, s_epoch, s_prefix;
+    __shared__ unsigned s_warp[kDecThreads / 32];
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        s_chunk = atomicAdd(&a.scr->ticket, 1u);
+        s_epoch = *(volatile unsigned*)&a.scr->epoch;
+    }
+    __syncthreads();
+    const unsigned c = s_chunk;
+    const unsigned epoch = s_epoch;
+    unsigned flags = 0;
+
+    if (c < a.segs.total_tiles) {
+        const int si = find_segment(a.segs, c);
+        const Segment& sg = a.segs.s[si];
+        const unsigned lc = c - sg.tile_start;
+        const unsigned base = sg.offset + lc * kDecChunk;
+        const unsigned end = sg.offset + min(sg.count, (lc + 1) * kDecChunk);
+
+        // normalisation factor, FP32 sequence of integrator.cpp:1376-1397
+        const long long acc = (long long)*(volatile unsigned long long*)&a.scr->sum_acc[si];
+        const float sumf = (float)((double)acc * a.inv_fixed_scale);
+        const float rcp = __fdiv_rn(1.0f, sumf);
+        const unsigned nspec = (a.n_spec_dev && si == 0) ? *a.n_spec_dev : sg.n_specular;
+        const float bud = (float)(unsigned)(sg.budget - nspec);
+        float nf = __fmul_rn(bud, rcp);
+        nf = __fmul_rn(nf, a.use_ceil ? 1.0f : a.normalize_rate);
+        const float scale = a.scale_up ? nf : (nf < 1.0f ? nf : 1.0f);
+
+        unsigned sv[kDecVPT];
+        unsigned st[kDecVPT];
+        unsigned local = 0;
+        const unsigned v0 = base + tid * kDecVPT;
+#pragma unroll
+        for (int j = 0; j < kDecVPT; ++j) {
+            const unsigned v = v0 + j;
+            sv[j] = 0;
+            st[j] = 0;
+            if (v < end) {
+                const float r = __fmul_rn(a.rrs[v], scale);
+                const unsigned stid = a.sidx ? a.sidx[v] : v;
+                if (a.rrs_norm) a.rrs_norm[stid] = r;
+                const unsigned s = split_count(r, a.rnd[v], &flags);
+                if (a.split) a.split[v] = (uint8_t)s;
+                sv[j] = s;
+                st[j] = stid;
+                local += s;
+            }
+        }
+
+        // block exclusive scan of the per-thread counts
+        const int lane = tid & 31, wid = tid >> 5;
+        unsigned incl = local;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) s_warp[wid] = incl;
+        __syncthreads();
+        if (wid == 0) {
+            unsigned w = lane < kDecThreads / 32 ? s_warp[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            if (lane < kDecThreads / 32) s_warp[lane] = w;  // inclusive warp prefix
+        }
+        __syncthreads();
+        const unsigned warp_excl = wid ? s_warp[wid - 1] : 0;
+        const unsigned thread_excl = warp_excl + incl - local;
+        const unsigned chunk_total = s_warp[kDecThreads / 32 - 1];
+
+        // decoupled look-back (one thread)
+        if (tid == 0) {
+            unsigned long long* states = a.states;
+            unsigned prefix = 0;
+            if (lc == 0) {
+                store_state(&states[c], pack_state(epoch, kFlagIncl, chunk_total));
+            } else {
+                store_state(&states[c], pack_state(epoch, kFlagAgg, chunk_total));
+                unsigned p = c - 1;
+                unsigned spins = 0;
+                bool timed_out = false;
+                for (;;) {
+                    const unsigned long long w = load_state(&states[p]);
+                    const unsigned we = (unsigned)(w >> 34);
+                    const unsigned long long wf = (w >> 32) & 3ull;
+                    if (we != (epoch & 0x3fffffffu) || wf == 0) {
+                        if (++spins > a.spin_limit) { timed_out = true; break; }
+                        __nanosleep(32);
+                        continue;
+                    }
+                    prefix = sat_add(prefix, (unsigned)w);
+                    if (wf == kFlagIncl || p == sg.tile_start) break;
+                    --p;
+                }
+                if (timed_out) flags |= NRRS_DEV_TIMEOUT;
+                store_state(&states[c], pack_state(epoch, kFlagIncl, sat_add(prefix, chunk_total)));
+            }
+            s_prefix = prefix;
+            if (c == sg.tile_start + (sg.count + kDecChunk - 1) / kDecChunk - 1)
+                a.next_size[si] = sat_add(prefix, chunk_total);
+        }
+        __syncthreads();
+
+        // emission: s copies of stid, vertex order, capacity-guarded
+        unsigned pos = s_prefix + thread_excl;
+        uint32_t* q = a.queue + sg.queue_offset;
+#pragma unroll
+        for (int j = 0; j < kDecVPT; ++j) {
+            for (unsigned k = 0; k < sv[j]; ++k, ++pos) {
+                if (pos < sg.queue_capacity) q[pos] = st[j];
+                else flags |= NRRS_DEV_OVERFLOW;
+            }
+        }
+    }
+
+    if (flags) atomicOr(&a.scr->status, flags);
+
+    // the last CTA restores the scratch for the next launch
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        const unsigned old = atomicAdd(&a.scr->done, 1u);
+        if (old == gridDim.x - 1) {
+            for (int k = 0; k < a.segs.n; ++k) {
+                if (a.segs.s[k].count == 0) a.next_size[k] = 0;
+                a.scr->sum_acc[k] = 0ull;
+            }
+            a.scr->ticket = 0;
+            a.scr->done = 0;
+            a.scr->epoch = a.scr->epoch + 1;
+            __threadfence();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kTile) k_sum(const __grid_constant__ SumArgs a) {
+    __shared__ long long s_part[kTile / 32];
+    unsigned flags = 0;
+    for (unsigned t = blockIdx.x; t < a.segs.total_tiles; t += gridDim.x) {
+        const int si = find_segment(a.segs, t);
+        const Segment& sg = a.segs.s[si];
+        const unsigned v = sg.offset + (t - sg.tile_start) * kTile + threadIdx.x;
+        long long term = 0;
+        if (v < sg.offset + sg.count) term = fixed_term(a.fp, a.rrs[v], &a.scr->status);
+        term = warp_sum_ll(term);
+        if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = term;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            long long tot = 0;
+#pragma unroll
+            for (int k = 0; k < kTile / 32; ++k) tot += s_part[k];
+            atomicAdd(&a.scr->sum_acc[si], (unsigned long long)tot);
+        }
+        __syncthreads();
+    }
+    (void)flags;
+}
+
+}  // namespace
+
+cudaError_t launch_decide(const DecideArgs& a, cudaStream_t s) {
+    if (a.segs.total_tiles == 0) return cudaSuccess;
+    k_decide<<<a.segs.total_tiles, kDecThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sum(const SumArgs& a, cudaStream_t s) {
+    if (a.segs.total_tiles == 0) return cudaSuccess;
+    const unsigned grid = a.segs.total_tiles < 148u * 8u ? a.segs.total_tiles : 148u * 8u;
+    k_sum<<<grid, kTile, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace nrrs

@@ -1,0 +1,124 @@
+// k_util.cu -- derived weight images and the FP16 table copy.
+//
+// The FP32 master weights are row-major W[out][in] per layer. Two derived images are rebuilt
+// after every optimizer step or parameter upload:
+//   * FP32 transposed Wt[in][out4] (out padded to a multiple of 4) for the SIMT path;
+//   * FP16/BF16 UMMA image: per layer an [Npad][K] K-major operand in the canonical
+//     no-swizzle core-matrix layout of tcgen05 (8 rows x 16 bytes per core matrix, adjacent
+//     K core matrices 128 B apart (LBO), adjacent 8-row groups K*16 B apart (SBO)).
+//     The output layers are padded to N = 16 rows with zeros.
+#include "kernels.hpp"
+
+namespace nrrs {
+
+namespace {
+
+struct LayerDesc {
+    int in, out;
+};
+
+__host__ __device__ inline int pad4(int x) { return (x + 3) / 4 * 4; }
+__host__ __device__ inline int npad16(int x) { return (x + 15) / 16 * 16; }
+
+// layer list of a network: in -> w (hidden) -> out
+__host__ __device__ inline LayerDesc layer_of(int in, int w, int hidden, int out, int l) {
+    LayerDesc d;
+    d.in = l == 0 ? in : w;
+    d.out = l == hidden ? out : w;
+    return d;
+}
+
+// element offset of (n, k) in a K-major core-matrix image with K columns
+__host__ __device__ inline size_t umma_offset(int n, int k, int K) {
+    return (size_t)(n >> 3) * (size_t)(K * 8) + (size_t)(k >> 3) * 64 + (size_t)(n & 7) * 8 +
+           (size_t)(k & 7);
+}
+
+struct PackArgs {
+    const float* master;
+    float* wt;
+    void* wpack;
+    int ws, hs, wr, hr, prec;
+};
+
+__global__ void k_pack(PackArgs a) {
+    // one thread per (network, layer, n, k) of the padded images; grid-stride
+    const int nets = 2;
+    size_t mofs = 0, tofs = 0, pofs = 0;
+    for (int net = 0; net < nets; ++net) {
+        const int in = net == 0 ? kStatIn : kRrsIn;
+        const int w = net == 0 ? a.ws : a.wr;
+        const int h = net == 0 ? a.hs : a.hr;
+        const int out = net == 0 ? kStatOut : 1;
+        for (int l = 0; l <= h; ++l) {
+            const LayerDesc d = layer_of(in, w, h, out, l);
+            const int op4 = pad4(d.out);
+            const int np = l == h ? npad16(d.out) : d.out;
+            const size_t cells = (size_t)np * d.in;
+            for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < cells;
+                 e += (size_t)gridDim.x * blockDim.x) {
+                const int n = (int)(e / d.in), k = (int)(e % d.in);
+                const float v = n < d.out ? a.master[mofs + (size_t)n * d.in + k] : 0.f;
+                if (n < op4) a.wt[tofs + (size_t)k * op4 + n] = v;
+                if (a.wpack) {
+                    const size_t o = pofs + umma_offset(n, k, d.in);
+                    if (a.prec == NRRS_PREC_BF16)
+                        reinterpret_cast<__nv_bfloat16*>(a.wpack)[o] = __float2bfloat16_rn(v);
+                    else
+                        reinterpret_cast<__half*>(a.wpack)[o] = __float2half_rn(v);
+                }
+            }
+            mofs += (size_t)d.out * d.in;
+            tofs += (size_t)d.in * op4;
+            pofs += cells;
+        }
+    }
+}
+
+__global__ void k_table_half(const float* t, __half* h, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        h[i] = __float2half_rn(t[i]);
+}
+
+}  // namespace
+
+size_t transposed_weight_floats(int ws, int hs, int wr, int hr) {
+    size_t t = 0;
+    for (int l = 0; l <= hs; ++l) {
+        LayerDesc d = layer_of(kStatIn, ws, hs, kStatOut, l);
+        t += (size_t)d.in * pad4(d.out);
+    }
+    for (int l = 0; l <= hr; ++l) {
+        LayerDesc d = layer_of(kRrsIn, wr, hr, 1, l);
+        t += (size_t)d.in * pad4(d.out);
+    }
+    return t;
+}
+
+size_t packed_weight_bytes(int ws, int hs, int wr, int hr) {
+    size_t t = 0;
+    for (int l = 0; l <= hs; ++l) {
+        LayerDesc d = layer_of(kStatIn, ws, hs, kStatOut, l);
+        t += (size_t)(l == hs ? npad16(d.out) : d.out) * d.in;
+    }
+    for (int l = 0; l <= hr; ++l) {
+        LayerDesc d = layer_of(kRrsIn, wr, hr, 1, l);
+        t += (size_t)(l == hr ? npad16(d.out) : d.out) * d.in;
+    }
+    return t * 2;
+}
+
+cudaError_t launch_pack_weights(const float* master_mlp, float* wt, void* wpack, int ws, int hs,
+                                int wr, int hr, int prec, cudaStream_t s) {
+    PackArgs a{master_mlp, wt, wpack, ws, hs, wr, hr, prec};
+    k_pack<<<64, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_table_to_half(const float* t, __half* h, size_t n, cudaStream_t s) {
+    k_table_half<<<148 * 4, 256, 0, s>>>(t, h, n);
+    return cudaGetLastError();
+}
+
+}  // namespace nrrs

@@ -1,0 +1,73 @@
+// kernels.hpp -- host-side launch wrappers of the NRRS kernels (internal to libnrrs_b200).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "nrrs_common.cuh"
+
+namespace nrrs {
+
+constexpr int kDecThreads = 256;
+constexpr int kDecVPT = 8;
+constexpr int kDecChunk = kDecThreads * kDecVPT;  // vertices per decision chunk
+
+struct DecideArgs {
+    const float* rrs;
+    const float* rnd;
+    const uint32_t* sidx;
+    float* rrs_norm;
+    uint8_t* split;
+    uint32_t* queue;
+    uint32_t* next_size;          // [n segments]
+    const uint32_t* n_spec_dev;   // optional override of segment 0's n_specular
+    DecideScratch* scr;
+    unsigned long long* states;   // one look-back word per chunk
+    SegmentTable segs;            // tile_start counts decision chunks
+    float normalize_rate;
+    int32_t use_ceil;
+    int32_t scale_up;
+    double inv_fixed_scale;
+    uint32_t spin_limit;
+};
+
+struct SumArgs {
+    const float* rrs;
+    DecideScratch* scr;
+    SegmentTable segs;            // tile_start counts sum tiles (kTile vertices)
+    FactorParams fp;
+};
+
+struct InferArgs {
+    VertexPtrs v;
+    EncodeParams enc;
+    FactorParams fp;
+    SegmentTable segs;            // tile_start counts kTile-vertex tiles
+    const float* table;           // FP32 table [rows][2]   (FP32 path)
+    const __half* table_h;        // FP16 table [rows][2]   (mixed path)
+    const float* wt_stat;         // transposed FP32 StatNet weights (FP32 path)
+    const float* wt_rrs;          // transposed FP32 RRSNet weights
+    const void* wpack;            // packed UMMA weights (mixed path)
+    float* stats;                 // [n][3] optional
+    float* rrs;                   // [n]
+    DecideScratch* scr;           // accumulate the exact sum when not null
+};
+
+// decision + emission (single pass, decoupled look-back)
+cudaError_t launch_decide(const DecideArgs& a, cudaStream_t s);
+// exact sum of rrs (or ceil) per segment into scr->sum_acc
+cudaError_t launch_sum(const SumArgs& a, cudaStream_t s);
+// FP32 SIMT inference
+cudaError_t launch_infer_fp32(const InferArgs& a, int ws, int hs, int wr, int hr, int sm_count,
+                              cudaStream_t s);
+// tcgen05 mixed-precision inference
+cudaError_t launch_infer_tc(const InferArgs& a, int ws, int hs, int wr, int hr, int prec,
+                            int sm_count, int ctas_per_sm, cudaStream_t s);
+size_t infer_tc_smem_bytes(int ws, int hs, int wr, int hr);
+// derived weight copies: FP32 transposed and the UMMA-packed FP16/BF16 images
+cudaError_t launch_pack_weights(const float* master_mlp, float* wt, void* wpack, int ws, int hs,
+                                int wr, int hr, int prec, cudaStream_t s);
+size_t packed_weight_bytes(int ws, int hs, int wr, int hr);
+size_t transposed_weight_floats(int ws, int hs, int wr, int hr);
+// FP32 table -> FP16 copy
+cudaError_t launch_table_to_half(const float* t, __half* h, size_t n, cudaStream_t s);
+
+}  // namespace nrrs

@@ -1,0 +1,669 @@
+// nrrs_api.cu -- the C-ABI of libnrrs_b200 (declared in include/nrrs.h).
+//
+// Host orchestration of the NRRS hot path. Each entry point validates its arguments, builds a
+// by-value kernel argument block and enqueues kernels on the caller's stream; nothing here
+// synchronises except the calls documented as synchronous. There is no CPU fallback: on a
+// machine without an sm_100 device nrrs_create returns NRRS_ERR_NO_DEVICE.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "context.hpp"
+
+using namespace nrrs;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+int fail(nrrs_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->last_error = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+int cuda_fail(nrrs_ctx* ctx, cudaError_t e, const char* where) {
+    return fail(ctx, NRRS_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+uint64_t splitmix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+// Level table of the Instant-NGP grid: N_l = floor(N_min * b^l), dense when (N_l+1)^3 <= T.
+uint64_t build_levels(const nrrs_config& c, EncodeParams& e) {
+    const uint64_t T = 1ull << c.log2_hashmap_size;
+    uint64_t off = 0;
+    for (int l = 0; l < c.n_levels; ++l) {
+        const uint32_t N =
+            (uint32_t)std::floor((double)c.base_resolution * std::pow((double)c.per_level_scale, (double)l));
+        const uint64_t R = (uint64_t)N + 1;
+        const uint64_t dense_n = R * R * R;
+        e.lv[l].res = N;
+        e.lv[l].dense = dense_n <= T;
+        e.lv[l].offset = (uint32_t)off;
+        e.lv[l].pad = 0;
+        off += e.lv[l].dense ? dense_n : T;
+    }
+    e.n_levels = (uint32_t)c.n_levels;
+    e.hash_mask = (uint32_t)(T - 1);
+    return off;
+}
+
+// normalizeSpatialCoord's AABB terms (nrctrain.h:111-115), FP32 on the host
+void aabb_terms(const nrrs_config& c, EncodeParams& e) {
+    e.normalize = c.normalize_pos;
+    float dg[3];
+    for (int d = 0; d < 3; ++d) dg[d] = c.aabb_max[d] - c.aabb_min[d];
+    const float inflate = sqrtf(dg[0] * dg[0] + dg[1] * dg[1] + dg[2] * dg[2]) * 0.005f;
+    for (int d = 0; d < 3; ++d) {
+        const float lo = c.aabb_min[d] - inflate, hi = c.aabb_max[d] + inflate;
+        e.center[d] = (lo + hi) * 0.5f;
+        e.diag[d] = hi - lo;
+    }
+}
+
+uint64_t mlp_params(int in, int w, int h, int out) {
+    return (uint64_t)in * w + (uint64_t)(h - 1) * w * w + (uint64_t)w * out;
+}
+
+// shift of the exact fixed-point normalisation sum: n * vmax < 2^(62 - shift), capped at 40
+int sum_shift(uint64_t n, float vmax) {
+    const double prod = (double)(n ? n : 1) * (double)(vmax > 1.f ? vmax : 1.f);
+    int e = 0;
+    std::frexp(prod, &e);
+    const int s = 62 - e;
+    return s > 40 ? 40 : s;
+}
+
+// The shift depends only on the context capacity and the clamp, so a depth gives the same
+// decisions whether it runs alone, batched, or sharded.
+FactorParams factor_params(const nrrs_ctx* ctx, const nrrs_decide_params* p) {
+    const uint64_t n = ctx->cfg.max_queue;
+    FactorParams f{};
+    f.clamp_min = p->clamp_min;
+    f.clamp_max = p->clamp_max;
+    f.ww = p->weight_window_size;
+    f.use_ww = p->use_weight_window;
+    f.use_ceil = p->use_ceil;
+    f.source = p->factor_source;
+    f.stat_eps = ctx->cfg.stat_eps;
+    f.ref_eps = ctx->cfg.ref_eps;
+    f.vmax = p->use_ceil ? ceilf(p->clamp_max) : p->clamp_max;
+    f.fixed_scale = std::ldexp(1.0, sum_shift(n, f.vmax));
+    return f;
+}
+
+int check_decide_params(nrrs_ctx* ctx, const nrrs_decide_params* p, uint64_t n_total) {
+    if (!p) return fail(ctx, NRRS_ERR_INVALID_ARG, "decide params are NULL");
+    if (!(p->clamp_min >= 0.f) || !(p->clamp_max >= p->clamp_min) || !std::isfinite(p->clamp_max))
+        return fail(ctx, NRRS_ERR_INVALID_ARG, "need 0 <= clamp_min <= clamp_max < inf");
+    if (p->factor_source != NRRS_FACTOR_ADRRS && p->factor_source != NRRS_FACTOR_RRSNET)
+        return fail(ctx, NRRS_ERR_INVALID_ARG, "factor_source must be 2 (ADRRS) or 3 (RRSNet)");
+    (void)n_total;
+    if (sum_shift(ctx->cfg.max_queue, p->use_ceil ? ceilf(p->clamp_max) : p->clamp_max) < 16)
+        return fail(ctx, NRRS_ERR_UNSUPPORTED, "n * clamp_max too large for the exact sum");
+    return NRRS_OK;
+}
+
+int check_vertices(nrrs_ctx* ctx, const nrrs_vertex_soa* v) {
+    if (!v || !v->pos || !v->wi || !v->normal || !v->roughness || !v->albedo || !v->thp)
+        return fail(ctx, NRRS_ERR_INVALID_ARG, "vertex SoA: pos/wi/normal/roughness/albedo/thp required");
+    return NRRS_OK;
+}
+
+VertexPtrs vptrs(const nrrs_vertex_soa* v) {
+    VertexPtrs p{};
+    p.pos = v->pos; p.wi = v->wi; p.normal = v->normal; p.rough = v->roughness;
+    p.albedo = v->albedo; p.thp = v->thp; p.depth = v->depth; p.ref = v->ref_mean;
+    p.sidx = v->scatter_index;
+    return p;
+}
+
+// segment table in units of `unit` vertices per tile
+SegmentTable make_segments(const nrrs_segment* segs, int n, uint32_t unit) {
+    SegmentTable t{};
+    t.n = n;
+    uint32_t tiles = 0;
+    for (int k = 0; k < n; ++k) {
+        t.s[k].offset = segs[k].offset;
+        t.s[k].count = segs[k].count;
+        t.s[k].tile_start = tiles;
+        t.s[k].budget = segs[k].budget;
+        t.s[k].n_specular = segs[k].n_specular;
+        t.s[k].queue_offset = segs[k].queue_offset;
+        t.s[k].queue_capacity = segs[k].queue_capacity;
+        tiles += (segs[k].count + unit - 1) / unit;
+    }
+    t.total_tiles = tiles;
+    return t;
+}
+
+int refresh_derived(nrrs_ctx* ctx, cudaStream_t s) {
+    const nrrs_config& c = ctx->cfg;
+    cudaError_t e = launch_pack_weights(ctx->params + ctx->n_table, ctx->wt, ctx->wpack,
+                                        c.statnet_width, c.statnet_hidden, c.rrsnet_width,
+                                        c.rrsnet_hidden, c.precision, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "pack weights");
+    if (ctx->table_h) {
+        e = launch_table_to_half(ctx->params, ctx->table_h, ctx->n_table, s);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "table to half");
+    }
+    return NRRS_OK;
+}
+
+int run_infer(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const SegmentTable& segs,
+              const nrrs_decide_params* p, uint64_t n_total, float* stats, float* rrs,
+              bool accumulate, cudaStream_t s) {
+    InferArgs a{};
+    a.v = vptrs(v);
+    a.enc = ctx->enc;
+    a.fp = factor_params(ctx, p);
+    a.segs = segs;
+    a.table = ctx->params;
+    a.table_h = ctx->table_h;
+    a.wt_stat = ctx->wt;
+    a.wt_rrs = ctx->wt + ctx->wt_rrs_offset;
+    a.wpack = ctx->wpack;
+    a.stats = stats;
+    a.rrs = rrs;
+    a.scr = accumulate ? ctx->scr : nullptr;
+    const nrrs_config& c = ctx->cfg;
+    cudaError_t e;
+    if (c.precision == NRRS_PREC_FP32)
+        e = launch_infer_fp32(a, c.statnet_width, c.statnet_hidden, c.rrsnet_width,
+                              c.rrsnet_hidden, ctx->sm_count, s);
+    else
+        e = launch_infer_tc(a, c.statnet_width, c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden,
+                            c.precision, ctx->sm_count, ctx->tc_ctas_per_sm, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "inference launch");
+    return NRRS_OK;
+}
+
+int run_decide(nrrs_ctx* ctx, const float* rrs, const float* rnd, const uint32_t* sidx,
+               const nrrs_segment* segs, int n_segs, uint64_t n_total,
+               const uint32_t* n_spec_dev, const nrrs_decide_params* p, float* rrs_norm,
+               uint8_t* split, uint32_t* queue, uint32_t* next_size, bool need_sum,
+               cudaStream_t s) {
+    const FactorParams fp = factor_params(ctx, p);
+    if (need_sum) {
+        SumArgs sa{};
+        sa.rrs = rrs;
+        sa.scr = ctx->scr;
+        sa.segs = make_segments(segs, n_segs, kTile);
+        sa.fp = fp;
+        cudaError_t e = launch_sum(sa, s);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "sum launch");
+    }
+    DecideArgs d{};
+    d.rrs = rrs;
+    d.rnd = rnd;
+    d.sidx = sidx;
+    d.rrs_norm = rrs_norm;
+    d.split = split;
+    d.queue = queue;
+    d.next_size = next_size;
+    d.n_spec_dev = n_spec_dev;
+    d.scr = ctx->scr;
+    d.states = ctx->states;
+    d.segs = make_segments(segs, n_segs, kDecChunk);
+    d.normalize_rate = p->normalize_rate;
+    d.use_ceil = p->use_ceil;
+    d.scale_up = p->scale_up;
+    d.inv_fixed_scale = 1.0 / fp.fixed_scale;
+    d.spin_limit = 1u << 22;
+    if (d.segs.total_tiles > ctx->max_chunks)
+        return fail(ctx, NRRS_ERR_INVALID_ARG, "too many decision chunks for max_queue");
+    if (d.segs.total_tiles == 0) {
+        cudaError_t e = cudaMemsetAsync(next_size, 0, sizeof(uint32_t) * n_segs, s);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "memset next_size");
+        return NRRS_OK;
+    }
+    cudaError_t e = launch_decide(d, s);
+    if (e != cudaSuccess) {
+        cudaMemsetAsync(ctx->scr, 0, offsetof(DecideScratch, epoch), s);
+        return cuda_fail(ctx, e, "decide launch");
+    }
+    return NRRS_OK;
+}
+
+void xavier_fill(std::vector<float>& h, uint64_t ofs, int in, int w, int hidden, int out,
+                 uint64_t seed, uint64_t salt) {
+    for (int l = 0; l <= hidden; ++l) {
+        const int li = l == 0 ? in : w;
+        const int lo = l == hidden ? out : w;
+        std::mt19937_64 eng(splitmix64(seed ^ splitmix64(salt + (uint64_t)l)));
+        const double a = std::sqrt(6.0 / (double)(li + lo));
+        for (uint64_t k = 0; k < (uint64_t)li * lo; ++k) {
+            const double u = (double)(eng() >> 11) * (1.0 / 9007199254740992.0);
+            h[ofs + k] = (float)((2.0 * u - 1.0) * a);
+        }
+        ofs += (uint64_t)li * lo;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void nrrs_config_default(nrrs_config* c) {
+    std::memset(c, 0, sizeof(*c));
+    c->n_levels = 16;
+    c->n_features_per_level = 2;
+    c->log2_hashmap_size = 19;
+    c->base_resolution = 16;
+    c->per_level_scale = 1.5f;
+    c->sh_degree = 4;
+    c->statnet_width = 64;
+    c->statnet_hidden = 2;
+    c->rrsnet_width = 64;
+    c->rrsnet_hidden = 2;
+    c->precision = NRRS_PREC_FP32;
+    c->seed = 0;
+    c->table_init_scale = 1e-4f;
+    c->lr = 1e-2f;
+    c->beta1 = 0.9f;
+    c->beta2 = 0.99f;
+    c->eps = 1e-15f;
+    c->l2_reg = 0.f;
+    c->stat_eps = 0.01f;
+    c->ref_eps = 0.01f;
+    c->loss_clamp_max = 10.f;
+    c->cost_offset = 1.f;
+    c->normalize_pos = 0;
+    for (int d = 0; d < 3; ++d) { c->aabb_min[d] = 0.f; c->aabb_max[d] = 1.f; }
+    c->max_queue = 1u << 20;
+    c->max_train = 1u << 18;
+    c->step = 3;
+}
+
+void nrrs_decide_params_default(nrrs_decide_params* p) {
+    // the reference's shipped decision settings (common/configs/nrrs/render/test.json:63-67:
+    // clamp_min 0.05, normalize_rate 0.85, use_ceil true, donnot_normalize_when_less_than_one
+    // true) with the split cap of the benchmark workload (8 instead of 20)
+    p->clamp_min = 0.05f;
+    p->clamp_max = 8.0f;
+    p->normalize_rate = 0.85f;
+    p->use_ceil = 1;
+    p->scale_up = 0;
+    p->use_weight_window = 0;
+    p->weight_window_size = 5.0f;
+    p->factor_source = NRRS_FACTOR_RRSNET;
+}
+
+const char* nrrs_status_string(int s) {
+    switch (s) {
+        case NRRS_OK: return "ok";
+        case NRRS_ERR_INVALID_ARG: return "invalid argument";
+        case NRRS_ERR_CAPACITY_OVERFLOW: return "capacity overflow";
+        case NRRS_ERR_NAN: return "non-finite value";
+        case NRRS_ERR_TIMEOUT: return "device wait timed out";
+        case NRRS_ERR_CUDA: return "CUDA error";
+        case NRRS_ERR_NO_DEVICE: return "no sm_100 device";
+        case NRRS_ERR_UNSUPPORTED: return "unsupported configuration";
+        case NRRS_ERR_IO: return "file I/O error";
+        default: return "unknown status";
+    }
+}
+
+const char* nrrs_last_error(const nrrs_ctx* ctx) {
+    return ctx ? ctx->last_error.c_str() : g_create_error.c_str();
+}
+
+int nrrs_device_available(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) { cudaGetLastError(); return 0; }
+    int dev = 0, major = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    return major == 10 ? 1 : 0;
+}
+
+int nrrs_create(const nrrs_config* cfg, nrrs_ctx** out) {
+    if (!cfg || !out) return fail(nullptr, NRRS_ERR_INVALID_ARG, "NULL argument");
+    *out = nullptr;
+    const nrrs_config& c = *cfg;
+    if (c.n_levels != 16 || c.n_features_per_level != 2)
+        return fail(nullptr, NRRS_ERR_UNSUPPORTED, "hash grid needs 16 levels x 2 features (32 lanes)");
+    if (c.sh_degree != 4) return fail(nullptr, NRRS_ERR_UNSUPPORTED, "sh_degree must be 4");
+    if (c.log2_hashmap_size < 10 || c.log2_hashmap_size > 24 || c.base_resolution < 2 ||
+        !(c.per_level_scale >= 1.0f))
+        return fail(nullptr, NRRS_ERR_INVALID_ARG, "bad hash-grid parameters");
+    const bool w64 = c.statnet_width == 64 && c.rrsnet_width == 64 && c.statnet_hidden == c.rrsnet_hidden &&
+                     (c.statnet_hidden == 2 || c.statnet_hidden == 3);
+    const bool w128 = c.statnet_width == 128 && c.rrsnet_width == 128 && c.statnet_hidden == 3 &&
+                      c.rrsnet_hidden == 3;
+    if (!w64 && !w128)
+        return fail(nullptr, NRRS_ERR_UNSUPPORTED, "networks: 64 wide x 2|3 hidden or 128 wide x 3 hidden");
+    if (c.precision < NRRS_PREC_FP32 || c.precision > NRRS_PREC_BF16)
+        return fail(nullptr, NRRS_ERR_INVALID_ARG, "bad precision");
+    if (c.max_queue == 0 || c.max_train == 0)
+        return fail(nullptr, NRRS_ERR_INVALID_ARG, "max_queue and max_train must be > 0");
+    if (!nrrs_device_available())
+        return fail(nullptr, NRRS_ERR_NO_DEVICE, "no sm_100 CUDA device (this library has no CPU path)");
+
+    nrrs_ctx* ctx = new nrrs_ctx();
+    ctx->cfg = c;
+    cudaGetDevice(&ctx->device);
+    cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, ctx->device);
+    ctx->table_rows = build_levels(c, ctx->enc);
+    aabb_terms(c, ctx->enc);
+    ctx->n_table = ctx->table_rows * 2;
+    ctx->n_stat = mlp_params(kStatIn, c.statnet_width, c.statnet_hidden, kStatOut);
+    ctx->n_rrs = mlp_params(kRrsIn, c.rrsnet_width, c.rrsnet_hidden, 1);
+    ctx->n_params = ctx->n_table + ctx->n_stat + ctx->n_rrs;
+    ctx->wt_floats = transposed_weight_floats(c.statnet_width, c.statnet_hidden, c.rrsnet_width,
+                                              c.rrsnet_hidden);
+    ctx->wt_rrs_offset = 0;
+    for (int l = 0; l <= c.statnet_hidden; ++l) {
+        const int li = l == 0 ? kStatIn : c.statnet_width;
+        const int lo = l == c.statnet_hidden ? kStatOut : c.statnet_width;
+        ctx->wt_rrs_offset += (size_t)li * ((lo + 3) / 4 * 4);
+    }
+    ctx->wpack_bytes = packed_weight_bytes(c.statnet_width, c.statnet_hidden, c.rrsnet_width,
+                                           c.rrsnet_hidden);
+    ctx->max_chunks = (c.max_queue + kDecChunk - 1) / kDecChunk + kMaxSegments;
+
+    cudaError_t e;
+    const size_t pb = sizeof(float) * ctx->n_params;
+#define NRRS_ALLOC(ptr, bytes)                                                         \
+    do {                                                                               \
+        e = cudaMalloc((void**)&(ptr), (bytes));                                       \
+        if (e != cudaSuccess) {                                                        \
+            nrrs_destroy(ctx);                                                         \
+            return fail(nullptr, NRRS_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e)); \
+        }                                                                              \
+    } while (0)
+    NRRS_ALLOC(ctx->params, pb);
+    NRRS_ALLOC(ctx->grads, pb);
+    NRRS_ALLOC(ctx->adam_m, pb);
+    NRRS_ALLOC(ctx->adam_v, pb);
+    NRRS_ALLOC(ctx->wt, sizeof(float) * ctx->wt_floats);
+    if (c.precision != NRRS_PREC_FP32) {
+        NRRS_ALLOC(ctx->table_h, sizeof(__half) * ctx->n_table);
+        NRRS_ALLOC(ctx->wpack, ctx->wpack_bytes);
+    }
+    const size_t scr_bytes = sizeof(DecideScratch) + sizeof(unsigned long long) * ctx->max_chunks;
+    NRRS_ALLOC(ctx->scr, scr_bytes);
+    ctx->states = reinterpret_cast<unsigned long long*>(ctx->scr + 1);
+    NRRS_ALLOC(ctx->loss_dev, sizeof(double) * 2);
+    ctx->train_scratch_bytes = train_scratch_bytes(c, c.max_train, ctx->sm_count);
+    NRRS_ALLOC(ctx->train_scratch, ctx->train_scratch_bytes);
+#undef NRRS_ALLOC
+
+    // parameters: table ~ U(-s, s), MLPs Xavier-uniform (seeded, host side)
+    std::vector<float> h(ctx->n_params);
+    {
+        std::mt19937_64 eng(splitmix64(c.seed ^ 0x7461626c65ull));
+        for (uint64_t k = 0; k < ctx->n_table; ++k) {
+            const double u = (double)(eng() >> 11) * (1.0 / 9007199254740992.0);
+            h[k] = (float)((2.0 * u - 1.0) * c.table_init_scale);
+        }
+    }
+    xavier_fill(h, ctx->n_table, kStatIn, c.statnet_width, c.statnet_hidden, kStatOut, c.seed, 100);
+    xavier_fill(h, ctx->n_table + ctx->n_stat, kRrsIn, c.rrsnet_width, c.rrsnet_hidden, 1, c.seed, 200);
+    e = cudaMemcpy(ctx->params, h.data(), pb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(ctx->grads, 0, pb);
+    if (e == cudaSuccess) e = cudaMemset(ctx->adam_m, 0, pb);
+    if (e == cudaSuccess) e = cudaMemset(ctx->adam_v, 0, pb);
+    if (e == cudaSuccess) e = cudaMemset(ctx->scr, 0, scr_bytes);
+    if (e == cudaSuccess) {
+        const unsigned one = 1;
+        e = cudaMemcpy(&ctx->scr->epoch, &one, sizeof(one), cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) e = cudaMemset(ctx->loss_dev, 0, sizeof(double) * 2);
+    if (e != cudaSuccess) {
+        nrrs_destroy(ctx);
+        return fail(nullptr, NRRS_ERR_CUDA, std::string("init: ") + cudaGetErrorString(e));
+    }
+    int rc = refresh_derived(ctx, 0);
+    if (rc == NRRS_OK) {
+        e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "init sync");
+    }
+    if (rc != NRRS_OK) {
+        g_create_error = ctx->last_error;
+        nrrs_destroy(ctx);
+        return rc;
+    }
+    *out = ctx;
+    return NRRS_OK;
+}
+
+void nrrs_destroy(nrrs_ctx* ctx) {
+    if (!ctx) return;
+    cudaFree(ctx->params);
+    cudaFree(ctx->grads);
+    cudaFree(ctx->adam_m);
+    cudaFree(ctx->adam_v);
+    cudaFree(ctx->table_h);
+    cudaFree(ctx->wt);
+    cudaFree(ctx->wpack);
+    cudaFree(ctx->scr);
+    cudaFree(ctx->loss_dev);
+    cudaFree(ctx->train_scratch);
+    delete ctx;
+}
+
+int nrrs_set_step(nrrs_ctx* ctx, int32_t step) {
+    if (!ctx) return NRRS_ERR_INVALID_ARG;
+    if (step < 0 || step > 3) return fail(ctx, NRRS_ERR_INVALID_ARG, "step must be 0..3");
+    ctx->cfg.step = step;
+    return NRRS_OK;
+}
+
+int nrrs_infer(nrrs_ctx* ctx, const nrrs_vertex_soa* v, uint32_t n, const nrrs_decide_params* p,
+               float* stats, float* rrs, void* stream) {
+    if (!ctx) return NRRS_ERR_INVALID_ARG;
+    int rc = check_vertices(ctx, v);
+    if (rc) return rc;
+    if ((rc = check_decide_params(ctx, p, n))) return rc;
+    if (!rrs) return fail(ctx, NRRS_ERR_INVALID_ARG, "rrs output is NULL");
+    if (n > ctx->cfg.max_queue) return fail(ctx, NRRS_ERR_INVALID_ARG, "n > max_queue");
+    if (n == 0) return NRRS_OK;
+    nrrs_segment sg{0, n, 0, 0, 0, 0};
+    return run_infer(ctx, v, make_segments(&sg, 1, kTile), p, n, stats, rrs, false,
+                     (cudaStream_t)stream);
+}
+
+int nrrs_decide_emit(nrrs_ctx* ctx, const float* rrs, const float* rnd,
+                     const uint32_t* scatter_index, uint32_t n, uint32_t budget,
+                     uint32_t n_specular, const uint32_t* n_specular_dev,
+                     const nrrs_decide_params* p, float* rrs_norm, uint8_t* split,
+                     uint32_t* next_queue, uint32_t capacity, uint32_t* next_size_dev,
+                     void* stream) {
+    if (!ctx) return NRRS_ERR_INVALID_ARG;
+    int rc = check_decide_params(ctx, p, n);
+    if (rc) return rc;
+    if (n && (!rrs || !rnd)) return fail(ctx, NRRS_ERR_INVALID_ARG, "rrs/rnd are NULL");
+    if (!next_size_dev || (capacity && !next_queue))
+        return fail(ctx, NRRS_ERR_INVALID_ARG, "next_queue/next_size are NULL");
+    if (n > ctx->cfg.max_queue) return fail(ctx, NRRS_ERR_INVALID_ARG, "n > max_queue");
+    nrrs_segment sg{0, n, budget, n_specular, 0, capacity};
+    return run_decide(ctx, rrs, rnd, scatter_index, &sg, 1, n, n_specular_dev, p, rrs_norm, split,
+                      next_queue, next_size_dev, true, (cudaStream_t)stream);
+}
+
+int nrrs_step(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* rnd, uint32_t n,
+              uint32_t budget, uint32_t n_specular, const nrrs_decide_params* p, float* stats,
+              float* rrs, float* rrs_norm, uint8_t* split, uint32_t* next_queue,
+              uint32_t capacity, uint32_t* next_size_dev, void* stream) {
+    if (!ctx) return NRRS_ERR_INVALID_ARG;
+    int rc = check_vertices(ctx, v);
+    if (rc) return rc;
+    if ((rc = check_decide_params(ctx, p, n))) return rc;
+    if (!rrs || (n && !rnd) || !next_size_dev || (capacity && !next_queue))
+        return fail(ctx, NRRS_ERR_INVALID_ARG, "rrs/rnd/next_queue/next_size NULL");
+    if (n > ctx->cfg.max_queue) return fail(ctx, NRRS_ERR_INVALID_ARG, "n > max_queue");
+    cudaStream_t s = (cudaStream_t)stream;
+    nrrs_segment sg{0, n, budget, n_specular, 0, capacity};
+    if (n) {
+        rc = run_infer(ctx, v, make_segments(&sg, 1, kTile), p, n, stats, rrs, true, s);
+        if (rc) return rc;
+    }
+    return run_decide(ctx, rrs, rnd, v->scatter_index, &sg, 1, n, nullptr, p, rrs_norm, split,
+                      next_queue, next_size_dev, false, s);
+}
+
+int nrrs_step_batched(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* rnd,
+                      const nrrs_segment* segs, int32_t n_segs, const nrrs_decide_params* p,
+                      float* stats, float* rrs, float* rrs_norm, uint8_t* split,
+                      uint32_t* next_queue, uint32_t* next_size_dev, void* stream) {
+    if (!ctx) return NRRS_ERR_INVALID_ARG;
+    if (!segs || n_segs < 1 || n_segs > kMaxSegments)
+        return fail(ctx, NRRS_ERR_INVALID_ARG, "1..16 segments required");
+    int rc = check_vertices(ctx, v);
+    if (rc) return rc;
+    uint64_t n_total = 0, n_max = 0;
+    for (int k = 0; k < n_segs; ++k) {
+        n_total += segs[k].count;
+        n_max = segs[k].count > n_max ? segs[k].count : n_max;
+        if (segs[k].queue_capacity && !next_queue)
+            return fail(ctx, NRRS_ERR_INVALID_ARG, "next_queue is NULL");
+    }
+    if ((rc = check_decide_params(ctx, p, n_max))) return rc;
+    if (n_total > ctx->cfg.max_queue) return fail(ctx, NRRS_ERR_INVALID_ARG, "sum of counts > max_queue");
+    if (!rrs || !rnd || !next_size_dev) return fail(ctx, NRRS_ERR_INVALID_ARG, "rrs/rnd/next_size NULL");
+    cudaStream_t s = (cudaStream_t)stream;
+    // the exact-sum scale is shared by all segments: use the largest segment
+    rc = run_infer(ctx, v, make_segments(segs, n_segs, kTile), p, n_max, stats, rrs, true, s);
+    if (rc) return rc;
+    return run_decide(ctx, rrs, rnd, v->scatter_index, segs, n_segs, n_max, nullptr, p, rrs_norm,
+                      split, next_queue, next_size_dev, false, s);
+}
+
+int nrrs_train_step(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* target, uint32_t n,
+                    double* loss_dev, void* stream) {
+    if (!ctx) return NRRS_ERR_INVALID_ARG;
+    int rc = check_vertices(ctx, v);
+    if (rc) return rc;
+    if (!target) return fail(ctx, NRRS_ERR_INVALID_ARG, "target is NULL");
+    if (n == 0 || n > ctx->cfg.max_train) return fail(ctx, NRRS_ERR_INVALID_ARG, "need 0 < n <= max_train");
+    rc = train_step_impl(ctx, vptrs(v), target, n, loss_dev, (cudaStream_t)stream);
+    if (rc) return rc;
+    return refresh_derived(ctx, (cudaStream_t)stream);
+}
+
+uint64_t nrrs_param_count(const nrrs_ctx* ctx) { return ctx ? ctx->n_params : 0; }
+
+int nrrs_param_layout(const nrrs_ctx* ctx, uint64_t* t, uint64_t* s, uint64_t* r) {
+    if (!ctx) return NRRS_ERR_INVALID_ARG;
+    if (t) *t = ctx->n_table;
+    if (s) *s = ctx->n_stat;
+    if (r) *r = ctx->n_rrs;
+    return NRRS_OK;
+}
+
+int nrrs_get_params(const nrrs_ctx* ctx, float* dst, uint64_t count) {
+    if (!ctx || !dst || count != ctx->n_params) return NRRS_ERR_INVALID_ARG;
+    cudaError_t e = cudaMemcpy(dst, ctx->params, sizeof(float) * count, cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? NRRS_OK : NRRS_ERR_CUDA;
+}
+
+int nrrs_set_params(nrrs_ctx* ctx, const float* src, uint64_t count) {
+    if (!ctx || !src || count != ctx->n_params) return ctx ? fail(ctx, NRRS_ERR_INVALID_ARG, "count mismatch") : NRRS_ERR_INVALID_ARG;
+    cudaError_t e = cudaMemcpy(ctx->params, src, sizeof(float) * count, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "set params");
+    int rc = refresh_derived(ctx, 0);
+    if (rc) return rc;
+    e = cudaDeviceSynchronize();
+    return e == cudaSuccess ? NRRS_OK : cuda_fail(ctx, e, "set params sync");
+}
+
+int nrrs_get_grads(const nrrs_ctx* ctx, float* dst, uint64_t count) {
+    if (!ctx || !dst || count != ctx->n_params) return NRRS_ERR_INVALID_ARG;
+    cudaError_t e = cudaMemcpy(dst, ctx->grads, sizeof(float) * count, cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? NRRS_OK : NRRS_ERR_CUDA;
+}
+
+int nrrs_get_adam_state(const nrrs_ctx* ctx, float* m, float* v, uint64_t count, uint64_t* t) {
+    if (!ctx || count != ctx->n_params) return NRRS_ERR_INVALID_ARG;
+    cudaError_t e = cudaSuccess;
+    if (m) e = cudaMemcpy(m, ctx->adam_m, sizeof(float) * count, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && v) e = cudaMemcpy(v, ctx->adam_v, sizeof(float) * count, cudaMemcpyDeviceToHost);
+    if (t) *t = ctx->adam_t;
+    return e == cudaSuccess ? NRRS_OK : NRRS_ERR_CUDA;
+}
+
+int nrrs_level_table(const nrrs_ctx* ctx, uint32_t* dst, int32_t max_levels) {
+    if (!ctx || !dst || max_levels < ctx->cfg.n_levels) return NRRS_ERR_INVALID_ARG;
+    for (int l = 0; l < ctx->cfg.n_levels; ++l) {
+        const LevelDev& L = ctx->enc.lv[l];
+        const uint64_t R = (uint64_t)L.res + 1;
+        dst[4 * l + 0] = L.offset;
+        dst[4 * l + 1] = (uint32_t)(L.dense ? R * R * R : (uint64_t)ctx->enc.hash_mask + 1);
+        dst[4 * l + 2] = L.res;
+        dst[4 * l + 3] = L.dense;
+    }
+    return NRRS_OK;
+}
+
+// checkpoint file: magic, version, config, adam step, params, m, v (all FP32)
+int nrrs_save(const nrrs_ctx* ctx, const char* path) {
+    if (!ctx || !path) return NRRS_ERR_INVALID_ARG;
+    std::vector<float> p(ctx->n_params), m(ctx->n_params), v(ctx->n_params);
+    if (nrrs_get_params(ctx, p.data(), ctx->n_params) ||
+        nrrs_get_adam_state(ctx, m.data(), v.data(), ctx->n_params, nullptr))
+        return NRRS_ERR_CUDA;
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return NRRS_ERR_IO;
+    const uint32_t hdr[2] = {0x5352524eu /* "NRRS" */, NRRS_ABI_VERSION};
+    bool ok = std::fwrite(hdr, sizeof(hdr), 1, f) == 1 &&
+              std::fwrite(&ctx->cfg, sizeof(nrrs_config), 1, f) == 1 &&
+              std::fwrite(&ctx->adam_t, sizeof(uint64_t), 1, f) == 1 &&
+              std::fwrite(p.data(), sizeof(float), p.size(), f) == p.size() &&
+              std::fwrite(m.data(), sizeof(float), m.size(), f) == m.size() &&
+              std::fwrite(v.data(), sizeof(float), v.size(), f) == v.size();
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? NRRS_OK : NRRS_ERR_IO;
+}
+
+int nrrs_load(nrrs_ctx* ctx, const char* path) {
+    if (!ctx || !path) return NRRS_ERR_INVALID_ARG;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(ctx, NRRS_ERR_IO, "cannot open checkpoint");
+    uint32_t hdr[2];
+    nrrs_config c;
+    uint64_t t = 0;
+    std::vector<float> p(ctx->n_params), m(ctx->n_params), v(ctx->n_params);
+    bool ok = std::fread(hdr, sizeof(hdr), 1, f) == 1 && hdr[0] == 0x5352524eu &&
+              hdr[1] == NRRS_ABI_VERSION && std::fread(&c, sizeof(c), 1, f) == 1 &&
+              std::fread(&t, sizeof(t), 1, f) == 1;
+    ok = ok && c.n_levels == ctx->cfg.n_levels && c.log2_hashmap_size == ctx->cfg.log2_hashmap_size &&
+         c.base_resolution == ctx->cfg.base_resolution && c.per_level_scale == ctx->cfg.per_level_scale &&
+         c.statnet_width == ctx->cfg.statnet_width && c.statnet_hidden == ctx->cfg.statnet_hidden &&
+         c.rrsnet_width == ctx->cfg.rrsnet_width && c.rrsnet_hidden == ctx->cfg.rrsnet_hidden;
+    ok = ok && std::fread(p.data(), sizeof(float), p.size(), f) == p.size() &&
+         std::fread(m.data(), sizeof(float), m.size(), f) == m.size() &&
+         std::fread(v.data(), sizeof(float), v.size(), f) == v.size();
+    std::fclose(f);
+    if (!ok) return fail(ctx, NRRS_ERR_IO, "checkpoint does not match this configuration");
+    const size_t b = sizeof(float) * ctx->n_params;
+    cudaError_t e = cudaMemcpy(ctx->adam_m, m.data(), b, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(ctx->adam_v, v.data(), b, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "load moments");
+    ctx->adam_t = t;
+    return nrrs_set_params(ctx, p.data(), ctx->n_params);
+}
+
+int nrrs_get_device_status(nrrs_ctx* ctx, uint32_t* flags, void* stream) {
+    if (!ctx || !flags) return NRRS_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned h = 0;
+    cudaError_t e = cudaMemcpyAsync(&h, &ctx->scr->status, sizeof(h), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(&ctx->scr->status, 0, sizeof(unsigned), s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "device status");
+    *flags = h;
+    if (h & NRRS_DEV_TIMEOUT) return NRRS_ERR_TIMEOUT;
+    if (h & NRRS_DEV_OVERFLOW) return NRRS_ERR_CAPACITY_OVERFLOW;
+    if (h & NRRS_DEV_NAN) return NRRS_ERR_NAN;
+    return NRRS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,268 @@
+// nrrs_common.cuh -- device-side definitions shared by every NRRS kernel (sm_100a).
+//
+// The maths restated here follows banbao990/NRRS-Code:
+//   activationSigma          src/render/nrrs/net/networkcommon.h:61-68
+//   box_cox_transform        src/render/nrrs/train.cu:19-39 (lambda = 0.5)
+//   warp_roughness           src/render/nrrs/train.h:95
+//   normalizeSpatialCoord    src/render/nrc/nrctrain.h:111-115
+//   RRSWeightWindow          src/render/common/commoncudautils.h:14-28
+//   factor + clamp + ceil    src/render/nrrs/integrator.cpp:1184-1298
+//   glue (RRSNet input)      src/render/nrrs/train.cu:41-112
+// The hash grid and the SH basis are the published Instant-NGP and real-SH definitions (the
+// reference takes them from its absent tiny-cuda-nn submodule).
+#pragma once
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "../../include/nrrs.h"
+
+namespace nrrs {
+
+constexpr int kMaxLevels = 16;
+constexpr int kStatIn = 64;      // StatNet input lanes
+constexpr int kRrsIn = 16;       // RRSNet input lanes
+constexpr int kStatOut = 3;      // log-statistics
+constexpr int kMaxSegments = 16; // depths per batched launch
+constexpr int kTile = 128;       // vertices per inference tile
+
+struct LevelDev {
+    uint32_t offset;  // first table row of the level
+    uint32_t res;     // N_l cells per axis (N_l + 1 grid points)
+    uint32_t dense;   // 1 = dense indexing
+    uint32_t pad;
+};
+
+struct EncodeParams {
+    LevelDev lv[kMaxLevels];
+    uint32_t n_levels;
+    uint32_t hash_mask;
+    int32_t normalize;
+    float center[3];
+    float diag[3];
+};
+
+struct VertexPtrs {
+    const float* pos;
+    const float* wi;
+    const float* normal;
+    const float* rough;
+    const float* albedo;
+    const float* thp;
+    const uint32_t* depth;
+    const float* ref;
+    const uint32_t* sidx;
+};
+
+struct FactorParams {
+    float clamp_min, clamp_max;
+    float ww;            // weight window size
+    int32_t use_ww;
+    int32_t use_ceil;
+    int32_t source;      // NRRS_FACTOR_*
+    float stat_eps, ref_eps;
+    double fixed_scale;  // 2^shift for the exact sum
+    float vmax;          // largest admissible summed term
+};
+
+// One depth of a (possibly batched) launch.
+struct Segment {
+    uint32_t offset;       // first vertex
+    uint32_t count;        // vertices
+    uint32_t tile_start;   // first inference tile / decision chunk of this segment
+    uint32_t budget;
+    uint32_t n_specular;
+    uint32_t queue_offset;
+    uint32_t queue_capacity;
+    uint32_t pad;
+};
+
+struct SegmentTable {
+    Segment s[kMaxSegments];
+    int32_t n;
+    uint32_t total_tiles;
+};
+
+// Scratch words of the decision kernel; lives in context memory (or a static array for the
+// allocation-free entry point). Self-resetting: the last CTA of every launch restores it.
+struct DecideScratch {
+    unsigned long long sum_acc[kMaxSegments];  // exact fixed-point normalisation sums
+    unsigned int ticket;                       // dynamic chunk ticket
+    unsigned int done;                         // finished CTAs
+    unsigned int epoch;                        // launch epoch tagging the look-back states
+    unsigned int status;                       // NRRS_DEV_* bits
+    unsigned long long pad[4];
+    // followed by the look-back state words (one unsigned long long per chunk)
+};
+
+__device__ __forceinline__ int find_segment(const SegmentTable& t, uint32_t tile) {
+    int s = 0;
+#pragma unroll 1
+    for (int k = 1; k < t.n; ++k)
+        if (tile >= t.s[k].tile_start) s = k;
+    return s;
+}
+
+// ---- scalar maths (FP32) ----
+__device__ __forceinline__ float act_sigma(float x) {
+    const float ln2 = 0.6931471805599453f;
+    return (x < 0.f) ? logf(1.0f + expf(x)) : (0.5f * x + ln2);
+}
+__device__ __forceinline__ float act_sigma_grad(float x) {
+    if (x < 0.f) { const float e = expf(x); return e / (1.0f + e); }
+    return 0.5f;
+}
+__device__ __forceinline__ float box_cox(float x) { return 2.0f * (sqrtf(x) - 1.0f); }
+__device__ __forceinline__ float warp_rough(float r) { return 1.0f - expf(-r); }
+
+// real SH bands 0..3 of a unit direction (16 coefficients)
+__device__ __forceinline__ void sh16(float x, float y, float z, float* o) {
+    const float xx = x * x, yy = y * y, zz = z * z;
+    o[0] = 0.28209479177387814f;
+    o[1] = -0.4886025119029199f * y;
+    o[2] = 0.4886025119029199f * z;
+    o[3] = -0.4886025119029199f * x;
+    o[4] = 1.0925484305920792f * x * y;
+    o[5] = -1.0925484305920792f * y * z;
+    o[6] = 0.31539156525252005f * (3.0f * zz - 1.0f);
+    o[7] = -1.0925484305920792f * x * z;
+    o[8] = 0.5462742152960396f * (xx - yy);
+    o[9] = -0.5900435899266435f * y * (3.0f * xx - yy);
+    o[10] = 2.890611442640554f * x * y * z;
+    o[11] = -0.4570457994644658f * y * (5.0f * zz - 1.0f);
+    o[12] = 0.3731763325901154f * z * (5.0f * zz - 3.0f);
+    o[13] = -0.4570457994644658f * x * (5.0f * zz - 1.0f);
+    o[14] = 1.445305721320277f * z * (xx - yy);
+    o[15] = -0.5900435899266435f * x * (xx - 3.0f * yy);
+}
+
+__device__ __forceinline__ float clamp01(float x) { return x < 0.f ? 0.f : (x > 1.f ? 1.f : x); }
+
+// normalised grid coordinate of vertex i
+__device__ __forceinline__ void norm_pos(const EncodeParams& e, const float* pos, uint32_t i,
+                                         float* p) {
+    const float x = pos[3 * (size_t)i], y = pos[3 * (size_t)i + 1], z = pos[3 * (size_t)i + 2];
+    if (e.normalize) {
+        p[0] = clamp01(__fadd_rn(0.5f, __fdiv_rn(__fsub_rn(x, e.center[0]), e.diag[0])));
+        p[1] = clamp01(__fadd_rn(0.5f, __fdiv_rn(__fsub_rn(y, e.center[1]), e.diag[1])));
+        p[2] = clamp01(__fadd_rn(0.5f, __fdiv_rn(__fsub_rn(z, e.center[2]), e.diag[2])));
+    } else {
+        p[0] = clamp01(x); p[1] = clamp01(y); p[2] = clamp01(z);
+    }
+}
+
+struct CellCoord {
+    uint32_t ix, iy, iz;
+    float fx, fy, fz;
+};
+
+// cell and fraction of a level: scaled coordinate rounded to FP32, floor clamped to [0, N-1]
+__device__ __forceinline__ CellCoord cell_of(const float* p, uint32_t N) {
+    CellCoord c;
+    const float Nf = (float)N;
+    float s, f;
+    int i;
+    s = __fmul_rn(p[0], Nf); i = (int)floorf(s); i = min(max(i, 0), (int)N - 1);
+    f = __fsub_rn(s, (float)i); c.ix = (uint32_t)i; c.fx = f;
+    s = __fmul_rn(p[1], Nf); i = (int)floorf(s); i = min(max(i, 0), (int)N - 1);
+    f = __fsub_rn(s, (float)i); c.iy = (uint32_t)i; c.fy = f;
+    s = __fmul_rn(p[2], Nf); i = (int)floorf(s); i = min(max(i, 0), (int)N - 1);
+    f = __fsub_rn(s, (float)i); c.iz = (uint32_t)i; c.fz = f;
+    return c;
+}
+
+__device__ __forceinline__ uint32_t grid_row(const LevelDev& L, uint32_t mask, uint32_t x,
+                                             uint32_t y, uint32_t z) {
+    uint32_t idx;
+    if (L.dense) {
+        const uint32_t R = L.res + 1;
+        idx = x + R * y + R * R * z;
+    } else {
+        idx = (x ^ (y * 2654435761u) ^ (z * 805459861u)) & mask;
+    }
+    return L.offset + idx;
+}
+
+__device__ __forceinline__ float corner_weight(const CellCoord& c, int k) {
+    const float wx = (k & 1) ? c.fx : 1.0f - c.fx;
+    const float wy = (k & 2) ? c.fy : 1.0f - c.fy;
+    const float wz = (k & 4) ? c.fz : 1.0f - c.fz;
+    return wx * wy * wz;
+}
+
+// Misc StatNet lanes [48, 64): normal, albedo, warped roughness, bias 1, zeros
+__device__ __forceinline__ void misc_lanes(const VertexPtrs& v, uint32_t i, float* o /*16*/) {
+    const size_t i3 = 3 * (size_t)i;
+    o[0] = v.normal[i3]; o[1] = v.normal[i3 + 1]; o[2] = v.normal[i3 + 2];
+    o[3] = v.albedo[i3]; o[4] = v.albedo[i3 + 1]; o[5] = v.albedo[i3 + 2];
+    o[6] = warp_rough(v.rough[i]);
+    o[7] = 1.0f;
+#pragma unroll
+    for (int k = 8; k < 16; ++k) o[k] = 0.f;
+}
+
+__device__ __forceinline__ float lin_stat(float y, float eps) {
+    const float L = expf(fminf(y, 20.0f)) - eps;
+    return L > 0.f ? L : 0.f;
+}
+
+// glue: RRSNet input lanes from the StatNet log-statistics (train.cu:41-112, 3-stat form)
+__device__ __forceinline__ void glue16(const FactorParams& fp, const float* y, const VertexPtrs& v,
+                                       uint32_t i, float* x1) {
+    const size_t i3 = 3 * (size_t)i;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        x1[c] = box_cox(lin_stat(y[c], fp.stat_eps));
+        x1[3 + c] = box_cox(v.thp[i3 + c]);
+    }
+    x1[6] = warp_rough(v.rough[i]);
+    x1[7] = box_cox(v.ref ? v.ref[i] : 0.5f);
+    x1[8] = (float)(v.depth ? v.depth[i] : 0u) * 0.125f;
+    x1[9] = 1.0f;
+#pragma unroll
+    for (int k = 10; k < 16; ++k) x1[k] = 0.f;
+}
+
+// factor + weight window + clamp (integrator.cpp:1184-1298)
+__device__ __forceinline__ float rrs_factor(const FactorParams& fp, const float* y, float raw,
+                                            const VertexPtrs& v, uint32_t i) {
+    float rrs;
+    if (fp.source == NRRS_FACTOR_ADRRS) {
+        const float ref = (v.ref ? v.ref[i] : 0.5f) + fp.ref_eps;
+        const size_t i3 = 3 * (size_t)i;
+        float acc = 0.f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float L = expf(fminf(y[c], 20.0f)) - fp.stat_eps;
+            L = L < 1e-4f ? 1e-4f : (L > 1e4f ? 1e4f : L);
+            acc += L * v.thp[i3 + c] / ref;
+        }
+        rrs = acc / 3.0f;
+    } else {
+        rrs = act_sigma(raw);
+    }
+    if (fp.use_ww) {
+        const float dminus = 2.0f / (1.0f + fp.ww);
+        const float dplus = dminus * fp.ww;
+        rrs = rrs < dminus ? rrs / dminus : (rrs > dplus ? rrs / dplus : 1.0f);
+    }
+    rrs = rrs < fp.clamp_min ? fp.clamp_min : (rrs > fp.clamp_max ? fp.clamp_max : rrs);
+    return rrs;
+}
+
+// exact fixed-point term of the normalisation sum (truncation toward zero)
+__device__ __forceinline__ long long fixed_term(const FactorParams& fp, float rrs,
+                                                unsigned int* status) {
+    float x = fp.use_ceil ? ceilf(rrs) : rrs;
+    if (!isfinite(x)) { atomicOr(status, NRRS_DEV_NAN); return 0; }
+    if (x > fp.vmax) { atomicOr(status, NRRS_DEV_SATURATED); x = fp.vmax; }
+    return __double2ll_rz((double)x * fp.fixed_scale);
+}
+
+__device__ __forceinline__ long long warp_sum_ll(long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+}  // namespace nrrs

@@ -1,0 +1,325 @@
+"""ctypes binding of libnrrs_b200 (include/nrrs.h) and a host-side mirror of the reference's
+NRRSNetwork interface (src/render/nrrs/net/network.h:22-214).
+
+The library is the product; this module only binds it. Device buffers are passed as raw
+pointers (`int` addresses, e.g. ``tensor.data_ptr()``), streams as raw ``cudaStream_t`` values.
+There is no CPU fallback: if the shared library is missing this module raises on first use,
+and on a machine without an sm_100 GPU ``NRRSNetwork`` raises ``NRRSError`` (NO_DEVICE).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "lib" / "libnrrs_b200.so"
+HEADER = HERE.parent / "include" / "nrrs.h"
+
+OK = 0
+ERR_INVALID_ARG = -1
+ERR_CAPACITY_OVERFLOW = -2
+ERR_NAN = -3
+ERR_TIMEOUT = -4
+ERR_CUDA = -5
+ERR_NO_DEVICE = -6
+ERR_UNSUPPORTED = -7
+ERR_IO = -8
+
+DEV_OVERFLOW = 0x1
+DEV_NAN = 0x2
+DEV_TIMEOUT = 0x4
+DEV_SATURATED = 0x8
+
+PREC_FP32, PREC_FP16, PREC_BF16 = 0, 1, 2
+FACTOR_ADRRS, FACTOR_RRSNET = 2, 3
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("n_levels", C.c_int32), ("n_features_per_level", C.c_int32),
+        ("log2_hashmap_size", C.c_int32), ("base_resolution", C.c_int32),
+        ("per_level_scale", C.c_float), ("sh_degree", C.c_int32),
+        ("statnet_width", C.c_int32), ("statnet_hidden", C.c_int32),
+        ("rrsnet_width", C.c_int32), ("rrsnet_hidden", C.c_int32),
+        ("precision", C.c_int32), ("seed", C.c_uint64), ("table_init_scale", C.c_float),
+        ("lr", C.c_float), ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float),
+        ("l2_reg", C.c_float), ("stat_eps", C.c_float), ("ref_eps", C.c_float),
+        ("loss_clamp_max", C.c_float), ("cost_offset", C.c_float),
+        ("normalize_pos", C.c_int32), ("aabb_min", C.c_float * 3), ("aabb_max", C.c_float * 3),
+        ("max_queue", C.c_uint32), ("max_train", C.c_uint32), ("step", C.c_int32),
+    ]
+
+
+class VertexSoA(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in
+                ("pos", "wi", "normal", "roughness", "albedo", "thp", "depth", "ref_mean",
+                 "scatter_index")]
+
+
+class DecideParams(C.Structure):
+    _fields_ = [
+        ("clamp_min", C.c_float), ("clamp_max", C.c_float), ("normalize_rate", C.c_float),
+        ("use_ceil", C.c_int32), ("scale_up", C.c_int32), ("use_weight_window", C.c_int32),
+        ("weight_window_size", C.c_float), ("factor_source", C.c_int32),
+    ]
+
+
+class Segment(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in
+                ("offset", "count", "budget", "n_specular", "queue_offset", "queue_capacity")]
+
+
+class NRRSError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{msg} (status {code})")
+        self.code = code
+
+
+_lib = None
+
+_SIGS = {
+    "nrrs_config_default": (None, [C.POINTER(Config)]),
+    "nrrs_decide_params_default": (None, [C.POINTER(DecideParams)]),
+    "nrrs_create": (C.c_int, [C.POINTER(Config), C.POINTER(C.c_void_p)]),
+    "nrrs_destroy": (None, [C.c_void_p]),
+    "nrrs_set_step": (C.c_int, [C.c_void_p, C.c_int32]),
+    "nrrs_last_error": (C.c_char_p, [C.c_void_p]),
+    "nrrs_status_string": (C.c_char_p, [C.c_int]),
+    "nrrs_device_available": (C.c_int, []),
+    "nrrs_infer": (C.c_int, [C.c_void_p, C.POINTER(VertexSoA), C.c_uint32,
+                             C.POINTER(DecideParams), C.c_void_p, C.c_void_p, C.c_void_p]),
+    "nrrs_decide_emit": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                   C.c_uint32, C.c_uint32, C.c_void_p, C.POINTER(DecideParams),
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
+                                   C.c_void_p]),
+    "nrrs_step": (C.c_int, [C.c_void_p, C.POINTER(VertexSoA), C.c_void_p, C.c_uint32, C.c_uint32,
+                            C.c_uint32, C.POINTER(DecideParams), C.c_void_p, C.c_void_p,
+                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
+                            C.c_void_p]),
+    "nrrs_step_batched": (C.c_int, [C.c_void_p, C.POINTER(VertexSoA), C.c_void_p,
+                                    C.POINTER(Segment), C.c_int32, C.POINTER(DecideParams),
+                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p]),
+    "nrrs_train_step": (C.c_int, [C.c_void_p, C.POINTER(VertexSoA), C.c_void_p, C.c_uint32,
+                                  C.c_void_p, C.c_void_p]),
+    "nrrs_param_count": (C.c_uint64, [C.c_void_p]),
+    "nrrs_param_layout": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                    C.POINTER(C.c_uint64)]),
+    "nrrs_get_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
+    "nrrs_set_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
+    "nrrs_get_grads": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
+    "nrrs_get_adam_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
+                                      C.POINTER(C.c_uint64)]),
+    "nrrs_level_table": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "nrrs_save": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "nrrs_load": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "nrrs_get_device_status": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.c_void_p]),
+    "nrrs_synth_vertices": (None, [C.c_uint64, C.c_uint64, C.c_uint64] + [C.c_void_p] * 10),
+}
+
+
+def lib():
+    """Load libnrrs_b200.so (built by nrrs-code_b200/build.py); raise if it is missing."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise FileNotFoundError(f"{LIB_PATH} is missing: run nrrs-code_b200/build.py")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def header_functions() -> list[str]:
+    """Names of every function declared in include/nrrs.h."""
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(nrrs_[a-z_0-9]+)\s*\(", text)))
+
+
+def default_config(**kw) -> Config:
+    c = Config()
+    lib().nrrs_config_default(C.byref(c))
+    for k, v in kw.items():
+        if k in ("aabb_min", "aabb_max"):
+            getattr(c, k)[:] = list(v)
+        else:
+            setattr(c, k, v)
+    return c
+
+
+def default_decide(**kw) -> DecideParams:
+    p = DecideParams()
+    lib().nrrs_decide_params_default(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def _ptr(x):
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    if hasattr(x, "ctypes"):
+        return x.ctypes.data
+    raise TypeError(type(x))
+
+
+def vertex_soa(pos, wi, normal, roughness, albedo, thp, depth=None, ref_mean=None,
+               scatter_index=None) -> VertexSoA:
+    return VertexSoA(*(_ptr(a) for a in (pos, wi, normal, roughness, albedo, thp, depth, ref_mean,
+                                         scatter_index)))
+
+
+def synth(seed: int, n: int, first: int = 0):
+    """Synthetic vertices as a dict of numpy arrays (host), from the library's generator."""
+    import numpy as np
+    out = {
+        "pos": np.empty((n, 3), np.float32), "wi": np.empty((n, 3), np.float32),
+        "normal": np.empty((n, 3), np.float32), "roughness": np.empty(n, np.float32),
+        "albedo": np.empty((n, 3), np.float32), "thp": np.empty((n, 3), np.float32),
+        "depth": np.empty(n, np.uint32), "rnd": np.empty(n, np.float32),
+        "ref_mean": np.empty(n, np.float32), "target": np.empty((n, 3), np.float32),
+    }
+    lib().nrrs_synth_vertices(seed, first, n, *(out[k].ctypes.data for k in
+                              ("pos", "wi", "normal", "roughness", "albedo", "thp", "depth",
+                               "rnd", "ref_mean", "target")))
+    return out
+
+
+VERTEX_FIELDS = ("pos", "wi", "normal", "roughness", "albedo", "thp", "depth", "ref_mean")
+
+
+class NRRSNetwork:
+    """Mirror of the reference NRRSNetwork over the C-ABI.
+
+    reference                                  here
+    NRRSNetwork(json) + reset/resize           NRRSNetwork(Config)         (nrrs_create)
+    setStep(int)                               setStep                     (nrrs_set_step)
+    prepareInferenceData + inference           inference                   (nrrs_infer)
+    generateRRSNumber (integrator)             generateRRSNumber           (nrrs_step)
+    calcSum2PassAsync + "Gen Tids"             decideEmit                  (nrrs_decide_emit)
+    train(input, output, offset, onlyLL2)      train                       (nrrs_train_step)
+    saveWeights / loadWeights (stubs there)    saveWeights / loadWeights   (nrrs_save/load)
+    """
+
+    def __init__(self, config: Config | None = None):
+        self.config = config if config is not None else default_config()
+        h = C.c_void_p()
+        rc = lib().nrrs_create(C.byref(self.config), C.byref(h))
+        if rc != OK:
+            raise NRRSError(rc, lib().nrrs_last_error(None).decode())
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().nrrs_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int):
+        if rc != OK:
+            raise NRRSError(rc, lib().nrrs_last_error(self._h).decode())
+        return rc
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ---- reference-named operations ----
+    def setStep(self, step: int):
+        self._check(lib().nrrs_set_step(self._h, step))
+
+    def inference(self, soa: VertexSoA, n: int, params: DecideParams, stats, rrs, stream=0):
+        return self._check(lib().nrrs_infer(self._h, C.byref(soa), n, C.byref(params),
+                                            _ptr(stats), _ptr(rrs), stream))
+
+    def decideEmit(self, rrs, rnd, n, budget, n_specular, params, rrs_norm, split, queue,
+                   capacity, next_size, scatter_index=None, n_specular_dev=None, stream=0):
+        return self._check(lib().nrrs_decide_emit(
+            self._h, _ptr(rrs), _ptr(rnd), _ptr(scatter_index), n, budget, n_specular,
+            _ptr(n_specular_dev), C.byref(params), _ptr(rrs_norm), _ptr(split), _ptr(queue),
+            capacity, _ptr(next_size), stream))
+
+    def generateRRSNumber(self, soa, rnd, n, budget, n_specular, params, stats, rrs, rrs_norm,
+                          split, queue, capacity, next_size, stream=0):
+        return self._check(lib().nrrs_step(
+            self._h, C.byref(soa), _ptr(rnd), n, budget, n_specular, C.byref(params), _ptr(stats),
+            _ptr(rrs), _ptr(rrs_norm), _ptr(split), _ptr(queue), capacity, _ptr(next_size),
+            stream))
+
+    def generateRRSNumberBatched(self, soa, rnd, segments, params, stats, rrs, rrs_norm, split,
+                                 queue, next_size, stream=0):
+        arr = (Segment * len(segments))(*segments)
+        return self._check(lib().nrrs_step_batched(
+            self._h, C.byref(soa), _ptr(rnd), arr, len(segments), C.byref(params), _ptr(stats),
+            _ptr(rrs), _ptr(rrs_norm), _ptr(split), _ptr(queue), _ptr(next_size), stream))
+
+    def train(self, soa: VertexSoA, target, n: int, loss_dev=None, stream=0):
+        return self._check(lib().nrrs_train_step(self._h, C.byref(soa), _ptr(target), n,
+                                                 _ptr(loss_dev), stream))
+
+    def saveWeights(self, path: str | os.PathLike):
+        self._check(lib().nrrs_save(self._h, str(path).encode()))
+
+    def loadWeights(self, path: str | os.PathLike):
+        self._check(lib().nrrs_load(self._h, str(path).encode()))
+
+    # ---- parameters ----
+    def param_count(self) -> int:
+        return int(lib().nrrs_param_count(self._h))
+
+    def param_layout(self):
+        t, s, r = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        self._check(lib().nrrs_param_layout(self._h, C.byref(t), C.byref(s), C.byref(r)))
+        return int(t.value), int(s.value), int(r.value)
+
+    def get_params(self):
+        import numpy as np
+        a = np.empty(self.param_count(), np.float32)
+        self._check(lib().nrrs_get_params(self._h, a.ctypes.data, a.size))
+        return a
+
+    def set_params(self, a):
+        import numpy as np
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        self._check(lib().nrrs_set_params(self._h, a.ctypes.data, a.size))
+
+    def get_grads(self):
+        import numpy as np
+        a = np.empty(self.param_count(), np.float32)
+        self._check(lib().nrrs_get_grads(self._h, a.ctypes.data, a.size))
+        return a
+
+    def get_adam_state(self):
+        import numpy as np
+        m = np.empty(self.param_count(), np.float32)
+        v = np.empty_like(m)
+        t = C.c_uint64()
+        self._check(lib().nrrs_get_adam_state(self._h, m.ctypes.data, v.ctypes.data, m.size,
+                                              C.byref(t)))
+        return m, v, int(t.value)
+
+    def level_table(self):
+        import numpy as np
+        a = np.zeros((self.config.n_levels, 4), np.uint32)
+        self._check(lib().nrrs_level_table(self._h, a.ctypes.data, self.config.n_levels))
+        return a
+
+    def device_status(self, stream=0) -> tuple[int, int]:
+        f = C.c_uint32()
+        rc = lib().nrrs_get_device_status(self._h, C.byref(f), stream)
+        return rc, int(f.value)

@@ -1,0 +1,84 @@
+/*
+ * nrrs_oracle.h -- CPU oracle for the NRRS per-vertex step. TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain-C restatement of the reference path (banbao990/NRRS-Code, src/render/nrrs) used by
+ * tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg as the checker and the timed
+ * CPU baseline. The product library never links or calls it.
+ *
+ * Parity status: the decision/normalisation maths and the glue are restated from the reference
+ * sources cited per function and pinned by hand-derived known answers (tests/golden). The
+ * reference's RRSWeightWindow is additionally compiled from its own header into oracle/_ref
+ * and compared. The encodings, MLPs, losses and optimizer live in the reference's tiny-cuda-nn
+ * submodule, which is absent and unpinned (branch `use-bb`, no commit): for those the oracle
+ * restates the published algorithms (Instant-NGP hash grid, real SH, bias-free MLP, Adam) and
+ * the written loss definitions, so PARITY WITH THE REFERENCE IS UNPINNED for them.
+ *
+ * Every entry point exists in an FP64 (_f64) and FP32 (_f32) flavour where arithmetic is
+ * floating point; the decision path is FP32 only because it must be bit-exact.
+ */
+#ifndef NRRS_ORACLE_H
+#define NRRS_ORACLE_H
+#include <stdint.h>
+#include "../include/nrrs.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* level table: out[l*4 + {0,1,2,3}] = {offset, entries, resolution, dense}; returns total entries */
+uint64_t oracle_level_table(const nrrs_config* cfg, uint32_t* out);
+uint64_t oracle_param_count(const nrrs_config* cfg, uint64_t* table, uint64_t* stat, uint64_t* rrs);
+void oracle_sh16_f64(const double* dir, double* out);
+/* activationSigma (networkcommon.h:61-68) and box_cox_transform (train.cu:19-39) in FP32 */
+float oracle_activation_sigma_f32(float x);
+float oracle_box_cox_f32(float x);
+float oracle_weight_window_f32(float x, float ww);
+/* normalizeSpatialCoord (nrctrain.h:111-115) for one point, FP32 */
+void oracle_normalize_pos_f32(const nrrs_config* cfg, const float* p, float* out);
+
+/* inference: params = FP32 master params (nrrs_get_params layout).
+ * Outputs (any may be NULL): x0 [n][64], stats [n][3], x1 [n][16], raw [n], rrs [n] (clamped). */
+void oracle_infer_f64(const nrrs_config* cfg, const float* params, uint64_t n,
+                      const nrrs_vertex_soa* v, const nrrs_decide_params* p,
+                      double* x0, double* stats, double* x1, double* raw, double* rrs);
+void oracle_infer_f32(const nrrs_config* cfg, const float* params, uint64_t n,
+                      const nrrs_vertex_soa* v, const nrrs_decide_params* p,
+                      float* x0, float* stats, float* x1, float* raw, float* rrs);
+
+/* exact fixed-point sum of rrs (or ceil(rrs)): returns the 64-bit accumulator, *sum = acc*2^-shift */
+int oracle_sum_shift(uint64_t n, float vmax);
+int64_t oracle_sum_fixed(const float* rrs, uint64_t n, int use_ceil, int shift, double* sum);
+
+/* decision + emission (integrator.cpp:1368-1460, commonworkqueue.h:19-25), FP32, bit-exact
+ * contract. Returns the total queue size (may exceed capacity; extra entries are dropped).
+ * shift_n sizes the exact sum's fixed-point shift (the library uses its max_queue; 0 = n).
+ * status_flags receives NRRS_DEV_* bits. */
+uint64_t oracle_decide_emit(const float* rrs, const float* rnd, const uint32_t* scatter_index,
+                            uint64_t n, uint32_t budget, uint32_t n_specular,
+                            const nrrs_decide_params* p, uint64_t shift_n, float* rrs_norm,
+                            uint8_t* split, uint32_t* queue, uint64_t capacity,
+                            uint32_t* status_flags);
+
+/* training: losses and gradients (no update). grads has nrrs_param_count entries.
+ * loss[0] = StatNet relative log-L2, loss[1] = RRSNet variance x cost (0 when step < 3). */
+void oracle_train_grads_f64(const nrrs_config* cfg, const float* params, uint64_t n,
+                            const nrrs_vertex_soa* v, const float* target, double* grads,
+                            double* loss);
+void oracle_train_grads_f32(const nrrs_config* cfg, const float* params, uint64_t n,
+                            const nrrs_vertex_soa* v, const float* target, float* grads,
+                            double* loss);
+/* loss only (for finite differences), FP64 */
+void oracle_train_loss_f64(const nrrs_config* cfg, const double* params, uint64_t n,
+                           const nrrs_vertex_soa* v, const float* target, double* loss);
+/* Adam update in FP32 over [first, first+count); t = step number after increment */
+void oracle_adam_f32(const nrrs_config* cfg, float* params, const float* grads, float* m,
+                     float* v, uint64_t first, uint64_t count, uint64_t t);
+
+/* threads used by the OpenMP loops (0 = runtime default) */
+void oracle_set_threads(int n);
+int oracle_get_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,188 @@
+"""ctypes wrapper of the CPU oracle (oracle/_build/libnrrs_oracle.so). TEST INFRASTRUCTURE ONLY:
+used by tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg as the checker and the
+timed CPU baseline, never by the product library.
+
+PARITY UNPINNED for the encodings, MLPs, losses and optimizer (the reference takes them from its
+absent tiny-cuda-nn submodule); the decision, normalisation, glue and activation restatements
+are pinned by tests/golden fixtures and, for RRSWeightWindow, by the reference's own header
+compiled into oracle/_ref (see oracle/Makefile).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "libnrrs_oracle.so"
+REF_LIB = HERE / "_ref" / "libnrrs_ref.so"
+REPO = HERE.parent
+sys.path.insert(0, str(REPO / "nrrs-code_b200"))
+import nrrs_b200 as nb  # noqa: E402  (struct definitions only)
+
+_lib = None
+_ref = None
+
+
+def build(ref: bool = False):
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    if ref:
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = C.CDLL(str(LIB))
+        vp = C.c_void_p
+        L.oracle_level_table.restype = C.c_uint64
+        L.oracle_level_table.argtypes = [C.POINTER(nb.Config), vp]
+        L.oracle_param_count.restype = C.c_uint64
+        L.oracle_param_count.argtypes = [C.POINTER(nb.Config), vp, vp, vp]
+        L.oracle_sh16_f64.argtypes = [vp, vp]
+        for f in ("oracle_activation_sigma_f32", "oracle_box_cox_f32"):
+            getattr(L, f).restype = C.c_float
+            getattr(L, f).argtypes = [C.c_float]
+        L.oracle_weight_window_f32.restype = C.c_float
+        L.oracle_weight_window_f32.argtypes = [C.c_float, C.c_float]
+        L.oracle_normalize_pos_f32.argtypes = [C.POINTER(nb.Config), vp, vp]
+        for f in ("oracle_infer_f64", "oracle_infer_f32"):
+            getattr(L, f).argtypes = [C.POINTER(nb.Config), vp, C.c_uint64, C.POINTER(nb.VertexSoA),
+                                      C.POINTER(nb.DecideParams), vp, vp, vp, vp, vp]
+        L.oracle_sum_shift.restype = C.c_int
+        L.oracle_sum_shift.argtypes = [C.c_uint64, C.c_float]
+        L.oracle_sum_fixed.restype = C.c_int64
+        L.oracle_sum_fixed.argtypes = [vp, C.c_uint64, C.c_int, C.c_int, C.POINTER(C.c_double)]
+        L.oracle_decide_emit.restype = C.c_uint64
+        L.oracle_decide_emit.argtypes = [vp, vp, vp, C.c_uint64, C.c_uint32, C.c_uint32,
+                                         C.POINTER(nb.DecideParams), C.c_uint64, vp, vp, vp,
+                                         C.c_uint64, C.POINTER(C.c_uint32)]
+        for f in ("oracle_train_grads_f64", "oracle_train_grads_f32"):
+            getattr(L, f).argtypes = [C.POINTER(nb.Config), vp, C.c_uint64, C.POINTER(nb.VertexSoA),
+                                      vp, vp, vp]
+        L.oracle_train_loss_f64.argtypes = [C.POINTER(nb.Config), vp, C.c_uint64,
+                                            C.POINTER(nb.VertexSoA), vp, vp]
+        L.oracle_adam_f32.argtypes = [C.POINTER(nb.Config), vp, vp, vp, vp, C.c_uint64,
+                                      C.c_uint64, C.c_uint64]
+        L.oracle_set_threads.argtypes = [C.c_int]
+        L.oracle_get_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def ref_lib():
+    """The reference's RRSWeightWindow compiled from its own header, or None if not built."""
+    global _ref
+    if _ref is None and REF_LIB.exists():
+        L = C.CDLL(str(REF_LIB))
+        L.ref_rrs_weight_window.restype = C.c_float
+        L.ref_rrs_weight_window.argtypes = [C.c_float, C.c_float]
+        _ref = L
+    return _ref
+
+
+def _soa(v: dict) -> nb.VertexSoA:
+    return nb.VertexSoA(*(v[k].ctypes.data if v.get(k) is not None else None
+                          for k in ("pos", "wi", "normal", "roughness", "albedo", "thp", "depth",
+                                    "ref_mean", "scatter_index")))
+
+
+def level_table(cfg):
+    out = np.zeros((cfg.n_levels, 4), np.uint32)
+    tot = lib().oracle_level_table(C.byref(cfg), out.ctypes.data)
+    return out, int(tot)
+
+
+def param_count(cfg):
+    t, s, r = C.c_uint64(), C.c_uint64(), C.c_uint64()
+    n = lib().oracle_param_count(C.byref(cfg), C.byref(t), C.byref(s), C.byref(r))
+    return int(n), int(t.value), int(s.value), int(r.value)
+
+
+def infer(cfg, params, v: dict, dp, precision: str = "f64", want=("stats", "rrs")):
+    n = v["pos"].shape[0]
+    dt = np.float64 if precision == "f64" else np.float32
+    outs = {"x0": (n, 64), "stats": (n, 3), "x1": (n, 16), "raw": (n,), "rrs": (n,)}
+    res = {k: np.empty(s, dt) for k, s in outs.items() if k in want}
+    f = lib().oracle_infer_f64 if precision == "f64" else lib().oracle_infer_f32
+    params = np.ascontiguousarray(params, np.float32)
+    soa = _soa(v)
+    f(C.byref(cfg), params.ctypes.data, n, C.byref(soa), C.byref(dp),
+      *(res[k].ctypes.data if k in res else None for k in ("x0", "stats", "x1", "raw", "rrs")))
+    return res
+
+
+def sum_fixed(rrs, use_ceil: bool, shift: int):
+    rrs = np.ascontiguousarray(rrs, np.float32)
+    s = C.c_double()
+    acc = lib().oracle_sum_fixed(rrs.ctypes.data, rrs.size, int(use_ceil), shift, C.byref(s))
+    return int(acc), s.value
+
+
+def sum_shift(n: int, vmax: float) -> int:
+    return int(lib().oracle_sum_shift(n, vmax))
+
+
+def decide_emit(rrs, rnd, budget, n_specular, dp, capacity=None, scatter_index=None, shift_n=0):
+    """shift_n: size that fixes the exact sum's shift (pass the library's max_queue)."""
+    rrs = np.ascontiguousarray(rrs, np.float32)
+    rnd = np.ascontiguousarray(rnd, np.float32)
+    n = rrs.size
+    cap = capacity if capacity is not None else int(n * (dp.clamp_max + 2)) + 8
+    queue = np.zeros(max(cap, 1), np.uint32)
+    nstid = int(scatter_index.max()) + 1 if scatter_index is not None and n else n
+    rrs_norm = np.zeros(max(nstid, 1), np.float32)
+    split = np.zeros(max(n, 1), np.uint8)
+    flags = C.c_uint32()
+    si = np.ascontiguousarray(scatter_index, np.uint32) if scatter_index is not None else None
+    total = lib().oracle_decide_emit(rrs.ctypes.data, rnd.ctypes.data,
+                                     si.ctypes.data if si is not None else None, n, budget,
+                                     n_specular, C.byref(dp), shift_n, rrs_norm.ctypes.data,
+                                     split.ctypes.data, queue.ctypes.data, cap, C.byref(flags))
+    return {"queue": queue[:min(int(total), cap)], "total": int(total), "rrs_norm": rrs_norm[:nstid],
+            "split": split[:n], "flags": int(flags.value)}
+
+
+def train_grads(cfg, params, v: dict, target, precision: str = "f64"):
+    n = v["pos"].shape[0]
+    npar = param_count(cfg)[0]
+    dt = np.float64 if precision == "f64" else np.float32
+    g = np.zeros(npar, dt)
+    loss = np.zeros(2, np.float64)
+    f = lib().oracle_train_grads_f64 if precision == "f64" else lib().oracle_train_grads_f32
+    params = np.ascontiguousarray(params, np.float32)
+    target = np.ascontiguousarray(target, np.float32)
+    soa = _soa(v)
+    f(C.byref(cfg), params.ctypes.data, n, C.byref(soa), target.ctypes.data, g.ctypes.data,
+      loss.ctypes.data)
+    return g, loss
+
+
+def train_loss(cfg, params64, v: dict, target):
+    n = v["pos"].shape[0]
+    loss = np.zeros(2, np.float64)
+    params64 = np.ascontiguousarray(params64, np.float64)
+    target = np.ascontiguousarray(target, np.float32)
+    soa = _soa(v)
+    lib().oracle_train_loss_f64(C.byref(cfg), params64.ctypes.data, n, C.byref(soa),
+                                target.ctypes.data, loss.ctypes.data)
+    return loss
+
+
+def adam(cfg, params, grads, m, v, t, first=0, count=None):
+    count = params.size - first if count is None else count
+    lib().oracle_adam_f32(C.byref(cfg), params.ctypes.data, grads.ctypes.data, m.ctypes.data,
+                          v.ctypes.data, first, count, t)
+
+
+def set_threads(n: int):
+    lib().oracle_set_threads(n)
+
+
+def threads() -> int:
+    return int(lib().oracle_get_threads())

@@ -1,0 +1,173 @@
+"""GPU parity of the fused inference kernels (encoding, StatNet, glue, RRSNet, activation,
+clamp) against the oracle, and of the fused/batched step against separate calls."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import nrrs_b200 as nb
+import oracle as O
+from gpu_util import empty, host, make_net, random_params, soa, stream, torch_cuda, upload
+
+pytestmark = pytest.mark.gpu
+MAXQ = 1 << 21  # max_queue of make_net(): fixes the exact sum's shift
+
+# FP32 path: same maths as the FP32 oracle up to FMA contraction and libm ulps
+FP32_RTOL, FP32_ATOL = 2e-4, 2e-5
+# factor target of the workload: within 1e-2 relative of the FP64 oracle (mixed precision)
+MIXED_RTOL = 1e-2
+
+
+def run_infer(net, v, dp, n):
+    d = upload(v)
+    stats, rrs = empty(3 * n), empty(n)
+    net.inference(soa(d), n, dp, stats, rrs, stream())
+    return host(stats)[:3 * n].reshape(n, 3), host(rrs)[:n]
+
+
+@pytest.fixture(scope="module")
+def fp32_net():
+    net = make_net()
+    yield net
+    net.close()
+
+
+@pytest.mark.parametrize("params", ["init", "random"])
+@pytest.mark.parametrize("source", [nb.FACTOR_RRSNET, nb.FACTOR_ADRRS])
+def test_fp32_infer_matches_oracle(fp32_net, params, source):
+    n = 65536
+    v = nb.synth(0, n)
+    if params == "random":
+        p = random_params(fp32_net, 1)
+    else:
+        fresh = make_net()
+        p = fresh.get_params()
+        fresh.close()
+        fp32_net.set_params(p)
+    dp = nb.default_decide(factor_source=source)
+    stats, rrs = run_infer(fp32_net, v, dp, n)
+    o32 = O.infer(fp32_net.config, p, v, dp, "f32")
+    o64 = O.infer(fp32_net.config, p, v, dp, "f64")
+    assert np.allclose(stats, o32["stats"], rtol=FP32_RTOL, atol=FP32_ATOL)
+    assert np.allclose(rrs, o32["rrs"], rtol=FP32_RTOL, atol=FP32_ATOL)
+    rel = np.abs(rrs - o64["rrs"]) / o64["rrs"]
+    assert rel.max() < 1e-4, rel.max()
+
+
+def test_fp32_ragged_sizes_and_normalized_positions():
+    net = make_net(normalize_pos=1, aabb_min=[-2, -1, 0], aabb_max=[3, 2, 5])
+    p = random_params(net, 2)
+    for n in (1, 127, 129, 1000):
+        v = nb.synth(11, n)
+        v["pos"] = (v["pos"] * np.array([5, 3, 5], np.float32) + np.array([-2, -1, 0], np.float32)).astype(np.float32)
+        dp = nb.default_decide()
+        stats, rrs = run_infer(net, v, dp, n)
+        o = O.infer(net.config, p, v, dp, "f32")
+        assert np.allclose(stats, o["stats"], rtol=FP32_RTOL, atol=FP32_ATOL), n
+        assert np.allclose(rrs, o["rrs"], rtol=FP32_RTOL, atol=FP32_ATOL), n
+    net.close()
+
+
+def test_step_equals_infer_then_decide(fp32_net):
+    torch = torch_cuda()
+    n = 200001
+    v = nb.synth(3, n)
+    random_params(fp32_net, 3)
+    dp = nb.default_decide()
+    d = upload(v)
+    s = soa(d)
+    cap = 9 * n
+    a = dict(stats=empty(3 * n), rrs=empty(n), norm=empty(n), split=empty(n, "uint8"),
+             q=empty(cap, "int32"), sz=empty(1, "int32"))
+    fp32_net.generateRRSNumber(s, d["rnd"], n, n, 0, dp, a["stats"], a["rrs"], a["norm"],
+                               a["split"], a["q"], cap, a["sz"], stream())
+    b = dict(stats=empty(3 * n), rrs=empty(n), norm=empty(n), split=empty(n, "uint8"),
+             q=empty(cap, "int32"), sz=empty(1, "int32"))
+    fp32_net.inference(s, n, dp, b["stats"], b["rrs"], stream())
+    fp32_net.decideEmit(b["rrs"], d["rnd"], n, n, 0, dp, b["norm"], b["split"], b["q"], cap,
+                        b["sz"], stream=stream())
+    torch.cuda.synchronize()
+    for k in a:
+        assert torch.equal(a[k], b[k]), k
+    # and the decision equals the oracle's on the GPU factors
+    o = O.decide_emit(host(a["rrs"])[:n], v["rnd"], n, 0, dp, shift_n=MAXQ)
+    tot = int(host(a["sz"], np.uint32)[0])
+    assert tot == o["total"]
+    assert np.array_equal(host(a["q"], np.uint32)[:tot], o["queue"])
+
+
+def test_batched_equals_per_depth(fp32_net):
+    torch = torch_cuda()
+    random_params(fp32_net, 4)
+    counts = [70000, 42000, 25200, 15120, 9072, 0, 3265]
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    N = int(offs[-1])
+    v = nb.synth(9, N)
+    d = upload(v)
+    s = soa(d)
+    dp = nb.default_decide()
+    caps = [9 * c for c in counts]
+    qoffs = np.concatenate([[0], np.cumsum(caps)]).astype(np.int64)
+    segs = [nb.Segment(int(offs[k]), counts[k], max(counts[k], 1), k, int(qoffs[k]), caps[k])
+            for k in range(len(counts))]
+    bat = dict(stats=empty(3 * N), rrs=empty(N), norm=empty(N), split=empty(N, "uint8"),
+               q=empty(int(qoffs[-1]), "int32"), sz=empty(len(counts), "int32"))
+    fp32_net.generateRRSNumberBatched(s, d["rnd"], segs, dp, bat["stats"], bat["rrs"],
+                                      bat["norm"], bat["split"], bat["q"], bat["sz"], stream())
+    sz = host(bat["sz"], np.uint32)
+    q = host(bat["q"], np.uint32)
+    split = host(bat["split"])
+    rrs_b = host(bat["rrs"])
+    for k, c in enumerate(counts):
+        o0, o1 = int(offs[k]), int(offs[k + 1])
+        if c == 0:
+            assert sz[k] == 0
+            continue
+        sub = {key: val[o0:o1].copy() for key, val in v.items()}
+        ds = upload(sub)
+        one = dict(stats=empty(3 * c), rrs=empty(c), norm=empty(c), split=empty(c, "uint8"),
+                   q=empty(caps[k], "int32"), sz=empty(1, "int32"))
+        fp32_net.generateRRSNumber(soa(ds), ds["rnd"], c, max(c, 1), k, dp, one["stats"],
+                                   one["rrs"], one["norm"], one["split"], one["q"], caps[k],
+                                   one["sz"], stream())
+        tot = int(host(one["sz"], np.uint32)[0])
+        assert sz[k] == tot, k
+        assert np.array_equal(host(one["rrs"])[:c], rrs_b[o0:o1])
+        assert np.array_equal(host(one["split"])[:c], split[o0:o1])
+        # the batched queue stores vertex indices of the concatenated SoA
+        assert np.array_equal(host(one["q"], np.uint32)[:tot] + o0,
+                              q[int(qoffs[k]):int(qoffs[k]) + tot])
+    torch.cuda.synchronize()
+
+
+def test_full_size_queue_properties(fp32_net):
+    n = 2_073_600
+    v = nb.synth(21, n)
+    random_params(fp32_net, 5)
+    dp = nb.default_decide()
+    d = upload(v)
+    cap = 9 * n
+    st, rrs, norm = empty(3 * n), empty(n), empty(n)
+    split, q, sz = empty(n, "uint8"), empty(cap, "int32"), empty(1, "int32")
+    fp32_net.generateRRSNumber(soa(d), d["rnd"], n, n, 0, dp, st, rrs, norm, split, q, cap, sz,
+                               stream())
+    tot = int(host(sz, np.uint32)[0])
+    s = host(split)[:n].astype(np.int64)
+    qq = host(q, np.uint32)[:tot]
+    assert tot == s.sum()
+    assert np.all(np.diff(qq.astype(np.int64)) >= 0)
+    assert np.array_equal(np.bincount(qq, minlength=n), s)
+    o = O.decide_emit(host(rrs)[:n], v["rnd"], n, 0, dp, shift_n=MAXQ)
+    assert tot == o["total"] and np.array_equal(s, o["split"])
+    rc, flags = fp32_net.device_status(stream())
+    assert rc == nb.OK and flags == 0
+
+
+def test_save_load_roundtrip(fp32_net, tmp_path):
+    p = random_params(fp32_net, 6)
+    f = tmp_path / "ckpt.bin"
+    fp32_net.saveWeights(f)
+    other = make_net()
+    other.loadWeights(f)
+    assert np.array_equal(other.get_params(), p)
+    other.close()
