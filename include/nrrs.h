@@ -214,6 +214,23 @@ int nrrs_load(nrrs_ctx* ctx, const char* path);
 /* ---- status: synchronises the stream, returns and clears the device status bits ---- */
 int nrrs_get_device_status(nrrs_ctx* ctx, uint32_t* flags, void* stream);
 
+/* ---- instrumentation: launch counters and optional CUDA-event timing per kernel kind.
+ *      The reference's equivalent is KiRaRay's PROFILE("...") scopes (integrator.cpp:1069,
+ *      1151, 1158, 1302, 1346, 2638). Timing records one event pair per launch on the launch
+ *      stream while enabled; nrrs_profile_read synchronises on those events. ---- */
+typedef enum {
+    NRRS_KERNEL_INFER_FP32 = 0, NRRS_KERNEL_INFER_TC = 1, NRRS_KERNEL_SUM = 2,
+    NRRS_KERNEL_DECIDE = 3, NRRS_KERNEL_PACK = 4, NRRS_KERNEL_TABLE_HALF = 5,
+    NRRS_KERNEL_TRAIN_STAT = 6, NRRS_KERNEL_TRAIN_RRS = 7, NRRS_KERNEL_TRAIN_WGRAD = 8,
+    NRRS_KERNEL_TRAIN_REDUCE = 9, NRRS_KERNEL_ADAM = 10, NRRS_KERNEL_KINDS = 11
+} nrrs_kernel_kind;
+uint64_t nrrs_launch_count(const nrrs_ctx* ctx);
+/* grid (CTAs) of the last inference launch: SMs x resident CTAs per SM */
+int32_t nrrs_last_infer_grid(const nrrs_ctx* ctx);
+const char* nrrs_kernel_name(int32_t kind);
+int nrrs_profile_enable(nrrs_ctx* ctx, int32_t enable);
+int nrrs_profile_read(nrrs_ctx* ctx, int32_t kind, uint64_t* launches, double* total_ms);
+
 /* ---- synthetic inputs (host, deterministic): mt19937_64 + explicit transforms. Buffers are
  *      HOST arrays sized as in nrrs_vertex_soa; any may be NULL to skip. target [n][3]. ---- */
 void nrrs_synth_vertices(uint64_t seed, uint64_t first, uint64_t n, float* pos, float* wi,

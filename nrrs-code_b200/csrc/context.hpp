@@ -7,8 +7,23 @@
 // allocates per frame size; capacities here are max_queue / max_train).
 #pragma once
 #include <string>
+#include <vector>
 
 #include "kernels.hpp"
+
+namespace nrrs {
+// launch counters and optional per-launch CUDA-event timing (nrrs_profile_*)
+struct Profiler {
+    bool enabled = false;
+    uint64_t launches[NRRS_KERNEL_KINDS] = {};
+    uint64_t total_launches = 0;
+    std::vector<cudaEvent_t> pool;                    // event pairs, reused
+    std::vector<std::pair<int, int>> pending[NRRS_KERNEL_KINDS];
+    size_t next = 0;
+    uint64_t timed_launches[NRRS_KERNEL_KINDS] = {};
+    double timed_ms[NRRS_KERNEL_KINDS] = {};
+};
+}  // namespace nrrs
 
 struct nrrs_ctx {
     nrrs_config cfg{};
@@ -39,9 +54,38 @@ struct nrrs_ctx {
     size_t train_scratch_bytes = 0;
     double* loss_dev = nullptr;  // [2] last losses
 
+    int last_infer_grid = 0;
     int tc_ctas_per_sm = 0;      // autotuned occupancy of the tcgen05 kernel (0 = default)
+    nrrs::Profiler prof;
     std::string last_error;
 };
+
+namespace nrrs {
+// RAII scope around one kernel launch: counts it and, when profiling is on, records an event
+// pair on the launch stream.
+struct ProfScope {
+    nrrs_ctx* ctx;
+    int kind;
+    cudaStream_t s;
+    int ev = -1;
+    ProfScope(nrrs_ctx* c, int k, cudaStream_t st) : ctx(c), kind(k), s(st) {
+        ++ctx->prof.launches[kind];
+        ++ctx->prof.total_launches;
+        Profiler& p = ctx->prof;
+        if (p.enabled && p.next + 2 <= p.pool.size()) {
+            ev = (int)p.next;
+            p.next += 2;
+            cudaEventRecord(p.pool[ev], s);
+        }
+    }
+    ~ProfScope() {
+        if (ev >= 0) {
+            cudaEventRecord(ctx->prof.pool[ev + 1], s);
+            ctx->prof.pending[kind].push_back({ev, ev + 1});
+        }
+    }
+};
+}  // namespace nrrs
 
 namespace nrrs {
 int train_step_impl(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint32_t n,

@@ -169,13 +169,11 @@ cudaError_t launch_cfg(const InferArgs& a, int sm_count, cudaStream_t s) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTile, smem);
-    if (e != cudaSuccess) return e;
-    if (per_sm < 1) per_sm = 1;
+    const int per_sm = resident_ctas((const void*)kern, kTile, smem, 32);
     unsigned grid = (unsigned)(sm_count * per_sm);
     if (grid > a.segs.total_tiles) grid = a.segs.total_tiles;
     if (grid == 0) return cudaSuccess;
+    g_last_grid = (int)grid;
     kern<<<grid, kTile, smem, s>>>(a);
     return cudaGetLastError();
 }

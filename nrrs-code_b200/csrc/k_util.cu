@@ -83,6 +83,27 @@ __global__ void k_table_half(const float* t, __half* h, size_t n) {
 
 }  // namespace
 
+thread_local int g_last_grid = 0;
+
+int resident_ctas(const void* kern, int threads, size_t dyn_smem, int cap) {
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess) return 1;
+    int dev = 0, smem_sm = 0, regs_sm = 0, thr_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
+    const size_t per_cta_smem = dyn_smem + fa.sharedSizeBytes + 1024;
+    int by_smem = (int)((size_t)smem_sm / per_cta_smem);
+    const int regs = (fa.numRegs + 7) / 8 * 8;  // allocation granularity per thread
+    int by_regs = regs > 0 ? regs_sm / (regs * threads) : 32;
+    int by_thr = thr_sm / threads;
+    int n = by_smem < by_regs ? by_smem : by_regs;
+    n = n < by_thr ? n : by_thr;
+    n = n < cap ? n : cap;
+    return n < 1 ? 1 : n;
+}
+
 size_t transposed_weight_floats(int ws, int hs, int wr, int hr) {
     size_t t = 0;
     for (int l = 0; l <= hs; ++l) {

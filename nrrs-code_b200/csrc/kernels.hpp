@@ -51,6 +51,12 @@ struct InferArgs {
     DecideScratch* scr;           // accumulate the exact sum when not null
 };
 
+// resident CTAs per SM of a kernel from its own resources (shared memory incl. the 1 KB the
+// runtime reserves per CTA, registers, warps), capped by `cap` (TMEM columns or a tuning choice)
+int resident_ctas(const void* kern, int threads, size_t dyn_smem, int cap);
+// grid of the last inference launch (diagnostics)
+extern thread_local int g_last_grid;
+
 // decision + emission (single pass, decoupled look-back)
 cudaError_t launch_decide(const DecideArgs& a, cudaStream_t s);
 // exact sum of rrs (or ceil) per segment into scr->sum_acc

@@ -146,11 +146,16 @@ SegmentTable make_segments(const nrrs_segment* segs, int n, uint32_t unit) {
 
 int refresh_derived(nrrs_ctx* ctx, cudaStream_t s) {
     const nrrs_config& c = ctx->cfg;
-    cudaError_t e = launch_pack_weights(ctx->params + ctx->n_table, ctx->wt, ctx->wpack,
-                                        c.statnet_width, c.statnet_hidden, c.rrsnet_width,
-                                        c.rrsnet_hidden, c.precision, s);
+    cudaError_t e;
+    {
+        ProfScope ps(ctx, NRRS_KERNEL_PACK, s);
+        e = launch_pack_weights(ctx->params + ctx->n_table, ctx->wt, ctx->wpack,
+                                c.statnet_width, c.statnet_hidden, c.rrsnet_width,
+                                c.rrsnet_hidden, c.precision, s);
+    }
     if (e != cudaSuccess) return cuda_fail(ctx, e, "pack weights");
     if (ctx->table_h) {
+        ProfScope ps(ctx, NRRS_KERNEL_TABLE_HALF, s);
         e = launch_table_to_half(ctx->params, ctx->table_h, ctx->n_table, s);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "table to half");
     }
@@ -175,6 +180,8 @@ int run_infer(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const SegmentTable& segs,
     a.scr = accumulate ? ctx->scr : nullptr;
     const nrrs_config& c = ctx->cfg;
     cudaError_t e;
+    if (segs.total_tiles == 0) return NRRS_OK;
+    ProfScope ps(ctx, c.precision == NRRS_PREC_FP32 ? NRRS_KERNEL_INFER_FP32 : NRRS_KERNEL_INFER_TC, s);
     if (c.precision == NRRS_PREC_FP32)
         e = launch_infer_fp32(a, c.statnet_width, c.statnet_hidden, c.rrsnet_width,
                               c.rrsnet_hidden, ctx->sm_count, s);
@@ -182,6 +189,7 @@ int run_infer(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const SegmentTable& segs,
         e = launch_infer_tc(a, c.statnet_width, c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden,
                             c.precision, ctx->sm_count, ctx->tc_ctas_per_sm, s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "inference launch");
+    ctx->last_infer_grid = g_last_grid;
     return NRRS_OK;
 }
 
@@ -197,7 +205,13 @@ int run_decide(nrrs_ctx* ctx, const float* rrs, const float* rnd, const uint32_t
         sa.scr = ctx->scr;
         sa.segs = make_segments(segs, n_segs, kTile);
         sa.fp = fp;
-        cudaError_t e = launch_sum(sa, s);
+        cudaError_t e;
+        if (sa.segs.total_tiles == 0) {
+            e = cudaSuccess;
+        } else {
+            ProfScope ps(ctx, NRRS_KERNEL_SUM, s);
+            e = launch_sum(sa, s);
+        }
         if (e != cudaSuccess) return cuda_fail(ctx, e, "sum launch");
     }
     DecideArgs d{};
@@ -224,7 +238,11 @@ int run_decide(nrrs_ctx* ctx, const float* rrs, const float* rnd, const uint32_t
         if (e != cudaSuccess) return cuda_fail(ctx, e, "memset next_size");
         return NRRS_OK;
     }
-    cudaError_t e = launch_decide(d, s);
+    cudaError_t e;
+    {
+        ProfScope ps(ctx, NRRS_KERNEL_DECIDE, s);
+        e = launch_decide(d, s);
+    }
     if (e != cudaSuccess) {
         cudaMemsetAsync(ctx->scr, 0, offsetof(DecideScratch, epoch), s);
         return cuda_fail(ctx, e, "decide launch");
@@ -437,6 +455,7 @@ int nrrs_create(const nrrs_config* cfg, nrrs_ctx** out) {
 
 void nrrs_destroy(nrrs_ctx* ctx) {
     if (!ctx) return;
+    for (cudaEvent_t ev : ctx->prof.pool) cudaEventDestroy(ev);
     cudaFree(ctx->params);
     cudaFree(ctx->grads);
     cudaFree(ctx->adam_m);
@@ -663,6 +682,54 @@ int nrrs_get_device_status(nrrs_ctx* ctx, uint32_t* flags, void* stream) {
     if (h & NRRS_DEV_TIMEOUT) return NRRS_ERR_TIMEOUT;
     if (h & NRRS_DEV_OVERFLOW) return NRRS_ERR_CAPACITY_OVERFLOW;
     if (h & NRRS_DEV_NAN) return NRRS_ERR_NAN;
+    return NRRS_OK;
+}
+
+uint64_t nrrs_launch_count(const nrrs_ctx* ctx) { return ctx ? ctx->prof.total_launches : 0; }
+
+int32_t nrrs_last_infer_grid(const nrrs_ctx* ctx) { return ctx ? ctx->last_infer_grid : 0; }
+
+const char* nrrs_kernel_name(int32_t kind) {
+    static const char* names[NRRS_KERNEL_KINDS] = {
+        "infer_fp32", "infer_tc", "sum", "decide", "pack_weights", "table_half",
+        "train_statnet", "train_rrsnet", "train_wgrad", "train_reduce", "adam"};
+    return (kind >= 0 && kind < NRRS_KERNEL_KINDS) ? names[kind] : "unknown";
+}
+
+int nrrs_profile_enable(nrrs_ctx* ctx, int32_t enable) {
+    if (!ctx) return NRRS_ERR_INVALID_ARG;
+    Profiler& p = ctx->prof;
+    if (enable && p.pool.empty()) {
+        p.pool.resize(16384);
+        for (auto& ev : p.pool) {
+            cudaError_t e = cudaEventCreate(&ev);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "event create");
+        }
+    }
+    p.enabled = enable != 0;
+    return NRRS_OK;
+}
+
+int nrrs_profile_read(nrrs_ctx* ctx, int32_t kind, uint64_t* launches, double* total_ms) {
+    if (!ctx || kind < 0 || kind >= NRRS_KERNEL_KINDS) return NRRS_ERR_INVALID_ARG;
+    Profiler& p = ctx->prof;
+    // fold every pending pair of every kind, then recycle the pool
+    for (int k = 0; k < NRRS_KERNEL_KINDS; ++k) {
+        for (auto& pr : p.pending[k]) {
+            cudaError_t e = cudaEventSynchronize(p.pool[pr.second]);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "event sync");
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, p.pool[pr.first], p.pool[pr.second]);
+            p.timed_ms[k] += ms;
+            ++p.timed_launches[k];
+        }
+        p.pending[k].clear();
+    }
+    p.next = 0;
+    if (launches) *launches = p.timed_launches[kind];
+    if (total_ms) *total_ms = p.timed_ms[kind];
+    p.timed_launches[kind] = 0;
+    p.timed_ms[kind] = 0.0;
     return NRRS_OK;
 }
 

@@ -117,7 +117,16 @@ _SIGS = {
     "nrrs_load": (C.c_int, [C.c_void_p, C.c_char_p]),
     "nrrs_get_device_status": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.c_void_p]),
     "nrrs_synth_vertices": (None, [C.c_uint64, C.c_uint64, C.c_uint64] + [C.c_void_p] * 10),
+    "nrrs_launch_count": (C.c_uint64, [C.c_void_p]),
+    "nrrs_last_infer_grid": (C.c_int32, [C.c_void_p]),
+    "nrrs_kernel_name": (C.c_char_p, [C.c_int32]),
+    "nrrs_profile_enable": (C.c_int, [C.c_void_p, C.c_int32]),
+    "nrrs_profile_read": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_uint64),
+                                    C.POINTER(C.c_double)]),
 }
+
+KERNEL_KINDS = ("infer_fp32", "infer_tc", "sum", "decide", "pack_weights", "table_half",
+                "train_statnet", "train_rrsnet", "train_wgrad", "train_reduce", "adam")
 
 
 def lib():
@@ -318,6 +327,25 @@ class NRRSNetwork:
         a = np.zeros((self.config.n_levels, 4), np.uint32)
         self._check(lib().nrrs_level_table(self._h, a.ctypes.data, self.config.n_levels))
         return a
+
+    def last_infer_grid(self) -> int:
+        return int(lib().nrrs_last_infer_grid(self._h))
+
+    def launch_count(self) -> int:
+        return int(lib().nrrs_launch_count(self._h))
+
+    def profile(self, enable: bool = True):
+        self._check(lib().nrrs_profile_enable(self._h, int(enable)))
+
+    def profile_read(self) -> dict:
+        """{kernel name: (launches, total ms)} of the launches timed since the last read"""
+        out = {}
+        for k, name in enumerate(KERNEL_KINDS):
+            n, ms = C.c_uint64(), C.c_double()
+            self._check(lib().nrrs_profile_read(self._h, k, C.byref(n), C.byref(ms)))
+            if n.value:
+                out[name] = (int(n.value), float(ms.value))
+        return out
 
     def device_status(self, stream=0) -> tuple[int, int]:
         f = C.c_uint32()

@@ -171,3 +171,63 @@ def test_save_load_roundtrip(fp32_net, tmp_path):
     other.loadWeights(f)
     assert np.array_equal(other.get_params(), p)
     other.close()
+
+
+SHAPES = {"w64h2": dict(statnet_width=64, statnet_hidden=2, rrsnet_width=64, rrsnet_hidden=2),
+          "w128h3": dict(statnet_width=128, statnet_hidden=3, rrsnet_width=128, rrsnet_hidden=3,
+                         log2_hashmap_size=22)}
+
+
+@pytest.mark.parametrize("prec", [nb.PREC_FP16, nb.PREC_BF16], ids=["fp16", "bf16"])
+@pytest.mark.parametrize("shape", list(SHAPES))
+def test_mixed_infer_vs_fp64_oracle(prec, shape):
+    """tcgen05 path: RRS factors within 1e-2 relative of the FP64 oracle (workload target)."""
+    net = make_net(precision=prec, **SHAPES[shape])
+    p = random_params(net, 7, table_scale=0.5, mlp_scale=0.15)
+    n = 16384 if shape == "w128h3" else 65536
+    v = nb.synth(1, n)
+    for source in (nb.FACTOR_RRSNET, nb.FACTOR_ADRRS):
+        dp = nb.default_decide(factor_source=source)
+        stats, rrs = run_infer(net, v, dp, n)
+        o = O.infer(net.config, p, v, dp, "f64")
+        rel = np.abs(rrs - o["rrs"]) / o["rrs"]
+        assert rel.max() < MIXED_RTOL, (source, rel.max())
+        err = np.abs(stats - o["stats"])
+        assert err.max() < 0.05 * max(1.0, np.abs(o["stats"]).max()), err.max()
+    net.close()
+
+
+@pytest.mark.parametrize("shape", list(SHAPES))
+def test_fp32_shapes_vs_oracle(shape):
+    net = make_net(**SHAPES[shape])
+    p = random_params(net, 8, table_scale=0.5, mlp_scale=0.15)
+    n = 8192
+    v = nb.synth(2, n)
+    dp = nb.default_decide()
+    stats, rrs = run_infer(net, v, dp, n)
+    o = O.infer(net.config, p, v, dp, "f32")
+    assert np.allclose(stats, o["stats"], rtol=FP32_RTOL, atol=FP32_ATOL)
+    assert np.allclose(rrs, o["rrs"], rtol=FP32_RTOL, atol=FP32_ATOL)
+    net.close()
+
+
+@pytest.mark.parametrize("prec", [nb.PREC_FP16, nb.PREC_BF16], ids=["fp16", "bf16"])
+def test_mixed_step_decisions_match_oracle(prec):
+    """decisions are bit-exact given the (mixed-precision) factors the GPU produced"""
+    net = make_net(precision=prec)
+    random_params(net, 9, table_scale=0.5, mlp_scale=0.15)
+    n = 300007
+    v = nb.synth(4, n)
+    d = upload(v)
+    dp = nb.default_decide()
+    cap = 9 * n
+    st, rrs, norm = empty(3 * n), empty(n), empty(n)
+    split, q, sz = empty(n, "uint8"), empty(cap, "int32"), empty(1, "int32")
+    net.generateRRSNumber(soa(d), d["rnd"], n, n, 0, dp, st, rrs, norm, split, q, cap, sz, stream())
+    tot = int(host(sz, np.uint32)[0])
+    o = O.decide_emit(host(rrs)[:n], v["rnd"], n, 0, dp, shift_n=MAXQ)
+    assert tot == o["total"]
+    assert np.array_equal(host(split)[:n], o["split"])
+    assert np.array_equal(host(q, np.uint32)[:tot], o["queue"])
+    assert np.array_equal(host(norm)[:n].view(np.uint32), o["rrs_norm"].view(np.uint32))
+    net.close()
