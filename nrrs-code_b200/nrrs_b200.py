@@ -117,6 +117,10 @@ _SIGS = {
     "nrrs_load": (C.c_int, [C.c_void_p, C.c_char_p]),
     "nrrs_get_device_status": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.c_void_p]),
     "nrrs_synth_vertices": (None, [C.c_uint64, C.c_uint64, C.c_uint64] + [C.c_void_p] * 10),
+    "nrrs_decide_emit_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                           C.c_uint32, C.c_uint32, C.POINTER(DecideParams),
+                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                           C.c_void_p, C.c_void_p]),
     "nrrs_launch_count": (C.c_uint64, [C.c_void_p]),
     "nrrs_last_infer_grid": (C.c_int32, [C.c_void_p]),
     "nrrs_kernel_name": (C.c_char_p, [C.c_int32]),
@@ -202,6 +206,19 @@ def synth(seed: int, n: int, first: int = 0):
                               ("pos", "wi", "normal", "roughness", "albedo", "thp", "depth",
                                "rnd", "ref_mean", "target")))
     return out
+
+
+NOALLOC_MAX_N = 1 << 24
+
+
+def decide_emit_noalloc(rrs, rnd, n, budget, n_specular, params, rrs_norm, split, queue,
+                        capacity, next_size, scatter_index=None, stream=0) -> int:
+    """nrrs_decide_emit_noalloc: the decision + emission without a context or any device
+    allocation (scratch lives in a static device array). Returns the status code."""
+    return lib().nrrs_decide_emit_noalloc(_ptr(rrs), _ptr(rnd), _ptr(scatter_index), n, budget,
+                                          n_specular, C.byref(params), _ptr(rrs_norm),
+                                          _ptr(split), _ptr(queue), capacity, _ptr(next_size),
+                                          stream)
 
 
 VERTEX_FIELDS = ("pos", "wi", "normal", "roughness", "albedo", "thp", "depth", "ref_mean")
