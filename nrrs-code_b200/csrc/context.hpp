@@ -41,6 +41,7 @@ struct nrrs_ctx {
 
     __half* table_h = nullptr; // FP16 table copy (mixed precision)
     float* wt = nullptr;       // transposed FP32 MLP weights
+    float* wrow = nullptr;     // aligned row-major copy of the FP32 MLP weights
     void* wpack = nullptr;     // UMMA-packed FP16/BF16 MLP weights
     size_t wt_floats = 0, wpack_bytes = 0;
     size_t wt_rrs_offset = 0;  // floats from wt to the RRSNet part

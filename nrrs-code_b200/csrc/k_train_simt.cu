@@ -1,10 +1,679 @@
-// k_train_simt.cu -- training step (placeholder until the kernels land).
+// k_train_simt.cu -- one training step of StatNet and RRSNet (replaces NRRSNetwork::train,
+// src/render/nrrs/net/network.cpp:196-295, and the two tcnn Trainer::training_step calls it makes:
+// myNetworkLL2.cpp:51 for StatNet, network.cpp:274 for RRSNet).
+//
+// Losses (the reference's NRRS_LL2 / NRRS_RRS live in the absent tiny-cuda-nn fork; these are
+// the workload's written definitions):
+//   StatNet: loss_S = mean over samples and RGB of (y_c - log(L_c + stat_eps))^2
+//   RRSNet:  q = activationSigma(raw), r = min(mean_c(thp_c L_c)/(ref + ref_eps), clamp),
+//            V = mean(r^2 / q), C = mean(cost_offset + q), loss_R = V * C
+//   RRSNet inputs come from the detached StatNet forward of the same step (the reference trains
+//   the networks separately and builds RRSNet's input after StatNet's step, train.cu:155-240).
+//
+// Pipeline (all on the caller's stream, no host synchronisation):
+//   k_train_stat  per sample: encode, StatNet forward, loss gradient, backward to the input,
+//                 hash-grid scatter-add (FP32 atomics), glue; RRSNet forward for the batch sums
+//                 V and C (FP64 per-CTA partials). Activations and deltas go to feature-major
+//                 scratch for the weight gradients.
+//   k_train_rrs   per sample: RRSNet forward and backward with the final V and C.
+//   k_wgrad       dW = sum_i delta_i (x) a_i for every layer, split over sample chunks.
+//   k_wreduce     chunk partials -> gradients, in fixed order (deterministic).
+//   k_adam        Adam on FP32 master weights/moments; writes the FP16 table copy in the same pass.
 #include "context.hpp"
 
 namespace nrrs {
-size_t train_scratch_bytes(const nrrs_config&, uint32_t, int) { return 256; }
-int train_step_impl(nrrs_ctx* ctx, const VertexPtrs&, const float*, uint32_t, double*, cudaStream_t) {
-    ctx->last_error = "training not built yet";
-    return NRRS_ERR_UNSUPPORTED;
+
+namespace {
+
+constexpr int kTT = 128;           // samples per tile (threads per CTA)
+constexpr int kChunk = 2048;       // samples per weight-gradient partial
+constexpr int kMaxJobs = 8;
+
+struct TrainArgs {
+    VertexPtrs v;
+    const float* target;
+    uint32_t n;
+    uint32_t ld;                   // row stride of the feature-major scratch
+    EncodeParams enc;
+    FactorParams fp;
+    float loss_clamp, cost_offset;
+    int32_t train_rrs;
+    const float* table;
+    float* table_grad;
+    const float* wt_stat;          // transposed [in][out4] (forward)
+    const float* wt_rrs;
+    const float* w_stat;           // row-major master [out][in] (backward)
+    const float* w_rrs;
+    float* act;                    // feature-major scratch
+    uint32_t r_x0, r_hs, r_dhs, r_dy, r_x1, r_hr, r_dhr, r_draw;
+    double* part;                  // [grid][4]: loss_S sum, V sum, C sum
+    uint32_t part_n;               // CTAs of k_train_stat
+    double* loss_out;              // [2]
+};
+
+// out_col[o] = sum_k W[k][o] * in_col[k] (Wt stored [IN][OUTP]); columns of this thread in smem
+template <int IN, int OUT, int OUTP, bool RELU>
+__device__ __forceinline__ void dense(const float* __restrict__ Wt, const float* in_col,
+                                      float* out_col, float* out_reg) {
+    float acc[OUT];
+#pragma unroll
+    for (int o = 0; o < OUT; ++o) acc[o] = 0.f;
+#pragma unroll 2
+    for (int k = 0; k < IN; ++k) {
+        const float xk = in_col[k * kTT];
+        const float4* w4 = reinterpret_cast<const float4*>(Wt + k * OUTP);
+#pragma unroll
+        for (int o4 = 0; o4 < OUTP / 4; ++o4) {
+            const float4 w = w4[o4];
+            if (4 * o4 + 0 < OUT) acc[4 * o4 + 0] = fmaf(w.x, xk, acc[4 * o4 + 0]);
+            if (4 * o4 + 1 < OUT) acc[4 * o4 + 1] = fmaf(w.y, xk, acc[4 * o4 + 1]);
+            if (4 * o4 + 2 < OUT) acc[4 * o4 + 2] = fmaf(w.z, xk, acc[4 * o4 + 2]);
+            if (4 * o4 + 3 < OUT) acc[4 * o4 + 3] = fmaf(w.w, xk, acc[4 * o4 + 3]);
+        }
+    }
+#pragma unroll
+    for (int o = 0; o < OUT; ++o) {
+        const float r = RELU ? fmaxf(acc[o], 0.f) : acc[o];
+        if (out_col) out_col[o * kTT] = r;
+        if (out_reg) out_reg[o] = r;
+    }
 }
+
+// backward through one layer with a row-major W [OUTF][INF]:
+// out_col[k] = sum_o W[o][k] * din[o]   (din: smem column), optionally masked by act > 0
+template <int OUTF, int INF, int INF_EFF>
+__device__ __forceinline__ void dense_t(const float* __restrict__ W, const float* din_col,
+                                        float* dout_col, const float* mask_g, uint32_t ld,
+                                        float* dout_g) {
+    // W rows are contiguous in k: treat W as "Wt" with IN = OUTF rows of INF outputs
+    float acc[INF_EFF];
+#pragma unroll
+    for (int k = 0; k < INF_EFF; ++k) acc[k] = 0.f;
+#pragma unroll 2
+    for (int o = 0; o < OUTF; ++o) {
+        const float d = din_col[o * kTT];
+        const float* wr = W + o * INF;
+#pragma unroll
+        for (int k4 = 0; k4 < INF_EFF / 4; ++k4) {
+            const float4 w = reinterpret_cast<const float4*>(wr)[k4];
+            acc[4 * k4 + 0] = fmaf(w.x, d, acc[4 * k4 + 0]);
+            acc[4 * k4 + 1] = fmaf(w.y, d, acc[4 * k4 + 1]);
+            acc[4 * k4 + 2] = fmaf(w.z, d, acc[4 * k4 + 2]);
+            acc[4 * k4 + 3] = fmaf(w.w, d, acc[4 * k4 + 3]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < INF_EFF; ++k) {
+        float g = acc[k];
+        if (mask_g && !(mask_g[(size_t)k * ld] > 0.f)) g = 0.f;
+        if (dout_col) dout_col[k * kTT] = g;
+        if (dout_g) dout_g[(size_t)k * ld] = g;
+    }
+}
+
+__device__ __forceinline__ double block_sum_d(double v, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+        for (int k = 0; k < kTT / 32; ++k) t += red[k];
+    return t;  // valid on thread 0
+}
+
+// relative contribution used by the RRS loss
+__device__ __forceinline__ float rel_contrib(const TrainArgs& a, uint32_t i) {
+    const size_t i3 = 3 * (size_t)i;
+    float acc = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) acc += a.v.thp[i3 + c] * a.target[i3 + c];
+    const float ref = (a.v.ref ? a.v.ref[i] : 0.5f) + a.fp.ref_eps;
+    const float r = acc / 3.0f / ref;
+    return r < a.loss_clamp ? r : a.loss_clamp;
+}
+
+template <int WS, int HS, int WR, int HR>
+__global__ void __launch_bounds__(kTT) k_train_stat(const __grid_constant__ TrainArgs a) {
+    constexpr int XW = WS > 64 ? WS : 64;
+    extern __shared__ float smem[];
+    __shared__ double red[kTT / 32];
+    float* colA = smem + threadIdx.x;            // activations
+    float* colB = smem + XW * kTT + threadIdx.x; // deltas
+    const int tid = threadIdx.x;
+    const uint32_t ld = a.ld;
+    double lossS = 0.0, sumV = 0.0, sumC = 0.0;
+    const float2* table = reinterpret_cast<const float2*>(a.table);
+    const uint32_t tiles = (a.n + kTT - 1) / kTT;
+    for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const uint32_t i = t * kTT + tid;
+        if (i >= a.n) continue;
+        float* act = a.act + i;
+        // ---- encode (StatNet input lanes 0..55) ----
+        float p[3];
+        norm_pos(a.enc, a.v.pos, i, p);
+#pragma unroll 2
+        for (int l = 0; l < kMaxLevels; ++l) {
+            const LevelDev L = a.enc.lv[l];
+            const CellCoord c = cell_of(p, L.res);
+            float f0 = 0.f, f1 = 0.f;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const uint32_t row = grid_row(L, a.enc.hash_mask, c.ix + (k & 1),
+                                              c.iy + ((k >> 1) & 1), c.iz + ((k >> 2) & 1));
+                const float2 tv = __ldg(table + row);
+                const float w = corner_weight(c, k);
+                f0 += w * tv.x;
+                f1 += w * tv.y;
+            }
+            colA[(2 * l) * kTT] = f0;
+            colA[(2 * l + 1) * kTT] = f1;
+        }
+        {
+            float sh[16], m[16];
+            const size_t i3 = 3 * (size_t)i;
+            sh16(a.v.wi[i3], a.v.wi[i3 + 1], a.v.wi[i3 + 2], sh);
+#pragma unroll
+            for (int k = 0; k < 16; ++k) colA[(32 + k) * kTT] = sh[k];
+            misc_lanes(a.v, i, m);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) colA[(48 + k) * kTT] = m[k];
+        }
+#pragma unroll 4
+        for (int k = 0; k < 56; ++k) act[(size_t)(a.r_x0 + k) * ld] = colA[k * kTT];
+
+        // ---- StatNet forward, storing every hidden activation ----
+        const float* Wt = a.wt_stat;
+        dense<56, WS, WS, true>(Wt, colA, colA, nullptr);
+        Wt += kStatIn * WS;
+#pragma unroll 4
+        for (int k = 0; k < WS; ++k) act[(size_t)(a.r_hs + k) * ld] = colA[k * kTT];
+#pragma unroll 1
+        for (int h = 1; h < HS; ++h) {
+            dense<WS, WS, WS, true>(Wt, colA, colA, nullptr);
+            Wt += WS * WS;
+#pragma unroll 4
+            for (int k = 0; k < WS; ++k) act[(size_t)(a.r_hs + h * WS + k) * ld] = colA[k * kTT];
+        }
+        float y[3];
+        dense<WS, 3, 4, false>(Wt, colA, nullptr, y);
+
+        // ---- StatNet loss gradient ----
+        const size_t i3 = 3 * (size_t)i;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float d = y[c] - logf(a.target[i3 + c] + a.fp.stat_eps);
+            lossS += (double)d * (double)d;
+            const float g = 2.0f * d / (3.0f * (float)a.n);
+            colB[c * kTT] = g;
+            act[(size_t)(a.r_dy + c) * ld] = g;
+        }
+
+        // ---- backward to the hash lanes ----
+        // output layer: W_out [3][WS]; d h_last = W_out^T dy, masked by h_last (in colA)
+        const float* W = a.w_stat;
+        const float* Wl[4];
+        Wl[0] = W;
+        Wl[1] = W + kStatIn * WS;
+        for (int h = 2; h <= HS; ++h) Wl[h] = Wl[h - 1] + WS * WS;
+        {
+            float acc[WS];
+#pragma unroll
+            for (int k = 0; k < WS; ++k) acc[k] = 0.f;
+#pragma unroll
+            for (int o = 0; o < 3; ++o) {
+                const float d = colB[o * kTT];
+                const float* wr = Wl[HS] + o * WS;
+#pragma unroll
+                for (int k = 0; k < WS; ++k) acc[k] = fmaf(wr[k], d, acc[k]);
+            }
+#pragma unroll
+            for (int k = 0; k < WS; ++k) {
+                const float g = colA[k * kTT] > 0.f ? acc[k] : 0.f;
+                colB[k * kTT] = g;
+                act[(size_t)(a.r_dhs + (HS - 1) * WS + k) * ld] = g;
+            }
+        }
+#pragma unroll 1
+        for (int h = HS - 1; h >= 1; --h) {
+            // d h_{h-1} = W_h^T d h_h masked by h_{h-1} (from scratch)
+            dense_t<WS, WS, WS>(Wl[h], colB, colB, act + (size_t)(a.r_hs + (h - 1) * WS) * ld, ld,
+                                act + (size_t)(a.r_dhs + (h - 1) * WS) * ld);
+        }
+        // dx0 lanes 0..31 = W_0^T d h_0
+        float dx[32];
+        {
+#pragma unroll
+            for (int k = 0; k < 32; ++k) dx[k] = 0.f;
+#pragma unroll 2
+            for (int o = 0; o < WS; ++o) {
+                const float d = colB[o * kTT];
+                const float4* wr = reinterpret_cast<const float4*>(Wl[0] + o * kStatIn);
+#pragma unroll
+                for (int k4 = 0; k4 < 8; ++k4) {
+                    const float4 w = wr[k4];
+                    dx[4 * k4 + 0] = fmaf(w.x, d, dx[4 * k4 + 0]);
+                    dx[4 * k4 + 1] = fmaf(w.y, d, dx[4 * k4 + 1]);
+                    dx[4 * k4 + 2] = fmaf(w.z, d, dx[4 * k4 + 2]);
+                    dx[4 * k4 + 3] = fmaf(w.w, d, dx[4 * k4 + 3]);
+                }
+            }
+        }
+        // hash-grid scatter-add (trilinear weights, FP32 atomics)
+#pragma unroll 2
+        for (int l = 0; l < kMaxLevels; ++l) {
+            const LevelDev L = a.enc.lv[l];
+            const CellCoord c = cell_of(p, L.res);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const uint32_t row = grid_row(L, a.enc.hash_mask, c.ix + (k & 1),
+                                              c.iy + ((k >> 1) & 1), c.iz + ((k >> 2) & 1));
+                const float w = corner_weight(c, k);
+                atomicAdd(a.table_grad + 2 * (size_t)row, w * dx[2 * l]);
+                atomicAdd(a.table_grad + 2 * (size_t)row + 1, w * dx[2 * l + 1]);
+            }
+        }
+
+        // ---- glue and RRSNet forward for the batch sums ----
+        if (a.train_rrs) {
+            float x1[16];
+            glue16(a.fp, y, a.v, i, x1);
+#pragma unroll
+            for (int k = 0; k < 10; ++k) {
+                colA[k * kTT] = x1[k];
+                act[(size_t)(a.r_x1 + k) * ld] = x1[k];
+            }
+            const float* Wr = a.wt_rrs;
+            dense<10, WR, WR, true>(Wr, colA, colA, nullptr);
+            Wr += kRrsIn * WR;
+#pragma unroll 1
+            for (int h = 1; h < HR; ++h) {
+                dense<WR, WR, WR, true>(Wr, colA, colA, nullptr);
+                Wr += WR * WR;
+            }
+            float raw;
+            dense<WR, 1, 4, false>(Wr, colA, nullptr, &raw);
+            const float q = act_sigma(raw);
+            const float r = rel_contrib(a, i);
+            sumV += (double)(r * r / q);
+            sumC += (double)(a.cost_offset + q);
+        }
+    }
+    const double s0 = block_sum_d(lossS, red);
+    const double s1 = block_sum_d(sumV, red);
+    const double s2 = block_sum_d(sumC, red);
+    if (threadIdx.x == 0) {
+        a.part[4 * blockIdx.x + 0] = s0;
+        a.part[4 * blockIdx.x + 1] = s1;
+        a.part[4 * blockIdx.x + 2] = s2;
+    }
+}
+
+template <int WR, int HR>
+__global__ void __launch_bounds__(kTT) k_train_rrs(const __grid_constant__ TrainArgs a) {
+    constexpr int XW = WR > 64 ? WR : 64;
+    extern __shared__ float smem[];
+    __shared__ double s_tot[3];
+    float* colA = smem + threadIdx.x;
+    float* colB = smem + XW * kTT + threadIdx.x;
+    const int tid = threadIdx.x;
+    const uint32_t ld = a.ld;
+    if (tid < 3) {
+        double t = 0.0;
+        for (uint32_t b = 0; b < a.part_n; ++b) t += a.part[4 * b + tid];
+        s_tot[tid] = t;
+    }
+    __syncthreads();
+    const double Vm = s_tot[1] / (double)a.n, Cm = s_tot[2] / (double)a.n;
+    if (blockIdx.x == 0 && tid == 0) {
+        a.loss_out[0] = s_tot[0] / (3.0 * (double)a.n);
+        a.loss_out[1] = a.train_rrs ? Vm * Cm : 0.0;
+    }
+    if (!a.train_rrs) return;
+    const float Vf = (float)Vm, Cf = (float)Cm;
+    const uint32_t tiles = (a.n + kTT - 1) / kTT;
+    const float* Wl[4];
+    Wl[0] = a.w_rrs;
+    Wl[1] = a.w_rrs + kRrsIn * WR;
+    for (int h = 2; h <= HR; ++h) Wl[h] = Wl[h - 1] + WR * WR;
+    for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const uint32_t i = t * kTT + tid;
+        if (i >= a.n) continue;
+        float* act = a.act + i;
+#pragma unroll
+        for (int k = 0; k < 10; ++k) colA[k * kTT] = act[(size_t)(a.r_x1 + k) * ld];
+        const float* Wt = a.wt_rrs;
+        dense<10, WR, WR, true>(Wt, colA, colA, nullptr);
+        Wt += kRrsIn * WR;
+#pragma unroll 4
+        for (int k = 0; k < WR; ++k) act[(size_t)(a.r_hr + k) * ld] = colA[k * kTT];
+#pragma unroll 1
+        for (int h = 1; h < HR; ++h) {
+            dense<WR, WR, WR, true>(Wt, colA, colA, nullptr);
+            Wt += WR * WR;
+#pragma unroll 4
+            for (int k = 0; k < WR; ++k) act[(size_t)(a.r_hr + h * WR + k) * ld] = colA[k * kTT];
+        }
+        float raw;
+        dense<WR, 1, 4, false>(Wt, colA, nullptr, &raw);
+        const float q = act_sigma(raw);
+        const float r = rel_contrib(a, i);
+        const float dq = (-(r * r) / (q * q) * Cf + Vf) / (float)a.n;
+        const float draw = dq * act_sigma_grad(raw);
+        act[(size_t)a.r_draw * ld] = draw;
+        // output layer W_out [1][WR]: d g_last = W_out^T draw masked by g_last
+        {
+            const float* wr = Wl[HR];
+#pragma unroll 4
+            for (int k = 0; k < WR; ++k) {
+                const float g = colA[k * kTT] > 0.f ? wr[k] * draw : 0.f;
+                colB[k * kTT] = g;
+                act[(size_t)(a.r_dhr + (HR - 1) * WR + k) * ld] = g;
+            }
+        }
+#pragma unroll 1
+        for (int h = HR - 1; h >= 1; --h)
+            dense_t<WR, WR, WR>(Wl[h], colB, colB, act + (size_t)(a.r_hr + (h - 1) * WR) * ld, ld,
+                                act + (size_t)(a.r_dhr + (h - 1) * WR) * ld);
+    }
+}
+
+// ---- weight gradients: dW[o][k] = sum_i D[o][i] * A[k][i] over the batch ----
+struct WJob {
+    uint32_t d_row, a_row;   // first scratch row of the deltas / activations
+    uint32_t M, N;           // outputs x inputs actually stored
+    uint32_t ldw;            // input width of the layer (row stride of W, >= N)
+    uint32_t out;            // offset of the layer in the MLP gradient vector
+};
+
+struct WGradArgs {
+    const float* act;
+    uint32_t ld, n, chunks;
+    float* partial;          // [chunks][total]
+    uint32_t total;          // MLP gradient length
+    int32_t njobs;
+    WJob job[kMaxJobs];
+};
+
+// one CTA: one job x one 64x64 output tile x one sample chunk
+__global__ void __launch_bounds__(256) k_wgrad(const __grid_constant__ WGradArgs a) {
+    __shared__ float sD[32][65];
+    __shared__ float sA[32][65];
+    const WJob& j = a.job[blockIdx.z];
+    const uint32_t tiles_n = (j.N + 63) / 64;
+    const uint32_t tm = blockIdx.y / tiles_n, tn = blockIdx.y % tiles_n;
+    if (tm * 64 >= j.M || tn * 64 >= j.N) return;
+    const uint32_t m0 = tm * 64, n0 = tn * 64;
+    const uint32_t i0 = blockIdx.x * kChunk;
+    const uint32_t i1 = min(a.n, i0 + kChunk);
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    float acc[4][4] = {};
+    for (uint32_t ib = i0; ib < i1; ib += 32) {
+        // stage 32 samples of 64 delta rows and 64 activation rows (samples contiguous)
+        for (int e = threadIdx.x; e < 32 * 64; e += 256) {
+            const int r = e / 32, s = e % 32;
+            const uint32_t i = ib + s;
+            const bool ok_i = i < i1;
+            sD[s][r] = (ok_i && m0 + r < j.M) ? a.act[(size_t)(j.d_row + m0 + r) * a.ld + i] : 0.f;
+            sA[s][r] = (ok_i && n0 + r < j.N) ? a.act[(size_t)(j.a_row + n0 + r) * a.ld + i] : 0.f;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int s = 0; s < 32; ++s) {
+            float d[4], x[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) d[u] = sD[s][ty * 4 + u];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) x[u] = sA[s][tx * 4 + u];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int w = 0; w < 4; ++w) acc[u][w] = fmaf(d[u], x[w], acc[u][w]);
+        }
+        __syncthreads();
+    }
+    float* out = a.partial + (size_t)blockIdx.x * a.total + j.out;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const uint32_t m = m0 + ty * 4 + u;
+        if (m >= j.M) continue;
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+            const uint32_t k = n0 + tx * 4 + w;
+            if (k < j.N) out[(size_t)m * j.ldw + k] = acc[u][w];
+        }
+    }
+}
+
+// gradients = sum of the chunk partials in chunk order; entries no job writes (zero input
+// lanes) are zero in every partial, set once at creation
+__global__ void k_wreduce(const float* partial, uint32_t chunks, uint32_t total, float* grad) {
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+        float s = 0.f;
+        for (uint32_t c = 0; c < chunks; ++c) s += partial[(size_t)c * total + e];
+        grad[e] = s;
+    }
+}
+
+struct AdamArgs {
+    float* p;
+    const float* g;
+    float* m;
+    float* v;
+    __half* table_h;       // FP16 copy of [0, n_table) refreshed in the same pass (may be null)
+    uint64_t n_table;
+    uint64_t first, count;
+    float lr, b1, b2, eps, l2, c1, c2;
+};
+
+__global__ void k_adam(const __grid_constant__ AdamArgs a) {
+    for (uint64_t k = a.first + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+         k < a.first + a.count; k += (uint64_t)gridDim.x * blockDim.x) {
+        const float w = a.p[k];
+        const float g = a.g[k] + a.l2 * w;
+        const float m = a.b1 * a.m[k] + (1.0f - a.b1) * g;
+        const float v = a.b2 * a.v[k] + (1.0f - a.b2) * g * g;
+        a.m[k] = m;
+        a.v[k] = v;
+        const float nw = w - a.lr * (m / a.c1) / (sqrtf(v / a.c2) + a.eps);
+        a.p[k] = nw;
+        if (a.table_h && k < a.n_table) a.table_h[k] = __float2half_rn(nw);
+    }
+}
+
+template <int WS, int HS, int WR, int HR>
+cudaError_t launch_train(nrrs_ctx* ctx, TrainArgs& a, cudaStream_t s) {
+    constexpr int XW = (WS > WR ? WS : WR) > 64 ? (WS > WR ? WS : WR) : 64;
+    const size_t smem = 2 * (size_t)XW * kTT * sizeof(float);
+    auto ks = k_train_stat<WS, HS, WR, HR>;
+    auto kr = k_train_rrs<WR, HR>;
+    cudaError_t e = cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const uint32_t tiles = (a.n + kTT - 1) / kTT;
+    uint32_t grid = (uint32_t)(ctx->sm_count * resident_ctas((const void*)ks, kTT, smem, 16));
+    if (grid > tiles) grid = tiles;
+    a.part_n = grid;
+    {
+        ProfScope ps(ctx, NRRS_KERNEL_TRAIN_STAT, s);
+        ks<<<grid, kTT, smem, s>>>(a);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    {
+        ProfScope ps(ctx, NRRS_KERNEL_TRAIN_RRS, s);
+        kr<<<grid, kTT, smem, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+struct Layout {
+    uint32_t r_x0, r_hs, r_dhs, r_dy, r_x1, r_hr, r_dhr, r_draw, rows;
+};
+
+Layout layout_of(const nrrs_config& c) {
+    Layout L{};
+    uint32_t r = 0;
+    L.r_x0 = r; r += 56;
+    L.r_hs = r; r += c.statnet_hidden * c.statnet_width;
+    L.r_dhs = r; r += c.statnet_hidden * c.statnet_width;
+    L.r_dy = r; r += 4;
+    L.r_x1 = r; r += 16;
+    L.r_hr = r; r += c.rrsnet_hidden * c.rrsnet_width;
+    L.r_dhr = r; r += c.rrsnet_hidden * c.rrsnet_width;
+    L.r_draw = r; r += 4;
+    L.rows = r;
+    return L;
+}
+
+uint32_t ld_of(uint32_t n) { return (n + 127) / 128 * 128; }
+
+}  // namespace
+
+size_t train_scratch_bytes(const nrrs_config& c, uint32_t n, int sm_count) {
+    const Layout L = layout_of(c);
+    const uint64_t mlp = (uint64_t)64 * c.statnet_width + (uint64_t)(c.statnet_hidden - 1) *
+                         c.statnet_width * c.statnet_width + 3ull * c.statnet_width +
+                         16ull * c.rrsnet_width + (uint64_t)(c.rrsnet_hidden - 1) * c.rrsnet_width *
+                         c.rrsnet_width + (uint64_t)c.rrsnet_width;
+    const uint64_t chunks = (n + kChunk - 1) / kChunk;
+    return sizeof(float) * (uint64_t)L.rows * ld_of(n) + sizeof(double) * 4 * (uint64_t)sm_count * 16 +
+           sizeof(float) * chunks * mlp + 1024;
+}
+
+int train_step_impl(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint32_t n,
+                    double* loss_dev, cudaStream_t s) {
+    const nrrs_config& c = ctx->cfg;
+    const Layout L = layout_of(c);
+    const uint32_t ld = ld_of(c.max_train);
+    const uint64_t chunks = (n + kChunk - 1) / kChunk;
+    const uint64_t mlp = ctx->n_stat + ctx->n_rrs;
+    uint8_t* base = reinterpret_cast<uint8_t*>(ctx->train_scratch);
+    float* act = reinterpret_cast<float*>(base);
+    double* part = reinterpret_cast<double*>(base + sizeof(float) * (size_t)L.rows * ld);
+    float* partial = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(part) +
+                                              sizeof(double) * 4 * (size_t)ctx->sm_count * 16);
+    const bool train_rrs = c.step >= 3;
+    cudaError_t e;
+
+    // gradients of this step only
+    e = cudaMemsetAsync(ctx->grads, 0, sizeof(float) * ctx->n_params, s);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(partial, 0, sizeof(float) * chunks * mlp, s);
+    if (e != cudaSuccess) {
+        ctx->last_error = std::string("train memset: ") + cudaGetErrorString(e);
+        return NRRS_ERR_CUDA;
+    }
+
+    TrainArgs a{};
+    a.v = v;
+    a.target = target;
+    a.n = n;
+    a.ld = ld;
+    a.enc = ctx->enc;
+    a.fp.stat_eps = c.stat_eps;
+    a.fp.ref_eps = c.ref_eps;
+    a.loss_clamp = c.loss_clamp_max;
+    a.cost_offset = c.cost_offset;
+    a.train_rrs = train_rrs;
+    a.table = ctx->params;
+    a.table_grad = ctx->grads;
+    a.wt_stat = ctx->wt;
+    a.wt_rrs = ctx->wt + ctx->wt_rrs_offset;
+    a.w_stat = ctx->wrow;
+    a.w_rrs = ctx->wrow + ctx->n_stat;
+    a.act = act;
+    a.r_x0 = L.r_x0; a.r_hs = L.r_hs; a.r_dhs = L.r_dhs; a.r_dy = L.r_dy;
+    a.r_x1 = L.r_x1; a.r_hr = L.r_hr; a.r_dhr = L.r_dhr; a.r_draw = L.r_draw;
+    a.part = part;
+    a.loss_out = loss_dev ? loss_dev : ctx->loss_dev;
+
+    if (c.statnet_width == 64 && c.statnet_hidden == 2)
+        e = launch_train<64, 2, 64, 2>(ctx, a, s);
+    else if (c.statnet_width == 64 && c.statnet_hidden == 3)
+        e = launch_train<64, 3, 64, 3>(ctx, a, s);
+    else
+        e = launch_train<128, 3, 128, 3>(ctx, a, s);
+    if (e != cudaSuccess) {
+        ctx->last_error = std::string("train launch: ") + cudaGetErrorString(e);
+        return NRRS_ERR_CUDA;
+    }
+
+    // weight-gradient jobs: (delta rows, activation rows, M, N, layer input width, offset)
+    WGradArgs w{};
+    w.act = act;
+    w.ld = ld;
+    w.n = n;
+    w.chunks = (uint32_t)chunks;
+    w.partial = partial;
+    w.total = (uint32_t)mlp;
+    int nj = 0;
+    uint32_t off = 0;
+    const uint32_t WS = c.statnet_width, HS = c.statnet_hidden;
+    const uint32_t WR = c.rrsnet_width, HR = c.rrsnet_hidden;
+    w.job[nj++] = WJob{L.r_dhs, L.r_x0, WS, 56, kStatIn, off};
+    off += WS * kStatIn;
+    for (uint32_t h = 1; h < HS; ++h) {
+        w.job[nj++] = WJob{L.r_dhs + h * WS, L.r_hs + (h - 1) * WS, WS, WS, WS, off};
+        off += WS * WS;
+    }
+    w.job[nj++] = WJob{L.r_dy, L.r_hs + (HS - 1) * WS, 3, WS, WS, off};
+    off += 3 * WS;
+    if (train_rrs) {
+        w.job[nj++] = WJob{L.r_dhr, L.r_x1, WR, 10, kRrsIn, off};
+        off += WR * kRrsIn;
+        for (uint32_t h = 1; h < HR; ++h) {
+            w.job[nj++] = WJob{L.r_dhr + h * WR, L.r_hr + (h - 1) * WR, WR, WR, WR, off};
+            off += WR * WR;
+        }
+        w.job[nj++] = WJob{L.r_draw, L.r_hr + (HR - 1) * WR, 1, WR, WR, off};
+    }
+    w.njobs = nj;
+    const uint32_t tiles_y = ((128 + 63) / 64) * ((128 + 63) / 64);
+    {
+        ProfScope ps(ctx, NRRS_KERNEL_TRAIN_WGRAD, s);
+        k_wgrad<<<dim3((unsigned)chunks, tiles_y, (unsigned)nj), 256, 0, s>>>(w);
+    }
+    {
+        ProfScope ps(ctx, NRRS_KERNEL_TRAIN_REDUCE, s);
+        k_wreduce<<<(unsigned)((mlp + 255) / 256), 256, 0, s>>>(partial, (uint32_t)chunks,
+                                                                (uint32_t)mlp,
+                                                                ctx->grads + ctx->n_table);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) {
+        ctx->last_error = std::string("wgrad launch: ") + cudaGetErrorString(e);
+        return NRRS_ERR_CUDA;
+    }
+
+    // Adam over the trained parameters: table + StatNet (+ RRSNet at step 3)
+    ctx->adam_t += 1;
+    AdamArgs ad{};
+    ad.p = ctx->params;
+    ad.g = ctx->grads;
+    ad.m = ctx->adam_m;
+    ad.v = ctx->adam_v;
+    ad.table_h = ctx->table_h;
+    ad.n_table = ctx->n_table;
+    ad.first = 0;
+    ad.count = ctx->n_table + ctx->n_stat + (train_rrs ? ctx->n_rrs : 0);
+    ad.lr = c.lr;
+    ad.b1 = c.beta1;
+    ad.b2 = c.beta2;
+    ad.eps = c.eps;
+    ad.l2 = c.l2_reg;
+    ad.c1 = 1.0f - powf(c.beta1, (float)ctx->adam_t);
+    ad.c2 = 1.0f - powf(c.beta2, (float)ctx->adam_t);
+    {
+        ProfScope ps(ctx, NRRS_KERNEL_ADAM, s);
+        k_adam<<<(unsigned)ctx->sm_count * 8, 256, 0, s>>>(ad);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) {
+        ctx->last_error = std::string("adam launch: ") + cudaGetErrorString(e);
+        return NRRS_ERR_CUDA;
+    }
+    return NRRS_OK;
+}
+
 }  // namespace nrrs

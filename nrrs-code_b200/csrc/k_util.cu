@@ -37,6 +37,7 @@ __host__ __device__ inline size_t umma_offset(int n, int k, int K) {
 struct PackArgs {
     const float* master;
     float* wt;
+    float* wrow;     // 16-byte aligned row-major copy of the master (backward passes)
     void* wpack;
     int ws, hs, wr, hr, prec;
 };
@@ -60,6 +61,7 @@ __global__ void k_pack(PackArgs a) {
                 const int n = (int)(e / d.in), k = (int)(e % d.in);
                 const float v = n < d.out ? a.master[mofs + (size_t)n * d.in + k] : 0.f;
                 if (n < op4) a.wt[tofs + (size_t)k * op4 + n] = v;
+                if (n < d.out && a.wrow) a.wrow[mofs + (size_t)n * d.in + k] = v;
                 if (a.wpack) {
                     const size_t o = pofs + umma_offset(n, k, d.in);
                     if (a.prec == NRRS_PREC_BF16)
@@ -130,9 +132,9 @@ size_t packed_weight_bytes(int ws, int hs, int wr, int hr) {
     return t * 2;
 }
 
-cudaError_t launch_pack_weights(const float* master_mlp, float* wt, void* wpack, int ws, int hs,
-                                int wr, int hr, int prec, cudaStream_t s) {
-    PackArgs a{master_mlp, wt, wpack, ws, hs, wr, hr, prec};
+cudaError_t launch_pack_weights(const float* master_mlp, float* wt, float* wrow, void* wpack,
+                                int ws, int hs, int wr, int hr, int prec, cudaStream_t s) {
+    PackArgs a{master_mlp, wt, wrow, wpack, ws, hs, wr, hr, prec};
     k_pack<<<64, 256, 0, s>>>(a);
     return cudaGetLastError();
 }

@@ -69,8 +69,8 @@ cudaError_t launch_infer_tc(const InferArgs& a, int ws, int hs, int wr, int hr, 
                             int sm_count, int ctas_per_sm, cudaStream_t s);
 size_t infer_tc_smem_bytes(int ws, int hs, int wr, int hr);
 // derived weight copies: FP32 transposed and the UMMA-packed FP16/BF16 images
-cudaError_t launch_pack_weights(const float* master_mlp, float* wt, void* wpack, int ws, int hs,
-                                int wr, int hr, int prec, cudaStream_t s);
+cudaError_t launch_pack_weights(const float* master_mlp, float* wt, float* wrow, void* wpack,
+                                int ws, int hs, int wr, int hr, int prec, cudaStream_t s);
 size_t packed_weight_bytes(int ws, int hs, int wr, int hr);
 size_t transposed_weight_floats(int ws, int hs, int wr, int hr);
 // FP32 table -> FP16 copy

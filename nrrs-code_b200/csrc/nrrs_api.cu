@@ -144,17 +144,17 @@ SegmentTable make_segments(const nrrs_segment* segs, int n, uint32_t unit) {
     return t;
 }
 
-int refresh_derived(nrrs_ctx* ctx, cudaStream_t s) {
+int refresh_derived(nrrs_ctx* ctx, cudaStream_t s, bool table = true) {
     const nrrs_config& c = ctx->cfg;
     cudaError_t e;
     {
         ProfScope ps(ctx, NRRS_KERNEL_PACK, s);
-        e = launch_pack_weights(ctx->params + ctx->n_table, ctx->wt, ctx->wpack,
+        e = launch_pack_weights(ctx->params + ctx->n_table, ctx->wt, ctx->wrow, ctx->wpack,
                                 c.statnet_width, c.statnet_hidden, c.rrsnet_width,
                                 c.rrsnet_hidden, c.precision, s);
     }
     if (e != cudaSuccess) return cuda_fail(ctx, e, "pack weights");
-    if (ctx->table_h) {
+    if (ctx->table_h && table) {
         ProfScope ps(ctx, NRRS_KERNEL_TABLE_HALF, s);
         e = launch_table_to_half(ctx->params, ctx->table_h, ctx->n_table, s);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "table to half");
@@ -402,6 +402,7 @@ int nrrs_create(const nrrs_config* cfg, nrrs_ctx** out) {
     NRRS_ALLOC(ctx->adam_m, pb);
     NRRS_ALLOC(ctx->adam_v, pb);
     NRRS_ALLOC(ctx->wt, sizeof(float) * ctx->wt_floats);
+    NRRS_ALLOC(ctx->wrow, sizeof(float) * (ctx->n_stat + ctx->n_rrs));
     if (c.precision != NRRS_PREC_FP32) {
         NRRS_ALLOC(ctx->table_h, sizeof(__half) * ctx->n_table);
         NRRS_ALLOC(ctx->wpack, ctx->wpack_bytes);
@@ -462,6 +463,7 @@ void nrrs_destroy(nrrs_ctx* ctx) {
     cudaFree(ctx->adam_v);
     cudaFree(ctx->table_h);
     cudaFree(ctx->wt);
+    cudaFree(ctx->wrow);
     cudaFree(ctx->wpack);
     cudaFree(ctx->scr);
     cudaFree(ctx->loss_dev);
@@ -565,7 +567,8 @@ int nrrs_train_step(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* target
     if (n == 0 || n > ctx->cfg.max_train) return fail(ctx, NRRS_ERR_INVALID_ARG, "need 0 < n <= max_train");
     rc = train_step_impl(ctx, vptrs(v), target, n, loss_dev, (cudaStream_t)stream);
     if (rc) return rc;
-    return refresh_derived(ctx, (cudaStream_t)stream);
+    // the Adam pass already refreshed the FP16 table
+    return refresh_derived(ctx, (cudaStream_t)stream, false);
 }
 
 uint64_t nrrs_param_count(const nrrs_ctx* ctx) { return ctx ? ctx->n_params : 0; }

@@ -1,0 +1,97 @@
+"""GPU parity of the training step (nrrs_train_step) against the oracle: losses, gradients of
+the hash table and both MLPs before the update, and the Adam update itself."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import nrrs_b200 as nb
+import oracle as O
+from gpu_util import host, make_net, random_params, soa, stream, torch_cuda, upload
+
+pytestmark = pytest.mark.gpu
+
+
+def run_step(net, v, n):
+    torch = torch_cuda()
+    d = upload(v)
+    loss = torch.zeros(2, dtype=torch.float64, device="cuda")
+    net.train(soa(d), d["target"], n, loss, stream())
+    torch.cuda.synchronize()
+    return loss.cpu().numpy()
+
+
+def rel_err(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+
+
+@pytest.mark.parametrize("step", [3, 2])
+def test_fp32_grads_and_losses_vs_fp64_oracle(step):
+    net = make_net(max_train=1 << 14, step=step, log2_hashmap_size=16)
+    p0 = random_params(net, 21, table_scale=0.5, mlp_scale=0.15)
+    n = 6000
+    v = nb.synth(31, n)
+    loss = run_step(net, v, n)
+    g = net.get_grads()
+    g64, l64 = O.train_grads(net.config, p0, v, v["target"], "f64")
+    assert loss[0] == pytest.approx(l64[0], rel=1e-5)
+    assert loss[1] == pytest.approx(l64[1], rel=1e-4, abs=1e-12)
+    ntab, nst, nrr = net.param_layout()
+    for name, sl in (("table", slice(0, ntab)), ("statnet", slice(ntab, ntab + nst)),
+                     ("rrsnet", slice(ntab + nst, ntab + nst + nrr))):
+        if name == "rrsnet" and step < 3:
+            assert not np.any(g[sl]), name
+            continue
+        e = rel_err(g[sl].astype(np.float64), g64[sl])
+        assert e < 2e-4, (name, e)
+    # Adam (t = 1) applied to the GPU's own gradients
+    p1 = net.get_params()
+    pe = p0.copy()
+    m = np.zeros_like(pe); vv = np.zeros_like(pe)
+    count = ntab + nst + (nrr if step >= 3 else 0)
+    O.adam(net.config, pe, g, m, vv, 1, 0, count)
+    assert np.allclose(p1, pe, rtol=1e-5, atol=1e-7)
+    if step < 3:
+        assert np.array_equal(p1[ntab + nst:], p0[ntab + nst:])
+    m1, v1, t = net.get_adam_state()
+    assert t == 1
+    assert np.allclose(m1[:count], 0.1 * g[:count], rtol=1e-5, atol=1e-12)
+    net.close()
+
+
+@pytest.mark.parametrize("shape", ["w64h3", "w128h3"])
+def test_fp32_other_shapes_grads(shape):
+    kw = {"w64h3": dict(statnet_width=64, statnet_hidden=3, rrsnet_width=64, rrsnet_hidden=3),
+          "w128h3": dict(statnet_width=128, statnet_hidden=3, rrsnet_width=128, rrsnet_hidden=3)}[shape]
+    net = make_net(max_train=1 << 13, log2_hashmap_size=15, **kw)
+    p0 = random_params(net, 22, table_scale=0.5, mlp_scale=0.1)
+    n = 3000
+    v = nb.synth(32, n)
+    loss = run_step(net, v, n)
+    g = net.get_grads()
+    g64, l64 = O.train_grads(net.config, p0, v, v["target"], "f64")
+    assert loss == pytest.approx(l64, rel=1e-4)
+    assert rel_err(g.astype(np.float64), g64) < 2e-4
+    net.close()
+
+
+def test_loss_decreases_over_steps():
+    net = make_net(max_train=1 << 14)
+    n = 8192
+    v = nb.synth(33, n)
+    losses = [run_step(net, v, n) for _ in range(30)]
+    assert losses[-1][0] < 0.8 * losses[0][0], (losses[0], losses[-1])
+    assert losses[-1][1] < losses[0][1], (losses[0], losses[-1])
+    rc, flags = net.device_status(stream())
+    assert rc == nb.OK and flags == 0
+    net.close()
+
+
+def test_full_batch_262144_runs_and_is_finite():
+    net = make_net(max_train=262144)
+    v = nb.synth(34, 262144)
+    loss = run_step(net, v, 262144)
+    assert np.all(np.isfinite(loss)) and loss[0] > 0 and loss[1] > 0
+    g = net.get_grads()
+    assert np.all(np.isfinite(g))
+    net.close()
