@@ -43,6 +43,7 @@ struct nrrs_ctx {
     float* wt = nullptr;       // transposed FP32 MLP weights
     float* wrow = nullptr;     // aligned row-major copy of the FP32 MLP weights
     void* wpack = nullptr;     // UMMA-packed FP16/BF16 MLP weights
+    void* tpack = nullptr;     // BF16 training image (forward + transposed layers)
     size_t wt_floats = 0, wpack_bytes = 0;
     size_t wt_rrs_offset = 0;  // floats from wt to the RRSNet part
 
@@ -92,4 +93,6 @@ namespace nrrs {
 int train_step_impl(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint32_t n,
                     double* loss_dev, cudaStream_t s);
 size_t train_scratch_bytes(const nrrs_config& cfg, uint32_t n, int sm_count);
+// the tensor-core training step covers 64-wide networks in mixed precision
+bool train_tc_supported(const nrrs_config& cfg);
 }  // namespace nrrs

@@ -449,11 +449,12 @@ __global__ void __launch_bounds__(256) k_wgrad(const __grid_constant__ WGradArgs
 
 // gradients = sum of the chunk partials in chunk order; entries no job writes (zero input
 // lanes) are zero in every partial, set once at creation
-__global__ void k_wreduce(const float* partial, uint32_t chunks, uint32_t total, float* grad) {
+__global__ void k_wreduce(const float* partial, uint32_t chunks, uint32_t total, float* grad,
+                          float scale) {
     for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
         float s = 0.f;
         for (uint32_t c = 0; c < chunks; ++c) s += partial[(size_t)c * total + e];
-        grad[e] = s;
+        grad[e] = s * scale;
     }
 }
 
@@ -532,7 +533,44 @@ uint32_t ld_of(uint32_t n) { return (n + 127) / 128 * 128; }
 
 }  // namespace
 
+cudaError_t launch_wreduce(const float* partial, uint32_t chunks, uint32_t total, float* grad,
+                           float scale, cudaStream_t s) {
+    k_wreduce<<<(total + 255) / 256, 256, 0, s>>>(partial, chunks, total, grad, scale);
+    return cudaGetLastError();
+}
+
+// Adam over the trained parameters: table + StatNet (+ RRSNet at step 3); refreshes the FP16 table
+cudaError_t launch_adam_step(nrrs_ctx* ctx, bool train_rrs, cudaStream_t s) {
+    const nrrs_config& c = ctx->cfg;
+    ctx->adam_t += 1;
+    AdamArgs ad{};
+    ad.p = ctx->params;
+    ad.g = ctx->grads;
+    ad.m = ctx->adam_m;
+    ad.v = ctx->adam_v;
+    ad.table_h = ctx->table_h;
+    ad.n_table = ctx->n_table;
+    ad.first = 0;
+    ad.count = ctx->n_table + ctx->n_stat + (train_rrs ? ctx->n_rrs : 0);
+    ad.lr = c.lr;
+    ad.b1 = c.beta1;
+    ad.b2 = c.beta2;
+    ad.eps = c.eps;
+    ad.l2 = c.l2_reg;
+    ad.c1 = 1.0f - powf(c.beta1, (float)ctx->adam_t);
+    ad.c2 = 1.0f - powf(c.beta2, (float)ctx->adam_t);
+    ProfScope ps(ctx, NRRS_KERNEL_ADAM, s);
+    k_adam<<<(unsigned)ctx->sm_count * 8, 256, 0, s>>>(ad);
+    return cudaGetLastError();
+}
+
+bool train_tc_supported(const nrrs_config& c);
+size_t train_tc_scratch_bytes(const nrrs_config& c, uint32_t n, int sm_count);
+int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint32_t n,
+                  double* loss_dev, cudaStream_t s);
+
 size_t train_scratch_bytes(const nrrs_config& c, uint32_t n, int sm_count) {
+    if (train_tc_supported(c)) return train_tc_scratch_bytes(c, n, sm_count);
     const Layout L = layout_of(c);
     const uint64_t mlp = (uint64_t)64 * c.statnet_width + (uint64_t)(c.statnet_hidden - 1) *
                          c.statnet_width * c.statnet_width + 3ull * c.statnet_width +
@@ -545,6 +583,7 @@ size_t train_scratch_bytes(const nrrs_config& c, uint32_t n, int sm_count) {
 
 int train_step_impl(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint32_t n,
                     double* loss_dev, cudaStream_t s) {
+    if (train_tc_supported(ctx->cfg)) return train_step_tc(ctx, v, target, n, loss_dev, s);
     const nrrs_config& c = ctx->cfg;
     const Layout L = layout_of(c);
     const uint32_t ld = ld_of(c.max_train);
@@ -638,38 +677,15 @@ int train_step_impl(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uin
     }
     {
         ProfScope ps(ctx, NRRS_KERNEL_TRAIN_REDUCE, s);
-        k_wreduce<<<(unsigned)((mlp + 255) / 256), 256, 0, s>>>(partial, (uint32_t)chunks,
-                                                                (uint32_t)mlp,
-                                                                ctx->grads + ctx->n_table);
+        e = launch_wreduce(partial, (uint32_t)chunks, (uint32_t)mlp, ctx->grads + ctx->n_table, 1.0f, s);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) {
         ctx->last_error = std::string("wgrad launch: ") + cudaGetErrorString(e);
         return NRRS_ERR_CUDA;
     }
 
-    // Adam over the trained parameters: table + StatNet (+ RRSNet at step 3)
-    ctx->adam_t += 1;
-    AdamArgs ad{};
-    ad.p = ctx->params;
-    ad.g = ctx->grads;
-    ad.m = ctx->adam_m;
-    ad.v = ctx->adam_v;
-    ad.table_h = ctx->table_h;
-    ad.n_table = ctx->n_table;
-    ad.first = 0;
-    ad.count = ctx->n_table + ctx->n_stat + (train_rrs ? ctx->n_rrs : 0);
-    ad.lr = c.lr;
-    ad.b1 = c.beta1;
-    ad.b2 = c.beta2;
-    ad.eps = c.eps;
-    ad.l2 = c.l2_reg;
-    ad.c1 = 1.0f - powf(c.beta1, (float)ctx->adam_t);
-    ad.c2 = 1.0f - powf(c.beta2, (float)ctx->adam_t);
-    {
-        ProfScope ps(ctx, NRRS_KERNEL_ADAM, s);
-        k_adam<<<(unsigned)ctx->sm_count * 8, 256, 0, s>>>(ad);
-    }
-    if ((e = cudaGetLastError()) != cudaSuccess) {
+    e = launch_adam_step(ctx, train_rrs, s);
+    if (e != cudaSuccess) {
         ctx->last_error = std::string("adam launch: ") + cudaGetErrorString(e);
         return NRRS_ERR_CUDA;
     }

@@ -1,0 +1,819 @@
+// k_train_tc.cu -- mixed-precision training step on the 5th-generation tensor cores (sm_100a).
+//
+// Same maths as k_train_simt.cu (losses of NRRSNetwork::train, network.cpp:196-295), with every
+// matrix product on tcgen05 (FP32 accumulation in TMEM, FP32 master weights and Adam state).
+// StatNet runs in FP16 (its activations and deltas are bounded); RRSNet in BF16, because its
+// loss gradient r^2/q^2 can exceed FP16's range.
+// Deltas are kept per sample (the 1/n of the batch mean is applied when the weight gradients are
+// reduced and in the hash-grid scatter), so they stay O(1) in BF16.
+//
+//   k_ttc_stat   per 128-sample tile: FP16-table encode -> StatNet forward (tcgen05) -> loss
+//                gradient -> input gradients through the transposed weight images (tcgen05) ->
+//                hash-grid scatter-add (FP32 atomics); glue -> RRSNet input tile. Every
+//                activation and delta tile is written to HBM with a bulk TMA store, in its
+//                shared-memory layout.
+//   k_ttc_rrs    <false>: RRSNet forward for the batch sums V and C; <true>: forward again,
+//                loss gradient with the final V and C, backward; tiles stored as above.
+//   k_wgrad_tc   dW = sum over samples of delta (x) activation: split-K over sample chunks,
+//                operands brought in by bulk TMA loads (double-buffered, mbarrier-tracked) and
+//                read as MN-major UMMA operands, accumulated in TMEM; FP32 chunk partials.
+//   k_wreduce / k_adam from k_train_simt.cu finish the step.
+#include "context.hpp"
+#include "tc_tile.cuh"
+
+namespace nrrs {
+
+namespace {
+
+using namespace tile;
+
+constexpr int kMaxH = 3;
+constexpr uint32_t kTcChunk = 4096;  // samples per weight-gradient partial
+
+struct Arr {
+    uint64_t off;  // byte offset of the tile-blocked array in the scratch
+    uint32_t F;    // features per row (tile = 128 rows x F BF16)
+    uint32_t pad;
+};
+
+struct TcTrainArgs {
+    VertexPtrs v;
+    const float* target;
+    uint32_t n;
+    EncodeParams enc;
+    FactorParams fp;
+    float loss_clamp, cost_offset, inv_n;
+    int32_t train_rrs;
+    const __half* table_h;
+    float* table_grad;
+    const uint8_t* tpack;   // BF16 training image
+    uint32_t s_bytes;       // StatNet forward + transposed images (bytes, at tpack + 0)
+    uint32_t r_off, r_bytes;// RRSNet forward + transposed images
+    uint8_t* act;           // tile-blocked BF16 scratch
+    Arr x0, hs[kMaxH], dhs[kMaxH], dy, x1, hr[kMaxH], dhr[kMaxH], draw;
+    double* part;           // [kMaxCtas][4]: loss_S, V, C
+    uint32_t part_rows;
+    double* loss_out;
+};
+
+__device__ __forceinline__ uint8_t* tile_ptr(uint8_t* act, const Arr& r, uint32_t t) {
+    return act + r.off + (size_t)t * 128u * r.F * 2u;
+}
+
+// bulk TMA store of one shared-memory tile to HBM, committed as its own bulk group
+__device__ __forceinline__ void store_tile(void* dst, const void* src, uint32_t bytes) {
+    tc::bulk_s2g(dst, src, bytes);
+    tc::bulk_commit();
+}
+
+// bulk-copy a weight image into shared memory and wait for it (thread 0 issues)
+__device__ __forceinline__ bool load_weights(uint8_t* sW, const uint8_t* src, uint32_t bytes,
+                                             uint64_t* bar, int tid) {
+    if (tid == 0) {
+        tc::mbar_arrive_expect_tx(bar, bytes);
+        for (uint32_t off = 0; off < bytes; off += 32768u) {
+            const uint32_t b = bytes - off < 32768u ? bytes - off : 32768u;
+            tc::bulk_g2s(sW + off, src + off, b, bar);
+        }
+    }
+    return tc::mbar_wait(bar, 0, kSpin);
+}
+
+__device__ __forceinline__ double block_sum_d(double v, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 4; ++k) t += red[k];
+    return t;
+}
+
+// ---------------------------------------------------------------------------------------------
+template <int W, int H>
+struct StatSmem {
+    static constexpr uint32_t kFwd = 2u * (W * kStatIn + (H - 1) * W * W + 16 * W);
+    static constexpr uint32_t kBwd = 2u * (kStatIn * W + (H - 1) * W * W + W * 16);
+    static constexpr uint32_t kW = (kFwd + kBwd + 1023u) / 1024u * 1024u;
+    static constexpr uint32_t kTileW = 128u * W * 2u;   // one [128 x W] tile
+    static constexpr uint32_t kX0 = 0 + kW;             // [128 x 64], reused as a delta tile
+    static constexpr uint32_t kH = kX0 + 128u * 64u * 2u;
+    static constexpr uint32_t kD = kH + H * kTileW;
+    static constexpr uint32_t kDY = kD + kTileW;
+    static constexpr uint32_t kX1 = kDY + 128u * 16u * 2u;
+    static constexpr uint32_t kBar = kX1 + 128u * 16u * 2u;
+    static constexpr size_t kSmem = 1024 + kBar + 64;
+};
+
+template <int W, int H>
+__global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcTrainArgs a) {
+    static_assert(W == 64, "the tensor-core training path keeps 64-wide tiles resident");
+    using S = StatSmem<W, H>;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023u) &
+                                               ~uintptr_t(1023));
+    uint8_t* sW = base;
+    uint8_t* sX0 = base + S::kX0;
+    uint8_t* sH[H];
+#pragma unroll
+    for (int h = 0; h < H; ++h) sH[h] = base + S::kH + h * S::kTileW;
+    uint8_t* sD = base + S::kD;
+    uint8_t* sDY = base + S::kDY;
+    uint8_t* sX1 = base + S::kX1;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(base + S::kBar);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2);
+    __shared__ int s_abort;
+    __shared__ double red[4];
+    const int tid = threadIdx.x, warp = tid >> 5;
+
+    if (tid == 0) {
+        tc::mbar_init(&bars[0], 1);
+        tc::mbar_init(&bars[1], 1);
+        tc::fence_mbar_init();
+        s_abort = 0;
+    }
+    if (warp == 0) {
+        tc::tmem_alloc(tslot, 64);
+        tc::tmem_relinquish();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *tslot;
+    if (!load_weights(sW, a.tpack, S::kFwd + S::kBwd, &bars[0], tid)) s_abort = 1;
+    __syncthreads();
+    unsigned flags = s_abort ? NRRS_DEV_TIMEOUT : 0u;
+    uint32_t phase = 0;
+    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+
+    // forward images, then the transposed images (same order as k_pack_train)
+    const uint8_t* wF[H + 1];
+    const uint8_t* wT[H + 1];
+    wF[0] = sW;
+    for (int h = 1; h <= H; ++h) wF[h] = wF[h - 1] + (h == 1 ? W * kStatIn * 2 : W * W * 2);
+    wT[0] = sW + S::kFwd;
+    for (int h = 1; h <= H; ++h) wT[h] = wT[h - 1] + (h == 1 ? kStatIn * W * 2 : W * W * 2);
+
+    double lossS = 0.0;
+    const __half2* table = reinterpret_cast<const __half2*>(a.table_h);
+    const uint32_t tiles = (a.n + 127) / 128;
+    for (uint32_t t = blockIdx.x; t < tiles && !flags; t += gridDim.x) {
+        if (tid == 0) tc::bulk_wait_read();  // the previous tile's stores have left smem
+        __syncthreads();
+        const uint32_t i = t * 128 + tid;
+        const bool valid = i < a.n;
+        float p[3] = {0.f, 0.f, 0.f};
+        // ---- encode (FP16 table, BF16 tile) ----
+        if (valid) {
+            norm_pos(a.enc, a.v.pos, i, p);
+#pragma unroll 1
+            for (int lq = 0; lq < 4; ++lq) {
+                float f[8];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const LevelDev L = a.enc.lv[lq * 4 + j];
+                    const CellCoord c = cell_of(p, L.res);
+                    float f0 = 0.f, f1 = 0.f;
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        const uint32_t row = grid_row(L, a.enc.hash_mask, c.ix + (k & 1),
+                                                      c.iy + ((k >> 1) & 1), c.iz + ((k >> 2) & 1));
+                        const float2 tv = __half22float2(__ldg(table + row));
+                        const float w = corner_weight(c, k);
+                        f0 += w * tv.x;
+                        f1 += w * tv.y;
+                    }
+                    f[2 * j] = f0;
+                    f[2 * j + 1] = f1;
+                }
+                store_chunk(sX0, tid, lq, 64, pack8<false>(f));
+            }
+            float sh[16], misc[16];
+            const size_t i3 = 3 * (size_t)i;
+            sh16(a.v.wi[i3], a.v.wi[i3 + 1], a.v.wi[i3 + 2], sh);
+            store_chunk(sX0, tid, 4, 64, pack8<false>(sh));
+            store_chunk(sX0, tid, 5, 64, pack8<false>(sh + 8));
+            misc_lanes(a.v, i, misc);
+            store_chunk(sX0, tid, 6, 64, pack8<false>(misc));
+            store_chunk(sX0, tid, 7, 64, make_uint4(0u, 0u, 0u, 0u));
+        } else {
+            zero_row(sX0, tid, 64);
+        }
+        sync_for_mma();
+        if (tid == 0) store_tile(tile_ptr(a.act, a.x0, t), sX0, 128u * 64u * 2u);
+
+        // ---- StatNet forward ----
+        bool ok = mma_layer<kStatIn, W, false>(sX0, wF[0], tmem, &bars[1], phase, tid);
+        epilogue_relu<W, false>(trow, sH[0], tid);
+        sync_for_mma();
+        if (tid == 0) store_tile(tile_ptr(a.act, a.hs[0], t), sH[0], S::kTileW);
+#pragma unroll 1
+        for (int h = 1; h < H; ++h) {
+            ok &= mma_layer<W, W, false>(sH[h - 1], wF[h], tmem, &bars[1], phase, tid);
+            epilogue_relu<W, false>(trow, sH[h], tid);
+            sync_for_mma();
+            if (tid == 0) store_tile(tile_ptr(a.act, a.hs[h], t), sH[h], S::kTileW);
+        }
+        ok &= mma_layer<W, 16, false>(sH[H - 1], wF[H], tmem, &bars[1], phase, tid);
+        float y[16];
+        tc::tmem_ld16(trow, y);
+        tc::tmem_wait_ld();
+
+        // ---- loss gradient (per sample) and RRSNet input ----
+        float dyv[16], x1[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) dyv[k] = 0.f, x1[k] = 0.f;
+        if (valid) {
+            const size_t i3 = 3 * (size_t)i;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const float d = y[c] - logf(a.target[i3 + c] + a.fp.stat_eps);
+                lossS += (double)d * (double)d;
+                dyv[c] = 2.0f * d / 3.0f;
+            }
+            glue16(a.fp, y, a.v, i, x1);
+        }
+        store_chunk(sDY, tid, 0, 16, pack8<false>(dyv));
+        store_chunk(sDY, tid, 1, 16, pack8<false>(dyv + 8));
+        store_chunk(sX1, tid, 0, 16, pack8<true>(x1));  // RRSNet input: BF16
+        store_chunk(sX1, tid, 1, 16, pack8<true>(x1 + 8));
+        sync_for_mma();
+        if (tid == 0) {
+            store_tile(tile_ptr(a.act, a.dy, t), sDY, 128u * 16u * 2u);
+            store_tile(tile_ptr(a.act, a.x1, t), sX1, 128u * 16u * 2u);
+        }
+
+        // ---- backward through the transposed images ----
+        ok &= mma_layer<16, W, false>(sDY, wT[H], tmem, &bars[1], phase, tid);
+        epilogue_mask<W, false>(trow, sH[H - 1], sD, tid);
+        sync_for_mma();
+        if (tid == 0) {
+            store_tile(tile_ptr(a.act, a.dhs[H - 1], t), sD, S::kTileW);
+        }
+        uint8_t* cur = sD;
+        uint8_t* other = sX0;  // free once its store has been read out
+#pragma unroll 1
+        for (int h = H - 1; h >= 1; --h) {
+            ok &= mma_layer<W, W, false>(cur, wT[h], tmem, &bars[1], phase, tid);
+            if (tid == 0) tc::bulk_wait_read();
+            __syncthreads();
+            epilogue_mask<W, false>(trow, sH[h - 1], other, tid);
+            sync_for_mma();
+            if (tid == 0) {
+                store_tile(tile_ptr(a.act, a.dhs[h - 1], t), other, S::kTileW);
+                }
+            uint8_t* tmp = cur;
+            cur = other;
+            other = tmp;
+        }
+        // input gradient of the 32 hash lanes (per sample; 1/n applied below)
+        ok &= mma_layer<W, 32, false>(cur, wT[0], tmem, &bars[1], phase, tid);
+        float dx[32];
+        tc::tmem_ld16(trow, dx);
+        tc::tmem_ld16(trow + 16, dx + 16);
+        tc::tmem_wait_ld();
+        tc::fence_before_sync();
+        __syncthreads();  // TMEM free for the next tile
+        if (valid) {
+#pragma unroll 2
+            for (int l = 0; l < kMaxLevels; ++l) {
+                const LevelDev L = a.enc.lv[l];
+                const CellCoord c = cell_of(p, L.res);
+                const float g0 = dx[2 * l] * a.inv_n, g1 = dx[2 * l + 1] * a.inv_n;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const uint32_t row = grid_row(L, a.enc.hash_mask, c.ix + (k & 1),
+                                                  c.iy + ((k >> 1) & 1), c.iz + ((k >> 2) & 1));
+                    const float w = corner_weight(c, k);
+                    atomicAdd(a.table_grad + 2 * (size_t)row, w * g0);
+                    atomicAdd(a.table_grad + 2 * (size_t)row + 1, w * g1);
+                }
+            }
+        }
+        if (!ok) s_abort = 1;
+        __syncthreads();
+        if (s_abort) flags |= NRRS_DEV_TIMEOUT;
+    }
+    const double s0 = block_sum_d(lossS, red);
+    if (tid == 0) {
+        a.part[4 * blockIdx.x + 0] = s0;
+        tc::bulk_wait_all();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem, 64);
+    }
+    (void)flags;
+}
+
+// ---------------------------------------------------------------------------------------------
+template <int W, int H>
+struct RrsSmem {
+    static constexpr uint32_t kFwd = 2u * (W * kRrsIn + (H - 1) * W * W + 16 * W);
+    static constexpr uint32_t kBwd = 2u * ((H - 1) * W * W + W * 16);
+    static constexpr uint32_t kW = (kFwd + kBwd + 1023u) / 1024u * 1024u;
+    static constexpr uint32_t kTileW = 128u * W * 2u;
+    static constexpr uint32_t kX1 = kW;
+    static constexpr uint32_t kG = kX1 + 128u * 16u * 2u;
+    static constexpr uint32_t kD = kG + H * kTileW;
+    static constexpr uint32_t kE = kD + kTileW;
+    static constexpr uint32_t kDR = kE + kTileW;
+    static constexpr uint32_t kBar = kDR + 128u * 16u * 2u;
+    static constexpr size_t kSmem = 1024 + kBar + 64;
+};
+
+__device__ __forceinline__ float rel_contrib_tc(const TcTrainArgs& a, uint32_t i) {
+    const size_t i3 = 3 * (size_t)i;
+    float acc = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) acc += a.v.thp[i3 + c] * a.target[i3 + c];
+    const float ref = (a.v.ref ? a.v.ref[i] : 0.5f) + a.fp.ref_eps;
+    const float r = acc / 3.0f / ref;
+    return r < a.loss_clamp ? r : a.loss_clamp;
+}
+
+template <int W, int H, bool BACKWARD>
+__global__ void __launch_bounds__(128, 1) k_ttc_rrs(const __grid_constant__ TcTrainArgs a) {
+    using S = RrsSmem<W, H>;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023u) &
+                                               ~uintptr_t(1023));
+    uint8_t* sW = base;
+    uint8_t* sX1 = base + S::kX1;
+    uint8_t* sG[H];
+#pragma unroll
+    for (int h = 0; h < H; ++h) sG[h] = base + S::kG + h * S::kTileW;
+    uint8_t* sD = base + S::kD;
+    uint8_t* sE = base + S::kE;
+    uint8_t* sDR = base + S::kDR;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(base + S::kBar);  // weights, mma, x1 load
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 3);
+    __shared__ int s_abort;
+    __shared__ double red[4];
+    __shared__ double s_tot[3];
+    const int tid = threadIdx.x, warp = tid >> 5;
+
+    if (tid == 0) {
+        tc::mbar_init(&bars[0], 1);
+        tc::mbar_init(&bars[1], 1);
+        tc::mbar_init(&bars[2], 1);
+        tc::fence_mbar_init();
+        s_abort = 0;
+    }
+    if (BACKWARD) {
+        if (tid < 3) {
+            double t = 0.0;
+            for (uint32_t b = 0; b < a.part_rows; ++b) t += a.part[4 * b + tid];
+            s_tot[tid] = t;
+        }
+        __syncthreads();
+        if (blockIdx.x == 0 && tid == 0) {
+            const double Vm = s_tot[1] / (double)a.n, Cm = s_tot[2] / (double)a.n;
+            a.loss_out[0] = s_tot[0] / (3.0 * (double)a.n);
+            a.loss_out[1] = a.train_rrs ? Vm * Cm : 0.0;
+        }
+        if (!a.train_rrs) return;  // StatNet-only steps: losses are all this launch writes
+    }
+    if (warp == 0) {
+        tc::tmem_alloc(tslot, 64);
+        tc::tmem_relinquish();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *tslot;
+    float Vf = 0.f, Cf = 0.f;
+    if (BACKWARD) {
+        Vf = (float)(s_tot[1] / (double)a.n);
+        Cf = (float)(s_tot[2] / (double)a.n);
+    }
+    if (!load_weights(sW, a.tpack + a.r_off, S::kFwd + S::kBwd, &bars[0], tid)) s_abort = 1;
+    __syncthreads();
+    unsigned flags = s_abort ? NRRS_DEV_TIMEOUT : 0u;
+    uint32_t phase = 0, xphase = 0;
+    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    const uint8_t* wF[H + 1];
+    const uint8_t* wT[H + 1];
+    wF[0] = sW;
+    for (int h = 1; h <= H; ++h) wF[h] = wF[h - 1] + (h == 1 ? W * kRrsIn * 2 : W * W * 2);
+    wT[0] = nullptr;
+    wT[1] = sW + S::kFwd;
+    for (int h = 2; h <= H; ++h) wT[h] = wT[h - 1] + W * W * 2;
+
+    double sumV = 0.0, sumC = 0.0;
+    const uint32_t tiles = (a.n + 127) / 128;
+    for (uint32_t t = blockIdx.x; t < tiles && !flags; t += gridDim.x) {
+        if (tid == 0) {
+            tc::bulk_wait_read();
+            tc::mbar_arrive_expect_tx(&bars[2], 128u * 16u * 2u);
+            tc::bulk_g2s(sX1, tile_ptr(a.act, a.x1, t), 128u * 16u * 2u, &bars[2]);
+        }
+        bool ok = tc::mbar_wait(&bars[2], xphase, kSpin);
+        xphase ^= 1u;
+        __syncthreads();
+        const uint32_t i = t * 128 + tid;
+        const bool valid = i < a.n;
+
+        ok &= mma_layer<kRrsIn, W, true>(sX1, wF[0], tmem, &bars[1], phase, tid);
+        epilogue_relu<W, true>(trow, sG[0], tid);
+        sync_for_mma();
+        if (BACKWARD && tid == 0) store_tile(tile_ptr(a.act, a.hr[0], t), sG[0], S::kTileW);
+#pragma unroll 1
+        for (int h = 1; h < H; ++h) {
+            ok &= mma_layer<W, W, true>(sG[h - 1], wF[h], tmem, &bars[1], phase, tid);
+            epilogue_relu<W, true>(trow, sG[h], tid);
+            sync_for_mma();
+            if (BACKWARD && tid == 0) store_tile(tile_ptr(a.act, a.hr[h], t), sG[h], S::kTileW);
+        }
+        ok &= mma_layer<W, 16, true>(sG[H - 1], wF[H], tmem, &bars[1], phase, tid);
+        float r16[16];
+        tc::tmem_ld16(trow, r16);
+        tc::tmem_wait_ld();
+        const float raw = r16[0];
+        float q = 0.f, r = 0.f;
+        if (valid) {
+            q = act_sigma(raw);
+            r = rel_contrib_tc(a, i);
+        }
+        if (!BACKWARD) {
+            if (valid) {
+                sumV += (double)(r * r / q);
+                sumC += (double)(a.cost_offset + q);
+            }
+            tc::fence_before_sync();
+            __syncthreads();
+        } else {
+            float dr[16];
+#pragma unroll
+            for (int k = 0; k < 16; ++k) dr[k] = 0.f;
+            if (valid) dr[0] = (-(r * r) / (q * q) * Cf + Vf) * act_sigma_grad(raw);
+            store_chunk(sDR, tid, 0, 16, pack8<true>(dr));
+            store_chunk(sDR, tid, 1, 16, pack8<true>(dr + 8));
+            sync_for_mma();
+            if (tid == 0) {
+                store_tile(tile_ptr(a.act, a.draw, t), sDR, 128u * 16u * 2u);
+                }
+            ok &= mma_layer<16, W, true>(sDR, wT[H], tmem, &bars[1], phase, tid);
+            epilogue_mask<W, true>(trow, sG[H - 1], sD, tid);
+            sync_for_mma();
+            if (tid == 0) {
+                store_tile(tile_ptr(a.act, a.dhr[H - 1], t), sD, S::kTileW);
+                }
+            uint8_t* cur = sD;
+            uint8_t* other = sE;
+#pragma unroll 1
+            for (int h = H - 1; h >= 1; --h) {
+                ok &= mma_layer<W, W, true>(cur, wT[h], tmem, &bars[1], phase, tid);
+                if (tid == 0) tc::bulk_wait_read();
+                __syncthreads();
+                epilogue_mask<W, true>(trow, sG[h - 1], other, tid);
+                sync_for_mma();
+                if (tid == 0) {
+                    store_tile(tile_ptr(a.act, a.dhr[h - 1], t), other, S::kTileW);
+                        }
+                uint8_t* tmp = cur;
+                cur = other;
+                other = tmp;
+            }
+            tc::fence_before_sync();
+            __syncthreads();
+        }
+        if (!ok) s_abort = 1;
+        __syncthreads();
+        if (s_abort) flags |= NRRS_DEV_TIMEOUT;
+    }
+    if (!BACKWARD) {
+        const double v = block_sum_d(sumV, red);
+        const double c = block_sum_d(sumC, red);
+        if (tid == 0) {
+            a.part[4 * blockIdx.x + 1] = v;
+            a.part[4 * blockIdx.x + 2] = c;
+        }
+    }
+    if (tid == 0) tc::bulk_wait_all();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem, 64);
+    }
+    (void)flags;
+}
+
+// ---------------------------------------------------------------------------------------------
+struct TcJob {
+    uint32_t bf16;    // operand type of this layer's tiles: 1 = BF16 (RRSNet), 0 = FP16 (StatNet)
+    uint32_t pad;
+    uint64_t d_off;   // deltas: tile-blocked array
+    uint32_t Fd, Mv;  // its features, valid output rows
+    uint32_t Fa, Nv;  // activations: features (= N of the MMA), valid input columns
+    uint64_t a_off;
+    uint32_t out, ldw;  // offset of the layer in the MLP gradient vector, its row stride
+};
+
+struct TcWGradArgs {
+    const uint8_t* act;
+    uint32_t n, chunks, total;
+    float* partial;
+    int32_t njobs;
+    TcJob job[8];
+};
+
+constexpr uint32_t kWgBuf = 16384;  // bytes per operand stage (64 samples x up to 128 features)
+
+template <int N>
+__device__ __forceinline__ void wgrad_epilogue(uint32_t trow, const TcJob& j, float* out, int m) {
+#pragma unroll
+    for (int c0 = 0; c0 < N; c0 += 16) {
+        float v[16];
+        tc::tmem_ld16(trow + c0, v);
+        tc::tmem_wait_ld();
+        if ((uint32_t)m < j.Mv) {
+#pragma unroll
+            for (int k = 0; k < 16; ++k)
+                if ((uint32_t)(c0 + k) < j.Nv) out[(size_t)m * j.ldw + c0 + k] = v[k];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128, 1) k_wgrad_tc(const __grid_constant__ TcWGradArgs a) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023u) &
+                                               ~uintptr_t(1023));
+    uint8_t* sA[2] = {base, base + 2 * kWgBuf};
+    uint8_t* sB[2] = {base + kWgBuf, base + 3 * kWgBuf};
+    uint64_t* bars = reinterpret_cast<uint64_t*>(base + 4 * kWgBuf);  // load[2], mma[2], done
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 5);
+    __shared__ int s_fail;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const TcJob& j = a.job[blockIdx.y];
+    const uint32_t c = blockIdx.x;
+    const uint32_t s0 = c * kTcChunk;
+    const uint32_t s1 = min(a.n, s0 + kTcChunk);
+    const uint32_t stages = (s1 - s0 + 63) / 64;
+
+    if (tid == 0) {
+        for (int k = 0; k < 5; ++k) tc::mbar_init(&bars[k], 1);
+        tc::fence_mbar_init();
+        s_fail = 0;
+    }
+    if (warp == 0) {
+        tc::tmem_alloc(tslot, 128);
+        tc::tmem_relinquish();
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = *tslot;
+
+    if (tid == 0) {
+        const uint32_t bytesA = 64u * j.Fd * 2u, bytesB = 64u * j.Fa * 2u;
+        const uint32_t lboA = j.Fd * 16u, lboB = j.Fa * 16u;
+        const uint32_t idesc = tc::idesc_f16_major(j.Fa, j.bf16, 1u, 1u);
+        auto issue = [&](uint32_t s) {
+            const uint32_t b = s & 1u;
+            const uint32_t smp = s0 + 64u * s;        // first sample of the stage
+            const uint32_t tile = smp >> 7, half = (smp >> 6) & 1u;
+            const uint8_t* ga = a.act + j.d_off + (size_t)tile * 128u * j.Fd * 2u + half * bytesA;
+            const uint8_t* gb = a.act + j.a_off + (size_t)tile * 128u * j.Fa * 2u + half * bytesB;
+            tc::mbar_arrive_expect_tx(&bars[b], bytesA + bytesB);
+            tc::bulk_g2s(sA[b], ga, bytesA, &bars[b]);
+            tc::bulk_g2s(sB[b], gb, bytesB, &bars[b]);
+        };
+        bool ok = true;
+        issue(0);
+        for (uint32_t s = 0; s < stages && ok; ++s) {
+            if (s + 1 < stages) {
+                const uint32_t nb = (s + 1) & 1u;
+                if (s + 1 >= 2) ok &= tc::mbar_wait(&bars[2 + nb], ((s - 1) >> 1) & 1u, kSpin);
+                issue(s + 1);
+            }
+            const uint32_t b = s & 1u;
+            ok &= tc::mbar_wait(&bars[b], (s >> 1) & 1u, kSpin);
+            tc::fence_after_sync();
+            const uint32_t a0 = tc::smem_u32(sA[b]), b0 = tc::smem_u32(sB[b]);
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) {
+                const uint64_t ad = tc::smem_desc(a0 + kk * 2 * lboA, lboA, 128);
+                const uint64_t bd = tc::smem_desc(b0 + kk * 2 * lboB, lboB, 128);
+                tc::mma_f16(tmem, ad, bd, idesc, (s > 0 || kk > 0) ? 1u : 0u);
+            }
+            tc::mma_commit(&bars[2 + b]);
+        }
+        tc::mma_commit(&bars[4]);
+        if (!ok) s_fail = 1;
+    }
+    __syncwarp();
+    const bool done = tc::mbar_wait(&bars[4], 0, kSpin);
+    tc::fence_after_sync();
+    __syncthreads();
+    if (!s_fail && done) {
+        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+        float* out = a.partial + (size_t)c * a.total + j.out;
+        const int m = tid;
+        if (j.Fa == 64) wgrad_epilogue<64>(trow, j, out, m);
+        else if (j.Fa == 16) wgrad_epilogue<16>(trow, j, out, m);
+        else wgrad_epilogue<128>(trow, j, out, m);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tmem, 128);
+    }
+}
+
+// scratch layout of the tensor-core path: tile-blocked BF16 arrays
+struct TcLayout {
+    Arr x0, hs[kMaxH], dhs[kMaxH], dy, x1, hr[kMaxH], dhr[kMaxH], draw;
+    uint64_t act_bytes;
+};
+
+TcLayout tc_layout(const nrrs_config& c, uint32_t max_n) {
+    const uint64_t tiles = (max_n + 127) / 128;
+    TcLayout L{};
+    uint64_t off = 0;
+    auto take = [&](Arr& r, uint32_t F) {
+        r.off = off;
+        r.F = F;
+        off += tiles * 128u * F * 2u;
+        off = (off + 255) / 256 * 256;
+    };
+    take(L.x0, 64);
+    for (int h = 0; h < c.statnet_hidden; ++h) take(L.hs[h], c.statnet_width);
+    for (int h = 0; h < c.statnet_hidden; ++h) take(L.dhs[h], c.statnet_width);
+    take(L.dy, 16);
+    take(L.x1, 16);
+    for (int h = 0; h < c.rrsnet_hidden; ++h) take(L.hr[h], c.rrsnet_width);
+    for (int h = 0; h < c.rrsnet_hidden; ++h) take(L.dhr[h], c.rrsnet_width);
+    take(L.draw, 16);
+    L.act_bytes = off;
+    return L;
+}
+
+template <int W, int H>
+cudaError_t launch_ttc(nrrs_ctx* ctx, TcTrainArgs& a, cudaStream_t s, bool train_rrs) {
+    using SS = StatSmem<W, H>;
+    using RS = RrsSmem<W, H>;
+    auto ks = k_ttc_stat<W, H>;
+    auto kr0 = k_ttc_rrs<W, H, false>;
+    auto kr1 = k_ttc_rrs<W, H, true>;
+    cudaError_t e = cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SS::kSmem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kr0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RS::kSmem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kr1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RS::kSmem);
+    if (e != cudaSuccess) return e;
+    const uint32_t tiles = (a.n + 127) / 128;
+    auto grid_of = [&](const void* k, size_t smem) {
+        uint32_t g = (uint32_t)(ctx->sm_count * resident_ctas(k, 128, smem, 8));
+        return g > tiles ? tiles : g;
+    };
+    {
+        ProfScope ps(ctx, NRRS_KERNEL_TRAIN_STAT, s);
+        ks<<<grid_of((const void*)ks, SS::kSmem), 128, SS::kSmem, s>>>(a);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (train_rrs) {
+        ProfScope ps(ctx, NRRS_KERNEL_TRAIN_RRS, s);
+        const uint32_t g = grid_of((const void*)kr0, RS::kSmem);
+        kr0<<<g, 128, RS::kSmem, s>>>(a);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        kr1<<<g, 128, RS::kSmem, s>>>(a);
+    } else {
+        // losses without the RRSNet: only the StatNet sum is present
+        ProfScope ps(ctx, NRRS_KERNEL_TRAIN_RRS, s);
+        kr1<<<1, 128, RS::kSmem, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+bool train_tc_supported(const nrrs_config& c) {
+    return c.precision != NRRS_PREC_FP32 && c.statnet_width == 64 && c.rrsnet_width == 64 &&
+           c.statnet_hidden == c.rrsnet_hidden && (c.statnet_hidden == 2 || c.statnet_hidden == 3);
+}
+
+size_t train_tc_scratch_bytes(const nrrs_config& c, uint32_t n, int sm_count) {
+    const TcLayout L = tc_layout(c, n);
+    const uint64_t mlp = (uint64_t)64 * c.statnet_width + (uint64_t)(c.statnet_hidden - 1) *
+                         c.statnet_width * c.statnet_width + 3ull * c.statnet_width +
+                         16ull * c.rrsnet_width + (uint64_t)(c.rrsnet_hidden - 1) * c.rrsnet_width *
+                         c.rrsnet_width + (uint64_t)c.rrsnet_width;
+    const uint64_t chunks = (n + kTcChunk - 1) / kTcChunk;
+    return L.act_bytes + sizeof(double) * 4 * (uint64_t)sm_count * 16 + sizeof(float) * chunks * mlp + 1024;
+}
+
+cudaError_t launch_wreduce(const float* partial, uint32_t chunks, uint32_t total, float* grad,
+                           float scale, cudaStream_t s);
+cudaError_t launch_adam_step(nrrs_ctx* ctx, bool train_rrs, cudaStream_t s);
+
+int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint32_t n,
+                  double* loss_dev, cudaStream_t s) {
+    const nrrs_config& c = ctx->cfg;
+    const TcLayout L = tc_layout(c, c.max_train);
+    const uint64_t chunks = (n + kTcChunk - 1) / kTcChunk;
+    const uint64_t mlp = ctx->n_stat + ctx->n_rrs;
+    uint8_t* act = reinterpret_cast<uint8_t*>(ctx->train_scratch);
+    double* part = reinterpret_cast<double*>(act + L.act_bytes);
+    const uint32_t part_rows = (uint32_t)ctx->sm_count * 16;
+    float* partial = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(part) +
+                                              sizeof(double) * 4 * (size_t)part_rows);
+    const bool train_rrs = c.step >= 3;
+    cudaError_t e = cudaMemsetAsync(ctx->grads, 0, sizeof(float) * ctx->n_params, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(part, 0, sizeof(double) * 4 * part_rows, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(partial, 0, sizeof(float) * chunks * mlp, s);
+    if (e != cudaSuccess) {
+        ctx->last_error = std::string("train memset: ") + cudaGetErrorString(e);
+        return NRRS_ERR_CUDA;
+    }
+    TcTrainArgs a{};
+    a.v = v;
+    a.target = target;
+    a.n = n;
+    a.enc = ctx->enc;
+    a.fp.stat_eps = c.stat_eps;
+    a.fp.ref_eps = c.ref_eps;
+    a.loss_clamp = c.loss_clamp_max;
+    a.cost_offset = c.cost_offset;
+    a.inv_n = 1.0f / (float)n;
+    a.train_rrs = train_rrs;
+    a.table_h = ctx->table_h;
+    a.table_grad = ctx->grads;
+    a.tpack = reinterpret_cast<const uint8_t*>(ctx->tpack);
+    const int W = c.statnet_width, H = c.statnet_hidden;
+    a.s_bytes = 2u * (uint32_t)(W * kStatIn + (H - 1) * W * W + 16 * W + kStatIn * W + (H - 1) * W * W + W * 16);
+    a.r_off = a.s_bytes;
+    a.r_bytes = 2u * (uint32_t)(W * kRrsIn + (H - 1) * W * W + 16 * W + (H - 1) * W * W + W * 16);
+    a.act = act;
+    a.x0 = L.x0; a.dy = L.dy; a.x1 = L.x1; a.draw = L.draw;
+    for (int h = 0; h < kMaxH; ++h) {
+        a.hs[h] = L.hs[h]; a.dhs[h] = L.dhs[h]; a.hr[h] = L.hr[h]; a.dhr[h] = L.dhr[h];
+    }
+    a.part = part;
+    a.part_rows = part_rows;
+    a.loss_out = loss_dev ? loss_dev : ctx->loss_dev;
+    e = H == 2 ? launch_ttc<64, 2>(ctx, a, s, train_rrs) : launch_ttc<64, 3>(ctx, a, s, train_rrs);
+    if (e != cudaSuccess) {
+        ctx->last_error = std::string("tensor-core train launch: ") + cudaGetErrorString(e);
+        return NRRS_ERR_CUDA;
+    }
+
+    TcWGradArgs w{};
+    w.act = act;
+    w.n = n;
+    w.chunks = (uint32_t)chunks;
+    w.total = (uint32_t)mlp;
+    w.partial = partial;
+    int nj = 0;
+    uint32_t off = 0;
+    w.job[nj++] = TcJob{0, 0, L.dhs[0].off, (uint32_t)W, (uint32_t)W, 64, 64, L.x0.off, off, kStatIn};
+    off += W * kStatIn;
+    for (int h = 1; h < H; ++h) {
+        w.job[nj++] = TcJob{0, 0, L.dhs[h].off, (uint32_t)W, (uint32_t)W, (uint32_t)W, (uint32_t)W,
+                            L.hs[h - 1].off, off, (uint32_t)W};
+        off += W * W;
+    }
+    w.job[nj++] = TcJob{0, 0, L.dy.off, 16, 3, (uint32_t)W, (uint32_t)W, L.hs[H - 1].off, off, (uint32_t)W};
+    off += 3 * W;
+    if (train_rrs) {
+        w.job[nj++] = TcJob{1, 0, L.dhr[0].off, (uint32_t)W, (uint32_t)W, 16, 16, L.x1.off, off, kRrsIn};
+        off += W * kRrsIn;
+        for (int h = 1; h < H; ++h) {
+            w.job[nj++] = TcJob{1, 0, L.dhr[h].off, (uint32_t)W, (uint32_t)W, (uint32_t)W, (uint32_t)W,
+                                L.hr[h - 1].off, off, (uint32_t)W};
+            off += W * W;
+        }
+        w.job[nj++] = TcJob{1, 0, L.draw.off, 16, 1, (uint32_t)W, (uint32_t)W, L.hr[H - 1].off, off, (uint32_t)W};
+    }
+    w.njobs = nj;
+    const size_t wsm = 1024 + 4 * kWgBuf + 64;
+    e = cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
+    if (e == cudaSuccess) {
+        ProfScope ps(ctx, NRRS_KERNEL_TRAIN_WGRAD, s);
+        k_wgrad_tc<<<dim3((unsigned)chunks, (unsigned)nj), 128, wsm, s>>>(w);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        ProfScope ps(ctx, NRRS_KERNEL_TRAIN_REDUCE, s);
+        e = launch_wreduce(partial, (uint32_t)chunks, (uint32_t)mlp, ctx->grads + ctx->n_table,
+                           1.0f / (float)n, s);
+    }
+    if (e != cudaSuccess) {
+        ctx->last_error = std::string("tensor-core wgrad launch: ") + cudaGetErrorString(e);
+        return NRRS_ERR_CUDA;
+    }
+    e = launch_adam_step(ctx, train_rrs, s);
+    if (e != cudaSuccess) {
+        ctx->last_error = std::string("adam launch: ") + cudaGetErrorString(e);
+        return NRRS_ERR_CUDA;
+    }
+    return NRRS_OK;
+}
+
+}  // namespace nrrs

@@ -77,6 +77,69 @@ __global__ void k_pack(PackArgs a) {
     }
 }
 
+// Training image: per network the forward layers [N][K] (as k_pack) followed by the transposed
+// layers used for input gradients: layer (in, out) -> [in rows][out padded to 16] K-major, i.e.
+// B[k = out][n = in] = W[out][in]. StatNet keeps all layers transposed (layer 0 feeds the
+// hash-grid gradient) and is stored in FP16 (its deltas are bounded); RRSNet needs no input
+// gradient, so its layer 0 is skipped, and it is stored in BF16 (its loss gradient r^2/q^2 can
+// exceed FP16's range).
+struct PackTrainArgs {
+    const float* master;
+    uint16_t* out;
+    int ws, hs, wr, hr;
+};
+
+__device__ __forceinline__ uint16_t to_bits(float v, bool bf) {
+    if (bf) {
+        const __nv_bfloat16 b = __float2bfloat16_rn(v);
+        return *reinterpret_cast<const uint16_t*>(&b);
+    }
+    const __half h = __float2half_rn(v);
+    return *reinterpret_cast<const uint16_t*>(&h);
+}
+
+__global__ void k_pack_train(PackTrainArgs a) {
+    size_t mofs = 0, pofs = 0;
+    for (int net = 0; net < 2; ++net) {
+        const int in = net == 0 ? kStatIn : kRrsIn;
+        const int w = net == 0 ? a.ws : a.wr;
+        const int h = net == 0 ? a.hs : a.hr;
+        const int out = net == 0 ? kStatOut : 1;
+        const size_t net_m = mofs;
+        // forward images
+        for (int l = 0; l <= h; ++l) {
+            const LayerDesc d = layer_of(in, w, h, out, l);
+            const int np = l == h ? npad16(d.out) : d.out;
+            const size_t cells = (size_t)np * d.in;
+            for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < cells;
+                 e += (size_t)gridDim.x * blockDim.x) {
+                const int n = (int)(e / d.in), k = (int)(e % d.in);
+                const float v = n < d.out ? a.master[mofs + (size_t)n * d.in + k] : 0.f;
+                a.out[pofs + umma_offset(n, k, d.in)] = to_bits(v, net == 1);
+            }
+            mofs += (size_t)d.out * d.in;
+            pofs += cells;
+        }
+        // transposed images
+        size_t lofs = net_m;
+        for (int l = 0; l <= h; ++l) {
+            const LayerDesc d = layer_of(in, w, h, out, l);
+            const size_t lsz = (size_t)d.out * d.in;
+            if (net == 1 && l == 0) { lofs += lsz; continue; }
+            const int kp = npad16(d.out);
+            const size_t cells = (size_t)d.in * kp;
+            for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < cells;
+                 e += (size_t)gridDim.x * blockDim.x) {
+                const int n = (int)(e / kp), k = (int)(e % kp);  // n = input, k = output
+                const float v = k < d.out ? a.master[lofs + (size_t)k * d.in + n] : 0.f;
+                a.out[pofs + umma_offset(n, k, kp)] = to_bits(v, net == 1);
+            }
+            lofs += lsz;
+            pofs += cells;
+        }
+    }
+}
+
 __global__ void k_table_half(const float* t, __half* h, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x)
@@ -136,6 +199,33 @@ cudaError_t launch_pack_weights(const float* master_mlp, float* wt, float* wrow,
                                 int ws, int hs, int wr, int hr, int prec, cudaStream_t s) {
     PackArgs a{master_mlp, wt, wrow, wpack, ws, hs, wr, hr, prec};
     k_pack<<<64, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+size_t train_pack_bytes(int ws, int hs, int wr, int hr) {
+    size_t t = 0;
+    for (int net = 0; net < 2; ++net) {
+        const int in = net == 0 ? kStatIn : kRrsIn;
+        const int w = net == 0 ? ws : wr;
+        const int h = net == 0 ? hs : hr;
+        const int out = net == 0 ? kStatOut : 1;
+        for (int l = 0; l <= h; ++l) {
+            const LayerDesc d = layer_of(in, w, h, out, l);
+            t += (size_t)(l == h ? npad16(d.out) : d.out) * d.in;
+        }
+        for (int l = 0; l <= h; ++l) {
+            if (net == 1 && l == 0) continue;
+            const LayerDesc d = layer_of(in, w, h, out, l);
+            t += (size_t)d.in * npad16(d.out);
+        }
+    }
+    return t * 2;
+}
+
+cudaError_t launch_pack_train(const float* master_mlp, void* out, int ws, int hs, int wr, int hr,
+                              cudaStream_t s) {
+    PackTrainArgs a{master_mlp, reinterpret_cast<uint16_t*>(out), ws, hs, wr, hr};
+    k_pack_train<<<64, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 

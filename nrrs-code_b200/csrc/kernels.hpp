@@ -73,6 +73,10 @@ cudaError_t launch_pack_weights(const float* master_mlp, float* wt, float* wrow,
                                 int ws, int hs, int wr, int hr, int prec, cudaStream_t s);
 size_t packed_weight_bytes(int ws, int hs, int wr, int hr);
 size_t transposed_weight_floats(int ws, int hs, int wr, int hr);
+// BF16 training image: forward layers + transposed layers for input gradients
+cudaError_t launch_pack_train(const float* master_mlp, void* out, int ws, int hs, int wr, int hr,
+                              cudaStream_t s);
+size_t train_pack_bytes(int ws, int hs, int wr, int hr);
 // FP32 table -> FP16 copy
 cudaError_t launch_table_to_half(const float* t, __half* h, size_t n, cudaStream_t s);
 

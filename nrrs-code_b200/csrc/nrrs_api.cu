@@ -154,6 +154,12 @@ int refresh_derived(nrrs_ctx* ctx, cudaStream_t s, bool table = true) {
                                 c.rrsnet_hidden, c.precision, s);
     }
     if (e != cudaSuccess) return cuda_fail(ctx, e, "pack weights");
+    if (ctx->tpack) {
+        ProfScope ps(ctx, NRRS_KERNEL_PACK, s);
+        e = launch_pack_train(ctx->params + ctx->n_table, ctx->tpack, c.statnet_width,
+                              c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden, s);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "pack training weights");
+    }
     if (ctx->table_h && table) {
         ProfScope ps(ctx, NRRS_KERNEL_TABLE_HALF, s);
         e = launch_table_to_half(ctx->params, ctx->table_h, ctx->n_table, s);
@@ -407,6 +413,9 @@ int nrrs_create(const nrrs_config* cfg, nrrs_ctx** out) {
         NRRS_ALLOC(ctx->table_h, sizeof(__half) * ctx->n_table);
         NRRS_ALLOC(ctx->wpack, ctx->wpack_bytes);
     }
+    if (train_tc_supported(c))
+        NRRS_ALLOC(ctx->tpack, train_pack_bytes(c.statnet_width, c.statnet_hidden,
+                                                c.rrsnet_width, c.rrsnet_hidden));
     const size_t scr_bytes = sizeof(DecideScratch) + sizeof(unsigned long long) * ctx->max_chunks;
     NRRS_ALLOC(ctx->scr, scr_bytes);
     ctx->states = reinterpret_cast<unsigned long long*>(ctx->scr + 1);
@@ -465,6 +474,7 @@ void nrrs_destroy(nrrs_ctx* ctx) {
     cudaFree(ctx->wt);
     cudaFree(ctx->wrow);
     cudaFree(ctx->wpack);
+    cudaFree(ctx->tpack);
     cudaFree(ctx->scr);
     cudaFree(ctx->loss_dev);
     cudaFree(ctx->train_scratch);

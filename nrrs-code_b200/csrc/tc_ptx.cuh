@@ -51,6 +51,24 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
         : "memory");
 }
 
+// ---- bulk TMA copy shared -> global (unicast), tracked as a bulk group ----
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+                 "r"(smem_u32(src)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() {
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+// wait until every committed bulk store has finished reading shared memory
+__device__ __forceinline__ void bulk_wait_read() {
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+// wait until every committed bulk store has completed (writes visible)
+__device__ __forceinline__ void bulk_wait_all() {
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
 // generic-proxy shared-memory writes -> visible to the async proxy (tensor core operand reads)
 __device__ __forceinline__ void fence_async_smem() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -91,6 +109,12 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
 // kind::f16 instruction descriptor: D = F32, A/B = F16 (0) or BF16 (1), both K-major, M = 128
 __host__ __device__ constexpr uint32_t idesc_f16(uint32_t n, uint32_t ab_bf16) {
     return (1u << 4) | (ab_bf16 << 7) | (ab_bf16 << 10) | ((n >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+// kind::f16 descriptor with explicit operand majors (1 = MN-major), M = 128
+__host__ __device__ constexpr uint32_t idesc_f16_major(uint32_t n, uint32_t ab_bf16, uint32_t a_mn,
+                                                       uint32_t b_mn) {
+    return idesc_f16(n, ab_bf16) | (a_mn << 15) | (b_mn << 16);
 }
 
 // D[tmem] (+)= A[smem] * B[smem]^T, issued by one thread

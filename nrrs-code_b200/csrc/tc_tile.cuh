@@ -1,0 +1,132 @@
+// tc_tile.cuh -- 128-row activation tiles for the tcgen05 kernels (inference and training).
+//
+// A tile holds 128 rows (vertices or samples) x K features in the canonical no-swizzle K-major
+// core-matrix layout: 8 rows x 16 bytes per core matrix, K-adjacent core matrices 128 B apart
+// (LBO), 8-row groups K*16 B apart (SBO). Row m of the tile is produced and consumed by thread m
+// (TMEM lane m), one 16-byte chunk of 8 features at a time. The same bytes read as an MN-major
+// operand (features contiguous, rows as the reduction dimension) with SBO = 128 B and
+// LBO = K*16 B, which the weight-gradient GEMM uses.
+#pragma once
+#include "nrrs_common.cuh"
+#include "tc_ptx.cuh"
+
+namespace nrrs {
+namespace tile {
+
+constexpr uint32_t kSpin = 1u << 24;
+
+template <bool BF>
+__device__ __forceinline__ uint32_t pack2(float a, float b) {
+    if constexpr (BF) {
+        __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+        return *reinterpret_cast<uint32_t*>(&h);
+    } else {
+        __half2 h = __floats2half2_rn(a, b);
+        return *reinterpret_cast<uint32_t*>(&h);
+    }
+}
+
+template <bool BF>
+__device__ __forceinline__ float2 unpack2(uint32_t u) {
+    if constexpr (BF) {
+        __nv_bfloat162 h = *reinterpret_cast<__nv_bfloat162*>(&u);
+        return __bfloat1622float2(h);
+    } else {
+        __half2 h = *reinterpret_cast<__half2*>(&u);
+        return __half22float2(h);
+    }
+}
+
+template <bool BF>
+__device__ __forceinline__ uint4 pack8(const float* f) {
+    return make_uint4(pack2<BF>(f[0], f[1]), pack2<BF>(f[2], f[3]), pack2<BF>(f[4], f[5]),
+                      pack2<BF>(f[6], f[7]));
+}
+
+__device__ __forceinline__ uint32_t chunk_offset(int m, int kchunk, int K) {
+    return (uint32_t)(m >> 3) * (uint32_t)(K * 16) + (uint32_t)kchunk * 128u + (uint32_t)(m & 7) * 16u;
+}
+
+// 8 consecutive K elements of row m
+__device__ __forceinline__ void store_chunk(uint8_t* sA, int m, int kchunk, int K, uint4 v) {
+    *reinterpret_cast<uint4*>(sA + chunk_offset(m, kchunk, K)) = v;
+}
+__device__ __forceinline__ uint4 load_chunk(const uint8_t* sA, int m, int kchunk, int K) {
+    return *reinterpret_cast<const uint4*>(sA + chunk_offset(m, kchunk, K));
+}
+
+__device__ __forceinline__ void zero_row(uint8_t* sA, int m, int K) {
+    for (int kc = 0; kc < K / 8; ++kc) store_chunk(sA, m, kc, K, make_uint4(0u, 0u, 0u, 0u));
+}
+
+// generic smem writes of all threads -> visible to the tensor cores; TMEM reads done
+__device__ __forceinline__ void sync_for_mma() {
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+}
+
+// D[TMEM, 128 x N] = A[128 x K] * B[N x K]^T, both K-major tiles; thread 0 issues, all wait
+template <int K, int N, bool BF>
+__device__ __forceinline__ bool mma_layer(const uint8_t* sA, const uint8_t* sB, uint32_t tmem,
+                                          uint64_t* bar, uint32_t& phase, int tid) {
+    if (tid == 0) {
+        tc::fence_after_sync();
+        const uint32_t a0 = tc::smem_u32(sA), b0 = tc::smem_u32(sB);
+        constexpr uint32_t idesc = tc::idesc_f16(N, BF ? 1u : 0u);
+#pragma unroll
+        for (int kk = 0; kk < K / 16; ++kk) {
+            const uint64_t ad = tc::smem_desc(a0 + kk * 256, 128, K * 16);
+            const uint64_t bd = tc::smem_desc(b0 + kk * 256, 128, K * 16);
+            tc::mma_f16(tmem, ad, bd, idesc, kk > 0 ? 1u : 0u);
+        }
+        tc::mma_commit(bar);
+    }
+    const bool ok = tc::mbar_wait(bar, phase, kSpin);
+    phase ^= 1u;
+    tc::fence_after_sync();
+    return ok;
+}
+
+// hidden-layer epilogue: TMEM row -> ReLU -> tile (K = N)
+template <int N, bool BF>
+__device__ __forceinline__ void epilogue_relu(uint32_t trow, uint8_t* sOut, int m) {
+#pragma unroll
+    for (int c0 = 0; c0 < N; c0 += 32) {
+        float v[32];
+        tc::tmem_ld16(trow + c0, v);
+        tc::tmem_ld16(trow + c0 + 16, v + 16);
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] = fmaxf(v[j], 0.f);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) store_chunk(sOut, m, c0 / 8 + j, N, pack8<BF>(v + 8 * j));
+    }
+}
+
+// backward epilogue: TMEM row -> zero where the forward activation (tile sH, K = N) is <= 0
+template <int N, bool BF>
+__device__ __forceinline__ void epilogue_mask(uint32_t trow, const uint8_t* sH, uint8_t* sOut, int m) {
+#pragma unroll
+    for (int c0 = 0; c0 < N; c0 += 32) {
+        float v[32];
+        tc::tmem_ld16(trow + c0, v);
+        tc::tmem_ld16(trow + c0 + 16, v + 16);
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint4 h = load_chunk(sH, m, c0 / 8 + j, N);
+            const uint32_t hw[4] = {h.x, h.y, h.z, h.w};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float2 hv = unpack2<BF>(hw[q]);
+                if (!(hv.x > 0.f)) v[8 * j + 2 * q] = 0.f;
+                if (!(hv.y > 0.f)) v[8 * j + 2 * q + 1] = 0.f;
+            }
+            store_chunk(sOut, m, c0 / 8 + j, N, pack8<BF>(v + 8 * j));
+        }
+    }
+}
+
+}  // namespace tile
+}  // namespace nrrs

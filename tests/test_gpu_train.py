@@ -95,3 +95,46 @@ def test_full_batch_262144_runs_and_is_finite():
     g = net.get_grads()
     assert np.all(np.isfinite(g))
     net.close()
+
+
+@pytest.mark.parametrize("prec", [nb.PREC_FP16, nb.PREC_BF16], ids=["fp16", "bf16"])
+@pytest.mark.parametrize("step", [3, 2])
+def test_mixed_training_vs_fp64_oracle(prec, step):
+    """tensor-core training step: FP16 StatNet / BF16 RRSNet MMAs with FP32 accumulation.
+    Stated error bars (relative L2 norm of the gradient error, per parameter group)."""
+    net = make_net(precision=prec, max_train=1 << 14, step=step, log2_hashmap_size=16)
+    p0 = random_params(net, 21, table_scale=0.5, mlp_scale=0.15)
+    n = 6000
+    v = nb.synth(31, n)
+    loss = run_step(net, v, n)
+    g = net.get_grads()
+    g64, l64 = O.train_grads(net.config, p0, v, v["target"], "f64")
+    assert loss[0] == pytest.approx(l64[0], rel=1e-4)
+    assert loss[1] == pytest.approx(l64[1], rel=1e-3, abs=1e-12)
+    ntab, nst, nrr = net.param_layout()
+    # measured on this batch: table 2.3e-2, StatNet 6.7e-3, RRSNet 4.1e-3 (FP32 path: 4e-7)
+    bars = {"table": 4e-2, "statnet": 1.5e-2, "rrsnet": 1e-2}
+    for name, sl in (("table", slice(0, ntab)), ("statnet", slice(ntab, ntab + nst)),
+                     ("rrsnet", slice(ntab + nst, ntab + nst + nrr))):
+        if name == "rrsnet" and step < 3:
+            assert not np.any(g[sl])
+            continue
+        e = rel_err(g[sl].astype(np.float64), g64[sl])
+        assert e < bars[name], (name, e)
+    rc, flags = net.device_status(stream())
+    assert rc == nb.OK and flags == 0
+    net.close()
+
+
+def test_mixed_loss_decreases_and_matches_fp32_trajectory():
+    torch = torch_cuda()
+    nets = [make_net(max_train=1 << 14, precision=p) for p in (nb.PREC_FP32, nb.PREC_FP16)]
+    n = 8192
+    v = nb.synth(35, n)
+    traj = [[run_step(net, v, n) for _ in range(20)] for net in nets]
+    for t in traj:
+        assert t[-1][0] < 0.9 * t[0][0]
+    # after 20 Adam steps the two precisions stay close
+    assert traj[1][-1][0] == pytest.approx(traj[0][-1][0], rel=5e-2)
+    for net in nets:
+        net.close()
