@@ -247,13 +247,29 @@ def run_ours(args, rank, world, local_rank):
     soas = [soa_of(b) for b in dev_b]
     tsoa = soa_of(td)
 
+    sharded = None
+    if world > 1:
+        # each rank holds one 1080p-sized shard of an N-times larger queue: one integer
+        # all-reduce of the exact sum per bounce, data-parallel gradients per train step
+        from nrrs_parallel import ShardedNRRS
+        sharded = ShardedNRRS(net)
+        acc = torch.zeros(1, dtype=torch.int64, device=dev)
+        grads_buf = torch.zeros(net.param_count(), dtype=torch.float32, device=dev)
+
     def frame():
         for d in range(BOUNCES):
             o = outs[d]
-            net.generateRRSNumber(soas[d], dev_b[d]["rnd"], N_VERT, N_VERT, 0, dp, o["stats"],
-                                  o["rrs"], o["norm"], o["split"], o["q"], cap, o["sz"], stream)
+            if sharded is None:
+                net.generateRRSNumber(soas[d], dev_b[d]["rnd"], N_VERT, N_VERT, 0, dp, o["stats"],
+                                      o["rrs"], o["norm"], o["split"], o["q"], cap, o["sz"], stream)
+            else:
+                sharded.step(soas[d], dev_b[d]["rnd"], N_VERT, N_VERT * world, 0, dp, o["stats"],
+                             o["rrs"], o["norm"], o["split"], o["q"], cap, o["sz"], acc, stream)
         if do_train:
-            net.train(tsoa, td["target"], TRAIN_BATCH, loss, stream)
+            if sharded is None:
+                net.train(tsoa, td["target"], TRAIN_BATCH, loss, stream)
+            else:
+                sharded.train_step(tsoa, td["target"], TRAIN_BATCH, grads_buf, loss, stream)
 
     # ---- device-timed region ----
     for _ in range(args.warmup):

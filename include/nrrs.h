@@ -204,6 +204,37 @@ int nrrs_step_batched(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* rnd,
                       float* stats, float* rrs, float* rrs_norm, uint8_t* split,
                       uint32_t* next_queue, uint32_t* next_size_dev, void* stream);
 
+/* ---- sharded inference and decision across GPUs (no counterpart in the single-GPU
+ *      reference; the reference's sum is calcSum2PassAsync, commoncudautilshost.cpp:6-22).
+ *      The normalisation sum is an exact 64-bit fixed-point integer, so shards add it with an
+ *      integer all-reduce (NCCL or any transport) and every shard decides bit-identically to a
+ *      single GPU processing the concatenated queue:
+ *        *sum = 0; nrrs_infer_accumulate(shard, sum); allreduce_sum_int64(sum);
+ *        nrrs_decide_emit_with_sum(shard, global budget, global n_specular, sum)
+ *      sum_acc_dev is a caller-owned int64 on the device; the shift is fixed by max_queue, so all
+ *      ranks must use the same max_queue and decision parameters. ---- */
+int nrrs_infer_accumulate(nrrs_ctx* ctx, const nrrs_vertex_soa* v, uint32_t n,
+                          const nrrs_decide_params* p, float* stats, float* rrs,
+                          int64_t* sum_acc_dev, void* stream);
+int nrrs_decide_emit_with_sum(nrrs_ctx* ctx, const float* rrs, const float* rnd,
+                              const uint32_t* scatter_index, uint32_t n, uint32_t budget,
+                              uint32_t n_specular, const int64_t* sum_acc_dev,
+                              const nrrs_decide_params* p, float* rrs_norm, uint8_t* split,
+                              uint32_t* next_queue, uint32_t capacity, uint32_t* next_size_dev,
+                              void* stream);
+/* exact-sum value of an accumulator: sum = acc * 2^-shift (host helper) */
+double nrrs_sum_from_accumulator(const nrrs_ctx* ctx, const nrrs_decide_params* p, int64_t acc);
+
+/* ---- data-parallel training: gradients without the update, then Adam on (all-reduced)
+ *      gradients. nrrs_train_grads leaves this step's gradients in the context;
+ *      nrrs_copy_grads copies them to a caller device buffer [nrrs_param_count] for the
+ *      all-reduce; nrrs_adam_apply runs Adam on grads_dev * scale (scale = 1/ranks for a mean)
+ *      and refreshes the derived weight images. nrrs_train_step == grads + apply(own, 1). ---- */
+int nrrs_train_grads(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* target, uint32_t n,
+                     double* loss_dev, void* stream);
+int nrrs_copy_grads(nrrs_ctx* ctx, float* grads_dev, void* stream);
+int nrrs_adam_apply(nrrs_ctx* ctx, const float* grads_dev, float scale, void* stream);
+
 /* ---- training: replaces NRRSNetwork::train (network.cpp:196-295) with the two
  *      tcnn training_step calls it makes. target is [n][3] radiance. loss_dev (may be
  *      NULL) receives {statnet_loss, rrsnet_loss} as FP64 on the device. ---- */

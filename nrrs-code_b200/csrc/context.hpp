@@ -90,8 +90,11 @@ struct ProfScope {
 }  // namespace nrrs
 
 namespace nrrs {
+// gradients of one step; with apply, the Adam update too
 int train_step_impl(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint32_t n,
-                    double* loss_dev, cudaStream_t s);
+                    double* loss_dev, cudaStream_t s, bool apply = true);
+// Adam on ctx->grads scaled by `scale` (copied in from grads_dev first when it is not ctx->grads)
+cudaError_t launch_adam_step(nrrs_ctx* ctx, bool train_rrs, cudaStream_t s, float scale = 1.0f);
 size_t train_scratch_bytes(const nrrs_config& cfg, uint32_t n, int sm_count);
 // the tensor-core training step covers 64-wide networks in mixed precision
 bool train_tc_supported(const nrrs_config& cfg);

@@ -73,7 +73,8 @@ __global__ void __launch_bounds__(kDecThreads) k_decide(const __grid_constant__ 
         const unsigned end = sg.offset + min(sg.count, (lc + 1) * kDecChunk);
 
         // normalisation factor, FP32 sequence of integrator.cpp:1376-1397
-        const long long acc = (long long)*(volatile unsigned long long*)&a.scr->sum_acc[si];
+        const long long acc = a.ext_sum ? *(const volatile long long*)a.ext_sum
+                                        : (long long)*(volatile unsigned long long*)&a.scr->sum_acc[si];
         const float sumf = (float)((double)acc * a.inv_fixed_scale);
         const float rcp = __fdiv_rn(1.0f, sumf);
         const unsigned nspec = (a.n_spec_dev && si == 0) ? *a.n_spec_dev : sg.n_specular;

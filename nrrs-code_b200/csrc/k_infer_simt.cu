@@ -146,12 +146,12 @@ __global__ void __launch_bounds__(kTile) k_infer_fp32(const __grid_constant__ In
                 a.stats[3 * (size_t)i + 2] = y[2];
             }
             a.rrs[i] = rrs;
-            if (a.scr) term = fixed_term(a.fp, rrs, &a.scr->status);
+            if (a.scr || a.ext_acc) term = fixed_term(a.fp, rrs, a.scr ? &a.scr->status : &g_dummy_status);
         }
-        if (a.scr) {
+        if (a.scr || a.ext_acc) {
             term = warp_sum_ll(term);
             if ((tid & 31) == 0 && term != 0)
-                atomicAdd(&a.scr->sum_acc[si], (unsigned long long)term);
+                atomicAdd(a.ext_acc ? a.ext_acc : &a.scr->sum_acc[si], (unsigned long long)term);
         }
     }
 }

@@ -461,6 +461,7 @@ __global__ void k_wreduce(const float* partial, uint32_t chunks, uint32_t total,
 struct AdamArgs {
     float* p;
     const float* g;
+    float gscale;
     float* m;
     float* v;
     __half* table_h;       // FP16 copy of [0, n_table) refreshed in the same pass (may be null)
@@ -473,7 +474,7 @@ __global__ void k_adam(const __grid_constant__ AdamArgs a) {
     for (uint64_t k = a.first + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
          k < a.first + a.count; k += (uint64_t)gridDim.x * blockDim.x) {
         const float w = a.p[k];
-        const float g = a.g[k] + a.l2 * w;
+        const float g = a.g[k] * a.gscale + a.l2 * w;
         const float m = a.b1 * a.m[k] + (1.0f - a.b1) * g;
         const float v = a.b2 * a.v[k] + (1.0f - a.b2) * g * g;
         a.m[k] = m;
@@ -540,12 +541,13 @@ cudaError_t launch_wreduce(const float* partial, uint32_t chunks, uint32_t total
 }
 
 // Adam over the trained parameters: table + StatNet (+ RRSNet at step 3); refreshes the FP16 table
-cudaError_t launch_adam_step(nrrs_ctx* ctx, bool train_rrs, cudaStream_t s) {
+cudaError_t launch_adam_step(nrrs_ctx* ctx, bool train_rrs, cudaStream_t s, float scale) {
     const nrrs_config& c = ctx->cfg;
     ctx->adam_t += 1;
     AdamArgs ad{};
     ad.p = ctx->params;
     ad.g = ctx->grads;
+    ad.gscale = scale;
     ad.m = ctx->adam_m;
     ad.v = ctx->adam_v;
     ad.table_h = ctx->table_h;
@@ -567,7 +569,7 @@ cudaError_t launch_adam_step(nrrs_ctx* ctx, bool train_rrs, cudaStream_t s) {
 bool train_tc_supported(const nrrs_config& c);
 size_t train_tc_scratch_bytes(const nrrs_config& c, uint32_t n, int sm_count);
 int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint32_t n,
-                  double* loss_dev, cudaStream_t s);
+                  double* loss_dev, cudaStream_t s, bool apply);
 
 size_t train_scratch_bytes(const nrrs_config& c, uint32_t n, int sm_count) {
     if (train_tc_supported(c)) return train_tc_scratch_bytes(c, n, sm_count);
@@ -582,8 +584,8 @@ size_t train_scratch_bytes(const nrrs_config& c, uint32_t n, int sm_count) {
 }
 
 int train_step_impl(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint32_t n,
-                    double* loss_dev, cudaStream_t s) {
-    if (train_tc_supported(ctx->cfg)) return train_step_tc(ctx, v, target, n, loss_dev, s);
+                    double* loss_dev, cudaStream_t s, bool apply) {
+    if (train_tc_supported(ctx->cfg)) return train_step_tc(ctx, v, target, n, loss_dev, s, apply);
     const nrrs_config& c = ctx->cfg;
     const Layout L = layout_of(c);
     const uint32_t ld = ld_of(c.max_train);
@@ -684,6 +686,7 @@ int train_step_impl(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uin
         return NRRS_ERR_CUDA;
     }
 
+    if (!apply) return NRRS_OK;
     e = launch_adam_step(ctx, train_rrs, s);
     if (e != cudaSuccess) {
         ctx->last_error = std::string("adam launch: ") + cudaGetErrorString(e);

@@ -711,10 +711,8 @@ size_t train_tc_scratch_bytes(const nrrs_config& c, uint32_t n, int sm_count) {
 
 cudaError_t launch_wreduce(const float* partial, uint32_t chunks, uint32_t total, float* grad,
                            float scale, cudaStream_t s);
-cudaError_t launch_adam_step(nrrs_ctx* ctx, bool train_rrs, cudaStream_t s);
-
 int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint32_t n,
-                  double* loss_dev, cudaStream_t s) {
+                  double* loss_dev, cudaStream_t s, bool apply) {
     const nrrs_config& c = ctx->cfg;
     const TcLayout L = tc_layout(c, c.max_train);
     const uint64_t chunks = (n + kTcChunk - 1) / kTcChunk;
@@ -808,6 +806,7 @@ int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint3
         ctx->last_error = std::string("tensor-core wgrad launch: ") + cudaGetErrorString(e);
         return NRRS_ERR_CUDA;
     }
+    if (!apply) return NRRS_OK;
     e = launch_adam_step(ctx, train_rrs, s);
     if (e != cudaSuccess) {
         ctx->last_error = std::string("adam launch: ") + cudaGetErrorString(e);

@@ -19,6 +19,7 @@ struct DecideArgs {
     uint32_t* queue;
     uint32_t* next_size;          // [n segments]
     const uint32_t* n_spec_dev;   // optional override of segment 0's n_specular
+    const long long* ext_sum;     // caller-owned exact sum of segment 0 (sharded decision) or null
     DecideScratch* scr;
     unsigned long long* states;   // one look-back word per chunk
     SegmentTable segs;            // tile_start counts decision chunks
@@ -49,6 +50,7 @@ struct InferArgs {
     float* stats;                 // [n][3] optional
     float* rrs;                   // [n]
     DecideScratch* scr;           // accumulate the exact sum when not null
+    unsigned long long* ext_acc;  // accumulate into this caller-owned sum instead (sharded)
 };
 
 // resident CTAs per SM of a kernel from its own resources (shared memory incl. the 1 KB the

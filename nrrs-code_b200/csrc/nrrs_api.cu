@@ -170,7 +170,7 @@ int refresh_derived(nrrs_ctx* ctx, cudaStream_t s, bool table = true) {
 
 int run_infer(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const SegmentTable& segs,
               const nrrs_decide_params* p, uint64_t n_total, float* stats, float* rrs,
-              bool accumulate, cudaStream_t s) {
+              bool accumulate, cudaStream_t s, unsigned long long* ext_acc = nullptr) {
     InferArgs a{};
     a.v = vptrs(v);
     a.enc = ctx->enc;
@@ -184,6 +184,7 @@ int run_infer(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const SegmentTable& segs,
     a.stats = stats;
     a.rrs = rrs;
     a.scr = accumulate ? ctx->scr : nullptr;
+    a.ext_acc = ext_acc;
     const nrrs_config& c = ctx->cfg;
     cudaError_t e;
     if (segs.total_tiles == 0) return NRRS_OK;
@@ -203,7 +204,7 @@ int run_decide(nrrs_ctx* ctx, const float* rrs, const float* rnd, const uint32_t
                const nrrs_segment* segs, int n_segs, uint64_t n_total,
                const uint32_t* n_spec_dev, const nrrs_decide_params* p, float* rrs_norm,
                uint8_t* split, uint32_t* queue, uint32_t* next_size, bool need_sum,
-               cudaStream_t s) {
+               cudaStream_t s, const long long* ext_sum = nullptr) {
     const FactorParams fp = factor_params(ctx, p);
     if (need_sum) {
         SumArgs sa{};
@@ -229,6 +230,7 @@ int run_decide(nrrs_ctx* ctx, const float* rrs, const float* rnd, const uint32_t
     d.queue = queue;
     d.next_size = next_size;
     d.n_spec_dev = n_spec_dev;
+    d.ext_sum = ext_sum;
     d.scr = ctx->scr;
     d.states = ctx->states;
     d.segs = make_segments(segs, n_segs, kDecChunk);
@@ -566,6 +568,76 @@ int nrrs_step_batched(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* rnd,
     if (rc) return rc;
     return run_decide(ctx, rrs, rnd, v->scatter_index, segs, n_segs, n_max, nullptr, p, rrs_norm,
                       split, next_queue, next_size_dev, false, s);
+}
+
+int nrrs_infer_accumulate(nrrs_ctx* ctx, const nrrs_vertex_soa* v, uint32_t n,
+                          const nrrs_decide_params* p, float* stats, float* rrs,
+                          int64_t* sum_acc_dev, void* stream) {
+    if (!ctx) return NRRS_ERR_INVALID_ARG;
+    int rc = check_vertices(ctx, v);
+    if (rc) return rc;
+    if ((rc = check_decide_params(ctx, p, n))) return rc;
+    if (!rrs || !sum_acc_dev) return fail(ctx, NRRS_ERR_INVALID_ARG, "rrs/sum_acc are NULL");
+    if (n > ctx->cfg.max_queue) return fail(ctx, NRRS_ERR_INVALID_ARG, "n > max_queue");
+    if (n == 0) return NRRS_OK;
+    nrrs_segment sg{0, n, 0, 0, 0, 0};
+    return run_infer(ctx, v, make_segments(&sg, 1, kTile), p, n, stats, rrs, false,
+                     (cudaStream_t)stream, reinterpret_cast<unsigned long long*>(sum_acc_dev));
+}
+
+int nrrs_decide_emit_with_sum(nrrs_ctx* ctx, const float* rrs, const float* rnd,
+                              const uint32_t* scatter_index, uint32_t n, uint32_t budget,
+                              uint32_t n_specular, const int64_t* sum_acc_dev,
+                              const nrrs_decide_params* p, float* rrs_norm, uint8_t* split,
+                              uint32_t* next_queue, uint32_t capacity, uint32_t* next_size_dev,
+                              void* stream) {
+    if (!ctx) return NRRS_ERR_INVALID_ARG;
+    int rc = check_decide_params(ctx, p, n);
+    if (rc) return rc;
+    if (!sum_acc_dev) return fail(ctx, NRRS_ERR_INVALID_ARG, "sum_acc is NULL");
+    if (n && (!rrs || !rnd)) return fail(ctx, NRRS_ERR_INVALID_ARG, "rrs/rnd are NULL");
+    if (!next_size_dev || (capacity && !next_queue))
+        return fail(ctx, NRRS_ERR_INVALID_ARG, "next_queue/next_size are NULL");
+    if (n > ctx->cfg.max_queue) return fail(ctx, NRRS_ERR_INVALID_ARG, "n > max_queue");
+    nrrs_segment sg{0, n, budget, n_specular, 0, capacity};
+    return run_decide(ctx, rrs, rnd, scatter_index, &sg, 1, n, nullptr, p, rrs_norm, split,
+                      next_queue, next_size_dev, false, (cudaStream_t)stream,
+                      reinterpret_cast<const long long*>(sum_acc_dev));
+}
+
+double nrrs_sum_from_accumulator(const nrrs_ctx* ctx, const nrrs_decide_params* p, int64_t acc) {
+    if (!ctx || !p) return 0.0;
+    return (double)acc / factor_params(ctx, p).fixed_scale;
+}
+
+int nrrs_train_grads(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* target, uint32_t n,
+                     double* loss_dev, void* stream) {
+    if (!ctx) return NRRS_ERR_INVALID_ARG;
+    int rc = check_vertices(ctx, v);
+    if (rc) return rc;
+    if (!target) return fail(ctx, NRRS_ERR_INVALID_ARG, "target is NULL");
+    if (n == 0 || n > ctx->cfg.max_train) return fail(ctx, NRRS_ERR_INVALID_ARG, "need 0 < n <= max_train");
+    return train_step_impl(ctx, vptrs(v), target, n, loss_dev, (cudaStream_t)stream, false);
+}
+
+int nrrs_copy_grads(nrrs_ctx* ctx, float* grads_dev, void* stream) {
+    if (!ctx || !grads_dev) return NRRS_ERR_INVALID_ARG;
+    cudaError_t e = cudaMemcpyAsync(grads_dev, ctx->grads, sizeof(float) * ctx->n_params,
+                                    cudaMemcpyDeviceToDevice, (cudaStream_t)stream);
+    return e == cudaSuccess ? NRRS_OK : cuda_fail(ctx, e, "copy grads");
+}
+
+int nrrs_adam_apply(nrrs_ctx* ctx, const float* grads_dev, float scale, void* stream) {
+    if (!ctx || !grads_dev || !std::isfinite(scale)) return NRRS_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (grads_dev != ctx->grads) {
+        cudaError_t e = cudaMemcpyAsync(ctx->grads, grads_dev, sizeof(float) * ctx->n_params,
+                                        cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "copy grads in");
+    }
+    cudaError_t e = launch_adam_step(ctx, ctx->cfg.step >= 3, s, scale);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "adam launch");
+    return refresh_derived(ctx, s, false);
 }
 
 int nrrs_train_step(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* target, uint32_t n,

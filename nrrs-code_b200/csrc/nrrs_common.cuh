@@ -250,6 +250,9 @@ __device__ __forceinline__ float rrs_factor(const FactorParams& fp, const float*
     return rrs;
 }
 
+// status sink for kernels launched without a context scratch
+static __device__ unsigned int g_dummy_status;
+
 // exact fixed-point term of the normalisation sum (truncation toward zero)
 __device__ __forceinline__ long long fixed_term(const FactorParams& fp, float rrs,
                                                 unsigned int* status) {

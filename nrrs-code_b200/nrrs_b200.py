@@ -121,6 +121,18 @@ _SIGS = {
                                            C.c_uint32, C.c_uint32, C.POINTER(DecideParams),
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                            C.c_void_p, C.c_void_p]),
+    "nrrs_infer_accumulate": (C.c_int, [C.c_void_p, C.POINTER(VertexSoA), C.c_uint32,
+                                        C.POINTER(DecideParams), C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p]),
+    "nrrs_decide_emit_with_sum": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                            C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p,
+                                            C.POINTER(DecideParams), C.c_void_p, C.c_void_p,
+                                            C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    "nrrs_sum_from_accumulator": (C.c_double, [C.c_void_p, C.POINTER(DecideParams), C.c_int64]),
+    "nrrs_train_grads": (C.c_int, [C.c_void_p, C.POINTER(VertexSoA), C.c_void_p, C.c_uint32,
+                                   C.c_void_p, C.c_void_p]),
+    "nrrs_copy_grads": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "nrrs_adam_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_void_p]),
     "nrrs_launch_count": (C.c_uint64, [C.c_void_p]),
     "nrrs_last_infer_grid": (C.c_int32, [C.c_void_p]),
     "nrrs_kernel_name": (C.c_char_p, [C.c_int32]),
@@ -297,6 +309,30 @@ class NRRSNetwork:
     def train(self, soa: VertexSoA, target, n: int, loss_dev=None, stream=0):
         return self._check(lib().nrrs_train_step(self._h, C.byref(soa), _ptr(target), n,
                                                  _ptr(loss_dev), stream))
+
+    # ---- sharded (multi-GPU) building blocks ----
+    def inferAccumulate(self, soa: VertexSoA, n: int, params: DecideParams, stats, rrs, sum_acc,
+                        stream=0):
+        return self._check(lib().nrrs_infer_accumulate(self._h, C.byref(soa), n, C.byref(params),
+                                                       _ptr(stats), _ptr(rrs), _ptr(sum_acc),
+                                                       stream))
+
+    def decideEmitWithSum(self, rrs, rnd, n, budget, n_specular, sum_acc, params, rrs_norm, split,
+                          queue, capacity, next_size, scatter_index=None, stream=0):
+        return self._check(lib().nrrs_decide_emit_with_sum(
+            self._h, _ptr(rrs), _ptr(rnd), _ptr(scatter_index), n, budget, n_specular,
+            _ptr(sum_acc), C.byref(params), _ptr(rrs_norm), _ptr(split), _ptr(queue), capacity,
+            _ptr(next_size), stream))
+
+    def trainGrads(self, soa: VertexSoA, target, n: int, loss_dev=None, stream=0):
+        return self._check(lib().nrrs_train_grads(self._h, C.byref(soa), _ptr(target), n,
+                                                  _ptr(loss_dev), stream))
+
+    def copyGrads(self, grads_dev, stream=0):
+        return self._check(lib().nrrs_copy_grads(self._h, _ptr(grads_dev), stream))
+
+    def adamApply(self, grads_dev, scale: float, stream=0):
+        return self._check(lib().nrrs_adam_apply(self._h, _ptr(grads_dev), scale, stream))
 
     def saveWeights(self, path: str | os.PathLike):
         self._check(lib().nrrs_save(self._h, str(path).encode()))

@@ -274,6 +274,12 @@ int64_t oracle_sum_fixed(const float* rrs, uint64_t n, int use_ceil, int shift, 
  *        s   = int(r); s += (rnd <= r - s)                          (:1415-1416, :1454)
  *      Order of the queue: vertex order, the s copies of one vertex contiguous (the
  *      reference's order is atomic-arrival; the multiset is the same). ---- */
+static uint64_t decide_core(const float* rrs, const float* rnd, const uint32_t* scatter_index,
+                            uint64_t n, uint32_t budget, uint32_t n_specular,
+                            const nrrs_decide_params* p, double sum, float* rrs_norm,
+                            uint8_t* split, uint32_t* queue, uint64_t capacity, uint32_t flags,
+                            uint32_t* status_flags);
+
 uint64_t oracle_decide_emit(const float* rrs, const float* rnd, const uint32_t* scatter_index,
                             uint64_t n, uint32_t budget, uint32_t n_specular,
                             const nrrs_decide_params* p, uint64_t shift_n, float* rrs_norm,
@@ -288,6 +294,25 @@ uint64_t oracle_decide_emit(const float* rrs, const float* rnd, const uint32_t* 
         if (!isfinite(x)) flags |= NRRS_DEV_NAN;
     }
     oracle_sum_fixed(rrs, n, p->use_ceil, shift, &sum);
+    return decide_core(rrs, rnd, scatter_index, n, budget, n_specular, p, sum, rrs_norm, split,
+                       queue, capacity, flags, status_flags);
+}
+
+/* the same decision for one shard of a queue, with the exact sum accumulated over all shards */
+uint64_t oracle_decide_emit_acc(const float* rrs, const float* rnd, const uint32_t* scatter_index,
+                                uint64_t n, uint32_t budget, uint32_t n_specular,
+                                const nrrs_decide_params* p, int64_t acc, int shift,
+                                float* rrs_norm, uint8_t* split, uint32_t* queue,
+                                uint64_t capacity, uint32_t* status_flags) {
+    return decide_core(rrs, rnd, scatter_index, n, budget, n_specular, p, ldexp((double)acc, -shift),
+                       rrs_norm, split, queue, capacity, 0u, status_flags);
+}
+
+static uint64_t decide_core(const float* rrs, const float* rnd, const uint32_t* scatter_index,
+                            uint64_t n, uint32_t budget, uint32_t n_specular,
+                            const nrrs_decide_params* p, double sum, float* rrs_norm,
+                            uint8_t* split, uint32_t* queue, uint64_t capacity, uint32_t flags,
+                            uint32_t* status_flags) {
     volatile float sumf = (float)sum;
     volatile float rcp = 1.0f / sumf;
     volatile float bud = (float)(uint32_t)(budget - n_specular);

@@ -59,6 +59,13 @@ uint64_t oracle_decide_emit(const float* rrs, const float* rnd, const uint32_t* 
                             uint8_t* split, uint32_t* queue, uint64_t capacity,
                             uint32_t* status_flags);
 
+/* decision of one shard given the exact accumulator of all shards (acc * 2^-shift = sum) */
+uint64_t oracle_decide_emit_acc(const float* rrs, const float* rnd, const uint32_t* scatter_index,
+                                uint64_t n, uint32_t budget, uint32_t n_specular,
+                                const nrrs_decide_params* p, int64_t acc, int shift,
+                                float* rrs_norm, uint8_t* split, uint32_t* queue,
+                                uint64_t capacity, uint32_t* status_flags);
+
 /* training: losses and gradients (no update). grads has nrrs_param_count entries.
  * loss[0] = StatNet relative log-L2, loss[1] = RRSNet variance x cost (0 when step < 3). */
 void oracle_train_grads_f64(const nrrs_config* cfg, const float* params, uint64_t n,

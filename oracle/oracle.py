@@ -62,6 +62,10 @@ def lib():
         L.oracle_decide_emit.argtypes = [vp, vp, vp, C.c_uint64, C.c_uint32, C.c_uint32,
                                          C.POINTER(nb.DecideParams), C.c_uint64, vp, vp, vp,
                                          C.c_uint64, C.POINTER(C.c_uint32)]
+        L.oracle_decide_emit_acc.restype = C.c_uint64
+        L.oracle_decide_emit_acc.argtypes = [vp, vp, vp, C.c_uint64, C.c_uint32, C.c_uint32,
+                                             C.POINTER(nb.DecideParams), C.c_int64, C.c_int, vp,
+                                             vp, vp, C.c_uint64, C.POINTER(C.c_uint32)]
         for f in ("oracle_train_grads_f64", "oracle_train_grads_f32"):
             getattr(L, f).argtypes = [C.POINTER(nb.Config), vp, C.c_uint64, C.POINTER(nb.VertexSoA),
                                       vp, vp, vp]
@@ -145,6 +149,23 @@ def decide_emit(rrs, rnd, budget, n_specular, dp, capacity=None, scatter_index=N
                                      n_specular, C.byref(dp), shift_n, rrs_norm.ctypes.data,
                                      split.ctypes.data, queue.ctypes.data, cap, C.byref(flags))
     return {"queue": queue[:min(int(total), cap)], "total": int(total), "rrs_norm": rrs_norm[:nstid],
+            "split": split[:n], "flags": int(flags.value)}
+
+
+def decide_emit_acc(rrs, rnd, budget, n_specular, dp, acc: int, shift: int, capacity=None):
+    """decision of one shard with the exact accumulator summed over all shards"""
+    rrs = np.ascontiguousarray(rrs, np.float32)
+    rnd = np.ascontiguousarray(rnd, np.float32)
+    n = rrs.size
+    cap = capacity if capacity is not None else int(n * (dp.clamp_max + 2)) + 8
+    queue = np.zeros(max(cap, 1), np.uint32)
+    rrs_norm = np.zeros(max(n, 1), np.float32)
+    split = np.zeros(max(n, 1), np.uint8)
+    flags = C.c_uint32()
+    total = lib().oracle_decide_emit_acc(rrs.ctypes.data, rnd.ctypes.data, None, n, budget,
+                                         n_specular, C.byref(dp), acc, shift, rrs_norm.ctypes.data,
+                                         split.ctypes.data, queue.ctypes.data, cap, C.byref(flags))
+    return {"queue": queue[:min(int(total), cap)], "total": int(total), "rrs_norm": rrs_norm[:n],
             "split": split[:n], "flags": int(flags.value)}
 
 
