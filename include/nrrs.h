@@ -263,6 +263,31 @@ int nrrs_load(nrrs_ctx* ctx, const char* path);
 /* ---- status: synchronises the stream, returns and clears the device status bits ---- */
 int nrrs_get_device_status(nrrs_ctx* ctx, uint32_t* flags, void* stream);
 
+/* ---- launch shape and autotuning (no counterpart in the reference, whose launches come from
+ *      the occupancy API, commoncudautilshost.cpp:10-21). The inference kernel's shape is
+ *      CTAs per SM x warpgroups per CTA (tcgen05 path; the FP32 path uses CTAs per SM only).
+ *      nrrs_autotune times every admissible shape on n synthetic vertices, keeps the fastest in
+ *      the context and, with a cache path, reuses or records the choice in a JSON file keyed by
+ *      device name, network shape and precision. report (may be NULL) receives a JSON summary.
+ *      Synchronous. ---- */
+int nrrs_autotune(nrrs_ctx* ctx, uint32_t n, const char* cache_path, char* report,
+                  size_t report_len);
+int nrrs_set_launch_shape(nrrs_ctx* ctx, int32_t ctas_per_sm, int32_t warpgroups);
+int nrrs_get_launch_shape(const nrrs_ctx* ctx, int32_t* ctas_per_sm, int32_t* warpgroups);
+
+/* ---- CUDA graph of the batched step: captures nrrs_step_batched on a private stream and
+ *      instantiates it; each nrrs_graph_launch replays the whole multi-depth step (inference
+ *      over all depths, then the decision and emission of all depths) with one launch. The
+ *      buffers and segment table are those given at capture. ---- */
+typedef struct nrrs_graph nrrs_graph;
+int nrrs_graph_capture_batched(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* rnd,
+                               const nrrs_segment* segs, int32_t n_segs,
+                               const nrrs_decide_params* p, float* stats, float* rrs,
+                               float* rrs_norm, uint8_t* split, uint32_t* next_queue,
+                               uint32_t* next_size_dev, nrrs_graph** out);
+int nrrs_graph_launch(nrrs_graph* g, void* stream);
+void nrrs_graph_destroy(nrrs_graph* g);
+
 /* ---- instrumentation: launch counters and optional CUDA-event timing per kernel kind.
  *      The reference's equivalent is KiRaRay's PROFILE("...") scopes (integrator.cpp:1069,
  *      1151, 1158, 1302, 1346, 2638). Timing records one event pair per launch on the launch

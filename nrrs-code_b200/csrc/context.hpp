@@ -58,6 +58,8 @@ struct nrrs_ctx {
 
     int last_infer_grid = 0;
     int tc_ctas_per_sm = 0;      // autotuned occupancy of the tcgen05 kernel (0 = default)
+    int tc_wgs = 1;              // autotuned warpgroups per CTA of the tcgen05 kernel (1 or 2)
+    int simt_ctas_per_sm = 0;    // autotuned occupancy of the FP32 kernel (0 = default)
     nrrs::Profiler prof;
     std::string last_error;
 };

@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(kTile) k_infer_fp32(const __grid_constant__ In
 }
 
 template <int WS, int HS, int WR, int HR>
-cudaError_t launch_cfg(const InferArgs& a, int sm_count, cudaStream_t s) {
+cudaError_t launch_cfg(const InferArgs& a, int sm_count, int ctas_per_sm, cudaStream_t s) {
     constexpr int NS = MlpShape<WS, HS, kStatIn, kStatOut>::kFloats;
     constexpr int NR = MlpShape<WR, HR, kRrsIn, 1>::kFloats;
     constexpr int XW = (WS > WR ? WS : WR) > kStatIn ? (WS > WR ? WS : WR) : kStatIn;
@@ -169,7 +169,8 @@ cudaError_t launch_cfg(const InferArgs& a, int sm_count, cudaStream_t s) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    const int per_sm = resident_ctas((const void*)kern, kTile, smem, 32);
+    int per_sm = resident_ctas((const void*)kern, kTile, smem, 32);
+    if (ctas_per_sm > 0 && ctas_per_sm < per_sm) per_sm = ctas_per_sm;
     unsigned grid = (unsigned)(sm_count * per_sm);
     if (grid > a.segs.total_tiles) grid = a.segs.total_tiles;
     if (grid == 0) return cudaSuccess;
@@ -181,12 +182,37 @@ cudaError_t launch_cfg(const InferArgs& a, int sm_count, cudaStream_t s) {
 }  // namespace
 
 cudaError_t launch_infer_fp32(const InferArgs& a, int ws, int hs, int wr, int hr, int sm_count,
-                              cudaStream_t s) {
-    if (ws == 64 && hs == 2 && wr == 64 && hr == 2) return launch_cfg<64, 2, 64, 2>(a, sm_count, s);
+                              int ctas_per_sm, cudaStream_t s) {
+    if (ws == 64 && hs == 2 && wr == 64 && hr == 2)
+        return launch_cfg<64, 2, 64, 2>(a, sm_count, ctas_per_sm, s);
     if (ws == 128 && hs == 3 && wr == 128 && hr == 3)
-        return launch_cfg<128, 3, 128, 3>(a, sm_count, s);
-    if (ws == 64 && hs == 3 && wr == 64 && hr == 3) return launch_cfg<64, 3, 64, 3>(a, sm_count, s);
+        return launch_cfg<128, 3, 128, 3>(a, sm_count, ctas_per_sm, s);
+    if (ws == 64 && hs == 3 && wr == 64 && hr == 3)
+        return launch_cfg<64, 3, 64, 3>(a, sm_count, ctas_per_sm, s);
     return cudaErrorInvalidValue;
+}
+
+template <int WS, int HS, int WR, int HR>
+int max_ctas_fp32() {
+    constexpr int NS = MlpShape<WS, HS, kStatIn, kStatOut>::kFloats;
+    constexpr int NR = MlpShape<WR, HR, kRrsIn, 1>::kFloats;
+    constexpr int XW = (WS > WR ? WS : WR) > kStatIn ? (WS > WR ? WS : WR) : kStatIn;
+    constexpr size_t xs_bytes = (size_t)XW * kTile * sizeof(float);
+    constexpr size_t w_bytes = (size_t)(NS + NR) * sizeof(float);
+    constexpr bool fits = xs_bytes + w_bytes <= 200 * 1024;
+    const size_t smem = fits ? xs_bytes + w_bytes : xs_bytes;
+    auto kern = k_infer_fp32<WS, HS, WR, HR, fits>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return 0;
+    return resident_ctas((const void*)kern, kTile, smem, 32);
+}
+
+int infer_max_ctas_fp32(int ws, int hs) {
+    if (ws == 64 && hs == 2) return max_ctas_fp32<64, 2, 64, 2>();
+    if (ws == 64 && hs == 3) return max_ctas_fp32<64, 3, 64, 3>();
+    if (ws == 128 && hs == 3) return max_ctas_fp32<128, 3, 128, 3>();
+    return 0;
 }
 
 }  // namespace nrrs

@@ -1,7 +1,7 @@
 // k_infer_tc.cu -- mixed-precision inference on the 5th-generation tensor cores (sm_100a).
 //
-// One CTA (one warpgroup, 128 threads) owns a 128-vertex tile at a time and runs the whole
-// per-vertex chain of the reference's inference (train.cu:269-287 data prep, tcnn HashGrid +
+// Each warpgroup (128 threads) owns a 128-vertex tile at a time and runs the whole per-vertex
+// chain of the reference's inference (train.cu:269-287 data prep, tcnn HashGrid +
 // FullyFusedMLP for StatNet and RRSNet, train.cu:41-112 glue, integrator.cpp:1184-1298 factor):
 //
 //   FP16 hash-table gathers + SH + misc lanes -> A tile [128 x 64] fp16/bf16 in shared memory
@@ -12,16 +12,18 @@
 //
 // Weights of both networks stay resident in shared memory for the CTA's lifetime; they are
 // loaded once by bulk TMA copies (cp.async.bulk, unicast) from an image that k_util.cu packs in
-// the canonical no-swizzle K-major core-matrix layout. Several CTAs per SM overlap the gather
-// phase of one tile with the MMA chain of another. Every wait is bounded (NRRS_DEV_TIMEOUT).
+// the canonical no-swizzle K-major core-matrix layout. A CTA holds WGS warpgroups that share
+// that weight copy, each with its own A tile, mbarrier, TMEM columns and named barrier, so the
+// gather phase of one tile overlaps the MMA chain of another; CTAs per SM and WGS are the
+// autotuner's knobs. Every wait is bounded (NRRS_DEV_TIMEOUT).
 #include "kernels.hpp"
-#include "tc_ptx.cuh"
+#include "tc_tile.cuh"
 
 namespace nrrs {
 
 namespace {
 
-constexpr uint32_t kSpin = 1u << 24;
+using namespace tile;
 
 template <int W, int H, int IN>
 struct PackedNet {
@@ -31,42 +33,28 @@ struct PackedNet {
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
 constexpr int tmem_cols(int w) { return w <= 32 ? 32 : (w <= 64 ? 64 : (w <= 128 ? 128 : 256)); }
 
-template <int WS, int HS, int WR, int HR>
+template <int WS, int HS, int WR, int HR, int WGS>
 struct TcShape {
     static constexpr int kStatElems = PackedNet<WS, HS, kStatIn>::kElems;
     static constexpr int kRrsElems = PackedNet<WR, HR, kRrsIn>::kElems;
     static constexpr uint32_t kWBytes = (uint32_t)(kStatElems + kRrsElems) * 2u;
     static constexpr int kKMax = cmax(64, cmax(WS, WR));
     static constexpr uint32_t kABytes = 128u * kKMax * 2u;
-    static constexpr uint32_t kCols = (uint32_t)tmem_cols(cmax(WS, WR));
-    static constexpr uint32_t kWOff = 0;
+    static constexpr uint32_t kColsWg = (uint32_t)tmem_cols(cmax(WS, WR));
+    static constexpr uint32_t kCols = kColsWg * WGS;
     static constexpr uint32_t kAOff = (kWBytes + 1023u) / 1024u * 1024u;
-    static constexpr uint32_t kBarOff = kAOff + kABytes;
+    static constexpr uint32_t kBarOff = kAOff + WGS * kABytes;
     static constexpr size_t kSmem = 1024 + kBarOff + 64;
 };
 
-template <bool BF>
-__device__ __forceinline__ uint32_t pack2(float a, float b) {
-    if constexpr (BF) {
-        __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
-        return *reinterpret_cast<uint32_t*>(&h);
-    } else {
-        __half2 h = __floats2half2_rn(a, b);
-        return *reinterpret_cast<uint32_t*>(&h);
-    }
+// named barrier of one warpgroup (id 0 is __syncthreads)
+__device__ __forceinline__ void wg_sync(int wg) {
+    asm volatile("bar.sync %0, 128;" ::"r"(1 + wg) : "memory");
 }
-
-// 8 consecutive K elements of row m into the core-matrix layout of a [128 x K] A tile
-__device__ __forceinline__ void store_chunk(uint8_t* sA, int m, int kchunk, int K, uint4 v) {
-    const uint32_t off = (uint32_t)(m >> 3) * (uint32_t)(K * 16) + (uint32_t)kchunk * 128u +
-                         (uint32_t)(m & 7) * 16u;
-    *reinterpret_cast<uint4*>(sA + off) = v;
-}
-
-template <bool BF>
-__device__ __forceinline__ uint4 pack8(const float* f) {
-    return make_uint4(pack2<BF>(f[0], f[1]), pack2<BF>(f[2], f[3]), pack2<BF>(f[4], f[5]),
-                      pack2<BF>(f[6], f[7]));
+__device__ __forceinline__ void wg_sync_for_mma(int wg) {
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    wg_sync(wg);
 }
 
 // StatNet input row of vertex i into A (K = 64): hash grid (FP16 table) + SH + misc + zeros
@@ -82,24 +70,9 @@ __device__ __forceinline__ void encode_row_tc(const InferArgs& a, uint32_t i, ui
         for (int j = 0; j < 4; ++j) {
             const LevelDev L = a.enc.lv[lq * 4 + j];
             const CellCoord c = cell_of(p, L.res);
-            uint32_t rows[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k)
-                rows[k] = grid_row(L, a.enc.hash_mask, c.ix + (k & 1), c.iy + ((k >> 1) & 1),
-                                   c.iz + ((k >> 2) & 1));
-            __half2 t[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) t[k] = __ldg(table + rows[k]);
-            float f0 = 0.f, f1 = 0.f;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const float w = corner_weight(c, k);
-                const float2 tv = __half22float2(t[k]);
-                f0 += w * tv.x;
-                f1 += w * tv.y;
-            }
-            f[2 * j] = f0;
-            f[2 * j + 1] = f1;
+            const float2 fv = level_features_h(table, L, a.enc.hash_mask, c);
+            f[2 * j] = fv.x;
+            f[2 * j + 1] = fv.y;
         }
         store_chunk(sA, m, lq, 64, pack8<BF>(f));
     }
@@ -114,11 +87,11 @@ __device__ __forceinline__ void encode_row_tc(const InferArgs& a, uint32_t i, ui
     store_chunk(sA, m, 7, 64, make_uint4(0u, 0u, 0u, 0u));
 }
 
-// issue one layer (thread 0), then everybody waits for its completion
+// one layer issued by the warpgroup's first thread; the warpgroup waits for its completion
 template <int K, int N, bool BF>
 __device__ __forceinline__ bool tc_layer(const uint8_t* sA, const uint8_t* sWl, uint32_t tmem,
-                                         uint64_t* bar, uint32_t& phase, int tid) {
-    if (tid == 0) {
+                                         uint64_t* bar, uint32_t& phase, int ltid) {
+    if (ltid == 0) {
         tc::fence_after_sync();
         const uint32_t a0 = tc::smem_u32(sA), b0 = tc::smem_u32(sWl);
         constexpr uint32_t idesc = tc::idesc_f16(N, BF ? 1u : 0u);
@@ -136,46 +109,26 @@ __device__ __forceinline__ bool tc_layer(const uint8_t* sA, const uint8_t* sWl, 
     return ok;
 }
 
-// hidden-layer epilogue: TMEM row -> ReLU -> next A tile (K = N)
-template <int N, bool BF>
-__device__ __forceinline__ void epilogue_hidden(uint32_t trow, uint8_t* sA, int m) {
-#pragma unroll
-    for (int c0 = 0; c0 < N; c0 += 32) {
-        float v[32];
-        tc::tmem_ld16(trow + c0, v);
-        tc::tmem_ld16(trow + c0 + 16, v + 16);
-        tc::tmem_wait_ld();
-#pragma unroll
-        for (int j = 0; j < 32; ++j) v[j] = fmaxf(v[j], 0.f);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) store_chunk(sA, m, c0 / 8 + j, N, pack8<BF>(v + 8 * j));
-    }
-}
-
-__device__ __forceinline__ void sync_for_mma() {
-    tc::fence_async_smem();
-    tc::fence_before_sync();
-    __syncthreads();
-}
-
-template <int WS, int HS, int WR, int HR, bool BF>
-__global__ void __launch_bounds__(128, 1) k_infer_tc(const __grid_constant__ InferArgs a) {
-    using S = TcShape<WS, HS, WR, HR>;
+template <int WS, int HS, int WR, int HR, bool BF, int WGS>
+__global__ void __launch_bounds__(128 * WGS, WGS == 2 ? 3 : 1) k_infer_tc(const __grid_constant__ InferArgs a) {
+    using S = TcShape<WS, HS, WR, HR, WGS>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* base = reinterpret_cast<uint8_t*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023u) & ~uintptr_t(1023));
-    uint8_t* sW = base + S::kWOff;
-    uint8_t* sA = base + S::kAOff;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(base + S::kBarOff);  // [0] weights, [1] mma
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2);
-    __shared__ int s_abort;
+    uint8_t* sW = base;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(base + S::kBarOff);  // [0] weights, [1+wg] mma
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 1 + WGS);
+    __shared__ int s_abort[WGS];
+    __shared__ int s_wabort;
     const int tid = threadIdx.x, warp = tid >> 5;
+    const int wg = tid >> 7, ltid = tid & 127;
+    uint8_t* sA = base + S::kAOff + wg * S::kABytes;
 
     if (tid == 0) {
-        tc::mbar_init(&bars[0], 1);
-        tc::mbar_init(&bars[1], 1);
+        for (int k = 0; k < 1 + WGS; ++k) tc::mbar_init(&bars[k], 1);
         tc::fence_mbar_init();
-        s_abort = 0;
+        for (int k = 0; k < WGS; ++k) s_abort[k] = 0;
+        s_wabort = 0;
     }
     if (warp == 0) {
         tc::tmem_alloc(tslot, S::kCols);
@@ -184,7 +137,7 @@ __global__ void __launch_bounds__(128, 1) k_infer_tc(const __grid_constant__ Inf
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    const uint32_t tmem = *tslot;
+    const uint32_t tmem = *tslot + (uint32_t)wg * S::kColsWg;
     if (tid == 0) {
         tc::mbar_arrive_expect_tx(&bars[0], S::kWBytes);
         const uint8_t* src = reinterpret_cast<const uint8_t*>(a.wpack);
@@ -194,11 +147,13 @@ __global__ void __launch_bounds__(128, 1) k_infer_tc(const __grid_constant__ Inf
         }
     }
     unsigned flags = 0;
-    if (!tc::mbar_wait(&bars[0], 0, kSpin)) s_abort = 1;
+    if (!tc::mbar_wait(&bars[0], 0, kSpin)) s_wabort = 1;
     __syncthreads();
-    if (s_abort) flags |= NRRS_DEV_TIMEOUT;  // uniform across the CTA
+    if (s_wabort) flags |= NRRS_DEV_TIMEOUT;  // uniform across the CTA
+    uint64_t* mbar = &bars[1 + wg];
     uint32_t phase = 0;
-    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    // warp w of a warpgroup reads TMEM lanes 32*(w % 4) .. +31, i.e. rows of its own threads
+    const uint32_t trow = tmem + ((uint32_t)((warp & 3) * 32) << 16);
 
     const uint8_t* wS0 = sW;
     const uint8_t* wSh = wS0 + WS * kStatIn * 2;
@@ -207,31 +162,28 @@ __global__ void __launch_bounds__(128, 1) k_infer_tc(const __grid_constant__ Inf
     const uint8_t* wRh = wR0 + WR * kRrsIn * 2;
     const uint8_t* wRo = wRh + (HR - 1) * WR * WR * 2;
 
-    for (uint32_t t = blockIdx.x; t < a.segs.total_tiles && !flags; t += gridDim.x) {
+    for (uint32_t t = blockIdx.x * WGS + wg; t < a.segs.total_tiles && !flags;
+         t += gridDim.x * WGS) {
         const int si = find_segment(a.segs, t);
         const Segment& sg = a.segs.s[si];
-        const uint32_t i = sg.offset + (t - sg.tile_start) * kTile + tid;
+        const uint32_t i = sg.offset + (t - sg.tile_start) * kTile + ltid;
         const bool valid = i < sg.offset + sg.count;
 
-        if (valid) {
-            encode_row_tc<BF>(a, i, sA, tid);
-        } else {
-#pragma unroll
-            for (int kc = 0; kc < 8; ++kc) store_chunk(sA, tid, kc, 64, make_uint4(0u, 0u, 0u, 0u));
-        }
-        sync_for_mma();
+        if (valid) encode_row_tc<BF>(a, i, sA, ltid);
+        else zero_row(sA, ltid, 64);
+        wg_sync_for_mma(wg);
 
         // ---- StatNet ----
-        bool ok = tc_layer<kStatIn, WS, BF>(sA, wS0, tmem, &bars[1], phase, tid);
-        epilogue_hidden<WS, BF>(trow, sA, tid);
-        sync_for_mma();
+        bool ok = tc_layer<kStatIn, WS, BF>(sA, wS0, tmem, mbar, phase, ltid);
+        epilogue_relu<WS, BF>(trow, sA, ltid);
+        wg_sync_for_mma(wg);
 #pragma unroll 1
         for (int h = 1; h < HS; ++h) {
-            ok &= tc_layer<WS, WS, BF>(sA, wSh + (h - 1) * WS * WS * 2, tmem, &bars[1], phase, tid);
-            epilogue_hidden<WS, BF>(trow, sA, tid);
-            sync_for_mma();
+            ok &= tc_layer<WS, WS, BF>(sA, wSh + (h - 1) * WS * WS * 2, tmem, mbar, phase, ltid);
+            epilogue_relu<WS, BF>(trow, sA, ltid);
+            wg_sync_for_mma(wg);
         }
-        ok &= tc_layer<WS, 16, BF>(sA, wSo, tmem, &bars[1], phase, tid);
+        ok &= tc_layer<WS, 16, BF>(sA, wSo, tmem, mbar, phase, ltid);
         float y[16];
         tc::tmem_ld16(trow, y);
         tc::tmem_wait_ld();
@@ -244,26 +196,26 @@ __global__ void __launch_bounds__(128, 1) k_infer_tc(const __grid_constant__ Inf
 #pragma unroll
             for (int k = 0; k < 16; ++k) x1[k] = 0.f;
         }
-        store_chunk(sA, tid, 0, 16, pack8<BF>(x1));
-        store_chunk(sA, tid, 1, 16, pack8<BF>(x1 + 8));
-        sync_for_mma();
+        store_chunk(sA, ltid, 0, 16, pack8<BF>(x1));
+        store_chunk(sA, ltid, 1, 16, pack8<BF>(x1 + 8));
+        wg_sync_for_mma(wg);
 
         // ---- RRSNet ----
-        ok &= tc_layer<kRrsIn, WR, BF>(sA, wR0, tmem, &bars[1], phase, tid);
-        epilogue_hidden<WR, BF>(trow, sA, tid);
-        sync_for_mma();
+        ok &= tc_layer<kRrsIn, WR, BF>(sA, wR0, tmem, mbar, phase, ltid);
+        epilogue_relu<WR, BF>(trow, sA, ltid);
+        wg_sync_for_mma(wg);
 #pragma unroll 1
         for (int h = 1; h < HR; ++h) {
-            ok &= tc_layer<WR, WR, BF>(sA, wRh + (h - 1) * WR * WR * 2, tmem, &bars[1], phase, tid);
-            epilogue_hidden<WR, BF>(trow, sA, tid);
-            sync_for_mma();
+            ok &= tc_layer<WR, WR, BF>(sA, wRh + (h - 1) * WR * WR * 2, tmem, mbar, phase, ltid);
+            epilogue_relu<WR, BF>(trow, sA, ltid);
+            wg_sync_for_mma(wg);
         }
-        ok &= tc_layer<WR, 16, BF>(sA, wRo, tmem, &bars[1], phase, tid);
+        ok &= tc_layer<WR, 16, BF>(sA, wRo, tmem, mbar, phase, ltid);
         float r[16];
         tc::tmem_ld16(trow, r);
         tc::tmem_wait_ld();
         tc::fence_before_sync();
-        __syncthreads();  // TMEM and A are free for the next tile
+        wg_sync(wg);  // TMEM columns and A tile free for the next tile
 
         if (!ok) flags |= NRRS_DEV_TIMEOUT;
         long long term = 0;
@@ -275,17 +227,18 @@ __global__ void __launch_bounds__(128, 1) k_infer_tc(const __grid_constant__ Inf
                 a.stats[3 * (size_t)i + 2] = y[2];
             }
             a.rrs[i] = rrs;
-            if (a.scr || a.ext_acc) term = fixed_term(a.fp, rrs, a.scr ? &a.scr->status : &g_dummy_status);
+            if (a.scr || a.ext_acc)
+                term = fixed_term(a.fp, rrs, a.scr ? &a.scr->status : &g_dummy_status);
         }
         if (a.scr || a.ext_acc) {
             term = warp_sum_ll(term);
             if ((tid & 31) == 0 && term != 0)
                 atomicAdd(a.ext_acc ? a.ext_acc : &a.scr->sum_acc[si], (unsigned long long)term);
         }
-        // all threads agree on the abort decision
-        if (flags) s_abort = 1;
-        __syncthreads();
-        if (s_abort) flags |= NRRS_DEV_TIMEOUT;
+        // the warpgroup agrees on the abort decision
+        if (flags) s_abort[wg] = 1;
+        wg_sync(wg);
+        if (s_abort[wg]) flags |= NRRS_DEV_TIMEOUT;
     }
 
     if (flags && a.scr) atomicOr(&a.scr->status, flags);
@@ -293,49 +246,88 @@ __global__ void __launch_bounds__(128, 1) k_infer_tc(const __grid_constant__ Inf
     __syncthreads();
     if (warp == 0) {
         tc::fence_after_sync();
-        tc::tmem_dealloc(tmem, S::kCols);
+        tc::tmem_dealloc(*tslot, S::kCols);
     }
 }
 
-template <int WS, int HS, int WR, int HR, bool BF>
+template <int WS, int HS, int WR, int HR, bool BF, int WGS>
 cudaError_t launch_tc(const InferArgs& a, int sm_count, int ctas_per_sm, cudaStream_t s) {
-    using S = TcShape<WS, HS, WR, HR>;
-    auto kern = k_infer_tc<WS, HS, WR, HR, BF>;
+    using S = TcShape<WS, HS, WR, HR, WGS>;
+    if (S::kSmem > 232448) return cudaErrorInvalidConfiguration;
+    auto kern = k_infer_tc<WS, HS, WR, HR, BF, WGS>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)S::kSmem);
     if (e != cudaSuccess) return e;
     // TMEM: the CTAs resident on one SM must fit in its 512 columns
-    int per_sm = resident_ctas((const void*)kern, 128, S::kSmem, 512 / (int)S::kCols);
+    int per_sm = resident_ctas((const void*)kern, 128 * WGS, S::kSmem, 512 / (int)S::kCols);
     if (ctas_per_sm > 0 && ctas_per_sm < per_sm) per_sm = ctas_per_sm;
+    const uint32_t ctas_needed = (a.segs.total_tiles + WGS - 1) / WGS;
     unsigned grid = (unsigned)(sm_count * per_sm);
-    if (grid > a.segs.total_tiles) grid = a.segs.total_tiles;
+    if (grid > ctas_needed) grid = ctas_needed;
     if (grid == 0) return cudaSuccess;
     g_last_grid = (int)grid;
-    kern<<<grid, 128, S::kSmem, s>>>(a);
+    kern<<<grid, 128 * WGS, S::kSmem, s>>>(a);
     return cudaGetLastError();
+}
+
+template <int WS, int HS, int WR, int HR, bool BF>
+cudaError_t launch_wgs(const InferArgs& a, int sm_count, int ctas_per_sm, int wgs,
+                       cudaStream_t s) {
+    if (wgs == 2) return launch_tc<WS, HS, WR, HR, BF, 2>(a, sm_count, ctas_per_sm, s);
+    return launch_tc<WS, HS, WR, HR, BF, 1>(a, sm_count, ctas_per_sm, s);
+}
+
+template <int WS, int HS, int WR, int HR, bool BF, int WGS>
+int max_ctas_tc() {
+    using S = TcShape<WS, HS, WR, HR, WGS>;
+    if (S::kSmem > 232448) return 0;
+    auto kern = k_infer_tc<WS, HS, WR, HR, BF, WGS>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kSmem) !=
+        cudaSuccess)
+        return 0;
+    return resident_ctas((const void*)kern, 128 * WGS, S::kSmem, 512 / (int)S::kCols);
 }
 
 }  // namespace
 
+int infer_max_ctas_fp32(int ws, int hs);
+
+int infer_max_ctas(int ws, int hs, int wr, int hr, int prec, int wgs) {
+    (void)wr;
+    (void)hr;
+    if (prec == NRRS_PREC_FP32) return wgs == 1 ? infer_max_ctas_fp32(ws, hs) : 0;
+    const bool bf = prec == NRRS_PREC_BF16;
+    if (ws == 64 && hs == 2)
+        return wgs == 2 ? (bf ? max_ctas_tc<64, 2, 64, 2, true, 2>() : max_ctas_tc<64, 2, 64, 2, false, 2>())
+                        : (bf ? max_ctas_tc<64, 2, 64, 2, true, 1>() : max_ctas_tc<64, 2, 64, 2, false, 1>());
+    if (ws == 64 && hs == 3)
+        return wgs == 2 ? (bf ? max_ctas_tc<64, 3, 64, 3, true, 2>() : max_ctas_tc<64, 3, 64, 3, false, 2>())
+                        : (bf ? max_ctas_tc<64, 3, 64, 3, true, 1>() : max_ctas_tc<64, 3, 64, 3, false, 1>());
+    if (ws == 128 && hs == 3)
+        return wgs == 2 ? (bf ? max_ctas_tc<128, 3, 128, 3, true, 2>() : max_ctas_tc<128, 3, 128, 3, false, 2>())
+                        : (bf ? max_ctas_tc<128, 3, 128, 3, true, 1>() : max_ctas_tc<128, 3, 128, 3, false, 1>());
+    return 0;
+}
+
 size_t infer_tc_smem_bytes(int ws, int hs, int wr, int hr) {
-    if (ws == 64 && hs == 2) return TcShape<64, 2, 64, 2>::kSmem;
-    if (ws == 64 && hs == 3) return TcShape<64, 3, 64, 3>::kSmem;
-    if (ws == 128 && hs == 3) return TcShape<128, 3, 128, 3>::kSmem;
+    if (ws == 64 && hs == 2) return TcShape<64, 2, 64, 2, 1>::kSmem;
+    if (ws == 64 && hs == 3) return TcShape<64, 3, 64, 3, 1>::kSmem;
+    if (ws == 128 && hs == 3) return TcShape<128, 3, 128, 3, 1>::kSmem;
     return 0;
 }
 
 cudaError_t launch_infer_tc(const InferArgs& a, int ws, int hs, int wr, int hr, int prec,
-                            int sm_count, int ctas_per_sm, cudaStream_t s) {
+                            int sm_count, int ctas_per_sm, int wgs, cudaStream_t s) {
     const bool bf = prec == NRRS_PREC_BF16;
     if (ws == 64 && hs == 2 && wr == 64 && hr == 2)
-        return bf ? launch_tc<64, 2, 64, 2, true>(a, sm_count, ctas_per_sm, s)
-                  : launch_tc<64, 2, 64, 2, false>(a, sm_count, ctas_per_sm, s);
+        return bf ? launch_wgs<64, 2, 64, 2, true>(a, sm_count, ctas_per_sm, wgs, s)
+                  : launch_wgs<64, 2, 64, 2, false>(a, sm_count, ctas_per_sm, wgs, s);
     if (ws == 64 && hs == 3 && wr == 64 && hr == 3)
-        return bf ? launch_tc<64, 3, 64, 3, true>(a, sm_count, ctas_per_sm, s)
-                  : launch_tc<64, 3, 64, 3, false>(a, sm_count, ctas_per_sm, s);
-    if (ws == 128 && hs == 3 && wr == 128 && hr == 3)
-        return bf ? launch_tc<128, 3, 128, 3, true>(a, sm_count, ctas_per_sm, s)
-                  : launch_tc<128, 3, 128, 3, false>(a, sm_count, ctas_per_sm, s);
+        return bf ? launch_wgs<64, 3, 64, 3, true>(a, sm_count, ctas_per_sm, wgs, s)
+                  : launch_wgs<64, 3, 64, 3, false>(a, sm_count, ctas_per_sm, wgs, s);
+    if (ws == 128 && hs == 3 && wr == 128 && hr == 3)  // 158 KB of weights: 1 CTA per SM
+        return bf ? launch_wgs<128, 3, 128, 3, true>(a, sm_count, ctas_per_sm, wgs, s)
+                  : launch_wgs<128, 3, 128, 3, false>(a, sm_count, ctas_per_sm, wgs, s);
     return cudaErrorInvalidValue;
 }
 

@@ -175,18 +175,9 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
                 for (int j = 0; j < 4; ++j) {
                     const LevelDev L = a.enc.lv[lq * 4 + j];
                     const CellCoord c = cell_of(p, L.res);
-                    float f0 = 0.f, f1 = 0.f;
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        const uint32_t row = grid_row(L, a.enc.hash_mask, c.ix + (k & 1),
-                                                      c.iy + ((k >> 1) & 1), c.iz + ((k >> 2) & 1));
-                        const float2 tv = __half22float2(__ldg(table + row));
-                        const float w = corner_weight(c, k);
-                        f0 += w * tv.x;
-                        f1 += w * tv.y;
-                    }
-                    f[2 * j] = f0;
-                    f[2 * j + 1] = f1;
+                    const float2 fv = level_features_h(table, L, a.enc.hash_mask, c);
+                    f[2 * j] = fv.x;
+                    f[2 * j + 1] = fv.y;
                 }
                 store_chunk(sX0, tid, lq, 64, pack8<false>(f));
             }

@@ -65,10 +65,12 @@ cudaError_t launch_decide(const DecideArgs& a, cudaStream_t s);
 cudaError_t launch_sum(const SumArgs& a, cudaStream_t s);
 // FP32 SIMT inference
 cudaError_t launch_infer_fp32(const InferArgs& a, int ws, int hs, int wr, int hr, int sm_count,
-                              cudaStream_t s);
+                              int ctas_per_sm, cudaStream_t s);
+// largest resident CTAs per SM of the inference kernel for a shape (0 = unsupported)
+int infer_max_ctas(int ws, int hs, int wr, int hr, int prec, int wgs);
 // tcgen05 mixed-precision inference
 cudaError_t launch_infer_tc(const InferArgs& a, int ws, int hs, int wr, int hr, int prec,
-                            int sm_count, int ctas_per_sm, cudaStream_t s);
+                            int sm_count, int ctas_per_sm, int wgs, cudaStream_t s);
 size_t infer_tc_smem_bytes(int ws, int hs, int wr, int hr);
 // derived weight copies: FP32 transposed and the UMMA-packed FP16/BF16 images
 cudaError_t launch_pack_weights(const float* master_mlp, float* wt, float* wrow, void* wpack,

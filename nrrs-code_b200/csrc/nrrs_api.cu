@@ -7,7 +7,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
 #include <random>
+#include <sstream>
+#include <string>
 #include <vector>
 
 #include "context.hpp"
@@ -191,10 +194,10 @@ int run_infer(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const SegmentTable& segs,
     ProfScope ps(ctx, c.precision == NRRS_PREC_FP32 ? NRRS_KERNEL_INFER_FP32 : NRRS_KERNEL_INFER_TC, s);
     if (c.precision == NRRS_PREC_FP32)
         e = launch_infer_fp32(a, c.statnet_width, c.statnet_hidden, c.rrsnet_width,
-                              c.rrsnet_hidden, ctx->sm_count, s);
+                              c.rrsnet_hidden, ctx->sm_count, ctx->simt_ctas_per_sm, s);
     else
         e = launch_infer_tc(a, c.statnet_width, c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden,
-                            c.precision, ctx->sm_count, ctx->tc_ctas_per_sm, s);
+                            c.precision, ctx->sm_count, ctx->tc_ctas_per_sm, ctx->tc_wgs, s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "inference launch");
     ctx->last_infer_grid = g_last_grid;
     return NRRS_OK;
@@ -412,7 +415,8 @@ int nrrs_create(const nrrs_config* cfg, nrrs_ctx** out) {
     NRRS_ALLOC(ctx->wt, sizeof(float) * ctx->wt_floats);
     NRRS_ALLOC(ctx->wrow, sizeof(float) * (ctx->n_stat + ctx->n_rrs));
     if (c.precision != NRRS_PREC_FP32) {
-        NRRS_ALLOC(ctx->table_h, sizeof(__half) * ctx->n_table);
+        // 4 spare rows: the paired gathers read whole 16-byte blocks of 4 rows
+        NRRS_ALLOC(ctx->table_h, sizeof(__half) * (ctx->n_table + 8));
         NRRS_ALLOC(ctx->wpack, ctx->wpack_bytes);
     }
     if (train_tc_supported(c))
@@ -816,6 +820,231 @@ int nrrs_profile_read(nrrs_ctx* ctx, int32_t kind, uint64_t* launches, double* t
     p.timed_launches[kind] = 0;
     p.timed_ms[kind] = 0.0;
     return NRRS_OK;
+}
+
+int nrrs_set_launch_shape(nrrs_ctx* ctx, int32_t ctas_per_sm, int32_t warpgroups) {
+    if (!ctx || ctas_per_sm < 0 || ctas_per_sm > 32) return NRRS_ERR_INVALID_ARG;
+    const nrrs_config& c = ctx->cfg;
+    if (c.precision == NRRS_PREC_FP32) {
+        if (warpgroups != 1) return fail(ctx, NRRS_ERR_INVALID_ARG, "the FP32 path has one warpgroup per CTA");
+        ctx->simt_ctas_per_sm = ctas_per_sm;
+        return NRRS_OK;
+    }
+    if (warpgroups != 1 && warpgroups != 2) return fail(ctx, NRRS_ERR_INVALID_ARG, "warpgroups must be 1 or 2");
+    if (infer_max_ctas(c.statnet_width, c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden,
+                       c.precision, warpgroups) <= 0)
+        return fail(ctx, NRRS_ERR_UNSUPPORTED, "launch shape not available for this network");
+    ctx->tc_ctas_per_sm = ctas_per_sm;
+    ctx->tc_wgs = warpgroups;
+    return NRRS_OK;
+}
+
+int nrrs_get_launch_shape(const nrrs_ctx* ctx, int32_t* ctas_per_sm, int32_t* warpgroups) {
+    if (!ctx) return NRRS_ERR_INVALID_ARG;
+    const bool fp32 = ctx->cfg.precision == NRRS_PREC_FP32;
+    if (ctas_per_sm) *ctas_per_sm = fp32 ? ctx->simt_ctas_per_sm : ctx->tc_ctas_per_sm;
+    if (warpgroups) *warpgroups = fp32 ? 1 : ctx->tc_wgs;
+    return NRRS_OK;
+}
+
+namespace {
+
+std::string tune_key(const nrrs_ctx* ctx) {
+    cudaDeviceProp prop{};
+    cudaGetDeviceProperties(&prop, ctx->device);
+    const nrrs_config& c = ctx->cfg;
+    std::ostringstream k;
+    k << prop.name << "|sm" << ctx->sm_count << "|w" << c.statnet_width << "h" << c.statnet_hidden
+      << "|p" << c.precision << "|T" << c.log2_hashmap_size;
+    return k.str();
+}
+
+// the cache is a JSON object of lines  "key": [ctas_per_sm, warpgroups],
+bool cache_lookup(const char* path, const std::string& key, int* ctas, int* wgs) {
+    std::ifstream f(path);
+    if (!f) return false;
+    std::string line;
+    const std::string needle = "\"" + key + "\"";
+    while (std::getline(f, line)) {
+        const size_t pos = line.find(needle);
+        if (pos == std::string::npos) continue;
+        const size_t lb = line.find('[', pos);
+        if (lb == std::string::npos) continue;
+        if (std::sscanf(line.c_str() + lb, "[%d, %d]", ctas, wgs) == 2) return true;
+    }
+    return false;
+}
+
+void cache_store(const char* path, const std::string& key, int ctas, int wgs) {
+    std::vector<std::string> keep;
+    {
+        std::ifstream f(path);
+        std::string line;
+        const std::string needle = "\"" + key + "\"";
+        while (std::getline(f, line))
+            if (line.find("\": [") != std::string::npos && line.find(needle) == std::string::npos) {
+                while (!line.empty() && (line.back() == ',' || line.back() == ' ')) line.pop_back();
+                keep.push_back(line);
+            }
+    }
+    char buf[512];
+    std::snprintf(buf, sizeof(buf), "  \"%s\": [%d, %d]", key.c_str(), ctas, wgs);
+    keep.push_back(buf);
+    std::ofstream o(path, std::ios::trunc);
+    o << "{\n";
+    for (size_t i = 0; i < keep.size(); ++i) o << keep[i] << (i + 1 < keep.size() ? ",\n" : "\n");
+    o << "}\n";
+}
+
+}  // namespace
+
+int nrrs_autotune(nrrs_ctx* ctx, uint32_t n, const char* cache_path, char* report,
+                  size_t report_len) {
+    if (!ctx || n == 0 || n > ctx->cfg.max_queue) return NRRS_ERR_INVALID_ARG;
+    const nrrs_config& c = ctx->cfg;
+    const std::string key = tune_key(ctx);
+    std::ostringstream rep;
+    int ctas = 0, wgs = 1;
+    if (cache_path && cache_lookup(cache_path, key, &ctas, &wgs) &&
+        nrrs_set_launch_shape(ctx, ctas, wgs) == NRRS_OK) {
+        rep << "{\"key\": \"" << key << "\", \"cached\": [" << ctas << ", " << wgs << "]}";
+        if (report && report_len) std::snprintf(report, report_len, "%s", rep.str().c_str());
+        return NRRS_OK;
+    }
+    // synthetic inputs on the device (the tuner's own buffers)
+    std::vector<float> pos(3 * (size_t)n), wi(3 * (size_t)n), nrm(3 * (size_t)n), rough(n),
+        alb(3 * (size_t)n), thp(3 * (size_t)n), ref(n);
+    std::vector<uint32_t> dep(n);
+    nrrs_synth_vertices(12345, 0, n, pos.data(), wi.data(), nrm.data(), rough.data(), alb.data(),
+                        thp.data(), dep.data(), nullptr, ref.data(), nullptr);
+    float* d = nullptr;
+    const size_t floats = 3 * (size_t)n * 5 + 2 * (size_t)n + (size_t)n * 2;
+    if (cudaMalloc(&d, sizeof(float) * floats + sizeof(uint32_t) * n) != cudaSuccess)
+        return fail(ctx, NRRS_ERR_CUDA, "autotune allocation");
+    float* p = d;
+    auto put = [&](const void* h, size_t bytes) {
+        cudaMemcpy(p, h, bytes, cudaMemcpyHostToDevice);
+        float* r = p;
+        p += bytes / sizeof(float);
+        return r;
+    };
+    nrrs_vertex_soa v{};
+    v.pos = put(pos.data(), 12 * (size_t)n);
+    v.wi = put(wi.data(), 12 * (size_t)n);
+    v.normal = put(nrm.data(), 12 * (size_t)n);
+    v.albedo = put(alb.data(), 12 * (size_t)n);
+    v.thp = put(thp.data(), 12 * (size_t)n);
+    v.roughness = put(rough.data(), 4 * (size_t)n);
+    v.ref_mean = put(ref.data(), 4 * (size_t)n);
+    float* rrs = p;
+    p += n;
+    float* stats = p;
+    p += n;  // stats are not written (NULL below); scratch only
+    v.depth = reinterpret_cast<const uint32_t*>(put(dep.data(), 4 * (size_t)n));
+    (void)stats;
+    nrrs_decide_params dp;
+    nrrs_decide_params_default(&dp);
+    nrrs_segment sg{0, n, 0, 0, 0, 0};
+    const SegmentTable segs = make_segments(&sg, 1, kTile);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const bool fp32 = c.precision == NRRS_PREC_FP32;
+    const int saved_ctas = fp32 ? ctx->simt_ctas_per_sm : ctx->tc_ctas_per_sm;
+    const int saved_wgs = ctx->tc_wgs;
+    float best = 1e30f;
+    int best_ctas = saved_ctas, best_wgs = saved_wgs;
+    rep << "{\"key\": \"" << key << "\", \"n\": " << n << ", \"trials\": [";
+    bool first = true;
+    for (int w = 1; w <= (fp32 ? 1 : 2); ++w) {
+        const int maxc = infer_max_ctas(c.statnet_width, c.statnet_hidden, c.rrsnet_width,
+                                        c.rrsnet_hidden, c.precision, w);
+        for (int k = 1; k <= maxc; ++k) {
+            if (nrrs_set_launch_shape(ctx, k, w) != NRRS_OK) continue;
+            int rc = NRRS_OK;
+            for (int it = 0; it < 2 && rc == NRRS_OK; ++it)
+                rc = run_infer(ctx, &v, segs, &dp, n, nullptr, rrs, false, 0);
+            cudaEventRecord(e0, 0);
+            for (int it = 0; it < 5 && rc == NRRS_OK; ++it)
+                rc = run_infer(ctx, &v, segs, &dp, n, nullptr, rrs, false, 0);
+            cudaEventRecord(e1, 0);
+            if (rc != NRRS_OK || cudaEventSynchronize(e1) != cudaSuccess) continue;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms /= 5.f;
+            rep << (first ? "" : ", ") << "{\"ctas_per_sm\": " << k << ", \"warpgroups\": " << w
+                << ", \"ms\": " << ms << "}";
+            first = false;
+            if (ms < best) {
+                best = ms;
+                best_ctas = k;
+                best_wgs = w;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(d);
+    nrrs_set_launch_shape(ctx, best_ctas, best_wgs);
+    rep << "], \"best\": [" << best_ctas << ", " << best_wgs << "], \"best_ms\": " << best << "}";
+    if (cache_path) cache_store(cache_path, key, best_ctas, best_wgs);
+    if (report && report_len) std::snprintf(report, report_len, "%s", rep.str().c_str());
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? NRRS_OK : cuda_fail(ctx, e, "autotune");
+}
+
+struct nrrs_graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+int nrrs_graph_capture_batched(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* rnd,
+                               const nrrs_segment* segs, int32_t n_segs,
+                               const nrrs_decide_params* p, float* stats, float* rrs,
+                               float* rrs_norm, uint8_t* split, uint32_t* next_queue,
+                               uint32_t* next_size_dev, nrrs_graph** out) {
+    if (!ctx || !out) return NRRS_ERR_INVALID_ARG;
+    *out = nullptr;
+    cudaStream_t cs;
+    cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "capture stream");
+    const bool prof = ctx->prof.enabled;
+    ctx->prof.enabled = false;  // no event nodes in the graph
+    nrrs_graph* g = new nrrs_graph();
+    e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    int rc = NRRS_OK;
+    if (e == cudaSuccess) {
+        rc = nrrs_step_batched(ctx, v, rnd, segs, n_segs, p, stats, rrs, rrs_norm, split,
+                               next_queue, next_size_dev, cs);
+        const cudaError_t e2 = cudaStreamEndCapture(cs, &g->graph);
+        if (e2 != cudaSuccess && rc == NRRS_OK) rc = cuda_fail(ctx, e2, "end capture");
+    } else {
+        rc = cuda_fail(ctx, e, "begin capture");
+    }
+    ctx->prof.enabled = prof;
+    if (rc == NRRS_OK) {
+        e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "graph instantiate");
+    }
+    cudaStreamDestroy(cs);
+    if (rc != NRRS_OK) {
+        nrrs_graph_destroy(g);
+        return rc;
+    }
+    *out = g;
+    return NRRS_OK;
+}
+
+int nrrs_graph_launch(nrrs_graph* g, void* stream) {
+    if (!g || !g->exec) return NRRS_ERR_INVALID_ARG;
+    return cudaGraphLaunch(g->exec, (cudaStream_t)stream) == cudaSuccess ? NRRS_OK : NRRS_ERR_CUDA;
+}
+
+void nrrs_graph_destroy(nrrs_graph* g) {
+    if (!g) return;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
 }
 
 }  // extern "C"

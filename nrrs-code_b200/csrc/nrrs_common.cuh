@@ -190,6 +190,29 @@ __device__ __forceinline__ float corner_weight(const CellCoord& c, int k) {
     return wx * wy * wz;
 }
 
+// Features of one level from an FP16 table [rows][2] (half2 per row): trilinear over the 8
+// corners, summed in corner order 0..7. Eight independent 4-byte gathers (measured faster than
+// 16-byte loads that serve both x-adjacent corners of a cell when they share a block).
+__device__ __forceinline__ float2 level_features_h(const __half2* table, const LevelDev& L,
+                                                   uint32_t mask, const CellCoord& c) {
+    uint32_t rows[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        rows[k] = grid_row(L, mask, c.ix + (k & 1), c.iy + ((k >> 1) & 1), c.iz + ((k >> 2) & 1));
+    __half2 t[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) t[k] = __ldg(table + rows[k]);
+    float f0 = 0.f, f1 = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const float w = corner_weight(c, k);
+        const float2 tv = __half22float2(t[k]);
+        f0 += w * tv.x;
+        f1 += w * tv.y;
+    }
+    return make_float2(f0, f1);
+}
+
 // Misc StatNet lanes [48, 64): normal, albedo, warped roughness, bias 1, zeros
 __device__ __forceinline__ void misc_lanes(const VertexPtrs& v, uint32_t i, float* o /*16*/) {
     const size_t i3 = 3 * (size_t)i;

@@ -134,6 +134,16 @@ _SIGS = {
     "nrrs_copy_grads": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "nrrs_adam_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_void_p]),
     "nrrs_launch_count": (C.c_uint64, [C.c_void_p]),
+    "nrrs_autotune": (C.c_int, [C.c_void_p, C.c_uint32, C.c_char_p, C.c_char_p, C.c_size_t]),
+    "nrrs_set_launch_shape": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+    "nrrs_get_launch_shape": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "nrrs_graph_capture_batched": (C.c_int, [C.c_void_p, C.POINTER(VertexSoA), C.c_void_p,
+                                             C.POINTER(Segment), C.c_int32,
+                                             C.POINTER(DecideParams), C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.POINTER(C.c_void_p)]),
+    "nrrs_graph_launch": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "nrrs_graph_destroy": (None, [C.c_void_p]),
     "nrrs_last_infer_grid": (C.c_int32, [C.c_void_p]),
     "nrrs_kernel_name": (C.c_char_p, [C.c_int32]),
     "nrrs_profile_enable": (C.c_int, [C.c_void_p, C.c_int32]),
@@ -234,6 +244,29 @@ def decide_emit_noalloc(rrs, rnd, n, budget, n_specular, params, rrs_norm, split
 
 
 VERTEX_FIELDS = ("pos", "wi", "normal", "roughness", "albedo", "thp", "depth", "ref_mean")
+
+
+class BatchedGraph:
+    """An instantiated CUDA graph of nrrs_step_batched (nrrs_graph_*)."""
+
+    def __init__(self, handle):
+        self._g = handle
+
+    def launch(self, stream=0):
+        rc = lib().nrrs_graph_launch(self._g, stream)
+        if rc != OK:
+            raise NRRSError(rc, "graph launch failed")
+
+    def close(self):
+        if getattr(self, "_g", None):
+            lib().nrrs_graph_destroy(self._g)
+            self._g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class NRRSNetwork:
@@ -380,6 +413,30 @@ class NRRSNetwork:
         a = np.zeros((self.config.n_levels, 4), np.uint32)
         self._check(lib().nrrs_level_table(self._h, a.ctypes.data, self.config.n_levels))
         return a
+
+    # ---- launch shape, autotuning and graphs ----
+    def autotune(self, n: int, cache_path=None) -> str:
+        buf = C.create_string_buffer(8192)
+        self._check(lib().nrrs_autotune(self._h, n, str(cache_path).encode() if cache_path else None,
+                                        buf, len(buf)))
+        return buf.value.decode()
+
+    def set_launch_shape(self, ctas_per_sm: int, warpgroups: int = 1):
+        self._check(lib().nrrs_set_launch_shape(self._h, ctas_per_sm, warpgroups))
+
+    def launch_shape(self) -> tuple[int, int]:
+        c, w = C.c_int32(), C.c_int32()
+        self._check(lib().nrrs_get_launch_shape(self._h, C.byref(c), C.byref(w)))
+        return int(c.value), int(w.value)
+
+    def captureBatched(self, soa, rnd, segments, params, stats, rrs, rrs_norm, split, queue,
+                       next_size) -> "BatchedGraph":
+        arr = (Segment * len(segments))(*segments)
+        g = C.c_void_p()
+        self._check(lib().nrrs_graph_capture_batched(
+            self._h, C.byref(soa), _ptr(rnd), arr, len(segments), C.byref(params), _ptr(stats),
+            _ptr(rrs), _ptr(rrs_norm), _ptr(split), _ptr(queue), _ptr(next_size), C.byref(g)))
+        return BatchedGraph(g)
 
     def last_infer_grid(self) -> int:
         return int(lib().nrrs_last_infer_grid(self._h))

@@ -1,0 +1,89 @@
+"""GPU tests of the launch-shape autotuner and of the CUDA graph of the batched step: every
+launch shape gives bit-identical outputs, the tuner's cache is reused, and one graph launch of
+the uneven multi-depth step equals the direct batched call."""
+from __future__ import annotations
+
+import json
+
+import numpy as np
+import pytest
+
+import nrrs_b200 as nb
+from gpu_util import empty, host, make_net, random_params, soa, stream, torch_cuda, upload
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("prec", [nb.PREC_FP16, nb.PREC_FP32], ids=["fp16", "fp32"])
+def test_launch_shapes_give_identical_outputs(prec):
+    torch = torch_cuda()
+    net = make_net(precision=prec)
+    random_params(net, 50, table_scale=0.5, mlp_scale=0.15)
+    n = 150_001
+    v = nb.synth(51, n)
+    d = upload(v)
+    dp = nb.default_decide()
+    shapes = [(1, 1), (2, 1), (0, 1)] + ([(1, 2), (0, 2)] if prec != nb.PREC_FP32 else [])
+    ref = None
+    for c, w in shapes:
+        net.set_launch_shape(c, w)
+        st, rr = empty(3 * n), empty(n)
+        net.inference(soa(d), n, dp, st, rr, stream())
+        torch.cuda.synchronize()
+        out = (host(st)[:3 * n].copy(), host(rr)[:n].copy())
+        if ref is None:
+            ref = out
+        else:
+            assert np.array_equal(out[0].view(np.uint32), ref[0].view(np.uint32)), (c, w)
+            assert np.array_equal(out[1].view(np.uint32), ref[1].view(np.uint32)), (c, w)
+    net.close()
+
+
+def test_autotune_picks_and_caches(tmp_path):
+    net = make_net(precision=nb.PREC_FP16)
+    cache = tmp_path / "tune.json"
+    rep = json.loads(net.autotune(262144, cache))
+    assert rep["trials"] and tuple(rep["best"]) == net.launch_shape()
+    assert min(t["ms"] for t in rep["trials"]) == pytest.approx(rep["best_ms"])
+    other = make_net(precision=nb.PREC_FP16)
+    rep2 = json.loads(other.autotune(262144, cache))
+    assert tuple(rep2["cached"]) == tuple(rep["best"]) == other.launch_shape()
+    json.loads(cache.read_text())
+    net.close()
+    other.close()
+
+
+def test_graph_of_batched_step_equals_direct_call():
+    torch = torch_cuda()
+    net = make_net(precision=nb.PREC_FP16)
+    random_params(net, 52, table_scale=0.5, mlp_scale=0.15)
+    counts = [int(round(300_000 * 0.6 ** k)) for k in range(10)]
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    N = int(offs[-1])
+    v = nb.synth(53, N)
+    d = upload(v)
+    dp = nb.default_decide()
+    caps = [9 * c for c in counts]
+    qoffs = np.concatenate([[0], np.cumsum(caps)]).astype(np.int64)
+    segs = [nb.Segment(int(offs[k]), counts[k], counts[k], 0, int(qoffs[k]), caps[k])
+            for k in range(len(counts))]
+
+    def bufs():
+        return dict(st=empty(3 * N), rrs=empty(N), norm=empty(N), split=empty(N, "uint8"),
+                    q=empty(int(qoffs[-1]), "int32"), sz=empty(len(counts), "int32"))
+
+    a, b = bufs(), bufs()
+    net.generateRRSNumberBatched(soa(d), d["rnd"], segs, dp, a["st"], a["rrs"], a["norm"],
+                                 a["split"], a["q"], a["sz"], stream())
+    g = net.captureBatched(soa(d), d["rnd"], segs, dp, b["st"], b["rrs"], b["norm"], b["split"],
+                           b["q"], b["sz"])
+    for _ in range(2):          # replays reuse the self-resetting scratch
+        b["sz"].zero_()
+        g.launch(stream())
+        torch.cuda.synchronize()
+        for k in a:
+            assert torch.equal(a[k], b[k]), k
+    g.close()
+    rc, flags = net.device_status(stream())
+    assert rc == nb.OK and flags == 0
+    net.close()
