@@ -110,7 +110,8 @@ __device__ __forceinline__ bool tc_layer(const uint8_t* sA, const uint8_t* sWl, 
 }
 
 template <int WS, int HS, int WR, int HR, bool BF, int WGS>
-__global__ void __launch_bounds__(128 * WGS, WGS == 2 ? 3 : 1) k_infer_tc(const __grid_constant__ InferArgs a) {
+__global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
+    k_infer_tc(const __grid_constant__ InferArgs a) {
     using S = TcShape<WS, HS, WR, HR, WGS>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* base = reinterpret_cast<uint8_t*>(
