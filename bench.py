@@ -1,18 +1,28 @@
 """Benchmark of the NRRS per-vertex step on B200 (one JSON line on rank 0).
 
-Workload (default "frame1080p"): one frame at 1920x1080 with 6 bounces. Each bounce runs
-inference, the RRS decision and emission on 2,073,600 synthetic path vertices. The frame then
-runs one training step on 262,144 samples. Mixed precision: FP16 table, FP16 tcgen05 MLPs with
-FP32 accumulation, exact 64-bit normalisation sums. Inputs are seeded synthetic records with
-the workload's distributions; each bounce has its own 158 MB vertex buffer, so inputs are
-larger than L2.
+Default workload "frame1080p": one frame at 1920x1080 with 6 bounces. Each bounce runs
+inference, the RRS decision and emission on 2,073,600 synthetic path vertices; the frame then
+runs one training step on 262,144 samples. Mixed precision: FP16 table, FP16 tcgen05 MLPs for
+inference (FP16 StatNet / BF16 RRSNet in training) with FP32 accumulation, FP32 master weights
+and Adam state, exact 64-bit normalisation sums. Inputs are seeded synthetic records with the
+workload's distributions; each bounce has its own 158 MB vertex buffer, so inputs are larger
+than L2.
+
+Other workloads (--workload):
+  batched   depths 0..9 with round(2,073,600 x 0.6^d) vertices each, 10 % of them split into
+            U{1..4} copies, concatenated in one SoA; after autotuning the launch shape the
+            whole multi-depth step is ONE CUDA-graph launch, timed beside launching each depth
+            separately on the same vertices (and checked to decide identically)
+  frame4k   3840x2160: 8,294,400 vertices per bounce, 10 bounces, MLPs 128 wide x 3 hidden
+            layers (BF16 by default), 2^22-entry table, 10 training steps of 262,144 samples
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--precision fp16|bf16|fp32] [--no-train]
+                  [--workload frame1080p|batched|frame4k] [--precision fp16|bf16|fp32]
+                  [--no-train]
 
-value    = vertices/s of the whole job (device-timed frames, max over ranks)
+value    = vertices/s of the whole job (device-timed steps, max over ranks)
 e2e      = the same metric through the C-ABI with host (pinned) inputs: the H2D copy of each
-           bounce's vertices and training batch and the D2H read of queue sizes and losses are
+           step's vertices and training batch and the D2H read of queue sizes and losses are
            inside the timed region
 roofline = dominant kernel (inference) achieved algorithmic GB/s vs the measured HBM peak
 --impl reference times the reference's CPU path (the oracle port of it, all host threads)
@@ -35,13 +45,20 @@ import numpy as np  # noqa: E402
 
 import nrrs_b200 as nb  # noqa: E402
 
-N_VERT = 2_073_600
-BOUNCES = 6
-TRAIN_BATCH = 262_144
 SOA_BYTES = 72            # pos, wi, normal, roughness, albedo, thp, depth, ref_mean
 RND_BYTES = 4
 TARGET_BYTES = 12
 METRIC = "RRS vertices/s and train samples/s, mixed-prec vs FP32 plain at stated error"
+FIELDS = ("pos", "wi", "normal", "roughness", "albedo", "thp", "depth", "ref_mean", "rnd")
+
+WORKLOADS = {
+    "frame1080p": dict(bounces=6, n_vert=2_073_600, train_steps=1, train_batch=262_144,
+                       width=64, hidden=2, log2_table=19, steps=50, precision="fp16"),
+    "batched": dict(bounces=10, n_vert=2_073_600, train_steps=0, train_batch=262_144,
+                    width=64, hidden=2, log2_table=19, steps=50, precision="fp16"),
+    "frame4k": dict(bounces=10, n_vert=8_294_400, train_steps=10, train_batch=262_144,
+                    width=128, hidden=3, log2_table=22, steps=5, precision="bf16"),
+}
 
 
 def env_int(k, d):
@@ -70,7 +87,7 @@ def traffic_per_vertex(kernel: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 100 ms during the timed region."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -79,6 +96,7 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.p = None
+        self.lines = []
 
     def __enter__(self):
         try:
@@ -91,7 +109,6 @@ class ClockSampler:
         return self
 
     def __exit__(self, *exc):
-        self.lines = []
         if self.p:
             self.p.terminate()
             try:
@@ -122,72 +139,90 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def make_config(precision: str, max_queue: int, max_train: int):
+def make_config(precision: str, wl: dict, max_queue: int, max_train: int):
     prec = {"fp16": nb.PREC_FP16, "bf16": nb.PREC_BF16, "fp32": nb.PREC_FP32}[precision]
-    return nb.default_config(precision=prec, max_queue=max_queue, max_train=max_train)
+    return nb.default_config(precision=prec, max_queue=max_queue, max_train=max_train,
+                             statnet_width=wl["width"], statnet_hidden=wl["hidden"],
+                             rrsnet_width=wl["width"], rrsnet_hidden=wl["hidden"],
+                             log2_hashmap_size=wl["log2_table"])
 
 
-def cpu_sample(precision_cfg, n_sample: int, seconds: float, train_n: int, do_train: bool):
-    """Oracle FP32 (OpenMP, all host threads) on a bounded sample of the frame workload;
-    returns frame-equivalent vertices/s and the sample description."""
+def do_train_of(args, wl):
+    return not args.no_train and wl["train_steps"] > 0
+
+
+def workload_name(args):
+    wl = WORKLOADS[args.workload]
+    if args.workload == "frame1080p" and wl["bounces"] == 6 and wl["n_vert"] == 2_073_600:
+        name = "frame1080p_6bounce_infer_decide_emit"
+    else:
+        name = (f"{args.workload}_{wl['bounces']}x{wl['n_vert']}_w{wl['width']}h{wl['hidden']}"
+                f"_infer_decide_emit")
+    if do_train_of(args, wl):
+        name += ("_train262144" if wl["train_steps"] == 1 else
+                 f"_train{wl['train_steps']}x{wl['train_batch']}")
+    return f"{name}_{args.precision}"
+
+
+def cpu_sample(cfg, wl, n_sample: int, seconds: float, train_n: int, do_train: bool):
+    """Oracle FP32 (OpenMP, all host threads) on a bounded sample of the workload; returns the
+    step-equivalent vertices/s, the cores used, a description of the sample and the step time."""
     sys.path.insert(0, str(REPO / "oracle"))
     import oracle as O
     O.set_threads(os.cpu_count() or 1)
     cores = O.threads()
-    net_cfg = precision_cfg
     v = nb.synth(7, n_sample)
-    params = None
-    # parameters: the library's initialisation is reproduced from the seed by the oracle's
-    # caller; for throughput only the shapes matter, so use small random weights
-    npar = O.param_count(net_cfg)[0]
+    npar = O.param_count(cfg)[0]
     params = (np.random.default_rng(0).uniform(-1, 1, npar) * 0.1).astype(np.float32)
     dp = nb.default_decide()
     t_inf, reps = 0.0, 0
     t0 = time.perf_counter()
     while True:
         a = time.perf_counter()
-        r = O.infer(net_cfg, params, v, dp, "f32", want=("stats", "rrs"))
+        r = O.infer(cfg, params, v, dp, "f32", want=("stats", "rrs"))
         O.decide_emit(r["rrs"].astype(np.float32), v["rnd"], n_sample, 0, dp)
         t_inf += time.perf_counter() - a
         reps += 1
         if time.perf_counter() - t0 > seconds * (0.6 if do_train else 1.0):
             break
     per_vertex = t_inf / (reps * n_sample)
-    t_train = 0.0
+    per_sample, treps = 0.0, 0
     if do_train:
         tv = nb.synth(8, train_n)
-        treps = 0
+        t_train = 0.0
         t1 = time.perf_counter()
         while True:
             a = time.perf_counter()
-            g, loss = O.train_grads(net_cfg, params, tv, tv["target"], "f32")
+            O.train_grads(cfg, params, tv, tv["target"], "f32")
             t_train += time.perf_counter() - a
             treps += 1
             if time.perf_counter() - t1 > seconds * 0.4:
                 break
         per_sample = t_train / (treps * train_n)
-    else:
-        per_sample = 0.0
-    frame_s = BOUNCES * N_VERT * per_vertex + (TRAIN_BATCH * per_sample if do_train else 0.0)
+    verts = wl["bounces"] * wl["n_vert"]
+    step_s = verts * per_vertex + wl["train_steps"] * wl["train_batch"] * per_sample
     sample = (f"{reps} x infer+decide on {n_sample} vertices"
               + (f", {treps} x train grads on {train_n} samples" if do_train else "")
-              + "; frame time extrapolated from per-vertex and per-sample costs")
-    return BOUNCES * N_VERT / frame_s, cores, sample, frame_s
+              + "; step time extrapolated from per-vertex and per-sample costs")
+    return verts / step_s, cores, sample, step_s
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
-    cfg = make_config("fp32", 1 << 21, 1 << 16)
-    value, cores, sample, frame_s = cpu_sample(cfg, 131072, 10.0 * max(1, args.steps) / 10, 8192,
-                                               not args.no_train)
+    wl = WORKLOADS[args.workload]
+    do_train = do_train_of(args, wl)
+    cfg = make_config("fp32", wl, 1 << 21, 1 << 16)
+    value, cores, sample, step_s = cpu_sample(cfg, wl, 131072, 10.0 * max(1, args.steps) / 10,
+                                              8192, do_train)
     line = {
         "metric": METRIC, "value": value, "unit": "vertices/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": frame_s * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic", "impl": "reference",
-        "config": {"workload": workload_name(args), "bounces": BOUNCES,
-                   "vertices_per_bounce": N_VERT, "train_batch": TRAIN_BATCH if not args.no_train else 0},
+        "config": {"workload": workload_name(args), "bounces": wl["bounces"],
+                   "vertices_per_bounce": wl["n_vert"],
+                   "train_batch": wl["train_batch"] if do_train else 0},
         "cpu_baseline": {"value": value, "unit": "vertices/s", "cores": cores, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": "vertices/s", "h2d_bytes_per_step": 0,
@@ -199,9 +234,40 @@ def run_reference(args, rank, world):
     return 0
 
 
-def workload_name(args):
-    return (f"frame1080p_{BOUNCES}bounce_infer_decide_emit"
-            + ("" if args.no_train else "_train262144") + f"_{args.precision}")
+def pinned(torch, v: dict, keys):
+    return {k: torch.from_numpy(v[k].view(np.int32) if v[k].dtype == np.uint32 else v[k]).pin_memory()
+            for k in keys}
+
+
+def soa_of(b):
+    return nb.vertex_soa(b["pos"], b["wi"], b["normal"], b["roughness"], b["albedo"], b["thp"],
+                         b["depth"], b["ref_mean"])
+
+
+def step_outputs(torch, dev, n, cap, n_sizes=1):
+    return dict(stats=torch.empty(3 * n, device=dev), rrs=torch.empty(n, device=dev),
+                norm=torch.empty(n, device=dev),
+                split=torch.empty(n, dtype=torch.uint8, device=dev),
+                q=torch.empty(cap, dtype=torch.int32, device=dev),
+                sz=torch.zeros(n_sizes, dtype=torch.int32, device=dev))
+
+
+def batched_vertices(n_top, depths, seed):
+    """Depth d holds round(n_top x 0.6^d) path vertices; 10 % of them are split into U{1..4}
+    copies (a split vertex re-enters the next queue several times). Returns the concatenated
+    records and the per-depth counts."""
+    rng = np.random.default_rng(seed)
+    counts, parts = [], []
+    for d in range(depths):
+        base = int(round(n_top * 0.6 ** d))
+        v = nb.synth(seed * 131 + d, base)
+        mult = np.where(rng.random(base) < 0.1, rng.integers(1, 5, base), 1)
+        idx = np.repeat(np.arange(base), mult)
+        sub = {k: np.ascontiguousarray(a[idx]) for k, a in v.items() if k in FIELDS}
+        sub["depth"] = np.full(idx.size, d, np.uint32)
+        counts.append(int(idx.size))
+        parts.append(sub)
+    return {k: np.concatenate([p[k] for p in parts]) for k in FIELDS}, counts
 
 
 def run_ours(args, rank, world, local_rank):
@@ -214,66 +280,120 @@ def run_ours(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local_rank)
     stream = torch.cuda.current_stream().cuda_stream
-    do_train = not args.no_train
-    net = nb.NRRSNetwork(make_config(args.precision, N_VERT, TRAIN_BATCH))
+    wl = WORKLOADS[args.workload]
+    B, N = wl["bounces"], wl["n_vert"]
+    do_train = do_train_of(args, wl)
+    batched = args.workload == "batched"
     dp = nb.default_decide()
-    cap = 9 * N_VERT
 
-    # ---- synthetic inputs: one buffer set per bounce (pinned host + device) ----
-    fields = ("pos", "wi", "normal", "roughness", "albedo", "thp", "depth", "ref_mean", "rnd")
-    host_b, dev_b = [], []
-    for d in range(BOUNCES):
-        v = nb.synth(1000 + 97 * rank + d, N_VERT)
-        v["depth"] = np.full(N_VERT, d, np.uint32)
-        hb = {k: torch.from_numpy(v[k].view(np.int32) if v[k].dtype == np.uint32 else v[k]).pin_memory()
-              for k in fields}
-        host_b.append(hb)
-        dev_b.append({k: t.to(dev) for k, t in hb.items()})
-    tv = nb.synth(5000 + rank, TRAIN_BATCH)
-    th = {k: torch.from_numpy(tv[k].view(np.int32) if tv[k].dtype == np.uint32 else tv[k]).pin_memory()
-          for k in fields + ("target",)}
-    td = {k: t.to(dev) for k, t in th.items()}
-    outs = [dict(stats=torch.empty(3 * N_VERT, device=dev), rrs=torch.empty(N_VERT, device=dev),
-                 norm=torch.empty(N_VERT, device=dev),
-                 split=torch.empty(N_VERT, dtype=torch.uint8, device=dev),
-                 q=torch.empty(cap, dtype=torch.int32, device=dev),
-                 sz=torch.zeros(1, dtype=torch.int32, device=dev)) for _ in range(BOUNCES)]
+    # ---- synthetic inputs: pinned host copies and device copies ----
+    if batched:
+        cat, counts = batched_vertices(N, B, 2024 + rank)
+        host_b = [pinned(torch, cat, FIELDS)]
+        total = int(sum(counts))
+    else:
+        host_b = []
+        for d in range(B):
+            v = nb.synth(1000 + 97 * rank + d, N)
+            v["depth"] = np.full(N, d, np.uint32)
+            host_b.append(pinned(torch, v, FIELDS))
+        total = B * N
+    dev_b = [{k: t.to(dev) for k, t in hb.items()} for hb in host_b]
+    max_q = total if batched else N
+    net = nb.NRRSNetwork(make_config(args.precision, wl, max_q, wl["train_batch"]))
+    tune = None
+    if args.launch_shape:
+        net.set_launch_shape(*[int(x) for x in args.launch_shape.split(",")])
+    elif args.workload != "frame1080p":
+        # the library's launch-shape tuner (CTAs per SM x warpgroups per CTA), on this shape
+        tune = json.loads(net.autotune(min(max_q, N)))
+    th = td = None
+    if do_train:
+        tv = nb.synth(5000 + rank, wl["train_batch"])
+        th = pinned(torch, tv, FIELDS + ("target",))
+        td = {k: t.to(dev) for k, t in th.items()}
     loss = torch.zeros(2, dtype=torch.float64, device=dev)
 
-    def soa_of(b):
-        return nb.vertex_soa(b["pos"], b["wi"], b["normal"], b["roughness"], b["albedo"],
-                             b["thp"], b["depth"], b["ref_mean"])
+    graph = None
+    if batched:
+        caps = [9 * c for c in counts]
+        offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        qoffs = np.concatenate([[0], np.cumsum(caps)]).astype(np.int64)
+        segs = [nb.Segment(int(offs[k]), counts[k], N, 0, int(qoffs[k]), caps[k]) for k in range(B)]
+        ob = step_outputs(torch, dev, total, int(qoffs[-1]), B)
+        soa = soa_of(dev_b[0])
+        l0 = net.launch_count()
+        graph = net.captureBatched(soa, dev_b[0]["rnd"], segs, dp, ob["stats"], ob["rrs"],
+                                   ob["norm"], ob["split"], ob["q"], ob["sz"])
+        kernels_per_graph = net.launch_count() - l0
+        # per-depth comparison: one step per depth, separate launches, the same vertices
+        per = []
+        for k in range(B):
+            sub = {f: t[int(offs[k]):int(offs[k + 1])] for f, t in dev_b[0].items()}
+            per.append((sub, soa_of(sub), step_outputs(torch, dev, counts[k], caps[k])))
 
-    soas = [soa_of(b) for b in dev_b]
-    tsoa = soa_of(td)
+        def step():
+            graph.launch(stream)
 
-    sharded = None
-    if world > 1:
-        # each rank holds one 1080p-sized shard of an N-times larger queue: one integer
-        # all-reduce of the exact sum per bounce, data-parallel gradients per train step
-        from nrrs_parallel import ShardedNRRS
-        sharded = ShardedNRRS(net)
-        acc = torch.zeros(1, dtype=torch.int64, device=dev)
-        grads_buf = torch.zeros(net.param_count(), dtype=torch.float32, device=dev)
+        def step_per_depth():
+            for k, (sub, s, p) in enumerate(per):
+                net.generateRRSNumber(s, sub["rnd"], counts[k], N, 0, dp, p["stats"], p["rrs"],
+                                      p["norm"], p["split"], p["q"], caps[k], p["sz"], stream)
+    else:
+        cap = 9 * N
+        outs = [step_outputs(torch, dev, N, cap) for _ in range(B)]
+        soas = [soa_of(b) for b in dev_b]
+        tsoa = soa_of(td) if do_train else None
+        sharded = None
+        if world > 1:
+            # each rank holds one shard of an N-times larger queue: one integer all-reduce of
+            # the exact sum per bounce, data-parallel gradients per train step
+            from nrrs_parallel import ShardedNRRS
+            sharded = ShardedNRRS(net)
+            acc = torch.zeros(1, dtype=torch.int64, device=dev)
+            grads_buf = torch.zeros(net.param_count(), dtype=torch.float32, device=dev)
 
-    def frame():
-        for d in range(BOUNCES):
-            o = outs[d]
-            if sharded is None:
-                net.generateRRSNumber(soas[d], dev_b[d]["rnd"], N_VERT, N_VERT, 0, dp, o["stats"],
-                                      o["rrs"], o["norm"], o["split"], o["q"], cap, o["sz"], stream)
-            else:
-                sharded.step(soas[d], dev_b[d]["rnd"], N_VERT, N_VERT * world, 0, dp, o["stats"],
-                             o["rrs"], o["norm"], o["split"], o["q"], cap, o["sz"], acc, stream)
-        if do_train:
-            if sharded is None:
-                net.train(tsoa, td["target"], TRAIN_BATCH, loss, stream)
-            else:
-                sharded.train_step(tsoa, td["target"], TRAIN_BATCH, grads_buf, loss, stream)
+        def step():
+            for d in range(B):
+                o = outs[d]
+                if sharded is None:
+                    net.generateRRSNumber(soas[d], dev_b[d]["rnd"], N, N, 0, dp, o["stats"],
+                                          o["rrs"], o["norm"], o["split"], o["q"], cap, o["sz"],
+                                          stream)
+                else:
+                    sharded.step(soas[d], dev_b[d]["rnd"], N, N * world, 0, dp, o["stats"],
+                                 o["rrs"], o["norm"], o["split"], o["q"], cap, o["sz"], acc,
+                                 stream)
+            for _ in range(wl["train_steps"] if do_train else 0):
+                if sharded is None:
+                    net.train(tsoa, td["target"], wl["train_batch"], loss, stream)
+                else:
+                    sharded.train_step(tsoa, td["target"], wl["train_batch"], grads_buf, loss,
+                                       stream)
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
 
     # ---- device-timed region ----
     for _ in range(args.warmup):
-        frame()
+        step()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -285,62 +405,74 @@ def run_ours(args, rank, world, local_rank):
     with ClockSampler(local_rank) as clk:
         e0.record()
         for _ in range(args.steps):
-            frame()
+            step()
         e1.record()
         torch.cuda.synchronize()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    launches = net.launch_count() - launches0
+    # a graph replay does not pass through the library, which counted the graph's kernels
+    # when it captured them
+    launches = (kernels_per_graph * args.steps) if batched else net.launch_count() - launches0
     prof = net.profile_read()
-    net.profile(False)
     if dist:
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     ms_step = ms / args.steps
-    verts = BOUNCES * N_VERT * world
+    verts = total * world
     value = verts / (ms_step * 1e-3)
+
+    extra = {}
+    inf_vertices = total * args.steps
+    if batched:
+        # per-depth launches (profiled: the graph's kernels carry no per-kernel events)
+        ms_pd = timed(step_per_depth, args.steps, 2) / args.steps
+        prof = net.profile_read()
+        n_inf_pd = prof.get("infer_tc", prof.get("infer_fp32", (0, 0.0)))[0]
+        inf_vertices = total * (n_inf_pd // B)
+        same = True
+        for k, (sub, s, p) in enumerate(per):
+            a0, a1 = int(offs[k]), int(offs[k + 1])
+            same &= bool(torch.equal(p["split"], ob["split"][a0:a1]))
+            same &= bool(torch.equal(p["rrs"], ob["rrs"][a0:a1]))
+            # batched queues hold indices into the concatenated SoA
+            same &= bool(torch.equal(p["q"][:int(p["sz"].item())] + int(offs[k]),
+                                     ob["q"][int(qoffs[k]):int(qoffs[k]) + int(ob["sz"][k].item())]))
+        extra = {"batched": {"graph_ms_per_step": ms_step, "per_depth_ms_per_step": ms_pd,
+                             "speedup_graph_vs_per_depth": ms_pd / ms_step,
+                             "decisions_equal_per_depth": same, "kernels_per_graph": kernels_per_graph,
+                             "vertices_per_depth": counts}}
+    net.profile(False)
     rc, flags = net.device_status(stream)
 
     # ---- end to end through the C-ABI with host buffers ----
-    h2d = BOUNCES * N_VERT * (SOA_BYTES + RND_BYTES) + (
-        TRAIN_BATCH * (SOA_BYTES + RND_BYTES + TARGET_BYTES) if do_train else 0)
-    d2h = BOUNCES * 4 + (16 if do_train else 0)
-    sizes_h = torch.zeros(BOUNCES, dtype=torch.int32).pin_memory()
+    # the training batch is copied once per step and reused by each of its train steps
+    h2d = total * (SOA_BYTES + RND_BYTES) + (
+        wl["train_batch"] * (SOA_BYTES + RND_BYTES + TARGET_BYTES) if do_train else 0)
+    d2h = B * 4 + (16 if do_train else 0)
+    sizes_h = torch.zeros(B, dtype=torch.int32).pin_memory()
     loss_h = torch.zeros(2, dtype=torch.float64).pin_memory()
 
-    def frame_e2e():
-        for d in range(BOUNCES):
-            for k in fields:
-                dev_b[d][k].copy_(host_b[d][k], non_blocking=True)
+    def step_e2e():
+        for hb, db in zip(host_b, dev_b):
+            for k in FIELDS:
+                db[k].copy_(hb[k], non_blocking=True)
         if do_train:
-            for k in fields + ("target",):
+            for k in FIELDS + ("target",):
                 td[k].copy_(th[k], non_blocking=True)
-        frame()
-        for d in range(BOUNCES):
-            sizes_h[d:d + 1].copy_(outs[d]["sz"], non_blocking=True)
+        step()
+        if batched:
+            sizes_h.copy_(ob["sz"], non_blocking=True)
+        else:
+            for d in range(B):
+                sizes_h[d:d + 1].copy_(outs[d]["sz"], non_blocking=True)
         if do_train:
             loss_h.copy_(loss, non_blocking=True)
 
-    for _ in range(min(2, args.warmup)):
-        frame_e2e()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
     e2 = max(2, args.steps // 2)
-    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a0.record()
-    for _ in range(e2):
-        frame_e2e()
-    a1.record()
-    torch.cuda.synchronize()
-    e2e_ms = a0.elapsed_time(a1) / e2
-    if dist:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = timed(step_e2e, e2, min(2, args.warmup)) / e2
 
     # ---- roofline of the dominant kernel ----
     kind = "infer_fp32" if args.precision == "fp32" else "infer_tc"
@@ -351,14 +483,17 @@ def run_ours(args, rank, world, local_rank):
     roof = None
     if n_inf:
         launch_ms = ms_inf / n_inf
-        achieved = b_vertex * N_VERT / (launch_ms * 1e-3) / 1e9
-        tpv = traffic_per_vertex(kind)
+        per_launch = inf_vertices / n_inf
+        achieved = b_vertex * per_launch / (launch_ms * 1e-3) / 1e9
+        tpv = traffic_per_vertex(kind) if args.workload == "frame1080p" else None
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": (tpv * N_VERT) if tpv else None, "kernel": kind,
-                "algorithmic_bytes_per_vertex": b_vertex, "launch_ms": launch_ms,
-                "note": "algorithmic bytes count 4 B (FP16) per hash-corner gather; the table is "
-                        "L2-resident, so the limiter is L2 sector throughput, see profiles/"}
+                "traffic": (tpv * per_launch) if tpv else None, "kernel": kind,
+                "algorithmic_bytes_per_vertex": b_vertex, "vertices_per_launch": per_launch,
+                "launch_ms": launch_ms,
+                "note": "algorithmic bytes count the 128 hash-corner gathers at table precision; "
+                        "with a table that fits in L2 the limiter is L1/L2 gather throughput, "
+                        "see profiles/"}
     kernels = {k: {"launches": n, "ms_total": t, "ms_per_launch": t / n} for k, (n, t) in prof.items()}
 
     line = {
@@ -367,11 +502,16 @@ def run_ours(args, rank, world, local_rank):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": {"fp16": "f16", "bf16": "bf16", "fp32": "f32"}[args.precision],
         "data": "synthetic",
-        "config": {"workload": workload_name(args), "bounces": BOUNCES,
-                   "vertices_per_bounce": N_VERT, "train_batch": TRAIN_BATCH if do_train else 0,
-                   "encoding": "hashgrid L16 F2 T2^19 Nmin16 b1.5 + SH deg4",
-                   "mlp": "StatNet 64->64x2->3, RRSNet 16->64x2->1",
-                   "l2": "inputs larger than L2 (one 158 MB vertex buffer per bounce)",
+        "config": {"workload": workload_name(args), "bounces": B, "vertices_per_bounce": N,
+                   "vertices_per_step": total,
+                   "train_steps": wl["train_steps"] if do_train else 0,
+                   "train_batch": wl["train_batch"] if do_train else 0,
+                   "encoding": f"hashgrid L16 F2 T2^{wl['log2_table']} Nmin16 b1.5 + SH deg4",
+                   "mlp": f"StatNet 64->{wl['width']}x{wl['hidden']}->3, "
+                          f"RRSNet 16->{wl['width']}x{wl['hidden']}->1",
+                   "l2": "inputs larger than L2 (one vertex buffer per bounce, >=158 MB)"
+                         if not batched else "inputs larger than L2 (one 450 MB SoA of all depths)",
+                   "launch_shape": list(net.launch_shape()),
                    "parallelism": f"dp{world}"},
         "clocks": clk.summary(),
         "e2e": {"value": verts / (e2e_ms * 1e-3), "unit": "vertices/s", "ms_per_step": e2e_ms,
@@ -382,17 +522,24 @@ def run_ours(args, rank, world, local_rank):
         "device_status": [rc, flags],
         "infer_grid": net.last_infer_grid(),
     }
+    if tune:
+        line["autotune"] = {"best": tune.get("best") or tune.get("cached"),
+                            "trials": tune.get("trials")}
+    line.update(extra)
     if do_train and "train_statnet" in prof:
         t_train = sum(t for k, (n, t) in prof.items() if k.startswith("train") or k == "adam"
                       or k in ("pack_weights", "table_half"))
-        line["train_samples_per_s"] = TRAIN_BATCH * args.steps / (t_train * 1e-3)
+        line["train_samples_per_s"] = (wl["train_steps"] * wl["train_batch"] * args.steps
+                                       / (t_train * 1e-3))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        value_c, cores, sample, _ = cpu_sample(make_config("fp32", 1 << 21, 1 << 16), 131072,
-                                               12.0, 8192, do_train)
+        value_c, cores, sample, _ = cpu_sample(make_config("fp32", wl, 1 << 21, 1 << 16), wl,
+                                               131072, 12.0, 8192, do_train)
         line["cpu_baseline"] = {"value": value_c, "unit": "vertices/s", "cores": cores,
                                 "kind": "port", "sample": sample}
     if rank == 0:
         print(json.dumps(line), flush=True)
+    if graph is not None:
+        graph.close()
     net.close()
     if dist:
         dist.destroy_process_group()
@@ -402,18 +549,28 @@ def run_ours(args, rank, world, local_rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--precision", choices=("fp16", "bf16", "fp32"), default="fp16")
+    ap.add_argument("--workload", choices=tuple(WORKLOADS), default="frame1080p")
+    ap.add_argument("--precision", choices=("fp16", "bf16", "fp32"), default=None)
     ap.add_argument("--no-train", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--bounces", type=int, default=BOUNCES, help="smaller cases for profiling")
-    ap.add_argument("--vertices", type=int, default=N_VERT, help="smaller cases for profiling")
+    ap.add_argument("--launch-shape", default=None,
+                    help="CTAS_PER_SM,WARPGROUPS of the inference kernel instead of autotuning")
+    ap.add_argument("--bounces", type=int, default=None, help="smaller cases for profiling")
+    ap.add_argument("--vertices", type=int, default=None, help="smaller cases for profiling")
     args = ap.parse_args()
-    globals()["BOUNCES"] = args.bounces
-    globals()["N_VERT"] = args.vertices
+    wl = WORKLOADS[args.workload]
     args.warmup = max(3, args.warmup)
+    if args.steps is None:
+        args.steps = wl["steps"]
+    if args.precision is None:
+        args.precision = wl["precision"]
+    if args.bounces:
+        wl["bounces"] = args.bounces
+    if args.vertices:
+        wl["n_vert"] = args.vertices
     rank, world = env_int("RANK", 0), env_int("WORLD_SIZE", 1)
     local_rank = env_int("LOCAL_RANK", 0)
     if args.impl == "reference":

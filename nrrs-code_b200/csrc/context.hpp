@@ -43,7 +43,7 @@ struct nrrs_ctx {
     float* wt = nullptr;       // transposed FP32 MLP weights
     float* wrow = nullptr;     // aligned row-major copy of the FP32 MLP weights
     void* wpack = nullptr;     // UMMA-packed FP16/BF16 MLP weights
-    void* tpack = nullptr;     // BF16 training image (forward + transposed layers)
+    void* tpack = nullptr;     // training image: forward layers, FP16 StatNet / BF16 RRSNet
     size_t wt_floats = 0, wpack_bytes = 0;
     size_t wt_rrs_offset = 0;  // floats from wt to the RRSNet part
 

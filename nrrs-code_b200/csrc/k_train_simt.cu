@@ -271,8 +271,7 @@ __global__ void __launch_bounds__(kTT) k_train_stat(const __grid_constant__ Trai
                 const uint32_t row = grid_row(L, a.enc.hash_mask, c.ix + (k & 1),
                                               c.iy + ((k >> 1) & 1), c.iz + ((k >> 2) & 1));
                 const float w = corner_weight(c, k);
-                atomicAdd(a.table_grad + 2 * (size_t)row, w * dx[2 * l]);
-                atomicAdd(a.table_grad + 2 * (size_t)row + 1, w * dx[2 * l + 1]);
+                red_add2(a.table_grad + 2 * (size_t)row, w * dx[2 * l], w * dx[2 * l + 1]);
             }
         }
 
@@ -470,16 +469,51 @@ struct AdamArgs {
     float lr, b1, b2, eps, l2, c1, c2;
 };
 
+__device__ __forceinline__ float adam_one(const AdamArgs& a, float w, float g0, float& m, float& v) {
+    const float g = g0 * a.gscale + a.l2 * w;
+    m = a.b1 * m + (1.0f - a.b1) * g;
+    v = a.b2 * v + (1.0f - a.b2) * g * g;
+    return w - a.lr * (m / a.c1) / (sqrtf(v / a.c2) + a.eps);
+}
+
+// HBM-bound (30 B per parameter): four parameters per thread with 16-byte loads and stores of
+// the weights, gradients and both moments; the FP16 copy of the table is written in the same
+// pass. first is a multiple of 4 and the arrays are 16-byte aligned; a scalar tail finishes.
 __global__ void k_adam(const __grid_constant__ AdamArgs a) {
-    for (uint64_t k = a.first + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t quads = a.count / 4;
+    for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q < quads;
+         q += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t k = a.first + 4 * q;
+        const float4 w = *reinterpret_cast<const float4*>(a.p + k);
+        const float4 g = *reinterpret_cast<const float4*>(a.g + k);
+        float4 m = *reinterpret_cast<const float4*>(a.m + k);
+        float4 v = *reinterpret_cast<const float4*>(a.v + k);
+        float4 nw;
+        nw.x = adam_one(a, w.x, g.x, m.x, v.x);
+        nw.y = adam_one(a, w.y, g.y, m.y, v.y);
+        nw.z = adam_one(a, w.z, g.z, m.z, v.z);
+        nw.w = adam_one(a, w.w, g.w, m.w, v.w);
+        *reinterpret_cast<float4*>(a.m + k) = m;
+        *reinterpret_cast<float4*>(a.v + k) = v;
+        *reinterpret_cast<float4*>(a.p + k) = nw;
+        if (a.table_h && k + 4 <= a.n_table) {
+            __half2 h0 = __floats2half2_rn(nw.x, nw.y), h1 = __floats2half2_rn(nw.z, nw.w);
+            uint2 u;
+            u.x = *reinterpret_cast<uint32_t*>(&h0);
+            u.y = *reinterpret_cast<uint32_t*>(&h1);
+            *reinterpret_cast<uint2*>(a.table_h + k) = u;
+        } else if (a.table_h) {
+            const float nv[4] = {nw.x, nw.y, nw.z, nw.w};
+            for (int j = 0; j < 4; ++j)
+                if (k + j < a.n_table) a.table_h[k + j] = __float2half_rn(nv[j]);
+        }
+    }
+    for (uint64_t k = a.first + 4 * quads + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
          k < a.first + a.count; k += (uint64_t)gridDim.x * blockDim.x) {
-        const float w = a.p[k];
-        const float g = a.g[k] * a.gscale + a.l2 * w;
-        const float m = a.b1 * a.m[k] + (1.0f - a.b1) * g;
-        const float v = a.b2 * a.v[k] + (1.0f - a.b2) * g * g;
+        float m = a.m[k], v = a.v[k];
+        const float nw = adam_one(a, a.p[k], a.g[k], m, v);
         a.m[k] = m;
         a.v[k] = v;
-        const float nw = w - a.lr * (m / a.c1) / (sqrtf(v / a.c2) + a.eps);
         a.p[k] = nw;
         if (a.table_h && k < a.n_table) a.table_h[k] = __float2half_rn(nw);
     }

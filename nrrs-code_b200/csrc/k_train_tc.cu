@@ -8,10 +8,10 @@
 // reduced and in the hash-grid scatter), so they stay O(1) in BF16.
 //
 //   k_ttc_stat   per 128-sample tile: FP16-table encode -> StatNet forward (tcgen05) -> loss
-//                gradient -> input gradients through the transposed weight images (tcgen05) ->
-//                hash-grid scatter-add (FP32 atomics); glue -> RRSNet input tile. Every
-//                activation and delta tile is written to HBM with a bulk TMA store, in its
-//                shared-memory layout.
+//                gradient -> input gradients with the forward weight images read as MN-major
+//                (transposed) operands (tcgen05) -> hash-grid scatter-add (vector FP32
+//                reductions); glue -> RRSNet input tile. Every activation and delta tile is
+//                written to HBM with a bulk TMA store, in its shared-memory layout.
 //   k_ttc_rrs    <false>: RRSNet forward for the batch sums V and C; <true>: forward again,
 //                loss gradient with the final V and C, backward; tiles stored as above.
 //   k_wgrad_tc   dW = sum over samples of delta (x) activation: split-K over sample chunks,
@@ -46,13 +46,14 @@ struct TcTrainArgs {
     int32_t train_rrs;
     const __half* table_h;
     float* table_grad;
-    const uint8_t* tpack;   // BF16 training image
-    uint32_t s_bytes;       // StatNet forward + transposed images (bytes, at tpack + 0)
-    uint32_t r_off, r_bytes;// RRSNet forward + transposed images
+    const uint8_t* tpack;   // training image (forward layers)
+    uint32_t s_bytes;       // StatNet image bytes (at tpack + 0)
+    uint32_t r_off, r_bytes;// RRSNet image
     uint8_t* act;           // tile-blocked BF16 scratch
     Arr x0, hs[kMaxH], dhs[kMaxH], dy, x1, hr[kMaxH], dhr[kMaxH], draw;
-    double* part;           // [kMaxCtas][4]: loss_S, V, C
+    double* part;           // [part_rows][4]: loss_S, V, C per CTA
     uint32_t part_rows;
+    uint32_t part_used;     // rows the StatNet and RRSNet-forward grids write
     double* loss_out;
 };
 
@@ -92,34 +93,35 @@ __device__ __forceinline__ double block_sum_d(double v, double* red) {
 }
 
 // ---------------------------------------------------------------------------------------------
+// Shared-memory plan of the StatNet kernel: the forward weight images (the backward reads them
+// as MN-major operands, i.e. transposed), two [128 x W] tiles that take turns as the input tile,
+// activations and deltas, and the two 16-wide tiles. The ReLU masks live in registers: row m of
+// every tile is produced and consumed by thread m.
 template <int W, int H>
 struct StatSmem {
     static constexpr uint32_t kFwd = 2u * (W * kStatIn + (H - 1) * W * W + 16 * W);
-    static constexpr uint32_t kBwd = 2u * (kStatIn * W + (H - 1) * W * W + W * 16);
-    static constexpr uint32_t kW = (kFwd + kBwd + 1023u) / 1024u * 1024u;
+    static constexpr uint32_t kW = (kFwd + 1023u) / 1024u * 1024u;
     static constexpr uint32_t kTileW = 128u * W * 2u;   // one [128 x W] tile
-    static constexpr uint32_t kX0 = 0 + kW;             // [128 x 64], reused as a delta tile
-    static constexpr uint32_t kH = kX0 + 128u * 64u * 2u;
-    static constexpr uint32_t kD = kH + H * kTileW;
-    static constexpr uint32_t kDY = kD + kTileW;
+    static constexpr uint32_t kB0 = kW;
+    static constexpr uint32_t kB1 = kB0 + kTileW;
+    static constexpr uint32_t kDY = kB1 + kTileW;
     static constexpr uint32_t kX1 = kDY + 128u * 16u * 2u;
     static constexpr uint32_t kBar = kX1 + 128u * 16u * 2u;
     static constexpr size_t kSmem = 1024 + kBar + 64;
 };
 
+// Layer h's activations go to buffer (h + 1) % 2 (buffer 0 first holds the input tile), its
+// deltas to buffer h % 2. Before an epilogue overwrites a buffer, thread 0 waits until the bulk
+// store that last read it has finished: the counts below are the bulk groups committed since.
 template <int W, int H>
 __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcTrainArgs a) {
-    static_assert(W == 64, "the tensor-core training path keeps 64-wide tiles resident");
+    static_assert((W == 64 || W == 128) && (H == 2 || H == 3), "tensor-core training shapes");
     using S = StatSmem<W, H>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023u) &
                                                ~uintptr_t(1023));
     uint8_t* sW = base;
-    uint8_t* sX0 = base + S::kX0;
-    uint8_t* sH[H];
-#pragma unroll
-    for (int h = 0; h < H; ++h) sH[h] = base + S::kH + h * S::kTileW;
-    uint8_t* sD = base + S::kD;
+    uint8_t* sB[2] = {base + S::kB0, base + S::kB1};
     uint8_t* sDY = base + S::kDY;
     uint8_t* sX1 = base + S::kX1;
     uint64_t* bars = reinterpret_cast<uint64_t*>(base + S::kBar);
@@ -135,26 +137,25 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
         s_abort = 0;
     }
     if (warp == 0) {
-        tc::tmem_alloc(tslot, 64);
+        tc::tmem_alloc(tslot, W);
         tc::tmem_relinquish();
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = *tslot;
-    if (!load_weights(sW, a.tpack, S::kFwd + S::kBwd, &bars[0], tid)) s_abort = 1;
+    if (!load_weights(sW, a.tpack, S::kFwd, &bars[0], tid)) s_abort = 1;
     __syncthreads();
     unsigned flags = s_abort ? NRRS_DEV_TIMEOUT : 0u;
     uint32_t phase = 0;
     const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
 
-    // forward images, then the transposed images (same order as k_pack_train)
+    // forward images: [W x 64], (H - 1) x [W x W], [16 x W]
     const uint8_t* wF[H + 1];
-    const uint8_t* wT[H + 1];
     wF[0] = sW;
-    for (int h = 1; h <= H; ++h) wF[h] = wF[h - 1] + (h == 1 ? W * kStatIn * 2 : W * W * 2);
-    wT[0] = sW + S::kFwd;
-    for (int h = 1; h <= H; ++h) wT[h] = wT[h - 1] + (h == 1 ? kStatIn * W * 2 : W * W * 2);
+    wF[1] = sW + W * kStatIn * 2;
+#pragma unroll
+    for (int h = 2; h <= H; ++h) wF[h] = wF[h - 1] + W * W * 2;
 
     double lossS = 0.0;
     const __half2* table = reinterpret_cast<const __half2*>(a.table_h);
@@ -165,7 +166,7 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
         const uint32_t i = t * 128 + tid;
         const bool valid = i < a.n;
         float p[3] = {0.f, 0.f, 0.f};
-        // ---- encode (FP16 table, BF16 tile) ----
+        // ---- encode (FP16 table, FP16 tile) into buffer 0 ----
         if (valid) {
             norm_pos(a.enc, a.v.pos, i, p);
 #pragma unroll 1
@@ -179,35 +180,38 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
                     f[2 * j] = fv.x;
                     f[2 * j + 1] = fv.y;
                 }
-                store_chunk(sX0, tid, lq, 64, pack8<false>(f));
+                store_chunk(sB[0], tid, lq, 64, pack8<false>(f));
             }
             float sh[16], misc[16];
             const size_t i3 = 3 * (size_t)i;
             sh16(a.v.wi[i3], a.v.wi[i3 + 1], a.v.wi[i3 + 2], sh);
-            store_chunk(sX0, tid, 4, 64, pack8<false>(sh));
-            store_chunk(sX0, tid, 5, 64, pack8<false>(sh + 8));
+            store_chunk(sB[0], tid, 4, 64, pack8<false>(sh));
+            store_chunk(sB[0], tid, 5, 64, pack8<false>(sh + 8));
             misc_lanes(a.v, i, misc);
-            store_chunk(sX0, tid, 6, 64, pack8<false>(misc));
-            store_chunk(sX0, tid, 7, 64, make_uint4(0u, 0u, 0u, 0u));
+            store_chunk(sB[0], tid, 6, 64, pack8<false>(misc));
+            store_chunk(sB[0], tid, 7, 64, make_uint4(0u, 0u, 0u, 0u));
         } else {
-            zero_row(sX0, tid, 64);
+            zero_row(sB[0], tid, 64);
         }
         sync_for_mma();
-        if (tid == 0) store_tile(tile_ptr(a.act, a.x0, t), sX0, 128u * 64u * 2u);
+        if (tid == 0) store_tile(tile_ptr(a.act, a.x0, t), sB[0], 128u * 64u * 2u);
 
         // ---- StatNet forward ----
-        bool ok = mma_layer<kStatIn, W, false>(sX0, wF[0], tmem, &bars[1], phase, tid);
-        epilogue_relu<W, false>(trow, sH[0], tid);
+        uint32_t mk[H][W / 32];
+        bool ok = mma_layer<kStatIn, W, false>(sB[0], wF[0], tmem, &bars[1], phase, tid);
+        epilogue_relu_bits<W, false>(trow, sB[1], tid, mk[0]);
         sync_for_mma();
-        if (tid == 0) store_tile(tile_ptr(a.act, a.hs[0], t), sH[0], S::kTileW);
-#pragma unroll 1
+        if (tid == 0) store_tile(tile_ptr(a.act, a.hs[0], t), sB[1], S::kTileW);
+#pragma unroll
         for (int h = 1; h < H; ++h) {
-            ok &= mma_layer<W, W, false>(sH[h - 1], wF[h], tmem, &bars[1], phase, tid);
-            epilogue_relu<W, false>(trow, sH[h], tid);
+            ok &= mma_layer<W, W, false>(sB[h % 2], wF[h], tmem, &bars[1], phase, tid);
+            if (tid == 0) tc::bulk_wait_read_n<1>();
+            __syncthreads();
+            epilogue_relu_bits<W, false>(trow, sB[(h + 1) % 2], tid, mk[h]);
             sync_for_mma();
-            if (tid == 0) store_tile(tile_ptr(a.act, a.hs[h], t), sH[h], S::kTileW);
+            if (tid == 0) store_tile(tile_ptr(a.act, a.hs[h], t), sB[(h + 1) % 2], S::kTileW);
         }
-        ok &= mma_layer<W, 16, false>(sH[H - 1], wF[H], tmem, &bars[1], phase, tid);
+        ok &= mma_layer<W, 16, false>(sB[H % 2], wF[H], tmem, &bars[1], phase, tid);
         float y[16];
         tc::tmem_ld16(trow, y);
         tc::tmem_wait_ld();
@@ -236,31 +240,27 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
             store_tile(tile_ptr(a.act, a.x1, t), sX1, 128u * 16u * 2u);
         }
 
-        // ---- backward through the transposed images ----
-        ok &= mma_layer<16, W, false>(sDY, wT[H], tmem, &bars[1], phase, tid);
-        epilogue_mask<W, false>(trow, sH[H - 1], sD, tid);
+        // ---- backward: delta of layer h -> buffer h % 2 ----
+        ok &= mma_layer_t<16, W, W, false>(sDY, wF[H], tmem, &bars[1], phase, tid);
+        if (tid == 0) tc::bulk_wait_read_n<3>();  // since: h[H-1], dy, x1
+        __syncthreads();
+        epilogue_mask_bits<W, false>(trow, mk[H - 1], sB[(H - 1) % 2], tid);
         sync_for_mma();
-        if (tid == 0) {
-            store_tile(tile_ptr(a.act, a.dhs[H - 1], t), sD, S::kTileW);
-        }
-        uint8_t* cur = sD;
-        uint8_t* other = sX0;  // free once its store has been read out
-#pragma unroll 1
+        if (tid == 0) store_tile(tile_ptr(a.act, a.dhs[H - 1], t), sB[(H - 1) % 2], S::kTileW);
+#pragma unroll
         for (int h = H - 1; h >= 1; --h) {
-            ok &= mma_layer<W, W, false>(cur, wT[h], tmem, &bars[1], phase, tid);
-            if (tid == 0) tc::bulk_wait_read();
-            __syncthreads();
-            epilogue_mask<W, false>(trow, sH[h - 1], other, tid);
-            sync_for_mma();
+            ok &= mma_layer_t<W, W, W, false>(sB[h % 2], wF[h], tmem, &bars[1], phase, tid);
             if (tid == 0) {
-                store_tile(tile_ptr(a.act, a.dhs[h - 1], t), other, S::kTileW);
-                }
-            uint8_t* tmp = cur;
-            cur = other;
-            other = tmp;
+                if (h == H - 1) tc::bulk_wait_read_n<3>();  // since: dy, x1, d[H-1]
+                else tc::bulk_wait_read_n<1>();             // since: d[h]
+            }
+            __syncthreads();
+            epilogue_mask_bits<W, false>(trow, mk[h - 1], sB[(h - 1) % 2], tid);
+            sync_for_mma();
+            if (tid == 0) store_tile(tile_ptr(a.act, a.dhs[h - 1], t), sB[(h - 1) % 2], S::kTileW);
         }
         // input gradient of the 32 hash lanes (per sample; 1/n applied below)
-        ok &= mma_layer<W, 32, false>(cur, wT[0], tmem, &bars[1], phase, tid);
+        ok &= mma_layer_t<W, 32, kStatIn, false>(sB[0], wF[0], tmem, &bars[1], phase, tid);
         float dx[32];
         tc::tmem_ld16(trow, dx);
         tc::tmem_ld16(trow + 16, dx + 16);
@@ -278,8 +278,7 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
                     const uint32_t row = grid_row(L, a.enc.hash_mask, c.ix + (k & 1),
                                                   c.iy + ((k >> 1) & 1), c.iz + ((k >> 2) & 1));
                     const float w = corner_weight(c, k);
-                    atomicAdd(a.table_grad + 2 * (size_t)row, w * g0);
-                    atomicAdd(a.table_grad + 2 * (size_t)row + 1, w * g1);
+                    red_add2(a.table_grad + 2 * (size_t)row, w * g0, w * g1);
                 }
             }
         }
@@ -296,23 +295,23 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
     __syncthreads();
     if (warp == 0) {
         tc::fence_after_sync();
-        tc::tmem_dealloc(tmem, 64);
+        tc::tmem_dealloc(tmem, W);
     }
     (void)flags;
 }
 
 // ---------------------------------------------------------------------------------------------
+// RRSNet: forward images, the BF16 input tile, two [128 x W] tiles (activations of layer h in
+// buffer h % 2, deltas of layer h in buffer (h + 1) % 2) and the output-delta tile.
 template <int W, int H>
 struct RrsSmem {
     static constexpr uint32_t kFwd = 2u * (W * kRrsIn + (H - 1) * W * W + 16 * W);
-    static constexpr uint32_t kBwd = 2u * ((H - 1) * W * W + W * 16);
-    static constexpr uint32_t kW = (kFwd + kBwd + 1023u) / 1024u * 1024u;
+    static constexpr uint32_t kW = (kFwd + 1023u) / 1024u * 1024u;
     static constexpr uint32_t kTileW = 128u * W * 2u;
     static constexpr uint32_t kX1 = kW;
-    static constexpr uint32_t kG = kX1 + 128u * 16u * 2u;
-    static constexpr uint32_t kD = kG + H * kTileW;
-    static constexpr uint32_t kE = kD + kTileW;
-    static constexpr uint32_t kDR = kE + kTileW;
+    static constexpr uint32_t kB0 = kX1 + 128u * 16u * 2u;
+    static constexpr uint32_t kB1 = kB0 + kTileW;
+    static constexpr uint32_t kDR = kB1 + kTileW;
     static constexpr uint32_t kBar = kDR + 128u * 16u * 2u;
     static constexpr size_t kSmem = 1024 + kBar + 64;
 };
@@ -329,17 +328,14 @@ __device__ __forceinline__ float rel_contrib_tc(const TcTrainArgs& a, uint32_t i
 
 template <int W, int H, bool BACKWARD>
 __global__ void __launch_bounds__(128, 1) k_ttc_rrs(const __grid_constant__ TcTrainArgs a) {
+    static_assert((W == 64 || W == 128) && (H == 2 || H == 3), "tensor-core training shapes");
     using S = RrsSmem<W, H>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023u) &
                                                ~uintptr_t(1023));
     uint8_t* sW = base;
     uint8_t* sX1 = base + S::kX1;
-    uint8_t* sG[H];
-#pragma unroll
-    for (int h = 0; h < H; ++h) sG[h] = base + S::kG + h * S::kTileW;
-    uint8_t* sD = base + S::kD;
-    uint8_t* sE = base + S::kE;
+    uint8_t* sB[2] = {base + S::kB0, base + S::kB1};
     uint8_t* sDR = base + S::kDR;
     uint64_t* bars = reinterpret_cast<uint64_t*>(base + S::kBar);  // weights, mma, x1 load
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 3);
@@ -356,11 +352,18 @@ __global__ void __launch_bounds__(128, 1) k_ttc_rrs(const __grid_constant__ TcTr
         s_abort = 0;
     }
     if (BACKWARD) {
-        if (tid < 3) {
-            double t = 0.0;
-            for (uint32_t b = 0; b < a.part_rows; ++b) t += a.part[4 * b + tid];
-            s_tot[tid] = t;
+        // batch sums of the loss partials (rows written by the StatNet and forward launches),
+        // in a fixed order, so every CTA holds the same V and C
+        double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+        for (uint32_t b = tid; b < a.part_used; b += 128) {
+            t0 += a.part[4 * b + 0];
+            t1 += a.part[4 * b + 1];
+            t2 += a.part[4 * b + 2];
         }
+        t0 = block_sum_d(t0, red);
+        t1 = block_sum_d(t1, red);
+        t2 = block_sum_d(t2, red);
+        if (tid == 0) s_tot[0] = t0, s_tot[1] = t1, s_tot[2] = t2;
         __syncthreads();
         if (blockIdx.x == 0 && tid == 0) {
             const double Vm = s_tot[1] / (double)a.n, Cm = s_tot[2] / (double)a.n;
@@ -370,7 +373,7 @@ __global__ void __launch_bounds__(128, 1) k_ttc_rrs(const __grid_constant__ TcTr
         if (!a.train_rrs) return;  // StatNet-only steps: losses are all this launch writes
     }
     if (warp == 0) {
-        tc::tmem_alloc(tslot, 64);
+        tc::tmem_alloc(tslot, W);
         tc::tmem_relinquish();
     }
     tc::fence_before_sync();
@@ -382,18 +385,17 @@ __global__ void __launch_bounds__(128, 1) k_ttc_rrs(const __grid_constant__ TcTr
         Vf = (float)(s_tot[1] / (double)a.n);
         Cf = (float)(s_tot[2] / (double)a.n);
     }
-    if (!load_weights(sW, a.tpack + a.r_off, S::kFwd + S::kBwd, &bars[0], tid)) s_abort = 1;
+    if (!load_weights(sW, a.tpack + a.r_off, S::kFwd, &bars[0], tid)) s_abort = 1;
     __syncthreads();
     unsigned flags = s_abort ? NRRS_DEV_TIMEOUT : 0u;
     uint32_t phase = 0, xphase = 0;
     const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    // forward images: [W x 16], (H - 1) x [W x W], [16 x W]
     const uint8_t* wF[H + 1];
-    const uint8_t* wT[H + 1];
     wF[0] = sW;
-    for (int h = 1; h <= H; ++h) wF[h] = wF[h - 1] + (h == 1 ? W * kRrsIn * 2 : W * W * 2);
-    wT[0] = nullptr;
-    wT[1] = sW + S::kFwd;
-    for (int h = 2; h <= H; ++h) wT[h] = wT[h - 1] + W * W * 2;
+    wF[1] = sW + W * kRrsIn * 2;
+#pragma unroll
+    for (int h = 2; h <= H; ++h) wF[h] = wF[h - 1] + W * W * 2;
 
     double sumV = 0.0, sumC = 0.0;
     const uint32_t tiles = (a.n + 127) / 128;
@@ -409,18 +411,23 @@ __global__ void __launch_bounds__(128, 1) k_ttc_rrs(const __grid_constant__ TcTr
         const uint32_t i = t * 128 + tid;
         const bool valid = i < a.n;
 
+        uint32_t mk[H][W / 32];
         ok &= mma_layer<kRrsIn, W, true>(sX1, wF[0], tmem, &bars[1], phase, tid);
-        epilogue_relu<W, true>(trow, sG[0], tid);
+        epilogue_relu_bits<W, true>(trow, sB[0], tid, mk[0]);
         sync_for_mma();
-        if (BACKWARD && tid == 0) store_tile(tile_ptr(a.act, a.hr[0], t), sG[0], S::kTileW);
-#pragma unroll 1
+        if (BACKWARD && tid == 0) store_tile(tile_ptr(a.act, a.hr[0], t), sB[0], S::kTileW);
+#pragma unroll
         for (int h = 1; h < H; ++h) {
-            ok &= mma_layer<W, W, true>(sG[h - 1], wF[h], tmem, &bars[1], phase, tid);
-            epilogue_relu<W, true>(trow, sG[h], tid);
+            ok &= mma_layer<W, W, true>(sB[(h - 1) % 2], wF[h], tmem, &bars[1], phase, tid);
+            if (BACKWARD) {
+                if (tid == 0) tc::bulk_wait_read_n<1>();  // since: h[h-1]
+                __syncthreads();
+            }
+            epilogue_relu_bits<W, true>(trow, sB[h % 2], tid, mk[h]);
             sync_for_mma();
-            if (BACKWARD && tid == 0) store_tile(tile_ptr(a.act, a.hr[h], t), sG[h], S::kTileW);
+            if (BACKWARD && tid == 0) store_tile(tile_ptr(a.act, a.hr[h], t), sB[h % 2], S::kTileW);
         }
-        ok &= mma_layer<W, 16, true>(sG[H - 1], wF[H], tmem, &bars[1], phase, tid);
+        ok &= mma_layer<W, 16, true>(sB[(H - 1) % 2], wF[H], tmem, &bars[1], phase, tid);
         float r16[16];
         tc::tmem_ld16(trow, r16);
         tc::tmem_wait_ld();
@@ -445,30 +452,24 @@ __global__ void __launch_bounds__(128, 1) k_ttc_rrs(const __grid_constant__ TcTr
             store_chunk(sDR, tid, 0, 16, pack8<true>(dr));
             store_chunk(sDR, tid, 1, 16, pack8<true>(dr + 8));
             sync_for_mma();
-            if (tid == 0) {
-                store_tile(tile_ptr(a.act, a.draw, t), sDR, 128u * 16u * 2u);
-                }
-            ok &= mma_layer<16, W, true>(sDR, wT[H], tmem, &bars[1], phase, tid);
-            epilogue_mask<W, true>(trow, sG[H - 1], sD, tid);
+            if (tid == 0) store_tile(tile_ptr(a.act, a.draw, t), sDR, 128u * 16u * 2u);
+            ok &= mma_layer_t<16, W, W, true>(sDR, wF[H], tmem, &bars[1], phase, tid);
+            if (tid == 0) tc::bulk_wait_read_n<2>();  // since: h[H-1], draw
+            __syncthreads();
+            epilogue_mask_bits<W, true>(trow, mk[H - 1], sB[H % 2], tid);
             sync_for_mma();
-            if (tid == 0) {
-                store_tile(tile_ptr(a.act, a.dhr[H - 1], t), sD, S::kTileW);
-                }
-            uint8_t* cur = sD;
-            uint8_t* other = sE;
-#pragma unroll 1
+            if (tid == 0) store_tile(tile_ptr(a.act, a.dhr[H - 1], t), sB[H % 2], S::kTileW);
+#pragma unroll
             for (int h = H - 1; h >= 1; --h) {
-                ok &= mma_layer<W, W, true>(cur, wT[h], tmem, &bars[1], phase, tid);
-                if (tid == 0) tc::bulk_wait_read();
-                __syncthreads();
-                epilogue_mask<W, true>(trow, sG[h - 1], other, tid);
-                sync_for_mma();
+                ok &= mma_layer_t<W, W, W, true>(sB[(h + 1) % 2], wF[h], tmem, &bars[1], phase, tid);
                 if (tid == 0) {
-                    store_tile(tile_ptr(a.act, a.dhr[h - 1], t), other, S::kTileW);
-                        }
-                uint8_t* tmp = cur;
-                cur = other;
-                other = tmp;
+                    if (h == H - 1) tc::bulk_wait_read_n<2>();  // since: draw, d[H-1]
+                    else tc::bulk_wait_read_n<1>();             // since: d[h]
+                }
+                __syncthreads();
+                epilogue_mask_bits<W, true>(trow, mk[h - 1], sB[h % 2], tid);
+                sync_for_mma();
+                if (tid == 0) store_tile(tile_ptr(a.act, a.dhr[h - 1], t), sB[h % 2], S::kTileW);
             }
             tc::fence_before_sync();
             __syncthreads();
@@ -490,7 +491,7 @@ __global__ void __launch_bounds__(128, 1) k_ttc_rrs(const __grid_constant__ TcTr
     __syncthreads();
     if (warp == 0) {
         tc::fence_after_sync();
-        tc::tmem_dealloc(tmem, 64);
+        tc::tmem_dealloc(tmem, W);
     }
     (void)flags;
 }
@@ -664,14 +665,17 @@ cudaError_t launch_ttc(nrrs_ctx* ctx, TcTrainArgs& a, cudaStream_t s, bool train
         uint32_t g = (uint32_t)(ctx->sm_count * resident_ctas(k, 128, smem, 8));
         return g > tiles ? tiles : g;
     };
+    const uint32_t gs = grid_of((const void*)ks, SS::kSmem);
+    const uint32_t g = grid_of((const void*)kr0, RS::kSmem);
+    a.part_used = gs > g ? gs : g;
+    if (a.part_used > a.part_rows) return cudaErrorInvalidConfiguration;
     {
         ProfScope ps(ctx, NRRS_KERNEL_TRAIN_STAT, s);
-        ks<<<grid_of((const void*)ks, SS::kSmem), 128, SS::kSmem, s>>>(a);
+        ks<<<gs, 128, SS::kSmem, s>>>(a);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (train_rrs) {
         ProfScope ps(ctx, NRRS_KERNEL_TRAIN_RRS, s);
-        const uint32_t g = grid_of((const void*)kr0, RS::kSmem);
         kr0<<<g, 128, RS::kSmem, s>>>(a);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         kr1<<<g, 128, RS::kSmem, s>>>(a);
@@ -686,8 +690,9 @@ cudaError_t launch_ttc(nrrs_ctx* ctx, TcTrainArgs& a, cudaStream_t s, bool train
 }  // namespace
 
 bool train_tc_supported(const nrrs_config& c) {
-    return c.precision != NRRS_PREC_FP32 && c.statnet_width == 64 && c.rrsnet_width == 64 &&
-           c.statnet_hidden == c.rrsnet_hidden && (c.statnet_hidden == 2 || c.statnet_hidden == 3);
+    return c.precision != NRRS_PREC_FP32 && c.statnet_width == c.rrsnet_width &&
+           (c.statnet_width == 64 || c.statnet_width == 128) && c.statnet_hidden == c.rrsnet_hidden &&
+           (c.statnet_hidden == 2 || c.statnet_hidden == 3);
 }
 
 size_t train_tc_scratch_bytes(const nrrs_config& c, uint32_t n, int sm_count) {
@@ -736,9 +741,9 @@ int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint3
     a.table_grad = ctx->grads;
     a.tpack = reinterpret_cast<const uint8_t*>(ctx->tpack);
     const int W = c.statnet_width, H = c.statnet_hidden;
-    a.s_bytes = 2u * (uint32_t)(W * kStatIn + (H - 1) * W * W + 16 * W + kStatIn * W + (H - 1) * W * W + W * 16);
+    a.s_bytes = 2u * (uint32_t)(W * kStatIn + (H - 1) * W * W + 16 * W);
     a.r_off = a.s_bytes;
-    a.r_bytes = 2u * (uint32_t)(W * kRrsIn + (H - 1) * W * W + 16 * W + (H - 1) * W * W + W * 16);
+    a.r_bytes = 2u * (uint32_t)(W * kRrsIn + (H - 1) * W * W + 16 * W);
     a.act = act;
     a.x0 = L.x0; a.dy = L.dy; a.x1 = L.x1; a.draw = L.draw;
     for (int h = 0; h < kMaxH; ++h) {
@@ -747,7 +752,8 @@ int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint3
     a.part = part;
     a.part_rows = part_rows;
     a.loss_out = loss_dev ? loss_dev : ctx->loss_dev;
-    e = H == 2 ? launch_ttc<64, 2>(ctx, a, s, train_rrs) : launch_ttc<64, 3>(ctx, a, s, train_rrs);
+    if (W == 64) e = H == 2 ? launch_ttc<64, 2>(ctx, a, s, train_rrs) : launch_ttc<64, 3>(ctx, a, s, train_rrs);
+    else e = H == 2 ? launch_ttc<128, 2>(ctx, a, s, train_rrs) : launch_ttc<128, 3>(ctx, a, s, train_rrs);
     if (e != cudaSuccess) {
         ctx->last_error = std::string("tensor-core train launch: ") + cudaGetErrorString(e);
         return NRRS_ERR_CUDA;

@@ -77,12 +77,10 @@ __global__ void k_pack(PackArgs a) {
     }
 }
 
-// Training image: per network the forward layers [N][K] (as k_pack) followed by the transposed
-// layers used for input gradients: layer (in, out) -> [in rows][out padded to 16] K-major, i.e.
-// B[k = out][n = in] = W[out][in]. StatNet keeps all layers transposed (layer 0 feeds the
-// hash-grid gradient) and is stored in FP16 (its deltas are bounded); RRSNet needs no input
-// gradient, so its layer 0 is skipped, and it is stored in BF16 (its loss gradient r^2/q^2 can
-// exceed FP16's range).
+// Training image: per network the forward layers [N][K] in the UMMA K-major layout (as k_pack).
+// The backward passes read the same bytes as MN-major operands, which is W^T, so no transposed
+// copy is kept. StatNet is stored in FP16 (its deltas are bounded), RRSNet in BF16 (its loss
+// gradient r^2/q^2 can exceed FP16's range).
 struct PackTrainArgs {
     const float* master;
     uint16_t* out;
@@ -105,7 +103,6 @@ __global__ void k_pack_train(PackTrainArgs a) {
         const int w = net == 0 ? a.ws : a.wr;
         const int h = net == 0 ? a.hs : a.hr;
         const int out = net == 0 ? kStatOut : 1;
-        const size_t net_m = mofs;
         // forward images
         for (int l = 0; l <= h; ++l) {
             const LayerDesc d = layer_of(in, w, h, out, l);
@@ -118,23 +115,6 @@ __global__ void k_pack_train(PackTrainArgs a) {
                 a.out[pofs + umma_offset(n, k, d.in)] = to_bits(v, net == 1);
             }
             mofs += (size_t)d.out * d.in;
-            pofs += cells;
-        }
-        // transposed images
-        size_t lofs = net_m;
-        for (int l = 0; l <= h; ++l) {
-            const LayerDesc d = layer_of(in, w, h, out, l);
-            const size_t lsz = (size_t)d.out * d.in;
-            if (net == 1 && l == 0) { lofs += lsz; continue; }
-            const int kp = npad16(d.out);
-            const size_t cells = (size_t)d.in * kp;
-            for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < cells;
-                 e += (size_t)gridDim.x * blockDim.x) {
-                const int n = (int)(e / kp), k = (int)(e % kp);  // n = input, k = output
-                const float v = k < d.out ? a.master[lofs + (size_t)k * d.in + n] : 0.f;
-                a.out[pofs + umma_offset(n, k, kp)] = to_bits(v, net == 1);
-            }
-            lofs += lsz;
             pofs += cells;
         }
     }
@@ -212,11 +192,6 @@ size_t train_pack_bytes(int ws, int hs, int wr, int hr) {
         for (int l = 0; l <= h; ++l) {
             const LayerDesc d = layer_of(in, w, h, out, l);
             t += (size_t)(l == h ? npad16(d.out) : d.out) * d.in;
-        }
-        for (int l = 0; l <= h; ++l) {
-            if (net == 1 && l == 0) continue;
-            const LayerDesc d = layer_of(in, w, h, out, l);
-            t += (size_t)d.in * npad16(d.out);
         }
     }
     return t * 2;

@@ -108,6 +108,12 @@ __device__ __forceinline__ float act_sigma(float x) {
     const float ln2 = 0.6931471805599453f;
     return (x < 0.f) ? logf(1.0f + expf(x)) : (0.5f * x + ln2);
 }
+// adds (a, b) to the 8-byte aligned float pair at p with one vector reduction (sm_90 and later)
+__device__ __forceinline__ void red_add2(float* p, float a, float b) {
+    asm volatile("red.relaxed.gpu.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(a), "f"(b)
+                 : "memory");
+}
+
 __device__ __forceinline__ float act_sigma_grad(float x) {
     if (x < 0.f) { const float e = expf(x); return e / (1.0f + e); }
     return 0.5f;

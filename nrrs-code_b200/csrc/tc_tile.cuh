@@ -88,6 +88,75 @@ __device__ __forceinline__ bool mma_layer(const uint8_t* sA, const uint8_t* sB, 
     return ok;
 }
 
+// D[TMEM, 128 x N] = A[128 x K] * W^T for a forward weight image W of K output rows and KIN
+// inputs (K-major, the B operand of mma_layer). Read as an MN-major operand (inputs contiguous,
+// output rows as the reduction dimension: SBO = 128 B, LBO = KIN*16 B) the same bytes are W^T;
+// its first N inputs are produced. Input gradients need no transposed copy of the weights.
+template <int K, int N, int KIN, bool BF>
+__device__ __forceinline__ bool mma_layer_t(const uint8_t* sA, const uint8_t* sW, uint32_t tmem,
+                                            uint64_t* bar, uint32_t& phase, int tid) {
+    static_assert(N % 16 == 0 && N <= KIN && K % 16 == 0, "transposed operand shape");
+    if (tid == 0) {
+        tc::fence_after_sync();
+        const uint32_t a0 = tc::smem_u32(sA), b0 = tc::smem_u32(sW);
+        constexpr uint32_t idesc = tc::idesc_f16_major(N, BF ? 1u : 0u, 0u, 1u);
+#pragma unroll
+        for (int kk = 0; kk < K / 16; ++kk) {
+            const uint64_t ad = tc::smem_desc(a0 + kk * 256, 128, K * 16);
+            const uint64_t bd = tc::smem_desc(b0 + kk * 2 * KIN * 16, KIN * 16, 128);
+            tc::mma_f16(tmem, ad, bd, idesc, kk > 0 ? 1u : 0u);
+        }
+        tc::mma_commit(bar);
+    }
+    const bool ok = tc::mbar_wait(bar, phase, kSpin);
+    phase ^= 1u;
+    tc::fence_after_sync();
+    return ok;
+}
+
+// hidden-layer epilogue that also records the ReLU mask of row m: bit j of bits[c / 32] is set
+// when column c = 32 * (c / 32) + j is positive (the backward of the same row, by the same
+// thread, applies it; no activation tile has to stay resident)
+template <int N, bool BF>
+__device__ __forceinline__ void epilogue_relu_bits(uint32_t trow, uint8_t* sOut, int m,
+                                                   uint32_t (&bits)[N / 32]) {
+#pragma unroll
+    for (int c0 = 0; c0 < N; c0 += 32) {
+        float v[32];
+        tc::tmem_ld16(trow + c0, v);
+        tc::tmem_ld16(trow + c0 + 16, v + 16);
+        tc::tmem_wait_ld();
+        uint32_t b = 0u;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            if (v[j] > 0.f) b |= 1u << j;
+            else v[j] = 0.f;
+        }
+        bits[c0 / 32] = b;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) store_chunk(sOut, m, c0 / 8 + j, N, pack8<BF>(v + 8 * j));
+    }
+}
+
+// backward epilogue with a recorded mask: TMEM row -> zero where the forward ReLU was inactive
+template <int N, bool BF>
+__device__ __forceinline__ void epilogue_mask_bits(uint32_t trow, const uint32_t (&bits)[N / 32],
+                                                   uint8_t* sOut, int m) {
+#pragma unroll
+    for (int c0 = 0; c0 < N; c0 += 32) {
+        float v[32];
+        tc::tmem_ld16(trow + c0, v);
+        tc::tmem_ld16(trow + c0 + 16, v + 16);
+        tc::tmem_wait_ld();
+        const uint32_t b = bits[c0 / 32];
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+            if (!((b >> j) & 1u)) v[j] = 0.f;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) store_chunk(sOut, m, c0 / 8 + j, N, pack8<BF>(v + 8 * j));
+    }
+}
+
 // hidden-layer epilogue: TMEM row -> ReLU -> tile (K = N)
 template <int N, bool BF>
 __device__ __forceinline__ void epilogue_relu(uint32_t trow, uint8_t* sOut, int m) {
@@ -101,30 +170,6 @@ __device__ __forceinline__ void epilogue_relu(uint32_t trow, uint8_t* sOut, int 
         for (int j = 0; j < 32; ++j) v[j] = fmaxf(v[j], 0.f);
 #pragma unroll
         for (int j = 0; j < 4; ++j) store_chunk(sOut, m, c0 / 8 + j, N, pack8<BF>(v + 8 * j));
-    }
-}
-
-// backward epilogue: TMEM row -> zero where the forward activation (tile sH, K = N) is <= 0
-template <int N, bool BF>
-__device__ __forceinline__ void epilogue_mask(uint32_t trow, const uint8_t* sH, uint8_t* sOut, int m) {
-#pragma unroll
-    for (int c0 = 0; c0 < N; c0 += 32) {
-        float v[32];
-        tc::tmem_ld16(trow + c0, v);
-        tc::tmem_ld16(trow + c0 + 16, v + 16);
-        tc::tmem_wait_ld();
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const uint4 h = load_chunk(sH, m, c0 / 8 + j, N);
-            const uint32_t hw[4] = {h.x, h.y, h.z, h.w};
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const float2 hv = unpack2<BF>(hw[q]);
-                if (!(hv.x > 0.f)) v[8 * j + 2 * q] = 0.f;
-                if (!(hv.y > 0.f)) v[8 * j + 2 * q + 1] = 0.f;
-            }
-            store_chunk(sOut, m, c0 / 8 + j, N, pack8<BF>(v + 8 * j));
-        }
     }
 }
 
