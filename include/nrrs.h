@@ -274,6 +274,14 @@ int nrrs_autotune(nrrs_ctx* ctx, uint32_t n, const char* cache_path, char* repor
                   size_t report_len);
 int nrrs_set_launch_shape(nrrs_ctx* ctx, int32_t ctas_per_sm, int32_t warpgroups);
 int nrrs_get_launch_shape(const nrrs_ctx* ctx, int32_t* ctas_per_sm, int32_t* warpgroups);
+/* Inference mode of the tensor-core path (the autotuner's third knob): 0 = fused (the MLP kernel
+ * gathers the hash-grid corners itself), 1 = split (a level-major encoding kernel writes every
+ * tile's hash features to HBM, four levels at a time so that the table slices in use stay in
+ * L2, and the MLP kernel bulk-loads them; for tables larger than L2). Both modes give
+ * bit-identical results. Selecting split allocates (max_queue/128 + 17) feature tiles of 8 KB;
+ * not available for the FP32 path. */
+int nrrs_set_infer_split(nrrs_ctx* ctx, int32_t split);
+int nrrs_get_infer_split(const nrrs_ctx* ctx, int32_t* split);
 
 /* ---- CUDA graph of the batched step: captures nrrs_step_batched on a private stream and
  *      instantiates it; each nrrs_graph_launch replays the whole multi-depth step (inference
@@ -296,7 +304,8 @@ typedef enum {
     NRRS_KERNEL_INFER_FP32 = 0, NRRS_KERNEL_INFER_TC = 1, NRRS_KERNEL_SUM = 2,
     NRRS_KERNEL_DECIDE = 3, NRRS_KERNEL_PACK = 4, NRRS_KERNEL_TABLE_HALF = 5,
     NRRS_KERNEL_TRAIN_STAT = 6, NRRS_KERNEL_TRAIN_RRS = 7, NRRS_KERNEL_TRAIN_WGRAD = 8,
-    NRRS_KERNEL_TRAIN_REDUCE = 9, NRRS_KERNEL_ADAM = 10, NRRS_KERNEL_KINDS = 11
+    NRRS_KERNEL_TRAIN_REDUCE = 9, NRRS_KERNEL_ADAM = 10, NRRS_KERNEL_ENCODE = 11,
+    NRRS_KERNEL_KINDS = 12
 } nrrs_kernel_kind;
 uint64_t nrrs_launch_count(const nrrs_ctx* ctx);
 /* grid (CTAs) of the last inference launch: SMs x resident CTAs per SM */

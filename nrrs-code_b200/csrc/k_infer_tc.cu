@@ -16,6 +16,12 @@
 // that weight copy, each with its own A tile, mbarrier, TMEM columns and named barrier, so the
 // gather phase of one tile overlaps the MMA chain of another; CTAs per SM and WGS are the
 // autotuner's knobs. Every wait is bounded (NRRS_DEV_TIMEOUT).
+//
+// Split mode (PRE): k_encode_levels has already written each tile's 32 hash features as a
+// [128 x 32] core-matrix block; one thread brings it in with an 8 KB bulk copy (prefetched for
+// the next tile as soon as the first layer has read the current one), the warpgroup computes
+// the SH and misc lanes into a second [128 x 32] block, and the first layer reads its K = 64
+// operand from the two blocks (K steps 0-1 and 2-3). No table gathers remain in this kernel.
 #include "kernels.hpp"
 #include "tc_tile.cuh"
 
@@ -33,7 +39,7 @@ struct PackedNet {
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
 constexpr int tmem_cols(int w) { return w <= 32 ? 32 : (w <= 64 ? 64 : (w <= 128 ? 128 : 256)); }
 
-template <int WS, int HS, int WR, int HR, int WGS>
+template <int WS, int HS, int WR, int HR, int WGS, bool PRE>
 struct TcShape {
     static constexpr int kStatElems = PackedNet<WS, HS, kStatIn>::kElems;
     static constexpr int kRrsElems = PackedNet<WR, HR, kRrsIn>::kElems;
@@ -43,8 +49,18 @@ struct TcShape {
     static constexpr uint32_t kColsWg = (uint32_t)tmem_cols(cmax(WS, WR));
     static constexpr uint32_t kCols = kColsWg * WGS;
     static constexpr uint32_t kAOff = (kWBytes + 1023u) / 1024u * 1024u;
-    static constexpr uint32_t kBarOff = kAOff + WGS * kABytes;
+    // split mode: per warpgroup a hash-feature block and an SH/misc block, kept apart from the
+    // activation tile so the next tile's features can be fetched during the MLP chain; where
+    // that does not fit (128-wide, two warpgroups) the blocks are the first 16 KB of the
+    // warpgroup's activation tile and the copy is issued when the tile is free again
+    static constexpr uint32_t kSepBytes = 2u * kEncTileBytes;
+    static constexpr bool kShare =
+        PRE && 1024 + kAOff + WGS * (kABytes + kSepBytes) + 64 > 232448u;
+    static constexpr uint32_t kHBytes = PRE && !kShare ? kSepBytes : 0u;
+    static constexpr uint32_t kHOff = kAOff + WGS * kABytes;
+    static constexpr uint32_t kBarOff = kHOff + WGS * kHBytes;
     static constexpr size_t kSmem = 1024 + kBarOff + 64;
+    static_assert(!kShare || kABytes >= kSepBytes, "feature blocks inside the activation tile");
 };
 
 // named barrier of one warpgroup (id 0 is __syncthreads)
@@ -87,6 +103,46 @@ __device__ __forceinline__ void encode_row_tc(const InferArgs& a, uint32_t i, ui
     store_chunk(sA, m, 7, 64, make_uint4(0u, 0u, 0u, 0u));
 }
 
+// split mode: SH and misc lanes of vertex i as row m of a [128 x 32] block (the StatNet
+// input columns 32-63: SH 16, normal/albedo/warped roughness/bias 8, zeros 8)
+template <bool BF>
+__device__ __forceinline__ void sh_misc_row_tc(const InferArgs& a, uint32_t i, uint8_t* sS, int m) {
+    float sh[16];
+    const size_t i3 = 3 * (size_t)i;
+    sh16(a.v.wi[i3], a.v.wi[i3 + 1], a.v.wi[i3 + 2], sh);
+    store_chunk(sS, m, 0, 32, pack8<BF>(sh));
+    store_chunk(sS, m, 1, 32, pack8<BF>(sh + 8));
+    float misc[16];
+    misc_lanes(a.v, i, misc);
+    store_chunk(sS, m, 2, 32, pack8<BF>(misc));
+    store_chunk(sS, m, 3, 32, make_uint4(0u, 0u, 0u, 0u));
+}
+
+// split mode, first StatNet layer: K = 64 from two [128 x 32] blocks (hash features, then SH
+// and misc), the same four K steps in the same order as the fused kernel's single A tile
+template <int N, bool BF>
+__device__ __forceinline__ bool tc_layer0_pre(const uint8_t* sH, const uint8_t* sS,
+                                              const uint8_t* sWl, uint32_t tmem, uint64_t* bar,
+                                              uint32_t& phase, int ltid) {
+    if (ltid == 0) {
+        tc::fence_after_sync();
+        const uint32_t h0 = tc::smem_u32(sH), s0 = tc::smem_u32(sS), b0 = tc::smem_u32(sWl);
+        constexpr uint32_t idesc = tc::idesc_f16(N, BF ? 1u : 0u);
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+            const uint32_t a0 = kk < 2 ? h0 + kk * 256 : s0 + (kk - 2) * 256;
+            const uint64_t ad = tc::smem_desc(a0, 128, 32 * 16);
+            const uint64_t bd = tc::smem_desc(b0 + kk * 256, 128, kStatIn * 16);
+            tc::mma_f16(tmem, ad, bd, idesc, kk > 0 ? 1u : 0u);
+        }
+        tc::mma_commit(bar);
+    }
+    const bool ok = tc::mbar_wait(bar, phase, kSpin);
+    phase ^= 1u;
+    tc::fence_after_sync();
+    return ok;
+}
+
 // one layer issued by the warpgroup's first thread; the warpgroup waits for its completion
 template <int K, int N, bool BF>
 __device__ __forceinline__ bool tc_layer(const uint8_t* sA, const uint8_t* sWl, uint32_t tmem,
@@ -109,24 +165,27 @@ __device__ __forceinline__ bool tc_layer(const uint8_t* sA, const uint8_t* sWl, 
     return ok;
 }
 
-template <int WS, int HS, int WR, int HR, bool BF, int WGS>
+template <int WS, int HS, int WR, int HR, bool BF, int WGS, bool PRE>
 __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
     k_infer_tc(const __grid_constant__ InferArgs a) {
-    using S = TcShape<WS, HS, WR, HR, WGS>;
+    using S = TcShape<WS, HS, WR, HR, WGS, PRE>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* base = reinterpret_cast<uint8_t*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023u) & ~uintptr_t(1023));
     uint8_t* sW = base;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(base + S::kBarOff);  // [0] weights, [1+wg] mma
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 1 + WGS);
+    // [0] weights, [1+wg] mma, [1+WGS+wg] feature block (split mode)
+    uint64_t* bars = reinterpret_cast<uint64_t*>(base + S::kBarOff);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 1 + 2 * WGS);
     __shared__ int s_abort[WGS];
     __shared__ int s_wabort;
     const int tid = threadIdx.x, warp = tid >> 5;
     const int wg = tid >> 7, ltid = tid & 127;
     uint8_t* sA = base + S::kAOff + wg * S::kABytes;
+    uint8_t* sH = S::kShare ? sA : base + S::kHOff + wg * S::kHBytes;  // split mode only
+    uint8_t* sS = sH + kEncTileBytes;
 
     if (tid == 0) {
-        for (int k = 0; k < 1 + WGS; ++k) tc::mbar_init(&bars[k], 1);
+        for (int k = 0; k < 1 + 2 * WGS; ++k) tc::mbar_init(&bars[k], 1);
         tc::fence_mbar_init();
         for (int k = 0; k < WGS; ++k) s_abort[k] = 0;
         s_wabort = 0;
@@ -163,19 +222,49 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
     const uint8_t* wRh = wR0 + WR * kRrsIn * 2;
     const uint8_t* wRo = wRh + (HR - 1) * WR * WR * 2;
 
-    for (uint32_t t = blockIdx.x * WGS + wg; t < a.segs.total_tiles && !flags;
-         t += gridDim.x * WGS) {
+    // split mode: feature-block copies, one in flight at most per warpgroup
+    uint64_t* hbar = &bars[1 + WGS + wg];
+    uint32_t hphase = 0;
+    bool h_pending = false;
+    const uint32_t t0 = blockIdx.x * WGS + wg, tstride = gridDim.x * WGS;
+    auto fetch_features = [&](uint32_t tt) {
+        if (ltid == 0) {
+            tc::mbar_arrive_expect_tx(hbar, kEncTileBytes);
+            tc::bulk_g2s(sH, a.enc_tiles + (size_t)tt * kEncTileBytes, kEncTileBytes, hbar);
+        }
+        h_pending = true;
+    };
+    if (PRE && !S::kShare && t0 < a.segs.total_tiles && !flags) fetch_features(t0);
+
+    for (uint32_t t = t0; t < a.segs.total_tiles && !flags; t += tstride) {
         const int si = find_segment(a.segs, t);
         const Segment& sg = a.segs.s[si];
         const uint32_t i = sg.offset + (t - sg.tile_start) * kTile + ltid;
         const bool valid = i < sg.offset + sg.count;
 
-        if (valid) encode_row_tc<BF>(a, i, sA, ltid);
-        else zero_row(sA, ltid, 64);
+        bool ok = true;
+        // shared layout: the previous tile's chain has finished with the activation tile
+        if (PRE && S::kShare) fetch_features(t);
+        if constexpr (PRE) {
+            if (valid) sh_misc_row_tc<BF>(a, i, sS, ltid);
+            else zero_row(sS, ltid, 32);
+            ok = tc::mbar_wait(hbar, hphase, kSpin);
+            hphase ^= 1u;
+            h_pending = false;
+        } else {
+            if (valid) encode_row_tc<BF>(a, i, sA, ltid);
+            else zero_row(sA, ltid, 64);
+        }
         wg_sync_for_mma(wg);
 
         // ---- StatNet ----
-        bool ok = tc_layer<kStatIn, WS, BF>(sA, wS0, tmem, mbar, phase, ltid);
+        if constexpr (PRE) {
+            ok &= tc_layer0_pre<WS, BF>(sH, sS, wS0, tmem, mbar, phase, ltid);
+            // the first layer has read the block: bring in the next tile's features
+            if (!S::kShare && ok && t + tstride < a.segs.total_tiles) fetch_features(t + tstride);
+        } else {
+            ok &= tc_layer<kStatIn, WS, BF>(sA, wS0, tmem, mbar, phase, ltid);
+        }
         epilogue_relu<WS, BF>(trow, sA, ltid);
         wg_sync_for_mma(wg);
 #pragma unroll 1
@@ -242,6 +331,8 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
         if (s_abort[wg]) flags |= NRRS_DEV_TIMEOUT;
     }
 
+    // a copy still in flight (the loop ended early) lands before the CTA leaves
+    if (PRE && h_pending && ltid == 0 && !tc::mbar_wait(hbar, hphase, kSpin)) flags |= NRRS_DEV_TIMEOUT;
     if (flags && a.scr) atomicOr(&a.scr->status, flags);
     tc::fence_before_sync();
     __syncthreads();
@@ -251,11 +342,11 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
     }
 }
 
-template <int WS, int HS, int WR, int HR, bool BF, int WGS>
+template <int WS, int HS, int WR, int HR, bool BF, int WGS, bool PRE>
 cudaError_t launch_tc(const InferArgs& a, int sm_count, int ctas_per_sm, cudaStream_t s) {
-    using S = TcShape<WS, HS, WR, HR, WGS>;
+    using S = TcShape<WS, HS, WR, HR, WGS, PRE>;
     if (S::kSmem > 232448) return cudaErrorInvalidConfiguration;
-    auto kern = k_infer_tc<WS, HS, WR, HR, BF, WGS>;
+    auto kern = k_infer_tc<WS, HS, WR, HR, BF, WGS, PRE>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)S::kSmem);
     if (e != cudaSuccess) return e;
@@ -274,15 +365,19 @@ cudaError_t launch_tc(const InferArgs& a, int sm_count, int ctas_per_sm, cudaStr
 template <int WS, int HS, int WR, int HR, bool BF>
 cudaError_t launch_wgs(const InferArgs& a, int sm_count, int ctas_per_sm, int wgs,
                        cudaStream_t s) {
-    if (wgs == 2) return launch_tc<WS, HS, WR, HR, BF, 2>(a, sm_count, ctas_per_sm, s);
-    return launch_tc<WS, HS, WR, HR, BF, 1>(a, sm_count, ctas_per_sm, s);
+    if (a.enc_tiles) {
+        if (wgs == 2) return launch_tc<WS, HS, WR, HR, BF, 2, true>(a, sm_count, ctas_per_sm, s);
+        return launch_tc<WS, HS, WR, HR, BF, 1, true>(a, sm_count, ctas_per_sm, s);
+    }
+    if (wgs == 2) return launch_tc<WS, HS, WR, HR, BF, 2, false>(a, sm_count, ctas_per_sm, s);
+    return launch_tc<WS, HS, WR, HR, BF, 1, false>(a, sm_count, ctas_per_sm, s);
 }
 
-template <int WS, int HS, int WR, int HR, bool BF, int WGS>
+template <int WS, int HS, int WR, int HR, bool BF, int WGS, bool PRE>
 int max_ctas_tc() {
-    using S = TcShape<WS, HS, WR, HR, WGS>;
+    using S = TcShape<WS, HS, WR, HR, WGS, PRE>;
     if (S::kSmem > 232448) return 0;
-    auto kern = k_infer_tc<WS, HS, WR, HR, BF, WGS>;
+    auto kern = k_infer_tc<WS, HS, WR, HR, BF, WGS, PRE>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kSmem) !=
         cudaSuccess)
         return 0;
@@ -293,27 +388,26 @@ int max_ctas_tc() {
 
 int infer_max_ctas_fp32(int ws, int hs);
 
-int infer_max_ctas(int ws, int hs, int wr, int hr, int prec, int wgs) {
-    (void)wr;
-    (void)hr;
-    if (prec == NRRS_PREC_FP32) return wgs == 1 ? infer_max_ctas_fp32(ws, hs) : 0;
+template <int WS, int HS, bool BF>
+int max_ctas_of(int wgs, bool pre) {
+    if (pre) return wgs == 2 ? max_ctas_tc<WS, HS, WS, HS, BF, 2, true>() : max_ctas_tc<WS, HS, WS, HS, BF, 1, true>();
+    return wgs == 2 ? max_ctas_tc<WS, HS, WS, HS, BF, 2, false>() : max_ctas_tc<WS, HS, WS, HS, BF, 1, false>();
+}
+
+int infer_max_ctas(int ws, int hs, int wr, int hr, int prec, int wgs, bool split) {
+    if (prec == NRRS_PREC_FP32) return wgs == 1 && !split ? infer_max_ctas_fp32(ws, hs) : 0;
+    if (wr != ws || hr != hs) return 0;
     const bool bf = prec == NRRS_PREC_BF16;
-    if (ws == 64 && hs == 2)
-        return wgs == 2 ? (bf ? max_ctas_tc<64, 2, 64, 2, true, 2>() : max_ctas_tc<64, 2, 64, 2, false, 2>())
-                        : (bf ? max_ctas_tc<64, 2, 64, 2, true, 1>() : max_ctas_tc<64, 2, 64, 2, false, 1>());
-    if (ws == 64 && hs == 3)
-        return wgs == 2 ? (bf ? max_ctas_tc<64, 3, 64, 3, true, 2>() : max_ctas_tc<64, 3, 64, 3, false, 2>())
-                        : (bf ? max_ctas_tc<64, 3, 64, 3, true, 1>() : max_ctas_tc<64, 3, 64, 3, false, 1>());
-    if (ws == 128 && hs == 3)
-        return wgs == 2 ? (bf ? max_ctas_tc<128, 3, 128, 3, true, 2>() : max_ctas_tc<128, 3, 128, 3, false, 2>())
-                        : (bf ? max_ctas_tc<128, 3, 128, 3, true, 1>() : max_ctas_tc<128, 3, 128, 3, false, 1>());
+    if (ws == 64 && hs == 2) return bf ? max_ctas_of<64, 2, true>(wgs, split) : max_ctas_of<64, 2, false>(wgs, split);
+    if (ws == 64 && hs == 3) return bf ? max_ctas_of<64, 3, true>(wgs, split) : max_ctas_of<64, 3, false>(wgs, split);
+    if (ws == 128 && hs == 3) return bf ? max_ctas_of<128, 3, true>(wgs, split) : max_ctas_of<128, 3, false>(wgs, split);
     return 0;
 }
 
 size_t infer_tc_smem_bytes(int ws, int hs, int wr, int hr) {
-    if (ws == 64 && hs == 2) return TcShape<64, 2, 64, 2, 1>::kSmem;
-    if (ws == 64 && hs == 3) return TcShape<64, 3, 64, 3, 1>::kSmem;
-    if (ws == 128 && hs == 3) return TcShape<128, 3, 128, 3, 1>::kSmem;
+    if (ws == 64 && hs == 2) return TcShape<64, 2, 64, 2, 1, false>::kSmem;
+    if (ws == 64 && hs == 3) return TcShape<64, 3, 64, 3, 1, false>::kSmem;
+    if (ws == 128 && hs == 3) return TcShape<128, 3, 128, 3, 1, false>::kSmem;
     return 0;
 }
 

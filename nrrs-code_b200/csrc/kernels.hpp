@@ -51,7 +51,20 @@ struct InferArgs {
     float* rrs;                   // [n]
     DecideScratch* scr;           // accumulate the exact sum when not null
     unsigned long long* ext_acc;  // accumulate into this caller-owned sum instead (sharded)
+    const uint8_t* enc_tiles;     // split mode: hash features per tile from k_encode_levels
 };
+
+// split inference mode: per tile, the 32 hash-grid features of its 128 vertices as a
+// [128 x 32] K-major core-matrix block (8 KB), written level-major by k_encode_levels
+constexpr uint32_t kEncTileBytes = 128u * 32u * 2u;
+struct EncodeLvArgs {
+    EncodeParams enc;
+    SegmentTable segs;
+    const float* pos;
+    const __half* table_h;
+    uint8_t* out;                 // total_tiles x kEncTileBytes
+};
+cudaError_t launch_encode_levels(const EncodeLvArgs& a, bool bf, int sm_count, cudaStream_t s);
 
 // resident CTAs per SM of a kernel from its own resources (shared memory incl. the 1 KB the
 // runtime reserves per CTA, registers, warps), capped by `cap` (TMEM columns or a tuning choice)
@@ -67,7 +80,7 @@ cudaError_t launch_sum(const SumArgs& a, cudaStream_t s);
 cudaError_t launch_infer_fp32(const InferArgs& a, int ws, int hs, int wr, int hr, int sm_count,
                               int ctas_per_sm, cudaStream_t s);
 // largest resident CTAs per SM of the inference kernel for a shape (0 = unsupported)
-int infer_max_ctas(int ws, int hs, int wr, int hr, int prec, int wgs);
+int infer_max_ctas(int ws, int hs, int wr, int hr, int prec, int wgs, bool split = false);
 // tcgen05 mixed-precision inference
 cudaError_t launch_infer_tc(const InferArgs& a, int ws, int hs, int wr, int hr, int prec,
                             int sm_count, int ctas_per_sm, int wgs, cudaStream_t s);

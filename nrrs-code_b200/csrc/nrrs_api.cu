@@ -191,13 +191,33 @@ int run_infer(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const SegmentTable& segs,
     const nrrs_config& c = ctx->cfg;
     cudaError_t e;
     if (segs.total_tiles == 0) return NRRS_OK;
-    ProfScope ps(ctx, c.precision == NRRS_PREC_FP32 ? NRRS_KERNEL_INFER_FP32 : NRRS_KERNEL_INFER_TC, s);
-    if (c.precision == NRRS_PREC_FP32)
-        e = launch_infer_fp32(a, c.statnet_width, c.statnet_hidden, c.rrsnet_width,
-                              c.rrsnet_hidden, ctx->sm_count, ctx->simt_ctas_per_sm, s);
-    else
-        e = launch_infer_tc(a, c.statnet_width, c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden,
-                            c.precision, ctx->sm_count, ctx->tc_ctas_per_sm, ctx->tc_wgs, s);
+    const bool split = c.precision != NRRS_PREC_FP32 && ctx->tc_split;
+    if (split) {
+        // level-major encoding into the feature tiles, then the MLP kernel reads them
+        if (!ctx->enc_tiles || segs.total_tiles > ctx->enc_tiles_cap)
+            return fail(ctx, NRRS_ERR_INVALID_ARG, "split inference: feature tiles too small");
+        EncodeLvArgs ea{};
+        ea.enc = ctx->enc;
+        ea.segs = segs;
+        ea.pos = a.v.pos;
+        ea.table_h = ctx->table_h;
+        ea.out = ctx->enc_tiles;
+        {
+            ProfScope ps(ctx, NRRS_KERNEL_ENCODE, s);
+            e = launch_encode_levels(ea, c.precision == NRRS_PREC_BF16, ctx->sm_count, s);
+        }
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "encoding launch");
+        a.enc_tiles = ctx->enc_tiles;
+    }
+    {
+        ProfScope ps(ctx, c.precision == NRRS_PREC_FP32 ? NRRS_KERNEL_INFER_FP32 : NRRS_KERNEL_INFER_TC, s);
+        if (c.precision == NRRS_PREC_FP32)
+            e = launch_infer_fp32(a, c.statnet_width, c.statnet_hidden, c.rrsnet_width,
+                                  c.rrsnet_hidden, ctx->sm_count, ctx->simt_ctas_per_sm, s);
+        else
+            e = launch_infer_tc(a, c.statnet_width, c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden,
+                                c.precision, ctx->sm_count, ctx->tc_ctas_per_sm, ctx->tc_wgs, s);
+    }
     if (e != cudaSuccess) return cuda_fail(ctx, e, "inference launch");
     ctx->last_infer_grid = g_last_grid;
     return NRRS_OK;
@@ -481,6 +501,7 @@ void nrrs_destroy(nrrs_ctx* ctx) {
     cudaFree(ctx->wrow);
     cudaFree(ctx->wpack);
     cudaFree(ctx->tpack);
+    cudaFree(ctx->enc_tiles);
     cudaFree(ctx->scr);
     cudaFree(ctx->loss_dev);
     cudaFree(ctx->train_scratch);
@@ -781,7 +802,7 @@ int32_t nrrs_last_infer_grid(const nrrs_ctx* ctx) { return ctx ? ctx->last_infer
 const char* nrrs_kernel_name(int32_t kind) {
     static const char* names[NRRS_KERNEL_KINDS] = {
         "infer_fp32", "infer_tc", "sum", "decide", "pack_weights", "table_half",
-        "train_statnet", "train_rrsnet", "train_wgrad", "train_reduce", "adam"};
+        "train_statnet", "train_rrsnet", "train_wgrad", "train_reduce", "adam", "encode"};
     return (kind >= 0 && kind < NRRS_KERNEL_KINDS) ? names[kind] : "unknown";
 }
 
@@ -832,10 +853,40 @@ int nrrs_set_launch_shape(nrrs_ctx* ctx, int32_t ctas_per_sm, int32_t warpgroups
     }
     if (warpgroups != 1 && warpgroups != 2) return fail(ctx, NRRS_ERR_INVALID_ARG, "warpgroups must be 1 or 2");
     if (infer_max_ctas(c.statnet_width, c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden,
-                       c.precision, warpgroups) <= 0)
+                       c.precision, warpgroups, ctx->tc_split != 0) <= 0)
         return fail(ctx, NRRS_ERR_UNSUPPORTED, "launch shape not available for this network");
     ctx->tc_ctas_per_sm = ctas_per_sm;
     ctx->tc_wgs = warpgroups;
+    return NRRS_OK;
+}
+
+int nrrs_set_infer_split(nrrs_ctx* ctx, int32_t split) {
+    if (!ctx || (split != 0 && split != 1)) return NRRS_ERR_INVALID_ARG;
+    const nrrs_config& c = ctx->cfg;
+    if (split && c.precision == NRRS_PREC_FP32)
+        return fail(ctx, NRRS_ERR_UNSUPPORTED, "split inference is a tensor-core path mode");
+    if (split && infer_max_ctas(c.statnet_width, c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden,
+                                c.precision, 1, true) <= 0)
+        return fail(ctx, NRRS_ERR_UNSUPPORTED, "split inference not available for this network");
+    if (split && !ctx->enc_tiles) {
+        const uint32_t cap = c.max_queue / kTile + kMaxSegments + 1;
+        if (cudaMalloc(&ctx->enc_tiles, (size_t)cap * kEncTileBytes) != cudaSuccess) {
+            ctx->enc_tiles = nullptr;
+            return fail(ctx, NRRS_ERR_CUDA, "split inference: feature tile allocation");
+        }
+        ctx->enc_tiles_cap = cap;
+    }
+    ctx->tc_split = split;
+    // the warpgroup count must exist in the new mode
+    if (infer_max_ctas(c.statnet_width, c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden,
+                       c.precision, ctx->tc_wgs, split != 0) <= 0)
+        ctx->tc_wgs = 1;
+    return NRRS_OK;
+}
+
+int nrrs_get_infer_split(const nrrs_ctx* ctx, int32_t* split) {
+    if (!ctx || !split) return NRRS_ERR_INVALID_ARG;
+    *split = ctx->tc_split;
     return NRRS_OK;
 }
 
@@ -859,8 +910,9 @@ std::string tune_key(const nrrs_ctx* ctx) {
     return k.str();
 }
 
-// the cache is a JSON object of lines  "key": [ctas_per_sm, warpgroups],
-bool cache_lookup(const char* path, const std::string& key, int* ctas, int* wgs) {
+// the cache is a JSON object of lines  "key": [ctas_per_sm, warpgroups, split],  (a missing
+// split reads as 0, the fused mode)
+bool cache_lookup(const char* path, const std::string& key, int* ctas, int* wgs, int* split) {
     std::ifstream f(path);
     if (!f) return false;
     std::string line;
@@ -870,12 +922,13 @@ bool cache_lookup(const char* path, const std::string& key, int* ctas, int* wgs)
         if (pos == std::string::npos) continue;
         const size_t lb = line.find('[', pos);
         if (lb == std::string::npos) continue;
-        if (std::sscanf(line.c_str() + lb, "[%d, %d]", ctas, wgs) == 2) return true;
+        *split = 0;
+        if (std::sscanf(line.c_str() + lb, "[%d, %d, %d]", ctas, wgs, split) >= 2) return true;
     }
     return false;
 }
 
-void cache_store(const char* path, const std::string& key, int ctas, int wgs) {
+void cache_store(const char* path, const std::string& key, int ctas, int wgs, int split) {
     std::vector<std::string> keep;
     {
         std::ifstream f(path);
@@ -888,7 +941,7 @@ void cache_store(const char* path, const std::string& key, int ctas, int wgs) {
             }
     }
     char buf[512];
-    std::snprintf(buf, sizeof(buf), "  \"%s\": [%d, %d]", key.c_str(), ctas, wgs);
+    std::snprintf(buf, sizeof(buf), "  \"%s\": [%d, %d, %d]", key.c_str(), ctas, wgs, split);
     keep.push_back(buf);
     std::ofstream o(path, std::ios::trunc);
     o << "{\n";
@@ -904,10 +957,11 @@ int nrrs_autotune(nrrs_ctx* ctx, uint32_t n, const char* cache_path, char* repor
     const nrrs_config& c = ctx->cfg;
     const std::string key = tune_key(ctx);
     std::ostringstream rep;
-    int ctas = 0, wgs = 1;
-    if (cache_path && cache_lookup(cache_path, key, &ctas, &wgs) &&
-        nrrs_set_launch_shape(ctx, ctas, wgs) == NRRS_OK) {
-        rep << "{\"key\": \"" << key << "\", \"cached\": [" << ctas << ", " << wgs << "]}";
+    int ctas = 0, wgs = 1, split = 0;
+    if (cache_path && cache_lookup(cache_path, key, &ctas, &wgs, &split) &&
+        nrrs_set_infer_split(ctx, split) == NRRS_OK && nrrs_set_launch_shape(ctx, ctas, wgs) == NRRS_OK) {
+        rep << "{\"key\": \"" << key << "\", \"cached\": [" << ctas << ", " << wgs << ", " << split
+            << "]}";
         if (report && report_len) std::snprintf(report, report_len, "%s", rep.str().c_str());
         return NRRS_OK;
     }
@@ -951,14 +1005,16 @@ int nrrs_autotune(nrrs_ctx* ctx, uint32_t n, const char* cache_path, char* repor
     cudaEventCreate(&e1);
     const bool fp32 = c.precision == NRRS_PREC_FP32;
     const int saved_ctas = fp32 ? ctx->simt_ctas_per_sm : ctx->tc_ctas_per_sm;
-    const int saved_wgs = ctx->tc_wgs;
+    const int saved_wgs = ctx->tc_wgs, saved_split = ctx->tc_split;
     float best = 1e30f;
-    int best_ctas = saved_ctas, best_wgs = saved_wgs;
+    int best_ctas = saved_ctas, best_wgs = saved_wgs, best_split = saved_split;
     rep << "{\"key\": \"" << key << "\", \"n\": " << n << ", \"trials\": [";
     bool first = true;
+    for (int sp = 0; sp <= (fp32 ? 0 : 1); ++sp)
     for (int w = 1; w <= (fp32 ? 1 : 2); ++w) {
         const int maxc = infer_max_ctas(c.statnet_width, c.statnet_hidden, c.rrsnet_width,
-                                        c.rrsnet_hidden, c.precision, w);
+                                        c.rrsnet_hidden, c.precision, w, sp != 0);
+        if (maxc > 0 && nrrs_set_infer_split(ctx, sp) != NRRS_OK) continue;
         for (int k = 1; k <= maxc; ++k) {
             if (nrrs_set_launch_shape(ctx, k, w) != NRRS_OK) continue;
             int rc = NRRS_OK;
@@ -973,21 +1029,24 @@ int nrrs_autotune(nrrs_ctx* ctx, uint32_t n, const char* cache_path, char* repor
             cudaEventElapsedTime(&ms, e0, e1);
             ms /= 5.f;
             rep << (first ? "" : ", ") << "{\"ctas_per_sm\": " << k << ", \"warpgroups\": " << w
-                << ", \"ms\": " << ms << "}";
+                << ", \"split\": " << sp << ", \"ms\": " << ms << "}";
             first = false;
             if (ms < best) {
                 best = ms;
                 best_ctas = k;
                 best_wgs = w;
+                best_split = sp;
             }
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(d);
+    nrrs_set_infer_split(ctx, best_split);
     nrrs_set_launch_shape(ctx, best_ctas, best_wgs);
-    rep << "], \"best\": [" << best_ctas << ", " << best_wgs << "], \"best_ms\": " << best << "}";
-    if (cache_path) cache_store(cache_path, key, best_ctas, best_wgs);
+    rep << "], \"best\": [" << best_ctas << ", " << best_wgs << ", " << best_split
+        << "], \"best_ms\": " << best << "}";
+    if (cache_path) cache_store(cache_path, key, best_ctas, best_wgs, best_split);
     if (report && report_len) std::snprintf(report, report_len, "%s", rep.str().c_str());
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? NRRS_OK : cuda_fail(ctx, e, "autotune");

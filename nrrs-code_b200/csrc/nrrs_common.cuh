@@ -219,6 +219,39 @@ __device__ __forceinline__ float2 level_features_h(const __half2* table, const L
     return make_float2(f0, f1);
 }
 
+// Features of LB consecutive levels l0 .. l0+LB-1 (FP16 table): every corner load of the batch
+// is issued before any is used (8 * LB gathers in flight per thread), then each level's
+// trilinear sum in corner order 0..7 -- the same arithmetic as level_features_h.
+template <int LB>
+__device__ __forceinline__ void levels_features_h(const __half2* table, const EncodeParams& enc,
+                                                  const float* p, int l0, float* f /*2*LB*/) {
+    __half2 t[8 * LB];
+    CellCoord cc[LB];
+#pragma unroll
+    for (int j = 0; j < LB; ++j) {
+        const LevelDev L = enc.lv[l0 + j];
+        const CellCoord c = cell_of(p, L.res);
+        cc[j] = c;
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            t[8 * j + k] = __ldg(table + grid_row(L, enc.hash_mask, c.ix + (k & 1),
+                                                  c.iy + ((k >> 1) & 1), c.iz + ((k >> 2) & 1)));
+    }
+#pragma unroll
+    for (int j = 0; j < LB; ++j) {
+        float f0 = 0.f, f1 = 0.f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const float w = corner_weight(cc[j], k);
+            const float2 tv = __half22float2(t[8 * j + k]);
+            f0 += w * tv.x;
+            f1 += w * tv.y;
+        }
+        f[2 * j] = f0;
+        f[2 * j + 1] = f1;
+    }
+}
+
 // Misc StatNet lanes [48, 64): normal, albedo, warped roughness, bias 1, zeros
 __device__ __forceinline__ void misc_lanes(const VertexPtrs& v, uint32_t i, float* o /*16*/) {
     const size_t i3 = 3 * (size_t)i;

@@ -137,6 +137,8 @@ _SIGS = {
     "nrrs_autotune": (C.c_int, [C.c_void_p, C.c_uint32, C.c_char_p, C.c_char_p, C.c_size_t]),
     "nrrs_set_launch_shape": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "nrrs_get_launch_shape": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "nrrs_set_infer_split": (C.c_int, [C.c_void_p, C.c_int32]),
+    "nrrs_get_infer_split": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "nrrs_graph_capture_batched": (C.c_int, [C.c_void_p, C.POINTER(VertexSoA), C.c_void_p,
                                              C.POINTER(Segment), C.c_int32,
                                              C.POINTER(DecideParams), C.c_void_p, C.c_void_p,
@@ -152,7 +154,7 @@ _SIGS = {
 }
 
 KERNEL_KINDS = ("infer_fp32", "infer_tc", "sum", "decide", "pack_weights", "table_half",
-                "train_statnet", "train_rrsnet", "train_wgrad", "train_reduce", "adam")
+                "train_statnet", "train_rrsnet", "train_wgrad", "train_reduce", "adam", "encode")
 
 
 def lib():
@@ -423,6 +425,15 @@ class NRRSNetwork:
 
     def set_launch_shape(self, ctas_per_sm: int, warpgroups: int = 1):
         self._check(lib().nrrs_set_launch_shape(self._h, ctas_per_sm, warpgroups))
+
+    def set_infer_split(self, split: bool):
+        """0 = fused inference, 1 = level-major encoding kernel + MLP kernel (large tables)."""
+        self._check(lib().nrrs_set_infer_split(self._h, int(bool(split))))
+
+    def infer_split(self) -> int:
+        v = C.c_int32()
+        self._check(lib().nrrs_get_infer_split(self._h, C.byref(v)))
+        return int(v.value)
 
     def launch_shape(self) -> tuple[int, int]:
         c, w = C.c_int32(), C.c_int32()

@@ -43,11 +43,14 @@ def test_autotune_picks_and_caches(tmp_path):
     net = make_net(precision=nb.PREC_FP16)
     cache = tmp_path / "tune.json"
     rep = json.loads(net.autotune(262144, cache))
-    assert rep["trials"] and tuple(rep["best"]) == net.launch_shape()
+    assert rep["trials"] and tuple(rep["best"][:2]) == net.launch_shape()
+    assert rep["best"][2] == net.infer_split()
+    assert {t["split"] for t in rep["trials"]} == {0, 1}   # both inference modes were timed
     assert min(t["ms"] for t in rep["trials"]) == pytest.approx(rep["best_ms"])
     other = make_net(precision=nb.PREC_FP16)
     rep2 = json.loads(other.autotune(262144, cache))
-    assert tuple(rep2["cached"]) == tuple(rep["best"]) == other.launch_shape()
+    assert tuple(rep2["cached"]) == tuple(rep["best"])
+    assert tuple(rep2["cached"][:2]) == other.launch_shape() and rep2["cached"][2] == other.infer_split()
     json.loads(cache.read_text())
     net.close()
     other.close()
@@ -86,4 +89,90 @@ def test_graph_of_batched_step_equals_direct_call():
     g.close()
     rc, flags = net.device_status(stream())
     assert rc == nb.OK and flags == 0
+    net.close()
+
+
+SPLIT_SHAPES = {
+    "w64h2_fp16": (nb.PREC_FP16, dict()),
+    "w64h3_bf16": (nb.PREC_BF16, dict(statnet_width=64, statnet_hidden=3, rrsnet_width=64,
+                                      rrsnet_hidden=3)),
+    "w128h3_bf16": (nb.PREC_BF16, dict(statnet_width=128, statnet_hidden=3, rrsnet_width=128,
+                                       rrsnet_hidden=3, log2_hashmap_size=22)),
+}
+
+
+@pytest.mark.parametrize("shape", list(SPLIT_SHAPES))
+def test_split_inference_equals_fused(shape):
+    """the level-major encoding kernel + feature-tile MLP kernel gives the fused kernel's
+    outputs bit for bit, for every warpgroup count, on a ragged multi-segment launch"""
+    torch = torch_cuda()
+    prec, kw = SPLIT_SHAPES[shape]
+    net = make_net(precision=prec, **kw)
+    random_params(net, 54, table_scale=0.5, mlp_scale=0.1)
+    counts = [70_001, 129, 1, 0, 33_333]
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    N = int(offs[-1])
+    v = nb.synth(55, N)
+    d = upload(v)
+    dp = nb.default_decide()
+    caps = [9 * c for c in counts]
+    qoffs = np.concatenate([[0], np.cumsum(caps)]).astype(np.int64)
+    segs = [nb.Segment(int(offs[k]), counts[k], max(counts[k], 1), 0, int(qoffs[k]), caps[k])
+            for k in range(len(counts))]
+
+    def run():
+        o = dict(st=empty(3 * N), rrs=empty(N), norm=empty(N), split=empty(N, "uint8"),
+                 q=empty(int(qoffs[-1]), "int32"), sz=empty(len(counts), "int32"))
+        net.generateRRSNumberBatched(soa(d), d["rnd"], segs, dp, o["st"], o["rrs"], o["norm"],
+                                     o["split"], o["q"], o["sz"], stream())
+        torch.cuda.synchronize()
+        return o
+
+    net.set_infer_split(False)
+    net.set_launch_shape(0, 1)
+    ref = run()
+    net.set_infer_split(True)
+    assert net.infer_split() == 1
+    for w in (1, 2):
+        net.set_launch_shape(0, w)
+        out = run()
+        for k in ref:
+            assert torch.equal(out[k], ref[k]), (shape, w, k)
+    rc, flags = net.device_status(stream())
+    assert rc == nb.OK and flags == 0
+    net.close()
+
+
+def test_split_mode_graph_equals_fused_direct():
+    torch = torch_cuda()
+    net = make_net(precision=nb.PREC_FP16)
+    random_params(net, 56, table_scale=0.5, mlp_scale=0.15)
+    counts = [int(round(200_000 * 0.6 ** k)) for k in range(6)]
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    N = int(offs[-1])
+    v = nb.synth(57, N)
+    d = upload(v)
+    dp = nb.default_decide()
+    caps = [9 * c for c in counts]
+    qoffs = np.concatenate([[0], np.cumsum(caps)]).astype(np.int64)
+    segs = [nb.Segment(int(offs[k]), counts[k], counts[k], 0, int(qoffs[k]), caps[k])
+            for k in range(len(counts))]
+
+    def bufs():
+        return dict(st=empty(3 * N), rrs=empty(N), norm=empty(N), split=empty(N, "uint8"),
+                    q=empty(int(qoffs[-1]), "int32"), sz=empty(len(counts), "int32"))
+
+    a, b = bufs(), bufs()
+    net.generateRRSNumberBatched(soa(d), d["rnd"], segs, dp, a["st"], a["rrs"], a["norm"],
+                                 a["split"], a["q"], a["sz"], stream())
+    net.set_infer_split(True)
+    l0 = net.launch_count()
+    g = net.captureBatched(soa(d), d["rnd"], segs, dp, b["st"], b["rrs"], b["norm"], b["split"],
+                           b["q"], b["sz"])
+    assert net.launch_count() - l0 == 3      # encode, MLP, decide
+    g.launch(stream())
+    torch.cuda.synchronize()
+    for k in a:
+        assert torch.equal(a[k], b[k]), k
+    g.close()
     net.close()
