@@ -303,7 +303,10 @@ def run_ours(args, rank, world, local_rank):
     net = nb.NRRSNetwork(make_config(args.precision, wl, max_q, wl["train_batch"]))
     tune = None
     if args.launch_shape:
-        net.set_launch_shape(*[int(x) for x in args.launch_shape.split(",")])
+        shape = [int(x) for x in args.launch_shape.split(",")]
+        if len(shape) > 2:
+            net.set_infer_split(shape[2])
+        net.set_launch_shape(shape[0], shape[1])
     elif args.workload != "frame1080p":
         # the library's launch-shape tuner (CTAs per SM x warpgroups per CTA), on this shape
         tune = json.loads(net.autotune(min(max_q, N)))
@@ -511,7 +514,8 @@ def run_ours(args, rank, world, local_rank):
                           f"RRSNet 16->{wl['width']}x{wl['hidden']}->1",
                    "l2": "inputs larger than L2 (one vertex buffer per bounce, >=158 MB)"
                          if not batched else "inputs larger than L2 (one 450 MB SoA of all depths)",
-                   "launch_shape": list(net.launch_shape()),
+                   "launch_shape": list(net.launch_shape()) + (
+                       [net.infer_split()] if args.precision != "fp32" else []),
                    "parallelism": f"dp{world}"},
         "clocks": clk.summary(),
         "e2e": {"value": verts / (e2e_ms * 1e-3), "unit": "vertices/s", "ms_per_step": e2e_ms,
@@ -557,7 +561,8 @@ def main():
     ap.add_argument("--no-train", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--launch-shape", default=None,
-                    help="CTAS_PER_SM,WARPGROUPS of the inference kernel instead of autotuning")
+                    help="CTAS_PER_SM,WARPGROUPS[,SPLIT] of the inference kernels instead of "
+                         "autotuning")
     ap.add_argument("--bounces", type=int, default=None, help="smaller cases for profiling")
     ap.add_argument("--vertices", type=int, default=None, help="smaller cases for profiling")
     args = ap.parse_args()
