@@ -307,8 +307,8 @@ def run_ours(args, rank, world, local_rank):
         if len(shape) > 2:
             net.set_infer_split(shape[2])
         net.set_launch_shape(shape[0], shape[1])
-    elif args.workload != "frame1080p":
-        # the library's launch-shape tuner (CTAs per SM x warpgroups per CTA), on this shape
+    else:
+        # the library's launch-shape tuner (CTAs per SM x warpgroups per CTA x inference mode)
         tune = json.loads(net.autotune(min(max_q, N)))
     th = td = None
     if do_train:

@@ -274,11 +274,21 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
                 const CellCoord c = cell_of(p, L.res);
                 const float g0 = dx[2 * l] * a.inv_n, g1 = dx[2 * l + 1] * a.inv_n;
 #pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    const uint32_t row = grid_row(L, a.enc.hash_mask, c.ix + (k & 1),
-                                                  c.iy + ((k >> 1) & 1), c.iz + ((k >> 2) & 1));
-                    const float w = corner_weight(c, k);
-                    red_add2(a.table_grad + 2 * (size_t)row, w * g0, w * g1);
+                for (int k2 = 0; k2 < 4; ++k2) {
+                    // corners x and x+1: one 16-byte reduction when they share an aligned pair
+                    // of table rows (half the time), two 8-byte ones otherwise
+                    const uint32_t y = c.iy + (k2 & 1), z = c.iz + ((k2 >> 1) & 1);
+                    const uint32_t r0 = grid_row(L, a.enc.hash_mask, c.ix, y, z);
+                    const uint32_t r1 = grid_row(L, a.enc.hash_mask, c.ix + 1, y, z);
+                    const float w0 = corner_weight(c, 2 * k2), w1 = corner_weight(c, 2 * k2 + 1);
+                    if ((r0 >> 1) == (r1 >> 1)) {
+                        float* q = a.table_grad + 4 * (size_t)(r0 >> 1);
+                        if (r0 & 1u) red_add4(q, w1 * g0, w1 * g1, w0 * g0, w0 * g1);
+                        else red_add4(q, w0 * g0, w0 * g1, w1 * g0, w1 * g1);
+                    } else {
+                        red_add2(a.table_grad + 2 * (size_t)r0, w0 * g0, w0 * g1);
+                        red_add2(a.table_grad + 2 * (size_t)r1, w1 * g0, w1 * g1);
+                    }
                 }
             }
         }
