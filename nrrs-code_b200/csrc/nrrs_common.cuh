@@ -203,9 +203,7 @@ __device__ __forceinline__ float corner_weight(const CellCoord& c, int k) {
     return wx * wy * wz;
 }
 
-// Features of one level from an FP16 table [rows][2] (half2 per row): trilinear over the 8
-// corners, summed in corner order 0..7. Eight independent 4-byte gathers (measured faster than
-// 16-byte loads that serve both x-adjacent corners of a cell when they share a block).
+// entry e (0..3) of a 16-byte quad of table rows
 __device__ __forceinline__ uint32_t quad_pick(const uint4& q, uint32_t e) {
     const uint32_t lo = (e & 1u) ? q.y : q.x, hi = (e & 1u) ? q.w : q.z;
     return (e & 2u) ? hi : lo;
