@@ -241,6 +241,9 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
         const Segment& sg = a.segs.s[si];
         const uint32_t i = sg.offset + (t - sg.tile_start) * kTile + ltid;
         const bool valid = i < sg.offset + sg.count;
+        // the glue's and the factor's inputs, in flight during the StatNet chain
+        VertexAux aux{};
+        if (valid) aux = load_aux(a.v, i);
 
         bool ok = true;
         // shared layout: the previous tile's chain has finished with the activation tile
@@ -281,7 +284,7 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
         // ---- glue -> RRSNet input (K = 16) ----
         float x1[16];
         if (valid) {
-            glue16(a.fp, y, a.v, i, x1);
+            glue16_aux(a.fp, y, aux, x1);
         } else {
 #pragma unroll
             for (int k = 0; k < 16; ++k) x1[k] = 0.f;
@@ -310,7 +313,7 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
         if (!ok) flags |= NRRS_DEV_TIMEOUT;
         long long term = 0;
         if (valid) {
-            const float rrs = rrs_factor(a.fp, y, r[0], a.v, i);
+            const float rrs = rrs_factor_aux(a.fp, y, r[0], aux);
             if (a.stats) {
                 a.stats[3 * (size_t)i] = y[0];
                 a.stats[3 * (size_t)i + 1] = y[1];

@@ -324,6 +324,67 @@ __device__ __forceinline__ void glue16(const FactorParams& fp, const float* y, c
     for (int k = 10; k < 16; ++k) x1[k] = 0.f;
 }
 
+// The per-vertex inputs of the glue and the factor, loaded at the start of a tile so that their
+// memory latency overlaps the StatNet chain instead of stalling it.
+struct VertexAux {
+    float thp[3];
+    float rough, ref;
+    uint32_t depth;
+};
+
+__device__ __forceinline__ VertexAux load_aux(const VertexPtrs& v, uint32_t i) {
+    VertexAux x;
+    const size_t i3 = 3 * (size_t)i;
+    x.thp[0] = v.thp[i3];
+    x.thp[1] = v.thp[i3 + 1];
+    x.thp[2] = v.thp[i3 + 2];
+    x.rough = v.rough[i];
+    x.ref = v.ref ? v.ref[i] : 0.5f;
+    x.depth = v.depth ? v.depth[i] : 0u;
+    return x;
+}
+
+// glue16 and rrs_factor on preloaded inputs (the same arithmetic)
+__device__ __forceinline__ void glue16_aux(const FactorParams& fp, const float* y,
+                                           const VertexAux& x, float* x1) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        x1[c] = box_cox(lin_stat(y[c], fp.stat_eps));
+        x1[3 + c] = box_cox(x.thp[c]);
+    }
+    x1[6] = warp_rough(x.rough);
+    x1[7] = box_cox(x.ref);
+    x1[8] = (float)x.depth * 0.125f;
+    x1[9] = 1.0f;
+#pragma unroll
+    for (int k = 10; k < 16; ++k) x1[k] = 0.f;
+}
+
+__device__ __forceinline__ float rrs_factor_aux(const FactorParams& fp, const float* y, float raw,
+                                                const VertexAux& x) {
+    float rrs;
+    if (fp.source == NRRS_FACTOR_ADRRS) {
+        const float ref = x.ref + fp.ref_eps;
+        float acc = 0.f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float L = expf(fminf(y[c], 20.0f)) - fp.stat_eps;
+            L = L < 1e-4f ? 1e-4f : (L > 1e4f ? 1e4f : L);
+            acc += L * x.thp[c] / ref;
+        }
+        rrs = acc / 3.0f;
+    } else {
+        rrs = act_sigma(raw);
+    }
+    if (fp.use_ww) {
+        const float dminus = 2.0f / (1.0f + fp.ww);
+        const float dplus = dminus * fp.ww;
+        rrs = rrs < dminus ? rrs / dminus : (rrs > dplus ? rrs / dplus : 1.0f);
+    }
+    rrs = rrs < fp.clamp_min ? fp.clamp_min : (rrs > fp.clamp_max ? fp.clamp_max : rrs);
+    return rrs;
+}
+
 // factor + weight window + clamp (integrator.cpp:1184-1298)
 __device__ __forceinline__ float rrs_factor(const FactorParams& fp, const float* y, float raw,
                                             const VertexPtrs& v, uint32_t i) {
