@@ -10,7 +10,9 @@
 // them does not change a bit (the reference's FP32 sum depends on the occupancy-chosen grid).
 // The emission is a single-pass prefix sum with decoupled look-back over 2048-vertex chunks:
 // chunks are taken in ticket order, so every predecessor of a waiting chunk has already
-// started and the wait ends; each wait is still bounded and reports NRRS_DEV_TIMEOUT.
+// started and the wait ends; each wait is still bounded and reports NRRS_DEV_TIMEOUT. One warp
+// reads 32 predecessor states at a time, so the look-back of a chunk takes about
+// (distance to the nearest inclusive prefix) / 32 dependent reads.
 // The queue is in vertex order with the s copies of a vertex contiguous.
 #include "kernels.hpp"
 
@@ -87,20 +89,65 @@ __global__ void __launch_bounds__(kDecThreads) k_decide(const __grid_constant__ 
         unsigned st[kDecVPT];
         unsigned local = 0;
         const unsigned v0 = base + tid * kDecVPT;
+        // a thread's 8 consecutive vertices: 16-byte loads and stores when the whole run is in
+        // the segment and aligned (the common case), element-wise otherwise
+        const bool vec = v0 + kDecVPT <= end &&
+                         ((reinterpret_cast<uintptr_t>(a.rrs + v0) |
+                           reinterpret_cast<uintptr_t>(a.rnd + v0)) & 15u) == 0;
+        float rv[kDecVPT], nv[kDecVPT];
+        if (vec) {
+            const float4 r0 = *reinterpret_cast<const float4*>(a.rrs + v0);
+            const float4 r1 = *reinterpret_cast<const float4*>(a.rrs + v0 + 4);
+            const float4 n0 = *reinterpret_cast<const float4*>(a.rnd + v0);
+            const float4 n1 = *reinterpret_cast<const float4*>(a.rnd + v0 + 4);
+            rv[0] = r0.x; rv[1] = r0.y; rv[2] = r0.z; rv[3] = r0.w;
+            rv[4] = r1.x; rv[5] = r1.y; rv[6] = r1.z; rv[7] = r1.w;
+            nv[0] = n0.x; nv[1] = n0.y; nv[2] = n0.z; nv[3] = n0.w;
+            nv[4] = n1.x; nv[5] = n1.y; nv[6] = n1.z; nv[7] = n1.w;
+        } else {
+#pragma unroll
+            for (int j = 0; j < kDecVPT; ++j) {
+                rv[j] = v0 + j < end ? a.rrs[v0 + j] : 0.f;
+                nv[j] = v0 + j < end ? a.rnd[v0 + j] : 0.f;
+            }
+        }
+        float rn[kDecVPT];
+        uint32_t sp[2] = {0u, 0u};
 #pragma unroll
         for (int j = 0; j < kDecVPT; ++j) {
             const unsigned v = v0 + j;
             sv[j] = 0;
             st[j] = 0;
+            rn[j] = 0.f;
             if (v < end) {
-                const float r = __fmul_rn(a.rrs[v], scale);
+                const float r = __fmul_rn(rv[j], scale);
                 const unsigned stid = a.sidx ? a.sidx[v] : v;
-                if (a.rrs_norm) a.rrs_norm[stid] = r;
-                const unsigned s = split_count(r, a.rnd[v], &flags);
-                if (a.split) a.split[v] = (uint8_t)s;
+                rn[j] = r;
+                if (a.rrs_norm && (a.sidx || !vec)) a.rrs_norm[stid] = r;
+                const unsigned s = split_count(r, nv[j], &flags);
+                if (a.split && !vec) a.split[v] = (uint8_t)s;
+                sp[j >> 2] |= s << (8 * (j & 3));
                 sv[j] = s;
                 st[j] = stid;
                 local += s;
+            }
+        }
+        if (vec) {
+            if (a.rrs_norm && !a.sidx &&
+                (reinterpret_cast<uintptr_t>(a.rrs_norm + v0) & 15u) == 0) {
+                *reinterpret_cast<float4*>(a.rrs_norm + v0) = make_float4(rn[0], rn[1], rn[2], rn[3]);
+                *reinterpret_cast<float4*>(a.rrs_norm + v0 + 4) = make_float4(rn[4], rn[5], rn[6], rn[7]);
+            } else if (a.rrs_norm && !a.sidx) {
+#pragma unroll
+                for (int j = 0; j < kDecVPT; ++j) a.rrs_norm[v0 + j] = rn[j];
+            }
+            if (a.split) {
+                if ((reinterpret_cast<uintptr_t>(a.split + v0) & 7u) == 0) {
+                    *reinterpret_cast<uint2*>(a.split + v0) = make_uint2(sp[0], sp[1]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < kDecVPT; ++j) a.split[v0 + j] = (uint8_t)sv[j];
+                }
             }
         }
 
@@ -128,36 +175,59 @@ __global__ void __launch_bounds__(kDecThreads) k_decide(const __grid_constant__ 
         const unsigned thread_excl = warp_excl + incl - local;
         const unsigned chunk_total = s_warp[kDecThreads / 32 - 1];
 
-        // decoupled look-back (one thread)
-        if (tid == 0) {
+        // decoupled look-back by warp 0: each read covers the 32 chunks before a window top;
+        // the closest inclusive prefix ends it, otherwise the window moves down by 32
+        if (wid == 0) {
             unsigned long long* states = a.states;
             unsigned prefix = 0;
             if (lc == 0) {
-                store_state(&states[c], pack_state(epoch, kFlagIncl, chunk_total));
+                if (lane == 0) store_state(&states[c], pack_state(epoch, kFlagIncl, chunk_total));
             } else {
-                store_state(&states[c], pack_state(epoch, kFlagAgg, chunk_total));
-                unsigned p = c - 1;
+                if (lane == 0) store_state(&states[c], pack_state(epoch, kFlagAgg, chunk_total));
+                const int first = (int)sg.tile_start;  // the segment's first chunk: inclusive
+                int top = (int)c - 1;
                 unsigned spins = 0;
                 bool timed_out = false;
+                unsigned long long acc = 0;
                 for (;;) {
-                    const unsigned long long w = load_state(&states[p]);
-                    const unsigned we = (unsigned)(w >> 34);
-                    const unsigned long long wf = (w >> 32) & 3ull;
-                    if (we != (epoch & 0x3fffffffu) || wf == 0) {
-                        if (++spins > a.spin_limit) { timed_out = true; break; }
+                    const int idx = top - lane;
+                    bool ready = true, incl = true;
+                    unsigned val = 0;
+                    if (idx >= first) {
+                        const unsigned long long w = load_state(&states[idx]);
+                        const unsigned long long wf = (w >> 32) & 3ull;
+                        ready = (unsigned)(w >> 34) == (epoch & 0x3fffffffu) && wf != 0;
+                        incl = wf == kFlagIncl;
+                        val = (unsigned)w;
+                    }
+                    if (!__all_sync(0xffffffffu, ready)) {
+                        if (++spins > a.spin_limit) {
+                            timed_out = true;
+                            break;
+                        }
                         __nanosleep(32);
                         continue;
                     }
-                    prefix = sat_add(prefix, (unsigned)w);
-                    if (wf == kFlagIncl || p == sg.tile_start) break;
-                    --p;
+                    const unsigned im = __ballot_sync(0xffffffffu, incl);
+                    const int stop = im ? __ffs(im) - 1 : 31;  // lanes 0..stop contribute
+                    unsigned long long part = lane <= stop ? (unsigned long long)val : 0ull;
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+                    acc += part;
+                    if (im) break;
+                    top -= 32;
                 }
-                if (timed_out) flags |= NRRS_DEV_TIMEOUT;
-                store_state(&states[c], pack_state(epoch, kFlagIncl, sat_add(prefix, chunk_total)));
+                prefix = acc > 0xffffffffull ? 0xffffffffu : (unsigned)acc;
+                if (lane == 0) {
+                    if (timed_out) flags |= NRRS_DEV_TIMEOUT;
+                    store_state(&states[c], pack_state(epoch, kFlagIncl, sat_add(prefix, chunk_total)));
+                }
             }
-            s_prefix = prefix;
-            if (c == sg.tile_start + (sg.count + kDecChunk - 1) / kDecChunk - 1)
-                a.next_size[si] = sat_add(prefix, chunk_total);
+            if (lane == 0) {
+                s_prefix = prefix;
+                if (c == sg.tile_start + (sg.count + kDecChunk - 1) / kDecChunk - 1)
+                    a.next_size[si] = sat_add(prefix, chunk_total);
+            }
         }
         __syncthreads();
 
