@@ -94,16 +94,16 @@ __global__ void __launch_bounds__(kDecThreads) k_decide(const __grid_constant__ 
         const bool vec = v0 + kDecVPT <= end &&
                          ((reinterpret_cast<uintptr_t>(a.rrs + v0) |
                            reinterpret_cast<uintptr_t>(a.rnd + v0)) & 15u) == 0;
+        constexpr int kQ = kDecVPT / 4;  // 16-byte groups per thread
         float rv[kDecVPT], nv[kDecVPT];
         if (vec) {
-            const float4 r0 = *reinterpret_cast<const float4*>(a.rrs + v0);
-            const float4 r1 = *reinterpret_cast<const float4*>(a.rrs + v0 + 4);
-            const float4 n0 = *reinterpret_cast<const float4*>(a.rnd + v0);
-            const float4 n1 = *reinterpret_cast<const float4*>(a.rnd + v0 + 4);
-            rv[0] = r0.x; rv[1] = r0.y; rv[2] = r0.z; rv[3] = r0.w;
-            rv[4] = r1.x; rv[5] = r1.y; rv[6] = r1.z; rv[7] = r1.w;
-            nv[0] = n0.x; nv[1] = n0.y; nv[2] = n0.z; nv[3] = n0.w;
-            nv[4] = n1.x; nv[5] = n1.y; nv[6] = n1.z; nv[7] = n1.w;
+#pragma unroll
+            for (int g = 0; g < kQ; ++g) {
+                const float4 r4 = *reinterpret_cast<const float4*>(a.rrs + v0 + 4 * g);
+                const float4 n4 = *reinterpret_cast<const float4*>(a.rnd + v0 + 4 * g);
+                rv[4 * g] = r4.x; rv[4 * g + 1] = r4.y; rv[4 * g + 2] = r4.z; rv[4 * g + 3] = r4.w;
+                nv[4 * g] = n4.x; nv[4 * g + 1] = n4.y; nv[4 * g + 2] = n4.z; nv[4 * g + 3] = n4.w;
+            }
         } else {
 #pragma unroll
             for (int j = 0; j < kDecVPT; ++j) {
@@ -112,7 +112,9 @@ __global__ void __launch_bounds__(kDecThreads) k_decide(const __grid_constant__ 
             }
         }
         float rn[kDecVPT];
-        uint32_t sp[2] = {0u, 0u};
+        uint32_t sp[kQ];
+#pragma unroll
+        for (int g = 0; g < kQ; ++g) sp[g] = 0u;
 #pragma unroll
         for (int j = 0; j < kDecVPT; ++j) {
             const unsigned v = v0 + j;
@@ -135,15 +137,18 @@ __global__ void __launch_bounds__(kDecThreads) k_decide(const __grid_constant__ 
         if (vec) {
             if (a.rrs_norm && !a.sidx &&
                 (reinterpret_cast<uintptr_t>(a.rrs_norm + v0) & 15u) == 0) {
-                *reinterpret_cast<float4*>(a.rrs_norm + v0) = make_float4(rn[0], rn[1], rn[2], rn[3]);
-                *reinterpret_cast<float4*>(a.rrs_norm + v0 + 4) = make_float4(rn[4], rn[5], rn[6], rn[7]);
+#pragma unroll
+                for (int g = 0; g < kQ; ++g)
+                    *reinterpret_cast<float4*>(a.rrs_norm + v0 + 4 * g) =
+                        make_float4(rn[4 * g], rn[4 * g + 1], rn[4 * g + 2], rn[4 * g + 3]);
             } else if (a.rrs_norm && !a.sidx) {
 #pragma unroll
                 for (int j = 0; j < kDecVPT; ++j) a.rrs_norm[v0 + j] = rn[j];
             }
             if (a.split) {
-                if ((reinterpret_cast<uintptr_t>(a.split + v0) & 7u) == 0) {
-                    *reinterpret_cast<uint2*>(a.split + v0) = make_uint2(sp[0], sp[1]);
+                if ((reinterpret_cast<uintptr_t>(a.split + v0) & 3u) == 0) {
+#pragma unroll
+                    for (int g = 0; g < kQ; ++g) reinterpret_cast<uint32_t*>(a.split + v0)[g] = sp[g];
                 } else {
 #pragma unroll
                     for (int j = 0; j < kDecVPT; ++j) a.split[v0 + j] = (uint8_t)sv[j];
