@@ -282,6 +282,13 @@ int nrrs_get_launch_shape(const nrrs_ctx* ctx, int32_t* ctas_per_sm, int32_t* wa
  * not available for the FP32 path. */
 int nrrs_set_infer_split(nrrs_ctx* ctx, int32_t split);
 int nrrs_get_infer_split(const nrrs_ctx* ctx, int32_t* split);
+/* Training mode of the tensor-core path: 1 (the default) = split: a level-major encoding kernel
+ * writes the hash features of the batch, the StatNet kernel trains on them and writes each
+ * sample's hash-lane gradients, and a level-major scatter kernel adds those into the table
+ * gradient; 0 = fused: the StatNet kernel gathers and scatters itself. The two modes differ only
+ * in the order of the FP32 gradient additions. */
+int nrrs_set_train_split(nrrs_ctx* ctx, int32_t split);
+int nrrs_get_train_split(const nrrs_ctx* ctx, int32_t* split);
 
 /* ---- CUDA graph of the batched step: captures nrrs_step_batched on a private stream and
  *      instantiates it; each nrrs_graph_launch replays the whole multi-depth step (inference
@@ -305,7 +312,7 @@ typedef enum {
     NRRS_KERNEL_DECIDE = 3, NRRS_KERNEL_PACK = 4, NRRS_KERNEL_TABLE_HALF = 5,
     NRRS_KERNEL_TRAIN_STAT = 6, NRRS_KERNEL_TRAIN_RRS = 7, NRRS_KERNEL_TRAIN_WGRAD = 8,
     NRRS_KERNEL_TRAIN_REDUCE = 9, NRRS_KERNEL_ADAM = 10, NRRS_KERNEL_ENCODE = 11,
-    NRRS_KERNEL_KINDS = 12
+    NRRS_KERNEL_TRAIN_SCATTER = 12, NRRS_KERNEL_TRAIN_ENCODE = 13, NRRS_KERNEL_KINDS = 14
 } nrrs_kernel_kind;
 uint64_t nrrs_launch_count(const nrrs_ctx* ctx);
 /* grid (CTAs) of the last inference launch: SMs x resident CTAs per SM */

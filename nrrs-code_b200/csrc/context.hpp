@@ -61,6 +61,7 @@ struct nrrs_ctx {
     int tc_wgs = 1;              // autotuned warpgroups per CTA of the tcgen05 kernel (1 or 2)
     int simt_ctas_per_sm = 0;    // autotuned occupancy of the FP32 kernel (0 = default)
     int tc_split = 0;            // inference mode of the tcgen05 path: 0 fused, 1 split
+    int train_split = 1;         // training mode of the tcgen05 path: 0 fused, 1 split
     uint8_t* enc_tiles = nullptr;  // split mode: hash-feature tiles (kEncTileBytes each)
     uint32_t enc_tiles_cap = 0;
     nrrs::Profiler prof;

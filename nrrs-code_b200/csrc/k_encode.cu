@@ -10,9 +10,10 @@
 // sweep instead of once per use.
 //
 // A work item writes the 8 features (levels 4q .. 4q+3, 2 each) of its 128 vertices as one
-// 16-byte chunk per vertex into tile t's [128 x 32] block in the no-swizzle K-major
-// core-matrix layout: the A-operand layout of the first tcgen05 layer, so the MLP kernel
-// brings a tile in with one 8 KB bulk copy. Rows past the end of a segment are zero.
+// 16-byte chunk per vertex into chunk q of tile t, in the no-swizzle K-major core-matrix layout
+// of a [128 x kdim] tile: the A-operand layout of the first tcgen05 layer. Inference uses 8 KB
+// [128 x 32] blocks; training writes the hash columns of its [128 x 64] input tiles, whose
+// other columns the training kernel fills. Rows past the end of a segment are zero.
 // The per-level arithmetic is that of the fused kernel (levels_features_h), so the features and
 // everything downstream are bit-identical between the two modes. The encoding is the
 // reference's tcnn HashGrid (common/configs/nrrs/nrrs/2net-simple.json:46).
@@ -42,8 +43,8 @@ __global__ void __launch_bounds__(kTile) k_encode_levels(const __grid_constant__
             levels_features_h<4>(table, a.enc, p, 4 * (int)q, f);
             v = tile::pack8<BF>(f);
         }
-        *reinterpret_cast<uint4*>(a.out + (size_t)t * kEncTileBytes +
-                                  tile::chunk_offset(m, (int)q, 32)) = v;
+        *reinterpret_cast<uint4*>(a.out + (size_t)t * a.tile_bytes +
+                                  tile::chunk_offset(m, (int)q, (int)a.kdim)) = v;
     }
 }
 

@@ -51,6 +51,8 @@ struct TcTrainArgs {
     uint32_t r_off, r_bytes;// RRSNet image
     uint8_t* act;           // tile-blocked BF16 scratch
     Arr x0, hs[kMaxH], dhs[kMaxH], dy, x1, hr[kMaxH], dhr[kMaxH], draw;
+    int32_t pre;            // the hash columns of the x0 tiles are already written (k_encode_levels)
+    float* dxs;             // when set: per-sample hash-lane gradients [n][32] out, no scatter here
     double* part;           // [part_rows][4]: loss_S, V, C per CTA
     uint32_t part_rows;
     uint32_t part_used;     // rows the StatNet and RRSNet-forward grids write
@@ -92,6 +94,28 @@ __device__ __forceinline__ double block_sum_d(double v, double* red) {
     return t;
 }
 
+// Hash-grid gradient of one level of one sample: corners x and x+1 of each (y, z) with one
+// 16-byte reduction when they share an aligned pair of table rows (half the time), two 8-byte
+// ones otherwise. g0, g1: the level's two feature gradients, already divided by the batch size.
+__device__ __forceinline__ void scatter_level(float* table_grad, const LevelDev& L, uint32_t mask,
+                                              const CellCoord& c, float g0, float g1) {
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) {
+        const uint32_t y = c.iy + (k2 & 1), z = c.iz + ((k2 >> 1) & 1);
+        const uint32_t r0 = grid_row(L, mask, c.ix, y, z);
+        const uint32_t r1 = grid_row(L, mask, c.ix + 1, y, z);
+        const float w0 = corner_weight(c, 2 * k2), w1 = corner_weight(c, 2 * k2 + 1);
+        if ((r0 >> 1) == (r1 >> 1)) {
+            float* q = table_grad + 4 * (size_t)(r0 >> 1);
+            if (r0 & 1u) red_add4(q, w1 * g0, w1 * g1, w0 * g0, w0 * g1);
+            else red_add4(q, w0 * g0, w0 * g1, w1 * g0, w1 * g1);
+        } else {
+            red_add2(table_grad + 2 * (size_t)r0, w0 * g0, w0 * g1);
+            red_add2(table_grad + 2 * (size_t)r1, w1 * g0, w1 * g1);
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------------------------
 // Shared-memory plan of the StatNet kernel: the forward weight images (the backward reads them
 // as MN-major operands, i.e. transposed), two [128 x W] tiles that take turns as the input tile,
@@ -124,8 +148,8 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
     uint8_t* sB[2] = {base + S::kB0, base + S::kB1};
     uint8_t* sDY = base + S::kDY;
     uint8_t* sX1 = base + S::kX1;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(base + S::kBar);
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(base + S::kBar);  // weights, mma, x0 tile
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 3);
     __shared__ int s_abort;
     __shared__ double red[4];
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -133,6 +157,7 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
     if (tid == 0) {
         tc::mbar_init(&bars[0], 1);
         tc::mbar_init(&bars[1], 1);
+        tc::mbar_init(&bars[2], 1);
         tc::fence_mbar_init();
         s_abort = 0;
     }
@@ -147,7 +172,7 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
     if (!load_weights(sW, a.tpack, S::kFwd, &bars[0], tid)) s_abort = 1;
     __syncthreads();
     unsigned flags = s_abort ? NRRS_DEV_TIMEOUT : 0u;
-    uint32_t phase = 0;
+    uint32_t phase = 0, xphase = 0;
     const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
 
     // forward images: [W x 64], (H - 1) x [W x W], [16 x W]
@@ -166,8 +191,34 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
         const uint32_t i = t * 128 + tid;
         const bool valid = i < a.n;
         float p[3] = {0.f, 0.f, 0.f};
-        // ---- encode (FP16 table, FP16 tile) into buffer 0 ----
-        if (valid) {
+        bool ok = true;
+        if (a.pre) {
+            // hash columns from k_encode_levels: bring the tile in, add the SH and misc lanes
+            if (tid == 0) {
+                tc::mbar_arrive_expect_tx(&bars[2], 128u * 64u * 2u);
+                tc::bulk_g2s(sB[0], tile_ptr(a.act, a.x0, t), 128u * 64u * 2u, &bars[2]);
+            }
+            float sh[16], misc[16];
+            if (valid) {
+                const size_t i3 = 3 * (size_t)i;
+                sh16(a.v.wi[i3], a.v.wi[i3 + 1], a.v.wi[i3 + 2], sh);
+                misc_lanes(a.v, i, misc);
+                if (!a.dxs) norm_pos(a.enc, a.v.pos, i, p);  // for the in-kernel scatter
+            }
+            ok = tc::mbar_wait(&bars[2], xphase, kSpin);
+            xphase ^= 1u;
+            if (valid) {
+                store_chunk(sB[0], tid, 4, 64, pack8<false>(sh));
+                store_chunk(sB[0], tid, 5, 64, pack8<false>(sh + 8));
+                store_chunk(sB[0], tid, 6, 64, pack8<false>(misc));
+            } else {
+                store_chunk(sB[0], tid, 4, 64, make_uint4(0u, 0u, 0u, 0u));
+                store_chunk(sB[0], tid, 5, 64, make_uint4(0u, 0u, 0u, 0u));
+                store_chunk(sB[0], tid, 6, 64, make_uint4(0u, 0u, 0u, 0u));
+            }
+            store_chunk(sB[0], tid, 7, 64, make_uint4(0u, 0u, 0u, 0u));
+        } else if (valid) {
+            // ---- encode (FP16 table, FP16 tile) into buffer 0 ----
             norm_pos(a.enc, a.v.pos, i, p);
 #pragma unroll 1
             for (int lq = 0; lq < 4; ++lq) {
@@ -198,7 +249,7 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
 
         // ---- StatNet forward ----
         uint32_t mk[H][W / 32];
-        bool ok = mma_layer<kStatIn, W, false>(sB[0], wF[0], tmem, &bars[1], phase, tid);
+        ok &= mma_layer<kStatIn, W, false>(sB[0], wF[0], tmem, &bars[1], phase, tid);
         epilogue_relu_bits<W, false>(trow, sB[1], tid, mk[0]);
         sync_for_mma();
         if (tid == 0) store_tile(tile_ptr(a.act, a.hs[0], t), sB[1], S::kTileW);
@@ -267,29 +318,18 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
         tc::tmem_wait_ld();
         tc::fence_before_sync();
         __syncthreads();  // TMEM free for the next tile
-        if (valid) {
+        if (valid && a.dxs) {
+            // the level-major scatter kernel applies them
+            float4* d = reinterpret_cast<float4*>(a.dxs + 32 * (size_t)i);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) d[k] = make_float4(dx[4 * k], dx[4 * k + 1], dx[4 * k + 2], dx[4 * k + 3]);
+        } else if (valid) {
 #pragma unroll 2
             for (int l = 0; l < kMaxLevels; ++l) {
                 const LevelDev L = a.enc.lv[l];
                 const CellCoord c = cell_of(p, L.res);
-                const float g0 = dx[2 * l] * a.inv_n, g1 = dx[2 * l + 1] * a.inv_n;
-#pragma unroll
-                for (int k2 = 0; k2 < 4; ++k2) {
-                    // corners x and x+1: one 16-byte reduction when they share an aligned pair
-                    // of table rows (half the time), two 8-byte ones otherwise
-                    const uint32_t y = c.iy + (k2 & 1), z = c.iz + ((k2 >> 1) & 1);
-                    const uint32_t r0 = grid_row(L, a.enc.hash_mask, c.ix, y, z);
-                    const uint32_t r1 = grid_row(L, a.enc.hash_mask, c.ix + 1, y, z);
-                    const float w0 = corner_weight(c, 2 * k2), w1 = corner_weight(c, 2 * k2 + 1);
-                    if ((r0 >> 1) == (r1 >> 1)) {
-                        float* q = a.table_grad + 4 * (size_t)(r0 >> 1);
-                        if (r0 & 1u) red_add4(q, w1 * g0, w1 * g1, w0 * g0, w0 * g1);
-                        else red_add4(q, w0 * g0, w0 * g1, w1 * g0, w1 * g1);
-                    } else {
-                        red_add2(a.table_grad + 2 * (size_t)r0, w0 * g0, w0 * g1);
-                        red_add2(a.table_grad + 2 * (size_t)r1, w1 * g0, w1 * g1);
-                    }
-                }
+                scatter_level(a.table_grad, L, a.enc.hash_mask, c, dx[2 * l] * a.inv_n,
+                              dx[2 * l + 1] * a.inv_n);
             }
         }
         if (!ok) s_abort = 1;
@@ -308,6 +348,41 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
         tc::tmem_dealloc(tmem, W);
     }
     (void)flags;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Level-major scatter of the hash-grid gradient (split training): work item (quad q, tile t) in
+// q-major order, so the reductions in flight target the gradient slices of four levels, which
+// stay in L2, instead of the whole table. dxs: the per-sample hash-lane gradients that
+// k_ttc_stat wrote; the 1/n of the batch mean is applied here.
+struct ScatterLvArgs {
+    EncodeParams enc;
+    const float* pos;
+    const float* dxs;
+    float* table_grad;
+    uint32_t n;
+    float inv_n;
+};
+
+__global__ void __launch_bounds__(128) k_scatter_levels(const __grid_constant__ ScatterLvArgs a) {
+    const uint32_t tiles = (a.n + 127) / 128;
+    for (uint32_t w = blockIdx.x; w < 4u * tiles; w += gridDim.x) {
+        const uint32_t q = w / tiles, t = w - q * tiles;
+        const uint32_t i = t * 128 + threadIdx.x;
+        if (i >= a.n) continue;
+        float p[3];
+        norm_pos(a.enc, a.pos, i, p);
+        const float4* d = reinterpret_cast<const float4*>(a.dxs + 32 * (size_t)i + 8 * q);
+        const float4 d0 = d[0], d1 = d[1];
+        const float g[8] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const LevelDev L = a.enc.lv[4 * q + j];
+            const CellCoord c = cell_of(p, L.res);
+            scatter_level(a.table_grad, L, a.enc.hash_mask, c, g[2 * j] * a.inv_n,
+                          g[2 * j + 1] * a.inv_n);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -712,7 +787,9 @@ size_t train_tc_scratch_bytes(const nrrs_config& c, uint32_t n, int sm_count) {
                          16ull * c.rrsnet_width + (uint64_t)(c.rrsnet_hidden - 1) * c.rrsnet_width *
                          c.rrsnet_width + (uint64_t)c.rrsnet_width;
     const uint64_t chunks = (n + kTcChunk - 1) / kTcChunk;
-    return L.act_bytes + sizeof(double) * 4 * (uint64_t)sm_count * 16 + sizeof(float) * chunks * mlp + 1024;
+    // + split mode: the per-sample hash-lane gradients [n][32] FP32
+    return L.act_bytes + sizeof(double) * 4 * (uint64_t)sm_count * 16 + sizeof(float) * chunks * mlp +
+           sizeof(float) * 32ull * n + 1024;
 }
 
 cudaError_t launch_wreduce(const float* partial, uint32_t chunks, uint32_t total, float* grad,
@@ -728,7 +805,11 @@ int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint3
     const uint32_t part_rows = (uint32_t)ctx->sm_count * 16;
     float* partial = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(part) +
                                               sizeof(double) * 4 * (size_t)part_rows);
+    const uint64_t chunks_max = (c.max_train + kTcChunk - 1) / kTcChunk;
+    float* dxs = reinterpret_cast<float*>(
+        (reinterpret_cast<uintptr_t>(partial + chunks_max * mlp) + 15u) & ~uintptr_t(15));
     const bool train_rrs = c.step >= 3;
+    const bool split = ctx->train_split != 0;
     cudaError_t e = cudaMemsetAsync(ctx->grads, 0, sizeof(float) * ctx->n_params, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(part, 0, sizeof(double) * 4 * part_rows, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(partial, 0, sizeof(float) * chunks * mlp, s);
@@ -762,8 +843,48 @@ int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint3
     a.part = part;
     a.part_rows = part_rows;
     a.loss_out = loss_dev ? loss_dev : ctx->loss_dev;
+    if (split) {
+        // hash columns of the x0 tiles, level-major (FP16, the StatNet training precision)
+        EncodeLvArgs ea{};
+        ea.enc = ctx->enc;
+        ea.segs.n = 1;
+        ea.segs.s[0].offset = 0;
+        ea.segs.s[0].count = n;
+        ea.segs.s[0].tile_start = 0;
+        ea.segs.total_tiles = (n + 127) / 128;
+        ea.pos = v.pos;
+        ea.table_h = ctx->table_h;
+        ea.out = act + L.x0.off;
+        ea.tile_bytes = 128u * 64u * 2u;
+        ea.kdim = 64;
+        {
+            ProfScope ps(ctx, NRRS_KERNEL_TRAIN_ENCODE, s);
+            e = launch_encode_levels(ea, false, ctx->sm_count, s);
+        }
+        if (e != cudaSuccess) {
+            ctx->last_error = std::string("training encoding launch: ") + cudaGetErrorString(e);
+            return NRRS_ERR_CUDA;
+        }
+        a.pre = 1;
+        a.dxs = dxs;
+    }
     if (W == 64) e = H == 2 ? launch_ttc<64, 2>(ctx, a, s, train_rrs) : launch_ttc<64, 3>(ctx, a, s, train_rrs);
     else e = H == 2 ? launch_ttc<128, 2>(ctx, a, s, train_rrs) : launch_ttc<128, 3>(ctx, a, s, train_rrs);
+    if (e == cudaSuccess && split) {
+        ScatterLvArgs sa{};
+        sa.enc = ctx->enc;
+        sa.pos = v.pos;
+        sa.dxs = dxs;
+        sa.table_grad = ctx->grads;
+        sa.n = n;
+        sa.inv_n = a.inv_n;
+        const uint32_t items = 4u * ((n + 127) / 128);
+        uint32_t g = (uint32_t)(ctx->sm_count * resident_ctas((const void*)k_scatter_levels, 128, 0, 16));
+        if (g > items) g = items;
+        ProfScope ps(ctx, NRRS_KERNEL_TRAIN_SCATTER, s);
+        if (g) k_scatter_levels<<<g, 128, 0, s>>>(sa);
+        e = cudaGetLastError();
+    }
     if (e != cudaSuccess) {
         ctx->last_error = std::string("tensor-core train launch: ") + cudaGetErrorString(e);
         return NRRS_ERR_CUDA;

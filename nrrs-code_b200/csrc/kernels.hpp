@@ -62,7 +62,9 @@ struct EncodeLvArgs {
     SegmentTable segs;
     const float* pos;
     const __half* table_h;
-    uint8_t* out;                 // total_tiles x kEncTileBytes
+    uint8_t* out;                 // total_tiles x tile_bytes
+    uint32_t tile_bytes;          // kEncTileBytes (inference) or the [128 x 64] training input tile
+    uint32_t kdim;                // K of the tile layout: 32 (inference) or 64 (training input)
 };
 cudaError_t launch_encode_levels(const EncodeLvArgs& a, bool bf, int sm_count, cudaStream_t s);
 

@@ -205,6 +205,8 @@ int run_infer(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const SegmentTable& segs,
         ea.pos = a.v.pos;
         ea.table_h = ctx->table_h;
         ea.out = ctx->enc_tiles;
+        ea.tile_bytes = kEncTileBytes;
+        ea.kdim = 32;
         {
             ProfScope ps(ctx, NRRS_KERNEL_ENCODE, s);
             e = launch_encode_levels(ea, c.precision == NRRS_PREC_BF16, ctx->sm_count, s);
@@ -805,7 +807,8 @@ int32_t nrrs_last_infer_grid(const nrrs_ctx* ctx) { return ctx ? ctx->last_infer
 const char* nrrs_kernel_name(int32_t kind) {
     static const char* names[NRRS_KERNEL_KINDS] = {
         "infer_fp32", "infer_tc", "sum", "decide", "pack_weights", "table_half",
-        "train_statnet", "train_rrsnet", "train_wgrad", "train_reduce", "adam", "encode"};
+        "train_statnet", "train_rrsnet", "train_wgrad", "train_reduce", "adam", "encode",
+        "train_scatter", "train_encode"};
     return (kind >= 0 && kind < NRRS_KERNEL_KINDS) ? names[kind] : "unknown";
 }
 
@@ -884,6 +887,18 @@ int nrrs_set_infer_split(nrrs_ctx* ctx, int32_t split) {
     if (infer_max_ctas(c.statnet_width, c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden,
                        c.precision, ctx->tc_wgs, split != 0) <= 0)
         ctx->tc_wgs = 1;
+    return NRRS_OK;
+}
+
+int nrrs_set_train_split(nrrs_ctx* ctx, int32_t split) {
+    if (!ctx || (split != 0 && split != 1)) return NRRS_ERR_INVALID_ARG;
+    ctx->train_split = split;
+    return NRRS_OK;
+}
+
+int nrrs_get_train_split(const nrrs_ctx* ctx, int32_t* split) {
+    if (!ctx || !split) return NRRS_ERR_INVALID_ARG;
+    *split = ctx->train_split;
     return NRRS_OK;
 }
 

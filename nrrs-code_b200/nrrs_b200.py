@@ -139,6 +139,8 @@ _SIGS = {
     "nrrs_get_launch_shape": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "nrrs_set_infer_split": (C.c_int, [C.c_void_p, C.c_int32]),
     "nrrs_get_infer_split": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "nrrs_set_train_split": (C.c_int, [C.c_void_p, C.c_int32]),
+    "nrrs_get_train_split": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "nrrs_graph_capture_batched": (C.c_int, [C.c_void_p, C.POINTER(VertexSoA), C.c_void_p,
                                              C.POINTER(Segment), C.c_int32,
                                              C.POINTER(DecideParams), C.c_void_p, C.c_void_p,
@@ -154,7 +156,8 @@ _SIGS = {
 }
 
 KERNEL_KINDS = ("infer_fp32", "infer_tc", "sum", "decide", "pack_weights", "table_half",
-                "train_statnet", "train_rrsnet", "train_wgrad", "train_reduce", "adam", "encode")
+                "train_statnet", "train_rrsnet", "train_wgrad", "train_reduce", "adam", "encode",
+                "train_scatter", "train_encode")
 
 
 def lib():
@@ -429,6 +432,15 @@ class NRRSNetwork:
     def set_infer_split(self, split: bool):
         """0 = fused inference, 1 = level-major encoding kernel + MLP kernel (large tables)."""
         self._check(lib().nrrs_set_infer_split(self._h, int(bool(split))))
+
+    def set_train_split(self, split: bool):
+        """1 = level-major encoding, StatNet kernel, level-major scatter; 0 = one fused kernel."""
+        self._check(lib().nrrs_set_train_split(self._h, int(bool(split))))
+
+    def train_split(self) -> int:
+        v = C.c_int32()
+        self._check(lib().nrrs_get_train_split(self._h, C.byref(v)))
+        return int(v.value)
 
     def infer_split(self) -> int:
         v = C.c_int32()

@@ -151,3 +151,33 @@ def test_mixed_loss_decreases_and_matches_fp32_trajectory():
     assert traj[1][-1][0] == pytest.approx(traj[0][-1][0], rel=5e-2)
     for net in nets:
         net.close()
+
+
+@pytest.mark.parametrize("shape", ["w64h2", "w128h3"])
+def test_split_training_equals_fused(shape):
+    """the level-major encoding + StatNet kernel + level-major scatter gives the fused kernel's
+    losses exactly and its gradients up to the order of the FP32 additions"""
+    kw, mlp_scale, _ = MIXED_SHAPES[shape]
+    net = make_net(precision=nb.PREC_FP16, max_train=1 << 14, step=3, log2_hashmap_size=16, **kw)
+    p0 = random_params(net, 24, table_scale=0.5, mlp_scale=mlp_scale)
+    n = 9000
+    v = nb.synth(36, n)
+    torch = torch_cuda()
+    d = upload(v)
+    out = {}
+    for split in (1, 0):
+        net.set_train_split(split)
+        assert net.train_split() == split
+        net.set_params(p0)
+        loss = torch.zeros(2, dtype=torch.float64, device="cuda")
+        net.trainGrads(soa(d), d["target"], n, loss, stream())
+        torch.cuda.synchronize()
+        out[split] = (loss.cpu().numpy(), net.get_grads().astype(np.float64))
+    assert np.array_equal(out[0][0], out[1][0])
+    ntab, nst, nrr = net.param_layout()
+    for sl in (slice(0, ntab), slice(ntab, ntab + nst), slice(ntab + nst, ntab + nst + nrr)):
+        e = rel_err(out[1][1][sl], out[0][1][sl])
+        assert e < 1e-5, (shape, sl, e)
+    rc, flags = net.device_status(stream())
+    assert rc == nb.OK and flags == 0
+    net.close()
