@@ -319,10 +319,11 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
         tc::fence_before_sync();
         __syncthreads();  // TMEM free for the next tile
         if (valid && a.dxs) {
-            // the level-major scatter kernel applies them
-            float4* d = reinterpret_cast<float4*>(a.dxs + 32 * (size_t)i);
+            // the level-major scatter kernel applies them; stored level-major ([16][n] pairs),
+            // so that kernel reads each level's gradients coalesced
+            float2* d = reinterpret_cast<float2*>(a.dxs);
 #pragma unroll
-            for (int k = 0; k < 8; ++k) d[k] = make_float4(dx[4 * k], dx[4 * k + 1], dx[4 * k + 2], dx[4 * k + 3]);
+            for (int l = 0; l < kMaxLevels; ++l) d[(size_t)l * a.n + i] = make_float2(dx[2 * l], dx[2 * l + 1]);
         } else if (valid) {
 #pragma unroll 2
             for (int l = 0; l < kMaxLevels; ++l) {
@@ -351,10 +352,11 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
 }
 
 // ---------------------------------------------------------------------------------------------
-// Level-major scatter of the hash-grid gradient (split training): work item (quad q, tile t) in
-// q-major order, so the reductions in flight target the gradient slices of four levels, which
-// stay in L2, instead of the whole table. dxs: the per-sample hash-lane gradients that
-// k_ttc_stat wrote; the 1/n of the batch mean is applied here.
+// Level-major scatter of the hash-grid gradient (split training): work item (level l, tile t) in
+// l-major order, so the reductions in flight target the gradient slice of one level (at most
+// 2^T x 8 bytes), which stays in L2, instead of the whole table. dxs: the per-sample hash-lane
+// gradients that k_ttc_stat wrote, [16][n] float pairs; the 1/n of the batch mean is applied
+// here. Levels [level_begin, level_end) of the launch.
 struct ScatterLvArgs {
     EncodeParams enc;
     const float* pos;
@@ -362,26 +364,24 @@ struct ScatterLvArgs {
     float* table_grad;
     uint32_t n;
     float inv_n;
+    uint32_t level_begin, level_end;
 };
 
 __global__ void __launch_bounds__(128) k_scatter_levels(const __grid_constant__ ScatterLvArgs a) {
     const uint32_t tiles = (a.n + 127) / 128;
-    for (uint32_t w = blockIdx.x; w < 4u * tiles; w += gridDim.x) {
-        const uint32_t q = w / tiles, t = w - q * tiles;
+    const uint32_t items = (a.level_end - a.level_begin) * tiles;
+    const float2* d = reinterpret_cast<const float2*>(a.dxs);
+    for (uint32_t w = blockIdx.x; w < items; w += gridDim.x) {
+        const uint32_t lq = w / tiles, t = w - lq * tiles;
+        const uint32_t l = a.level_begin + lq;
         const uint32_t i = t * 128 + threadIdx.x;
         if (i >= a.n) continue;
         float p[3];
         norm_pos(a.enc, a.pos, i, p);
-        const float4* d = reinterpret_cast<const float4*>(a.dxs + 32 * (size_t)i + 8 * q);
-        const float4 d0 = d[0], d1 = d[1];
-        const float g[8] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w};
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const LevelDev L = a.enc.lv[4 * q + j];
-            const CellCoord c = cell_of(p, L.res);
-            scatter_level(a.table_grad, L, a.enc.hash_mask, c, g[2 * j] * a.inv_n,
-                          g[2 * j + 1] * a.inv_n);
-        }
+        const float2 g = d[(size_t)l * a.n + i];
+        const LevelDev L = a.enc.lv[l];
+        const CellCoord c = cell_of(p, L.res);
+        scatter_level(a.table_grad, L, a.enc.hash_mask, c, g.x * a.inv_n, g.y * a.inv_n);
     }
 }
 
@@ -878,7 +878,9 @@ int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint3
         sa.table_grad = ctx->grads;
         sa.n = n;
         sa.inv_n = a.inv_n;
-        const uint32_t items = 4u * ((n + 127) / 128);
+        sa.level_begin = 0;
+        sa.level_end = kMaxLevels;
+        const uint32_t items = kMaxLevels * ((n + 127) / 128);
         uint32_t g = (uint32_t)(ctx->sm_count * resident_ctas((const void*)k_scatter_levels, 128, 0, 16));
         if (g > items) g = items;
         ProfScope ps(ctx, NRRS_KERNEL_TRAIN_SCATTER, s);
