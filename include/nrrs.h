@@ -265,7 +265,8 @@ int nrrs_get_device_status(nrrs_ctx* ctx, uint32_t* flags, void* stream);
 
 /* ---- launch shape and autotuning (no counterpart in the reference, whose launches come from
  *      the occupancy API, commoncudautilshost.cpp:10-21). The inference kernel's shape is
- *      CTAs per SM x warpgroups per CTA (tcgen05 path; the FP32 path uses CTAs per SM only).
+ *      CTAs per SM x warpgroups per CTA (tcgen05 path: 1, 2 or 4, one 128-vertex tile in
+ *      flight each, as the shared memory allows; the FP32 path uses CTAs per SM only).
  *      nrrs_autotune times every admissible shape on n synthetic vertices, keeps the fastest in
  *      the context and, with a cache path, reuses or records the choice in a JSON file keyed by
  *      device name, network shape and precision. report (may be NULL) receives a JSON summary.
@@ -277,8 +278,11 @@ int nrrs_get_launch_shape(const nrrs_ctx* ctx, int32_t* ctas_per_sm, int32_t* wa
 /* Inference mode of the tensor-core path (the autotuner's third knob): 0 = fused (the MLP kernel
  * gathers the hash-grid corners itself), 1 = split (a level-major encoding kernel writes every
  * tile's hash features to HBM, four levels at a time so that the table slices in use stay in
- * L2, and the MLP kernel bulk-loads them; for tables larger than L2). Both modes give
- * bit-identical results. Selecting split allocates (max_queue/128 + 17) feature tiles of 8 KB;
+ * L2, and the MLP kernel bulk-loads them; for tables larger than L2), 2 = split with the MLP
+ * in two kernels (StatNet, which writes each tile's RRSNet input to HBM, then RRSNet; each
+ * holds only its own weights, so more tiles are in flight per SM; with ADRRS factors only the
+ * StatNet kernel runs). All modes give bit-identical results. Selecting split allocates
+ * (max_queue/128 + 17) feature tiles of 8 KB, and mode 2 as many RRSNet input tiles of 4 KB;
  * not available for the FP32 path. */
 int nrrs_set_infer_split(nrrs_ctx* ctx, int32_t split);
 int nrrs_get_infer_split(const nrrs_ctx* ctx, int32_t* split);
@@ -312,7 +316,8 @@ typedef enum {
     NRRS_KERNEL_DECIDE = 3, NRRS_KERNEL_PACK = 4, NRRS_KERNEL_TABLE_HALF = 5,
     NRRS_KERNEL_TRAIN_STAT = 6, NRRS_KERNEL_TRAIN_RRS = 7, NRRS_KERNEL_TRAIN_WGRAD = 8,
     NRRS_KERNEL_TRAIN_REDUCE = 9, NRRS_KERNEL_ADAM = 10, NRRS_KERNEL_ENCODE = 11,
-    NRRS_KERNEL_TRAIN_SCATTER = 12, NRRS_KERNEL_TRAIN_ENCODE = 13, NRRS_KERNEL_KINDS = 14
+    NRRS_KERNEL_TRAIN_SCATTER = 12, NRRS_KERNEL_TRAIN_ENCODE = 13, NRRS_KERNEL_INFER_RRS = 14,
+    NRRS_KERNEL_KINDS = 15
 } nrrs_kernel_kind;
 uint64_t nrrs_launch_count(const nrrs_ctx* ctx);
 /* grid (CTAs) of the last inference launch: SMs x resident CTAs per SM */

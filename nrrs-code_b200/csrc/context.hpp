@@ -64,6 +64,7 @@ struct nrrs_ctx {
     int train_split = 1;         // training mode of the tcgen05 path: 0 fused, 1 split
     uint8_t* enc_tiles = nullptr;  // split mode: hash-feature tiles (kEncTileBytes each)
     uint32_t enc_tiles_cap = 0;
+    uint8_t* x1_tiles = nullptr;   // split mode 2: RRSNet input tiles (kX1TileBytes each)
     nrrs::Profiler prof;
     std::string last_error;
 };

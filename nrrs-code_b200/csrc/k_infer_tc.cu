@@ -39,27 +39,33 @@ struct PackedNet {
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
 constexpr int tmem_cols(int w) { return w <= 32 ? 32 : (w <= 64 ? 64 : (w <= 128 ? 128 : 256)); }
 
-template <int WS, int HS, int WR, int HR, int WGS, bool PRE>
+// PART: 0 = both networks in one kernel; 1 = StatNet only (writes the RRSNet input tiles);
+// 2 = RRSNet only (reads them). Each kernel holds only the weights of the networks it runs.
+template <int WS, int HS, int WR, int HR, int WGS, bool PRE, int PART = 0>
 struct TcShape {
     static constexpr int kStatElems = PackedNet<WS, HS, kStatIn>::kElems;
     static constexpr int kRrsElems = PackedNet<WR, HR, kRrsIn>::kElems;
-    static constexpr uint32_t kWBytes = (uint32_t)(kStatElems + kRrsElems) * 2u;
-    static constexpr int kKMax = cmax(64, cmax(WS, WR));
+    static constexpr uint32_t kWBytes =
+        (uint32_t)(PART == 0 ? kStatElems + kRrsElems : (PART == 1 ? kStatElems : kRrsElems)) * 2u;
+    static constexpr uint32_t kWSrcOff = PART == 2 ? (uint32_t)kStatElems * 2u : 0u;
+    static constexpr int kKMax =
+        PART == 0 ? cmax(64, cmax(WS, WR)) : (PART == 1 ? cmax(64, WS) : cmax(16, WR));
     static constexpr uint32_t kABytes = 128u * kKMax * 2u;
-    static constexpr uint32_t kColsWg = (uint32_t)tmem_cols(cmax(WS, WR));
+    static constexpr uint32_t kColsWg =
+        (uint32_t)tmem_cols(PART == 0 ? cmax(WS, WR) : (PART == 1 ? WS : WR));
     static constexpr uint32_t kCols = kColsWg * WGS;
     static constexpr uint32_t kAOff = (kWBytes + 1023u) / 1024u * 1024u;
     // split mode: per warpgroup a hash-feature block and an SH/misc block, kept apart from the
     // activation tile so the next tile's features can be fetched during the MLP chain; where
-    // that does not fit (128-wide, two warpgroups) the blocks are the first 16 KB of the
-    // warpgroup's activation tile and the copy is issued when the tile is free again
+    // that does not fit the blocks are the first 16 KB of the warpgroup's activation tile and
+    // the copy is issued when the tile is free again
     static constexpr uint32_t kSepBytes = 2u * kEncTileBytes;
     static constexpr bool kShare =
-        PRE && 1024 + kAOff + WGS * (kABytes + kSepBytes) + 64 > 232448u;
-    static constexpr uint32_t kHBytes = PRE && !kShare ? kSepBytes : 0u;
+        PRE && PART != 2 && 1024 + kAOff + WGS * (kABytes + kSepBytes) + 64 > 232448u;
+    static constexpr uint32_t kHBytes = PRE && PART != 2 && !kShare ? kSepBytes : 0u;
     static constexpr uint32_t kHOff = kAOff + WGS * kABytes;
     static constexpr uint32_t kBarOff = kHOff + WGS * kHBytes;
-    static constexpr size_t kSmem = 1024 + kBarOff + 64;
+    static constexpr size_t kSmem = 1024 + kBarOff + 96;
     static_assert(!kShare || kABytes >= kSepBytes, "feature blocks inside the activation tile");
 };
 
@@ -165,15 +171,16 @@ __device__ __forceinline__ bool tc_layer(const uint8_t* sA, const uint8_t* sWl, 
     return ok;
 }
 
-template <int WS, int HS, int WR, int HR, bool BF, int WGS, bool PRE>
+template <int WS, int HS, int WR, int HR, bool BF, int WGS, bool PRE, int PART>
 __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
     k_infer_tc(const __grid_constant__ InferArgs a) {
-    using S = TcShape<WS, HS, WR, HR, WGS, PRE>;
+    using S = TcShape<WS, HS, WR, HR, WGS, PRE, PART>;
+    constexpr bool kStat = PART != 2, kRrs = PART != 1;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* base = reinterpret_cast<uint8_t*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023u) & ~uintptr_t(1023));
     uint8_t* sW = base;
-    // [0] weights, [1+wg] mma, [1+WGS+wg] feature block (split mode)
+    // [0] weights, [1+wg] mma, [1+WGS+wg] copies into the tile (feature block or RRSNet input)
     uint64_t* bars = reinterpret_cast<uint64_t*>(base + S::kBarOff);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 1 + 2 * WGS);
     __shared__ int s_abort[WGS];
@@ -200,7 +207,7 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
     const uint32_t tmem = *tslot + (uint32_t)wg * S::kColsWg;
     if (tid == 0) {
         tc::mbar_arrive_expect_tx(&bars[0], S::kWBytes);
-        const uint8_t* src = reinterpret_cast<const uint8_t*>(a.wpack);
+        const uint8_t* src = reinterpret_cast<const uint8_t*>(a.wpack) + S::kWSrcOff;
         for (uint32_t off = 0; off < S::kWBytes; off += 32768u) {
             const uint32_t bytes = S::kWBytes - off < 32768u ? S::kWBytes - off : 32768u;
             tc::bulk_g2s(sW + off, src + off, bytes, &bars[0]);
@@ -215,14 +222,16 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
     // warp w of a warpgroup reads TMEM lanes 32*(w % 4) .. +31, i.e. rows of its own threads
     const uint32_t trow = tmem + ((uint32_t)((warp & 3) * 32) << 16);
 
+    // weight images in this kernel's shared copy: StatNet then RRSNet (each only if run here)
     const uint8_t* wS0 = sW;
     const uint8_t* wSh = wS0 + WS * kStatIn * 2;
     const uint8_t* wSo = wSh + (HS - 1) * WS * WS * 2;
-    const uint8_t* wR0 = wSo + 16 * WS * 2;
+    const uint8_t* wR0 = kStat ? wSo + 16 * WS * 2 : sW;
     const uint8_t* wRh = wR0 + WR * kRrsIn * 2;
     const uint8_t* wRo = wRh + (HR - 1) * WR * WR * 2;
 
-    // split mode: feature-block copies, one in flight at most per warpgroup
+    // copies into the tile: feature blocks (split modes) or RRSNet input tiles (PART 2); one in
+    // flight at most per warpgroup
     uint64_t* hbar = &bars[1 + WGS + wg];
     uint32_t hphase = 0;
     bool h_pending = false;
@@ -234,7 +243,7 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
         }
         h_pending = true;
     };
-    if (PRE && !S::kShare && t0 < a.segs.total_tiles && !flags) fetch_features(t0);
+    if (PRE && kStat && !S::kShare && t0 < a.segs.total_tiles && !flags) fetch_features(t0);
 
     for (uint32_t t = t0; t < a.segs.total_tiles && !flags; t += tstride) {
         const int si = find_segment(a.segs, t);
@@ -243,87 +252,117 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
         const bool valid = i < sg.offset + sg.count;
         // the glue's and the factor's inputs, in flight during the StatNet chain
         VertexAux aux{};
-        if (valid) aux = load_aux(a.v, i);
+        if (kStat && valid) aux = load_aux(a.v, i);
 
         bool ok = true;
-        // shared layout: the previous tile's chain has finished with the activation tile
-        if (PRE && S::kShare) fetch_features(t);
-        if constexpr (PRE) {
-            if (valid) sh_misc_row_tc<BF>(a, i, sS, ltid);
-            else zero_row(sS, ltid, 32);
-            ok = tc::mbar_wait(hbar, hphase, kSpin);
-            hphase ^= 1u;
-            h_pending = false;
-        } else {
-            if (valid) encode_row_tc<BF>(a, i, sA, ltid);
-            else zero_row(sA, ltid, 64);
+        float y[16];
+        if constexpr (!kStat) {
+#pragma unroll
+            for (int k = 0; k < 16; ++k) y[k] = 0.f;  // not used by the RRSNet factor
         }
-        wg_sync_for_mma(wg);
+        if constexpr (kStat) {
+            // the previous tile's RRSNet-input store (PART 1) has finished reading the A tile
+            if (PART == 1 && ltid == 0) tc::bulk_wait_read();
+            // shared layout: the previous tile's chain has finished with the activation tile
+            if (PRE && S::kShare) fetch_features(t);
+            if constexpr (PRE) {
+                if (valid) sh_misc_row_tc<BF>(a, i, sS, ltid);
+                else zero_row(sS, ltid, 32);
+                ok = tc::mbar_wait(hbar, hphase, kSpin);
+                hphase ^= 1u;
+                h_pending = false;
+            } else {
+                if (valid) encode_row_tc<BF>(a, i, sA, ltid);
+                else zero_row(sA, ltid, 64);
+            }
+            wg_sync_for_mma(wg);
 
-        // ---- StatNet ----
-        if constexpr (PRE) {
-            ok &= tc_layer0_pre<WS, BF>(sH, sS, wS0, tmem, mbar, phase, ltid);
-            // the first layer has read the block: bring in the next tile's features
-            if (!S::kShare && ok && t + tstride < a.segs.total_tiles) fetch_features(t + tstride);
-        } else {
-            ok &= tc_layer<kStatIn, WS, BF>(sA, wS0, tmem, mbar, phase, ltid);
-        }
-        epilogue_relu<WS, BF>(trow, sA, ltid);
-        wg_sync_for_mma(wg);
-#pragma unroll 1
-        for (int h = 1; h < HS; ++h) {
-            ok &= tc_layer<WS, WS, BF>(sA, wSh + (h - 1) * WS * WS * 2, tmem, mbar, phase, ltid);
+            // ---- StatNet ----
+            if constexpr (PRE) {
+                ok &= tc_layer0_pre<WS, BF>(sH, sS, wS0, tmem, mbar, phase, ltid);
+                // the first layer has read the block: bring in the next tile's features
+                if (!S::kShare && ok && t + tstride < a.segs.total_tiles) fetch_features(t + tstride);
+            } else {
+                ok &= tc_layer<kStatIn, WS, BF>(sA, wS0, tmem, mbar, phase, ltid);
+            }
             epilogue_relu<WS, BF>(trow, sA, ltid);
             wg_sync_for_mma(wg);
-        }
-        ok &= tc_layer<WS, 16, BF>(sA, wSo, tmem, mbar, phase, ltid);
-        float y[16];
-        tc::tmem_ld16(trow, y);
-        tc::tmem_wait_ld();
-
-        // ---- glue -> RRSNet input (K = 16) ----
-        float x1[16];
-        if (valid) {
-            glue16_aux(a.fp, y, aux, x1);
-        } else {
-#pragma unroll
-            for (int k = 0; k < 16; ++k) x1[k] = 0.f;
-        }
-        store_chunk(sA, ltid, 0, 16, pack8<BF>(x1));
-        store_chunk(sA, ltid, 1, 16, pack8<BF>(x1 + 8));
-        wg_sync_for_mma(wg);
-
-        // ---- RRSNet ----
-        ok &= tc_layer<kRrsIn, WR, BF>(sA, wR0, tmem, mbar, phase, ltid);
-        epilogue_relu<WR, BF>(trow, sA, ltid);
-        wg_sync_for_mma(wg);
 #pragma unroll 1
-        for (int h = 1; h < HR; ++h) {
-            ok &= tc_layer<WR, WR, BF>(sA, wRh + (h - 1) * WR * WR * 2, tmem, mbar, phase, ltid);
+            for (int h = 1; h < HS; ++h) {
+                ok &= tc_layer<WS, WS, BF>(sA, wSh + (h - 1) * WS * WS * 2, tmem, mbar, phase, ltid);
+                epilogue_relu<WS, BF>(trow, sA, ltid);
+                wg_sync_for_mma(wg);
+            }
+            ok &= tc_layer<WS, 16, BF>(sA, wSo, tmem, mbar, phase, ltid);
+            tc::tmem_ld16(trow, y);
+            tc::tmem_wait_ld();
+
+            // ---- glue -> RRSNet input (K = 16) ----
+            float x1[16];
+            if (valid) {
+                glue16_aux(a.fp, y, aux, x1);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 16; ++k) x1[k] = 0.f;
+            }
+            store_chunk(sA, ltid, 0, 16, pack8<BF>(x1));
+            store_chunk(sA, ltid, 1, 16, pack8<BF>(x1 + 8));
+            wg_sync_for_mma(wg);
+            if (PART == 1 && ltid == 0) {
+                tc::bulk_s2g(a.x1_tiles + (size_t)t * kX1TileBytes, sA, kX1TileBytes);
+                tc::bulk_commit();
+            }
+        } else {
+            // PART 2: this tile's RRSNet input from the StatNet kernel
+            if (ltid == 0) {
+                tc::mbar_arrive_expect_tx(hbar, kX1TileBytes);
+                tc::bulk_g2s(sA, a.x1_tiles + (size_t)t * kX1TileBytes, kX1TileBytes, hbar);
+            }
+            ok = tc::mbar_wait(hbar, hphase, kSpin);
+            hphase ^= 1u;
+            tc::fence_after_sync();
+        }
+
+        float r[16];
+        if constexpr (kRrs) {
+            // ---- RRSNet ----
+            ok &= tc_layer<kRrsIn, WR, BF>(sA, wR0, tmem, mbar, phase, ltid);
             epilogue_relu<WR, BF>(trow, sA, ltid);
             wg_sync_for_mma(wg);
+#pragma unroll 1
+            for (int h = 1; h < HR; ++h) {
+                ok &= tc_layer<WR, WR, BF>(sA, wRh + (h - 1) * WR * WR * 2, tmem, mbar, phase, ltid);
+                epilogue_relu<WR, BF>(trow, sA, ltid);
+                wg_sync_for_mma(wg);
+            }
+            ok &= tc_layer<WR, 16, BF>(sA, wRo, tmem, mbar, phase, ltid);
+            tc::tmem_ld16(trow, r);
+            tc::tmem_wait_ld();
+        } else {
+            r[0] = 0.f;
         }
-        ok &= tc_layer<WR, 16, BF>(sA, wRo, tmem, mbar, phase, ltid);
-        float r[16];
-        tc::tmem_ld16(trow, r);
-        tc::tmem_wait_ld();
         tc::fence_before_sync();
         wg_sync(wg);  // TMEM columns and A tile free for the next tile
 
         if (!ok) flags |= NRRS_DEV_TIMEOUT;
+        // the factor: here when this kernel has what it needs (PART 1 only for ADRRS factors,
+        // whose RRSNet kernel is not launched)
+        const bool factor_here = PART != 1 || a.fp.source == NRRS_FACTOR_ADRRS;
         long long term = 0;
         if (valid) {
-            const float rrs = rrs_factor_aux(a.fp, y, r[0], aux);
-            if (a.stats) {
+            if (kStat && a.stats) {
                 a.stats[3 * (size_t)i] = y[0];
                 a.stats[3 * (size_t)i + 1] = y[1];
                 a.stats[3 * (size_t)i + 2] = y[2];
             }
-            a.rrs[i] = rrs;
-            if (a.scr || a.ext_acc)
-                term = fixed_term(a.fp, rrs, a.scr ? &a.scr->status : &g_dummy_status);
+            if (factor_here) {
+                const float rrs = rrs_factor_aux(a.fp, y, r[0], aux);
+                a.rrs[i] = rrs;
+                if (a.scr || a.ext_acc)
+                    term = fixed_term(a.fp, rrs, a.scr ? &a.scr->status : &g_dummy_status);
+            }
         }
-        if (a.scr || a.ext_acc) {
+        if (factor_here && (a.scr || a.ext_acc)) {
             term = warp_sum_ll(term);
             if ((tid & 31) == 0 && term != 0)
                 atomicAdd(a.ext_acc ? a.ext_acc : &a.scr->sum_acc[si], (unsigned long long)term);
@@ -334,8 +373,10 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
         if (s_abort[wg]) flags |= NRRS_DEV_TIMEOUT;
     }
 
-    // a copy still in flight (the loop ended early) lands before the CTA leaves
-    if (PRE && h_pending && ltid == 0 && !tc::mbar_wait(hbar, hphase, kSpin)) flags |= NRRS_DEV_TIMEOUT;
+    // a copy still in flight (the loop ended early) lands before the CTA leaves; the RRSNet
+    // input stores are complete
+    if (h_pending && ltid == 0 && !tc::mbar_wait(hbar, hphase, kSpin)) flags |= NRRS_DEV_TIMEOUT;
+    if (PART == 1 && ltid == 0) tc::bulk_wait_all();
     if (flags && a.scr) atomicOr(&a.scr->status, flags);
     tc::fence_before_sync();
     __syncthreads();
@@ -345,11 +386,11 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
     }
 }
 
-template <int WS, int HS, int WR, int HR, bool BF, int WGS, bool PRE>
+template <int WS, int HS, int WR, int HR, bool BF, int WGS, bool PRE, int PART>
 cudaError_t launch_tc(const InferArgs& a, int sm_count, int ctas_per_sm, cudaStream_t s) {
-    using S = TcShape<WS, HS, WR, HR, WGS, PRE>;
+    using S = TcShape<WS, HS, WR, HR, WGS, PRE, PART>;
     if (S::kSmem > 232448) return cudaErrorInvalidConfiguration;
-    auto kern = k_infer_tc<WS, HS, WR, HR, BF, WGS, PRE>;
+    auto kern = k_infer_tc<WS, HS, WR, HR, BF, WGS, PRE, PART>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)S::kSmem);
     if (e != cudaSuccess) return e;
@@ -365,39 +406,68 @@ cudaError_t launch_tc(const InferArgs& a, int sm_count, int ctas_per_sm, cudaStr
     return cudaGetLastError();
 }
 
+// part: 0 both networks (fused or split-1), 1 StatNet only, 2 RRSNet only (split-2)
 template <int WS, int HS, int WR, int HR, bool BF>
-cudaError_t launch_wgs(const InferArgs& a, int sm_count, int ctas_per_sm, int wgs,
+cudaError_t launch_wgs(const InferArgs& a, int sm_count, int ctas_per_sm, int wgs, int part,
                        cudaStream_t s) {
-    if (a.enc_tiles) {
-        if (wgs == 2) return launch_tc<WS, HS, WR, HR, BF, 2, true>(a, sm_count, ctas_per_sm, s);
-        return launch_tc<WS, HS, WR, HR, BF, 1, true>(a, sm_count, ctas_per_sm, s);
+    if (part == 1) {
+        if (wgs == 4) return launch_tc<WS, HS, WR, HR, BF, 4, true, 1>(a, sm_count, ctas_per_sm, s);
+        if (wgs == 2) return launch_tc<WS, HS, WR, HR, BF, 2, true, 1>(a, sm_count, ctas_per_sm, s);
+        return launch_tc<WS, HS, WR, HR, BF, 1, true, 1>(a, sm_count, ctas_per_sm, s);
     }
-    if (wgs == 2) return launch_tc<WS, HS, WR, HR, BF, 2, false>(a, sm_count, ctas_per_sm, s);
-    return launch_tc<WS, HS, WR, HR, BF, 1, false>(a, sm_count, ctas_per_sm, s);
+    if (part == 2) {
+        if (wgs == 4) return launch_tc<WS, HS, WR, HR, BF, 4, true, 2>(a, sm_count, ctas_per_sm, s);
+        if (wgs == 2) return launch_tc<WS, HS, WR, HR, BF, 2, true, 2>(a, sm_count, ctas_per_sm, s);
+        return launch_tc<WS, HS, WR, HR, BF, 1, true, 2>(a, sm_count, ctas_per_sm, s);
+    }
+    if (a.enc_tiles) {
+        if (wgs == 2) return launch_tc<WS, HS, WR, HR, BF, 2, true, 0>(a, sm_count, ctas_per_sm, s);
+        if (wgs == 1) return launch_tc<WS, HS, WR, HR, BF, 1, true, 0>(a, sm_count, ctas_per_sm, s);
+        return cudaErrorInvalidConfiguration;
+    }
+    if (wgs == 2) return launch_tc<WS, HS, WR, HR, BF, 2, false, 0>(a, sm_count, ctas_per_sm, s);
+    if (wgs == 1) return launch_tc<WS, HS, WR, HR, BF, 1, false, 0>(a, sm_count, ctas_per_sm, s);
+    return cudaErrorInvalidConfiguration;
 }
 
-template <int WS, int HS, int WR, int HR, bool BF, int WGS, bool PRE>
+template <int WS, int HS, int WR, int HR, bool BF, int WGS, bool PRE, int PART>
 int max_ctas_tc() {
-    using S = TcShape<WS, HS, WR, HR, WGS, PRE>;
+    using S = TcShape<WS, HS, WR, HR, WGS, PRE, PART>;
     if (S::kSmem > 232448) return 0;
-    auto kern = k_infer_tc<WS, HS, WR, HR, BF, WGS, PRE>;
+    auto kern = k_infer_tc<WS, HS, WR, HR, BF, WGS, PRE, PART>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kSmem) !=
         cudaSuccess)
         return 0;
     return resident_ctas((const void*)kern, 128 * WGS, S::kSmem, 512 / (int)S::kCols);
 }
 
+template <int WS, int HS, bool BF, int WGS>
+int max_ctas_split2() {
+    const int m1 = max_ctas_tc<WS, HS, WS, HS, BF, WGS, true, 1>();
+    const int m2 = max_ctas_tc<WS, HS, WS, HS, BF, WGS, true, 2>();
+    return m1 < m2 ? m1 : m2;
+}
+
+// split: 0 fused, 1 encoding kernel + one MLP kernel, 2 encoding + StatNet + RRSNet kernels
+template <int WS, int HS, bool BF>
+int max_ctas_of(int wgs, int split) {
+    if (split == 2) {
+        if (wgs == 4) return max_ctas_split2<WS, HS, BF, 4>();
+        if (wgs == 2) return max_ctas_split2<WS, HS, BF, 2>();
+        if (wgs == 1) return max_ctas_split2<WS, HS, BF, 1>();
+        return 0;
+    }
+    if (wgs != 1 && wgs != 2) return 0;
+    if (split == 1)
+        return wgs == 2 ? max_ctas_tc<WS, HS, WS, HS, BF, 2, true, 0>() : max_ctas_tc<WS, HS, WS, HS, BF, 1, true, 0>();
+    return wgs == 2 ? max_ctas_tc<WS, HS, WS, HS, BF, 2, false, 0>() : max_ctas_tc<WS, HS, WS, HS, BF, 1, false, 0>();
+}
+
 }  // namespace
 
 int infer_max_ctas_fp32(int ws, int hs);
 
-template <int WS, int HS, bool BF>
-int max_ctas_of(int wgs, bool pre) {
-    if (pre) return wgs == 2 ? max_ctas_tc<WS, HS, WS, HS, BF, 2, true>() : max_ctas_tc<WS, HS, WS, HS, BF, 1, true>();
-    return wgs == 2 ? max_ctas_tc<WS, HS, WS, HS, BF, 2, false>() : max_ctas_tc<WS, HS, WS, HS, BF, 1, false>();
-}
-
-int infer_max_ctas(int ws, int hs, int wr, int hr, int prec, int wgs, bool split) {
+int infer_max_ctas(int ws, int hs, int wr, int hr, int prec, int wgs, int split) {
     if (prec == NRRS_PREC_FP32) return wgs == 1 && !split ? infer_max_ctas_fp32(ws, hs) : 0;
     if (wr != ws || hr != hs) return 0;
     const bool bf = prec == NRRS_PREC_BF16;
@@ -408,24 +478,24 @@ int infer_max_ctas(int ws, int hs, int wr, int hr, int prec, int wgs, bool split
 }
 
 size_t infer_tc_smem_bytes(int ws, int hs, int wr, int hr) {
-    if (ws == 64 && hs == 2) return TcShape<64, 2, 64, 2, 1, false>::kSmem;
-    if (ws == 64 && hs == 3) return TcShape<64, 3, 64, 3, 1, false>::kSmem;
-    if (ws == 128 && hs == 3) return TcShape<128, 3, 128, 3, 1, false>::kSmem;
+    if (ws == 64 && hs == 2) return TcShape<64, 2, 64, 2, 1, false, 0>::kSmem;
+    if (ws == 64 && hs == 3) return TcShape<64, 3, 64, 3, 1, false, 0>::kSmem;
+    if (ws == 128 && hs == 3) return TcShape<128, 3, 128, 3, 1, false, 0>::kSmem;
     return 0;
 }
 
 cudaError_t launch_infer_tc(const InferArgs& a, int ws, int hs, int wr, int hr, int prec,
-                            int sm_count, int ctas_per_sm, int wgs, cudaStream_t s) {
+                            int sm_count, int ctas_per_sm, int wgs, int part, cudaStream_t s) {
     const bool bf = prec == NRRS_PREC_BF16;
     if (ws == 64 && hs == 2 && wr == 64 && hr == 2)
-        return bf ? launch_wgs<64, 2, 64, 2, true>(a, sm_count, ctas_per_sm, wgs, s)
-                  : launch_wgs<64, 2, 64, 2, false>(a, sm_count, ctas_per_sm, wgs, s);
+        return bf ? launch_wgs<64, 2, 64, 2, true>(a, sm_count, ctas_per_sm, wgs, part, s)
+                  : launch_wgs<64, 2, 64, 2, false>(a, sm_count, ctas_per_sm, wgs, part, s);
     if (ws == 64 && hs == 3 && wr == 64 && hr == 3)
-        return bf ? launch_wgs<64, 3, 64, 3, true>(a, sm_count, ctas_per_sm, wgs, s)
-                  : launch_wgs<64, 3, 64, 3, false>(a, sm_count, ctas_per_sm, wgs, s);
-    if (ws == 128 && hs == 3 && wr == 128 && hr == 3)  // 158 KB of weights: 1 CTA per SM
-        return bf ? launch_wgs<128, 3, 128, 3, true>(a, sm_count, ctas_per_sm, wgs, s)
-                  : launch_wgs<128, 3, 128, 3, false>(a, sm_count, ctas_per_sm, wgs, s);
+        return bf ? launch_wgs<64, 3, 64, 3, true>(a, sm_count, ctas_per_sm, wgs, part, s)
+                  : launch_wgs<64, 3, 64, 3, false>(a, sm_count, ctas_per_sm, wgs, part, s);
+    if (ws == 128 && hs == 3 && wr == 128 && hr == 3)  // 158 KB of weights in one kernel
+        return bf ? launch_wgs<128, 3, 128, 3, true>(a, sm_count, ctas_per_sm, wgs, part, s)
+                  : launch_wgs<128, 3, 128, 3, false>(a, sm_count, ctas_per_sm, wgs, part, s);
     return cudaErrorInvalidValue;
 }
 

@@ -52,11 +52,13 @@ struct InferArgs {
     DecideScratch* scr;           // accumulate the exact sum when not null
     unsigned long long* ext_acc;  // accumulate into this caller-owned sum instead (sharded)
     const uint8_t* enc_tiles;     // split mode: hash features per tile from k_encode_levels
+    uint8_t* x1_tiles;            // split mode 2: RRSNet input per tile ([128 x 16], 4 KB)
 };
 
 // split inference mode: per tile, the 32 hash-grid features of its 128 vertices as a
 // [128 x 32] K-major core-matrix block (8 KB), written level-major by k_encode_levels
 constexpr uint32_t kEncTileBytes = 128u * 32u * 2u;
+constexpr uint32_t kX1TileBytes = 128u * 16u * 2u;
 struct EncodeLvArgs {
     EncodeParams enc;
     SegmentTable segs;
@@ -82,10 +84,11 @@ cudaError_t launch_sum(const SumArgs& a, cudaStream_t s);
 cudaError_t launch_infer_fp32(const InferArgs& a, int ws, int hs, int wr, int hr, int sm_count,
                               int ctas_per_sm, cudaStream_t s);
 // largest resident CTAs per SM of the inference kernel for a shape (0 = unsupported)
-int infer_max_ctas(int ws, int hs, int wr, int hr, int prec, int wgs, bool split = false);
-// tcgen05 mixed-precision inference
+// split: 0 fused, 1 encoding + MLP kernel, 2 encoding + StatNet kernel + RRSNet kernel
+int infer_max_ctas(int ws, int hs, int wr, int hr, int prec, int wgs, int split = 0);
+// tcgen05 mixed-precision inference; part: 0 both networks, 1 StatNet only, 2 RRSNet only
 cudaError_t launch_infer_tc(const InferArgs& a, int ws, int hs, int wr, int hr, int prec,
-                            int sm_count, int ctas_per_sm, int wgs, cudaStream_t s);
+                            int sm_count, int ctas_per_sm, int wgs, int part, cudaStream_t s);
 size_t infer_tc_smem_bytes(int ws, int hs, int wr, int hr);
 // derived weight copies: FP32 transposed and the UMMA-packed FP16/BF16 images
 cudaError_t launch_pack_weights(const float* master_mlp, float* wt, float* wrow, void* wpack,

@@ -191,7 +191,7 @@ int run_infer(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const SegmentTable& segs,
     const nrrs_config& c = ctx->cfg;
     cudaError_t e;
     if (segs.total_tiles == 0) return NRRS_OK;
-    const bool split = c.precision != NRRS_PREC_FP32 && ctx->tc_split;
+    const int split = c.precision != NRRS_PREC_FP32 ? ctx->tc_split : 0;
     if (split) {
         // level-major encoding into the feature tiles, then the MLP kernel reads them. Running
         // the two concurrently in chunks (encoding of chunk c+1 on a second stream) was measured
@@ -214,6 +214,26 @@ int run_infer(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const SegmentTable& segs,
         if (e != cudaSuccess) return cuda_fail(ctx, e, "encoding launch");
         a.enc_tiles = ctx->enc_tiles;
     }
+    if (split == 2) {
+        // StatNet kernel (writes the RRSNet input tiles; computes ADRRS factors itself), then
+        // the RRSNet kernel when the factor comes from RRSNet. Each holds only its own weights,
+        // so more 128-vertex tiles are in flight per SM.
+        if (!ctx->x1_tiles) return fail(ctx, NRRS_ERR_INVALID_ARG, "split inference: no RRSNet input tiles");
+        a.x1_tiles = ctx->x1_tiles;
+        {
+            ProfScope ps(ctx, NRRS_KERNEL_INFER_TC, s);
+            e = launch_infer_tc(a, c.statnet_width, c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden,
+                                c.precision, ctx->sm_count, ctx->tc_ctas_per_sm, ctx->tc_wgs, 1, s);
+        }
+        if (e == cudaSuccess && a.fp.source == NRRS_FACTOR_RRSNET) {
+            ProfScope ps(ctx, NRRS_KERNEL_INFER_RRS, s);
+            e = launch_infer_tc(a, c.statnet_width, c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden,
+                                c.precision, ctx->sm_count, ctx->tc_ctas_per_sm, ctx->tc_wgs, 2, s);
+        }
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "inference launch");
+        ctx->last_infer_grid = g_last_grid;
+        return NRRS_OK;
+    }
     {
         ProfScope ps(ctx, c.precision == NRRS_PREC_FP32 ? NRRS_KERNEL_INFER_FP32 : NRRS_KERNEL_INFER_TC, s);
         if (c.precision == NRRS_PREC_FP32)
@@ -221,7 +241,7 @@ int run_infer(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const SegmentTable& segs,
                                   c.rrsnet_hidden, ctx->sm_count, ctx->simt_ctas_per_sm, s);
         else
             e = launch_infer_tc(a, c.statnet_width, c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden,
-                                c.precision, ctx->sm_count, ctx->tc_ctas_per_sm, ctx->tc_wgs, s);
+                                c.precision, ctx->sm_count, ctx->tc_ctas_per_sm, ctx->tc_wgs, 0, s);
     }
     if (e != cudaSuccess) return cuda_fail(ctx, e, "inference launch");
     ctx->last_infer_grid = g_last_grid;
@@ -507,6 +527,7 @@ void nrrs_destroy(nrrs_ctx* ctx) {
     cudaFree(ctx->wpack);
     cudaFree(ctx->tpack);
     cudaFree(ctx->enc_tiles);
+    cudaFree(ctx->x1_tiles);
     cudaFree(ctx->scr);
     cudaFree(ctx->loss_dev);
     cudaFree(ctx->train_scratch);
@@ -808,7 +829,7 @@ const char* nrrs_kernel_name(int32_t kind) {
     static const char* names[NRRS_KERNEL_KINDS] = {
         "infer_fp32", "infer_tc", "sum", "decide", "pack_weights", "table_half",
         "train_statnet", "train_rrsnet", "train_wgrad", "train_reduce", "adam", "encode",
-        "train_scatter", "train_encode"};
+        "train_scatter", "train_encode", "infer_rrs"};
     return (kind >= 0 && kind < NRRS_KERNEL_KINDS) ? names[kind] : "unknown";
 }
 
@@ -857,9 +878,10 @@ int nrrs_set_launch_shape(nrrs_ctx* ctx, int32_t ctas_per_sm, int32_t warpgroups
         ctx->simt_ctas_per_sm = ctas_per_sm;
         return NRRS_OK;
     }
-    if (warpgroups != 1 && warpgroups != 2) return fail(ctx, NRRS_ERR_INVALID_ARG, "warpgroups must be 1 or 2");
+    if (warpgroups != 1 && warpgroups != 2 && warpgroups != 4)
+        return fail(ctx, NRRS_ERR_INVALID_ARG, "warpgroups must be 1, 2 or 4");
     if (infer_max_ctas(c.statnet_width, c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden,
-                       c.precision, warpgroups, ctx->tc_split != 0) <= 0)
+                       c.precision, warpgroups, ctx->tc_split) <= 0)
         return fail(ctx, NRRS_ERR_UNSUPPORTED, "launch shape not available for this network");
     ctx->tc_ctas_per_sm = ctas_per_sm;
     ctx->tc_wgs = warpgroups;
@@ -867,13 +889,22 @@ int nrrs_set_launch_shape(nrrs_ctx* ctx, int32_t ctas_per_sm, int32_t warpgroups
 }
 
 int nrrs_set_infer_split(nrrs_ctx* ctx, int32_t split) {
-    if (!ctx || (split != 0 && split != 1)) return NRRS_ERR_INVALID_ARG;
+    if (!ctx || split < 0 || split > 2) return NRRS_ERR_INVALID_ARG;
     const nrrs_config& c = ctx->cfg;
     if (split && c.precision == NRRS_PREC_FP32)
         return fail(ctx, NRRS_ERR_UNSUPPORTED, "split inference is a tensor-core path mode");
     if (split && infer_max_ctas(c.statnet_width, c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden,
-                                c.precision, 1, true) <= 0)
+                                c.precision, 1, split) <= 0 &&
+        infer_max_ctas(c.statnet_width, c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden,
+                       c.precision, 2, split) <= 0)
         return fail(ctx, NRRS_ERR_UNSUPPORTED, "split inference not available for this network");
+    if (split == 2 && !ctx->x1_tiles) {
+        const uint32_t cap = c.max_queue / kTile + kMaxSegments + 1;
+        if (cudaMalloc(&ctx->x1_tiles, (size_t)cap * kX1TileBytes) != cudaSuccess) {
+            ctx->x1_tiles = nullptr;
+            return fail(ctx, NRRS_ERR_CUDA, "split inference: RRSNet input tile allocation");
+        }
+    }
     if (split && !ctx->enc_tiles) {
         const uint32_t cap = c.max_queue / kTile + kMaxSegments + 1;
         if (cudaMalloc(&ctx->enc_tiles, (size_t)cap * kEncTileBytes) != cudaSuccess) {
@@ -885,8 +916,9 @@ int nrrs_set_infer_split(nrrs_ctx* ctx, int32_t split) {
     ctx->tc_split = split;
     // the warpgroup count must exist in the new mode
     if (infer_max_ctas(c.statnet_width, c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden,
-                       c.precision, ctx->tc_wgs, split != 0) <= 0)
-        ctx->tc_wgs = 1;
+                       c.precision, ctx->tc_wgs, split) <= 0)
+        ctx->tc_wgs = infer_max_ctas(c.statnet_width, c.statnet_hidden, c.rrsnet_width,
+                                     c.rrsnet_hidden, c.precision, 1, split) > 0 ? 1 : 2;
     return NRRS_OK;
 }
 
@@ -1028,10 +1060,10 @@ int nrrs_autotune(nrrs_ctx* ctx, uint32_t n, const char* cache_path, char* repor
     int best_ctas = saved_ctas, best_wgs = saved_wgs, best_split = saved_split;
     rep << "{\"key\": \"" << key << "\", \"n\": " << n << ", \"trials\": [";
     bool first = true;
-    for (int sp = 0; sp <= (fp32 ? 0 : 1); ++sp)
-    for (int w = 1; w <= (fp32 ? 1 : 2); ++w) {
+    for (int sp = 0; sp <= (fp32 ? 0 : 2); ++sp)
+    for (int w = 1; w <= (fp32 ? 1 : 4); w *= 2) {
         const int maxc = infer_max_ctas(c.statnet_width, c.statnet_hidden, c.rrsnet_width,
-                                        c.rrsnet_hidden, c.precision, w, sp != 0);
+                                        c.rrsnet_hidden, c.precision, w, sp);
         if (maxc > 0 && nrrs_set_infer_split(ctx, sp) != NRRS_OK) continue;
         for (int k = 1; k <= maxc; ++k) {
             if (nrrs_set_launch_shape(ctx, k, w) != NRRS_OK) continue;

@@ -157,7 +157,7 @@ _SIGS = {
 
 KERNEL_KINDS = ("infer_fp32", "infer_tc", "sum", "decide", "pack_weights", "table_half",
                 "train_statnet", "train_rrsnet", "train_wgrad", "train_reduce", "adam", "encode",
-                "train_scatter", "train_encode")
+                "train_scatter", "train_encode", "infer_rrs")
 
 
 def lib():
@@ -429,9 +429,10 @@ class NRRSNetwork:
     def set_launch_shape(self, ctas_per_sm: int, warpgroups: int = 1):
         self._check(lib().nrrs_set_launch_shape(self._h, ctas_per_sm, warpgroups))
 
-    def set_infer_split(self, split: bool):
-        """0 = fused inference, 1 = level-major encoding kernel + MLP kernel (large tables)."""
-        self._check(lib().nrrs_set_infer_split(self._h, int(bool(split))))
+    def set_infer_split(self, split: int):
+        """0 = fused inference, 1 = level-major encoding kernel + MLP kernel (large tables),
+        2 = encoding kernel + StatNet kernel + RRSNet kernel."""
+        self._check(lib().nrrs_set_infer_split(self._h, int(split)))
 
     def set_train_split(self, split: bool):
         """1 = level-major encoding, StatNet kernel, level-major scatter; 0 = one fused kernel."""

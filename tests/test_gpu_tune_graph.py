@@ -45,7 +45,7 @@ def test_autotune_picks_and_caches(tmp_path):
     rep = json.loads(net.autotune(262144, cache))
     assert rep["trials"] and tuple(rep["best"][:2]) == net.launch_shape()
     assert rep["best"][2] == net.infer_split()
-    assert {t["split"] for t in rep["trials"]} == {0, 1}   # both inference modes were timed
+    assert {t["split"] for t in rep["trials"]} == {0, 1, 2}   # every inference mode was timed
     assert min(t["ms"] for t in rep["trials"]) == pytest.approx(rep["best_ms"])
     other = make_net(precision=nb.PREC_FP16)
     rep2 = json.loads(other.autotune(262144, cache))
@@ -101,20 +101,24 @@ SPLIT_SHAPES = {
 }
 
 
+@pytest.mark.parametrize("factor", [nb.FACTOR_RRSNET, nb.FACTOR_ADRRS], ids=["rrsnet", "adrrs"])
 @pytest.mark.parametrize("shape", list(SPLIT_SHAPES))
-def test_split_inference_equals_fused(shape):
-    """the level-major encoding kernel + feature-tile MLP kernel gives the fused kernel's
-    outputs bit for bit, for every warpgroup count, on a ragged multi-segment launch"""
+def test_split_inference_equals_fused(shape, factor):
+    """both split modes (encoding kernel + one MLP kernel; encoding + StatNet + RRSNet kernels)
+    give the fused kernel's outputs bit for bit, for every warpgroup count that fits, on a ragged
+    multi-segment launch, with RRSNet and ADRRS factors"""
     torch = torch_cuda()
     prec, kw = SPLIT_SHAPES[shape]
     net = make_net(precision=prec, **kw)
     random_params(net, 54, table_scale=0.5, mlp_scale=0.1)
+    if factor == nb.FACTOR_ADRRS:
+        net.setStep(2)
     counts = [70_001, 129, 1, 0, 33_333]
     offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
     N = int(offs[-1])
     v = nb.synth(55, N)
     d = upload(v)
-    dp = nb.default_decide()
+    dp = nb.default_decide(factor_source=factor)
     caps = [9 * c for c in counts]
     qoffs = np.concatenate([[0], np.cumsum(caps)]).astype(np.int64)
     segs = [nb.Segment(int(offs[k]), counts[k], max(counts[k], 1), 0, int(qoffs[k]), caps[k])
@@ -128,16 +132,23 @@ def test_split_inference_equals_fused(shape):
         torch.cuda.synchronize()
         return o
 
-    net.set_infer_split(False)
+    net.set_infer_split(0)
     net.set_launch_shape(0, 1)
     ref = run()
-    net.set_infer_split(True)
-    assert net.infer_split() == 1
-    for w in (1, 2):
-        net.set_launch_shape(0, w)
-        out = run()
-        for k in ref:
-            assert torch.equal(out[k], ref[k]), (shape, w, k)
+    tried = 0
+    for mode in (1, 2):
+        net.set_infer_split(mode)
+        assert net.infer_split() == mode
+        for w in (1, 2, 4):
+            try:
+                net.set_launch_shape(0, w)
+            except nb.NRRSError:
+                continue                      # that many warpgroups do not fit in this mode
+            tried += 1
+            out = run()
+            for k in ref:
+                assert torch.equal(out[k], ref[k]), (shape, mode, w, k)
+    assert tried >= 4
     rc, flags = net.device_status(stream())
     assert rc == nb.OK and flags == 0
     net.close()
