@@ -39,8 +39,10 @@ __global__ void __launch_bounds__(kTile) k_encode_levels(const __grid_constant__
         if (i < sg.offset + sg.count) {
             float p[3];
             norm_pos(a.enc, a.pos, i, p);
+            // two levels per batch of loads: half the registers of four, twice the CTAs per SM
             float f[8];
-            levels_features_h<4>(table, a.enc, p, 4 * (int)q, f);
+            levels_features_h<2>(table, a.enc, p, 4 * (int)q, f);
+            levels_features_h<2>(table, a.enc, p, 4 * (int)q + 2, f + 4);
             v = tile::pack8<BF>(f);
         }
         *reinterpret_cast<uint4*>(a.out + (size_t)t * a.tile_bytes +
