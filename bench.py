@@ -15,9 +15,14 @@ Other workloads (--workload):
             separately on the same vertices (and checked to decide identically)
   frame4k   3840x2160: 8,294,400 vertices per bounce, 10 bounces, MLPs 128 wide x 3 hidden
             layers (BF16 by default), 2^22-entry table, 10 training steps of 262,144 samples
+  records1080p
+            the training-data side of a 1920x1080 frame: 8 bounces of path vertices (about
+            10.1M) record 7.0M path nodes and 7.5M radiance contributions, then the training
+            batch and the sample weights are built; metric path nodes/s (one step = one frame)
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload frame1080p|batched|frame4k] [--precision fp16|bf16|fp32]
+                  [--workload frame1080p|batched|frame4k|records1080p]
+                  [--precision fp16|bf16|fp32]
                   [--no-train]
 
 value    = vertices/s of the whole job (device-timed steps, max over ranks)
@@ -59,6 +64,9 @@ WORKLOADS = {
                     width=64, hidden=2, log2_table=19, steps=50, precision="fp16"),
     "frame4k": dict(bounces=10, n_vert=8_294_400, train_steps=10, train_batch=262_144,
                     width=128, hidden=3, log2_table=22, steps=5, precision="bf16"),
+    # the reference's shipped settings (render/test.json:75-82): node buffer 10 x pixels,
+    # throughput scaled by rrs, later siblings without RRSNet target; zero-L samples kept
+    "records1080p": dict(bounces=8, n_vert=2_073_600, node_rate=10, steps=20, precision="fp32"),
 }
 
 
@@ -626,6 +634,283 @@ def run_ours(args, rank, world, local_rank):
     return 0
 
 
+# ---- records1080p: path-node records, radiance and the training batch ------------------------
+
+RECORD_KEYS = ("pos", "wi", "normal", "albedo", "roughness", "thp", "depth", "pixel", "rrs",
+               "record", "parent")
+CONTRIB_KEYS = ("contrib_node", "contrib")
+
+
+def records_params():
+    return nb.default_train_data_params(ignore_zero_l=0, copy_rrs_node=1, dedupe_rrs_target=1)
+
+
+def records_frame(seed: int, wl: dict):
+    P = wl["n_vert"]
+    bounces, image = nb.synth_paths(seed, P, bounces=wl["bounces"],
+                                    capacity=wl["node_rate"] * P)
+    return bounces, image
+
+
+def records_name(wl):
+    return f"records_{wl['bounces']}bounce_{wl['n_vert']}px_rate{wl['node_rate']}"
+
+
+def records_cpu(wl, bounces, image, seconds: float):
+    """The oracle (sequential C, one core) on whole frames of the workload until `seconds`."""
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle as O
+    P = wl["n_vert"]
+    prm = records_params()
+    t, reps, nodes = 0.0, 0, 0
+    while True:
+        a = time.perf_counter()
+        r = O.frame_training_data(bounces, image, wl["node_rate"] * P, prm)
+        t += time.perf_counter() - a
+        reps += 1
+        nodes = r["nodes"].size
+        if t > seconds:
+            break
+    return nodes * reps / t, reps, t / reps
+
+
+def run_records_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    wl = WORKLOADS[args.workload]
+    bounces, image = records_frame(4242, wl)
+    secs = max(1.0, 1.0 * args.steps)
+    value, reps, frame_s = records_cpu(wl, bounces, image, secs)
+    line = {
+        "metric": "path nodes/s (records + radiance + training batch + weights)",
+        "value": value, "unit": "nodes/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": frame_s * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "impl": "reference", "config": {"workload": records_name(wl)},
+        "cpu_baseline": {"value": value, "unit": "nodes/s", "cores": 1, "kind": "port",
+                         "sample": f"{reps} whole frames"},
+        "e2e": {"value": value, "unit": "nodes/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": "reference CPU path = sequential C restatement (oracle/records.c) of "
+                "recordNode/recordRadiance/nrrs_generate_training_data/"
+                "nrrs_calculate_sample_weight; the reference runs them on the GPU inside its "
+                "OptiX integrator, which cannot be built here",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_records(args, rank, world, local_rank):
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local_rank)
+    cur = torch.cuda.current_stream()
+    stream = cur.cuda_stream
+    wl = WORKLOADS[args.workload]
+    P = wl["n_vert"]
+    cap = wl["node_rate"] * P
+    bounces, image = records_frame(4242 + rank, wl)
+    prm = records_params()
+
+    def to_t(a):
+        a = np.ascontiguousarray(a)
+        return torch.from_numpy(a.view(np.int32) if a.dtype == np.uint32 else a)
+
+    host_b = [{k: to_t(b[k]).pin_memory() for k in RECORD_KEYS + CONTRIB_KEYS} for b in bounces]
+    dev_b = [{k: t.to(dev) for k, t in hb.items()} for hb in host_b]
+    n_of = [len(b["pixel"]) for b in bounces]
+    m_of = [len(b["contrib_node"]) for b in bounces]
+    outs = [torch.empty(max(n, 1), dtype=torch.int32, device=dev) for n in n_of]
+    soas = [nb.vertex_soa(d["pos"], d["wi"], d["normal"], d["roughness"], d["albedo"], d["thp"],
+                          d["depth"]) for d in dev_b]
+    nbytes = nb.path_nodes_bytes(cap, max(n_of))
+    block = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    pn = nb.NRRSPathNodesBuffer(block.data_ptr(), nbytes, cap, max(n_of), stream)
+    widths = {"pos": 3, "wi": 3, "normal": 3, "albedo": 3, "roughness": 1, "thp": 3, "depth": 1,
+              "ref_mean": 1, "target": 3, "rrs_target": 1, "pixel": 1}
+    batch = {k: torch.empty((cap, w) if w > 1 else cap,
+                            dtype=torch.int32 if k in ("depth", "pixel") else torch.float32,
+                            device=dev) for k, w in widths.items()}
+    tb = nb.train_batch(**batch)
+    counts = torch.zeros(P, dtype=torch.int32, device=dev)
+    weights = torch.empty(cap, dtype=torch.float32, device=dev)
+    size_d = torch.zeros(1, dtype=torch.int32, device=dev)
+    img_d = torch.from_numpy(image).to(dev)
+    img_h = torch.from_numpy(image).pin_memory()
+    size_h = torch.zeros(1, dtype=torch.int32).pin_memory()
+
+    def step(pre=None, post=None, ev=None):
+        pn.reset(stream)
+        for d, db in enumerate(dev_b):
+            if pre:
+                pre(d)
+            if ev:
+                ev[("rec", d)][0].record(cur)
+            pn.recordNode(soas[d], db["parent"], db["pixel"], db["rrs"], db["record"], n_of[d],
+                          outs[d], stream)
+            if ev:
+                ev[("rec", d)][1].record(cur)
+            pn.recordRadiance(db["contrib_node"], db["contrib"], m_of[d], stream)
+            if ev:
+                ev[("rad", d)][1].record(cur)
+            if post:
+                post(d)
+        counts.zero_()      # mTrainingSamples is zeroed once per frame (integrator.cpp:1041)
+        if pre:
+            pre("image")
+        if ev:
+            ev["gen"][0].record(cur)
+        pn.generate_training_data(prm, tb, cap, size_d, image=img_d, image_channels=4,
+                                  n_pixels=P, pixel_samples=counts, stream=stream)
+        if ev:
+            ev["gen"][1].record(cur)
+        nb.calculate_sample_weight(batch["pixel"], counts, P, size_d, cap, weights, stream)
+        if ev:
+            ev["wgt"][1].record(cur)
+        if post:
+            post("image")
+
+    launches_per_step = 2 * len(bounces) + 3   # + propagate, generate, weights (zero_ is torch's)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    n_nodes, dropped, flags = pn.status(stream)
+    total = int(size_d.item())
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(cur)
+        for _ in range(args.steps):
+            step()
+        e1.record(cur)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    # ---- e2e: host inputs uploaded every frame on a copy stream, the batch size read back ----
+    copy_stream = torch.cuda.Stream(device=dev)
+    keys = list(range(len(dev_b))) + ["image"]
+    ev_copied = {k: torch.cuda.Event() for k in keys}
+    ev_used = {k: torch.cuda.Event() for k in keys}
+    for k in keys:
+        ev_used[k].record(cur)
+
+    def step_e2e():
+        with torch.cuda.stream(copy_stream):
+            for d, (hb, db) in enumerate(zip(host_b, dev_b)):
+                copy_stream.wait_event(ev_used[d])
+                for k in hb:
+                    db[k].copy_(hb[k], non_blocking=True)
+                ev_copied[d].record(copy_stream)
+            copy_stream.wait_event(ev_used["image"])
+            img_d.copy_(img_h, non_blocking=True)
+            ev_copied["image"].record(copy_stream)
+        step(pre=lambda k: cur.wait_event(ev_copied[k]), post=lambda k: ev_used[k].record(cur))
+        size_h.copy_(size_d, non_blocking=True)
+
+    h2d = sum(t.numel() * t.element_size() for hb in host_b for t in hb.values()) + img_h.numel() * 4
+    for _ in range(2):
+        step_e2e()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2 = max(2, args.steps // 2)
+    a0.record(cur)
+    copy_stream.wait_event(a0)
+    for _ in range(e2):
+        step_e2e()
+    a1.record(cur)
+    torch.cuda.synchronize()
+    e2e_ms = a0.elapsed_time(a1) / e2
+    if dist:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    assert int(size_h.item()) == total
+
+    # ---- per-call device time (one instrumented frame after the timed ones) ----
+    ev = {("rec", d): (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for d in range(len(bounces))}
+    ev.update({("rad", d): (ev[("rec", d)][1], torch.cuda.Event(enable_timing=True))
+               for d in range(len(bounces))})
+    ev["gen"] = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    ev["wgt"] = (ev["gen"][1], torch.cuda.Event(enable_timing=True))
+    step(ev=ev)
+    torch.cuda.synchronize()
+    t_rec = sum(ev[("rec", d)][0].elapsed_time(ev[("rec", d)][1]) for d in range(len(bounces)))
+    t_rad = sum(ev[("rad", d)][0].elapsed_time(ev[("rad", d)][1]) for d in range(len(bounces)))
+    t_gen = ev["gen"][0].elapsed_time(ev["gen"][1])
+    t_wgt = ev["wgt"][0].elapsed_time(ev["wgt"][1])
+
+    # algorithmic bytes (each array element read or written once; an atomic add counts its
+    # 8-byte read and write)
+    n_vert, n_contrib = sum(n_of), sum(m_of)
+    recorded = n_nodes
+    b_rec = n_vert * (60 + 20 + 1 + 4) + recorded * (60 + 20 + 72 + 12) + recorded * 16
+    limbs_nz = 6                                    # nonzero limbs of a typical contribution
+    b_rad = n_contrib * (4 + 12 + 4) + n_contrib * limbs_nz * 16
+    b_gen = (recorded * (4 + 4 + 72 + 4 + 4 + limbs_nz * 16 + 8)      # radiance pass
+             + recorded * (72 + 12 + 4 + 24 + 4 + 4)                     # batch: read
+             + total * (24 + 4 + 4 + 4 + 4 + 16 + 92 + 8))              # kept: read, write
+    b_wgt = total * (4 + 4 + 4)
+    calls = {"record_nodes": (t_rec, b_rec, len(bounces)), "record_radiance": (t_rad, b_rad, len(bounces)),
+             "generate_training_data": (t_gen, b_gen, 1), "sample_weights": (t_wgt, b_wgt, 1)}
+    peak, peak_kind = measured_peaks()
+    dom = max(calls, key=lambda k: calls[k][0])
+    t_dom, b_dom, n_dom = calls[dom]
+    achieved = b_dom / (t_dom * 1e-3) / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_kind, "traffic": None, "kernel": dom,
+            "algorithmic_bytes_per_launch": b_dom / n_dom, "launch_ms": t_dom / n_dom,
+            "note": "generate_training_data is two kernels (radiance pass, batch); atomics are "
+                    "random 8-byte read-modify-writes"}
+    line = {
+        "metric": "path nodes/s (records + radiance + training batch + weights)",
+        "value": recorded * world / (ms * 1e-3), "unit": "nodes/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": records_name(wl), "pixels": P, "bounces": len(bounces),
+                   "vertices_per_frame": n_vert, "nodes_per_frame": recorded,
+                   "contributions_per_frame": n_contrib, "samples_per_frame": total,
+                   "node_capacity": cap,
+                   "switches": "copy_the_rrs_node, ignore_same_training_data_for_rrs_net",
+                   "l2": "inputs larger than L2 (about 0.8 GB of vertex and contribution "
+                         "arrays per frame, a 3.4 GB node block)",
+                   "parallelism": f"replicas{world}"},
+        "clocks": clk.summary(),
+        "e2e": {"value": recorded * world / (e2e_ms * 1e-3), "unit": "nodes/s",
+                "ms_per_step": e2e_ms, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 4,
+                "h2d_gbs": h2d / (e2e_ms * 1e-3) / 1e9,
+                "overlap": "uploads on a copy stream, bounce d+1 during the records of bounce d"},
+        "gpu_launches": launches_per_step * args.steps,
+        "roofline": roof,
+        "calls": {k: {"ms_per_frame": t, "gbs": b / (t * 1e-3) / 1e9, "launches": n}
+                  for k, (t, b, n) in calls.items()},
+        "device_status": [dropped, flags],
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        value_c, reps, frame_s = records_cpu(wl, bounces, image, 10.0)
+        line["cpu_baseline"] = {"value": value_c, "unit": "nodes/s", "cores": 1, "kind": "port",
+                                "sample": f"{reps} whole frames of the workload"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -650,10 +935,16 @@ def main():
         args.precision = wl["precision"]
     if args.bounces:
         wl["bounces"] = args.bounces
-    if args.vertices:
+    if args.vertices and args.workload != "records1080p":
         wl["n_vert"] = args.vertices
     rank, world = env_int("RANK", 0), env_int("WORLD_SIZE", 1)
     local_rank = env_int("LOCAL_RANK", 0)
+    if args.workload == "records1080p":
+        if args.vertices:
+            wl["n_vert"] = args.vertices
+        if args.impl == "reference":
+            return run_records_reference(args, rank, world)
+        return run_records(args, rank, world, local_rank)
     if args.impl == "reference":
         return run_reference(args, rank, world)
     return run_ours(args, rank, world, local_rank)

@@ -52,6 +52,7 @@ typedef enum {
 #define NRRS_DEV_NAN        0x2u    /* non-finite factor or loss                */
 #define NRRS_DEV_TIMEOUT    0x4u    /* look-back / barrier wait ran out         */
 #define NRRS_DEV_SATURATED  0x8u    /* a split count above 255 was clamped      */
+#define NRRS_DEV_BAD_INDEX  0x10u   /* a pixel or parent index out of range was skipped */
 
 typedef enum {
     NRRS_PREC_FP32 = 0,   /* plain path: FP32 table, FP32 SIMT MLP                         */
@@ -325,6 +326,126 @@ int32_t nrrs_last_infer_grid(const nrrs_ctx* ctx);
 const char* nrrs_kernel_name(int32_t kind);
 int nrrs_profile_enable(nrrs_ctx* ctx, int32_t enable);
 int nrrs_profile_read(nrrs_ctx* ctx, int32_t kind, uint64_t* launches, double* total_ms);
+
+/* ==== path records and training data =========================================================
+ * The training side of the path tracer, beside the hot path: the per-node records of the
+ * training paths, their radiance, and the training batch built from them. No context: the
+ * records live in one caller-owned device block. Replaces, in the reference:
+ *   NRRSPathNodesBuffer (reset, recordNode, recordRadiance, size)  src/render/nrrs/workqueue.h:108-188
+ *   nrrs_generate_training_data                                    src/render/nrrs/train.cu:432-570
+ *   nrrs_calculate_sample_weight                                   src/render/nrrs/train.cu:572-592
+ *   their call sites in NRRSPathTracer       integrator.cpp:704, 730, 824-831, 1430-1438, 2572-2605
+ * Deterministic where the reference depends on atomic order:
+ *   - the nodes of one nrrs_record_nodes call are numbered in vertex order (reference: atomicAdd);
+ *   - radiance is summed as exact fixed-point integers, three signed 64-bit limbs per channel
+ *     with the lowest bit worth 2^-64 (a contribution keeps every bit at or above 2^-64), so the
+ *     node totals do not depend on the order of contributions (reference: FP32 atomicAdd);
+ *   - the training batch is in node order (reference: atomic push order);
+ *   - of the children of one node, the one with the lowest node index keeps its RRSNet target
+ *     (reference: the first to reach an atomic counter, train.cu:462-466).
+ * The entry points of one node block run in stream order on one stream; none synchronises
+ * except nrrs_path_nodes_status. */
+typedef struct {
+    uint32_t capacity;      /* nodes (nAlloc)                                                   */
+    uint32_t max_record;    /* largest n of one nrrs_record_nodes call                          */
+    float* pos;             /* [capacity][3] world position (intr.p)                            */
+    float* wi;              /* [capacity][3] unit direction, as nrrs_vertex_soa.wi (the reference
+                               stores intr.wo as lat-long, workqueue.h:159)                     */
+    float* normal;          /* [capacity][3] the network's normal lanes (not in the reference's
+                               record; 0 when the vertex SoA has none)                          */
+    float* albedo;          /* [capacity][3] the network's albedo lanes (likewise)              */
+    float* roughness;       /* [capacity]                                                       */
+    float* thp;             /* [capacity][3] throughput given at record time                    */
+    int32_t* parent;        /* [capacity] mLastNodeIdx; -1 = first node of its path             */
+    uint32_t* pixel;        /* [capacity]                                                       */
+    float* rrs;             /* [capacity]                                                       */
+    uint32_t* depth;        /* [capacity]                                                       */
+    int64_t* radiance;      /* [capacity][3 channels][3 limbs]: channel value =
+                               (limb0 + limb1 * 2^32 + limb2 * 2^64) * 2^-64                    */
+    uint32_t* first_child;  /* [capacity] lowest index among the node's children, or ~0u        */
+    uint32_t* children;     /* [capacity] children recorded (consumed by the radiance pass)     */
+    uint32_t* node_flags;   /* [capacity] bit 0: a non-finite contribution reached this node    */
+    uint32_t* header;       /* device words: size, dropped, status, scan state                  */
+    uint64_t* scan_states;  /* device scratch of the order-preserving scans                     */
+} nrrs_path_nodes;
+
+/* Bytes of the device block for capacity nodes and record calls of up to max_record vertices. */
+uint64_t nrrs_path_nodes_bytes(uint32_t capacity, uint32_t max_record);
+/* Carves the arrays of *out from dev_mem (256-byte aligned, at least nrrs_path_nodes_bytes) and
+ * clears the header and scan scratch on the stream (NRRSPathNodesBuffer(n, alloc)). */
+int nrrs_path_nodes_init(void* dev_mem, uint64_t bytes, uint32_t capacity, uint32_t max_record,
+                         nrrs_path_nodes* out, void* stream);
+/* NRRSPathNodesBuffer::reset (workqueue.h:113-120): no nodes, no dropped records. */
+int nrrs_path_nodes_reset(const nrrs_path_nodes* nodes, void* stream);
+/* Synchronises the stream; *size = nodes recorded, *dropped = records refused at capacity
+ * (mInvalidNode), *flags = NRRS_DEV_* bits since the last read (then cleared). Any may be NULL. */
+int nrrs_path_nodes_status(const nrrs_path_nodes* nodes, uint32_t* size, uint32_t* dropped,
+                           uint32_t* flags, void* stream);
+
+/* NRRSPathNodesBuffer::recordNode (workqueue.h:142-170) for a wavefront: every vertex i with
+ * record[i] != 0 (record NULL = all) becomes a node whose fields come from v (pos, wi, thp;
+ * normal, albedo, roughness, depth: NULL = 0), parent[i], pixel[i] and rrs[i] (NULL = 1, the work item's
+ * default, device.cu:83). Nodes are numbered after the existing ones in vertex order.
+ * node_out[i] receives the vertex's node index, or parent[i] when it records nothing or the
+ * buffer is full (the reference's fallback, integrator.cpp:828-830, 1436-1438); node_out may be
+ * parent (in place). n <= max_record. */
+int nrrs_record_nodes(const nrrs_path_nodes* nodes, const nrrs_vertex_soa* v,
+                      const int32_t* parent, const uint32_t* pixel, const float* rrs,
+                      const uint8_t* record, uint32_t n, int32_t* node_out, void* stream);
+
+/* NRRSPathNodesBuffer::recordRadiance (workqueue.h:122-136) for a queue of contributions:
+ * contrib[i] ([n][3]) is added to node[i] and every ancestor. node[i] = -1 or >= size is skipped,
+ * as in the reference. The ancestors receive it in nrrs_generate_training_data's radiance pass
+ * (one pass over the nodes, each node's total added once into its parent) or, after that pass,
+ * here directly; the totals are the same integers either way. A non-finite contribution is not
+ * added: it marks its node and ancestors, whose samples are then dropped (the reference's NaN
+ * filter, train.cu:514), and sets NRRS_DEV_NAN. */
+int nrrs_record_radiance(const nrrs_path_nodes* nodes, const int32_t* node, const float* contrib,
+                         uint32_t n, void* stream);
+
+/* Switches of nrrs_generate_training_data (NRRSPathTracer members, integrator.h). */
+typedef struct {
+    int32_t ignore_zero_l;      /* mNRRSParams.mIgnoreZeroL: drop samples with mean(L) == 0      */
+    int32_t copy_rrs_node;      /* mCopyTheRRSNode: training throughput = thp * rrs             */
+    int32_t dedupe_rrs_target;  /* mIgnoreSameTrainingDataForRRSNet: later siblings get -1      */
+    float thp_eps;              /* L_c = radiance_c / thp_c only where thp_c > thp_eps
+                                   (KiRaRay's M_EPSILON)                                         */
+} nrrs_train_data_params;
+
+/* The training batch: the arrays of nrrs_vertex_soa and nrrs_train_step's target, plus the
+ * reference's per-sample side arrays. All [capacity] device arrays; any may be NULL to skip. */
+typedef struct {
+    float* pos;             /* [cap][3] node position (NRRSNetworkInput0::mPos before the AABB map) */
+    float* wi;              /* [cap][3]                                                         */
+    float* normal;          /* [cap][3]                                                         */
+    float* albedo;          /* [cap][3]                                                         */
+    float* roughness;       /* [cap] (unwarped; the network warps it)                           */
+    float* thp;             /* [cap][3] thpForTraining                                          */
+    uint32_t* depth;        /* [cap]                                                            */
+    float* ref_mean;        /* [cap] refMeanForTraining: mean of the image's RGB at the pixel    */
+    float* target;          /* [cap][3] NRRSNetworkOutputTraining0::mL = max(radiance/thp, 0)    */
+    float* rrs_target;      /* [cap] NRRSNetworkOutputTraining1::mRRS: node rrs, or -1           */
+    uint32_t* pixel;        /* [cap] rayPixelID                                                 */
+} nrrs_train_batch;
+
+/* nrrs_generate_training_data (train.cu:432-570): one sample per node with finite radiance,
+ * finite position and direction and (ignore_zero_l) mean(L) > 0, in node order; at most
+ * capacity (further samples are dropped and flag NRRS_DEV_OVERFLOW). First completes the
+ * radiance of every node (see nrrs_record_radiance), once per reset. image (may be NULL) is
+ * [n_pixels][image_channels] float, channels 3 or 4 (MyFilm::getPixel); pixel_samples (may be
+ * NULL) is [n_pixels] and gains one per sample that keeps its RRSNet target (mTrainingSamples,
+ * which the caller zeroes per frame, integrator.cpp:1041). A pixel >= n_pixels flags
+ * NRRS_DEV_BAD_INDEX and reads and counts nothing. *size_dev receives the sample count. */
+int nrrs_generate_training_data(const nrrs_path_nodes* nodes, const nrrs_train_data_params* p,
+                                const float* image, int32_t image_channels, uint32_t n_pixels,
+                                uint32_t* pixel_samples, const nrrs_train_batch* out,
+                                uint32_t capacity, uint32_t* size_dev, void* stream);
+
+/* nrrs_calculate_sample_weight (train.cu:572-592): weight[t] = 1 / pixel_samples[pixel[t]]
+ * (0 where that count is 0 or the pixel is >= n_pixels) for t < *size_dev; max_n bounds the
+ * grid (the reference's host copy of the size). */
+int nrrs_sample_weights(const uint32_t* pixel, const uint32_t* pixel_samples, uint32_t n_pixels,
+                        const uint32_t* size_dev, uint32_t max_n, float* weight, void* stream);
 
 /* ---- synthetic inputs (host, deterministic): mt19937_64 + explicit transforms. Buffers are
  *      HOST arrays sized as in nrrs_vertex_soa; any may be NULL to skip. target [n][3]. ---- */

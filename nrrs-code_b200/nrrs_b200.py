@@ -31,6 +31,7 @@ DEV_OVERFLOW = 0x1
 DEV_NAN = 0x2
 DEV_TIMEOUT = 0x4
 DEV_SATURATED = 0x8
+DEV_BAD_INDEX = 0x10
 
 PREC_FP32, PREC_FP16, PREC_BF16 = 0, 1, 2
 FACTOR_ADRRS, FACTOR_RRSNET = 2, 3
@@ -69,6 +70,28 @@ class DecideParams(C.Structure):
 class Segment(C.Structure):
     _fields_ = [(n, C.c_uint32) for n in
                 ("offset", "count", "budget", "n_specular", "queue_offset", "queue_capacity")]
+
+
+class PathNodes(C.Structure):
+    """nrrs_path_nodes: the node block's capacity and device arrays."""
+    _fields_ = [("capacity", C.c_uint32), ("max_record", C.c_uint32)] + [
+        (n, C.c_void_p) for n in ("pos", "wi", "normal", "albedo", "roughness", "thp", "parent",
+                                  "pixel", "rrs",
+                                  "depth", "radiance", "first_child", "children", "node_flags",
+                                  "header", "scan_states")]
+
+
+class TrainDataParams(C.Structure):
+    _fields_ = [("ignore_zero_l", C.c_int32), ("copy_rrs_node", C.c_int32),
+                ("dedupe_rrs_target", C.c_int32), ("thp_eps", C.c_float)]
+
+
+TRAIN_BATCH_FIELDS = ("pos", "wi", "normal", "albedo", "roughness", "thp", "depth", "ref_mean",
+                      "target", "rrs_target", "pixel")
+
+
+class TrainBatch(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in TRAIN_BATCH_FIELDS]
 
 
 class NRRSError(RuntimeError):
@@ -148,6 +171,24 @@ _SIGS = {
                                              C.POINTER(C.c_void_p)]),
     "nrrs_graph_launch": (C.c_int, [C.c_void_p, C.c_void_p]),
     "nrrs_graph_destroy": (None, [C.c_void_p]),
+    "nrrs_path_nodes_bytes": (C.c_uint64, [C.c_uint32, C.c_uint32]),
+    "nrrs_path_nodes_init": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32,
+                                       C.POINTER(PathNodes), C.c_void_p]),
+    "nrrs_path_nodes_reset": (C.c_int, [C.POINTER(PathNodes), C.c_void_p]),
+    "nrrs_path_nodes_status": (C.c_int, [C.POINTER(PathNodes), C.POINTER(C.c_uint32),
+                                         C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                         C.c_void_p]),
+    "nrrs_record_nodes": (C.c_int, [C.POINTER(PathNodes), C.POINTER(VertexSoA), C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
+                                    C.c_void_p]),
+    "nrrs_record_radiance": (C.c_int, [C.POINTER(PathNodes), C.c_void_p, C.c_void_p, C.c_uint32,
+                                       C.c_void_p]),
+    "nrrs_generate_training_data": (C.c_int, [C.POINTER(PathNodes), C.POINTER(TrainDataParams),
+                                              C.c_void_p, C.c_int32, C.c_uint32, C.c_void_p,
+                                              C.POINTER(TrainBatch), C.c_uint32, C.c_void_p,
+                                              C.c_void_p]),
+    "nrrs_sample_weights": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
+                                      C.c_void_p, C.c_void_p]),
     "nrrs_last_infer_grid": (C.c_int32, [C.c_void_p]),
     "nrrs_kernel_name": (C.c_char_p, [C.c_int32]),
     "nrrs_profile_enable": (C.c_int, [C.c_void_p, C.c_int32]),
@@ -235,6 +276,74 @@ def synth(seed: int, n: int, first: int = 0):
     return out
 
 
+def synth_paths(seed: int, n_pixels: int, bounces: int = 8, capacity: int | None = None,
+                record_prob: float = 0.7, split_probs=(0.35, 0.5, 0.1, 0.05),
+                contrib_probs=(0.4, 0.45, 0.15), zero_contrib: float = 0.1):
+    """A synthetic training frame for the path-record entry points, as numpy arrays (host).
+
+    Bounce 0 has one vertex per pixel with no parent node. Each vertex records a node with
+    probability record_prob, emits 0, 1 or 2 radiance contributions (contrib_probs; a fraction
+    zero_contrib of them are zero) to its node, and spawns 0..3 vertices of the next bounce
+    (split_probs, mean 0.85) that inherit its pixel and take its node as their parent, as the
+    reference's ray payload carries mNodeIdx (integrator.cpp:824-831). Node numbers follow the
+    library's rule (recorded vertices in vertex order, until capacity), so each bounce's parent
+    array and the expected node_out are known in advance.
+
+    Returns (bounces, image): a list of dicts with pos, wi, normal, albedo, roughness, thp,
+    depth, pixel, rrs,
+    record, parent, node (expected node_out), contrib_node, contrib; and an RGBA image
+    [n_pixels][4] standing in for the rendered frame."""
+    import numpy as np
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    n_nodes = 0
+    pixel = np.arange(n_pixels, dtype=np.uint32)
+    parent = np.full(n_pixels, -1, np.int32)
+    thp_prev = np.ones((n_pixels, 3), np.float32)
+    for d in range(bounces):
+        n = len(pixel)
+        if n == 0:
+            break
+        wi = rng.normal(size=(n, 3)).astype(np.float32)
+        wi /= np.linalg.norm(wi, axis=1, keepdims=True)
+        thp = (thp_prev * rng.uniform(0.3, 1.0, size=(n, 3))).astype(np.float32)
+        nrm = rng.normal(size=(n, 3)).astype(np.float32)
+        nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+        b = {
+            "pos": rng.uniform(0.0, 1.0, size=(n, 3)).astype(np.float32),
+            "wi": wi.astype(np.float32),
+            "normal": nrm.astype(np.float32),
+            "albedo": rng.uniform(0.0, 1.0, size=(n, 3)).astype(np.float32),
+            "roughness": rng.uniform(0.0, 1.0, size=n).astype(np.float32),
+            "thp": thp,
+            "depth": np.full(n, d, np.uint32),
+            "pixel": pixel,
+            "rrs": rng.uniform(0.2, 3.0, size=n).astype(np.float32),
+            "record": (rng.uniform(size=n) < record_prob).astype(np.uint8),
+            "parent": parent,
+        }
+        rec = b["record"].astype(bool)
+        idx = n_nodes + np.cumsum(rec) - 1
+        ok = rec & (idx < (capacity if capacity is not None else np.iinfo(np.int64).max))
+        node = np.where(ok, idx, parent).astype(np.int32)
+        n_nodes = min(n_nodes + int(rec.sum()), capacity) if capacity is not None else n_nodes + int(rec.sum())
+        b["node"] = node
+        k = rng.choice(3, size=n, p=contrib_probs)
+        src = np.repeat(np.arange(n), k)
+        le = rng.lognormal(0.0, 1.5, size=(len(src), 3)).astype(np.float32)
+        le[rng.uniform(size=len(src)) < zero_contrib] = 0.0
+        b["contrib_node"] = node[src]
+        b["contrib"] = (thp[src] * le).astype(np.float32)
+        out.append(b)
+        s = rng.choice(4, size=n, p=split_probs)
+        nxt = np.repeat(np.arange(n), s)
+        pixel = pixel[nxt]
+        parent = node[nxt]
+        thp_prev = thp[nxt]
+    image = rng.uniform(0.0, 2.0, size=(n_pixels, 4)).astype(np.float32)
+    return out, image
+
+
 NOALLOC_MAX_N = 1 << 24
 
 
@@ -246,6 +355,85 @@ def decide_emit_noalloc(rrs, rnd, n, budget, n_specular, params, rrs_norm, split
                                           n_specular, C.byref(params), _ptr(rrs_norm),
                                           _ptr(split), _ptr(queue), capacity, _ptr(next_size),
                                           stream)
+
+
+def _check(rc: int, what: str):
+    if rc != OK:
+        raise NRRSError(rc, f"{what}: {lib().nrrs_status_string(rc).decode()}")
+
+
+def path_nodes_bytes(capacity: int, max_record: int) -> int:
+    """Bytes of the device block of a node buffer (nrrs_path_nodes_bytes)."""
+    return lib().nrrs_path_nodes_bytes(capacity, max_record)
+
+
+def default_train_data_params(**kw) -> TrainDataParams:
+    """The reference's defaults: zero-L samples kept, thp not scaled by rrs, no deduplication,
+    thp threshold 1e-5."""
+    p = TrainDataParams(0, 0, 0, 1e-5)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def train_batch(**arrays) -> TrainBatch:
+    """A TrainBatch from device arrays (any field may be omitted)."""
+    bad = set(arrays) - set(TRAIN_BATCH_FIELDS)
+    if bad:
+        raise KeyError(sorted(bad))
+    return TrainBatch(*(_ptr(arrays.get(k)) for k in TRAIN_BATCH_FIELDS))
+
+
+class NRRSPathNodesBuffer:
+    """Mirror of the reference's NRRSPathNodesBuffer (src/render/nrrs/workqueue.h:108-188) over
+    a caller-owned device block (e.g. a uint8 CUDA tensor of path_nodes_bytes bytes)."""
+
+    def __init__(self, dev_ptr: int, nbytes: int, capacity: int, max_record: int, stream=0):
+        self.nodes = PathNodes()
+        _check(lib().nrrs_path_nodes_init(dev_ptr, nbytes, capacity, max_record,
+                                          C.byref(self.nodes), stream), "nrrs_path_nodes_init")
+
+    def reset(self, stream=0):
+        _check(lib().nrrs_path_nodes_reset(C.byref(self.nodes), stream), "nrrs_path_nodes_reset")
+
+    def status(self, stream=0) -> tuple[int, int, int]:
+        """(size, dropped, device flags); synchronises the stream and clears the flags."""
+        size, dropped, flags = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        _check(lib().nrrs_path_nodes_status(C.byref(self.nodes), C.byref(size),
+                                            C.byref(dropped), C.byref(flags), stream),
+               "nrrs_path_nodes_status")
+        return size.value, dropped.value, flags.value
+
+    def size(self, stream=0) -> int:
+        return self.status(stream)[0]
+
+    def recordNode(self, v: VertexSoA, parent, pixel, rrs, record, n: int, node_out, stream=0):
+        """recordNode for a wavefront (nrrs_record_nodes)."""
+        _check(lib().nrrs_record_nodes(C.byref(self.nodes), C.byref(v), _ptr(parent),
+                                       _ptr(pixel), _ptr(rrs), _ptr(record), n, _ptr(node_out),
+                                       stream), "nrrs_record_nodes")
+
+    def recordRadiance(self, node, contrib, n: int, stream=0):
+        """recordRadiance for a queue of contributions (nrrs_record_radiance)."""
+        _check(lib().nrrs_record_radiance(C.byref(self.nodes), _ptr(node), _ptr(contrib), n,
+                                          stream), "nrrs_record_radiance")
+
+    def generate_training_data(self, params: TrainDataParams, batch: TrainBatch, capacity: int,
+                               size_dev, image=None, image_channels: int = 4, n_pixels: int = 0,
+                               pixel_samples=None, stream=0):
+        """nrrs_generate_training_data (train.cu:432-570)."""
+        _check(lib().nrrs_generate_training_data(C.byref(self.nodes), C.byref(params),
+                                                 _ptr(image), image_channels, n_pixels,
+                                                 _ptr(pixel_samples), C.byref(batch), capacity,
+                                                 _ptr(size_dev), stream),
+               "nrrs_generate_training_data")
+
+
+def calculate_sample_weight(pixel, pixel_samples, n_pixels: int, size_dev, max_n: int, weight,
+                            stream=0):
+    """nrrs_sample_weights (nrrs_calculate_sample_weight, train.cu:572-592)."""
+    _check(lib().nrrs_sample_weights(_ptr(pixel), _ptr(pixel_samples), n_pixels, _ptr(size_dev),
+                                     max_n, _ptr(weight), stream), "nrrs_sample_weights")
 
 
 VERTEX_FIELDS = ("pos", "wi", "normal", "roughness", "albedo", "thp", "depth", "ref_mean")

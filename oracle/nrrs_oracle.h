@@ -81,6 +81,23 @@ void oracle_train_loss_f64(const nrrs_config* cfg, const double* params, uint64_
 void oracle_adam_f32(const nrrs_config* cfg, float* params, const float* grads, float* m,
                      float* v, uint64_t first, uint64_t count, uint64_t t);
 
+/* path-node records and the training batch (records.c); the node block points at HOST arrays */
+void oracle_fixed_limbs(float x, int64_t* l);
+float oracle_fixed_to_float(int64_t l0, int64_t l1, int64_t l2);
+float oracle_fixed_to_float_gcc(int64_t l0, int64_t l1, int64_t l2);
+void oracle_nodes_reset(nrrs_path_nodes* nb);
+void oracle_record_nodes(nrrs_path_nodes* nb, const nrrs_vertex_soa* v, const int32_t* parent,
+                         const uint32_t* pixel, const float* rrs, const uint8_t* record,
+                         uint64_t n, int32_t* node_out);
+void oracle_record_radiance(nrrs_path_nodes* nb, const int32_t* node, const float* contrib,
+                            uint64_t n);
+uint64_t oracle_generate_training_data(nrrs_path_nodes* nb, const nrrs_train_data_params* p,
+                                       const float* image, int channels, uint32_t n_pixels,
+                                       uint32_t* pixel_samples, const nrrs_train_batch* o,
+                                       uint64_t capacity);
+void oracle_sample_weights(const uint32_t* pixel, const uint32_t* pixel_samples,
+                           uint32_t n_pixels, uint64_t n, float* weight);
+
 /* threads used by the OpenMP loops (0 = runtime default) */
 void oracle_set_threads(int n);
 int oracle_get_threads(void);

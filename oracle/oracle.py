@@ -73,6 +73,20 @@ def lib():
                                             C.POINTER(nb.VertexSoA), vp, vp]
         L.oracle_adam_f32.argtypes = [C.POINTER(nb.Config), vp, vp, vp, vp, C.c_uint64,
                                       C.c_uint64, C.c_uint64]
+        L.oracle_fixed_limbs.argtypes = [C.c_float, vp]
+        for f in ("oracle_fixed_to_float", "oracle_fixed_to_float_gcc"):
+            getattr(L, f).restype = C.c_float
+            getattr(L, f).argtypes = [C.c_int64, C.c_int64, C.c_int64]
+        L.oracle_nodes_reset.argtypes = [C.POINTER(nb.PathNodes)]
+        L.oracle_record_nodes.argtypes = [C.POINTER(nb.PathNodes), C.POINTER(nb.VertexSoA), vp,
+                                          vp, vp, vp, C.c_uint64, vp]
+        L.oracle_record_radiance.argtypes = [C.POINTER(nb.PathNodes), vp, vp, C.c_uint64]
+        L.oracle_generate_training_data.restype = C.c_uint64
+        L.oracle_generate_training_data.argtypes = [C.POINTER(nb.PathNodes),
+                                                    C.POINTER(nb.TrainDataParams), vp, C.c_int,
+                                                    C.c_uint32, vp, C.POINTER(nb.TrainBatch),
+                                                    C.c_uint64]
+        L.oracle_sample_weights.argtypes = [vp, vp, C.c_uint32, C.c_uint64, vp]
         L.oracle_set_threads.argtypes = [C.c_int]
         L.oracle_get_threads.restype = C.c_int
         _lib = L
@@ -207,3 +221,124 @@ def set_threads(n: int):
 
 def threads() -> int:
     return int(lib().oracle_get_threads())
+
+
+# ---- path-node records and the training batch (records.c) ----------------------------------
+
+def fixed_limbs(x: float) -> tuple[int, int, int]:
+    out = np.zeros(3, np.int64)
+    lib().oracle_fixed_limbs(C.c_float(x), out.ctypes.data)
+    return int(out[0]), int(out[1]), int(out[2])
+
+
+def fixed_to_float(l0: int, l1: int, l2: int, gcc: bool = False) -> float:
+    f = lib().oracle_fixed_to_float_gcc if gcc else lib().oracle_fixed_to_float
+    return float(f(l0, l1, l2))
+
+
+NODE_ARRAYS = {"pos": (np.float32, 3), "wi": (np.float32, 3), "normal": (np.float32, 3),
+               "albedo": (np.float32, 3), "roughness": (np.float32, 1),
+               "thp": (np.float32, 3), "parent": (np.int32, 1), "pixel": (np.uint32, 1),
+               "rrs": (np.float32, 1), "depth": (np.uint32, 1), "radiance": (np.int64, 9),
+               "first_child": (np.uint32, 1), "children": (np.uint32, 1),
+               "node_flags": (np.uint32, 1)}
+
+
+class HostNodes:
+    """A node block in host memory, for the oracle: the library's nrrs_path_nodes struct
+    pointing at numpy arrays."""
+
+    def __init__(self, capacity: int):
+        self.capacity = capacity
+        self.a = {k: np.zeros((capacity, w) if w > 1 else capacity, dt)
+                  for k, (dt, w) in NODE_ARRAYS.items()}
+        self.header = np.zeros(16, np.uint32)
+        self.nodes = nb.PathNodes(capacity, 0, *(self.a[k].ctypes.data for k in NODE_ARRAYS),
+                                  self.header.ctypes.data, None)
+
+    @property
+    def size(self) -> int:
+        return int(self.header[0])
+
+    @property
+    def dropped(self) -> int:
+        return int(self.header[1])
+
+    @property
+    def status(self) -> int:
+        return int(self.header[3])
+
+    def reset(self):
+        lib().oracle_nodes_reset(C.byref(self.nodes))
+
+    def record_nodes(self, b: dict) -> np.ndarray:
+        n = len(b["pixel"])
+        opt = lambda k: b[k].ctypes.data if b.get(k) is not None else None  # noqa: E731
+        v = nb.VertexSoA(b["pos"].ctypes.data, b["wi"].ctypes.data, opt("normal"),
+                         opt("roughness"), opt("albedo"), b["thp"].ctypes.data,
+                         b["depth"].ctypes.data if b.get("depth") is not None else None,
+                         None, None)
+        out = np.zeros(n, np.int32)
+        rrs = b.get("rrs")
+        rec = b.get("record")
+        lib().oracle_record_nodes(C.byref(self.nodes), C.byref(v), b["parent"].ctypes.data,
+                                  b["pixel"].ctypes.data,
+                                  rrs.ctypes.data if rrs is not None else None,
+                                  rec.ctypes.data if rec is not None else None, n,
+                                  out.ctypes.data)
+        return out
+
+    def record_radiance(self, node, contrib):
+        node = np.ascontiguousarray(node, np.int32)
+        contrib = np.ascontiguousarray(contrib, np.float32)
+        lib().oracle_record_radiance(C.byref(self.nodes), node.ctypes.data, contrib.ctypes.data,
+                                     len(node))
+
+    def generate(self, params, capacity: int, image=None, n_pixels: int = 0,
+                 pixel_samples=None) -> tuple[dict, int]:
+        """The training batch as numpy arrays (the first min(total, capacity) rows) and the
+        total sample count."""
+        cap = max(capacity, 1)
+        out = {"pos": np.zeros((cap, 3), np.float32), "wi": np.zeros((cap, 3), np.float32),
+               "normal": np.zeros((cap, 3), np.float32), "albedo": np.zeros((cap, 3), np.float32),
+               "roughness": np.zeros(cap, np.float32), "thp": np.zeros((cap, 3), np.float32),
+               "depth": np.zeros(cap, np.uint32), "ref_mean": np.zeros(cap, np.float32),
+               "target": np.zeros((cap, 3), np.float32), "rrs_target": np.zeros(cap, np.float32),
+               "pixel": np.zeros(cap, np.uint32)}
+        batch = nb.TrainBatch(*(out[k].ctypes.data for k in nb.TRAIN_BATCH_FIELDS))
+        if image is not None:
+            image = np.ascontiguousarray(image, np.float32)
+        ch = image.shape[1] if image is not None else 0
+        total = lib().oracle_generate_training_data(
+            C.byref(self.nodes), C.byref(params),
+            image.ctypes.data if image is not None else None, ch, n_pixels,
+            pixel_samples.ctypes.data if pixel_samples is not None else None, C.byref(batch),
+            capacity)
+        m = min(int(total), capacity)
+        return {k: v[:m] for k, v in out.items()}, int(total)
+
+
+def sample_weights(pixel, pixel_samples, n_pixels: int) -> np.ndarray:
+    pixel = np.ascontiguousarray(pixel, np.uint32)
+    pixel_samples = np.ascontiguousarray(pixel_samples, np.uint32)
+    w = np.zeros(max(len(pixel), 1), np.float32)
+    lib().oracle_sample_weights(pixel.ctypes.data, pixel_samples.ctypes.data, n_pixels,
+                                len(pixel), w.ctypes.data)
+    return w[:len(pixel)]
+
+
+def frame_training_data(bounces, image, capacity: int, params, batch_capacity=None):
+    """The oracle's run of a whole synthetic frame: per bounce record the nodes, then the
+    contributions; then the batch, the per-pixel counts and the weights."""
+    hn = HostNodes(capacity)
+    node_outs = []
+    for b in bounces:
+        node_outs.append(hn.record_nodes(b))
+        hn.record_radiance(b["contrib_node"], b["contrib"])
+    n_pixels = image.shape[0]
+    counts = np.zeros(n_pixels, np.uint32)
+    bc = capacity if batch_capacity is None else batch_capacity
+    batch, total = hn.generate(params, bc, image=image, n_pixels=n_pixels, pixel_samples=counts)
+    weights = sample_weights(batch["pixel"], counts, n_pixels)
+    return {"nodes": hn, "node_outs": node_outs, "batch": batch, "total": total,
+            "counts": counts, "weights": weights}

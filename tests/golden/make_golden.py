@@ -9,6 +9,8 @@ reference formulas, written out below in float32 numpy arithmetic independent of
   RRSWeightWindow        src/render/common/commoncudautils.h:14-28
   normalizeSpatialCoord  src/render/nrc/nrctrain.h:111-115
   decision / emission    src/render/nrrs/integrator.cpp:1368-1460, commonworkqueue.h:19-25
+  path records, training data and sample weights
+                         src/render/nrrs/workqueue.h:122-170, train.cu:432-592
 
 Each decision case also lists the expected split counts worked out by hand in its comment.
 Run: python tests/golden/make_golden.py  (rewrites the JSON files next to this script).
@@ -88,6 +90,120 @@ def decide(rrs, rnd, budget, nspec, use_ceil, rate, scale_up, sidx=None, capacit
     return {"split": split, "queue": queue, "total": total, "rrs_norm": norm, "flags": flags}
 
 
+def records_expected(case):
+    """Sequential restatement of recordNode / recordRadiance / nrrs_generate_training_data /
+    nrrs_calculate_sample_weight in Python with exact rational radiance sums, under the library's
+    ordering rules (nodes and samples in input order; the lowest-index child keeps its target)."""
+    from fractions import Fraction
+    cap = case["capacity"]
+    nodes = []          # dicts per node
+    size, dropped = 0, 0
+    node_outs = []
+    for b in case["bounces"]:
+        outs = []
+        for i in range(len(b["pixel"])):
+            p = b["parent"][i]
+            if b["record"][i]:
+                if size < cap:
+                    nodes.append(dict(pos=b["pos"][i], wi=b["wi"][i], thp=b["thp"][i],
+                                      rough=b["roughness"][i], parent=p, pixel=b["pixel"][i],
+                                      rrs=b["rrs"][i], depth=b["depth"][i],
+                                      rad=[Fraction(0)] * 3, bad=False))
+                    outs.append(size)
+                    size += 1
+                else:
+                    dropped += 1
+                    outs.append(p)
+            else:
+                outs.append(p)
+        node_outs.append(outs)
+        for nd, c in zip(b["contrib_node"], b["contrib"]):
+            if nd < 0 or nd >= size:
+                continue
+            finite = all(math.isfinite(x) for x in c)
+            cur = nd
+            while cur != -1:        # the chain walk of workqueue.h:127-134
+                if finite:
+                    nodes[cur]["rad"] = [r + Fraction(x) for r, x in zip(nodes[cur]["rad"], c)]
+                else:
+                    nodes[cur]["bad"] = True
+                cur = nodes[cur]["parent"]
+    first_child = {}
+    for i, n in enumerate(nodes):
+        if n["parent"] >= 0 and n["parent"] not in first_child:
+            first_child[n["parent"]] = i
+    prm = case["params"]
+    img = case["image"]
+    counts = [0] * len(img)
+    batch = []
+    for i, n in enumerate(nodes):
+        L = []
+        for ch in range(3):
+            rad = F(float(n["rad"][ch]))
+            th = F(n["thp"][ch])
+            l = F(rad / th) if th > F(prm["thp_eps"]) else F(0)
+            L.append(F(0) if l < 0 else l)
+        mean = F(F(F(L[0] + L[1]) + L[2]) / F(3))
+        same = bool(prm["dedupe_rrs_target"]) and n["parent"] >= 0 and first_child[n["parent"]] != i
+        if n["bad"] or (prm["ignore_zero_l"] and not mean > 0):
+            continue
+        thp = [F(F(t) * F(n["rrs"])) if prm["copy_rrs_node"] else F(t) for t in n["thp"]]
+        q = img[n["pixel"]]
+        batch.append(dict(node=i, target=[float(x) for x in L], thp=[float(x) for x in thp],
+                          rrs_target=-1.0 if same else float(F(n["rrs"])), pixel=n["pixel"],
+                          ref_mean=float(F(F(F(F(q[0]) + F(q[1])) + F(q[2])) / F(3)))))
+        if not same:
+            counts[n["pixel"]] += 1
+    weights = [float(F(F(1) / F(counts[b["pixel"]]))) if counts[b["pixel"]] else 0.0 for b in batch]
+    return dict(size=size, dropped=dropped, node_outs=node_outs, batch=batch, counts=counts,
+                weights=weights)
+
+
+def records_cases():
+    """Hand-built path trees. Worked answer of "tree" (dyadic values, all sums exact):
+      bounce 0: v0 (px 0) and v2 (px 2) record nodes 0 and 1; v1 records nothing (node -1)
+      bounce 1: two children of node 0 -> nodes 2, 3; one of node 1 -> node 4; v1's -> node 5
+      radiance: node 2 (1, .5, .25), node 3 (.25, 0, 0), node 4 (2, 0, 0), node 5 NaN,
+                node 0 = own (.5, .25, 0) + nodes 2, 3 = (1.75, .75, .25), node 1 = (2, 0, 0);
+                v1's (1, 1, 1) is dropped (no node)
+      L = rad / thp: node 0 (3.5, 1.5, 0: thp 1e-6 <= eps), node 1 (2, 0, 0), node 2 (4, 1, .5),
+                node 3 (.5, 0, 0), node 4 (4, 0, 0); node 5 dropped (NaN)
+      dedupe: node 3 is node 0's second child -> rrs target -1, not counted
+      counts: px 0 -> nodes 0, 2 = 2; px 2 -> nodes 1, 4 = 2 -> every weight 1/2"""
+    nan = float("nan")
+    tree_bounces = [
+        dict(pos=[[0.1, 0.2, 0.3], [0.4, 0.5, 0.6], [0.7, 0.8, 0.9]],
+             wi=[[0.0, 0.0, 1.0], [0.0, 1.0, 0.0], [1.0, 0.0, 0.0]],
+             roughness=[0.25, 0.5, 0.75], thp=[[0.5, 0.5, 1e-6], [1.0, 1.0, 1.0], [1.0, 1.0, 1.0]],
+             depth=[0, 0, 0], pixel=[0, 1, 2], rrs=[2.0, 0.5, 0.5], record=[1, 0, 1],
+             parent=[-1, -1, -1],
+             contrib_node=[0, -1], contrib=[[0.5, 0.25, 0.0], [1.0, 1.0, 1.0]]),
+        dict(pos=[[0.15, 0.25, 0.35], [0.45, 0.55, 0.65], [0.75, 0.85, 0.95], [0.05, 0.05, 0.05]],
+             wi=[[0.6, 0.0, 0.8], [0.0, 0.6, 0.8], [0.8, 0.6, 0.0], [0.0, 0.0, -1.0]],
+             roughness=[0.1, 0.2, 0.3, 0.4],
+             thp=[[0.25, 0.5, 0.5], [0.5, 0.5, 0.5], [0.5, 1.0, 1.0], [1.0, 1.0, 1.0]],
+             depth=[1, 1, 1, 1], pixel=[0, 0, 2, 1], rrs=[1.5, 1.5, 1.0, 0.75],
+             record=[1, 1, 1, 1], parent=[0, 0, 1, -1],
+             contrib_node=[2, 3, 4, 5],
+             contrib=[[1.0, 0.5, 0.25], [0.25, 0.0, 0.0], [2.0, 0.0, 0.0], [nan, 0.0, 0.0]]),
+    ]
+    image = [[0.3, 0.6, 0.9, 1.0], [0.0, 0.0, 0.0, 1.0], [1.0, 2.0, 4.0, 1.0]]
+    cases = []
+    for name, comment, cap, prm in (
+        ("tree", "dedupe, zero-L filter, thp * rrs, thp <= eps, NaN chain, no-node contribution",
+         16, dict(ignore_zero_l=1, copy_rrs_node=1, dedupe_rrs_target=1, thp_eps=1e-5)),
+        ("tree_plain", "the reference defaults: no filter, no dedupe, thp as recorded",
+         16, dict(ignore_zero_l=0, copy_rrs_node=0, dedupe_rrs_target=0, thp_eps=1e-5)),
+        ("tree_full", "capacity 5: v1's child is refused (dropped 1, node_out = parent -1)",
+         5, dict(ignore_zero_l=1, copy_rrs_node=1, dedupe_rrs_target=1, thp_eps=1e-5)),
+    ):
+        case = dict(name=name, comment=comment, capacity=cap, params=prm, bounces=tree_bounces,
+                    image=image)
+        case["expect"] = records_expected(case)
+        cases.append(case)
+    return cases
+
+
 def main():
     ka = {
         "activation_sigma": [[x, float(act_sigma(x))] for x in (-10.0, -1.0, -0.5, 0.0, 0.5, 1.0, 10.0)],
@@ -155,8 +271,11 @@ def main():
         rrs=[], rnd=[], budget=10, nspec=0, use_ceil=True, rate=0.85, scale_up=False)
 
     (HERE / "known_answers.json").write_text(json.dumps(ka, indent=1) + "\n")
+    rc = records_cases()
+    (HERE / "records_cases.json").write_text(json.dumps(rc, indent=1, allow_nan=True) + "\n")
     (HERE / "decide_cases.json").write_text(json.dumps(cases, indent=1) + "\n")
-    print("wrote", HERE / "known_answers.json", HERE / "decide_cases.json")
+    print("wrote", HERE / "known_answers.json", HERE / "decide_cases.json",
+          HERE / "records_cases.json")
 
 
 if __name__ == "__main__":
