@@ -363,7 +363,8 @@ typedef struct {
     int64_t* radiance;      /* [capacity][3 channels][3 limbs]: channel value =
                                (limb0 + limb1 * 2^32 + limb2 * 2^64) * 2^-64                    */
     uint32_t* first_child;  /* [capacity] lowest index among the node's children, or ~0u        */
-    uint32_t* children;     /* [capacity] children recorded (consumed by the radiance pass)     */
+    uint32_t* children;     /* [capacity] children recorded                                     */
+    uint32_t* arrived;      /* [capacity] children whose radiance the radiance pass has added   */
     uint32_t* node_flags;   /* [capacity] bit 0: a non-finite contribution reached this node    */
     uint32_t* header;       /* device words: size, dropped, status, scan state                  */
     uint64_t* scan_states;  /* device scratch of the order-preserving scans                     */

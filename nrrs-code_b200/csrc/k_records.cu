@@ -9,14 +9,19 @@
 // The reference numbers nodes and training samples with atomicAdd and sums radiance with FP32
 // atomics, so both its order and its bits depend on scheduling. Here:
 //   * nodes and samples are compacted in input order by a single-pass scan with decoupled
-//     look-back over 2048-element chunks (one ballot per warp and pass);
+//     look-back over 1024-element chunks (one ballot per warp and pass); the whole CTA reads
+//     256 predecessor states per look-back step;
 //   * radiance is a fixed-point integer, three signed 64-bit limbs per channel with the lowest
 //     bit worth 2^-64: a contribution x (|x| < 2^62) becomes trunc(|x| 2^64) split into a
 //     32-bit low limb, a 32-bit middle limb and the integer part, each signed like x. Integer
 //     additions commute, so every node total is the same integer in any order;
 //   * a contribution is added to its own node only; one pass then adds each node's complete
-//     total into its parent once, a child that finds itself the last of its siblings carrying on
-//     upwards. That is one addition per node instead of one per ancestor per contribution.
+//     total into its parent once, walking up from the leaves: an only child hands its total up in
+//     registers (plain loads and stores), siblings add theirs with atomics and the last to arrive
+//     carries on. That is one addition per node instead of one per ancestor per contribution;
+//   * a warp's compacted outputs form one contiguous run, so three-float fields go out through a
+//     small per-warp shared-memory stage as contiguous words, and every field of an element is
+//     loaded before any is stored.
 #include <cmath>
 
 #include "records.hpp"
@@ -55,23 +60,30 @@ __device__ __forceinline__ unsigned lanemask_lt() {
     return m;
 }
 
-// Called by all of warp 0. Publishes this chunk's total, reads the predecessors' states 32 at a
-// time until an inclusive prefix, publishes its own inclusive prefix and returns the exclusive
-// one. Chunk 0 starts from seed. Every wait is bounded; running out sets NRRS_DEV_TIMEOUT.
-__device__ unsigned lookback(unsigned long long* states, unsigned c, unsigned epoch,
-                             unsigned total, unsigned seed, unsigned spin_limit, unsigned* flags) {
-    const int lane = threadIdx.x & 31;
+// Called by every thread of the CTA. Publishes this chunk's total, reads the 256 predecessor
+// states below a window top until an inclusive prefix, publishes its own inclusive prefix and
+// returns the exclusive one (to every thread). Chunk 0 starts from seed. Every wait is bounded;
+// running out sets NRRS_DEV_TIMEOUT.
+struct LookbackSmem {
+    unsigned first[kRecThreads / 32];
+    unsigned long long part[kRecThreads / 32];
+};
+
+__device__ unsigned lookback_block(unsigned long long* states, unsigned c, unsigned epoch,
+                                   unsigned total, unsigned seed, unsigned spin_limit,
+                                   unsigned* flags, LookbackSmem& sm) {
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     if (c == 0) {
-        if (lane == 0) store_state(&states[0], pack_state(epoch, kFlagIncl, sat_add(seed, total)));
+        if (tid == 0) store_state(&states[0], pack_state(epoch, kFlagIncl, sat_add(seed, total)));
         return seed;
     }
-    if (lane == 0) store_state(&states[c], pack_state(epoch, kFlagAgg, total));
+    if (tid == 0) store_state(&states[c], pack_state(epoch, kFlagAgg, total));
     int top = (int)c - 1;
     unsigned spins = 0;
     bool timed_out = false;
     unsigned long long acc = 0;
     for (;;) {
-        const int idx = top - lane;
+        const int idx = top - tid;
         bool ready = true, incl = true;
         unsigned val = 0;
         if (idx >= 0) {
@@ -81,47 +93,75 @@ __device__ unsigned lookback(unsigned long long* states, unsigned c, unsigned ep
             incl = wf == kFlagIncl;
             val = (unsigned)w;
         }
-        if (!__all_sync(0xffffffffu, ready)) {
+        if (!__syncthreads_and(ready)) {
             if (++spins > spin_limit) {
                 timed_out = true;
                 break;
             }
-            __nanosleep(32);
+            __nanosleep(64);
             continue;
         }
         const unsigned im = __ballot_sync(0xffffffffu, incl);
-        const int stop = im ? __ffs(im) - 1 : 31;
-        unsigned long long part = lane <= stop ? (unsigned long long)val : 0ull;
+        if (lane == 0) sm.first[wid] = im ? (unsigned)(wid * 32 + __ffs(im) - 1) : 0xffffffffu;
+        __syncthreads();
+        unsigned stop = 0xffffffffu;
+#pragma unroll
+        for (int k = 0; k < kRecThreads / 32; ++k) stop = min(stop, sm.first[k]);
+        unsigned long long part = (unsigned)tid <= stop ? (unsigned long long)val : 0ull;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-        acc += part;
-        if (im) break;
-        top -= 32;
+        if (lane == 0) sm.part[wid] = part;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kRecThreads / 32; ++k) acc += sm.part[k];
+        __syncthreads();
+        if (stop != 0xffffffffu) break;
+        top -= kRecThreads;
     }
     const unsigned prefix = acc > 0xffffffffull ? 0xffffffffu : (unsigned)acc;
-    if (lane == 0) {
+    if (tid == 0) {
         if (timed_out) *flags |= NRRS_DEV_TIMEOUT;
         store_state(&states[c], pack_state(epoch, kFlagIncl, sat_add(prefix, total)));
     }
     return prefix;
 }
 
-// Exclusive scan of the 64 per-(pass, warp) counts in s_cnt (pass-major), by warp 0; returns
-// the chunk total to every lane.
-__device__ __forceinline__ unsigned scan64(unsigned* s_cnt) {
+// Exclusive scan, by warp 0, of the kRecPasses x warps per-(pass, warp) counts in s_cnt
+// (pass-major, one per lane); returns the chunk total to every lane of warp 0.
+__device__ __forceinline__ unsigned scan_counts(unsigned* s_cnt) {
+    static_assert(kRecPasses * (kRecThreads / 32) == 32, "one count per lane");
     const int lane = threadIdx.x & 31;
-    const unsigned e0 = s_cnt[2 * lane], e1 = s_cnt[2 * lane + 1];
-    const unsigned t = e0 + e1;
+    const unsigned t = s_cnt[lane];
     unsigned incl = t;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += y;
     }
-    const unsigned excl = incl - t;
-    s_cnt[2 * lane] = excl;
-    s_cnt[2 * lane + 1] = excl + e0;
+    s_cnt[lane] = incl - t;
     return __shfl_sync(0xffffffffu, incl, 31);
+}
+
+// A warp's compacted three-float records: lane `rank` holds one (when `active`), the warp's
+// records go to dst[0 .. 3*cnt) as contiguous words through the per-warp stage of 96 floats.
+__device__ __forceinline__ void store3_compact(float* dst, bool active, unsigned rank,
+                                               unsigned cnt, float x, float y, float z,
+                                               float* stage) {
+    const int lane = threadIdx.x & 31;
+    if (active) {
+        stage[3 * rank] = x;
+        stage[3 * rank + 1] = y;
+        stage[3 * rank + 2] = z;
+    }
+    __syncwarp();
+    for (unsigned j = lane; j < 3 * cnt; j += 32) dst[j] = stage[j];
+    __syncwarp();
+}
+
+__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
 }
 
 // trunc(|x| 2^64) as three limbs signed like x; x finite with |x| < 2^62
@@ -141,31 +181,27 @@ __device__ __forceinline__ void fixed_limbs(float x, long long l[3]) {
     l[0] = l0; l[1] = l1; l[2] = l2;
 }
 
-// (l0 + l1 2^32 + l2 2^64) 2^-64 rounded to the nearest float, ties to even
+// (l0 + l1 2^32 + l2 2^64) 2^-64 rounded to the nearest float, ties to even. The magnitude M
+// (< 2^127) is cut to its top 64 bits with the bits below folded into bit 0 (sticky); the
+// hardware's correctly rounded u64 -> f32 conversion then rounds exactly as M itself would
+// round (the folded bit lies 39 places below the rounding position), and the power-of-two
+// scale is exact.
 __device__ __forceinline__ float fixed_to_float(long long l0, long long l1, long long l2) {
     using u128 = unsigned __int128;
     const u128 U = ((u128)(__int128)l2 << 64) + ((u128)(__int128)l1 << 32) + (u128)(__int128)l0;
     const unsigned neg = (unsigned)(U >> 127) & 1u;
     const u128 mag = neg ? (u128)0 - U : U;
-    if (mag == 0) return 0.0f;
     const unsigned long long hi = (unsigned long long)(mag >> 64), lo = (unsigned long long)mag;
-    const int msb = hi ? 127 - __clzll((long long)hi) : 63 - __clzll((long long)lo);
-    int ex = msb - 64;
-    unsigned mant;
-    if (msb <= 23) {
-        mant = (unsigned)(lo << (23 - msb));
+    float f;
+    if (hi == 0) {
+        f = __fmul_rn(__ull2float_rn(lo), 0x1p-64f);
     } else {
-        const int sh = msb - 23;
-        const u128 q = mag >> sh;
-        const u128 rem = mag - (q << sh);
-        const u128 half = (u128)1 << (sh - 1);
-        mant = (unsigned)q;
-        if (rem > half || (rem == half && (mant & 1u))) {
-            ++mant;
-            if (mant == (1u << 24)) { mant >>= 1; ++ex; }
-        }
+        const int sh = 64 - __clzll((long long)hi);  // bits of hi: 1..63
+        const unsigned long long top = (hi << (64 - sh)) | (lo >> sh) |
+                                       ((lo << (64 - sh)) != 0ull ? 1ull : 0ull);
+        f = __fmul_rn(__ull2float_rn(top), __uint_as_float((unsigned)(127 + sh - 64) << 23));
     }
-    return __uint_as_float((neg << 31) | ((unsigned)(ex + 127) << 23) | (mant & 0x7fffffu));
+    return neg ? -f : f;
 }
 
 __device__ __forceinline__ bool fixed_ok(float x) { return fabsf(x) < kFixedMax; }
@@ -193,17 +229,44 @@ __device__ __forceinline__ bool finish_launch(uint32_t* hdr) {
 
 // ---- recordNode for a wavefront -------------------------------------------------------------
 __global__ void __launch_bounds__(kRecThreads) k_record_nodes(const __grid_constant__ RecordArgs a) {
-    __shared__ unsigned s_chunk, s_epoch, s_prefix;
+    __shared__ unsigned s_chunk, s_epoch, s_size0;
     __shared__ unsigned s_cnt[kRecPasses * (kRecThreads / 32)];
+    __shared__ LookbackSmem s_lb;
+    __shared__ float s_stage[kRecThreads / 32][96];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const NodeView& nb = a.nb;
+    const float* __restrict__ in_pos = a.pos;
+    const float* __restrict__ in_wi = a.wi;
+    const float* __restrict__ in_nrm = a.normal;
+    const float* __restrict__ in_alb = a.albedo;
+    const float* __restrict__ in_thp = a.thp;
     if (tid == 0) s_epoch = *(volatile unsigned*)&nb.hdr[kHdrEpoch];
     unsigned flags = 0, dropped = 0;
+    const unsigned lt = lanemask_lt();
+    unsigned long long* call_base = reinterpret_cast<unsigned long long*>(nb.hdr + kHdrCallBase);
     for (;;) {
-        if (tid == 0) s_chunk = atomicAdd(&nb.hdr[kHdrTicket], 1u);
+        if (tid == 0) {
+            s_chunk = atomicAdd(&nb.hdr[kHdrTicket], 1u);
+            // chunk 0 publishes the node count at the start of the call, tagged with this
+            // launch's epoch; every chunk needs it to tell this call's nodes from earlier ones
+            if (s_chunk == 0) {
+                s_size0 = *(volatile unsigned*)&nb.hdr[kHdrSize];
+                store_state(call_base, ((unsigned long long)(s_epoch + 1u) << 32) | s_size0);
+            } else if (s_chunk < a.chunks) {
+                unsigned spins = 0;
+                unsigned long long w = load_state(call_base);
+                while ((unsigned)(w >> 32) != s_epoch + 1u && ++spins <= a.spin_limit) {
+                    __nanosleep(32);
+                    w = load_state(call_base);
+                }
+                if ((unsigned)(w >> 32) != s_epoch + 1u) flags |= NRRS_DEV_TIMEOUT;
+                s_size0 = (unsigned)w;
+            }
+        }
         __syncthreads();
         const unsigned c = s_chunk;
         if (c >= a.chunks) break;
+        const unsigned call0 = s_size0;
         const unsigned v0 = c * kRecChunk;
         unsigned m[kRecPasses];
 #pragma unroll
@@ -214,66 +277,89 @@ __global__ void __launch_bounds__(kRecThreads) k_record_nodes(const __grid_const
             if (lane == 0) s_cnt[j * (kRecThreads / 32) + wid] = __popc(m[j]);
         }
         __syncthreads();
-        if (wid == 0) {
-            const unsigned total = scan64(s_cnt);
-            unsigned seed = 0;
-            if (c == 0) seed = __shfl_sync(0xffffffffu, lane == 0 ? *(volatile unsigned*)&nb.hdr[kHdrSize] : 0u, 0);
-            const unsigned prefix = lookback(nb.states, c, s_epoch, total, seed, a.spin_limit, &flags);
-            if (lane == 0) {
-                s_prefix = prefix;
-                if (c == a.chunks - 1) {
-                    const unsigned end = sat_add(prefix, total);
-                    nb.hdr[kHdrSize] = end < nb.capacity ? end : nb.capacity;
-                }
-            }
-        }
+        unsigned total = 0;
+        if (wid == 0) total = scan_counts(s_cnt);
+        if (tid == 0) s_lb.part[0] = total;  // hand the total to every thread
         __syncthreads();
-        const unsigned lt = lanemask_lt();
+        total = (unsigned)s_lb.part[0];
+        __syncthreads();
+        const unsigned prefix = lookback_block(nb.states, c, s_epoch, total, c == 0 ? s_size0 : 0u,
+                                               a.spin_limit, &flags, s_lb);
+        if (tid == 0 && c == a.chunks - 1) {
+            const unsigned end = sat_add(prefix, total);
+            const unsigned sz = end < nb.capacity ? end : nb.capacity;
+            nb.hdr[kHdrSize] = sz;
+            const unsigned L = nb.hdr[kHdrLevels];
+            if (L < (unsigned)kMaxLevels) nb.hdr[kHdrLevelTable + L] = sz;
+            if (L <= (unsigned)kMaxLevels) nb.hdr[kHdrLevels] = L + 1;
+        }
 #pragma unroll
         for (int j = 0; j < kRecPasses; ++j) {
             const unsigned v = v0 + j * kRecThreads + tid;
-            if (v >= a.n) continue;
-            const int p = a.parent[v];
-            int out = p;
-            if ((m[j] >> lane) & 1u) {
-                const unsigned long long idx64 = (unsigned long long)s_prefix +
-                    s_cnt[j * (kRecThreads / 32) + wid] + __popc(m[j] & lt);
-                if (idx64 < nb.capacity) {
-                    const unsigned idx = (unsigned)idx64;
+            const bool valid = v < a.n;
+            const bool active = (m[j] >> lane) & 1u;
+            const unsigned rank = __popc(m[j] & lt);
+            const unsigned long long base = (unsigned long long)prefix + s_cnt[j * (kRecThreads / 32) + wid];
+            const unsigned cnt = __popc(m[j]);
+            const unsigned room = base >= nb.capacity ? 0u
+                                  : (unsigned)min((unsigned long long)cnt, nb.capacity - base);
+            const bool keep = active && rank < room;
+            // every field first, then the stores
+            int p = 0;
+            float q[15];
+            float rough = 0.f, rrs = 1.f;
+            unsigned px = 0, dep = 0;
+            if (valid) p = a.parent[v];
+            // a parent must be a node of an earlier call: any other link is cut and flagged
+            const bool bad_parent = p >= 0 && (unsigned)p >= call0;
+            const int pn = bad_parent ? -1 : p;
+            if (keep) {
 #pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        const size_t si = 3 * (size_t)v + k, di = 3 * (size_t)idx + k;
-                        nb.pos[di] = a.pos[si];
-                        nb.wi[di] = a.wi[si];
-                        nb.normal[di] = a.normal ? a.normal[si] : 0.f;
-                        nb.albedo[di] = a.albedo ? a.albedo[si] : 0.f;
-                        nb.thp[di] = a.thp[si];
-                    }
-                    nb.rough[idx] = a.rough ? a.rough[v] : 0.f;
-                    nb.parent[idx] = p;
-                    nb.pixel[idx] = a.pixel[v];
-                    nb.rrs[idx] = a.rrs ? a.rrs[v] : 1.f;
-                    nb.depth[idx] = a.depth ? a.depth[v] : 0u;
-                    long long* r = nb.rad + (size_t)idx * kLimbs;
-#pragma unroll
-                    for (int k = 0; k < kLimbs; ++k) r[k] = 0;
-                    nb.first_child[idx] = 0xffffffffu;
-                    nb.children[idx] = 0;
-                    nb.flags[idx] = 0;
-                    if (p >= 0) {
-                        if ((unsigned)p < idx) {
-                            atomicMin(&nb.first_child[p], idx);
-                            atomicAdd(&nb.children[p], 1u);
-                        } else {
-                            flags |= NRRS_DEV_BAD_INDEX;
-                        }
-                    }
-                    out = (int)idx;
-                } else {
-                    ++dropped;
+                for (int k = 0; k < 3; ++k) {
+                    const size_t si = 3 * (size_t)v + k;
+                    q[k] = in_pos[si];
+                    q[3 + k] = in_wi[si];
+                    q[6 + k] = in_nrm ? in_nrm[si] : 0.f;
+                    q[9 + k] = in_alb ? in_alb[si] : 0.f;
+                    q[12 + k] = in_thp[si];
                 }
+                if (a.rough) rough = a.rough[v];
+                if (a.rrs) rrs = a.rrs[v];
+                if (a.depth) dep = a.depth[v];
+                px = a.pixel[v];
+            } else {
+#pragma unroll
+                for (int k = 0; k < 15; ++k) q[k] = 0.f;
             }
-            a.node_out[v] = out;
+            const unsigned idx = (unsigned)(base + rank);
+            if (room) {  // warp-uniform
+                store3_compact(nb.pos + 3 * base, keep, rank, room, q[0], q[1], q[2], s_stage[wid]);
+                store3_compact(nb.wi + 3 * base, keep, rank, room, q[3], q[4], q[5], s_stage[wid]);
+                store3_compact(nb.normal + 3 * base, keep, rank, room, q[6], q[7], q[8], s_stage[wid]);
+                store3_compact(nb.albedo + 3 * base, keep, rank, room, q[9], q[10], q[11], s_stage[wid]);
+                store3_compact(nb.thp + 3 * base, keep, rank, room, q[12], q[13], q[14], s_stage[wid]);
+                long long* r = nb.rad + (size_t)base * kLimbs;
+                for (unsigned k = lane; k < kLimbs * room; k += 32) r[k] = 0;
+            }
+            if (keep) {
+                nb.rough[idx] = rough;
+                nb.parent[idx] = pn;
+                nb.pixel[idx] = px;
+                nb.rrs[idx] = rrs;
+                nb.depth[idx] = dep;
+                nb.first_child[idx] = 0xffffffffu;
+                nb.children[idx] = 0;
+                nb.arrived[idx] = 0;
+                nb.flags[idx] = 0;
+                if (pn >= 0) {
+                    atomicMin(&nb.first_child[pn], idx);
+                    atomicAdd(&nb.children[pn], 1u);
+                }
+                if (bad_parent) flags |= NRRS_DEV_BAD_INDEX;
+            } else if (active) {
+                ++dropped;
+            }
+            if (valid) a.node_out[v] = keep ? (int)idx : p;
         }
         __syncthreads();
     }
@@ -326,64 +412,149 @@ __global__ void __launch_bounds__(256) k_record_radiance(const __grid_constant__
     if (flags) atomicOr(&nb.hdr[kHdrStatus], flags);
 }
 
-// ---- radiance of the descendants: each node's total into its parent, once --------------------
-// A leaf (no children) starts a walk up its chain. After adding a complete node into its parent
-// a thread decrements the parent's pending-children count; the child that brings it to zero
-// continues with the parent, whose total is then complete. Indices strictly decrease along a
-// chain, so every walk ends. Runs once per reset: a later launch returns at once.
-__global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ NodeView nb) {
-    __shared__ unsigned s_skip;
-    if (threadIdx.x == 0) s_skip = *(volatile unsigned*)&nb.hdr[kHdrPropagated];
-    __syncthreads();
-    unsigned flags = 0;
-    if (!s_skip) {
-        const unsigned size = nb.hdr[kHdrSize];
-        for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < size;
-             i += gridDim.x * blockDim.x) {
-            if (nb.first_child[i] != 0xffffffffu) continue;  // not a leaf
-            unsigned cur = i;
-            for (;;) {
-                const int p = nb.parent[cur];
-                if (p < 0) break;
-                if ((unsigned)p >= cur) { flags |= NRRS_DEV_BAD_INDEX; break; }
-                long long l[kLimbs];
-                const long long* src = nb.rad + (size_t)cur * kLimbs;
-#pragma unroll
-                for (int k = 0; k < kLimbs; ++k) l[k] = __ldcg(src + k);
-                add_limbs(nb.rad + (size_t)p * kLimbs, l);
-                const unsigned f = __ldcg(nb.flags + cur);
-                if (f) atomicOr(&nb.flags[p], f);
-                __threadfence();
-                if (atomicSub(&nb.children[p], 1u) != 1u) break;
-                __threadfence();
-                cur = (unsigned)p;
-            }
-        }
-    }
-    if (flags) atomicOr(&nb.hdr[kHdrStatus], flags);
-    // the last CTA marks the radiance complete
+// ---- radiance of the descendants ------------------------------------------------------------
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Barrier of a cooperative (co-resident) grid on two header words; the wait is bounded and
+// running out sets NRRS_DEV_TIMEOUT.
+__device__ void grid_barrier(uint32_t* hdr, unsigned spin_limit, unsigned* flags) {
     __syncthreads();
     if (threadIdx.x == 0) {
+        unsigned* count = hdr + kHdrBarCount;
+        unsigned* gen = hdr + kHdrBarGen;
+        const unsigned g = ld_acquire(gen);
         __threadfence();
-        const unsigned old = atomicAdd(&nb.hdr[kHdrDone], 1u);
-        if (old == gridDim.x - 1) {
-            nb.hdr[kHdrDone] = 0;
-            nb.hdr[kHdrPropagated] = 1;
-            __threadfence();
+        if (atomicAdd(count, 1u) == gridDim.x - 1) {
+            *(volatile unsigned*)count = 0;
+            st_release(gen, g + 1u);
+        } else {
+            unsigned spins = 0;
+            while (ld_acquire(gen) == g) {
+                if (++spins > spin_limit) {
+                    *flags |= NRRS_DEV_TIMEOUT;
+                    break;
+                }
+                __nanosleep(64);
+            }
         }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+// Level by level: the nodes of one record call all have their parents in earlier calls, so going
+// from the last call to the first, every node's total is complete when its level comes and is
+// added into its parent once, with atomics and no waiting; a grid barrier separates levels.
+__device__ void propagate_levels(const NodeView& nb, unsigned levels, unsigned spin_limit,
+                                 unsigned* flags) {
+    const unsigned* lt = nb.hdr + kHdrLevelTable;
+    for (int k = (int)levels - 1; k >= 1; --k) {
+        const unsigned lo = lt[k - 1], hi = lt[k];
+        for (unsigned i = lo + blockIdx.x * blockDim.x + threadIdx.x; i < hi;
+             i += gridDim.x * blockDim.x) {
+            const int p = nb.parent[i];
+            if (p < 0) continue;
+            long long l[kLimbs];
+            const long long* src = nb.rad + (size_t)i * kLimbs;
+#pragma unroll
+            for (int q = 0; q < kLimbs; ++q) l[q] = __ldcg(src + q);
+            add_limbs(nb.rad + (size_t)p * kLimbs, l);
+            if (__ldcg(nb.flags + i) & 1u) atomicOr(&nb.flags[p], 1u);
+        }
+        grid_barrier(nb.hdr, spin_limit, flags);
+    }
+}
+
+// Walking the parent chains, for more record calls than the level table keeps. A leaf starts a
+// walk carrying the complete total of the node it stands on. Into an only child's parent the
+// total goes by plain loads and stores: nobody else touches that parent. Into a parent with
+// siblings it goes by atomic additions, and an acquire-release count of arrivals tells the last
+// sibling, which reads the parent's now complete total and carries on. Indices strictly
+// decrease along a chain, so every walk ends.
+__device__ void propagate_chains(const NodeView& nb, unsigned* flags) {
+    const unsigned size = nb.hdr[kHdrSize];
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < size;
+         i += gridDim.x * blockDim.x) {
+        if (nb.first_child[i] != 0xffffffffu) continue;  // not a leaf
+        unsigned cur = i;
+        long long t[kLimbs];
+        const long long* src = nb.rad + (size_t)i * kLimbs;
+#pragma unroll
+        for (int k = 0; k < kLimbs; ++k) t[k] = src[k];
+        unsigned bad = nb.flags[i] & 1u;
+        for (;;) {
+            const int p = nb.parent[cur];
+            if (p < 0) break;
+            if ((unsigned)p >= cur) { *flags |= NRRS_DEV_BAD_INDEX; break; }
+            long long* dst = nb.rad + (size_t)p * kLimbs;
+            const unsigned nc = nb.children[p];
+            if (nc == 1u) {
+                long long own[kLimbs];
+#pragma unroll
+                for (int k = 0; k < kLimbs; ++k) own[k] = dst[k];
+                const unsigned pf = nb.flags[p];
+#pragma unroll
+                for (int k = 0; k < kLimbs; ++k) {
+                    t[k] = (long long)((unsigned long long)t[k] + (unsigned long long)own[k]);
+                    dst[k] = t[k];
+                }
+                bad |= pf & 1u;
+                if (bad && !(pf & 1u)) nb.flags[p] = pf | 1u;
+            } else {
+                add_limbs(dst, t);
+                if (bad) atomicOr(&nb.flags[p], 1u);
+                if (atom_add_acq_rel(&nb.arrived[p], 1u) + 1u != nc) break;
+#pragma unroll
+                for (int k = 0; k < kLimbs; ++k) t[k] = __ldcg(dst + k);
+                bad = __ldcg(nb.flags + p) & 1u;
+            }
+            cur = (unsigned)p;
+        }
+    }
+}
+
+// One cooperative launch; runs once per reset (a later launch returns at once).
+__global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ NodeView nb,
+                                                   unsigned spin_limit) {
+    __shared__ unsigned s_skip, s_levels;
+    if (threadIdx.x == 0) {
+        s_skip = *(volatile unsigned*)&nb.hdr[kHdrPropagated];
+        s_levels = *(volatile unsigned*)&nb.hdr[kHdrLevels];
+    }
+    __syncthreads();
+    if (s_skip) return;  // the same in every CTA: the mark is only set after the last barrier
+    unsigned flags = 0;
+    if (s_levels <= (unsigned)kMaxLevels) propagate_levels(nb, s_levels, spin_limit, &flags);
+    else propagate_chains(nb, &flags);
+    if (flags) atomicOr(&nb.hdr[kHdrStatus], flags);
+    grid_barrier(nb.hdr, spin_limit, &flags);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        nb.hdr[kHdrPropagated] = 1;
+        if (flags & NRRS_DEV_TIMEOUT) atomicOr(&nb.hdr[kHdrStatus], NRRS_DEV_TIMEOUT);
     }
 }
 
 // ---- the training batch, in node order ------------------------------------------------------
 __global__ void __launch_bounds__(kRecThreads) k_generate(const __grid_constant__ GenerateArgs a) {
-    __shared__ unsigned s_chunk, s_epoch, s_prefix;
+    __shared__ unsigned s_chunk, s_epoch;
     __shared__ unsigned s_cnt[kRecPasses * (kRecThreads / 32)];
+    __shared__ LookbackSmem s_lb;
     __shared__ float s_L[kRecPasses][3][kRecThreads];
+    __shared__ float s_stage[kRecThreads / 32][96];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const NodeView& nb = a.nb;
     if (tid == 0) s_epoch = *(volatile unsigned*)&nb.hdr[kHdrEpoch];
     const unsigned size = *(volatile unsigned*)&nb.hdr[kHdrSize];
     const unsigned chunks = (size + kRecChunk - 1) / kRecChunk;
+    const unsigned lt = lanemask_lt();
     unsigned flags = 0;
     for (;;) {
         if (tid == 0) s_chunk = atomicAdd(&nb.hdr[kHdrTicket], 1u);
@@ -397,90 +568,118 @@ __global__ void __launch_bounds__(kRecThreads) k_generate(const __grid_constant_
             const unsigned i = i0 + j * kRecThreads + tid;
             bool keep = false, same = false;
             if (i < size) {
-                const long long* r = nb.rad + (size_t)i * kLimbs;
+                long long r[kLimbs];
+                const long long* rp = nb.rad + (size_t)i * kLimbs;
+#pragma unroll
+                for (int k = 0; k < kLimbs; ++k) r[k] = rp[k];
+                float th[3], ps[3], w[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    th[k] = nb.thp[3 * (size_t)i + k];
+                    ps[k] = nb.pos[3 * (size_t)i + k];
+                    w[k] = nb.wi[3 * (size_t)i + k];
+                }
+                const unsigned nf = nb.flags[i];
+                const int p = a.dedupe ? nb.parent[i] : -1;
+                unsigned fc = 0;
+                if (p >= 0) {
+                    if ((unsigned)p < i) fc = nb.first_child[p];
+                    else flags |= NRRS_DEV_BAD_INDEX;
+                }
                 float L[3];
-                bool finite = nb.flags[i] == 0;
 #pragma unroll
                 for (int ch = 0; ch < 3; ++ch) {
                     const float rad = fixed_to_float(r[3 * ch], r[3 * ch + 1], r[3 * ch + 2]);
-                    const float t = nb.thp[3 * (size_t)i + ch];
                     float l = 0.f;
-                    if (t > a.thp_eps) l = __fdiv_rn(rad, t);
+                    if (th[ch] > a.thp_eps) l = __fdiv_rn(rad, th[ch]);
                     L[ch] = l < 0.f ? 0.f : l;  // max(L, 0): a NaN stays NaN
                     s_L[j][ch][tid] = L[ch];
                 }
                 const float mean = __fdiv_rn(__fadd_rn(__fadd_rn(L[0], L[1]), L[2]), 3.0f);
                 bool nan = false;
 #pragma unroll
-                for (int k = 0; k < 3; ++k)
-                    nan |= isnan(nb.pos[3 * (size_t)i + k]) || isnan(L[k]);
-                nan |= isnan(nb.wi[3 * (size_t)i]) || isnan(nb.wi[3 * (size_t)i + 1]) ||
-                       isnan(nb.wi[3 * (size_t)i + 2]);
-                keep = finite && !nan && (!a.ignore_zero_l || mean > 0.f);
-                if (a.dedupe) {
-                    const int p = nb.parent[i];
-                    if (p >= 0) {
-                        if ((unsigned)p < i) same = nb.first_child[p] != i;
-                        else flags |= NRRS_DEV_BAD_INDEX;
-                    }
-                }
+                for (int k = 0; k < 3; ++k) nan |= isnan(ps[k]) || isnan(w[k]) || isnan(L[k]);
+                keep = (nf & 1u) == 0 && !nan && (!a.ignore_zero_l || mean > 0.f);
+                same = p >= 0 && (unsigned)p < i && fc != i;
             }
             m[j] = __ballot_sync(0xffffffffu, keep);
             same_m[j] = __ballot_sync(0xffffffffu, same);
             if (lane == 0) s_cnt[j * (kRecThreads / 32) + wid] = __popc(m[j]);
         }
         __syncthreads();
-        if (wid == 0) {
-            const unsigned total = scan64(s_cnt);
-            const unsigned prefix = lookback(nb.states, c, s_epoch, total, 0u, a.spin_limit, &flags);
-            if (lane == 0) {
-                s_prefix = prefix;
-                if (c == chunks - 1) {
-                    const unsigned end = sat_add(prefix, total);
-                    *a.size_dev = end < a.capacity ? end : a.capacity;
-                    if (end > a.capacity) flags |= NRRS_DEV_OVERFLOW;
-                }
-            }
-        }
+        unsigned total = 0;
+        if (wid == 0) total = scan_counts(s_cnt);
+        if (tid == 0) s_lb.part[0] = total;
         __syncthreads();
-        const unsigned lt = lanemask_lt();
+        total = (unsigned)s_lb.part[0];
+        __syncthreads();
+        const unsigned prefix = lookback_block(nb.states, c, s_epoch, total, 0u, a.spin_limit,
+                                               &flags, s_lb);
+        if (tid == 0 && c == chunks - 1) {
+            const unsigned end = sat_add(prefix, total);
+            *a.size_dev = end < a.capacity ? end : a.capacity;
+            if (end > a.capacity) flags |= NRRS_DEV_OVERFLOW;
+        }
         const nrrs_train_batch& o = a.out;
 #pragma unroll
         for (int j = 0; j < kRecPasses; ++j) {
-            if (!((m[j] >> lane) & 1u)) continue;
             const unsigned i = i0 + j * kRecThreads + tid;
-            const unsigned long long t64 = (unsigned long long)s_prefix +
-                s_cnt[j * (kRecThreads / 32) + wid] + __popc(m[j] & lt);
-            if (t64 >= a.capacity) continue;
-            const size_t t = (size_t)t64;
+            const bool active = (m[j] >> lane) & 1u;
+            const unsigned rank = __popc(m[j] & lt);
+            const unsigned long long base = (unsigned long long)prefix + s_cnt[j * (kRecThreads / 32) + wid];
+            const unsigned cnt = __popc(m[j]);
+            const unsigned room = base >= a.capacity ? 0u
+                                  : (unsigned)min((unsigned long long)cnt, a.capacity - base);
+            if (room == 0) continue;  // warp-uniform
+            const bool keep = active && rank < room;
             const bool same = (same_m[j] >> lane) & 1u;
-            const float rrs = nb.rrs[i];
-            const unsigned px = nb.pixel[i];
+            // every field first, then the stores
+            float q[15], rough = 0.f, rrs = 0.f, rm = 0.f;
+            unsigned px = 0, dep = 0;
 #pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                if (o.pos) o.pos[3 * t + k] = nb.pos[3 * (size_t)i + k];
-                if (o.wi) o.wi[3 * t + k] = nb.wi[3 * (size_t)i + k];
-                if (o.normal) o.normal[3 * t + k] = nb.normal[3 * (size_t)i + k];
-                if (o.albedo) o.albedo[3 * t + k] = nb.albedo[3 * (size_t)i + k];
-                if (o.target) o.target[3 * t + k] = s_L[j][k][tid];
-                const float th = nb.thp[3 * (size_t)i + k];
-                if (o.thp) o.thp[3 * t + k] = a.copy_rrs_node ? __fmul_rn(th, rrs) : th;
-            }
-            if (o.roughness) o.roughness[t] = nb.rough[i];
-            if (o.depth) o.depth[t] = nb.depth[i];
-            if (o.rrs_target) o.rrs_target[t] = same ? -1.0f : rrs;
-            if (o.pixel) o.pixel[t] = px;
-            const bool px_ok = px < a.n_pixels;
-            if (!px_ok && (a.image || a.pixel_samples)) flags |= NRRS_DEV_BAD_INDEX;
-            if (o.ref_mean && a.image) {
-                float rm = 0.f;
-                if (px_ok) {
-                    const float* q = a.image + (size_t)px * a.channels;
-                    rm = __fdiv_rn(__fadd_rn(__fadd_rn(q[0], q[1]), q[2]), 3.0f);
+            for (int k = 0; k < 15; ++k) q[k] = 0.f;
+            bool px_ok = false;
+            if (keep) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const size_t si = 3 * (size_t)i + k;
+                    q[k] = nb.pos[si];
+                    q[3 + k] = nb.wi[si];
+                    q[6 + k] = nb.normal[si];
+                    q[9 + k] = nb.albedo[si];
+                    q[12 + k] = nb.thp[si];
                 }
-                o.ref_mean[t] = rm;
+                rough = nb.rough[i];
+                rrs = nb.rrs[i];
+                dep = nb.depth[i];
+                px = nb.pixel[i];
+                px_ok = px < a.n_pixels;
+                if (px_ok && a.image) {
+                    const float* im = a.image + (size_t)px * a.channels;
+                    rm = __fdiv_rn(__fadd_rn(__fadd_rn(im[0], im[1]), im[2]), 3.0f);
+                }
+                if (a.copy_rrs_node) {
+#pragma unroll
+                    for (int k = 12; k < 15; ++k) q[k] = __fmul_rn(q[k], rrs);
+                }
             }
-            if (!same && px_ok && a.pixel_samples) atomicAdd(&a.pixel_samples[px], 1u);
+            const size_t t = (size_t)(base + rank);
+            if (o.pos) store3_compact(o.pos + 3 * base, keep, rank, room, q[0], q[1], q[2], s_stage[wid]);
+            if (o.wi) store3_compact(o.wi + 3 * base, keep, rank, room, q[3], q[4], q[5], s_stage[wid]);
+            if (o.normal) store3_compact(o.normal + 3 * base, keep, rank, room, q[6], q[7], q[8], s_stage[wid]);
+            if (o.albedo) store3_compact(o.albedo + 3 * base, keep, rank, room, q[9], q[10], q[11], s_stage[wid]);
+            if (o.thp) store3_compact(o.thp + 3 * base, keep, rank, room, q[12], q[13], q[14], s_stage[wid]);
+            if (o.target) store3_compact(o.target + 3 * base, keep, rank, room, s_L[j][0][tid],
+                                         s_L[j][1][tid], s_L[j][2][tid], s_stage[wid]);
+            if (keep) {
+                if (o.roughness) o.roughness[t] = rough;
+                if (o.depth) o.depth[t] = dep;
+                if (o.rrs_target) o.rrs_target[t] = same ? -1.0f : rrs;
+                if (o.pixel) o.pixel[t] = px;
+                if (!px_ok && (a.image || a.pixel_samples)) flags |= NRRS_DEV_BAD_INDEX;
+                if (o.ref_mean && a.image) o.ref_mean[t] = rm;
+                if (!same && px_ok && a.pixel_samples) atomicAdd(&a.pixel_samples[px], 1u);
+            }
         }
         __syncthreads();
     }
@@ -511,9 +710,20 @@ cudaError_t launch_record_radiance(const RadianceArgs& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_propagate(const NodeView& nb, int grid, cudaStream_t s) {
-    k_propagate<<<grid, 256, 0, s>>>(nb);
-    return cudaGetLastError();
+cudaError_t launch_propagate(const NodeView& nb, cudaStream_t s) {
+    // co-resident grid: SMs x resident CTAs of k_propagate
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_propagate, 256, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    const int grid = sms * (per_sm < 4 ? per_sm : 4);
+    NodeView v = nb;
+    unsigned spin = 1u << 22;
+    void* args[] = {&v, &spin};
+    return cudaLaunchCooperativeKernel((const void*)k_propagate, dim3(grid), dim3(256), args, 0, s);
 }
 
 cudaError_t launch_generate(const GenerateArgs& a, int grid, cudaStream_t s) {

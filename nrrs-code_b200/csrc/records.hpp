@@ -18,15 +18,21 @@ enum : int {
     kHdrSize = 0,        // nodes recorded, <= capacity
     kHdrDropped = 1,     // records refused at capacity (mInvalidNode)
     kHdrPropagated = 2,  // 1 once node radiance includes the descendants' contributions
-    kHdrStatus = 3,      // NRRS_DEV_* bits
-    kHdrTicket = 4,      // scan chunk tickets of the running launch
-    kHdrDone = 5,        // CTAs finished in the running launch
-    kHdrEpoch = 6,       // launch counter tagging the look-back states
-    kHdrWords = 16
+    kHdrLevels = 3,      // record calls since the reset (kMaxLevels + 1: too many to keep)
+    kHdrStatus = 4,      // NRRS_DEV_* bits
+    kHdrTicket = 5,      // scan chunk tickets of the running launch
+    kHdrDone = 6,        // CTAs finished in the running launch
+    kHdrEpoch = 7,       // launch counter tagging the look-back states
+    kHdrBarCount = 8,    // grid barrier of the radiance pass: arrivals
+    kHdrBarGen = 9,      //   and generation
+    kHdrCallBase = 10,   // u64 (words 10-11): epoch << 32 | node count when the call started
+    kHdrLevelTable = 32, // node count after each record call since the reset
+    kHdrWords = 128
 };
+constexpr int kMaxLevels = 64;
 
 constexpr int kRecThreads = 256;
-constexpr int kRecPasses = 8;
+constexpr int kRecPasses = 4;
 constexpr int kRecChunk = kRecThreads * kRecPasses;  // vertices (or nodes) per scan chunk
 constexpr int kLimbs = 9;                            // 3 channels x 3 limbs of the radiance
 
@@ -44,6 +50,7 @@ struct NodeView {
     long long* rad;  // [capacity][kLimbs]
     uint32_t* first_child;
     uint32_t* children;
+    uint32_t* arrived;
     uint32_t* flags;
     uint32_t* hdr;
     unsigned long long* states;
@@ -95,8 +102,10 @@ struct WeightArgs {
 
 cudaError_t launch_record_nodes(const RecordArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_record_radiance(const RadianceArgs& a, cudaStream_t s);
-// completes every node's radiance with its descendants' (once per reset), then builds the batch
-cudaError_t launch_propagate(const NodeView& nb, int grid, cudaStream_t s);
+// completes every node's radiance with its descendants' (once per reset): level by level in one
+// cooperative launch when the record calls since the reset are at most kMaxLevels, else by
+// walking the parent chains
+cudaError_t launch_propagate(const NodeView& nb, cudaStream_t s);
 cudaError_t launch_generate(const GenerateArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_sample_weights(const WeightArgs& a, cudaStream_t s);
 

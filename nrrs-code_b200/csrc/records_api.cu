@@ -24,7 +24,7 @@ uint32_t scan_chunks(uint32_t capacity, uint32_t max_record) {
 // byte offsets of every array in the block; returns the total
 struct Layout {
     uint64_t hdr, states, pos, wi, normal, albedo, rough, thp, parent, pixel, rrs, depth, rad,
-        first_child, children, flags, total;
+        first_child, children, arrived, flags, total;
 };
 
 Layout layout(uint32_t capacity, uint32_t max_record) {
@@ -47,6 +47,7 @@ Layout layout(uint32_t capacity, uint32_t max_record) {
     L.rad = take(8ull * kLimbs * C);
     L.first_child = take(4 * C);
     L.children = take(4 * C);
+    L.arrived = take(4 * C);
     L.flags = take(4 * C);
     L.total = o;
     return L;
@@ -67,6 +68,7 @@ NodeView view(const nrrs_path_nodes* n) {
     v.rad = reinterpret_cast<long long*>(n->radiance);
     v.first_child = n->first_child;
     v.children = n->children;
+    v.arrived = n->arrived;
     v.flags = n->node_flags;
     v.hdr = n->header;
     v.states = reinterpret_cast<unsigned long long*>(n->scan_states);
@@ -77,7 +79,7 @@ NodeView view(const nrrs_path_nodes* n) {
 bool valid(const nrrs_path_nodes* n) {
     return n && n->capacity && n->header && n->scan_states && n->pos && n->wi && n->normal &&
            n->albedo && n->roughness && n->thp && n->parent && n->pixel && n->rrs && n->depth &&
-           n->radiance && n->first_child && n->children && n->node_flags;
+           n->radiance && n->first_child && n->children && n->arrived && n->node_flags;
 }
 
 // persistent grids: SMs x resident CTAs, looked up once per device
@@ -138,6 +140,7 @@ extern "C" int nrrs_path_nodes_init(void* dev_mem, uint64_t bytes, uint32_t capa
     n.radiance = reinterpret_cast<int64_t*>(b + L.rad);
     n.first_child = reinterpret_cast<uint32_t*>(b + L.first_child);
     n.children = reinterpret_cast<uint32_t*>(b + L.children);
+    n.arrived = reinterpret_cast<uint32_t*>(b + L.arrived);
     n.node_flags = reinterpret_cast<uint32_t*>(b + L.flags);
     n.header = reinterpret_cast<uint32_t*>(b + L.hdr);
     n.scan_states = reinterpret_cast<uint64_t*>(b + L.states);
@@ -149,10 +152,11 @@ extern "C" int nrrs_path_nodes_init(void* dev_mem, uint64_t bytes, uint32_t capa
 
 extern "C" int nrrs_path_nodes_reset(const nrrs_path_nodes* nodes, void* stream) {
     if (!valid(nodes)) return NRRS_ERR_INVALID_ARG;
-    // size, dropped and the radiance-complete mark; the epoch keeps counting so that no stale
-    // look-back state can match a later launch
-    static_assert(kHdrSize == 0 && kHdrDropped == 1 && kHdrPropagated == 2, "header layout");
-    return cudaMemsetAsync(nodes->header, 0, 3 * sizeof(uint32_t), (cudaStream_t)stream) ==
+    // size, dropped, the radiance-complete mark and the record calls; the epoch and the barrier
+    // keep counting so that no stale look-back state or arrival can match a later launch
+    static_assert(kHdrSize == 0 && kHdrDropped == 1 && kHdrPropagated == 2 && kHdrLevels == 3,
+                  "header layout");
+    return cudaMemsetAsync(nodes->header, 0, 4 * sizeof(uint32_t), (cudaStream_t)stream) ==
                    cudaSuccess ? NRRS_OK : NRRS_ERR_CUDA;
 }
 
@@ -227,9 +231,8 @@ extern "C" int nrrs_generate_training_data(const nrrs_path_nodes* nodes,
     if (!(p->thp_eps >= 0.f)) return NRRS_ERR_INVALID_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const NodeView nb = view(nodes);
-    const int gp = persistent_grid(nodes->capacity, 256, 8);
-    if (gp <= 0) return NRRS_ERR_NO_DEVICE;
-    if (launch_propagate(nb, gp, s) != cudaSuccess) return NRRS_ERR_CUDA;
+    if (sm_count() <= 0) return NRRS_ERR_NO_DEVICE;
+    if (launch_propagate(nb, s) != cudaSuccess) return NRRS_ERR_CUDA;
     GenerateArgs a{};
     a.nb = nb;
     a.out = *out;

@@ -77,7 +77,8 @@ class PathNodes(C.Structure):
     _fields_ = [("capacity", C.c_uint32), ("max_record", C.c_uint32)] + [
         (n, C.c_void_p) for n in ("pos", "wi", "normal", "albedo", "roughness", "thp", "parent",
                                   "pixel", "rrs",
-                                  "depth", "radiance", "first_child", "children", "node_flags",
+                                  "depth", "radiance", "first_child", "children", "arrived",
+                                  "node_flags",
                                   "header", "scan_states")]
 
 

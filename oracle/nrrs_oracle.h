@@ -85,6 +85,7 @@ void oracle_adam_f32(const nrrs_config* cfg, float* params, const float* grads, 
 void oracle_fixed_limbs(float x, int64_t* l);
 float oracle_fixed_to_float(int64_t l0, int64_t l1, int64_t l2);
 float oracle_fixed_to_float_gcc(int64_t l0, int64_t l1, int64_t l2);
+float oracle_fixed_to_float_fast(int64_t l0, int64_t l1, int64_t l2);
 void oracle_nodes_reset(nrrs_path_nodes* nb);
 void oracle_record_nodes(nrrs_path_nodes* nb, const nrrs_vertex_soa* v, const int32_t* parent,
                          const uint32_t* pixel, const float* rrs, const uint8_t* record,

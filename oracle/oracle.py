@@ -74,7 +74,8 @@ def lib():
         L.oracle_adam_f32.argtypes = [C.POINTER(nb.Config), vp, vp, vp, vp, C.c_uint64,
                                       C.c_uint64, C.c_uint64]
         L.oracle_fixed_limbs.argtypes = [C.c_float, vp]
-        for f in ("oracle_fixed_to_float", "oracle_fixed_to_float_gcc"):
+        for f in ("oracle_fixed_to_float", "oracle_fixed_to_float_gcc",
+                  "oracle_fixed_to_float_fast"):
             getattr(L, f).restype = C.c_float
             getattr(L, f).argtypes = [C.c_int64, C.c_int64, C.c_int64]
         L.oracle_nodes_reset.argtypes = [C.POINTER(nb.PathNodes)]
@@ -231,8 +232,9 @@ def fixed_limbs(x: float) -> tuple[int, int, int]:
     return int(out[0]), int(out[1]), int(out[2])
 
 
-def fixed_to_float(l0: int, l1: int, l2: int, gcc: bool = False) -> float:
-    f = lib().oracle_fixed_to_float_gcc if gcc else lib().oracle_fixed_to_float
+def fixed_to_float(l0: int, l1: int, l2: int, gcc: bool = False, fast: bool = False) -> float:
+    f = (lib().oracle_fixed_to_float_gcc if gcc else
+         lib().oracle_fixed_to_float_fast if fast else lib().oracle_fixed_to_float)
     return float(f(l0, l1, l2))
 
 
@@ -241,6 +243,7 @@ NODE_ARRAYS = {"pos": (np.float32, 3), "wi": (np.float32, 3), "normal": (np.floa
                "thp": (np.float32, 3), "parent": (np.int32, 1), "pixel": (np.uint32, 1),
                "rrs": (np.float32, 1), "depth": (np.uint32, 1), "radiance": (np.int64, 9),
                "first_child": (np.uint32, 1), "children": (np.uint32, 1),
+               "arrived": (np.uint32, 1),
                "node_flags": (np.uint32, 1)}
 
 
@@ -266,7 +269,7 @@ class HostNodes:
 
     @property
     def status(self) -> int:
-        return int(self.header[3])
+        return int(self.header[4])
 
     def reset(self):
         lib().oracle_nodes_reset(C.byref(self.nodes))

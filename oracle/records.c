@@ -23,7 +23,7 @@
 
 #include "nrrs_oracle.h"
 
-enum { HDR_SIZE = 0, HDR_DROPPED = 1, HDR_STATUS = 3 };
+enum { HDR_SIZE = 0, HDR_DROPPED = 1, HDR_STATUS = 4 };
 
 #define FIXED_MAX 4611686018427387904.0f /* 2^62 */
 
@@ -72,6 +72,26 @@ float oracle_fixed_to_float(int64_t l0, int64_t l1, int64_t l2) {
     return f;
 }
 
+/* The library's formulation of the same rounding: the top 64 bits of the magnitude with the
+ * bits below folded into bit 0, one correctly rounded u64 -> float conversion, an exact
+ * power-of-two scale. Must equal oracle_fixed_to_float everywhere. */
+float oracle_fixed_to_float_fast(int64_t l0, int64_t l1, int64_t l2) {
+    typedef unsigned __int128 u128;
+    const u128 U = ((u128)(__int128)l2 << 64) + ((u128)(__int128)l1 << 32) + (u128)(__int128)l0;
+    const uint32_t neg = (uint32_t)(U >> 127) & 1u;
+    const u128 mag = neg ? (u128)0 - U : U;
+    const uint64_t hi = (uint64_t)(mag >> 64), lo = (uint64_t)mag;
+    float f;
+    if (hi == 0) {
+        f = (float)lo * 0x1p-64f;
+    } else {
+        const int sh = 64 - __builtin_clzll(hi);
+        const uint64_t top = (hi << (64 - sh)) | (lo >> sh) | ((lo << (64 - sh)) != 0 ? 1u : 0u);
+        f = ldexpf((float)top, sh - 64);
+    }
+    return neg ? -f : f;
+}
+
 /* the same value through gcc's own __int128 -> float conversion (round to nearest), for tests */
 float oracle_fixed_to_float_gcc(int64_t l0, int64_t l1, int64_t l2) {
     typedef unsigned __int128 u128;
@@ -83,6 +103,7 @@ void oracle_nodes_reset(nrrs_path_nodes* nb) {
     nb->header[HDR_SIZE] = 0;
     nb->header[HDR_DROPPED] = 0;
     nb->header[2] = 0;
+    nb->header[3] = 0;
 }
 
 /* recordNode (workqueue.h:142-170) for each recorded vertex, in vertex order; node_out[i] =
@@ -91,8 +112,12 @@ void oracle_nodes_reset(nrrs_path_nodes* nb) {
 void oracle_record_nodes(nrrs_path_nodes* nb, const nrrs_vertex_soa* v, const int32_t* parent,
                          const uint32_t* pixel, const float* rrs, const uint8_t* record,
                          uint64_t n, int32_t* node_out) {
+    const uint32_t call0 = nb->header[HDR_SIZE];  /* nodes of earlier calls: [0, call0) */
     for (uint64_t i = 0; i < n; ++i) {
         const int32_t p = parent[i];
+        /* a parent must be a node of an earlier call: any other link is cut and flagged */
+        const int bad_parent = p >= 0 && (uint32_t)p >= call0;
+        const int32_t pn = bad_parent ? -1 : p;
         int32_t out = p;
         if (!record || record[i]) {
             const uint32_t idx = nb->header[HDR_SIZE];
@@ -107,7 +132,7 @@ void oracle_record_nodes(nrrs_path_nodes* nb, const nrrs_vertex_soa* v, const in
                     nb->thp[di] = v->thp[si];
                 }
                 nb->roughness[idx] = v->roughness ? v->roughness[i] : 0.f;
-                nb->parent[idx] = p;
+                nb->parent[idx] = pn;
                 nb->pixel[idx] = pixel[i];
                 nb->rrs[idx] = rrs ? rrs[i] : 1.f;  /* the work item's default (device.cu:83) */
                 nb->depth[idx] = v->depth ? v->depth[i] : 0u;
@@ -115,14 +140,11 @@ void oracle_record_nodes(nrrs_path_nodes* nb, const nrrs_vertex_soa* v, const in
                 nb->first_child[idx] = 0xffffffffu;
                 nb->children[idx] = 0;
                 nb->node_flags[idx] = 0;
-                if (p >= 0) {
-                    if ((uint32_t)p < idx) {
-                        if (idx < nb->first_child[p]) nb->first_child[p] = idx;
-                        nb->children[p] += 1;
-                    } else {
-                        nb->header[HDR_STATUS] |= NRRS_DEV_BAD_INDEX;
-                    }
+                if (pn >= 0) {
+                    if (idx < nb->first_child[pn]) nb->first_child[pn] = idx;
+                    nb->children[pn] += 1;
                 }
+                if (bad_parent) nb->header[HDR_STATUS] |= NRRS_DEV_BAD_INDEX;
                 out = (int32_t)idx;
             } else {
                 nb->header[HDR_DROPPED] += 1;  /* mInvalidNode */

@@ -12,7 +12,7 @@ import pytest
 import nrrs_b200 as nb
 import oracle as O
 from gpu_util import host, make_net, random_params, stream, torch_cuda
-from test_records_oracle import CASES, bounce_arrays, check_against_expect
+from test_records_oracle import CASES, bounce_arrays, check_against_expect, split_calls
 
 pytestmark = pytest.mark.gpu
 
@@ -22,7 +22,8 @@ NODE_FIELDS = {"pos": (np.float32, 3), "wi": (np.float32, 3), "normal": (np.floa
                "albedo": (np.float32, 3), "roughness": (np.float32, 1), "thp": (np.float32, 3),
                "parent": (np.int32, 1), "pixel": (np.uint32, 1), "rrs": (np.float32, 1),
                "depth": (np.uint32, 1), "radiance": (np.int64, 9),
-               "first_child": (np.uint32, 1), "node_flags": (np.uint32, 1)}
+               "first_child": (np.uint32, 1), "children": (np.uint32, 1),
+               "node_flags": (np.uint32, 1)}
 BATCH_SHAPES = {"pos": 3, "wi": 3, "normal": 3, "albedo": 3, "roughness": 1, "thp": 3, "depth": 1,
                 "ref_mean": 1, "target": 3, "rrs_target": 1, "pixel": 1}
 
@@ -327,3 +328,29 @@ def test_gpu_batch_feeds_the_training_step():
     _, l64 = O.train_grads(net.config, p0, ob, ob["target"], "f64")
     assert host(loss) == pytest.approx(l64, rel=1e-4)
     net.close()
+
+
+def test_gpu_parent_in_the_same_call_is_cut():
+    g = GpuNodes(16, 4)
+    hn = O.HostNodes(16)
+    b = dict(pos=np.zeros((3, 3), np.float32), wi=np.ones((3, 3), np.float32),
+             thp=np.ones((3, 3), np.float32), pixel=np.zeros(3, np.uint32),
+             parent=np.array([-1, 0, 7], np.int32))
+    b2 = dict(b, parent=np.array([2, 4, 1], np.int32))
+    for x in (b, b2):
+        assert host(g.record(x)).tolist() == hn.record_nodes(x).tolist()
+    for k in ("parent", "first_child", "children"):
+        assert g.field(k, 6).tobytes() == hn.a[k][:6].tobytes(), k
+    assert g.pn.status(stream()) == (6, 0, nb.DEV_BAD_INDEX)
+
+
+@pytest.mark.parametrize("parts", [8, 9])
+def test_gpu_many_record_calls(parts):
+    """8 bounces in `parts` calls each: 64 calls keep the level table (level-by-level radiance
+    pass), 72 overflow it (the chain walk); both must match the oracle bit for bit."""
+    bounces, image = nb.synth_paths(91, 6000, capacity=24000)
+    calls = split_calls(bounces, parts)
+    prm = PARAMS["filters"]
+    o = O.frame_training_data(calls, image, 24000, prm)
+    r = run_frame(calls, image, 24000, prm)
+    assert_frame_matches_oracle(r, o, calls, 24000)

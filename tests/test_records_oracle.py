@@ -83,7 +83,9 @@ def test_fixed_point_conversion_matches_gcc_rounding():
     for l0, l1, l2 in cases:
         a = O.fixed_to_float(l0, l1, l2)
         g = O.fixed_to_float(l0, l1, l2, gcc=True)
+        f = O.fixed_to_float(l0, l1, l2, fast=True)
         assert np.float32(a).tobytes() == np.float32(g).tobytes(), (l0, l1, l2, a, g)
+        assert np.float32(a).tobytes() == np.float32(f).tobytes(), (l0, l1, l2, a, f)
 
 
 def test_fixed_point_round_trip_and_truncation():
@@ -151,7 +153,7 @@ def test_oracle_capacity_overflow_falls_back_to_parent():
     want = sum(int(b["record"].sum()) for b in bounces) - 3000
     assert hn.dropped == want > 0 and hn.status & nb.DEV_OVERFLOW
     # a batch capacity below the sample count keeps the first samples and flags overflow
-    hn.header[3] = 0
+    hn.header[4] = 0
     batch, total = hn.generate(nb.default_train_data_params(), 100)
     assert total > 100 and len(batch["target"]) == 100 and hn.status & nb.DEV_OVERFLOW
     full, total2 = hn.generate(nb.default_train_data_params(), total)
@@ -165,3 +167,48 @@ def test_sample_weight_matches_reference_formula():
     w = O.sample_weights(px, counts, 4)
     assert w.tolist() == [1.0, np.float32(1) / np.float32(3), 0.0, 0.0, 0.0]
     assert math.isclose(w[1], 1 / 3, rel_tol=1e-7)
+
+
+def test_parent_recorded_in_the_same_call_is_cut():
+    """Parents must be nodes of earlier record calls; a link to a node of the same call (or to no
+    node yet) is stored as -1 and flagged, so node trees stay levelled by call."""
+    hn = O.HostNodes(16)
+    b = dict(pos=np.zeros((3, 3), np.float32), wi=np.ones((3, 3), np.float32),
+             thp=np.ones((3, 3), np.float32), pixel=np.zeros(3, np.uint32),
+             parent=np.array([-1, 0, 7], np.int32))
+    out = hn.record_nodes(b)
+    assert out.tolist() == [0, 1, 2]
+    assert hn.a["parent"][:3].tolist() == [-1, -1, -1]
+    assert hn.status == nb.DEV_BAD_INDEX
+    assert hn.a["children"][:3].tolist() == [0, 0, 0]
+    b2 = dict(b, parent=np.array([2, 4, 1], np.int32))   # 2 and 1: earlier call; 4: this call
+    out = hn.record_nodes(b2)
+    assert out.tolist() == [3, 4, 5]
+    assert hn.a["parent"][3:6].tolist() == [2, -1, 1]
+    assert hn.a["first_child"][:3].tolist() == [0xffffffff, 5, 3]
+
+
+def split_calls(bounces, parts: int):
+    """Each bounce recorded in `parts` consecutive slices (more record calls, same nodes)."""
+    out = []
+    for b in bounces:
+        n = len(b["pixel"])
+        cuts = np.linspace(0, n, parts + 1).astype(int)
+        node_keys = ("pos", "wi", "normal", "albedo", "roughness", "thp", "depth", "pixel", "rrs",
+                     "record", "parent", "node")
+        for k in range(parts):
+            s = {key: np.ascontiguousarray(b[key][cuts[k]:cuts[k + 1]]) for key in node_keys}
+            s["contrib_node"] = b["contrib_node"] if k == parts - 1 else b["contrib_node"][:0]
+            s["contrib"] = b["contrib"] if k == parts - 1 else b["contrib"][:0]
+            out.append(s)
+    return out
+
+
+def test_oracle_split_calls_give_the_same_frame():
+    bounces, image = nb.synth_paths(14, 3000, capacity=12000)
+    prm = nb.default_train_data_params(dedupe_rrs_target=1)
+    a = O.frame_training_data(bounces, image, 12000, prm)
+    b = O.frame_training_data(split_calls(bounces, 9), image, 12000, prm)
+    for k in a["batch"]:
+        assert a["batch"][k].tobytes() == b["batch"][k].tobytes()
+    assert a["nodes"].status == b["nodes"].status == 0
