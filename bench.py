@@ -775,7 +775,9 @@ def run_records(args, rank, world, local_rank):
         if post:
             post("image")
 
-    launches_per_step = 2 * len(bounces) + 3   # + propagate, generate, weights (zero_ is torch's)
+    # per bounce: record count, record writes, radiance; then radiance pass, batch, weights
+    # (the counts' zero_ is torch's)
+    launches_per_step = 3 * len(bounces) + 3
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()

@@ -25,6 +25,7 @@
 #include <cmath>
 
 #include "records.hpp"
+#include "tc_ptx.cuh"
 
 namespace nrrs {
 
@@ -228,147 +229,228 @@ __device__ __forceinline__ bool finish_launch(uint32_t* hdr) {
 }
 
 // ---- recordNode for a wavefront -------------------------------------------------------------
-__global__ void __launch_bounds__(kRecThreads) k_record_nodes(const __grid_constant__ RecordArgs a) {
-    __shared__ unsigned s_chunk, s_epoch, s_size0;
+// One chunk of the wavefront's inputs at a time in shared memory: with BULK every array of a full
+// chunk arrives by one unicast bulk copy each on one mbarrier (all bytes in flight at once); the
+// last, partial chunk and inputs not 16-byte aligned are copied by the threads in coalesced
+// loops. Two CTAs per SM.
+struct RecordStage {
+    float pos[3 * kRecChunk], wi[3 * kRecChunk], nrm[3 * kRecChunk], alb[3 * kRecChunk],
+        thp[3 * kRecChunk];
+    float rough[kRecChunk], rrs[kRecChunk];
+    unsigned depth[kRecChunk], pixel[kRecChunk];
+    int parent[kRecChunk];
+    uint8_t record[kRecChunk];
+    uint64_t bar;
+};
+
+template <typename T>
+__device__ __forceinline__ void copy_in(T* dst, const T* __restrict__ src, unsigned count) {
+    for (unsigned j = threadIdx.x; j < count; j += kRecThreads) dst[j] = src[j];
+}
+
+// Counts of the chunks' records; the last CTA to finish turns them into node offsets (from the
+// node count at the start of the call), sets the new node count and appends the call to the
+// level table. No CTA waits for another.
+__global__ void __launch_bounds__(kRecThreads) k_record_count(const __grid_constant__ RecordArgs a) {
+    __shared__ unsigned s_part[kRecThreads / 32];
+    __shared__ unsigned s_last;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const NodeView& nb = a.nb;
+    const unsigned c = blockIdx.x, v0 = c * kRecChunk;
+    const unsigned cnt_c = min((unsigned)kRecChunk, a.n - v0);
+    unsigned k = 0;
+    if (a.record) {
+#pragma unroll
+        for (int j = 0; j < kRecPasses; ++j) {
+            const unsigned lv = j * kRecThreads + tid;
+            k += (lv < cnt_c && a.record[v0 + lv] != 0) ? 1u : 0u;
+        }
+    } else if (tid == 0) {
+        k = cnt_c;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) k += __shfl_xor_sync(0xffffffffu, k, o);
+    if (lane == 0) s_part[wid] = k;
+    __syncthreads();
+    if (tid == 0) {
+        unsigned t = 0;
+#pragma unroll
+        for (int w = 0; w < kRecThreads / 32; ++w) t += s_part[w];
+        a.chunk_count[c] = t;
+        __threadfence();
+        s_last = atomicAdd(&nb.hdr[kHdrDone], 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    // ---- the last CTA: exclusive scan of every chunk's count ----
+    __threadfence();
+    const unsigned chunks = a.chunks;
+    const unsigned per = (chunks + kRecThreads - 1) / kRecThreads;  // a strip per thread
+    const unsigned lo = min(chunks, tid * per), hi = min(chunks, lo + per);
+    unsigned long long strip = 0;
+    for (unsigned q = lo; q < hi; ++q) strip += __ldcg(a.chunk_count + q);
+    // block exclusive scan of the strip sums
+    unsigned long long incl = strip;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    __shared__ unsigned long long s_w[kRecThreads / 32];
+    if (lane == 31) s_w[wid] = incl;
+    __syncthreads();
+    unsigned long long before = 0;
+    for (int w = 0; w < wid; ++w) before += s_w[w];
+    const unsigned base = *(volatile unsigned*)&nb.hdr[kHdrSize];
+    unsigned long long run = base + before + incl - strip;
+    for (unsigned q = lo; q < hi; ++q) {
+        a.chunk_offset[q] = run > 0xffffffffull ? 0xffffffffu : (unsigned)run;
+        run += __ldcg(a.chunk_count + q);
+    }
+    __syncthreads();
+    if (tid == kRecThreads - 1) {
+        const unsigned long long end = run;   // the last thread's strip ends the scan
+        const unsigned sz = end < nb.capacity ? (unsigned)end : nb.capacity;
+        nb.hdr[kHdrCallBase] = base;
+        nb.hdr[kHdrSize] = sz;
+        const unsigned L = nb.hdr[kHdrLevels];
+        if (L < (unsigned)kMaxLevels) nb.hdr[kHdrLevelTable + L] = sz;
+        if (L <= (unsigned)kMaxLevels) nb.hdr[kHdrLevels] = L + 1;
+        nb.hdr[kHdrDone] = 0;
+        __threadfence();
+    }
+}
+
+// The writes: every chunk knows its first node index, so chunks run independently. With BULK
+// the inputs of a full chunk arrive by unicast bulk copies on one mbarrier.
+template <bool BULK>
+__global__ void __launch_bounds__(kRecThreads, 2)
+k_record_nodes(const __grid_constant__ RecordArgs a) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    RecordStage& S = *reinterpret_cast<RecordStage*>(smem_raw);
     __shared__ unsigned s_cnt[kRecPasses * (kRecThreads / 32)];
-    __shared__ LookbackSmem s_lb;
     __shared__ float s_stage[kRecThreads / 32][96];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const NodeView& nb = a.nb;
-    const float* __restrict__ in_pos = a.pos;
-    const float* __restrict__ in_wi = a.wi;
-    const float* __restrict__ in_nrm = a.normal;
-    const float* __restrict__ in_alb = a.albedo;
-    const float* __restrict__ in_thp = a.thp;
-    if (tid == 0) s_epoch = *(volatile unsigned*)&nb.hdr[kHdrEpoch];
+    const unsigned c = blockIdx.x, v0 = c * kRecChunk;
+    const unsigned cnt_c = min((unsigned)kRecChunk, a.n - v0);
     unsigned flags = 0, dropped = 0;
-    const unsigned lt = lanemask_lt();
-    unsigned long long* call_base = reinterpret_cast<unsigned long long*>(nb.hdr + kHdrCallBase);
-    for (;;) {
+    if (BULK && cnt_c == (unsigned)kRecChunk) {
         if (tid == 0) {
-            s_chunk = atomicAdd(&nb.hdr[kHdrTicket], 1u);
-            // chunk 0 publishes the node count at the start of the call, tagged with this
-            // launch's epoch; every chunk needs it to tell this call's nodes from earlier ones
-            if (s_chunk == 0) {
-                s_size0 = *(volatile unsigned*)&nb.hdr[kHdrSize];
-                store_state(call_base, ((unsigned long long)(s_epoch + 1u) << 32) | s_size0);
-            } else if (s_chunk < a.chunks) {
-                unsigned spins = 0;
-                unsigned long long w = load_state(call_base);
-                while ((unsigned)(w >> 32) != s_epoch + 1u && ++spins <= a.spin_limit) {
-                    __nanosleep(32);
-                    w = load_state(call_base);
-                }
-                if ((unsigned)(w >> 32) != s_epoch + 1u) flags |= NRRS_DEV_TIMEOUT;
-                s_size0 = (unsigned)w;
-            }
+            tc::mbar_init(&S.bar, 1);
+            tc::fence_mbar_init();
+            const unsigned v3 = 3 * kRecChunk * 4, v1 = kRecChunk * 4;
+            const unsigned bytes = v3 * (3 + (a.normal ? 1 : 0) + (a.albedo ? 1 : 0)) +
+                                   v1 * (2 + (a.rough ? 1 : 0) + (a.rrs ? 1 : 0) +
+                                         (a.depth ? 1 : 0)) +
+                                   (a.record ? kRecChunk : 0);
+            tc::mbar_arrive_expect_tx(&S.bar, bytes);
+            tc::bulk_g2s(S.pos, a.pos + 3 * (size_t)v0, v3, &S.bar);
+            tc::bulk_g2s(S.wi, a.wi + 3 * (size_t)v0, v3, &S.bar);
+            tc::bulk_g2s(S.thp, a.thp + 3 * (size_t)v0, v3, &S.bar);
+            if (a.normal) tc::bulk_g2s(S.nrm, a.normal + 3 * (size_t)v0, v3, &S.bar);
+            if (a.albedo) tc::bulk_g2s(S.alb, a.albedo + 3 * (size_t)v0, v3, &S.bar);
+            tc::bulk_g2s(S.pixel, a.pixel + v0, v1, &S.bar);
+            tc::bulk_g2s(S.parent, a.parent + v0, v1, &S.bar);
+            if (a.rough) tc::bulk_g2s(S.rough, a.rough + v0, v1, &S.bar);
+            if (a.rrs) tc::bulk_g2s(S.rrs, a.rrs + v0, v1, &S.bar);
+            if (a.depth) tc::bulk_g2s(S.depth, a.depth + v0, v1, &S.bar);
+            if (a.record) tc::bulk_g2s(S.record, a.record + v0, kRecChunk, &S.bar);
         }
-        __syncthreads();
-        const unsigned c = s_chunk;
-        if (c >= a.chunks) break;
-        const unsigned call0 = s_size0;
-        const unsigned v0 = c * kRecChunk;
-        unsigned m[kRecPasses];
-#pragma unroll
-        for (int j = 0; j < kRecPasses; ++j) {
-            const unsigned v = v0 + j * kRecThreads + tid;
-            const bool r = v < a.n && (!a.record || a.record[v] != 0);
-            m[j] = __ballot_sync(0xffffffffu, r);
-            if (lane == 0) s_cnt[j * (kRecThreads / 32) + wid] = __popc(m[j]);
+        __syncthreads();  // the barrier is initialised before anyone waits on it
+        if (!tc::mbar_wait(&S.bar, 0, a.spin_limit)) {
+            // the copies must land before this CTA's shared memory can be given up
+            tc::mbar_wait(&S.bar, 0, a.spin_limit);
+            if (tid == 0) atomicOr(&nb.hdr[kHdrStatus], NRRS_DEV_TIMEOUT);
+            return;
         }
+    } else {
+        copy_in(S.pos, a.pos + 3 * (size_t)v0, 3 * cnt_c);
+        copy_in(S.wi, a.wi + 3 * (size_t)v0, 3 * cnt_c);
+        copy_in(S.thp, a.thp + 3 * (size_t)v0, 3 * cnt_c);
+        if (a.normal) copy_in(S.nrm, a.normal + 3 * (size_t)v0, 3 * cnt_c);
+        if (a.albedo) copy_in(S.alb, a.albedo + 3 * (size_t)v0, 3 * cnt_c);
+        copy_in(S.pixel, a.pixel + v0, cnt_c);
+        copy_in(S.parent, a.parent + v0, cnt_c);
+        if (a.rough) copy_in(S.rough, a.rough + v0, cnt_c);
+        if (a.rrs) copy_in(S.rrs, a.rrs + v0, cnt_c);
+        if (a.depth) copy_in(S.depth, a.depth + v0, cnt_c);
+        if (a.record) copy_in(S.record, a.record + v0, cnt_c);
         __syncthreads();
-        unsigned total = 0;
-        if (wid == 0) total = scan_counts(s_cnt);
-        if (tid == 0) s_lb.part[0] = total;  // hand the total to every thread
-        __syncthreads();
-        total = (unsigned)s_lb.part[0];
-        __syncthreads();
-        const unsigned prefix = lookback_block(nb.states, c, s_epoch, total, c == 0 ? s_size0 : 0u,
-                                               a.spin_limit, &flags, s_lb);
-        if (tid == 0 && c == a.chunks - 1) {
-            const unsigned end = sat_add(prefix, total);
-            const unsigned sz = end < nb.capacity ? end : nb.capacity;
-            nb.hdr[kHdrSize] = sz;
-            const unsigned L = nb.hdr[kHdrLevels];
-            if (L < (unsigned)kMaxLevels) nb.hdr[kHdrLevelTable + L] = sz;
-            if (L <= (unsigned)kMaxLevels) nb.hdr[kHdrLevels] = L + 1;
+    }
+    const unsigned call0 = *(volatile unsigned*)&nb.hdr[kHdrCallBase];
+    const unsigned prefix = a.chunk_offset[c];
+    unsigned m[kRecPasses];
+#pragma unroll
+    for (int j = 0; j < kRecPasses; ++j) {
+        const unsigned lv = j * kRecThreads + tid;
+        const bool r = lv < cnt_c && (!a.record || S.record[lv] != 0);
+        m[j] = __ballot_sync(0xffffffffu, r);
+        if (lane == 0) s_cnt[j * (kRecThreads / 32) + wid] = __popc(m[j]);
+    }
+    __syncthreads();
+    if (wid == 0) scan_counts(s_cnt);
+    __syncthreads();
+    const unsigned lt = lanemask_lt();
+#pragma unroll
+    for (int j = 0; j < kRecPasses; ++j) {
+        const unsigned lv = j * kRecThreads + tid;
+        const unsigned v = v0 + lv;
+        const bool valid = lv < cnt_c;
+        const bool active = (m[j] >> lane) & 1u;
+        const unsigned rank = __popc(m[j] & lt);
+        const unsigned long long base = (unsigned long long)prefix + s_cnt[j * (kRecThreads / 32) + wid];
+        const unsigned cnt = __popc(m[j]);
+        const unsigned room = base >= nb.capacity ? 0u
+                              : (unsigned)min((unsigned long long)cnt, nb.capacity - base);
+        const bool keep = active && rank < room;
+        const int p = valid ? S.parent[lv] : 0;
+        // a parent must be a node of an earlier call: any other link is cut and flagged
+        const bool bad_parent = p >= 0 && (unsigned)p >= call0;
+        const int pn = bad_parent ? -1 : p;
+        const unsigned idx = (unsigned)(base + rank);
+        if (room) {  // warp-uniform
+            const unsigned l3 = 3 * lv;
+            store3_compact(nb.pos + 3 * base, keep, rank, room, S.pos[l3], S.pos[l3 + 1],
+                           S.pos[l3 + 2], s_stage[wid]);
+            store3_compact(nb.wi + 3 * base, keep, rank, room, S.wi[l3], S.wi[l3 + 1],
+                           S.wi[l3 + 2], s_stage[wid]);
+            store3_compact(nb.normal + 3 * base, keep, rank, room,
+                           a.normal ? S.nrm[l3] : 0.f, a.normal ? S.nrm[l3 + 1] : 0.f,
+                           a.normal ? S.nrm[l3 + 2] : 0.f, s_stage[wid]);
+            store3_compact(nb.albedo + 3 * base, keep, rank, room,
+                           a.albedo ? S.alb[l3] : 0.f, a.albedo ? S.alb[l3 + 1] : 0.f,
+                           a.albedo ? S.alb[l3 + 2] : 0.f, s_stage[wid]);
+            store3_compact(nb.thp + 3 * base, keep, rank, room, S.thp[l3], S.thp[l3 + 1],
+                           S.thp[l3 + 2], s_stage[wid]);
+            long long* r = nb.rad + (size_t)base * kLimbs;
+            for (unsigned k = lane; k < kLimbs * room; k += 32) r[k] = 0;
         }
-#pragma unroll
-        for (int j = 0; j < kRecPasses; ++j) {
-            const unsigned v = v0 + j * kRecThreads + tid;
-            const bool valid = v < a.n;
-            const bool active = (m[j] >> lane) & 1u;
-            const unsigned rank = __popc(m[j] & lt);
-            const unsigned long long base = (unsigned long long)prefix + s_cnt[j * (kRecThreads / 32) + wid];
-            const unsigned cnt = __popc(m[j]);
-            const unsigned room = base >= nb.capacity ? 0u
-                                  : (unsigned)min((unsigned long long)cnt, nb.capacity - base);
-            const bool keep = active && rank < room;
-            // every field first, then the stores
-            int p = 0;
-            float q[15];
-            float rough = 0.f, rrs = 1.f;
-            unsigned px = 0, dep = 0;
-            if (valid) p = a.parent[v];
-            // a parent must be a node of an earlier call: any other link is cut and flagged
-            const bool bad_parent = p >= 0 && (unsigned)p >= call0;
-            const int pn = bad_parent ? -1 : p;
-            if (keep) {
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    const size_t si = 3 * (size_t)v + k;
-                    q[k] = in_pos[si];
-                    q[3 + k] = in_wi[si];
-                    q[6 + k] = in_nrm ? in_nrm[si] : 0.f;
-                    q[9 + k] = in_alb ? in_alb[si] : 0.f;
-                    q[12 + k] = in_thp[si];
-                }
-                if (a.rough) rough = a.rough[v];
-                if (a.rrs) rrs = a.rrs[v];
-                if (a.depth) dep = a.depth[v];
-                px = a.pixel[v];
-            } else {
-#pragma unroll
-                for (int k = 0; k < 15; ++k) q[k] = 0.f;
+        if (keep) {
+            nb.rough[idx] = a.rough ? S.rough[lv] : 0.f;
+            nb.parent[idx] = pn;
+            nb.pixel[idx] = S.pixel[lv];
+            nb.rrs[idx] = a.rrs ? S.rrs[lv] : 1.f;
+            nb.depth[idx] = a.depth ? S.depth[lv] : 0u;
+            nb.first_child[idx] = 0xffffffffu;
+            nb.children[idx] = 0;
+            nb.arrived[idx] = 0;
+            nb.flags[idx] = 0;
+            if (pn >= 0) {
+                atomicMin(&nb.first_child[pn], idx);
+                atomicAdd(&nb.children[pn], 1u);
             }
-            const unsigned idx = (unsigned)(base + rank);
-            if (room) {  // warp-uniform
-                store3_compact(nb.pos + 3 * base, keep, rank, room, q[0], q[1], q[2], s_stage[wid]);
-                store3_compact(nb.wi + 3 * base, keep, rank, room, q[3], q[4], q[5], s_stage[wid]);
-                store3_compact(nb.normal + 3 * base, keep, rank, room, q[6], q[7], q[8], s_stage[wid]);
-                store3_compact(nb.albedo + 3 * base, keep, rank, room, q[9], q[10], q[11], s_stage[wid]);
-                store3_compact(nb.thp + 3 * base, keep, rank, room, q[12], q[13], q[14], s_stage[wid]);
-                long long* r = nb.rad + (size_t)base * kLimbs;
-                for (unsigned k = lane; k < kLimbs * room; k += 32) r[k] = 0;
-            }
-            if (keep) {
-                nb.rough[idx] = rough;
-                nb.parent[idx] = pn;
-                nb.pixel[idx] = px;
-                nb.rrs[idx] = rrs;
-                nb.depth[idx] = dep;
-                nb.first_child[idx] = 0xffffffffu;
-                nb.children[idx] = 0;
-                nb.arrived[idx] = 0;
-                nb.flags[idx] = 0;
-                if (pn >= 0) {
-                    atomicMin(&nb.first_child[pn], idx);
-                    atomicAdd(&nb.children[pn], 1u);
-                }
-                if (bad_parent) flags |= NRRS_DEV_BAD_INDEX;
-            } else if (active) {
-                ++dropped;
-            }
-            if (valid) a.node_out[v] = keep ? (int)idx : p;
+            if (bad_parent) flags |= NRRS_DEV_BAD_INDEX;
+        } else if (active) {
+            ++dropped;
         }
-        __syncthreads();
+        if (valid) a.node_out[v] = keep ? (int)idx : p;
     }
     if (dropped) {
         atomicAdd(&nb.hdr[kHdrDropped], dropped);
         flags |= NRRS_DEV_OVERFLOW;
     }
     if (flags) atomicOr(&nb.hdr[kHdrStatus], flags);
-    finish_launch(nb.hdr);
 }
 
 // ---- recordRadiance for a queue of contributions -------------------------------------------
@@ -698,9 +780,26 @@ __global__ void __launch_bounds__(256) k_sample_weights(const __grid_constant__ 
 
 }  // namespace
 
-cudaError_t launch_record_nodes(const RecordArgs& a, int grid, cudaStream_t s) {
+cudaError_t launch_record_nodes(const RecordArgs& a, cudaStream_t s) {
     if (a.chunks == 0) return cudaSuccess;
-    k_record_nodes<<<grid, kRecThreads, 0, s>>>(a);
+    auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+    const bool bulk = al(a.pos) && al(a.wi) && al(a.thp) && al(a.normal) && al(a.albedo) &&
+                      al(a.pixel) && al(a.parent) && al(a.rough) && al(a.rrs) && al(a.depth) &&
+                      al(a.record);
+    const int smem = (int)sizeof(RecordStage);
+    static bool attr_set = false;  // the attribute is per function, not per device
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(k_record_nodes<true>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_record_nodes<false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    k_record_count<<<a.chunks, kRecThreads, 0, s>>>(a);
+    if (bulk) k_record_nodes<true><<<a.chunks, kRecThreads, smem, s>>>(a);
+    else k_record_nodes<false><<<a.chunks, kRecThreads, smem, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -71,6 +71,8 @@ struct RecordArgs {
     const float* rrs;
     const uint8_t* record;
     int32_t* node_out;
+    uint32_t* chunk_count;   // [chunks] records per chunk (scratch)
+    uint32_t* chunk_offset;  // [chunks] first node index of each chunk (scratch)
     uint32_t n, chunks, spin_limit;
 };
 
@@ -100,7 +102,13 @@ struct WeightArgs {
     uint32_t n_pixels, max_n;
 };
 
-cudaError_t launch_record_nodes(const RecordArgs& a, int grid, cudaStream_t s);
+// two launches: per-chunk counts, whose last CTA turns them into offsets, then the writes
+cudaError_t launch_record_nodes(const RecordArgs& a, cudaStream_t s);
+// device scratch of nrrs_record_nodes inside the node block's scan region
+inline uint32_t state_words(uint32_t capacity) { return (capacity + kRecChunk - 1) / kRecChunk + 1; }
+inline uint32_t record_chunks_max(uint32_t max_record) {
+    return (max_record + kRecChunk - 1) / kRecChunk + 1;
+}
 cudaError_t launch_record_radiance(const RadianceArgs& a, cudaStream_t s);
 // completes every node's radiance with its descendants' (once per reset): level by level in one
 // cooperative launch when the record calls since the reset are at most kMaxLevels, else by

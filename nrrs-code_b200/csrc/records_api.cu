@@ -16,9 +16,11 @@ constexpr uint32_t kSpinLimit = 1u << 22;
 
 uint64_t align_up(uint64_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
-uint32_t scan_chunks(uint32_t capacity, uint32_t max_record) {
-    const uint32_t m = capacity > max_record ? capacity : max_record;
-    return (uint32_t)(((uint64_t)m + kRecChunk - 1) / kRecChunk) + 1;
+// the scan region: look-back states of the batch (one per node chunk), then the record calls'
+// per-chunk counts and offsets
+uint64_t scan_bytes(uint32_t capacity, uint32_t max_record) {
+    return sizeof(unsigned long long) * (uint64_t)state_words(capacity) +
+           2ull * sizeof(uint32_t) * record_chunks_max(max_record);
 }
 
 // byte offsets of every array in the block; returns the total
@@ -33,7 +35,7 @@ Layout layout(uint32_t capacity, uint32_t max_record) {
     uint64_t o = 0;
     auto take = [&](uint64_t bytes) { const uint64_t at = o; o = align_up(o + bytes); return at; };
     L.hdr = take(sizeof(uint32_t) * kHdrWords);
-    L.states = take(sizeof(unsigned long long) * scan_chunks(capacity, max_record));
+    L.states = take(scan_bytes(capacity, max_record));
     L.pos = take(12 * C);
     L.wi = take(12 * C);
     L.normal = take(12 * C);
@@ -201,10 +203,12 @@ extern "C" int nrrs_record_nodes(const nrrs_path_nodes* nodes, const nrrs_vertex
     a.n = n;
     a.chunks = (n + kRecChunk - 1) / kRecChunk;
     a.spin_limit = kSpinLimit;
-    const int grid = persistent_grid(n, kRecChunk, 8);
-    if (grid <= 0) return NRRS_ERR_NO_DEVICE;
-    return launch_record_nodes(a, grid, (cudaStream_t)stream) == cudaSuccess ? NRRS_OK
-                                                                            : NRRS_ERR_CUDA;
+    uint32_t* scratch = reinterpret_cast<uint32_t*>(
+        reinterpret_cast<unsigned long long*>(nodes->scan_states) + state_words(nodes->capacity));
+    a.chunk_count = scratch;
+    a.chunk_offset = scratch + record_chunks_max(nodes->max_record);
+    if (sm_count() <= 0) return NRRS_ERR_NO_DEVICE;
+    return launch_record_nodes(a, (cudaStream_t)stream) == cudaSuccess ? NRRS_OK : NRRS_ERR_CUDA;
 }
 
 extern "C" int nrrs_record_radiance(const nrrs_path_nodes* nodes, const int32_t* node,
