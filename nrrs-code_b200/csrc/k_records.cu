@@ -127,19 +127,20 @@ __device__ unsigned lookback_block(unsigned long long* states, unsigned c, unsig
     return prefix;
 }
 
-// Exclusive scan, by warp 0, of the kRecPasses x warps per-(pass, warp) counts in s_cnt
-// (pass-major, one per lane); returns the chunk total to every lane of warp 0.
+// Exclusive scan, by warp 0, of the N (<= 32) per-(pass, warp) counts in s_cnt (pass-major,
+// one per lane); returns the total to every lane of warp 0.
+template <int N = kRecPasses * (kRecThreads / 32)>
 __device__ __forceinline__ unsigned scan_counts(unsigned* s_cnt) {
-    static_assert(kRecPasses * (kRecThreads / 32) == 32, "one count per lane");
+    static_assert(N <= 32, "one count per lane");
     const int lane = threadIdx.x & 31;
-    const unsigned t = s_cnt[lane];
+    const unsigned t = lane < N ? s_cnt[lane] : 0u;
     unsigned incl = t;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += y;
     }
-    s_cnt[lane] = incl - t;
+    if (lane < N) s_cnt[lane] = incl - t;
     return __shfl_sync(0xffffffffu, incl, 31);
 }
 
@@ -233,6 +234,9 @@ __device__ __forceinline__ bool finish_launch(uint32_t* hdr) {
 // chunk arrives by one unicast bulk copy each on one mbarrier (all bytes in flight at once); the
 // last, partial chunk and inputs not 16-byte aligned are copied by the threads in coalesced
 // loops. Two CTAs per SM.
+constexpr int kWrThreads = 512;                      // write kernel: 16 warps, 2 passes
+constexpr int kWrPasses = kRecChunk / kWrThreads;
+
 struct RecordStage {
     float pos[3 * kRecChunk], wi[3 * kRecChunk], nrm[3 * kRecChunk], alb[3 * kRecChunk],
         thp[3 * kRecChunk];
@@ -245,7 +249,7 @@ struct RecordStage {
 
 template <typename T>
 __device__ __forceinline__ void copy_in(T* dst, const T* __restrict__ src, unsigned count) {
-    for (unsigned j = threadIdx.x; j < count; j += kRecThreads) dst[j] = src[j];
+    for (unsigned j = threadIdx.x; j < count; j += blockDim.x) dst[j] = src[j];
 }
 
 // Counts of the chunks' records; the last CTA to finish turns them into node offsets (from the
@@ -324,12 +328,12 @@ __global__ void __launch_bounds__(kRecThreads) k_record_count(const __grid_const
 // The writes: every chunk knows its first node index, so chunks run independently. With BULK
 // the inputs of a full chunk arrive by unicast bulk copies on one mbarrier.
 template <bool BULK>
-__global__ void __launch_bounds__(kRecThreads, 2)
+__global__ void __launch_bounds__(kWrThreads, 2)
 k_record_nodes(const __grid_constant__ RecordArgs a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     RecordStage& S = *reinterpret_cast<RecordStage*>(smem_raw);
-    __shared__ unsigned s_cnt[kRecPasses * (kRecThreads / 32)];
-    __shared__ float s_stage[kRecThreads / 32][96];
+    __shared__ unsigned s_cnt[kWrPasses * (kWrThreads / 32)];
+    __shared__ float s_stage[kWrThreads / 32][96];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const NodeView& nb = a.nb;
     const unsigned c = blockIdx.x, v0 = c * kRecChunk;
@@ -380,26 +384,26 @@ k_record_nodes(const __grid_constant__ RecordArgs a) {
     }
     const unsigned call0 = *(volatile unsigned*)&nb.hdr[kHdrCallBase];
     const unsigned prefix = a.chunk_offset[c];
-    unsigned m[kRecPasses];
+    unsigned m[kWrPasses];
 #pragma unroll
-    for (int j = 0; j < kRecPasses; ++j) {
-        const unsigned lv = j * kRecThreads + tid;
+    for (int j = 0; j < kWrPasses; ++j) {
+        const unsigned lv = j * kWrThreads + tid;
         const bool r = lv < cnt_c && (!a.record || S.record[lv] != 0);
         m[j] = __ballot_sync(0xffffffffu, r);
-        if (lane == 0) s_cnt[j * (kRecThreads / 32) + wid] = __popc(m[j]);
+        if (lane == 0) s_cnt[j * (kWrThreads / 32) + wid] = __popc(m[j]);
     }
     __syncthreads();
-    if (wid == 0) scan_counts(s_cnt);
+    if (wid == 0) scan_counts<kWrPasses * (kWrThreads / 32)>(s_cnt);
     __syncthreads();
     const unsigned lt = lanemask_lt();
 #pragma unroll
-    for (int j = 0; j < kRecPasses; ++j) {
-        const unsigned lv = j * kRecThreads + tid;
+    for (int j = 0; j < kWrPasses; ++j) {
+        const unsigned lv = j * kWrThreads + tid;
         const unsigned v = v0 + lv;
         const bool valid = lv < cnt_c;
         const bool active = (m[j] >> lane) & 1u;
         const unsigned rank = __popc(m[j] & lt);
-        const unsigned long long base = (unsigned long long)prefix + s_cnt[j * (kRecThreads / 32) + wid];
+        const unsigned long long base = (unsigned long long)prefix + s_cnt[j * (kWrThreads / 32) + wid];
         const unsigned cnt = __popc(m[j]);
         const unsigned room = base >= nb.capacity ? 0u
                               : (unsigned)min((unsigned long long)cnt, nb.capacity - base);
@@ -538,18 +542,45 @@ __device__ void grid_barrier(uint32_t* hdr, unsigned spin_limit, unsigned* flags
 __device__ void propagate_levels(const NodeView& nb, unsigned levels, unsigned spin_limit,
                                  unsigned* flags) {
     const unsigned* lt = nb.hdr + kHdrLevelTable;
+    const int lane = threadIdx.x & 31;
+    const unsigned warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned warps = (gridDim.x * blockDim.x) >> 5;
+    constexpr int G = 2;  // 32-node groups per warp and step, loaded before any addition
     for (int k = (int)levels - 1; k >= 1; --k) {
         const unsigned lo = lt[k - 1], hi = lt[k];
-        for (unsigned i = lo + blockIdx.x * blockDim.x + threadIdx.x; i < hi;
-             i += gridDim.x * blockDim.x) {
-            const int p = nb.parent[i];
-            if (p < 0) continue;
-            long long l[kLimbs];
-            const long long* src = nb.rad + (size_t)i * kLimbs;
+        for (unsigned g0 = lo + 32u * warp * G; g0 < hi; g0 += 32u * warps * G) {
+            // lane l holds limb word l + 32 q of each group's 32 x 9 words, and the group's
+            // parent and flags of node l
+            long long w[G][kLimbs];
+            int par[G];
+            unsigned fl[G];
 #pragma unroll
-            for (int q = 0; q < kLimbs; ++q) l[q] = __ldcg(src + q);
-            add_limbs(nb.rad + (size_t)p * kLimbs, l);
-            if (__ldcg(nb.flags + i) & 1u) atomicOr(&nb.flags[p], 1u);
+            for (int g = 0; g < G; ++g) {
+                const unsigned gb = g0 + 32u * g;
+                const unsigned nn = gb < hi ? min(32u, hi - gb) : 0u;
+                par[g] = lane < (int)nn ? __ldcg(nb.parent + gb + lane) : -1;
+                fl[g] = lane < (int)nn ? __ldcg(nb.flags + gb + lane) : 0u;
+                const long long* src = nb.rad + (size_t)gb * kLimbs;
+#pragma unroll
+                for (int q = 0; q < kLimbs; ++q) {
+                    const unsigned word = lane + 32u * q;
+                    w[g][q] = word < kLimbs * nn ? __ldcg(src + word) : 0ll;
+                }
+            }
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+#pragma unroll
+                for (int q = 0; q < kLimbs; ++q) {
+                    const unsigned word = lane + 32u * q;
+                    const int node = word / kLimbs;   // 0..31 within the group
+                    const int pp = __shfl_sync(0xffffffffu, par[g], node);
+                    if (pp >= 0 && w[g][q] != 0)
+                        atomicAdd(reinterpret_cast<unsigned long long*>(nb.rad + (size_t)pp * kLimbs +
+                                                                        (word - node * kLimbs)),
+                                  (unsigned long long)w[g][q]);
+                }
+                if (par[g] >= 0 && (fl[g] & 1u)) atomicOr(&nb.flags[par[g]], 1u);
+            }
         }
         grid_barrier(nb.hdr, spin_limit, flags);
     }
@@ -771,11 +802,12 @@ __global__ void __launch_bounds__(kRecThreads) k_generate(const __grid_constant_
 
 // ---- 1 / samples of the sample's pixel -------------------------------------------------------
 __global__ void __launch_bounds__(256) k_sample_weights(const __grid_constant__ WeightArgs a) {
-    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= a.max_n || t >= *a.size_dev) return;
-    const unsigned px = a.pixel[t];
-    const unsigned cnt = px < a.n_pixels ? a.pixel_samples[px] : 0u;
-    a.weight[t] = cnt ? __fdiv_rn(1.0f, (float)cnt) : 0.0f;
+    const unsigned n = min(a.max_n, *a.size_dev);
+    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const unsigned px = a.pixel[t];
+        const unsigned cnt = px < a.n_pixels ? a.pixel_samples[px] : 0u;
+        a.weight[t] = cnt ? __fdiv_rn(1.0f, (float)cnt) : 0.0f;
+    }
 }
 
 }  // namespace
@@ -798,8 +830,8 @@ cudaError_t launch_record_nodes(const RecordArgs& a, cudaStream_t s) {
         attr_set = true;
     }
     k_record_count<<<a.chunks, kRecThreads, 0, s>>>(a);
-    if (bulk) k_record_nodes<true><<<a.chunks, kRecThreads, smem, s>>>(a);
-    else k_record_nodes<false><<<a.chunks, kRecThreads, smem, s>>>(a);
+    if (bulk) k_record_nodes<true><<<a.chunks, kWrThreads, smem, s>>>(a);
+    else k_record_nodes<false><<<a.chunks, kWrThreads, smem, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -818,7 +850,7 @@ cudaError_t launch_propagate(const NodeView& nb, cudaStream_t s) {
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_propagate, 256, 0);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
-    const int grid = sms * (per_sm < 4 ? per_sm : 4);
+    const int grid = sms * per_sm;
     NodeView v = nb;
     unsigned spin = 1u << 22;
     void* args[] = {&v, &spin};
@@ -832,7 +864,12 @@ cudaError_t launch_generate(const GenerateArgs& a, int grid, cudaStream_t s) {
 
 cudaError_t launch_sample_weights(const WeightArgs& a, cudaStream_t s) {
     if (a.max_n == 0) return cudaSuccess;
-    k_sample_weights<<<(a.max_n + 255) / 256, 256, 0, s>>>(a);
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    const unsigned need = (a.max_n + 255) / 256, cap = (unsigned)sms * 8u;
+    k_sample_weights<<<need < cap ? need : cap, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 
