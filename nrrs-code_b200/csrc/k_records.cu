@@ -656,9 +656,10 @@ __global__ void __launch_bounds__(256) k_propagate(const __grid_constant__ NodeV
 }
 
 // ---- the training batch, in node order ------------------------------------------------------
-__global__ void __launch_bounds__(kRecThreads) k_generate(const __grid_constant__ GenerateArgs a) {
+__global__ void __launch_bounds__(kRecThreads, 5) k_generate(const __grid_constant__ GenerateArgs a) {
     __shared__ unsigned s_chunk, s_epoch;
     __shared__ unsigned s_cnt[kRecPasses * (kRecThreads / 32)];
+    __shared__ unsigned s_keep[kRecPasses][kRecThreads / 32], s_same[kRecPasses][kRecThreads / 32];
     __shared__ LookbackSmem s_lb;
     __shared__ float s_L[kRecPasses][3][kRecThreads];
     __shared__ float s_stage[kRecThreads / 32][96];
@@ -675,7 +676,6 @@ __global__ void __launch_bounds__(kRecThreads) k_generate(const __grid_constant_
         const unsigned c = s_chunk;
         if (c >= chunks) break;
         const unsigned i0 = c * kRecChunk;
-        unsigned m[kRecPasses], same_m[kRecPasses];
 #pragma unroll
         for (int j = 0; j < kRecPasses; ++j) {
             const unsigned i = i0 + j * kRecThreads + tid;
@@ -715,9 +715,13 @@ __global__ void __launch_bounds__(kRecThreads) k_generate(const __grid_constant_
                 keep = (nf & 1u) == 0 && !nan && (!a.ignore_zero_l || mean > 0.f);
                 same = p >= 0 && (unsigned)p < i && fc != i;
             }
-            m[j] = __ballot_sync(0xffffffffu, keep);
-            same_m[j] = __ballot_sync(0xffffffffu, same);
-            if (lane == 0) s_cnt[j * (kRecThreads / 32) + wid] = __popc(m[j]);
+            const unsigned mk = __ballot_sync(0xffffffffu, keep);
+            const unsigned ms = __ballot_sync(0xffffffffu, same);
+            if (lane == 0) {
+                s_cnt[j * (kRecThreads / 32) + wid] = __popc(mk);
+                s_keep[j][wid] = mk;
+                s_same[j][wid] = ms;
+            }
         }
         __syncthreads();
         unsigned total = 0;
@@ -737,15 +741,16 @@ __global__ void __launch_bounds__(kRecThreads) k_generate(const __grid_constant_
 #pragma unroll
         for (int j = 0; j < kRecPasses; ++j) {
             const unsigned i = i0 + j * kRecThreads + tid;
-            const bool active = (m[j] >> lane) & 1u;
-            const unsigned rank = __popc(m[j] & lt);
+            const unsigned mk = s_keep[j][wid];
+            const bool active = (mk >> lane) & 1u;
+            const unsigned rank = __popc(mk & lt);
             const unsigned long long base = (unsigned long long)prefix + s_cnt[j * (kRecThreads / 32) + wid];
-            const unsigned cnt = __popc(m[j]);
+            const unsigned cnt = __popc(mk);
             const unsigned room = base >= a.capacity ? 0u
                                   : (unsigned)min((unsigned long long)cnt, a.capacity - base);
             if (room == 0) continue;  // warp-uniform
             const bool keep = active && rank < room;
-            const bool same = (same_m[j] >> lane) & 1u;
+            const bool same = (s_same[j][wid] >> lane) & 1u;
             // every field first, then the stores
             float q[15], rough = 0.f, rrs = 0.f, rm = 0.f;
             unsigned px = 0, dep = 0;
