@@ -8,6 +8,8 @@
  *      compaction of survivors into the next-bounce queue         (nrrs_decide_emit)
  *   3. both fused (nrrs_step) and batched over uneven depths      (nrrs_step_batched)
  *   4. one training step of StatNet and RRSNet on a sample batch  (nrrs_train_step)
+ *   5. the training frame's path-node records, their radiance and the training batch built
+ *      from them                                   (nrrs_record_nodes ... nrrs_sample_weights)
  *
  * Everything is asynchronous on the caller's CUDA stream (passed as void*; NULL = legacy
  * default stream). Input and output buffers are device pointers owned by the caller. The
@@ -21,6 +23,9 @@
  *   NRRSPathTracer::trainStep            src/render/nrrs/integrator.cpp:2337-2657
  *   calcSum2PassAsync<true>              src/render/common/commoncudautilshost.cpp:6-22
  *   TidQueue::push / pushCheck           src/render/common/commonworkqueue.h:19-42
+ *   NRRSPathNodesBuffer                  src/render/nrrs/workqueue.h:108-188
+ *   nrrs_generate_training_data          src/render/nrrs/train.cu:432-570
+ *   nrrs_calculate_sample_weight         src/render/nrrs/train.cu:572-592
  */
 #ifndef NRRS_B200_H
 #define NRRS_B200_H
