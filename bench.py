@@ -642,34 +642,69 @@ RECORD_KEYS = ("pos", "wi", "normal", "albedo", "roughness", "thp", "depth", "pi
 CONTRIB_KEYS = ("contrib_node", "contrib")
 
 
-def records_params():
-    return nb.default_train_data_params(ignore_zero_l=0, copy_rrs_node=1, dedupe_rrs_target=1)
+def records_params(**kw):
+    return nb.default_train_data_params(ignore_zero_l=0, copy_rrs_node=1, dedupe_rrs_target=1,
+                                        **kw)
 
 
 def records_frame(seed: int, wl: dict):
+    """The synthetic frame: path records, the film (RGBA per pixel) and the frame's radiance per
+    pixel (the sum of its samples, spp 1)."""
     P = wl["n_vert"]
     bounces, image = nb.synth_paths(seed, P, bounces=wl["bounces"],
                                     capacity=wl["node_rate"] * P)
-    return bounces, image
+    rng = np.random.default_rng(seed + 1)
+    pixel_l = (image[:, :3] * rng.lognormal(0.0, 0.5, size=(P, 3))).astype(np.float32)
+    return bounces, image, pixel_l
+
+
+def records_geom(wl):
+    """Frame width and height of the workload (a one-row frame for other pixel counts)."""
+    P = wl["n_vert"]
+    return (1920, 1080) if P == 1920 * 1080 else (P, 1)
 
 
 def records_name(wl):
     return f"records_{wl['bounces']}bounce_{wl['n_vert']}px_rate{wl['node_rate']}"
 
 
-def records_cpu(wl, bounces, image, seconds: float):
-    """The oracle (sequential C, one core) on whole frames of the workload until `seconds`."""
+def records_cpu(wl, bounces, image, pixel_l, seconds: float):
+    """The oracle (sequential C, one core) on whole frames of the workload until `seconds`: the
+    patch counts, the per-pixel error and its sum, then the records, the batch and the weights."""
     sys.path.insert(0, str(REPO / "oracle"))
     import oracle as O
     P = wl["n_vert"]
-    prm = records_params()
+    W, H = records_geom(wl)
+    pe = nb.default_pixel_error_params(W, H)
+    wl_ = np.zeros((P, 3), np.float32)
+    cur = np.zeros((P, 3), np.float32)
+    acc = np.zeros(P, np.uint32)
+    err = np.zeros(2 * P, np.float32)
+    spp = np.zeros(P, np.float32)
+    prm = records_params(frame_width=W, error_image_scale=1, error_per_pixel=err.ctypes.data,
+                         samples_per_patch=spp.ctypes.data)
+    cap = wl["node_rate"] * P
+    hn = O.HostNodes(cap)                 # allocated once, reset per frame, as a renderer would
+    out = O.batch_arrays(cap)
+    counts = np.zeros(P, np.uint32)
     t, reps, nodes = 0.0, 0, 0
     while True:
         a = time.perf_counter()
-        r = O.frame_training_data(bounces, image, wl["node_rate"] * P, prm)
+        spp[:] = 0
+        hn.reset()
+        for b in bounces:
+            hn.record_nodes(b)
+            hn.record_radiance(b["contrib_node"], b["contrib"])
+            O.count_patch_samples(pe, b["pixel"], spp)
+        O.accumulate_weighted_l(pe, pixel_l, 1, False, wl_, cur, acc)
+        O.update_weighted_l(pe, cur, acc, wl_)
+        O.calculate_error(pe, image, wl_, spp, err)
+        counts[:] = 0
+        batch, total = hn.generate(prm, cap, image=image, n_pixels=P, pixel_samples=counts, out=out)
+        O.sample_weights(batch["pixel"], counts, P)
         t += time.perf_counter() - a
         reps += 1
-        nodes = r["nodes"].size
+        nodes = hn.size
         if t > seconds:
             break
     return nodes * reps / t, reps, t / reps
@@ -679,9 +714,9 @@ def run_records_reference(args, rank, world):
     if rank != 0:
         return 0
     wl = WORKLOADS[args.workload]
-    bounces, image = records_frame(4242, wl)
-    secs = max(1.0, 1.0 * args.steps)
-    value, reps, frame_s = records_cpu(wl, bounces, image, secs)
+    bounces, image, pixel_l = records_frame(4242, wl)
+    secs = min(60.0, max(1.0, 0.05 * args.steps))
+    value, reps, frame_s = records_cpu(wl, bounces, image, pixel_l, secs)
     line = {
         "metric": "path nodes/s (records + radiance + training batch + weights)",
         "value": value, "unit": "nodes/s", "n_gpus": args.gpus, "steps": args.steps,
@@ -694,8 +729,9 @@ def run_records_reference(args, rank, world):
                 "d2h_bytes_per_step": 0},
         "note": "reference CPU path = sequential C restatement (oracle/records.c) of "
                 "recordNode/recordRadiance/nrrs_generate_training_data/"
-                "nrrs_calculate_sample_weight; the reference runs them on the GPU inside its "
-                "OptiX integrator, which cannot be built here",
+                "nrrs_calculate_sample_weight and the per-pixel error of trainStep; the "
+                "reference runs them on the GPU inside its OptiX integrator, which cannot be "
+                "built here",
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -715,8 +751,9 @@ def run_records(args, rank, world, local_rank):
     wl = WORKLOADS[args.workload]
     P = wl["n_vert"]
     cap = wl["node_rate"] * P
-    bounces, image = records_frame(4242 + rank, wl)
-    prm = records_params()
+    bounces, image, pixel_l = records_frame(4242 + rank, wl)
+    W, H = records_geom(wl)
+    pe = nb.default_pixel_error_params(W, H)
 
     def to_t(a):
         a = np.ascontiguousarray(a)
@@ -743,10 +780,22 @@ def run_records(args, rank, world, local_rank):
     size_d = torch.zeros(1, dtype=torch.int32, device=dev)
     img_d = torch.from_numpy(image).to(dev)
     img_h = torch.from_numpy(image).pin_memory()
+    pl_d = torch.from_numpy(pixel_l).to(dev)
+    pl_h = torch.from_numpy(pixel_l).pin_memory()
     size_h = torch.zeros(1, dtype=torch.int32).pin_memory()
+    # per-pixel error of the RRSNet loss (trainStep STEP#1-#2), patches of one pixel
+    wl_d = torch.zeros((P, 3), dtype=torch.float32, device=dev)
+    cur_d = torch.zeros((P, 3), dtype=torch.float32, device=dev)
+    acc_d = torch.zeros(P, dtype=torch.int32, device=dev)
+    err_d = torch.zeros(2 * P, dtype=torch.float32, device=dev)
+    spp_d = torch.zeros(P, dtype=torch.float32, device=dev)
+    esum_d = torch.zeros(32, dtype=torch.uint8, device=dev)
+    prm = records_params(frame_width=W, error_image_scale=1, error_per_pixel=err_d.data_ptr(),
+                         samples_per_patch=spp_d.data_ptr())
 
     def step(pre=None, post=None, ev=None):
         pn.reset(stream)
+        spp_d.zero_()       # the patch sample counts restart every frame (integrator.cpp:1029)
         for d, db in enumerate(dev_b):
             if pre:
                 pre(d)
@@ -759,11 +808,21 @@ def run_records(args, rank, world, local_rank):
             pn.recordRadiance(db["contrib_node"], db["contrib"], m_of[d], stream)
             if ev:
                 ev[("rad", d)][1].record(cur)
+            nb.count_patch_samples(pe, db["pixel"], n_of[d], spp_d, stream)
+            if ev:
+                ev[("cnt", d)][1].record(cur)
             if post:
                 post(d)
         counts.zero_()      # mTrainingSamples is zeroed once per frame (integrator.cpp:1041)
         if pre:
             pre("image")
+        if ev:
+            ev["pe"][0].record(cur)
+        nb.accumulate_weighted_l(pe, pl_d, 1, False, wl_d, cur_d, acc_d, stream)
+        nb.update_weighted_l(pe, cur_d, acc_d, wl_d, stream)
+        nb.calculate_error(pe, img_d, 4, wl_d, spp_d, err_d, esum_d, stream)
+        if ev:
+            ev["pe"][1].record(cur)
         if ev:
             ev["gen"][0].record(cur)
         pn.generate_training_data(prm, tb, cap, size_d, image=img_d, image_channels=4,
@@ -783,9 +842,9 @@ def run_records(args, rank, world, local_rank):
         if post:
             post("image")
 
-    # per bounce: record count, record writes, radiance; then radiance pass, batch, weights
-    # (the counts' zero_ is torch's)
-    launches_per_step = 3 * len(bounces) + 3
+    # per bounce: record count, record writes, radiance, patch counts; then the pixel error
+    # (3), radiance pass, batch, weights (the zero_ fills are torch's)
+    launches_per_step = 4 * len(bounces) + 6
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -824,11 +883,13 @@ def run_records(args, rank, world, local_rank):
                 ev_copied[d].record(copy_stream)
             copy_stream.wait_event(ev_used["image"])
             img_d.copy_(img_h, non_blocking=True)
+            pl_d.copy_(pl_h, non_blocking=True)
             ev_copied["image"].record(copy_stream)
         step(pre=lambda k: cur.wait_event(ev_copied[k]), post=lambda k: ev_used[k].record(cur))
         size_h.copy_(size_d, non_blocking=True)
 
-    h2d = sum(t.numel() * t.element_size() for hb in host_b for t in hb.values()) + img_h.numel() * 4
+    h2d = (sum(t.numel() * t.element_size() for hb in host_b for t in hb.values()) +
+           img_h.numel() * 4 + pl_h.numel() * 4)
     for _ in range(2):
         step_e2e()
     torch.cuda.synchronize()
@@ -855,6 +916,9 @@ def run_records(args, rank, world, local_rank):
           for d in range(len(bounces))}
     ev.update({("rad", d): (ev[("rec", d)][1], torch.cuda.Event(enable_timing=True))
                for d in range(len(bounces))})
+    ev.update({("cnt", d): (ev[("rad", d)][1], torch.cuda.Event(enable_timing=True))
+               for d in range(len(bounces))})
+    ev["pe"] = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
     ev["gen"] = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
     ev["batch"] = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
     ev["wgt"] = (ev["batch"][1], torch.cuda.Event(enable_timing=True))
@@ -866,6 +930,8 @@ def run_records(args, rank, world, local_rank):
     t_gen = ev["batch"][0].elapsed_time(ev["batch"][1])
     t_prop = max(t_call - t_gen, 1e-6)
     t_wgt = ev["wgt"][0].elapsed_time(ev["wgt"][1])
+    t_pe = (ev["pe"][0].elapsed_time(ev["pe"][1]) +
+            sum(ev[("cnt", d)][0].elapsed_time(ev[("cnt", d)][1]) for d in range(len(bounces))))
 
     # algorithmic bytes (each array element read or written once; an atomic add counts its
     # 8-byte read and write)
@@ -885,10 +951,17 @@ def run_records(args, rank, world, local_rank):
     # sample written and the pixel count incremented
     b_gen = recorded * (72 + 12 + 4 + 12 + 12 + 4 + 4) + total * (24 + 16 + 16 + 92 + 8)
     b_wgt = total * (4 + 4 + 4)
+    # pixel error: per ray its pixel read and one atomic on its patch count; per pixel the
+    # radiance read, the current sum and count written, blended (read 28 B, write 12 B), the
+    # film, estimate and count read and two errors written
+    b_pe = n_vert * (4 + 16) + P * (12 + 16 + 28 + 12 + 32 + 8)
+    # the batch also gathers each sample's two errors and sample count
+    b_gen += total * 12
     calls = {"record_nodes": (t_rec, b_rec, 2 * len(bounces)),
              "record_radiance": (t_rad, b_rad, len(bounces)),
              "radiance_pass": (t_prop, b_prop, 1), "batch": (t_gen, b_gen, 1),
-             "sample_weights": (t_wgt, b_wgt, 1)}
+             "sample_weights": (t_wgt, b_wgt, 1),
+             "pixel_error": (t_pe, b_pe, len(bounces) + 3)}
     peak, peak_kind = measured_peaks()
     dom = max(calls, key=lambda k: calls[k][0])
     t_dom, b_dom, n_dom = calls[dom]
@@ -925,7 +998,7 @@ def run_records(args, rank, world, local_rank):
         "device_status": [dropped, flags],
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        value_c, reps, frame_s = records_cpu(wl, bounces, image, 10.0)
+        value_c, reps, frame_s = records_cpu(wl, bounces, image, pixel_l, 10.0)
         line["cpu_baseline"] = {"value": value_c, "unit": "nodes/s", "cores": 1, "kind": "port",
                                 "sample": f"{reps} whole frames of the workload"}
     if rank == 0:

@@ -10,6 +10,8 @@
  *   4. one training step of StatNet and RRSNet on a sample batch  (nrrs_train_step)
  *   5. the training frame's path-node records, their radiance and the training batch built
  *      from them                                   (nrrs_record_nodes ... nrrs_sample_weights)
+ *   6. the per-pixel error of the RRSNet loss      (nrrs_count_patch_samples ...
+ *                                                   nrrs_calculate_error)
  *
  * Everything is asynchronous on the caller's CUDA stream (passed as void*; NULL = legacy
  * default stream). Input and output buffers are device pointers owned by the caller. The
@@ -26,6 +28,7 @@
  *   NRRSPathNodesBuffer                  src/render/nrrs/workqueue.h:108-188
  *   nrrs_generate_training_data          src/render/nrrs/train.cu:432-570
  *   nrrs_calculate_sample_weight         src/render/nrrs/train.cu:572-592
+ *   nrrs_update_weighted_L, nrrs_calculate_error   src/render/nrrs/train.cu:344-430
  */
 #ifndef NRRS_B200_H
 #define NRRS_B200_H
@@ -416,6 +419,12 @@ typedef struct {
     int32_t dedupe_rrs_target;  /* mIgnoreSameTrainingDataForRRSNet: later siblings get -1      */
     float thp_eps;              /* L_c = radiance_c / thp_c only where thp_c > thp_eps
                                    (KiRaRay's M_EPSILON)                                         */
+    /* the error image (see nrrs_calculate_error); all zero / NULL when not used */
+    uint32_t frame_width;       /* frame width in pixels; needed when error_image_scale > 1    */
+    uint32_t error_image_scale; /* 0 or 1: image and error arrays are per frame pixel; s > 1:
+                                   per s x s patch (offsetFrame2Scaled, myFilm.h:6-15)          */
+    const float* error_per_pixel;   /* [2][n_pixels] of nrrs_calculate_error, or NULL          */
+    const float* samples_per_patch; /* [patches] of nrrs_count_patch_samples, or NULL          */
 } nrrs_train_data_params;
 
 /* The training batch: the arrays of nrrs_vertex_soa and nrrs_train_step's target, plus the
@@ -432,13 +441,17 @@ typedef struct {
     float* target;          /* [cap][3] NRRSNetworkOutputTraining0::mL = max(radiance/thp, 0)    */
     float* rrs_target;      /* [cap] NRRSNetworkOutputTraining1::mRRS: node rrs, or -1           */
     uint32_t* pixel;        /* [cap] rayPixelID                                                 */
+    float* error;           /* [cap] errorForTraining = error_per_pixel[patch]     (train.cu:537-543) */
+    float* error_for_avg;   /* [cap] errorForAvgForTraining = error_per_pixel[n_pixels + patch] */
+    float* number_samples;  /* [cap] numSamples = samples_per_patch[patch]                      */
 } nrrs_train_batch;
 
 /* nrrs_generate_training_data (train.cu:432-570): one sample per node with finite radiance,
  * finite position and direction and (ignore_zero_l) mean(L) > 0, in node order; at most
  * capacity (further samples are dropped and flag NRRS_DEV_OVERFLOW). First completes the
  * radiance of every node (see nrrs_record_radiance), once per reset. image (may be NULL) is
- * [n_pixels][image_channels] float, channels 3 or 4 (MyFilm::getPixel); pixel_samples (may be
+ * the rendered film, [patches][image_channels] float, channels 3 or 4, read at the sample's
+ * patch (MyFilm::getPixel; with error_image_scale <= 1 a patch is a pixel); pixel_samples (may be
  * NULL) is [n_pixels] and gains one per sample that keeps its RRSNet target (mTrainingSamples,
  * which the caller zeroes per frame, integrator.cpp:1041). A pixel >= n_pixels flags
  * NRRS_DEV_BAD_INDEX and reads and counts nothing. *size_dev receives the sample count. */
@@ -452,6 +465,70 @@ int nrrs_generate_training_data(const nrrs_path_nodes* nodes, const nrrs_train_d
  * grid (the reference's host copy of the size). */
 int nrrs_sample_weights(const uint32_t* pixel, const uint32_t* pixel_samples, uint32_t n_pixels,
                         const uint32_t* size_dev, uint32_t max_n, float* weight, void* stream);
+
+/* ==== per-pixel error of the RRSNet loss =========================================================
+ * The image-space inputs of the RRSNet loss, computed once per training frame (trainStep,
+ * integrator.cpp:2358-2471): a blended estimate of each patch's radiance, its relative error
+ * against the rendered image, and the sum of the errors. A patch is a scale x scale block of
+ * frame pixels (error_image_scale; 1, a single pixel, in the shipped configuration). Where the
+ * reference adds a patch's pixels with FP32 atomics, these kernels add them in pixel order, so
+ * every result is deterministic; all arithmetic is FP32 without contraction. Replaces:
+ *   the patch sample counts        integrator.cpp:1027-1050, 803-808
+ *   weighted L, first frame + STEP#1.1   integrator.cpp:2358-2395
+ *   nrrs_update_weighted_L         train.cu:344-363
+ *   nrrs_calculate_error           train.cu:365-430
+ *   the error sum (calcSum2PassAsync<false>)   integrator.cpp:2466-2471
+ * The optional denoiser between these steps (OptiX, integrator.cpp:2412-2462) is not part of this
+ * library: a caller that denoises runs it between nrrs_update_weighted_l and
+ * nrrs_calculate_error on its own buffers. */
+typedef struct {
+    uint32_t frame_width, frame_height;  /* the frame; both divisible by scale               */
+    uint32_t scale;                      /* error_image_scale (integrator.h:549); 0 means 1  */
+    float blend_weight;                  /* blend_weight_for_error, 0.5 (integrator.h:527)   */
+    int32_t clamp;                       /* clamp_pixel_error, on (network.cpp:519): <= 100  */
+    int32_t multiply_samples;            /* pixel_error_multiply_samples, off (network.cpp:520):
+                                            error_for_avg = error * sqrt(samples of the patch) */
+} nrrs_pixel_error_params;
+
+/* Exact sum of the errors: caller-owned device struct, zeroed once (cudaMemset); every call
+ * leaves acc and done at zero again and writes value. */
+typedef struct {
+    int64_t acc[3];                      /* fixed-point limbs, lowest bit 2^-64              */
+    uint32_t done;                       /* CTAs finished                                    */
+    float value;                         /* the sum, rounded to nearest; NaN if any error is
+                                            not finite                                        */
+} nrrs_error_sum;
+
+/* Adds 1 to samples_per_patch[patch of pixel[i]] for every i (camera rays, integrator.cpp:1050;
+ * scattered rays, :803-808). samples_per_patch is zeroed by the caller per frame. */
+int nrrs_count_patch_samples(const nrrs_pixel_error_params* p, const uint32_t* pixel, uint32_t n,
+                             float* samples_per_patch, void* stream);
+
+/* The frame's radiance per patch: pixel_l is [frame pixels][3] (mPixelState->mL, the sum of
+ * this frame's spp samples). weighted_l_current[patch] = sum of the patch's pixel_l in pixel
+ * order and weighted_l_current_acc[patch] = spp x pixels per patch (STEP#1.1, replacing the
+ * per-frame reset of integrator.cpp:1027-1028 and its atomics); with first_frame,
+ * weighted_l[patch] = sum of pixel_l / spp as well (integrator.cpp:2358-2375). */
+int nrrs_accumulate_weighted_l(const nrrs_pixel_error_params* p, const float* pixel_l,
+                               uint32_t spp_this_frame, int32_t first_frame, float* weighted_l,
+                               float* weighted_l_current, uint32_t* weighted_l_current_acc,
+                               void* stream);
+
+/* nrrs_update_weighted_L (train.cu:344-363): weighted_l = weighted_l * (1 - blend) +
+ * (weighted_l_current / acc) * blend, per patch and channel. */
+int nrrs_update_weighted_l(const nrrs_pixel_error_params* p, const float* weighted_l_current,
+                           const uint32_t* weighted_l_current_acc, float* weighted_l,
+                           void* stream);
+
+/* nrrs_calculate_error (train.cu:365-430) and the error sum (integrator.cpp:2466-2471).
+ * ref is the rendered film per patch, [patches][ref_channels] (3 or 4). For each patch:
+ * err = mean_c (L_c - ref_c)^2 / (ref_c^2 + 0.01), min(err, 100) when clamp;
+ * error[patch] = err; error[frame pixels + patch] = err x sqrt(samples_per_patch[patch]) when
+ * multiply_samples, else err. error is [2][frame pixels]; sum (may be NULL) receives the exact
+ * sum of the second half over the patches. */
+int nrrs_calculate_error(const nrrs_pixel_error_params* p, const float* ref, int32_t ref_channels,
+                         const float* weighted_l, const float* samples_per_patch, float* error,
+                         nrrs_error_sum* sum, void* stream);
 
 /* ---- synthetic inputs (host, deterministic): mt19937_64 + explicit transforms. Buffers are
  *      HOST arrays sized as in nrrs_vertex_soa; any may be NULL to skip. target [n][3]. ---- */

@@ -25,6 +25,7 @@
 #include <cmath>
 
 #include "records.hpp"
+#include "fixed_point.cuh"
 #include "tc_ptx.cuh"
 
 namespace nrrs {
@@ -33,7 +34,6 @@ namespace {
 
 constexpr unsigned long long kFlagAgg = 1ull;
 constexpr unsigned long long kFlagIncl = 2ull;
-constexpr float kFixedMax = 4611686018427387904.0f;  // 2^62: larger contributions are refused
 
 __device__ __forceinline__ unsigned long long pack_state(unsigned epoch, unsigned long long flag,
                                                          unsigned value) {
@@ -165,48 +165,6 @@ __device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
     asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
     return old;
 }
-
-// trunc(|x| 2^64) as three limbs signed like x; x finite with |x| < 2^62
-__device__ __forceinline__ void fixed_limbs(float x, long long l[3]) {
-    const unsigned bits = __float_as_uint(x);
-    const unsigned e = (bits >> 23) & 0xffu;
-    const unsigned long long m = (bits & 0x7fffffu) | (e ? 0x800000u : 0u);
-    const int sh = (int)(e ? e : 1u) - 150 + 64;  // |x| 2^64 = m 2^sh
-    unsigned __int128 X;
-    if (sh >= 0) X = (unsigned __int128)m << sh;
-    else X = (-sh) >= 24 ? (unsigned __int128)0 : (unsigned __int128)(m >> (-sh));
-    const unsigned long long lo = (unsigned long long)X;
-    long long l0 = (long long)(lo & 0xffffffffull);
-    long long l1 = (long long)(lo >> 32);
-    long long l2 = (long long)(unsigned long long)(X >> 64);
-    if (bits >> 31) { l0 = -l0; l1 = -l1; l2 = -l2; }
-    l[0] = l0; l[1] = l1; l[2] = l2;
-}
-
-// (l0 + l1 2^32 + l2 2^64) 2^-64 rounded to the nearest float, ties to even. The magnitude M
-// (< 2^127) is cut to its top 64 bits with the bits below folded into bit 0 (sticky); the
-// hardware's correctly rounded u64 -> f32 conversion then rounds exactly as M itself would
-// round (the folded bit lies 39 places below the rounding position), and the power-of-two
-// scale is exact.
-__device__ __forceinline__ float fixed_to_float(long long l0, long long l1, long long l2) {
-    using u128 = unsigned __int128;
-    const u128 U = ((u128)(__int128)l2 << 64) + ((u128)(__int128)l1 << 32) + (u128)(__int128)l0;
-    const unsigned neg = (unsigned)(U >> 127) & 1u;
-    const u128 mag = neg ? (u128)0 - U : U;
-    const unsigned long long hi = (unsigned long long)(mag >> 64), lo = (unsigned long long)mag;
-    float f;
-    if (hi == 0) {
-        f = __fmul_rn(__ull2float_rn(lo), 0x1p-64f);
-    } else {
-        const int sh = 64 - __clzll((long long)hi);  // bits of hi: 1..63
-        const unsigned long long top = (hi << (64 - sh)) | (lo >> sh) |
-                                       ((lo << (64 - sh)) != 0ull ? 1ull : 0ull);
-        f = __fmul_rn(__ull2float_rn(top), __uint_as_float((unsigned)(127 + sh - 64) << 23));
-    }
-    return neg ? -f : f;
-}
-
-__device__ __forceinline__ bool fixed_ok(float x) { return fabsf(x) < kFixedMax; }
 
 __device__ __forceinline__ void add_limbs(long long* dst, const long long* l) {
 #pragma unroll
@@ -752,7 +710,7 @@ __global__ void __launch_bounds__(kRecThreads, 5) k_generate(const __grid_consta
             const bool keep = active && rank < room;
             const bool same = (s_same[j][wid] >> lane) & 1u;
             // every field first, then the stores
-            float q[15], rough = 0.f, rrs = 0.f, rm = 0.f;
+            float q[15], rough = 0.f, rrs = 0.f, rm = 0.f, er = 0.f, era = 0.f, ns = 0.f;
             unsigned px = 0, dep = 0;
 #pragma unroll
             for (int k = 0; k < 15; ++k) q[k] = 0.f;
@@ -772,9 +730,21 @@ __global__ void __launch_bounds__(kRecThreads, 5) k_generate(const __grid_consta
                 dep = nb.depth[i];
                 px = nb.pixel[i];
                 px_ok = px < a.n_pixels;
-                if (px_ok && a.image) {
-                    const float* im = a.image + (size_t)px * a.channels;
-                    rm = __fdiv_rn(__fadd_rn(__fadd_rn(im[0], im[1]), im[2]), 3.0f);
+                if (px_ok) {
+                    // the sample's patch of the film and error images (offsetFrame2Scaled)
+                    const unsigned pq = a.scale > 1u
+                        ? (px % a.frame_width) / a.scale +
+                              ((px / a.frame_width) / a.scale) * (a.frame_width / a.scale)
+                        : px;
+                    if (a.image) {
+                        const float* im = a.image + (size_t)pq * a.channels;
+                        rm = __fdiv_rn(__fadd_rn(__fadd_rn(im[0], im[1]), im[2]), 3.0f);
+                    }
+                    if (a.error_pp) {
+                        er = a.error_pp[pq];
+                        era = a.error_pp[(size_t)a.n_pixels + pq];
+                    }
+                    if (a.spp_patch) ns = a.spp_patch[pq];
                 }
                 if (a.copy_rrs_node) {
 #pragma unroll
@@ -794,8 +764,12 @@ __global__ void __launch_bounds__(kRecThreads, 5) k_generate(const __grid_consta
                 if (o.depth) o.depth[t] = dep;
                 if (o.rrs_target) o.rrs_target[t] = same ? -1.0f : rrs;
                 if (o.pixel) o.pixel[t] = px;
-                if (!px_ok && (a.image || a.pixel_samples)) flags |= NRRS_DEV_BAD_INDEX;
+                if (!px_ok && (a.image || a.pixel_samples || a.error_pp || a.spp_patch))
+                    flags |= NRRS_DEV_BAD_INDEX;
                 if (o.ref_mean && a.image) o.ref_mean[t] = rm;
+                if (o.error && a.error_pp) o.error[t] = er;
+                if (o.error_for_avg && a.error_pp) o.error_for_avg[t] = era;
+                if (o.number_samples && a.spp_patch) o.number_samples[t] = ns;
                 if (!same && px_ok && a.pixel_samples) atomicAdd(&a.pixel_samples[px], 1u);
             }
         }

@@ -92,6 +92,9 @@ struct GenerateArgs {
     uint32_t channels, n_pixels, capacity, spin_limit;
     int32_t ignore_zero_l, copy_rrs_node, dedupe;
     float thp_eps;
+    const float* error_pp;      // [2][n_pixels] per-pixel error, or null
+    const float* spp_patch;     // [patches] samples per patch, or null
+    uint32_t frame_width, scale;  // scale > 1: image and error arrays are per patch
 };
 
 struct WeightArgs {

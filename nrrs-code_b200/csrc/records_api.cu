@@ -233,6 +233,10 @@ extern "C" int nrrs_generate_training_data(const nrrs_path_nodes* nodes,
     if (!valid(nodes) || !p || !out || !size_dev) return NRRS_ERR_INVALID_ARG;
     if (image && image_channels != 3 && image_channels != 4) return NRRS_ERR_INVALID_ARG;
     if (!(p->thp_eps >= 0.f)) return NRRS_ERR_INVALID_ARG;
+    if (p->error_image_scale > 1u) {   // whole patches only
+        const uint32_t w = p->frame_width, sc = p->error_image_scale;
+        if (w == 0 || n_pixels % w || w % sc || (n_pixels / w) % sc) return NRRS_ERR_INVALID_ARG;
+    }
     cudaStream_t s = (cudaStream_t)stream;
     const NodeView nb = view(nodes);
     if (sm_count() <= 0) return NRRS_ERR_NO_DEVICE;
@@ -251,6 +255,10 @@ extern "C" int nrrs_generate_training_data(const nrrs_path_nodes* nodes,
     a.copy_rrs_node = p->copy_rrs_node;
     a.dedupe = p->dedupe_rrs_target;
     a.thp_eps = p->thp_eps;
+    a.error_pp = p->error_per_pixel;
+    a.spp_patch = p->samples_per_patch;
+    a.frame_width = p->frame_width;
+    a.scale = p->error_image_scale;
     const int gg = persistent_grid(nodes->capacity, kRecChunk, 8);
     return launch_generate(a, gg, s) == cudaSuccess ? NRRS_OK : NRRS_ERR_CUDA;
 }

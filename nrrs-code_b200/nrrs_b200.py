@@ -84,11 +84,26 @@ class PathNodes(C.Structure):
 
 class TrainDataParams(C.Structure):
     _fields_ = [("ignore_zero_l", C.c_int32), ("copy_rrs_node", C.c_int32),
-                ("dedupe_rrs_target", C.c_int32), ("thp_eps", C.c_float)]
+                ("dedupe_rrs_target", C.c_int32), ("thp_eps", C.c_float),
+                ("frame_width", C.c_uint32), ("error_image_scale", C.c_uint32),
+                ("error_per_pixel", C.c_void_p), ("samples_per_patch", C.c_void_p)]
 
 
 TRAIN_BATCH_FIELDS = ("pos", "wi", "normal", "albedo", "roughness", "thp", "depth", "ref_mean",
-                      "target", "rrs_target", "pixel")
+                      "target", "rrs_target", "pixel", "error", "error_for_avg",
+                      "number_samples")
+
+
+class PixelErrorParams(C.Structure):
+    """nrrs_pixel_error_params: the frame, its patches and the error switches."""
+    _fields_ = [("frame_width", C.c_uint32), ("frame_height", C.c_uint32), ("scale", C.c_uint32),
+                ("blend_weight", C.c_float), ("clamp", C.c_int32),
+                ("multiply_samples", C.c_int32)]
+
+
+class ErrorSum(C.Structure):
+    """nrrs_error_sum: exact sum of the errors (device struct, zeroed once)."""
+    _fields_ = [("acc", C.c_int64 * 3), ("done", C.c_uint32), ("value", C.c_float)]
 
 
 class TrainBatch(C.Structure):
@@ -190,6 +205,16 @@ _SIGS = {
                                               C.c_void_p]),
     "nrrs_sample_weights": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
                                       C.c_void_p, C.c_void_p]),
+    "nrrs_count_patch_samples": (C.c_int, [C.POINTER(PixelErrorParams), C.c_void_p, C.c_uint32,
+                                           C.c_void_p, C.c_void_p]),
+    "nrrs_accumulate_weighted_l": (C.c_int, [C.POINTER(PixelErrorParams), C.c_void_p, C.c_uint32,
+                                             C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_void_p]),
+    "nrrs_update_weighted_l": (C.c_int, [C.POINTER(PixelErrorParams), C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_void_p]),
+    "nrrs_calculate_error": (C.c_int, [C.POINTER(PixelErrorParams), C.c_void_p, C.c_int32,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p]),
     "nrrs_last_infer_grid": (C.c_int32, [C.c_void_p]),
     "nrrs_kernel_name": (C.c_char_p, [C.c_int32]),
     "nrrs_profile_enable": (C.c_int, [C.c_void_p, C.c_int32]),
@@ -371,7 +396,7 @@ def path_nodes_bytes(capacity: int, max_record: int) -> int:
 def default_train_data_params(**kw) -> TrainDataParams:
     """The reference's defaults: zero-L samples kept, thp not scaled by rrs, no deduplication,
     thp threshold 1e-5."""
-    p = TrainDataParams(0, 0, 0, 1e-5)
+    p = TrainDataParams(0, 0, 0, 1e-5, 0, 0, None, None)
     for k, v in kw.items():
         setattr(p, k, v)
     return p
@@ -428,6 +453,50 @@ class NRRSPathNodesBuffer:
                                                  _ptr(pixel_samples), C.byref(batch), capacity,
                                                  _ptr(size_dev), stream),
                "nrrs_generate_training_data")
+
+
+def default_pixel_error_params(frame_width: int, frame_height: int, **kw) -> PixelErrorParams:
+    """The reference's defaults: patches of one pixel (the shipped error_image_scale), blend
+    weight 0.5, error clamped at 100, error_for_avg not scaled by the sample count."""
+    p = PixelErrorParams(frame_width, frame_height, 1, 0.5, 1, 0)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def count_patch_samples(params: PixelErrorParams, pixel, n: int, samples_per_patch, stream=0):
+    """nrrs_count_patch_samples: +1 per ray in its pixel's patch."""
+    _check(lib().nrrs_count_patch_samples(C.byref(params), _ptr(pixel), n,
+                                          _ptr(samples_per_patch), stream),
+           "nrrs_count_patch_samples")
+
+
+def accumulate_weighted_l(params: PixelErrorParams, pixel_l, spp: int, first_frame: bool,
+                          weighted_l, weighted_l_current, weighted_l_current_acc, stream=0):
+    """nrrs_accumulate_weighted_l: this frame's radiance per patch (trainStep STEP#1.1)."""
+    _check(lib().nrrs_accumulate_weighted_l(C.byref(params), _ptr(pixel_l), spp,
+                                            1 if first_frame else 0, _ptr(weighted_l),
+                                            _ptr(weighted_l_current),
+                                            _ptr(weighted_l_current_acc), stream),
+           "nrrs_accumulate_weighted_l")
+
+
+def update_weighted_l(params: PixelErrorParams, weighted_l_current, weighted_l_current_acc,
+                      weighted_l, stream=0):
+    """nrrs_update_weighted_l (nrrs_update_weighted_L, train.cu:344-363)."""
+    _check(lib().nrrs_update_weighted_l(C.byref(params), _ptr(weighted_l_current),
+                                        _ptr(weighted_l_current_acc), _ptr(weighted_l), stream),
+           "nrrs_update_weighted_l")
+
+
+def calculate_error(params: PixelErrorParams, ref, ref_channels: int, weighted_l,
+                    samples_per_patch, error, error_sum=None, stream=0):
+    """nrrs_calculate_error (train.cu:365-430) and the exact error sum into error_sum, a device
+    buffer of at least sizeof(ErrorSum) bytes zeroed once."""
+    _check(lib().nrrs_calculate_error(C.byref(params), _ptr(ref), ref_channels, _ptr(weighted_l),
+                                      _ptr(samples_per_patch), _ptr(error), _ptr(error_sum),
+                                      stream),
+           "nrrs_calculate_error")
 
 
 def calculate_sample_weight(pixel, pixel_samples, n_pixels: int, size_dev, max_n: int, weight,

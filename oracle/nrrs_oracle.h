@@ -99,6 +99,16 @@ uint64_t oracle_generate_training_data(nrrs_path_nodes* nb, const nrrs_train_dat
 void oracle_sample_weights(const uint32_t* pixel, const uint32_t* pixel_samples,
                            uint32_t n_pixels, uint64_t n, float* weight);
 
+/* per-pixel error of the RRSNet loss (records.c); HOST arrays */
+void oracle_count_patch_samples(const nrrs_pixel_error_params* p, const uint32_t* pixel,
+                                uint64_t n, float* spp);
+void oracle_accumulate_weighted_l(const nrrs_pixel_error_params* p, const float* pl, uint32_t spp,
+                                  int first, float* wl, float* cur, uint32_t* acc);
+void oracle_update_weighted_l(const nrrs_pixel_error_params* p, const float* cur,
+                              const uint32_t* acc, float* wl);
+float oracle_calculate_error(const nrrs_pixel_error_params* p, const float* ref, int ch,
+                             const float* wl, const float* spp, float* err_out);
+
 /* threads used by the OpenMP loops (0 = runtime default) */
 void oracle_set_threads(int n);
 int oracle_get_threads(void);

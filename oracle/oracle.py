@@ -88,6 +88,12 @@ def lib():
                                                     C.c_uint32, vp, C.POINTER(nb.TrainBatch),
                                                     C.c_uint64]
         L.oracle_sample_weights.argtypes = [vp, vp, C.c_uint32, C.c_uint64, vp]
+        pe = C.POINTER(nb.PixelErrorParams)
+        L.oracle_count_patch_samples.argtypes = [pe, vp, C.c_uint64, vp]
+        L.oracle_accumulate_weighted_l.argtypes = [pe, vp, C.c_uint32, C.c_int, vp, vp, vp]
+        L.oracle_update_weighted_l.argtypes = [pe, vp, vp, vp]
+        L.oracle_calculate_error.restype = C.c_float
+        L.oracle_calculate_error.argtypes = [pe, vp, C.c_int, vp, vp, vp]
         L.oracle_set_threads.argtypes = [C.c_int]
         L.oracle_get_threads.restype = C.c_int
         _lib = L
@@ -298,16 +304,18 @@ class HostNodes:
                                      len(node))
 
     def generate(self, params, capacity: int, image=None, n_pixels: int = 0,
-                 pixel_samples=None) -> tuple[dict, int]:
+                 pixel_samples=None, out=None) -> tuple[dict, int]:
         """The training batch as numpy arrays (the first min(total, capacity) rows) and the
-        total sample count."""
+        total sample count. out (optional) is a dict of preallocated batch arrays to reuse."""
         cap = max(capacity, 1)
-        out = {"pos": np.zeros((cap, 3), np.float32), "wi": np.zeros((cap, 3), np.float32),
+        out = out if out is not None else {"pos": np.zeros((cap, 3), np.float32), "wi": np.zeros((cap, 3), np.float32),
                "normal": np.zeros((cap, 3), np.float32), "albedo": np.zeros((cap, 3), np.float32),
                "roughness": np.zeros(cap, np.float32), "thp": np.zeros((cap, 3), np.float32),
                "depth": np.zeros(cap, np.uint32), "ref_mean": np.zeros(cap, np.float32),
                "target": np.zeros((cap, 3), np.float32), "rrs_target": np.zeros(cap, np.float32),
-               "pixel": np.zeros(cap, np.uint32)}
+               "pixel": np.zeros(cap, np.uint32), "error": np.zeros(cap, np.float32),
+               "error_for_avg": np.zeros(cap, np.float32),
+               "number_samples": np.zeros(cap, np.float32)}
         batch = nb.TrainBatch(*(out[k].ctypes.data for k in nb.TRAIN_BATCH_FIELDS))
         if image is not None:
             image = np.ascontiguousarray(image, np.float32)
@@ -330,7 +338,8 @@ def sample_weights(pixel, pixel_samples, n_pixels: int) -> np.ndarray:
     return w[:len(pixel)]
 
 
-def frame_training_data(bounces, image, capacity: int, params, batch_capacity=None):
+def frame_training_data(bounces, image, capacity: int, params, batch_capacity=None,
+                        n_pixels=None):
     """The oracle's run of a whole synthetic frame: per bounce record the nodes, then the
     contributions; then the batch, the per-pixel counts and the weights."""
     hn = HostNodes(capacity)
@@ -338,10 +347,45 @@ def frame_training_data(bounces, image, capacity: int, params, batch_capacity=No
     for b in bounces:
         node_outs.append(hn.record_nodes(b))
         hn.record_radiance(b["contrib_node"], b["contrib"])
-    n_pixels = image.shape[0]
+    n_pixels = image.shape[0] if n_pixels is None else n_pixels
     counts = np.zeros(n_pixels, np.uint32)
     bc = capacity if batch_capacity is None else batch_capacity
     batch, total = hn.generate(params, bc, image=image, n_pixels=n_pixels, pixel_samples=counts)
     weights = sample_weights(batch["pixel"], counts, n_pixels)
     return {"nodes": hn, "node_outs": node_outs, "batch": batch, "total": total,
             "counts": counts, "weights": weights}
+
+
+# ---- per-pixel error of the RRSNet loss (records.c) -------------------------------------------
+
+def count_patch_samples(params, pixel, spp):
+    pixel = np.ascontiguousarray(pixel, np.uint32)
+    lib().oracle_count_patch_samples(C.byref(params), pixel.ctypes.data, len(pixel), spp.ctypes.data)
+
+
+def accumulate_weighted_l(params, pixel_l, spp: int, first: bool, wl, cur, acc):
+    pixel_l = np.ascontiguousarray(pixel_l, np.float32)
+    lib().oracle_accumulate_weighted_l(C.byref(params), pixel_l.ctypes.data, spp, int(first),
+                                       wl.ctypes.data, cur.ctypes.data, acc.ctypes.data)
+
+
+def update_weighted_l(params, cur, acc, wl):
+    lib().oracle_update_weighted_l(C.byref(params), cur.ctypes.data, acc.ctypes.data,
+                                   wl.ctypes.data)
+
+
+def calculate_error(params, ref, wl, spp, err) -> float:
+    ref = np.ascontiguousarray(ref, np.float32)
+    return float(lib().oracle_calculate_error(C.byref(params), ref.ctypes.data, ref.shape[1],
+                                              wl.ctypes.data,
+                                              spp.ctypes.data if spp is not None else None,
+                                              err.ctypes.data))
+
+
+def batch_arrays(capacity: int) -> dict:
+    """Preallocated batch arrays for HostNodes.generate(out=...)."""
+    cap = max(capacity, 1)
+    v3 = ("pos", "wi", "normal", "albedo", "thp", "target")
+    return {k: np.zeros((cap, 3) if k in v3 else cap,
+                        np.uint32 if k in ("depth", "pixel") else np.float32)
+            for k in nb.TRAIN_BATCH_FIELDS}

@@ -241,15 +241,27 @@ uint64_t oracle_generate_training_data(nrrs_path_nodes* nb, const nrrs_train_dat
             if (o->rrs_target) o->rrs_target[t] = same ? -1.0f : rrs;       /* :520-535 */
             if (o->pixel) o->pixel[t] = px;
             const int px_ok = px < n_pixels;
-            if (!px_ok && (image || pixel_samples)) nb->header[HDR_STATUS] |= NRRS_DEV_BAD_INDEX;
+            if (!px_ok && (image || pixel_samples || p->error_per_pixel || p->samples_per_patch))
+                nb->header[HDR_STATUS] |= NRRS_DEV_BAD_INDEX;
+            /* the sample's patch of the film and error images (offsetFrame2Scaled) */
+            const uint32_t sc = p->error_image_scale, fw = p->frame_width;
+            const uint32_t pq = !px_ok ? 0u
+                                : sc > 1u ? (px % fw) / sc + ((px / fw) / sc) * (fw / sc) : px;
             if (o->ref_mean && image) {                                        /* :528-529 */
                 float rm = 0.f;
                 if (px_ok) {
-                    const float* q = image + (uint64_t)px * (uint64_t)channels;
+                    const float* q = image + (uint64_t)pq * (uint64_t)channels;
                     rm = ((q[0] + q[1]) + q[2]) / 3.0f;
                 }
                 o->ref_mean[t] = rm;
             }
+            if (p->error_per_pixel) {                                          /* :537-545 */
+                if (o->error) o->error[t] = px_ok ? p->error_per_pixel[pq] : 0.f;
+                if (o->error_for_avg)
+                    o->error_for_avg[t] = px_ok ? p->error_per_pixel[(uint64_t)n_pixels + pq] : 0.f;
+            }
+            if (p->samples_per_patch && o->number_samples)
+                o->number_samples[t] = px_ok ? p->samples_per_patch[pq] : 0.f;
             if (!same && px_ok && pixel_samples) pixel_samples[px] += 1;     /* :532-533 */
         }
         ++t;
@@ -265,4 +277,104 @@ void oracle_sample_weights(const uint32_t* pixel, const uint32_t* pixel_samples,
         const uint32_t c = pixel[t] < n_pixels ? pixel_samples[pixel[t]] : 0u;
         weight[t] = c ? 1.0f / (float)c : 0.0f;
     }
+}
+
+/* ---- per-pixel error of the RRSNet loss (one patch = scale x scale frame pixels) ---------------- */
+
+typedef struct {
+    uint32_t w, h, s, pw, ph;
+} geom_t;
+
+static geom_t geom_of(const nrrs_pixel_error_params* p) {
+    geom_t g;
+    g.w = p->frame_width;
+    g.h = p->frame_height;
+    g.s = p->scale ? p->scale : 1u;
+    g.pw = g.w / g.s;
+    g.ph = g.h / g.s;
+    return g;
+}
+
+/* offsetFrame2Scaled (myFilm.h:6-15) */
+static uint32_t patch_of(const geom_t* g, uint32_t px) {
+    return (px % g->w) / g->s + ((px / g->w) / g->s) * g->pw;
+}
+
+/* patch sample counts: +1 per camera ray (integrator.cpp:1050) and scattered ray (:803-808) */
+void oracle_count_patch_samples(const nrrs_pixel_error_params* p, const uint32_t* pixel,
+                                uint64_t n, float* spp) {
+    const geom_t g = geom_of(p);
+    for (uint64_t i = 0; i < n; ++i)
+        if (pixel[i] < g.w * g.h) spp[patch_of(&g, pixel[i])] += 1.0f;
+}
+
+/* STEP#1.1 after the per-frame reset (integrator.cpp:1027-1028, 2379-2395) and the first-frame
+ * initialisation (:2358-2375); a patch's pixels are added in pixel order */
+void oracle_accumulate_weighted_l(const nrrs_pixel_error_params* p, const float* pl, uint32_t spp,
+                                  int first, float* wl, float* cur, uint32_t* acc) {
+    const geom_t g = geom_of(p);
+    const float fspp = (float)spp;
+    for (uint32_t ps = 0; ps < g.pw * g.ph; ++ps) {
+        const uint32_t x0 = (ps % g.pw) * g.s, y0 = (ps / g.pw) * g.s;
+        float c[3] = {0.f, 0.f, 0.f}, f[3] = {0.f, 0.f, 0.f};
+        for (uint32_t dy = 0; dy < g.s; ++dy)
+            for (uint32_t dx = 0; dx < g.s; ++dx) {
+                const uint64_t px = (uint64_t)(y0 + dy) * g.w + x0 + dx;
+                for (int k = 0; k < 3; ++k) {
+                    c[k] = c[k] + pl[3 * px + k];
+                    if (first) f[k] = f[k] + pl[3 * px + k] / fspp;
+                }
+            }
+        for (int k = 0; k < 3; ++k) {
+            cur[3 * (uint64_t)ps + k] = c[k];
+            if (first) wl[3 * (uint64_t)ps + k] = f[k];
+        }
+        acc[ps] = spp * g.s * g.s;
+    }
+}
+
+/* nrrs_update_weighted_L (train.cu:344-363) */
+void oracle_update_weighted_l(const nrrs_pixel_error_params* p, const float* cur,
+                              const uint32_t* acc, float* wl) {
+    const geom_t g = geom_of(p);
+    const float keep = 1.0f - p->blend_weight;
+    for (uint32_t ps = 0; ps < g.pw * g.ph; ++ps) {
+        const float n = (float)acc[ps];
+        for (int k = 0; k < 3; ++k) {
+            const float lc = cur[3 * (uint64_t)ps + k] / n;
+            const float lb = wl[3 * (uint64_t)ps + k];
+            wl[3 * (uint64_t)ps + k] = lb * keep + lc * p->blend_weight;
+        }
+    }
+}
+
+/* nrrs_calculate_error (train.cu:365-430); returns the exact sum of error[npix + patch]
+ * (integrator.cpp:2466-2471) rounded to float, NaN if a term is not finite or >= 2^62 */
+float oracle_calculate_error(const nrrs_pixel_error_params* p, const float* ref, int ch,
+                             const float* wl, const float* spp, float* err_out) {
+    const geom_t g = geom_of(p);
+    const uint64_t npix = (uint64_t)g.w * g.h;
+    int64_t acc[3] = {0, 0, 0};
+    int bad = 0;
+    for (uint32_t ps = 0; ps < g.pw * g.ph; ++ps) {
+        float q[3];
+        for (int k = 0; k < 3; ++k) {
+            const float r = ref[(uint64_t)ps * ch + k];
+            const float d = wl[3 * (uint64_t)ps + k] - r;
+            q[k] = (d * d) / (r * r + 0.01f);
+        }
+        float e = ((q[0] + q[1]) + q[2]) / 3.0f;
+        if (p->clamp) e = fminf(e, 100.0f);
+        err_out[ps] = e;
+        if (p->multiply_samples) e = e * sqrtf(spp[ps]);
+        err_out[npix + ps] = e;
+        if (fabsf(e) < FIXED_MAX) {
+            int64_t l[3];
+            oracle_fixed_limbs(e, l);
+            for (int k = 0; k < 3; ++k) acc[k] = (int64_t)((uint64_t)acc[k] + (uint64_t)l[k]);
+        } else {
+            bad = 1;
+        }
+    }
+    return bad ? NAN : oracle_fixed_to_float(acc[0], acc[1], acc[2]);
 }

@@ -11,6 +11,8 @@ reference formulas, written out below in float32 numpy arithmetic independent of
   decision / emission    src/render/nrrs/integrator.cpp:1368-1460, commonworkqueue.h:19-25
   path records, training data and sample weights
                          src/render/nrrs/workqueue.h:122-170, train.cu:432-592
+  per-pixel error (weighted L, relative error, clamp, sqrt(spp), error sum)
+                         src/render/nrrs/train.cu:344-430, integrator.cpp:2358-2471
 
 Each decision case also lists the expected split counts worked out by hand in its comment.
 Run: python tests/golden/make_golden.py  (rewrites the JSON files next to this script).
@@ -204,6 +206,85 @@ def records_cases():
     return cases
 
 
+def pixel_error_expected(case):
+    """Float32 restatement of weighted L (first frame, STEP#1.1), nrrs_update_weighted_L and
+    nrrs_calculate_error, with patches added in pixel order and the error sum exact."""
+    from fractions import Fraction
+    w, h, sc = case["frame_width"], case["frame_height"], case["scale"]
+    pw, ph = w // sc, h // sc
+    pl = [[F(x) for x in px] for px in case["pixel_l"]]
+    spp = F(case["spp"])
+    cur, first, acc = [], [], []
+    for ps in range(pw * ph):
+        x0, y0 = (ps % pw) * sc, (ps // pw) * sc
+        c, f = [F(0)] * 3, [F(0)] * 3
+        for dy in range(sc):
+            for dx in range(sc):
+                px = (y0 + dy) * w + x0 + dx
+                c = [F(c[k] + pl[px][k]) for k in range(3)]
+                f = [F(f[k] + F(pl[px][k] / spp)) for k in range(3)]
+        cur.append(c)
+        first.append(f)
+        acc.append(case["spp"] * sc * sc)
+    b = F(case["blend"])
+    keep = F(F(1) - b)
+    wl = []
+    for ps in range(pw * ph):
+        n = F(acc[ps])
+        wl.append([F(F(first[ps][k] * keep) + F(F(cur[ps][k] / n) * b)) for k in range(3)])
+    err, err_avg = [], []
+    for ps in range(pw * ph):
+        q = []
+        for k in range(3):
+            r = F(case["ref"][ps][k])
+            d = F(wl[ps][k] - r)
+            q.append(F(F(d * d) / F(F(r * r) + F(0.01))))
+        e = F(F(F(q[0] + q[1]) + q[2]) / F(3))
+        if case["clamp"]:
+            e = F(100) if math.isnan(e) else min(e, F(100))
+        err.append(e)
+        if case["multiply_samples"]:
+            e = F(e * F(math.sqrt(float(F(case["spp_patch"][ps])))))
+        err_avg.append(e)
+    total = sum(Fraction(float(e)) for e in err_avg)
+    return dict(current=[[float(x) for x in c] for c in cur], acc=acc,
+                first=[[float(x) for x in f] for f in first],
+                weighted=[[float(x) for x in v] for v in wl],
+                error=[float(e) for e in err], error_for_avg=[float(e) for e in err_avg],
+                sum=float(F(float(total))))
+
+
+def pixel_error_cases():
+    """Worked values of "patch2x2": frame 4x2, patches of 2x2 pixels, spp 2.
+      patch 0 (pixels 0,1,4,5): pixel L (1,2,0.5) (3,0,0.5) (0,2,1) (4,4,0) -> current (8,8,2),
+        acc 8, first frame sum of L/2 = (4,4,1); blend 0.5: 0.5*(4,4,1) + 0.5*(1,1,0.25)
+        = (2.5, 2.5, 0.625)
+      patch 1 (pixels 2,3,6,7): all L 0 -> current 0, weighted 0
+      errors against ref (2.5,2.5,0.625) and (0,0,0): 0 and 0 (clamp on, no sample scaling)"""
+    nan = float("nan")
+    cases = [
+        dict(name="patch2x2", frame_width=4, frame_height=2, scale=2, spp=2, blend=0.5,
+             clamp=1, multiply_samples=0,
+             pixel_l=[[1, 2, 0.5], [3, 0, 0.5], [0, 0, 0], [0, 0, 0],
+                      [0, 2, 1], [4, 4, 0], [0, 0, 0], [0, 0, 0]],
+             ref=[[2.5, 2.5, 0.625, 1], [0, 0, 0, 1]], spp_patch=[8, 8]),
+        dict(name="clamp_nan_sqrt", frame_width=2, frame_height=2, scale=1, spp=1, blend=0.25,
+             clamp=1, multiply_samples=1,
+             # pixel 0: error 100*(2^2+...)/3 far above 100 -> clamped; pixel 1: NaN -> 100;
+             # pixel 2: small error scaled by sqrt(9) = 3; pixel 3: exact match -> 0
+             pixel_l=[[2, 2, 2], [nan, 0, 0], [1.5, 0.5, 1], [0.25, 0.5, 0.75]],
+             ref=[[0, 0, 0, 1], [1, 1, 1, 1], [1, 1, 1, 1], [0.25, 0.5, 0.75, 1]],
+             spp_patch=[4, 1, 9, 16]),
+        dict(name="no_clamp", frame_width=2, frame_height=1, scale=1, spp=4, blend=0.5,
+             clamp=0, multiply_samples=0,
+             pixel_l=[[8, 8, 8], [4, 0, 0]], ref=[[0, 0, 0, 0], [1, 0, 0, 0]],
+             spp_patch=[1, 1]),
+    ]
+    for c in cases:
+        c["expect"] = pixel_error_expected(c)
+    return cases
+
+
 def main():
     ka = {
         "activation_sigma": [[x, float(act_sigma(x))] for x in (-10.0, -1.0, -0.5, 0.0, 0.5, 1.0, 10.0)],
@@ -271,6 +352,8 @@ def main():
         rrs=[], rnd=[], budget=10, nspec=0, use_ceil=True, rate=0.85, scale_up=False)
 
     (HERE / "known_answers.json").write_text(json.dumps(ka, indent=1) + "\n")
+    pe = pixel_error_cases()
+    (HERE / "pixel_error_cases.json").write_text(json.dumps(pe, indent=1, allow_nan=True) + "\n")
     rc = records_cases()
     (HERE / "records_cases.json").write_text(json.dumps(rc, indent=1, allow_nan=True) + "\n")
     (HERE / "decide_cases.json").write_text(json.dumps(cases, indent=1) + "\n")
