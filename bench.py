@@ -681,6 +681,7 @@ def records_cpu(wl, bounces, image, pixel_l, seconds: float):
     acc = np.zeros(P, np.uint32)
     err = np.zeros(2 * P, np.float32)
     spp = np.zeros(P, np.float32)
+    uerr = np.zeros(P, np.float32)
     prm = records_params(frame_width=W, error_image_scale=1, error_per_pixel=err.ctypes.data,
                          samples_per_patch=spp.ctypes.data)
     cap = wl["node_rate"] * P
@@ -699,6 +700,7 @@ def records_cpu(wl, bounces, image, pixel_l, seconds: float):
         O.accumulate_weighted_l(pe, pixel_l, 1, False, wl_, cur, acc)
         O.update_weighted_l(pe, cur, acc, wl_)
         O.calculate_error(pe, image, wl_, spp, err)
+        O.ubs_error(pe, pixel_l, 1, image, uerr)
         counts[:] = 0
         batch, total = hn.generate(prm, cap, image=image, n_pixels=P, pixel_samples=counts, out=out)
         O.sample_weights(batch["pixel"], counts, P)
@@ -790,6 +792,8 @@ def run_records(args, rank, world, local_rank):
     err_d = torch.zeros(2 * P, dtype=torch.float32, device=dev)
     spp_d = torch.zeros(P, dtype=torch.float32, device=dev)
     esum_d = torch.zeros(32, dtype=torch.uint8, device=dev)
+    uerr_d = torch.zeros(P, dtype=torch.float32, device=dev)
+    usum_d = torch.zeros(32, dtype=torch.uint8, device=dev)
     prm = records_params(frame_width=W, error_image_scale=1, error_per_pixel=err_d.data_ptr(),
                          samples_per_patch=spp_d.data_ptr())
 
@@ -821,6 +825,8 @@ def run_records(args, rank, world, local_rank):
         nb.accumulate_weighted_l(pe, pl_d, 1, False, wl_d, cur_d, acc_d, stream)
         nb.update_weighted_l(pe, cur_d, acc_d, wl_d, stream)
         nb.calculate_error(pe, img_d, 4, wl_d, spp_d, err_d, esum_d, stream)
+        # the frame's error as the per-depth strategy search scores it (UBSAnalyseFrame)
+        nb.ubs_error(pe, pl_d, 1, img_d, 4, uerr_d, usum_d, stream)
         if ev:
             ev["pe"][1].record(cur)
         if ev:
@@ -843,8 +849,8 @@ def run_records(args, rank, world, local_rank):
             post("image")
 
     # per bounce: record count, record writes, radiance, patch counts; then the pixel error
-    # (3), radiance pass, batch, weights (the zero_ fills are torch's)
-    launches_per_step = 4 * len(bounces) + 6
+    # (3) and the UBS error, radiance pass, batch, weights (the zero_ fills are torch's)
+    launches_per_step = 4 * len(bounces) + 7
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -954,14 +960,14 @@ def run_records(args, rank, world, local_rank):
     # pixel error: per ray its pixel read and one atomic on its patch count; per pixel the
     # radiance read, the current sum and count written, blended (read 28 B, write 12 B), the
     # film, estimate and count read and two errors written
-    b_pe = n_vert * (4 + 16) + P * (12 + 16 + 28 + 12 + 32 + 8)
+    b_pe = n_vert * (4 + 16) + P * (12 + 16 + 28 + 12 + 32 + 8) + P * (12 + 16 + 4)
     # the batch also gathers each sample's two errors and sample count
     b_gen += total * 12
     calls = {"record_nodes": (t_rec, b_rec, 2 * len(bounces)),
              "record_radiance": (t_rad, b_rad, len(bounces)),
              "radiance_pass": (t_prop, b_prop, 1), "batch": (t_gen, b_gen, 1),
              "sample_weights": (t_wgt, b_wgt, 1),
-             "pixel_error": (t_pe, b_pe, len(bounces) + 3)}
+             "pixel_error": (t_pe, b_pe, len(bounces) + 4)}
     peak, peak_kind = measured_peaks()
     dom = max(calls, key=lambda k: calls[k][0])
     t_dom, b_dom, n_dom = calls[dom]

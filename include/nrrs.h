@@ -12,6 +12,8 @@
  *      from them                                   (nrrs_record_nodes ... nrrs_sample_weights)
  *   6. the per-pixel error of the RRSNet loss      (nrrs_count_patch_samples ...
  *                                                   nrrs_calculate_error)
+ *   7. the per-depth strategy search and the training schedule (host; nrrs_ubs_*,
+ *      nrrs_train_schedule_*)
  *
  * Everything is asynchronous on the caller's CUDA stream (passed as void*; NULL = legacy
  * default stream). Input and output buffers are device pointers owned by the caller. The
@@ -529,6 +531,81 @@ int nrrs_update_weighted_l(const nrrs_pixel_error_params* p, const float* weight
 int nrrs_calculate_error(const nrrs_pixel_error_params* p, const float* ref, int32_t ref_channels,
                          const float* weighted_l, const float* samples_per_patch, float* error,
                          nrrs_error_sum* sum, void* stream);
+
+/* UBS per-pixel error (nrrs_UBS_calc_error, train.cu:594-608) and its sum (integrator.cpp:
+ * 2875-2886): error[pixel] = mean_c (L_c - ref_c)^2 / (ref_c^2 + 0.01) with L = pixel_l / spp
+ * and ref the film read at the pixel's patch; sum (may be NULL) receives the exact sum. */
+int nrrs_ubs_error(const nrrs_pixel_error_params* p, const float* pixel_l, uint32_t spp,
+                   const float* ref, int32_t ref_channels, float* error, nrrs_error_sum* sum,
+                   void* stream);
+
+/* ==== per-depth strategy search (UBS) and the training schedule =================================
+ * Host-side control of which factor source the path uses per depth, and when training moves
+ * through steps 0-3. No GPU work; all calls are synchronous. Replaces, in NRRSPathTracer:
+ *   UBS ("use best strategy")       integrator.h:324-439, integrator.cpp:2787-2891, 1088-1090, 1610,
+ *                                   1780-1783; isInferMode integrator.h:67-71
+ *   autoTrainControl                integrator.cpp:2659-2736 */
+typedef enum {
+    NRRS_UBS_FIXED_RR = 0,          /* no inference at this depth (the tracer's own RR)          */
+    NRRS_UBS_ADRRS = 1,             /* ADRRS factors (step 2)                                     */
+    NRRS_UBS_NRRS = 2,              /* RRSNet factors (step 3)                                    */
+    NRRS_UBS_COUNT = 3
+} nrrs_ubs_strategy;
+
+typedef struct nrrs_ubs nrrs_ubs;
+/* max_depth: strategies searched per depth 0..max_depth-1 (mMaxDepth, at most 19 so that every
+ * strategy string fits in 32 bits). error_eval_seconds: the cost of computing the error, taken off
+ * each frame's time (0.17e-3, integrator.cpp:2856-2858). */
+int nrrs_ubs_create(int32_t max_depth, double error_eval_seconds, nrrs_ubs** out);
+void nrrs_ubs_destroy(nrrs_ubs* u);
+/* UBSResetAndBeginSearch (integrator.h:376-389) */
+int nrrs_ubs_begin_search(nrrs_ubs* u);
+/* At the start of a frame while searching: UBSNextState (integrator.cpp:2798-2820); when the
+ * enumeration is over, UBSEndSearch (integrator.h:391-405) makes the best strategy current and
+ * this returns 0; 1 while the search goes on. */
+int nrrs_ubs_next_state(nrrs_ubs* u);
+/* At the end of a frame while searching: UBSAnalyseFrame's bookkeeping (integrator.cpp:
+ * 2822-2877). now_seconds is the caller's clock at this call; frame_error_sum the exact sum of
+ * nrrs_ubs_error over the frame just rendered, used at the next call as the reference uses its
+ * asynchronous copy; resolution the frame's pixels. */
+int nrrs_ubs_analyse_frame(nrrs_ubs* u, double now_seconds, double frame_error_sum,
+                           uint32_t resolution);
+/* The strategy of a depth: while searching, digit `depth` of the search state; with a best (or
+ * set) strategy in use, its entry; -1 when neither (no strategy chooses). Depths at or beyond
+ * max_depth (up to 63) are NRRS_UBS_FIXED_RR, as the reference's zero-filled array gives. */
+int nrrs_ubs_get_strategy(const nrrs_ubs* u, int32_t depth);
+/* Whether depth runs inference (isInferMode) and with which factor source: *factor_source is
+ * NRRS_FACTOR_ADRRS or NRRS_FACTOR_RRSNET (may be NULL); without search or a best strategy the
+ * source is use_net_output_rrs ? RRSNET : ADRRS (mLossUseNetworkOutputRRS). */
+int nrrs_ubs_need_infer(const nrrs_ubs* u, int32_t depth, int32_t enable_rrs, float clamp_min,
+                        float clamp_max, int32_t max_rrs_depth, int32_t use_net_output_rrs,
+                        int32_t* factor_source);
+/* The best strategy per depth ([max_depth]) and its efficiency (resolution / (time x error)). */
+int nrrs_ubs_best(const nrrs_ubs* u, int32_t* strategy, float* efficiency);
+/* mUBSArrayChar (UBSUpdateAccordingArrayChar, integrator.h:364-374): one digit 0-2 per depth;
+ * other characters become 0. Sets the best strategy and uses it (mUseBestStrategy). */
+int nrrs_ubs_set_best(nrrs_ubs* u, const char* digits);
+/* searching (1) or not (0) */
+int nrrs_ubs_searching(const nrrs_ubs* u);
+
+/* autoTrainControl (integrator.cpp:2659-2736): the steps by elapsed time. durations: seconds of
+ * states 0-3 (mAutoTrainStateTime). Each tick returns the state to apply this frame. */
+typedef struct {
+    int32_t state;                  /* 0..4                                                       */
+    int32_t step;                   /* nrrs_set_step value                                        */
+    int32_t enable_rrs;             /* mEnableRRS                                                 */
+    int32_t use_net_output_rrs;     /* mLossUseNetworkOutputRRS                                   */
+    int32_t stop_training;          /* mStopTraining                                              */
+    int32_t request_exit;           /* mAutoTrainRequestExit                                      */
+    double seconds_per_frame;       /* measured over 100 frames after training (0 before)         */
+} nrrs_train_schedule_state;
+typedef struct nrrs_train_schedule nrrs_train_schedule;
+int nrrs_train_schedule_create(const double durations[4], nrrs_train_schedule** out);
+void nrrs_train_schedule_destroy(nrrs_train_schedule* s);
+/* elapsed: seconds since the schedule started (the reference's clock() difference); now_seconds:
+ * a wall clock for the 100-frame timing. */
+int nrrs_train_schedule_tick(nrrs_train_schedule* s, double elapsed, double now_seconds,
+                             nrrs_train_schedule_state* out);
 
 /* ---- synthetic inputs (host, deterministic): mt19937_64 + explicit transforms. Buffers are
  *      HOST arrays sized as in nrrs_vertex_soa; any may be NULL to skip. target [n][3]. ---- */

@@ -8,6 +8,7 @@
 //   nrrs_update_weighted_L         src/render/nrrs/train.cu:344-363
 //   nrrs_calculate_error           src/render/nrrs/train.cu:365-430
 //   the error sum                  src/render/nrrs/integrator.cpp:2466-2471
+//   nrrs_UBS_calc_error and its sum  src/render/nrrs/train.cu:594-608, integrator.cpp:2875-2886
 //
 // A patch is a scale x scale block of frame pixels (offsetFrame2Scaled, myFilm.h:6-15). The
 // reference adds a patch's pixels with FP32 atomics in scheduling order; here one thread per
@@ -93,37 +94,14 @@ __global__ void __launch_bounds__(256) k_update(PatchGeom g, const float* __rest
 
 constexpr uint32_t kSumNaN = 0x80000000u;  // `done` bit: some error was not summable
 
-__global__ void __launch_bounds__(256) k_error(PatchGeom g, const float* __restrict__ ref,
-                                               uint32_t ch, const float* __restrict__ wl,
-                                               const float* __restrict__ spp, int clamp,
-                                               int mult, float* err_out, nrrs_error_sum* sum) {
+// Adds each thread's limbs l (or its bad mark) into sum, one atomic per limb and CTA; the last
+// CTA rounds the total once and leaves the accumulators at zero. Every thread of the CTA calls.
+__device__ void add_to_sum(const long long l[3], bool bad, nrrs_error_sum* sum) {
     __shared__ long long s_part[3][8];
-    __shared__ unsigned s_bad, s_last;
-    const uint32_t ps = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t np = g.pw * g.ph, npix = g.w * g.h;
+    __shared__ unsigned s_bad;
     if (threadIdx.x == 0) s_bad = 0;
     __syncthreads();
-    long long l[3] = {0, 0, 0};
-    if (ps < np) {
-        float q[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const float r = ref[(size_t)ps * ch + k];
-            const float d = __fsub_rn(wl[3 * (size_t)ps + k], r);
-            q[k] = __fdiv_rn(__fmul_rn(d, d), __fadd_rn(__fmul_rn(r, r), 0.01f));
-        }
-        float e = __fdiv_rn(__fadd_rn(__fadd_rn(q[0], q[1]), q[2]), 3.0f);
-        if (clamp) e = fminf(e, 100.0f);   // fminf: a NaN error becomes 100, as min() does there
-        err_out[ps] = e;
-        if (mult) e = __fmul_rn(e, __fsqrt_rn(spp[ps]));
-        err_out[npix + ps] = e;
-        if (sum) {
-            if (fixed_ok(e)) fixed_limbs(e, l);
-            else s_bad = 1;
-        }
-    }
-    if (!sum) return;
-    // block sums of the limbs, then one atomic per limb and CTA
+    if (bad) s_bad = 1;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -133,28 +111,77 @@ __global__ void __launch_bounds__(256) k_error(PatchGeom g, const float* __restr
         if (lane == 0) s_part[k][wid] = v;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int k = 0; k < 3; ++k) {
-            unsigned long long t = 0;
-            for (int w = 0; w < (int)(blockDim.x / 32); ++w) t += (unsigned long long)s_part[k][w];
-            if (t) atomicAdd(reinterpret_cast<unsigned long long*>(&sum->acc[k]), t);
-        }
-        if (s_bad) atomicOr(&sum->done, kSumNaN);
-        __threadfence();
-        const unsigned old = atomicAdd(&sum->done, 1u);
-        s_last = ((old & ~kSumNaN) == gridDim.x - 1) ? 1u : 0u;
-        if (s_last) {
-            __threadfence();
-            const long long a0 = (long long)atomicAdd(reinterpret_cast<unsigned long long*>(&sum->acc[0]), 0ull);
-            const long long a1 = (long long)atomicAdd(reinterpret_cast<unsigned long long*>(&sum->acc[1]), 0ull);
-            const long long a2 = (long long)atomicAdd(reinterpret_cast<unsigned long long*>(&sum->acc[2]), 0ull);
-            const bool bad = (old & kSumNaN) || s_bad;
-            sum->value = bad ? __int_as_float(0x7fc00000) : fixed_to_float(a0, a1, a2);
-            sum->acc[0] = sum->acc[1] = sum->acc[2] = 0;
-            sum->done = 0;
-            __threadfence();
-        }
+    if (threadIdx.x != 0) return;
+    for (int k = 0; k < 3; ++k) {
+        unsigned long long t = 0;
+        for (int w = 0; w < (int)(blockDim.x / 32); ++w) t += (unsigned long long)s_part[k][w];
+        if (t) atomicAdd(reinterpret_cast<unsigned long long*>(&sum->acc[k]), t);
     }
+    if (s_bad) atomicOr(&sum->done, kSumNaN);
+    __threadfence();
+    const unsigned old = atomicAdd(&sum->done, 1u);
+    if ((old & ~kSumNaN) != gridDim.x - 1) return;
+    __threadfence();
+    long long a[3];
+    for (int k = 0; k < 3; ++k)
+        a[k] = (long long)atomicAdd(reinterpret_cast<unsigned long long*>(&sum->acc[k]), 0ull);
+    const bool nan = (old & kSumNaN) || s_bad;
+    sum->value = nan ? __int_as_float(0x7fc00000) : fixed_to_float(a[0], a[1], a[2]);
+    sum->acc[0] = sum->acc[1] = sum->acc[2] = 0;
+    sum->done = 0;
+    __threadfence();
+}
+
+// mean_c (l_c - r_c)^2 / (r_c^2 + 0.01), FP32 written out
+__device__ __forceinline__ float rel_error(const float* l, const float* r) {
+    float q[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float d = __fsub_rn(l[k], r[k]);
+        q[k] = __fdiv_rn(__fmul_rn(d, d), __fadd_rn(__fmul_rn(r[k], r[k]), 0.01f));
+    }
+    return __fdiv_rn(__fadd_rn(__fadd_rn(q[0], q[1]), q[2]), 3.0f);
+}
+
+__global__ void __launch_bounds__(256) k_error(PatchGeom g, const float* __restrict__ ref,
+                                               uint32_t ch, const float* __restrict__ wl,
+                                               const float* __restrict__ spp, int clamp,
+                                               int mult, float* err_out, nrrs_error_sum* sum) {
+    const uint32_t ps = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t np = g.pw * g.ph, npix = g.w * g.h;
+    long long l[3] = {0, 0, 0};
+    bool bad = false;
+    if (ps < np) {
+        float e = rel_error(wl + 3 * (size_t)ps, ref + (size_t)ps * ch);
+        if (clamp) e = fminf(e, 100.0f);   // fminf: a NaN error becomes 100, as min() does there
+        err_out[ps] = e;
+        if (mult) e = __fmul_rn(e, __fsqrt_rn(spp[ps]));
+        err_out[npix + ps] = e;
+        if (fixed_ok(e)) fixed_limbs(e, l);
+        else bad = true;
+    }
+    if (sum) add_to_sum(l, bad, sum);
+}
+
+// nrrs_UBS_calc_error (train.cu:594-608): per frame pixel, the film read at its patch
+__global__ void __launch_bounds__(256) k_ubs_error(PatchGeom g, const float* __restrict__ pl,
+                                                   uint32_t spp, const float* __restrict__ ref,
+                                                   uint32_t ch, float* err_out,
+                                                   nrrs_error_sum* sum) {
+    const uint32_t px = blockIdx.x * blockDim.x + threadIdx.x;
+    long long l[3] = {0, 0, 0};
+    bool bad = false;
+    if (px < g.w * g.h) {
+        const float fspp = (float)spp;
+        float L[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) L[k] = __fdiv_rn(pl[3 * (size_t)px + k], fspp);
+        const float e = rel_error(L, ref + (size_t)patch_of(g, px) * ch);
+        err_out[px] = e;
+        if (fixed_ok(e)) fixed_limbs(e, l);
+        else bad = true;
+    }
+    if (sum) add_to_sum(l, bad, sum);
 }
 
 int check_geom(const nrrs_pixel_error_params* p) {
@@ -227,5 +254,19 @@ extern "C" int nrrs_calculate_error(const nrrs_pixel_error_params* p, const floa
     k_error<<<(np + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
         g, ref, (uint32_t)ref_channels, weighted_l, samples_per_patch, p->clamp ? 1 : 0,
         p->multiply_samples ? 1 : 0, error, sum);
+    return done(cudaGetLastError());
+}
+
+extern "C" int nrrs_ubs_error(const nrrs_pixel_error_params* p, const float* pixel_l, uint32_t spp,
+                              const float* ref, int32_t ref_channels, float* error,
+                              nrrs_error_sum* sum, void* stream) {
+    int rc = check_geom(p);
+    if (rc != NRRS_OK) return rc;
+    if (!pixel_l || !ref || (ref_channels != 3 && ref_channels != 4) || !error)
+        return NRRS_ERR_INVALID_ARG;
+    const PatchGeom g = geom_of(*p);
+    const uint32_t n = g.w * g.h;
+    k_ubs_error<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+        g, pixel_l, spp, ref, (uint32_t)ref_channels, error, sum);
     return done(cudaGetLastError());
 }

@@ -215,6 +215,22 @@ _SIGS = {
     "nrrs_calculate_error": (C.c_int, [C.POINTER(PixelErrorParams), C.c_void_p, C.c_int32,
                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                        C.c_void_p]),
+    "nrrs_ubs_error": (C.c_int, [C.POINTER(PixelErrorParams), C.c_void_p, C.c_uint32, C.c_void_p,
+                                 C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "nrrs_ubs_create": (C.c_int, [C.c_int32, C.c_double, C.POINTER(C.c_void_p)]),
+    "nrrs_ubs_destroy": (None, [C.c_void_p]),
+    "nrrs_ubs_begin_search": (C.c_int, [C.c_void_p]),
+    "nrrs_ubs_next_state": (C.c_int, [C.c_void_p]),
+    "nrrs_ubs_analyse_frame": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_uint32]),
+    "nrrs_ubs_get_strategy": (C.c_int, [C.c_void_p, C.c_int32]),
+    "nrrs_ubs_need_infer": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_float, C.c_float,
+                                      C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
+    "nrrs_ubs_best": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_float)]),
+    "nrrs_ubs_set_best": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "nrrs_ubs_searching": (C.c_int, [C.c_void_p]),
+    "nrrs_train_schedule_create": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_void_p)]),
+    "nrrs_train_schedule_destroy": (None, [C.c_void_p]),
+    "nrrs_train_schedule_tick": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_void_p]),
     "nrrs_last_infer_grid": (C.c_int32, [C.c_void_p]),
     "nrrs_kernel_name": (C.c_char_p, [C.c_int32]),
     "nrrs_profile_enable": (C.c_int, [C.c_void_p, C.c_int32]),
@@ -497,6 +513,99 @@ def calculate_error(params: PixelErrorParams, ref, ref_channels: int, weighted_l
                                       _ptr(samples_per_patch), _ptr(error), _ptr(error_sum),
                                       stream),
            "nrrs_calculate_error")
+
+
+def ubs_error(params: PixelErrorParams, pixel_l, spp: int, ref, ref_channels: int, error,
+              error_sum=None, stream=0):
+    """nrrs_ubs_error (nrrs_UBS_calc_error, train.cu:594-608) and its exact sum."""
+    _check(lib().nrrs_ubs_error(C.byref(params), _ptr(pixel_l), spp, _ptr(ref), ref_channels,
+                                _ptr(error), _ptr(error_sum), stream), "nrrs_ubs_error")
+
+
+UBS_FIXED_RR, UBS_ADRRS, UBS_NRRS = 0, 1, 2
+
+
+class UBS:
+    """The per-depth strategy search of the reference's NRRSPathTracer (integrator.h:324-439,
+    integrator.cpp:2787-2891) over nrrs_ubs_*."""
+
+    def __init__(self, max_depth: int = 6, error_eval_seconds: float = 0.17e-3):
+        self._h = None
+        h = C.c_void_p()
+        _check(lib().nrrs_ubs_create(max_depth, error_eval_seconds, C.byref(h)), "nrrs_ubs_create")
+        self._h = h
+        self.max_depth = max_depth
+
+    def close(self):
+        if self._h:
+            lib().nrrs_ubs_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def UBSResetAndBeginSearch(self):
+        _check(lib().nrrs_ubs_begin_search(self._h), "nrrs_ubs_begin_search")
+
+    def UBSNextState(self) -> bool:
+        return lib().nrrs_ubs_next_state(self._h) == 1
+
+    def UBSAnalyseFrame(self, now_seconds: float, frame_error_sum: float, resolution: int):
+        _check(lib().nrrs_ubs_analyse_frame(self._h, now_seconds, frame_error_sum, resolution),
+               "nrrs_ubs_analyse_frame")
+
+    def strategy(self, depth: int) -> int:
+        return lib().nrrs_ubs_get_strategy(self._h, depth)
+
+    def isInferMode(self, depth: int, enable_rrs=True, clamp_min=0.05, clamp_max=8.0,
+                    max_rrs_depth=6, use_net_output_rrs=True) -> tuple[bool, int]:
+        """(infer at this depth, factor source) -- isInferMode and the factor choice."""
+        src = C.c_int32()
+        r = lib().nrrs_ubs_need_infer(self._h, depth, int(enable_rrs), clamp_min, clamp_max,
+                                      max_rrs_depth, int(use_net_output_rrs), C.byref(src))
+        return r == 1, src.value
+
+    def best(self) -> tuple[list, float]:
+        arr = (C.c_int32 * self.max_depth)()
+        eff = C.c_float()
+        _check(lib().nrrs_ubs_best(self._h, arr, C.byref(eff)), "nrrs_ubs_best")
+        return list(arr), eff.value
+
+    def set_best(self, digits: str):
+        _check(lib().nrrs_ubs_set_best(self._h, digits.encode()), "nrrs_ubs_set_best")
+
+    @property
+    def searching(self) -> bool:
+        return lib().nrrs_ubs_searching(self._h) == 1
+
+
+class TrainScheduleState(C.Structure):
+    _fields_ = [("state", C.c_int32), ("step", C.c_int32), ("enable_rrs", C.c_int32),
+                ("use_net_output_rrs", C.c_int32), ("stop_training", C.c_int32),
+                ("request_exit", C.c_int32), ("seconds_per_frame", C.c_double)]
+
+
+class TrainSchedule:
+    """autoTrainControl (integrator.cpp:2659-2736) over nrrs_train_schedule_*."""
+
+    def __init__(self, durations):
+        self._h = None
+        h = C.c_void_p()
+        d = (C.c_double * 4)(*durations)
+        _check(lib().nrrs_train_schedule_create(d, C.byref(h)), "nrrs_train_schedule_create")
+        self._h = h
+
+    def close(self):
+        if self._h:
+            lib().nrrs_train_schedule_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def tick(self, elapsed: float, now_seconds: float) -> TrainScheduleState:
+        st = TrainScheduleState()
+        _check(lib().nrrs_train_schedule_tick(self._h, elapsed, now_seconds, C.byref(st)),
+               "nrrs_train_schedule_tick")
+        return st
 
 
 def calculate_sample_weight(pixel, pixel_samples, n_pixels: int, size_dev, max_n: int, weight,

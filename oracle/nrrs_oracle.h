@@ -108,6 +108,8 @@ void oracle_update_weighted_l(const nrrs_pixel_error_params* p, const float* cur
                               const uint32_t* acc, float* wl);
 float oracle_calculate_error(const nrrs_pixel_error_params* p, const float* ref, int ch,
                              const float* wl, const float* spp, float* err_out);
+float oracle_ubs_error(const nrrs_pixel_error_params* p, const float* pl, uint32_t spp,
+                       const float* ref, int ch, float* err_out);
 
 /* threads used by the OpenMP loops (0 = runtime default) */
 void oracle_set_threads(int n);

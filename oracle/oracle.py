@@ -94,6 +94,8 @@ def lib():
         L.oracle_update_weighted_l.argtypes = [pe, vp, vp, vp]
         L.oracle_calculate_error.restype = C.c_float
         L.oracle_calculate_error.argtypes = [pe, vp, C.c_int, vp, vp, vp]
+        L.oracle_ubs_error.restype = C.c_float
+        L.oracle_ubs_error.argtypes = [pe, vp, C.c_uint32, vp, C.c_int, vp]
         L.oracle_set_threads.argtypes = [C.c_int]
         L.oracle_get_threads.restype = C.c_int
         _lib = L
@@ -389,3 +391,10 @@ def batch_arrays(capacity: int) -> dict:
     return {k: np.zeros((cap, 3) if k in v3 else cap,
                         np.uint32 if k in ("depth", "pixel") else np.float32)
             for k in nb.TRAIN_BATCH_FIELDS}
+
+
+def ubs_error(params, pixel_l, spp: int, ref, err) -> float:
+    pixel_l = np.ascontiguousarray(pixel_l, np.float32)
+    ref = np.ascontiguousarray(ref, np.float32)
+    return float(lib().oracle_ubs_error(C.byref(params), pixel_l.ctypes.data, spp,
+                                        ref.ctypes.data, ref.shape[1], err.ctypes.data))

@@ -378,3 +378,32 @@ float oracle_calculate_error(const nrrs_pixel_error_params* p, const float* ref,
     }
     return bad ? NAN : oracle_fixed_to_float(acc[0], acc[1], acc[2]);
 }
+
+/* nrrs_UBS_calc_error (train.cu:594-608) and the exact sum (integrator.cpp:2875-2886): the film
+ * read at the pixel's patch, L = pixel_l / spp */
+float oracle_ubs_error(const nrrs_pixel_error_params* p, const float* pl, uint32_t spp,
+                       const float* ref, int ch, float* err_out) {
+    const geom_t g = geom_of(p);
+    int64_t acc[3] = {0, 0, 0};
+    int bad = 0;
+    const float fspp = (float)spp;
+    for (uint32_t px = 0; px < g.w * g.h; ++px) {
+        const float* r = ref + (uint64_t)patch_of(&g, px) * ch;
+        float q[3];
+        for (int k = 0; k < 3; ++k) {
+            const float l = pl[3 * (uint64_t)px + k] / fspp;
+            const float d = l - r[k];
+            q[k] = (d * d) / (r[k] * r[k] + 0.01f);
+        }
+        const float e = ((q[0] + q[1]) + q[2]) / 3.0f;
+        err_out[px] = e;
+        if (fabsf(e) < FIXED_MAX) {
+            int64_t l[3];
+            oracle_fixed_limbs(e, l);
+            for (int k = 0; k < 3; ++k) acc[k] = (int64_t)((uint64_t)acc[k] + (uint64_t)l[k]);
+        } else {
+            bad = 1;
+        }
+    }
+    return bad ? NAN : oracle_fixed_to_float(acc[0], acc[1], acc[2]);
+}

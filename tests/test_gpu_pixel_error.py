@@ -170,3 +170,24 @@ def test_gpu_batch_gathers_the_pixel_error(scale):
     for k in outs:
         assert host(outs[k])[:m].tobytes() == o["batch"][k].tobytes(), k
     assert g.pn.status(stream())[2] == 0
+
+
+@pytest.mark.parametrize("w,h,scale", [(1920, 1080, 1), (640, 360, 2)])
+def test_gpu_ubs_error_matches_oracle(w, h, scale):
+    """nrrs_ubs_error (nrrs_UBS_calc_error) and its exact sum, two calls in a row."""
+    torch = torch_cuda()
+    p = nb.PixelErrorParams(w, h, scale, 0.5, 1, 0)
+    npix, npatch = w * h, (w // scale) * (h // scale)
+    rng = np.random.default_rng(w)
+    esum = torch.zeros(C.sizeof(nb.ErrorSum), dtype=torch.uint8, device="cuda")
+    err = torch.full((npix,), -5.0, device="cuda")
+    for spp in (1, 4):
+        pixel_l = (rng.lognormal(-1, 1.5, size=(npix, 3)) * spp).astype(np.float32)
+        ref = rng.lognormal(-1, 1.2, size=(npatch, 4)).astype(np.float32)
+        nb.ubs_error(p, dev(pixel_l), spp, dev(ref), 4, err, esum, stream())
+        want = np.zeros(npix, np.float32)
+        total = O.ubs_error(p, pixel_l, spp, ref, want)
+        assert host(err).tobytes() == want.tobytes()
+        raw = host(esum)
+        assert not raw[:28].any()
+        assert raw[28:32].view(np.float32)[0] == np.float32(total)
