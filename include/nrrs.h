@@ -607,6 +607,122 @@ void nrrs_train_schedule_destroy(nrrs_train_schedule* s);
 int nrrs_train_schedule_tick(nrrs_train_schedule* s, double elapsed, double now_seconds,
                              nrrs_train_schedule_state* out);
 
+/* ==== the wavefront steps either side of the path: trace and scatter ============================
+ * A CUDA ray tracer around the NRRS step, in place of the reference's OptiX programs and its
+ * scatter step:
+ *   trace (closest hit, shadow any-hit)      src/render/nrrs/device.cu:48-161 (OptiX programs)
+ *   handleHit / handleMiss                   src/render/nrrs/integrator.cpp:686-735
+ *   handleIntersections, generateScatteredRays   src/render/nrrs/integrator.cpp:737-887
+ *   generateCameraRays                       src/render/nrrs/integrator.cpp:889-935
+ * Scenes are triangle meshes with diffuse (Lambertian) materials; emissive triangles are area
+ * lights, sampled uniformly by light then by area, and misses see a constant environment. Next-
+ * event estimation and BSDF sampling are combined with the power heuristic (the reference's
+ * evalMIS, KiRaRay). The BVH is built on the host when the scene is created; traversal runs on
+ * the GPU. Random numbers are a counter-based hash of (seed, depth, ray slot, dimension), so a
+ * frame is deterministic. Radiance goes to an exact fixed-point film: [pixels][3 channels][3
+ * limbs] int64, as the path nodes' radiance (lowest bit 2^-64), resolved once per frame. */
+typedef struct nrrs_scene nrrs_scene;
+/* vertices [n_vertices][3], triangles [n_triangles][3] vertex indices, tri_material
+ * [n_triangles], materials [n_materials][6] = albedo rgb, emission rgb, environment [3] (may be
+ * NULL = black). HOST arrays; the scene's device copy and BVH belong to the handle. */
+int nrrs_scene_create(const float* vertices, uint32_t n_vertices, const uint32_t* triangles,
+                      uint32_t n_triangles, const uint32_t* tri_material, const float* materials,
+                      uint32_t n_materials, const float* environment, nrrs_scene** out);
+void nrrs_scene_destroy(nrrs_scene* s);
+/* BVH nodes, emissive triangles and the BVH depth */
+int nrrs_scene_info(const nrrs_scene* s, uint32_t* n_nodes, uint32_t* n_lights,
+                    uint32_t* max_depth);
+
+/* A queue of rays, [capacity] device arrays. pdf: the BSDF pdf (solid angle) the ray was sampled
+ * with, 0 for camera rays (no MIS weight on what they hit); thp 0 marks an unused slot. */
+typedef struct {
+    float* origin;          /* [cap][3]  */
+    float* dir;             /* [cap][3] unit */
+    float* thp;             /* [cap][3]  */
+    float* pdf;             /* [cap]     */
+    uint32_t* pixel;        /* [cap]     */
+    int32_t* node;          /* [cap] path node of the vertex the ray leaves (-1 = none) */
+} nrrs_ray_soa;
+
+/* Closest hits: prim = triangle index of the scene's input order, ~0u for a miss. */
+typedef struct {
+    uint32_t* prim;
+    float* t;
+    float* u;               /* barycentrics of the hit */
+    float* v;
+} nrrs_hit_soa;
+
+/* Shadow rays of next-event estimation: contrib is the radiance the pixel gains if the light is
+ * visible (thp x f x Le x cos / pdf x MIS weight); tmax the distance to the light sample. */
+typedef struct {
+    float* origin;          /* [cap][3]  */
+    float* dir;             /* [cap][3]  */
+    float* tmax;            /* [cap]     */
+    float* contrib;         /* [cap][3]; 0 = no shadow ray in this slot */
+    uint32_t* pixel;        /* [cap]     */
+    int32_t* node;          /* [cap]     */
+} nrrs_shadow_soa;
+
+/* The path vertices of one depth, compacted in ray order: the fields of nrrs_vertex_soa (pos, wi
+ * = -ray direction, normal facing the ray, albedo, roughness 1, thp, depth) plus the pixel, the
+ * path node and the pdf of the ray that found the vertex. [cap] device arrays. */
+typedef struct {
+    float* pos;
+    float* wi;
+    float* normal;
+    float* albedo;
+    float* roughness;
+    float* thp;
+    uint32_t* depth;
+    uint32_t* pixel;
+    int32_t* node;
+} nrrs_path_vertices;
+
+typedef struct {
+    float pos[3], forward[3], up[3];
+    float tan_half_fov_y;   /* tan of half the vertical field of view */
+    uint32_t width, height;
+} nrrs_camera;
+
+/* generateCameraRays: one ray per pixel (width x height), jittered inside the pixel by the hash
+ * of (seed, sample, pixel); thp 1, pdf 0, node -1. */
+int nrrs_camera_rays(const nrrs_camera* c, uint32_t sample, uint32_t seed,
+                     const nrrs_ray_soa* rays, void* stream);
+
+/* Closest hits of the first *n_dev rays (max_n bounds the grid). Ties in t go to the lower
+ * triangle index, so the result does not depend on the BVH. */
+int nrrs_trace(const nrrs_scene* s, const nrrs_ray_soa* rays, const uint32_t* n_dev,
+               uint32_t max_n, const nrrs_hit_soa* hits, void* stream);
+
+/* handleHit / handleMiss and the vertex queue: for each of the first *n_dev rays, an emissive hit
+ * adds Le x thp (MIS-weighted against light sampling when pdf > 0) and a miss adds environment x
+ * thp to film[pixel] and contrib[ray] ([max_n][3], 0 otherwise; the ray's node receives it through
+ * nrrs_record_radiance). Rays that hit a surface become the vertices out[0 .. *n_out_dev) in ray
+ * order. scratch: nrrs_shade_scratch_bytes(max_n) bytes of device memory. */
+uint64_t nrrs_shade_scratch_bytes(uint32_t max_n);
+int nrrs_shade(const nrrs_scene* s, const nrrs_ray_soa* rays, const nrrs_hit_soa* hits,
+               const uint32_t* n_dev, uint32_t max_n, uint32_t depth, int64_t* film,
+               float* contrib, const nrrs_path_vertices* out, uint32_t* n_out_dev,
+               void* scratch, void* stream);
+
+/* handleIntersections (the RRS branch) + generateScatteredRays for the first *queue_size_dev
+ * entries of the emitted queue (nrrs_step's next_queue, each vertex once per split): the vertex's
+ * thp is divided by its normalised factor rrs_norm[vertex] (integrator.cpp:787-791), then one
+ * shadow ray (next-event estimation) and one BSDF ray go to slot j of shadow and rays. */
+int nrrs_scatter(const nrrs_scene* s, const nrrs_path_vertices* v, const float* rrs_norm,
+                 const uint32_t* queue, const uint32_t* queue_size_dev, uint32_t max_queue,
+                 uint32_t depth, uint32_t seed, const nrrs_ray_soa* rays,
+                 const nrrs_shadow_soa* shadow, void* stream);
+
+/* The shadow rays of the first *n_dev slots: a visible light adds the slot's contrib to
+ * film[pixel] and leaves it in contrib_out ([max_n][3]); an occluded one leaves 0. */
+int nrrs_trace_shadow(const nrrs_scene* s, const nrrs_shadow_soa* shadow, const uint32_t* n_dev,
+                      uint32_t max_n, int64_t* film, float* contrib_out, void* stream);
+
+/* film [n_pixels][9] limbs -> image [n_pixels][3] = radiance x scale, rounded once */
+int nrrs_film_resolve(const int64_t* film, uint32_t n_pixels, float scale, float* image,
+                      void* stream);
+
 /* ---- synthetic inputs (host, deterministic): mt19937_64 + explicit transforms. Buffers are
  *      HOST arrays sized as in nrrs_vertex_soa; any may be NULL to skip. target [n][3]. ---- */
 void nrrs_synth_vertices(uint64_t seed, uint64_t first, uint64_t n, float* pos, float* wi,

@@ -1,0 +1,684 @@
+// k_render.cu -- the wavefront steps either side of the NRRS step: camera rays, BVH traversal
+// (closest hit and shadow any-hit), the hit/miss shading that forms the next vertex queue, and
+// the scatter step that consumes the emitted queue (thp / rrs, next-event estimation, BSDF
+// sampling). Kernels, the host BVH build and the C-ABI (include/nrrs.h).
+//
+// Replaces, in banbao990/NRRS-Code:
+//   OptiX closest-hit / any-hit programs        src/render/nrrs/device.cu:48-161
+//   handleEmissiveHit / handleMiss              src/render/nrrs/integrator.cpp:688-735
+//   handleIntersections, generateScatteredRays  src/render/nrrs/integrator.cpp:737-887
+//   generateCameraRays                          src/render/nrrs/integrator.cpp:889-935
+//
+// Everything a frame computes is reproducible: random numbers are a counter-based hash of
+// (seed, depth, slot, dimension); every FP32 operation is written out without contraction; ties
+// between equally close triangles go to the lower triangle index; the film and the contributions
+// are exact fixed-point sums. A C restatement of the same steps (brute-force intersection instead
+// of the BVH) checks the kernels bit for bit.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <vector>
+
+#include "fixed_point.cuh"
+#include "nrrs.h"
+
+struct nrrs_scene {
+    float* tris = nullptr;        // [nt][9] v0, e1, e2 in BVH leaf order
+    uint32_t* tri_id = nullptr;   // [nt] input index of each leaf-order triangle
+    uint32_t* tri_mat = nullptr;  // [nt] material, input order
+    float* tri_in = nullptr;      // [nt][9] v0, e1, e2 in input order
+    float* nodes = nullptr;       // [nn][8] bmin, left_or_first (bits), bmax, count | axis << 16
+    float* mats = nullptr;        // [nm][6]
+    uint32_t* lights = nullptr;   // [nl] emissive triangles (input index)
+    float* light_area = nullptr;  // [nl]
+    float env[3] = {0.f, 0.f, 0.f};
+    uint32_t nt = 0, nn = 0, nl = 0, nm = 0, max_depth = 0;
+};
+
+namespace nrrs {
+namespace {
+
+constexpr float kInvPi = 0.318309886183790671f;
+constexpr float kOffset = 1e-4f;        // ray origins leave the surface along the normal
+constexpr int kStack = 64;
+constexpr int kLeafMax = 4;
+constexpr uint32_t kMiss = 0xffffffffu;
+
+// ---- counter-based random numbers (shared with the C restatement) ----
+// lowbias32 (C. Wellons), a published 32-bit integer hash
+__host__ __device__ __forceinline__ uint32_t hash32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+__device__ __forceinline__ float rnd(uint32_t seed, uint32_t depth, uint32_t slot, uint32_t dim) {
+    const uint32_t h = hash32(hash32(hash32(seed) ^ (depth * 0x9e3779b9u)) ^ (slot * 32u + dim));
+    return (float)(h >> 8) * 0x1p-24f;
+}
+
+// ---- FP32 vector arithmetic, every operation rounded on its own ----
+struct V3 { float x, y, z; };
+__device__ __forceinline__ V3 v3(const float* p) { return {p[0], p[1], p[2]}; }
+__device__ __forceinline__ V3 add(V3 a, V3 b) { return {__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z)}; }
+__device__ __forceinline__ V3 sub(V3 a, V3 b) { return {__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)}; }
+__device__ __forceinline__ V3 mul(V3 a, float s) { return {__fmul_rn(a.x, s), __fmul_rn(a.y, s), __fmul_rn(a.z, s)}; }
+__device__ __forceinline__ V3 vmul(V3 a, V3 b) { return {__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y), __fmul_rn(a.z, b.z)}; }
+__device__ __forceinline__ V3 divs(V3 a, float s) { return {__fdiv_rn(a.x, s), __fdiv_rn(a.y, s), __fdiv_rn(a.z, s)}; }
+__device__ __forceinline__ float dot(V3 a, V3 b) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+__device__ __forceinline__ V3 cross(V3 a, V3 b) {
+    return {__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)),
+            __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+            __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x))};
+}
+__device__ __forceinline__ V3 normalize(V3 a) { return divs(a, __fsqrt_rn(dot(a, a))); }
+__device__ __forceinline__ void put(float* p, V3 a) { p[0] = a.x; p[1] = a.y; p[2] = a.z; }
+__device__ __forceinline__ bool nonzero(V3 a) { return a.x != 0.f || a.y != 0.f || a.z != 0.f; }
+
+// Moller-Trumbore, two-sided; t in (0, tmax)
+__device__ __forceinline__ bool intersect(const float* tri, V3 o, V3 d, float tmax, float* t,
+                                          float* u, float* v) {
+    const V3 v0 = v3(tri), e1 = v3(tri + 3), e2 = v3(tri + 6);
+    const V3 pv = cross(d, e2);
+    const float det = dot(e1, pv);
+    if (fabsf(det) < 1e-12f) return false;
+    const float inv = __fdiv_rn(1.0f, det);
+    const V3 tv = sub(o, v0);
+    const float uu = __fmul_rn(dot(tv, pv), inv);
+    if (uu < 0.f || uu > 1.f) return false;
+    const V3 qv = cross(tv, e1);
+    const float vv = __fmul_rn(dot(d, qv), inv);
+    if (vv < 0.f || __fadd_rn(uu, vv) > 1.f) return false;
+    const float tt = __fmul_rn(dot(e2, qv), inv);
+    if (!(tt > 0.f && tt < tmax)) return false;
+    *t = tt; *u = uu; *v = vv;
+    return true;
+}
+
+// slab test; the interval [t0, t1] of the box along the ray, clipped to [0, tmax]
+__device__ __forceinline__ bool box_hit(const float* nd, V3 o, V3 inv, float tmax, float* tnear) {
+    float t0 = 0.f, t1 = tmax;
+    const float oo[3] = {o.x, o.y, o.z}, ii[3] = {inv.x, inv.y, inv.z};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float a = (nd[k] - oo[k]) * ii[k], b = (nd[4 + k] - oo[k]) * ii[k];
+        if (a > b) { const float s = a; a = b; b = s; }
+        t0 = a > t0 ? a : t0;      // NaN (0 x inf) leaves the bound as it was
+        t1 = b < t1 ? b : t1;
+    }
+    *tnear = t0;
+    return t0 <= t1;
+}
+
+struct Hit { uint32_t prim; float t, u, v; };
+
+// closest hit; ties in t go to the lower input index. any = true stops at the first hit.
+template <bool ANY>
+__device__ Hit traverse(const nrrs_scene& s, V3 o, V3 d, float tmax) {
+    Hit h{kMiss, tmax, 0.f, 0.f};
+    const V3 inv = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+    int stack[kStack];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        const float* nd = s.nodes + 8 * (size_t)stack[--sp];
+        float tn;
+        if (!box_hit(nd, o, inv, h.prim == kMiss ? tmax : h.t, &tn)) continue;
+        const uint32_t lf = __float_as_uint(nd[3]), ca = __float_as_uint(nd[7]);
+        const uint32_t cnt = ca & 0xffffu;
+        if (cnt) {
+            for (uint32_t i = lf; i < lf + cnt; ++i) {
+                float t, u, v;
+                if (!intersect(s.tris + 9 * (size_t)i, o, d, tmax, &t, &u, &v)) continue;
+                const uint32_t id = s.tri_id[i];
+                if (h.prim == kMiss || t < h.t || (t == h.t && id < h.prim)) h = {id, t, u, v};
+                if (ANY) return h;
+            }
+        } else {
+            // near child first: by the sign of the ray on the node's split axis
+            const uint32_t axis = ca >> 16;
+            const float da = axis == 0 ? d.x : (axis == 1 ? d.y : d.z);
+            const int first = (int)lf, second = (int)lf + 1;
+            if (sp + 2 > kStack) continue;   // depth is bounded at build time; never taken
+            if (da < 0.f) { stack[sp++] = first; stack[sp++] = second; }
+            else { stack[sp++] = second; stack[sp++] = first; }
+        }
+    }
+    return h;
+}
+
+__device__ __forceinline__ void film_add(int64_t* film, uint32_t pixel, V3 c) {
+    const float cc[3] = {c.x, c.y, c.z};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (cc[k] == 0.f || !fixed_ok(cc[k])) continue;
+        long long l[3];
+        fixed_limbs(cc[k], l);
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+            if (l[q]) atomicAdd(reinterpret_cast<unsigned long long*>(film + 9 * (size_t)pixel + 3 * k + q),
+                                (unsigned long long)l[q]);
+    }
+}
+
+__device__ __forceinline__ float power_heuristic(float a, float b) {
+    const float a2 = __fmul_rn(a, a);
+    return __fdiv_rn(a2, __fadd_rn(a2, __fmul_rn(b, b)));
+}
+
+// ---- kernels ----
+__global__ void __launch_bounds__(256) k_camera(nrrs_camera c, uint32_t sample, uint32_t seed,
+                                                nrrs_ray_soa r) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= c.width * c.height) return;
+    const V3 fw = normalize(v3(c.forward));
+    const V3 right = normalize(cross(fw, v3(c.up)));
+    const V3 up = cross(right, fw);
+    const float jx = rnd(seed, 0xffffffffu - sample, p, 0), jy = rnd(seed, 0xffffffffu - sample, p, 1);
+    const float w = (float)c.width, hgt = (float)c.height;
+    const float px = __fsub_rn(__fmul_rn(__fdiv_rn(__fadd_rn((float)(p % c.width), jx), w), 2.0f), 1.0f);
+    const float py = __fsub_rn(1.0f, __fmul_rn(__fdiv_rn(__fadd_rn((float)(p / c.width), jy), hgt), 2.0f));
+    const float sx = __fmul_rn(__fmul_rn(px, c.tan_half_fov_y), __fdiv_rn(w, hgt));
+    const float sy = __fmul_rn(py, c.tan_half_fov_y);
+    const V3 d = normalize(add(add(fw, mul(right, sx)), mul(up, sy)));
+    put(r.origin + 3 * (size_t)p, v3(c.pos));
+    put(r.dir + 3 * (size_t)p, d);
+    put(r.thp + 3 * (size_t)p, {1.f, 1.f, 1.f});
+    r.pdf[p] = 0.f;
+    r.pixel[p] = p;
+    r.node[p] = -1;
+}
+
+__global__ void __launch_bounds__(128) k_trace(const __grid_constant__ nrrs_scene s,
+                                               nrrs_ray_soa r, const uint32_t* n_dev,
+                                               uint32_t max_n, nrrs_hit_soa h) {
+    const uint32_t n = min(*n_dev, max_n);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        Hit x{kMiss, 0.f, 0.f, 0.f};
+        if (nonzero(v3(r.thp + 3 * (size_t)i)))
+            x = traverse<false>(s, v3(r.origin + 3 * (size_t)i), v3(r.dir + 3 * (size_t)i), INFINITY);
+        h.prim[i] = x.prim;
+        h.t[i] = x.t;
+        h.u[i] = x.u;
+        h.v[i] = x.v;
+    }
+}
+
+constexpr int kShadeChunk = 1024;
+
+// hits per chunk of rays; the last CTA turns the counts into offsets and the total
+__global__ void __launch_bounds__(256) k_shade_count(nrrs_ray_soa r, nrrs_hit_soa h,
+                                                     const uint32_t* n_dev, uint32_t max_n,
+                                                     uint32_t* scratch, uint32_t* n_out) {
+    __shared__ unsigned s_part[8], s_last;
+    __shared__ unsigned long long s_w[8];
+    const uint32_t n = min(*n_dev, max_n);
+    const uint32_t chunks = (max_n + kShadeChunk - 1) / kShadeChunk;
+    uint32_t* counts = scratch + 4;
+    uint32_t* offsets = counts + chunks;
+    const uint32_t c = blockIdx.x;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned k = 0;
+    for (uint32_t i = c * kShadeChunk + threadIdx.x; i < min(n, (c + 1) * kShadeChunk); i += 256)
+        k += (h.prim[i] != kMiss && nonzero(v3(r.thp + 3 * (size_t)i))) ? 1u : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) k += __shfl_xor_sync(0xffffffffu, k, o);
+    if (lane == 0) s_part[wid] = k;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned t = 0;
+        for (int w = 0; w < 8; ++w) t += s_part[w];
+        counts[c] = t;
+        __threadfence();
+        s_last = atomicAdd(scratch, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    // the last CTA: exclusive scan of the chunk counts, a strip per thread
+    __threadfence();
+    const uint32_t per = (chunks + 255) / 256;
+    const uint32_t lo = min(chunks, threadIdx.x * per), hi = min(chunks, lo + per);
+    unsigned long long strip = 0;
+    for (uint32_t q = lo; q < hi; ++q) strip += __ldcg(counts + q);
+    unsigned long long incl = strip;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_w[wid] = incl;
+    __syncthreads();
+    unsigned long long run = incl - strip;
+    for (int w = 0; w < wid; ++w) run += s_w[w];
+    for (uint32_t q = lo; q < hi; ++q) {
+        offsets[q] = (uint32_t)run;
+        run += __ldcg(counts + q);
+    }
+    if (threadIdx.x == 255) {
+        *n_out = (uint32_t)run;
+        scratch[0] = 0;
+        __threadfence();
+    }
+}
+
+__global__ void __launch_bounds__(256) k_shade(const __grid_constant__ nrrs_scene s,
+                                               nrrs_ray_soa r, nrrs_hit_soa h,
+                                               const uint32_t* n_dev, uint32_t max_n,
+                                               uint32_t depth, int64_t* film, float* contrib,
+                                               nrrs_path_vertices out, const uint32_t* scratch) {
+    __shared__ unsigned s_warp[8];
+    const uint32_t n = min(*n_dev, max_n);
+    const uint32_t chunks = (max_n + kShadeChunk - 1) / kShadeChunk;
+    const uint32_t c = blockIdx.x;
+    const uint32_t base = scratch[4 + chunks + c];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned lt;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+    unsigned run = 0;   // vertices of the earlier passes of this chunk
+    for (uint32_t j = 0; j < kShadeChunk / 256; ++j) {
+        const uint32_t i = c * kShadeChunk + j * 256 + threadIdx.x;
+        bool vert = false;
+        V3 add_c = {0.f, 0.f, 0.f};
+        V3 pos{}, nrm{}, alb{}, thp{}, d{};
+        if (i < n) {
+            thp = v3(r.thp + 3 * (size_t)i);
+            d = v3(r.dir + 3 * (size_t)i);
+            const uint32_t prim = h.prim[i];
+            if (nonzero(thp)) {
+                if (prim == kMiss) {
+                    add_c = vmul(v3(s.env), thp);
+                } else {
+                    const float* tri = s.tri_in + 9 * (size_t)prim;
+                    const float t = h.t[i];
+                    pos = add(v3(r.origin + 3 * (size_t)i), mul(d, t));
+                    const V3 g = cross(v3(tri + 3), v3(tri + 6));
+                    nrm = normalize(g);
+                    if (dot(nrm, d) > 0.f) nrm = mul(nrm, -1.0f);
+                    const float* m = s.mats + 6 * (size_t)s.tri_mat[prim];
+                    alb = v3(m);
+                    const V3 le = v3(m + 3);
+                    if (nonzero(le)) {
+                        float w = 1.0f;
+                        const float pdf = r.pdf[i];
+                        if (pdf > 0.f && s.nl) {
+                            // the light pdf (solid angle) of sampling this point by NEE
+                            const float area = __fmul_rn(0.5f, __fsqrt_rn(dot(g, g)));
+                            const float cosl = fabsf(dot(nrm, d));
+                            const float pl = __fdiv_rn(__fmul_rn(t, t),
+                                                       __fmul_rn(__fmul_rn(cosl, area), (float)s.nl));
+                            w = power_heuristic(pdf, pl);
+                        }
+                        add_c = mul(vmul(le, thp), w);
+                    }
+                    vert = true;
+                }
+            }
+            if (contrib) put(contrib + 3 * (size_t)i, add_c);
+            if (nonzero(add_c)) film_add(film, r.pixel[i], add_c);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, vert);
+        if (lane == 0) s_warp[wid] = __popc(m);
+        __syncthreads();
+        unsigned before = 0, total = 0;
+        for (int w = 0; w < 8; ++w) {
+            before += w < wid ? s_warp[w] : 0u;
+            total += s_warp[w];
+        }
+        if (vert) {
+            const size_t o = (size_t)base + run + before + __popc(m & lt);
+            put(out.pos + 3 * o, pos);
+            put(out.wi + 3 * o, mul(d, -1.0f));
+            put(out.normal + 3 * o, nrm);
+            put(out.albedo + 3 * o, alb);
+            out.roughness[o] = 1.0f;
+            put(out.thp + 3 * o, thp);
+            out.depth[o] = depth;
+            out.pixel[o] = r.pixel[i];
+            out.node[o] = r.node[i];
+        }
+        run += total;
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(128) k_scatter(const __grid_constant__ nrrs_scene s,
+                                                 nrrs_path_vertices v, const float* rrs_norm,
+                                                 const uint32_t* queue, const uint32_t* q_dev,
+                                                 uint32_t max_q, uint32_t depth, uint32_t seed,
+                                                 nrrs_ray_soa r, nrrs_shadow_soa sh) {
+    const uint32_t n = min(*q_dev, max_q);
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const uint32_t x = queue[j];
+        const float rr = rrs_norm[x];
+        const V3 thp = divs(v3(v.thp + 3 * (size_t)x), rr);   // sitem.mThp /= sitem.mRRS
+        const V3 p = v3(v.pos + 3 * (size_t)x), nn = v3(v.normal + 3 * (size_t)x);
+        const V3 alb = v3(v.albedo + 3 * (size_t)x);
+        const V3 f = mul(alb, kInvPi);
+        const V3 org = add(p, mul(nn, kOffset));
+        const uint32_t px = v.pixel[x];
+        const int node = v.node[x];
+        // next-event estimation: a light by index, a point by area
+        V3 sc = {0.f, 0.f, 0.f}, wl = {0.f, 0.f, 1.f};
+        float dist = 0.f;
+        if (s.nl) {
+            const uint32_t k = min((uint32_t)(rnd(seed, depth, j, 0) * (float)s.nl), s.nl - 1);
+            const uint32_t lt = s.lights[k];
+            const float* tri = s.tri_in + 9 * (size_t)lt;
+            const float su = __fsqrt_rn(rnd(seed, depth, j, 1));
+            const float b1 = __fsub_rn(1.0f, su), b2 = __fmul_rn(rnd(seed, depth, j, 2), su);
+            const V3 q = add(add(v3(tri), mul(v3(tri + 3), b1)), mul(v3(tri + 6), b2));
+            const V3 dv = sub(q, p);
+            const float d2 = dot(dv, dv);
+            dist = __fsqrt_rn(d2);
+            wl = divs(dv, dist);
+            const float cosv = dot(nn, wl);
+            const float cosl = fabsf(dot(normalize(cross(v3(tri + 3), v3(tri + 6))), wl));
+            const V3 le = v3(s.mats + 6 * (size_t)s.tri_mat[lt] + 3);
+            if (cosv > 0.f && cosl > 0.f && nonzero(le) && d2 > 0.f) {
+                const float pl = __fdiv_rn(d2, __fmul_rn(__fmul_rn(cosl, s.light_area[k]), (float)s.nl));
+                const float w = power_heuristic(pl, __fmul_rn(cosv, kInvPi));
+                sc = divs(mul(mul(vmul(vmul(thp, f), le), cosv), w), pl);
+            }
+        }
+        put(sh.origin + 3 * (size_t)j, org);
+        put(sh.dir + 3 * (size_t)j, wl);
+        sh.tmax[j] = __fmul_rn(dist, 0.9999f);
+        put(sh.contrib + 3 * (size_t)j, sc);
+        sh.pixel[j] = px;
+        sh.node[j] = node;
+        // BSDF: cosine-weighted, as normalize(n + a point uniform on the unit sphere), the
+        // sphere point by bounded rejection from the cube
+        V3 sp = {0.f, 0.f, 1.f};
+        for (uint32_t t = 0; t < 8; ++t) {
+            const V3 c = {__fsub_rn(__fmul_rn(rnd(seed, depth, j, 3 + 3 * t), 2.0f), 1.0f),
+                          __fsub_rn(__fmul_rn(rnd(seed, depth, j, 4 + 3 * t), 2.0f), 1.0f),
+                          __fsub_rn(__fmul_rn(rnd(seed, depth, j, 5 + 3 * t), 2.0f), 1.0f)};
+            const float c2 = dot(c, c);
+            if (c2 <= 1.0f && c2 > 1e-6f) {
+                sp = divs(c, __fsqrt_rn(c2));
+                break;
+            }
+        }
+        V3 d = add(nn, sp);
+        const float l2 = dot(d, d);
+        d = l2 > 1e-12f ? divs(d, __fsqrt_rn(l2)) : nn;
+        const float pdf = __fmul_rn(dot(nn, d), kInvPi);
+        const V3 tn = pdf > 0.f ? vmul(thp, alb) : V3{0.f, 0.f, 0.f};
+        put(r.origin + 3 * (size_t)j, org);
+        put(r.dir + 3 * (size_t)j, d);
+        put(r.thp + 3 * (size_t)j, tn);
+        r.pdf[j] = pdf > 0.f ? pdf : 0.f;
+        r.pixel[j] = px;
+        r.node[j] = node;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_shadow(const __grid_constant__ nrrs_scene s,
+                                                nrrs_shadow_soa sh, const uint32_t* n_dev,
+                                                uint32_t max_n, int64_t* film, float* cout) {
+    const uint32_t n = min(*n_dev, max_n);
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        V3 c = v3(sh.contrib + 3 * (size_t)j);
+        if (nonzero(c)) {
+            const Hit x = traverse<true>(s, v3(sh.origin + 3 * (size_t)j), v3(sh.dir + 3 * (size_t)j),
+                                         sh.tmax[j]);
+            if (x.prim != kMiss) c = {0.f, 0.f, 0.f};
+            else film_add(film, sh.pixel[j], c);
+        }
+        if (cout) put(cout + 3 * (size_t)j, c);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_resolve(const int64_t* film, uint32_t n, float scale,
+                                                 float* img) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int64_t* l = film + 9 * (size_t)p + 3 * k;
+        img[3 * (size_t)p + k] = __fmul_rn(fixed_to_float(l[0], l[1], l[2]), scale);
+    }
+}
+
+// ---- host: BVH over triangle centroids, median split on the longest axis ----
+struct Build {
+    const std::vector<float>* tri;   // [nt][9] input order
+    std::vector<uint32_t> order;
+    std::vector<float> nodes;
+    uint32_t max_depth = 0;
+
+    void bounds(uint32_t lo, uint32_t hi, float* bmin, float* bmax) const {
+        for (int k = 0; k < 3; ++k) { bmin[k] = INFINITY; bmax[k] = -INFINITY; }
+        for (uint32_t i = lo; i < hi; ++i) {
+            const float* t = tri->data() + 9 * (size_t)order[i];
+            for (int k = 0; k < 3; ++k) {
+                const float a = t[k], b = t[k] + t[3 + k], c = t[k] + t[6 + k];
+                bmin[k] = std::min({bmin[k], a, b, c});
+                bmax[k] = std::max({bmax[k], a, b, c});
+            }
+        }
+        for (int k = 0; k < 3; ++k) {   // grow by a relative epsilon: the slab test must not
+            const float e = 1e-5f * (std::fabs(bmin[k]) + std::fabs(bmax[k]) + 1e-3f);  // miss
+            bmin[k] -= e;
+            bmax[k] += e;
+        }
+    }
+    float centroid(uint32_t id, int k) const {
+        const float* t = tri->data() + 9 * (size_t)id;
+        return t[k] + (t[3 + k] + t[6 + k]) / 3.0f;
+    }
+    uint32_t alloc() {
+        nodes.resize(nodes.size() + 8);
+        return (uint32_t)(nodes.size() / 8 - 1);
+    }
+    void set_word(uint32_t me, int at, uint32_t w) { std::memcpy(&nodes[8 * (size_t)me + at], &w, 4); }
+    // fills node `me` for triangles [lo, hi); children are allocated as adjacent pairs
+    void build(uint32_t me, uint32_t lo, uint32_t hi, uint32_t depth) {
+        max_depth = std::max(max_depth, depth);
+        float bmin[3], bmax[3];
+        bounds(lo, hi, bmin, bmax);
+        for (int k = 0; k < 3; ++k) {
+            nodes[8 * (size_t)me + k] = bmin[k];
+            nodes[8 * (size_t)me + 4 + k] = bmax[k];
+        }
+        if (hi - lo <= (uint32_t)kLeafMax || depth + 1 >= (uint32_t)(kStack / 2)) {
+            set_word(me, 3, lo);
+            set_word(me, 7, hi - lo);
+            return;
+        }
+        int axis = 0;
+        for (int k = 1; k < 3; ++k)
+            if (bmax[k] - bmin[k] > bmax[axis] - bmin[axis]) axis = k;
+        const uint32_t mid = lo + (hi - lo) / 2;
+        std::nth_element(order.begin() + lo, order.begin() + mid, order.begin() + hi,
+                         [&](uint32_t a, uint32_t b) {
+                             const float ca = centroid(a, axis), cb = centroid(b, axis);
+                             return ca < cb || (ca == cb && a < b);
+                         });
+        const uint32_t left = alloc();
+        alloc();
+        set_word(me, 3, left);
+        set_word(me, 7, (uint32_t)axis << 16);
+        build(left, lo, mid, depth + 1);
+        build(left + 1, mid, hi, depth + 1);
+    }
+};
+
+template <typename T>
+cudaError_t upload(T** dst, const T* src, size_t count) {
+    if (count == 0) { *dst = nullptr; return cudaSuccess; }
+    cudaError_t e = cudaMalloc(dst, sizeof(T) * count);
+    if (e == cudaSuccess) e = cudaMemcpy(*dst, src, sizeof(T) * count, cudaMemcpyHostToDevice);
+    return e;
+}
+
+int grid_of(uint32_t n, int threads) {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint64_t need = ((uint64_t)n + threads - 1) / threads;
+    const uint64_t cap = (uint64_t)sms * 16;
+    return (int)std::max<uint64_t>(1, std::min(need, cap));
+}
+
+int ok(cudaError_t e) { return e == cudaSuccess ? NRRS_OK : NRRS_ERR_CUDA; }
+
+}  // namespace
+}  // namespace nrrs
+
+using namespace nrrs;
+
+extern "C" int nrrs_scene_create(const float* vertices, uint32_t n_vertices,
+                                 const uint32_t* triangles, uint32_t n_triangles,
+                                 const uint32_t* tri_material, const float* materials,
+                                 uint32_t n_materials, const float* environment,
+                                 nrrs_scene** out) {
+    if (!out || !vertices || !triangles || !tri_material || !materials || n_triangles == 0 ||
+        n_materials == 0 || n_triangles > (1u << 30))
+        return NRRS_ERR_INVALID_ARG;
+    if (nrrs_device_available() != 1) return NRRS_ERR_NO_DEVICE;
+    std::vector<float> tri(9 * (size_t)n_triangles);
+    std::vector<uint32_t> lights;
+    std::vector<float> areas;
+    for (uint32_t i = 0; i < n_triangles; ++i) {
+        uint32_t idx[3];
+        for (int k = 0; k < 3; ++k) {
+            idx[k] = triangles[3 * (size_t)i + k];
+            if (idx[k] >= n_vertices) return NRRS_ERR_INVALID_ARG;
+        }
+        if (tri_material[i] >= n_materials) return NRRS_ERR_INVALID_ARG;
+        const float* a = vertices + 3 * (size_t)idx[0];
+        const float* b = vertices + 3 * (size_t)idx[1];
+        const float* c = vertices + 3 * (size_t)idx[2];
+        float* t = &tri[9 * (size_t)i];
+        for (int k = 0; k < 3; ++k) { t[k] = a[k]; t[3 + k] = b[k] - a[k]; t[6 + k] = c[k] - a[k]; }
+        const float* m = materials + 6 * (size_t)tri_material[i];
+        if (m[3] != 0.f || m[4] != 0.f || m[5] != 0.f) {
+            // area = 0.5 |e1 x e2|, each operation rounded on its own
+            const float cx = t[4] * t[8] - t[5] * t[7], cy = t[5] * t[6] - t[3] * t[8],
+                        cz = t[3] * t[7] - t[4] * t[6];
+            const float area = 0.5f * std::sqrt((cx * cx + cy * cy) + cz * cz);
+            if (area > 0.f) { lights.push_back(i); areas.push_back(area); }
+        }
+    }
+    Build b;
+    b.tri = &tri;
+    b.order.resize(n_triangles);
+    std::iota(b.order.begin(), b.order.end(), 0u);
+    b.build(b.alloc(), 0, n_triangles, 0);
+    std::vector<float> tri_leaf(9 * (size_t)n_triangles);
+    for (uint32_t i = 0; i < n_triangles; ++i)
+        std::memcpy(&tri_leaf[9 * (size_t)i], &tri[9 * (size_t)b.order[i]], 36);
+    nrrs_scene* s = new (std::nothrow) nrrs_scene();
+    if (!s) return NRRS_ERR_INVALID_ARG;
+    s->nt = n_triangles;
+    s->nn = (uint32_t)(b.nodes.size() / 8);
+    s->nl = (uint32_t)lights.size();
+    s->nm = n_materials;
+    s->max_depth = b.max_depth;
+    if (environment) for (int k = 0; k < 3; ++k) s->env[k] = environment[k];
+    cudaError_t e = upload(&s->tris, tri_leaf.data(), tri_leaf.size());
+    if (e == cudaSuccess) e = upload(&s->tri_id, b.order.data(), b.order.size());
+    if (e == cudaSuccess) e = upload(&s->tri_mat, tri_material, n_triangles);
+    if (e == cudaSuccess) e = upload(&s->tri_in, tri.data(), tri.size());
+    if (e == cudaSuccess) e = upload(&s->nodes, b.nodes.data(), b.nodes.size());
+    if (e == cudaSuccess) e = upload(&s->mats, materials, 6 * (size_t)n_materials);
+    if (e == cudaSuccess) e = upload(&s->lights, lights.data(), lights.size());
+    if (e == cudaSuccess) e = upload(&s->light_area, areas.data(), areas.size());
+    if (e != cudaSuccess) {
+        nrrs_scene_destroy(s);
+        return NRRS_ERR_CUDA;
+    }
+    *out = s;
+    return NRRS_OK;
+}
+
+extern "C" void nrrs_scene_destroy(nrrs_scene* s) {
+    if (!s) return;
+    cudaFree(s->tris); cudaFree(s->tri_id); cudaFree(s->tri_mat); cudaFree(s->tri_in);
+    cudaFree(s->nodes); cudaFree(s->mats); cudaFree(s->lights); cudaFree(s->light_area);
+    delete s;
+}
+
+extern "C" int nrrs_scene_info(const nrrs_scene* s, uint32_t* n_nodes, uint32_t* n_lights,
+                               uint32_t* max_depth) {
+    if (!s) return NRRS_ERR_INVALID_ARG;
+    if (n_nodes) *n_nodes = s->nn;
+    if (n_lights) *n_lights = s->nl;
+    if (max_depth) *max_depth = s->max_depth;
+    return NRRS_OK;
+}
+
+extern "C" int nrrs_camera_rays(const nrrs_camera* c, uint32_t sample, uint32_t seed,
+                                const nrrs_ray_soa* rays, void* stream) {
+    if (!c || !rays || c->width == 0 || c->height == 0) return NRRS_ERR_INVALID_ARG;
+    const uint32_t n = c->width * c->height;
+    k_camera<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(*c, sample, seed, *rays);
+    return ok(cudaGetLastError());
+}
+
+extern "C" int nrrs_trace(const nrrs_scene* s, const nrrs_ray_soa* rays, const uint32_t* n_dev,
+                          uint32_t max_n, const nrrs_hit_soa* hits, void* stream) {
+    if (!s || !rays || !n_dev || !hits) return NRRS_ERR_INVALID_ARG;
+    if (max_n == 0) return NRRS_OK;
+    k_trace<<<grid_of(max_n, 128), 128, 0, (cudaStream_t)stream>>>(*s, *rays, n_dev, max_n, *hits);
+    return ok(cudaGetLastError());
+}
+
+extern "C" uint64_t nrrs_shade_scratch_bytes(uint32_t max_n) {
+    const uint64_t chunks = ((uint64_t)max_n + kShadeChunk - 1) / kShadeChunk;
+    return 4ull * (4 + 2 * chunks);
+}
+
+extern "C" int nrrs_shade(const nrrs_scene* s, const nrrs_ray_soa* rays, const nrrs_hit_soa* hits,
+                          const uint32_t* n_dev, uint32_t max_n, uint32_t depth, int64_t* film,
+                          float* contrib, const nrrs_path_vertices* out, uint32_t* n_out_dev,
+                          void* scratch, void* stream) {
+    if (!s || !rays || !hits || !n_dev || !film || !out || !n_out_dev || !scratch)
+        return NRRS_ERR_INVALID_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (max_n == 0) return ok(cudaMemsetAsync(n_out_dev, 0, 4, st));
+    const uint32_t chunks = (max_n + kShadeChunk - 1) / kShadeChunk;
+    uint32_t* sc = static_cast<uint32_t*>(scratch);
+    if (cudaMemsetAsync(sc, 0, 4, st) != cudaSuccess) return NRRS_ERR_CUDA;   // the done counter
+    k_shade_count<<<chunks, 256, 0, st>>>(*rays, *hits, n_dev, max_n, sc, n_out_dev);
+    k_shade<<<chunks, 256, 0, st>>>(*s, *rays, *hits, n_dev, max_n, depth, film, contrib, *out, sc);
+    return ok(cudaGetLastError());
+}
+
+extern "C" int nrrs_scatter(const nrrs_scene* s, const nrrs_path_vertices* v, const float* rrs_norm,
+                            const uint32_t* queue, const uint32_t* queue_size_dev,
+                            uint32_t max_queue, uint32_t depth, uint32_t seed,
+                            const nrrs_ray_soa* rays, const nrrs_shadow_soa* shadow,
+                            void* stream) {
+    if (!s || !v || !rrs_norm || !queue || !queue_size_dev || !rays || !shadow)
+        return NRRS_ERR_INVALID_ARG;
+    if (max_queue == 0) return NRRS_OK;
+    k_scatter<<<grid_of(max_queue, 128), 128, 0, (cudaStream_t)stream>>>(
+        *s, *v, rrs_norm, queue, queue_size_dev, max_queue, depth, seed, *rays, *shadow);
+    return ok(cudaGetLastError());
+}
+
+extern "C" int nrrs_trace_shadow(const nrrs_scene* s, const nrrs_shadow_soa* shadow,
+                                 const uint32_t* n_dev, uint32_t max_n, int64_t* film,
+                                 float* contrib_out, void* stream) {
+    if (!s || !shadow || !n_dev || !film) return NRRS_ERR_INVALID_ARG;
+    if (max_n == 0) return NRRS_OK;
+    k_shadow<<<grid_of(max_n, 128), 128, 0, (cudaStream_t)stream>>>(*s, *shadow, n_dev, max_n,
+                                                                     film, contrib_out);
+    return ok(cudaGetLastError());
+}
+
+extern "C" int nrrs_film_resolve(const int64_t* film, uint32_t n_pixels, float scale, float* image,
+                                 void* stream) {
+    if (!film || !image) return NRRS_ERR_INVALID_ARG;
+    if (n_pixels == 0) return NRRS_OK;
+    k_resolve<<<(n_pixels + 255) / 256, 256, 0, (cudaStream_t)stream>>>(film, n_pixels, scale, image);
+    return ok(cudaGetLastError());
+}

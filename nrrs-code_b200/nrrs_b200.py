@@ -110,6 +110,31 @@ class TrainBatch(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in TRAIN_BATCH_FIELDS]
 
 
+class RaySoA(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("origin", "dir", "thp", "pdf", "pixel", "node")]
+
+
+class HitSoA(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("prim", "t", "u", "v")]
+
+
+class ShadowSoA(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("origin", "dir", "tmax", "contrib", "pixel", "node")]
+
+
+PATH_VERTEX_FIELDS = ("pos", "wi", "normal", "albedo", "roughness", "thp", "depth", "pixel",
+                      "node")
+
+
+class PathVertices(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in PATH_VERTEX_FIELDS]
+
+
+class Camera(C.Structure):
+    _fields_ = [("pos", C.c_float * 3), ("forward", C.c_float * 3), ("up", C.c_float * 3),
+                ("tan_half_fov_y", C.c_float), ("width", C.c_uint32), ("height", C.c_uint32)]
+
+
 class NRRSError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{msg} (status {code})")
@@ -231,6 +256,25 @@ _SIGS = {
     "nrrs_train_schedule_create": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_void_p)]),
     "nrrs_train_schedule_destroy": (None, [C.c_void_p]),
     "nrrs_train_schedule_tick": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_void_p]),
+    "nrrs_scene_create": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p,
+                                    C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "nrrs_scene_destroy": (None, [C.c_void_p]),
+    "nrrs_scene_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                  C.POINTER(C.c_uint32)]),
+    "nrrs_camera_rays": (C.c_int, [C.POINTER(Camera), C.c_uint32, C.c_uint32, C.POINTER(RaySoA),
+                                   C.c_void_p]),
+    "nrrs_trace": (C.c_int, [C.c_void_p, C.POINTER(RaySoA), C.c_void_p, C.c_uint32,
+                             C.POINTER(HitSoA), C.c_void_p]),
+    "nrrs_shade_scratch_bytes": (C.c_uint64, [C.c_uint32]),
+    "nrrs_shade": (C.c_int, [C.c_void_p, C.POINTER(RaySoA), C.POINTER(HitSoA), C.c_void_p,
+                             C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p,
+                             C.POINTER(PathVertices), C.c_void_p, C.c_void_p, C.c_void_p]),
+    "nrrs_scatter": (C.c_int, [C.c_void_p, C.POINTER(PathVertices), C.c_void_p, C.c_void_p,
+                               C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(RaySoA),
+                               C.POINTER(ShadowSoA), C.c_void_p]),
+    "nrrs_trace_shadow": (C.c_int, [C.c_void_p, C.POINTER(ShadowSoA), C.c_void_p, C.c_uint32,
+                                    C.c_void_p, C.c_void_p, C.c_void_p]),
+    "nrrs_film_resolve": (C.c_int, [C.c_void_p, C.c_uint32, C.c_float, C.c_void_p, C.c_void_p]),
     "nrrs_last_infer_grid": (C.c_int32, [C.c_void_p]),
     "nrrs_kernel_name": (C.c_char_p, [C.c_int32]),
     "nrrs_profile_enable": (C.c_int, [C.c_void_p, C.c_int32]),
@@ -606,6 +650,135 @@ class TrainSchedule:
         _check(lib().nrrs_train_schedule_tick(self._h, elapsed, now_seconds, C.byref(st)),
                "nrrs_train_schedule_tick")
         return st
+
+
+class Scene:
+    """A triangle scene on the device with its BVH (nrrs_scene_*); arrays are host numpy."""
+
+    def __init__(self, vertices, triangles, tri_material, materials, environment=None):
+        import numpy as np
+        self._h = None
+        self.vertices = np.ascontiguousarray(vertices, np.float32)
+        self.triangles = np.ascontiguousarray(triangles, np.uint32)
+        self.tri_material = np.ascontiguousarray(tri_material, np.uint32)
+        self.materials = np.ascontiguousarray(materials, np.float32)
+        self.environment = (np.ascontiguousarray(environment, np.float32)
+                            if environment is not None else None)
+        h = C.c_void_p()
+        _check(lib().nrrs_scene_create(
+            self.vertices.ctypes.data, len(self.vertices), self.triangles.ctypes.data,
+            len(self.triangles), self.tri_material.ctypes.data, self.materials.ctypes.data,
+            len(self.materials),
+            self.environment.ctypes.data if self.environment is not None else None,
+            C.byref(h)), "nrrs_scene_create")
+        self._h = h
+
+    def close(self):
+        if self._h:
+            lib().nrrs_scene_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def info(self) -> tuple[int, int, int]:
+        a, b, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        _check(lib().nrrs_scene_info(self._h, C.byref(a), C.byref(b), C.byref(c)),
+               "nrrs_scene_info")
+        return a.value, b.value, c.value
+
+
+def soa(cls, arrays: dict):
+    """A ctypes SoA struct (RaySoA, HitSoA, ShadowSoA, PathVertices) from a dict of arrays."""
+    return cls(*(_ptr(arrays.get(n)) for n, _ in cls._fields_))
+
+
+def camera_rays(cam: Camera, sample: int, seed: int, rays: RaySoA, stream=0):
+    _check(lib().nrrs_camera_rays(C.byref(cam), sample, seed, C.byref(rays), stream),
+           "nrrs_camera_rays")
+
+
+def trace(scene: Scene, rays: RaySoA, n_dev, max_n: int, hits: HitSoA, stream=0):
+    _check(lib().nrrs_trace(scene._h, C.byref(rays), _ptr(n_dev), max_n, C.byref(hits), stream),
+           "nrrs_trace")
+
+
+def shade_scratch_bytes(max_n: int) -> int:
+    return lib().nrrs_shade_scratch_bytes(max_n)
+
+
+def shade(scene: Scene, rays: RaySoA, hits: HitSoA, n_dev, max_n: int, depth: int, film,
+          contrib, out: PathVertices, n_out_dev, scratch, stream=0):
+    _check(lib().nrrs_shade(scene._h, C.byref(rays), C.byref(hits), _ptr(n_dev), max_n, depth,
+                            _ptr(film), _ptr(contrib), C.byref(out), _ptr(n_out_dev),
+                            _ptr(scratch), stream), "nrrs_shade")
+
+
+def scatter(scene: Scene, v: PathVertices, rrs_norm, queue, queue_size_dev, max_queue: int,
+            depth: int, seed: int, rays: RaySoA, shadow: ShadowSoA, stream=0):
+    _check(lib().nrrs_scatter(scene._h, C.byref(v), _ptr(rrs_norm), _ptr(queue),
+                              _ptr(queue_size_dev), max_queue, depth, seed, C.byref(rays),
+                              C.byref(shadow), stream), "nrrs_scatter")
+
+
+def trace_shadow(scene: Scene, shadow: ShadowSoA, n_dev, max_n: int, film, contrib_out,
+                 stream=0):
+    _check(lib().nrrs_trace_shadow(scene._h, C.byref(shadow), _ptr(n_dev), max_n, _ptr(film),
+                                   _ptr(contrib_out), stream), "nrrs_trace_shadow")
+
+
+def film_resolve(film, n_pixels: int, scale: float, image, stream=0):
+    _check(lib().nrrs_film_resolve(_ptr(film), n_pixels, scale, _ptr(image), stream),
+           "nrrs_film_resolve")
+
+
+def synth_scene(seed: int, n_boxes: int = 40, size: float = 1.0):
+    """A closed room (white walls, a red and a green wall, an emissive ceiling quad) filled with
+    n_boxes random axis-aligned boxes of random albedo, as numpy arrays: vertices, triangles,
+    tri_material, materials, environment. Deterministic in seed."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    verts, tris, mat = [], [], []
+    mats = [[0.75, 0.75, 0.75, 0, 0, 0], [0.7, 0.1, 0.1, 0, 0, 0], [0.1, 0.7, 0.1, 0, 0, 0],
+            [0.0, 0.0, 0.0, 12.0, 11.0, 9.0]]
+
+    def quad(a, b, c, d, m):
+        i = len(verts)
+        verts.extend([a, b, c, d])
+        tris.extend([[i, i + 1, i + 2], [i, i + 2, i + 3]])
+        mat.extend([m, m])
+
+    S = size
+    quad([0, 0, 0], [S, 0, 0], [S, 0, S], [0, 0, S], 0)          # floor
+    quad([0, S, 0], [0, S, S], [S, S, S], [S, S, 0], 0)          # ceiling
+    quad([0, 0, S], [S, 0, S], [S, S, S], [0, S, S], 0)          # back
+    quad([0, 0, 0], [0, 0, S], [0, S, S], [0, S, 0], 1)          # left, red
+    quad([S, 0, 0], [S, S, 0], [S, S, S], [S, 0, S], 2)          # right, green
+    c, h = 0.5 * S, 0.12 * S
+    quad([c - h, S * 0.999, c - h], [c + h, S * 0.999, c - h], [c + h, S * 0.999, c + h],
+         [c - h, S * 0.999, c + h], 3)                           # the light
+    for _ in range(n_boxes):
+        mats.append(list(rng.uniform(0.2, 0.9, 3)) + [0, 0, 0])
+        m = len(mats) - 1
+        lo = rng.uniform(0.05, 0.8, 3) * S
+        hi = lo + rng.uniform(0.03, 0.15, 3) * S
+        x0, y0, z0 = lo
+        x1, y1, z1 = hi
+        quad([x0, y0, z0], [x1, y0, z0], [x1, y1, z0], [x0, y1, z0], m)
+        quad([x0, y0, z1], [x0, y1, z1], [x1, y1, z1], [x1, y0, z1], m)
+        quad([x0, y0, z0], [x0, y1, z0], [x0, y1, z1], [x0, y0, z1], m)
+        quad([x1, y0, z0], [x1, y0, z1], [x1, y1, z1], [x1, y1, z0], m)
+        quad([x0, y0, z0], [x0, y0, z1], [x1, y0, z1], [x1, y0, z0], m)
+        quad([x0, y1, z0], [x1, y1, z0], [x1, y1, z1], [x0, y1, z1], m)
+    return (np.asarray(verts, np.float32), np.asarray(tris, np.uint32),
+            np.asarray(mat, np.uint32), np.asarray(mats, np.float32),
+            np.asarray([0.05, 0.05, 0.08], np.float32))
+
+
+def room_camera(width: int, height: int, size: float = 1.0) -> Camera:
+    """A camera looking into synth_scene's room through its open front."""
+    return Camera((C.c_float * 3)(0.5 * size, 0.5 * size, -1.3 * size),
+                  (C.c_float * 3)(0.0, 0.0, 1.0), (C.c_float * 3)(0.0, 1.0, 0.0),
+                  0.42, width, height)
 
 
 def calculate_sample_weight(pixel, pixel_samples, n_pixels: int, size_dev, max_n: int, weight,

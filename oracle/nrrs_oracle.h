@@ -111,6 +111,35 @@ float oracle_calculate_error(const nrrs_pixel_error_params* p, const float* ref,
 float oracle_ubs_error(const nrrs_pixel_error_params* p, const float* pl, uint32_t spp,
                        const float* ref, int ch, float* err_out);
 
+/* the wavefront steps around the path (render.c); HOST arrays, triangles as v0, e1, e2 */
+uint32_t oracle_scene_tris(const float* vertices, const uint32_t* tris, uint32_t nt,
+                           const uint32_t* tri_mat, const float* mats, float* tri_out,
+                           uint32_t* lights, float* areas);
+void oracle_camera_rays(const nrrs_camera* c, uint32_t sample, uint32_t seed, float* origin,
+                        float* dir);
+void oracle_trace(const float* tri, const uint32_t* mat, const float* mats, uint32_t nt,
+                  const float* origin, const float* dir, const float* thp, uint32_t n,
+                  uint32_t* prim, float* t, float* u, float* v);
+uint32_t oracle_shade(const float* tri, const uint32_t* mat, const float* mats, uint32_t nt,
+                      uint32_t nl, const float* env, const float* origin, const float* dir,
+                      const float* thp, const float* pdf, const uint32_t* pixel,
+                      const int32_t* node, const uint32_t* prim, const float* t, uint32_t n,
+                      uint32_t depth, int64_t* film, float* contrib, float* o_pos, float* o_wi,
+                      float* o_nrm, float* o_alb, float* o_rough, float* o_thp,
+                      uint32_t* o_depth, uint32_t* o_pixel, int32_t* o_node);
+void oracle_scatter(const float* tri, const uint32_t* mat, const float* mats, uint32_t nt,
+                    const uint32_t* lights, const float* area, uint32_t nl, const float* pos,
+                    const float* nrm, const float* alb, const float* thp, const uint32_t* pixel,
+                    const int32_t* node, const float* rrs_norm, const uint32_t* queue,
+                    uint32_t nq, uint32_t depth, uint32_t seed, float* r_origin, float* r_dir,
+                    float* r_thp, float* r_pdf, uint32_t* r_pixel, int32_t* r_node,
+                    float* s_origin, float* s_dir, float* s_tmax, float* s_contrib,
+                    uint32_t* s_pixel, int32_t* s_node);
+void oracle_shadow(const float* tri, uint32_t nt, const float* origin, const float* dir,
+                   const float* tmax, const float* contrib, const uint32_t* pixel, uint32_t n,
+                   int64_t* film, float* cout);
+void oracle_film_resolve(const int64_t* film, uint32_t n, float scale, float* img);
+
 /* threads used by the OpenMP loops (0 = runtime default) */
 void oracle_set_threads(int n);
 int oracle_get_threads(void);

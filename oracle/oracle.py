@@ -398,3 +398,116 @@ def ubs_error(params, pixel_l, spp: int, ref, err) -> float:
     ref = np.ascontiguousarray(ref, np.float32)
     return float(lib().oracle_ubs_error(C.byref(params), pixel_l.ctypes.data, spp,
                                         ref.ctypes.data, ref.shape[1], err.ctypes.data))
+
+
+# ---- the wavefront steps around the path (render.c) -------------------------------------------
+
+class HostScene:
+    """A scene for the oracle: triangles as v0, e1, e2 in input order and the light list, built
+    as the library builds them."""
+
+    def __init__(self, vertices, triangles, tri_material, materials, environment=None):
+        self.tm = np.ascontiguousarray(tri_material, np.uint32)
+        self.mats = np.ascontiguousarray(materials, np.float32)
+        self.env = (np.ascontiguousarray(environment, np.float32) if environment is not None
+                    else np.zeros(3, np.float32))
+        nt = len(triangles)
+        self.nt = nt
+        self.tri = np.zeros((nt, 9), np.float32)
+        self.lights = np.zeros(nt, np.uint32)
+        self.area = np.zeros(nt, np.float32)
+        v = np.ascontiguousarray(vertices, np.float32)
+        t = np.ascontiguousarray(triangles, np.uint32)
+        vp = C.c_void_p
+        L = lib()
+        L.oracle_scene_tris.restype = C.c_uint32
+        L.oracle_scene_tris.argtypes = [vp, vp, C.c_uint32, vp, vp, vp, vp, vp]
+        self.nl = int(L.oracle_scene_tris(v.ctypes.data, t.ctypes.data, nt, self.tm.ctypes.data,
+                                          self.mats.ctypes.data, self.tri.ctypes.data,
+                                          self.lights.ctypes.data, self.area.ctypes.data))
+
+    def camera_rays(self, cam, sample: int, seed: int):
+        n = cam.width * cam.height
+        o, d = np.zeros((n, 3), np.float32), np.zeros((n, 3), np.float32)
+        lib().oracle_camera_rays.argtypes = [C.POINTER(nb.Camera), C.c_uint32, C.c_uint32,
+                                             C.c_void_p, C.c_void_p]
+        lib().oracle_camera_rays(C.byref(cam), sample, seed, o.ctypes.data, d.ctypes.data)
+        return {"origin": o, "dir": d, "thp": np.ones((n, 3), np.float32),
+                "pdf": np.zeros(n, np.float32), "pixel": np.arange(n, dtype=np.uint32),
+                "node": np.full(n, -1, np.int32)}
+
+    def trace(self, rays: dict):
+        n = len(rays["pixel"])
+        h = {"prim": np.zeros(n, np.uint32), "t": np.zeros(n, np.float32),
+             "u": np.zeros(n, np.float32), "v": np.zeros(n, np.float32)}
+        f = lib().oracle_trace
+        f.argtypes = [C.c_void_p] * 3 + [C.c_uint32] + [C.c_void_p] * 3 + [C.c_uint32] + \
+            [C.c_void_p] * 4
+        f(self.tri.ctypes.data, self.tm.ctypes.data, self.mats.ctypes.data, self.nt,
+          *(np.ascontiguousarray(rays[k]).ctypes.data for k in ("origin", "dir", "thp")), n,
+          *(h[k].ctypes.data for k in ("prim", "t", "u", "v")))
+        return h
+
+    def shade(self, rays: dict, hits: dict, depth: int, film):
+        n = len(rays["pixel"])
+        out = {"pos": np.zeros((n, 3), np.float32), "wi": np.zeros((n, 3), np.float32),
+               "normal": np.zeros((n, 3), np.float32), "albedo": np.zeros((n, 3), np.float32),
+               "roughness": np.zeros(n, np.float32), "thp": np.zeros((n, 3), np.float32),
+               "depth": np.zeros(n, np.uint32), "pixel": np.zeros(n, np.uint32),
+               "node": np.zeros(n, np.int32)}
+        contrib = np.zeros((n, 3), np.float32)
+        f = lib().oracle_shade
+        f.restype = C.c_uint32
+        f.argtypes = [C.c_void_p] * 3 + [C.c_uint32, C.c_uint32] + [C.c_void_p] * 9 + \
+            [C.c_uint32, C.c_uint32] + [C.c_void_p] * 11
+        m = f(self.tri.ctypes.data, self.tm.ctypes.data, self.mats.ctypes.data, self.nt, self.nl,
+              self.env.ctypes.data,
+              *(np.ascontiguousarray(rays[k]).ctypes.data for k in
+                ("origin", "dir", "thp", "pdf", "pixel", "node")),
+              hits["prim"].ctypes.data, hits["t"].ctypes.data, n, depth, film.ctypes.data,
+              contrib.ctypes.data,
+              *(out[k].ctypes.data for k in ("pos", "wi", "normal", "albedo", "roughness", "thp",
+                                             "depth", "pixel", "node")))
+        return {k: v[:m] for k, v in out.items()}, contrib
+
+    def scatter(self, v: dict, rrs_norm, queue, depth: int, seed: int):
+        nq = len(queue)
+        r = {"origin": np.zeros((nq, 3), np.float32), "dir": np.zeros((nq, 3), np.float32),
+             "thp": np.zeros((nq, 3), np.float32), "pdf": np.zeros(nq, np.float32),
+             "pixel": np.zeros(nq, np.uint32), "node": np.zeros(nq, np.int32)}
+        sh = {"origin": np.zeros((nq, 3), np.float32), "dir": np.zeros((nq, 3), np.float32),
+              "tmax": np.zeros(nq, np.float32), "contrib": np.zeros((nq, 3), np.float32),
+              "pixel": np.zeros(nq, np.uint32), "node": np.zeros(nq, np.int32)}
+        rrs_norm = np.ascontiguousarray(rrs_norm, np.float32)
+        queue = np.ascontiguousarray(queue, np.uint32)
+        f = lib().oracle_scatter
+        f.argtypes = [C.c_void_p] * 3 + [C.c_uint32] + [C.c_void_p] * 2 + [C.c_uint32] + \
+            [C.c_void_p] * 8 + [C.c_uint32, C.c_uint32, C.c_uint32] + [C.c_void_p] * 12
+        f(self.tri.ctypes.data, self.tm.ctypes.data, self.mats.ctypes.data, self.nt,
+          self.lights.ctypes.data, self.area.ctypes.data, self.nl,
+          *(np.ascontiguousarray(v[k]).ctypes.data for k in ("pos", "normal", "albedo", "thp",
+                                                             "pixel", "node")),
+          rrs_norm.ctypes.data, queue.ctypes.data, nq, depth, seed,
+          *(r[k].ctypes.data for k in ("origin", "dir", "thp", "pdf", "pixel", "node")),
+          *(sh[k].ctypes.data for k in ("origin", "dir", "tmax", "contrib", "pixel", "node")))
+        return r, sh
+
+    def shadow(self, sh: dict, film):
+        n = len(sh["pixel"])
+        cout = np.zeros((n, 3), np.float32)
+        f = lib().oracle_shadow
+        f.argtypes = [C.c_void_p, C.c_uint32] + [C.c_void_p] * 5 + [C.c_uint32] + [C.c_void_p] * 2
+        f(self.tri.ctypes.data, self.nt,
+          *(np.ascontiguousarray(sh[k]).ctypes.data for k in ("origin", "dir", "tmax", "contrib",
+                                                             "pixel")),
+          n, film.ctypes.data, cout.ctypes.data)
+        return cout
+
+    @staticmethod
+    def resolve(film, scale: float):
+        n = film.shape[0]
+        img = np.zeros((n, 3), np.float32)
+        f = lib().oracle_film_resolve
+        f.argtypes = [C.c_void_p, C.c_uint32, C.c_float, C.c_void_p]
+        f(film.ctypes.data, n, scale, img.ctypes.data)
+        return img

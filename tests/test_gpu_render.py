@@ -1,0 +1,238 @@
+"""GPU parity of the wavefront steps around the NRRS step (nrrs_camera_rays, nrrs_trace,
+nrrs_shade, nrrs_scatter, nrrs_trace_shadow, nrrs_film_resolve) against the C restatement, bit
+for bit: BVH closest hits against brute force on camera rays and random rays, a whole frame of
+four bounces with the emitted queue of the library's decision between them, and the film. Also
+checks that splitting and killing by the RRS factors leave the image unbiased."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import nrrs_b200 as nb
+import oracle as O
+from gpu_util import host, stream, torch_cuda
+
+pytestmark = pytest.mark.gpu
+
+V3 = ("origin", "dir", "thp", "pos", "wi", "normal", "albedo", "contrib")
+
+
+def dev_dict(d: dict):
+    torch = torch_cuda()
+    out = {}
+    for k, a in d.items():
+        a = np.ascontiguousarray(a)
+        if a.dtype == np.uint32:
+            a = a.view(np.int32)
+        out[k] = torch.from_numpy(a).cuda()
+    return out
+
+
+def empty_rays(n):
+    torch = torch_cuda()
+    f = lambda *s: torch.zeros(*s, dtype=torch.float32, device="cuda")  # noqa: E731
+    i = lambda *s: torch.zeros(*s, dtype=torch.int32, device="cuda")   # noqa: E731
+    return {"origin": f(n, 3), "dir": f(n, 3), "thp": f(n, 3), "pdf": f(n), "pixel": i(n),
+            "node": i(n)}
+
+
+def empty_hits(n):
+    torch = torch_cuda()
+    return {"prim": torch.zeros(n, dtype=torch.int32, device="cuda"),
+            "t": torch.zeros(n, device="cuda"), "u": torch.zeros(n, device="cuda"),
+            "v": torch.zeros(n, device="cuda")}
+
+
+def empty_vertices(n):
+    torch = torch_cuda()
+    f = lambda *s: torch.full(s, -9.0, dtype=torch.float32, device="cuda")  # noqa: E731
+    i = lambda *s: torch.zeros(*s, dtype=torch.int32, device="cuda")       # noqa: E731
+    return {"pos": f(n, 3), "wi": f(n, 3), "normal": f(n, 3), "albedo": f(n, 3),
+            "roughness": f(n), "thp": f(n, 3), "depth": i(n), "pixel": i(n), "node": i(n)}
+
+
+def empty_shadow(n):
+    torch = torch_cuda()
+    f = lambda *s: torch.zeros(*s, dtype=torch.float32, device="cuda")  # noqa: E731
+    i = lambda *s: torch.zeros(*s, dtype=torch.int32, device="cuda")   # noqa: E731
+    return {"origin": f(n, 3), "dir": f(n, 3), "tmax": f(n), "contrib": f(n, 3), "pixel": i(n),
+            "node": i(n)}
+
+
+def to_host(d: dict, n: int):
+    out = {}
+    for k, t in d.items():
+        a = host(t)[:n]
+        out[k] = a.view(np.uint32) if k in ("prim", "pixel", "depth") else a
+    return out
+
+
+def same(a, b, keys):
+    for k in keys:
+        assert np.asarray(a[k]).tobytes() == np.asarray(b[k]).tobytes(), k
+
+
+def scene_pair(seed=1, boxes=60):
+    v, t, m, ma, e = nb.synth_scene(seed, n_boxes=boxes)
+    return nb.Scene(v, t, m, ma, e), O.HostScene(v, t, m, ma, e)
+
+
+def test_gpu_trace_matches_brute_force():
+    torch = torch_cuda()
+    gs, hs = scene_pair(2, boxes=250)
+    nn, nl, depth = gs.info()
+    assert nl == 2 and nn > 100 and depth < 32
+    cam = nb.room_camera(160, 120)
+    n = 160 * 120
+    rays = empty_rays(2 * n)
+    nb.camera_rays(cam, 3, 11, nb.soa(nb.RaySoA, rays), stream())
+    r_cam = hs.camera_rays(cam, 3, 11)
+    got = to_host(rays, n)
+    same(got, r_cam, ("origin", "dir", "thp", "pdf", "pixel", "node"))
+    # and random rays from inside the room
+    rng = np.random.default_rng(0)
+    o = rng.uniform(0.02, 0.98, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r_rand = {"origin": o, "dir": d, "thp": np.ones((n, 3), np.float32),
+              "pdf": np.zeros(n, np.float32), "pixel": np.zeros(n, np.uint32),
+              "node": np.full(n, -1, np.int32)}
+    dr = dev_dict(r_rand)
+    for k in r_rand:
+        rays[k][n:2 * n].copy_(dr[k])
+    r_all = {k: np.concatenate([r_cam[k], r_rand[k]]) for k in r_cam}
+    hits = empty_hits(2 * n)
+    cnt = torch.tensor([2 * n], dtype=torch.int32, device="cuda")
+    nb.trace(gs, nb.soa(nb.RaySoA, rays), cnt, 2 * n, nb.soa(nb.HitSoA, hits), stream())
+    want = hs.trace(r_all)
+    got = to_host(hits, 2 * n)
+    same(got, want, ("prim", "t", "u", "v"))
+    assert (want["prim"] != 0xffffffff).mean() > 0.5
+
+
+def run_frame_pair(gs, hs, cam, seed, bounces, factors):
+    """One frame on the GPU and in the oracle, bounce by bounce, with the emitted queue of the
+    library's decision (nrrs_decide_emit_noalloc) on the given factor generator between them;
+    every array compared as it is produced. Returns both films."""
+    torch = torch_cuda()
+    n = cam.width * cam.height
+    cap = 4 * n
+    film = torch.zeros((n, 9), dtype=torch.int64, device="cuda")
+    hfilm = np.zeros((n, 9), np.int64)
+    rays, hits = empty_rays(cap), empty_hits(cap)
+    verts, shadow = empty_vertices(cap), empty_shadow(cap)
+    contrib = torch.zeros((cap, 3), device="cuda")
+    scontrib = torch.zeros((cap, 3), device="cuda")
+    scratch = torch.zeros(nb.shade_scratch_bytes(cap), dtype=torch.uint8, device="cuda")
+    n_rays = torch.tensor([n], dtype=torch.int32, device="cuda")
+    n_vert = torch.zeros(1, dtype=torch.int32, device="cuda")
+    qsize = torch.zeros(1, dtype=torch.int32, device="cuda")
+    queue = torch.zeros(cap, dtype=torch.int32, device="cuda")
+    rrs_norm = torch.zeros(cap, device="cuda")
+    nb.camera_rays(cam, 0, seed, nb.soa(nb.RaySoA, rays), stream())
+    hr = hs.camera_rays(cam, 0, seed)
+    dp = nb.default_decide(clamp_max=4.0)
+    rng = np.random.default_rng(seed)
+    for depth in range(bounces):
+        nr = int(host(n_rays)[0])
+        nb.trace(gs, nb.soa(nb.RaySoA, rays), n_rays, cap, nb.soa(nb.HitSoA, hits), stream())
+        hh = hs.trace(hr)
+        same(to_host(hits, nr), hh, ("prim", "t", "u", "v"))
+        nb.shade(gs, nb.soa(nb.RaySoA, rays), nb.soa(nb.HitSoA, hits), n_rays, cap, depth, film,
+                 contrib, nb.soa(nb.PathVertices, verts), n_vert, scratch, stream())
+        hv, hc = hs.shade(hr, hh, depth, hfilm)
+        nv = int(host(n_vert)[0])
+        assert nv == len(hv["pos"])
+        same(to_host(verts, nv), hv, nb.PATH_VERTEX_FIELDS)
+        assert host(contrib)[:nr].tobytes() == hc.tobytes()
+        assert host(film).tobytes() == hfilm.tobytes()
+        if nv == 0:
+            break
+        # the emitted queue: the library's decision on synthetic factors (as nrrs_step would)
+        f = factors(rng, nv).astype(np.float32)
+        rnd = rng.uniform(size=nv).astype(np.float32)
+        split = torch.zeros(nv, dtype=torch.uint8, device="cuda")
+        rc = nb.decide_emit_noalloc(torch.from_numpy(f).cuda(), torch.from_numpy(rnd).cuda(), nv,
+                                    nv, 0, dp, rrs_norm, split, queue, cap, qsize, None, stream())
+        assert rc == 0
+        o = O.decide_emit(f, rnd, nv, 0, dp, capacity=cap, shift_n=nb.NOALLOC_MAX_N)
+        nq = int(host(qsize)[0])
+        assert nq == o["total"] and host(queue)[:nq].view(np.uint32).tolist() == o["queue"].tolist()
+        nb.scatter(gs, nb.soa(nb.PathVertices, verts), rrs_norm, queue, qsize, cap, depth, seed,
+                   nb.soa(nb.RaySoA, rays), nb.soa(nb.ShadowSoA, shadow), stream())
+        hr, hsh = hs.scatter(hv, o["rrs_norm"], o["queue"], depth, seed)
+        same(to_host(rays, nq), hr, ("origin", "dir", "thp", "pdf", "pixel", "node"))
+        same(to_host(shadow, nq), hsh, ("origin", "dir", "tmax", "contrib", "pixel", "node"))
+        nb.trace_shadow(gs, nb.soa(nb.ShadowSoA, shadow), qsize, cap, film, scontrib, stream())
+        hco = hs.shadow(hsh, hfilm)
+        assert host(scontrib)[:nq].tobytes() == hco.tobytes()
+        assert host(film).tobytes() == hfilm.tobytes()
+        n_rays.copy_(qsize)
+    img = torch.zeros((n, 3), device="cuda")
+    nb.film_resolve(film, n, 1.0, img, stream())
+    himg = hs.resolve(hfilm, 1.0)
+    assert host(img).tobytes() == himg.tobytes()
+    return host(img), himg
+
+
+def test_gpu_frame_matches_oracle():
+    gs, hs = scene_pair(3, boxes=40)
+    cam = nb.room_camera(64, 48)
+    img, _ = run_frame_pair(gs, hs, cam, 5, 4,
+                            lambda rng, n: rng.uniform(0.3, 2.5, n))
+    assert img.mean() > 0
+
+
+def test_gpu_rrs_keeps_the_image_unbiased():
+    """The mean image over frames with random kill/split factors matches the mean with factor 1
+    (no decision: every vertex continues once) within the frames' standard error."""
+    torch = torch_cuda()
+    gs, _ = scene_pair(4, boxes=20)
+    cam = nb.room_camera(48, 36)
+    n = cam.width * cam.height
+    cap = 8 * n
+
+    def frame(seed, factor):
+        film = torch.zeros((n, 9), dtype=torch.int64, device="cuda")
+        rays, hits = empty_rays(cap), empty_hits(cap)
+        verts, shadow = empty_vertices(cap), empty_shadow(cap)
+        scratch = torch.zeros(nb.shade_scratch_bytes(cap), dtype=torch.uint8, device="cuda")
+        n_rays = torch.tensor([n], dtype=torch.int32, device="cuda")
+        n_vert, qsize = (torch.zeros(1, dtype=torch.int32, device="cuda") for _ in range(2))
+        queue = torch.zeros(cap, dtype=torch.int32, device="cuda")
+        rrs_norm = torch.zeros(cap, device="cuda")
+        dp = nb.default_decide(clamp_max=4.0, clamp_min=0.0, use_ceil=0, normalize_rate=1.0,
+                               scale_up=1)
+        nb.camera_rays(cam, seed, 99, nb.soa(nb.RaySoA, rays), stream())
+        rng = np.random.default_rng(seed)
+        for depth in range(5):
+            nb.trace(gs, nb.soa(nb.RaySoA, rays), n_rays, cap, nb.soa(nb.HitSoA, hits), stream())
+            nb.shade(gs, nb.soa(nb.RaySoA, rays), nb.soa(nb.HitSoA, hits), n_rays, cap, depth,
+                     film, None, nb.soa(nb.PathVertices, verts), n_vert, scratch, stream())
+            nv = int(host(n_vert)[0])
+            if nv == 0:
+                break
+            f = factor(rng, nv).astype(np.float32)
+            # budget = sum of factors: the normalisation leaves the factors as they are
+            budget = max(1, int(round(float(f.sum()))))
+            f *= np.float32(budget / max(float(f.sum()), 1e-6))
+            rnd = rng.uniform(size=nv).astype(np.float32)
+            nb.decide_emit_noalloc(torch.from_numpy(f).cuda(), torch.from_numpy(rnd).cuda(), nv,
+                                   budget, 0, dp, rrs_norm, None, queue, cap, qsize, None,
+                                   stream())
+            nb.scatter(gs, nb.soa(nb.PathVertices, verts), rrs_norm, queue, qsize, cap, depth,
+                       seed * 7 + 1, nb.soa(nb.RaySoA, rays), nb.soa(nb.ShadowSoA, shadow),
+                       stream())
+            nb.trace_shadow(gs, nb.soa(nb.ShadowSoA, shadow), qsize, cap, film, None, stream())
+            n_rays.copy_(qsize)
+        img = torch.zeros((n, 3), device="cuda")
+        nb.film_resolve(film, n, 1.0, img, stream())
+        return float(host(img).mean())
+
+    ones = [frame(s, lambda rng, k: np.ones(k)) for s in range(24)]
+    rrs = [frame(s, lambda rng, k: rng.choice([0.5, 1.0, 2.0], k)) for s in range(24)]
+    a, b = np.mean(ones), np.mean(rrs)
+    se = np.sqrt(np.var(ones) / len(ones) + np.var(rrs) / len(rrs))
+    assert abs(a - b) < 4 * se + 0.02 * a, (a, b, se)
