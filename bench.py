@@ -15,13 +15,19 @@ Other workloads (--workload):
             separately on the same vertices (and checked to decide identically)
   frame4k   3840x2160: 8,294,400 vertices per bounce, 10 bounces, MLPs 128 wide x 3 hidden
             layers (BF16 by default), 2^22-entry table, 10 training steps of 262,144 samples
+  render1080p
+            a path-traced 1920x1080 frame around the NRRS step: camera rays, then per bounce
+            (up to 6) BVH trace, shading into the vertex queue, nrrs_step (mixed precision),
+            scatter (NEE + BSDF rays) and shadow rays, in a closed room of 3000 boxes
+            (36k triangles) seen from inside;
+            metric path vertices/s
   records1080p
             the training-data side of a 1920x1080 frame: 8 bounces of path vertices (about
             10.1M) record 7.0M path nodes and 7.5M radiance contributions, then the training
             batch and the sample weights are built; metric path nodes/s (one step = one frame)
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload frame1080p|batched|frame4k|records1080p]
+                  [--workload frame1080p|batched|frame4k|records1080p|render1080p]
                   [--precision fp16|bf16|fp32]
                   [--no-train]
 
@@ -68,6 +74,9 @@ WORKLOADS = {
     # throughput scaled by rrs, later siblings without RRSNet target; zero-L samples kept
     # 600 frames: about a second of timed work, so that the clock sampler sees it
     "records1080p": dict(bounces=8, n_vert=2_073_600, node_rate=10, steps=600, precision="fp32"),
+    "render1080p": dict(bounces=6, n_vert=2_073_600, width=64, hidden=2, log2_table=19,
+                        steps=40, precision="fp16", boxes=3000, train_steps=0,
+                        train_batch=0),
 }
 
 
@@ -1014,6 +1023,156 @@ def run_records(args, rank, world, local_rank):
     return 0
 
 
+# ---- render1080p: the path tracer around the NRRS step ---------------------------------------
+
+def run_render(args, rank, world, local_rank):
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local_rank)
+    cur = torch.cuda.current_stream()
+    stream = cur.cuda_stream
+    wl = WORKLOADS[args.workload]
+    W, H = (1920, 1080) if wl["n_vert"] == 1920 * 1080 else (wl["n_vert"], 1)
+    P = W * H
+    cap = 3 * P
+    v, t, m, ma, env = nb.synth_scene(7 + rank, n_boxes=wl["boxes"], closed=True)
+    scene = nb.Scene(v, t, m, ma, env)
+    n_nodes, n_lights, bvh_depth = scene.info()
+    cam = nb.room_camera(W, H, inside=True)
+    net = nb.NRRSNetwork(make_config(args.precision, wl, cap, 1 << 16))
+    net.setStep(3)
+    # factors clamped at 1 or above: the normalisation to the pixel budget then keeps about one
+    # path per pixel per bounce, as a trained network would; an untrained one kills most paths
+    dp = nb.default_decide(clamp_min=1.0)
+
+    f = lambda *sh: torch.zeros(*sh, dtype=torch.float32, device=dev)  # noqa: E731
+    i = lambda *sh: torch.zeros(*sh, dtype=torch.int32, device=dev)    # noqa: E731
+    rays = {"origin": f(cap, 3), "dir": f(cap, 3), "thp": f(cap, 3), "pdf": f(cap),
+            "pixel": i(cap), "node": i(cap)}
+    hits = {"prim": i(cap), "t": f(cap), "u": f(cap), "v": f(cap)}
+    verts = {"pos": f(cap, 3), "wi": f(cap, 3), "normal": f(cap, 3), "albedo": f(cap, 3),
+             "roughness": f(cap), "thp": f(cap, 3), "depth": i(cap), "pixel": i(cap),
+             "node": i(cap)}
+    shadow = {"origin": f(cap, 3), "dir": f(cap, 3), "tmax": f(cap), "contrib": f(cap, 3),
+              "pixel": i(cap), "node": i(cap)}
+    film = torch.zeros((P, 9), dtype=torch.int64, device=dev)
+    img = f(P, 3)
+    scratch = torch.zeros(nb.shade_scratch_bytes(cap), dtype=torch.uint8, device=dev)
+    n_rays, n_vert, qsize = i(1), i(1), i(1)
+    rnd = torch.rand(cap, device=dev, generator=torch.Generator(device=dev).manual_seed(5))
+    stats, rrs, rrs_norm = f(3 * cap), f(cap), f(cap)
+    split = torch.zeros(cap, dtype=torch.uint8, device=dev)
+    queue = i(cap)
+    R, Hh, V, S = (nb.soa(nb.RaySoA, rays), nb.soa(nb.HitSoA, hits),
+                   nb.soa(nb.PathVertices, verts), nb.soa(nb.ShadowSoA, shadow))
+    vsoa = nb.vertex_soa(verts["pos"], verts["wi"], verts["normal"], verts["roughness"],
+                         verts["albedo"], verts["thp"], verts["depth"])
+    ev = {}
+
+    bounces_run = [0]
+
+    def frame(sample, timing=False):
+        vertices = 0
+        film.zero_()
+        nb.camera_rays(cam, sample, 1234, R, stream)
+        n_rays.fill_(P)
+        for depth in range(wl["bounces"]):
+            if timing:
+                ev.setdefault(("trace", depth), (torch.cuda.Event(enable_timing=True),
+                                                 torch.cuda.Event(enable_timing=True)))
+                ev[("trace", depth)][0].record(cur)
+            nb.trace(scene, R, n_rays, cap, Hh, stream)
+            if timing:
+                ev[("trace", depth)][1].record(cur)
+            nb.shade(scene, R, Hh, n_rays, cap, depth, film, None, V, n_vert, scratch, stream)
+            nv = int(n_vert.item())          # the reference reads the queue size back too
+            if nv == 0:
+                break
+            vertices += nv
+            bounces_run[0] += 1
+            if timing:
+                ev.setdefault(("nrrs", depth), (torch.cuda.Event(enable_timing=True),
+                                                torch.cuda.Event(enable_timing=True)))
+                ev[("nrrs", depth)][0].record(cur)
+            net.generateRRSNumber(vsoa, rnd, nv, P, 0, dp, stats, rrs, rrs_norm, split, queue,
+                                  cap, qsize, stream)
+            if timing:
+                ev[("nrrs", depth)][1].record(cur)
+            nb.scatter(scene, V, rrs_norm, queue, qsize, cap, depth, 1234 + sample, R, S, stream)
+            if timing:
+                ev.setdefault(("shadow", depth), (torch.cuda.Event(enable_timing=True),
+                                                  torch.cuda.Event(enable_timing=True)))
+                ev[("shadow", depth)][0].record(cur)
+            nb.trace_shadow(scene, S, qsize, cap, film, None, stream)
+            if timing:
+                ev[("shadow", depth)][1].record(cur)
+            n_rays.copy_(qsize)
+        nb.film_resolve(film, P, 1.0, img, stream)
+        return vertices
+
+    for w in range(args.warmup):
+        frame(w)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    total_v = 0
+    bounces_run[0] = 0
+    launches0 = net.launch_count()
+    with ClockSampler(local_rank) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(cur)
+        for k in range(args.steps):
+            total_v += frame(100 + k)
+        e1.record(cur)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    verts_per_frame = total_v / args.steps
+    # camera + resolve per frame; trace, shade (2), scatter, shadow per bounce run, and the last
+    # trace + shade of a frame whose queue ran out; plus the NRRS step's own launches
+    launches = (args.steps * 2 + bounces_run[0] * 5 + (net.launch_count() - launches0))
+    if dist:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    frame(999, timing=True)
+    torch.cuda.synchronize()
+    t_trace = sum(a.elapsed_time(b) for (k, _), (a, b) in ev.items() if k == "trace")
+    t_nrrs = sum(a.elapsed_time(b) for (k, _), (a, b) in ev.items() if k == "nrrs")
+    t_shadow = sum(a.elapsed_time(b) for (k, _), (a, b) in ev.items() if k == "shadow")
+    rays_traced = verts_per_frame  # closest-hit rays per frame are about the vertices plus misses
+    line = {
+        "metric": "path vertices/s (path-traced frame around the NRRS step)",
+        "value": verts_per_frame * world / (ms * 1e-3), "unit": "vertices/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f16", "data": "synthetic",
+        "config": {"workload": f"render_{W}x{H}_{wl['bounces']}bounce_{len(t)}tri",
+                   "triangles": int(len(t)), "bvh_nodes": n_nodes, "bvh_depth": bvh_depth,
+                   "lights": n_lights, "vertices_per_frame": verts_per_frame,
+                   "parallelism": f"replicas{world}",
+                   "l2": "queues of 2-6M entries per bounce (hundreds of MB) are larger than L2; "
+                         "the scene (2.5 MB) is L2-resident"},
+        "clocks": clk.summary(),
+        "gpu_launches": launches,
+        "calls_ms_per_frame": {"trace": t_trace, "nrrs_step": t_nrrs, "shadow": t_shadow},
+        "rays_per_s_trace": rays_traced / (t_trace * 1e-3) if t_trace else None,
+        "note": "a step is one frame; per bounce the vertex count is read back (as the "
+                "reference reads its queue size) before nrrs_step",
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    scene.close()
+    net.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1038,10 +1197,18 @@ def main():
         args.precision = wl["precision"]
     if args.bounces:
         wl["bounces"] = args.bounces
-    if args.vertices and args.workload != "records1080p":
+    if args.vertices and args.workload not in ("records1080p", "render1080p"):
         wl["n_vert"] = args.vertices
     rank, world = env_int("RANK", 0), env_int("WORLD_SIZE", 1)
     local_rank = env_int("LOCAL_RANK", 0)
+    if args.workload == "render1080p":
+        if args.vertices:
+            wl["n_vert"] = args.vertices
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference traces with "
+                              "OptiX inside its KiRaRay integrator, which cannot be built here"}))
+            return 0
+        return run_render(args, rank, world, local_rank)
     if args.workload == "records1080p":
         if args.vertices:
             wl["n_vert"] = args.vertices

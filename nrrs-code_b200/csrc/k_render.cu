@@ -25,7 +25,7 @@
 #include "nrrs.h"
 
 struct nrrs_scene {
-    float* tris = nullptr;        // [nt][9] v0, e1, e2 in BVH leaf order
+    float* tris = nullptr;        // [nt][12] v0, e1, e2, pad in BVH leaf order
     uint32_t* tri_id = nullptr;   // [nt] input index of each leaf-order triangle
     uint32_t* tri_mat = nullptr;  // [nt] material, input order
     float* tri_in = nullptr;      // [nt][9] v0, e1, e2 in input order
@@ -82,9 +82,8 @@ __device__ __forceinline__ void put(float* p, V3 a) { p[0] = a.x; p[1] = a.y; p[
 __device__ __forceinline__ bool nonzero(V3 a) { return a.x != 0.f || a.y != 0.f || a.z != 0.f; }
 
 // Moller-Trumbore, two-sided; t in (0, tmax)
-__device__ __forceinline__ bool intersect(const float* tri, V3 o, V3 d, float tmax, float* t,
-                                          float* u, float* v) {
-    const V3 v0 = v3(tri), e1 = v3(tri + 3), e2 = v3(tri + 6);
+__device__ __forceinline__ bool intersect_v(V3 v0, V3 e1, V3 e2, V3 o, V3 d, float tmax, float* t,
+                                            float* u, float* v) {
     const V3 pv = cross(d, e2);
     const float det = dot(e1, pv);
     if (fabsf(det) < 1e-12f) return false;
@@ -101,13 +100,24 @@ __device__ __forceinline__ bool intersect(const float* tri, V3 o, V3 d, float tm
     return true;
 }
 
+// a leaf-order triangle of 12 floats, read as three 16-byte loads
+__device__ __forceinline__ bool intersect_leaf(const float* tri, V3 o, V3 d, float tmax, float* t,
+                                               float* u, float* v) {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(tri));
+    const float4 b = __ldg(reinterpret_cast<const float4*>(tri) + 1);
+    const float4 c = __ldg(reinterpret_cast<const float4*>(tri) + 2);
+    return intersect_v({a.x, a.y, a.z}, {a.w, b.x, b.y}, {b.z, b.w, c.x}, o, d, tmax, t, u, v);
+}
+
 // slab test; the interval [t0, t1] of the box along the ray, clipped to [0, tmax]
-__device__ __forceinline__ bool box_hit(const float* nd, V3 o, V3 inv, float tmax, float* tnear) {
+__device__ __forceinline__ bool box_hit(float4 lo, float4 hi, V3 o, V3 inv, float tmax,
+                                        float* tnear) {
     float t0 = 0.f, t1 = tmax;
     const float oo[3] = {o.x, o.y, o.z}, ii[3] = {inv.x, inv.y, inv.z};
+    const float bl[3] = {lo.x, lo.y, lo.z}, bh[3] = {hi.x, hi.y, hi.z};
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        float a = (nd[k] - oo[k]) * ii[k], b = (nd[4 + k] - oo[k]) * ii[k];
+        float a = (bl[k] - oo[k]) * ii[k], b = (bh[k] - oo[k]) * ii[k];
         if (a > b) { const float s = a; a = b; b = s; }
         t0 = a > t0 ? a : t0;      // NaN (0 x inf) leaves the bound as it was
         t1 = b < t1 ? b : t1;
@@ -127,15 +137,16 @@ __device__ Hit traverse(const nrrs_scene& s, V3 o, V3 d, float tmax) {
     int sp = 0;
     stack[sp++] = 0;
     while (sp > 0) {
-        const float* nd = s.nodes + 8 * (size_t)stack[--sp];
+        const float4* nd = reinterpret_cast<const float4*>(s.nodes) + 2 * (size_t)stack[--sp];
+        const float4 lo = __ldg(nd), hi = __ldg(nd + 1);
         float tn;
-        if (!box_hit(nd, o, inv, h.prim == kMiss ? tmax : h.t, &tn)) continue;
-        const uint32_t lf = __float_as_uint(nd[3]), ca = __float_as_uint(nd[7]);
+        if (!box_hit(lo, hi, o, inv, h.prim == kMiss ? tmax : h.t, &tn)) continue;
+        const uint32_t lf = __float_as_uint(lo.w), ca = __float_as_uint(hi.w);
         const uint32_t cnt = ca & 0xffffu;
         if (cnt) {
             for (uint32_t i = lf; i < lf + cnt; ++i) {
                 float t, u, v;
-                if (!intersect(s.tris + 9 * (size_t)i, o, d, tmax, &t, &u, &v)) continue;
+                if (!intersect_leaf(s.tris + 12 * (size_t)i, o, d, tmax, &t, &u, &v)) continue;
                 const uint32_t id = s.tri_id[i];
                 if (h.prim == kMiss || t < h.t || (t == h.t && id < h.prim)) h = {id, t, u, v};
                 if (ANY) return h;
@@ -469,6 +480,10 @@ struct Build {
             bmax[k] += e;
         }
     }
+    static float area_of(const float* lo, const float* hi) {
+        const float x = hi[0] - lo[0], y = hi[1] - lo[1], z = hi[2] - lo[2];
+        return x * y + y * z + z * x;
+    }
     float centroid(uint32_t id, int k) const {
         const float* t = tri->data() + 9 * (size_t)id;
         return t[k] + (t[3 + k] + t[6 + k]) / 3.0f;
@@ -492,15 +507,82 @@ struct Build {
             set_word(me, 7, hi - lo);
             return;
         }
-        int axis = 0;
-        for (int k = 1; k < 3; ++k)
-            if (bmax[k] - bmin[k] > bmax[axis] - bmin[axis]) axis = k;
-        const uint32_t mid = lo + (hi - lo) / 2;
-        std::nth_element(order.begin() + lo, order.begin() + mid, order.begin() + hi,
-                         [&](uint32_t a, uint32_t b) {
-                             const float ca = centroid(a, axis), cb = centroid(b, axis);
-                             return ca < cb || (ca == cb && a < b);
-                         });
+        // binned surface-area heuristic over the centroids (16 bins per axis); a median split
+        // on the longest axis when no binned cut costs less than the node's own area × count
+        // (leaves stay at most kLeafMax triangles either way)
+        float cmin[3], cmax[3];
+        for (int k = 0; k < 3; ++k) { cmin[k] = INFINITY; cmax[k] = -INFINITY; }
+        for (uint32_t i = lo; i < hi; ++i)
+            for (int k = 0; k < 3; ++k) {
+                const float c = centroid(order[i], k);
+                cmin[k] = std::min(cmin[k], c);
+                cmax[k] = std::max(cmax[k], c);
+            }
+        constexpr int kBins = 16;
+        int axis = -1, cut = 0;
+        float best = (float)(hi - lo) * area_of(bmin, bmax);   // the leaf's cost
+        for (int k = 0; k < 3; ++k) {
+            const float ext = cmax[k] - cmin[k];
+            if (!(ext > 0.f)) continue;
+            float lo3[kBins][3], hi3[kBins][3];
+            uint32_t cnt[kBins] = {};
+            for (int q = 0; q < kBins; ++q)
+                for (int j = 0; j < 3; ++j) { lo3[q][j] = INFINITY; hi3[q][j] = -INFINITY; }
+            for (uint32_t i = lo; i < hi; ++i) {
+                const uint32_t id = order[i];
+                int q = (int)((centroid(id, k) - cmin[k]) / ext * kBins);
+                q = std::min(std::max(q, 0), kBins - 1);
+                ++cnt[q];
+                const float* t = tri->data() + 9 * (size_t)id;
+                for (int j = 0; j < 3; ++j) {
+                    const float a0 = t[j], a1 = t[j] + t[3 + j], a2 = t[j] + t[6 + j];
+                    lo3[q][j] = std::min({lo3[q][j], a0, a1, a2});
+                    hi3[q][j] = std::max({hi3[q][j], a0, a1, a2});
+                }
+            }
+            // sweep: the cost of cutting after bin q
+            float rl[kBins][3], rh[kBins][3];
+            uint32_t rc[kBins];
+            float al[3] = {INFINITY, INFINITY, INFINITY}, ah[3] = {-INFINITY, -INFINITY, -INFINITY};
+            uint32_t ac = 0;
+            for (int q = kBins - 1; q > 0; --q) {
+                for (int j = 0; j < 3; ++j) { al[j] = std::min(al[j], lo3[q][j]); ah[j] = std::max(ah[j], hi3[q][j]); }
+                ac += cnt[q];
+                for (int j = 0; j < 3; ++j) { rl[q][j] = al[j]; rh[q][j] = ah[j]; }
+                rc[q] = ac;
+            }
+            float ll[3] = {INFINITY, INFINITY, INFINITY}, lh[3] = {-INFINITY, -INFINITY, -INFINITY};
+            uint32_t lc = 0;
+            for (int q = 0; q < kBins - 1; ++q) {
+                for (int j = 0; j < 3; ++j) { ll[j] = std::min(ll[j], lo3[q][j]); lh[j] = std::max(lh[j], hi3[q][j]); }
+                lc += cnt[q];
+                if (lc == 0 || rc[q + 1] == 0) continue;
+                const float c = (float)lc * area_of(ll, lh) + (float)rc[q + 1] * area_of(rl[q + 1], rh[q + 1]);
+                if (c < best) { best = c; axis = k; cut = q; }
+            }
+        }
+        uint32_t mid;
+        if (axis >= 0) {
+            const float ext = cmax[axis] - cmin[axis];
+            const auto it = std::partition(order.begin() + lo, order.begin() + hi, [&](uint32_t id) {
+                int q = (int)((centroid(id, axis) - cmin[axis]) / ext * kBins);
+                q = std::min(std::max(q, 0), kBins - 1);
+                return q <= cut;
+            });
+            mid = (uint32_t)(it - order.begin());
+            if (mid == lo || mid == hi) axis = -1;
+        }
+        if (axis < 0) {
+            axis = 0;
+            for (int k = 1; k < 3; ++k)
+                if (bmax[k] - bmin[k] > bmax[axis] - bmin[axis]) axis = k;
+            mid = lo + (hi - lo) / 2;
+            std::nth_element(order.begin() + lo, order.begin() + mid, order.begin() + hi,
+                             [&](uint32_t a, uint32_t b) {
+                                 const float ca = centroid(a, axis), cb = centroid(b, axis);
+                                 return ca < cb || (ca == cb && a < b);
+                             });
+        }
         const uint32_t left = alloc();
         alloc();
         set_word(me, 3, left);
@@ -572,9 +654,9 @@ extern "C" int nrrs_scene_create(const float* vertices, uint32_t n_vertices,
     b.order.resize(n_triangles);
     std::iota(b.order.begin(), b.order.end(), 0u);
     b.build(b.alloc(), 0, n_triangles, 0);
-    std::vector<float> tri_leaf(9 * (size_t)n_triangles);
+    std::vector<float> tri_leaf(12 * (size_t)n_triangles, 0.f);
     for (uint32_t i = 0; i < n_triangles; ++i)
-        std::memcpy(&tri_leaf[9 * (size_t)i], &tri[9 * (size_t)b.order[i]], 36);
+        std::memcpy(&tri_leaf[12 * (size_t)i], &tri[9 * (size_t)b.order[i]], 36);
     nrrs_scene* s = new (std::nothrow) nrrs_scene();
     if (!s) return NRRS_ERR_INVALID_ARG;
     s->nt = n_triangles;

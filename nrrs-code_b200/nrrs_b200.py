@@ -731,10 +731,10 @@ def film_resolve(film, n_pixels: int, scale: float, image, stream=0):
            "nrrs_film_resolve")
 
 
-def synth_scene(seed: int, n_boxes: int = 40, size: float = 1.0):
-    """A closed room (white walls, a red and a green wall, an emissive ceiling quad) filled with
-    n_boxes random axis-aligned boxes of random albedo, as numpy arrays: vertices, triangles,
-    tri_material, materials, environment. Deterministic in seed."""
+def synth_scene(seed: int, n_boxes: int = 40, size: float = 1.0, closed: bool = False):
+    """A room (white walls, a red and a green wall, an emissive ceiling quad; open at the front
+    unless closed) filled with n_boxes random axis-aligned boxes of random albedo, as numpy
+    arrays: vertices, triangles, tri_material, materials, environment. Deterministic in seed."""
     import numpy as np
     rng = np.random.default_rng(seed)
     verts, tris, mat = [], [], []
@@ -753,6 +753,8 @@ def synth_scene(seed: int, n_boxes: int = 40, size: float = 1.0):
     quad([0, 0, S], [S, 0, S], [S, S, S], [0, S, S], 0)          # back
     quad([0, 0, 0], [0, 0, S], [0, S, S], [0, S, 0], 1)          # left, red
     quad([S, 0, 0], [S, S, 0], [S, S, S], [S, 0, S], 2)          # right, green
+    if closed:
+        quad([0, 0, 0], [0, S, 0], [S, S, 0], [S, 0, 0], 0)      # front
     c, h = 0.5 * S, 0.12 * S
     quad([c - h, S * 0.999, c - h], [c + h, S * 0.999, c - h], [c + h, S * 0.999, c + h],
          [c - h, S * 0.999, c + h], 3)                           # the light
@@ -774,11 +776,13 @@ def synth_scene(seed: int, n_boxes: int = 40, size: float = 1.0):
             np.asarray([0.05, 0.05, 0.08], np.float32))
 
 
-def room_camera(width: int, height: int, size: float = 1.0) -> Camera:
-    """A camera looking into synth_scene's room through its open front."""
-    return Camera((C.c_float * 3)(0.5 * size, 0.5 * size, -1.3 * size),
+def room_camera(width: int, height: int, size: float = 1.0, inside: bool = False) -> Camera:
+    """A camera looking into synth_scene's room through its open front, or from just inside
+    its front wall."""
+    z, tan = (0.02 * size, 0.75) if inside else (-1.3 * size, 0.42)
+    return Camera((C.c_float * 3)(0.5 * size, 0.5 * size, z),
                   (C.c_float * 3)(0.0, 0.0, 1.0), (C.c_float * 3)(0.0, 1.0, 0.0),
-                  0.42, width, height)
+                  tan, width, height)
 
 
 def calculate_sample_weight(pixel, pixel_samples, n_pixels: int, size_dev, max_n: int, weight,
