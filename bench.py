@@ -1037,7 +1037,9 @@ def run_render(args, rank, world, local_rank):
     cur = torch.cuda.current_stream()
     stream = cur.cuda_stream
     wl = WORKLOADS[args.workload]
-    W, H = (1920, 1080) if wl["n_vert"] == 1920 * 1080 else (wl["n_vert"], 1)
+    n_pix = wl["n_vert"]               # --vertices gives a smaller 16:9 frame for profiling
+    H = 1080 if n_pix == 1920 * 1080 else max(1, int(round((n_pix * 9 / 16) ** 0.5)))
+    W = n_pix // H
     P = W * H
     cap = 3 * P
     v, t, m, ma, env = nb.synth_scene(7 + rank, n_boxes=wl["boxes"], closed=True)
@@ -1075,9 +1077,11 @@ def run_render(args, rank, world, local_rank):
     ev = {}
 
     bounces_run = [0]
+    rays_run = [0, 0]   # closest-hit and shadow rays of the timing frame
 
     def frame(sample, timing=False):
         vertices = 0
+        n_prev = 0
         film.zero_()
         nb.camera_rays(cam, sample, 1234, R, stream)
         n_rays.fill_(P)
@@ -1111,6 +1115,9 @@ def run_render(args, rank, world, local_rank):
             nb.trace_shadow(scene, S, qsize, cap, film, None, stream)
             if timing:
                 ev[("shadow", depth)][1].record(cur)
+                rays_run[0] += P if depth == 0 else n_prev
+                n_prev = int(qsize.item())
+                rays_run[1] += n_prev
             n_rays.copy_(qsize)
         nb.film_resolve(film, P, 1.0, img, stream)
         return vertices
@@ -1145,7 +1152,6 @@ def run_render(args, rank, world, local_rank):
     t_trace = sum(a.elapsed_time(b) for (k, _), (a, b) in ev.items() if k == "trace")
     t_nrrs = sum(a.elapsed_time(b) for (k, _), (a, b) in ev.items() if k == "nrrs")
     t_shadow = sum(a.elapsed_time(b) for (k, _), (a, b) in ev.items() if k == "shadow")
-    rays_traced = verts_per_frame  # closest-hit rays per frame are about the vertices plus misses
     line = {
         "metric": "path vertices/s (path-traced frame around the NRRS step)",
         "value": verts_per_frame * world / (ms * 1e-3), "unit": "vertices/s", "n_gpus": world,
@@ -1160,7 +1166,9 @@ def run_render(args, rank, world, local_rank):
         "clocks": clk.summary(),
         "gpu_launches": launches,
         "calls_ms_per_frame": {"trace": t_trace, "nrrs_step": t_nrrs, "shadow": t_shadow},
-        "rays_per_s_trace": rays_traced / (t_trace * 1e-3) if t_trace else None,
+        "rays_per_frame": {"closest_hit": rays_run[0], "shadow": rays_run[1]},
+        "rays_per_s_trace": rays_run[0] / (t_trace * 1e-3) if t_trace else None,
+        "rays_per_s_shadow": rays_run[1] / (t_shadow * 1e-3) if t_shadow else None,
         "note": "a step is one frame; per bounce the vertex count is read back (as the "
                 "reference reads its queue size) before nrrs_step",
     }

@@ -81,47 +81,55 @@ __device__ __forceinline__ V3 normalize(V3 a) { return divs(a, __fsqrt_rn(dot(a,
 __device__ __forceinline__ void put(float* p, V3 a) { p[0] = a.x; p[1] = a.y; p[2] = a.z; }
 __device__ __forceinline__ bool nonzero(V3 a) { return a.x != 0.f || a.y != 0.f || a.z != 0.f; }
 
-// Moller-Trumbore, two-sided; t in (0, tmax)
-__device__ __forceinline__ bool intersect_v(V3 v0, V3 e1, V3 e2, V3 o, V3 d, float tmax, float* t,
-                                            float* u, float* v) {
-    const V3 pv = cross(d, e2);
-    const float det = dot(e1, pv);
+// the intersection's dot and cross products with fused multiply-adds (each fmaf rounded once; the
+// C restatement calls fmaf in the same order)
+__device__ __forceinline__ float fdot(V3 a, V3 b) {
+    return __fmaf_rn(a.x, b.x, __fmaf_rn(a.y, b.y, __fmul_rn(a.z, b.z)));
+}
+__device__ __forceinline__ V3 fcross(V3 a, V3 b) {
+    return {__fmaf_rn(a.y, b.z, -__fmul_rn(a.z, b.y)), __fmaf_rn(a.z, b.x, -__fmul_rn(a.x, b.z)),
+            __fmaf_rn(a.x, b.y, -__fmul_rn(a.y, b.x))};
+}
+
+// Moller-Trumbore, two-sided; t in (0, tmax) and t <= bound (the closest hit so far: a hit at
+// the same t must still reach the tie rule)
+__device__ __forceinline__ bool intersect_v(V3 v0, V3 e1, V3 e2, V3 o, V3 d, float tmax,
+                                            float bound, float* t, float* u, float* v) {
+    const V3 pv = fcross(d, e2);
+    const float det = fdot(e1, pv);
     if (fabsf(det) < 1e-12f) return false;
     const float inv = __fdiv_rn(1.0f, det);
     const V3 tv = sub(o, v0);
-    const float uu = __fmul_rn(dot(tv, pv), inv);
+    const float uu = __fmul_rn(fdot(tv, pv), inv);
     if (uu < 0.f || uu > 1.f) return false;
-    const V3 qv = cross(tv, e1);
-    const float vv = __fmul_rn(dot(d, qv), inv);
+    const V3 qv = fcross(tv, e1);
+    const float vv = __fmul_rn(fdot(d, qv), inv);
     if (vv < 0.f || __fadd_rn(uu, vv) > 1.f) return false;
-    const float tt = __fmul_rn(dot(e2, qv), inv);
-    if (!(tt > 0.f && tt < tmax)) return false;
+    const float tt = __fmul_rn(fdot(e2, qv), inv);
+    if (!(tt > 0.f && tt < tmax && tt <= bound)) return false;
     *t = tt; *u = uu; *v = vv;
     return true;
 }
 
 // a leaf-order triangle of 12 floats, read as three 16-byte loads
-__device__ __forceinline__ bool intersect_leaf(const float* tri, V3 o, V3 d, float tmax, float* t,
-                                               float* u, float* v) {
+__device__ __forceinline__ bool intersect_leaf(const float* tri, V3 o, V3 d, float tmax,
+                                               float bound, float* t, float* u, float* v) {
     const float4 a = __ldg(reinterpret_cast<const float4*>(tri));
     const float4 b = __ldg(reinterpret_cast<const float4*>(tri) + 1);
     const float4 c = __ldg(reinterpret_cast<const float4*>(tri) + 2);
-    return intersect_v({a.x, a.y, a.z}, {a.w, b.x, b.y}, {b.z, b.w, c.x}, o, d, tmax, t, u, v);
+    return intersect_v({a.x, a.y, a.z}, {a.w, b.x, b.y}, {b.z, b.w, c.x}, o, d, tmax, bound, t, u, v);
 }
 
-// slab test; the interval [t0, t1] of the box along the ray, clipped to [0, tmax]
+// slab test: the interval of the box along the ray, clipped to [0, tmax]. A 0 x inf product (a
+// ray parallel to a slab, starting on its plane) is NaN, which fminf/fmaxf drop; the box is grown
+// at build time, so such a ray cannot reach a triangle inside it and the miss it gives is right.
 __device__ __forceinline__ bool box_hit(float4 lo, float4 hi, V3 o, V3 inv, float tmax,
                                         float* tnear) {
-    float t0 = 0.f, t1 = tmax;
-    const float oo[3] = {o.x, o.y, o.z}, ii[3] = {inv.x, inv.y, inv.z};
-    const float bl[3] = {lo.x, lo.y, lo.z}, bh[3] = {hi.x, hi.y, hi.z};
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        float a = (bl[k] - oo[k]) * ii[k], b = (bh[k] - oo[k]) * ii[k];
-        if (a > b) { const float s = a; a = b; b = s; }
-        t0 = a > t0 ? a : t0;      // NaN (0 x inf) leaves the bound as it was
-        t1 = b < t1 ? b : t1;
-    }
+    const float ax = (lo.x - o.x) * inv.x, bx = (hi.x - o.x) * inv.x;
+    const float ay = (lo.y - o.y) * inv.y, by = (hi.y - o.y) * inv.y;
+    const float az = (lo.z - o.z) * inv.z, bz = (hi.z - o.z) * inv.z;
+    const float t0 = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), 0.f));
+    const float t1 = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fminf(fmaxf(az, bz), tmax));
     *tnear = t0;
     return t0 <= t1;
 }
@@ -129,39 +137,69 @@ __device__ __forceinline__ bool box_hit(float4 lo, float4 hi, V3 o, V3 inv, floa
 struct Hit { uint32_t prim; float t, u, v; };
 
 // closest hit; ties in t go to the lower input index. any = true stops at the first hit.
-template <bool ANY>
-__device__ Hit traverse(const nrrs_scene& s, V3 o, V3 d, float tmax) {
-    Hit h{kMiss, tmax, 0.f, 0.f};
+// Closest hit; ties in t go to the lower input index. Stack traversal, near child first by the
+// sign of the ray on the node's split axis. Each pass of the outer loop first pops nodes until this
+// lane holds a leaf whose box the ray enters (or the stack is empty), then tests that leaf: lanes
+// of a warp reconverge between the two loops, so the triangle tests run with the warp together.
+__device__ Hit closest_hit(const nrrs_scene& s, V3 o, V3 d, float tmax) {
+    Hit h{kMiss, tmax, 0.f, 0.f};   // h.t is the culling bound: tmax until the first hit
     const V3 inv = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+    const float4* nodes = reinterpret_cast<const float4*>(s.nodes);
+    int stack[kStack];
+    int sp = 0;
+    stack[sp++] = 0;
+    for (;;) {
+        uint32_t first = 0, cnt = 0;
+        while (sp > 0) {
+            const float4* nd = nodes + 2 * (size_t)stack[--sp];
+            const float4 lo = __ldg(nd), hi = __ldg(nd + 1);
+            float tn;
+            if (!box_hit(lo, hi, o, inv, h.t, &tn)) continue;
+            const uint32_t lf = __float_as_uint(lo.w), ca = __float_as_uint(hi.w);
+            if (ca & 0xffffu) { first = lf; cnt = ca & 0xffffu; break; }
+            const uint32_t axis = ca >> 16;
+            const float da = axis == 0 ? d.x : (axis == 1 ? d.y : d.z);
+            if (sp + 2 > kStack) continue;   // depth is bounded at build time; never taken
+            if (da < 0.f) { stack[sp++] = (int)lf; stack[sp++] = (int)lf + 1; }
+            else { stack[sp++] = (int)lf + 1; stack[sp++] = (int)lf; }
+        }
+        if (cnt == 0) break;
+        for (uint32_t i = first; i < first + cnt; ++i) {
+            float t, u, v;
+            if (!intersect_leaf(s.tris + 12 * (size_t)i, o, d, tmax, h.t, &t, &u, &v)) continue;
+            const uint32_t id = s.tri_id[i];
+            if (h.prim == kMiss || t < h.t || (t == h.t && id < h.prim)) h = {id, t, u, v};
+        }
+    }
+    return h;
+}
+
+// Any hit in (0, tmax): one node per pass, ending at the first triangle hit.
+__device__ bool any_hit(const nrrs_scene& s, V3 o, V3 d, float tmax) {
+    const V3 inv = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+    const float4* nodes = reinterpret_cast<const float4*>(s.nodes);
     int stack[kStack];
     int sp = 0;
     stack[sp++] = 0;
     while (sp > 0) {
-        const float4* nd = reinterpret_cast<const float4*>(s.nodes) + 2 * (size_t)stack[--sp];
+        const float4* nd = nodes + 2 * (size_t)stack[--sp];
         const float4 lo = __ldg(nd), hi = __ldg(nd + 1);
         float tn;
-        if (!box_hit(lo, hi, o, inv, h.prim == kMiss ? tmax : h.t, &tn)) continue;
+        if (!box_hit(lo, hi, o, inv, tmax, &tn)) continue;
         const uint32_t lf = __float_as_uint(lo.w), ca = __float_as_uint(hi.w);
         const uint32_t cnt = ca & 0xffffu;
         if (cnt) {
             for (uint32_t i = lf; i < lf + cnt; ++i) {
                 float t, u, v;
-                if (!intersect_leaf(s.tris + 12 * (size_t)i, o, d, tmax, &t, &u, &v)) continue;
-                const uint32_t id = s.tri_id[i];
-                if (h.prim == kMiss || t < h.t || (t == h.t && id < h.prim)) h = {id, t, u, v};
-                if (ANY) return h;
+                if (intersect_leaf(s.tris + 12 * (size_t)i, o, d, tmax, tmax, &t, &u, &v)) return true;
             }
         } else {
-            // near child first: by the sign of the ray on the node's split axis
-            const uint32_t axis = ca >> 16;
-            const float da = axis == 0 ? d.x : (axis == 1 ? d.y : d.z);
-            const int first = (int)lf, second = (int)lf + 1;
             if (sp + 2 > kStack) continue;   // depth is bounded at build time; never taken
-            if (da < 0.f) { stack[sp++] = first; stack[sp++] = second; }
-            else { stack[sp++] = second; stack[sp++] = first; }
+            stack[sp++] = (int)lf + 1;
+            stack[sp++] = (int)lf;
         }
     }
-    return h;
+    return false;
 }
 
 __device__ __forceinline__ void film_add(int64_t* film, uint32_t pixel, V3 c) {
@@ -213,7 +251,7 @@ __global__ void __launch_bounds__(128) k_trace(const __grid_constant__ nrrs_scen
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         Hit x{kMiss, 0.f, 0.f, 0.f};
         if (nonzero(v3(r.thp + 3 * (size_t)i)))
-            x = traverse<false>(s, v3(r.origin + 3 * (size_t)i), v3(r.dir + 3 * (size_t)i), INFINITY);
+            x = closest_hit(s, v3(r.origin + 3 * (size_t)i), v3(r.dir + 3 * (size_t)i), INFINITY);
         h.prim[i] = x.prim;
         h.t[i] = x.t;
         h.u[i] = x.u;
@@ -437,9 +475,8 @@ __global__ void __launch_bounds__(128) k_shadow(const __grid_constant__ nrrs_sce
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         V3 c = v3(sh.contrib + 3 * (size_t)j);
         if (nonzero(c)) {
-            const Hit x = traverse<true>(s, v3(sh.origin + 3 * (size_t)j), v3(sh.dir + 3 * (size_t)j),
-                                         sh.tmax[j]);
-            if (x.prim != kMiss) c = {0.f, 0.f, 0.f};
+            if (any_hit(s, v3(sh.origin + 3 * (size_t)j), v3(sh.dir + 3 * (size_t)j), sh.tmax[j]))
+                c = {0.f, 0.f, 0.f};
             else film_add(film, sh.pixel[j], c);
         }
         if (cout) put(cout + 3 * (size_t)j, c);
@@ -600,12 +637,14 @@ cudaError_t upload(T** dst, const T* src, size_t count) {
     return e;
 }
 
-int grid_of(uint32_t n, int threads) {
+// a grid-stride kernel's grid: per_sm CTAs per SM, or fewer when n needs fewer. The traversal
+// kernels take 64: rays differ widely in cost, and many short CTAs let the SMs refill as they end.
+int grid_of(uint32_t n, int threads, int per_sm = 16) {
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess)
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const uint64_t need = ((uint64_t)n + threads - 1) / threads;
-    const uint64_t cap = (uint64_t)sms * 16;
+    const uint64_t cap = (uint64_t)sms * per_sm;
     return (int)std::max<uint64_t>(1, std::min(need, cap));
 }
 
@@ -709,7 +748,8 @@ extern "C" int nrrs_trace(const nrrs_scene* s, const nrrs_ray_soa* rays, const u
                           uint32_t max_n, const nrrs_hit_soa* hits, void* stream) {
     if (!s || !rays || !n_dev || !hits) return NRRS_ERR_INVALID_ARG;
     if (max_n == 0) return NRRS_OK;
-    k_trace<<<grid_of(max_n, 128), 128, 0, (cudaStream_t)stream>>>(*s, *rays, n_dev, max_n, *hits);
+    k_trace<<<grid_of(max_n, 128, 64), 128, 0, (cudaStream_t)stream>>>(*s, *rays, n_dev,
+                                                                                 max_n, *hits);
     return ok(cudaGetLastError());
 }
 
@@ -752,8 +792,8 @@ extern "C" int nrrs_trace_shadow(const nrrs_scene* s, const nrrs_shadow_soa* sha
                                  float* contrib_out, void* stream) {
     if (!s || !shadow || !n_dev || !film) return NRRS_ERR_INVALID_ARG;
     if (max_n == 0) return NRRS_OK;
-    k_shadow<<<grid_of(max_n, 128), 128, 0, (cudaStream_t)stream>>>(*s, *shadow, n_dev, max_n,
-                                                                     film, contrib_out);
+    k_shadow<<<grid_of(max_n, 128, 64), 128, 0, (cudaStream_t)stream>>>(
+        *s, *shadow, n_dev, max_n, film, contrib_out);
     return ok(cudaGetLastError());
 }
 

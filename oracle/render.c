@@ -8,7 +8,8 @@
  * handleEmissiveHit / handleMiss (integrator.cpp:688-735), handleIntersections and
  * generateScatteredRays (:737-887) and generateCameraRays (:889-935), with KiRaRay's diffuse BSDF
  * and area lights. This restatement follows the library's definitions operation by operation (FP32,
- * no contraction), so its results equal the GPU's bit for bit; intersection ties go to the lower
+ * no contraction; the intersection's explicit fmaf calls are the library's __fmaf_rn), so its
+ * results equal the GPU's bit for bit; intersection ties go to the lower
  * triangle index in both, so the BVH does not matter.
  */
 #include <math.h>
@@ -85,19 +86,27 @@ uint32_t oracle_scene_tris(const float* vertices, const uint32_t* tris, uint32_t
     return nl;
 }
 
+/* the intersection's dot and cross products with fused multiply-adds, as the library's (fmaf is
+ * correctly rounded: one rounding per call) */
+static float fdot(v3 a, v3 b) { return fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)); }
+static v3 fcross(v3 a, v3 b) {
+    v3 r = {fmaf(a.y, b.z, -(a.z * b.y)), fmaf(a.z, b.x, -(a.x * b.z)), fmaf(a.x, b.y, -(a.y * b.x))};
+    return r;
+}
+
 static int intersect(const float* tri, v3 o, v3 d, float tmax, float* t, float* u, float* v) {
     const v3 v0 = ld(tri), e1 = ld(tri + 3), e2 = ld(tri + 6);
-    const v3 pv = cross(d, e2);
-    const float det = dot(e1, pv);
+    const v3 pv = fcross(d, e2);
+    const float det = fdot(e1, pv);
     if (fabsf(det) < 1e-12f) return 0;
     const float inv = 1.0f / det;
     const v3 tv = sub(o, v0);
-    const float uu = dot(tv, pv) * inv;
+    const float uu = fdot(tv, pv) * inv;
     if (uu < 0.f || uu > 1.f) return 0;
-    const v3 qv = cross(tv, e1);
-    const float vv = dot(d, qv) * inv;
+    const v3 qv = fcross(tv, e1);
+    const float vv = fdot(d, qv) * inv;
     if (vv < 0.f || uu + vv > 1.f) return 0;
-    const float tt = dot(e2, qv) * inv;
+    const float tt = fdot(e2, qv) * inv;
     if (!(tt > 0.f && tt < tmax)) return 0;
     *t = tt; *u = uu; *v = vv;
     return 1;
