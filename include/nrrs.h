@@ -611,7 +611,7 @@ int nrrs_train_schedule_tick(nrrs_train_schedule* s, double elapsed, double now_
  * A CUDA ray tracer around the NRRS step, in place of the reference's OptiX programs and its
  * scatter step:
  *   trace (closest hit, shadow any-hit)      src/render/nrrs/device.cu:48-161 (OptiX programs)
- *   handleHit / handleMiss                   src/render/nrrs/integrator.cpp:686-735
+ *   handleEmissiveHit / handleMiss           src/render/nrrs/integrator.cpp:688-735
  *   handleIntersections, generateScatteredRays   src/render/nrrs/integrator.cpp:737-887
  *   generateCameraRays                       src/render/nrrs/integrator.cpp:889-935
  * Scenes are triangle meshes with diffuse (Lambertian) materials; emissive triangles are area
@@ -694,11 +694,12 @@ int nrrs_camera_rays(const nrrs_camera* c, uint32_t sample, uint32_t seed,
 int nrrs_trace(const nrrs_scene* s, const nrrs_ray_soa* rays, const uint32_t* n_dev,
                uint32_t max_n, const nrrs_hit_soa* hits, void* stream);
 
-/* handleHit / handleMiss and the vertex queue: for each of the first *n_dev rays, an emissive hit
- * adds Le x thp (MIS-weighted against light sampling when pdf > 0) and a miss adds environment x
- * thp to film[pixel] and contrib[ray] ([max_n][3], 0 otherwise; the ray's node receives it through
- * nrrs_record_radiance). Rays that hit a surface become the vertices out[0 .. *n_out_dev) in ray
- * order. scratch: nrrs_shade_scratch_bytes(max_n) bytes of device memory. */
+/* handleEmissiveHit / handleMiss and the vertex queue: for each of the first *n_dev rays, an
+ * emissive hit adds Le x thp (MIS-weighted against light sampling when pdf > 0) and a miss adds
+ * environment x thp to film[pixel] and contrib[ray] ([max_n][3], 0 otherwise; the ray's node
+ * receives it through nrrs_record_radiance). Rays that hit a surface become the vertices
+ * out[0 .. *n_out_dev) in ray order. scratch: nrrs_shade_scratch_bytes(max_n) bytes of device
+ * memory. */
 uint64_t nrrs_shade_scratch_bytes(uint32_t max_n);
 int nrrs_shade(const nrrs_scene* s, const nrrs_ray_soa* rays, const nrrs_hit_soa* hits,
                const uint32_t* n_dev, uint32_t max_n, uint32_t depth, int64_t* film,

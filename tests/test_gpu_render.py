@@ -74,8 +74,8 @@ def same(a, b, keys):
         assert np.asarray(a[k]).tobytes() == np.asarray(b[k]).tobytes(), k
 
 
-def scene_pair(seed=1, boxes=60):
-    v, t, m, ma, e = nb.synth_scene(seed, n_boxes=boxes)
+def scene_pair(seed=1, boxes=60, closed=False):
+    v, t, m, ma, e = nb.synth_scene(seed, n_boxes=boxes, closed=closed)
     return nb.Scene(v, t, m, ma, e), O.HostScene(v, t, m, ma, e)
 
 
@@ -183,6 +183,44 @@ def test_gpu_frame_matches_oracle():
     img, _ = run_frame_pair(gs, hs, cam, 5, 4,
                             lambda rng, n: rng.uniform(0.3, 2.5, n))
     assert img.mean() > 0
+
+
+def test_gpu_closed_room_frame_matches_oracle():
+    """The render benchmark's kind of scene: a closed room seen from inside, where no ray
+    escapes; five bounces with splitting and killing."""
+    gs, hs = scene_pair(7, boxes=120, closed=True)
+    cam = nb.room_camera(48, 32, inside=True)
+    img, _ = run_frame_pair(gs, hs, cam, 9, 5, lambda rng, n: rng.uniform(0.3, 2.5, n))
+    assert img.mean() > 0
+
+
+def test_gpu_trace_benchmark_scene_matches_brute_force():
+    """The render benchmark's own scene (3000 boxes, 36k triangles, a BVH 20+ levels deep):
+    closest hits of a sample of its 1920x1080 camera rays and of random rays inside the room,
+    against brute force."""
+    torch = torch_cuda()
+    gs, hs = scene_pair(7, boxes=3000, closed=True)
+    nn, nl, depth = gs.info()
+    assert nn > 10000 and depth >= 16
+    cam = nb.room_camera(1920, 1080, inside=True)
+    r_cam = hs.camera_rays(cam, 100, 1234)
+    rng = np.random.default_rng(3)
+    pick = np.sort(rng.choice(1920 * 1080, 3000, replace=False))
+    n = 3000
+    o = rng.uniform(0.02, 0.98, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r_all = {k: np.concatenate([np.asarray(r_cam[k])[pick],
+                                {"origin": o, "dir": d, "thp": np.ones((n, 3), np.float32),
+                                 "pdf": np.zeros(n, np.float32), "pixel": np.zeros(n, np.uint32),
+                                 "node": np.full(n, -1, np.int32)}[k]]) for k in r_cam}
+    rays = dev_dict(r_all)
+    hits = empty_hits(2 * n)
+    cnt = torch.tensor([2 * n], dtype=torch.int32, device="cuda")
+    nb.trace(gs, nb.soa(nb.RaySoA, rays), cnt, 2 * n, nb.soa(nb.HitSoA, hits), stream())
+    want = hs.trace(r_all)
+    same(to_host(hits, 2 * n), want, ("prim", "t", "u", "v"))
+    assert (want["prim"] != 0xffffffff).mean() > 0.99   # closed: (almost) nothing escapes
 
 
 def test_gpu_rrs_keeps_the_image_unbiased():
