@@ -715,6 +715,16 @@ int nrrs_scatter(const nrrs_scene* s, const nrrs_path_vertices* v, const float* 
                  uint32_t depth, uint32_t seed, const nrrs_ray_soa* rays,
                  const nrrs_shadow_soa* shadow, void* stream);
 
+/* handleIntersections, the fixed Russian-roulette branch (integrator.cpp:744-769), for depths
+ * that run no inference (the strategy search's fixed-RR depths): vertex j of the first *n_dev
+ * survives when dimension 31 of its slot's random hash is below rr, its thp divided by rr, and
+ * scatters into slot j of rays and shadow as nrrs_scatter does. A killed vertex leaves slot j
+ * empty (thp 0, contrib 0), which the next trace and shade skip, so the next ray count is *n_dev.
+ * rr in (0, 1]; rr = 1 (the reference's training frames) keeps every vertex. */
+int nrrs_scatter_fixed_rr(const nrrs_scene* s, const nrrs_path_vertices* v, const uint32_t* n_dev,
+                          uint32_t max_n, float rr, uint32_t depth, uint32_t seed,
+                          const nrrs_ray_soa* rays, const nrrs_shadow_soa* shadow, void* stream);
+
 /* The shadow rays of the first *n_dev slots: a visible light adds the slot's contrib to
  * film[pixel] and leaves it in contrib_out ([max_n][3]); an occluded one leaves 0. */
 int nrrs_trace_shadow(const nrrs_scene* s, const nrrs_shadow_soa* shadow, const uint32_t* n_dev,

@@ -45,6 +45,7 @@ constexpr float kOffset = 1e-4f;        // ray origins leave the surface along t
 constexpr int kStack = 64;
 constexpr int kLeafMax = 4;
 constexpr uint32_t kMiss = 0xffffffffu;
+constexpr uint32_t kRRDim = 31;     // hash dimension of the fixed-RR decision
 
 // ---- counter-based random numbers (shared with the C restatement) ----
 // lowbias32 (C. Wellons), a published 32-bit integer hash
@@ -396,6 +397,73 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ nrrs_scen
     }
 }
 
+// generateScatteredRays for vertex x into slot j, with its throughput already divided by the RRS
+// (or fixed RR) factor: one next-event-estimation shadow ray and one BSDF ray
+__device__ __forceinline__ void scatter_one(const nrrs_scene& s, const nrrs_path_vertices& v,
+                                            uint32_t x, uint32_t j, V3 thp, uint32_t depth,
+                                            uint32_t seed, const nrrs_ray_soa& r,
+                                            const nrrs_shadow_soa& sh) {
+    const V3 p = v3(v.pos + 3 * (size_t)x), nn = v3(v.normal + 3 * (size_t)x);
+    const V3 alb = v3(v.albedo + 3 * (size_t)x);
+    const V3 f = mul(alb, kInvPi);
+    const V3 org = add(p, mul(nn, kOffset));
+    const uint32_t px = v.pixel[x];
+    const int node = v.node[x];
+    // next-event estimation: a light by index, a point by area
+    V3 sc = {0.f, 0.f, 0.f}, wl = {0.f, 0.f, 1.f};
+    float dist = 0.f;
+    if (s.nl) {
+        const uint32_t k = min((uint32_t)(rnd(seed, depth, j, 0) * (float)s.nl), s.nl - 1);
+        const uint32_t lt = s.lights[k];
+        const float* tri = s.tri_in + 9 * (size_t)lt;
+        const float su = __fsqrt_rn(rnd(seed, depth, j, 1));
+        const float b1 = __fsub_rn(1.0f, su), b2 = __fmul_rn(rnd(seed, depth, j, 2), su);
+        const V3 q = add(add(v3(tri), mul(v3(tri + 3), b1)), mul(v3(tri + 6), b2));
+        const V3 dv = sub(q, p);
+        const float d2 = dot(dv, dv);
+        dist = __fsqrt_rn(d2);
+        wl = divs(dv, dist);
+        const float cosv = dot(nn, wl);
+        const float cosl = fabsf(dot(normalize(cross(v3(tri + 3), v3(tri + 6))), wl));
+        const V3 le = v3(s.mats + 6 * (size_t)s.tri_mat[lt] + 3);
+        if (cosv > 0.f && cosl > 0.f && nonzero(le) && d2 > 0.f) {
+            const float pl = __fdiv_rn(d2, __fmul_rn(__fmul_rn(cosl, s.light_area[k]), (float)s.nl));
+            const float w = power_heuristic(pl, __fmul_rn(cosv, kInvPi));
+            sc = divs(mul(mul(vmul(vmul(thp, f), le), cosv), w), pl);
+        }
+    }
+    put(sh.origin + 3 * (size_t)j, org);
+    put(sh.dir + 3 * (size_t)j, wl);
+    sh.tmax[j] = __fmul_rn(dist, 0.9999f);
+    put(sh.contrib + 3 * (size_t)j, sc);
+    sh.pixel[j] = px;
+    sh.node[j] = node;
+    // BSDF: cosine-weighted, as normalize(n + a point uniform on the unit sphere), the
+    // sphere point by bounded rejection from the cube
+    V3 sp = {0.f, 0.f, 1.f};
+    for (uint32_t t = 0; t < 8; ++t) {
+        const V3 c = {__fsub_rn(__fmul_rn(rnd(seed, depth, j, 3 + 3 * t), 2.0f), 1.0f),
+                      __fsub_rn(__fmul_rn(rnd(seed, depth, j, 4 + 3 * t), 2.0f), 1.0f),
+                      __fsub_rn(__fmul_rn(rnd(seed, depth, j, 5 + 3 * t), 2.0f), 1.0f)};
+        const float c2 = dot(c, c);
+        if (c2 <= 1.0f && c2 > 1e-6f) {
+            sp = divs(c, __fsqrt_rn(c2));
+            break;
+        }
+    }
+    V3 d = add(nn, sp);
+    const float l2 = dot(d, d);
+    d = l2 > 1e-12f ? divs(d, __fsqrt_rn(l2)) : nn;
+    const float pdf = __fmul_rn(dot(nn, d), kInvPi);
+    const V3 tn = pdf > 0.f ? vmul(thp, alb) : V3{0.f, 0.f, 0.f};
+    put(r.origin + 3 * (size_t)j, org);
+    put(r.dir + 3 * (size_t)j, d);
+    put(r.thp + 3 * (size_t)j, tn);
+    r.pdf[j] = pdf > 0.f ? pdf : 0.f;
+    r.pixel[j] = px;
+    r.node[j] = node;
+}
+
 __global__ void __launch_bounds__(128) k_scatter(const __grid_constant__ nrrs_scene s,
                                                  nrrs_path_vertices v, const float* rrs_norm,
                                                  const uint32_t* queue, const uint32_t* q_dev,
@@ -405,66 +473,37 @@ __global__ void __launch_bounds__(128) k_scatter(const __grid_constant__ nrrs_sc
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         const uint32_t x = queue[j];
         const float rr = rrs_norm[x];
-        const V3 thp = divs(v3(v.thp + 3 * (size_t)x), rr);   // sitem.mThp /= sitem.mRRS
-        const V3 p = v3(v.pos + 3 * (size_t)x), nn = v3(v.normal + 3 * (size_t)x);
-        const V3 alb = v3(v.albedo + 3 * (size_t)x);
-        const V3 f = mul(alb, kInvPi);
-        const V3 org = add(p, mul(nn, kOffset));
-        const uint32_t px = v.pixel[x];
-        const int node = v.node[x];
-        // next-event estimation: a light by index, a point by area
-        V3 sc = {0.f, 0.f, 0.f}, wl = {0.f, 0.f, 1.f};
-        float dist = 0.f;
-        if (s.nl) {
-            const uint32_t k = min((uint32_t)(rnd(seed, depth, j, 0) * (float)s.nl), s.nl - 1);
-            const uint32_t lt = s.lights[k];
-            const float* tri = s.tri_in + 9 * (size_t)lt;
-            const float su = __fsqrt_rn(rnd(seed, depth, j, 1));
-            const float b1 = __fsub_rn(1.0f, su), b2 = __fmul_rn(rnd(seed, depth, j, 2), su);
-            const V3 q = add(add(v3(tri), mul(v3(tri + 3), b1)), mul(v3(tri + 6), b2));
-            const V3 dv = sub(q, p);
-            const float d2 = dot(dv, dv);
-            dist = __fsqrt_rn(d2);
-            wl = divs(dv, dist);
-            const float cosv = dot(nn, wl);
-            const float cosl = fabsf(dot(normalize(cross(v3(tri + 3), v3(tri + 6))), wl));
-            const V3 le = v3(s.mats + 6 * (size_t)s.tri_mat[lt] + 3);
-            if (cosv > 0.f && cosl > 0.f && nonzero(le) && d2 > 0.f) {
-                const float pl = __fdiv_rn(d2, __fmul_rn(__fmul_rn(cosl, s.light_area[k]), (float)s.nl));
-                const float w = power_heuristic(pl, __fmul_rn(cosv, kInvPi));
-                sc = divs(mul(mul(vmul(vmul(thp, f), le), cosv), w), pl);
-            }
+        // sitem.mThp /= sitem.mRRS
+        scatter_one(s, v, x, j, divs(v3(v.thp + 3 * (size_t)x), rr), depth, seed, r, sh);
+    }
+}
+
+// the fixed Russian-roulette branch: vertex j survives when its uniform number (dimension 31 of
+// the slot's hash) is below rr, with thp / rr; a killed vertex leaves an empty slot
+__global__ void __launch_bounds__(128) k_scatter_fixed_rr(const __grid_constant__ nrrs_scene s,
+                                                          nrrs_path_vertices v, const uint32_t* n_dev,
+                                                          uint32_t max_n, float rr, uint32_t depth,
+                                                          uint32_t seed, nrrs_ray_soa r,
+                                                          nrrs_shadow_soa sh) {
+    const uint32_t n = min(*n_dev, max_n);
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        if (rnd(seed, depth, j, kRRDim) < rr) {
+            scatter_one(s, v, j, j, divs(v3(v.thp + 3 * (size_t)j), rr), depth, seed, r, sh);
+            continue;
         }
-        put(sh.origin + 3 * (size_t)j, org);
-        put(sh.dir + 3 * (size_t)j, wl);
-        sh.tmax[j] = __fmul_rn(dist, 0.9999f);
-        put(sh.contrib + 3 * (size_t)j, sc);
-        sh.pixel[j] = px;
-        sh.node[j] = node;
-        // BSDF: cosine-weighted, as normalize(n + a point uniform on the unit sphere), the
-        // sphere point by bounded rejection from the cube
-        V3 sp = {0.f, 0.f, 1.f};
-        for (uint32_t t = 0; t < 8; ++t) {
-            const V3 c = {__fsub_rn(__fmul_rn(rnd(seed, depth, j, 3 + 3 * t), 2.0f), 1.0f),
-                          __fsub_rn(__fmul_rn(rnd(seed, depth, j, 4 + 3 * t), 2.0f), 1.0f),
-                          __fsub_rn(__fmul_rn(rnd(seed, depth, j, 5 + 3 * t), 2.0f), 1.0f)};
-            const float c2 = dot(c, c);
-            if (c2 <= 1.0f && c2 > 1e-6f) {
-                sp = divs(c, __fsqrt_rn(c2));
-                break;
-            }
-        }
-        V3 d = add(nn, sp);
-        const float l2 = dot(d, d);
-        d = l2 > 1e-12f ? divs(d, __fsqrt_rn(l2)) : nn;
-        const float pdf = __fmul_rn(dot(nn, d), kInvPi);
-        const V3 tn = pdf > 0.f ? vmul(thp, alb) : V3{0.f, 0.f, 0.f};
-        put(r.origin + 3 * (size_t)j, org);
-        put(r.dir + 3 * (size_t)j, d);
-        put(r.thp + 3 * (size_t)j, tn);
-        r.pdf[j] = pdf > 0.f ? pdf : 0.f;
-        r.pixel[j] = px;
-        r.node[j] = node;
+        const V3 zero = {0.f, 0.f, 0.f}, up = {0.f, 0.f, 1.f};
+        put(sh.origin + 3 * (size_t)j, zero);
+        put(sh.dir + 3 * (size_t)j, up);
+        sh.tmax[j] = 0.f;
+        put(sh.contrib + 3 * (size_t)j, zero);
+        sh.pixel[j] = v.pixel[j];
+        sh.node[j] = v.node[j];
+        put(r.origin + 3 * (size_t)j, zero);
+        put(r.dir + 3 * (size_t)j, up);
+        put(r.thp + 3 * (size_t)j, zero);
+        r.pdf[j] = 0.f;
+        r.pixel[j] = v.pixel[j];
+        r.node[j] = v.node[j];
     }
 }
 
@@ -784,6 +823,18 @@ extern "C" int nrrs_scatter(const nrrs_scene* s, const nrrs_path_vertices* v, co
     if (max_queue == 0) return NRRS_OK;
     k_scatter<<<grid_of(max_queue, 128), 128, 0, (cudaStream_t)stream>>>(
         *s, *v, rrs_norm, queue, queue_size_dev, max_queue, depth, seed, *rays, *shadow);
+    return ok(cudaGetLastError());
+}
+
+extern "C" int nrrs_scatter_fixed_rr(const nrrs_scene* s, const nrrs_path_vertices* v,
+                                     const uint32_t* n_dev, uint32_t max_n, float rr,
+                                     uint32_t depth, uint32_t seed, const nrrs_ray_soa* rays,
+                                     const nrrs_shadow_soa* shadow, void* stream) {
+    if (!s || !v || !n_dev || !rays || !shadow || !(rr > 0.f && rr <= 1.f))
+        return NRRS_ERR_INVALID_ARG;
+    if (max_n == 0) return NRRS_OK;
+    k_scatter_fixed_rr<<<grid_of(max_n, 128), 128, 0, (cudaStream_t)stream>>>(
+        *s, *v, n_dev, max_n, rr, depth, seed, *rays, *shadow);
     return ok(cudaGetLastError());
 }
 

@@ -272,6 +272,9 @@ _SIGS = {
     "nrrs_scatter": (C.c_int, [C.c_void_p, C.POINTER(PathVertices), C.c_void_p, C.c_void_p,
                                C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(RaySoA),
                                C.POINTER(ShadowSoA), C.c_void_p]),
+    "nrrs_scatter_fixed_rr": (C.c_int, [C.c_void_p, C.POINTER(PathVertices), C.c_void_p,
+                                        C.c_uint32, C.c_float, C.c_uint32, C.c_uint32,
+                                        C.POINTER(RaySoA), C.POINTER(ShadowSoA), C.c_void_p]),
     "nrrs_trace_shadow": (C.c_int, [C.c_void_p, C.POINTER(ShadowSoA), C.c_void_p, C.c_uint32,
                                     C.c_void_p, C.c_void_p, C.c_void_p]),
     "nrrs_film_resolve": (C.c_int, [C.c_void_p, C.c_uint32, C.c_float, C.c_void_p, C.c_void_p]),
@@ -718,6 +721,15 @@ def scatter(scene: Scene, v: PathVertices, rrs_norm, queue, queue_size_dev, max_
     _check(lib().nrrs_scatter(scene._h, C.byref(v), _ptr(rrs_norm), _ptr(queue),
                               _ptr(queue_size_dev), max_queue, depth, seed, C.byref(rays),
                               C.byref(shadow), stream), "nrrs_scatter")
+
+
+def scatter_fixed_rr(scene: Scene, v: PathVertices, n_dev, max_n: int, rr: float, depth: int,
+                     seed: int, rays: RaySoA, shadow: ShadowSoA, stream=0):
+    """The fixed Russian-roulette branch of handleIntersections (depths without inference):
+    slot j keeps vertex j with probability rr, thp / rr; a killed vertex leaves an empty slot."""
+    _check(lib().nrrs_scatter_fixed_rr(scene._h, C.byref(v), _ptr(n_dev), max_n, rr, depth, seed,
+                                       C.byref(rays), C.byref(shadow), stream),
+           "nrrs_scatter_fixed_rr")
 
 
 def trace_shadow(scene: Scene, shadow: ShadowSoA, n_dev, max_n: int, film, contrib_out,

@@ -135,6 +135,14 @@ void oracle_scatter(const float* tri, const uint32_t* mat, const float* mats, ui
                     float* r_thp, float* r_pdf, uint32_t* r_pixel, int32_t* r_node,
                     float* s_origin, float* s_dir, float* s_tmax, float* s_contrib,
                     uint32_t* s_pixel, int32_t* s_node);
+void oracle_scatter_fixed_rr(const float* tri, const uint32_t* mat, const float* mats,
+                             const uint32_t* lights, const float* area, uint32_t nl,
+                             const float* pos, const float* nrm, const float* alb,
+                             const float* thp, const uint32_t* pixel, const int32_t* node,
+                             uint32_t n, float rr, uint32_t depth, uint32_t seed, float* r_origin,
+                             float* r_dir, float* r_thp, float* r_pdf, uint32_t* r_pixel,
+                             int32_t* r_node, float* s_origin, float* s_dir, float* s_tmax,
+                             float* s_contrib, uint32_t* s_pixel, int32_t* s_node);
 void oracle_shadow(const float* tri, uint32_t nt, const float* origin, const float* dir,
                    const float* tmax, const float* contrib, const uint32_t* pixel, uint32_t n,
                    int64_t* film, float* cout);

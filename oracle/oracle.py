@@ -492,6 +492,26 @@ class HostScene:
           *(sh[k].ctypes.data for k in ("origin", "dir", "tmax", "contrib", "pixel", "node")))
         return r, sh
 
+    def scatter_fixed_rr(self, v: dict, rr: float, depth: int, seed: int):
+        n = len(v["pixel"])
+        r = {"origin": np.zeros((n, 3), np.float32), "dir": np.zeros((n, 3), np.float32),
+             "thp": np.zeros((n, 3), np.float32), "pdf": np.zeros(n, np.float32),
+             "pixel": np.zeros(n, np.uint32), "node": np.zeros(n, np.int32)}
+        sh = {"origin": np.zeros((n, 3), np.float32), "dir": np.zeros((n, 3), np.float32),
+              "tmax": np.zeros(n, np.float32), "contrib": np.zeros((n, 3), np.float32),
+              "pixel": np.zeros(n, np.uint32), "node": np.zeros(n, np.int32)}
+        f = lib().oracle_scatter_fixed_rr
+        f.argtypes = [C.c_void_p] * 5 + [C.c_uint32] + [C.c_void_p] * 6 + \
+            [C.c_uint32, C.c_float, C.c_uint32, C.c_uint32] + [C.c_void_p] * 12
+        f(self.tri.ctypes.data, self.tm.ctypes.data, self.mats.ctypes.data,
+          self.lights.ctypes.data, self.area.ctypes.data, self.nl,
+          *(np.ascontiguousarray(v[k]).ctypes.data for k in ("pos", "normal", "albedo", "thp",
+                                                             "pixel", "node")),
+          n, rr, depth, seed,
+          *(r[k].ctypes.data for k in ("origin", "dir", "thp", "pdf", "pixel", "node")),
+          *(sh[k].ctypes.data for k in ("origin", "dir", "tmax", "contrib", "pixel", "node")))
+        return r, sh
+
     def shadow(self, sh: dict, film):
         n = len(sh["pixel"])
         cout = np.zeros((n, 3), np.float32)

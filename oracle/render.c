@@ -20,6 +20,7 @@
 
 #define INV_PI 0.318309886183790671f
 #define OFFSET 1e-4f
+#define RR_DIM 31u   /* hash dimension of the fixed-RR decision */
 #define MISS 0xffffffffu
 #define FIXED_MAX_R 4611686018427387904.0f
 
@@ -230,6 +231,96 @@ uint32_t oracle_shade(const float* tri, const uint32_t* mat, const float* mats, 
     return m;
 }
 
+/* the scene arrays of the scatter steps */
+typedef struct {
+    const float* tri;
+    const uint32_t* mat;
+    const float* mats;
+    const uint32_t* lights;
+    const float* area;
+    uint32_t nl;
+} lights_t;
+
+/* the output arrays of the scatter steps */
+typedef struct {
+    float *r_origin, *r_dir, *r_thp, *r_pdf;
+    uint32_t* r_pixel;
+    int32_t* r_node;
+    float *s_origin, *s_dir, *s_tmax, *s_contrib;
+    uint32_t* s_pixel;
+    int32_t* s_node;
+} scatter_out_t;
+
+/* generateScatteredRays for vertex x into slot j with its throughput already divided */
+static void scatter_one(const lights_t* L, const float* pos, const float* nrm, const float* alb,
+                        const uint32_t* pixel, const int32_t* node, uint32_t x, uint32_t j, v3 th,
+                        uint32_t depth, uint32_t seed, const scatter_out_t* o) {
+    const float* tri = L->tri;
+    const uint32_t* mat = L->mat;
+    const float* mats = L->mats;
+    const uint32_t* lights = L->lights;
+    const float* area = L->area;
+    const uint32_t nl = L->nl;
+    float *r_origin = o->r_origin, *r_dir = o->r_dir, *r_thp = o->r_thp, *r_pdf = o->r_pdf;
+    uint32_t* r_pixel = o->r_pixel;
+    int32_t* r_node = o->r_node;
+    float *s_origin = o->s_origin, *s_dir = o->s_dir, *s_tmax = o->s_tmax, *s_contrib = o->s_contrib;
+    uint32_t* s_pixel = o->s_pixel;
+    int32_t* s_node = o->s_node;
+    const v3 p = ld(pos + 3 * (uint64_t)x), nn = ld(nrm + 3 * (uint64_t)x);
+    const v3 al = ld(alb + 3 * (uint64_t)x);
+    const v3 f = mul(al, INV_PI);
+    const v3 org = add(p, mul(nn, OFFSET));
+    v3 sc = {0.f, 0.f, 0.f}, wl = {0.f, 0.f, 1.f};
+    float dist = 0.f;
+    if (nl) {
+        uint32_t k = (uint32_t)(rnd(seed, depth, j, 0) * (float)nl);
+        if (k > nl - 1) k = nl - 1;
+        const uint32_t lt = lights[k];
+        const float* tr = tri + 9 * (uint64_t)lt;
+        const float su = sqrtf(rnd(seed, depth, j, 1));
+        const float b1 = 1.0f - su, b2 = rnd(seed, depth, j, 2) * su;
+        const v3 q = add(add(ld(tr), mul(ld(tr + 3), b1)), mul(ld(tr + 6), b2));
+        const v3 dv = sub(q, p);
+        const float d2 = dot(dv, dv);
+        dist = sqrtf(d2);
+        wl = divs(dv, dist);
+        const float cosv = dot(nn, wl);
+        const float cosl = fabsf(dot(normalize(cross(ld(tr + 3), ld(tr + 6))), wl));
+        const v3 le = ld(mats + 6 * (uint64_t)mat[lt] + 3);
+        if (cosv > 0.f && cosl > 0.f && nonzero(le) && d2 > 0.f) {
+            const float pl = d2 / ((cosl * area[k]) * (float)nl);
+            const float w = power_heuristic(pl, cosv * INV_PI);
+            sc = divs(mul(mul(vmul(vmul(th, f), le), cosv), w), pl);
+        }
+    }
+    st(s_origin + 3 * (uint64_t)j, org);
+    st(s_dir + 3 * (uint64_t)j, wl);
+    s_tmax[j] = dist * 0.9999f;
+    st(s_contrib + 3 * (uint64_t)j, sc);
+    s_pixel[j] = pixel[x];
+    s_node[j] = node[x];
+    v3 sp = {0.f, 0.f, 1.f};
+    for (uint32_t t = 0; t < 8; ++t) {
+        const v3 c = {rnd(seed, depth, j, 3 + 3 * t) * 2.0f - 1.0f,
+                      rnd(seed, depth, j, 4 + 3 * t) * 2.0f - 1.0f,
+                      rnd(seed, depth, j, 5 + 3 * t) * 2.0f - 1.0f};
+        const float c2 = dot(c, c);
+        if (c2 <= 1.0f && c2 > 1e-6f) { sp = divs(c, sqrtf(c2)); break; }
+    }
+    v3 d = add(nn, sp);
+    const float l2 = dot(d, d);
+    d = l2 > 1e-12f ? divs(d, sqrtf(l2)) : nn;
+    const float pdf = dot(nn, d) * INV_PI;
+    const v3 zero = {0.f, 0.f, 0.f};
+    st(r_origin + 3 * (uint64_t)j, org);
+    st(r_dir + 3 * (uint64_t)j, d);
+    st(r_thp + 3 * (uint64_t)j, pdf > 0.f ? vmul(th, al) : zero);
+    r_pdf[j] = pdf > 0.f ? pdf : 0.f;
+    r_pixel[j] = pixel[x];
+    r_node[j] = node[x];
+}
+
 /* handleIntersections (RRS branch) + generateScatteredRays for queue entries [0, nq) */
 void oracle_scatter(const float* tri, const uint32_t* mat, const float* mats, uint32_t nt,
                     const uint32_t* lights, const float* area, uint32_t nl, const float* pos,
@@ -240,61 +331,49 @@ void oracle_scatter(const float* tri, const uint32_t* mat, const float* mats, ui
                     float* s_origin, float* s_dir, float* s_tmax, float* s_contrib,
                     uint32_t* s_pixel, int32_t* s_node) {
     (void)nt;
+    const lights_t L = {tri, mat, mats, lights, area, nl};
+    const scatter_out_t o = {r_origin, r_dir, r_thp, r_pdf, r_pixel, r_node,
+                             s_origin, s_dir, s_tmax, s_contrib, s_pixel, s_node};
     for (uint32_t j = 0; j < nq; ++j) {
         const uint32_t x = queue[j];
         const v3 th = divs(ld(thp + 3 * (uint64_t)x), rrs_norm[x]);
-        const v3 p = ld(pos + 3 * (uint64_t)x), nn = ld(nrm + 3 * (uint64_t)x);
-        const v3 al = ld(alb + 3 * (uint64_t)x);
-        const v3 f = mul(al, INV_PI);
-        const v3 org = add(p, mul(nn, OFFSET));
-        v3 sc = {0.f, 0.f, 0.f}, wl = {0.f, 0.f, 1.f};
-        float dist = 0.f;
-        if (nl) {
-            uint32_t k = (uint32_t)(rnd(seed, depth, j, 0) * (float)nl);
-            if (k > nl - 1) k = nl - 1;
-            const uint32_t lt = lights[k];
-            const float* tr = tri + 9 * (uint64_t)lt;
-            const float su = sqrtf(rnd(seed, depth, j, 1));
-            const float b1 = 1.0f - su, b2 = rnd(seed, depth, j, 2) * su;
-            const v3 q = add(add(ld(tr), mul(ld(tr + 3), b1)), mul(ld(tr + 6), b2));
-            const v3 dv = sub(q, p);
-            const float d2 = dot(dv, dv);
-            dist = sqrtf(d2);
-            wl = divs(dv, dist);
-            const float cosv = dot(nn, wl);
-            const float cosl = fabsf(dot(normalize(cross(ld(tr + 3), ld(tr + 6))), wl));
-            const v3 le = ld(mats + 6 * (uint64_t)mat[lt] + 3);
-            if (cosv > 0.f && cosl > 0.f && nonzero(le) && d2 > 0.f) {
-                const float pl = d2 / ((cosl * area[k]) * (float)nl);
-                const float w = power_heuristic(pl, cosv * INV_PI);
-                sc = divs(mul(mul(vmul(vmul(th, f), le), cosv), w), pl);
-            }
+        scatter_one(&L, pos, nrm, alb, pixel, node, x, j, th, depth, seed, &o);
+    }
+}
+
+/* handleIntersections' fixed Russian-roulette branch (integrator.cpp:744-769): vertex j survives
+ * when dimension 31 of its slot's hash is below rr, with thp / rr; a killed vertex leaves an
+ * empty slot (zero origin and throughput, direction +z, pixel and node kept) */
+void oracle_scatter_fixed_rr(const float* tri, const uint32_t* mat, const float* mats,
+                             const uint32_t* lights, const float* area, uint32_t nl,
+                             const float* pos, const float* nrm, const float* alb,
+                             const float* thp, const uint32_t* pixel, const int32_t* node,
+                             uint32_t n, float rr, uint32_t depth, uint32_t seed, float* r_origin,
+                             float* r_dir, float* r_thp, float* r_pdf, uint32_t* r_pixel,
+                             int32_t* r_node, float* s_origin, float* s_dir, float* s_tmax,
+                             float* s_contrib, uint32_t* s_pixel, int32_t* s_node) {
+    const lights_t L = {tri, mat, mats, lights, area, nl};
+    const scatter_out_t o = {r_origin, r_dir, r_thp, r_pdf, r_pixel, r_node,
+                             s_origin, s_dir, s_tmax, s_contrib, s_pixel, s_node};
+    const v3 zero = {0.f, 0.f, 0.f}, up = {0.f, 0.f, 1.f};
+    for (uint32_t j = 0; j < n; ++j) {
+        if (rnd(seed, depth, j, RR_DIM) < rr) {
+            scatter_one(&L, pos, nrm, alb, pixel, node, j, j, divs(ld(thp + 3 * (uint64_t)j), rr),
+                        depth, seed, &o);
+            continue;
         }
-        st(s_origin + 3 * (uint64_t)j, org);
-        st(s_dir + 3 * (uint64_t)j, wl);
-        s_tmax[j] = dist * 0.9999f;
-        st(s_contrib + 3 * (uint64_t)j, sc);
-        s_pixel[j] = pixel[x];
-        s_node[j] = node[x];
-        v3 sp = {0.f, 0.f, 1.f};
-        for (uint32_t t = 0; t < 8; ++t) {
-            const v3 c = {rnd(seed, depth, j, 3 + 3 * t) * 2.0f - 1.0f,
-                          rnd(seed, depth, j, 4 + 3 * t) * 2.0f - 1.0f,
-                          rnd(seed, depth, j, 5 + 3 * t) * 2.0f - 1.0f};
-            const float c2 = dot(c, c);
-            if (c2 <= 1.0f && c2 > 1e-6f) { sp = divs(c, sqrtf(c2)); break; }
-        }
-        v3 d = add(nn, sp);
-        const float l2 = dot(d, d);
-        d = l2 > 1e-12f ? divs(d, sqrtf(l2)) : nn;
-        const float pdf = dot(nn, d) * INV_PI;
-        const v3 zero = {0.f, 0.f, 0.f};
-        st(r_origin + 3 * (uint64_t)j, org);
-        st(r_dir + 3 * (uint64_t)j, d);
-        st(r_thp + 3 * (uint64_t)j, pdf > 0.f ? vmul(th, al) : zero);
-        r_pdf[j] = pdf > 0.f ? pdf : 0.f;
-        r_pixel[j] = pixel[x];
-        r_node[j] = node[x];
+        st(s_origin + 3 * (uint64_t)j, zero);
+        st(s_dir + 3 * (uint64_t)j, up);
+        s_tmax[j] = 0.f;
+        st(s_contrib + 3 * (uint64_t)j, zero);
+        s_pixel[j] = pixel[j];
+        s_node[j] = node[j];
+        st(r_origin + 3 * (uint64_t)j, zero);
+        st(r_dir + 3 * (uint64_t)j, up);
+        st(r_thp + 3 * (uint64_t)j, zero);
+        r_pdf[j] = 0.f;
+        r_pixel[j] = pixel[j];
+        r_node[j] = node[j];
     }
 }
 

@@ -1,8 +1,9 @@
 """GPU parity of the wavefront steps around the NRRS step (nrrs_camera_rays, nrrs_trace,
-nrrs_shade, nrrs_scatter, nrrs_trace_shadow, nrrs_film_resolve) against the C restatement, bit
-for bit: BVH closest hits against brute force on camera rays and random rays, a whole frame of
-four bounces with the emitted queue of the library's decision between them, and the film. Also
-checks that splitting and killing by the RRS factors leave the image unbiased."""
+nrrs_shade, nrrs_scatter, nrrs_scatter_fixed_rr, nrrs_trace_shadow, nrrs_film_resolve) against
+the C restatement, bit for bit: BVH closest hits against brute force on camera rays and random
+rays, whole frames with the emitted queue of the library's decision (or fixed Russian roulette)
+between bounces, and the film. Also checks that splitting and killing by the RRS factors leave
+the image unbiased."""
 from __future__ import annotations
 
 import ctypes as C
@@ -112,10 +113,11 @@ def test_gpu_trace_matches_brute_force():
     assert (want["prim"] != 0xffffffff).mean() > 0.5
 
 
-def run_frame_pair(gs, hs, cam, seed, bounces, factors):
+def run_frame_pair(gs, hs, cam, seed, bounces, factors, fixed_rr=None):
     """One frame on the GPU and in the oracle, bounce by bounce, with the emitted queue of the
-    library's decision (nrrs_decide_emit_noalloc) on the given factor generator between them;
-    every array compared as it is produced. Returns both films."""
+    library's decision (nrrs_decide_emit_noalloc) on the given factor generator between them, or
+    at the depths in fixed_rr ({depth: rr}) the fixed Russian-roulette scatter; every array
+    compared as it is produced. Returns both films."""
     torch = torch_cuda()
     n = cam.width * cam.height
     cap = 4 * n
@@ -150,6 +152,22 @@ def run_frame_pair(gs, hs, cam, seed, bounces, factors):
         assert host(film).tobytes() == hfilm.tobytes()
         if nv == 0:
             break
+        if fixed_rr and depth in fixed_rr:
+            rr = fixed_rr[depth]
+            nb.scatter_fixed_rr(gs, nb.soa(nb.PathVertices, verts), n_vert, cap, rr, depth, seed,
+                                nb.soa(nb.RaySoA, rays), nb.soa(nb.ShadowSoA, shadow), stream())
+            hr, hsh = hs.scatter_fixed_rr(hv, rr, depth, seed)
+            same(to_host(rays, nv), hr, ("origin", "dir", "thp", "pdf", "pixel", "node"))
+            same(to_host(shadow, nv), hsh, ("origin", "dir", "tmax", "contrib", "pixel", "node"))
+            kept = (hr["thp"] != 0).any(axis=1).mean()
+            assert rr == 1.0 or 0.0 < kept < 1.0
+            nb.trace_shadow(gs, nb.soa(nb.ShadowSoA, shadow), n_vert, cap, film, scontrib,
+                            stream())
+            hco = hs.shadow(hsh, hfilm)
+            assert host(scontrib)[:nv].tobytes() == hco.tobytes()
+            assert host(film).tobytes() == hfilm.tobytes()
+            n_rays.copy_(n_vert)
+            continue
         # the emitted queue: the library's decision on synthetic factors (as nrrs_step would)
         f = factors(rng, nv).astype(np.float32)
         rnd = rng.uniform(size=nv).astype(np.float32)
@@ -192,6 +210,29 @@ def test_gpu_closed_room_frame_matches_oracle():
     cam = nb.room_camera(48, 32, inside=True)
     img, _ = run_frame_pair(gs, hs, cam, 9, 5, lambda rng, n: rng.uniform(0.3, 2.5, n))
     assert img.mean() > 0
+
+
+def test_gpu_fixed_rr_depths_match_oracle():
+    """Depths that run no inference (the strategy search's fixed-RR depths) scatter through the
+    fixed Russian-roulette branch; mixed with RRS depths in one frame, bit for bit, including a
+    training-style rr = 1 depth that keeps every vertex."""
+    gs, hs = scene_pair(5, boxes=50)
+    cam = nb.room_camera(56, 40)
+    img, _ = run_frame_pair(gs, hs, cam, 13, 5, lambda rng, n: rng.uniform(0.3, 2.5, n),
+                            fixed_rr={0: 0.8, 2: 1.0, 3: 0.55})
+    assert img.mean() > 0
+
+
+def test_gpu_scatter_fixed_rr_rejects_bad_rr():
+    torch_cuda()
+    gs, _ = scene_pair(5, boxes=5)
+    n = 16
+    verts, rays, shadow = empty_vertices(n), empty_rays(n), empty_shadow(n)
+    cnt = torch_cuda().tensor([n], dtype=torch_cuda().int32, device="cuda")
+    for rr in (0.0, -0.5, 1.5, float("nan")):
+        with pytest.raises(nb.NRRSError):
+            nb.scatter_fixed_rr(gs, nb.soa(nb.PathVertices, verts), cnt, n, rr, 0, 1,
+                                nb.soa(nb.RaySoA, rays), nb.soa(nb.ShadowSoA, shadow), stream())
 
 
 def test_gpu_trace_benchmark_scene_matches_brute_force():
