@@ -1,0 +1,139 @@
+"""A whole training frame through the library, as the reference's integrator runs one
+(renderInternal<true>, integrator.cpp:1485-1644, with trainStep's data side, :2572-2605): camera
+rays; per bounce trace, shade, the emitted radiance recorded at the rays' nodes, the decision on
+the vertices, the vertices recorded as path nodes (in place on their node indices), scatter,
+shadow rays and their radiance recorded; then the training batch from the nodes and the rendered
+image, the per-pixel sample counts and the sample weights. The same frame runs in the C
+restatement (HostScene + HostNodes), and every node field, the batch, the counts and the weights
+must agree bit for bit. The GPU batch then feeds the training step, whose losses must equal the
+oracle's on the oracle's batch."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import nrrs_b200 as nb
+import oracle as O
+from gpu_util import host, make_net, random_params, stream, torch_cuda
+from test_gpu_records import NODE_FIELDS, GpuNodes, assert_same_batch
+from test_gpu_render import (empty_hits, empty_rays, empty_shadow, empty_vertices, same,
+                             scene_pair, to_host)
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("closed", [False, True], ids=["open", "closed"])
+def test_gpu_training_frame_matches_oracle(closed):
+    torch = torch_cuda()
+    gs, hs = scene_pair(11, boxes=60, closed=closed)
+    cam = nb.room_camera(48, 36, inside=closed)
+    n = cam.width * cam.height
+    cap = 4 * n
+    bounces, seed = 4, 21
+    node_cap = 12 * n
+    g = GpuNodes(node_cap, cap)
+    hn = O.HostNodes(node_cap)
+
+    film = torch.zeros((n, 9), dtype=torch.int64, device="cuda")
+    hfilm = np.zeros((n, 9), np.int64)
+    rays, hits = empty_rays(cap), empty_hits(cap)
+    verts, shadow = empty_vertices(cap), empty_shadow(cap)
+    contrib = torch.zeros((cap, 3), device="cuda")
+    scontrib = torch.zeros((cap, 3), device="cuda")
+    scratch = torch.zeros(nb.shade_scratch_bytes(cap), dtype=torch.uint8, device="cuda")
+    n_rays = torch.tensor([n], dtype=torch.int32, device="cuda")
+    n_vert = torch.zeros(1, dtype=torch.int32, device="cuda")
+    qsize = torch.zeros(1, dtype=torch.int32, device="cuda")
+    queue = torch.zeros(cap, dtype=torch.int32, device="cuda")
+    rrs_norm = torch.zeros(cap, device="cuda")
+    nb.camera_rays(cam, 0, seed, nb.soa(nb.RaySoA, rays), stream())
+    hr = hs.camera_rays(cam, 0, seed)
+    dp = nb.default_decide(clamp_max=4.0)
+    rng = np.random.default_rng(seed)
+    recorded = 0
+    for depth in range(bounces):
+        nr = int(host(n_rays)[0])
+        nb.trace(gs, nb.soa(nb.RaySoA, rays), n_rays, cap, nb.soa(nb.HitSoA, hits), stream())
+        hh = hs.trace(hr)
+        nb.shade(gs, nb.soa(nb.RaySoA, rays), nb.soa(nb.HitSoA, hits), n_rays, cap, depth, film,
+                 contrib, nb.soa(nb.PathVertices, verts), n_vert, scratch, stream())
+        hv, hc = hs.shade(hr, hh, depth, hfilm)
+        # handleEmissiveHit / handleMiss: the radiance reaches the node the ray left
+        g.pn.recordRadiance(rays["node"], contrib, nr, stream())
+        hn.record_radiance(hr["node"], hc)
+        nv = int(host(n_vert)[0])
+        assert nv == len(hv["pos"])
+        if nv == 0:
+            break
+        # the decision (the library's, on synthetic factors) between the bounces
+        f = rng.uniform(0.3, 2.5, nv).astype(np.float32)
+        rnd = rng.uniform(size=nv).astype(np.float32)
+        split = torch.zeros(nv, dtype=torch.uint8, device="cuda")
+        rc = nb.decide_emit_noalloc(torch.from_numpy(f).cuda(), torch.from_numpy(rnd).cuda(), nv,
+                                    nv, 0, dp, rrs_norm, split, queue, cap, qsize, None, stream())
+        assert rc == 0
+        o = O.decide_emit(f, rnd, nv, 0, dp, capacity=cap, shift_n=nb.NOALLOC_MAX_N)
+        # recordNode for the vertices that continue, in place on their node indices
+        record = (split > 0).to(torch.uint8)
+        vs = nb.vertex_soa(verts["pos"], verts["wi"], verts["normal"], verts["roughness"],
+                           verts["albedo"], verts["thp"], verts["depth"])
+        g.pn.recordNode(vs, verts["node"], verts["pixel"], rrs_norm, record, nv, verts["node"],
+                        stream())
+        hb = {k: np.ascontiguousarray(hv[k]) for k in ("pos", "wi", "normal", "albedo",
+                                                        "roughness", "thp", "depth", "pixel")}
+        hb["parent"] = np.ascontiguousarray(hv["node"], np.int32)
+        hb["rrs"] = np.ascontiguousarray(o["rrs_norm"][:nv], np.float32)
+        hb["record"] = (o["split"] > 0).astype(np.uint8)
+        hv = dict(hv)
+        hv["node"] = hn.record_nodes(hb)
+        assert host(verts["node"])[:nv].tolist() == hv["node"].tolist()
+        recorded += int((hv["node"] >= 0).sum())
+        # scatter and shadow rays; the shadow radiance reaches the new nodes
+        nb.scatter(gs, nb.soa(nb.PathVertices, verts), rrs_norm, queue, qsize, cap, depth, seed,
+                   nb.soa(nb.RaySoA, rays), nb.soa(nb.ShadowSoA, shadow), stream())
+        hr, hsh = hs.scatter(hv, o["rrs_norm"], o["queue"], depth, seed)
+        nq = int(host(qsize)[0])
+        same(to_host(rays, nq), hr, ("origin", "dir", "thp", "pdf", "pixel", "node"))
+        nb.trace_shadow(gs, nb.soa(nb.ShadowSoA, shadow), qsize, cap, film, scontrib, stream())
+        hco = hs.shadow(hsh, hfilm)
+        g.pn.recordRadiance(shadow["node"], scontrib, nq, stream())
+        hn.record_radiance(hsh["node"], hco)
+        n_rays.copy_(qsize)
+    assert recorded > n
+    assert host(film).tobytes() == hfilm.tobytes()
+    himg = hs.resolve(hfilm, 1.0)
+    image = np.concatenate([himg, np.ones((n, 1), np.float32)], axis=1)
+
+    # the node buffers
+    size, dropped, flags = g.pn.status(stream())
+    assert (size, dropped, flags) == (hn.size, hn.dropped, hn.status)
+    assert dropped == 0 and flags == 0
+    # trainStep's data side: the batch, the per-pixel counts, the weights
+    prm = nb.default_train_data_params(copy_rrs_node=1, dedupe_rrs_target=1)
+    batch, total, counts, weights = g.generate(prm, node_cap, image=image, n_pixels=n)
+    for k in NODE_FIELDS:
+        assert g.field(k, hn.size).tobytes() == hn.a[k][:hn.size].tobytes(), k
+    hcounts = np.zeros(n, np.uint32)
+    hbatch, htotal = hn.generate(prm, node_cap, image=image, n_pixels=n, pixel_samples=hcounts)
+    assert total == htotal > 0
+    assert_same_batch(batch, hbatch)
+    assert counts.tobytes() == hcounts.tobytes()
+    assert weights.tobytes() == O.sample_weights(hbatch["pixel"], hcounts, n).tobytes()
+
+    # the batch trains the networks: the library's FP32 losses on the GPU batch equal the
+    # oracle's FP64 losses on the oracle's batch
+    m = min(total, 8192)
+    net = make_net(max_train=1 << 13, step=3, log2_hashmap_size=15, precision=nb.PREC_FP32)
+    p0 = random_params(net, 5, table_scale=0.5, mlp_scale=0.15)
+    d = {k: torch.from_numpy(np.ascontiguousarray(
+        batch[k][:m].view(np.int32) if batch[k].dtype == np.uint32 else batch[k][:m])).cuda()
+        for k in ("pos", "wi", "normal", "roughness", "albedo", "thp", "depth", "ref_mean",
+                  "target")}
+    loss = torch.zeros(2, dtype=torch.float64, device="cuda")
+    net.trainGrads(nb.vertex_soa(d["pos"], d["wi"], d["normal"], d["roughness"], d["albedo"],
+                                 d["thp"], d["depth"], d["ref_mean"]), d["target"], m, loss,
+                   stream())
+    ob = {k: np.ascontiguousarray(hbatch[k][:m]) for k in hbatch}
+    _, l64 = O.train_grads(net.config, p0, ob, ob["target"], "f64")
+    assert host(loss) == pytest.approx(l64, rel=1e-4)
+    net.close()
