@@ -1162,7 +1162,7 @@ def run_render(args, rank, world, local_rank):
                    "lights": n_lights, "vertices_per_frame": verts_per_frame,
                    "parallelism": f"replicas{world}",
                    "l2": "queues of 2-6M entries per bounce (hundreds of MB) are larger than L2; "
-                         "the scene (2.5 MB) is L2-resident"},
+                         "the scene (4 MB of nodes and triangles) is L2-resident"},
         "clocks": clk.summary(),
         "gpu_launches": launches,
         "calls_ms_per_frame": {"trace": t_trace, "nrrs_step": t_nrrs, "shadow": t_shadow},

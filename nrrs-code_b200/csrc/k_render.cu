@@ -43,7 +43,7 @@ namespace {
 constexpr float kInvPi = 0.318309886183790671f;
 constexpr float kOffset = 1e-4f;        // ray origins leave the surface along the normal
 constexpr int kStack = 64;
-constexpr int kLeafMax = 4;
+constexpr int kLeafMax = 1;   // one triangle per leaf: its tight box culls the costly test
 constexpr uint32_t kMiss = 0xffffffffu;
 constexpr uint32_t kRRDim = 31;     // hash dimension of the fixed-RR decision
 
@@ -583,9 +583,9 @@ struct Build {
             set_word(me, 7, hi - lo);
             return;
         }
-        // binned surface-area heuristic over the centroids (16 bins per axis); a median split
+        // binned surface-area heuristic over the centroids (32 bins per axis); a median split
         // on the longest axis when no binned cut costs less than the node's own area × count
-        // (leaves stay at most kLeafMax triangles either way)
+        // (leaves hold at most kLeafMax triangles, except at the depth cap)
         float cmin[3], cmax[3];
         for (int k = 0; k < 3; ++k) { cmin[k] = INFINITY; cmax[k] = -INFINITY; }
         for (uint32_t i = lo; i < hi; ++i)
@@ -594,7 +594,7 @@ struct Build {
                 cmin[k] = std::min(cmin[k], c);
                 cmax[k] = std::max(cmax[k], c);
             }
-        constexpr int kBins = 16;
+        constexpr int kBins = 32;
         int axis = -1, cut = 0;
         float best = (float)(hi - lo) * area_of(bmin, bmax);   // the leaf's cost
         for (int k = 0; k < 3; ++k) {
