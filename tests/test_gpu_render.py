@@ -315,3 +315,96 @@ def test_gpu_rrs_keeps_the_image_unbiased():
     a, b = np.mean(ones), np.mean(rrs)
     se = np.sqrt(np.var(ones) / len(ones) + np.var(rrs) / len(rrs))
     assert abs(a - b) < 4 * se + 0.02 * a, (a, b, se)
+
+
+def test_gpu_scene_without_lights_matches_oracle():
+    """No emissive triangle: next-event estimation is skipped (no light to pick) and the only
+    light is the environment seen through the open front."""
+    v, t, m, ma, _ = nb.synth_scene(6, n_boxes=30)
+    ma = ma.copy()
+    ma[:, 3:] = 0.0
+    env = np.array([0.6, 0.7, 0.8], np.float32)
+    gs, hs = nb.Scene(v, t, m, ma, env), O.HostScene(v, t, m, ma, env)
+    assert gs.info()[1] == 0
+    img, _ = run_frame_pair(gs, hs, nb.room_camera(40, 30), 17, 4,
+                            lambda rng, n: rng.uniform(0.5, 2.0, n))
+    assert img.mean() > 0
+
+
+def test_gpu_degenerate_triangles_match_brute_force():
+    """Zero-area triangles (collapsed to a point or a line, one of them emissive) are never hit
+    and never sampled as lights; the rest of the scene traces as before."""
+    torch = torch_cuda()
+    v, t, m, ma, e = nb.synth_scene(8, n_boxes=40)
+    base = len(v)
+    extra_v = np.array([[0.3, 0.3, 0.3], [0.3, 0.3, 0.3], [0.3, 0.3, 0.3],     # a point
+                        [0.2, 0.5, 0.5], [0.4, 0.5, 0.5], [0.8, 0.5, 0.5]],    # a line
+                       np.float32)
+    v2 = np.concatenate([v, extra_v])
+    t2 = np.concatenate([t, np.array([[base, base + 1, base + 2], [base + 3, base + 4, base + 5],
+                                      [base + 5, base + 3, base + 4]], np.uint32)])
+    emissive = int(np.nonzero(ma[:, 3] > 0)[0][0])
+    m2 = np.concatenate([m, np.array([emissive, emissive, 0], np.uint32)])
+    gs, hs = nb.Scene(v2, t2, m2, ma, e), O.HostScene(v2, t2, m2, ma, e)
+    assert gs.info()[1] == nb.Scene(v, t, m, ma, e).info()[1]    # no zero-area light
+    n = 20000
+    rng = np.random.default_rng(4)
+    o = rng.uniform(0.05, 0.95, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    # rays aimed straight at the degenerate triangles too
+    o[:200] = np.array([0.3, 0.3, 0.05], np.float32)
+    d[:200] = np.array([0.0, 0.0, 1.0], np.float32)
+    o[200:400] = np.array([0.5, 0.5, 0.05], np.float32)
+    r = {"origin": o, "dir": d, "thp": np.ones((n, 3), np.float32), "pdf": np.zeros(n, np.float32),
+         "pixel": np.zeros(n, np.uint32), "node": np.full(n, -1, np.int32)}
+    rays, hits = dev_dict(r), empty_hits(n)
+    cnt = torch.tensor([n], dtype=torch.int32, device="cuda")
+    nb.trace(gs, nb.soa(nb.RaySoA, rays), cnt, n, nb.soa(nb.HitSoA, hits), stream())
+    want = hs.trace(r)
+    same(to_host(hits, n), want, ("prim", "t", "u", "v"))
+    assert not np.isin(want["prim"], np.arange(len(t), len(t2))).any()
+
+
+def test_gpu_scene_create_rejects_bad_input():
+    torch_cuda()
+    v, t, m, ma, e = nb.synth_scene(1, n_boxes=2)
+    bad_vertex = t.copy()
+    bad_vertex[3, 1] = len(v)
+    bad_material = m.copy()
+    bad_material[0] = len(ma)
+    for args in ((v, t[:0], m[:0], ma, e), (v, bad_vertex, m, ma, e), (v, t, bad_material, ma, e),
+                 (v, t, m, ma[:0], e)):
+        with pytest.raises(nb.NRRSError):
+            nb.Scene(*args)
+
+
+def test_gpu_empty_queues_are_no_ops():
+    """A queue size of 0 on the device: every step returns at once and writes nothing."""
+    torch = torch_cuda()
+    gs, _ = scene_pair(2, boxes=5)
+    n = 64
+    rays, hits = empty_rays(n), empty_hits(n)
+    verts, shadow = empty_vertices(n), empty_shadow(n)
+    hits["prim"].fill_(-5)
+    zero = torch.zeros(1, dtype=torch.int32, device="cuda")
+    n_out = torch.full((1,), 77, dtype=torch.int32, device="cuda")
+    film = torch.zeros((n, 9), dtype=torch.int64, device="cuda")
+    scratch = torch.zeros(nb.shade_scratch_bytes(n), dtype=torch.uint8, device="cuda")
+    before = {k: host(t).copy() for k, t in verts.items()}
+    nb.trace(gs, nb.soa(nb.RaySoA, rays), zero, n, nb.soa(nb.HitSoA, hits), stream())
+    nb.shade(gs, nb.soa(nb.RaySoA, rays), nb.soa(nb.HitSoA, hits), zero, n, 0, film, None,
+             nb.soa(nb.PathVertices, verts), n_out, scratch, stream())
+    rrs = torch.ones(n, device="cuda")
+    queue = torch.zeros(n, dtype=torch.int32, device="cuda")
+    nb.scatter(gs, nb.soa(nb.PathVertices, verts), rrs, queue, zero, n, 0, 1,
+               nb.soa(nb.RaySoA, rays), nb.soa(nb.ShadowSoA, shadow), stream())
+    nb.scatter_fixed_rr(gs, nb.soa(nb.PathVertices, verts), zero, n, 0.5, 0, 1,
+                        nb.soa(nb.RaySoA, rays), nb.soa(nb.ShadowSoA, shadow), stream())
+    nb.trace_shadow(gs, nb.soa(nb.ShadowSoA, shadow), zero, n, film, None, stream())
+    assert int(host(n_out)[0]) == 0
+    assert (host(hits["prim"]) == -5).all()
+    assert not host(film).any()
+    for k, t in verts.items():
+        assert host(t).tobytes() == before[k].tobytes(), k
+    assert not host(rays["thp"]).any() and not host(shadow["contrib"]).any()
