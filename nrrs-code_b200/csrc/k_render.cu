@@ -539,6 +539,7 @@ struct Build {
     std::vector<uint32_t> order;
     std::vector<float> nodes;
     uint32_t max_depth = 0;
+    float margin = 0.f;   // 1e-5 of the scene's largest extent (set before the build)
 
     void bounds(uint32_t lo, uint32_t hi, float* bmin, float* bmax) const {
         for (int k = 0; k < 3; ++k) { bmin[k] = INFINITY; bmax[k] = -INFINITY; }
@@ -550,8 +551,12 @@ struct Build {
                 bmax[k] = std::max({bmax[k], a, b, c});
             }
         }
-        for (int k = 0; k < 3; ++k) {   // grow by a relative epsilon: the slab test must not
-            const float e = 1e-5f * (std::fabs(bmin[k]) + std::fabs(bmax[k]) + 1e-3f);  // miss
+        // Grow the box so that the slab test never misses a triangle the exact test hits. A slab
+        // distance (lo - o) * inv carries a relative error of about 1.2e-7 of |lo - o|; the margin,
+        // relative to the coordinates and to the scene's extent, stays far above that for ray
+        // origins within some 80 scene extents.
+        for (int k = 0; k < 3; ++k) {
+            const float e = 1e-5f * (std::fabs(bmin[k]) + std::fabs(bmax[k])) + margin;
             bmin[k] -= e;
             bmax[k] += e;
         }
@@ -731,6 +736,13 @@ extern "C" int nrrs_scene_create(const float* vertices, uint32_t n_vertices,
     b.tri = &tri;
     b.order.resize(n_triangles);
     std::iota(b.order.begin(), b.order.end(), 0u);
+    {
+        float lo[3], hi[3];
+        b.bounds(0, n_triangles, lo, hi);   // margin 0 here: the scene's own bounds
+        float ext = 0.f;
+        for (int k = 0; k < 3; ++k) ext = std::max(ext, hi[k] - lo[k]);
+        b.margin = 1e-5f * ext;
+    }
     b.build(b.alloc(), 0, n_triangles, 0);
     std::vector<float> tri_leaf(12 * (size_t)n_triangles, 0.f);
     for (uint32_t i = 0; i < n_triangles; ++i)
