@@ -629,6 +629,10 @@ int nrrs_scene_create(const float* vertices, uint32_t n_vertices, const uint32_t
                       uint32_t n_triangles, const uint32_t* tri_material, const float* materials,
                       uint32_t n_materials, const float* environment, nrrs_scene** out);
 void nrrs_scene_destroy(nrrs_scene* s);
+/* mEnableNEE (integrator.h:139, on by default): 0 turns next-event estimation off. Scatter then
+ * writes no shadow contribution, and an emitter hit by a BSDF ray counts in full (no MIS
+ * weight). Takes effect for the launches that follow. */
+int nrrs_scene_set_nee(nrrs_scene* s, int32_t enable);
 /* BVH nodes, emissive triangles and the BVH depth */
 int nrrs_scene_info(const nrrs_scene* s, uint32_t* n_nodes, uint32_t* n_lights,
                     uint32_t* max_depth);

@@ -35,6 +35,7 @@ struct nrrs_scene {
     float* light_area = nullptr;  // [nl]
     float env[3] = {0.f, 0.f, 0.f};
     uint32_t nt = 0, nn = 0, nl = 0, nm = 0, max_depth = 0;
+    uint32_t nee = 1;             // next-event estimation on (mEnableNEE)
 };
 
 namespace nrrs {
@@ -356,7 +357,7 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ nrrs_scen
                     if (nonzero(le)) {
                         float w = 1.0f;
                         const float pdf = r.pdf[i];
-                        if (pdf > 0.f && s.nl) {
+                        if (pdf > 0.f && s.nl && s.nee) {
                             // the light pdf (solid angle) of sampling this point by NEE
                             const float area = __fmul_rn(0.5f, __fsqrt_rn(dot(g, g)));
                             const float cosl = fabsf(dot(nrm, d));
@@ -409,10 +410,12 @@ __device__ __forceinline__ void scatter_one(const nrrs_scene& s, const nrrs_path
     const V3 org = add(p, mul(nn, kOffset));
     const uint32_t px = v.pixel[x];
     const int node = v.node[x];
-    // next-event estimation: a light by index, a point by area
-    V3 sc = {0.f, 0.f, 0.f}, wl = {0.f, 0.f, 1.f};
-    float dist = 0.f;
-    if (s.nl) {
+    // next-event estimation: a light by index, a point by area. The shading terms use the
+    // direction from the vertex; the visibility test runs from the offset origin to the light
+    // point itself and stops short of it, so the light's own triangle never occludes the sample.
+    V3 sc = {0.f, 0.f, 0.f}, sdir = {0.f, 0.f, 1.f};
+    float smax = 0.f;
+    if (s.nl && s.nee) {
         const uint32_t k = min((uint32_t)(rnd(seed, depth, j, 0) * (float)s.nl), s.nl - 1);
         const uint32_t lt = s.lights[k];
         const float* tri = s.tri_in + 9 * (size_t)lt;
@@ -421,20 +424,23 @@ __device__ __forceinline__ void scatter_one(const nrrs_scene& s, const nrrs_path
         const V3 q = add(add(v3(tri), mul(v3(tri + 3), b1)), mul(v3(tri + 6), b2));
         const V3 dv = sub(q, p);
         const float d2 = dot(dv, dv);
-        dist = __fsqrt_rn(d2);
-        wl = divs(dv, dist);
+        const V3 wl = divs(dv, __fsqrt_rn(d2));
         const float cosv = dot(nn, wl);
         const float cosl = fabsf(dot(normalize(cross(v3(tri + 3), v3(tri + 6))), wl));
         const V3 le = v3(s.mats + 6 * (size_t)s.tri_mat[lt] + 3);
-        if (cosv > 0.f && cosl > 0.f && nonzero(le) && d2 > 0.f) {
+        const V3 ds = sub(q, org);
+        const float sl = __fsqrt_rn(dot(ds, ds));
+        if (cosv > 0.f && cosl > 0.f && nonzero(le) && d2 > 0.f && sl > 0.f) {
             const float pl = __fdiv_rn(d2, __fmul_rn(__fmul_rn(cosl, s.light_area[k]), (float)s.nl));
             const float w = power_heuristic(pl, __fmul_rn(cosv, kInvPi));
             sc = divs(mul(mul(vmul(vmul(thp, f), le), cosv), w), pl);
+            sdir = divs(ds, sl);
+            smax = __fmul_rn(sl, 0.9999f);
         }
     }
     put(sh.origin + 3 * (size_t)j, org);
-    put(sh.dir + 3 * (size_t)j, wl);
-    sh.tmax[j] = __fmul_rn(dist, 0.9999f);
+    put(sh.dir + 3 * (size_t)j, sdir);
+    sh.tmax[j] = smax;
     put(sh.contrib + 3 * (size_t)j, sc);
     sh.pixel[j] = px;
     sh.node[j] = node;
@@ -776,6 +782,12 @@ extern "C" void nrrs_scene_destroy(nrrs_scene* s) {
     cudaFree(s->tris); cudaFree(s->tri_id); cudaFree(s->tri_mat); cudaFree(s->tri_in);
     cudaFree(s->nodes); cudaFree(s->mats); cudaFree(s->lights); cudaFree(s->light_area);
     delete s;
+}
+
+extern "C" int nrrs_scene_set_nee(nrrs_scene* s, int32_t enable) {
+    if (!s || (enable != 0 && enable != 1)) return NRRS_ERR_INVALID_ARG;
+    s->nee = (uint32_t)enable;
+    return NRRS_OK;
 }
 
 extern "C" int nrrs_scene_info(const nrrs_scene* s, uint32_t* n_nodes, uint32_t* n_lights,

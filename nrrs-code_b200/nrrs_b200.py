@@ -272,6 +272,7 @@ _SIGS = {
     "nrrs_scatter": (C.c_int, [C.c_void_p, C.POINTER(PathVertices), C.c_void_p, C.c_void_p,
                                C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(RaySoA),
                                C.POINTER(ShadowSoA), C.c_void_p]),
+    "nrrs_scene_set_nee": (C.c_int, [C.c_void_p, C.c_int32]),
     "nrrs_scatter_fixed_rr": (C.c_int, [C.c_void_p, C.POINTER(PathVertices), C.c_void_p,
                                         C.c_uint32, C.c_float, C.c_uint32, C.c_uint32,
                                         C.POINTER(RaySoA), C.POINTER(ShadowSoA), C.c_void_p]),
@@ -682,6 +683,10 @@ class Scene:
             self._h = None
 
     __del__ = close
+
+    def set_nee(self, enable: bool):
+        """Next-event estimation on or off (the reference's mEnableNEE)."""
+        _check(lib().nrrs_scene_set_nee(self._h, int(bool(enable))), "nrrs_scene_set_nee")
 
     def info(self) -> tuple[int, int, int]:
         a, b, c = C.c_uint32(), C.c_uint32(), C.c_uint32()

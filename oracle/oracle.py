@@ -425,6 +425,12 @@ class HostScene:
         self.nl = int(L.oracle_scene_tris(v.ctypes.data, t.ctypes.data, nt, self.tm.ctypes.data,
                                           self.mats.ctypes.data, self.tri.ctypes.data,
                                           self.lights.ctypes.data, self.area.ctypes.data))
+        self.nee = True
+
+    @property
+    def nl_sampled(self) -> int:
+        """The lights next-event estimation samples (and MIS weighs against): none when off."""
+        return self.nl if self.nee else 0
 
     def camera_rays(self, cam, sample: int, seed: int):
         n = cam.width * cam.height
@@ -460,7 +466,8 @@ class HostScene:
         f.restype = C.c_uint32
         f.argtypes = [C.c_void_p] * 3 + [C.c_uint32, C.c_uint32] + [C.c_void_p] * 9 + \
             [C.c_uint32, C.c_uint32] + [C.c_void_p] * 11
-        m = f(self.tri.ctypes.data, self.tm.ctypes.data, self.mats.ctypes.data, self.nt, self.nl,
+        m = f(self.tri.ctypes.data, self.tm.ctypes.data, self.mats.ctypes.data, self.nt,
+              self.nl_sampled,
               self.env.ctypes.data,
               *(np.ascontiguousarray(rays[k]).ctypes.data for k in
                 ("origin", "dir", "thp", "pdf", "pixel", "node")),
@@ -484,7 +491,7 @@ class HostScene:
         f.argtypes = [C.c_void_p] * 3 + [C.c_uint32] + [C.c_void_p] * 2 + [C.c_uint32] + \
             [C.c_void_p] * 8 + [C.c_uint32, C.c_uint32, C.c_uint32] + [C.c_void_p] * 12
         f(self.tri.ctypes.data, self.tm.ctypes.data, self.mats.ctypes.data, self.nt,
-          self.lights.ctypes.data, self.area.ctypes.data, self.nl,
+          self.lights.ctypes.data, self.area.ctypes.data, self.nl_sampled,
           *(np.ascontiguousarray(v[k]).ctypes.data for k in ("pos", "normal", "albedo", "thp",
                                                              "pixel", "node")),
           rrs_norm.ctypes.data, queue.ctypes.data, nq, depth, seed,
@@ -504,7 +511,7 @@ class HostScene:
         f.argtypes = [C.c_void_p] * 5 + [C.c_uint32] + [C.c_void_p] * 6 + \
             [C.c_uint32, C.c_float, C.c_uint32, C.c_uint32] + [C.c_void_p] * 12
         f(self.tri.ctypes.data, self.tm.ctypes.data, self.mats.ctypes.data,
-          self.lights.ctypes.data, self.area.ctypes.data, self.nl,
+          self.lights.ctypes.data, self.area.ctypes.data, self.nl_sampled,
           *(np.ascontiguousarray(v[k]).ctypes.data for k in ("pos", "normal", "albedo", "thp",
                                                              "pixel", "node")),
           n, rr, depth, seed,

@@ -271,8 +271,10 @@ static void scatter_one(const lights_t* L, const float* pos, const float* nrm, c
     const v3 al = ld(alb + 3 * (uint64_t)x);
     const v3 f = mul(al, INV_PI);
     const v3 org = add(p, mul(nn, OFFSET));
-    v3 sc = {0.f, 0.f, 0.f}, wl = {0.f, 0.f, 1.f};
-    float dist = 0.f;
+    /* the shading terms use the direction from the vertex; the visibility test runs from the
+     * offset origin to the light point and stops short of it */
+    v3 sc = {0.f, 0.f, 0.f}, sdir = {0.f, 0.f, 1.f};
+    float smax = 0.f;
     if (nl) {
         uint32_t k = (uint32_t)(rnd(seed, depth, j, 0) * (float)nl);
         if (k > nl - 1) k = nl - 1;
@@ -283,20 +285,23 @@ static void scatter_one(const lights_t* L, const float* pos, const float* nrm, c
         const v3 q = add(add(ld(tr), mul(ld(tr + 3), b1)), mul(ld(tr + 6), b2));
         const v3 dv = sub(q, p);
         const float d2 = dot(dv, dv);
-        dist = sqrtf(d2);
-        wl = divs(dv, dist);
+        const v3 wl = divs(dv, sqrtf(d2));
         const float cosv = dot(nn, wl);
         const float cosl = fabsf(dot(normalize(cross(ld(tr + 3), ld(tr + 6))), wl));
         const v3 le = ld(mats + 6 * (uint64_t)mat[lt] + 3);
-        if (cosv > 0.f && cosl > 0.f && nonzero(le) && d2 > 0.f) {
+        const v3 ds = sub(q, org);
+        const float sl = sqrtf(dot(ds, ds));
+        if (cosv > 0.f && cosl > 0.f && nonzero(le) && d2 > 0.f && sl > 0.f) {
             const float pl = d2 / ((cosl * area[k]) * (float)nl);
             const float w = power_heuristic(pl, cosv * INV_PI);
             sc = divs(mul(mul(vmul(vmul(th, f), le), cosv), w), pl);
+            sdir = divs(ds, sl);
+            smax = sl * 0.9999f;
         }
     }
     st(s_origin + 3 * (uint64_t)j, org);
-    st(s_dir + 3 * (uint64_t)j, wl);
-    s_tmax[j] = dist * 0.9999f;
+    st(s_dir + 3 * (uint64_t)j, sdir);
+    s_tmax[j] = smax;
     st(s_contrib + 3 * (uint64_t)j, sc);
     s_pixel[j] = pixel[x];
     s_node[j] = node[x];

@@ -408,3 +408,61 @@ def test_gpu_empty_queues_are_no_ops():
     for k, t in verts.items():
         assert host(t).tobytes() == before[k].tobytes(), k
     assert not host(rays["thp"]).any() and not host(shadow["contrib"]).any()
+
+
+def test_gpu_nee_off_matches_oracle():
+    """mEnableNEE off: no shadow contributions and emitters hit by BSDF rays count in full."""
+    gs, hs = scene_pair(3, boxes=40)
+    gs.set_nee(False)
+    hs.nee = False
+    img, _ = run_frame_pair(gs, hs, nb.room_camera(48, 36), 5, 4,
+                            lambda rng, n: rng.uniform(0.3, 2.5, n))
+    assert img.mean() > 0
+    with pytest.raises(nb.NRRSError):
+        lib_rc = nb.lib().nrrs_scene_set_nee(gs._h, 2)
+        nb._check(lib_rc, "nrrs_scene_set_nee")
+
+
+def test_gpu_nee_and_bsdf_sampling_agree():
+    """Next-event estimation with the power heuristic and pure BSDF sampling estimate the same
+    image: the mean over frames agrees within the frames' standard error. Both run D bounces
+    of scatter and a final trace and shade, so that each light-sampled path has its BSDF-sampled
+    counterpart."""
+    torch = torch_cuda()
+    gs, _ = scene_pair(4, boxes=20, closed=True)
+    cam = nb.room_camera(48, 36, inside=True)
+    n = cam.width * cam.height
+    cap = 2 * n
+    D = 3
+
+    def frame(seed, nee):
+        gs.set_nee(nee)
+        film = torch.zeros((n, 9), dtype=torch.int64, device="cuda")
+        rays, hits = empty_rays(cap), empty_hits(cap)
+        verts, shadow = empty_vertices(cap), empty_shadow(cap)
+        scratch = torch.zeros(nb.shade_scratch_bytes(cap), dtype=torch.uint8, device="cuda")
+        n_rays = torch.tensor([n], dtype=torch.int32, device="cuda")
+        n_vert = torch.zeros(1, dtype=torch.int32, device="cuda")
+        nb.camera_rays(cam, seed, 99, nb.soa(nb.RaySoA, rays), stream())
+        for depth in range(D + 1):
+            nb.trace(gs, nb.soa(nb.RaySoA, rays), n_rays, cap, nb.soa(nb.HitSoA, hits), stream())
+            nb.shade(gs, nb.soa(nb.RaySoA, rays), nb.soa(nb.HitSoA, hits), n_rays, cap, depth,
+                     film, None, nb.soa(nb.PathVertices, verts), n_vert, scratch, stream())
+            if depth == D:
+                break
+            nb.scatter_fixed_rr(gs, nb.soa(nb.PathVertices, verts), n_vert, cap, 1.0, depth,
+                                seed * 7 + 1, nb.soa(nb.RaySoA, rays),
+                                nb.soa(nb.ShadowSoA, shadow), stream())
+            nb.trace_shadow(gs, nb.soa(nb.ShadowSoA, shadow), n_vert, cap, film, None, stream())
+            n_rays.copy_(n_vert)
+        img = torch.zeros((n, 3), device="cuda")
+        nb.film_resolve(film, n, 1.0, img, stream())
+        return float(host(img).mean())
+
+    on = [frame(s, True) for s in range(32)]
+    off = [frame(s, False) for s in range(32)]
+    gs.set_nee(True)
+    a, b = np.mean(on), np.mean(off)
+    se = np.sqrt(np.var(on) / len(on) + np.var(off) / len(off))
+    assert a > 0 and abs(a - b) < 4 * se + 0.01 * a, (a, b, se)
+    assert np.std(on) < np.std(off)        # light sampling lowers the variance
