@@ -21,13 +21,18 @@ Other workloads (--workload):
             scatter (NEE + BSDF rays) and shadow rays, in a closed room of 3000 boxes
             (36k triangles) seen from inside;
             metric path vertices/s
+  render_train1080p
+            the same frame as a training frame: the radiance of every shaded and shadow ray
+            and the surviving vertices go to the path records, then the per-pixel error, the
+            training batch and one training step of 262,144 samples; metric path vertices/s
   records1080p
             the training-data side of a 1920x1080 frame: 8 bounces of path vertices (about
             10.1M) record 7.0M path nodes and 7.5M radiance contributions, then the training
             batch and the sample weights are built; metric path nodes/s (one step = one frame)
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload frame1080p|batched|frame4k|records1080p|render1080p]
+                  [--workload frame1080p|batched|frame4k|records1080p|render1080p|
+                              render_train1080p]
                   [--precision fp16|bf16|fp32]
                   [--no-train]
 
@@ -77,6 +82,9 @@ WORKLOADS = {
     "render1080p": dict(bounces=6, n_vert=2_073_600, width=64, hidden=2, log2_table=19,
                         steps=40, precision="fp16", boxes=3000, train_steps=0,
                         train_batch=0),
+    "render_train1080p": dict(bounces=6, n_vert=2_073_600, width=64, hidden=2, log2_table=19,
+                              steps=20, precision="fp16", boxes=3000, train_steps=1,
+                              train_batch=262_144, node_rate=8),
 }
 
 
@@ -1046,7 +1054,8 @@ def run_render(args, rank, world, local_rank):
     scene = nb.Scene(v, t, m, ma, env)
     n_nodes, n_lights, bvh_depth = scene.info()
     cam = nb.room_camera(W, H, inside=True)
-    net = nb.NRRSNetwork(make_config(args.precision, wl, cap, 1 << 16))
+    train = wl.get("train_steps", 0) > 0
+    net = nb.NRRSNetwork(make_config(args.precision, wl, cap, max(wl["train_batch"], 1 << 16)))
     net.setStep(3)
     # factors clamped at 1 or above: the normalisation to the pixel budget then keeps about one
     # path per pixel per bounce, as a trained network would; an untrained one kills most paths
@@ -1076,15 +1085,46 @@ def run_render(args, rank, world, local_rank):
                          verts["albedo"], verts["thp"], verts["depth"])
     ev = {}
 
+    # ---- a training frame (renderInternal<true> + trainStep): path records, radiance, the
+    # per-pixel error, the batch and one training step on it ----
+    if train:
+        node_cap = wl["node_rate"] * P
+        nbytes = nb.path_nodes_bytes(node_cap, cap)
+        block = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        pn = nb.NRRSPathNodesBuffer(block.data_ptr(), nbytes, node_cap, cap, stream)
+        contrib, scontrib = f(cap, 3), f(cap, 3)
+        widths = {"pos": 3, "wi": 3, "normal": 3, "albedo": 3, "roughness": 1, "thp": 3,
+                  "depth": 1, "ref_mean": 1, "target": 3, "rrs_target": 1, "pixel": 1,
+                  "error": 1, "error_for_avg": 1, "number_samples": 1}
+        batch = {k: (f(node_cap, w) if w > 1 else f(node_cap)) if k not in ("depth", "pixel")
+                 else i(node_cap) for k, w in widths.items()}
+        tb = nb.train_batch(**batch)
+        counts, size_d = i(P), i(1)
+        pe = nb.default_pixel_error_params(W, H)
+        wl_d, cur_d, acc_d = f(P, 3), f(P, 3), i(P)
+        err_d, spp_d = f(2 * P), f(P)
+        esum_d = torch.zeros(32, dtype=torch.uint8, device=dev)
+        tprm = records_params(frame_width=W, error_image_scale=1,
+                              error_per_pixel=err_d.data_ptr(), samples_per_patch=spp_d.data_ptr())
+        tsoa = nb.vertex_soa(batch["pos"], batch["wi"], batch["normal"], batch["roughness"],
+                             batch["albedo"], batch["thp"], batch["depth"], batch["ref_mean"])
+        loss = torch.zeros(2, dtype=torch.float64, device=dev)
+        trained = [0, 0]   # samples in the batches, samples trained
+
     bounces_run = [0]
     rays_run = [0, 0]   # closest-hit and shadow rays of the timing frame
 
     def frame(sample, timing=False):
         vertices = 0
         n_prev = 0
+        n_cur = P          # rays of this bounce on the host (training frames read them back)
         film.zero_()
         nb.camera_rays(cam, sample, 1234, R, stream)
         n_rays.fill_(P)
+        if train:
+            pn.reset(stream)
+            spp_d.zero_()
+            nb.count_patch_samples(pe, rays["pixel"], P, spp_d, stream)
         for depth in range(wl["bounces"]):
             if timing:
                 ev.setdefault(("trace", depth), (torch.cuda.Event(enable_timing=True),
@@ -1093,7 +1133,10 @@ def run_render(args, rank, world, local_rank):
             nb.trace(scene, R, n_rays, cap, Hh, stream)
             if timing:
                 ev[("trace", depth)][1].record(cur)
-            nb.shade(scene, R, Hh, n_rays, cap, depth, film, None, V, n_vert, scratch, stream)
+            nb.shade(scene, R, Hh, n_rays, cap, depth, film, contrib if train else None, V,
+                     n_vert, scratch, stream)
+            if train:   # handleEmissiveHit / handleMiss: radiance to the node the ray left
+                pn.recordRadiance(rays["node"], contrib, n_cur, stream)
             nv = int(n_vert.item())          # the reference reads the queue size back too
             if nv == 0:
                 break
@@ -1107,19 +1150,52 @@ def run_render(args, rank, world, local_rank):
                                   cap, qsize, stream)
             if timing:
                 ev[("nrrs", depth)][1].record(cur)
+            if train:   # recordNode for the surviving vertices, in place on their node indices
+                pn.recordNode(vsoa, verts["node"], verts["pixel"], rrs_norm, split, nv,
+                              verts["node"], stream)
             nb.scatter(scene, V, rrs_norm, queue, qsize, cap, depth, 1234 + sample, R, S, stream)
             if timing:
                 ev.setdefault(("shadow", depth), (torch.cuda.Event(enable_timing=True),
                                                   torch.cuda.Event(enable_timing=True)))
                 ev[("shadow", depth)][0].record(cur)
-            nb.trace_shadow(scene, S, qsize, cap, film, None, stream)
+            nb.trace_shadow(scene, S, qsize, cap, film, scontrib if train else None, stream)
             if timing:
                 ev[("shadow", depth)][1].record(cur)
                 rays_run[0] += P if depth == 0 else n_prev
                 n_prev = int(qsize.item())
                 rays_run[1] += n_prev
+            if train:
+                n_cur = int(qsize.item())
+                nb.count_patch_samples(pe, rays["pixel"], n_cur, spp_d, stream)
+                pn.recordRadiance(shadow["node"], scontrib, n_cur, stream)
             n_rays.copy_(qsize)
         nb.film_resolve(film, P, 1.0, img, stream)
+        if train:
+            if timing:
+                ev.setdefault("train_data", (torch.cuda.Event(enable_timing=True),
+                                             torch.cuda.Event(enable_timing=True)))
+                ev["train_data"][0].record(cur)
+            # trainStep STEP#1-#2 (this frame's image stands for both the pixel radiance and
+            # the rendered film), then the batch and its per-pixel counts
+            nb.accumulate_weighted_l(pe, img, 1, False, wl_d, cur_d, acc_d, stream)
+            nb.update_weighted_l(pe, cur_d, acc_d, wl_d, stream)
+            nb.calculate_error(pe, img, 3, wl_d, spp_d, err_d, esum_d, stream)
+            counts.zero_()
+            pn.generate_training_data(tprm, tb, node_cap, size_d, image=img, image_channels=3,
+                                      n_pixels=P, pixel_samples=counts, stream=stream)
+            m = min(int(size_d.item()), wl["train_batch"])   # the reference reads it back too
+            if timing:
+                ev["train_data"][1].record(cur)
+                ev.setdefault("train", (torch.cuda.Event(enable_timing=True),
+                                        torch.cuda.Event(enable_timing=True)))
+                ev["train"][0].record(cur)
+            m -= m % 256
+            if m:
+                net.train(tsoa, batch["target"], m, loss, stream)
+            if timing:
+                ev["train"][1].record(cur)
+            trained[0] += int(size_d.item())
+            trained[1] += m
         return vertices
 
     for w in range(args.warmup):
@@ -1130,6 +1206,8 @@ def run_render(args, rank, world, local_rank):
     torch.cuda.synchronize()
     total_v = 0
     bounces_run[0] = 0
+    if train:
+        trained[0] = trained[1] = 0
     launches0 = net.launch_count()
     with ClockSampler(local_rank) as clk:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -1143,15 +1221,27 @@ def run_render(args, rank, world, local_rank):
     # camera + resolve per frame; trace, shade (2), scatter, shadow per bounce run, and the last
     # trace + shade of a frame whose queue ran out; plus the NRRS step's own launches
     launches = (args.steps * 2 + bounces_run[0] * 5 + (net.launch_count() - launches0))
+    if train:
+        # per bounce: radiance of the shaded rays, record count + writes, patch counts, shadow
+        # radiance; per frame: camera patch counts, pixel error (3), radiance pass + batch
+        launches += bounces_run[0] * 5 + args.steps * 6
+        batch_per_frame = trained[0] / args.steps
+        trained_per_frame = trained[1] / args.steps
     if dist:
         tt = torch.tensor([ms], device=dev)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
+    net.profile(True)
     frame(999, timing=True)
     torch.cuda.synchronize()
-    t_trace = sum(a.elapsed_time(b) for (k, _), (a, b) in ev.items() if k == "trace")
-    t_nrrs = sum(a.elapsed_time(b) for (k, _), (a, b) in ev.items() if k == "nrrs")
-    t_shadow = sum(a.elapsed_time(b) for (k, _), (a, b) in ev.items() if k == "shadow")
+    kern = net.profile_read()
+    net.profile(False)
+    t_trace = sum(a.elapsed_time(b) for k, (a, b) in ev.items()
+                  if isinstance(k, tuple) and k[0] == "trace")
+    t_nrrs = sum(a.elapsed_time(b) for k, (a, b) in ev.items()
+                 if isinstance(k, tuple) and k[0] == "nrrs")
+    t_shadow = sum(a.elapsed_time(b) for k, (a, b) in ev.items()
+                   if isinstance(k, tuple) and k[0] == "shadow")
     line = {
         "metric": "path vertices/s (path-traced frame around the NRRS step)",
         "value": verts_per_frame * world / (ms * 1e-3), "unit": "vertices/s", "n_gpus": world,
@@ -1172,6 +1262,19 @@ def run_render(args, rank, world, local_rank):
         "note": "a step is one frame; per bounce the vertex count is read back (as the "
                 "reference reads its queue size) before nrrs_step",
     }
+    if train:
+        line["metric"] = ("path vertices/s (training frame: path-traced frame around the NRRS "
+                          "step, path records, pixel error, training batch, one training step)")
+        line["config"]["workload"] = "train_" + line["config"]["workload"]
+        line["config"]["train_batch"] = wl["train_batch"]
+        line["calls_ms_per_frame"]["train_data"] = ev["train_data"][0].elapsed_time(ev["train_data"][1])
+        line["calls_ms_per_frame"]["train_step"] = ev["train"][0].elapsed_time(ev["train"][1])
+        line["training"] = {"batch_samples_per_frame": batch_per_frame,
+                            "samples_trained_per_frame": trained_per_frame,
+                            "loss": [float(x) for x in loss.tolist()]}
+        line["note"] += ("; the batch size is read back before the training step, which trains "
+                         "on the first train_batch samples of the batch")
+    line["kernels_ms_timing_frame"] = {k: round(ms, 4) for k, (n, ms) in kern.items()}
     if rank == 0:
         print(json.dumps(line), flush=True)
     scene.close()
@@ -1205,11 +1308,11 @@ def main():
         args.precision = wl["precision"]
     if args.bounces:
         wl["bounces"] = args.bounces
-    if args.vertices and args.workload not in ("records1080p", "render1080p"):
+    if args.vertices and args.workload not in ("records1080p", "render1080p", "render_train1080p"):
         wl["n_vert"] = args.vertices
     rank, world = env_int("RANK", 0), env_int("WORLD_SIZE", 1)
     local_rank = env_int("LOCAL_RANK", 0)
-    if args.workload == "render1080p":
+    if args.workload in ("render1080p", "render_train1080p"):
         if args.vertices:
             wl["n_vert"] = args.vertices
         if args.impl == "reference":
