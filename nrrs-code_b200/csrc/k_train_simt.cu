@@ -261,17 +261,16 @@ __global__ void __launch_bounds__(kTT) k_train_stat(const __grid_constant__ Trai
                 }
             }
         }
-        // hash-grid scatter-add (trilinear weights, FP32 atomics)
+        // hash-grid scatter-add (trilinear weights, FP32 reductions; runs of lanes in one cell
+        // summed in the warp first)
+        {
+            const unsigned lanes = valid_lanes(i - (uint32_t)(tid & 31), a.n);
 #pragma unroll 2
-        for (int l = 0; l < kMaxLevels; ++l) {
-            const LevelDev L = a.enc.lv[l];
-            const CellCoord c = cell_of(p, L.res);
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const uint32_t row = grid_row(L, a.enc.hash_mask, c.ix + (k & 1),
-                                              c.iy + ((k >> 1) & 1), c.iz + ((k >> 2) & 1));
-                const float w = corner_weight(c, k);
-                red_add2(a.table_grad + 2 * (size_t)row, w * dx[2 * l], w * dx[2 * l + 1]);
+            for (int l = 0; l < kMaxLevels; ++l) {
+                const LevelDev L = a.enc.lv[l];
+                const CellCoord c = cell_of(p, L.res);
+                warp_scatter_level(a.table_grad, L, a.enc.hash_mask, c, dx[2 * l], dx[2 * l + 1],
+                                   lanes);
             }
         }
 

@@ -94,28 +94,6 @@ __device__ __forceinline__ double block_sum_d(double v, double* red) {
     return t;
 }
 
-// Hash-grid gradient of one level of one sample: corners x and x+1 of each (y, z) with one
-// 16-byte reduction when they share an aligned pair of table rows (half the time), two 8-byte
-// ones otherwise. g0, g1: the level's two feature gradients, already divided by the batch size.
-__device__ __forceinline__ void scatter_level(float* table_grad, const LevelDev& L, uint32_t mask,
-                                              const CellCoord& c, float g0, float g1) {
-#pragma unroll
-    for (int k2 = 0; k2 < 4; ++k2) {
-        const uint32_t y = c.iy + (k2 & 1), z = c.iz + ((k2 >> 1) & 1);
-        const uint32_t r0 = grid_row(L, mask, c.ix, y, z);
-        const uint32_t r1 = grid_row(L, mask, c.ix + 1, y, z);
-        const float w0 = corner_weight(c, 2 * k2), w1 = corner_weight(c, 2 * k2 + 1);
-        if ((r0 >> 1) == (r1 >> 1)) {
-            float* q = table_grad + 4 * (size_t)(r0 >> 1);
-            if (r0 & 1u) red_add4(q, w1 * g0, w1 * g1, w0 * g0, w0 * g1);
-            else red_add4(q, w0 * g0, w0 * g1, w1 * g0, w1 * g1);
-        } else {
-            red_add2(table_grad + 2 * (size_t)r0, w0 * g0, w0 * g1);
-            red_add2(table_grad + 2 * (size_t)r1, w1 * g0, w1 * g1);
-        }
-    }
-}
-
 // ---------------------------------------------------------------------------------------------
 // Shared-memory plan of the StatNet kernel: the forward weight images (the backward reads them
 // as MN-major operands, i.e. transposed), two [128 x W] tiles that take turns as the input tile,
@@ -325,12 +303,13 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
 #pragma unroll
             for (int l = 0; l < kMaxLevels; ++l) d[(size_t)l * a.n + i] = make_float2(dx[2 * l], dx[2 * l + 1]);
         } else if (valid) {
+            const unsigned lanes = valid_lanes(i - (uint32_t)(tid & 31), a.n);
 #pragma unroll 2
             for (int l = 0; l < kMaxLevels; ++l) {
                 const LevelDev L = a.enc.lv[l];
                 const CellCoord c = cell_of(p, L.res);
-                scatter_level(a.table_grad, L, a.enc.hash_mask, c, dx[2 * l] * a.inv_n,
-                              dx[2 * l + 1] * a.inv_n);
+                warp_scatter_level(a.table_grad, L, a.enc.hash_mask, c, dx[2 * l] * a.inv_n,
+                                   dx[2 * l + 1] * a.inv_n, lanes);
             }
         }
         if (!ok) s_abort = 1;
@@ -367,83 +346,22 @@ struct ScatterLvArgs {
     uint32_t level_begin, level_end;
 };
 
-// The 8 corner rows of cell c with the given per-corner feature gradients v[2k], v[2k+1]; the
-// pairs of one (y, z) that share an aligned pair of rows go as one 16-byte reduction.
-__device__ __forceinline__ void scatter_corners(float* table_grad, const LevelDev& L,
-                                                uint32_t mask, const CellCoord& c, const float* v) {
-#pragma unroll
-    for (int k2 = 0; k2 < 4; ++k2) {
-        const uint32_t y = c.iy + (k2 & 1), z = c.iz + ((k2 >> 1) & 1);
-        const uint32_t r0 = grid_row(L, mask, c.ix, y, z);
-        const uint32_t r1 = grid_row(L, mask, c.ix + 1, y, z);
-        const float* a = v + 4 * k2;   // corner x: a[0], a[1]; corner x + 1: a[2], a[3]
-        if ((r0 >> 1) == (r1 >> 1)) {
-            float* q = table_grad + 4 * (size_t)(r0 >> 1);
-            if (r0 & 1u) red_add4(q, a[2], a[3], a[0], a[1]);
-            else red_add4(q, a[0], a[1], a[2], a[3]);
-        } else {
-            red_add2(table_grad + 2 * (size_t)r0, a[0], a[1]);
-            red_add2(table_grad + 2 * (size_t)r1, a[2], a[3]);
-        }
-    }
-}
-
-// One sample per thread at one level. The samples of a batch built from a tracer's queues come
-// in pixel order, so at the coarse and middle levels runs of neighbouring lanes fall into the
-// same cell and their reductions would serialise on the same rows. A warp with such runs first
-// sums each run's 16 corner gradients by a segmented shuffle scan and lets the run's last lane
-// reduce once; a warp without runs (uniform samples) reduces per lane as before.
 __global__ void __launch_bounds__(128) k_scatter_levels(const __grid_constant__ ScatterLvArgs a) {
     const uint32_t tiles = (a.n + 127) / 128;
     const uint32_t items = (a.level_end - a.level_begin) * tiles;
     const float2* d = reinterpret_cast<const float2*>(a.dxs);
-    const uint32_t lane = threadIdx.x & 31u;
     for (uint32_t w = blockIdx.x; w < items; w += gridDim.x) {
         const uint32_t lq = w / tiles, t = w - lq * tiles;
         const uint32_t l = a.level_begin + lq;
         const uint32_t i = t * 128 + threadIdx.x;
-        const bool ok = i < a.n;
+        if (i >= a.n) continue;
+        float p[3];
+        norm_pos(a.enc, a.pos, i, p);
+        const float2 g = d[(size_t)l * a.n + i];
         const LevelDev L = a.enc.lv[l];
-        CellCoord c{};
-        float v[16];
-        if (ok) {
-            float p[3];
-            norm_pos(a.enc, a.pos, i, p);
-            const float2 g = d[(size_t)l * a.n + i];
-            c = cell_of(p, L.res);
-            const float g0 = g.x * a.inv_n, g1 = g.y * a.inv_n;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const float wk = corner_weight(c, k);
-                v[2 * k] = wk * g0;
-                v[2 * k + 1] = wk * g1;
-            }
-        } else {
-            c.ix = c.iy = c.iz = 0xffffffffu;   // no cell: never joins a run
-#pragma unroll
-            for (int k = 0; k < 16; ++k) v[k] = 0.f;
-        }
-        // runs of lanes in the same cell (the whole warp takes the loop's iterations together)
-        const uint32_t px = __shfl_up_sync(0xffffffffu, c.ix, 1);
-        const uint32_t py = __shfl_up_sync(0xffffffffu, c.iy, 1);
-        const uint32_t pz = __shfl_up_sync(0xffffffffu, c.iz, 1);
-        const bool head = lane == 0 || px != c.ix || py != c.iy || pz != c.iz || !ok;
-        const unsigned heads = __ballot_sync(0xffffffffu, head);
-        if (heads == 0xffffffffu) {
-            if (ok) scatter_corners(a.table_grad, L, a.enc.hash_mask, c, v);
-            continue;
-        }
-        const uint32_t start = 31u - __clz(heads & (0xffffffffu >> (31u - lane)));
-#pragma unroll
-        for (int dd = 1; dd < 32; dd <<= 1) {
-#pragma unroll
-            for (int k = 0; k < 16; ++k) {
-                const float u = __shfl_up_sync(0xffffffffu, v[k], dd);
-                if (lane >= start + (uint32_t)dd) v[k] += u;
-            }
-        }
-        const bool tail = lane == 31u || ((heads >> (lane + 1)) & 1u);
-        if (ok && tail) scatter_corners(a.table_grad, L, a.enc.hash_mask, c, v);
+        const CellCoord c = cell_of(p, L.res);
+        warp_scatter_level(a.table_grad, L, a.enc.hash_mask, c, g.x * a.inv_n, g.y * a.inv_n,
+                           valid_lanes(i - (threadIdx.x & 31u), a.n));
     }
 }
 

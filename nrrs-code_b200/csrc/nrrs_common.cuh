@@ -203,6 +203,73 @@ __device__ __forceinline__ float corner_weight(const CellCoord& c, int k) {
     return wx * wy * wz;
 }
 
+// The 8 corner rows of cell c with per-corner feature gradients v[2k], v[2k+1] (corner order);
+// the x-neighbours of one (y, z) that share an aligned pair of rows go as one 16-byte
+// reduction, the others as two 8-byte ones.
+__device__ __forceinline__ void scatter_corners(float* table_grad, const LevelDev& L,
+                                                uint32_t mask, const CellCoord& c, const float* v) {
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) {
+        const uint32_t y = c.iy + (k2 & 1), z = c.iz + ((k2 >> 1) & 1);
+        const uint32_t r0 = grid_row(L, mask, c.ix, y, z);
+        const uint32_t r1 = grid_row(L, mask, c.ix + 1, y, z);
+        const float* a = v + 4 * k2;   // corner x: a[0], a[1]; corner x + 1: a[2], a[3]
+        if ((r0 >> 1) == (r1 >> 1)) {
+            float* q = table_grad + 4 * (size_t)(r0 >> 1);
+            if (r0 & 1u) red_add4(q, a[2], a[3], a[0], a[1]);
+            else red_add4(q, a[0], a[1], a[2], a[3]);
+        } else {
+            red_add2(table_grad + 2 * (size_t)r0, a[0], a[1]);
+            red_add2(table_grad + 2 * (size_t)r1, a[2], a[3]);
+        }
+    }
+}
+
+// Hash-grid gradient of one level: this lane's sample adds (g0, g1) x the trilinear weights to
+// the 8 corner rows of cell c. Every lane in `lanes` (a prefix of the warp: lanes 0 .. k-1) calls
+// it together. Samples that come in pixel order (a tracer's batch) put runs of neighbouring lanes
+// in the same cell, whose reductions would serialise on the same rows: such runs are summed by a
+// segmented shuffle scan and reduced once, by the run's last lane. A warp without runs (uniform
+// samples) reduces per lane.
+__device__ __forceinline__ void warp_scatter_level(float* table_grad, const LevelDev& L,
+                                                   uint32_t mask, const CellCoord& c, float g0,
+                                                   float g1, unsigned lanes) {
+    const uint32_t lane = threadIdx.x & 31u;
+    float v[16];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const float wk = corner_weight(c, k);
+        v[2 * k] = wk * g0;
+        v[2 * k + 1] = wk * g1;
+    }
+    const uint32_t px = __shfl_up_sync(lanes, c.ix, 1);
+    const uint32_t py = __shfl_up_sync(lanes, c.iy, 1);
+    const uint32_t pz = __shfl_up_sync(lanes, c.iz, 1);
+    const bool head = lane == 0 || px != c.ix || py != c.iy || pz != c.iz;
+    const unsigned heads = __ballot_sync(lanes, head);
+    if (heads == lanes) {
+        scatter_corners(table_grad, L, mask, c, v);
+        return;
+    }
+    const uint32_t start = 31u - __clz(heads & (0xffffffffu >> (31u - lane)));
+#pragma unroll
+    for (int dd = 1; dd < 32; dd <<= 1) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const float u = __shfl_up_sync(lanes, v[k], dd);
+            if (lane >= start + (uint32_t)dd) v[k] += u;
+        }
+    }
+    const bool tail = lane == 31u || !((lanes >> (lane + 1)) & 1u) || ((heads >> (lane + 1)) & 1u);
+    if (tail) scatter_corners(table_grad, L, mask, c, v);
+}
+
+// the lanes of this warp whose sample index (base of the warp's first lane + lane) is below n
+__device__ __forceinline__ unsigned valid_lanes(uint32_t warp_base, uint32_t n) {
+    const uint32_t k = n > warp_base ? n - warp_base : 0u;
+    return k >= 32u ? 0xffffffffu : ((1u << k) - 1u);
+}
+
 // entry e (0..3) of a 16-byte quad of table rows
 __device__ __forceinline__ uint32_t quad_pick(const uint4& q, uint32_t e) {
     const uint32_t lo = (e & 1u) ? q.y : q.x, hi = (e & 1u) ? q.w : q.z;
