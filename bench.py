@@ -17,7 +17,7 @@ Other workloads (--workload):
             layers (BF16 by default), 2^22-entry table, 10 training steps of 262,144 samples
   render1080p
             a path-traced 1920x1080 frame around the NRRS step: camera rays, then per bounce
-            (up to 6) BVH trace, shading into the vertex queue, nrrs_step (mixed precision),
+            (up to 6) BVH trace (rays sorted first), shading into the vertex queue, nrrs_step,
             scatter (NEE + BSDF rays) and shadow rays, in a closed room of 3000 boxes
             (36k triangles) seen from inside;
             metric path vertices/s
@@ -1074,6 +1074,7 @@ def run_render(args, rank, world, local_rank):
     film = torch.zeros((P, 9), dtype=torch.int64, device=dev)
     img = f(P, 3)
     scratch = torch.zeros(nb.shade_scratch_bytes(cap), dtype=torch.uint8, device=dev)
+    tscratch = torch.zeros(nb.trace_scratch_bytes(cap), dtype=torch.uint8, device=dev)
     n_rays, n_vert, qsize = i(1), i(1), i(1)
     rnd = torch.rand(cap, device=dev, generator=torch.Generator(device=dev).manual_seed(5))
     stats, rrs, rrs_norm = f(3 * cap), f(cap), f(cap)
@@ -1130,7 +1131,7 @@ def run_render(args, rank, world, local_rank):
                 ev.setdefault(("trace", depth), (torch.cuda.Event(enable_timing=True),
                                                  torch.cuda.Event(enable_timing=True)))
                 ev[("trace", depth)][0].record(cur)
-            nb.trace(scene, R, n_rays, cap, Hh, stream)
+            nb.trace_sorted(scene, R, n_rays, cap, Hh, tscratch, stream)
             if timing:
                 ev[("trace", depth)][1].record(cur)
             nb.shade(scene, R, Hh, n_rays, cap, depth, film, contrib if train else None, V,
@@ -1218,9 +1219,9 @@ def run_render(args, rank, world, local_rank):
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
     verts_per_frame = total_v / args.steps
-    # camera + resolve per frame; trace, shade (2), scatter, shadow per bounce run, and the last
-    # trace + shade of a frame whose queue ran out; plus the NRRS step's own launches
-    launches = (args.steps * 2 + bounces_run[0] * 5 + (net.launch_count() - launches0))
+    # camera + resolve per frame; ray sort (2), trace, shade (2), scatter, shadow per bounce run,
+    # and the last trace + shade of a frame whose queue ran out; plus the NRRS step's own launches
+    launches = (args.steps * 2 + bounces_run[0] * 7 + (net.launch_count() - launches0))
     if train:
         # per bounce: radiance of the shaded rays, record count + writes, patch counts, shadow
         # radiance; per frame: camera patch counts, pixel error (3), radiance pass + batch

@@ -698,6 +698,16 @@ int nrrs_camera_rays(const nrrs_camera* c, uint32_t sample, uint32_t seed,
 int nrrs_trace(const nrrs_scene* s, const nrrs_ray_soa* rays, const uint32_t* n_dev,
                uint32_t max_n, const nrrs_hit_soa* hits, void* stream);
 
+/* nrrs_trace with the rays walked in a spatial order: a counting sort of the ray indices by
+ * (direction octant, 12-bit Morton code of the origin in the scene's box) runs first, so that a
+ * warp's rays start close together and head the same way. Same hits as nrrs_trace, bit for bit
+ * (each written at its ray's own index). scratch: nrrs_trace_scratch_bytes(max_n) bytes of
+ * device memory, 4-byte aligned, not shared with a concurrent call. Below 65,536 rays (max_n)
+ * the sort is skipped. */
+uint64_t nrrs_trace_scratch_bytes(uint32_t max_n);
+int nrrs_trace_sorted(const nrrs_scene* s, const nrrs_ray_soa* rays, const uint32_t* n_dev,
+                      uint32_t max_n, const nrrs_hit_soa* hits, void* scratch, void* stream);
+
 /* handleEmissiveHit / handleMiss and the vertex queue: for each of the first *n_dev rays, an
  * emissive hit adds Le x thp (MIS-weighted against light sampling when pdf > 0) and a miss adds
  * environment x thp to film[pixel] and contrib[ray] ([max_n][3], 0 otherwise; the ray's node

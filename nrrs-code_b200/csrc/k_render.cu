@@ -246,11 +246,117 @@ __global__ void __launch_bounds__(256) k_camera(nrrs_camera c, uint32_t sample, 
     r.node[p] = -1;
 }
 
+// ---- ray order for the closest-hit trace: a counting sort by (direction octant, 12-bit Morton
+// code of the origin in the scene's box), so that the lanes of a warp start close together and
+// head the same way. Hits are written at the rays' own indices: the result does not depend on
+// the order. Scratch: kSortBins + 1 counters (the last one counts finished CTAs), then the order.
+constexpr uint32_t kSortBins = 1u << 15;
+constexpr uint32_t kSortMinRays = 65536;   // below this the sort costs more than it saves
+constexpr int kSortThreads = 256;
+
+__device__ __forceinline__ uint32_t ray_key(const nrrs_scene& s, const nrrs_ray_soa& r, uint32_t i) {
+    const V3 o = v3(r.origin + 3 * (size_t)i), d = v3(r.dir + 3 * (size_t)i);
+    const float oo[3] = {o.x, o.y, o.z};
+    uint32_t q[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {   // the root box: s.nodes[0..2] and [4..6]
+        const float f = (oo[k] - s.nodes[k]) / (s.nodes[4 + k] - s.nodes[k]) * 16.0f;
+        q[k] = f > 0.f ? min((uint32_t)f, 15u) : 0u;   // NaN and negative go to 0
+    }
+    uint32_t key = 0;
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+        key |= (((q[0] >> b) & 1u) << (3 * b)) | (((q[1] >> b) & 1u) << (3 * b + 1)) |
+               (((q[2] >> b) & 1u) << (3 * b + 2));
+    const uint32_t oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+    return (oct << 12) | key;
+}
+
+// counts per key (lanes of a warp with the same key take one atomic); the last CTA turns the
+// counts into exclusive offsets in place
+__global__ void __launch_bounds__(kSortThreads) k_sort_count(const __grid_constant__ nrrs_scene s,
+                                                             nrrs_ray_soa r, const uint32_t* n_dev,
+                                                             uint32_t max_n, uint32_t* hist) {
+    const uint32_t n = min(*n_dev, max_n);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = gridDim.x * (kSortThreads / 32);
+    const uint32_t w = blockIdx.x * (kSortThreads / 32) + (threadIdx.x >> 5);
+    for (uint32_t base = w * 32; base < n; base += warps * 32) {
+        const uint32_t i = base + lane;
+        const bool ok = i < n;
+        const uint32_t key = ok ? ray_key(s, r, i) : 0xffffffffu;
+        const unsigned same = __match_any_sync(0xffffffffu, key);
+        if (ok && lane == (uint32_t)(__ffs(same) - 1)) atomicAdd(&hist[key], (uint32_t)__popc(same));
+    }
+    __shared__ bool s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(&hist[kSortBins], 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    constexpr uint32_t kStrip = kSortBins / kSortThreads;   // 128 bins per thread
+    __shared__ uint32_t s_part[kSortThreads];
+    uint32_t* h = hist + threadIdx.x * kStrip;
+    uint32_t sum = 0;
+    for (uint32_t c = 0; c < kStrip; c += 32) {
+        uint32_t v[32];
+#pragma unroll
+        for (int k = 0; k < 32; ++k) v[k] = __ldcg(h + c + k);
+#pragma unroll
+        for (int k = 0; k < 32; ++k) sum += v[k];
+    }
+    s_part[threadIdx.x] = sum;
+    __syncthreads();
+    for (uint32_t off = 1; off < kSortThreads; off <<= 1) {
+        const uint32_t t = threadIdx.x >= off ? s_part[threadIdx.x - off] : 0u;
+        __syncthreads();
+        s_part[threadIdx.x] += t;
+        __syncthreads();
+    }
+    uint32_t run = s_part[threadIdx.x] - sum;
+    for (uint32_t c = 0; c < kStrip; c += 32) {
+        uint32_t v[32];
+#pragma unroll
+        for (int k = 0; k < 32; ++k) v[k] = __ldcg(h + c + k);
+#pragma unroll
+        for (int k = 0; k < 32; ++k) { h[c + k] = run; run += v[k]; }
+    }
+}
+
+// each ray index at its key's next slot
+__global__ void __launch_bounds__(kSortThreads) k_sort_scatter(const __grid_constant__ nrrs_scene s,
+                                                               nrrs_ray_soa r, const uint32_t* n_dev,
+                                                               uint32_t max_n, uint32_t* hist,
+                                                               uint32_t* order) {
+    const uint32_t n = min(*n_dev, max_n);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = gridDim.x * (kSortThreads / 32);
+    const uint32_t w = blockIdx.x * (kSortThreads / 32) + (threadIdx.x >> 5);
+    unsigned lt;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+    for (uint32_t base = w * 32; base < n; base += warps * 32) {
+        const uint32_t i = base + lane;
+        const bool ok = i < n;
+        const uint32_t key = ok ? ray_key(s, r, i) : 0xffffffffu;
+        const unsigned same = __match_any_sync(0xffffffffu, key);
+        const uint32_t leader = (uint32_t)(__ffs(same) - 1);
+        uint32_t slot = 0;
+        if (ok && lane == leader) slot = atomicAdd(&hist[key], (uint32_t)__popc(same));
+        slot = __shfl_sync(0xffffffffu, slot, (int)leader) + (uint32_t)__popc(same & lt);
+        if (ok && slot < n) order[slot] = i;
+    }
+}
+
+// closest hits of the first *n_dev rays, walked in `order` when given (null = queue order)
 __global__ void __launch_bounds__(128) k_trace(const __grid_constant__ nrrs_scene s,
                                                nrrs_ray_soa r, const uint32_t* n_dev,
-                                               uint32_t max_n, nrrs_hit_soa h) {
+                                               uint32_t max_n, nrrs_hit_soa h,
+                                               const uint32_t* order) {
     const uint32_t n = min(*n_dev, max_n);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t i = order ? order[k] : k;
+        if (i >= n) continue;
         Hit x{kMiss, 0.f, 0.f, 0.f};
         if (nonzero(v3(r.thp + 3 * (size_t)i)))
             x = closest_hit(s, v3(r.origin + 3 * (size_t)i), v3(r.dir + 3 * (size_t)i), INFINITY);
@@ -811,8 +917,33 @@ extern "C" int nrrs_trace(const nrrs_scene* s, const nrrs_ray_soa* rays, const u
                           uint32_t max_n, const nrrs_hit_soa* hits, void* stream) {
     if (!s || !rays || !n_dev || !hits) return NRRS_ERR_INVALID_ARG;
     if (max_n == 0) return NRRS_OK;
-    k_trace<<<grid_of(max_n, 128, 64), 128, 0, (cudaStream_t)stream>>>(*s, *rays, n_dev,
-                                                                                 max_n, *hits);
+    k_trace<<<grid_of(max_n, 128, 64), 128, 0, (cudaStream_t)stream>>>(*s, *rays, n_dev, max_n,
+                                                                        *hits, nullptr);
+    return ok(cudaGetLastError());
+}
+
+extern "C" uint64_t nrrs_trace_scratch_bytes(uint32_t max_n) {
+    return 4ull * (kSortBins + 64) + 4ull * max_n;
+}
+
+extern "C" int nrrs_trace_sorted(const nrrs_scene* s, const nrrs_ray_soa* rays,
+                                 const uint32_t* n_dev, uint32_t max_n, const nrrs_hit_soa* hits,
+                                 void* scratch, void* stream) {
+    if (!s || !rays || !n_dev || !hits || !scratch) return NRRS_ERR_INVALID_ARG;
+    if (max_n == 0) return NRRS_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint32_t* order = nullptr;
+    if (max_n >= kSortMinRays) {
+        uint32_t* hist = static_cast<uint32_t*>(scratch);
+        uint32_t* ord = hist + kSortBins + 64;
+        if (cudaMemsetAsync(hist, 0, 4ull * (kSortBins + 1), st) != cudaSuccess)
+            return NRRS_ERR_CUDA;
+        const int g = grid_of(max_n, kSortThreads, 8);
+        k_sort_count<<<g, kSortThreads, 0, st>>>(*s, *rays, n_dev, max_n, hist);
+        k_sort_scatter<<<g, kSortThreads, 0, st>>>(*s, *rays, n_dev, max_n, hist, ord);
+        order = ord;
+    }
+    k_trace<<<grid_of(max_n, 128, 64), 128, 0, st>>>(*s, *rays, n_dev, max_n, *hits, order);
     return ok(cudaGetLastError());
 }
 

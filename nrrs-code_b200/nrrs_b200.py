@@ -273,6 +273,9 @@ _SIGS = {
                                C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(RaySoA),
                                C.POINTER(ShadowSoA), C.c_void_p]),
     "nrrs_scene_set_nee": (C.c_int, [C.c_void_p, C.c_int32]),
+    "nrrs_trace_scratch_bytes": (C.c_uint64, [C.c_uint32]),
+    "nrrs_trace_sorted": (C.c_int, [C.c_void_p, C.POINTER(RaySoA), C.c_void_p, C.c_uint32,
+                                    C.POINTER(HitSoA), C.c_void_p, C.c_void_p]),
     "nrrs_scatter_fixed_rr": (C.c_int, [C.c_void_p, C.POINTER(PathVertices), C.c_void_p,
                                         C.c_uint32, C.c_float, C.c_uint32, C.c_uint32,
                                         C.POINTER(RaySoA), C.POINTER(ShadowSoA), C.c_void_p]),
@@ -726,6 +729,16 @@ def scatter(scene: Scene, v: PathVertices, rrs_norm, queue, queue_size_dev, max_
     _check(lib().nrrs_scatter(scene._h, C.byref(v), _ptr(rrs_norm), _ptr(queue),
                               _ptr(queue_size_dev), max_queue, depth, seed, C.byref(rays),
                               C.byref(shadow), stream), "nrrs_scatter")
+
+
+def trace_scratch_bytes(max_n: int) -> int:
+    return int(lib().nrrs_trace_scratch_bytes(max_n))
+
+
+def trace_sorted(scene: Scene, rays: RaySoA, n_dev, max_n: int, hits: HitSoA, scratch, stream=0):
+    """nrrs_trace with the rays walked in (direction octant, origin Morton) order; same hits."""
+    _check(lib().nrrs_trace_sorted(scene._h, C.byref(rays), _ptr(n_dev), max_n, C.byref(hits),
+                                   _ptr(scratch), stream), "nrrs_trace_sorted")
 
 
 def scatter_fixed_rr(scene: Scene, v: PathVertices, n_dev, max_n: int, rr: float, depth: int,

@@ -113,7 +113,7 @@ def test_gpu_trace_matches_brute_force():
     assert (want["prim"] != 0xffffffff).mean() > 0.5
 
 
-def run_frame_pair(gs, hs, cam, seed, bounces, factors, fixed_rr=None):
+def run_frame_pair(gs, hs, cam, seed, bounces, factors, fixed_rr=None, sorted_trace=False):
     """One frame on the GPU and in the oracle, bounce by bounce, with the emitted queue of the
     library's decision (nrrs_decide_emit_noalloc) on the given factor generator between them, or
     at the depths in fixed_rr ({depth: rr}) the fixed Russian-roulette scatter; every array
@@ -128,6 +128,7 @@ def run_frame_pair(gs, hs, cam, seed, bounces, factors, fixed_rr=None):
     contrib = torch.zeros((cap, 3), device="cuda")
     scontrib = torch.zeros((cap, 3), device="cuda")
     scratch = torch.zeros(nb.shade_scratch_bytes(cap), dtype=torch.uint8, device="cuda")
+    tscratch = torch.zeros(nb.trace_scratch_bytes(cap), dtype=torch.uint8, device="cuda")
     n_rays = torch.tensor([n], dtype=torch.int32, device="cuda")
     n_vert = torch.zeros(1, dtype=torch.int32, device="cuda")
     qsize = torch.zeros(1, dtype=torch.int32, device="cuda")
@@ -139,7 +140,11 @@ def run_frame_pair(gs, hs, cam, seed, bounces, factors, fixed_rr=None):
     rng = np.random.default_rng(seed)
     for depth in range(bounces):
         nr = int(host(n_rays)[0])
-        nb.trace(gs, nb.soa(nb.RaySoA, rays), n_rays, cap, nb.soa(nb.HitSoA, hits), stream())
+        if sorted_trace:
+            nb.trace_sorted(gs, nb.soa(nb.RaySoA, rays), n_rays, cap, nb.soa(nb.HitSoA, hits),
+                            tscratch, stream())
+        else:
+            nb.trace(gs, nb.soa(nb.RaySoA, rays), n_rays, cap, nb.soa(nb.HitSoA, hits), stream())
         hh = hs.trace(hr)
         same(to_host(hits, nr), hh, ("prim", "t", "u", "v"))
         nb.shade(gs, nb.soa(nb.RaySoA, rays), nb.soa(nb.HitSoA, hits), n_rays, cap, depth, film,
@@ -205,10 +210,11 @@ def test_gpu_frame_matches_oracle():
 
 def test_gpu_closed_room_frame_matches_oracle():
     """The render benchmark's kind of scene: a closed room seen from inside, where no ray
-    escapes; five bounces with splitting and killing."""
+    escapes; three bounces with splitting and killing, traced in the sorted order."""
     gs, hs = scene_pair(7, boxes=120, closed=True)
-    cam = nb.room_camera(48, 32, inside=True)
-    img, _ = run_frame_pair(gs, hs, cam, 9, 5, lambda rng, n: rng.uniform(0.3, 2.5, n))
+    cam = nb.room_camera(320, 240, inside=True)   # 76,800 rays: the sorted trace sorts
+    img, _ = run_frame_pair(gs, hs, cam, 9, 3, lambda rng, n: rng.uniform(0.3, 2.5, n),
+                            sorted_trace=True)
     assert img.mean() > 0
 
 
@@ -466,3 +472,36 @@ def test_gpu_nee_and_bsdf_sampling_agree():
     se = np.sqrt(np.var(on) / len(on) + np.var(off) / len(off))
     assert a > 0 and abs(a - b) < 4 * se + 0.01 * a, (a, b, se)
     assert np.std(on) < np.std(off)        # light sampling lowers the variance
+
+
+def test_gpu_trace_sorted_equals_trace():
+    """The sorted trace writes the same hits as the plain one, bit for bit: on the benchmark's
+    scene with a queue large enough to sort (camera rays and random rays, with empty slots and a
+    device count below the capacity), and below the sorting threshold."""
+    torch = torch_cuda()
+    v, t, m, ma, e = nb.synth_scene(7, n_boxes=3000, closed=True)
+    gs = nb.Scene(v, t, m, ma, e)
+    rng = np.random.default_rng(12)
+    for n, cap in ((150_000, 160_000), (40_000, 40_000)):
+        cam = nb.room_camera(500, n // 500, inside=True)
+        rays = empty_rays(cap)
+        nb.camera_rays(cam, 2, 5, nb.soa(nb.RaySoA, rays), stream())
+        k = n // 2   # the second half: random rays inside the room, some of them empty slots
+        o = rng.uniform(0.02, 0.98, (k, 3)).astype(np.float32)
+        d = rng.normal(size=(k, 3)).astype(np.float32)
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        thp = np.ones((k, 3), np.float32)
+        thp[::7] = 0.0
+        rays["origin"][n - k:n] = torch.from_numpy(o).cuda()
+        rays["dir"][n - k:n] = torch.from_numpy(d).cuda()
+        rays["thp"][n - k:n] = torch.from_numpy(thp).cuda()
+        cnt = torch.tensor([n], dtype=torch.int32, device="cuda")
+        a, b = empty_hits(cap), empty_hits(cap)
+        b["prim"].fill_(-3)
+        scratch = torch.zeros(nb.trace_scratch_bytes(cap), dtype=torch.uint8, device="cuda")
+        nb.trace(gs, nb.soa(nb.RaySoA, rays), cnt, cap, nb.soa(nb.HitSoA, a), stream())
+        nb.trace_sorted(gs, nb.soa(nb.RaySoA, rays), cnt, cap, nb.soa(nb.HitSoA, b), scratch,
+                        stream())
+        same(to_host(a, n), to_host(b, n), ("prim", "t", "u", "v"))
+        assert (host(b["prim"])[n:] == -3).all()      # nothing written past the device count
+    gs.close()
