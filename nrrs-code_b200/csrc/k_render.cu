@@ -1,7 +1,8 @@
 // k_render.cu -- the wavefront steps either side of the NRRS step: camera rays, BVH traversal
-// (closest hit and shadow any-hit), the hit/miss shading that forms the next vertex queue, and
-// the scatter step that consumes the emitted queue (thp / rrs, next-event estimation, BSDF
-// sampling). Kernels, the host BVH build and the C-ABI (include/nrrs.h).
+// (closest hit, optionally in a sorted ray order, and shadow any-hit), the hit/miss shading that
+// forms the next vertex queue, and the scatter step that consumes the emitted queue (thp / rrs,
+// next-event estimation, BSDF sampling) or runs fixed Russian roulette. Kernels, the host BVH
+// build and the C-ABI (include/nrrs.h).
 //
 // Replaces, in banbao990/NRRS-Code:
 //   OptiX closest-hit / any-hit programs        src/render/nrrs/device.cu:48-161
@@ -9,11 +10,15 @@
 //   handleIntersections, generateScatteredRays  src/render/nrrs/integrator.cpp:737-887
 //   generateCameraRays                          src/render/nrrs/integrator.cpp:889-935
 //
-// Everything a frame computes is reproducible: random numbers are a counter-based hash of
-// (seed, depth, slot, dimension); every FP32 operation is written out without contraction; ties
-// between equally close triangles go to the lower triangle index; the film and the contributions
-// are exact fixed-point sums. A C restatement of the same steps (brute-force intersection instead
-// of the BVH) checks the kernels bit for bit.
+// Everything a frame computes is reproducible:
+// - random numbers are a counter-based hash of (seed, depth, slot, dimension);
+// - every FP32 operation is written out and rounded on its own, except the triangle test's
+//   products, which are explicit fused multiply-adds;
+// - ties between equally close triangles go to the lower triangle index, whatever the BVH or
+//   the order the rays are walked in;
+// - the film and the contributions are exact fixed-point sums.
+// A C restatement of the same steps (brute-force intersection instead of the BVH) checks the
+// kernels bit for bit.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
