@@ -41,6 +41,7 @@ struct nrrs_scene {
     float env[3] = {0.f, 0.f, 0.f};
     uint32_t nt = 0, nn = 0, nl = 0, nm = 0, max_depth = 0;
     uint32_t nee = 1;             // next-event estimation on (mEnableNEE)
+    uint8_t* mat_spec = nullptr;  // [nm] 1 = perfect mirror (null: no mirrors)
 };
 
 namespace nrrs {
@@ -374,36 +375,15 @@ __global__ void __launch_bounds__(128) k_trace(const __grid_constant__ nrrs_scen
 
 constexpr int kShadeChunk = 1024;
 
-// hits per chunk of rays; the last CTA turns the counts into offsets and the total
-__global__ void __launch_bounds__(256) k_shade_count(nrrs_ray_soa r, nrrs_hit_soa h,
-                                                     const uint32_t* n_dev, uint32_t max_n,
-                                                     uint32_t* scratch, uint32_t* n_out) {
-    __shared__ unsigned s_part[8], s_last;
-    __shared__ unsigned long long s_w[8];
-    const uint32_t n = min(*n_dev, max_n);
-    const uint32_t chunks = (max_n + kShadeChunk - 1) / kShadeChunk;
-    uint32_t* counts = scratch + 4;
-    uint32_t* offsets = counts + chunks;
-    const uint32_t c = blockIdx.x;
+__device__ __forceinline__ bool mirror_hit(const nrrs_scene& s, uint32_t prim) {
+    return s.mat_spec && s.mat_spec[s.tri_mat[prim]];
+}
+
+// exclusive scan of counts[0 .. chunks) into offsets by one CTA of 256 threads (a strip per
+// thread); returns the total to every thread
+__device__ uint32_t block_scan_chunks(const uint32_t* counts, uint32_t* offsets, uint32_t chunks,
+                                      unsigned long long* s_w) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    unsigned k = 0;
-    for (uint32_t i = c * kShadeChunk + threadIdx.x; i < min(n, (c + 1) * kShadeChunk); i += 256)
-        k += (h.prim[i] != kMiss && nonzero(v3(r.thp + 3 * (size_t)i))) ? 1u : 0u;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) k += __shfl_xor_sync(0xffffffffu, k, o);
-    if (lane == 0) s_part[wid] = k;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned t = 0;
-        for (int w = 0; w < 8; ++w) t += s_part[w];
-        counts[c] = t;
-        __threadfence();
-        s_last = atomicAdd(scratch, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!s_last) return;
-    // the last CTA: exclusive scan of the chunk counts, a strip per thread
-    __threadfence();
     const uint32_t per = (chunks + 255) / 256;
     const uint32_t lo = min(chunks, threadIdx.x * per), hi = min(chunks, lo + per);
     unsigned long long strip = 0;
@@ -414,38 +394,110 @@ __global__ void __launch_bounds__(256) k_shade_count(nrrs_ray_soa r, nrrs_hit_so
         const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += y;
     }
+    __syncthreads();
     if (lane == 31) s_w[wid] = incl;
     __syncthreads();
-    unsigned long long run = incl - strip;
-    for (int w = 0; w < wid; ++w) run += s_w[w];
+    unsigned long long run = incl - strip, total = 0;
+    for (int w = 0; w < 8; ++w) {
+        if (w < wid) run += s_w[w];
+        total += s_w[w];
+    }
     for (uint32_t q = lo; q < hi; ++q) {
         offsets[q] = (uint32_t)run;
         run += __ldcg(counts + q);
     }
+    return (uint32_t)total;
+}
+
+// surface hits per chunk of rays (inference queue and, with split, mirror queue); the last CTA
+// turns the counts into offsets and the totals
+__global__ void __launch_bounds__(256) k_shade_count(const __grid_constant__ nrrs_scene s,
+                                                     nrrs_ray_soa r, nrrs_hit_soa h,
+                                                     const uint32_t* n_dev, uint32_t max_n,
+                                                     uint32_t* scratch, uint32_t* n_out,
+                                                     uint32_t* n_spec_out) {
+    __shared__ unsigned s_part[2][8], s_last;
+    __shared__ unsigned long long s_w[8];
+    const uint32_t n = min(*n_dev, max_n);
+    const uint32_t chunks = (max_n + kShadeChunk - 1) / kShadeChunk;
+    uint32_t* counts = scratch + 4;
+    uint32_t* offsets = counts + chunks;
+    uint32_t* counts_s = offsets + chunks;
+    uint32_t* offsets_s = counts_s + chunks;
+    const bool split = n_spec_out != nullptr;
+    const uint32_t c = blockIdx.x;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned k = 0, ks = 0;
+    for (uint32_t i = c * kShadeChunk + threadIdx.x; i < min(n, (c + 1) * kShadeChunk); i += 256) {
+        const uint32_t prim = h.prim[i];
+        if (prim == kMiss || !nonzero(v3(r.thp + 3 * (size_t)i))) continue;
+        if (split && mirror_hit(s, prim)) ++ks;
+        else ++k;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        k += __shfl_xor_sync(0xffffffffu, k, o);
+        ks += __shfl_xor_sync(0xffffffffu, ks, o);
+    }
+    if (lane == 0) { s_part[0][wid] = k; s_part[1][wid] = ks; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned t = 0, ts = 0;
+        for (int w = 0; w < 8; ++w) { t += s_part[0][w]; ts += s_part[1][w]; }
+        counts[c] = t;
+        counts_s[c] = ts;
+        __threadfence();
+        s_last = atomicAdd(scratch, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    // the last CTA: exclusive scans of the chunk counts
+    __threadfence();
+    const uint32_t total = block_scan_chunks(counts, offsets, chunks, s_w);
+    const uint32_t total_s = split ? block_scan_chunks(counts_s, offsets_s, chunks, s_w) : 0u;
     if (threadIdx.x == 255) {
-        *n_out = (uint32_t)run;
+        *n_out = total;
+        if (split) *n_spec_out = total_s;
         scratch[0] = 0;
         __threadfence();
     }
 }
 
+__device__ __forceinline__ void put_vertex(const nrrs_path_vertices& out, size_t o, V3 pos, V3 d,
+                                           V3 nrm, V3 alb, float rough, V3 thp, uint32_t depth,
+                                           uint32_t pixel, int32_t node) {
+    put(out.pos + 3 * o, pos);
+    put(out.wi + 3 * o, mul(d, -1.0f));
+    put(out.normal + 3 * o, nrm);
+    put(out.albedo + 3 * o, alb);
+    out.roughness[o] = rough;
+    put(out.thp + 3 * o, thp);
+    out.depth[o] = depth;
+    out.pixel[o] = pixel;
+    out.node[o] = node;
+}
+
+// emission and misses into the film; surface hits compacted in ray order into the inference
+// queue `out` or, when `split` and the material is a mirror, the specular queue `outs`
 __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ nrrs_scene s,
                                                nrrs_ray_soa r, nrrs_hit_soa h,
                                                const uint32_t* n_dev, uint32_t max_n,
                                                uint32_t depth, int64_t* film, float* contrib,
-                                               nrrs_path_vertices out, const uint32_t* scratch) {
-    __shared__ unsigned s_warp[8];
+                                               nrrs_path_vertices out, nrrs_path_vertices outs,
+                                               int split, const uint32_t* scratch) {
+    __shared__ unsigned s_warp[2][8];
     const uint32_t n = min(*n_dev, max_n);
     const uint32_t chunks = (max_n + kShadeChunk - 1) / kShadeChunk;
     const uint32_t c = blockIdx.x;
     const uint32_t base = scratch[4 + chunks + c];
+    const uint32_t base_s = split ? scratch[4 + 3 * chunks + c] : 0u;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     unsigned lt;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
-    unsigned run = 0;   // vertices of the earlier passes of this chunk
+    unsigned run = 0, run_s = 0;   // vertices of the earlier passes of this chunk
     for (uint32_t j = 0; j < kShadeChunk / 256; ++j) {
         const uint32_t i = c * kShadeChunk + j * 256 + threadIdx.x;
-        bool vert = false;
+        bool vert = false, mirror = false;
         V3 add_c = {0.f, 0.f, 0.f};
         V3 pos{}, nrm{}, alb{}, thp{}, d{};
         if (i < n) {
@@ -478,35 +530,61 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ nrrs_scen
                         }
                         add_c = mul(vmul(le, thp), w);
                     }
-                    vert = true;
+                    mirror = split && mirror_hit(s, prim);
+                    vert = !mirror;
                 }
             }
             if (contrib) put(contrib + 3 * (size_t)i, add_c);
             if (nonzero(add_c)) film_add(film, r.pixel[i], add_c);
         }
         const unsigned m = __ballot_sync(0xffffffffu, vert);
-        if (lane == 0) s_warp[wid] = __popc(m);
+        const unsigned ms = __ballot_sync(0xffffffffu, mirror);
+        if (lane == 0) { s_warp[0][wid] = __popc(m); s_warp[1][wid] = __popc(ms); }
         __syncthreads();
-        unsigned before = 0, total = 0;
+        unsigned before = 0, total = 0, before_s = 0, total_s = 0;
         for (int w = 0; w < 8; ++w) {
-            before += w < wid ? s_warp[w] : 0u;
-            total += s_warp[w];
+            before += w < wid ? s_warp[0][w] : 0u;
+            total += s_warp[0][w];
+            before_s += w < wid ? s_warp[1][w] : 0u;
+            total_s += s_warp[1][w];
         }
-        if (vert) {
-            const size_t o = (size_t)base + run + before + __popc(m & lt);
-            put(out.pos + 3 * o, pos);
-            put(out.wi + 3 * o, mul(d, -1.0f));
-            put(out.normal + 3 * o, nrm);
-            put(out.albedo + 3 * o, alb);
-            out.roughness[o] = 1.0f;
-            put(out.thp + 3 * o, thp);
-            out.depth[o] = depth;
-            out.pixel[o] = r.pixel[i];
-            out.node[o] = r.node[i];
-        }
+        if (vert)
+            put_vertex(out, (size_t)base + run + before + __popc(m & lt), pos, d, nrm, alb, 1.0f,
+                       thp, depth, r.pixel[i], r.node[i]);
+        if (mirror)
+            put_vertex(outs, (size_t)base_s + run_s + before_s + __popc(ms & lt), pos, d, nrm, alb,
+                       0.0f, thp, depth, r.pixel[i], r.node[i]);
         run += total;
+        run_s += total_s;
         __syncthreads();
     }
+}
+
+// the mirror bounce of the first *n_dev specular vertices into ray slots *off_dev + j: reflected
+// direction, thp x albedo, pdf 0 (the next emitter hit counts in full), no light sampling and
+// no RRS (the reference pushes these vertices to the emitted queue once, with rrs 1). Slots at
+// or past max_rays are dropped; *n_rays_out = min(*off_dev + *n_dev, max_rays).
+__global__ void __launch_bounds__(128) k_scatter_specular(nrrs_path_vertices v,
+                                                          const uint32_t* n_dev, uint32_t max_n,
+                                                          const uint32_t* off_dev,
+                                                          uint32_t max_rays, nrrs_ray_soa r,
+                                                          uint32_t* n_rays_out) {
+    const uint32_t n = min(*n_dev, max_n);
+    const uint32_t off = *off_dev;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const uint64_t slot = (uint64_t)off + j;
+        if (slot >= max_rays) continue;
+        const V3 nn = v3(v.normal + 3 * (size_t)j), din = mul(v3(v.wi + 3 * (size_t)j), -1.0f);
+        const V3 rf = normalize(sub(din, mul(nn, __fmul_rn(2.0f, dot(din, nn)))));
+        put(r.origin + 3 * slot, add(v3(v.pos + 3 * (size_t)j), mul(nn, kOffset)));
+        put(r.dir + 3 * slot, rf);
+        put(r.thp + 3 * slot, vmul(v3(v.thp + 3 * (size_t)j), v3(v.albedo + 3 * (size_t)j)));
+        r.pdf[slot] = 0.f;
+        r.pixel[slot] = v.pixel[j];
+        r.node[slot] = v.node[j];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        *n_rays_out = (uint32_t)min((uint64_t)off + n, (uint64_t)max_rays);
 }
 
 // generateScatteredRays for vertex x into slot j, with its throughput already divided by the RRS
@@ -892,6 +970,7 @@ extern "C" void nrrs_scene_destroy(nrrs_scene* s) {
     if (!s) return;
     cudaFree(s->tris); cudaFree(s->tri_id); cudaFree(s->tri_mat); cudaFree(s->tri_in);
     cudaFree(s->nodes); cudaFree(s->mats); cudaFree(s->lights); cudaFree(s->light_area);
+    cudaFree(s->mat_spec);
     delete s;
 }
 
@@ -954,23 +1033,64 @@ extern "C" int nrrs_trace_sorted(const nrrs_scene* s, const nrrs_ray_soa* rays,
 
 extern "C" uint64_t nrrs_shade_scratch_bytes(uint32_t max_n) {
     const uint64_t chunks = ((uint64_t)max_n + kShadeChunk - 1) / kShadeChunk;
-    return 4ull * (4 + 2 * chunks);
+    return 4ull * (4 + 4 * chunks);
+}
+
+extern "C" int nrrs_shade_split(const nrrs_scene* s, const nrrs_ray_soa* rays,
+                                const nrrs_hit_soa* hits, const uint32_t* n_dev, uint32_t max_n,
+                                uint32_t depth, int64_t* film, float* contrib,
+                                const nrrs_path_vertices* out, uint32_t* n_out_dev,
+                                const nrrs_path_vertices* out_specular, uint32_t* n_specular_dev,
+                                void* scratch, void* stream) {
+    if (!s || !rays || !hits || !n_dev || !film || !out || !n_out_dev || !scratch ||
+        (!out_specular) != (!n_specular_dev))
+        return NRRS_ERR_INVALID_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (max_n == 0) {
+        if (n_specular_dev && cudaMemsetAsync(n_specular_dev, 0, 4, st) != cudaSuccess)
+            return NRRS_ERR_CUDA;
+        return ok(cudaMemsetAsync(n_out_dev, 0, 4, st));
+    }
+    const uint32_t chunks = (max_n + kShadeChunk - 1) / kShadeChunk;
+    uint32_t* sc = static_cast<uint32_t*>(scratch);
+    if (cudaMemsetAsync(sc, 0, 4, st) != cudaSuccess) return NRRS_ERR_CUDA;   // the done counter
+    const int split = out_specular != nullptr;
+    k_shade_count<<<chunks, 256, 0, st>>>(*s, *rays, *hits, n_dev, max_n, sc, n_out_dev,
+                                          n_specular_dev);
+    k_shade<<<chunks, 256, 0, st>>>(*s, *rays, *hits, n_dev, max_n, depth, film, contrib, *out,
+                                    split ? *out_specular : *out, split, sc);
+    return ok(cudaGetLastError());
 }
 
 extern "C" int nrrs_shade(const nrrs_scene* s, const nrrs_ray_soa* rays, const nrrs_hit_soa* hits,
                           const uint32_t* n_dev, uint32_t max_n, uint32_t depth, int64_t* film,
                           float* contrib, const nrrs_path_vertices* out, uint32_t* n_out_dev,
                           void* scratch, void* stream) {
-    if (!s || !rays || !hits || !n_dev || !film || !out || !n_out_dev || !scratch)
+    return nrrs_shade_split(s, rays, hits, n_dev, max_n, depth, film, contrib, out, n_out_dev,
+                            nullptr, nullptr, scratch, stream);
+}
+
+extern "C" int nrrs_scatter_specular(const nrrs_scene* s, const nrrs_path_vertices* v,
+                                     const uint32_t* n_dev, uint32_t max_n,
+                                     const uint32_t* ray_offset_dev, uint32_t max_rays,
+                                     const nrrs_ray_soa* rays, uint32_t* n_rays_out_dev,
+                                     void* stream) {
+    if (!s || !v || !n_dev || !ray_offset_dev || !rays || !n_rays_out_dev ||
+        n_rays_out_dev == ray_offset_dev)
         return NRRS_ERR_INVALID_ARG;
-    cudaStream_t st = (cudaStream_t)stream;
-    if (max_n == 0) return ok(cudaMemsetAsync(n_out_dev, 0, 4, st));
-    const uint32_t chunks = (max_n + kShadeChunk - 1) / kShadeChunk;
-    uint32_t* sc = static_cast<uint32_t*>(scratch);
-    if (cudaMemsetAsync(sc, 0, 4, st) != cudaSuccess) return NRRS_ERR_CUDA;   // the done counter
-    k_shade_count<<<chunks, 256, 0, st>>>(*rays, *hits, n_dev, max_n, sc, n_out_dev);
-    k_shade<<<chunks, 256, 0, st>>>(*s, *rays, *hits, n_dev, max_n, depth, film, contrib, *out, sc);
+    k_scatter_specular<<<grid_of(std::max(max_n, 1u), 128), 128, 0, (cudaStream_t)stream>>>(
+        *v, n_dev, max_n, ray_offset_dev, max_rays, *rays, n_rays_out_dev);
     return ok(cudaGetLastError());
+}
+
+extern "C" int nrrs_scene_set_specular(nrrs_scene* s, const uint8_t* specular,
+                                       uint32_t n_materials) {
+    if (!s || !specular || n_materials != s->nm) return NRRS_ERR_INVALID_ARG;
+    if (!s->mat_spec && cudaMalloc(&s->mat_spec, n_materials) != cudaSuccess) {
+        s->mat_spec = nullptr;
+        return NRRS_ERR_CUDA;
+    }
+    return ok(cudaMemcpy(s->mat_spec, specular, n_materials, cudaMemcpyHostToDevice));
 }
 
 extern "C" int nrrs_scatter(const nrrs_scene* s, const nrrs_path_vertices* v, const float* rrs_norm,

@@ -274,6 +274,14 @@ _SIGS = {
                                C.POINTER(ShadowSoA), C.c_void_p]),
     "nrrs_scene_set_nee": (C.c_int, [C.c_void_p, C.c_int32]),
     "nrrs_trace_scratch_bytes": (C.c_uint64, [C.c_uint32]),
+    "nrrs_shade_split": (C.c_int, [C.c_void_p, C.POINTER(RaySoA), C.POINTER(HitSoA), C.c_void_p,
+                                   C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p,
+                                   C.POINTER(PathVertices), C.c_void_p, C.POINTER(PathVertices),
+                                   C.c_void_p, C.c_void_p, C.c_void_p]),
+    "nrrs_scene_set_specular": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
+    "nrrs_scatter_specular": (C.c_int, [C.c_void_p, C.POINTER(PathVertices), C.c_void_p,
+                                        C.c_uint32, C.c_void_p, C.c_uint32, C.POINTER(RaySoA),
+                                        C.c_void_p, C.c_void_p]),
     "nrrs_trace_sorted": (C.c_int, [C.c_void_p, C.POINTER(RaySoA), C.c_void_p, C.c_uint32,
                                     C.POINTER(HitSoA), C.c_void_p, C.c_void_p]),
     "nrrs_scatter_fixed_rr": (C.c_int, [C.c_void_p, C.POINTER(PathVertices), C.c_void_p,
@@ -687,6 +695,13 @@ class Scene:
 
     __del__ = close
 
+    def set_specular(self, specular):
+        """Mirror materials: specular[m] != 0 makes material m a perfect mirror."""
+        import numpy as np
+        a = np.ascontiguousarray(np.asarray(specular) != 0, np.uint8)
+        _check(lib().nrrs_scene_set_specular(self._h, a.ctypes.data, len(a)),
+               "nrrs_scene_set_specular")
+
     def set_nee(self, enable: bool):
         """Next-event estimation on or off (the reference's mEnableNEE)."""
         _check(lib().nrrs_scene_set_nee(self._h, int(bool(enable))), "nrrs_scene_set_nee")
@@ -729,6 +744,24 @@ def scatter(scene: Scene, v: PathVertices, rrs_norm, queue, queue_size_dev, max_
     _check(lib().nrrs_scatter(scene._h, C.byref(v), _ptr(rrs_norm), _ptr(queue),
                               _ptr(queue_size_dev), max_queue, depth, seed, C.byref(rays),
                               C.byref(shadow), stream), "nrrs_scatter")
+
+
+def shade_split(scene: Scene, rays: RaySoA, hits: HitSoA, n_dev, max_n: int, depth: int, film,
+                contrib, out: PathVertices, n_out_dev, out_specular: PathVertices,
+                n_specular_dev, scratch, stream=0):
+    """nrrs_shade with mirror hits in their own queue (the closest-hit specular branch)."""
+    _check(lib().nrrs_shade_split(scene._h, C.byref(rays), C.byref(hits), _ptr(n_dev), max_n,
+                                  depth, _ptr(film), _ptr(contrib), C.byref(out), _ptr(n_out_dev),
+                                  C.byref(out_specular), _ptr(n_specular_dev), _ptr(scratch),
+                                  stream), "nrrs_shade_split")
+
+
+def scatter_specular(scene: Scene, v: PathVertices, n_dev, max_n: int, ray_offset_dev,
+                     max_rays: int, rays: RaySoA, n_rays_out_dev, stream=0):
+    """The mirror bounce of the specular vertices into ray slots after the RRS-scattered ones."""
+    _check(lib().nrrs_scatter_specular(scene._h, C.byref(v), _ptr(n_dev), max_n,
+                                       _ptr(ray_offset_dev), max_rays, C.byref(rays),
+                                       _ptr(n_rays_out_dev), stream), "nrrs_scatter_specular")
 
 
 def trace_scratch_bytes(max_n: int) -> int:

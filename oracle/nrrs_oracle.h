@@ -135,6 +135,22 @@ void oracle_scatter(const float* tri, const uint32_t* mat, const float* mats, ui
                     float* r_thp, float* r_pdf, uint32_t* r_pixel, int32_t* r_node,
                     float* s_origin, float* s_dir, float* s_tmax, float* s_contrib,
                     uint32_t* s_pixel, int32_t* s_node);
+uint32_t oracle_shade_split(const float* tri, const uint32_t* mat, const float* mats, uint32_t nt,
+                            uint32_t nl, const float* env, const uint8_t* mat_spec,
+                            const float* origin, const float* dir, const float* thp,
+                            const float* pdf, const uint32_t* pixel, const int32_t* node,
+                            const uint32_t* prim, const float* t, uint32_t n, uint32_t depth,
+                            int64_t* film, float* contrib, float* o_pos, float* o_wi,
+                            float* o_nrm, float* o_alb, float* o_rough, float* o_thp,
+                            uint32_t* o_depth, uint32_t* o_pixel, int32_t* o_node,
+                            float* s_pos, float* s_wi, float* s_nrm, float* s_alb,
+                            float* s_rough, float* s_thp, uint32_t* s_depth, uint32_t* s_pixel,
+                            int32_t* s_node, uint32_t* n_spec);
+void oracle_scatter_specular(const float* pos, const float* wi, const float* nrm, const float* alb,
+                             const float* thp, const uint32_t* pixel, const int32_t* node,
+                             uint32_t n, uint32_t off, uint32_t max_rays, float* r_origin,
+                             float* r_dir, float* r_thp, float* r_pdf, uint32_t* r_pixel,
+                             int32_t* r_node);
 void oracle_scatter_fixed_rr(const float* tri, const uint32_t* mat, const float* mats,
                              const uint32_t* lights, const float* area, uint32_t nl,
                              const float* pos, const float* nrm, const float* alb,

@@ -426,6 +426,10 @@ class HostScene:
                                           self.mats.ctypes.data, self.tri.ctypes.data,
                                           self.lights.ctypes.data, self.area.ctypes.data))
         self.nee = True
+        self.spec = None          # [materials] uint8 mirror flags (set_specular)
+
+    def set_specular(self, specular):
+        self.spec = np.ascontiguousarray(np.asarray(specular) != 0, np.uint8)
 
     @property
     def nl_sampled(self) -> int:
@@ -453,6 +457,44 @@ class HostScene:
           *(np.ascontiguousarray(rays[k]).ctypes.data for k in ("origin", "dir", "thp")), n,
           *(h[k].ctypes.data for k in ("prim", "t", "u", "v")))
         return h
+
+    def shade_split(self, rays: dict, hits: dict, depth: int, film):
+        """(inference-queue vertices, specular-queue vertices, contributions)"""
+        n = len(rays["pixel"])
+        keys = ("pos", "wi", "normal", "albedo", "roughness", "thp", "depth", "pixel", "node")
+
+        def arrays():
+            return {"pos": np.zeros((n, 3), np.float32), "wi": np.zeros((n, 3), np.float32),
+                    "normal": np.zeros((n, 3), np.float32), "albedo": np.zeros((n, 3), np.float32),
+                    "roughness": np.zeros(n, np.float32), "thp": np.zeros((n, 3), np.float32),
+                    "depth": np.zeros(n, np.uint32), "pixel": np.zeros(n, np.uint32),
+                    "node": np.zeros(n, np.int32)}
+        out, outs = arrays(), arrays()
+        contrib = np.zeros((n, 3), np.float32)
+        ns = np.zeros(1, np.uint32)
+        spec = self.spec if self.spec is not None else np.zeros(len(self.mats), np.uint8)
+        f = lib().oracle_shade_split
+        f.restype = C.c_uint32
+        f.argtypes = [C.c_void_p] * 3 + [C.c_uint32, C.c_uint32] + [C.c_void_p] * 10 + \
+            [C.c_uint32, C.c_uint32] + [C.c_void_p] * 21
+        m = f(self.tri.ctypes.data, self.tm.ctypes.data, self.mats.ctypes.data, self.nt,
+              self.nl_sampled, self.env.ctypes.data, spec.ctypes.data,
+              *(np.ascontiguousarray(rays[k]).ctypes.data for k in
+                ("origin", "dir", "thp", "pdf", "pixel", "node")),
+              hits["prim"].ctypes.data, hits["t"].ctypes.data, n, depth, film.ctypes.data,
+              contrib.ctypes.data, *(out[k].ctypes.data for k in keys),
+              *(outs[k].ctypes.data for k in keys), ns.ctypes.data)
+        return ({k: v[:m] for k, v in out.items()}, {k: v[:int(ns[0])] for k, v in outs.items()},
+                contrib)
+
+    def scatter_specular(self, vs: dict, rays: dict, off: int, max_rays: int):
+        """writes the mirror bounces into rays (a dict of [max_rays] arrays) from slot off"""
+        n = len(vs["pixel"])
+        f = lib().oracle_scatter_specular
+        f.argtypes = [C.c_void_p] * 7 + [C.c_uint32] * 3 + [C.c_void_p] * 6
+        f(*(np.ascontiguousarray(vs[k]).ctypes.data for k in
+            ("pos", "wi", "normal", "albedo", "thp", "pixel", "node")), n, off, max_rays,
+          *(rays[k].ctypes.data for k in ("origin", "dir", "thp", "pdf", "pixel", "node")))
 
     def shade(self, rays: dict, hits: dict, depth: int, film):
         n = len(rays["pixel"])

@@ -180,15 +180,39 @@ void oracle_trace(const float* tri, const uint32_t* mat, const float* mats, uint
 }
 
 /* handleEmissiveHit / handleMiss and the vertex queue; returns the number of vertices */
-uint32_t oracle_shade(const float* tri, const uint32_t* mat, const float* mats, uint32_t nt,
-                      uint32_t nl, const float* env, const float* origin, const float* dir,
-                      const float* thp, const float* pdf, const uint32_t* pixel,
-                      const int32_t* node, const uint32_t* prim, const float* t, uint32_t n,
-                      uint32_t depth, int64_t* film, float* contrib, float* o_pos, float* o_wi,
-                      float* o_nrm, float* o_alb, float* o_rough, float* o_thp,
-                      uint32_t* o_depth, uint32_t* o_pixel, int32_t* o_node) {
+/* a path vertex into output slot m */
+static void put_vertex(float* o_pos, float* o_wi, float* o_nrm, float* o_alb, float* o_rough,
+                       float* o_thp, uint32_t* o_depth, uint32_t* o_pixel, int32_t* o_node,
+                       uint32_t m, v3 p, v3 d, v3 nn, const float* alb, float rough, v3 th,
+                       uint32_t depth, uint32_t pixel, int32_t node) {
+    st(o_pos + 3 * (uint64_t)m, p);
+    st(o_wi + 3 * (uint64_t)m, mul(d, -1.0f));
+    st(o_nrm + 3 * (uint64_t)m, nn);
+    st(o_alb + 3 * (uint64_t)m, ld(alb));
+    o_rough[m] = rough;
+    st(o_thp + 3 * (uint64_t)m, th);
+    o_depth[m] = depth;
+    o_pixel[m] = pixel;
+    o_node[m] = node;
+}
+
+/* handleEmissiveHit / handleMiss and the vertex queues. mat_spec (may be NULL) marks mirror
+ * materials: with s_* outputs given, their hits go to the specular queue (roughness 0) instead
+ * of the inference queue, as the reference's closest-hit program pushes specular hits straight
+ * to the scatter queue (device.cu:91-95). Returns the inference-queue size; *n_spec the other. */
+uint32_t oracle_shade_split(const float* tri, const uint32_t* mat, const float* mats, uint32_t nt,
+                            uint32_t nl, const float* env, const uint8_t* mat_spec,
+                            const float* origin, const float* dir, const float* thp,
+                            const float* pdf, const uint32_t* pixel, const int32_t* node,
+                            const uint32_t* prim, const float* t, uint32_t n, uint32_t depth,
+                            int64_t* film, float* contrib, float* o_pos, float* o_wi,
+                            float* o_nrm, float* o_alb, float* o_rough, float* o_thp,
+                            uint32_t* o_depth, uint32_t* o_pixel, int32_t* o_node,
+                            float* s_pos, float* s_wi, float* s_nrm, float* s_alb,
+                            float* s_rough, float* s_thp, uint32_t* s_depth, uint32_t* s_pixel,
+                            int32_t* s_node, uint32_t* n_spec) {
     scene_t s = mk(tri, mat, mats, nt, NULL, NULL, nl, env);
-    uint32_t m = 0;
+    uint32_t m = 0, ms = 0;
     for (uint32_t i = 0; i < n; ++i) {
         const v3 th = ld(thp + 3 * (uint64_t)i), d = ld(dir + 3 * (uint64_t)i);
         v3 c = {0.f, 0.f, 0.f};
@@ -213,22 +237,56 @@ uint32_t oracle_shade(const float* tri, const uint32_t* mat, const float* mats, 
                     }
                     c = mul(vmul(le, th), w);
                 }
-                st(o_pos + 3 * (uint64_t)m, p);
-                st(o_wi + 3 * (uint64_t)m, mul(d, -1.0f));
-                st(o_nrm + 3 * (uint64_t)m, nn);
-                st(o_alb + 3 * (uint64_t)m, ld(mm));
-                o_rough[m] = 1.0f;
-                st(o_thp + 3 * (uint64_t)m, th);
-                o_depth[m] = depth;
-                o_pixel[m] = pixel[i];
-                o_node[m] = node[i];
-                ++m;
+                if (s_pos && mat_spec && mat_spec[mat[prim[i]]]) {
+                    put_vertex(s_pos, s_wi, s_nrm, s_alb, s_rough, s_thp, s_depth, s_pixel, s_node,
+                               ms++, p, d, nn, mm, 0.0f, th, depth, pixel[i], node[i]);
+                } else {
+                    put_vertex(o_pos, o_wi, o_nrm, o_alb, o_rough, o_thp, o_depth, o_pixel, o_node,
+                               m++, p, d, nn, mm, 1.0f, th, depth, pixel[i], node[i]);
+                }
             }
         }
         st(contrib + 3 * (uint64_t)i, c);
         if (nonzero(c)) film_add(film, pixel[i], c);
     }
+    if (n_spec) *n_spec = ms;
     return m;
+}
+
+uint32_t oracle_shade(const float* tri, const uint32_t* mat, const float* mats, uint32_t nt,
+                      uint32_t nl, const float* env, const float* origin, const float* dir,
+                      const float* thp, const float* pdf, const uint32_t* pixel,
+                      const int32_t* node, const uint32_t* prim, const float* t, uint32_t n,
+                      uint32_t depth, int64_t* film, float* contrib, float* o_pos, float* o_wi,
+                      float* o_nrm, float* o_alb, float* o_rough, float* o_thp,
+                      uint32_t* o_depth, uint32_t* o_pixel, int32_t* o_node) {
+    return oracle_shade_split(tri, mat, mats, nt, nl, env, NULL, origin, dir, thp, pdf, pixel,
+                              node, prim, t, n, depth, film, contrib, o_pos, o_wi, o_nrm, o_alb,
+                              o_rough, o_thp, o_depth, o_pixel, o_node, NULL, NULL, NULL, NULL,
+                              NULL, NULL, NULL, NULL, NULL, NULL);
+}
+
+/* the specular bounce of the first n specular vertices (perfect mirror, reflectance = albedo)
+ * into ray slots off .. off + n - 1 (slots at or past max_rays are dropped): no light sampling
+ * and no RRS (the reference pushes these vertices to the emitted queue once, with rrs 1); the
+ * ray's pdf is 0, so the emitter it hits counts without an MIS weight. */
+void oracle_scatter_specular(const float* pos, const float* wi, const float* nrm, const float* alb,
+                             const float* thp, const uint32_t* pixel, const int32_t* node,
+                             uint32_t n, uint32_t off, uint32_t max_rays, float* r_origin,
+                             float* r_dir, float* r_thp, float* r_pdf, uint32_t* r_pixel,
+                             int32_t* r_node) {
+    for (uint32_t j = 0; j < n; ++j) {
+        const uint64_t slot = (uint64_t)off + j;
+        if (slot >= max_rays) continue;
+        const v3 nn = ld(nrm + 3 * (uint64_t)j), din = mul(ld(wi + 3 * (uint64_t)j), -1.0f);
+        const v3 rf = normalize(sub(din, mul(nn, 2.0f * dot(din, nn))));
+        st(r_origin + 3 * slot, add(ld(pos + 3 * (uint64_t)j), mul(nn, OFFSET)));
+        st(r_dir + 3 * slot, rf);
+        st(r_thp + 3 * slot, vmul(ld(thp + 3 * (uint64_t)j), ld(alb + 3 * (uint64_t)j)));
+        r_pdf[slot] = 0.f;
+        r_pixel[slot] = pixel[j];
+        r_node[slot] = node[j];
+    }
 }
 
 /* the scene arrays of the scatter steps */

@@ -505,3 +505,97 @@ def test_gpu_trace_sorted_equals_trace():
         same(to_host(a, n), to_host(b, n), ("prim", "t", "u", "v"))
         assert (host(b["prim"])[n:] == -3).all()      # nothing written past the device count
     gs.close()
+
+
+@pytest.mark.parametrize("closed", [False, True], ids=["open", "closed"])
+def test_gpu_mirror_frame_matches_oracle(closed):
+    """Mirror materials: their hits bypass the inference queue (the closest-hit program's
+    specular branch) and count as n_specular against the budget; their vertices bounce once,
+    unconditionally, into the ray slots after the RRS-scattered ones. A whole frame, bit for bit,
+    with every array compared as it is produced."""
+    torch = torch_cuda()
+    v, t, m, ma, e = nb.synth_scene(13, n_boxes=60, closed=closed)
+    spec = np.zeros(len(ma), np.uint8)
+    spec[4::3] = 1                                    # every third box material is a mirror
+    gs, hs = nb.Scene(v, t, m, ma, e), O.HostScene(v, t, m, ma, e)
+    gs.set_specular(spec)
+    hs.set_specular(spec)
+    cam = nb.room_camera(64, 48, inside=closed)
+    n = cam.width * cam.height
+    cap = 4 * n
+    seed = 31
+    film = torch.zeros((n, 9), dtype=torch.int64, device="cuda")
+    hfilm = np.zeros((n, 9), np.int64)
+    rays, hits = empty_rays(cap), empty_hits(cap)
+    verts, verts_s, shadow = empty_vertices(cap), empty_vertices(cap), empty_shadow(cap)
+    contrib = torch.zeros((cap, 3), device="cuda")
+    scontrib = torch.zeros((cap, 3), device="cuda")
+    scratch = torch.zeros(nb.shade_scratch_bytes(cap), dtype=torch.uint8, device="cuda")
+    i32 = lambda: torch.zeros(1, dtype=torch.int32, device="cuda")  # noqa: E731
+    n_rays, n_vert, n_spec, qsize, n_next = i32(), i32(), i32(), i32(), i32()
+    n_rays.fill_(n)
+    queue = torch.zeros(cap, dtype=torch.int32, device="cuda")
+    rrs_norm = torch.zeros(cap, device="cuda")
+    nb.camera_rays(cam, 0, seed, nb.soa(nb.RaySoA, rays), stream())
+    hr = hs.camera_rays(cam, 0, seed)
+    dp = nb.default_decide(clamp_max=4.0)
+    rng = np.random.default_rng(seed)
+    mirrored = 0
+    for depth in range(5):
+        nr = int(host(n_rays)[0])
+        assert nr == len(hr["pixel"])
+        nb.trace(gs, nb.soa(nb.RaySoA, rays), n_rays, cap, nb.soa(nb.HitSoA, hits), stream())
+        hh = hs.trace(hr)
+        same(to_host(hits, nr), hh, ("prim", "t", "u", "v"))
+        nb.shade_split(gs, nb.soa(nb.RaySoA, rays), nb.soa(nb.HitSoA, hits), n_rays, cap, depth,
+                       film, contrib, nb.soa(nb.PathVertices, verts), n_vert,
+                       nb.soa(nb.PathVertices, verts_s), n_spec, scratch, stream())
+        hv, hvs, hc = hs.shade_split(hr, hh, depth, hfilm)
+        nv, ns = int(host(n_vert)[0]), int(host(n_spec)[0])
+        assert (nv, ns) == (len(hv["pos"]), len(hvs["pos"]))
+        same(to_host(verts, nv), hv, nb.PATH_VERTEX_FIELDS)
+        same(to_host(verts_s, ns), hvs, nb.PATH_VERTEX_FIELDS)
+        assert host(contrib)[:nr].tobytes() == hc.tobytes()
+        assert host(film).tobytes() == hfilm.tobytes()
+        mirrored += ns
+        if nv + ns == 0:
+            break
+        # the decision on the inference queue; the budget counts the specular vertices too
+        f = rng.uniform(0.3, 2.5, nv).astype(np.float32)
+        rnd = rng.uniform(size=nv).astype(np.float32)
+        nq = 0
+        if nv:
+            rc = nb.decide_emit_noalloc(torch.from_numpy(f).cuda(), torch.from_numpy(rnd).cuda(),
+                                        nv, nv + ns, ns, dp, rrs_norm, None, queue, cap, qsize,
+                                        None, stream())
+            assert rc == 0
+            o = O.decide_emit(f, rnd, nv + ns, ns, dp, capacity=cap, shift_n=nb.NOALLOC_MAX_N)
+            nq = int(host(qsize)[0])
+            assert nq == o["total"]
+        else:
+            qsize.zero_()
+        nb.scatter(gs, nb.soa(nb.PathVertices, verts), rrs_norm, queue, qsize, cap, depth, seed,
+                   nb.soa(nb.RaySoA, rays), nb.soa(nb.ShadowSoA, shadow), stream())
+        nb.scatter_specular(gs, nb.soa(nb.PathVertices, verts_s), n_spec, cap, qsize, cap,
+                            nb.soa(nb.RaySoA, rays), n_next, stream())
+        full = {"origin": np.zeros((cap, 3), np.float32), "dir": np.zeros((cap, 3), np.float32),
+                "thp": np.zeros((cap, 3), np.float32), "pdf": np.zeros(cap, np.float32),
+                "pixel": np.zeros(cap, np.uint32), "node": np.zeros(cap, np.int32)}
+        if nq:
+            hr_d, hsh = hs.scatter(hv, o["rrs_norm"], o["queue"], depth, seed)
+            for k in full:
+                full[k][:nq] = hr_d[k]
+        hs.scatter_specular(hvs, full, nq, cap)
+        hr = {k: a[:nq + ns] for k, a in full.items()}
+        assert int(host(n_next)[0]) == nq + ns
+        same(to_host(rays, nq + ns), hr, ("origin", "dir", "thp", "pdf", "pixel", "node"))
+        if nq:
+            nb.trace_shadow(gs, nb.soa(nb.ShadowSoA, shadow), qsize, cap, film, scontrib, stream())
+            hco = hs.shadow(hsh, hfilm)
+            assert host(scontrib)[:nq].tobytes() == hco.tobytes()
+        assert host(film).tobytes() == hfilm.tobytes()
+        n_rays.copy_(n_next)
+    assert mirrored > 100
+    img = torch.zeros((n, 3), device="cuda")
+    nb.film_resolve(film, n, 1.0, img, stream())
+    assert host(img).tobytes() == hs.resolve(hfilm, 1.0).tobytes()
