@@ -720,8 +720,8 @@ int nrrs_shade(const nrrs_scene* s, const nrrs_ray_soa* rays, const nrrs_hit_soa
                float* contrib, const nrrs_path_vertices* out, uint32_t* n_out_dev,
                void* scratch, void* stream);
 /* nrrs_shade with the closest-hit program's specular branch (device.cu:88-95): hits on mirror
- * materials (nrrs_scene_set_specular) go, in ray order, to out_specular[0 .. *n_specular_dev)
- * (roughness 0) instead of the inference queue `out`, as the reference pushes specular hits to
+ * or glass materials (nrrs_scene_set_specular) go, in ray order, to out_specular[0 ..
+ * *n_specular_dev) (roughness 0 for a mirror, -1 for glass) instead of the inference queue `out`, as the reference pushes specular hits to
  * its emitted queue directly and excludes them from the budget (the decision's n_specular).
  * Same scratch as nrrs_shade. */
 int nrrs_shade_split(const nrrs_scene* s, const nrrs_ray_soa* rays, const nrrs_hit_soa* hits,
@@ -729,8 +729,9 @@ int nrrs_shade_split(const nrrs_scene* s, const nrrs_ray_soa* rays, const nrrs_h
                      float* contrib, const nrrs_path_vertices* out, uint32_t* n_out_dev,
                      const nrrs_path_vertices* out_specular, uint32_t* n_specular_dev,
                      void* scratch, void* stream);
-/* Mirror materials: specular[m] = 1 makes material m a perfect mirror whose reflectance is its
- * albedo ([n_materials] HOST array, n_materials as at creation). */
+/* Specular materials ([n_materials] HOST array, n_materials as at creation): specular[m] = 1
+ * makes material m a perfect mirror, 2 a thin glass sheet (index 1.5, air on both sides); the
+ * albedo tints either. 0 keeps it diffuse; other values are rejected. */
 int nrrs_scene_set_specular(nrrs_scene* s, const uint8_t* specular, uint32_t n_materials);
 
 /* handleIntersections (the RRS branch) + generateScatteredRays for the first *queue_size_dev
@@ -753,14 +754,18 @@ int nrrs_scatter_fixed_rr(const nrrs_scene* s, const nrrs_path_vertices* v, cons
                           const nrrs_ray_soa* rays, const nrrs_shadow_soa* shadow, void* stream);
 
 /* generateScatteredRays for the specular vertices (the emitted queue's specular entries, rrs 1):
- * the mirror bounce of the first *n_dev vertices of v into ray slots *ray_offset_dev + j (after
- * the nrrs_scatter rays: pass its queue size), with thp x albedo, pdf 0 (the emitter the ray hits
- * counts without an MIS weight) and no light sampling (integrator.cpp:833: NEE needs a smooth
- * BSDF). Slots at or past max_rays are dropped. *n_rays_out_dev (not ray_offset_dev) receives
- * min(*ray_offset_dev + *n_dev, max_rays), the next bounce's ray count. */
+ * the bounce of the first *n_dev vertices of v into ray slots *ray_offset_dev + j (after the
+ * nrrs_scatter rays: pass its queue size). A mirror reflects; thin glass reflects with the
+ * sheet's reflectance 2F/(1+F) (F: one face's unpolarised Fresnel reflectance), chosen by the
+ * slot's random hash of (seed, depth), and otherwise passes straight through. thp x albedo,
+ * pdf 0 (the emitter the ray hits counts without an MIS weight), no light sampling
+ * (integrator.cpp:833: NEE needs a smooth BSDF). Slots at or past max_rays are dropped.
+ * *n_rays_out_dev (not ray_offset_dev) receives min(*ray_offset_dev + *n_dev, max_rays), the
+ * next bounce's ray count. */
 int nrrs_scatter_specular(const nrrs_scene* s, const nrrs_path_vertices* v, const uint32_t* n_dev,
                           uint32_t max_n, const uint32_t* ray_offset_dev, uint32_t max_rays,
-                          const nrrs_ray_soa* rays, uint32_t* n_rays_out_dev, void* stream);
+                          uint32_t depth, uint32_t seed, const nrrs_ray_soa* rays,
+                          uint32_t* n_rays_out_dev, void* stream);
 
 /* The shadow rays of the first *n_dev slots: a visible light adds the slot's contrib to
  * film[pixel] and leaves it in contrib_out ([max_n][3]); an occluded one leaves 0. */

@@ -41,7 +41,7 @@ struct nrrs_scene {
     float env[3] = {0.f, 0.f, 0.f};
     uint32_t nt = 0, nn = 0, nl = 0, nm = 0, max_depth = 0;
     uint32_t nee = 1;             // next-event estimation on (mEnableNEE)
-    uint8_t* mat_spec = nullptr;  // [nm] 1 = perfect mirror (null: no mirrors)
+    uint8_t* mat_spec = nullptr;  // [nm] 1 = perfect mirror, 2 = thin glass (null: neither)
 };
 
 namespace nrrs {
@@ -498,6 +498,7 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ nrrs_scen
     for (uint32_t j = 0; j < kShadeChunk / 256; ++j) {
         const uint32_t i = c * kShadeChunk + j * 256 + threadIdx.x;
         bool vert = false, mirror = false;
+        float spec_rough = 0.0f;   // specular queue: 0 = mirror, -1 = thin glass
         V3 add_c = {0.f, 0.f, 0.f};
         V3 pos{}, nrm{}, alb{}, thp{}, d{};
         if (i < n) {
@@ -532,6 +533,7 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ nrrs_scen
                     }
                     mirror = split && mirror_hit(s, prim);
                     vert = !mirror;
+                    if (mirror && s.mat_spec[s.tri_mat[prim]] == 2) spec_rough = -1.0f;
                 }
             }
             if (contrib) put(contrib + 3 * (size_t)i, add_c);
@@ -553,21 +555,39 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ nrrs_scen
                        thp, depth, r.pixel[i], r.node[i]);
         if (mirror)
             put_vertex(outs, (size_t)base_s + run_s + before_s + __popc(ms & lt), pos, d, nrm, alb,
-                       0.0f, thp, depth, r.pixel[i], r.node[i]);
+                       spec_rough, thp, depth, r.pixel[i], r.node[i]);
         run += total;
         run_s += total_s;
         __syncthreads();
     }
 }
 
-// the mirror bounce of the first *n_dev specular vertices into ray slots *off_dev + j: reflected
-// direction, thp x albedo, pdf 0 (the next emitter hit counts in full), no light sampling and
-// no RRS (the reference pushes these vertices to the emitted queue once, with rrs 1). Slots at
-// or past max_rays are dropped; *n_rays_out = min(*off_dev + *n_dev, max_rays).
+// the specular bounce of the first *n_dev specular vertices into ray slots *off_dev + j, with
+// pdf 0 (the next emitter hit counts in full), no light sampling and no RRS (the reference pushes
+// these vertices to the emitted queue once, with rrs 1). A mirror (roughness 0) reflects. Thin
+// glass (roughness -1, index 1.5 between air on both sides) reflects with the sheet's
+// reflectance 2F/(1+F), F the unpolarised Fresnel reflectance of one face, and otherwise passes
+// straight through; the choice is dimension 30 of the slot's random hash. thp x albedo either
+// way. Slots at or past max_rays are dropped; *n_rays_out = min(*off_dev + *n_dev, max_rays).
+constexpr uint32_t kGlassDim = 30;
+__device__ __forceinline__ float sq(float x) { return __fmul_rn(x, x); }
+__device__ __forceinline__ float thin_glass_reflectance(float cosi) {
+    const float eta = 1.5f;
+    const float sin2t = __fdiv_rn(__fsub_rn(1.0f, sq(cosi)), sq(eta));
+    const float cost = __fsqrt_rn(fmaxf(__fsub_rn(1.0f, sin2t), 0.0f));
+    const float rs = sq(__fdiv_rn(__fsub_rn(cosi, __fmul_rn(eta, cost)),
+                                  __fadd_rn(cosi, __fmul_rn(eta, cost))));
+    const float rp = sq(__fdiv_rn(__fsub_rn(__fmul_rn(eta, cosi), cost),
+                                  __fadd_rn(__fmul_rn(eta, cosi), cost)));
+    const float f = __fmul_rn(0.5f, __fadd_rn(rs, rp));
+    return __fdiv_rn(__fmul_rn(2.0f, f), __fadd_rn(1.0f, f));
+}
+
 __global__ void __launch_bounds__(128) k_scatter_specular(nrrs_path_vertices v,
                                                           const uint32_t* n_dev, uint32_t max_n,
                                                           const uint32_t* off_dev,
-                                                          uint32_t max_rays, nrrs_ray_soa r,
+                                                          uint32_t max_rays, uint32_t depth,
+                                                          uint32_t seed, nrrs_ray_soa r,
                                                           uint32_t* n_rays_out) {
     const uint32_t n = min(*n_dev, max_n);
     const uint32_t off = *off_dev;
@@ -575,9 +595,14 @@ __global__ void __launch_bounds__(128) k_scatter_specular(nrrs_path_vertices v,
         const uint64_t slot = (uint64_t)off + j;
         if (slot >= max_rays) continue;
         const V3 nn = v3(v.normal + 3 * (size_t)j), din = mul(v3(v.wi + 3 * (size_t)j), -1.0f);
-        const V3 rf = normalize(sub(din, mul(nn, __fmul_rn(2.0f, dot(din, nn)))));
-        put(r.origin + 3 * slot, add(v3(v.pos + 3 * (size_t)j), mul(nn, kOffset)));
-        put(r.dir + 3 * slot, rf);
+        const V3 p = v3(v.pos + 3 * (size_t)j);
+        const float dn = dot(din, nn);
+        bool reflect = true;
+        if (v.roughness[j] < 0.0f)   // thin glass
+            reflect = rnd(seed, depth, j, kGlassDim) < thin_glass_reflectance(fabsf(dn));
+        const V3 dir = reflect ? normalize(sub(din, mul(nn, __fmul_rn(2.0f, dn)))) : din;
+        put(r.origin + 3 * slot, add(p, mul(nn, reflect ? kOffset : -kOffset)));
+        put(r.dir + 3 * slot, dir);
         put(r.thp + 3 * slot, vmul(v3(v.thp + 3 * (size_t)j), v3(v.albedo + 3 * (size_t)j)));
         r.pdf[slot] = 0.f;
         r.pixel[slot] = v.pixel[j];
@@ -1073,19 +1098,21 @@ extern "C" int nrrs_shade(const nrrs_scene* s, const nrrs_ray_soa* rays, const n
 extern "C" int nrrs_scatter_specular(const nrrs_scene* s, const nrrs_path_vertices* v,
                                      const uint32_t* n_dev, uint32_t max_n,
                                      const uint32_t* ray_offset_dev, uint32_t max_rays,
-                                     const nrrs_ray_soa* rays, uint32_t* n_rays_out_dev,
-                                     void* stream) {
+                                     uint32_t depth, uint32_t seed, const nrrs_ray_soa* rays,
+                                     uint32_t* n_rays_out_dev, void* stream) {
     if (!s || !v || !n_dev || !ray_offset_dev || !rays || !n_rays_out_dev ||
         n_rays_out_dev == ray_offset_dev)
         return NRRS_ERR_INVALID_ARG;
     k_scatter_specular<<<grid_of(std::max(max_n, 1u), 128), 128, 0, (cudaStream_t)stream>>>(
-        *v, n_dev, max_n, ray_offset_dev, max_rays, *rays, n_rays_out_dev);
+        *v, n_dev, max_n, ray_offset_dev, max_rays, depth, seed, *rays, n_rays_out_dev);
     return ok(cudaGetLastError());
 }
 
 extern "C" int nrrs_scene_set_specular(nrrs_scene* s, const uint8_t* specular,
                                        uint32_t n_materials) {
     if (!s || !specular || n_materials != s->nm) return NRRS_ERR_INVALID_ARG;
+    for (uint32_t m = 0; m < n_materials; ++m)
+        if (specular[m] > 2) return NRRS_ERR_INVALID_ARG;
     if (!s->mat_spec && cudaMalloc(&s->mat_spec, n_materials) != cudaSuccess) {
         s->mat_spec = nullptr;
         return NRRS_ERR_CUDA;

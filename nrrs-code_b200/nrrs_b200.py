@@ -280,8 +280,8 @@ _SIGS = {
                                    C.c_void_p, C.c_void_p, C.c_void_p]),
     "nrrs_scene_set_specular": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
     "nrrs_scatter_specular": (C.c_int, [C.c_void_p, C.POINTER(PathVertices), C.c_void_p,
-                                        C.c_uint32, C.c_void_p, C.c_uint32, C.POINTER(RaySoA),
-                                        C.c_void_p, C.c_void_p]),
+                                        C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32,
+                                        C.c_uint32, C.POINTER(RaySoA), C.c_void_p, C.c_void_p]),
     "nrrs_trace_sorted": (C.c_int, [C.c_void_p, C.POINTER(RaySoA), C.c_void_p, C.c_uint32,
                                     C.POINTER(HitSoA), C.c_void_p, C.c_void_p]),
     "nrrs_scatter_fixed_rr": (C.c_int, [C.c_void_p, C.POINTER(PathVertices), C.c_void_p,
@@ -696,9 +696,9 @@ class Scene:
     __del__ = close
 
     def set_specular(self, specular):
-        """Mirror materials: specular[m] != 0 makes material m a perfect mirror."""
+        """Specular materials: specular[m] = 1 makes material m a perfect mirror, 2 thin glass."""
         import numpy as np
-        a = np.ascontiguousarray(np.asarray(specular) != 0, np.uint8)
+        a = np.ascontiguousarray(np.asarray(specular), np.uint8)
         _check(lib().nrrs_scene_set_specular(self._h, a.ctypes.data, len(a)),
                "nrrs_scene_set_specular")
 
@@ -757,11 +757,14 @@ def shade_split(scene: Scene, rays: RaySoA, hits: HitSoA, n_dev, max_n: int, dep
 
 
 def scatter_specular(scene: Scene, v: PathVertices, n_dev, max_n: int, ray_offset_dev,
-                     max_rays: int, rays: RaySoA, n_rays_out_dev, stream=0):
-    """The mirror bounce of the specular vertices into ray slots after the RRS-scattered ones."""
+                     max_rays: int, depth: int, seed: int, rays: RaySoA, n_rays_out_dev,
+                     stream=0):
+    """The specular bounce (mirror or thin glass) of the specular vertices into ray slots after
+    the RRS-scattered ones."""
     _check(lib().nrrs_scatter_specular(scene._h, C.byref(v), _ptr(n_dev), max_n,
-                                       _ptr(ray_offset_dev), max_rays, C.byref(rays),
-                                       _ptr(n_rays_out_dev), stream), "nrrs_scatter_specular")
+                                       _ptr(ray_offset_dev), max_rays, depth, seed,
+                                       C.byref(rays), _ptr(n_rays_out_dev), stream),
+           "nrrs_scatter_specular")
 
 
 def trace_scratch_bytes(max_n: int) -> int:

@@ -147,10 +147,10 @@ uint32_t oracle_shade_split(const float* tri, const uint32_t* mat, const float* 
                             float* s_rough, float* s_thp, uint32_t* s_depth, uint32_t* s_pixel,
                             int32_t* s_node, uint32_t* n_spec);
 void oracle_scatter_specular(const float* pos, const float* wi, const float* nrm, const float* alb,
-                             const float* thp, const uint32_t* pixel, const int32_t* node,
-                             uint32_t n, uint32_t off, uint32_t max_rays, float* r_origin,
-                             float* r_dir, float* r_thp, float* r_pdf, uint32_t* r_pixel,
-                             int32_t* r_node);
+                             const float* thp, const float* rough, const uint32_t* pixel,
+                             const int32_t* node, uint32_t n, uint32_t off, uint32_t max_rays,
+                             uint32_t depth, uint32_t seed, float* r_origin, float* r_dir,
+                             float* r_thp, float* r_pdf, uint32_t* r_pixel, int32_t* r_node);
 void oracle_scatter_fixed_rr(const float* tri, const uint32_t* mat, const float* mats,
                              const uint32_t* lights, const float* area, uint32_t nl,
                              const float* pos, const float* nrm, const float* alb,

@@ -429,7 +429,7 @@ class HostScene:
         self.spec = None          # [materials] uint8 mirror flags (set_specular)
 
     def set_specular(self, specular):
-        self.spec = np.ascontiguousarray(np.asarray(specular) != 0, np.uint8)
+        self.spec = np.ascontiguousarray(np.asarray(specular), np.uint8)
 
     @property
     def nl_sampled(self) -> int:
@@ -487,13 +487,15 @@ class HostScene:
         return ({k: v[:m] for k, v in out.items()}, {k: v[:int(ns[0])] for k, v in outs.items()},
                 contrib)
 
-    def scatter_specular(self, vs: dict, rays: dict, off: int, max_rays: int):
-        """writes the mirror bounces into rays (a dict of [max_rays] arrays) from slot off"""
+    def scatter_specular(self, vs: dict, rays: dict, off: int, max_rays: int, depth: int,
+                         seed: int):
+        """writes the specular bounces into rays (a dict of [max_rays] arrays) from slot off"""
         n = len(vs["pixel"])
         f = lib().oracle_scatter_specular
-        f.argtypes = [C.c_void_p] * 7 + [C.c_uint32] * 3 + [C.c_void_p] * 6
+        f.argtypes = [C.c_void_p] * 8 + [C.c_uint32] * 5 + [C.c_void_p] * 6
         f(*(np.ascontiguousarray(vs[k]).ctypes.data for k in
-            ("pos", "wi", "normal", "albedo", "thp", "pixel", "node")), n, off, max_rays,
+            ("pos", "wi", "normal", "albedo", "thp", "roughness", "pixel", "node")), n, off,
+          max_rays, depth, seed,
           *(rays[k].ctypes.data for k in ("origin", "dir", "thp", "pdf", "pixel", "node")))
 
     def shade(self, rays: dict, hits: dict, depth: int, film):

@@ -238,8 +238,9 @@ uint32_t oracle_shade_split(const float* tri, const uint32_t* mat, const float* 
                     c = mul(vmul(le, th), w);
                 }
                 if (s_pos && mat_spec && mat_spec[mat[prim[i]]]) {
+                    const float rough = mat_spec[mat[prim[i]]] == 2 ? -1.0f : 0.0f;
                     put_vertex(s_pos, s_wi, s_nrm, s_alb, s_rough, s_thp, s_depth, s_pixel, s_node,
-                               ms++, p, d, nn, mm, 0.0f, th, depth, pixel[i], node[i]);
+                               ms++, p, d, nn, mm, rough, th, depth, pixel[i], node[i]);
                 } else {
                     put_vertex(o_pos, o_wi, o_nrm, o_alb, o_rough, o_thp, o_depth, o_pixel, o_node,
                                m++, p, d, nn, mm, 1.0f, th, depth, pixel[i], node[i]);
@@ -266,22 +267,42 @@ uint32_t oracle_shade(const float* tri, const uint32_t* mat, const float* mats, 
                               NULL, NULL, NULL, NULL, NULL, NULL);
 }
 
-/* the specular bounce of the first n specular vertices (perfect mirror, reflectance = albedo)
- * into ray slots off .. off + n - 1 (slots at or past max_rays are dropped): no light sampling
- * and no RRS (the reference pushes these vertices to the emitted queue once, with rrs 1); the
- * ray's pdf is 0, so the emitter it hits counts without an MIS weight. */
+/* thin glass (index 1.5, air on both sides): the sheet's reflectance 2F/(1+F), F the
+ * unpolarised Fresnel reflectance of one face at incidence cosine cosi */
+static float thin_glass_reflectance(float cosi) {
+    const float eta = 1.5f;
+    const float sin2t = (1.0f - cosi * cosi) / (eta * eta);
+    const float ct = 1.0f - sin2t;
+    const float cost = sqrtf(ct > 0.0f ? ct : 0.0f);
+    const float a = (cosi - eta * cost) / (cosi + eta * cost);
+    const float b = (eta * cosi - cost) / (eta * cosi + cost);
+    const float f = 0.5f * (a * a + b * b);
+    return (2.0f * f) / (1.0f + f);
+}
+
+/* the specular bounce of the first n specular vertices into ray slots off .. off + n - 1 (slots
+ * at or past max_rays are dropped): a mirror (roughness 0) reflects; thin glass (roughness -1)
+ * reflects when dimension 30 of the slot's hash is below the sheet's reflectance and otherwise
+ * passes straight through; thp x albedo; no light sampling and no RRS (the reference pushes these
+ * vertices to the emitted queue once, with rrs 1); pdf 0, so the emitter the ray hits counts
+ * without an MIS weight. */
 void oracle_scatter_specular(const float* pos, const float* wi, const float* nrm, const float* alb,
-                             const float* thp, const uint32_t* pixel, const int32_t* node,
-                             uint32_t n, uint32_t off, uint32_t max_rays, float* r_origin,
-                             float* r_dir, float* r_thp, float* r_pdf, uint32_t* r_pixel,
-                             int32_t* r_node) {
+                             const float* thp, const float* rough, const uint32_t* pixel,
+                             const int32_t* node, uint32_t n, uint32_t off, uint32_t max_rays,
+                             uint32_t depth, uint32_t seed, float* r_origin, float* r_dir,
+                             float* r_thp, float* r_pdf, uint32_t* r_pixel, int32_t* r_node) {
     for (uint32_t j = 0; j < n; ++j) {
         const uint64_t slot = (uint64_t)off + j;
         if (slot >= max_rays) continue;
         const v3 nn = ld(nrm + 3 * (uint64_t)j), din = mul(ld(wi + 3 * (uint64_t)j), -1.0f);
-        const v3 rf = normalize(sub(din, mul(nn, 2.0f * dot(din, nn))));
-        st(r_origin + 3 * slot, add(ld(pos + 3 * (uint64_t)j), mul(nn, OFFSET)));
-        st(r_dir + 3 * slot, rf);
+        const v3 p = ld(pos + 3 * (uint64_t)j);
+        const float dn = dot(din, nn);
+        int reflect = 1;
+        if (rough[j] < 0.0f)
+            reflect = rnd(seed, depth, j, 30u) < thin_glass_reflectance(fabsf(dn));
+        const v3 dir = reflect ? normalize(sub(din, mul(nn, 2.0f * dn))) : din;
+        st(r_origin + 3 * slot, add(p, mul(nn, reflect ? OFFSET : -OFFSET)));
+        st(r_dir + 3 * slot, dir);
         st(r_thp + 3 * slot, vmul(ld(thp + 3 * (uint64_t)j), ld(alb + 3 * (uint64_t)j)));
         r_pdf[slot] = 0.f;
         r_pixel[slot] = pixel[j];

@@ -507,16 +507,20 @@ def test_gpu_trace_sorted_equals_trace():
     gs.close()
 
 
-@pytest.mark.parametrize("closed", [False, True], ids=["open", "closed"])
-def test_gpu_mirror_frame_matches_oracle(closed):
-    """Mirror materials: their hits bypass the inference queue (the closest-hit program's
-    specular branch) and count as n_specular against the budget; their vertices bounce once,
-    unconditionally, into the ray slots after the RRS-scattered ones. A whole frame, bit for bit,
-    with every array compared as it is produced."""
+@pytest.mark.parametrize("closed,glass", [(False, False), (True, False), (True, True)],
+                         ids=["open-mirrors", "closed-mirrors", "closed-mirrors-glass"])
+def test_gpu_mirror_frame_matches_oracle(closed, glass):
+    """Mirror and thin-glass materials: their hits bypass the inference queue (the closest-hit
+    program's specular branch) and count as n_specular against the budget; their vertices bounce
+    once, unconditionally, into the ray slots after the RRS-scattered ones (glass reflecting or
+    passing through by its Fresnel reflectance). A whole frame, bit for bit, with every array
+    compared as it is produced."""
     torch = torch_cuda()
     v, t, m, ma, e = nb.synth_scene(13, n_boxes=60, closed=closed)
     spec = np.zeros(len(ma), np.uint8)
     spec[4::3] = 1                                    # every third box material is a mirror
+    if glass:
+        spec[5::3] = 2                                # and as many are thin glass
     gs, hs = nb.Scene(v, t, m, ma, e), O.HostScene(v, t, m, ma, e)
     gs.set_specular(spec)
     hs.set_specular(spec)
@@ -540,7 +544,7 @@ def test_gpu_mirror_frame_matches_oracle(closed):
     hr = hs.camera_rays(cam, 0, seed)
     dp = nb.default_decide(clamp_max=4.0)
     rng = np.random.default_rng(seed)
-    mirrored = 0
+    mirrored = transmitted = 0
     for depth in range(5):
         nr = int(host(n_rays)[0])
         assert nr == len(hr["pixel"])
@@ -576,8 +580,8 @@ def test_gpu_mirror_frame_matches_oracle(closed):
             qsize.zero_()
         nb.scatter(gs, nb.soa(nb.PathVertices, verts), rrs_norm, queue, qsize, cap, depth, seed,
                    nb.soa(nb.RaySoA, rays), nb.soa(nb.ShadowSoA, shadow), stream())
-        nb.scatter_specular(gs, nb.soa(nb.PathVertices, verts_s), n_spec, cap, qsize, cap,
-                            nb.soa(nb.RaySoA, rays), n_next, stream())
+        nb.scatter_specular(gs, nb.soa(nb.PathVertices, verts_s), n_spec, cap, qsize, cap, depth,
+                            seed, nb.soa(nb.RaySoA, rays), n_next, stream())
         full = {"origin": np.zeros((cap, 3), np.float32), "dir": np.zeros((cap, 3), np.float32),
                 "thp": np.zeros((cap, 3), np.float32), "pdf": np.zeros(cap, np.float32),
                 "pixel": np.zeros(cap, np.uint32), "node": np.zeros(cap, np.int32)}
@@ -585,8 +589,10 @@ def test_gpu_mirror_frame_matches_oracle(closed):
             hr_d, hsh = hs.scatter(hv, o["rrs_norm"], o["queue"], depth, seed)
             for k in full:
                 full[k][:nq] = hr_d[k]
-        hs.scatter_specular(hvs, full, nq, cap)
+        hs.scatter_specular(hvs, full, nq, cap, depth, seed)
         hr = {k: a[:nq + ns] for k, a in full.items()}
+        # glass vertices that passed straight through keep the incoming direction
+        transmitted += int((np.abs((hr["dir"][nq:] + hvs["wi"]).sum(axis=1)) == 0).sum())
         assert int(host(n_next)[0]) == nq + ns
         same(to_host(rays, nq + ns), hr, ("origin", "dir", "thp", "pdf", "pixel", "node"))
         if nq:
@@ -596,6 +602,8 @@ def test_gpu_mirror_frame_matches_oracle(closed):
         assert host(film).tobytes() == hfilm.tobytes()
         n_rays.copy_(n_next)
     assert mirrored > 100
+    if glass:
+        assert transmitted > 0
     img = torch.zeros((n, 3), device="cuda")
     nb.film_resolve(film, n, 1.0, img, stream())
     assert host(img).tobytes() == hs.resolve(hfilm, 1.0).tobytes()
