@@ -1131,7 +1131,10 @@ def run_render(args, rank, world, local_rank):
                 ev.setdefault(("trace", depth), (torch.cuda.Event(enable_timing=True),
                                                  torch.cuda.Event(enable_timing=True)))
                 ev[("trace", depth)][0].record(cur)
-            nb.trace_sorted(scene, R, n_rays, cap, Hh, tscratch, stream)
+            if depth == 0:    # camera rays come in pixel order, already coherent
+                nb.trace(scene, R, n_rays, cap, Hh, stream)
+            else:
+                nb.trace_sorted(scene, R, n_rays, cap, Hh, tscratch, stream)
             if timing:
                 ev[("trace", depth)][1].record(cur)
             nb.shade(scene, R, Hh, n_rays, cap, depth, film, contrib if train else None, V,
@@ -1219,9 +1222,11 @@ def run_render(args, rank, world, local_rank):
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
     verts_per_frame = total_v / args.steps
-    # camera + resolve per frame; ray sort (2), trace, shade (2), scatter, shadow per bounce run,
-    # and the last trace + shade of a frame whose queue ran out; plus the NRRS step's own launches
-    launches = (args.steps * 2 + bounces_run[0] * 7 + (net.launch_count() - launches0))
+    # camera + resolve per frame; ray sort (2, not for the camera rays), trace, shade (2),
+    # scatter, shadow per bounce run, and the last trace + shade of a frame whose queue ran out;
+    # plus the NRRS step's own launches
+    launches = (args.steps * 2 + bounces_run[0] * 7 - args.steps * 2 +
+                (net.launch_count() - launches0))
     if train:
         # per bounce: radiance of the shaded rays, record count + writes, patch counts, shadow
         # radiance; per frame: camera patch counts, pixel error (3), radiance pass + batch
