@@ -137,3 +137,85 @@ def test_gpu_training_frame_matches_oracle(closed):
     _, l64 = O.train_grads(net.config, p0, ob, ob["target"], "f64")
     assert host(loss) == pytest.approx(l64, rel=1e-4)
     net.close()
+
+
+def test_gpu_training_frames_learn():
+    """The loop closes: frames rendered through the library (trace, shade, records, the step
+    with the network's own factors, scatter, shadow), each one's batch trains the networks, and
+    the StatNet loss on fresh frames falls as the frames go by."""
+    torch = torch_cuda()
+    gs, _ = scene_pair(11, boxes=60, closed=True)
+    cam = nb.room_camera(64, 48, inside=True)
+    n = cam.width * cam.height
+    cap = 4 * n
+    node_cap = 12 * n
+    net = make_net(precision=nb.PREC_FP16, max_queue=cap, max_train=1 << 14)
+    net.setStep(3)
+    dp = nb.default_decide(clamp_min=1.0)
+    g = GpuNodes(node_cap, cap)
+    f = lambda *s: torch.zeros(*s, device="cuda")                       # noqa: E731
+    i = lambda *s: torch.zeros(*s, dtype=torch.int32, device="cuda")    # noqa: E731
+    rays, hits = empty_rays(cap), empty_hits(cap)
+    verts, shadow = empty_vertices(cap), empty_shadow(cap)
+    contrib, scontrib, film = f(cap, 3), f(cap, 3), torch.zeros((n, 9), dtype=torch.int64,
+                                                                 device="cuda")
+    scratch = torch.zeros(nb.shade_scratch_bytes(cap), dtype=torch.uint8, device="cuda")
+    n_rays, n_vert, qsize = i(1), i(1), i(1)
+    stats, rrs, rrs_norm = f(3 * cap), f(cap), f(cap)
+    split = torch.zeros(cap, dtype=torch.uint8, device="cuda")
+    queue = i(cap)
+    img = f(n, 3)
+    widths = {"pos": 3, "wi": 3, "normal": 3, "albedo": 3, "roughness": 1, "thp": 3, "depth": 1,
+              "ref_mean": 1, "target": 3, "rrs_target": 1, "pixel": 1}
+    batch = {k: (f(node_cap, w) if w > 1 else f(node_cap)) if k not in ("depth", "pixel")
+             else i(node_cap) for k, w in widths.items()}
+    tb = nb.train_batch(**batch)
+    counts, size_d = i(n), i(1)
+    prm = nb.default_train_data_params(copy_rrs_node=1, dedupe_rrs_target=1)
+    tsoa = nb.vertex_soa(batch["pos"], batch["wi"], batch["normal"], batch["roughness"],
+                         batch["albedo"], batch["thp"], batch["depth"], batch["ref_mean"])
+    loss = torch.zeros(2, dtype=torch.float64, device="cuda")
+    R, Hh, V, S = (nb.soa(nb.RaySoA, rays), nb.soa(nb.HitSoA, hits),
+                   nb.soa(nb.PathVertices, verts), nb.soa(nb.ShadowSoA, shadow))
+    vsoa = nb.vertex_soa(verts["pos"], verts["wi"], verts["normal"], verts["roughness"],
+                         verts["albedo"], verts["thp"], verts["depth"])
+    losses = []
+    for frame in range(40):
+        g.pn.reset(stream())
+        film.zero_()
+        nb.camera_rays(cam, frame, 77, R, stream())
+        n_rays.fill_(n)
+        n_cur = n
+        for depth in range(4):
+            nb.trace(gs, R, n_rays, cap, Hh, stream())
+            nb.shade(gs, R, Hh, n_rays, cap, depth, film, contrib, V, n_vert, scratch, stream())
+            g.pn.recordRadiance(rays["node"], contrib, n_cur, stream())
+            nv = int(host(n_vert)[0])
+            if nv == 0:
+                break
+            rnd = torch.rand(nv, device="cuda", generator=torch.Generator(device="cuda")
+                             .manual_seed(1000 * frame + depth))
+            net.generateRRSNumber(vsoa, rnd, nv, n, 0, dp, stats, rrs, rrs_norm, split, queue,
+                                  cap, qsize, stream())
+            g.pn.recordNode(vsoa, verts["node"], verts["pixel"], rrs_norm, split, nv,
+                            verts["node"], stream())
+            nb.scatter(gs, V, rrs_norm, queue, qsize, cap, depth, 500 + frame, R, S, stream())
+            nb.trace_shadow(gs, S, qsize, cap, film, scontrib, stream())
+            n_cur = int(host(qsize)[0])
+            g.pn.recordRadiance(shadow["node"], scontrib, n_cur, stream())
+            n_rays.copy_(qsize)
+        nb.film_resolve(film, n, 1.0, img, stream())
+        counts.zero_()
+        g.pn.generate_training_data(prm, tb, node_cap, size_d, image=img, image_channels=3,
+                                    n_pixels=n, pixel_samples=counts, stream=stream())
+        m = min(int(host(size_d)[0]), 1 << 14)
+        m -= m % 256
+        assert m >= 1024
+        net.train(tsoa, batch["target"], m, loss, stream())
+        losses.append(float(host(loss)[0]))
+    first, last = np.mean(losses[:5]), np.mean(losses[-5:])
+    assert np.isfinite(losses).all()
+    assert last < 0.7 * first, (first, last, losses)
+    rc, flags = net.device_status(stream())
+    assert rc == nb.OK and flags == 0
+    net.close()
