@@ -219,3 +219,108 @@ def test_gpu_training_frames_learn():
     rc, flags = net.device_status(stream())
     assert rc == nb.OK and flags == 0
     net.close()
+
+
+def test_gpu_ubs_search_drives_rendered_frames():
+    """The per-depth strategy search on real frames: at the start of each frame the search
+    moves to its next state. The renderer then runs, depth by depth, the factor source it asks
+    for (the RRS step with ADRRS or RRSNet factors, or the fixed-RR scatter when it runs no
+    inference). nrrs_ubs_error scores the frame against a reference image, and the frame's
+    time and error sum go back to the search. The library's search and the restatement make the
+    same choices every frame and end on the same best string, in 3^d + 3 frames."""
+    import ctypes as C
+
+    from schedule import UBSRef
+
+    torch = torch_cuda()
+    gs, _ = scene_pair(9, boxes=30)
+    cam = nb.room_camera(40, 30)
+    n = cam.width * cam.height
+    cap = 4 * n
+    max_depth = 2
+    net = make_net(precision=nb.PREC_FP16, max_queue=cap)
+    random_params(net, 4, table_scale=0.5, mlp_scale=0.1)
+    net.setStep(3)
+    f = lambda *s: torch.zeros(*s, device="cuda")                       # noqa: E731
+    i = lambda *s: torch.zeros(*s, dtype=torch.int32, device="cuda")    # noqa: E731
+    rays, hits = empty_rays(cap), empty_hits(cap)
+    verts, shadow = empty_vertices(cap), empty_shadow(cap)
+    film = torch.zeros((n, 9), dtype=torch.int64, device="cuda")
+    scratch = torch.zeros(nb.shade_scratch_bytes(cap), dtype=torch.uint8, device="cuda")
+    n_rays, n_vert, qsize = i(1), i(1), i(1)
+    stats, rrs, rrs_norm = f(3 * cap), f(cap), f(cap)
+    split = torch.zeros(cap, dtype=torch.uint8, device="cuda")
+    queue = i(cap)
+    R, Hh, V, S = (nb.soa(nb.RaySoA, rays), nb.soa(nb.HitSoA, hits),
+                   nb.soa(nb.PathVertices, verts), nb.soa(nb.ShadowSoA, shadow))
+    vsoa = nb.vertex_soa(verts["pos"], verts["wi"], verts["normal"], verts["roughness"],
+                         verts["albedo"], verts["thp"], verts["depth"])
+
+    def frame(sample, choose):
+        """one frame; choose(depth) -> None (fixed RR) or a factor source"""
+        film.zero_()
+        nb.camera_rays(cam, sample, 5, R, stream())
+        n_rays.fill_(n)
+        used = []
+        for depth in range(3):
+            nb.trace(gs, R, n_rays, cap, Hh, stream())
+            nb.shade(gs, R, Hh, n_rays, cap, depth, film, None, V, n_vert, scratch, stream())
+            nv = int(host(n_vert)[0])
+            if nv == 0:
+                break
+            src = choose(depth)
+            used.append(src)
+            if src is None:
+                nb.scatter_fixed_rr(gs, V, n_vert, cap, 0.8, depth, 90 + sample, R, S, stream())
+                qsize.copy_(n_vert)
+            else:
+                rnd = torch.rand(nv, device="cuda", generator=torch.Generator(device="cuda")
+                                 .manual_seed(sample * 10 + depth))
+                dp = nb.default_decide(factor_source=src, clamp_min=0.5)
+                net.generateRRSNumber(vsoa, rnd, nv, n, 0, dp, stats, rrs, rrs_norm, split,
+                                      queue, cap, qsize, stream())
+                nb.scatter(gs, V, rrs_norm, queue, qsize, cap, depth, 90 + sample, R, S, stream())
+            nb.trace_shadow(gs, S, qsize, cap, film, None, stream())
+            n_rays.copy_(qsize)
+        img = f(n, 3)
+        nb.film_resolve(film, n, 1.0, img, stream())
+        return img, used
+
+    # the reference image: the mean of 16 frames with fixed Russian roulette
+    ref = f(n, 3)
+    for k in range(16):
+        img, _ = frame(1000 + k, lambda d: None)
+        ref += img / 16
+    pe = nb.default_pixel_error_params(cam.width, cam.height)
+    err = f(n)
+    esum = torch.zeros(C.sizeof(nb.ErrorSum), dtype=torch.uint8, device="cuda")
+
+    lib, oracle = nb.UBS(max_depth), UBSRef(max_depth)
+    lib.UBSResetAndBeginSearch()
+    oracle.begin()
+    t, frames = 0.0, 0
+    while True:
+        a, b = lib.UBSNextState(), oracle.next_state()
+        assert a == b
+        if not a:
+            break
+
+        def choose(depth):
+            infer, src = lib.isInferMode(depth)
+            assert (infer, src) == oracle.need_infer(depth, 1, 0.05, 8.0, 6, 1)
+            return src if infer else None
+
+        img, used = frame(frames, choose)
+        nb.ubs_error(pe, img, 1, ref, 3, err, esum, stream())
+        err_sum = float(host(esum)[28:32].view(np.float32)[0])
+        assert np.isfinite(err_sum) and err_sum > 0
+        t += 0.02 + 0.001 * len([u for u in used if u is not None])   # the frame's clock
+        lib.UBSAnalyseFrame(t, err_sum, n)
+        oracle.analyse(t, err_sum, n)
+        frames += 1
+        assert frames < 50
+    assert frames == 3 ** max_depth + 3
+    best, eff = lib.best()
+    assert best == oracle.array[:max_depth] and np.float32(eff) == oracle.best_eff
+    assert not lib.searching
+    net.close()
