@@ -1057,6 +1057,8 @@ def run_render(args, rank, world, local_rank):
     train = wl.get("train_steps", 0) > 0
     net = nb.NRRSNetwork(make_config(args.precision, wl, cap, max(wl["train_batch"], 1 << 16)))
     net.setStep(3)
+    # the library's launch-shape tuner on a queue of one bounce's size, as for the step workloads
+    tune = json.loads(net.autotune(P))
     # factors clamped at 1 or above: the normalisation to the pixel budget then keeps about one
     # path per pixel per bounce, as a trained network would; an untrained one kills most paths
     dp = nb.default_decide(clamp_min=1.0)
@@ -1262,6 +1264,7 @@ def run_render(args, rank, world, local_rank):
         "clocks": clk.summary(),
         "gpu_launches": launches,
         "calls_ms_per_frame": {"trace": t_trace, "nrrs_step": t_nrrs, "shadow": t_shadow},
+        "autotune": tune.get("best") or tune.get("cached"),
         "rays_per_frame": {"closest_hit": rays_run[0], "shadow": rays_run[1]},
         "rays_per_s_trace": rays_run[0] / (t_trace * 1e-3) if t_trace else None,
         "rays_per_s_shadow": rays_run[1] / (t_shadow * 1e-3) if t_shadow else None,
