@@ -146,30 +146,37 @@ struct Hit { uint32_t prim; float t, u, v; };
 
 // closest hit; ties in t go to the lower input index. any = true stops at the first hit.
 // Closest hit; ties in t go to the lower input index. Stack traversal, near child first by the
-// sign of the ray on the node's split axis. Each pass of the outer loop first pops nodes until this
-// lane holds a leaf whose box the ray enters (or the stack is empty), then tests that leaf: lanes
-// of a warp reconverge between the two loops, so the triangle tests run with the warp together.
+// sign of the ray on the node's split axis: the near child is held in a register as the next
+// node and only the far one goes onto the stack. Each pass of the outer loop first walks nodes
+// until this lane holds a leaf whose box the ray enters (or the stack is empty), then tests that
+// leaf: lanes of a warp reconverge between the two loops, so the triangle tests run with the
+// warp together.
 __device__ Hit closest_hit(const nrrs_scene& s, V3 o, V3 d, float tmax) {
     Hit h{kMiss, tmax, 0.f, 0.f};   // h.t is the culling bound: tmax until the first hit
     const V3 inv = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
     const float4* nodes = reinterpret_cast<const float4*>(s.nodes);
     int stack[kStack];
     int sp = 0;
-    stack[sp++] = 0;
+    int node = 0;   // the next node to visit, held in a register (-1: pop one)
     for (;;) {
         uint32_t first = 0, cnt = 0;
-        while (sp > 0) {
-            const float4* nd = nodes + 2 * (size_t)stack[--sp];
+        for (;;) {
+            if (node < 0) {
+                if (sp == 0) break;
+                node = stack[--sp];
+            }
+            const float4* nd = nodes + 2 * (size_t)node;
             const float4 lo = __ldg(nd), hi = __ldg(nd + 1);
             float tn;
-            if (!box_hit(lo, hi, o, inv, h.t, &tn)) continue;
+            if (!box_hit(lo, hi, o, inv, h.t, &tn)) { node = -1; continue; }
             const uint32_t lf = __float_as_uint(lo.w), ca = __float_as_uint(hi.w);
-            if (ca & 0xffffu) { first = lf; cnt = ca & 0xffffu; break; }
+            if (ca & 0xffffu) { first = lf; cnt = ca & 0xffffu; node = -1; break; }
             const uint32_t axis = ca >> 16;
             const float da = axis == 0 ? d.x : (axis == 1 ? d.y : d.z);
-            if (sp + 2 > kStack) continue;   // depth is bounded at build time; never taken
-            if (da < 0.f) { stack[sp++] = (int)lf; stack[sp++] = (int)lf + 1; }
-            else { stack[sp++] = (int)lf + 1; stack[sp++] = (int)lf; }
+            if (sp + 1 > kStack) { node = -1; continue; }   // depth is bounded at build time
+            // near child next, the far one on the stack
+            if (da < 0.f) { stack[sp++] = (int)lf; node = (int)lf + 1; }
+            else { stack[sp++] = (int)lf + 1; node = (int)lf; }
         }
         if (cnt == 0) break;
         for (uint32_t i = first; i < first + cnt; ++i) {
