@@ -187,20 +187,27 @@ int nrrs_decide_emit(nrrs_ctx* ctx, const float* rrs, const float* rnd,
 /* ---- decision + emission without any device allocation. No counterpart in the reference:
  *      for callers that cannot call cudaMalloc (a plugin whose host framework owns all device
  *      memory, a fixed start-up memory budget, a frame loop that must not take cudaMalloc's
- *      implicit synchronisation). Needs no context; same arguments and results as
- *      nrrs_decide_emit on a context whose max_queue is NRRS_NOALLOC_MAX_N. Its scratch is a
- *      static device array of about 66 KB (NRRS_NOALLOC_MAX_N vertices), resident on every
- *      GPU that loads the library until exit; n above NRRS_NOALLOC_MAX_N returns
- *      NRRS_ERR_INVALID_ARG. The first call on a device looks up the array's device address
- *      (cudaGetSymbolAddress) with that device current, so make that first call before any
- *      stream capture. All calls share the array: calls that overlap on the GPU (other streams,
- *      other host threads) race and must be serialised by the caller. ---- */
+ *      implicit synchronisation). Needs no context; the same results as nrrs_decide_emit on a
+ *      context whose max_queue is NRRS_NOALLOC_MAX_N, with one difference in the arguments:
+ *      n_specular is a host value only (there is no n_specular_dev). Its scratch is a static
+ *      device array of about 66 KB (NRRS_NOALLOC_MAX_N vertices), resident on every GPU that
+ *      loads the library until exit; n above NRRS_NOALLOC_MAX_N returns NRRS_ERR_INVALID_ARG.
+ *      The first call in a CUDA context looks up the array's device address
+ *      (cudaGetSymbolAddress) with that context current, so make that first call before any
+ *      stream capture; a context created again after cudaDeviceReset gets a new lookup. All
+ *      calls share the array: calls that overlap on the GPU (other streams, other host threads)
+ *      race and must be serialised by the caller. ---- */
 #define NRRS_NOALLOC_MAX_N (1u << 24)
 int nrrs_decide_emit_noalloc(const float* rrs, const float* rnd, const uint32_t* scatter_index,
                              uint32_t n, uint32_t budget, uint32_t n_specular,
                              const nrrs_decide_params* p, float* rrs_norm, uint8_t* split,
                              uint32_t* next_queue, uint32_t capacity, uint32_t* next_size_dev,
                              void* stream);
+/* Device status bits (NRRS_DEV_*) that nrrs_decide_emit_noalloc calls have raised since the last
+ * read, from the same static array: synchronises the stream, returns and clears them. The return
+ * code follows nrrs_get_device_status (TIMEOUT, then CAPACITY_OVERFLOW, then NAN, else OK).
+ * No counterpart in the reference (its overflow and NaN checks only printf). */
+int nrrs_noalloc_device_status(uint32_t* flags, void* stream);
 
 /* ---- fused: infer + decide + emit for one depth (generateRRSNumber<false,*>) ---- */
 int nrrs_step(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* rnd, uint32_t n,

@@ -2,9 +2,23 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cmath>
+
 #include "nrrs_common.cuh"
 
 namespace nrrs {
+
+// Fixed-point shift of the exact normalisation sum for queues of up to n vertices whose summed
+// terms are at most vmax: n * vmax < 2^(62 - shift), capped at 40 fractional bits. Every path
+// that decides a queue (context, sharded, allocation-free) takes its shift from here, so the
+// same capacity gives the same bits.
+inline int sum_shift(uint64_t n, float vmax) {
+    const double prod = (double)(n ? n : 1) * (double)(vmax > 1.f ? vmax : 1.f);
+    int e = 0;
+    std::frexp(prod, &e);
+    const int s = 62 - e;
+    return s > 40 ? 40 : s;
+}
 
 constexpr int kDecThreads = 256;
 constexpr int kDecVPT = 8;

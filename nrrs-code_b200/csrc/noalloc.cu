@@ -11,9 +11,19 @@
 //
 // The array holds NRRS_NOALLOC_MAX_N vertices' worth of look-back state (about 66 KB) and stays
 // resident on every GPU that loads the library until the process exits. In host code its name
-// is only a host-side stand-in, so its device address is looked up with cudaGetSymbolAddress,
-// once per device, the first time the entry point runs with that device current.
+// is only a host-side stand-in, so its device address is looked up with cudaGetSymbolAddress
+// with the device current. The lookup is cached per CUDA context (keyed by the driver's context
+// id, which is never reused within a process), so a context that is destroyed and created again
+// (cudaDeviceReset) gets a fresh lookup instead of a stale address. The first call in each
+// context does the lookup; make it before any stream capture.
+//
+// The kernels' device status bits (look-back timeout, non-finite factor, saturated or
+// overflowing counts) accumulate in the array's status word across calls; each call clears
+// everything else it uses. nrrs_noalloc_device_status reads and clears them.
+#include <cuda.h>
+
 #include <cmath>
+#include <cstddef>
 #include <mutex>
 
 #include "kernels.hpp"
@@ -27,30 +37,70 @@ constexpr size_t kNoAllocBytes = sizeof(DecideScratch) + sizeof(unsigned long lo
 // shared by every call on a device; keeps the last call's contents
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void* g_addr[kMaxDevices] = {};
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
 
-int scratch_address(void** out) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return NRRS_ERR_CUDA;
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_addr[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) return NRRS_ERR_CUDA;
-        g_addr[dev] = p;
+struct AddrCache {
+    std::mutex mu;
+    bool resolved = false;
+    CtxGetCurrentFn get_current = nullptr;
+    CtxGetIdFn get_id = nullptr;
+    static constexpr int kSlots = 64;
+    unsigned long long ctx_id[kSlots] = {};
+    void* addr[kSlots] = {};
+    int used = 0, next = 0;
+};
+AddrCache g_cache;
+
+// id of the context current on this thread (0 when none is current or the driver lacks the call)
+unsigned long long current_ctx_id(AddrCache& c) {
+    if (!c.resolved) {
+        c.resolved = true;
+        cudaDriverEntryPointQueryResult q{};
+        void* f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess && q == cudaDriverEntryPointSuccess)
+            c.get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess && q == cudaDriverEntryPointSuccess)
+            c.get_id = reinterpret_cast<CtxGetIdFn>(f);
+        cudaGetLastError();
     }
-    *out = g_addr[dev];
-    return NRRS_OK;
+    if (!c.get_current || !c.get_id) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (c.get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    if (c.get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
 }
 
-int sum_shift_noalloc(float vmax) {
-    const double prod = (double)NRRS_NOALLOC_MAX_N * (double)(vmax > 1.f ? vmax : 1.f);
-    int e = 0;
-    std::frexp(prod, &e);
-    const int s = 62 - e;
-    return s > 40 ? 40 : s;
+// device address of the scratch array in the current context
+int scratch_address(void** out) {
+    std::lock_guard<std::mutex> lock(g_cache.mu);
+    unsigned long long id = current_ctx_id(g_cache);
+    if (id) {
+        for (int k = 0; k < g_cache.used; ++k)
+            if (g_cache.ctx_id[k] == id) {
+                *out = g_cache.addr[k];
+                return NRRS_OK;
+            }
+    }
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        return NRRS_ERR_CUDA;
+    }
+    if (!id) id = current_ctx_id(g_cache);  // the lookup made the primary context current
+    if (id) {
+        const int k = g_cache.used < AddrCache::kSlots ? g_cache.used++ : g_cache.next;
+        g_cache.next = (k + 1) % AddrCache::kSlots;
+        g_cache.ctx_id[k] = id;
+        g_cache.addr[k] = p;
+    }
+    *out = p;
+    return NRRS_OK;
 }
 
 }  // namespace
@@ -73,7 +123,8 @@ extern "C" int nrrs_decide_emit_noalloc(const float* rrs, const float* rnd,
     if (p->factor_source != NRRS_FACTOR_ADRRS && p->factor_source != NRRS_FACTOR_RRSNET)
         return NRRS_ERR_INVALID_ARG;
     const float vmax = p->use_ceil ? ceilf(p->clamp_max) : p->clamp_max;
-    const int shift = sum_shift_noalloc(vmax);
+    // the shift a context with max_queue = NRRS_NOALLOC_MAX_N uses, so both give the same bits
+    const int shift = sum_shift(NRRS_NOALLOC_MAX_N, vmax);
     if (shift < 16) return NRRS_ERR_UNSUPPORTED;
 
     void* base = nullptr;
@@ -95,11 +146,13 @@ extern "C" int nrrs_decide_emit_noalloc(const float* rrs, const float* rnd,
     sg.queue_capacity = capacity;
     const uint32_t chunks = (n + kDecChunk - 1) / kDecChunk;
 
-    // The array keeps whatever the previous call (or an aborted one) left: clear the header
-    // (sums, ticket, done counter, status) and the look-back states this call will use.
+    // The array keeps whatever the previous call (or an aborted one) left: clear the sums,
+    // ticket, done counter and epoch, and the look-back states this call will use. The status
+    // word is left alone so that nrrs_noalloc_device_status sees every call's flags.
     DecideScratch* scr = reinterpret_cast<DecideScratch*>(base);
-    if (cudaMemsetAsync(base, 0, sizeof(DecideScratch) + sizeof(unsigned long long) * chunks, s) !=
-        cudaSuccess)
+    unsigned long long* states = reinterpret_cast<unsigned long long*>(scr + 1);
+    if (cudaMemsetAsync(base, 0, offsetof(DecideScratch, status), s) != cudaSuccess ||
+        cudaMemsetAsync(states, 0, sizeof(unsigned long long) * chunks, s) != cudaSuccess)
         return NRRS_ERR_CUDA;
 
     SumArgs sa{};
@@ -123,7 +176,7 @@ extern "C" int nrrs_decide_emit_noalloc(const float* rrs, const float* rnd,
     d.next_size = next_size_dev;
     d.n_spec_dev = nullptr;
     d.scr = scr;
-    d.states = reinterpret_cast<unsigned long long*>(scr + 1);
+    d.states = states;
     d.segs.n = 1;
     d.segs.s[0] = sg;
     d.segs.total_tiles = chunks;
@@ -133,5 +186,24 @@ extern "C" int nrrs_decide_emit_noalloc(const float* rrs, const float* rnd,
     d.inv_fixed_scale = 1.0 / sa.fp.fixed_scale;
     d.spin_limit = 1u << 22;
     if (launch_decide(d, s) != cudaSuccess) return NRRS_ERR_CUDA;
+    return NRRS_OK;
+}
+
+extern "C" int nrrs_noalloc_device_status(uint32_t* flags, void* stream) {
+    if (!flags) return NRRS_ERR_INVALID_ARG;
+    void* base = nullptr;
+    int rc = scratch_address(&base);
+    if (rc != NRRS_OK) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned int* status = &reinterpret_cast<DecideScratch*>(base)->status;
+    uint32_t h = 0;
+    if (cudaMemcpyAsync(&h, status, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaMemsetAsync(status, 0, sizeof(unsigned int), s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return NRRS_ERR_CUDA;
+    *flags = h;
+    if (h & NRRS_DEV_TIMEOUT) return NRRS_ERR_TIMEOUT;
+    if (h & NRRS_DEV_OVERFLOW) return NRRS_ERR_CAPACITY_OVERFLOW;
+    if (h & NRRS_DEV_NAN) return NRRS_ERR_NAN;
     return NRRS_OK;
 }

@@ -75,15 +75,6 @@ uint64_t mlp_params(int in, int w, int h, int out) {
     return (uint64_t)in * w + (uint64_t)(h - 1) * w * w + (uint64_t)w * out;
 }
 
-// shift of the exact fixed-point normalisation sum: n * vmax < 2^(62 - shift), capped at 40
-int sum_shift(uint64_t n, float vmax) {
-    const double prod = (double)(n ? n : 1) * (double)(vmax > 1.f ? vmax : 1.f);
-    int e = 0;
-    std::frexp(prod, &e);
-    const int s = 62 - e;
-    return s > 40 ? 40 : s;
-}
-
 // The shift depends only on the context capacity and the clamp, so a depth gives the same
 // decisions whether it runs alone, batched, or sharded.
 FactorParams factor_params(const nrrs_ctx* ctx, const nrrs_decide_params* p) {

@@ -185,6 +185,7 @@ _SIGS = {
                                            C.c_uint32, C.c_uint32, C.POINTER(DecideParams),
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                            C.c_void_p, C.c_void_p]),
+    "nrrs_noalloc_device_status": (C.c_int, [C.POINTER(C.c_uint32), C.c_void_p]),
     "nrrs_infer_accumulate": (C.c_int, [C.c_void_p, C.POINTER(VertexSoA), C.c_uint32,
                                         C.POINTER(DecideParams), C.c_void_p, C.c_void_p,
                                         C.c_void_p, C.c_void_p]),
@@ -456,6 +457,14 @@ def decide_emit_noalloc(rrs, rnd, n, budget, n_specular, params, rrs_norm, split
                                           n_specular, C.byref(params), _ptr(rrs_norm),
                                           _ptr(split), _ptr(queue), capacity, _ptr(next_size),
                                           stream)
+
+
+def noalloc_device_status(stream=0) -> tuple[int, int]:
+    """nrrs_noalloc_device_status: (status code, NRRS_DEV_* bits) raised by
+    nrrs_decide_emit_noalloc calls since the last read; synchronises the stream and clears them."""
+    f = C.c_uint32(0)
+    rc = lib().nrrs_noalloc_device_status(C.byref(f), stream)
+    return rc, int(f.value)
 
 
 def _check(rc: int, what: str):

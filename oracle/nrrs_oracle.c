@@ -150,6 +150,11 @@ float oracle_activation_sigma_f32(float x) {
     return (x < 0) ? logf(1.0f + expf(x)) : (0.5f * x + ln2);
 }
 float oracle_box_cox_f32(float x) { return 2.0f * (sqrtf(x) - 1.0f); }
+/* warp_roughness, train.h:95 */
+float oracle_warp_roughness_f32(float r) { return 1.0f - expf(-r); }
+/* the StatNet's radiance estimate L from a log-statistic y = log(L + eps), before the ADRRS
+ * clamp (the factor's first step, the same expression as factor() below) */
+float oracle_stat_to_l_f32(float y, float eps) { return expf(y < 20.0f ? y : 20.0f) - eps; }
 
 /* RRSWeightWindow, src/render/common/commoncudautils.h:14-28 */
 float oracle_weight_window_f32(float x, float ww) {

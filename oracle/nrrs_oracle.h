@@ -32,6 +32,8 @@ void oracle_sh16_f64(const double* dir, double* out);
 /* activationSigma (networkcommon.h:61-68) and box_cox_transform (train.cu:19-39) in FP32 */
 float oracle_activation_sigma_f32(float x);
 float oracle_box_cox_f32(float x);
+float oracle_warp_roughness_f32(float r);
+float oracle_stat_to_l_f32(float y, float eps);
 float oracle_weight_window_f32(float x, float ww);
 /* normalizeSpatialCoord (nrctrain.h:111-115) for one point, FP32 */
 void oracle_normalize_pos_f32(const nrrs_config* cfg, const float* p, float* out);

@@ -45,9 +45,11 @@ def lib():
         L.oracle_param_count.restype = C.c_uint64
         L.oracle_param_count.argtypes = [C.POINTER(nb.Config), vp, vp, vp]
         L.oracle_sh16_f64.argtypes = [vp, vp]
-        for f in ("oracle_activation_sigma_f32", "oracle_box_cox_f32"):
+        for f in ("oracle_activation_sigma_f32", "oracle_box_cox_f32", "oracle_warp_roughness_f32"):
             getattr(L, f).restype = C.c_float
             getattr(L, f).argtypes = [C.c_float]
+        L.oracle_stat_to_l_f32.restype = C.c_float
+        L.oracle_stat_to_l_f32.argtypes = [C.c_float, C.c_float]
         L.oracle_weight_window_f32.restype = C.c_float
         L.oracle_weight_window_f32.argtypes = [C.c_float, C.c_float]
         L.oracle_normalize_pos_f32.argtypes = [C.POINTER(nb.Config), vp, vp]
@@ -98,19 +100,112 @@ def lib():
         L.oracle_ubs_error.argtypes = [pe, vp, C.c_uint32, vp, C.c_int, vp]
         L.oracle_set_threads.argtypes = [C.c_int]
         L.oracle_get_threads.restype = C.c_int
+        L.nrrs_synth_vertices.restype = None
+        L.nrrs_synth_vertices.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64] + [vp] * 10
         _lib = L
     return _lib
 
 
 def ref_lib():
-    """The reference's RRSWeightWindow compiled from its own header, or None if not built."""
+    """Reference code compiled from the reference checkout (oracle/ref_harness.cpp): its
+    RRSWeightWindow, activationSigma, warp_roughness, box_cox_transform and the "Gen RRS Number"
+    and "Gen Tids" lambdas of the integrator; None where it was not built."""
     global _ref
     if _ref is None and REF_LIB.exists():
         L = C.CDLL(str(REF_LIB))
+        vp = C.c_void_p
         L.ref_rrs_weight_window.restype = C.c_float
         L.ref_rrs_weight_window.argtypes = [C.c_float, C.c_float]
+        for f in ("ref_activation_sigma", "ref_warp_roughness", "ref_box_cox"):
+            getattr(L, f).restype = C.c_float
+            getattr(L, f).argtypes = [C.c_float]
+        L.ref_gen_rrs_number.restype = None
+        L.ref_gen_rrs_number.argtypes = [C.c_uint32, C.c_int, vp, vp, vp, C.c_int, C.c_float,
+                                         C.c_float, C.c_int, vp, vp]
+        L.ref_gen_tids.restype = C.c_uint64
+        L.ref_gen_tids.argtypes = [C.c_uint32, vp, vp, C.c_uint32, C.c_uint32, C.c_float, C.c_int,
+                                   C.c_float, C.c_int, vp, vp, C.c_uint64]
         _ref = L
     return _ref
+
+
+def ref_gen_rrs_number(net_out, thp, ref_rgb, dp):
+    """The reference's factor lambda (integrator.cpp:1186-1297) on [n][16] network outputs."""
+    L = ref_lib()
+    n = len(thp)
+    net_out = np.ascontiguousarray(net_out, np.float32)
+    thp = np.ascontiguousarray(thp, np.float32)
+    ref_rgb = np.ascontiguousarray(ref_rgb, np.float32)
+    rrs = np.empty(n, np.float32)
+    ceil = np.zeros(n, np.float32)
+    L.ref_gen_rrs_number(n, 1 if dp.factor_source == nb.FACTOR_RRSNET else 0, net_out.ctypes.data,
+                         thp.ctypes.data, ref_rgb.ctypes.data, dp.use_weight_window, dp.clamp_min,
+                         dp.clamp_max, dp.use_ceil, rrs.ctypes.data, ceil.ctypes.data)
+    return rrs, ceil
+
+
+def ref_gen_tids(rrs, rnd, budget, n_specular, rcp_sum, dp, capacity=None):
+    """The reference's decision and emission lambda (integrator.cpp:1370-1457)."""
+    L = ref_lib()
+    n = len(rrs)
+    rrs = np.ascontiguousarray(rrs, np.float32)
+    rnd = np.ascontiguousarray(rnd, np.float32)
+    cap = 9 * n if capacity is None else capacity
+    norm = np.empty(n, np.float32)
+    q = np.zeros(max(cap, 1), np.uint32)
+    tot = L.ref_gen_tids(n, rrs.ctypes.data, rnd.ctypes.data, budget, n_specular,
+                         np.float32(rcp_sum), dp.use_ceil, dp.normalize_rate, dp.scale_up,
+                         norm.ctypes.data, q.ctypes.data, cap)
+    return {"total": int(tot), "queue": q[:min(tot, cap)], "rrs_norm": norm}
+
+
+def synth(seed: int, n: int, first: int = 0) -> dict:
+    """Seeded synthetic vertices (host numpy arrays) from the oracle library's copy of the
+    generator (the same source as the product library's nrrs_synth_vertices), so that CPU-only
+    callers draw identical inputs without loading the product library."""
+    out = {
+        "pos": np.empty((n, 3), np.float32), "wi": np.empty((n, 3), np.float32),
+        "normal": np.empty((n, 3), np.float32), "roughness": np.empty(n, np.float32),
+        "albedo": np.empty((n, 3), np.float32), "thp": np.empty((n, 3), np.float32),
+        "depth": np.empty(n, np.uint32), "rnd": np.empty(n, np.float32),
+        "ref_mean": np.empty(n, np.float32), "target": np.empty((n, 3), np.float32),
+    }
+    lib().nrrs_synth_vertices(seed, first, n, *(out[k].ctypes.data for k in
+                              ("pos", "wi", "normal", "roughness", "albedo", "thp", "depth",
+                               "rnd", "ref_mean", "target")))
+    return out
+
+
+# The library's defaults (nrrs_config_default, nrrs_decide_params_default), restated so that
+# the CPU baseline can build its configuration without loading the product library;
+# tests/test_oracle.py checks that the two agree field by field.
+_CONFIG_DEFAULTS = dict(
+    n_levels=16, n_features_per_level=2, log2_hashmap_size=19, base_resolution=16,
+    per_level_scale=1.5, sh_degree=4, statnet_width=64, statnet_hidden=2, rrsnet_width=64,
+    rrsnet_hidden=2, precision=0, seed=0, table_init_scale=1e-4, lr=1e-2, beta1=0.9, beta2=0.99,
+    eps=1e-15, l2_reg=0.0, stat_eps=0.01, ref_eps=0.01, loss_clamp_max=10.0, cost_offset=1.0,
+    normalize_pos=0, aabb_min=(0.0, 0.0, 0.0), aabb_max=(1.0, 1.0, 1.0), max_queue=1 << 20,
+    max_train=1 << 18, step=3)
+_DECIDE_DEFAULTS = dict(clamp_min=0.05, clamp_max=8.0, normalize_rate=0.85, use_ceil=1,
+                        scale_up=0, use_weight_window=0, weight_window_size=5.0,
+                        factor_source=nb.FACTOR_RRSNET)
+
+
+def default_config(**kw) -> nb.Config:
+    c = nb.Config()
+    for k, v in {**_CONFIG_DEFAULTS, **kw}.items():
+        if k in ("aabb_min", "aabb_max"):
+            getattr(c, k)[:] = list(v)
+        else:
+            setattr(c, k, v)
+    return c
+
+
+def default_decide(**kw) -> nb.DecideParams:
+    p = nb.DecideParams()
+    for k, v in {**_DECIDE_DEFAULTS, **kw}.items():
+        setattr(p, k, v)
+    return p
 
 
 def _soa(v: dict) -> nb.VertexSoA:

@@ -27,9 +27,11 @@ def _ensure_built():
         subprocess.run([sys.executable, str(PKG / "build.py")], check=True)
     if not (ORACLE / "_build" / "libnrrs_oracle.so").exists():
         subprocess.run(["make", "-s", "-C", str(ORACLE)], check=True)
-    if not (ORACLE / "_ref" / "libnrrs_ref.so").exists():
+    ref = os.environ.get("NRRS_REFERENCE", "/root/reference")
+    if not (ORACLE / "_ref" / "libnrrs_ref.so").exists() and Path(ref).is_dir():
         # builds only where the reference checkout is present (see oracle/Makefile)
-        subprocess.run(["make", "-s", "-C", str(ORACLE), "ref-if-present"], check=False)
+        subprocess.run(["make", "-s", "-C", str(ORACLE), "ref-if-present", f"REF={ref}"],
+                       check=False)
 
 
 _ensure_built()

@@ -82,6 +82,85 @@ def test_weight_window_matches_reference_header():
                 O.lib().oracle_weight_window_f32(x, ww))
 
 
+def _ref_or_skip():
+    ref = O.ref_lib()
+    if ref is None:
+        pytest.skip("oracle/_ref not built (reference checkout absent)")
+    return ref
+
+
+def test_scalar_helpers_match_reference_sources():
+    """activationSigma (networkcommon.h:61-68), warp_roughness (train.h:95) and the scalar
+    box_cox_transform (train.cu:19-28), compiled from the reference's own text."""
+    ref = _ref_or_skip()
+    L = O.lib()
+    xs = np.concatenate([np.linspace(-30, 30, 6001), [-1e-30, 0.0, 1e-30, -88.0, 88.0]])
+    for x in xs.astype(np.float32):
+        assert np.float32(ref.ref_activation_sigma(x)) == np.float32(L.oracle_activation_sigma_f32(x))
+    for r in np.linspace(0, 8, 2001).astype(np.float32):
+        assert np.float32(ref.ref_warp_roughness(r)) == np.float32(L.oracle_warp_roughness_f32(r))
+    for x in np.concatenate([np.linspace(0, 100, 4001), np.geomspace(1e-8, 1e6, 2001)]).astype(np.float32):
+        assert np.float32(ref.ref_box_cox(x)) == np.float32(L.oracle_box_cox_f32(x))
+
+
+@pytest.mark.parametrize("source", [nb.FACTOR_RRSNET, nb.FACTOR_ADRRS], ids=["rrsnet", "adrrs"])
+@pytest.mark.parametrize("ww", [0, 1])
+def test_factor_matches_reference_lambda(source, ww):
+    """The oracle's FP32 factor (activation or ADRRS estimate, weight window, clamp) equals the
+    reference's "Gen RRS Number" lambda (integrator.cpp:1186-1297) run on the same network
+    outputs, bit for bit. The pixel colour is grey (every channel = ref_mean), the case the
+    vertex record's single ref_mean describes."""
+    _ref_or_skip()
+    L = O.lib()
+    cfg = nb.default_config(max_queue=1 << 16)
+    ntab, nst, nrr = O.param_count(cfg)[1:]
+    rng = np.random.default_rng(5)
+    p = np.concatenate([rng.uniform(-0.5, 0.5, ntab), rng.uniform(-0.3, 0.3, nst + nrr)]).astype(np.float32)
+    n = 4096
+    v = nb_synth(7, n)
+    dp = nb.default_decide(factor_source=source, use_weight_window=ww, clamp_max=8.0)
+    o = O.infer(cfg, p, v, dp, "f32", want=("stats", "raw", "rrs"))
+    net_out = np.zeros((n, 16), np.float32)
+    if source == nb.FACTOR_RRSNET:
+        net_out[:, 0] = o["raw"]
+    else:
+        for c in range(3):
+            net_out[:, c] = [L.oracle_stat_to_l_f32(y, cfg.stat_eps) for y in o["stats"][:, c]]
+    ref_rgb = np.repeat(v["ref_mean"][:, None], 3, axis=1)
+    rrs, ceil = O.ref_gen_rrs_number(net_out, v["thp"], ref_rgb, dp)
+    assert np.array_equal(rrs.view(np.uint32), o["rrs"].astype(np.float32).view(np.uint32))
+    assert np.array_equal(ceil, np.ceil(rrs))
+
+
+@pytest.mark.parametrize("use_ceil,scale_up", [(1, 0), (0, 0), (0, 1), (1, 1)])
+def test_decision_matches_reference_lambda(use_ceil, scale_up):
+    """The oracle's decision and emission equal the reference's "Gen Tids" lambda
+    (integrator.cpp:1370-1457, with TidQueue::push run in vertex order) on the same factors,
+    draws and normalisation sum: normalised factors, split counts and the queue, bit for bit."""
+    _ref_or_skip()
+    rng = np.random.default_rng(17 + use_ceil + 2 * scale_up)
+    n = 50_000
+    rrs = np.clip(rng.lognormal(-0.3, 1.0, n), 0.05, 8).astype(np.float32)
+    rnd = rng.random(n, dtype=np.float32)
+    rnd[:64] = 0.0
+    rnd[64:128] = np.float32(0.99999994)
+    dp = nb.default_decide(use_ceil=use_ceil, scale_up=scale_up, normalize_rate=0.85)
+    budget, nspec = n, n // 50
+    o = O.decide_emit(rrs, rnd, budget, nspec, dp)
+    shift = O.sum_shift(n, float(np.ceil(dp.clamp_max)) if use_ceil else dp.clamp_max)
+    _, s = O.sum_fixed(rrs, use_ceil, shift)
+    rcp = np.float32(1.0) / np.float32(s)
+    r = O.ref_gen_tids(rrs, rnd, budget, nspec, rcp, dp)
+    assert r["total"] == o["total"]
+    assert np.array_equal(r["rrs_norm"].view(np.uint32), o["rrs_norm"].view(np.uint32))
+    assert np.array_equal(r["queue"], o["queue"])
+    assert np.array_equal(np.bincount(r["queue"], minlength=n), o["split"].astype(np.int64))
+
+
+def nb_synth(seed, n):
+    return O.synth(seed, n)
+
+
 @pytest.mark.parametrize("case", json.loads((GOLD / "decide_cases.json").read_text()),
                          ids=lambda c: c["name"])
 def test_decide_golden(case):
@@ -234,3 +313,20 @@ def test_adam_matches_textbook():
     mh = (0.9 * 0.1 * g + 0.1 * g) / (1 - 0.9 ** 2)
     vh = (0.99 * 0.01 * g * g + 0.01 * g * g) / (1 - 0.99 ** 2)
     assert np.allclose(p0 - p, 1e-2 * np.sign(g) + 1e-2 * mh / np.sqrt(vh), rtol=1e-5)
+
+
+def test_oracle_defaults_and_generator_agree_with_library():
+    """The CPU baseline builds its configuration and inputs from oracle/ alone; they must be the
+    library's own defaults and generator output."""
+    a, b = O.default_config(), nb.default_config()
+    for name, _ in nb.Config._fields_:
+        x, y = getattr(a, name), getattr(b, name)
+        if name in ("aabb_min", "aabb_max"):
+            x, y = list(x), list(y)
+        assert x == y, name
+    a, b = O.default_decide(), nb.default_decide()
+    for name, _ in nb.DecideParams._fields_:
+        assert getattr(a, name) == getattr(b, name), name
+    va, vb = O.synth(3, 70_000, first=1234), nb.synth(3, 70_000, first=1234)
+    for k in va:
+        assert np.array_equal(va[k], vb[k]), k
