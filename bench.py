@@ -1,49 +1,43 @@
 """Benchmark of the NRRS per-vertex step on B200 (one JSON line on rank 0).
 
-Default workload "frame1080p": one frame at 1920x1080 with 6 bounces. Each bounce runs
-inference, the RRS decision and emission on 2,073,600 synthetic path vertices; the frame then
-runs one training step on 262,144 samples. Mixed precision: FP16 table, FP16 tcgen05 MLPs for
-inference (FP16 StatNet / BF16 RRSNet in training) with FP32 accumulation, FP32 master weights
-and Adam state, exact 64-bit normalisation sums. Inputs are seeded synthetic records with the
-workload's distributions; each bounce has its own 158 MB vertex buffer, so inputs are larger
-than L2.
+The metric is "RRS vertices/s and train samples/s, mixed precision vs plain FP32 at stated
+error". The default run measures it on the largest single-GPU configuration of the workload
+definition and puts the other two configurations beside it:
 
-Other workloads (--workload):
-  batched   depths 0..9 with round(2,073,600 x 0.6^d) vertices each, 10 % of them split into
-            U{1..4} copies, concatenated in one SoA; after autotuning the launch shape the
-            whole multi-depth step is ONE CUDA-graph launch, timed beside launching each depth
-            separately on the same vertices (and checked to decide identically)
-  frame4k   3840x2160: 8,294,400 vertices per bounce, 10 bounces, MLPs 128 wide x 3 hidden
-            layers (BF16 by default), 2^22-entry table, 10 training steps of 262,144 samples
-  render1080p
-            a path-traced 1920x1080 frame around the NRRS step: camera rays, then per bounce
-            (up to 6) BVH trace (rays sorted first), shading into the vertex queue, nrrs_step,
-            scatter (NEE + BSDF rays) and shadow rays, in a closed room of 3000 boxes
-            (36k triangles) seen from inside;
-            metric path vertices/s
-  render_train1080p
-            the same frame as a training frame: the radiance of every shaded and shadow ray
-            and the surviving vertices go to the path records, then the per-pixel error, the
-            training batch and one training step of 262,144 samples; metric path vertices/s
-  records1080p
-            the training-data side of a 1920x1080 frame: 8 bounces of path vertices (about
-            10.1M) record 7.0M path nodes and 7.5M radiance contributions, then the training
-            batch and the sample weights are built; metric path nodes/s (one step = one frame)
+  frame4k (headline, `value`)
+            one online train-and-infer frame at 3840x2160: 10 bounces of inference, RRS
+            decision and emission on 8,294,400 path vertices each, then 10 training steps of
+            262,144 samples; StatNet and RRSNet 128 wide with 3 hidden layers in BF16 on the
+            tensor cores (FP32 accumulation, FP32 master weights and Adam state), a 2^22-entry
+            FP16 hash table, exact 64-bit normalisation sums
+  fp32_per_depth
+            the same frame on the plain FP32 path (FP32 table, FP32 SIMT MLPs), one launch
+            sequence per bounce, on the same GPU and the same inputs
+  errors    stats, factors and training losses of both paths against the FP64 oracle and
+            against each other; decisions of the mixed path against the oracle's at equal
+            factors
+  secondary.frame1080p
+            the 1080p frame: 6 bounces x 2,073,600 vertices + 1 training step, 64 wide x 2
+            hidden, FP16, 2^19 table; mixed against plain FP32
+  secondary.batched
+            depths 0..9 with round(2,073,600 x 0.6^d) vertices, 10 % of them split into U{1..4}
+            copies (5,925,732 vertices): the mixed path as ONE CUDA-graph launch of the batched
+            step, against the plain FP32 path launched depth by depth
+
+Single workloads (--workload frame4k|frame1080p|batched|records1080p|render1080p|
+render_train1080p, with --only) run one arm for profiling.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload frame1080p|batched|frame4k|records1080p|render1080p|
-                              render_train1080p]
-                  [--precision fp16|bf16|fp32]
-                  [--no-train]
+                  [--workload ...] [--only] [--precision fp16|bf16|fp32] [--no-train]
 
 value    = vertices/s of the whole job (device-timed steps, max over ranks)
 e2e      = the same metric through the C-ABI with host (pinned) inputs: the H2D copy of each
            step's vertices and training batch and the D2H read of queue sizes and losses are
            inside the timed region; uploads run on a copy stream, overlapping the compute of
            the previous bounce
-roofline = dominant kernel (inference) achieved algorithmic GB/s vs the measured HBM peak
---impl reference times the reference's CPU path (the oracle port of it, all host threads)
-on a bounded sample of the same workload.
+roofline = the dominant kernel's algorithmic GB/s against the measured HBM peak
+--impl reference times the reference's CPU path (the oracle's FP32 restatement, all host
+threads) on a bounded sample of the same workload per step; it loads no product library.
 """
 from __future__ import annotations
 
@@ -57,24 +51,29 @@ from pathlib import Path
 
 REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO / "nrrs-code_b200"))
+sys.path.insert(0, str(REPO / "oracle"))
 
 import numpy as np  # noqa: E402
 
-import nrrs_b200 as nb  # noqa: E402
+# The product binding is imported by the GPU arms only (load_product()); the reference arm
+# never loads the product library.
+nb = None
 
 SOA_BYTES = 72            # pos, wi, normal, roughness, albedo, thp, depth, ref_mean
 RND_BYTES = 4
 TARGET_BYTES = 12
 METRIC = "RRS vertices/s and train samples/s, mixed-prec vs FP32 plain at stated error"
 FIELDS = ("pos", "wi", "normal", "roughness", "albedo", "thp", "depth", "ref_mean", "rnd")
+PREC = {"fp32": 0, "fp16": 1, "bf16": 2}   # nrrs_precision
+FACTOR_RRSNET = 3
 
 WORKLOADS = {
+    "frame4k": dict(bounces=10, n_vert=8_294_400, train_steps=10, train_batch=262_144,
+                    width=128, hidden=3, log2_table=22, steps=5, precision="bf16"),
     "frame1080p": dict(bounces=6, n_vert=2_073_600, train_steps=1, train_batch=262_144,
                        width=64, hidden=2, log2_table=19, steps=50, precision="fp16"),
     "batched": dict(bounces=10, n_vert=2_073_600, train_steps=0, train_batch=262_144,
                     width=64, hidden=2, log2_table=19, steps=50, precision="fp16"),
-    "frame4k": dict(bounces=10, n_vert=8_294_400, train_steps=10, train_batch=262_144,
-                    width=128, hidden=3, log2_table=22, steps=5, precision="bf16"),
     # the reference's shipped settings (render/test.json:75-82): node buffer 10 x pixels,
     # throughput scaled by rrs, later siblings without RRSNet target; zero-L samples kept
     # 600 frames: about a second of timed work, so that the clock sampler sees it
@@ -88,6 +87,14 @@ WORKLOADS = {
 }
 
 
+def load_product():
+    global nb
+    if nb is None:
+        import nrrs_b200
+        nb = nrrs_b200
+    return nb
+
+
 def env_int(k, d):
     try:
         return int(os.environ.get(k, d))
@@ -96,20 +103,20 @@ def env_int(k, d):
 
 
 def measured_peaks():
+    """(HBM GB/s, BF16 TFLOP/s burst, source) from MEASURED_PEAKS.json, else the fallback."""
     f = REPO / "MEASURED_PEAKS.json"
     if f.exists():
         j = json.loads(f.read_text())
-        return j.get("hbm_gbs", 6650.0), "measured"
-    return 6650.0, "fallback"
+        return j.get("hbm_gbs", 6650.0), j.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
 
 
-def traffic_per_vertex(kernel: str):
-    """DRAM bytes per vertex of the kernel from the committed ncu summary, if any."""
+def traffic_per_vertex(kernel: str, workload: str):
+    """DRAM bytes per vertex of the kernel on the workload from the committed ncu summary."""
     f = REPO / "profiles" / "traffic.json"
     if f.exists():
         j = json.loads(f.read_text())
-        if kernel in j:
-            return j[kernel]
+        return j.get(workload, {}).get(kernel)
     return None
 
 
@@ -166,100 +173,157 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def config_fields(precision: str, wl: dict, max_queue: int, max_train: int) -> dict:
+    return dict(precision=PREC[precision], max_queue=max_queue, max_train=max_train,
+                statnet_width=wl["width"], statnet_hidden=wl["hidden"],
+                rrsnet_width=wl["width"], rrsnet_hidden=wl["hidden"],
+                log2_hashmap_size=wl["log2_table"])
+
+
 def make_config(precision: str, wl: dict, max_queue: int, max_train: int):
-    prec = {"fp16": nb.PREC_FP16, "bf16": nb.PREC_BF16, "fp32": nb.PREC_FP32}[precision]
-    return nb.default_config(precision=prec, max_queue=max_queue, max_train=max_train,
-                             statnet_width=wl["width"], statnet_hidden=wl["hidden"],
-                             rrsnet_width=wl["width"], rrsnet_hidden=wl["hidden"],
-                             log2_hashmap_size=wl["log2_table"])
+    return load_product().default_config(**config_fields(precision, wl, max_queue, max_train))
 
 
 def do_train_of(args, wl):
     return not args.no_train and wl["train_steps"] > 0
 
 
-def workload_name(args):
-    wl = WORKLOADS[args.workload]
-    if args.workload == "frame1080p" and wl["bounces"] == 6 and wl["n_vert"] == 2_073_600:
-        name = "frame1080p_6bounce_infer_decide_emit"
-    else:
-        name = (f"{args.workload}_{wl['bounces']}x{wl['n_vert']}_w{wl['width']}h{wl['hidden']}"
-                f"_infer_decide_emit")
-    if do_train_of(args, wl):
-        name += ("_train262144" if wl["train_steps"] == 1 else
-                 f"_train{wl['train_steps']}x{wl['train_batch']}")
-    return f"{name}_{args.precision}"
+def workload_name(name: str, wl: dict, train: bool, precision: str) -> str:
+    s = (f"{name}_{wl['bounces']}x{wl['n_vert']}_w{wl['width']}h{wl['hidden']}"
+         f"_T2^{wl['log2_table']}_infer_decide_emit")
+    if train:
+        s += f"_train{wl['train_steps']}x{wl['train_batch']}"
+    return f"{s}_{precision}"
 
 
-def cpu_sample(cfg, wl, n_sample: int, seconds: float, train_n: int, do_train: bool):
-    """Oracle FP32 (OpenMP, all host threads) on a bounded sample of the workload; returns the
-    step-equivalent vertices/s, the cores used, a description of the sample and the step time."""
-    sys.path.insert(0, str(REPO / "oracle"))
-    import oracle as O
-    O.set_threads(os.cpu_count() or 1)
-    cores = O.threads()
-    v = nb.synth(7, n_sample)
-    npar = O.param_count(cfg)[0]
-    params = (np.random.default_rng(0).uniform(-1, 1, npar) * 0.1).astype(np.float32)
-    dp = nb.default_decide()
-    t_inf, reps = 0.0, 0
-    t0 = time.perf_counter()
-    while True:
+def frame_config(name: str, wl: dict, train: bool, precision: str, world: int) -> dict:
+    """The `config` object of a frame workload; identical in the GPU arm and the reference arm."""
+    batched = name == "batched"
+    total = batched_total(wl) if batched else wl["bounces"] * wl["n_vert"]
+    return {"workload": workload_name(name, wl, train, precision), "bounces": wl["bounces"],
+            "vertices_per_bounce": wl["n_vert"], "vertices_per_step": total,
+            "train_steps": wl["train_steps"] if train else 0,
+            "train_batch": wl["train_batch"] if train else 0,
+            "encoding": f"hashgrid L16 F2 T2^{wl['log2_table']} Nmin16 b1.5 (FP16 table) + SH deg4",
+            "mlp": f"StatNet 64->{wl['width']}x{wl['hidden']}->3, "
+                   f"RRSNet 16->{wl['width']}x{wl['hidden']}->1, {precision} MMA / FP32 accumulate",
+            "l2": "inputs larger than L2 (one vertex buffer per bounce)" if not batched else
+                  "inputs larger than L2 (one 450 MB SoA of all depths)",
+            "parallelism": f"dp{world}"}
+
+
+# ---- the reference's CPU path: the oracle's FP32 restatement on the host cores ----------------
+
+class CpuFrameSample:
+    """Bounded samples of a frame workload on the host cores with the oracle's FP32 path
+    (OpenMP, all host threads). One step processes a fraction f of the frame: inference,
+    decision and emission on S vertices (f = S / vertices per frame), the gradients of f x the
+    frame's training samples, and Adam over f x the frame's training steps x the parameter count
+    (a rotating slice of the parameter array: Adam is element-wise). Nothing is extrapolated:
+    a step's time is measured whole, and value = S / step time."""
+
+    def __init__(self, wl: dict, train: bool, target_s: float = 0.5):
+        import oracle as O
+        self.O = O
+        O.set_threads(os.cpu_count() or 1)
+        self.cores = O.threads()
+        self.wl, self.train = wl, train
+        self.cfg = O.default_config(**config_fields("fp32", wl, 1 << 21, 1 << 18))
+        npar, ntab, _, _ = O.param_count(self.cfg)
+        rng = np.random.default_rng(0)
+        self.params = np.concatenate([rng.uniform(-0.5, 0.5, ntab),
+                                      rng.uniform(-0.1, 0.1, npar - ntab)]).astype(np.float32)
+        self.m = np.zeros_like(self.params)
+        self.v = np.zeros_like(self.params)
+        self.g = np.zeros_like(self.params)   # gradient buffer, reused as a trainer would
+        self.t = 0
+        self.slice0 = 0
+        self.dp = O.default_decide()
+        self.frame_vertices = wl["bounces"] * wl["n_vert"]
+        self._size(32_768)
         a = time.perf_counter()
-        r = O.infer(cfg, params, v, dp, "f32", want=("stats", "rrs"))
-        O.decide_emit(r["rrs"].astype(np.float32), v["rnd"], n_sample, 0, dp)
-        t_inf += time.perf_counter() - a
-        reps += 1
-        if time.perf_counter() - t0 > seconds * (0.6 if do_train else 1.0):
-            break
-    per_vertex = t_inf / (reps * n_sample)
-    per_sample, treps = 0.0, 0
-    if do_train:
-        tv = nb.synth(8, train_n)
-        t_train = 0.0
-        t1 = time.perf_counter()
+        self.step()
+        dt = time.perf_counter() - a
+        s = int(min(262_144, max(32_768, 32_768 * target_s / max(dt, 1e-3))))
+        self._size(s // 1024 * 1024)
+
+    def _size(self, s: int):
+        wl, O = self.wl, self.O
+        self.S = s
+        self.f = s / self.frame_vertices
+        self.vx = O.synth(7, s)
+        self.nt = max(256, int(round(self.f * wl["train_steps"] * wl["train_batch"]))) \
+            if self.train else 0
+        self.tv = O.synth(8, self.nt) if self.train else None
+        self.n_adam = int(round(self.f * wl["train_steps"] * self.params.size)) if self.train else 0
+
+    def step(self):
+        O = self.O
+        r = O.infer(self.cfg, self.params, self.vx, self.dp, "f32", want=("stats", "rrs"))
+        O.decide_emit(r["rrs"].astype(np.float32), self.vx["rnd"], self.S, 0, self.dp,
+                      shift_n=self.S)
+        if self.train:
+            g, _ = O.train_grads(self.cfg, self.params, self.tv, self.tv["target"], "f32",
+                                 out=self.g)
+            self.t += 1
+            first = self.slice0
+            count = min(self.n_adam, self.params.size - first)
+            O.adam(self.cfg, self.params, g, self.m, self.v, self.t, first, count)
+            self.slice0 = (first + count) % self.params.size
+
+    def describe(self) -> str:
+        s = f"per step: infer+decide+emit on {self.S} vertices"
+        if self.train:
+            s += (f", train gradients on {self.nt} samples and Adam over {self.n_adam} "
+                  f"parameters (the same fraction {self.f:.2e} of the frame)")
+        return s
+
+    def run(self, steps: int, warmup: int, seconds: float | None = None):
+        """(vertices/s, mean step seconds, steps timed)"""
+        for _ in range(warmup):
+            self.step()
+        times = []
+        t0 = time.perf_counter()
         while True:
             a = time.perf_counter()
-            O.train_grads(cfg, params, tv, tv["target"], "f32")
-            t_train += time.perf_counter() - a
-            treps += 1
-            if time.perf_counter() - t1 > seconds * 0.4:
+            self.step()
+            times.append(time.perf_counter() - a)
+            if seconds is None and len(times) >= steps:
                 break
-        per_sample = t_train / (treps * train_n)
-    verts = wl["bounces"] * wl["n_vert"]
-    step_s = verts * per_vertex + wl["train_steps"] * wl["train_batch"] * per_sample
-    sample = (f"{reps} x infer+decide on {n_sample} vertices"
-              + (f", {treps} x train grads on {train_n} samples" if do_train else "")
-              + "; step time extrapolated from per-vertex and per-sample costs")
-    return verts / step_s, cores, sample, step_s
+            if seconds is not None and time.perf_counter() - t0 > seconds:
+                break
+        step_s = float(np.mean(times))
+        return self.S / step_s, step_s, len(times)
 
 
 def run_reference(args, rank, world):
+    """--impl reference: the reference's CPU path on the host cores, on rank 0 only."""
     if rank != 0:
         return 0
     wl = WORKLOADS[args.workload]
-    do_train = do_train_of(args, wl)
-    cfg = make_config("fp32", wl, 1 << 21, 1 << 16)
-    value, cores, sample, step_s = cpu_sample(cfg, wl, 131072, 10.0 * max(1, args.steps) / 10,
-                                              8192, do_train)
+    train = do_train_of(args, wl)
+    cpu = CpuFrameSample(wl, train)
+    value, step_s, k = cpu.run(args.steps, args.warmup)
     line = {
         "metric": METRIC, "value": value, "unit": "vertices/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
+        "steps": k, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic", "impl": "reference",
-        "config": {"workload": workload_name(args), "bounces": wl["bounces"],
-                   "vertices_per_bounce": wl["n_vert"],
-                   "train_batch": wl["train_batch"] if do_train else 0},
-        "cpu_baseline": {"value": value, "unit": "vertices/s", "cores": cores, "kind": "port",
-                         "sample": sample},
+        "config": frame_config(args.workload, wl, train, args.precision, world),
+        "cpu_baseline": {"value": value, "unit": "vertices/s", "cores": cpu.cores,
+                         "kind": "port", "sample": cpu.describe()},
         "e2e": {"value": value, "unit": "vertices/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
-        "note": "reference CPU path = FP32 C restatement (oracle/) with OpenMP; the reference "
-                "itself needs OptiX/KiRaRay/tiny-cuda-nn and cannot be built",
+        "note": "the reference's CPU path: the FP32 C restatement in oracle/ (encoding, MLPs, glue, "
+                "factor, decision and emission, losses, gradients, Adam) with OpenMP on all host "
+                "threads; the reference itself needs OptiX, KiRaRay and tiny-cuda-nn and cannot be "
+                "built here. Each step is a bounded sample of the frame, timed whole",
     }
     print(json.dumps(line), flush=True)
     return 0
 
+
+# ---- the GPU arms ---------------------------------------------------------------------------
 
 def pinned(torch, v: dict, keys):
     return {k: torch.from_numpy(v[k].view(np.int32) if v[k].dtype == np.uint32 else v[k]).pin_memory()
@@ -279,16 +343,28 @@ def step_outputs(torch, dev, n, cap, n_sizes=1):
                 sz=torch.zeros(n_sizes, dtype=torch.int32, device=dev))
 
 
-def batched_vertices(n_top, depths, seed):
+def batched_counts(n_top, depths, seed):
     """Depth d holds round(n_top x 0.6^d) path vertices; 10 % of them are split into U{1..4}
-    copies (a split vertex re-enters the next queue several times). Returns the concatenated
-    records and the per-depth counts."""
+    copies. Returns, per depth, the base count and the copy multipliers."""
     rng = np.random.default_rng(seed)
-    counts, parts = [], []
+    out = []
     for d in range(depths):
         base = int(round(n_top * 0.6 ** d))
-        v = nb.synth(seed * 131 + d, base)
         mult = np.where(rng.random(base) < 0.1, rng.integers(1, 5, base), 1)
+        out.append((base, mult))
+    return out
+
+
+def batched_total(wl) -> int:
+    return int(sum(int(m.sum()) for _, m in batched_counts(wl["n_vert"], wl["bounces"], 2024)))
+
+
+def batched_vertices(n_top, depths, seed):
+    """The concatenated records of all depths (a split vertex re-enters the next queue several
+    times) and the per-depth counts."""
+    counts, parts = [], []
+    for d, (base, mult) in enumerate(batched_counts(n_top, depths, 2024)):
+        v = nb.synth(seed * 131 + d, base)
         idx = np.repeat(np.arange(base), mult)
         sub = {k: np.ascontiguousarray(a[idx]) for k, a in v.items() if k in FIELDS}
         sub["depth"] = np.full(idx.size, d, np.uint32)
@@ -297,212 +373,374 @@ def batched_vertices(n_top, depths, seed):
     return {k: np.concatenate([p[k] for p in parts]) for k in FIELDS}, counts
 
 
-def run_ours(args, rank, world, local_rank):
-    import torch
-    torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    dev = torch.device("cuda", local_rank)
-    stream = torch.cuda.current_stream().cuda_stream
-    wl = WORKLOADS[args.workload]
-    B, N = wl["bounces"], wl["n_vert"]
-    do_train = do_train_of(args, wl)
-    batched = args.workload == "batched"
-    dp = nb.default_decide()
+class Timer:
+    """Device time of K steps on the current stream (CUDA events), max over ranks."""
 
-    # ---- synthetic inputs: pinned host copies and device copies ----
-    if batched:
-        cat, counts = batched_vertices(N, B, 2024 + rank)
-        host_b = [pinned(torch, cat, FIELDS)]
-        total = int(sum(counts))
-    else:
-        host_b = []
-        for d in range(B):
-            v = nb.synth(1000 + 97 * rank + d, N)
-            v["depth"] = np.full(N, d, np.uint32)
-            host_b.append(pinned(torch, v, FIELDS))
-        total = B * N
-    dev_b = [{k: t.to(dev) for k, t in hb.items()} for hb in host_b]
-    max_q = total if batched else N
-    net = nb.NRRSNetwork(make_config(args.precision, wl, max_q, wl["train_batch"]))
-    tune = None
-    if args.launch_shape:
-        shape = [int(x) for x in args.launch_shape.split(",")]
-        if len(shape) > 2:
-            net.set_infer_split(shape[2])
-        net.set_launch_shape(shape[0], shape[1])
-    else:
-        # the library's launch-shape tuner (CTAs per SM x warpgroups per CTA x inference mode)
-        tune = json.loads(net.autotune(min(max_q, N)))
+    def __init__(self, torch, dist, dev):
+        self.torch, self.dist, self.dev = torch, dist, dev
+
+    def sync(self):
+        self.torch.cuda.synchronize()
+        if self.dist:
+            self.dist.barrier()
+        self.torch.cuda.synchronize()
+
+    def __call__(self, fn, steps, warmup, clocks=None):
+        torch = self.torch
+        for _ in range(warmup):
+            fn()
+        self.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ctx = clocks if clocks is not None else _Null()
+        with ctx:
+            e0.record()
+            for _ in range(steps):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+        self.sync()
+        ms = e0.elapsed_time(e1)
+        if self.dist:
+            t = torch.tensor([ms], device=self.dev)
+            self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms / steps
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+class FrameArm:
+    """One precision of a per-bounce frame workload on this GPU: the network, its outputs and the
+    step (every bounce's nrrs_step, then the frame's training steps)."""
+
+    def __init__(self, torch, dev, stream, wl, precision, dev_b, td, train, world,
+                 launch_shape=None, tune=True, sharded=False):
+        self.torch, self.dev, self.stream, self.wl = torch, dev, stream, wl
+        self.B, self.N = wl["bounces"], wl["n_vert"]
+        self.precision = precision
+        self.dev_b, self.td, self.train = dev_b, td, train
+        self.net = nb.NRRSNetwork(make_config(precision, wl, self.N, wl["train_batch"]))
+        self.tune = None
+        if launch_shape:
+            shape = [int(x) for x in launch_shape.split(",")]
+            if len(shape) > 2 and precision != "fp32":
+                self.net.set_infer_split(shape[2])
+            self.net.set_launch_shape(shape[0], shape[1])
+        elif tune:
+            self.tune = json.loads(self.net.autotune(self.N))
+        self.cap = 9 * self.N
+        self.outs = [step_outputs(torch, dev, self.N, self.cap) for _ in range(self.B)]
+        self.soas = [soa_of(b) for b in dev_b]
+        self.tsoa = soa_of(td) if train else None
+        self.loss = torch.zeros(2, dtype=torch.float64, device=dev)
+        self.dp = nb.default_decide()
+        self.sharded = None
+        self.world = world
+        if sharded:
+            # each rank holds one shard of an N-times larger queue: one integer all-reduce of the
+            # exact sum per bounce, data-parallel gradients per train step
+            from nrrs_parallel import ShardedNRRS
+            self.sharded = ShardedNRRS(self.net)
+            self.acc = torch.zeros(1, dtype=torch.int64, device=dev)
+            self.grads_buf = torch.zeros(self.net.param_count(), dtype=torch.float32, device=dev)
+
+    def step(self, pre=None, post=None):
+        net, dp, N, s = self.net, self.dp, self.N, self.stream
+        for d in range(self.B):
+            o = self.outs[d]
+            if pre:
+                pre(d)
+            if self.sharded is None:
+                net.generateRRSNumber(self.soas[d], self.dev_b[d]["rnd"], N, N, 0, dp, o["stats"],
+                                      o["rrs"], o["norm"], o["split"], o["q"], self.cap, o["sz"], s)
+            else:
+                self.sharded.step(self.soas[d], self.dev_b[d]["rnd"], N, N * self.world, 0, dp,
+                                  o["stats"], o["rrs"], o["norm"], o["split"], o["q"], self.cap,
+                                  o["sz"], self.acc, s)
+            if post:
+                post(d)
+        if self.train and pre:
+            pre("train")
+        for _ in range(self.wl["train_steps"] if self.train else 0):
+            if self.sharded is None:
+                net.train(self.tsoa, self.td["target"], self.wl["train_batch"], self.loss, s)
+            else:
+                self.sharded.train_step(self.tsoa, self.td["target"], self.wl["train_batch"],
+                                        self.grads_buf, self.loss, s)
+        if self.train and post:
+            post("train")
+
+    def measure(self, timer, steps, warmup, clocks=None):
+        """ms per step, per-kernel profile and our kernel launches in the timed region"""
+        net = self.net
+        for _ in range(warmup):
+            self.step()
+        timer.sync()
+        l0 = net.launch_count()
+        net.profile(True)
+        net.profile_read()
+        ms = timer(self.step, steps, 0, clocks)
+        launches = net.launch_count() - l0
+        prof = net.profile_read()
+        net.profile(False)
+        return ms, prof, launches
+
+    def close(self):
+        self.net.close()
+
+
+def train_rate(prof, wl, steps):
+    t_train = sum(t for k, (n, t) in prof.items() if k.startswith("train") or k == "adam"
+                  or k in ("pack_weights", "table_half"))
+    return wl["train_steps"] * wl["train_batch"] * steps / (t_train * 1e-3) if t_train else None
+
+
+def frame_inputs(torch, dev, wl, seed0, rank, train):
+    host_b, dev_b = [], []
+    for d in range(wl["bounces"]):
+        v = nb.synth(seed0 + 97 * rank + d, wl["n_vert"])
+        v["depth"] = np.full(wl["n_vert"], d, np.uint32)
+        hb = pinned(torch, v, FIELDS)
+        host_b.append(hb)
+        dev_b.append({k: t.to(dev) for k, t in hb.items()})
     th = td = None
-    if do_train:
+    if train:
         tv = nb.synth(5000 + rank, wl["train_batch"])
         th = pinned(torch, tv, FIELDS + ("target",))
         td = {k: t.to(dev) for k, t in th.items()}
-    loss = torch.zeros(2, dtype=torch.float64, device=dev)
+    return host_b, dev_b, th, td
 
-    graph = None
-    if batched:
-        caps = [9 * c for c in counts]
-        offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
-        qoffs = np.concatenate([[0], np.cumsum(caps)]).astype(np.int64)
-        segs = [nb.Segment(int(offs[k]), counts[k], N, 0, int(qoffs[k]), caps[k]) for k in range(B)]
-        ob = step_outputs(torch, dev, total, int(qoffs[-1]), B)
-        soa = soa_of(dev_b[0])
-        l0 = net.launch_count()
-        graph = net.captureBatched(soa, dev_b[0]["rnd"], segs, dp, ob["stats"], ob["rrs"],
-                                   ob["norm"], ob["split"], ob["q"], ob["sz"])
-        kernels_per_graph = net.launch_count() - l0
-        # per-depth comparison: one step per depth, separate launches, the same vertices
-        per = []
-        for k in range(B):
-            sub = {f: t[int(offs[k]):int(offs[k + 1])] for f, t in dev_b[0].items()}
-            per.append((sub, soa_of(sub), step_outputs(torch, dev, counts[k], caps[k])))
 
-        def step(pre=None, post=None):
-            if pre:
-                pre(0)
-            graph.launch(stream)
-            if post:
-                post(0)
+def roofline_of(prof, precision, mode, wl, inf_vertices, workload):
+    """Algorithmic bytes per vertex of each inference kernel (every hash-corner gather at table
+    precision) for the HBM line; StatNet + RRSNet FLOPs over the MLP kernels for the tensor line."""
+    hbm, bf16, src = measured_peaks()
+    feat_bytes = 4 if precision == "fp32" else 2
+    gathered = 16 * 8 * 2 * feat_bytes
+    attrs = 12 * 5 + 4 * 3                        # wi, normal, albedo, thp, pos; rough, ref, depth
+    w_, h_ = wl["width"], wl["hidden"]
+    flop_stat = 2 * (64 * w_ + (h_ - 1) * w_ * w_ + w_ * 3)
+    flop_rrs = 2 * (16 * w_ + (h_ - 1) * w_ * w_ + w_)
+    b_of = {"infer_fp32": SOA_BYTES + gathered + 16,
+            "encode": 4 * 12 + gathered + 64,
+            "infer_tc": (SOA_BYTES + gathered + 16 if mode == 0 else
+                         (64 + attrs - 12 + 16 if mode == 1 else 64 + attrs - 12 + 12 + 32)),
+            "infer_rrs": 32 + 4}
+    roof = mlp = None
+    cands = {k: prof[k] for k in b_of if k in prof and prof[k][0]}
+    if cands:
+        kind = max(cands, key=lambda k: cands[k][1])
+        n_l, ms_l = cands[kind]
+        launch_ms = ms_l / n_l
+        per_launch = inf_vertices / n_l
+        b_vertex = b_of[kind]
+        achieved = b_vertex * per_launch / (launch_ms * 1e-3) / 1e9
+        tpv = traffic_per_vertex(kind, workload)
+        roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_source": src,
+                "traffic": (tpv * per_launch) if tpv else None, "kernel": kind,
+                "algorithmic_bytes_per_vertex": b_vertex, "vertices_per_launch": per_launch,
+                "launch_ms": launch_ms, "inference_mode": mode}
+    mlp_kinds = [k for k in ("infer_tc", "infer_rrs") if k in prof and prof[k][0]]
+    if precision != "fp32" and mlp_kinds:
+        ms_mlp = sum(prof[k][1] for k in mlp_kinds)
+        n_launch = prof["infer_tc"][0]
+        tflops = (flop_stat + flop_rrs) * inf_vertices / (ms_mlp * 1e-3) / 1e12
+        mlp = {"bound": "tensor", "kernels": mlp_kinds, "achieved": tflops, "peak": bf16,
+               "unit": "TFLOP/s", "frac": tflops / bf16, "peak_source": src,
+               "flop_per_vertex": flop_stat + flop_rrs, "ms_per_launch": ms_mlp / n_launch,
+               "note": "StatNet + RRSNet MLP FLOPs (true layer sizes) over the time of the "
+                       "kernels that run them; in the fused mode that kernel also gathers"}
+    return roof, mlp
 
-        def step_per_depth():
-            for k, (sub, s, p) in enumerate(per):
-                net.generateRRSNumber(s, sub["rnd"], counts[k], N, 0, dp, p["stats"], p["rrs"],
-                                      p["norm"], p["split"], p["q"], caps[k], p["sz"], stream)
-    else:
-        cap = 9 * N
-        outs = [step_outputs(torch, dev, N, cap) for _ in range(B)]
-        soas = [soa_of(b) for b in dev_b]
-        tsoa = soa_of(td) if do_train else None
-        sharded = None
-        if world > 1:
-            # each rank holds one shard of an N-times larger queue: one integer all-reduce of
-            # the exact sum per bounce, data-parallel gradients per train step
-            from nrrs_parallel import ShardedNRRS
-            sharded = ShardedNRRS(net)
-            acc = torch.zeros(1, dtype=torch.int64, device=dev)
-            grads_buf = torch.zeros(net.param_count(), dtype=torch.float32, device=dev)
 
-        def step(pre=None, post=None):
-            for d in range(B):
-                o = outs[d]
-                if pre:
-                    pre(d)
-                if sharded is None:
-                    net.generateRRSNumber(soas[d], dev_b[d]["rnd"], N, N, 0, dp, o["stats"],
-                                          o["rrs"], o["norm"], o["split"], o["q"], cap, o["sz"],
-                                          stream)
-                else:
-                    sharded.step(soas[d], dev_b[d]["rnd"], N, N * world, 0, dp, o["stats"],
-                                 o["rrs"], o["norm"], o["split"], o["q"], cap, o["sz"], acc,
-                                 stream)
-                if post:
-                    post(d)
-            if do_train and pre:
-                pre("train")
-            for _ in range(wl["train_steps"] if do_train else 0):
-                if sharded is None:
-                    net.train(tsoa, td["target"], wl["train_batch"], loss, stream)
-                else:
-                    sharded.train_step(tsoa, td["target"], wl["train_batch"], grads_buf, loss,
-                                       stream)
-            if do_train and post:
-                post("train")
+def rel_stats(a, b, floor=None):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    d = np.abs(a - b) / (np.maximum(np.abs(b), floor) if floor else np.abs(b))
+    return {"max": float(d.max()), "mean": float(d.mean())}
 
-    def timed(fn, steps, warmup):
-        for _ in range(warmup):
-            fn()
+
+def frame_errors(torch, mixed: FrameArm, fp32: FrameArm, sample_stride: int = 509):
+    """Errors of both paths at equal parameters (the mixed network's trained state): stats and
+    factors of bounce 0 against the FP64 oracle on a strided sample and against each other on
+    every vertex; losses of one training step (gradients only) on a 16,384-sample batch; the
+    mixed path's decision against the oracle's on the same factors."""
+    import oracle as O
+    s = mixed.stream
+    p = mixed.net.get_params()
+    fp32.net.set_params(p)
+    N = mixed.N
+    d0 = mixed.dev_b[0]
+    res = {}
+    outs = {}
+    for name, arm in (("mixed", mixed), ("fp32", fp32)):
+        st = torch.empty(3 * N, device=mixed.dev)
+        rr = torch.empty(N, device=mixed.dev)
+        arm.net.inference(mixed.soas[0], N, arm.dp, st, rr, s)
         torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
+        outs[name] = (st.cpu().numpy().reshape(N, 3), rr.cpu().numpy())
+    idx = np.arange(0, N, sample_stride)
+    host = {k: t.cpu().numpy() for k, t in d0.items()}
+    sub = {k: np.ascontiguousarray(host[k][idx]) for k in FIELDS}
+    sub["depth"] = sub["depth"].view(np.uint32)
+    O.set_threads(os.cpu_count() or 1)
+    o64 = O.infer(mixed.net.config, p, sub, mixed.dp, "f64", want=("stats", "rrs"))
+    for name in ("mixed", "fp32"):
+        st, rr = outs[name]
+        res[name + "_vs_fp64_oracle"] = {
+            "stats": rel_stats(st[idx], o64["stats"], floor=1.0),
+            "factors": rel_stats(rr[idx], o64["rrs"])}
+    res["mixed_vs_fp32_path"] = {"stats": rel_stats(outs["mixed"][0], outs["fp32"][0], floor=1.0),
+                                 "factors": rel_stats(outs["mixed"][1], outs["fp32"][1])}
+    # losses of one training step at p (gradients only, no update) on a 16,384-sample batch
+    nt = 16_384
+    tv = {k: np.ascontiguousarray(t[:nt].cpu().numpy()) for k, t in mixed.td.items()}
+    tv["depth"] = tv["depth"].view(np.uint32)
+    tsoa = soa_of({k: t[:nt] for k, t in mixed.td.items()})
+    losses = {}
+    for name, arm in (("mixed", mixed), ("fp32", fp32)):
+        l = torch.zeros(2, dtype=torch.float64, device=mixed.dev)
+        arm.net.trainGrads(tsoa, mixed.td["target"][:nt], nt, l, s)
         torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(steps):
-            fn()
-        e1.record()
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
-
-    # ---- device-timed region ----
-    for _ in range(args.warmup):
-        step()
+        losses[name] = l.cpu().numpy()
+    _, l64 = O.train_grads(mixed.net.config, p, tv, tv["target"], "f64")
+    for name in ("mixed", "fp32"):
+        res[name + "_vs_fp64_oracle"]["loss"] = rel_stats(losses[name], l64)
+    res["mixed_vs_fp32_path"]["loss"] = rel_stats(losses["mixed"], losses["fp32"])
+    # decisions at equal factors: the mixed factors through the library and through the oracle
+    rr_dev = torch.from_numpy(outs["mixed"][1]).to(mixed.dev)
+    o = step_outputs(torch, mixed.dev, N, 9 * N)
+    mixed.net.decideEmit(rr_dev, d0["rnd"], N, N, 0, mixed.dp, o["norm"], o["split"], o["q"],
+                         9 * N, o["sz"], stream=s)
     torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    launches0 = net.launch_count()
-    net.profile(True)
-    net.profile_read()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local_rank) as clk:
-        e0.record()
-        for _ in range(args.steps):
-            step()
-        e1.record()
-        torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    # a graph replay does not pass through the library, which counted the graph's kernels
-    # when it captured them
-    launches = (kernels_per_graph * args.steps) if batched else net.launch_count() - launches0
-    prof = net.profile_read()
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    ms_step = ms / args.steps
-    verts = total * world
-    value = verts / (ms_step * 1e-3)
+    od = O.decide_emit(outs["mixed"][1], host["rnd"], N, 0, mixed.dp, capacity=9 * N,
+                       shift_n=mixed.net.config.max_queue)
+    tot = int(o["sz"].cpu().numpy().view(np.uint32)[0])
+    same = (tot == od["total"] and
+            np.array_equal(o["split"].cpu().numpy(), od["split"]) and
+            np.array_equal(o["q"][:tot].cpu().numpy().view(np.uint32), od["queue"]))
+    res["decisions_bit_exact_at_equal_factors"] = bool(same)
+    res["decision_vertices"] = N
+    res["sample"] = (f"stats and factors: bounce 0 of the frame, every {sample_stride}th of {N} "
+                     f"vertices against the FP64 oracle ({idx.size} vertices), all {N} between "
+                     f"the paths; loss: one step's losses on {nt} training samples; relative "
+                     f"error |a-b|/|b| (stats: log-statistics, denominator floored at 1); "
+                     f"parameters: the mixed network after the timed frames, set on both paths")
+    return res
 
-    extra = {}
-    inf_vertices = total * args.steps
-    if batched:
-        # per-depth launches (profiled: the graph's kernels carry no per-kernel events)
-        ms_pd = timed(step_per_depth, args.steps, 2) / args.steps
-        prof = net.profile_read()
-        n_inf_pd = prof.get("infer_tc", prof.get("infer_fp32", (0, 0.0)))[0]
-        inf_vertices = total * (n_inf_pd // B)
-        same = True
+
+def run_frame_pair(args, torch, dev, stream, timer, name, steps, warmup, fp32_steps, rank, world,
+                   headline):
+    """The mixed arm and the plain FP32 per-depth arm of one frame workload on the same inputs."""
+    wl = WORKLOADS[name]
+    train = do_train_of(args, wl)
+    host_b, dev_b, th, td = frame_inputs(torch, dev, wl, 1000, rank, train)
+    prec = args.precision if headline and args.precision else wl["precision"]
+    mixed = FrameArm(torch, dev, stream, wl, prec, dev_b, td, train, world,
+                     launch_shape=args.launch_shape, sharded=world > 1)
+    out = {"name": name, "wl": wl, "train": train, "precision": prec, "arm": mixed,
+           "host_b": host_b, "dev_b": dev_b, "th": th, "td": td}
+    clk = ClockSampler(env_int("LOCAL_RANK", 0)) if headline else None
+    ms, prof, launches = mixed.measure(timer, steps, warmup, clk)
+    out.update(ms=ms, prof=prof, launches=launches, clocks=clk.summary() if clk else None)
+    out["value"] = wl["bounces"] * wl["n_vert"] * world / (ms * 1e-3)
+    out["train_rate"] = train_rate(prof, wl, steps) if train else None
+    out["status"] = mixed.net.device_status(stream)
+    if world == 1 and fp32_steps > 0 and prec != "fp32":
+        fp = FrameArm(torch, dev, stream, wl, "fp32", dev_b, td, train, 1,
+                      tune=True)
+        clk32 = ClockSampler(env_int("LOCAL_RANK", 0)) if headline else None
+        ms32, prof32, _ = fp.measure(timer, fp32_steps, 1, clk32)
+        out["fp32"] = {"value": wl["bounces"] * wl["n_vert"] / (ms32 * 1e-3), "ms_per_step": ms32,
+                       "train_samples_per_s": train_rate(prof32, wl, fp32_steps) if train else None,
+                       "steps": fp32_steps, "warmup": 1,
+                       "clocks": clk32.summary() if clk32 else None,
+                       "kernels": {k: {"launches": n, "ms_total": t} for k, (n, t) in prof32.items()}}
+        if headline and args.errors:
+            out["errors"] = frame_errors(torch, mixed, fp)
+        fp.close()
+    return out
+
+
+def run_batched(args, torch, dev, stream, timer, steps, warmup, rank):
+    """Config 3: the mixed path's batched step as one CUDA-graph launch against the plain FP32
+    path launched depth by depth, on the same vertices."""
+    wl = WORKLOADS["batched"]
+    B, N = wl["bounces"], wl["n_vert"]
+    cat, counts = batched_vertices(N, B, 2024 + rank)
+    db = {k: t.to(dev) for k, t in pinned(torch, cat, FIELDS).items()}
+    total = int(sum(counts))
+    dp = nb.default_decide()
+    net = nb.NRRSNetwork(make_config(wl["precision"], wl, total, wl["train_batch"]))
+    tune = json.loads(net.autotune(N))
+    caps = [9 * c for c in counts]
+    offs = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    qoffs = np.concatenate([[0], np.cumsum(caps)]).astype(np.int64)
+    segs = [nb.Segment(int(offs[k]), counts[k], N, 0, int(qoffs[k]), caps[k]) for k in range(B)]
+    ob = step_outputs(torch, dev, total, int(qoffs[-1]), B)
+    l0 = net.launch_count()
+    graph = net.captureBatched(soa_of(db), db["rnd"], segs, dp, ob["stats"], ob["rrs"], ob["norm"],
+                               ob["split"], ob["q"], ob["sz"])
+    kernels_per_graph = net.launch_count() - l0
+    ms_graph = timer(lambda: graph.launch(stream), steps, warmup)
+    per = []
+    for k in range(B):
+        sub = {f: t[int(offs[k]):int(offs[k + 1])] for f, t in db.items()}
+        per.append((sub, soa_of(sub), step_outputs(torch, dev, counts[k], caps[k])))
+
+    def per_depth(n_):
         for k, (sub, s, p) in enumerate(per):
-            a0, a1 = int(offs[k]), int(offs[k + 1])
-            same &= bool(torch.equal(p["split"], ob["split"][a0:a1]))
-            same &= bool(torch.equal(p["rrs"], ob["rrs"][a0:a1]))
-            # batched queues hold indices into the concatenated SoA
-            same &= bool(torch.equal(p["q"][:int(p["sz"].item())] + int(offs[k]),
-                                     ob["q"][int(qoffs[k]):int(qoffs[k]) + int(ob["sz"][k].item())]))
-        extra = {"batched": {"graph_ms_per_step": ms_step, "per_depth_ms_per_step": ms_pd,
-                             "speedup_graph_vs_per_depth": ms_pd / ms_step,
-                             "decisions_equal_per_depth": same, "kernels_per_graph": kernels_per_graph,
-                             "vertices_per_depth": counts}}
-    net.profile(False)
-    rc, flags = net.device_status(stream)
+            n_.generateRRSNumber(s, sub["rnd"], counts[k], N, 0, dp, p["stats"], p["rrs"],
+                                 p["norm"], p["split"], p["q"], caps[k], p["sz"], stream)
 
-    # ---- end to end through the C-ABI with host buffers ----
-    # the training batch is copied once per step and reused by each of its train steps
+    ms_mixed_pd = timer(lambda: per_depth(net), steps, 2)
+    same = True
+    for k, (sub, s, p) in enumerate(per):
+        a0, a1 = int(offs[k]), int(offs[k + 1])
+        same &= bool(torch.equal(p["split"], ob["split"][a0:a1]))
+        same &= bool(torch.equal(p["rrs"], ob["rrs"][a0:a1]))
+        same &= bool(torch.equal(p["q"][:int(p["sz"].item())] + int(offs[k]),
+                                 ob["q"][int(qoffs[k]):int(qoffs[k]) + int(ob["sz"][k].item())]))
+    fp = nb.NRRSNetwork(make_config("fp32", wl, N, wl["train_batch"]))
+    fp.autotune(N)
+    ms_fp32_pd = timer(lambda: per_depth(fp), max(3, steps // 5), 1)
+    graph.close()
+    net.close()
+    fp.close()
+    return {"workload": workload_name("batched", wl, False, wl["precision"]),
+            "vertices_per_step": total, "vertices_per_depth": counts,
+            "mixed_graph": {"value": total / (ms_graph * 1e-3), "ms_per_step": ms_graph,
+                            "kernels_per_graph": kernels_per_graph, "launches_per_step": 1},
+            "mixed_per_depth": {"value": total / (ms_mixed_pd * 1e-3), "ms_per_step": ms_mixed_pd},
+            "fp32_per_depth": {"value": total / (ms_fp32_pd * 1e-3), "ms_per_step": ms_fp32_pd},
+            "mixed_graph_vs_fp32_per_depth": ms_fp32_pd / ms_graph,
+            "graph_decisions_equal_per_depth": same,
+            "autotune_best": tune.get("best") or tune.get("cached")}
+
+
+def e2e_of(torch, dev, timer, arm: FrameArm, host_b, th, steps, warmup):
+    """The headline metric end to end through the C-ABI with host-resident inputs."""
+    B, wl, train = arm.B, arm.wl, arm.train
+    dev_b, td = arm.dev_b, arm.td
+    total = B * arm.N
     h2d = total * (SOA_BYTES + RND_BYTES) + (
-        wl["train_batch"] * (SOA_BYTES + RND_BYTES + TARGET_BYTES) if do_train else 0)
-    d2h = B * 4 + (16 if do_train else 0)
+        wl["train_batch"] * (SOA_BYTES + RND_BYTES + TARGET_BYTES) if train else 0)
+    d2h = B * 4 + (16 if train else 0)
     sizes_h = torch.zeros(B, dtype=torch.int32).pin_memory()
     loss_h = torch.zeros(2, dtype=torch.float64).pin_memory()
-
-    # A caller with host-resident inputs overlaps the upload of the next bounce with the
-    # compute of the current one: copies run on their own stream, each bounce waits for its
-    # inputs, and a buffer is refilled only after the previous step's compute has used it.
+    # A caller with host-resident inputs overlaps the upload of the next bounce with the compute
+    # of the current one: copies run on their own stream, each bounce waits for its inputs, and a
+    # buffer is refilled only after the previous step's compute has used it.
     cur = torch.cuda.current_stream()
     copy_stream = torch.cuda.Stream(device=dev)
-    keys = list(range(len(dev_b))) + (["train"] if do_train else [])
+    keys = list(range(B)) + (["train"] if train else [])
     ev_copied = {k: torch.cuda.Event() for k in keys}
     ev_used = {k: torch.cuda.Event() for k in keys}
     for k in keys:
@@ -515,138 +753,139 @@ def run_ours(args, rank, world, local_rank):
                 for k in FIELDS:
                     db[k].copy_(hb[k], non_blocking=True)
                 ev_copied[d].record(copy_stream)
-            if do_train:
+            if train:
                 copy_stream.wait_event(ev_used["train"])
                 for k in FIELDS + ("target",):
                     td[k].copy_(th[k], non_blocking=True)
                 ev_copied["train"].record(copy_stream)
-        step(pre=lambda k: cur.wait_event(ev_copied[k]), post=lambda k: ev_used[k].record(cur))
-        if batched:
-            sizes_h.copy_(ob["sz"], non_blocking=True)
-        else:
-            for d in range(B):
-                sizes_h[d:d + 1].copy_(outs[d]["sz"], non_blocking=True)
-        if do_train:
-            loss_h.copy_(loss, non_blocking=True)
+        arm.step(pre=lambda k: cur.wait_event(ev_copied[k]), post=lambda k: ev_used[k].record(cur))
+        for d in range(B):
+            sizes_h[d:d + 1].copy_(arm.outs[d]["sz"], non_blocking=True)
+        if train:
+            loss_h.copy_(arm.loss, non_blocking=True)
 
-    e2 = max(2, args.steps // 2)
-    for _ in range(min(2, args.warmup)):
+    for _ in range(warmup):
         step_e2e()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
+    timer.sync()
     a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a0.record(cur)
     copy_stream.wait_event(a0)      # no upload starts before the timed region does
-    for _ in range(e2):
+    for _ in range(steps):
         step_e2e()
     a1.record(cur)                  # after the last compute, which waited for every upload
     torch.cuda.synchronize()
-    e2e_ms = a0.elapsed_time(a1) / e2
-    if dist:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    ms = a0.elapsed_time(a1) / steps
+    if timer.dist:
+        t = torch.tensor([ms], device=dev)
+        timer.dist.all_reduce(t, op=timer.dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return {"value": total * arm.world / (ms * 1e-3), "unit": "vertices/s", "ms_per_step": ms,
+            "h2d_gbs": h2d / (ms * 1e-3) / 1e9,
+            "overlap": "uploads on a copy stream, bounce d+1 during the compute of bounce d",
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": steps}
 
-    # ---- roofline of the dominant inference kernel ----
-    # Algorithmic bytes per vertex of each inference kernel (every hash-corner gather counted at
-    # table precision); the MLP kernels of the split modes are tensor-pipe work and get a
-    # second, FLOP-based line.
-    feat_bytes = 4 if args.precision == "fp32" else 2
-    gathered = 16 * 8 * 2 * feat_bytes
-    attrs = 12 * 5 + 4 * 3                       # wi, normal, albedo, thp, pos; rough, ref, depth
-    mode = net.infer_split() if args.precision != "fp32" else 0
-    w_, h_ = wl["width"], wl["hidden"]
-    flop_stat = 2 * (64 * w_ + (h_ - 1) * w_ * w_ + w_ * 3)
-    flop_rrs = 2 * (16 * w_ + (h_ - 1) * w_ * w_ + w_)
-    b_of = {"infer_fp32": SOA_BYTES + gathered + 16,
-            "encode": 4 * 12 + gathered + 64,
-            "infer_tc": (SOA_BYTES + gathered + 16 if mode == 0 else
-                         (64 + attrs - 12 + 16 if mode == 1 else 64 + attrs - 12 + 12 + 32)),
-            "infer_rrs": 32 + 4}
-    peak, peak_kind = measured_peaks()
-    roof, mlp_roof = None, None
-    cands = {k: prof[k] for k in b_of if k in prof and prof[k][0]}
-    if cands:
-        kind = max(cands, key=lambda k: cands[k][1])
-        n_l, ms_l = cands[kind]
-        launch_ms = ms_l / n_l
-        per_launch = inf_vertices / n_l   # training encodes have their own kind
-        b_vertex = b_of[kind]
-        achieved = b_vertex * per_launch / (launch_ms * 1e-3) / 1e9
-        tpv = traffic_per_vertex(kind) if args.workload == "frame1080p" and mode == 0 else None
-        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": (tpv * per_launch) if tpv else None, "kernel": kind,
-                "algorithmic_bytes_per_vertex": b_vertex, "vertices_per_launch": per_launch,
-                "launch_ms": launch_ms, "inference_mode": mode,
-                "note": "algorithmic bytes count the 128 hash-corner gathers at table precision; "
-                        "these random 4-byte gathers are bound by L1-to-L2 sector requests, not by "
-                        "HBM bandwidth (see profiles/)"}
-    mlp_kinds = [k for k in ("infer_tc", "infer_rrs") if k in prof and prof[k][0]]
-    if args.precision != "fp32" and mlp_kinds:
-        ms_mlp = sum(prof[k][1] for k in mlp_kinds)
-        n_launch = prof["infer_tc"][0]
-        tflops = (flop_stat + flop_rrs) * inf_vertices / (ms_mlp * 1e-3) / 1e12
-        pk = json.loads((REPO / "MEASURED_PEAKS.json").read_text()).get("bf16_tflops", 1590.0) \
-            if (REPO / "MEASURED_PEAKS.json").exists() else 1590.0
-        mlp_roof = {"bound": "tensor", "kernels": mlp_kinds, "achieved": tflops, "peak": pk,
-                    "unit": "TFLOP/s", "frac": tflops / pk, "flop_per_vertex": flop_stat + flop_rrs,
-                    "ms_per_launch": ms_mlp / n_launch,
-                    "note": "StatNet + RRSNet MLP FLOPs (true layer sizes) over the time of the "
-                            "kernels that run them; in the fused mode that kernel also gathers"}
-    kernels = {k: {"launches": n, "ms_total": t, "ms_per_launch": t / n} for k, (n, t) in prof.items()}
 
+def pair_summary(p):
+    s = {"workload": workload_name(p["name"], p["wl"], p["train"], p["precision"]),
+         "mixed": {"value": p["value"], "ms_per_step": p["ms"],
+                   "train_samples_per_s": p["train_rate"]}}
+    if "fp32" in p:
+        f = p["fp32"]
+        s["fp32_per_depth"] = {k: f[k] for k in ("value", "ms_per_step", "train_samples_per_s",
+                                                 "steps")}
+        s["mixed_vs_fp32"] = {"vertices_per_s": p["value"] / f["value"],
+                              "train_samples_per_s": (p["train_rate"] / f["train_samples_per_s"]
+                                                      if p["train_rate"] and f["train_samples_per_s"]
+                                                      else None)}
+    return s
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    load_product()
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.current_stream().cuda_stream
+    timer = Timer(torch, dist, dev)
+    name = args.workload
+    if name == "batched":
+        b = run_batched(args, torch, dev, stream, timer, args.steps, args.warmup, rank)
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": b["mixed_graph"]["value"],
+                              "unit": "vertices/s", "n_gpus": world, "steps": args.steps,
+                              "warmup": args.warmup, "ms_per_step": b["mixed_graph"]["ms_per_step"],
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                              "dtype": "f16", "data": "synthetic", "batched": b}), flush=True)
+        return 0
+
+    # ---- headline: the frame workload, mixed and plain FP32 on the same inputs ----
+    wl = WORKLOADS[name]
+    fp32_steps = 0 if args.only else max(2, min(args.steps, 3))
+    p = run_frame_pair(args, torch, dev, stream, timer, name, args.steps, args.warmup,
+                       fp32_steps, rank, world, headline=True)
+    arm = p["arm"]
+    prof = p["prof"]
+    mode = arm.net.infer_split() if p["precision"] != "fp32" else 0
+    inf_vertices = wl["bounces"] * wl["n_vert"] * args.steps
+    roof, mlp_roof = roofline_of(prof, p["precision"], mode, wl, inf_vertices, name)
+    e2e = e2e_of(torch, dev, timer, arm, p["host_b"], p["th"], max(2, min(args.steps, 10)),
+                 min(2, args.warmup))
     line = {
-        "metric": METRIC, "value": value, "unit": "vertices/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "metric": METRIC, "value": p["value"], "unit": "vertices/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": p["ms"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": {"fp16": "f16", "bf16": "bf16", "fp32": "f32"}[args.precision],
-        "data": "synthetic",
-        "config": {"workload": workload_name(args), "bounces": B, "vertices_per_bounce": N,
-                   "vertices_per_step": total,
-                   "train_steps": wl["train_steps"] if do_train else 0,
-                   "train_batch": wl["train_batch"] if do_train else 0,
-                   "encoding": f"hashgrid L16 F2 T2^{wl['log2_table']} Nmin16 b1.5 + SH deg4",
-                   "mlp": f"StatNet 64->{wl['width']}x{wl['hidden']}->3, "
-                          f"RRSNet 16->{wl['width']}x{wl['hidden']}->1",
-                   "l2": "inputs larger than L2 (one vertex buffer per bounce, >=158 MB)"
-                         if not batched else "inputs larger than L2 (one 450 MB SoA of all depths)",
-                   "launch_shape": list(net.launch_shape()) + (
-                       [net.infer_split()] if args.precision != "fp32" else []),
-                   "parallelism": f"dp{world}"},
-        "clocks": clk.summary(),
-        "e2e": {"value": verts / (e2e_ms * 1e-3), "unit": "vertices/s", "ms_per_step": e2e_ms,
-                "h2d_gbs": h2d / (e2e_ms * 1e-3) / 1e9,
-                "overlap": "uploads on a copy stream, bounce d+1 during the compute of bounce d",
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": launches,
+        "dtype": {"fp16": "f16", "bf16": "bf16", "fp32": "f32"}[p["precision"]],
+        "data": "synthetic (seeded; the distributions of the workload definition)",
+        "config": frame_config(name, wl, p["train"], p["precision"], world),
+        "clocks": p["clocks"],
+        "e2e": e2e,
+        "gpu_launches": p["launches"],
         "roofline": roof,
         "mlp_roofline": mlp_roof,
-        "kernels": kernels,
-        "device_status": [rc, flags],
-        "infer_grid": net.last_infer_grid(),
+        "train_samples_per_s": p["train_rate"],
     }
-    if tune:
-        line["autotune"] = {"best": tune.get("best") or tune.get("cached"),
-                            "trials": tune.get("trials")}
-    line.update(extra)
-    if do_train and "train_statnet" in prof:
-        t_train = sum(t for k, (n, t) in prof.items() if k.startswith("train") or k == "adam"
-                      or k in ("pack_weights", "table_half"))
-        line["train_samples_per_s"] = (wl["train_steps"] * wl["train_batch"] * args.steps
-                                       / (t_train * 1e-3))
+    if "fp32" in p:
+        f = p["fp32"]
+        line["fp32_per_depth"] = f
+        line["mixed_vs_fp32"] = pair_summary(p)["mixed_vs_fp32"]
+        if "errors" in p:
+            line["errors"] = p["errors"]
+    line["kernels"] = {k: {"launches": n, "ms_total": t, "ms_per_launch": t / n}
+                       for k, (n, t) in prof.items()}
+    line["launch_shape"] = list(arm.net.launch_shape()) + (
+        [arm.net.infer_split()] if p["precision"] != "fp32" else [])
+    if arm.tune:
+        line["autotune"] = {"best": arm.tune.get("best") or arm.tune.get("cached"),
+                            "trials": arm.tune.get("trials")}
+    line["device_status"] = list(p["status"])
+    arm.close()
+    del p, arm
+    torch.cuda.empty_cache()
+
+    # ---- the other configurations of the workload definition, beside the headline ----
+    if world == 1 and not args.only:
+        sec = {}
+        if name != "frame1080p":
+            q = run_frame_pair(args, torch, dev, stream, timer, "frame1080p", 20, 3, 5, rank, 1,
+                               headline=False)
+            sec["frame1080p"] = pair_summary(q)
+            q["arm"].close()
+            del q
+            torch.cuda.empty_cache()
+        sec["batched"] = run_batched(args, torch, dev, stream, timer, 20, 3, rank)
+        line["secondary"] = sec
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        value_c, cores, sample, _ = cpu_sample(make_config("fp32", wl, 1 << 21, 1 << 16), wl,
-                                               131072, 12.0, 8192, do_train)
-        line["cpu_baseline"] = {"value": value_c, "unit": "vertices/s", "cores": cores,
-                                "kind": "port", "sample": sample}
+        cpu = CpuFrameSample(wl, do_train_of(args, wl))
+        v_c, _, k = cpu.run(0, 1, seconds=12.0)
+        line["cpu_baseline"] = {"value": v_c, "unit": "vertices/s", "cores": cpu.cores,
+                                "kind": "port", "sample": f"{k} steps; " + cpu.describe()}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if graph is not None:
-        graph.close()
-    net.close()
     if dist:
         dist.destroy_process_group()
     return 0
@@ -985,7 +1224,7 @@ def run_records(args, rank, world, local_rank):
              "radiance_pass": (t_prop, b_prop, 1), "batch": (t_gen, b_gen, 1),
              "sample_weights": (t_wgt, b_wgt, 1),
              "pixel_error": (t_pe, b_pe, len(bounces) + 4)}
-    peak, peak_kind = measured_peaks()
+    peak, _, peak_kind = measured_peaks()
     dom = max(calls, key=lambda k: calls[k][0])
     t_dom, b_dom, n_dom = calls[dom]
     achieved = b_dom / (t_dom * 1e-3) / 1e9
@@ -1293,13 +1532,18 @@ def run_render(args, rank, world, local_rank):
     return 0
 
 
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--workload", choices=tuple(WORKLOADS), default="frame1080p")
+    ap.add_argument("--workload", choices=tuple(WORKLOADS), default="frame4k")
+    ap.add_argument("--only", action="store_true",
+                    help="the workload's own arm only (no FP32 arm, no secondary configurations)")
+    ap.add_argument("--no-errors", dest="errors", action="store_false",
+                    help="skip the error measurement against the FP64 oracle")
     ap.add_argument("--precision", choices=("fp16", "bf16", "fp32"), default=None)
     ap.add_argument("--no-train", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -1317,21 +1561,19 @@ def main():
         args.precision = wl["precision"]
     if args.bounces:
         wl["bounces"] = args.bounces
-    if args.vertices and args.workload not in ("records1080p", "render1080p", "render_train1080p"):
+    if args.vertices:
         wl["n_vert"] = args.vertices
     rank, world = env_int("RANK", 0), env_int("WORLD_SIZE", 1)
     local_rank = env_int("LOCAL_RANK", 0)
     if args.workload in ("render1080p", "render_train1080p"):
-        if args.vertices:
-            wl["n_vert"] = args.vertices
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference traces with "
                               "OptiX inside its KiRaRay integrator, which cannot be built here"}))
             return 0
+        load_product()
         return run_render(args, rank, world, local_rank)
     if args.workload == "records1080p":
-        if args.vertices:
-            wl["n_vert"] = args.vertices
+        load_product()   # the synthetic path records come from the library's generator
         if args.impl == "reference":
             return run_records_reference(args, rank, world)
         return run_records(args, rank, world, local_rank)

@@ -287,11 +287,14 @@ def decide_emit_acc(rrs, rnd, budget, n_specular, dp, acc: int, shift: int, capa
             "split": split[:n], "flags": int(flags.value)}
 
 
-def train_grads(cfg, params, v: dict, target, precision: str = "f64"):
+def train_grads(cfg, params, v: dict, target, precision: str = "f64", out=None):
+    """(gradients, losses); out, when given, is a reused gradient array of the right size and
+    precision (the oracle clears it itself)."""
     n = v["pos"].shape[0]
     npar = param_count(cfg)[0]
     dt = np.float64 if precision == "f64" else np.float32
-    g = np.zeros(npar, dt)
+    g = out if out is not None else np.empty(npar, dt)
+    assert g.dtype == dt and g.size == npar
     loss = np.zeros(2, np.float64)
     f = lib().oracle_train_grads_f64 if precision == "f64" else lib().oracle_train_grads_f32
     params = np.ascontiguousarray(params, np.float32)
