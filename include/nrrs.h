@@ -222,6 +222,37 @@ int nrrs_step_batched(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* rnd,
                       float* stats, float* rrs, float* rrs_norm, uint8_t* split,
                       uint32_t* next_queue, uint32_t* next_size_dev, void* stream);
 
+/* ---- device-resident queue sizes. The reference's inference queue size lives on the device:
+ *      the closest-hit program pushes vertices with an atomic and the integrator reads the size
+ *      back before each depth (integrator.cpp:1073-1085, 1533-1555). These forms take the size
+ *      as a device word (*n_dev) and a host bound max_n, which sizes every grid and capacity,
+ *      so a depth loop needs no host read between the trace and the step and can be captured
+ *      whole in a CUDA graph. The kernels read the count on the device; a count above max_n is
+ *      clamped to max_n and flags NRRS_DEV_OVERFLOW. Results equal the host-size forms on the
+ *      same count, bit for bit. All other arguments are those of the host-size forms. ---- */
+int nrrs_infer_dev(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const uint32_t* n_dev,
+                   uint32_t max_n, const nrrs_decide_params* p, float* stats, float* rrs,
+                   void* stream);
+int nrrs_decide_emit_dev(nrrs_ctx* ctx, const float* rrs, const float* rnd,
+                         const uint32_t* scatter_index, const uint32_t* n_dev, uint32_t max_n,
+                         uint32_t budget, uint32_t n_specular, const uint32_t* n_specular_dev,
+                         const nrrs_decide_params* p, float* rrs_norm, uint8_t* split,
+                         uint32_t* next_queue, uint32_t capacity, uint32_t* next_size_dev,
+                         void* stream);
+/* generateRRSNumber<false,*> (integrator.cpp:1057-1483) on a device-sized queue */
+int nrrs_step_dev(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* rnd,
+                  const uint32_t* n_dev, uint32_t max_n, uint32_t budget, uint32_t n_specular,
+                  const uint32_t* n_specular_dev, const nrrs_decide_params* p, float* stats,
+                  float* rrs, float* rrs_norm, uint8_t* split, uint32_t* next_queue,
+                  uint32_t capacity, uint32_t* next_size_dev, void* stream);
+/* batched depths with device-resident counts: segs[k].count is the largest count of depth k
+ * (its SoA range and queue capacity are sized for it), counts_dev[k] the actual count */
+int nrrs_step_batched_dev(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* rnd,
+                          const nrrs_segment* segs, const uint32_t* counts_dev, int32_t n_segs,
+                          const nrrs_decide_params* p, float* stats, float* rrs, float* rrs_norm,
+                          uint8_t* split, uint32_t* next_queue, uint32_t* next_size_dev,
+                          void* stream);
+
 /* ---- sharded inference and decision across GPUs (no counterpart in the single-GPU
  *      reference; the reference's sum is calcSum2PassAsync, commoncudautilshost.cpp:6-22).
  *      The normalisation sum is an exact 64-bit fixed-point integer, so shards add it with an

@@ -50,6 +50,9 @@ struct nrrs_ctx {
     nrrs::DecideScratch* scr = nullptr;
     unsigned long long* states = nullptr;
     uint32_t max_chunks = 0;
+    // segment tables resolved on the device from device-resident queue sizes: [0] in inference
+    // tiles, [1] in decision chunks (the *_dev entry points)
+    nrrs::SegmentTable* segs_dev = nullptr;
 
     // training scratch
     void* train_scratch = nullptr;

@@ -66,10 +66,11 @@ __global__ void __launch_bounds__(kDecThreads) k_decide(const __grid_constant__ 
     const unsigned c = s_chunk;
     const unsigned epoch = s_epoch;
     unsigned flags = 0;
+    const SegmentTable& S = seg_table(a.segs);
 
-    if (c < a.segs.total_tiles) {
-        const int si = find_segment(a.segs, c);
-        const Segment& sg = a.segs.s[si];
+    if (c < S.total_tiles) {
+        const int si = find_segment(S, c);
+        const Segment& sg = S.s[si];
         const unsigned lc = c - sg.tile_start;
         const unsigned base = sg.offset + lc * kDecChunk;
         const unsigned end = sg.offset + min(sg.count, (lc + 1) * kDecChunk);
@@ -256,8 +257,8 @@ __global__ void __launch_bounds__(kDecThreads) k_decide(const __grid_constant__ 
         __threadfence();
         const unsigned old = atomicAdd(&a.scr->done, 1u);
         if (old == gridDim.x - 1) {
-            for (int k = 0; k < a.segs.n; ++k) {
-                if (a.segs.s[k].count == 0) a.next_size[k] = 0;
+            for (int k = 0; k < S.n; ++k) {
+                if (S.s[k].count == 0) a.next_size[k] = 0;
                 a.scr->sum_acc[k] = 0ull;
             }
             a.scr->ticket = 0;
@@ -271,9 +272,10 @@ __global__ void __launch_bounds__(kDecThreads) k_decide(const __grid_constant__ 
 __global__ void __launch_bounds__(kTile) k_sum(const __grid_constant__ SumArgs a) {
     __shared__ long long s_part[kTile / 32];
     unsigned flags = 0;
-    for (unsigned t = blockIdx.x; t < a.segs.total_tiles; t += gridDim.x) {
-        const int si = find_segment(a.segs, t);
-        const Segment& sg = a.segs.s[si];
+    const SegmentTable& S = seg_table(a.segs);
+    for (unsigned t = blockIdx.x; t < S.total_tiles; t += gridDim.x) {
+        const int si = find_segment(S, t);
+        const Segment& sg = S.s[si];
         const unsigned v = sg.offset + (t - sg.tile_start) * kTile + threadIdx.x;
         long long term = 0;
         if (v < sg.offset + sg.count) term = fixed_term(a.fp, a.rrs[v], &a.scr->status);
@@ -291,7 +293,42 @@ __global__ void __launch_bounds__(kTile) k_sum(const __grid_constant__ SumArgs a
     (void)flags;
 }
 
+// Builds, on the device, the segment tables of the actual queue sizes: count k is
+// min(counts[k], the largest count the host sized the launch for; more flags NRRS_DEV_OVERFLOW),
+// and the tile starts are the prefix sums in units of kTile (inference, sum, encoding) and of
+// kDecChunk (decision). One thread: at most 16 segments.
+__global__ void k_resolve_segments(const __grid_constant__ SegmentTable host, const uint32_t* counts,
+                                   SegmentTable* tiles, SegmentTable* chunks, unsigned* status) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    uint32_t t_tiles = 0, t_chunks = 0;
+    unsigned flags = 0;
+    for (int k = 0; k < host.n; ++k) {
+        Segment sg = host.s[k];
+        uint32_t c = counts[k];
+        if (c > sg.count) { c = sg.count; flags |= NRRS_DEV_OVERFLOW; }
+        sg.count = c;
+        sg.tile_start = t_tiles;
+        tiles->s[k] = sg;
+        sg.tile_start = t_chunks;
+        chunks->s[k] = sg;
+        t_tiles += (c + kTile - 1) / kTile;
+        t_chunks += (c + kDecChunk - 1) / kDecChunk;
+    }
+    tiles->n = chunks->n = host.n;
+    tiles->total_tiles = t_tiles;
+    chunks->total_tiles = t_chunks;
+    tiles->resolved = chunks->resolved = nullptr;
+    if (flags) atomicOr(status, flags);
+}
+
 }  // namespace
+
+cudaError_t launch_resolve_segments(const SegmentTable& host_max, const uint32_t* counts_dev,
+                                    SegmentTable* tiles_dev, SegmentTable* chunks_dev,
+                                    unsigned* status, cudaStream_t s) {
+    k_resolve_segments<<<1, 32, 0, s>>>(host_max, counts_dev, tiles_dev, chunks_dev, status);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_decide(const DecideArgs& a, cudaStream_t s) {
     if (a.segs.total_tiles == 0) return cudaSuccess;

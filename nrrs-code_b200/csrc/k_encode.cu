@@ -26,14 +26,18 @@ namespace {
 
 template <bool BF>
 __global__ void __launch_bounds__(kTile) k_encode_levels(const __grid_constant__ EncodeLvArgs a) {
+    // work items are (level group, tile) over the tiles the host sized the launch for; with
+    // device-resident sizes the tiles past the actual total are skipped
     const uint32_t tiles = a.segs.total_tiles;
     const uint32_t items = 4u * tiles;
+    const SegmentTable& S = seg_table(a.segs);
     const __half2* table = reinterpret_cast<const __half2*>(a.table_h);
     const int m = threadIdx.x;
     for (uint32_t w = blockIdx.x; w < items; w += gridDim.x) {
         const uint32_t q = w / tiles, t = w - q * tiles;
-        const int si = find_segment(a.segs, t);
-        const Segment& sg = a.segs.s[si];
+        if (t >= S.total_tiles) continue;
+        const int si = find_segment(S, t);
+        const Segment& sg = S.s[si];
         const uint32_t i = sg.offset + (t - sg.tile_start) * kTile + m;
         uint4 v = make_uint4(0u, 0u, 0u, 0u);
         if (i < sg.offset + sg.count) {

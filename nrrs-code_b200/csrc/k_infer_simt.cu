@@ -123,9 +123,10 @@ __global__ void __launch_bounds__(kTile) k_infer_fp32(const __grid_constant__ In
         wrt = smem + NS;
         xs = smem + NS + NR;
     }
-    for (uint32_t t = blockIdx.x; t < a.segs.total_tiles; t += gridDim.x) {
-        const int si = find_segment(a.segs, t);
-        const Segment& sg = a.segs.s[si];
+    const SegmentTable& S = seg_table(a.segs);
+    for (uint32_t t = blockIdx.x; t < S.total_tiles; t += gridDim.x) {
+        const int si = find_segment(S, t);
+        const Segment& sg = S.s[si];
         const uint32_t i = sg.offset + (t - sg.tile_start) * kTile + tid;
         const bool valid = i < sg.offset + sg.count;
         long long term = 0;

@@ -243,11 +243,13 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
         }
         h_pending = true;
     };
-    if (PRE && kStat && !S::kShare && t0 < a.segs.total_tiles && !flags) fetch_features(t0);
+    const SegmentTable& ST = seg_table(a.segs);
+    const uint32_t total_tiles = ST.total_tiles;
+    if (PRE && kStat && !S::kShare && t0 < total_tiles && !flags) fetch_features(t0);
 
-    for (uint32_t t = t0; t < a.segs.total_tiles && !flags; t += tstride) {
-        const int si = find_segment(a.segs, t);
-        const Segment& sg = a.segs.s[si];
+    for (uint32_t t = t0; t < total_tiles && !flags; t += tstride) {
+        const int si = find_segment(ST, t);
+        const Segment& sg = ST.s[si];
         const uint32_t i = sg.offset + (t - sg.tile_start) * kTile + ltid;
         const bool valid = i < sg.offset + sg.count;
         // the glue's and the factor's inputs, in flight during the StatNet chain
@@ -281,7 +283,7 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
             if constexpr (PRE) {
                 ok &= tc_layer0_pre<WS, BF>(sH, sS, wS0, tmem, mbar, phase, ltid);
                 // the first layer has read the block: bring in the next tile's features
-                if (!S::kShare && ok && t + tstride < a.segs.total_tiles) fetch_features(t + tstride);
+                if (!S::kShare && ok && t + tstride < total_tiles) fetch_features(t + tstride);
             } else {
                 ok &= tc_layer<kStatIn, WS, BF>(sA, wS0, tmem, mbar, phase, ltid);
             }

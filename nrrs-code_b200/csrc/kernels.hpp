@@ -92,6 +92,12 @@ extern thread_local int g_last_grid;
 
 // decision + emission (single pass, decoupled look-back)
 cudaError_t launch_decide(const DecideArgs& a, cudaStream_t s);
+// device-side segment tables of device-resident queue sizes (counts_dev[host_max.n]), in units
+// of kTile (tiles_dev) and kDecChunk (chunks_dev); counts above the host maxima are clamped and
+// flag NRRS_DEV_OVERFLOW in *status
+cudaError_t launch_resolve_segments(const SegmentTable& host_max, const uint32_t* counts_dev,
+                                    SegmentTable* tiles_dev, SegmentTable* chunks_dev,
+                                    unsigned* status, cudaStream_t s);
 // exact sum of rrs (or ceil) per segment into scr->sum_acc
 cudaError_t launch_sum(const SumArgs& a, cudaStream_t s);
 // FP32 SIMT inference

@@ -164,12 +164,14 @@ int refresh_derived(nrrs_ctx* ctx, cudaStream_t s, bool table = true) {
 
 int run_infer(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const SegmentTable& segs,
               const nrrs_decide_params* p, uint64_t n_total, float* stats, float* rrs,
-              bool accumulate, cudaStream_t s, unsigned long long* ext_acc = nullptr) {
+              bool accumulate, cudaStream_t s, unsigned long long* ext_acc = nullptr,
+              const SegmentTable* resolved = nullptr) {
     InferArgs a{};
     a.v = vptrs(v);
     a.enc = ctx->enc;
     a.fp = factor_params(ctx, p);
     a.segs = segs;
+    a.segs.resolved = resolved;
     a.table = ctx->params;
     a.table_h = ctx->table_h;
     a.wt_stat = ctx->wt;
@@ -193,6 +195,7 @@ int run_infer(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const SegmentTable& segs,
         EncodeLvArgs ea{};
         ea.enc = ctx->enc;
         ea.segs = segs;
+        ea.segs.resolved = resolved;
         ea.pos = a.v.pos;
         ea.table_h = ctx->table_h;
         ea.out = ctx->enc_tiles;
@@ -243,13 +246,14 @@ int run_decide(nrrs_ctx* ctx, const float* rrs, const float* rnd, const uint32_t
                const nrrs_segment* segs, int n_segs, uint64_t n_total,
                const uint32_t* n_spec_dev, const nrrs_decide_params* p, float* rrs_norm,
                uint8_t* split, uint32_t* queue, uint32_t* next_size, bool need_sum,
-               cudaStream_t s, const long long* ext_sum = nullptr) {
+               cudaStream_t s, const long long* ext_sum = nullptr, bool resolved = false) {
     const FactorParams fp = factor_params(ctx, p);
     if (need_sum) {
         SumArgs sa{};
         sa.rrs = rrs;
         sa.scr = ctx->scr;
         sa.segs = make_segments(segs, n_segs, kTile);
+        sa.segs.resolved = resolved ? &ctx->segs_dev[0] : nullptr;
         sa.fp = fp;
         cudaError_t e;
         if (sa.segs.total_tiles == 0) {
@@ -273,6 +277,7 @@ int run_decide(nrrs_ctx* ctx, const float* rrs, const float* rnd, const uint32_t
     d.scr = ctx->scr;
     d.states = ctx->states;
     d.segs = make_segments(segs, n_segs, kDecChunk);
+    d.segs.resolved = resolved ? &ctx->segs_dev[1] : nullptr;
     d.normalize_rate = p->normalize_rate;
     d.use_ceil = p->use_ceil;
     d.scale_up = p->scale_up;
@@ -295,6 +300,17 @@ int run_decide(nrrs_ctx* ctx, const float* rrs, const float* rnd, const uint32_t
         return cuda_fail(ctx, e, "decide launch");
     }
     return NRRS_OK;
+}
+
+// Device-resident queue sizes: the host segments carry the largest counts (they size every
+// grid); k_resolve_segments builds the tables of the actual counts in ctx->segs_dev, which the
+// kernels of this call read.
+int resolve_counts(nrrs_ctx* ctx, const nrrs_segment* segs_max, int n_segs,
+                   const uint32_t* counts_dev, cudaStream_t s) {
+    const SegmentTable host = make_segments(segs_max, n_segs, kTile);
+    const cudaError_t e = launch_resolve_segments(host, counts_dev, &ctx->segs_dev[0],
+                                                  &ctx->segs_dev[1], &ctx->scr->status, s);
+    return e == cudaSuccess ? NRRS_OK : cuda_fail(ctx, e, "resolve queue sizes");
 }
 
 void xavier_fill(std::vector<float>& h, uint64_t ofs, int in, int w, int hidden, int out,
@@ -462,6 +478,7 @@ int nrrs_create(const nrrs_config* cfg, nrrs_ctx** out) {
     NRRS_ALLOC(ctx->scr, scr_bytes);
     ctx->states = reinterpret_cast<unsigned long long*>(ctx->scr + 1);
     NRRS_ALLOC(ctx->loss_dev, sizeof(double) * 2);
+    NRRS_ALLOC(ctx->segs_dev, sizeof(SegmentTable) * 2);
     ctx->train_scratch_bytes = train_scratch_bytes(c, c.max_train, ctx->sm_count);
     NRRS_ALLOC(ctx->train_scratch, ctx->train_scratch_bytes);
 #undef NRRS_ALLOC
@@ -521,6 +538,7 @@ void nrrs_destroy(nrrs_ctx* ctx) {
     cudaFree(ctx->x1_tiles);
     cudaFree(ctx->scr);
     cudaFree(ctx->loss_dev);
+    cudaFree(ctx->segs_dev);
     cudaFree(ctx->train_scratch);
     delete ctx;
 }
@@ -610,6 +628,96 @@ int nrrs_step_batched(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* rnd,
     if (rc) return rc;
     return run_decide(ctx, rrs, rnd, v->scatter_index, segs, n_segs, n_max, nullptr, p, rrs_norm,
                       split, next_queue, next_size_dev, false, s);
+}
+
+int nrrs_infer_dev(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const uint32_t* n_dev,
+                   uint32_t max_n, const nrrs_decide_params* p, float* stats, float* rrs,
+                   void* stream) {
+    if (!ctx) return NRRS_ERR_INVALID_ARG;
+    int rc = check_vertices(ctx, v);
+    if (rc) return rc;
+    if ((rc = check_decide_params(ctx, p, max_n))) return rc;
+    if (!rrs || !n_dev) return fail(ctx, NRRS_ERR_INVALID_ARG, "rrs/n_dev are NULL");
+    if (max_n > ctx->cfg.max_queue) return fail(ctx, NRRS_ERR_INVALID_ARG, "max_n > max_queue");
+    if (max_n == 0) return NRRS_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    nrrs_segment sg{0, max_n, 0, 0, 0, 0};
+    if ((rc = resolve_counts(ctx, &sg, 1, n_dev, s))) return rc;
+    return run_infer(ctx, v, make_segments(&sg, 1, kTile), p, max_n, stats, rrs, false, s,
+                     nullptr, &ctx->segs_dev[0]);
+}
+
+int nrrs_decide_emit_dev(nrrs_ctx* ctx, const float* rrs, const float* rnd,
+                         const uint32_t* scatter_index, const uint32_t* n_dev, uint32_t max_n,
+                         uint32_t budget, uint32_t n_specular, const uint32_t* n_specular_dev,
+                         const nrrs_decide_params* p, float* rrs_norm, uint8_t* split,
+                         uint32_t* next_queue, uint32_t capacity, uint32_t* next_size_dev,
+                         void* stream) {
+    if (!ctx) return NRRS_ERR_INVALID_ARG;
+    int rc = check_decide_params(ctx, p, max_n);
+    if (rc) return rc;
+    if (!n_dev || (max_n && (!rrs || !rnd))) return fail(ctx, NRRS_ERR_INVALID_ARG, "n_dev/rrs/rnd are NULL");
+    if (!next_size_dev || (capacity && !next_queue))
+        return fail(ctx, NRRS_ERR_INVALID_ARG, "next_queue/next_size are NULL");
+    if (max_n > ctx->cfg.max_queue) return fail(ctx, NRRS_ERR_INVALID_ARG, "max_n > max_queue");
+    cudaStream_t s = (cudaStream_t)stream;
+    nrrs_segment sg{0, max_n, budget, n_specular, 0, capacity};
+    if (max_n && (rc = resolve_counts(ctx, &sg, 1, n_dev, s))) return rc;
+    return run_decide(ctx, rrs, rnd, scatter_index, &sg, 1, max_n, n_specular_dev, p, rrs_norm,
+                      split, next_queue, next_size_dev, true, s, nullptr, true);
+}
+
+int nrrs_step_dev(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* rnd,
+                  const uint32_t* n_dev, uint32_t max_n, uint32_t budget, uint32_t n_specular,
+                  const uint32_t* n_specular_dev, const nrrs_decide_params* p, float* stats,
+                  float* rrs, float* rrs_norm, uint8_t* split, uint32_t* next_queue,
+                  uint32_t capacity, uint32_t* next_size_dev, void* stream) {
+    if (!ctx) return NRRS_ERR_INVALID_ARG;
+    int rc = check_vertices(ctx, v);
+    if (rc) return rc;
+    if ((rc = check_decide_params(ctx, p, max_n))) return rc;
+    if (!n_dev || !rrs || (max_n && !rnd) || !next_size_dev || (capacity && !next_queue))
+        return fail(ctx, NRRS_ERR_INVALID_ARG, "n_dev/rrs/rnd/next_queue/next_size NULL");
+    if (max_n > ctx->cfg.max_queue) return fail(ctx, NRRS_ERR_INVALID_ARG, "max_n > max_queue");
+    cudaStream_t s = (cudaStream_t)stream;
+    nrrs_segment sg{0, max_n, budget, n_specular, 0, capacity};
+    if (max_n) {
+        if ((rc = resolve_counts(ctx, &sg, 1, n_dev, s))) return rc;
+        rc = run_infer(ctx, v, make_segments(&sg, 1, kTile), p, max_n, stats, rrs, true, s,
+                       nullptr, &ctx->segs_dev[0]);
+        if (rc) return rc;
+    }
+    return run_decide(ctx, rrs, rnd, v->scatter_index, &sg, 1, max_n, n_specular_dev, p,
+                      rrs_norm, split, next_queue, next_size_dev, false, s, nullptr, max_n != 0);
+}
+
+int nrrs_step_batched_dev(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* rnd,
+                          const nrrs_segment* segs, const uint32_t* counts_dev, int32_t n_segs,
+                          const nrrs_decide_params* p, float* stats, float* rrs, float* rrs_norm,
+                          uint8_t* split, uint32_t* next_queue, uint32_t* next_size_dev,
+                          void* stream) {
+    if (!ctx) return NRRS_ERR_INVALID_ARG;
+    if (!segs || !counts_dev || n_segs < 1 || n_segs > kMaxSegments)
+        return fail(ctx, NRRS_ERR_INVALID_ARG, "1..16 segments and their device counts required");
+    int rc = check_vertices(ctx, v);
+    if (rc) return rc;
+    uint64_t n_total = 0, n_max = 0;
+    for (int k = 0; k < n_segs; ++k) {
+        n_total += segs[k].count;
+        n_max = segs[k].count > n_max ? segs[k].count : n_max;
+        if (segs[k].queue_capacity && !next_queue)
+            return fail(ctx, NRRS_ERR_INVALID_ARG, "next_queue is NULL");
+    }
+    if ((rc = check_decide_params(ctx, p, n_max))) return rc;
+    if (n_total > ctx->cfg.max_queue) return fail(ctx, NRRS_ERR_INVALID_ARG, "sum of counts > max_queue");
+    if (!rrs || !rnd || !next_size_dev) return fail(ctx, NRRS_ERR_INVALID_ARG, "rrs/rnd/next_size NULL");
+    cudaStream_t s = (cudaStream_t)stream;
+    if ((rc = resolve_counts(ctx, segs, n_segs, counts_dev, s))) return rc;
+    rc = run_infer(ctx, v, make_segments(segs, n_segs, kTile), p, n_max, stats, rrs, true, s,
+                   nullptr, &ctx->segs_dev[0]);
+    if (rc) return rc;
+    return run_decide(ctx, rrs, rnd, v->scatter_index, segs, n_segs, n_max, nullptr, p, rrs_norm,
+                      split, next_queue, next_size_dev, false, s, nullptr, true);
 }
 
 int nrrs_infer_accumulate(nrrs_ctx* ctx, const nrrs_vertex_soa* v, uint32_t n,

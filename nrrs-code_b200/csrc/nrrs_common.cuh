@@ -81,7 +81,16 @@ struct SegmentTable {
     Segment s[kMaxSegments];
     int32_t n;
     uint32_t total_tiles;
+    // When the queue sizes live on the device, the host table holds the largest counts (which
+    // size the grid) and `resolved` points at the table k_resolve_segments built on the device
+    // from the actual counts; kernels read that one (seg_table).
+    const struct SegmentTable* resolved;
 };
+
+// the table a kernel works on: the device-resolved one when there is one
+__device__ __forceinline__ const SegmentTable& seg_table(const SegmentTable& t) {
+    return t.resolved ? *t.resolved : t;
+}
 
 // Scratch words of the decision kernel; lives in context memory (or a static array for the
 // allocation-free entry point). Self-resetting: the last CTA of every launch restores it.

@@ -186,6 +186,21 @@ _SIGS = {
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                            C.c_void_p, C.c_void_p]),
     "nrrs_noalloc_device_status": (C.c_int, [C.POINTER(C.c_uint32), C.c_void_p]),
+    "nrrs_infer_dev": (C.c_int, [C.c_void_p, C.POINTER(VertexSoA), C.c_void_p, C.c_uint32,
+                                 C.POINTER(DecideParams), C.c_void_p, C.c_void_p, C.c_void_p]),
+    "nrrs_decide_emit_dev": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p,
+                                       C.POINTER(DecideParams), C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    "nrrs_step_dev": (C.c_int, [C.c_void_p, C.POINTER(VertexSoA), C.c_void_p, C.c_void_p,
+                                C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p,
+                                C.POINTER(DecideParams), C.c_void_p, C.c_void_p, C.c_void_p,
+                                C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    "nrrs_step_batched_dev": (C.c_int, [C.c_void_p, C.POINTER(VertexSoA), C.c_void_p,
+                                        C.POINTER(Segment), C.c_void_p, C.c_int32,
+                                        C.POINTER(DecideParams), C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p]),
     "nrrs_infer_accumulate": (C.c_int, [C.c_void_p, C.POINTER(VertexSoA), C.c_uint32,
                                         C.POINTER(DecideParams), C.c_void_p, C.c_void_p,
                                         C.c_void_p, C.c_void_p]),
@@ -962,6 +977,36 @@ class NRRSNetwork:
         return self._check(lib().nrrs_step_batched(
             self._h, C.byref(soa), _ptr(rnd), arr, len(segments), C.byref(params), _ptr(stats),
             _ptr(rrs), _ptr(rrs_norm), _ptr(split), _ptr(queue), _ptr(next_size), stream))
+
+    # ---- device-resident queue sizes (n_dev: a device uint32 word; max_n: host bound) ----
+    def inferDev(self, soa: VertexSoA, n_dev, max_n: int, params: DecideParams, stats, rrs,
+                 stream=0):
+        return self._check(lib().nrrs_infer_dev(self._h, C.byref(soa), _ptr(n_dev), max_n,
+                                                C.byref(params), _ptr(stats), _ptr(rrs), stream))
+
+    def decideEmitDev(self, rrs, rnd, n_dev, max_n, budget, n_specular, params, rrs_norm, split,
+                      queue, capacity, next_size, scatter_index=None, n_specular_dev=None,
+                      stream=0):
+        return self._check(lib().nrrs_decide_emit_dev(
+            self._h, _ptr(rrs), _ptr(rnd), _ptr(scatter_index), _ptr(n_dev), max_n, budget,
+            n_specular, _ptr(n_specular_dev), C.byref(params), _ptr(rrs_norm), _ptr(split),
+            _ptr(queue), capacity, _ptr(next_size), stream))
+
+    def generateRRSNumberDev(self, soa, rnd, n_dev, max_n, budget, n_specular, params, stats,
+                             rrs, rrs_norm, split, queue, capacity, next_size,
+                             n_specular_dev=None, stream=0):
+        return self._check(lib().nrrs_step_dev(
+            self._h, C.byref(soa), _ptr(rnd), _ptr(n_dev), max_n, budget, n_specular,
+            _ptr(n_specular_dev), C.byref(params), _ptr(stats), _ptr(rrs), _ptr(rrs_norm),
+            _ptr(split), _ptr(queue), capacity, _ptr(next_size), stream))
+
+    def generateRRSNumberBatchedDev(self, soa, rnd, segments, counts_dev, params, stats, rrs,
+                                    rrs_norm, split, queue, next_size, stream=0):
+        arr = (Segment * len(segments))(*segments)
+        return self._check(lib().nrrs_step_batched_dev(
+            self._h, C.byref(soa), _ptr(rnd), arr, _ptr(counts_dev), len(segments),
+            C.byref(params), _ptr(stats), _ptr(rrs), _ptr(rrs_norm), _ptr(split), _ptr(queue),
+            _ptr(next_size), stream))
 
     def train(self, soa: VertexSoA, target, n: int, loss_dev=None, stream=0):
         return self._check(lib().nrrs_train_step(self._h, C.byref(soa), _ptr(target), n,
