@@ -708,8 +708,8 @@ def run_batched(args, torch, dev, stream, timer, steps, warmup, rank):
         same &= bool(torch.equal(p["rrs"], ob["rrs"][a0:a1]))
         same &= bool(torch.equal(p["q"][:int(p["sz"].item())] + int(offs[k]),
                                  ob["q"][int(qoffs[k]):int(qoffs[k]) + int(ob["sz"][k].item())]))
-    fp = nb.NRRSNetwork(make_config("fp32", wl, N, wl["train_batch"]))
-    fp.autotune(N)
+    fp = nb.NRRSNetwork(make_config("fp32", wl, max(counts), wl["train_batch"]))
+    fp.autotune(max(counts))
     ms_fp32_pd = timer(lambda: per_depth(fp), max(3, steps // 5), 1)
     graph.close()
     net.close()
@@ -871,13 +871,19 @@ def run_ours(args, rank, world, local_rank):
     if world == 1 and not args.only:
         sec = {}
         if name != "frame1080p":
-            q = run_frame_pair(args, torch, dev, stream, timer, "frame1080p", 20, 3, 5, rank, 1,
-                               headline=False)
-            sec["frame1080p"] = pair_summary(q)
-            q["arm"].close()
-            del q
+            try:
+                q = run_frame_pair(args, torch, dev, stream, timer, "frame1080p", 20, 3, 5, rank,
+                                   1, headline=False)
+                sec["frame1080p"] = pair_summary(q)
+                q["arm"].close()
+                del q
+            except Exception as exc:   # the headline line is printed regardless
+                sec["frame1080p"] = {"error": f"{type(exc).__name__}: {exc}"}
             torch.cuda.empty_cache()
-        sec["batched"] = run_batched(args, torch, dev, stream, timer, 20, 3, rank)
+        try:
+            sec["batched"] = run_batched(args, torch, dev, stream, timer, 20, 3, rank)
+        except Exception as exc:
+            sec["batched"] = {"error": f"{type(exc).__name__}: {exc}"}
         line["secondary"] = sec
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = CpuFrameSample(wl, do_train_of(args, wl))

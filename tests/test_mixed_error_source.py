@@ -82,3 +82,41 @@ def test_mixed_table_gradient_error_comes_from_the_fp16_forward():
         assert 3e-3 < e < 5e-2, (name, e)
     assert 1e-2 < forward < 5e-2, forward
     assert split < 1e-3, split
+
+
+def test_fp32_table_gradient_error_at_training_size_is_one_mask_flip():
+    """The plain FP32 path at the training size (262,144 samples, 2^19 table) replayed in
+    numpy float32: one hidden unit of one sample flips its ReLU mask against FP64, and that
+    sample carries almost all of the hash-lane gradient error (about 5.7e-4 relative L2, the
+    GPU's 5.1e-4)."""
+    cfg = O.default_config(max_train=262_144, log2_hashmap_size=19)
+    npar, ntab, nst, nrr = O.param_count(cfg)
+    rng = np.random.default_rng(61)   # the draws of tests/test_gpu_configs.py's parameters
+    p = np.empty(npar, np.float32)
+    p[:ntab] = rng.uniform(-0.5, 0.5, ntab)
+    p[ntab:] = rng.uniform(-0.15, 0.15, nst + nrr)
+    n = 262_144
+    v = O.synth(62, n)
+    x0 = O.infer(cfg, p, v, O.default_decide(), "f64", want=("x0",))["x0"]
+    W = p[ntab:ntab + nst].astype(np.float64)
+    W0, W1, W2 = W[:4096].reshape(64, 64), W[4096:8192].reshape(64, 64), W[8192:].reshape(3, 64)
+    tgt = np.log(v["target"].astype(np.float64) + cfg.stat_eps)
+
+    def run(dt):
+        x, a0, a1, a2, t = (m.astype(dt) for m in (x0, W0, W1, W2, tgt))
+        z1 = x @ a0.T
+        h1 = np.maximum(z1, 0)
+        z2 = h1 @ a1.T
+        y = np.maximum(z2, 0) @ a2.T
+        dh2 = ((2 * (y - t) / 3) @ a2) * (z2 > 0)
+        dh1 = (dh2 @ a1) * (z1 > 0)
+        return (dh1 @ a0)[:, :32].astype(np.float64), (z1 > 0), (z2 > 0)
+
+    a, m1a, m2a = run(np.float64)
+    b, m1b, m2b = run(np.float32)
+    flips = int(np.sum(m1a != m1b) + np.sum(m2a != m2b))
+    per = np.linalg.norm(b - a, axis=1)
+    rel = float(np.linalg.norm(b - a) / np.linalg.norm(a))
+    assert flips >= 1
+    assert 2e-4 < rel < 2e-3, rel
+    assert per.max() ** 2 / (per ** 2).sum() > 0.99
