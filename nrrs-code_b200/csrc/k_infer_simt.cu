@@ -1,5 +1,5 @@
 // k_infer_simt.cu -- plain FP32 inference: hash grid + SH encoding, StatNet, glue, RRSNet,
-// activation, clamp and the exact normalisation sum, one thread per vertex (SIMT FP32).
+// activation, clamp and the exact normalisation sum, on the FP32 SIMT pipes.
 //
 // This is the "plain FP32 per-depth path" the mixed-precision tcgen05 path is measured
 // against. It fuses what the reference runs as nrrs_generate_inference_data (train.cu:269-287),
@@ -7,71 +7,140 @@
 // nrrs_generate_inference_data_from_0to1 (train.cu:41-112) and the "Gen RRS Number" lambda
 // (integrator.cpp:1184-1298), so the AoS round trips of the reference disappear.
 //
-// Layout: each thread keeps its activation column in shared memory (xs[lane][thread], conflict
-// free); weights are stored transposed ([in][out], out padded to 4) and read as broadcast
-// float4 loads from shared memory when they fit, else from global memory through L1.
+// A CTA of 128 threads works on 64 vertices at a time (half of a 128-vertex tile of the segment
+// table). Their activations live in one shared-memory tile, K-major ([k][64 vertices + 4 pad]).
+// Every hidden layer is a register-tiled FP32 GEMM: each thread owns an 8 x (W/16) block of outputs
+// (8 vertices x 8 or 4 neurons), and per k it reads 8 activations and 8 (or 4) weights as
+// float4 and issues 64 (or 32) FMAs. The layer's transposed weights ([in][out]) come from L2 in
+// 32-row chunks, double-buffered with cp.async while the previous chunk is consumed. Every output
+// is accumulated as fmaf(w_k, x_k, acc) over k ascending, the same sequence for any launch shape.
+// The narrow layers (3 and 1 outputs), the glue, the factor and the exact-sum term run one thread
+// per vertex on that vertex's column of the tile.
 #include "kernels.hpp"
 
 namespace nrrs {
 
 namespace {
 
-template <int IN, int OUT, int OUTP, bool RELU>
-__device__ __forceinline__ void dense_layer(const float* __restrict__ Wt, float* xs, int tid,
-                                            float* out_reg) {
+constexpr int kTM = 64;        // vertices per work item (half of a segment-table tile)
+// row stride of the activation tile: 4 floats of padding keep float4 alignment and spread the
+// epilogue's stores (neuron rows 4 apart) over twice as many banks
+constexpr int kLd = kTM + 4;
+constexpr int kThr = 128;      // threads per CTA
+constexpr int kKC = 32;        // weight rows per chunk
+
+constexpr int pad4(int x) { return (x + 3) / 4 * 4; }
+constexpr int imax(int a, int b) { return a > b ? a : b; }
+
+template <int W>
+struct FpShape {
+    static constexpr int kRows = imax(kStatIn, W);                 // rows of the activation tile
+    static constexpr int kActFloats = kRows * kLd;
+    static constexpr int kChunkFloats = kKC * W;
+    static constexpr size_t kSmem = sizeof(float) * (kActFloats + 2 * kChunkFloats);
+};
+
+__device__ __forceinline__ void cp_async16(float* smem_dst, const float* gmem_src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// rows x W floats of a transposed weight matrix into a shared-memory chunk
+template <int W>
+__device__ __forceinline__ void load_chunk(float* dst, const float* __restrict__ src, int rows,
+                                           int tid) {
+    const int n4 = rows * (W / 4);
+    for (int q = tid; q < n4; q += kThr) cp_async16(dst + 4 * q, src + 4 * q);
+}
+
+// out[n][m] = max(0, sum_k wt[k][n] act[k][m]) for k < k_eff, in place on the activation tile
+// (every read of the layer's input ends at the chunk loop's last barrier, before any write).
+// wt is [k_rows][W] in global memory; rows k_eff .. k_rows-1 are loaded but multiply zeros.
+template <int W>
+__device__ __forceinline__ void hidden_layer(const float* __restrict__ wt, int k_rows, int k_eff,
+                                             float* act, float* wch, int tid) {
+    constexpr int C = W / 16;                 // neurons per thread: 8 (W = 128) or 4 (W = 64)
+    const int lane = tid & 31, warp = tid >> 5;
+    const int tx = lane & 15, ty = warp * 2 + (lane >> 4);   // ty 0..7: vertices ty*8 .. +7
+    float acc[8][C];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < C; ++j) acc[i][j] = 0.f;
+    const int nch = (k_rows + kKC - 1) / kKC;
+    load_chunk<W>(wch, wt, k_rows < kKC ? k_rows : kKC, tid);
+    cp_async_commit();
+#pragma unroll 1
+    for (int c = 0; c < nch; ++c) {
+        if (c + 1 < nch) {
+            const int r = k_rows - (c + 1) * kKC;
+            load_chunk<W>(wch + ((c + 1) & 1) * kKC * W, wt + (size_t)(c + 1) * kKC * W,
+                          r < kKC ? r : kKC, tid);
+        }
+        cp_async_commit();
+        cp_async_wait1();   // every group but the newest: chunk c has landed
+        __syncthreads();
+        const float* B = wch + (c & 1) * kKC * W + tx * 4;
+        const float* A = act + (size_t)(c * kKC) * kLd + ty * 8;
+        const int kn = k_eff - c * kKC < kKC ? k_eff - c * kKC : kKC;
+#pragma unroll 4
+        for (int kk = 0; kk < kn; ++kk) {
+            const float4 a0 = *reinterpret_cast<const float4*>(A + kk * kLd);
+            const float4 a1 = *reinterpret_cast<const float4*>(A + kk * kLd + 4);
+            const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            float bv[C];
+            const float4 b0 = *reinterpret_cast<const float4*>(B + kk * W);
+            bv[0] = b0.x; bv[1] = b0.y; bv[2] = b0.z; bv[3] = b0.w;
+            if constexpr (C == 8) {
+                const float4 b1 = *reinterpret_cast<const float4*>(B + kk * W + 64);
+                bv[4] = b1.x; bv[5] = b1.y; bv[6] = b1.z; bv[7] = b1.w;
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < C; ++j) acc[i][j] = fmaf(bv[j], av[i], acc[i][j]);
+        }
+        __syncthreads();    // the buffer read here is refilled by the next iteration's prefetch
+    }
+#pragma unroll
+    for (int j = 0; j < C; ++j) {
+        const int n = (j < 4 ? 0 : 64) + tx * 4 + (j & 3);
+        float* o = act + (size_t)n * kLd + ty * 8;
+        *reinterpret_cast<float4*>(o) = make_float4(fmaxf(acc[0][j], 0.f), fmaxf(acc[1][j], 0.f),
+                                                    fmaxf(acc[2][j], 0.f), fmaxf(acc[3][j], 0.f));
+        *reinterpret_cast<float4*>(o + 4) = make_float4(fmaxf(acc[4][j], 0.f), fmaxf(acc[5][j], 0.f),
+                                                        fmaxf(acc[6][j], 0.f), fmaxf(acc[7][j], 0.f));
+    }
+    __syncthreads();
+}
+
+// the network's narrow output layer for vertex column m: y[o] = sum_k wt[k][o] act[k][m]
+template <int W, int OUT>
+__device__ __forceinline__ void output_layer(const float* __restrict__ wt, const float* act, int m,
+                                             float* y) {
     float acc[OUT];
 #pragma unroll
     for (int o = 0; o < OUT; ++o) acc[o] = 0.f;
-#pragma unroll 2
-    for (int k = 0; k < IN; ++k) {
-        const float xk = xs[k * kTile + tid];
-        const float4* w4 = reinterpret_cast<const float4*>(Wt + k * OUTP);
-#pragma unroll
-        for (int o4 = 0; o4 < OUTP / 4; ++o4) {
-            const float4 w = w4[o4];
-            if (4 * o4 + 0 < OUT) acc[4 * o4 + 0] = fmaf(w.x, xk, acc[4 * o4 + 0]);
-            if (4 * o4 + 1 < OUT) acc[4 * o4 + 1] = fmaf(w.y, xk, acc[4 * o4 + 1]);
-            if (4 * o4 + 2 < OUT) acc[4 * o4 + 2] = fmaf(w.z, xk, acc[4 * o4 + 2]);
-            if (4 * o4 + 3 < OUT) acc[4 * o4 + 3] = fmaf(w.w, xk, acc[4 * o4 + 3]);
-        }
+#pragma unroll 4
+    for (int k = 0; k < W; ++k) {
+        const float x = act[k * kLd + m];
+        const float4 w = __ldg(reinterpret_cast<const float4*>(wt + 4 * k));
+        acc[0] = fmaf(w.x, x, acc[0]);
+        if (OUT > 1) acc[1] = fmaf(w.y, x, acc[1]);
+        if (OUT > 2) acc[2] = fmaf(w.z, x, acc[2]);
     }
-    if (out_reg) {
 #pragma unroll
-        for (int o = 0; o < OUT; ++o) out_reg[o] = RELU ? fmaxf(acc[o], 0.f) : acc[o];
-    } else {
-#pragma unroll
-        for (int o = 0; o < OUT; ++o) xs[o * kTile + tid] = RELU ? fmaxf(acc[o], 0.f) : acc[o];
-    }
+    for (int o = 0; o < OUT; ++o) y[o] = acc[o];
 }
 
-constexpr int pad4(int x) { return (x + 3) / 4 * 4; }
-
-template <int W, int H, int IN, int OUT>
-struct MlpShape {
-    static constexpr int kFloats = IN * W + (H - 1) * W * W + W * pad4(OUT);
-};
-
-// forward through a bias-free ReLU MLP whose input column is xs[0, IN_EFF)
-template <int W, int H, int IN, int IN_EFF, int OUT>
-__device__ __forceinline__ void mlp_simt(const float* __restrict__ Wt, float* xs, int tid,
-                                         float* y) {
-    dense_layer<IN_EFF, W, W, true>(Wt, xs, tid, nullptr);
-    Wt += IN * W;
-#pragma unroll 1
-    for (int h = 1; h < H; ++h) {
-        dense_layer<W, W, W, true>(Wt, xs, tid, nullptr);
-        Wt += W * W;
-    }
-    dense_layer<W, OUT, pad4(OUT), false>(Wt, xs, tid, y);
-}
-
-// hash grid + SH + misc lanes of vertex i into this thread's column xs[0, 56)
-__device__ __forceinline__ void encode_simt(const InferArgs& a, uint32_t i, float* xs, int tid) {
-    float p[3];
-    norm_pos(a.enc, a.v.pos, i, p);
+// hash-grid levels l0 .. l0+7 of vertex i into its column of the tile (FP32 table)
+__device__ __forceinline__ void encode_levels8(const InferArgs& a, const float* p, int l0, float* act,
+                                               int m) {
     const float2* table = reinterpret_cast<const float2*>(a.table);
 #pragma unroll 2
-    for (int l = 0; l < kMaxLevels; ++l) {
+    for (int l = l0; l < l0 + 8; ++l) {
         const LevelDev L = a.enc.lv[l];
         const CellCoord c = cell_of(p, L.res);
         uint32_t rows[8];
@@ -89,65 +158,93 @@ __device__ __forceinline__ void encode_simt(const InferArgs& a, uint32_t i, floa
             f0 += w * t[k].x;
             f1 += w * t[k].y;
         }
-        xs[(2 * l) * kTile + tid] = f0;
-        xs[(2 * l + 1) * kTile + tid] = f1;
+        act[(2 * l) * kLd + m] = f0;
+        act[(2 * l + 1) * kLd + m] = f1;
     }
-    float sh[16];
-    const size_t i3 = 3 * (size_t)i;
-    sh16(a.v.wi[i3], a.v.wi[i3 + 1], a.v.wi[i3 + 2], sh);
-#pragma unroll
-    for (int k = 0; k < 16; ++k) xs[(32 + k) * kTile + tid] = sh[k];
-    float m[16];
-    misc_lanes(a.v, i, m);
-#pragma unroll
-    for (int k = 0; k < 8; ++k) xs[(48 + k) * kTile + tid] = m[k];
 }
 
-template <int WS, int HS, int WR, int HR, bool WSMEM>
-__global__ void __launch_bounds__(kTile) k_infer_fp32(const __grid_constant__ InferArgs a) {
+template <int WS, int HS, int WR, int HR>
+__global__ void __launch_bounds__(kThr) k_infer_fp32(const __grid_constant__ InferArgs a) {
+    static_assert(WS == WR, "one tile shape for both networks");
+    using S = FpShape<WS>;
     extern __shared__ float4 smem4[];
-    float* smem = reinterpret_cast<float*>(smem4);
-    constexpr int NS = MlpShape<WS, HS, kStatIn, kStatOut>::kFloats;
-    constexpr int NR = MlpShape<WR, HR, kRrsIn, 1>::kFloats;
+    float* act = reinterpret_cast<float*>(smem4);
+    float* wch = act + S::kActFloats;
     const int tid = threadIdx.x;
-    const float* wst = a.wt_stat;
-    const float* wrt = a.wt_rrs;
-    float* xs = smem;
-    if (WSMEM) {
-        const float4* s4 = reinterpret_cast<const float4*>(a.wt_stat);
-        const float4* r4 = reinterpret_cast<const float4*>(a.wt_rrs);
-        for (int k = tid; k < NS / 4; k += kTile) smem4[k] = s4[k];
-        for (int k = tid; k < NR / 4; k += kTile) smem4[NS / 4 + k] = r4[k];
-        __syncthreads();
-        wst = smem;
-        wrt = smem + NS;
-        xs = smem + NS + NR;
-    }
-    const SegmentTable& S = seg_table(a.segs);
-    for (uint32_t t = blockIdx.x; t < S.total_tiles; t += gridDim.x) {
-        const int si = find_segment(S, t);
-        const Segment& sg = S.s[si];
-        const uint32_t i = sg.offset + (t - sg.tile_start) * kTile + tid;
+    const int m = tid & (kTM - 1);
+    const bool lead = tid < kTM;               // the thread that owns vertex column m
+    const SegmentTable& ST = seg_table(a.segs);
+    const uint32_t items = 2u * ST.total_tiles;
+    // transposed layer images: [in][out] (outputs padded to 4), StatNet then RRSNet
+    const float* s0 = a.wt_stat;
+    const float* s_out = s0 + (size_t)kStatIn * WS + (size_t)(HS - 1) * WS * WS;
+    const float* r0 = a.wt_rrs;
+    const float* r_out = r0 + (size_t)kRrsIn * WR + (size_t)(HR - 1) * WR * WR;
+
+#pragma unroll 1
+    for (uint32_t u = blockIdx.x; u < items; u += gridDim.x) {
+        const uint32_t t = u >> 1;
+        const int si = find_segment(ST, t);
+        const Segment& sg = ST.s[si];
+        const uint32_t i = sg.offset + (t - sg.tile_start) * kTile + (u & 1u) * kTM + m;
         const bool valid = i < sg.offset + sg.count;
-        long long term = 0;
+        __syncthreads();   // the previous item's column reads are over
+        // encoding: two threads per vertex (levels 0-7 + SH, levels 8-15 + misc lanes)
         if (valid) {
-            encode_simt(a, i, xs, tid);
-            float y[3];
-            mlp_simt<WS, HS, kStatIn, 56, kStatOut>(wst, xs, tid, y);
-            float x1[16];
-            glue16(a.fp, y, a.v, i, x1);
+            float p[3];
+            norm_pos(a.enc, a.v.pos, i, p);
+            if (lead) {
+                encode_levels8(a, p, 0, act, m);
+                float sh[16];
+                const size_t i3 = 3 * (size_t)i;
+                sh16(a.v.wi[i3], a.v.wi[i3 + 1], a.v.wi[i3 + 2], sh);
 #pragma unroll
-            for (int k = 0; k < 10; ++k) xs[k * kTile + tid] = x1[k];
+                for (int k = 0; k < 16; ++k) act[(32 + k) * kLd + m] = sh[k];
+            } else {
+                encode_levels8(a, p, 8, act, m);
+                float misc[16];
+                misc_lanes(a.v, i, misc);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) act[(48 + k) * kLd + m] = misc[k];
+            }
+        } else {
+            for (int k = lead ? 0 : 28; k < (lead ? 28 : 56); ++k) act[k * kLd + m] = 0.f;
+        }
+        VertexAux aux{};
+        if (lead && valid) aux = load_aux(a.v, i);
+        // StatNet: 56 live input lanes (48..55 misc, 56..63 zero)
+        hidden_layer<WS>(s0, kStatIn, 56, act, wch, tid);
+#pragma unroll 1
+        for (int h = 1; h < HS; ++h)
+            hidden_layer<WS>(s0 + (size_t)kStatIn * WS + (size_t)(h - 1) * WS * WS, WS, WS, act,
+                             wch, tid);
+        float y[3] = {0.f, 0.f, 0.f};
+        if (lead) {
+            output_layer<WS, 3>(s_out, act, m, y);
+            // glue: the RRSNet input in this vertex's column (10 live lanes)
+            float x1[16];
+            glue16_aux(a.fp, y, aux, x1);
+#pragma unroll
+            for (int k = 0; k < 10; ++k) act[k * kLd + m] = x1[k];
+        }
+        hidden_layer<WR>(r0, kRrsIn, 10, act, wch, tid);
+#pragma unroll 1
+        for (int h = 1; h < HR; ++h)
+            hidden_layer<WR>(r0 + (size_t)kRrsIn * WR + (size_t)(h - 1) * WR * WR, WR, WR, act,
+                             wch, tid);
+        long long term = 0;
+        if (lead && valid) {
             float raw;
-            mlp_simt<WR, HR, kRrsIn, 10, 1>(wrt, xs, tid, &raw);
-            const float rrs = rrs_factor(a.fp, y, raw, a.v, i);
+            output_layer<WR, 1>(r_out, act, m, &raw);
+            const float rrs = rrs_factor_aux(a.fp, y, raw, aux);
             if (a.stats) {
                 a.stats[3 * (size_t)i] = y[0];
                 a.stats[3 * (size_t)i + 1] = y[1];
                 a.stats[3 * (size_t)i + 2] = y[2];
             }
             a.rrs[i] = rrs;
-            if (a.scr || a.ext_acc) term = fixed_term(a.fp, rrs, a.scr ? &a.scr->status : &g_dummy_status);
+            if (a.scr || a.ext_acc)
+                term = fixed_term(a.fp, rrs, a.scr ? &a.scr->status : &g_dummy_status);
         }
         if (a.scr || a.ext_acc) {
             term = warp_sum_ll(term);
@@ -159,24 +256,19 @@ __global__ void __launch_bounds__(kTile) k_infer_fp32(const __grid_constant__ In
 
 template <int WS, int HS, int WR, int HR>
 cudaError_t launch_cfg(const InferArgs& a, int sm_count, int ctas_per_sm, cudaStream_t s) {
-    constexpr int NS = MlpShape<WS, HS, kStatIn, kStatOut>::kFloats;
-    constexpr int NR = MlpShape<WR, HR, kRrsIn, 1>::kFloats;
-    constexpr int XW = (WS > WR ? WS : WR) > kStatIn ? (WS > WR ? WS : WR) : kStatIn;
-    constexpr size_t xs_bytes = (size_t)XW * kTile * sizeof(float);
-    constexpr size_t w_bytes = (size_t)(NS + NR) * sizeof(float);
-    constexpr bool fits = xs_bytes + w_bytes <= 200 * 1024;
-    const size_t smem = fits ? xs_bytes + w_bytes : xs_bytes;
-    auto kern = k_infer_fp32<WS, HS, WR, HR, fits>;
+    using S = FpShape<WS>;
+    auto kern = k_infer_fp32<WS, HS, WR, HR>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+                                         (int)S::kSmem);
     if (e != cudaSuccess) return e;
-    int per_sm = resident_ctas((const void*)kern, kTile, smem, 32);
+    int per_sm = resident_ctas((const void*)kern, kThr, S::kSmem, 32);
     if (ctas_per_sm > 0 && ctas_per_sm < per_sm) per_sm = ctas_per_sm;
+    const uint32_t items = 2u * a.segs.total_tiles;
     unsigned grid = (unsigned)(sm_count * per_sm);
-    if (grid > a.segs.total_tiles) grid = a.segs.total_tiles;
+    if (grid > items) grid = items;
     if (grid == 0) return cudaSuccess;
     g_last_grid = (int)grid;
-    kern<<<grid, kTile, smem, s>>>(a);
+    kern<<<grid, kThr, S::kSmem, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -195,18 +287,12 @@ cudaError_t launch_infer_fp32(const InferArgs& a, int ws, int hs, int wr, int hr
 
 template <int WS, int HS, int WR, int HR>
 int max_ctas_fp32() {
-    constexpr int NS = MlpShape<WS, HS, kStatIn, kStatOut>::kFloats;
-    constexpr int NR = MlpShape<WR, HR, kRrsIn, 1>::kFloats;
-    constexpr int XW = (WS > WR ? WS : WR) > kStatIn ? (WS > WR ? WS : WR) : kStatIn;
-    constexpr size_t xs_bytes = (size_t)XW * kTile * sizeof(float);
-    constexpr size_t w_bytes = (size_t)(NS + NR) * sizeof(float);
-    constexpr bool fits = xs_bytes + w_bytes <= 200 * 1024;
-    const size_t smem = fits ? xs_bytes + w_bytes : xs_bytes;
-    auto kern = k_infer_fp32<WS, HS, WR, HR, fits>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+    using S = FpShape<WS>;
+    auto kern = k_infer_fp32<WS, HS, WR, HR>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kSmem) !=
         cudaSuccess)
         return 0;
-    return resident_ctas((const void*)kern, kTile, smem, 32);
+    return resident_ctas((const void*)kern, kThr, S::kSmem, 32);
 }
 
 int infer_max_ctas_fp32(int ws, int hs) {
