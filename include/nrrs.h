@@ -506,6 +506,37 @@ int nrrs_generate_training_data(const nrrs_path_nodes* nodes, const nrrs_train_d
 int nrrs_sample_weights(const uint32_t* pixel, const uint32_t* pixel_samples, uint32_t n_pixels,
                         const uint32_t* size_dev, uint32_t max_n, float* weight, void* stream);
 
+/* ---- training on the batch built from the path records, with the reference's per-sample loss
+ *      inputs. Replaces NRRSNetwork::train (network.cpp:196-295) with the loss hyper-parameters
+ *      and side arrays the reference passes to its NRRS_LL2 / NRRS_RRS losses
+ *      (network.cpp:423-435, 532-557): sample_weight (nrrs_sample_weights, train.cu:572-592),
+ *      the batch's error, error_for_avg and number_samples (train.cu:537-543), the RRSNet target
+ *      whose -1 marks a duplicate sibling to skip (train.cu:520-523), its thp and ref_mean, the
+ *      error sum (nrrs_calculate_error), gamma1..4 and clamp_on / clamp_max. The loss arithmetic
+ *      of the reference lives in its absent tiny-cuda-nn fork; this library's definition (also
+ *      restated in the oracle) is, per sample i with s = sample_weight (1 when NULL):
+ *        w_i = s_i, or 0 where rrs_target[i] < 0;  e_mean = *error_sum_dev / n_pixels (1 when NULL)
+ *        e_i = error[i] / e_mean,  a_i = error_for_avg[i] / e_mean  (1 when NULL; each clamped to
+ *              clamp_max when clamp_on);  u_i = gamma1 + gamma2 e_i + gamma3 a_i
+ *        k_i = max(number_samples[i], 1) (1 when NULL)
+ *        loss_S = sum s_i sum_c (y_ic - log(L_ic + stat_eps))^2 / (3 sum s)
+ *        V = sum w u r^2 / (k q) / sum w,  C = sum w (cost_offset + q) / sum w,
+ *        R = sum w (ln q)^2 / sum w,  loss_R = V C + gamma4 R
+ *      with q and r as in nrrs_train_step. With every side array NULL and the default
+ *      parameters (gamma 1, 0, 0, 0) it is nrrs_train_step's loss. n is a host value (the
+ *      reference reads the batch size back too, integrator.cpp:2619-2625). ---- */
+typedef struct {
+    float gamma1, gamma2, gamma3, gamma4; /* NRRS_RRS gammas (2net-simple.json level1.loss)    */
+    int32_t clamp_on;                     /* clamp the error ratios at clamp_max               */
+    float clamp_max;
+    uint32_t n_pixels;                    /* pixels (patches) of the error image              */
+} nrrs_loss_params;
+void nrrs_loss_params_default(nrrs_loss_params* p);
+int nrrs_train_step_batch(nrrs_ctx* ctx, const nrrs_train_batch* batch, uint32_t n,
+                          const float* sample_weight, const float* error_sum_dev,
+                          const nrrs_loss_params* lp, double* loss_dev, void* stream);
+
+
 /* ==== per-pixel error of the RRSNet loss =========================================================
  * The image-space inputs of the RRSNet loss, computed once per training frame (trainStep,
  * integrator.cpp:2358-2471): a blended estimate of each patch's radiance, its relative error

@@ -58,6 +58,7 @@ struct nrrs_ctx {
     void* train_scratch = nullptr;
     size_t train_scratch_bytes = 0;
     double* loss_dev = nullptr;  // [2] last losses
+    double* loss_sums = nullptr; // [4] batch sums of the loss weights (nrrs_train_step_batch)
 
     int last_infer_grid = 0;
     int tc_ctas_per_sm = 0;      // autotuned occupancy of the tcgen05 kernel (0 = default)
@@ -101,8 +102,13 @@ struct ProfScope {
 
 namespace nrrs {
 // gradients of one step; with apply, the Adam update too
+// (lw: per-sample loss weights of nrrs_train_step_batch; NULL = plain means)
 int train_step_impl(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint32_t n,
-                    double* loss_dev, cudaStream_t s, bool apply = true);
+                    double* loss_dev, cudaStream_t s, bool apply = true,
+                    const LossWeights* lw = nullptr);
+// batch sums of the loss weights into out[3] (sum s, sum w, mean pixel error)
+cudaError_t launch_loss_sums(const LossWeights& w, uint32_t n, const float* error_sum,
+                             uint32_t n_pixels, double* out, cudaStream_t s);
 // Adam on ctx->grads scaled by `scale` (copied in from grads_dev first when it is not ctx->grads)
 cudaError_t launch_adam_step(nrrs_ctx* ctx, bool train_rrs, cudaStream_t s, float scale = 1.0f);
 size_t train_scratch_bytes(const nrrs_config& cfg, uint32_t n, int sm_count);

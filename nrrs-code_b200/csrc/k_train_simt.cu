@@ -46,9 +46,10 @@ struct TrainArgs {
     const float* w_rrs;
     float* act;                    // feature-major scratch
     uint32_t r_x0, r_hs, r_dhs, r_dy, r_x1, r_hr, r_dhr, r_draw;
-    double* part;                  // [grid][4]: loss_S sum, V sum, C sum
+    double* part;                  // [grid][4]: loss_S sum, V sum, C sum, R sum
     uint32_t part_n;               // CTAs of k_train_stat
     double* loss_out;              // [2]
+    LossWeights lw;                // per-sample loss weights (inactive: plain means)
 };
 
 // out_col[o] = sum_k W[k][o] * in_col[k] (Wt stored [IN][OUTP]); columns of this thread in smem
@@ -144,7 +145,7 @@ __global__ void __launch_bounds__(kTT) k_train_stat(const __grid_constant__ Trai
     float* colB = smem + XW * kTT + threadIdx.x; // deltas
     const int tid = threadIdx.x;
     const uint32_t ld = a.ld;
-    double lossS = 0.0, sumV = 0.0, sumC = 0.0;
+    double lossS = 0.0, sumV = 0.0, sumC = 0.0, sumR = 0.0;
     const float2* table = reinterpret_cast<const float2*>(a.table);
     const uint32_t tiles = (a.n + kTT - 1) / kTT;
     for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
@@ -202,11 +203,18 @@ __global__ void __launch_bounds__(kTT) k_train_stat(const __grid_constant__ Trai
 
         // ---- StatNet loss gradient ----
         const size_t i3 = 3 * (size_t)i;
+        const SampleMul mu = sample_mul(a.lw, i, a.n);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             const float d = y[c] - logf(a.target[i3 + c] + a.fp.stat_eps);
-            lossS += (double)d * (double)d;
-            const float g = 2.0f * d / (3.0f * (float)a.n);
+            float g;
+            if (a.lw.active) {
+                lossS += (double)mu.stat * (double)d * (double)d;
+                g = mu.stat * (2.0f * d) / (3.0f * (float)a.n);
+            } else {
+                lossS += (double)d * (double)d;
+                g = 2.0f * d / (3.0f * (float)a.n);
+            }
             colB[c * kTT] = g;
             act[(size_t)(a.r_dy + c) * ld] = g;
         }
@@ -295,17 +303,26 @@ __global__ void __launch_bounds__(kTT) k_train_stat(const __grid_constant__ Trai
             dense<WR, 1, 4, false>(Wr, colA, nullptr, &raw);
             const float q = act_sigma(raw);
             const float r = rel_contrib(a, i);
-            sumV += (double)(r * r / q);
-            sumC += (double)(a.cost_offset + q);
+            if (a.lw.active) {
+                const float lq = logf(q);
+                sumV += (double)(mu.var * (r * r / q));
+                sumC += (double)(mu.cost * (a.cost_offset + q));
+                sumR += (double)(mu.reg * (lq * lq));
+            } else {
+                sumV += (double)(r * r / q);
+                sumC += (double)(a.cost_offset + q);
+            }
         }
     }
     const double s0 = block_sum_d(lossS, red);
     const double s1 = block_sum_d(sumV, red);
     const double s2 = block_sum_d(sumC, red);
+    const double s3 = block_sum_d(sumR, red);
     if (threadIdx.x == 0) {
         a.part[4 * blockIdx.x + 0] = s0;
         a.part[4 * blockIdx.x + 1] = s1;
         a.part[4 * blockIdx.x + 2] = s2;
+        a.part[4 * blockIdx.x + 3] = s3;
     }
 }
 
@@ -313,12 +330,12 @@ template <int WR, int HR>
 __global__ void __launch_bounds__(kTT) k_train_rrs(const __grid_constant__ TrainArgs a) {
     constexpr int XW = WR > 64 ? WR : 64;
     extern __shared__ float smem[];
-    __shared__ double s_tot[3];
+    __shared__ double s_tot[4];
     float* colA = smem + threadIdx.x;
     float* colB = smem + XW * kTT + threadIdx.x;
     const int tid = threadIdx.x;
     const uint32_t ld = a.ld;
-    if (tid < 3) {
+    if (tid < 4) {
         double t = 0.0;
         for (uint32_t b = 0; b < a.part_n; ++b) t += a.part[4 * b + tid];
         s_tot[tid] = t;
@@ -327,7 +344,8 @@ __global__ void __launch_bounds__(kTT) k_train_rrs(const __grid_constant__ Train
     const double Vm = s_tot[1] / (double)a.n, Cm = s_tot[2] / (double)a.n;
     if (blockIdx.x == 0 && tid == 0) {
         a.loss_out[0] = s_tot[0] / (3.0 * (double)a.n);
-        a.loss_out[1] = a.train_rrs ? Vm * Cm : 0.0;
+        a.loss_out[1] = a.train_rrs ? (a.lw.active ? Vm * Cm + s_tot[3] / (double)a.n : Vm * Cm)
+                                    : 0.0;
     }
     if (!a.train_rrs) return;
     const float Vf = (float)Vm, Cf = (float)Cm;
@@ -358,7 +376,14 @@ __global__ void __launch_bounds__(kTT) k_train_rrs(const __grid_constant__ Train
         dense<WR, 1, 4, false>(Wt, colA, nullptr, &raw);
         const float q = act_sigma(raw);
         const float r = rel_contrib(a, i);
-        const float dq = (-(r * r) / (q * q) * Cf + Vf) / (float)a.n;
+        float dq;
+        if (a.lw.active) {
+            const SampleMul mu = sample_mul(a.lw, i, a.n);
+            dq = (mu.var * (-(r * r) / (q * q)) * Cf + mu.cost * Vf +
+                  mu.reg * (2.0f * logf(q) / q)) / (float)a.n;
+        } else {
+            dq = (-(r * r) / (q * q) * Cf + Vf) / (float)a.n;
+        }
         const float draw = dq * act_sigma_grad(raw);
         act[(size_t)a.r_draw * ld] = draw;
         // output layer W_out [1][WR]: d g_last = W_out^T draw masked by g_last
@@ -377,6 +402,52 @@ __global__ void __launch_bounds__(kTT) k_train_rrs(const __grid_constant__ Train
                                 act + (size_t)(a.r_dhr + (h - 1) * WR) * ld);
     }
 }
+
+// ---- batch sums of the loss weights (one block, fixed order: deterministic) ----
+// out[0] = sum s_i, out[1] = sum w_i, out[2] = the mean pixel error error_sum / n_pixels (1 when
+// no error sum is given)
+__global__ void __launch_bounds__(1024) k_loss_sums(const __grid_constant__ LossWeights w,
+                                                   uint32_t n, const float* error_sum,
+                                                   uint32_t n_pixels, double* out) {
+    __shared__ double red[2][32];
+    double s = 0.0, ww = 0.0;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        s += (double)loss_w_stat(w, i);
+        ww += (double)loss_w_rrs(w, i);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+        ww += __shfl_xor_sync(0xffffffffu, ww, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = s;
+        red[1][threadIdx.x >> 5] = ww;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double ts = 0.0, tw = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) ts += red[0][k], tw += red[1][k];
+        out[0] = ts;
+        out[1] = tw;
+        double em = 1.0;
+        if (error_sum && n_pixels) {
+            em = (double)*error_sum / (double)n_pixels;
+            if (!(em > 1e-30)) em = 1e-30;
+        }
+        out[2] = em;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_loss_sums(const LossWeights& w, uint32_t n, const float* error_sum,
+                             uint32_t n_pixels, double* out, cudaStream_t s) {
+    k_loss_sums<<<1, 1024, 0, s>>>(w, n, error_sum, n_pixels, out);
+    return cudaGetLastError();
+}
+
+namespace {
 
 // ---- weight gradients: dW[o][k] = sum_i D[o][i] * A[k][i] over the batch ----
 struct WJob {
@@ -605,7 +676,7 @@ cudaError_t launch_adam_step(nrrs_ctx* ctx, bool train_rrs, cudaStream_t s, floa
 bool train_tc_supported(const nrrs_config& c);
 size_t train_tc_scratch_bytes(const nrrs_config& c, uint32_t n, int sm_count);
 int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint32_t n,
-                  double* loss_dev, cudaStream_t s, bool apply);
+                  double* loss_dev, cudaStream_t s, bool apply, const LossWeights* lw);
 
 size_t train_scratch_bytes(const nrrs_config& c, uint32_t n, int sm_count) {
     if (train_tc_supported(c)) return train_tc_scratch_bytes(c, n, sm_count);
@@ -620,8 +691,9 @@ size_t train_scratch_bytes(const nrrs_config& c, uint32_t n, int sm_count) {
 }
 
 int train_step_impl(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint32_t n,
-                    double* loss_dev, cudaStream_t s, bool apply) {
-    if (train_tc_supported(ctx->cfg)) return train_step_tc(ctx, v, target, n, loss_dev, s, apply);
+                    double* loss_dev, cudaStream_t s, bool apply, const LossWeights* lw) {
+    if (train_tc_supported(ctx->cfg))
+        return train_step_tc(ctx, v, target, n, loss_dev, s, apply, lw);
     const nrrs_config& c = ctx->cfg;
     const Layout L = layout_of(c);
     const uint32_t ld = ld_of(c.max_train);
@@ -666,6 +738,7 @@ int train_step_impl(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uin
     a.r_x1 = L.r_x1; a.r_hr = L.r_hr; a.r_dhr = L.r_dhr; a.r_draw = L.r_draw;
     a.part = part;
     a.loss_out = loss_dev ? loss_dev : ctx->loss_dev;
+    if (lw) a.lw = *lw;
 
     if (c.statnet_width == 64 && c.statnet_hidden == 2)
         e = launch_train<64, 2, 64, 2>(ctx, a, s);

@@ -53,10 +53,11 @@ struct TcTrainArgs {
     Arr x0, hs[kMaxH], dhs[kMaxH], dy, x1, hr[kMaxH], dhr[kMaxH], draw;
     int32_t pre;            // the hash columns of the x0 tiles are already written (k_encode_levels)
     float* dxs;             // when set: per-sample hash-lane gradients [n][32] out, no scatter here
-    double* part;           // [part_rows][4]: loss_S, V, C per CTA
+    double* part;           // [part_rows][4]: loss_S, V, C, R per CTA
     uint32_t part_rows;
     uint32_t part_used;     // rows the StatNet and RRSNet-forward grids write
     double* loss_out;
+    LossWeights lw;         // per-sample loss weights (inactive: plain means)
 };
 
 __device__ __forceinline__ uint8_t* tile_ptr(uint8_t* act, const Arr& r, uint32_t t) {
@@ -251,11 +252,17 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
         for (int k = 0; k < 16; ++k) dyv[k] = 0.f, x1[k] = 0.f;
         if (valid) {
             const size_t i3 = 3 * (size_t)i;
+            const float ws = a.lw.active ? sample_mul(a.lw, i, a.n).stat : 1.f;
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 const float d = y[c] - logf(a.target[i3 + c] + a.fp.stat_eps);
-                lossS += (double)d * (double)d;
-                dyv[c] = 2.0f * d / 3.0f;
+                if (a.lw.active) {
+                    lossS += (double)ws * (double)d * (double)d;
+                    dyv[c] = ws * (2.0f * d / 3.0f);
+                } else {
+                    lossS += (double)d * (double)d;
+                    dyv[c] = 2.0f * d / 3.0f;
+                }
             }
             glue16(a.fp, y, a.v, i, x1);
         }
@@ -406,7 +413,7 @@ __global__ void __launch_bounds__(128, 1) k_ttc_rrs(const __grid_constant__ TcTr
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 3);
     __shared__ int s_abort;
     __shared__ double red[4];
-    __shared__ double s_tot[3];
+    __shared__ double s_tot[4];
     const int tid = threadIdx.x, warp = tid >> 5;
 
     if (tid == 0) {
@@ -419,21 +426,24 @@ __global__ void __launch_bounds__(128, 1) k_ttc_rrs(const __grid_constant__ TcTr
     if (BACKWARD) {
         // batch sums of the loss partials (rows written by the StatNet and forward launches),
         // in a fixed order, so every CTA holds the same V and C
-        double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+        double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
         for (uint32_t b = tid; b < a.part_used; b += 128) {
             t0 += a.part[4 * b + 0];
             t1 += a.part[4 * b + 1];
             t2 += a.part[4 * b + 2];
+            t3 += a.part[4 * b + 3];
         }
         t0 = block_sum_d(t0, red);
         t1 = block_sum_d(t1, red);
         t2 = block_sum_d(t2, red);
-        if (tid == 0) s_tot[0] = t0, s_tot[1] = t1, s_tot[2] = t2;
+        t3 = block_sum_d(t3, red);
+        if (tid == 0) s_tot[0] = t0, s_tot[1] = t1, s_tot[2] = t2, s_tot[3] = t3;
         __syncthreads();
         if (blockIdx.x == 0 && tid == 0) {
             const double Vm = s_tot[1] / (double)a.n, Cm = s_tot[2] / (double)a.n;
             a.loss_out[0] = s_tot[0] / (3.0 * (double)a.n);
-            a.loss_out[1] = a.train_rrs ? Vm * Cm : 0.0;
+            a.loss_out[1] = a.train_rrs ? (a.lw.active ? Vm * Cm + s_tot[3] / (double)a.n : Vm * Cm)
+                                        : 0.0;
         }
         if (!a.train_rrs) return;  // StatNet-only steps: losses are all this launch writes
     }
@@ -462,7 +472,7 @@ __global__ void __launch_bounds__(128, 1) k_ttc_rrs(const __grid_constant__ TcTr
 #pragma unroll
     for (int h = 2; h <= H; ++h) wF[h] = wF[h - 1] + W * W * 2;
 
-    double sumV = 0.0, sumC = 0.0;
+    double sumV = 0.0, sumC = 0.0, sumR = 0.0;
     const uint32_t tiles = (a.n + 127) / 128;
     for (uint32_t t = blockIdx.x; t < tiles && !flags; t += gridDim.x) {
         if (tid == 0) {
@@ -498,14 +508,23 @@ __global__ void __launch_bounds__(128, 1) k_ttc_rrs(const __grid_constant__ TcTr
         tc::tmem_wait_ld();
         const float raw = r16[0];
         float q = 0.f, r = 0.f;
+        SampleMul mu{1.f, 1.f, 1.f, 0.f};
         if (valid) {
             q = act_sigma(raw);
             r = rel_contrib_tc(a, i);
+            if (a.lw.active) mu = sample_mul(a.lw, i, a.n);
         }
         if (!BACKWARD) {
             if (valid) {
-                sumV += (double)(r * r / q);
-                sumC += (double)(a.cost_offset + q);
+                if (a.lw.active) {
+                    const float lq = logf(q);
+                    sumV += (double)(mu.var * (r * r / q));
+                    sumC += (double)(mu.cost * (a.cost_offset + q));
+                    sumR += (double)(mu.reg * (lq * lq));
+                } else {
+                    sumV += (double)(r * r / q);
+                    sumC += (double)(a.cost_offset + q);
+                }
             }
             tc::fence_before_sync();
             __syncthreads();
@@ -513,7 +532,13 @@ __global__ void __launch_bounds__(128, 1) k_ttc_rrs(const __grid_constant__ TcTr
             float dr[16];
 #pragma unroll
             for (int k = 0; k < 16; ++k) dr[k] = 0.f;
-            if (valid) dr[0] = (-(r * r) / (q * q) * Cf + Vf) * act_sigma_grad(raw);
+            if (valid) {
+                if (a.lw.active)
+                    dr[0] = (mu.var * (-(r * r) / (q * q)) * Cf + mu.cost * Vf +
+                             mu.reg * (2.0f * logf(q) / q)) * act_sigma_grad(raw);
+                else
+                    dr[0] = (-(r * r) / (q * q) * Cf + Vf) * act_sigma_grad(raw);
+            }
             store_chunk(sDR, tid, 0, 16, pack8<true>(dr));
             store_chunk(sDR, tid, 1, 16, pack8<true>(dr + 8));
             sync_for_mma();
@@ -546,9 +571,11 @@ __global__ void __launch_bounds__(128, 1) k_ttc_rrs(const __grid_constant__ TcTr
     if (!BACKWARD) {
         const double v = block_sum_d(sumV, red);
         const double c = block_sum_d(sumC, red);
+        const double rr = block_sum_d(sumR, red);
         if (tid == 0) {
             a.part[4 * blockIdx.x + 1] = v;
             a.part[4 * blockIdx.x + 2] = c;
+            a.part[4 * blockIdx.x + 3] = rr;
         }
     }
     if (tid == 0) tc::bulk_wait_all();
@@ -775,7 +802,7 @@ size_t train_tc_scratch_bytes(const nrrs_config& c, uint32_t n, int sm_count) {
 cudaError_t launch_wreduce(const float* partial, uint32_t chunks, uint32_t total, float* grad,
                            float scale, cudaStream_t s);
 int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint32_t n,
-                  double* loss_dev, cudaStream_t s, bool apply) {
+                  double* loss_dev, cudaStream_t s, bool apply, const LossWeights* lw) {
     const nrrs_config& c = ctx->cfg;
     const TcLayout L = tc_layout(c, c.max_train);
     const uint64_t chunks = (n + kTcChunk - 1) / kTcChunk;
@@ -823,6 +850,7 @@ int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint3
     a.part = part;
     a.part_rows = part_rows;
     a.loss_out = loss_dev ? loss_dev : ctx->loss_dev;
+    if (lw) a.lw = *lw;
     if (split) {
         // hash columns of the x0 tiles, level-major (FP16, the StatNet training precision)
         EncodeLvArgs ea{};

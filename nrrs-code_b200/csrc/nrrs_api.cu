@@ -479,6 +479,7 @@ int nrrs_create(const nrrs_config* cfg, nrrs_ctx** out) {
     ctx->states = reinterpret_cast<unsigned long long*>(ctx->scr + 1);
     NRRS_ALLOC(ctx->loss_dev, sizeof(double) * 2);
     NRRS_ALLOC(ctx->segs_dev, sizeof(SegmentTable) * 2);
+    NRRS_ALLOC(ctx->loss_sums, sizeof(double) * 4);
     ctx->train_scratch_bytes = train_scratch_bytes(c, c.max_train, ctx->sm_count);
     NRRS_ALLOC(ctx->train_scratch, ctx->train_scratch_bytes);
 #undef NRRS_ALLOC
@@ -539,6 +540,7 @@ void nrrs_destroy(nrrs_ctx* ctx) {
     cudaFree(ctx->scr);
     cudaFree(ctx->loss_dev);
     cudaFree(ctx->segs_dev);
+    cudaFree(ctx->loss_sums);
     cudaFree(ctx->train_scratch);
     delete ctx;
 }
@@ -788,6 +790,49 @@ int nrrs_adam_apply(nrrs_ctx* ctx, const float* grads_dev, float scale, void* st
     cudaError_t e = launch_adam_step(ctx, ctx->cfg.step >= 3, s, scale);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "adam launch");
     return refresh_derived(ctx, s, false);
+}
+
+void nrrs_loss_params_default(nrrs_loss_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->gamma1 = 1.0f;          // u = 1: the plain variance term
+    p->clamp_on = 0;
+    p->clamp_max = 10.0f;      // the reference's clamp_max (2net-simple.json)
+    p->n_pixels = 0;
+}
+
+int nrrs_train_step_batch(nrrs_ctx* ctx, const nrrs_train_batch* b, uint32_t n,
+                          const float* sample_weight, const float* error_sum_dev,
+                          const nrrs_loss_params* lp, double* loss_dev, void* stream) {
+    if (!ctx) return NRRS_ERR_INVALID_ARG;
+    if (!b || !lp) return fail(ctx, NRRS_ERR_INVALID_ARG, "batch/loss params are NULL");
+    if (!b->pos || !b->wi || !b->normal || !b->roughness || !b->albedo || !b->thp || !b->target)
+        return fail(ctx, NRRS_ERR_INVALID_ARG,
+                    "batch: pos/wi/normal/roughness/albedo/thp/target required");
+    if (n == 0 || n > ctx->cfg.max_train) return fail(ctx, NRRS_ERR_INVALID_ARG, "need 0 < n <= max_train");
+    if (!std::isfinite(lp->gamma1) || !std::isfinite(lp->gamma2) || !std::isfinite(lp->gamma3) ||
+        !std::isfinite(lp->gamma4) || (lp->clamp_on && !(lp->clamp_max > 0.f)))
+        return fail(ctx, NRRS_ERR_INVALID_ARG, "loss params: finite gammas, clamp_max > 0");
+    if (error_sum_dev && lp->n_pixels == 0)
+        return fail(ctx, NRRS_ERR_INVALID_ARG, "an error sum needs n_pixels");
+    VertexPtrs v{};
+    v.pos = b->pos; v.wi = b->wi; v.normal = b->normal; v.rough = b->roughness;
+    v.albedo = b->albedo; v.thp = b->thp; v.depth = b->depth; v.ref = b->ref_mean;
+    LossWeights lw{};
+    lw.active = 1;
+    lw.sample_weight = sample_weight;
+    lw.rrs_target = b->rrs_target;
+    lw.error = b->error;
+    lw.error_for_avg = b->error_for_avg;
+    lw.number_samples = b->number_samples;
+    lw.g1 = lp->gamma1; lw.g2 = lp->gamma2; lw.g3 = lp->gamma3; lw.g4 = lp->gamma4;
+    lw.clamp_on = lp->clamp_on;
+    lw.clamp_max = lp->clamp_max;
+    lw.sums = ctx->loss_sums;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = launch_loss_sums(lw, n, error_sum_dev, lp->n_pixels, ctx->loss_sums, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "loss weight sums");
+    return train_step_impl(ctx, v, b->target, n, loss_dev, s, true, &lw);
 }
 
 int nrrs_train_step(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* target, uint32_t n,

@@ -488,6 +488,71 @@ __device__ __forceinline__ float rrs_factor(const FactorParams& fp, const float*
     return rrs;
 }
 
+// ---- per-sample weights of the two losses (nrrs_train_step_batch) ----
+// The reference hands its losses per-sample side arrays (network.cpp:408-435, 532-557) whose
+// arithmetic lives in the absent tiny-cuda-nn fork. This build defines them (restated, unpinned):
+//   s_i   = sample_weight[i] (1 when absent)             the pixel share of the sample
+//   w_i   = s_i, or 0 where rrs_target[i] < 0            (the -1 mark, train.cu:520-523)
+//   e_i   = error[i] / e_mean, a_i = error_for_avg[i] / e_mean (1 when absent), each clamped to
+//           clamp_max when clamp_on; e_mean = error_sum / n_pixels
+//   u_i   = gamma1 + gamma2 e_i + gamma3 a_i             error emphasis of the variance term
+//   k_i   = max(number_samples[i], 1) (1 when absent)    samples averaged by the pixel
+//   loss_S = sum_i s_i sum_c d_ic^2 / (3 sum s)
+//   V = sum w u r^2 / (k q) / sum w,  C = sum w (cost_offset + q) / sum w,
+//   R = sum w (ln q)^2 / sum w,  loss_R = V C + gamma4 R
+// The kernels keep their per-sample form with 1/n applied later, so each sample carries the
+// multipliers below, relative to the batch mean (n / sum s, n / sum w).
+struct LossWeights {
+    int32_t active;                  // 0: plain means (every multiplier 1, reg 0)
+    const float* sample_weight;
+    const float* rrs_target;
+    const float* error;
+    const float* error_for_avg;
+    const float* number_samples;
+    float g1, g2, g3, g4;
+    int32_t clamp_on;
+    float clamp_max;
+    const double* sums;              // [sum s, sum w, e_mean] from k_loss_sums
+};
+
+struct SampleMul {
+    float stat;   // StatNet term
+    float var;    // variance term of the RRSNet loss
+    float cost;   // cost term
+    float reg;    // gamma4 x regulariser
+};
+
+__device__ __forceinline__ float loss_w_stat(const LossWeights& w, uint32_t i) {
+    return w.sample_weight ? w.sample_weight[i] : 1.0f;
+}
+__device__ __forceinline__ float loss_w_rrs(const LossWeights& w, uint32_t i) {
+    const float s = loss_w_stat(w, i);
+    return (w.rrs_target && w.rrs_target[i] < 0.f) ? 0.f : s;
+}
+
+__device__ __forceinline__ SampleMul sample_mul(const LossWeights& w, uint32_t i, uint32_t n) {
+    SampleMul m{1.f, 1.f, 1.f, 0.f};
+    if (!w.active) return m;
+    const double sum_s = w.sums[0], sum_w = w.sums[1];
+    const float emean = (float)w.sums[2];
+    const float rs = sum_s > 0.0 ? (float)((double)n / sum_s) : 0.f;
+    const float rw = sum_w > 0.0 ? (float)((double)n / sum_w) : 0.f;
+    const float s = loss_w_stat(w, i), ww = loss_w_rrs(w, i);
+    float e = w.error ? w.error[i] / emean : 1.f;
+    float ea = w.error_for_avg ? w.error_for_avg[i] / emean : 1.f;
+    if (w.clamp_on) {
+        e = fminf(e, w.clamp_max);
+        ea = fminf(ea, w.clamp_max);
+    }
+    const float u = w.g1 + w.g2 * e + w.g3 * ea;
+    const float k = w.number_samples ? fmaxf(w.number_samples[i], 1.f) : 1.f;
+    m.stat = s * rs;
+    m.var = ww * rw * u / k;
+    m.cost = ww * rw;
+    m.reg = w.g4 * ww * rw;
+    return m;
+}
+
 // status sink for kernels launched without a context scratch
 static __device__ unsigned int g_dummy_status;
 

@@ -110,6 +110,13 @@ class TrainBatch(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in TRAIN_BATCH_FIELDS]
 
 
+class LossParams(C.Structure):
+    """nrrs_loss_params: the RRSNet loss settings of nrrs_train_step_batch"""
+    _fields_ = [("gamma1", C.c_float), ("gamma2", C.c_float), ("gamma3", C.c_float),
+                ("gamma4", C.c_float), ("clamp_on", C.c_int32), ("clamp_max", C.c_float),
+                ("n_pixels", C.c_uint32)]
+
+
 class RaySoA(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("origin", "dir", "thp", "pdf", "pixel", "node")]
 
@@ -186,6 +193,10 @@ _SIGS = {
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                            C.c_void_p, C.c_void_p]),
     "nrrs_noalloc_device_status": (C.c_int, [C.POINTER(C.c_uint32), C.c_void_p]),
+    "nrrs_loss_params_default": (None, [C.POINTER(LossParams)]),
+    "nrrs_train_step_batch": (C.c_int, [C.c_void_p, C.POINTER(TrainBatch), C.c_uint32,
+                                        C.c_void_p, C.c_void_p, C.POINTER(LossParams),
+                                        C.c_void_p, C.c_void_p]),
     "nrrs_infer_dev": (C.c_int, [C.c_void_p, C.POINTER(VertexSoA), C.c_void_p, C.c_uint32,
                                  C.POINTER(DecideParams), C.c_void_p, C.c_void_p, C.c_void_p]),
     "nrrs_decide_emit_dev": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -490,6 +501,15 @@ def _check(rc: int, what: str):
 def path_nodes_bytes(capacity: int, max_record: int) -> int:
     """Bytes of the device block of a node buffer (nrrs_path_nodes_bytes)."""
     return lib().nrrs_path_nodes_bytes(capacity, max_record)
+
+
+def default_loss_params(**kw) -> LossParams:
+    """nrrs_loss_params_default (gamma 1, 0, 0, 0, no clamp: nrrs_train_step's loss), then kw."""
+    p = LossParams()
+    lib().nrrs_loss_params_default(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
 
 
 def default_train_data_params(**kw) -> TrainDataParams:
@@ -1007,6 +1027,14 @@ class NRRSNetwork:
             self._h, C.byref(soa), _ptr(rnd), arr, _ptr(counts_dev), len(segments),
             C.byref(params), _ptr(stats), _ptr(rrs), _ptr(rrs_norm), _ptr(split), _ptr(queue),
             _ptr(next_size), stream))
+
+    def trainStepBatch(self, batch: TrainBatch, n: int, sample_weight, error_sum_dev,
+                       params: LossParams, loss_dev=None, stream=0):
+        """nrrs_train_step_batch: NRRSNetwork::train on a training batch with the reference's
+        per-sample loss inputs"""
+        return self._check(lib().nrrs_train_step_batch(
+            self._h, C.byref(batch), n, _ptr(sample_weight), _ptr(error_sum_dev),
+            C.byref(params), _ptr(loss_dev), stream))
 
     def train(self, soa: VertexSoA, target, n: int, loss_dev=None, stream=0):
         return self._check(lib().nrrs_train_step(self._h, C.byref(soa), _ptr(target), n,

@@ -204,18 +204,37 @@ void oracle_train_grads_f64(const nrrs_config* cfg, const float* params, uint64_
                             const nrrs_vertex_soa* v, const float* target, double* grads,
                             double* loss) {
     double* pd = promote(params, oracle_param_count(cfg, NULL, NULL, NULL));
-    train_impl_f64(cfg, pd, n, v, target, grads, loss);
+    train_impl_f64(cfg, pd, n, v, target, grads, loss, NULL);
     free(pd);
 }
 void oracle_train_grads_f32(const nrrs_config* cfg, const float* params, uint64_t n,
                             const nrrs_vertex_soa* v, const float* target, float* grads,
                             double* loss) {
-    train_impl_f32(cfg, params, n, v, target, grads, loss);
+    train_impl_f32(cfg, params, n, v, target, grads, loss, NULL);
+}
+/* the same with the per-sample loss weights of nrrs_train_step_batch */
+void oracle_train_grads_w_f64(const nrrs_config* cfg, const float* params, uint64_t n,
+                              const nrrs_vertex_soa* v, const float* target,
+                              const oracle_loss_w* w, double* grads, double* loss) {
+    double* pd = promote(params, oracle_param_count(cfg, NULL, NULL, NULL));
+    train_impl_f64(cfg, pd, n, v, target, grads, loss, w);
+    free(pd);
+}
+void oracle_train_grads_w_f32(const nrrs_config* cfg, const float* params, uint64_t n,
+                              const nrrs_vertex_soa* v, const float* target,
+                              const oracle_loss_w* w, float* grads, double* loss) {
+    train_impl_f32(cfg, params, n, v, target, grads, loss, w);
 }
 
 /* losses only, FP64 parameters (finite differences perturb them in FP64) */
 void oracle_train_loss_f64(const nrrs_config* cfg, const double* params, uint64_t n,
                            const nrrs_vertex_soa* v, const float* target, double* loss) {
+    oracle_train_loss_w_f64(cfg, params, n, v, target, NULL, loss);
+}
+
+void oracle_train_loss_w_f64(const nrrs_config* cfg, const double* params, uint64_t n,
+                             const nrrs_vertex_soa* v, const float* target,
+                             const oracle_loss_w* w, double* loss) {
     level_t lv[32];
     const uint64_t tab = build_levels(cfg, lv);
     const double* table = params;
@@ -223,28 +242,33 @@ void oracle_train_loss_f64(const nrrs_config* cfg, const double* params, uint64_
     const double* Wr = Ws + statnet_params(cfg);
     const int ws = cfg->statnet_width, wr = cfg->rrsnet_width;
     const int hs = cfg->statnet_hidden, hr = cfg->rrsnet_hidden;
-    double lossS = 0, sumV = 0, sumC = 0;
-#pragma omp parallel for schedule(static) reduction(+ : lossS, sumV, sumC)
+    double lossS = 0, sumV = 0, sumC = 0, sumR = 0, sum_s = 0, sum_w = 0;
+#pragma omp parallel for schedule(static) reduction(+ : lossS, sumV, sumC, sumR, sum_s, sum_w)
     for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
         const uint64_t i = (uint64_t)ii;
         double x0[64], acts[4 * 128], y[3], x1[16], g[4 * 128], raw;
+        const double sw = lw_s_f64(w, i), ww = lw_w_f64(w, i);
+        sum_s += sw;
+        sum_w += ww;
         build_x0_f64(cfg, lv, table, v, i, x0, NULL, NULL);
         mlp_fwd_f64(Ws, 64, ws, hs, 3, x0, acts, y);
         for (int c = 0; c < 3; ++c) {
             const double d = y[c] - log((double)target[3 * i + c] + (double)cfg->stat_eps);
-            lossS += d * d;
+            lossS += sw * d * d;
         }
         if (cfg->step >= 3) {
             glue_f64(cfg, y, v, i, x1);
             mlp_fwd_f64(Wr, 16, wr, hr, 1, x1, g, &raw);
             const double q = act_sigma_f64(raw);
             const double r = rel_contrib_f64(cfg, v, target, i);
-            sumV += r * r / q;
-            sumC += (double)cfg->cost_offset + q;
+            sumV += ww * lw_u_f64(w, i) * r * r / (lw_k_f64(w, i) * q);
+            sumC += ww * ((double)cfg->cost_offset + q);
+            sumR += ww * log(q) * log(q);
         }
     }
-    loss[0] = lossS / (3.0 * (double)n);
-    loss[1] = cfg->step >= 3 ? (sumV / (double)n) * (sumC / (double)n) : 0.0;
+    const double g4 = w ? (double)w->gamma4 : 0.0;
+    loss[0] = lossS / (3.0 * sum_s);
+    loss[1] = cfg->step >= 3 ? (sumV / sum_w) * (sumC / sum_w) + g4 * sumR / sum_w : 0.0;
 }
 
 /* ---- exact normalisation sum (replaces calcSum2PassAsync<true>, commoncudautilshost.cpp:6-22,

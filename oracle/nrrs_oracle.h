@@ -68,6 +68,20 @@ uint64_t oracle_decide_emit_acc(const float* rrs, const float* rnd, const uint32
                                 float* rrs_norm, uint8_t* split, uint32_t* queue,
                                 uint64_t capacity, uint32_t* status_flags);
 
+/* per-sample loss weights of nrrs_train_step_batch (include/nrrs.h gives the definition); any
+ * array may be NULL (absent) */
+typedef struct {
+    const float* sample_weight;
+    const float* rrs_target;
+    const float* error;
+    const float* error_for_avg;
+    const float* number_samples;
+    double error_mean;             /* error_sum / n_pixels, or 1 */
+    float gamma1, gamma2, gamma3, gamma4;
+    int32_t clamp_on;
+    float clamp_max;
+} oracle_loss_w;
+
 /* training: losses and gradients (no update). grads has nrrs_param_count entries.
  * loss[0] = StatNet relative log-L2, loss[1] = RRSNet variance x cost (0 when step < 3). */
 void oracle_train_grads_f64(const nrrs_config* cfg, const float* params, uint64_t n,
@@ -76,6 +90,15 @@ void oracle_train_grads_f64(const nrrs_config* cfg, const float* params, uint64_
 void oracle_train_grads_f32(const nrrs_config* cfg, const float* params, uint64_t n,
                             const nrrs_vertex_soa* v, const float* target, float* grads,
                             double* loss);
+void oracle_train_grads_w_f64(const nrrs_config* cfg, const float* params, uint64_t n,
+                              const nrrs_vertex_soa* v, const float* target,
+                              const oracle_loss_w* w, double* grads, double* loss);
+void oracle_train_grads_w_f32(const nrrs_config* cfg, const float* params, uint64_t n,
+                              const nrrs_vertex_soa* v, const float* target,
+                              const oracle_loss_w* w, float* grads, double* loss);
+void oracle_train_loss_w_f64(const nrrs_config* cfg, const double* params, uint64_t n,
+                             const nrrs_vertex_soa* v, const float* target,
+                             const oracle_loss_w* w, double* loss);
 /* loss only (for finite differences), FP64 */
 void oracle_train_loss_f64(const nrrs_config* cfg, const double* params, uint64_t n,
                            const nrrs_vertex_soa* v, const float* target, double* loss);

@@ -253,6 +253,29 @@ static REAL FN(rel_contrib)(const nrrs_config* cfg, const nrrs_vertex_soa* v, co
     return r < (REAL)cfg->loss_clamp_max ? r : (REAL)cfg->loss_clamp_max;
 }
 
+/* per-sample loss weights of nrrs_train_step_batch (the definition in include/nrrs.h):
+ * stat weight s, RRSNet weight w (0 for a -1 RRSNet target), error emphasis u, sample count k */
+static REAL FN(lw_s)(const oracle_loss_w* w, uint64_t i) {
+    return (w && w->sample_weight) ? (REAL)w->sample_weight[i] : (REAL)1;
+}
+static REAL FN(lw_w)(const oracle_loss_w* w, uint64_t i) {
+    return (w && w->rrs_target && w->rrs_target[i] < 0.f) ? (REAL)0 : FN(lw_s)(w, i);
+}
+static REAL FN(lw_u)(const oracle_loss_w* w, uint64_t i) {
+    if (!w) return 1;
+    REAL e = w->error ? (REAL)w->error[i] / (REAL)w->error_mean : (REAL)1;
+    REAL a = w->error_for_avg ? (REAL)w->error_for_avg[i] / (REAL)w->error_mean : (REAL)1;
+    if (w->clamp_on) {
+        e = e < (REAL)w->clamp_max ? e : (REAL)w->clamp_max;
+        a = a < (REAL)w->clamp_max ? a : (REAL)w->clamp_max;
+    }
+    return (REAL)w->gamma1 + (REAL)w->gamma2 * e + (REAL)w->gamma3 * a;
+}
+static REAL FN(lw_k)(const oracle_loss_w* w, uint64_t i) {
+    if (!w || !w->number_samples) return 1;
+    return w->number_samples[i] > 1.f ? (REAL)w->number_samples[i] : (REAL)1;
+}
+
 /* Losses and gradients of one training step (no update).
  * StatNet: loss_S = 1/(3n) sum_i sum_c (y_ic - log(L_ic + stat_eps))^2   (relative log-L2)
  * RRSNet:  q_i = activationSigma(raw_i), a_i = rel_contrib_i^2,
@@ -260,7 +283,7 @@ static REAL FN(rel_contrib)(const nrrs_config* cfg, const nrrs_vertex_soa* v, co
  *          RRSNet inputs come from the (detached) StatNet forward of the same step. */
 static void FN(train_impl)(const nrrs_config* cfg, const REAL* params, uint64_t n,
                             const nrrs_vertex_soa* v, const float* target, REAL* grads,
-                            double* loss) {
+                            double* loss, const oracle_loss_w* w) {
     level_t lv[32];
     uint64_t tab = build_levels(cfg, lv);
     const uint64_t np_table = tab * 2, np_stat = statnet_params(cfg), np_rrs = rrsnet_params(cfg);
@@ -272,11 +295,21 @@ static void FN(train_impl)(const nrrs_config* cfg, const REAL* params, uint64_t 
     const int hs = cfg->statnet_hidden, hr = cfg->rrsnet_hidden;
     const int train_rrs = cfg->step >= 3;
     memset(grads, 0, sizeof(REAL) * np);
-    double lossS = 0, sumV = 0, sumC = 0;
+    double lossS = 0, sumV = 0, sumC = 0, sumR = 0;
+    /* weighted losses: the batch sums of the weights, and the divisors of the means */
+    double sum_s = (double)n, sum_w = (double)n;
+    if (w) {
+        sum_s = 0;
+        sum_w = 0;
+        for (uint64_t i = 0; i < n; ++i) {
+            sum_s += (double)FN(lw_s)(w, i);
+            sum_w += (double)FN(lw_w)(w, i);
+        }
+    }
 
     /* pass 1: RRSNet forward for the batch sums V and C */
     if (train_rrs) {
-#pragma omp parallel for schedule(static) reduction(+ : sumV, sumC)
+#pragma omp parallel for schedule(static) reduction(+ : sumV, sumC, sumR)
         for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
             const uint64_t i = (uint64_t)ii;
             REAL x0[64], acts[4 * 128], y[3], x1[16], g[4 * 128], raw;
@@ -286,11 +319,19 @@ static void FN(train_impl)(const nrrs_config* cfg, const REAL* params, uint64_t 
             FN(mlp_fwd)(Wr, 16, wr, hr, 1, x1, g, &raw);
             const REAL q = FN(act_sigma)(raw);
             const REAL r = FN(rel_contrib)(cfg, v, target, i);
-            sumV += (double)(r * r / q);
-            sumC += (double)((REAL)cfg->cost_offset + q);
+            if (w) {
+                const REAL ww = FN(lw_w)(w, i), lq = R_LOG(q);
+                sumV += (double)(ww * FN(lw_u)(w, i) * r * r / (FN(lw_k)(w, i) * q));
+                sumC += (double)(ww * ((REAL)cfg->cost_offset + q));
+                sumR += (double)(ww * lq * lq);
+            } else {
+                sumV += (double)(r * r / q);
+                sumC += (double)((REAL)cfg->cost_offset + q);
+            }
         }
     }
-    const double Vm = sumV / (double)n, Cm = sumC / (double)n;
+    const double Vm = sumV / sum_w, Cm = sumC / sum_w, Rm = sumR / sum_w;
+    const double g4 = w ? (double)w->gamma4 : 0.0;
 
     /* pass 2: per-sample backward */
     int nt = 1;
@@ -314,11 +355,17 @@ static void FN(train_impl)(const nrrs_config* cfg, const REAL* params, uint64_t 
             uint32_t cidx[16 * 8];
             FN(build_x0)(cfg, lv, table, v, i, x0, cidx, cw);
             FN(mlp_fwd)(Ws, 64, ws, hs, 3, x0, acts, y);
+            const REAL sw = FN(lw_s)(w, i);
             for (int c = 0; c < 3; ++c) {
                 const REAL t = R_LOG((REAL)target[3 * i + c] + (REAL)cfg->stat_eps);
                 const REAL d = y[c] - t;
-                lossS += (double)(d * d);
-                dy[c] = (REAL)2 * d / ((REAL)3 * (REAL)n);
+                if (w) {
+                    lossS += (double)(sw * d * d);
+                    dy[c] = (REAL)2 * sw * d / ((REAL)3 * (REAL)sum_s);
+                } else {
+                    lossS += (double)(d * d);
+                    dy[c] = (REAL)2 * d / ((REAL)3 * (REAL)n);
+                }
             }
             FN(mlp_bwd)(Ws, 64, ws, hs, 3, x0, acts, dy, dWs, dx0);
             for (int l = 0; l < cfg->n_levels; ++l)
@@ -337,7 +384,14 @@ static void FN(train_impl)(const nrrs_config* cfg, const REAL* params, uint64_t 
                 FN(mlp_fwd)(Wr, 16, wr, hr, 1, x1, g, &raw);
                 const REAL q = FN(act_sigma)(raw);
                 const REAL r = FN(rel_contrib)(cfg, v, target, i);
-                const REAL dq = (-(r * r) / (q * q) * (REAL)Cm + (REAL)Vm) / (REAL)n;
+                REAL dq;
+                if (w) {
+                    const REAL ww = FN(lw_w)(w, i);
+                    dq = (ww * FN(lw_u)(w, i) * (-(r * r)) / (FN(lw_k)(w, i) * q * q) * (REAL)Cm +
+                          ww * (REAL)Vm + (REAL)g4 * ww * (REAL)2 * R_LOG(q) / q) / (REAL)sum_w;
+                } else {
+                    dq = (-(r * r) / (q * q) * (REAL)Cm + (REAL)Vm) / (REAL)n;
+                }
                 draw = dq * FN(act_sigma_grad)(raw);
                 FN(mlp_bwd)(Wr, 16, wr, hr, 1, x1, g, &draw, dWr, NULL);
             }
@@ -346,8 +400,8 @@ static void FN(train_impl)(const nrrs_config* cfg, const REAL* params, uint64_t 
     for (int t = 0; t < nt; ++t)
         for (uint64_t k = 0; k < np_mlp; ++k) grads[np_table + k] += priv[(uint64_t)t * np_mlp + k];
     free(priv);
-    loss[0] = lossS / (3.0 * (double)n);
-    loss[1] = train_rrs ? Vm * Cm : 0.0;
+    loss[0] = lossS / (3.0 * sum_s);
+    loss[1] = train_rrs ? Vm * Cm + g4 * Rm : 0.0;
 }
 
 #undef R_EXP

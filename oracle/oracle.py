@@ -73,6 +73,11 @@ def lib():
                                       vp, vp, vp]
         L.oracle_train_loss_f64.argtypes = [C.POINTER(nb.Config), vp, C.c_uint64,
                                             C.POINTER(nb.VertexSoA), vp, vp]
+        for f in ("oracle_train_grads_w_f64", "oracle_train_grads_w_f32"):
+            getattr(L, f).argtypes = [C.POINTER(nb.Config), vp, C.c_uint64, C.POINTER(nb.VertexSoA),
+                                      vp, C.POINTER(LossW), vp, vp]
+        L.oracle_train_loss_w_f64.argtypes = [C.POINTER(nb.Config), vp, C.c_uint64,
+                                              C.POINTER(nb.VertexSoA), vp, C.POINTER(LossW), vp]
         L.oracle_adam_f32.argtypes = [C.POINTER(nb.Config), vp, vp, vp, vp, C.c_uint64,
                                       C.c_uint64, C.c_uint64]
         L.oracle_fixed_limbs.argtypes = [C.c_float, vp]
@@ -287,32 +292,63 @@ def decide_emit_acc(rrs, rnd, budget, n_specular, dp, acc: int, shift: int, capa
             "split": split[:n], "flags": int(flags.value)}
 
 
-def train_grads(cfg, params, v: dict, target, precision: str = "f64", out=None):
+class LossW(C.Structure):
+    """oracle_loss_w: the per-sample loss weights of nrrs_train_step_batch"""
+    _fields_ = [("sample_weight", C.c_void_p), ("rrs_target", C.c_void_p), ("error", C.c_void_p),
+                ("error_for_avg", C.c_void_p), ("number_samples", C.c_void_p),
+                ("error_mean", C.c_double), ("gamma1", C.c_float), ("gamma2", C.c_float),
+                ("gamma3", C.c_float), ("gamma4", C.c_float), ("clamp_on", C.c_int32),
+                ("clamp_max", C.c_float)]
+
+
+def loss_weights(arrays: dict, gammas=(1.0, 0.0, 0.0, 0.0), clamp_on=0, clamp_max=10.0,
+                 error_mean=1.0):
+    """LossW over host arrays (kept alive by the returned tuple's second element)."""
+    keep = {k: np.ascontiguousarray(arrays[k], np.float32) for k in
+            ("sample_weight", "rrs_target", "error", "error_for_avg", "number_samples")
+            if arrays.get(k) is not None}
+    w = LossW(*(keep[k].ctypes.data if k in keep else None for k in
+                ("sample_weight", "rrs_target", "error", "error_for_avg", "number_samples")),
+              float(error_mean), *map(float, gammas), int(clamp_on), float(clamp_max))
+    return w, keep
+
+
+def train_grads(cfg, params, v: dict, target, precision: str = "f64", out=None, weights=None):
     """(gradients, losses); out, when given, is a reused gradient array of the right size and
-    precision (the oracle clears it itself)."""
+    precision (the oracle clears it itself); weights: a LossW (loss_weights()) for the weighted
+    losses of nrrs_train_step_batch."""
     n = v["pos"].shape[0]
     npar = param_count(cfg)[0]
     dt = np.float64 if precision == "f64" else np.float32
     g = out if out is not None else np.empty(npar, dt)
     assert g.dtype == dt and g.size == npar
     loss = np.zeros(2, np.float64)
-    f = lib().oracle_train_grads_f64 if precision == "f64" else lib().oracle_train_grads_f32
     params = np.ascontiguousarray(params, np.float32)
     target = np.ascontiguousarray(target, np.float32)
     soa = _soa(v)
-    f(C.byref(cfg), params.ctypes.data, n, C.byref(soa), target.ctypes.data, g.ctypes.data,
-      loss.ctypes.data)
+    if weights is None:
+        f = lib().oracle_train_grads_f64 if precision == "f64" else lib().oracle_train_grads_f32
+        f(C.byref(cfg), params.ctypes.data, n, C.byref(soa), target.ctypes.data, g.ctypes.data,
+          loss.ctypes.data)
+    else:
+        f = lib().oracle_train_grads_w_f64 if precision == "f64" else lib().oracle_train_grads_w_f32
+        f(C.byref(cfg), params.ctypes.data, n, C.byref(soa), target.ctypes.data,
+          C.byref(weights), g.ctypes.data, loss.ctypes.data)
     return g, loss
 
 
-def train_loss(cfg, params64, v: dict, target):
+def train_loss(cfg, params64, v: dict, target, weights=None):
     n = v["pos"].shape[0]
     loss = np.zeros(2, np.float64)
     params64 = np.ascontiguousarray(params64, np.float64)
     target = np.ascontiguousarray(target, np.float32)
     soa = _soa(v)
-    lib().oracle_train_loss_f64(C.byref(cfg), params64.ctypes.data, n, C.byref(soa),
-                                target.ctypes.data, loss.ctypes.data)
+    if weights is None:
+        lib().oracle_train_loss_f64(C.byref(cfg), params64.ctypes.data, n, C.byref(soa),
+                                    target.ctypes.data, loss.ctypes.data)
+    else:
+        lib().oracle_train_loss_w_f64(C.byref(cfg), params64.ctypes.data, n, C.byref(soa),
+                                      target.ctypes.data, C.byref(weights), loss.ctypes.data)
     return loss
 
 

@@ -181,3 +181,93 @@ def test_split_training_equals_fused(shape):
     rc, flags = net.device_status(stream())
     assert rc == nb.OK and flags == 0
     net.close()
+
+
+def _batch_dev(v, extra):
+    torch = torch_cuda()
+    d = upload(v)
+    arrays = {k: d[k] for k in ("pos", "wi", "normal", "roughness", "albedo", "thp", "depth",
+                                "ref_mean", "target")}
+    for k, a in extra.items():
+        arrays[k] = torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+    return arrays
+
+
+def _weighted_arrays(n, seed):
+    rng = np.random.default_rng(seed)
+    rt = rng.uniform(0.1, 3.0, n).astype(np.float32)
+    rt[rng.random(n) < 0.25] = -1.0
+    return {"rrs_target": rt, "error": rng.uniform(0.0, 4.0, n).astype(np.float32),
+            "error_for_avg": rng.uniform(0.0, 6.0, n).astype(np.float32),
+            "number_samples": rng.integers(0, 9, n).astype(np.float32)}, \
+        rng.uniform(0.1, 1.0, n).astype(np.float32)
+
+
+@pytest.mark.parametrize("prec", [nb.PREC_FP32, nb.PREC_FP16, nb.PREC_BF16],
+                         ids=["fp32", "fp16", "bf16"])
+def test_train_step_batch_weighted_losses_vs_fp64_oracle(prec):
+    """nrrs_train_step_batch with every per-sample side array, the error sum and the shipped
+    gammas: losses and gradients (before the update) against the FP64 oracle's weighted losses."""
+    torch = torch_cuda()
+    net = make_net(precision=prec, max_train=1 << 14, step=3, log2_hashmap_size=16)
+    p0 = random_params(net, 41, table_scale=0.5, mlp_scale=0.15)
+    n = 6000
+    v = nb.synth(42, n)
+    extra, sw = _weighted_arrays(n, 43)
+    b = _batch_dev(v, extra)
+    n_pix = 1500
+    esum = 2.5 * n_pix
+    d_esum = torch.tensor([esum], dtype=torch.float32, device="cuda")
+    lp = nb.default_loss_params(gamma1=0.01, gamma2=0.05, gamma3=0.02, gamma4=0.01, clamp_on=1,
+                                clamp_max=3.0, n_pixels=n_pix)
+    loss = torch.zeros(2, dtype=torch.float64, device="cuda")
+    net.trainStepBatch(nb.train_batch(**b), n, torch.from_numpy(sw).cuda(), d_esum, lp, loss,
+                       stream())
+    torch.cuda.synchronize()
+    g = net.get_grads().astype(np.float64)
+    ov = dict(v)
+    ov.update(extra)
+    ov["sample_weight"] = sw
+    w, keep = O.loss_weights(ov, gammas=(0.01, 0.05, 0.02, 0.01), clamp_on=1, clamp_max=3.0,
+                             error_mean=esum / n_pix)
+    g64, l64 = O.train_grads(net.config, p0, v, v["target"], "f64", weights=w)
+    l = loss.cpu().numpy()
+    fp32 = prec == nb.PREC_FP32
+    assert l[0] == pytest.approx(l64[0], rel=1e-5 if fp32 else 1e-4)
+    assert l[1] == pytest.approx(l64[1], rel=1e-4 if fp32 else 2e-3)
+    ntab, nst, nrr = net.param_layout()
+    bars = ({"table": 2e-4, "statnet": 2e-4, "rrsnet": 2e-4} if fp32 else
+            {"table": 4e-2, "statnet": 1.5e-2, "rrsnet": 1.5e-2})
+    for name, sl in (("table", slice(0, ntab)), ("statnet", slice(ntab, ntab + nst)),
+                     ("rrsnet", slice(ntab + nst, ntab + nst + nrr))):
+        e = rel_err(g[sl], g64[sl])
+        assert e < bars[name], (name, e)
+    rc, flags = net.device_status(stream())
+    assert rc == nb.OK and flags == 0
+    net.close()
+
+
+@pytest.mark.parametrize("prec", [nb.PREC_FP32, nb.PREC_FP16], ids=["fp32", "fp16"])
+def test_train_step_batch_defaults_equal_train_step(prec):
+    """with no side arrays and the default loss parameters the batch step is nrrs_train_step"""
+    torch = torch_cuda()
+    n = 5000
+    v = nb.synth(44, n)
+    out = []
+    for batch_form in (False, True):
+        net = make_net(precision=prec, max_train=1 << 13, step=3, log2_hashmap_size=15)
+        random_params(net, 45, table_scale=0.5, mlp_scale=0.15)
+        b = _batch_dev(v, {})
+        loss = torch.zeros(2, dtype=torch.float64, device="cuda")
+        if batch_form:
+            net.trainStepBatch(nb.train_batch(**b), n, None, None, nb.default_loss_params(),
+                               loss, stream())
+        else:
+            net.train(soa(b), b["target"], n, loss, stream())
+        torch.cuda.synchronize()
+        out.append((loss.cpu().numpy(), net.get_grads().astype(np.float64), net.get_params()))
+        net.close()
+    (la, ga, pa), (lb, gb, pb) = out
+    assert np.allclose(la, lb, rtol=1e-6, atol=0)
+    assert rel_err(gb, ga) < 1e-6
+    assert np.allclose(pa, pb, rtol=1e-5, atol=1e-7)

@@ -22,8 +22,9 @@ from test_gpu_render import (empty_hits, empty_rays, empty_shadow, empty_vertice
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("closed", [False, True], ids=["open", "closed"])
-def test_gpu_training_frame_matches_oracle(closed):
+def run_training_frame(closed):
+    """The frame on the GPU and in the C restatement; returns the GPU node block, the host
+    nodes, the rendered image (RGBA per pixel), the pixel count and the node capacity."""
     torch = torch_cuda()
     gs, hs = scene_pair(11, boxes=60, closed=closed)
     cam = nb.room_camera(48, 36, inside=closed)
@@ -103,6 +104,13 @@ def test_gpu_training_frame_matches_oracle(closed):
     assert host(film).tobytes() == hfilm.tobytes()
     himg = hs.resolve(hfilm, 1.0)
     image = np.concatenate([himg, np.ones((n, 1), np.float32)], axis=1)
+    return g, hn, image, n, node_cap
+
+
+@pytest.mark.parametrize("closed", [False, True], ids=["open", "closed"])
+def test_gpu_training_frame_matches_oracle(closed):
+    torch = torch_cuda()
+    g, hn, image, n, node_cap = run_training_frame(closed)
 
     # the node buffers
     size, dropped, flags = g.pn.status(stream())
@@ -323,4 +331,82 @@ def test_gpu_ubs_search_drives_rendered_frames():
     best, eff = lib.best()
     assert best == oracle.array[:max_depth] and np.float32(eff) == oracle.best_eff
     assert not lib.searching
+    net.close()
+
+
+@pytest.mark.parametrize("prec", [nb.PREC_FP32, nb.PREC_FP16], ids=["fp32", "fp16"])
+def test_gpu_records_batch_feeds_weighted_training_step(prec):
+    """trainStep end to end on the device: the training batch built from this frame's nodes
+    (with the per-pixel error arrays and sample counts of the error image gathered into it, the
+    -1 RRSNet targets of later siblings, the sample weights and the error sum) goes straight into
+    nrrs_train_step_batch with the reference's shipped loss settings (gamma 0.01 / 0.05 / 0 /
+    0.01, clamp on at 10). Losses and gradients equal the FP64 oracle's weighted losses on the
+    oracle's own batch."""
+    torch = torch_cuda()
+    g, hn, image, n, node_cap = run_training_frame(False)
+    rng = np.random.default_rng(90)
+    err = rng.uniform(0.0, 3.0, 2 * n).astype(np.float32)
+    err[rng.random(2 * n) < 0.02] = 40.0          # a few pixels far above the clamp
+    spp = rng.integers(1, 9, n).astype(np.float32)
+    d_err, d_spp = torch.from_numpy(err).cuda(), torch.from_numpy(spp).cuda()
+    prm = nb.default_train_data_params(copy_rrs_node=1, dedupe_rrs_target=1,
+                                       error_per_pixel=d_err.data_ptr(),
+                                       samples_per_patch=d_spp.data_ptr())
+    cap = node_cap
+    f32 = lambda *s: torch.zeros(*s, dtype=torch.float32, device="cuda")   # noqa: E731
+    i32 = lambda *s: torch.zeros(*s, dtype=torch.int32, device="cuda")     # noqa: E731
+    out = {"pos": f32(cap, 3), "wi": f32(cap, 3), "normal": f32(cap, 3), "albedo": f32(cap, 3),
+           "roughness": f32(cap), "thp": f32(cap, 3), "depth": i32(cap), "ref_mean": f32(cap),
+           "target": f32(cap, 3), "rrs_target": f32(cap), "pixel": i32(cap), "error": f32(cap),
+           "error_for_avg": f32(cap), "number_samples": f32(cap)}
+    counts = i32(n)
+    size = i32(1)
+    img = torch.from_numpy(image).cuda()
+    g.pn.generate_training_data(prm, nb.train_batch(**out), cap, size, image=img,
+                                image_channels=4, n_pixels=n, pixel_samples=counts,
+                                stream=stream())
+    weights = f32(cap)
+    nb.calculate_sample_weight(out["pixel"], counts, n, size, cap, weights, stream())
+    total = int(host(size)[0])
+    m = min(total, 8192)
+    assert m > 1000
+    esum = float(np.sum(err[n:].astype(np.float64)))
+    d_esum = torch.tensor([esum], dtype=torch.float32, device="cuda")
+    lp = nb.default_loss_params(gamma1=0.01, gamma2=0.05, gamma3=0.0, gamma4=0.01, clamp_on=1,
+                                clamp_max=10.0, n_pixels=n)
+    net = make_net(max_train=1 << 13, step=3, log2_hashmap_size=15, precision=prec)
+    p0 = random_params(net, 5, table_scale=0.5, mlp_scale=0.15)
+    loss = torch.zeros(2, dtype=torch.float64, device="cuda")
+    net.trainStepBatch(nb.train_batch(**out), m, weights, d_esum, lp, loss, stream())
+    torch.cuda.synchronize()
+    gg = net.get_grads().astype(np.float64)
+    rc, flags = net.device_status(stream())
+    assert rc == nb.OK and flags == 0
+
+    # the oracle's batch, weights and error sum from the C restatement of the same frame
+    prm_h = nb.default_train_data_params(copy_rrs_node=1, dedupe_rrs_target=1,
+                                         error_per_pixel=err.ctypes.data,
+                                         samples_per_patch=spp.ctypes.data)
+    hcounts = np.zeros(n, np.uint32)
+    hbatch, htotal = hn.generate(prm_h, node_cap, image=image, n_pixels=n, pixel_samples=hcounts)
+    assert htotal == total
+    hw = O.sample_weights(hbatch["pixel"], hcounts, n)
+    ob = {k: np.ascontiguousarray(hbatch[k][:m]) for k in hbatch}
+    assert (ob["rrs_target"] < 0).any() and (ob["error"] > 0).any()
+    for k in ("error", "error_for_avg", "number_samples", "rrs_target", "thp", "target"):
+        assert host(out[k]).reshape(cap, -1)[:m].tobytes() == ob[k].reshape(m, -1).tobytes(), k
+    ob["sample_weight"] = hw[:m]
+    w, keep = O.loss_weights(ob, gammas=(0.01, 0.05, 0.0, 0.01), clamp_on=1, clamp_max=10.0,
+                             error_mean=float(np.float32(esum)) / n)
+    g64, l64 = O.train_grads(net.config, p0, ob, ob["target"], "f64", weights=w)
+    l = host(loss)
+    assert l[0] == pytest.approx(l64[0], rel=1e-4 if prec == nb.PREC_FP32 else 1e-3)
+    assert l[1] == pytest.approx(l64[1], rel=1e-4 if prec == nb.PREC_FP32 else 2e-3)
+    ntab, nst, nrr = net.param_layout()
+    bars = ({"table": 2e-4, "statnet": 2e-4, "rrsnet": 2e-4} if prec == nb.PREC_FP32 else
+            {"table": 5e-2, "statnet": 2e-2, "rrsnet": 2e-2})
+    for name, sl in (("table", slice(0, ntab)), ("statnet", slice(ntab, ntab + nst)),
+                     ("rrsnet", slice(ntab + nst, ntab + nst + nrr))):
+        e = np.linalg.norm(gg[sl] - g64[sl]) / max(np.linalg.norm(g64[sl]), 1e-30)
+        assert e < bars[name], (name, e)
     net.close()

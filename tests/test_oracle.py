@@ -330,3 +330,64 @@ def test_oracle_defaults_and_generator_agree_with_library():
     va, vb = O.synth(3, 70_000, first=1234), nb.synth(3, 70_000, first=1234)
     for k in va:
         assert np.array_equal(va[k], vb[k]), k
+
+
+def _weighted_case(n, seed):
+    rng = np.random.default_rng(seed)
+    rt = rng.uniform(0.1, 3.0, n).astype(np.float32)
+    rt[rng.random(n) < 0.25] = -1.0                       # duplicate siblings: no RRSNet term
+    arrays = {"sample_weight": rng.uniform(0.1, 1.0, n), "rrs_target": rt,
+              "error": rng.uniform(0.0, 4.0, n), "error_for_avg": rng.uniform(0.0, 6.0, n),
+              "number_samples": rng.integers(0, 9, n).astype(np.float32)}
+    return O.loss_weights(arrays, gammas=(0.3, 0.5, 0.2, 0.1), clamp_on=1, clamp_max=4.0,
+                          error_mean=1.7)
+
+
+def test_weighted_losses_default_equal_plain_losses():
+    """nrrs_train_step_batch's losses with no side arrays and gamma (1, 0, 0, 0) are the plain
+    losses of nrrs_train_step."""
+    cfg = small_cfg(step=3)
+    v = nb.synth(9, 400)
+    p = rand_params(cfg, 9, 0.3)
+    w, _ = O.loss_weights({})
+    g0, l0 = O.train_grads(cfg, p, v, v["target"], "f64")
+    g1, l1 = O.train_grads(cfg, p, v, v["target"], "f64", weights=w)
+    assert np.allclose(l0, l1, rtol=1e-13, atol=0)
+    assert np.allclose(g0, g1, rtol=1e-11, atol=1e-15)
+    assert np.allclose(O.train_loss(cfg, p.astype(np.float64), v, v["target"], weights=w), l0,
+                       rtol=1e-13)
+
+
+def test_weighted_losses_fd_gradients_fp64():
+    """central finite differences (h = 1e-3, FP64) of the weighted losses on 256 parameters"""
+    cfg = small_cfg(step=3)
+    n = 96
+    v = nb.synth(6, n)
+    tgt = v["target"]
+    p = rand_params(cfg, 6, 0.3)
+    w, keep = _weighted_case(n, 7)
+    g, loss = O.train_grads(cfg, p, v, tgt, "f64", weights=w)
+    assert np.allclose(O.train_loss(cfg, p.astype(np.float64), v, tgt, weights=w), loss,
+                       rtol=1e-12)
+    ntab, nst, nrr = O.param_count(cfg)[1:]
+    rng = np.random.default_rng(8)
+    touched = np.nonzero(g[:ntab])[0]
+    picks = np.concatenate([rng.choice(touched, 96, replace=False),
+                            ntab + rng.choice(nst, 96, replace=False),
+                            ntab + nst + rng.choice(nrr, 64, replace=False)])
+    p64 = p.astype(np.float64)
+    for k in picks:
+        which = 1 if k >= ntab + nst else 0
+        for h in (1e-3, 1e-6):
+            floor = 1e-11 * max(1.0, loss[which]) / h
+            q = p64.copy()
+            q[k] += h
+            lp = O.train_loss(cfg, q, v, tgt, weights=w)[which]
+            q[k] -= 2 * h
+            lm = O.train_loss(cfg, q, v, tgt, weights=w)[which]
+            fd = (lp - lm) / (2 * h)
+            tol = (1e-3 if h == 1e-3 else 1e-4) * max(abs(fd), abs(g[k])) + floor
+            if abs(fd - g[k]) <= tol:
+                break
+        else:
+            raise AssertionError((int(k), fd, g[k]))
