@@ -42,7 +42,7 @@
 extern "C" {
 #endif
 
-#define NRRS_ABI_VERSION 1
+#define NRRS_ABI_VERSION 2
 
 /* ---- status codes (the reference has none: Log(Fatal) aborts, overflow only printf's) ---- */
 typedef enum {
@@ -109,7 +109,26 @@ typedef struct {
     uint32_t max_queue;            /* largest n for infer/decide        */
     uint32_t max_train;            /* largest batch for nrrs_train_step */
     int32_t step;                  /* setStep: 0..3 (network.cpp:578-589) */
+    /* network family (nrrs_network_family): NRRS_NET_WORKLOAD or NRRS_NET_REFERENCE; fill the
+     * reference family with nrrs_config_reference_network */
+    int32_t network;
 } nrrs_config;
+
+/* The two network families.
+ * NRRS_NET_WORKLOAD: the benchmark workload's network. StatNet input 64 lanes (16-level hash
+ *   grid, SH degree 4 of wi, normal, albedo, warped roughness, a bias lane); ReLU MLPs 64 or 128
+ *   wide; 3 log-statistics log(L + stat_eps); RRSNet input [bc(L) x3, bc(thp) x3, warped
+ *   roughness, bc(ref_mean), depth / 8, 1, 0 x6].
+ * NRRS_NET_REFERENCE: the network the reference ships (common/configs/nrrs/nrrs/2net-simple.json
+ *   level0/level1, myNetworkLL2.h:86, train.cu:41-112). StatNet input 32 lanes: HashGrid 8 levels
+ *   x 2 features, base 16, scale 2.0 (16 lanes), OneBlob 4 bins on each lat-long coordinate of wi
+ *   (8 lanes), OneBlob 8 bins on the warped roughness (8 lanes); no bias lane. LeakyReLU (slope
+ *   0.01) MLPs 32 wide x 3 hidden layers; 6 outputs L RGB and L^2 RGB (L2_OFFSET 3). RRSNet
+ *   input [bc(max(L,0)) x3, bc(max(L^2,0)) x3, bc(thp) x3, warped roughness, bc(ref_mean), 1,
+ *   0 x4]. The StatNet loss is the relative squared error of L and L^2 against the target L and
+ *   its square, (y - T)^2 / (T^2 + 0.01), averaged over the 6 outputs (the reference's NRRS_LL2
+ *   lives in its absent tiny-cuda-nn fork). */
+typedef enum { NRRS_NET_WORKLOAD = 0, NRRS_NET_REFERENCE = 1 } nrrs_network_family;
 
 /* Input record of one path vertex, SoA (NRRSInferenceWorkItem, src/render/nrrs/workitem.h:9-15,
  * extended with the fields of the synthetic benchmark record). vec3 fields are [n][3] float. */
@@ -151,6 +170,10 @@ typedef struct nrrs_ctx nrrs_ctx;
 
 /* ---- lifetime ---- */
 void nrrs_config_default(nrrs_config* cfg);
+/* the reference's shipped network (NRRS_NET_REFERENCE) with its grid, widths and optimizer
+ * settings (2net-simple.json: HashGrid 8 x 2, 2^19, base 16, scale 2.0; 32 x 3; Adam lr 5e-3,
+ * beta 0.9 / 0.99, eps 1e-15, l2 3e-6); the other fields keep nrrs_config_default's values */
+void nrrs_config_reference_network(nrrs_config* cfg);
 /* NRRSNetwork::NRRSNetwork + reset + resize (network.cpp:443-576, 351-441). */
 int nrrs_create(const nrrs_config* cfg, nrrs_ctx** out);
 void nrrs_destroy(nrrs_ctx* ctx);

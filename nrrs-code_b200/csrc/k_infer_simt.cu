@@ -16,104 +16,35 @@
 // is accumulated as fmaf(w_k, x_k, acc) over k ascending, the same sequence for any launch shape.
 // The narrow layers (3 and 1 outputs), the glue, the factor and the exact-sum term run one thread
 // per vertex on that vertex's column of the tile.
-#include "kernels.hpp"
+#include "simt_gemm.cuh"
 
 namespace nrrs {
 
 namespace {
 
-constexpr int kTM = 64;        // vertices per work item (half of a segment-table tile)
-// row stride of the activation tile: 4 floats of padding keep float4 alignment and spread the
-// epilogue's stores (neuron rows 4 apart) over twice as many banks
-constexpr int kLd = kTM + 4;
-constexpr int kThr = 128;      // threads per CTA
-constexpr int kKC = 32;        // weight rows per chunk
-
-constexpr int pad4(int x) { return (x + 3) / 4 * 4; }
-constexpr int imax(int a, int b) { return a > b ? a : b; }
+using simt::kLd;
+using simt::kThr;
+using simt::kTM;
 
 template <int W>
 struct FpShape {
-    static constexpr int kRows = imax(kStatIn, W);                 // rows of the activation tile
+    static constexpr int kRows = simt::imax(kStatIn, W);           // rows of the activation tile
     static constexpr int kActFloats = kRows * kLd;
-    static constexpr int kChunkFloats = kKC * W;
+    static constexpr int kChunkFloats = simt::kKC * W;
     static constexpr size_t kSmem = sizeof(float) * (kActFloats + 2 * kChunkFloats);
 };
 
-__device__ __forceinline__ void cp_async16(float* smem_dst, const float* gmem_src) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
-
-// rows x W floats of a transposed weight matrix into a shared-memory chunk
-template <int W>
-__device__ __forceinline__ void load_chunk(float* dst, const float* __restrict__ src, int rows,
-                                           int tid) {
-    const int n4 = rows * (W / 4);
-    for (int q = tid; q < n4; q += kThr) cp_async16(dst + 4 * q, src + 4 * q);
-}
-
-// out[n][m] = max(0, sum_k wt[k][n] act[k][m]) for k < k_eff, in place on the activation tile
-// (every read of the layer's input ends at the chunk loop's last barrier, before any write).
+// out[n][m] = max(0, sum_k wt[k][n] act[k][m]) for k < k_eff, in place on the activation tile;
 // wt is [k_rows][W] in global memory; rows k_eff .. k_rows-1 are loaded but multiply zeros.
 template <int W>
 __device__ __forceinline__ void hidden_layer(const float* __restrict__ wt, int k_rows, int k_eff,
                                              float* act, float* wch, int tid) {
-    constexpr int C = W / 16;                 // neurons per thread: 8 (W = 128) or 4 (W = 64)
-    const int lane = tid & 31, warp = tid >> 5;
-    const int tx = lane & 15, ty = warp * 2 + (lane >> 4);   // ty 0..7: vertices ty*8 .. +7
-    float acc[8][C];
+    simt::tile_gemm<W>(wt, k_rows, k_eff, act, wch, tid, [&](int n, int m0, const float* v) {
+        float r[8];
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < C; ++j) acc[i][j] = 0.f;
-    const int nch = (k_rows + kKC - 1) / kKC;
-    load_chunk<W>(wch, wt, k_rows < kKC ? k_rows : kKC, tid);
-    cp_async_commit();
-#pragma unroll 1
-    for (int c = 0; c < nch; ++c) {
-        if (c + 1 < nch) {
-            const int r = k_rows - (c + 1) * kKC;
-            load_chunk<W>(wch + ((c + 1) & 1) * kKC * W, wt + (size_t)(c + 1) * kKC * W,
-                          r < kKC ? r : kKC, tid);
-        }
-        cp_async_commit();
-        cp_async_wait1();   // every group but the newest: chunk c has landed
-        __syncthreads();
-        const float* B = wch + (c & 1) * kKC * W + tx * 4;
-        const float* A = act + (size_t)(c * kKC) * kLd + ty * 8;
-        const int kn = k_eff - c * kKC < kKC ? k_eff - c * kKC : kKC;
-#pragma unroll 4
-        for (int kk = 0; kk < kn; ++kk) {
-            const float4 a0 = *reinterpret_cast<const float4*>(A + kk * kLd);
-            const float4 a1 = *reinterpret_cast<const float4*>(A + kk * kLd + 4);
-            const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-            float bv[C];
-            const float4 b0 = *reinterpret_cast<const float4*>(B + kk * W);
-            bv[0] = b0.x; bv[1] = b0.y; bv[2] = b0.z; bv[3] = b0.w;
-            if constexpr (C == 8) {
-                const float4 b1 = *reinterpret_cast<const float4*>(B + kk * W + 64);
-                bv[4] = b1.x; bv[5] = b1.y; bv[6] = b1.z; bv[7] = b1.w;
-            }
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-#pragma unroll
-                for (int j = 0; j < C; ++j) acc[i][j] = fmaf(bv[j], av[i], acc[i][j]);
-        }
-        __syncthreads();    // the buffer read here is refilled by the next iteration's prefetch
-    }
-#pragma unroll
-    for (int j = 0; j < C; ++j) {
-        const int n = (j < 4 ? 0 : 64) + tx * 4 + (j & 3);
-        float* o = act + (size_t)n * kLd + ty * 8;
-        *reinterpret_cast<float4*>(o) = make_float4(fmaxf(acc[0][j], 0.f), fmaxf(acc[1][j], 0.f),
-                                                    fmaxf(acc[2][j], 0.f), fmaxf(acc[3][j], 0.f));
-        *reinterpret_cast<float4*>(o + 4) = make_float4(fmaxf(acc[4][j], 0.f), fmaxf(acc[5][j], 0.f),
-                                                        fmaxf(acc[6][j], 0.f), fmaxf(acc[7][j], 0.f));
-    }
-    __syncthreads();
+        for (int i = 0; i < 8; ++i) r[i] = fmaxf(v[i], 0.f);
+        simt::tile_store8(act, n, m0, r);
+    });
 }
 
 // the network's narrow output layer for vertex column m: y[o] = sum_k wt[k][o] act[k][m]

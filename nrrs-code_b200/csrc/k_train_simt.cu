@@ -20,12 +20,13 @@
 //   k_wreduce     chunk partials -> gradients, in fixed order (deterministic).
 //   k_adam        Adam on FP32 master weights/moments; writes the FP16 table copy in the same pass.
 #include "context.hpp"
+#include "simt_gemm.cuh"
 
 namespace nrrs {
 
 namespace {
 
-constexpr int kTT = 128;           // samples per tile (threads per CTA)
+constexpr int kTT = 128;           // threads per CTA of the training kernels
 constexpr int kChunk = 2048;       // samples per weight-gradient partial
 constexpr int kMaxJobs = 8;
 
@@ -52,66 +53,6 @@ struct TrainArgs {
     LossWeights lw;                // per-sample loss weights (inactive: plain means)
 };
 
-// out_col[o] = sum_k W[k][o] * in_col[k] (Wt stored [IN][OUTP]); columns of this thread in smem
-template <int IN, int OUT, int OUTP, bool RELU>
-__device__ __forceinline__ void dense(const float* __restrict__ Wt, const float* in_col,
-                                      float* out_col, float* out_reg) {
-    float acc[OUT];
-#pragma unroll
-    for (int o = 0; o < OUT; ++o) acc[o] = 0.f;
-#pragma unroll 2
-    for (int k = 0; k < IN; ++k) {
-        const float xk = in_col[k * kTT];
-        const float4* w4 = reinterpret_cast<const float4*>(Wt + k * OUTP);
-#pragma unroll
-        for (int o4 = 0; o4 < OUTP / 4; ++o4) {
-            const float4 w = w4[o4];
-            if (4 * o4 + 0 < OUT) acc[4 * o4 + 0] = fmaf(w.x, xk, acc[4 * o4 + 0]);
-            if (4 * o4 + 1 < OUT) acc[4 * o4 + 1] = fmaf(w.y, xk, acc[4 * o4 + 1]);
-            if (4 * o4 + 2 < OUT) acc[4 * o4 + 2] = fmaf(w.z, xk, acc[4 * o4 + 2]);
-            if (4 * o4 + 3 < OUT) acc[4 * o4 + 3] = fmaf(w.w, xk, acc[4 * o4 + 3]);
-        }
-    }
-#pragma unroll
-    for (int o = 0; o < OUT; ++o) {
-        const float r = RELU ? fmaxf(acc[o], 0.f) : acc[o];
-        if (out_col) out_col[o * kTT] = r;
-        if (out_reg) out_reg[o] = r;
-    }
-}
-
-// backward through one layer with a row-major W [OUTF][INF]:
-// out_col[k] = sum_o W[o][k] * din[o]   (din: smem column), optionally masked by act > 0
-template <int OUTF, int INF, int INF_EFF>
-__device__ __forceinline__ void dense_t(const float* __restrict__ W, const float* din_col,
-                                        float* dout_col, const float* mask_g, uint32_t ld,
-                                        float* dout_g) {
-    // W rows are contiguous in k: treat W as "Wt" with IN = OUTF rows of INF outputs
-    float acc[INF_EFF];
-#pragma unroll
-    for (int k = 0; k < INF_EFF; ++k) acc[k] = 0.f;
-#pragma unroll 2
-    for (int o = 0; o < OUTF; ++o) {
-        const float d = din_col[o * kTT];
-        const float* wr = W + o * INF;
-#pragma unroll
-        for (int k4 = 0; k4 < INF_EFF / 4; ++k4) {
-            const float4 w = reinterpret_cast<const float4*>(wr)[k4];
-            acc[4 * k4 + 0] = fmaf(w.x, d, acc[4 * k4 + 0]);
-            acc[4 * k4 + 1] = fmaf(w.y, d, acc[4 * k4 + 1]);
-            acc[4 * k4 + 2] = fmaf(w.z, d, acc[4 * k4 + 2]);
-            acc[4 * k4 + 3] = fmaf(w.w, d, acc[4 * k4 + 3]);
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < INF_EFF; ++k) {
-        float g = acc[k];
-        if (mask_g && !(mask_g[(size_t)k * ld] > 0.f)) g = 0.f;
-        if (dout_col) dout_col[k * kTT] = g;
-        if (dout_g) dout_g[(size_t)k * ld] = g;
-    }
-}
-
 __device__ __forceinline__ double block_sum_d(double v, double* red) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -136,181 +77,248 @@ __device__ __forceinline__ float rel_contrib(const TrainArgs& a, uint32_t i) {
     return r < a.loss_clamp ? r : a.loss_clamp;
 }
 
+using simt::kLd;
+using simt::kTM;
+
+// activation tile rows and weight-chunk floats of the training kernels
+template <int W>
+struct TrShape {
+    static constexpr int kRows = simt::imax(kStatIn, W);
+    static constexpr int kChunk = simt::kKC * simt::imax(64, W);
+    static constexpr size_t kSmem = sizeof(float) * ((size_t)kRows * kLd + 2 * kChunk);
+};
+
+// forward layer: ReLU in place, and the activations to scratch rows row0 + n (samples i0 ..)
+template <int W>
+__device__ __forceinline__ void fwd_layer(const float* __restrict__ wt, int k_rows, int k_eff,
+                                          float* tile, float* wch, int tid, float* scr,
+                                          uint32_t ld, uint32_t i0, uint32_t row0, bool store) {
+    simt::tile_gemm<W>(wt, k_rows, k_eff, tile, wch, tid, [&](int n, int m0, const float* v) {
+        float r[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) r[i] = fmaxf(v[i], 0.f);
+        simt::tile_store8(tile, n, m0, r);
+        if (store) {
+            float* g = scr + (size_t)(row0 + n) * ld + i0 + m0;
+            *reinterpret_cast<float4*>(g) = make_float4(r[0], r[1], r[2], r[3]);
+            *reinterpret_cast<float4*>(g + 4) = make_float4(r[4], r[5], r[6], r[7]);
+        }
+    });
+}
+
+// backward layer through row-major W [k_rows = outputs of the forward layer][W = its inputs]:
+// delta_in[n][m] = (sum_k W[k][n] delta_out[k][m]) masked by the forward activation stored in
+// scratch rows mask0 + n; in place, and to scratch rows out0 + n
+template <int W>
+__device__ __forceinline__ void bwd_layer(const float* __restrict__ w, int k_rows, float* tile,
+                                          float* wch, int tid, float* scr, uint32_t ld, uint32_t i0,
+                                          uint32_t mask0, uint32_t out0) {
+    simt::tile_gemm<W>(w, k_rows, k_rows, tile, wch, tid, [&](int n, int m0, const float* v) {
+        const float* h = scr + (size_t)(mask0 + n) * ld + i0 + m0;
+        const float4 h0 = *reinterpret_cast<const float4*>(h);
+        const float4 h1 = *reinterpret_cast<const float4*>(h + 4);
+        const float hv[8] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
+        float r[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) r[i] = hv[i] > 0.f ? v[i] : 0.f;
+        simt::tile_store8(tile, n, m0, r);
+        float* g = scr + (size_t)(out0 + n) * ld + i0 + m0;
+        *reinterpret_cast<float4*>(g) = make_float4(r[0], r[1], r[2], r[3]);
+        *reinterpret_cast<float4*>(g + 4) = make_float4(r[4], r[5], r[6], r[7]);
+    });
+}
+
+// y[o] = sum_k wt[k][o] tile[k][m] for a narrow output layer (wt [W][4])
+template <int W, int OUT>
+__device__ __forceinline__ void narrow_out(const float* __restrict__ wt, const float* tile, int m,
+                                           float* y) {
+    float acc[OUT];
+#pragma unroll
+    for (int o = 0; o < OUT; ++o) acc[o] = 0.f;
+#pragma unroll 4
+    for (int k = 0; k < W; ++k) {
+        const float x = tile[k * kLd + m];
+        const float4 w = __ldg(reinterpret_cast<const float4*>(wt + 4 * k));
+        acc[0] = fmaf(w.x, x, acc[0]);
+        if (OUT > 1) acc[1] = fmaf(w.y, x, acc[1]);
+        if (OUT > 2) acc[2] = fmaf(w.z, x, acc[2]);
+    }
+#pragma unroll
+    for (int o = 0; o < OUT; ++o) y[o] = acc[o];
+}
+
+// The StatNet step and the RRSNet forward sums on 64-sample tiles (128 threads): encoding (two
+// threads per sample), the forward layers as tile GEMMs storing every activation, the loss
+// gradient, the backward layers as tile GEMMs through the row-major weights (masks from the
+// stored activations), the input gradient of the 32 hash lanes, the hash-grid scatter (two
+// threads per sample, eight levels each), then the glue and the RRSNet forward for the sums.
 template <int WS, int HS, int WR, int HR>
-__global__ void __launch_bounds__(kTT) k_train_stat(const __grid_constant__ TrainArgs a) {
-    constexpr int XW = WS > 64 ? WS : 64;
-    extern __shared__ float smem[];
+__global__ void __launch_bounds__(simt::kThr) k_train_stat(const __grid_constant__ TrainArgs a) {
+    static_assert(WS == WR, "one tile shape for both networks");
+    using S = TrShape<WS>;
+    extern __shared__ float4 smem4[];
+    float* tile = reinterpret_cast<float*>(smem4);
+    float* wch = tile + S::kRows * kLd;
     __shared__ double red[kTT / 32];
-    float* colA = smem + threadIdx.x;            // activations
-    float* colB = smem + XW * kTT + threadIdx.x; // deltas
     const int tid = threadIdx.x;
+    const int m = tid & (kTM - 1);
+    const bool lead = tid < kTM;
+    const int half = tid >> 6;
     const uint32_t ld = a.ld;
+    float* scr = a.act;
     double lossS = 0.0, sumV = 0.0, sumC = 0.0, sumR = 0.0;
     const float2* table = reinterpret_cast<const float2*>(a.table);
-    const uint32_t tiles = (a.n + kTT - 1) / kTT;
-    for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-        const uint32_t i = t * kTT + tid;
-        if (i >= a.n) continue;
-        float* act = a.act + i;
-        // ---- encode (StatNet input lanes 0..55) ----
-        float p[3];
-        norm_pos(a.enc, a.v.pos, i, p);
-#pragma unroll 2
-        for (int l = 0; l < kMaxLevels; ++l) {
-            const LevelDev L = a.enc.lv[l];
-            const CellCoord c = cell_of(p, L.res);
-            float f0 = 0.f, f1 = 0.f;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const uint32_t row = grid_row(L, a.enc.hash_mask, c.ix + (k & 1),
-                                              c.iy + ((k >> 1) & 1), c.iz + ((k >> 2) & 1));
-                const float2 tv = __ldg(table + row);
-                const float w = corner_weight(c, k);
-                f0 += w * tv.x;
-                f1 += w * tv.y;
-            }
-            colA[(2 * l) * kTT] = f0;
-            colA[(2 * l + 1) * kTT] = f1;
-        }
-        {
-            float sh[16], m[16];
-            const size_t i3 = 3 * (size_t)i;
-            sh16(a.v.wi[i3], a.v.wi[i3 + 1], a.v.wi[i3 + 2], sh);
-#pragma unroll
-            for (int k = 0; k < 16; ++k) colA[(32 + k) * kTT] = sh[k];
-            misc_lanes(a.v, i, m);
-#pragma unroll
-            for (int k = 0; k < 8; ++k) colA[(48 + k) * kTT] = m[k];
-        }
-#pragma unroll 4
-        for (int k = 0; k < 56; ++k) act[(size_t)(a.r_x0 + k) * ld] = colA[k * kTT];
-
-        // ---- StatNet forward, storing every hidden activation ----
-        const float* Wt = a.wt_stat;
-        dense<56, WS, WS, true>(Wt, colA, colA, nullptr);
-        Wt += kStatIn * WS;
-#pragma unroll 4
-        for (int k = 0; k < WS; ++k) act[(size_t)(a.r_hs + k) * ld] = colA[k * kTT];
+    // forward (transposed) and backward (row-major) layer images
+    const float* ts = a.wt_stat;
+    const float* ts_out = ts + (size_t)kStatIn * WS + (size_t)(HS - 1) * WS * WS;
+    const float* rs = a.w_stat;
+    const float* rs_out = rs + (size_t)kStatIn * WS + (size_t)(HS - 1) * WS * WS;   // [3][WS]
+    const float* tr = a.wt_rrs;
+    const float* tr_out = tr + (size_t)kRrsIn * WR + (size_t)(HR - 1) * WR * WR;
+    const uint32_t items = (a.n + kTM - 1) / kTM;
 #pragma unroll 1
-        for (int h = 1; h < HS; ++h) {
-            dense<WS, WS, WS, true>(Wt, colA, colA, nullptr);
-            Wt += WS * WS;
-#pragma unroll 4
-            for (int k = 0; k < WS; ++k) act[(size_t)(a.r_hs + h * WS + k) * ld] = colA[k * kTT];
-        }
-        float y[3];
-        dense<WS, 3, 4, false>(Wt, colA, nullptr, y);
-
-        // ---- StatNet loss gradient ----
-        const size_t i3 = 3 * (size_t)i;
-        const SampleMul mu = sample_mul(a.lw, i, a.n);
+    for (uint32_t u = blockIdx.x; u < items; u += gridDim.x) {
+        const uint32_t i0 = u * kTM, i = i0 + m;
+        const bool valid = i < a.n;
+        __syncthreads();   // the previous tile's column reads are over
+        // ---- encode: lanes 0..55 of this sample's column (half 0: levels 0-7 + SH, 1: 8-15 +
+        //      misc), copied to the x0 scratch rows ----
+        float p[3] = {0.f, 0.f, 0.f};
+        if (valid) {
+            norm_pos(a.enc, a.v.pos, i, p);
+#pragma unroll 2
+            for (int l = half * 8; l < half * 8 + 8; ++l) {
+                const LevelDev L = a.enc.lv[l];
+                const CellCoord c = cell_of(p, L.res);
+                float f0 = 0.f, f1 = 0.f;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const float d = y[c] - logf(a.target[i3 + c] + a.fp.stat_eps);
-            float g;
-            if (a.lw.active) {
-                lossS += (double)mu.stat * (double)d * (double)d;
-                g = mu.stat * (2.0f * d) / (3.0f * (float)a.n);
+                for (int k = 0; k < 8; ++k) {
+                    const uint32_t row = grid_row(L, a.enc.hash_mask, c.ix + (k & 1),
+                                                  c.iy + ((k >> 1) & 1), c.iz + ((k >> 2) & 1));
+                    const float2 tv = __ldg(table + row);
+                    const float w = corner_weight(c, k);
+                    f0 += w * tv.x;
+                    f1 += w * tv.y;
+                }
+                tile[(2 * l) * kLd + m] = f0;
+                tile[(2 * l + 1) * kLd + m] = f1;
+            }
+            if (half == 0) {
+                float sh[16];
+                const size_t i3 = 3 * (size_t)i;
+                sh16(a.v.wi[i3], a.v.wi[i3 + 1], a.v.wi[i3 + 2], sh);
+#pragma unroll
+                for (int k = 0; k < 16; ++k) tile[(32 + k) * kLd + m] = sh[k];
             } else {
-                lossS += (double)d * (double)d;
-                g = 2.0f * d / (3.0f * (float)a.n);
+                float mm[16];
+                misc_lanes(a.v, i, mm);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) tile[(48 + k) * kLd + m] = mm[k];
             }
-            colB[c * kTT] = g;
-            act[(size_t)(a.r_dy + c) * ld] = g;
+            const int k0 = half ? 16 : 0, k1 = half ? 32 : 16;   // hash lanes of this half
+            for (int k = k0; k < k1; ++k) scr[(size_t)(a.r_x0 + k) * ld + i] = tile[k * kLd + m];
+            const int q0 = half ? 48 : 32, q1 = half ? 56 : 48;  // SH or misc lanes
+            for (int k = q0; k < q1; ++k) scr[(size_t)(a.r_x0 + k) * ld + i] = tile[k * kLd + m];
+        } else {
+            for (int k = half ? 28 : 0; k < (half ? 56 : 28); ++k) tile[k * kLd + m] = 0.f;
         }
 
-        // ---- backward to the hash lanes ----
-        // output layer: W_out [3][WS]; d h_last = W_out^T dy, masked by h_last (in colA)
-        const float* W = a.w_stat;
-        const float* Wl[4];
-        Wl[0] = W;
-        Wl[1] = W + kStatIn * WS;
-        for (int h = 2; h <= HS; ++h) Wl[h] = Wl[h - 1] + WS * WS;
-        {
-            float acc[WS];
-#pragma unroll
-            for (int k = 0; k < WS; ++k) acc[k] = 0.f;
-#pragma unroll
-            for (int o = 0; o < 3; ++o) {
-                const float d = colB[o * kTT];
-                const float* wr = Wl[HS] + o * WS;
-#pragma unroll
-                for (int k = 0; k < WS; ++k) acc[k] = fmaf(wr[k], d, acc[k]);
-            }
-#pragma unroll
-            for (int k = 0; k < WS; ++k) {
-                const float g = colA[k * kTT] > 0.f ? acc[k] : 0.f;
-                colB[k * kTT] = g;
-                act[(size_t)(a.r_dhs + (HS - 1) * WS + k) * ld] = g;
-            }
-        }
+        // ---- StatNet forward, every hidden activation to scratch ----
+        fwd_layer<WS>(ts, kStatIn, 56, tile, wch, tid, scr, ld, i0, a.r_hs, true);
 #pragma unroll 1
-        for (int h = HS - 1; h >= 1; --h) {
-            // d h_{h-1} = W_h^T d h_h masked by h_{h-1} (from scratch)
-            dense_t<WS, WS, WS>(Wl[h], colB, colB, act + (size_t)(a.r_hs + (h - 1) * WS) * ld, ld,
-                                act + (size_t)(a.r_dhs + (h - 1) * WS) * ld);
+        for (int h = 1; h < HS; ++h)
+            fwd_layer<WS>(ts + (size_t)kStatIn * WS + (size_t)(h - 1) * WS * WS, WS, WS, tile, wch,
+                          tid, scr, ld, i0, a.r_hs + h * WS, true);
+
+        // ---- output, loss gradient, and the delta of the last hidden layer (own column) ----
+        float y[3] = {0.f, 0.f, 0.f};
+        SampleMul mu{1.f, 1.f, 1.f, 0.f};
+        if (lead) {
+            narrow_out<WS, 3>(ts_out, tile, m, y);
+            float g[3] = {0.f, 0.f, 0.f};
+            if (valid) {
+                const size_t i3 = 3 * (size_t)i;
+                mu = sample_mul(a.lw, i, a.n);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const float d = y[c] - logf(a.target[i3 + c] + a.fp.stat_eps);
+                    if (a.lw.active) {
+                        lossS += (double)mu.stat * (double)d * (double)d;
+                        g[c] = mu.stat * (2.0f * d) / (3.0f * (float)a.n);
+                    } else {
+                        lossS += (double)d * (double)d;
+                        g[c] = 2.0f * d / (3.0f * (float)a.n);
+                    }
+                    scr[(size_t)(a.r_dy + c) * ld + i] = g[c];
+                }
+            }
+            // d h_last = W_out^T g, masked by h_last (this column of the tile)
+            float* dl = scr + (size_t)(a.r_dhs + (HS - 1) * WS) * ld + i;
+#pragma unroll 4
+            for (int k = 0; k < WS; ++k) {
+                float acc = 0.f;
+#pragma unroll
+                for (int o = 0; o < 3; ++o) acc = fmaf(rs_out[o * WS + k], g[o], acc);
+                const float dk = tile[k * kLd + m] > 0.f ? acc : 0.f;
+                tile[k * kLd + m] = dk;
+                if (valid) dl[(size_t)k * ld] = dk;
+            }
         }
-        // dx0 lanes 0..31 = W_0^T d h_0
-        float dx[32];
+
+        // ---- backward through the hidden layers, then the 32 hash-lane gradients ----
+#pragma unroll 1
+        for (int h = HS - 1; h >= 1; --h)
+            bwd_layer<WS>(rs + (size_t)kStatIn * WS + (size_t)(h - 1) * WS * WS, WS, tile, wch,
+                          tid, scr, ld, i0, a.r_hs + (h - 1) * WS, a.r_dhs + (h - 1) * WS);
+        simt::tile_gemm<64>(rs, WS, WS, tile, wch, tid, [&](int n, int m0, const float* v) {
+            simt::tile_store8(tile, n, m0, v);
+        });
+
+        // ---- hash-grid scatter: two threads per sample, eight levels each ----
         {
-#pragma unroll
-            for (int k = 0; k < 32; ++k) dx[k] = 0.f;
+            const unsigned lanes = valid_lanes(i0 + (uint32_t)(m & ~31), a.n);
+            if (valid) {
 #pragma unroll 2
-            for (int o = 0; o < WS; ++o) {
-                const float d = colB[o * kTT];
-                const float4* wr = reinterpret_cast<const float4*>(Wl[0] + o * kStatIn);
-#pragma unroll
-                for (int k4 = 0; k4 < 8; ++k4) {
-                    const float4 w = wr[k4];
-                    dx[4 * k4 + 0] = fmaf(w.x, d, dx[4 * k4 + 0]);
-                    dx[4 * k4 + 1] = fmaf(w.y, d, dx[4 * k4 + 1]);
-                    dx[4 * k4 + 2] = fmaf(w.z, d, dx[4 * k4 + 2]);
-                    dx[4 * k4 + 3] = fmaf(w.w, d, dx[4 * k4 + 3]);
+                for (int l = half * 8; l < half * 8 + 8; ++l) {
+                    const LevelDev L = a.enc.lv[l];
+                    const CellCoord c = cell_of(p, L.res);
+                    warp_scatter_level(a.table_grad, L, a.enc.hash_mask, c, tile[(2 * l) * kLd + m],
+                                       tile[(2 * l + 1) * kLd + m], lanes);
                 }
             }
         }
-        // hash-grid scatter-add (trilinear weights, FP32 reductions; runs of lanes in one cell
-        // summed in the warp first)
-        {
-            const unsigned lanes = valid_lanes(i - (uint32_t)(tid & 31), a.n);
-#pragma unroll 2
-            for (int l = 0; l < kMaxLevels; ++l) {
-                const LevelDev L = a.enc.lv[l];
-                const CellCoord c = cell_of(p, L.res);
-                warp_scatter_level(a.table_grad, L, a.enc.hash_mask, c, dx[2 * l], dx[2 * l + 1],
-                                   lanes);
-            }
-        }
+        __syncthreads();
 
-        // ---- glue and RRSNet forward for the batch sums ----
+        // ---- glue and the RRSNet forward for the batch sums ----
         if (a.train_rrs) {
-            float x1[16];
-            glue16(a.fp, y, a.v, i, x1);
+            if (lead) {
+                float x1[16];
+                glue16(a.fp, y, a.v, valid ? i : 0u, x1);
 #pragma unroll
-            for (int k = 0; k < 10; ++k) {
-                colA[k * kTT] = x1[k];
-                act[(size_t)(a.r_x1 + k) * ld] = x1[k];
+                for (int k = 0; k < 10; ++k) {
+                    tile[k * kLd + m] = valid ? x1[k] : 0.f;
+                    if (valid) scr[(size_t)(a.r_x1 + k) * ld + i] = x1[k];
+                }
             }
-            const float* Wr = a.wt_rrs;
-            dense<10, WR, WR, true>(Wr, colA, colA, nullptr);
-            Wr += kRrsIn * WR;
+            fwd_layer<WR>(tr, kRrsIn, 10, tile, wch, tid, scr, ld, i0, 0, false);
 #pragma unroll 1
-            for (int h = 1; h < HR; ++h) {
-                dense<WR, WR, WR, true>(Wr, colA, colA, nullptr);
-                Wr += WR * WR;
-            }
-            float raw;
-            dense<WR, 1, 4, false>(Wr, colA, nullptr, &raw);
-            const float q = act_sigma(raw);
-            const float r = rel_contrib(a, i);
-            if (a.lw.active) {
-                const float lq = logf(q);
-                sumV += (double)(mu.var * (r * r / q));
-                sumC += (double)(mu.cost * (a.cost_offset + q));
-                sumR += (double)(mu.reg * (lq * lq));
-            } else {
-                sumV += (double)(r * r / q);
-                sumC += (double)(a.cost_offset + q);
+            for (int h = 1; h < HR; ++h)
+                fwd_layer<WR>(tr + (size_t)kRrsIn * WR + (size_t)(h - 1) * WR * WR, WR, WR, tile,
+                              wch, tid, scr, ld, i0, 0, false);
+            if (lead && valid) {
+                float raw;
+                narrow_out<WR, 1>(tr_out, tile, m, &raw);
+                const float q = act_sigma(raw);
+                const float r = rel_contrib(a, i);
+                if (a.lw.active) {
+                    const float lq = logf(q);
+                    sumV += (double)(mu.var * (r * r / q));
+                    sumC += (double)(mu.cost * (a.cost_offset + q));
+                    sumR += (double)(mu.reg * (lq * lq));
+                } else {
+                    sumV += (double)(r * r / q);
+                    sumC += (double)(a.cost_offset + q);
+                }
             }
         }
     }
@@ -326,15 +334,20 @@ __global__ void __launch_bounds__(kTT) k_train_stat(const __grid_constant__ Trai
     }
 }
 
+// The RRSNet step on 64-sample tiles: the forward layers again (activations to scratch), the
+// loss gradient with the batch's V and C, and the backward layers.
 template <int WR, int HR>
-__global__ void __launch_bounds__(kTT) k_train_rrs(const __grid_constant__ TrainArgs a) {
-    constexpr int XW = WR > 64 ? WR : 64;
-    extern __shared__ float smem[];
+__global__ void __launch_bounds__(simt::kThr) k_train_rrs(const __grid_constant__ TrainArgs a) {
+    using S = TrShape<WR>;
+    extern __shared__ float4 smem4[];
+    float* tile = reinterpret_cast<float*>(smem4);
+    float* wch = tile + S::kRows * kLd;
     __shared__ double s_tot[4];
-    float* colA = smem + threadIdx.x;
-    float* colB = smem + XW * kTT + threadIdx.x;
     const int tid = threadIdx.x;
+    const int m = tid & (kTM - 1);
+    const bool lead = tid < kTM;
     const uint32_t ld = a.ld;
+    float* scr = a.act;
     if (tid < 4) {
         double t = 0.0;
         for (uint32_t b = 0; b < a.part_n; ++b) t += a.part[4 * b + tid];
@@ -349,57 +362,57 @@ __global__ void __launch_bounds__(kTT) k_train_rrs(const __grid_constant__ Train
     }
     if (!a.train_rrs) return;
     const float Vf = (float)Vm, Cf = (float)Cm;
-    const uint32_t tiles = (a.n + kTT - 1) / kTT;
-    const float* Wl[4];
-    Wl[0] = a.w_rrs;
-    Wl[1] = a.w_rrs + kRrsIn * WR;
-    for (int h = 2; h <= HR; ++h) Wl[h] = Wl[h - 1] + WR * WR;
-    for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-        const uint32_t i = t * kTT + tid;
-        if (i >= a.n) continue;
-        float* act = a.act + i;
-#pragma unroll
-        for (int k = 0; k < 10; ++k) colA[k * kTT] = act[(size_t)(a.r_x1 + k) * ld];
-        const float* Wt = a.wt_rrs;
-        dense<10, WR, WR, true>(Wt, colA, colA, nullptr);
-        Wt += kRrsIn * WR;
-#pragma unroll 4
-        for (int k = 0; k < WR; ++k) act[(size_t)(a.r_hr + k) * ld] = colA[k * kTT];
+    const float* tr = a.wt_rrs;
+    const float* tr_out = tr + (size_t)kRrsIn * WR + (size_t)(HR - 1) * WR * WR;
+    const float* rr = a.w_rrs;
+    const float* rr_out = rr + (size_t)kRrsIn * WR + (size_t)(HR - 1) * WR * WR;   // [1][WR]
+    const uint32_t items = (a.n + kTM - 1) / kTM;
 #pragma unroll 1
-        for (int h = 1; h < HR; ++h) {
-            dense<WR, WR, WR, true>(Wt, colA, colA, nullptr);
-            Wt += WR * WR;
-#pragma unroll 4
-            for (int k = 0; k < WR; ++k) act[(size_t)(a.r_hr + h * WR + k) * ld] = colA[k * kTT];
+    for (uint32_t u = blockIdx.x; u < items; u += gridDim.x) {
+        const uint32_t i0 = u * kTM, i = i0 + m;
+        const bool valid = i < a.n;
+        __syncthreads();
+        if (lead) {
+#pragma unroll
+            for (int k = 0; k < 10; ++k)
+                tile[k * kLd + m] = valid ? scr[(size_t)(a.r_x1 + k) * ld + i] : 0.f;
         }
-        float raw;
-        dense<WR, 1, 4, false>(Wt, colA, nullptr, &raw);
-        const float q = act_sigma(raw);
-        const float r = rel_contrib(a, i);
-        float dq;
-        if (a.lw.active) {
-            const SampleMul mu = sample_mul(a.lw, i, a.n);
-            dq = (mu.var * (-(r * r) / (q * q)) * Cf + mu.cost * Vf +
-                  mu.reg * (2.0f * logf(q) / q)) / (float)a.n;
-        } else {
-            dq = (-(r * r) / (q * q) * Cf + Vf) / (float)a.n;
-        }
-        const float draw = dq * act_sigma_grad(raw);
-        act[(size_t)a.r_draw * ld] = draw;
-        // output layer W_out [1][WR]: d g_last = W_out^T draw masked by g_last
-        {
-            const float* wr = Wl[HR];
+        fwd_layer<WR>(tr, kRrsIn, 10, tile, wch, tid, scr, ld, i0, a.r_hr, true);
+#pragma unroll 1
+        for (int h = 1; h < HR; ++h)
+            fwd_layer<WR>(tr + (size_t)kRrsIn * WR + (size_t)(h - 1) * WR * WR, WR, WR, tile, wch,
+                          tid, scr, ld, i0, a.r_hr + h * WR, true);
+        if (lead) {
+            float draw = 0.f;
+            if (valid) {
+                float raw;
+                narrow_out<WR, 1>(tr_out, tile, m, &raw);
+                const float q = act_sigma(raw);
+                const float r = rel_contrib(a, i);
+                float dq;
+                if (a.lw.active) {
+                    const SampleMul mu = sample_mul(a.lw, i, a.n);
+                    dq = (mu.var * (-(r * r) / (q * q)) * Cf + mu.cost * Vf +
+                          mu.reg * (2.0f * logf(q) / q)) / (float)a.n;
+                } else {
+                    dq = (-(r * r) / (q * q) * Cf + Vf) / (float)a.n;
+                }
+                draw = dq * act_sigma_grad(raw);
+                scr[(size_t)a.r_draw * ld + i] = draw;
+            }
+            // d g_last = V_out^T draw, masked by g_last (this column of the tile)
+            float* dl = scr + (size_t)(a.r_dhr + (HR - 1) * WR) * ld + i;
 #pragma unroll 4
             for (int k = 0; k < WR; ++k) {
-                const float g = colA[k * kTT] > 0.f ? wr[k] * draw : 0.f;
-                colB[k * kTT] = g;
-                act[(size_t)(a.r_dhr + (HR - 1) * WR + k) * ld] = g;
+                const float dk = tile[k * kLd + m] > 0.f ? rr_out[k] * draw : 0.f;
+                tile[k * kLd + m] = dk;
+                if (valid) dl[(size_t)k * ld] = dk;
             }
         }
 #pragma unroll 1
         for (int h = HR - 1; h >= 1; --h)
-            dense_t<WR, WR, WR>(Wl[h], colB, colB, act + (size_t)(a.r_hr + (h - 1) * WR) * ld, ld,
-                                act + (size_t)(a.r_dhr + (h - 1) * WR) * ld);
+            bwd_layer<WR>(rr + (size_t)kRrsIn * WR + (size_t)(h - 1) * WR * WR, WR, tile, wch, tid,
+                          scr, ld, i0, a.r_hr + (h - 1) * WR, a.r_dhr + (h - 1) * WR);
     }
 }
 
@@ -594,26 +607,25 @@ __global__ void k_adam(const __grid_constant__ AdamArgs a) {
 
 template <int WS, int HS, int WR, int HR>
 cudaError_t launch_train(nrrs_ctx* ctx, TrainArgs& a, cudaStream_t s) {
-    constexpr int XW = (WS > WR ? WS : WR) > 64 ? (WS > WR ? WS : WR) : 64;
-    const size_t smem = 2 * (size_t)XW * kTT * sizeof(float);
+    const size_t smem = TrShape<WS>::kSmem;
     auto ks = k_train_stat<WS, HS, WR, HR>;
     auto kr = k_train_rrs<WR, HR>;
     cudaError_t e = cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    const uint32_t tiles = (a.n + kTT - 1) / kTT;
-    uint32_t grid = (uint32_t)(ctx->sm_count * resident_ctas((const void*)ks, kTT, smem, 16));
+    const uint32_t tiles = (a.n + kTM - 1) / kTM;
+    uint32_t grid = (uint32_t)(ctx->sm_count * resident_ctas((const void*)ks, simt::kThr, smem, 16));
     if (grid > tiles) grid = tiles;
     a.part_n = grid;
     {
         ProfScope ps(ctx, NRRS_KERNEL_TRAIN_STAT, s);
-        ks<<<grid, kTT, smem, s>>>(a);
+        ks<<<grid, simt::kThr, smem, s>>>(a);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     {
         ProfScope ps(ctx, NRRS_KERNEL_TRAIN_RRS, s);
-        kr<<<grid, kTT, smem, s>>>(a);
+        kr<<<grid, simt::kThr, smem, s>>>(a);
     }
     return cudaGetLastError();
 }

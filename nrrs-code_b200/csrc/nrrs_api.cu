@@ -363,6 +363,26 @@ void nrrs_config_default(nrrs_config* c) {
     c->step = 3;
 }
 
+void nrrs_config_reference_network(nrrs_config* c) {
+    if (!c) return;
+    // common/configs/nrrs/nrrs/2net-simple.json level0 / level1
+    c->network = NRRS_NET_REFERENCE;
+    c->n_levels = 8;
+    c->n_features_per_level = 2;
+    c->log2_hashmap_size = 19;
+    c->base_resolution = 16;
+    c->per_level_scale = 2.0f;
+    c->statnet_width = 32;
+    c->statnet_hidden = 3;
+    c->rrsnet_width = 32;
+    c->rrsnet_hidden = 3;
+    c->lr = 5e-3f;
+    c->beta1 = 0.9f;
+    c->beta2 = 0.99f;
+    c->eps = 1e-15f;
+    c->l2_reg = 3e-6f;
+}
+
 void nrrs_decide_params_default(nrrs_decide_params* p) {
     // the reference's shipped decision settings (common/configs/nrrs/render/test.json:63-67:
     // clamp_min 0.05, normalize_rate 0.85, use_ceil true, donnot_normalize_when_less_than_one

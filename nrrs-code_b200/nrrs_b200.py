@@ -35,6 +35,7 @@ DEV_BAD_INDEX = 0x10
 
 PREC_FP32, PREC_FP16, PREC_BF16 = 0, 1, 2
 FACTOR_ADRRS, FACTOR_RRSNET = 2, 3
+NET_WORKLOAD, NET_REFERENCE = 0, 1
 
 
 class Config(C.Structure):
@@ -50,6 +51,7 @@ class Config(C.Structure):
         ("loss_clamp_max", C.c_float), ("cost_offset", C.c_float),
         ("normalize_pos", C.c_int32), ("aabb_min", C.c_float * 3), ("aabb_max", C.c_float * 3),
         ("max_queue", C.c_uint32), ("max_train", C.c_uint32), ("step", C.c_int32),
+        ("network", C.c_int32),
     ]
 
 
@@ -152,6 +154,7 @@ _lib = None
 
 _SIGS = {
     "nrrs_config_default": (None, [C.POINTER(Config)]),
+    "nrrs_config_reference_network": (None, [C.POINTER(Config)]),
     "nrrs_decide_params_default": (None, [C.POINTER(DecideParams)]),
     "nrrs_create": (C.c_int, [C.POINTER(Config), C.POINTER(C.c_void_p)]),
     "nrrs_destroy": (None, [C.c_void_p]),
@@ -354,6 +357,19 @@ def header_functions() -> list[str]:
 def default_config(**kw) -> Config:
     c = Config()
     lib().nrrs_config_default(C.byref(c))
+    for k, v in kw.items():
+        if k in ("aabb_min", "aabb_max"):
+            getattr(c, k)[:] = list(v)
+        else:
+            setattr(c, k, v)
+    return c
+
+
+def reference_config(**kw) -> Config:
+    """nrrs_config_reference_network (the reference's shipped network), then kw"""
+    c = Config()
+    lib().nrrs_config_default(C.byref(c))
+    lib().nrrs_config_reference_network(C.byref(c))
     for k, v in kw.items():
         if k in ("aabb_min", "aabb_max"):
             getattr(c, k)[:] = list(v)

@@ -68,9 +68,15 @@ static inline uint32_t grid_index(const level_t* lv, uint32_t x, uint32_t y, uin
     return (x ^ (y * 2654435761u) ^ (z * 805459861u)) & lv->hash_mask;
 }
 
+/* the shape of the two network families (include/nrrs.h, nrrs_network_family) */
+static int net_ref(const nrrs_config* c) { return c->network == NRRS_NET_REFERENCE; }
+static int net_stat_in(const nrrs_config* c) { return net_ref(c) ? 32 : 64; }
+static int net_stat_out(const nrrs_config* c) { return net_ref(c) ? 6 : 3; }
+
 static uint64_t statnet_params(const nrrs_config* c) {
     const uint64_t w = (uint64_t)c->statnet_width;
-    return 64 * w + (uint64_t)(c->statnet_hidden - 1) * w * w + 3 * w;
+    return (uint64_t)net_stat_in(c) * w + (uint64_t)(c->statnet_hidden - 1) * w * w +
+           (uint64_t)net_stat_out(c) * w;
 }
 static uint64_t rrsnet_params(const nrrs_config* c) {
     const uint64_t w = (uint64_t)c->rrsnet_width;
@@ -246,19 +252,28 @@ void oracle_train_loss_w_f64(const nrrs_config* cfg, const double* params, uint6
 #pragma omp parallel for schedule(static) reduction(+ : lossS, sumV, sumC, sumR, sum_s, sum_w)
     for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
         const uint64_t i = (uint64_t)ii;
-        double x0[64], acts[4 * 128], y[3], x1[16], g[4 * 128], raw;
+        double x0[64], acts[4 * 128], y[6], x1[16], g[4 * 128], raw;
         const double sw = lw_s_f64(w, i), ww = lw_w_f64(w, i);
         sum_s += sw;
         sum_w += ww;
         build_x0_f64(cfg, lv, table, v, i, x0, NULL, NULL);
-        mlp_fwd_f64(Ws, 64, ws, hs, 3, x0, acts, y);
-        for (int c = 0; c < 3; ++c) {
-            const double d = y[c] - log((double)target[3 * i + c] + (double)cfg->stat_eps);
-            lossS += sw * d * d;
+        mlp_fwd_f64(Ws, net_stat_in(cfg), ws, hs, net_stat_out(cfg), x0, acts, y, net_ref(cfg));
+        if (net_ref(cfg)) {
+            for (int c = 0; c < 6; ++c) {
+                const double L = (double)target[3 * i + (c % 3)];
+                const double T = c < 3 ? L : L * L;
+                const double d = y[c] - T;
+                lossS += sw * d * d / (T * T + 0.01);
+            }
+        } else {
+            for (int c = 0; c < 3; ++c) {
+                const double d = y[c] - log((double)target[3 * i + c] + (double)cfg->stat_eps);
+                lossS += sw * d * d;
+            }
         }
         if (cfg->step >= 3) {
             glue_f64(cfg, y, v, i, x1);
-            mlp_fwd_f64(Wr, 16, wr, hr, 1, x1, g, &raw);
+            mlp_fwd_f64(Wr, 16, wr, hr, 1, x1, g, &raw, net_ref(cfg));
             const double q = act_sigma_f64(raw);
             const double r = rel_contrib_f64(cfg, v, target, i);
             sumV += ww * lw_u_f64(w, i) * r * r / (lw_k_f64(w, i) * q);
@@ -267,7 +282,7 @@ void oracle_train_loss_w_f64(const nrrs_config* cfg, const double* params, uint6
         }
     }
     const double g4 = w ? (double)w->gamma4 : 0.0;
-    loss[0] = lossS / (3.0 * sum_s);
+    loss[0] = lossS / ((net_ref(cfg) ? 6.0 : 3.0) * sum_s);
     loss[1] = cfg->step >= 3 ? (sumV / sum_w) * (sumC / sum_w) + g4 * sumR / sum_w : 0.0;
 }
 

@@ -9,11 +9,15 @@
 
 #if REAL_IS_DOUBLE
 #define R_EXP exp
+#define R_ATAN2 atan2
+#define R_ACOS acos
 #define R_LOG log
 #define R_SQRT sqrt
 #define R_CEIL ceil
 #else
 #define R_EXP expf
+#define R_ATAN2 atan2f
+#define R_ACOS acosf
 #define R_LOG logf
 #define R_SQRT sqrtf
 #define R_CEIL ceilf
@@ -92,6 +96,31 @@ static void FN(hash_encode)(const level_t* lv, int L, const REAL* table, const f
     }
 }
 
+/* One-blob encoding of x in [0,1] into `bins` lanes (Mueller et al. 2019) with the compact
+ * quartic (biweight) kernel of radius 1/bins that tiny-cuda-nn's OneBlob uses: lane k holds the
+ * kernel mass centred at x that falls into bin [k/bins, (k+1)/bins), F(b - x) - F(a - x), where
+ * F is the kernel's CDF, F(t) = 15/16 (u - 2u^3/3 + u^5/5) + 1/2 at u = t bins clamped to [-1,1]. */
+static REAL FN(quartic_cdf)(REAL t, int bins) {
+    REAL u = t * (REAL)bins;
+    u = u < (REAL)-1 ? (REAL)-1 : (u > (REAL)1 ? (REAL)1 : u);
+    const REAL u2 = u * u;
+    return (REAL)15 / (REAL)16 * u * ((REAL)1 - (REAL)2 / (REAL)3 * u2 + u2 * u2 / (REAL)5) +
+           (REAL)0.5;
+}
+static void FN(one_blob)(REAL x, int bins, REAL* out) {
+    for (int k = 0; k < bins; ++k)
+        out[k] = FN(quartic_cdf)((REAL)(k + 1) / (REAL)bins - x, bins) -
+                 FN(quartic_cdf)((REAL)k / (REAL)bins - x, bins);
+}
+/* lat-long coordinates of a unit direction (the reference's work item stores wi as lat-long,
+ * workqueue.h:159, through KiRaRay's worldToLatLong, absent from the checkout):
+ * u = atan2(y, x) / 2pi + 1/2, v = acos(z) / pi */
+static void FN(latlong)(const float* d, REAL* uv) {
+    const REAL z = (REAL)d[2] < (REAL)-1 ? (REAL)-1 : ((REAL)d[2] > (REAL)1 ? (REAL)1 : (REAL)d[2]);
+    uv[0] = R_ATAN2((REAL)d[1], (REAL)d[0]) * (REAL)0.15915494309189535 + (REAL)0.5;
+    uv[1] = R_ACOS(z) * (REAL)0.3183098861837907;
+}
+
 /* StatNet input row x0[64]: [0,32) hash features, [32,48) SH(wi), [48,51) normal,
  * [51,54) albedo, [54] 1-exp(-roughness) (warp_roughness, train.h:95), [55] 1 (bias), rest 0 */
 static void FN(build_x0)(const nrrs_config* cfg, const level_t* lv, const REAL* table,
@@ -100,6 +129,16 @@ static void FN(build_x0)(const nrrs_config* cfg, const level_t* lv, const REAL* 
     float pn[3];
     oracle_normalize_pos_f32(cfg, v->pos + 3 * i, pn);
     FN(hash_encode)(lv, cfg->n_levels, table, pn, x0, cidx, cw);
+    if (net_ref(cfg)) {
+        /* the reference network: [0,16) hash features, [16,20) and [20,24) one-blob of the
+         * lat-long u and v, [24,32) one-blob of the warped roughness */
+        REAL uv[2];
+        FN(latlong)(v->wi + 3 * i, uv);
+        FN(one_blob)(uv[0], 4, x0 + 16);
+        FN(one_blob)(uv[1], 4, x0 + 20);
+        FN(one_blob)((REAL)1 - R_EXP(-(REAL)v->roughness[i]), 8, x0 + 24);
+        return;
+    }
     FN(sh16)(v->wi + 3 * i, x0 + 32);
     for (int d = 0; d < 3; ++d) x0[48 + d] = (REAL)v->normal[3 * i + d];
     for (int d = 0; d < 3; ++d) x0[51 + d] = (REAL)v->albedo[3 * i + d];
@@ -118,16 +157,21 @@ static void FN(matvec)(const REAL* W, int out, int in, const REAL* x, REAL* y) {
     }
 }
 static void FN(relu)(REAL* x, int n) { for (int k = 0; k < n; ++k) x[k] = x[k] > 0 ? x[k] : 0; }
+/* LeakyReLU with tiny-cuda-nn's slope 0.01 (the reference network's activation) */
+static void FN(leaky)(REAL* x, int n) {
+    for (int k = 0; k < n; ++k) x[k] = x[k] > 0 ? x[k] : (REAL)0.01 * x[k];
+}
 
 /* forward through a bias-free ReLU MLP; acts[l] receives the post-activation of hidden l;
  * layer widths: in -> w (hidden times) -> out */
 static void FN(mlp_fwd)(const REAL* W, int in, int w, int hidden, int out, const REAL* x,
-                        REAL* acts /* [hidden][w] */, REAL* y) {
+                        REAL* acts /* [hidden][w] */, REAL* y, int leaky) {
     const REAL* cur = x;
     int cur_in = in;
     for (int h = 0; h < hidden; ++h) {
         FN(matvec)(W, w, cur_in, cur, acts + h * w);
-        FN(relu)(acts + h * w, w);
+        if (leaky) FN(leaky)(acts + h * w, w);
+        else FN(relu)(acts + h * w, w);
         W += (uint64_t)w * cur_in;
         cur = acts + h * w;
         cur_in = w;
@@ -137,7 +181,7 @@ static void FN(mlp_fwd)(const REAL* W, int in, int w, int hidden, int out, const
 
 /* backward through the same MLP: dy -> weight grads (accumulated into dW) and dx (optional) */
 static void FN(mlp_bwd)(const REAL* W, int in, int w, int hidden, int out, const REAL* x,
-                        const REAL* acts, const REAL* dy, REAL* dW, REAL* dx) {
+                        const REAL* acts, const REAL* dy, REAL* dW, REAL* dx, int leaky) {
     /* offsets of each layer in W / dW */
     uint64_t off[8];
     int ins[8], outs[8];
@@ -163,7 +207,8 @@ static void FN(mlp_bwd)(const REAL* W, int in, int w, int hidden, int out, const
             dprev[k] = acc;
         }
         if (h > 0) {
-            for (int k = 0; k < ins[h]; ++k) dcur[k] = a[k] > 0 ? dprev[k] : 0;
+            for (int k = 0; k < ins[h]; ++k)
+                dcur[k] = a[k] > 0 ? dprev[k] : (leaky ? (REAL)0.01 * dprev[k] : (REAL)0);
         } else {
             for (int k = 0; k < ins[h]; ++k) dx[k] = dprev[k];
         }
@@ -175,6 +220,20 @@ static void FN(mlp_bwd)(const REAL* W, int in, int w, int hidden, int out, const
  * Lhat_c = max(exp(min(y_c, 20)) - stat_eps, 0) */
 static void FN(glue)(const nrrs_config* cfg, const REAL* y, const nrrs_vertex_soa* v, uint64_t i,
                      REAL* x1) {
+    if (net_ref(cfg)) {
+        /* the reference's own glue (train.cu:41-112): [bc(max(L,0)) x3, bc(max(L^2,0)) x3,
+         * bc(thp) x3, warped roughness, bc(ref_mean), 1, 0 x4] */
+        for (int c = 0; c < 3; ++c) {
+            x1[c] = FN(box_cox)(y[c] > 0 ? y[c] : (REAL)0);
+            x1[3 + c] = FN(box_cox)(y[3 + c] > 0 ? y[3 + c] : (REAL)0);
+            x1[6 + c] = FN(box_cox)((REAL)v->thp[3 * i + c]);
+        }
+        x1[9] = (REAL)1 - R_EXP(-(REAL)v->roughness[i]);
+        x1[10] = FN(box_cox)(v->ref_mean ? (REAL)v->ref_mean[i] : (REAL)0.5);
+        x1[11] = 1;
+        for (int k = 12; k < 16; ++k) x1[k] = 0;
+        return;
+    }
     for (int c = 0; c < 3; ++c) {
         REAL yc = y[c] < (REAL)20 ? y[c] : (REAL)20;
         REAL L = R_EXP(yc) - (REAL)cfg->stat_eps;
@@ -198,8 +257,13 @@ static REAL FN(factor)(const nrrs_config* cfg, const nrrs_decide_params* p, cons
         const REAL ref = (v->ref_mean ? (REAL)v->ref_mean[i] : (REAL)0.5) + (REAL)cfg->ref_eps;
         REAL acc = 0;
         for (int c = 0; c < 3; ++c) {
-            REAL yc = y[c] < (REAL)20 ? y[c] : (REAL)20;
-            REAL L = R_EXP(yc) - (REAL)cfg->stat_eps;
+            REAL L;
+            if (net_ref(cfg)) {
+                L = y[c];   /* the reference network outputs L itself */
+            } else {
+                REAL yc = y[c] < (REAL)20 ? y[c] : (REAL)20;
+                L = R_EXP(yc) - (REAL)cfg->stat_eps;
+            }
             L = L < (REAL)1e-4 ? (REAL)1e-4 : (L > (REAL)1e4 ? (REAL)1e4 : L);
             acc += L * (REAL)v->thp[3 * i + c] / ref;
         }
@@ -227,16 +291,18 @@ static void FN(infer_impl)(const nrrs_config* cfg, const REAL* params, uint64_t 
     const REAL* Wr = Ws + statnet_params(cfg);
     const int ws = cfg->statnet_width, wr = cfg->rrsnet_width;
     const int hs = cfg->statnet_hidden, hr = cfg->rrsnet_hidden;
+    const int sin_ = net_stat_in(cfg), sout = net_stat_out(cfg), leaky = net_ref(cfg);
 #pragma omp parallel for schedule(static)
     for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
         const uint64_t i = (uint64_t)ii;
-        REAL x0[64], acts[4 * 128], y[3], x1[16], g[4 * 128], raw;
+        REAL x0[64], acts[4 * 128], y[6], x1[16], g[4 * 128], raw;
+        for (int k = 0; k < 64; ++k) x0[k] = 0;
         FN(build_x0)(cfg, lv, table, v, i, x0, NULL, NULL);
-        FN(mlp_fwd)(Ws, 64, ws, hs, 3, x0, acts, y);
+        FN(mlp_fwd)(Ws, sin_, ws, hs, sout, x0, acts, y, leaky);
         FN(glue)(cfg, y, v, i, x1);
-        FN(mlp_fwd)(Wr, 16, wr, hr, 1, x1, g, &raw);
+        FN(mlp_fwd)(Wr, 16, wr, hr, 1, x1, g, &raw, leaky);
         if (x0o) for (int k = 0; k < 64; ++k) x0o[i * 64 + k] = x0[k];
-        if (stats) for (int k = 0; k < 3; ++k) stats[i * 3 + k] = y[k];
+        if (stats) for (int k = 0; k < sout; ++k) stats[i * sout + k] = y[k];
         if (x1o) for (int k = 0; k < 16; ++k) x1o[i * 16 + k] = x1[k];
         if (rawo) rawo[i] = raw;
         if (rrso) rrso[i] = FN(factor)(cfg, p, y, raw, v, i);
@@ -294,6 +360,7 @@ static void FN(train_impl)(const nrrs_config* cfg, const REAL* params, uint64_t 
     const int ws = cfg->statnet_width, wr = cfg->rrsnet_width;
     const int hs = cfg->statnet_hidden, hr = cfg->rrsnet_hidden;
     const int train_rrs = cfg->step >= 3;
+    const int sin_ = net_stat_in(cfg), sout = net_stat_out(cfg), leaky = net_ref(cfg);
     memset(grads, 0, sizeof(REAL) * np);
     double lossS = 0, sumV = 0, sumC = 0, sumR = 0;
     /* weighted losses: the batch sums of the weights, and the divisors of the means */
@@ -312,11 +379,11 @@ static void FN(train_impl)(const nrrs_config* cfg, const REAL* params, uint64_t 
 #pragma omp parallel for schedule(static) reduction(+ : sumV, sumC, sumR)
         for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
             const uint64_t i = (uint64_t)ii;
-            REAL x0[64], acts[4 * 128], y[3], x1[16], g[4 * 128], raw;
+            REAL x0[64], acts[4 * 128], y[6], x1[16], g[4 * 128], raw;
             FN(build_x0)(cfg, lv, table, v, i, x0, NULL, NULL);
-            FN(mlp_fwd)(Ws, 64, ws, hs, 3, x0, acts, y);
+            FN(mlp_fwd)(Ws, sin_, ws, hs, sout, x0, acts, y, leaky);
             FN(glue)(cfg, y, v, i, x1);
-            FN(mlp_fwd)(Wr, 16, wr, hr, 1, x1, g, &raw);
+            FN(mlp_fwd)(Wr, 16, wr, hr, 1, x1, g, &raw, leaky);
             const REAL q = FN(act_sigma)(raw);
             const REAL r = FN(rel_contrib)(cfg, v, target, i);
             if (w) {
@@ -351,23 +418,36 @@ static void FN(train_impl)(const nrrs_config* cfg, const REAL* params, uint64_t 
 #pragma omp for schedule(static)
         for (int64_t ii = 0; ii < (int64_t)n; ++ii) {
             const uint64_t i = (uint64_t)ii;
-            REAL x0[64], acts[4 * 128], y[3], dy[3], dx0[64], cw[16 * 8];
+            REAL x0[64], acts[4 * 128], y[6], dy[6], dx0[64], cw[16 * 8];
             uint32_t cidx[16 * 8];
             FN(build_x0)(cfg, lv, table, v, i, x0, cidx, cw);
-            FN(mlp_fwd)(Ws, 64, ws, hs, 3, x0, acts, y);
+            FN(mlp_fwd)(Ws, sin_, ws, hs, sout, x0, acts, y, leaky);
             const REAL sw = FN(lw_s)(w, i);
-            for (int c = 0; c < 3; ++c) {
-                const REAL t = R_LOG((REAL)target[3 * i + c] + (REAL)cfg->stat_eps);
-                const REAL d = y[c] - t;
-                if (w) {
-                    lossS += (double)(sw * d * d);
-                    dy[c] = (REAL)2 * sw * d / ((REAL)3 * (REAL)sum_s);
-                } else {
-                    lossS += (double)(d * d);
-                    dy[c] = (REAL)2 * d / ((REAL)3 * (REAL)n);
+            if (leaky) {
+                /* the reference network: relative squared error of L and L^2 against the target
+                 * L and its square, (y - T)^2 / (T^2 + 0.01), mean over the 6 outputs */
+                for (int c = 0; c < 6; ++c) {
+                    const REAL L = (REAL)target[3 * i + (c % 3)];
+                    const REAL T = c < 3 ? L : L * L;
+                    const REAL den = T * T + (REAL)0.01;
+                    const REAL d = y[c] - T;
+                    lossS += (double)(sw * d * d / den);
+                    dy[c] = (REAL)2 * sw * d / (den * (REAL)6 * (REAL)sum_s);
+                }
+            } else {
+                for (int c = 0; c < 3; ++c) {
+                    const REAL t = R_LOG((REAL)target[3 * i + c] + (REAL)cfg->stat_eps);
+                    const REAL d = y[c] - t;
+                    if (w) {
+                        lossS += (double)(sw * d * d);
+                        dy[c] = (REAL)2 * sw * d / ((REAL)3 * (REAL)sum_s);
+                    } else {
+                        lossS += (double)(d * d);
+                        dy[c] = (REAL)2 * d / ((REAL)3 * (REAL)n);
+                    }
                 }
             }
-            FN(mlp_bwd)(Ws, 64, ws, hs, 3, x0, acts, dy, dWs, dx0);
+            FN(mlp_bwd)(Ws, sin_, ws, hs, sout, x0, acts, dy, dWs, dx0, leaky);
             for (int l = 0; l < cfg->n_levels; ++l)
                 for (int c = 0; c < 8; ++c) {
                     const uint64_t row = cidx[l * 8 + c];
@@ -381,7 +461,7 @@ static void FN(train_impl)(const nrrs_config* cfg, const REAL* params, uint64_t 
             if (train_rrs) {
                 REAL x1[16], g[4 * 128], raw, draw;
                 FN(glue)(cfg, y, v, i, x1);
-                FN(mlp_fwd)(Wr, 16, wr, hr, 1, x1, g, &raw);
+                FN(mlp_fwd)(Wr, 16, wr, hr, 1, x1, g, &raw, leaky);
                 const REAL q = FN(act_sigma)(raw);
                 const REAL r = FN(rel_contrib)(cfg, v, target, i);
                 REAL dq;
@@ -393,18 +473,20 @@ static void FN(train_impl)(const nrrs_config* cfg, const REAL* params, uint64_t 
                     dq = (-(r * r) / (q * q) * (REAL)Cm + (REAL)Vm) / (REAL)n;
                 }
                 draw = dq * FN(act_sigma_grad)(raw);
-                FN(mlp_bwd)(Wr, 16, wr, hr, 1, x1, g, &draw, dWr, NULL);
+                FN(mlp_bwd)(Wr, 16, wr, hr, 1, x1, g, &draw, dWr, NULL, leaky);
             }
         }
     }
     for (int t = 0; t < nt; ++t)
         for (uint64_t k = 0; k < np_mlp; ++k) grads[np_table + k] += priv[(uint64_t)t * np_mlp + k];
     free(priv);
-    loss[0] = lossS / (3.0 * sum_s);
+    loss[0] = lossS / ((double)(leaky ? 6 : 3) * sum_s);
     loss[1] = train_rrs ? Vm * Cm + g4 * Rm : 0.0;
 }
 
 #undef R_EXP
+#undef R_ATAN2
+#undef R_ACOS
 #undef R_LOG
 #undef R_SQRT
 #undef R_CEIL

@@ -391,3 +391,83 @@ def test_weighted_losses_fd_gradients_fp64():
                 break
         else:
             raise AssertionError((int(k), fd, g[k]))
+
+
+def ref_cfg(**kw):
+    base = dict(log2_hashmap_size=12, table_init_scale=0.5)
+    base.update(kw)
+    return O.reference_config(**base)
+
+
+def test_reference_network_shapes_and_one_blob():
+    cfg = O.reference_config()
+    lv, tot = O.level_table(cfg)
+    assert lv[:, 2].tolist() == [16 * 2 ** l for l in range(8)]
+    assert lv[:, 3].tolist() == [1, 1, 1, 0, 0, 0, 0, 0]
+    npar, ntab, nst, nrr = O.param_count(cfg)
+    assert (nst, nrr) == (32 * 32 + 2 * 32 * 32 + 6 * 32, 16 * 32 + 2 * 32 * 32 + 32)
+    # the StatNet input: 16 hash lanes, 8 one-blob lanes of the direction, 8 of the roughness
+    v = O.synth(3, 500)
+    p = rand_params(cfg, 3, 0.3)
+    x0 = O.infer(cfg, p, v, O.default_decide(), "f64", want=("x0", "stats"))["x0"]
+    assert np.all(x0[:, 32:] == 0)
+    for a, b, bins in ((16, 20, 4), (20, 24, 4), (24, 32, 8)):
+        blob = x0[:, a:b]
+        assert np.all(blob >= -1e-15) and np.all(blob.sum(1) <= 1 + 1e-12)
+        assert np.all(blob.sum(1) > 0.45)        # at least half the kernel mass lands inside
+    # one-blob of the lat-long v = acos(z)/pi: the blob's centre of mass follows v
+    zc = np.arccos(np.clip(v["wi"][:, 2].astype(np.float64), -1, 1)) / np.pi
+    centres = (x0[:, 20:24] * (np.arange(4) + 0.5) / 4).sum(1) / x0[:, 20:24].sum(1)
+    inner = (zc > 0.3) & (zc < 0.7)
+    assert np.max(np.abs(centres[inner] - zc[inner])) < 0.02
+
+
+@pytest.mark.parametrize("step", [3, 2])
+def test_reference_network_fd_gradients_fp64(step):
+    """central finite differences (h = 1e-3, FP64) of the reference network's losses"""
+    cfg = ref_cfg(step=step)
+    n = 96
+    v = O.synth(15, n)
+    tgt = v["target"]
+    p = rand_params(cfg, 15, 0.3)
+    g, loss = O.train_grads(cfg, p, v, tgt, "f64")
+    assert np.allclose(O.train_loss(cfg, p.astype(np.float64), v, tgt), loss, rtol=1e-12)
+    ntab, nst, nrr = O.param_count(cfg)[1:]
+    rng = np.random.default_rng(16)
+    touched = np.nonzero(g[:ntab])[0]
+    picks = np.concatenate([rng.choice(touched, 96, replace=False),
+                            ntab + rng.choice(nst, 96, replace=False),
+                            ntab + nst + rng.choice(nrr, 64, replace=False)])
+    p64 = p.astype(np.float64)
+    for k in picks:
+        which = 1 if k >= ntab + nst else 0
+        if which == 1 and step < 3:
+            assert g[k] == 0
+            continue
+        for h in (1e-3, 1e-6):
+            floor = 1e-11 * max(1.0, loss[which]) / h
+            q = p64.copy()
+            q[k] += h
+            lp = O.train_loss(cfg, q, v, tgt)[which]
+            q[k] -= 2 * h
+            lm = O.train_loss(cfg, q, v, tgt)[which]
+            fd = (lp - lm) / (2 * h)
+            if abs(fd - g[k]) <= (1e-3 if h == 1e-3 else 1e-4) * max(abs(fd), abs(g[k])) + floor:
+                break
+        else:
+            raise AssertionError((int(k), fd, g[k]))
+
+
+def test_reference_network_fp32_matches_fp64():
+    cfg = ref_cfg()
+    v = O.synth(17, 2000)
+    p = rand_params(cfg, 17, 0.3)
+    dp = O.default_decide()
+    a = O.infer(cfg, p, v, dp, "f64", want=("stats", "rrs"))
+    b = O.infer(cfg, p, v, dp, "f32", want=("stats", "rrs"))
+    assert np.allclose(b["stats"], a["stats"], rtol=1e-4, atol=1e-5)
+    assert np.allclose(b["rrs"], a["rrs"], rtol=1e-4)
+    g64, l64 = O.train_grads(cfg, p, v, v["target"], "f64")
+    g32, l32 = O.train_grads(cfg, p, v, v["target"], "f32")
+    assert np.allclose(l32, l64, rtol=1e-4)
+    assert np.linalg.norm(g32 - g64) / np.linalg.norm(g64) < 1e-4
