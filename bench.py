@@ -120,6 +120,32 @@ def traffic_per_vertex(kernel: str, workload: str):
     return None
 
 
+def requests_per_vertex(kernel: str, workload: str):
+    """L2-to-L1 read sectors per vertex of the kernel on the workload (one L1-to-L2 request
+    each: the gathers are random one-sector loads) from the committed ncu summary"""
+    f = REPO / "profiles" / "traffic.json"
+    if f.exists():
+        j = json.loads(f.read_text())
+        return j.get("l1_requests", {}).get(workload, {}).get(kernel)
+    return None
+
+
+def request_bound(roof, workload, sm_mhz, sm_count):
+    """The gather kernels' real roofline: the L1-to-crossbar interface carries one request per
+    cycle per SM, and every random gather sector is one request."""
+    if not roof:
+        return None
+    spv = requests_per_vertex(roof["kernel"], workload)
+    if not spv:
+        return None
+    achieved = spv * roof["vertices_per_launch"] / (roof["launch_ms"] * 1e-3) / 1e9
+    peak = sm_count * (sm_mhz or 1965.0) / 1e3
+    return {"bound": "l1_to_l2_requests", "achieved": achieved, "peak": peak,
+            "unit": "G requests/s", "frac": achieved / peak, "sectors_per_vertex": spv,
+            "peak_basis": "1 request per cycle per SM x SMs x median SM clock under load",
+            "sectors_source": "ncu l1tex__m_xbar2l1tex_read_sectors_mem_lg_op_ld (profiles/)"}
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 100 ms during the timed region."""
 
@@ -420,12 +446,14 @@ class FrameArm:
     step (every bounce's nrrs_step, then the frame's training steps)."""
 
     def __init__(self, torch, dev, stream, wl, precision, dev_b, td, train, world,
-                 launch_shape=None, tune=True, sharded=False):
+                 launch_shape=None, tune=True, sharded=False, cell_image=True):
         self.torch, self.dev, self.stream, self.wl = torch, dev, stream, wl
         self.B, self.N = wl["bounces"], wl["n_vert"]
         self.precision = precision
         self.dev_b, self.td, self.train = dev_b, td, train
         self.net = nb.NRRSNetwork(make_config(precision, wl, self.N, wl["train_batch"]))
+        if not cell_image and self.net.cell_image():
+            self.net.set_cell_image(False)
         self.tune = None
         if launch_shape:
             shape = [int(x) for x in launch_shape.split(",")]
@@ -644,7 +672,8 @@ def run_frame_pair(args, torch, dev, stream, timer, name, steps, warmup, fp32_st
     host_b, dev_b, th, td = frame_inputs(torch, dev, wl, 1000, rank, train)
     prec = args.precision if headline and args.precision else wl["precision"]
     mixed = FrameArm(torch, dev, stream, wl, prec, dev_b, td, train, world,
-                     launch_shape=args.launch_shape, sharded=world > 1)
+                     launch_shape=args.launch_shape, sharded=world > 1,
+                     cell_image=args.cell_image)
     out = {"name": name, "wl": wl, "train": train, "precision": prec, "arm": mixed,
            "host_b": host_b, "dev_b": dev_b, "th": th, "td": td}
     clk = ClockSampler(env_int("LOCAL_RANK", 0)) if headline else None
@@ -833,6 +862,11 @@ def run_ours(args, rank, world, local_rank):
     mode = arm.net.infer_split() if p["precision"] != "fp32" else 0
     inf_vertices = wl["bounces"] * wl["n_vert"] * args.steps
     roof, mlp_roof = roofline_of(prof, p["precision"], mode, wl, inf_vertices, name)
+    if roof:
+        rb = request_bound(roof, name, (p["clocks"] or {}).get("sm_mhz"),
+                           torch.cuda.get_device_properties(dev).multi_processor_count)
+        if rb:
+            roof["request_bound"] = rb
     e2e = e2e_of(torch, dev, timer, arm, p["host_b"], p["th"], max(2, min(args.steps, 10)),
                  min(2, args.warmup))
     line = {
@@ -859,6 +893,8 @@ def run_ours(args, rank, world, local_rank):
                        for k, (n, t) in prof.items()}
     line["launch_shape"] = list(arm.net.launch_shape()) + (
         [arm.net.infer_split()] if p["precision"] != "fp32" else [])
+    if p["precision"] != "fp32":
+        line["cell_image"] = arm.net.cell_image()
     if arm.tune:
         line["autotune"] = {"best": arm.tune.get("best") or arm.tune.get("cached"),
                             "trials": arm.tune.get("trials")}
@@ -1556,6 +1592,9 @@ def main():
     ap.add_argument("--launch-shape", default=None,
                     help="CTAS_PER_SM,WARPGROUPS[,SPLIT] of the inference kernels instead of "
                          "autotuning")
+    ap.add_argument("--no-cell-image", dest="cell_image", action="store_false",
+                    help="gather the dense hash-grid levels from the table rows instead of the "
+                         "cell image (bit-identical; for comparisons)")
     ap.add_argument("--bounces", type=int, default=None, help="smaller cases for profiling")
     ap.add_argument("--vertices", type=int, default=None, help="smaller cases for profiling")
     args = ap.parse_args()

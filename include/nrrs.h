@@ -112,6 +112,12 @@ typedef struct {
     /* network family (nrrs_network_family): NRRS_NET_WORKLOAD or NRRS_NET_REFERENCE; fill the
      * reference family with nrrs_config_reference_network */
     int32_t network;
+    /* Exponential moving average of the weights for inference (the Ema optimizer that wraps
+     * Adam in 2net-simple.json:17-20, decay 0.95 there): after every Adam step
+     * e <- d e + (1 - d) w over all parameters (e starts at 0 when parameters are uploaded),
+     * and the inference entry points use e / (1 - d^t), t the number of steps since; training
+     * keeps using w. 0 (the default) = off: inference uses w. */
+    float ema_decay;
 } nrrs_config;
 
 /* The two network families.
@@ -320,6 +326,9 @@ int nrrs_param_layout(const nrrs_ctx* ctx, uint64_t* table_params, uint64_t* sta
                       uint64_t* rrsnet_params);
 int nrrs_get_params(const nrrs_ctx* ctx, float* host_dst, uint64_t count);
 int nrrs_set_params(nrrs_ctx* ctx, const float* host_src, uint64_t count);
+/* the weights the inference entry points use: the debiased moving average when ema_decay > 0
+ * (equal to the trained weights right after an upload), else the trained weights */
+int nrrs_get_inference_params(const nrrs_ctx* ctx, float* host_dst, uint64_t count);
 /* gradients of the last nrrs_train_step (before the Adam update); host copy */
 int nrrs_get_grads(const nrrs_ctx* ctx, float* host_dst, uint64_t count);
 /* Adam step count and moments (host copies, count each) */
@@ -353,11 +362,22 @@ int nrrs_get_launch_shape(const nrrs_ctx* ctx, int32_t* ctas_per_sm, int32_t* wa
  * L2, and the MLP kernel bulk-loads them; for tables larger than L2), 2 = split with the MLP
  * in two kernels (StatNet, which writes each tile's RRSNet input to HBM, then RRSNet; each
  * holds only its own weights, so more tiles are in flight per SM; with ADRRS factors only the
- * StatNet kernel runs). All modes give bit-identical results. Selecting split allocates
- * (max_queue/128 + 17) feature tiles of 8 KB, and mode 2 as many RRSNet input tiles of 4 KB;
- * not available for the FP32 path. */
+ * StatNet kernel runs), 3 = as 2 with each hidden layer's activations kept in TMEM as the next
+ * layer's A operand (tcgen05.mma reads only the weights from shared memory; 1 or 2 warpgroups).
+ * All modes give bit-identical results. Selecting split allocates (max_queue/128 + 17) feature
+ * tiles of 8 KB, and modes 2 and 3 as many RRSNet input tiles of 4 KB; not available for the
+ * FP32 path. */
 int nrrs_set_infer_split(nrrs_ctx* ctx, int32_t split);
 int nrrs_get_infer_split(const nrrs_ctx* ctx, int32_t* split);
+/* Cell image of the dense hash-grid levels (mixed-precision contexts with at least one dense
+ * level): for every cell of a dense level, its 8 FP16 corner entries in one 32-byte block, rebuilt
+ * after every table update (32 bytes x the dense cells: 7.1 MB for 16 levels at 2^19, 81 MB at
+ * 2^22). With it on (the default) a dense level costs the gathers one 32-byte load instead of
+ * four 16-byte row loads. The corner values and their summation order are the table's, so
+ * results are bit-identical either way. Enabling it where there is none returns
+ * NRRS_ERR_UNSUPPORTED. */
+int nrrs_set_cell_image(nrrs_ctx* ctx, int32_t enable);
+int nrrs_get_cell_image(const nrrs_ctx* ctx, int32_t* enable);
 /* Training mode of the tensor-core path: 1 (the default) = split: a level-major encoding kernel
  * writes the hash features of the batch, the StatNet kernel trains on them and writes each
  * sample's hash-lane gradients, and a level-major scatter kernel adds those into the table
@@ -389,7 +409,7 @@ typedef enum {
     NRRS_KERNEL_TRAIN_STAT = 6, NRRS_KERNEL_TRAIN_RRS = 7, NRRS_KERNEL_TRAIN_WGRAD = 8,
     NRRS_KERNEL_TRAIN_REDUCE = 9, NRRS_KERNEL_ADAM = 10, NRRS_KERNEL_ENCODE = 11,
     NRRS_KERNEL_TRAIN_SCATTER = 12, NRRS_KERNEL_TRAIN_ENCODE = 13, NRRS_KERNEL_INFER_RRS = 14,
-    NRRS_KERNEL_KINDS = 15
+    NRRS_KERNEL_CELL_IMAGE = 15, NRRS_KERNEL_KINDS = 16
 } nrrs_kernel_kind;
 uint64_t nrrs_launch_count(const nrrs_ctx* ctx);
 /* grid (CTAs) of the last inference launch: SMs x resident CTAs per SM */

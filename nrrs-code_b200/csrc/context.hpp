@@ -40,6 +40,16 @@ struct nrrs_ctx {
     uint64_t adam_t = 0;
 
     __half* table_h = nullptr; // FP16 table copy (mixed precision)
+    uint4* cells = nullptr;    // cell image of the FP16 table's dense levels (EncodeParams::cells)
+    uint32_t n_cells = 0;
+    // moving average of the weights (ema_decay > 0): the raw average, its debiased copy and the
+    // inference images derived from that copy (the training images above stay on params)
+    float* ema = nullptr;          // [n_params]
+    float* params_inf = nullptr;   // [n_params] ema / (1 - d^t)
+    float* wt_inf = nullptr;       // transposed FP32 MLP weights of params_inf
+    __half* table_h_inf = nullptr; // FP16 table of params_inf (mixed precision)
+    uint4* cells_inf = nullptr;    // its cell image
+    uint64_t ema_t = 0;
     float* wt = nullptr;       // transposed FP32 MLP weights
     float* wrow = nullptr;     // aligned row-major copy of the FP32 MLP weights
     void* wpack = nullptr;     // UMMA-packed FP16/BF16 MLP weights

@@ -28,50 +28,58 @@ using simt::kTM;
 
 template <int W>
 struct FpShape {
-    static constexpr int kRows = simt::imax(kStatIn, W);           // rows of the activation tile
+    static constexpr int kRows = simt::imax(stat_in_of(W), W);     // rows of the activation tile
     static constexpr int kActFloats = kRows * kLd;
     static constexpr int kChunkFloats = simt::kKC * W;
     static constexpr size_t kSmem = sizeof(float) * (kActFloats + 2 * kChunkFloats);
 };
 
-// out[n][m] = max(0, sum_k wt[k][n] act[k][m]) for k < k_eff, in place on the activation tile;
-// wt is [k_rows][W] in global memory; rows k_eff .. k_rows-1 are loaded but multiply zeros.
+// out[n][m] = act(sum_k wt[k][n] act[k][m]) for k < k_eff, in place on the activation tile, with
+// ReLU (the workload's network) or LeakyReLU (the reference network, W = 32); wt is [k_rows][W]
+// in global memory; rows k_eff .. k_rows-1 are loaded but multiply zeros.
 template <int W>
 __device__ __forceinline__ void hidden_layer(const float* __restrict__ wt, int k_rows, int k_eff,
                                              float* act, float* wch, int tid) {
     simt::tile_gemm<W>(wt, k_rows, k_eff, act, wch, tid, [&](int n, int m0, const float* v) {
         float r[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) r[i] = fmaxf(v[i], 0.f);
+        for (int i = 0; i < 8; ++i) r[i] = W == 32 ? leaky(v[i]) : fmaxf(v[i], 0.f);
         simt::tile_store8(act, n, m0, r);
     });
 }
 
-// the network's narrow output layer for vertex column m: y[o] = sum_k wt[k][o] act[k][m]
+// the network's narrow output layer for vertex column m: y[o] = sum_k wt[k][o] act[k][m], with
+// wt [W][OUT rounded up to 4]
 template <int W, int OUT>
 __device__ __forceinline__ void output_layer(const float* __restrict__ wt, const float* act, int m,
                                              float* y) {
+    constexpr int OP = (OUT + 3) / 4 * 4;
     float acc[OUT];
 #pragma unroll
     for (int o = 0; o < OUT; ++o) acc[o] = 0.f;
 #pragma unroll 4
     for (int k = 0; k < W; ++k) {
         const float x = act[k * kLd + m];
-        const float4 w = __ldg(reinterpret_cast<const float4*>(wt + 4 * k));
-        acc[0] = fmaf(w.x, x, acc[0]);
-        if (OUT > 1) acc[1] = fmaf(w.y, x, acc[1]);
-        if (OUT > 2) acc[2] = fmaf(w.z, x, acc[2]);
+#pragma unroll
+        for (int q = 0; q < OP / 4; ++q) {
+            const float4 w = __ldg(reinterpret_cast<const float4*>(wt + OP * k + 4 * q));
+            const float wv[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                if (4 * q + e < OUT) acc[4 * q + e] = fmaf(wv[e], x, acc[4 * q + e]);
+        }
     }
 #pragma unroll
     for (int o = 0; o < OUT; ++o) y[o] = acc[o];
 }
 
-// hash-grid levels l0 .. l0+7 of vertex i into its column of the tile (FP32 table)
+// hash-grid levels l0 .. l0+NL-1 of vertex i into its column of the tile (FP32 table)
+template <int NL = 8>
 __device__ __forceinline__ void encode_levels8(const InferArgs& a, const float* p, int l0, float* act,
                                                int m) {
     const float2* table = reinterpret_cast<const float2*>(a.table);
 #pragma unroll 2
-    for (int l = l0; l < l0 + 8; ++l) {
+    for (int l = l0; l < l0 + NL; ++l) {
         const LevelDev L = a.enc.lv[l];
         const CellCoord c = cell_of(p, L.res);
         uint32_t rows[8];
@@ -97,6 +105,8 @@ __device__ __forceinline__ void encode_levels8(const InferArgs& a, const float* 
 template <int WS, int HS, int WR, int HR>
 __global__ void __launch_bounds__(kThr) k_infer_fp32(const __grid_constant__ InferArgs a) {
     static_assert(WS == WR, "one tile shape for both networks");
+    constexpr bool REF = WS == 32;             // the reference's shipped network
+    constexpr int SIN = stat_in_of(WS), SOUT = stat_out_of(WS);
     using S = FpShape<WS>;
     extern __shared__ float4 smem4[];
     float* act = reinterpret_cast<float*>(smem4);
@@ -108,7 +118,7 @@ __global__ void __launch_bounds__(kThr) k_infer_fp32(const __grid_constant__ Inf
     const uint32_t items = 2u * ST.total_tiles;
     // transposed layer images: [in][out] (outputs padded to 4), StatNet then RRSNet
     const float* s0 = a.wt_stat;
-    const float* s_out = s0 + (size_t)kStatIn * WS + (size_t)(HS - 1) * WS * WS;
+    const float* s_out = s0 + (size_t)SIN * WS + (size_t)(HS - 1) * WS * WS;
     const float* r0 = a.wt_rrs;
     const float* r_out = r0 + (size_t)kRrsIn * WR + (size_t)(HR - 1) * WR * WR;
 
@@ -120,8 +130,22 @@ __global__ void __launch_bounds__(kThr) k_infer_fp32(const __grid_constant__ Inf
         const uint32_t i = sg.offset + (t - sg.tile_start) * kTile + (u & 1u) * kTM + m;
         const bool valid = i < sg.offset + sg.count;
         __syncthreads();   // the previous item's column reads are over
-        // encoding: two threads per vertex (levels 0-7 + SH, levels 8-15 + misc lanes)
-        if (valid) {
+        // encoding: two threads per vertex (levels 0-7 + SH, levels 8-15 + misc lanes; the
+        // reference network: levels 0-3 + direction blobs, levels 4-7 + roughness blob)
+        if (REF) {
+            if (valid) {
+                float p[3];
+                norm_pos(a.enc, a.v.pos, i, p);
+                encode_levels8<4>(a, p, lead ? 0 : 4, act, m);
+                float blob[16];
+                ref_blob_lanes(a.v, i, blob);
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    act[(16 + (lead ? 0 : 8) + k) * kLd + m] = lead ? blob[k] : blob[8 + k];
+            } else {
+                for (int k = lead ? 0 : 16; k < (lead ? 16 : 32); ++k) act[k * kLd + m] = 0.f;
+            }
+        } else if (valid) {
             float p[3];
             norm_pos(a.enc, a.v.pos, i, p);
             if (lead) {
@@ -143,22 +167,25 @@ __global__ void __launch_bounds__(kThr) k_infer_fp32(const __grid_constant__ Inf
         }
         VertexAux aux{};
         if (lead && valid) aux = load_aux(a.v, i);
-        // StatNet: 56 live input lanes (48..55 misc, 56..63 zero)
-        hidden_layer<WS>(s0, kStatIn, 56, act, wch, tid);
+        // StatNet: 56 live input lanes (48..55 misc, 56..63 zero); the reference network's 32
+        hidden_layer<WS>(s0, SIN, REF ? 32 : 56, act, wch, tid);
 #pragma unroll 1
         for (int h = 1; h < HS; ++h)
-            hidden_layer<WS>(s0 + (size_t)kStatIn * WS + (size_t)(h - 1) * WS * WS, WS, WS, act,
+            hidden_layer<WS>(s0 + (size_t)SIN * WS + (size_t)(h - 1) * WS * WS, WS, WS, act,
                              wch, tid);
-        float y[3] = {0.f, 0.f, 0.f};
-        if (lead) {
-            output_layer<WS, 3>(s_out, act, m, y);
-            // glue: the RRSNet input in this vertex's column (10 live lanes)
-            float x1[16];
-            glue16_aux(a.fp, y, aux, x1);
+        float y[SOUT];
 #pragma unroll
-            for (int k = 0; k < 10; ++k) act[k * kLd + m] = x1[k];
+        for (int k = 0; k < SOUT; ++k) y[k] = 0.f;
+        if (lead) {
+            output_layer<WS, SOUT>(s_out, act, m, y);
+            // glue: the RRSNet input in this vertex's column (10 live lanes; the reference's 12)
+            float x1[16];
+            if (REF) glue16_ref_aux(y, aux, x1);
+            else glue16_aux(a.fp, y, aux, x1);
+#pragma unroll
+            for (int k = 0; k < (REF ? kRefRrsLanes : 10); ++k) act[k * kLd + m] = x1[k];
         }
-        hidden_layer<WR>(r0, kRrsIn, 10, act, wch, tid);
+        hidden_layer<WR>(r0, kRrsIn, REF ? kRefRrsLanes : 10, act, wch, tid);
 #pragma unroll 1
         for (int h = 1; h < HR; ++h)
             hidden_layer<WR>(r0 + (size_t)kRrsIn * WR + (size_t)(h - 1) * WR * WR, WR, WR, act,
@@ -167,11 +194,10 @@ __global__ void __launch_bounds__(kThr) k_infer_fp32(const __grid_constant__ Inf
         if (lead && valid) {
             float raw;
             output_layer<WR, 1>(r_out, act, m, &raw);
-            const float rrs = rrs_factor_aux(a.fp, y, raw, aux);
+            const float rrs = rrs_factor_aux<REF>(a.fp, y, raw, aux);
             if (a.stats) {
-                a.stats[3 * (size_t)i] = y[0];
-                a.stats[3 * (size_t)i + 1] = y[1];
-                a.stats[3 * (size_t)i + 2] = y[2];
+#pragma unroll
+                for (int k = 0; k < SOUT; ++k) a.stats[SOUT * (size_t)i + k] = y[k];
             }
             a.rrs[i] = rrs;
             if (a.scr || a.ext_acc)
@@ -213,6 +239,8 @@ cudaError_t launch_infer_fp32(const InferArgs& a, int ws, int hs, int wr, int hr
         return launch_cfg<128, 3, 128, 3>(a, sm_count, ctas_per_sm, s);
     if (ws == 64 && hs == 3 && wr == 64 && hr == 3)
         return launch_cfg<64, 3, 64, 3>(a, sm_count, ctas_per_sm, s);
+    if (ws == 32 && hs == 3 && wr == 32 && hr == 3)   // the reference network
+        return launch_cfg<32, 3, 32, 3>(a, sm_count, ctas_per_sm, s);
     return cudaErrorInvalidValue;
 }
 
@@ -230,6 +258,7 @@ int infer_max_ctas_fp32(int ws, int hs) {
     if (ws == 64 && hs == 2) return max_ctas_fp32<64, 2, 64, 2>();
     if (ws == 64 && hs == 3) return max_ctas_fp32<64, 3, 64, 3>();
     if (ws == 128 && hs == 3) return max_ctas_fp32<128, 3, 128, 3>();
+    if (ws == 32 && hs == 3) return max_ctas_fp32<32, 3, 32, 3>();
     return 0;
 }
 

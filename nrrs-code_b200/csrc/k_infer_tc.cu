@@ -22,6 +22,13 @@
 // the next tile as soon as the first layer has read the current one), the warpgroup computes
 // the SH and misc lanes into a second [128 x 32] block, and the first layer reads its K = 64
 // operand from the two blocks (K steps 0-1 and 2-3). No table gathers remain in this kernel.
+//
+// Activations in TMEM (TA, split mode 3): an SS MMA reads both operands from shared memory, and
+// at M = 128, N = 128 that alone uses the SM's whole shared-memory bandwidth, so with the
+// epilogue's tile writes on top the tensor pipe idles. With TA each warpgroup also owns an A
+// region in TMEM: the epilogue of a hidden layer writes its FP16/BF16 activations there with
+// tcgen05.st, and the next layer's tcgen05.mma reads A from TMEM and only the weights from
+// shared memory. The first layer of each network still reads its input tile from shared memory.
 #include "kernels.hpp"
 #include "tc_tile.cuh"
 
@@ -41,9 +48,9 @@ constexpr int tmem_cols(int w) { return w <= 32 ? 32 : (w <= 64 ? 64 : (w <= 128
 
 // PART: 0 = both networks in one kernel; 1 = StatNet only (writes the RRSNet input tiles);
 // 2 = RRSNet only (reads them). Each kernel holds only the weights of the networks it runs.
-template <int WS, int HS, int WR, int HR, int WGS, bool PRE, int PART = 0>
+template <int WS, int HS, int WR, int HR, int WGS, bool PRE, int PART = 0, bool TA = false>
 struct TcShape {
-    static constexpr int kStatElems = PackedNet<WS, HS, kStatIn>::kElems;
+    static constexpr int kStatElems = PackedNet<WS, HS, stat_in_of(WS)>::kElems;
     static constexpr int kRrsElems = PackedNet<WR, HR, kRrsIn>::kElems;
     static constexpr uint32_t kWBytes =
         (uint32_t)(PART == 0 ? kStatElems + kRrsElems : (PART == 1 ? kStatElems : kRrsElems)) * 2u;
@@ -51,8 +58,10 @@ struct TcShape {
     static constexpr int kKMax =
         PART == 0 ? cmax(64, cmax(WS, WR)) : (PART == 1 ? cmax(64, WS) : cmax(16, WR));
     static constexpr uint32_t kABytes = 128u * kKMax * 2u;
-    static constexpr uint32_t kColsWg =
+    // TMEM per warpgroup: the accumulator D, and with TA the A region after it
+    static constexpr uint32_t kColsD =
         (uint32_t)tmem_cols(PART == 0 ? cmax(WS, WR) : (PART == 1 ? WS : WR));
+    static constexpr uint32_t kColsWg = TA ? 2 * kColsD : kColsD;
     static constexpr uint32_t kCols = kColsWg * WGS;
     static constexpr uint32_t kAOff = (kWBytes + 1023u) / 1024u * 1024u;
     // split mode: per warpgroup a hash-feature block and an SH/misc block, kept apart from the
@@ -92,7 +101,7 @@ __device__ __forceinline__ void encode_row_tc(const InferArgs& a, uint32_t i, ui
         for (int j = 0; j < 4; ++j) {
             const LevelDev L = a.enc.lv[lq * 4 + j];
             const CellCoord c = cell_of(p, L.res);
-            const float2 fv = level_features_h(table, L, a.enc.hash_mask, c);
+            const float2 fv = level_features_h(table, a.enc.cells, L, a.enc.hash_mask, c);
             f[2 * j] = fv.x;
             f[2 * j + 1] = fv.y;
         }
@@ -107,6 +116,33 @@ __device__ __forceinline__ void encode_row_tc(const InferArgs& a, uint32_t i, ui
     misc_lanes(a.v, i, misc);
     store_chunk(sA, m, 6, 64, pack8<BF>(misc));
     store_chunk(sA, m, 7, 64, make_uint4(0u, 0u, 0u, 0u));
+}
+
+// the reference network's StatNet input row of vertex i (K = 32): 8 hash levels (FP16 table),
+// then the one-blob lanes of the lat-long direction and of the warped roughness
+template <bool BF>
+__device__ __forceinline__ void encode_row_tc_ref(const InferArgs& a, uint32_t i, uint8_t* sA,
+                                                  int m) {
+    float p[3];
+    norm_pos(a.enc, a.v.pos, i, p);
+    const __half2* table = reinterpret_cast<const __half2*>(a.table_h);
+#pragma unroll 1
+    for (int lq = 0; lq < 2; ++lq) {
+        float f[8];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const LevelDev L = a.enc.lv[lq * 4 + j];
+            const CellCoord c = cell_of(p, L.res);
+            const float2 fv = level_features_h(table, a.enc.cells, L, a.enc.hash_mask, c);
+            f[2 * j] = fv.x;
+            f[2 * j + 1] = fv.y;
+        }
+        store_chunk(sA, m, lq, kRefStatIn, pack8<BF>(f));
+    }
+    float blob[16];
+    ref_blob_lanes(a.v, i, blob);
+    store_chunk(sA, m, 2, kRefStatIn, pack8<BF>(blob));
+    store_chunk(sA, m, 3, kRefStatIn, pack8<BF>(blob + 8));
 }
 
 // split mode: SH and misc lanes of vertex i as row m of a [128 x 32] block (the StatNet
@@ -171,11 +207,41 @@ __device__ __forceinline__ bool tc_layer(const uint8_t* sA, const uint8_t* sWl, 
     return ok;
 }
 
-template <int WS, int HS, int WR, int HR, bool BF, int WGS, bool PRE, int PART>
-__global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
+// a hidden or output layer with A in TMEM (8 columns per K = 16 step) and B in shared memory
+template <int K, int N, bool BF>
+__device__ __forceinline__ bool tc_layer_ts(uint32_t tmem_a, const uint8_t* sWl, uint32_t tmem,
+                                            uint64_t* bar, uint32_t& phase, int ltid) {
+    if (ltid == 0) {
+        tc::fence_after_sync();
+        const uint32_t b0 = tc::smem_u32(sWl);
+        constexpr uint32_t idesc = tc::idesc_f16(N, BF ? 1u : 0u);
+#pragma unroll
+        for (int kk = 0; kk < K / 16; ++kk) {
+            const uint64_t bd = tc::smem_desc(b0 + kk * 256, 128, K * 16);
+            tc::mma_f16_ts(tmem, tmem_a + 8u * kk, bd, idesc, kk > 0 ? 1u : 0u);
+        }
+        tc::mma_commit(bar);
+    }
+    const bool ok = tc::mbar_wait(bar, phase, kSpin);
+    phase ^= 1u;
+    tc::fence_after_sync();
+    return ok;
+}
+
+// the TMEM stores of the warpgroup's epilogue are complete before its next MMA is issued
+__device__ __forceinline__ void wg_sync_tmem(int wg) {
+    tc::fence_before_sync();
+    wg_sync(wg);
+}
+
+template <int WS, int HS, int WR, int HR, bool BF, int WGS, bool PRE, int PART, bool TA = false>
+__global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64 && !TA) ? 3 : 1)
     k_infer_tc(const __grid_constant__ InferArgs a) {
-    using S = TcShape<WS, HS, WR, HR, WGS, PRE, PART>;
+    using S = TcShape<WS, HS, WR, HR, WGS, PRE, PART, TA>;
+    static_assert(!TA || PART != 0, "activations in TMEM: split mode 3 kernels");
     constexpr bool kStat = PART != 2, kRrs = PART != 1;
+    constexpr bool REF = WS == 32;   // the reference's shipped network (fused mode only)
+    static_assert(!REF || (!PRE && PART == 0), "the reference network runs fused");
     extern __shared__ uint8_t smem_raw[];
     uint8_t* base = reinterpret_cast<uint8_t*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023u) & ~uintptr_t(1023));
@@ -221,10 +287,12 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
     uint32_t phase = 0;
     // warp w of a warpgroup reads TMEM lanes 32*(w % 4) .. +31, i.e. rows of its own threads
     const uint32_t trow = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    // TA: the A region after D (the whole warpgroup's for the MMA, this warp's rows for stores)
+    const uint32_t tmem_a = tmem + S::kColsD, trow_a = trow + S::kColsD;
 
     // weight images in this kernel's shared copy: StatNet then RRSNet (each only if run here)
     const uint8_t* wS0 = sW;
-    const uint8_t* wSh = wS0 + WS * kStatIn * 2;
+    const uint8_t* wSh = wS0 + WS * stat_in_of(WS) * 2;
     const uint8_t* wSo = wSh + (HS - 1) * WS * WS * 2;
     const uint8_t* wR0 = kStat ? wSo + 16 * WS * 2 : sW;
     const uint8_t* wRh = wR0 + WR * kRrsIn * 2;
@@ -274,8 +342,11 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
                 hphase ^= 1u;
                 h_pending = false;
             } else {
-                if (valid) encode_row_tc<BF>(a, i, sA, ltid);
-                else zero_row(sA, ltid, 64);
+                if (valid) {
+                    if constexpr (REF) encode_row_tc_ref<BF>(a, i, sA, ltid);
+                    else encode_row_tc<BF>(a, i, sA, ltid);
+                }
+                else zero_row(sA, ltid, REF ? kRefStatIn : 64);
             }
             wg_sync_for_mma(wg);
 
@@ -285,24 +356,39 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
                 // the first layer has read the block: bring in the next tile's features
                 if (!S::kShare && ok && t + tstride < total_tiles) fetch_features(t + tstride);
             } else {
-                ok &= tc_layer<kStatIn, WS, BF>(sA, wS0, tmem, mbar, phase, ltid);
+                ok &= tc_layer<stat_in_of(WS), WS, BF>(sA, wS0, tmem, mbar, phase, ltid);
             }
-            epilogue_relu<WS, BF>(trow, sA, ltid);
-            wg_sync_for_mma(wg);
+            if constexpr (TA) {
+                epilogue_act_tmem<WS, BF, REF>(trow, trow_a);
+                wg_sync_tmem(wg);
 #pragma unroll 1
-            for (int h = 1; h < HS; ++h) {
-                ok &= tc_layer<WS, WS, BF>(sA, wSh + (h - 1) * WS * WS * 2, tmem, mbar, phase, ltid);
-                epilogue_relu<WS, BF>(trow, sA, ltid);
+                for (int h = 1; h < HS; ++h) {
+                    ok &= tc_layer_ts<WS, WS, BF>(tmem_a, wSh + (h - 1) * WS * WS * 2, tmem, mbar,
+                                                  phase, ltid);
+                    epilogue_act_tmem<WS, BF, REF>(trow, trow_a);
+                    wg_sync_tmem(wg);
+                }
+                ok &= tc_layer_ts<WS, 16, BF>(tmem_a, wSo, tmem, mbar, phase, ltid);
+            } else {
+                epilogue_act<WS, BF, REF>(trow, sA, ltid);
                 wg_sync_for_mma(wg);
+#pragma unroll 1
+                for (int h = 1; h < HS; ++h) {
+                    ok &= tc_layer<WS, WS, BF>(sA, wSh + (h - 1) * WS * WS * 2, tmem, mbar, phase,
+                                               ltid);
+                    epilogue_act<WS, BF, REF>(trow, sA, ltid);
+                    wg_sync_for_mma(wg);
+                }
+                ok &= tc_layer<WS, 16, BF>(sA, wSo, tmem, mbar, phase, ltid);
             }
-            ok &= tc_layer<WS, 16, BF>(sA, wSo, tmem, mbar, phase, ltid);
             tc::tmem_ld16(trow, y);
             tc::tmem_wait_ld();
 
             // ---- glue -> RRSNet input (K = 16) ----
             float x1[16];
             if (valid) {
-                glue16_aux(a.fp, y, aux, x1);
+                if constexpr (REF) glue16_ref_aux(y, aux, x1);
+                else glue16_aux(a.fp, y, aux, x1);
             } else {
 #pragma unroll
                 for (int k = 0; k < 16; ++k) x1[k] = 0.f;
@@ -329,15 +415,29 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
         if constexpr (kRrs) {
             // ---- RRSNet ----
             ok &= tc_layer<kRrsIn, WR, BF>(sA, wR0, tmem, mbar, phase, ltid);
-            epilogue_relu<WR, BF>(trow, sA, ltid);
-            wg_sync_for_mma(wg);
+            if constexpr (TA) {
+                epilogue_act_tmem<WR, BF, REF>(trow, trow_a);
+                wg_sync_tmem(wg);
 #pragma unroll 1
-            for (int h = 1; h < HR; ++h) {
-                ok &= tc_layer<WR, WR, BF>(sA, wRh + (h - 1) * WR * WR * 2, tmem, mbar, phase, ltid);
-                epilogue_relu<WR, BF>(trow, sA, ltid);
+                for (int h = 1; h < HR; ++h) {
+                    ok &= tc_layer_ts<WR, WR, BF>(tmem_a, wRh + (h - 1) * WR * WR * 2, tmem, mbar,
+                                                  phase, ltid);
+                    epilogue_act_tmem<WR, BF, REF>(trow, trow_a);
+                    wg_sync_tmem(wg);
+                }
+                ok &= tc_layer_ts<WR, 16, BF>(tmem_a, wRo, tmem, mbar, phase, ltid);
+            } else {
+                epilogue_act<WR, BF, REF>(trow, sA, ltid);
                 wg_sync_for_mma(wg);
+#pragma unroll 1
+                for (int h = 1; h < HR; ++h) {
+                    ok &= tc_layer<WR, WR, BF>(sA, wRh + (h - 1) * WR * WR * 2, tmem, mbar, phase,
+                                               ltid);
+                    epilogue_act<WR, BF, REF>(trow, sA, ltid);
+                    wg_sync_for_mma(wg);
+                }
+                ok &= tc_layer<WR, 16, BF>(sA, wRo, tmem, mbar, phase, ltid);
             }
-            ok &= tc_layer<WR, 16, BF>(sA, wRo, tmem, mbar, phase, ltid);
             tc::tmem_ld16(trow, r);
             tc::tmem_wait_ld();
         } else {
@@ -353,12 +453,11 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
         long long term = 0;
         if (valid) {
             if (kStat && a.stats) {
-                a.stats[3 * (size_t)i] = y[0];
-                a.stats[3 * (size_t)i + 1] = y[1];
-                a.stats[3 * (size_t)i + 2] = y[2];
+#pragma unroll
+                for (int k = 0; k < stat_out_of(WS); ++k) a.stats[stat_out_of(WS) * (size_t)i + k] = y[k];
             }
             if (factor_here) {
-                const float rrs = rrs_factor_aux(a.fp, y, r[0], aux);
+                const float rrs = rrs_factor_aux<REF>(a.fp, y, r[0], aux);
                 a.rrs[i] = rrs;
                 if (a.scr || a.ext_acc)
                     term = fixed_term(a.fp, rrs, a.scr ? &a.scr->status : &g_dummy_status);
@@ -388,11 +487,11 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64) ? 3 : 1)
     }
 }
 
-template <int WS, int HS, int WR, int HR, bool BF, int WGS, bool PRE, int PART>
+template <int WS, int HS, int WR, int HR, bool BF, int WGS, bool PRE, int PART, bool TA = false>
 cudaError_t launch_tc(const InferArgs& a, int sm_count, int ctas_per_sm, cudaStream_t s) {
-    using S = TcShape<WS, HS, WR, HR, WGS, PRE, PART>;
-    if (S::kSmem > 232448) return cudaErrorInvalidConfiguration;
-    auto kern = k_infer_tc<WS, HS, WR, HR, BF, WGS, PRE, PART>;
+    using S = TcShape<WS, HS, WR, HR, WGS, PRE, PART, TA>;
+    if (S::kSmem > 232448 || S::kCols > 512) return cudaErrorInvalidConfiguration;
+    auto kern = k_infer_tc<WS, HS, WR, HR, BF, WGS, PRE, PART, TA>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)S::kSmem);
     if (e != cudaSuccess) return e;
@@ -408,10 +507,22 @@ cudaError_t launch_tc(const InferArgs& a, int sm_count, int ctas_per_sm, cudaStr
     return cudaGetLastError();
 }
 
-// part: 0 both networks (fused or split-1), 1 StatNet only, 2 RRSNet only (split-2)
+// part: 0 both networks (fused or split-1), 1 StatNet only, 2 RRSNet only (split-2); tmem_act:
+// parts 1 and 2 with the activations in TMEM (split-3; 1 or 2 warpgroups)
 template <int WS, int HS, int WR, int HR, bool BF>
 cudaError_t launch_wgs(const InferArgs& a, int sm_count, int ctas_per_sm, int wgs, int part,
-                       cudaStream_t s) {
+                       bool tmem_act, cudaStream_t s) {
+    if (tmem_act) {
+        if (part == 1) {
+            if (wgs == 2) return launch_tc<WS, HS, WR, HR, BF, 2, true, 1, true>(a, sm_count, ctas_per_sm, s);
+            if (wgs == 1) return launch_tc<WS, HS, WR, HR, BF, 1, true, 1, true>(a, sm_count, ctas_per_sm, s);
+        }
+        if (part == 2) {
+            if (wgs == 2) return launch_tc<WS, HS, WR, HR, BF, 2, true, 2, true>(a, sm_count, ctas_per_sm, s);
+            if (wgs == 1) return launch_tc<WS, HS, WR, HR, BF, 1, true, 2, true>(a, sm_count, ctas_per_sm, s);
+        }
+        return cudaErrorInvalidConfiguration;
+    }
     if (part == 1) {
         if (wgs == 4) return launch_tc<WS, HS, WR, HR, BF, 4, true, 1>(a, sm_count, ctas_per_sm, s);
         if (wgs == 2) return launch_tc<WS, HS, WR, HR, BF, 2, true, 1>(a, sm_count, ctas_per_sm, s);
@@ -432,27 +543,33 @@ cudaError_t launch_wgs(const InferArgs& a, int sm_count, int ctas_per_sm, int wg
     return cudaErrorInvalidConfiguration;
 }
 
-template <int WS, int HS, int WR, int HR, bool BF, int WGS, bool PRE, int PART>
+template <int WS, int HS, int WR, int HR, bool BF, int WGS, bool PRE, int PART, bool TA = false>
 int max_ctas_tc() {
-    using S = TcShape<WS, HS, WR, HR, WGS, PRE, PART>;
-    if (S::kSmem > 232448) return 0;
-    auto kern = k_infer_tc<WS, HS, WR, HR, BF, WGS, PRE, PART>;
+    using S = TcShape<WS, HS, WR, HR, WGS, PRE, PART, TA>;
+    if (S::kSmem > 232448 || S::kCols > 512) return 0;
+    auto kern = k_infer_tc<WS, HS, WR, HR, BF, WGS, PRE, PART, TA>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kSmem) !=
         cudaSuccess)
         return 0;
     return resident_ctas((const void*)kern, 128 * WGS, S::kSmem, 512 / (int)S::kCols);
 }
 
-template <int WS, int HS, bool BF, int WGS>
+template <int WS, int HS, bool BF, int WGS, bool TA = false>
 int max_ctas_split2() {
-    const int m1 = max_ctas_tc<WS, HS, WS, HS, BF, WGS, true, 1>();
-    const int m2 = max_ctas_tc<WS, HS, WS, HS, BF, WGS, true, 2>();
+    const int m1 = max_ctas_tc<WS, HS, WS, HS, BF, WGS, true, 1, TA>();
+    const int m2 = max_ctas_tc<WS, HS, WS, HS, BF, WGS, true, 2, TA>();
     return m1 < m2 ? m1 : m2;
 }
 
-// split: 0 fused, 1 encoding kernel + one MLP kernel, 2 encoding + StatNet + RRSNet kernels
+// split: 0 fused, 1 encoding kernel + one MLP kernel, 2 encoding + StatNet + RRSNet kernels,
+// 3 as 2 with the hidden activations in TMEM
 template <int WS, int HS, bool BF>
 int max_ctas_of(int wgs, int split) {
+    if (split == 3) {
+        if (wgs == 2) return max_ctas_split2<WS, HS, BF, 2, true>();
+        if (wgs == 1) return max_ctas_split2<WS, HS, BF, 1, true>();
+        return 0;
+    }
     if (split == 2) {
         if (wgs == 4) return max_ctas_split2<WS, HS, BF, 4>();
         if (wgs == 2) return max_ctas_split2<WS, HS, BF, 2>();
@@ -476,6 +593,11 @@ int infer_max_ctas(int ws, int hs, int wr, int hr, int prec, int wgs, int split)
     if (ws == 64 && hs == 2) return bf ? max_ctas_of<64, 2, true>(wgs, split) : max_ctas_of<64, 2, false>(wgs, split);
     if (ws == 64 && hs == 3) return bf ? max_ctas_of<64, 3, true>(wgs, split) : max_ctas_of<64, 3, false>(wgs, split);
     if (ws == 128 && hs == 3) return bf ? max_ctas_of<128, 3, true>(wgs, split) : max_ctas_of<128, 3, false>(wgs, split);
+    if (ws == 32 && hs == 3) {   // the reference network: fused mode, 1 or 2 warpgroups
+        if (split != 0 || (wgs != 1 && wgs != 2)) return 0;
+        if (wgs == 2) return bf ? max_ctas_tc<32, 3, 32, 3, true, 2, false, 0>() : max_ctas_tc<32, 3, 32, 3, false, 2, false, 0>();
+        return bf ? max_ctas_tc<32, 3, 32, 3, true, 1, false, 0>() : max_ctas_tc<32, 3, 32, 3, false, 1, false, 0>();
+    }
     return 0;
 }
 
@@ -483,21 +605,34 @@ size_t infer_tc_smem_bytes(int ws, int hs, int wr, int hr) {
     if (ws == 64 && hs == 2) return TcShape<64, 2, 64, 2, 1, false, 0>::kSmem;
     if (ws == 64 && hs == 3) return TcShape<64, 3, 64, 3, 1, false, 0>::kSmem;
     if (ws == 128 && hs == 3) return TcShape<128, 3, 128, 3, 1, false, 0>::kSmem;
+    if (ws == 32 && hs == 3) return TcShape<32, 3, 32, 3, 1, false, 0>::kSmem;
     return 0;
 }
 
 cudaError_t launch_infer_tc(const InferArgs& a, int ws, int hs, int wr, int hr, int prec,
-                            int sm_count, int ctas_per_sm, int wgs, int part, cudaStream_t s) {
+                            int sm_count, int ctas_per_sm, int wgs, int part, bool tmem_act,
+                            cudaStream_t s) {
     const bool bf = prec == NRRS_PREC_BF16;
+    const bool ta = tmem_act;
     if (ws == 64 && hs == 2 && wr == 64 && hr == 2)
-        return bf ? launch_wgs<64, 2, 64, 2, true>(a, sm_count, ctas_per_sm, wgs, part, s)
-                  : launch_wgs<64, 2, 64, 2, false>(a, sm_count, ctas_per_sm, wgs, part, s);
+        return bf ? launch_wgs<64, 2, 64, 2, true>(a, sm_count, ctas_per_sm, wgs, part, ta, s)
+                  : launch_wgs<64, 2, 64, 2, false>(a, sm_count, ctas_per_sm, wgs, part, ta, s);
     if (ws == 64 && hs == 3 && wr == 64 && hr == 3)
-        return bf ? launch_wgs<64, 3, 64, 3, true>(a, sm_count, ctas_per_sm, wgs, part, s)
-                  : launch_wgs<64, 3, 64, 3, false>(a, sm_count, ctas_per_sm, wgs, part, s);
+        return bf ? launch_wgs<64, 3, 64, 3, true>(a, sm_count, ctas_per_sm, wgs, part, ta, s)
+                  : launch_wgs<64, 3, 64, 3, false>(a, sm_count, ctas_per_sm, wgs, part, ta, s);
     if (ws == 128 && hs == 3 && wr == 128 && hr == 3)  // 158 KB of weights in one kernel
-        return bf ? launch_wgs<128, 3, 128, 3, true>(a, sm_count, ctas_per_sm, wgs, part, s)
-                  : launch_wgs<128, 3, 128, 3, false>(a, sm_count, ctas_per_sm, wgs, part, s);
+        return bf ? launch_wgs<128, 3, 128, 3, true>(a, sm_count, ctas_per_sm, wgs, part, ta, s)
+                  : launch_wgs<128, 3, 128, 3, false>(a, sm_count, ctas_per_sm, wgs, part, ta, s);
+    if (ws == 32 && hs == 3 && wr == 32 && hr == 3) {  // the reference network: fused only
+        if (part != 0 || a.enc_tiles || tmem_act) return cudaErrorInvalidValue;
+        if (wgs == 2)
+            return bf ? launch_tc<32, 3, 32, 3, true, 2, false, 0>(a, sm_count, ctas_per_sm, s)
+                      : launch_tc<32, 3, 32, 3, false, 2, false, 0>(a, sm_count, ctas_per_sm, s);
+        if (wgs == 1)
+            return bf ? launch_tc<32, 3, 32, 3, true, 1, false, 0>(a, sm_count, ctas_per_sm, s)
+                      : launch_tc<32, 3, 32, 3, false, 1, false, 0>(a, sm_count, ctas_per_sm, s);
+        return cudaErrorInvalidConfiguration;
+    }
     return cudaErrorInvalidValue;
 }
 

@@ -83,12 +83,13 @@ using simt::kTM;
 // activation tile rows and weight-chunk floats of the training kernels
 template <int W>
 struct TrShape {
-    static constexpr int kRows = simt::imax(kStatIn, W);
-    static constexpr int kChunk = simt::kKC * simt::imax(64, W);
+    static constexpr int kRows = simt::imax(stat_in_of(W), W);
+    static constexpr int kChunk = simt::kKC * simt::imax(stat_in_of(W), W);
     static constexpr size_t kSmem = sizeof(float) * ((size_t)kRows * kLd + 2 * kChunk);
 };
 
-// forward layer: ReLU in place, and the activations to scratch rows row0 + n (samples i0 ..)
+// forward layer: ReLU (LeakyReLU for the reference network, W = 32) in place, and the activations
+// to scratch rows row0 + n (samples i0 ..)
 template <int W>
 __device__ __forceinline__ void fwd_layer(const float* __restrict__ wt, int k_rows, int k_eff,
                                           float* tile, float* wch, int tid, float* scr,
@@ -96,7 +97,7 @@ __device__ __forceinline__ void fwd_layer(const float* __restrict__ wt, int k_ro
     simt::tile_gemm<W>(wt, k_rows, k_eff, tile, wch, tid, [&](int n, int m0, const float* v) {
         float r[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) r[i] = fmaxf(v[i], 0.f);
+        for (int i = 0; i < 8; ++i) r[i] = W == 32 ? leaky(v[i]) : fmaxf(v[i], 0.f);
         simt::tile_store8(tile, n, m0, r);
         if (store) {
             float* g = scr + (size_t)(row0 + n) * ld + i0 + m0;
@@ -107,8 +108,9 @@ __device__ __forceinline__ void fwd_layer(const float* __restrict__ wt, int k_ro
 }
 
 // backward layer through row-major W [k_rows = outputs of the forward layer][W = its inputs]:
-// delta_in[n][m] = (sum_k W[k][n] delta_out[k][m]) masked by the forward activation stored in
-// scratch rows mask0 + n; in place, and to scratch rows out0 + n
+// delta_in[n][m] = (sum_k W[k][n] delta_out[k][m]) times the activation's slope at the forward
+// activation stored in scratch rows mask0 + n (ReLU: 1 or 0; LeakyReLU: 1 or 0.01); in place, and
+// to scratch rows out0 + n
 template <int W>
 __device__ __forceinline__ void bwd_layer(const float* __restrict__ w, int k_rows, float* tile,
                                           float* wch, int tid, float* scr, uint32_t ld, uint32_t i0,
@@ -120,7 +122,7 @@ __device__ __forceinline__ void bwd_layer(const float* __restrict__ w, int k_row
         const float hv[8] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
         float r[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) r[i] = hv[i] > 0.f ? v[i] : 0.f;
+        for (int i = 0; i < 8; ++i) r[i] = hv[i] > 0.f ? v[i] : (W == 32 ? 0.01f * v[i] : 0.f);
         simt::tile_store8(tile, n, m0, r);
         float* g = scr + (size_t)(out0 + n) * ld + i0 + m0;
         *reinterpret_cast<float4*>(g) = make_float4(r[0], r[1], r[2], r[3]);
@@ -132,16 +134,21 @@ __device__ __forceinline__ void bwd_layer(const float* __restrict__ w, int k_row
 template <int W, int OUT>
 __device__ __forceinline__ void narrow_out(const float* __restrict__ wt, const float* tile, int m,
                                            float* y) {
+    constexpr int OP = (OUT + 3) / 4 * 4;   // wt is [W][OUT rounded up to 4]
     float acc[OUT];
 #pragma unroll
     for (int o = 0; o < OUT; ++o) acc[o] = 0.f;
 #pragma unroll 4
     for (int k = 0; k < W; ++k) {
         const float x = tile[k * kLd + m];
-        const float4 w = __ldg(reinterpret_cast<const float4*>(wt + 4 * k));
-        acc[0] = fmaf(w.x, x, acc[0]);
-        if (OUT > 1) acc[1] = fmaf(w.y, x, acc[1]);
-        if (OUT > 2) acc[2] = fmaf(w.z, x, acc[2]);
+#pragma unroll
+        for (int q = 0; q < OP / 4; ++q) {
+            const float4 w = __ldg(reinterpret_cast<const float4*>(wt + OP * k + 4 * q));
+            const float wv[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                if (4 * q + e < OUT) acc[4 * q + e] = fmaf(wv[e], x, acc[4 * q + e]);
+        }
     }
 #pragma unroll
     for (int o = 0; o < OUT; ++o) y[o] = acc[o];
@@ -155,6 +162,10 @@ __device__ __forceinline__ void narrow_out(const float* __restrict__ wt, const f
 template <int WS, int HS, int WR, int HR>
 __global__ void __launch_bounds__(simt::kThr) k_train_stat(const __grid_constant__ TrainArgs a) {
     static_assert(WS == WR, "one tile shape for both networks");
+    constexpr bool REF = WS == 32;             // the reference's shipped network
+    constexpr int SIN = stat_in_of(WS), SOUT = stat_out_of(WS);
+    constexpr int NLH = REF ? kRefLevels / 2 : 8;   // hash levels per thread (two per sample)
+    constexpr int X1 = REF ? kRefRrsLanes : 10;     // live RRSNet input lanes
     using S = TrShape<WS>;
     extern __shared__ float4 smem4[];
     float* tile = reinterpret_cast<float*>(smem4);
@@ -170,9 +181,9 @@ __global__ void __launch_bounds__(simt::kThr) k_train_stat(const __grid_constant
     const float2* table = reinterpret_cast<const float2*>(a.table);
     // forward (transposed) and backward (row-major) layer images
     const float* ts = a.wt_stat;
-    const float* ts_out = ts + (size_t)kStatIn * WS + (size_t)(HS - 1) * WS * WS;
+    const float* ts_out = ts + (size_t)SIN * WS + (size_t)(HS - 1) * WS * WS;
     const float* rs = a.w_stat;
-    const float* rs_out = rs + (size_t)kStatIn * WS + (size_t)(HS - 1) * WS * WS;   // [3][WS]
+    const float* rs_out = rs + (size_t)SIN * WS + (size_t)(HS - 1) * WS * WS;   // [SOUT][WS]
     const float* tr = a.wt_rrs;
     const float* tr_out = tr + (size_t)kRrsIn * WR + (size_t)(HR - 1) * WR * WR;
     const uint32_t items = (a.n + kTM - 1) / kTM;
@@ -187,7 +198,7 @@ __global__ void __launch_bounds__(simt::kThr) k_train_stat(const __grid_constant
         if (valid) {
             norm_pos(a.enc, a.v.pos, i, p);
 #pragma unroll 2
-            for (int l = half * 8; l < half * 8 + 8; ++l) {
+            for (int l = half * NLH; l < half * NLH + NLH; ++l) {
                 const LevelDev L = a.enc.lv[l];
                 const CellCoord c = cell_of(p, L.res);
                 float f0 = 0.f, f1 = 0.f;
@@ -203,7 +214,14 @@ __global__ void __launch_bounds__(simt::kThr) k_train_stat(const __grid_constant
                 tile[(2 * l) * kLd + m] = f0;
                 tile[(2 * l + 1) * kLd + m] = f1;
             }
-            if (half == 0) {
+            if (REF) {
+                // the reference network: direction blobs (half 0) or roughness blob (half 1)
+                float blob[16];
+                ref_blob_lanes(a.v, i, blob);
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    tile[(16 + 8 * half + k) * kLd + m] = half ? blob[8 + k] : blob[k];
+            } else if (half == 0) {
                 float sh[16];
                 const size_t i3 = 3 * (size_t)i;
                 sh16(a.v.wi[i3], a.v.wi[i3 + 1], a.v.wi[i3 + 2], sh);
@@ -215,71 +233,92 @@ __global__ void __launch_bounds__(simt::kThr) k_train_stat(const __grid_constant
 #pragma unroll
                 for (int k = 0; k < 8; ++k) tile[(48 + k) * kLd + m] = mm[k];
             }
-            const int k0 = half ? 16 : 0, k1 = half ? 32 : 16;   // hash lanes of this half
-            for (int k = k0; k < k1; ++k) scr[(size_t)(a.r_x0 + k) * ld + i] = tile[k * kLd + m];
-            const int q0 = half ? 48 : 32, q1 = half ? 56 : 48;  // SH or misc lanes
+            const int hl = 2 * NLH;                              // hash lanes of this half
+            for (int k = half * hl; k < half * hl + hl; ++k)
+                scr[(size_t)(a.r_x0 + k) * ld + i] = tile[k * kLd + m];
+            const int q0 = REF ? 16 + 8 * half : (half ? 48 : 32);
+            const int q1 = REF ? q0 + 8 : (half ? 56 : 48);      // the other lanes of this half
             for (int k = q0; k < q1; ++k) scr[(size_t)(a.r_x0 + k) * ld + i] = tile[k * kLd + m];
         } else {
-            for (int k = half ? 28 : 0; k < (half ? 56 : 28); ++k) tile[k * kLd + m] = 0.f;
+            constexpr int LANES = REF ? 32 : 56;
+            for (int k = half * LANES / 2; k < (half + 1) * LANES / 2; ++k) tile[k * kLd + m] = 0.f;
         }
 
         // ---- StatNet forward, every hidden activation to scratch ----
-        fwd_layer<WS>(ts, kStatIn, 56, tile, wch, tid, scr, ld, i0, a.r_hs, true);
+        fwd_layer<WS>(ts, SIN, REF ? 32 : 56, tile, wch, tid, scr, ld, i0, a.r_hs, true);
 #pragma unroll 1
         for (int h = 1; h < HS; ++h)
-            fwd_layer<WS>(ts + (size_t)kStatIn * WS + (size_t)(h - 1) * WS * WS, WS, WS, tile, wch,
+            fwd_layer<WS>(ts + (size_t)SIN * WS + (size_t)(h - 1) * WS * WS, WS, WS, tile, wch,
                           tid, scr, ld, i0, a.r_hs + h * WS, true);
 
         // ---- output, loss gradient, and the delta of the last hidden layer (own column) ----
-        float y[3] = {0.f, 0.f, 0.f};
+        float y[SOUT];
+#pragma unroll
+        for (int k = 0; k < SOUT; ++k) y[k] = 0.f;
         SampleMul mu{1.f, 1.f, 1.f, 0.f};
         if (lead) {
-            narrow_out<WS, 3>(ts_out, tile, m, y);
-            float g[3] = {0.f, 0.f, 0.f};
+            narrow_out<WS, SOUT>(ts_out, tile, m, y);
+            float g[SOUT];
+#pragma unroll
+            for (int k = 0; k < SOUT; ++k) g[k] = 0.f;
             if (valid) {
                 const size_t i3 = 3 * (size_t)i;
                 mu = sample_mul(a.lw, i, a.n);
+                if (REF) {
+                    // relative squared error of L and L^2 against the target L and its square
 #pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    const float d = y[c] - logf(a.target[i3 + c] + a.fp.stat_eps);
-                    if (a.lw.active) {
-                        lossS += (double)mu.stat * (double)d * (double)d;
-                        g[c] = mu.stat * (2.0f * d) / (3.0f * (float)a.n);
-                    } else {
-                        lossS += (double)d * (double)d;
-                        g[c] = 2.0f * d / (3.0f * (float)a.n);
+                    for (int c = 0; c < 6; ++c) {
+                        const float L = a.target[i3 + (c % 3)];
+                        const float T = c < 3 ? L : L * L;
+                        const float den = T * T + 0.01f;
+                        const float d = y[c] - T;
+                        lossS += (double)mu.stat * (double)d * (double)d / (double)den;
+                        g[c] = mu.stat * (2.0f * d) / (den * 6.0f * (float)a.n);
+                        scr[(size_t)(a.r_dy + c) * ld + i] = g[c];
                     }
-                    scr[(size_t)(a.r_dy + c) * ld + i] = g[c];
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const float d = y[c] - logf(a.target[i3 + c] + a.fp.stat_eps);
+                        if (a.lw.active) {
+                            lossS += (double)mu.stat * (double)d * (double)d;
+                            g[c] = mu.stat * (2.0f * d) / (3.0f * (float)a.n);
+                        } else {
+                            lossS += (double)d * (double)d;
+                            g[c] = 2.0f * d / (3.0f * (float)a.n);
+                        }
+                        scr[(size_t)(a.r_dy + c) * ld + i] = g[c];
+                    }
                 }
             }
-            // d h_last = W_out^T g, masked by h_last (this column of the tile)
+            // d h_last = W_out^T g times the activation's slope at h_last (this column)
             float* dl = scr + (size_t)(a.r_dhs + (HS - 1) * WS) * ld + i;
 #pragma unroll 4
             for (int k = 0; k < WS; ++k) {
                 float acc = 0.f;
 #pragma unroll
-                for (int o = 0; o < 3; ++o) acc = fmaf(rs_out[o * WS + k], g[o], acc);
-                const float dk = tile[k * kLd + m] > 0.f ? acc : 0.f;
+                for (int o = 0; o < SOUT; ++o) acc = fmaf(rs_out[o * WS + k], g[o], acc);
+                const float dk = tile[k * kLd + m] > 0.f ? acc : (REF ? 0.01f * acc : 0.f);
                 tile[k * kLd + m] = dk;
                 if (valid) dl[(size_t)k * ld] = dk;
             }
         }
 
-        // ---- backward through the hidden layers, then the 32 hash-lane gradients ----
+        // ---- backward through the hidden layers, then the hash-lane gradients ----
 #pragma unroll 1
         for (int h = HS - 1; h >= 1; --h)
-            bwd_layer<WS>(rs + (size_t)kStatIn * WS + (size_t)(h - 1) * WS * WS, WS, tile, wch,
+            bwd_layer<WS>(rs + (size_t)SIN * WS + (size_t)(h - 1) * WS * WS, WS, tile, wch,
                           tid, scr, ld, i0, a.r_hs + (h - 1) * WS, a.r_dhs + (h - 1) * WS);
-        simt::tile_gemm<64>(rs, WS, WS, tile, wch, tid, [&](int n, int m0, const float* v) {
+        simt::tile_gemm<SIN>(rs, WS, WS, tile, wch, tid, [&](int n, int m0, const float* v) {
             simt::tile_store8(tile, n, m0, v);
         });
 
-        // ---- hash-grid scatter: two threads per sample, eight levels each ----
+        // ---- hash-grid scatter: two threads per sample, half the levels each ----
         {
             const unsigned lanes = valid_lanes(i0 + (uint32_t)(m & ~31), a.n);
             if (valid) {
 #pragma unroll 2
-                for (int l = half * 8; l < half * 8 + 8; ++l) {
+                for (int l = half * NLH; l < half * NLH + NLH; ++l) {
                     const LevelDev L = a.enc.lv[l];
                     const CellCoord c = cell_of(p, L.res);
                     warp_scatter_level(a.table_grad, L, a.enc.hash_mask, c, tile[(2 * l) * kLd + m],
@@ -293,14 +332,15 @@ __global__ void __launch_bounds__(simt::kThr) k_train_stat(const __grid_constant
         if (a.train_rrs) {
             if (lead) {
                 float x1[16];
-                glue16(a.fp, y, a.v, valid ? i : 0u, x1);
+                if (REF) glue16_ref_aux(y, load_aux(a.v, valid ? i : 0u), x1);
+                else glue16(a.fp, y, a.v, valid ? i : 0u, x1);
 #pragma unroll
-                for (int k = 0; k < 10; ++k) {
+                for (int k = 0; k < X1; ++k) {
                     tile[k * kLd + m] = valid ? x1[k] : 0.f;
                     if (valid) scr[(size_t)(a.r_x1 + k) * ld + i] = x1[k];
                 }
             }
-            fwd_layer<WR>(tr, kRrsIn, 10, tile, wch, tid, scr, ld, i0, 0, false);
+            fwd_layer<WR>(tr, kRrsIn, X1, tile, wch, tid, scr, ld, i0, 0, false);
 #pragma unroll 1
             for (int h = 1; h < HR; ++h)
                 fwd_layer<WR>(tr + (size_t)kRrsIn * WR + (size_t)(h - 1) * WR * WR, WR, WR, tile,
@@ -338,6 +378,8 @@ __global__ void __launch_bounds__(simt::kThr) k_train_stat(const __grid_constant
 // loss gradient with the batch's V and C, and the backward layers.
 template <int WR, int HR>
 __global__ void __launch_bounds__(simt::kThr) k_train_rrs(const __grid_constant__ TrainArgs a) {
+    constexpr bool REF = WR == 32;             // the reference's shipped network
+    constexpr int X1 = REF ? kRefRrsLanes : 10;
     using S = TrShape<WR>;
     extern __shared__ float4 smem4[];
     float* tile = reinterpret_cast<float*>(smem4);
@@ -356,7 +398,7 @@ __global__ void __launch_bounds__(simt::kThr) k_train_rrs(const __grid_constant_
     __syncthreads();
     const double Vm = s_tot[1] / (double)a.n, Cm = s_tot[2] / (double)a.n;
     if (blockIdx.x == 0 && tid == 0) {
-        a.loss_out[0] = s_tot[0] / (3.0 * (double)a.n);
+        a.loss_out[0] = s_tot[0] / ((REF ? 6.0 : 3.0) * (double)a.n);
         a.loss_out[1] = a.train_rrs ? (a.lw.active ? Vm * Cm + s_tot[3] / (double)a.n : Vm * Cm)
                                     : 0.0;
     }
@@ -374,10 +416,10 @@ __global__ void __launch_bounds__(simt::kThr) k_train_rrs(const __grid_constant_
         __syncthreads();
         if (lead) {
 #pragma unroll
-            for (int k = 0; k < 10; ++k)
+            for (int k = 0; k < X1; ++k)
                 tile[k * kLd + m] = valid ? scr[(size_t)(a.r_x1 + k) * ld + i] : 0.f;
         }
-        fwd_layer<WR>(tr, kRrsIn, 10, tile, wch, tid, scr, ld, i0, a.r_hr, true);
+        fwd_layer<WR>(tr, kRrsIn, X1, tile, wch, tid, scr, ld, i0, a.r_hr, true);
 #pragma unroll 1
         for (int h = 1; h < HR; ++h)
             fwd_layer<WR>(tr + (size_t)kRrsIn * WR + (size_t)(h - 1) * WR * WR, WR, WR, tile, wch,
@@ -404,7 +446,8 @@ __global__ void __launch_bounds__(simt::kThr) k_train_rrs(const __grid_constant_
             float* dl = scr + (size_t)(a.r_dhr + (HR - 1) * WR) * ld + i;
 #pragma unroll 4
             for (int k = 0; k < WR; ++k) {
-                const float dk = tile[k * kLd + m] > 0.f ? rr_out[k] * draw : 0.f;
+                const float dk = tile[k * kLd + m] > 0.f ? rr_out[k] * draw
+                                                         : (REF ? 0.01f * (rr_out[k] * draw) : 0.f);
                 tile[k * kLd + m] = dk;
                 if (valid) dl[(size_t)k * ld] = dk;
             }
@@ -605,6 +648,28 @@ __global__ void k_adam(const __grid_constant__ AdamArgs a) {
     }
 }
 
+struct EmaArgs {
+    const float* p;
+    float* e;
+    float* pi;             // the debiased average
+    __half* table_h;       // FP16 copy of pi over [0, n_table) (may be null)
+    uint64_t n_table, count;
+    float d, omd, inv;     // decay, 1 - decay, 1 / (1 - decay^t)
+};
+
+// the moving average after an Adam step: e = d e + (1 - d) w, pi = e / (1 - d^t), each product
+// and the sum rounded separately (no contraction), so a float32 restatement gives the same bits
+__global__ void k_ema(const __grid_constant__ EmaArgs a) {
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < a.count;
+         k += (uint64_t)gridDim.x * blockDim.x) {
+        const float e = __fadd_rn(__fmul_rn(a.d, a.e[k]), __fmul_rn(a.omd, a.p[k]));
+        const float pi = __fmul_rn(e, a.inv);
+        a.e[k] = e;
+        a.pi[k] = pi;
+        if (a.table_h && k < a.n_table) a.table_h[k] = __float2half_rn(pi);
+    }
+}
+
 template <int WS, int HS, int WR, int HR>
 cudaError_t launch_train(nrrs_ctx* ctx, TrainArgs& a, cudaStream_t s) {
     const size_t smem = TrShape<WS>::kSmem;
@@ -637,10 +702,11 @@ struct Layout {
 Layout layout_of(const nrrs_config& c) {
     Layout L{};
     uint32_t r = 0;
-    L.r_x0 = r; r += 56;
+    const bool ref = c.network == NRRS_NET_REFERENCE;
+    L.r_x0 = r; r += ref ? kRefStatIn : 56;
     L.r_hs = r; r += c.statnet_hidden * c.statnet_width;
     L.r_dhs = r; r += c.statnet_hidden * c.statnet_width;
-    L.r_dy = r; r += 4;
+    L.r_dy = r; r += ref ? 8 : 4;
     L.r_x1 = r; r += 16;
     L.r_hr = r; r += c.rrsnet_hidden * c.rrsnet_width;
     L.r_dhr = r; r += c.rrsnet_hidden * c.rrsnet_width;
@@ -680,9 +746,37 @@ cudaError_t launch_adam_step(nrrs_ctx* ctx, bool train_rrs, cudaStream_t s, floa
     ad.l2 = c.l2_reg;
     ad.inv_c1 = 1.0f / (1.0f - powf(c.beta1, (float)ctx->adam_t));
     ad.inv_c2 = 1.0f / (1.0f - powf(c.beta2, (float)ctx->adam_t));
-    ProfScope ps(ctx, NRRS_KERNEL_ADAM, s);
-    k_adam<<<(unsigned)ctx->sm_count * 8, 256, 0, s>>>(ad);
-    return cudaGetLastError();
+    {
+        ProfScope ps(ctx, NRRS_KERNEL_ADAM, s);
+        k_adam<<<(unsigned)ctx->sm_count * 8, 256, 0, s>>>(ad);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && ctx->cells) {
+        ProfScope ps(ctx, NRRS_KERNEL_CELL_IMAGE, s);
+        e = launch_cell_image(ctx->table_h, ctx->enc, ctx->cells, ctx->n_cells, ctx->sm_count, s);
+    }
+    if (e != cudaSuccess || !ctx->ema) return e;
+    // the moving average of every parameter and the inference table derived from it
+    ctx->ema_t += 1;
+    EmaArgs ea{};
+    ea.p = ctx->params;
+    ea.e = ctx->ema;
+    ea.pi = ctx->params_inf;
+    ea.table_h = ctx->table_h_inf;
+    ea.n_table = ctx->n_table;
+    ea.count = ctx->n_params;
+    ea.d = c.ema_decay;
+    ea.omd = 1.0f - c.ema_decay;
+    ea.inv = (float)(1.0 / (1.0 - std::pow((double)c.ema_decay, (double)ctx->ema_t)));
+    {
+        ProfScope ps(ctx, NRRS_KERNEL_ADAM, s);
+        k_ema<<<(unsigned)ctx->sm_count * 8, 256, 0, s>>>(ea);
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess || !ctx->cells_inf) return e;
+    ProfScope ps(ctx, NRRS_KERNEL_CELL_IMAGE, s);
+    return launch_cell_image(ctx->table_h_inf, ctx->enc, ctx->cells_inf, ctx->n_cells,
+                             ctx->sm_count, s);
 }
 
 bool train_tc_supported(const nrrs_config& c);
@@ -756,6 +850,8 @@ int train_step_impl(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uin
         e = launch_train<64, 2, 64, 2>(ctx, a, s);
     else if (c.statnet_width == 64 && c.statnet_hidden == 3)
         e = launch_train<64, 3, 64, 3>(ctx, a, s);
+    else if (c.statnet_width == 32)   // the reference network
+        e = launch_train<32, 3, 32, 3>(ctx, a, s);
     else
         e = launch_train<128, 3, 128, 3>(ctx, a, s);
     if (e != cudaSuccess) {
@@ -775,16 +871,18 @@ int train_step_impl(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uin
     uint32_t off = 0;
     const uint32_t WS = c.statnet_width, HS = c.statnet_hidden;
     const uint32_t WR = c.rrsnet_width, HR = c.rrsnet_hidden;
-    w.job[nj++] = WJob{L.r_dhs, L.r_x0, WS, 56, kStatIn, off};
-    off += WS * kStatIn;
+    const bool ref = c.network == NRRS_NET_REFERENCE;
+    const uint32_t sin = stat_in_of((int)WS), sout = stat_out_of((int)WS);
+    w.job[nj++] = WJob{L.r_dhs, L.r_x0, WS, ref ? (uint32_t)kRefStatIn : 56u, sin, off};
+    off += WS * sin;
     for (uint32_t h = 1; h < HS; ++h) {
         w.job[nj++] = WJob{L.r_dhs + h * WS, L.r_hs + (h - 1) * WS, WS, WS, WS, off};
         off += WS * WS;
     }
-    w.job[nj++] = WJob{L.r_dy, L.r_hs + (HS - 1) * WS, 3, WS, WS, off};
-    off += 3 * WS;
+    w.job[nj++] = WJob{L.r_dy, L.r_hs + (HS - 1) * WS, sout, WS, WS, off};
+    off += sout * WS;
     if (train_rrs) {
-        w.job[nj++] = WJob{L.r_dhr, L.r_x1, WR, 10, kRrsIn, off};
+        w.job[nj++] = WJob{L.r_dhr, L.r_x1, WR, ref ? (uint32_t)kRefRrsLanes : 10u, kRrsIn, off};
         off += WR * kRrsIn;
         for (uint32_t h = 1; h < HR; ++h) {
             w.job[nj++] = WJob{L.r_dhr + h * WR, L.r_hr + (h - 1) * WR, WR, WR, WR, off};

@@ -206,7 +206,8 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
                 for (int j = 0; j < 4; ++j) {
                     const LevelDev L = a.enc.lv[lq * 4 + j];
                     const CellCoord c = cell_of(p, L.res);
-                    const float2 fv = level_features_h<(W < 128)>(table, L, a.enc.hash_mask, c);
+                    const float2 fv =
+                        level_features_h<(W < 128)>(table, a.enc.cells, L, a.enc.hash_mask, c);
                     f[2 * j] = fv.x;
                     f[2 * j + 1] = fv.y;
                 }

@@ -47,10 +47,10 @@ __global__ void k_pack(PackArgs a) {
     const int nets = 2;
     size_t mofs = 0, tofs = 0, pofs = 0;
     for (int net = 0; net < nets; ++net) {
-        const int in = net == 0 ? kStatIn : kRrsIn;
+        const int in = net == 0 ? stat_in_of(a.ws) : kRrsIn;
         const int w = net == 0 ? a.ws : a.wr;
         const int h = net == 0 ? a.hs : a.hr;
-        const int out = net == 0 ? kStatOut : 1;
+        const int out = net == 0 ? stat_out_of(a.ws) : 1;
         for (int l = 0; l <= h; ++l) {
             const LayerDesc d = layer_of(in, w, h, out, l);
             const int op4 = pad4(d.out);
@@ -99,10 +99,10 @@ __device__ __forceinline__ uint16_t to_bits(float v, bool bf) {
 __global__ void k_pack_train(PackTrainArgs a) {
     size_t mofs = 0, pofs = 0;
     for (int net = 0; net < 2; ++net) {
-        const int in = net == 0 ? kStatIn : kRrsIn;
+        const int in = net == 0 ? stat_in_of(a.ws) : kRrsIn;
         const int w = net == 0 ? a.ws : a.wr;
         const int h = net == 0 ? a.hs : a.hr;
-        const int out = net == 0 ? kStatOut : 1;
+        const int out = net == 0 ? stat_out_of(a.ws) : 1;
         // forward images
         for (int l = 0; l <= h; ++l) {
             const LayerDesc d = layer_of(in, w, h, out, l);
@@ -126,7 +126,40 @@ __global__ void k_table_half(const float* t, __half* h, size_t n) {
         h[i] = __float2half_rn(t[i]);
 }
 
+// The cell image of the FP16 table's dense levels: cell (x, y, z) of level L gets its 8 corner
+// entries (raw FP16 pairs) in corner order k = x-bit + 2 y-bit + 4 z-bit, the order in which
+// the gathers sum them, so features from the image equal features from the table bit for bit.
+// Threads walk cells in x-fastest order: the corner reads of a warp are mostly contiguous rows.
+__global__ void k_cell_image(const uint32_t* __restrict__ rows,
+                             const __grid_constant__ EncodeParams e, uint4* __restrict__ cells,
+                             uint32_t n_cells) {
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < n_cells;
+         g += gridDim.x * blockDim.x) {
+        // the dense levels are a prefix of the levels (N_l grows with l)
+        int l = 0;
+        while (l + 1 < (int)e.n_levels && e.lv[l + 1].dense && e.lv[l + 1].cell <= g) ++l;
+        const LevelDev L = e.lv[l];
+        const uint32_t N = L.res, r = g - L.cell;
+        const uint32_t x = r % N, y = (r / N) % N, z = r / (N * N);
+        uint32_t t[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            t[k] = rows[grid_row(L, e.hash_mask, x + (k & 1), y + ((k >> 1) & 1),
+                                 z + ((k >> 2) & 1))];
+        cells[2 * (size_t)g] = make_uint4(t[0], t[1], t[2], t[3]);
+        cells[2 * (size_t)g + 1] = make_uint4(t[4], t[5], t[6], t[7]);
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_cell_image(const __half* table_h, const EncodeParams& e, uint4* cells,
+                              uint32_t n_cells, int sm_count, cudaStream_t s) {
+    if (!cells || n_cells == 0) return cudaSuccess;
+    k_cell_image<<<sm_count * 8, 256, 0, s>>>(reinterpret_cast<const uint32_t*>(table_h), e,
+                                              cells, n_cells);
+    return cudaGetLastError();
+}
 
 thread_local int g_last_grid = 0;
 
@@ -152,7 +185,7 @@ int resident_ctas(const void* kern, int threads, size_t dyn_smem, int cap) {
 size_t transposed_weight_floats(int ws, int hs, int wr, int hr) {
     size_t t = 0;
     for (int l = 0; l <= hs; ++l) {
-        LayerDesc d = layer_of(kStatIn, ws, hs, kStatOut, l);
+        LayerDesc d = layer_of(stat_in_of(ws), ws, hs, stat_out_of(ws), l);
         t += (size_t)d.in * pad4(d.out);
     }
     for (int l = 0; l <= hr; ++l) {
@@ -165,7 +198,7 @@ size_t transposed_weight_floats(int ws, int hs, int wr, int hr) {
 size_t packed_weight_bytes(int ws, int hs, int wr, int hr) {
     size_t t = 0;
     for (int l = 0; l <= hs; ++l) {
-        LayerDesc d = layer_of(kStatIn, ws, hs, kStatOut, l);
+        LayerDesc d = layer_of(stat_in_of(ws), ws, hs, stat_out_of(ws), l);
         t += (size_t)(l == hs ? npad16(d.out) : d.out) * d.in;
     }
     for (int l = 0; l <= hr; ++l) {
@@ -185,10 +218,10 @@ cudaError_t launch_pack_weights(const float* master_mlp, float* wt, float* wrow,
 size_t train_pack_bytes(int ws, int hs, int wr, int hr) {
     size_t t = 0;
     for (int net = 0; net < 2; ++net) {
-        const int in = net == 0 ? kStatIn : kRrsIn;
+        const int in = net == 0 ? stat_in_of(ws) : kRrsIn;
         const int w = net == 0 ? ws : wr;
         const int h = net == 0 ? hs : hr;
-        const int out = net == 0 ? kStatOut : 1;
+        const int out = net == 0 ? stat_out_of(ws) : 1;
         for (int l = 0; l <= h; ++l) {
             const LayerDesc d = layer_of(in, w, h, out, l);
             t += (size_t)(l == h ? npad16(d.out) : d.out) * d.in;

@@ -104,11 +104,14 @@ cudaError_t launch_sum(const SumArgs& a, cudaStream_t s);
 cudaError_t launch_infer_fp32(const InferArgs& a, int ws, int hs, int wr, int hr, int sm_count,
                               int ctas_per_sm, cudaStream_t s);
 // largest resident CTAs per SM of the inference kernel for a shape (0 = unsupported)
-// split: 0 fused, 1 encoding + MLP kernel, 2 encoding + StatNet kernel + RRSNet kernel
+// split: 0 fused, 1 encoding + MLP kernel, 2 encoding + StatNet kernel + RRSNet kernel,
+// 3 as 2 with the hidden activations in TMEM
 int infer_max_ctas(int ws, int hs, int wr, int hr, int prec, int wgs, int split = 0);
-// tcgen05 mixed-precision inference; part: 0 both networks, 1 StatNet only, 2 RRSNet only
+// tcgen05 mixed-precision inference; part: 0 both networks, 1 StatNet only, 2 RRSNet only;
+// tmem_act: parts 1 and 2 with the hidden activations in TMEM
 cudaError_t launch_infer_tc(const InferArgs& a, int ws, int hs, int wr, int hr, int prec,
-                            int sm_count, int ctas_per_sm, int wgs, int part, cudaStream_t s);
+                            int sm_count, int ctas_per_sm, int wgs, int part, bool tmem_act,
+                            cudaStream_t s);
 size_t infer_tc_smem_bytes(int ws, int hs, int wr, int hr);
 // derived weight copies: FP32 transposed and the UMMA-packed FP16/BF16 images
 cudaError_t launch_pack_weights(const float* master_mlp, float* wt, float* wrow, void* wpack,
@@ -121,5 +124,8 @@ cudaError_t launch_pack_train(const float* master_mlp, void* out, int ws, int hs
 size_t train_pack_bytes(int ws, int hs, int wr, int hr);
 // FP32 table -> FP16 copy
 cudaError_t launch_table_to_half(const float* t, __half* h, size_t n, cudaStream_t s);
+// the cell image of the dense levels (EncodeParams::cells) from the FP16 table
+cudaError_t launch_cell_image(const __half* table_h, const EncodeParams& e, uint4* cells,
+                              uint32_t n_cells, int sm_count, cudaStream_t s);
 
 }  // namespace nrrs

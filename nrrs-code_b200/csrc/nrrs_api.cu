@@ -41,7 +41,7 @@ uint64_t splitmix64(uint64_t x) {
 // Level table of the Instant-NGP grid: N_l = floor(N_min * b^l), dense when (N_l+1)^3 <= T.
 uint64_t build_levels(const nrrs_config& c, EncodeParams& e) {
     const uint64_t T = 1ull << c.log2_hashmap_size;
-    uint64_t off = 0;
+    uint64_t off = 0, cells = 0;
     for (int l = 0; l < c.n_levels; ++l) {
         const uint32_t N =
             (uint32_t)std::floor((double)c.base_resolution * std::pow((double)c.per_level_scale, (double)l));
@@ -50,9 +50,11 @@ uint64_t build_levels(const nrrs_config& c, EncodeParams& e) {
         e.lv[l].res = N;
         e.lv[l].dense = dense_n <= T;
         e.lv[l].offset = (uint32_t)off;
-        e.lv[l].pad = 0;
+        e.lv[l].cell = e.lv[l].dense ? (uint32_t)cells : 0u;
+        if (e.lv[l].dense) cells += (uint64_t)N * N * N;
         off += e.lv[l].dense ? dense_n : T;
     }
+    e.cells = nullptr;
     e.n_levels = (uint32_t)c.n_levels;
     e.hash_mask = (uint32_t)(T - 1);
     return off;
@@ -138,16 +140,41 @@ SegmentTable make_segments(const nrrs_segment* segs, int n, uint32_t unit) {
     return t;
 }
 
+// Restart the moving average at an upload of the parameters: e = 0, t = 0, and the inference
+// weights are the uploaded ones.
+int ema_restart(nrrs_ctx* ctx, cudaStream_t s) {
+    if (!ctx->ema) return NRRS_OK;
+    ctx->ema_t = 0;
+    const size_t b = sizeof(float) * ctx->n_params;
+    cudaError_t e = cudaMemsetAsync(ctx->ema, 0, b, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(ctx->params_inf, ctx->params, b, cudaMemcpyDeviceToDevice, s);
+    return e == cudaSuccess ? NRRS_OK : cuda_fail(ctx, e, "moving average restart");
+}
+
+// The images derived from the weights: from params the training images (transposed and row-major
+// FP32 MLP weights, the tensor-core training image, the FP16 table and its cell image); from the
+// inference weights (params_inf with a moving average, else params) the inference images (the
+// UMMA weight image, and with a moving average its own transposed weights, FP16 table and cell
+// image). table = false skips the tables (the Adam and moving-average passes wrote them).
 int refresh_derived(nrrs_ctx* ctx, cudaStream_t s, bool table = true) {
     const nrrs_config& c = ctx->cfg;
+    const bool ema = ctx->ema != nullptr;
     cudaError_t e;
     {
         ProfScope ps(ctx, NRRS_KERNEL_PACK, s);
-        e = launch_pack_weights(ctx->params + ctx->n_table, ctx->wt, ctx->wrow, ctx->wpack,
-                                c.statnet_width, c.statnet_hidden, c.rrsnet_width,
-                                c.rrsnet_hidden, c.precision, s);
+        e = launch_pack_weights(ctx->params + ctx->n_table, ctx->wt, ctx->wrow,
+                                ema ? nullptr : ctx->wpack, c.statnet_width, c.statnet_hidden,
+                                c.rrsnet_width, c.rrsnet_hidden, c.precision, s);
     }
     if (e != cudaSuccess) return cuda_fail(ctx, e, "pack weights");
+    if (ema) {
+        ProfScope ps(ctx, NRRS_KERNEL_PACK, s);
+        e = launch_pack_weights(ctx->params_inf + ctx->n_table, ctx->wt_inf, nullptr, ctx->wpack,
+                                c.statnet_width, c.statnet_hidden, c.rrsnet_width,
+                                c.rrsnet_hidden, c.precision, s);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "pack inference weights");
+    }
     if (ctx->tpack) {
         ProfScope ps(ctx, NRRS_KERNEL_PACK, s);
         e = launch_pack_train(ctx->params + ctx->n_table, ctx->tpack, c.statnet_width,
@@ -158,6 +185,22 @@ int refresh_derived(nrrs_ctx* ctx, cudaStream_t s, bool table = true) {
         ProfScope ps(ctx, NRRS_KERNEL_TABLE_HALF, s);
         e = launch_table_to_half(ctx->params, ctx->table_h, ctx->n_table, s);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "table to half");
+    }
+    if (ctx->cells && table) {
+        ProfScope ps(ctx, NRRS_KERNEL_CELL_IMAGE, s);
+        e = launch_cell_image(ctx->table_h, ctx->enc, ctx->cells, ctx->n_cells, ctx->sm_count, s);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "cell image");
+    }
+    if (ema && ctx->table_h_inf && table) {
+        ProfScope ps(ctx, NRRS_KERNEL_TABLE_HALF, s);
+        e = launch_table_to_half(ctx->params_inf, ctx->table_h_inf, ctx->n_table, s);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "inference table to half");
+    }
+    if (ema && ctx->cells_inf && table) {
+        ProfScope ps(ctx, NRRS_KERNEL_CELL_IMAGE, s);
+        e = launch_cell_image(ctx->table_h_inf, ctx->enc, ctx->cells_inf, ctx->n_cells,
+                              ctx->sm_count, s);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "inference cell image");
     }
     return NRRS_OK;
 }
@@ -172,10 +215,13 @@ int run_infer(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const SegmentTable& segs,
     a.fp = factor_params(ctx, p);
     a.segs = segs;
     a.segs.resolved = resolved;
-    a.table = ctx->params;
-    a.table_h = ctx->table_h;
-    a.wt_stat = ctx->wt;
-    a.wt_rrs = ctx->wt + ctx->wt_rrs_offset;
+    // the inference weights: the debiased moving average when there is one
+    const bool ema = ctx->ema != nullptr;
+    if (ema) a.enc.cells = ctx->enc.cells ? ctx->cells_inf : nullptr;
+    a.table = ema ? ctx->params_inf : ctx->params;
+    a.table_h = ema ? ctx->table_h_inf : ctx->table_h;
+    a.wt_stat = ema ? ctx->wt_inf : ctx->wt;
+    a.wt_rrs = a.wt_stat + ctx->wt_rrs_offset;
     a.wpack = ctx->wpack;
     a.stats = stats;
     a.rrs = rrs;
@@ -193,11 +239,11 @@ int run_infer(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const SegmentTable& segs,
         if (!ctx->enc_tiles || segs.total_tiles > ctx->enc_tiles_cap)
             return fail(ctx, NRRS_ERR_INVALID_ARG, "split inference: feature tiles too small");
         EncodeLvArgs ea{};
-        ea.enc = ctx->enc;
+        ea.enc = a.enc;
         ea.segs = segs;
         ea.segs.resolved = resolved;
         ea.pos = a.v.pos;
-        ea.table_h = ctx->table_h;
+        ea.table_h = a.table_h;
         ea.out = ctx->enc_tiles;
         ea.tile_bytes = kEncTileBytes;
         ea.kdim = 32;
@@ -208,21 +254,23 @@ int run_infer(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const SegmentTable& segs,
         if (e != cudaSuccess) return cuda_fail(ctx, e, "encoding launch");
         a.enc_tiles = ctx->enc_tiles;
     }
-    if (split == 2) {
+    if (split >= 2) {
         // StatNet kernel (writes the RRSNet input tiles; computes ADRRS factors itself), then
         // the RRSNet kernel when the factor comes from RRSNet. Each holds only its own weights,
-        // so more 128-vertex tiles are in flight per SM.
+        // so more 128-vertex tiles are in flight per SM. Mode 3 keeps the hidden activations in
+        // TMEM as the next layer's A operand.
         if (!ctx->x1_tiles) return fail(ctx, NRRS_ERR_INVALID_ARG, "split inference: no RRSNet input tiles");
         a.x1_tiles = ctx->x1_tiles;
+        const bool ta = split == 3;
         {
             ProfScope ps(ctx, NRRS_KERNEL_INFER_TC, s);
             e = launch_infer_tc(a, c.statnet_width, c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden,
-                                c.precision, ctx->sm_count, ctx->tc_ctas_per_sm, ctx->tc_wgs, 1, s);
+                                c.precision, ctx->sm_count, ctx->tc_ctas_per_sm, ctx->tc_wgs, 1, ta, s);
         }
         if (e == cudaSuccess && a.fp.source == NRRS_FACTOR_RRSNET) {
             ProfScope ps(ctx, NRRS_KERNEL_INFER_RRS, s);
             e = launch_infer_tc(a, c.statnet_width, c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden,
-                                c.precision, ctx->sm_count, ctx->tc_ctas_per_sm, ctx->tc_wgs, 2, s);
+                                c.precision, ctx->sm_count, ctx->tc_ctas_per_sm, ctx->tc_wgs, 2, ta, s);
         }
         if (e != cudaSuccess) return cuda_fail(ctx, e, "inference launch");
         ctx->last_infer_grid = g_last_grid;
@@ -235,7 +283,7 @@ int run_infer(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const SegmentTable& segs,
                                   c.rrsnet_hidden, ctx->sm_count, ctx->simt_ctas_per_sm, s);
         else
             e = launch_infer_tc(a, c.statnet_width, c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden,
-                                c.precision, ctx->sm_count, ctx->tc_ctas_per_sm, ctx->tc_wgs, 0, s);
+                                c.precision, ctx->sm_count, ctx->tc_ctas_per_sm, ctx->tc_wgs, 0, false, s);
     }
     if (e != cudaSuccess) return cuda_fail(ctx, e, "inference launch");
     ctx->last_infer_grid = g_last_grid;
@@ -381,6 +429,7 @@ void nrrs_config_reference_network(nrrs_config* c) {
     c->beta2 = 0.99f;
     c->eps = 1e-15f;
     c->l2_reg = 3e-6f;
+    c->ema_decay = 0.95f;   // "otype": "Ema", "decay": 0.95
 }
 
 void nrrs_decide_params_default(nrrs_decide_params* p) {
@@ -429,9 +478,21 @@ int nrrs_create(const nrrs_config* cfg, nrrs_ctx** out) {
     if (!cfg || !out) return fail(nullptr, NRRS_ERR_INVALID_ARG, "NULL argument");
     *out = nullptr;
     const nrrs_config& c = *cfg;
-    if (c.n_levels != 16 || c.n_features_per_level != 2)
-        return fail(nullptr, NRRS_ERR_UNSUPPORTED, "hash grid needs 16 levels x 2 features (32 lanes)");
-    if (c.sh_degree != 4) return fail(nullptr, NRRS_ERR_UNSUPPORTED, "sh_degree must be 4");
+    const bool ref_net = c.network == NRRS_NET_REFERENCE;
+    if (c.network != NRRS_NET_WORKLOAD && !ref_net)
+        return fail(nullptr, NRRS_ERR_INVALID_ARG, "network must be NRRS_NET_WORKLOAD or NRRS_NET_REFERENCE");
+    if (ref_net) {
+        // the reference's shipped network: its StatNet input is 16 hash lanes + 16 one-blob lanes
+        if (c.n_levels != kRefLevels || c.n_features_per_level != 2)
+            return fail(nullptr, NRRS_ERR_UNSUPPORTED, "reference network: 8 levels x 2 features");
+        if (c.statnet_width != 32 || c.rrsnet_width != 32 || c.statnet_hidden != 3 ||
+            c.rrsnet_hidden != 3)
+            return fail(nullptr, NRRS_ERR_UNSUPPORTED, "reference network: 32 wide x 3 hidden");
+    } else {
+        if (c.n_levels != 16 || c.n_features_per_level != 2)
+            return fail(nullptr, NRRS_ERR_UNSUPPORTED, "hash grid needs 16 levels x 2 features (32 lanes)");
+        if (c.sh_degree != 4) return fail(nullptr, NRRS_ERR_UNSUPPORTED, "sh_degree must be 4");
+    }
     if (c.log2_hashmap_size < 10 || c.log2_hashmap_size > 24 || c.base_resolution < 2 ||
         !(c.per_level_scale >= 1.0f))
         return fail(nullptr, NRRS_ERR_INVALID_ARG, "bad hash-grid parameters");
@@ -439,12 +500,14 @@ int nrrs_create(const nrrs_config* cfg, nrrs_ctx** out) {
                      (c.statnet_hidden == 2 || c.statnet_hidden == 3);
     const bool w128 = c.statnet_width == 128 && c.rrsnet_width == 128 && c.statnet_hidden == 3 &&
                       c.rrsnet_hidden == 3;
-    if (!w64 && !w128)
+    if (!w64 && !w128 && !ref_net)
         return fail(nullptr, NRRS_ERR_UNSUPPORTED, "networks: 64 wide x 2|3 hidden or 128 wide x 3 hidden");
     if (c.precision < NRRS_PREC_FP32 || c.precision > NRRS_PREC_BF16)
         return fail(nullptr, NRRS_ERR_INVALID_ARG, "bad precision");
     if (c.max_queue == 0 || c.max_train == 0)
         return fail(nullptr, NRRS_ERR_INVALID_ARG, "max_queue and max_train must be > 0");
+    if (!(c.ema_decay >= 0.f && c.ema_decay < 1.f))
+        return fail(nullptr, NRRS_ERR_INVALID_ARG, "ema_decay must be in [0, 1)");
     if (!nrrs_device_available())
         return fail(nullptr, NRRS_ERR_NO_DEVICE, "no sm_100 CUDA device (this library has no CPU path)");
 
@@ -455,15 +518,16 @@ int nrrs_create(const nrrs_config* cfg, nrrs_ctx** out) {
     ctx->table_rows = build_levels(c, ctx->enc);
     aabb_terms(c, ctx->enc);
     ctx->n_table = ctx->table_rows * 2;
-    ctx->n_stat = mlp_params(kStatIn, c.statnet_width, c.statnet_hidden, kStatOut);
+    ctx->n_stat = mlp_params(stat_in_of(c.statnet_width), c.statnet_width, c.statnet_hidden,
+                             stat_out_of(c.statnet_width));
     ctx->n_rrs = mlp_params(kRrsIn, c.rrsnet_width, c.rrsnet_hidden, 1);
     ctx->n_params = ctx->n_table + ctx->n_stat + ctx->n_rrs;
     ctx->wt_floats = transposed_weight_floats(c.statnet_width, c.statnet_hidden, c.rrsnet_width,
                                               c.rrsnet_hidden);
     ctx->wt_rrs_offset = 0;
     for (int l = 0; l <= c.statnet_hidden; ++l) {
-        const int li = l == 0 ? kStatIn : c.statnet_width;
-        const int lo = l == c.statnet_hidden ? kStatOut : c.statnet_width;
+        const int li = l == 0 ? stat_in_of(c.statnet_width) : c.statnet_width;
+        const int lo = l == c.statnet_hidden ? stat_out_of(c.statnet_width) : c.statnet_width;
         ctx->wt_rrs_offset += (size_t)li * ((lo + 3) / 4 * 4);
     }
     ctx->wpack_bytes = packed_weight_bytes(c.statnet_width, c.statnet_hidden, c.rrsnet_width,
@@ -490,6 +554,24 @@ int nrrs_create(const nrrs_config* cfg, nrrs_ctx** out) {
         // 4 spare rows: the paired gathers read whole 16-byte blocks of 4 rows
         NRRS_ALLOC(ctx->table_h, sizeof(__half) * (ctx->n_table + 8));
         NRRS_ALLOC(ctx->wpack, ctx->wpack_bytes);
+        // the cell image of the dense levels: 32 bytes per cell
+        uint64_t nc = 0;
+        for (int l = 0; l < c.n_levels; ++l)
+            if (ctx->enc.lv[l].dense)
+                nc = (uint64_t)ctx->enc.lv[l].cell +
+                     (uint64_t)ctx->enc.lv[l].res * ctx->enc.lv[l].res * ctx->enc.lv[l].res;
+        if (nc > 0 && nc < (1ull << 31)) {
+            NRRS_ALLOC(ctx->cells, 32 * (size_t)nc);
+            ctx->n_cells = (uint32_t)nc;
+            ctx->enc.cells = ctx->cells;
+        }
+    }
+    if (c.ema_decay > 0.f) {
+        NRRS_ALLOC(ctx->ema, pb);
+        NRRS_ALLOC(ctx->params_inf, pb);
+        NRRS_ALLOC(ctx->wt_inf, sizeof(float) * ctx->wt_floats);
+        if (ctx->table_h) NRRS_ALLOC(ctx->table_h_inf, sizeof(__half) * (ctx->n_table + 8));
+        if (ctx->cells) NRRS_ALLOC(ctx->cells_inf, 32 * (size_t)ctx->n_cells);
     }
     if (train_tc_supported(c))
         NRRS_ALLOC(ctx->tpack, train_pack_bytes(c.statnet_width, c.statnet_hidden,
@@ -513,7 +595,8 @@ int nrrs_create(const nrrs_config* cfg, nrrs_ctx** out) {
             h[k] = (float)((2.0 * u - 1.0) * c.table_init_scale);
         }
     }
-    xavier_fill(h, ctx->n_table, kStatIn, c.statnet_width, c.statnet_hidden, kStatOut, c.seed, 100);
+    xavier_fill(h, ctx->n_table, stat_in_of(c.statnet_width), c.statnet_width, c.statnet_hidden,
+                stat_out_of(c.statnet_width), c.seed, 100);
     xavier_fill(h, ctx->n_table + ctx->n_stat, kRrsIn, c.rrsnet_width, c.rrsnet_hidden, 1, c.seed, 200);
     e = cudaMemcpy(ctx->params, h.data(), pb, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(ctx->grads, 0, pb);
@@ -529,7 +612,8 @@ int nrrs_create(const nrrs_config* cfg, nrrs_ctx** out) {
         nrrs_destroy(ctx);
         return fail(nullptr, NRRS_ERR_CUDA, std::string("init: ") + cudaGetErrorString(e));
     }
-    int rc = refresh_derived(ctx, 0);
+    int rc = ema_restart(ctx, 0);
+    if (rc == NRRS_OK) rc = refresh_derived(ctx, 0);
     if (rc == NRRS_OK) {
         e = cudaDeviceSynchronize();
         if (e != cudaSuccess) rc = cuda_fail(ctx, e, "init sync");
@@ -551,6 +635,12 @@ void nrrs_destroy(nrrs_ctx* ctx) {
     cudaFree(ctx->adam_m);
     cudaFree(ctx->adam_v);
     cudaFree(ctx->table_h);
+    cudaFree(ctx->cells);
+    cudaFree(ctx->ema);
+    cudaFree(ctx->params_inf);
+    cudaFree(ctx->wt_inf);
+    cudaFree(ctx->table_h_inf);
+    cudaFree(ctx->cells_inf);
     cudaFree(ctx->wt);
     cudaFree(ctx->wrow);
     cudaFree(ctx->wpack);
@@ -852,7 +942,10 @@ int nrrs_train_step_batch(nrrs_ctx* ctx, const nrrs_train_batch* b, uint32_t n,
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = launch_loss_sums(lw, n, error_sum_dev, lp->n_pixels, ctx->loss_sums, s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "loss weight sums");
-    return train_step_impl(ctx, v, b->target, n, loss_dev, s, true, &lw);
+    const int rc = train_step_impl(ctx, v, b->target, n, loss_dev, s, true, &lw);
+    if (rc) return rc;
+    // the Adam pass refreshed the FP16 table and its cell image; the MLP images follow
+    return refresh_derived(ctx, s, false);
 }
 
 int nrrs_train_step(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* target, uint32_t n,
@@ -884,11 +977,20 @@ int nrrs_get_params(const nrrs_ctx* ctx, float* dst, uint64_t count) {
     return e == cudaSuccess ? NRRS_OK : NRRS_ERR_CUDA;
 }
 
+int nrrs_get_inference_params(const nrrs_ctx* ctx, float* dst, uint64_t count) {
+    if (!ctx || !dst || count != ctx->n_params) return NRRS_ERR_INVALID_ARG;
+    const float* src = ctx->ema ? ctx->params_inf : ctx->params;
+    cudaError_t e = cudaMemcpy(dst, src, sizeof(float) * count, cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? NRRS_OK : NRRS_ERR_CUDA;
+}
+
 int nrrs_set_params(nrrs_ctx* ctx, const float* src, uint64_t count) {
     if (!ctx || !src || count != ctx->n_params) return ctx ? fail(ctx, NRRS_ERR_INVALID_ARG, "count mismatch") : NRRS_ERR_INVALID_ARG;
     cudaError_t e = cudaMemcpy(ctx->params, src, sizeof(float) * count, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "set params");
-    int rc = refresh_derived(ctx, 0);
+    int rc = ema_restart(ctx, 0);
+    if (rc) return rc;
+    rc = refresh_derived(ctx, 0);
     if (rc) return rc;
     e = cudaDeviceSynchronize();
     return e == cudaSuccess ? NRRS_OK : cuda_fail(ctx, e, "set params sync");
@@ -993,7 +1095,7 @@ const char* nrrs_kernel_name(int32_t kind) {
     static const char* names[NRRS_KERNEL_KINDS] = {
         "infer_fp32", "infer_tc", "sum", "decide", "pack_weights", "table_half",
         "train_statnet", "train_rrsnet", "train_wgrad", "train_reduce", "adam", "encode",
-        "train_scatter", "train_encode", "infer_rrs"};
+        "train_scatter", "train_encode", "infer_rrs", "cell_image"};
     return (kind >= 0 && kind < NRRS_KERNEL_KINDS) ? names[kind] : "unknown";
 }
 
@@ -1053,7 +1155,7 @@ int nrrs_set_launch_shape(nrrs_ctx* ctx, int32_t ctas_per_sm, int32_t warpgroups
 }
 
 int nrrs_set_infer_split(nrrs_ctx* ctx, int32_t split) {
-    if (!ctx || split < 0 || split > 2) return NRRS_ERR_INVALID_ARG;
+    if (!ctx || split < 0 || split > 3) return NRRS_ERR_INVALID_ARG;
     const nrrs_config& c = ctx->cfg;
     if (split && c.precision == NRRS_PREC_FP32)
         return fail(ctx, NRRS_ERR_UNSUPPORTED, "split inference is a tensor-core path mode");
@@ -1062,7 +1164,7 @@ int nrrs_set_infer_split(nrrs_ctx* ctx, int32_t split) {
         infer_max_ctas(c.statnet_width, c.statnet_hidden, c.rrsnet_width, c.rrsnet_hidden,
                        c.precision, 2, split) <= 0)
         return fail(ctx, NRRS_ERR_UNSUPPORTED, "split inference not available for this network");
-    if (split == 2 && !ctx->x1_tiles) {
+    if (split >= 2 && !ctx->x1_tiles) {
         const uint32_t cap = c.max_queue / kTile + kMaxSegments + 1;
         if (cudaMalloc(&ctx->x1_tiles, (size_t)cap * kX1TileBytes) != cudaSuccess) {
             ctx->x1_tiles = nullptr;
@@ -1101,6 +1203,20 @@ int nrrs_get_train_split(const nrrs_ctx* ctx, int32_t* split) {
 int nrrs_get_infer_split(const nrrs_ctx* ctx, int32_t* split) {
     if (!ctx || !split) return NRRS_ERR_INVALID_ARG;
     *split = ctx->tc_split;
+    return NRRS_OK;
+}
+
+int nrrs_set_cell_image(nrrs_ctx* ctx, int32_t enable) {
+    if (!ctx) return NRRS_ERR_INVALID_ARG;
+    if (enable && !ctx->cells)
+        return fail(ctx, NRRS_ERR_UNSUPPORTED, "no cell image (FP32 context or no dense level)");
+    ctx->enc.cells = enable ? ctx->cells : nullptr;
+    return NRRS_OK;
+}
+
+int nrrs_get_cell_image(const nrrs_ctx* ctx, int32_t* enable) {
+    if (!ctx || !enable) return NRRS_ERR_INVALID_ARG;
+    *enable = ctx->enc.cells != nullptr;
     return NRRS_OK;
 }
 
@@ -1224,7 +1340,7 @@ int nrrs_autotune(nrrs_ctx* ctx, uint32_t n, const char* cache_path, char* repor
     int best_ctas = saved_ctas, best_wgs = saved_wgs, best_split = saved_split;
     rep << "{\"key\": \"" << key << "\", \"n\": " << n << ", \"trials\": [";
     bool first = true;
-    for (int sp = 0; sp <= (fp32 ? 0 : 2); ++sp)
+    for (int sp = 0; sp <= (fp32 ? 0 : 3); ++sp)
     for (int w = 1; w <= (fp32 ? 1 : 4); w *= 2) {
         const int maxc = infer_max_ctas(c.statnet_width, c.statnet_hidden, c.rrsnet_width,
                                         c.rrsnet_hidden, c.precision, w, sp);

@@ -30,7 +30,7 @@ struct LevelDev {
     uint32_t offset;  // first table row of the level
     uint32_t res;     // N_l cells per axis (N_l + 1 grid points)
     uint32_t dense;   // 1 = dense indexing
-    uint32_t pad;
+    uint32_t cell;    // dense levels: first cell of the level in the cell image
 };
 
 struct EncodeParams {
@@ -40,6 +40,11 @@ struct EncodeParams {
     int32_t normalize;
     float center[3];
     float diag[3];
+    // The cell image of the FP16 table's dense levels (NULL when absent): for every cell
+    // (x, y, z) of a dense level, its 8 corner entries in corner order, 32 bytes, at
+    // cells[2 * (L.cell + x + N (y + N z))]. One 32-byte load then fetches what four row
+    // gathers fetch from the table. It is rebuilt from the table after every table update.
+    const uint4* cells;
 };
 
 struct VertexPtrs {
@@ -291,8 +296,23 @@ __device__ __forceinline__ uint32_t quad_pick(const uint4& q, uint32_t e) {
 // x+1 differ in the low bits: 3 times in 4) and from a predicated 4-byte load otherwise. That is
 // about 5 L1 requests per level instead of 8 for the same values; the table carries 16 bytes of
 // padding for the last quad.
-__device__ __forceinline__ void level_corners_h(const __half2* table, const LevelDev& L,
-                                                uint32_t mask, const CellCoord& c, uint32_t* t) {
+// the 8 corner entries of cell c of dense level L from the cell image: one 32-byte load
+__device__ __forceinline__ void cell_corners(const uint4* cells, const LevelDev& L,
+                                             const CellCoord& c, uint32_t* t) {
+    const uint4* q = cells + 2 * ((size_t)L.cell + c.ix + L.res * (c.iy + (size_t)L.res * c.iz));
+    asm("ld.global.nc.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(t[0]), "=r"(t[1]), "=r"(t[2]), "=r"(t[3]), "=r"(t[4]), "=r"(t[5]), "=r"(t[6]),
+          "=r"(t[7])
+        : "l"(q));
+}
+
+__device__ __forceinline__ void level_corners_h(const __half2* table, const uint4* cells,
+                                                const LevelDev& L, uint32_t mask,
+                                                const CellCoord& c, uint32_t* t) {
+    if (cells && L.dense) {
+        cell_corners(cells, L, c, t);
+        return;
+    }
     const uint4* q4 = reinterpret_cast<const uint4*>(table);
     const uint32_t* t1 = reinterpret_cast<const uint32_t*>(table);
 #pragma unroll
@@ -324,9 +344,13 @@ __device__ __forceinline__ float2 corners_sum_h(const uint32_t* t, const CellCoo
 
 // The same 8 entries with one 4-byte load each: fewer registers in flight, which measured
 // faster in the 128-wide training kernel (one CTA of four warps per SM, latency-bound)
-__device__ __forceinline__ void level_corners_h_scalar(const __half2* table, const LevelDev& L,
-                                                       uint32_t mask, const CellCoord& c,
-                                                       uint32_t* t) {
+__device__ __forceinline__ void level_corners_h_scalar(const __half2* table, const uint4* cells,
+                                                       const LevelDev& L, uint32_t mask,
+                                                       const CellCoord& c, uint32_t* t) {
+    if (cells && L.dense) {
+        cell_corners(cells, L, c, t);
+        return;
+    }
     const uint32_t* t1 = reinterpret_cast<const uint32_t*>(table);
 #pragma unroll
     for (int k = 0; k < 8; ++k)
@@ -337,11 +361,12 @@ __device__ __forceinline__ void level_corners_h_scalar(const __half2* table, con
 // Features of one level from an FP16 table [rows][2] (half2 per row): trilinear over the 8
 // corners, summed in corner order 0..7.
 template <bool QUAD = true>
-__device__ __forceinline__ float2 level_features_h(const __half2* table, const LevelDev& L,
-                                                   uint32_t mask, const CellCoord& c) {
+__device__ __forceinline__ float2 level_features_h(const __half2* table, const uint4* cells,
+                                                   const LevelDev& L, uint32_t mask,
+                                                   const CellCoord& c) {
     uint32_t t[8];
-    if constexpr (QUAD) level_corners_h(table, L, mask, c, t);
-    else level_corners_h_scalar(table, L, mask, c, t);
+    if constexpr (QUAD) level_corners_h(table, cells, L, mask, c, t);
+    else level_corners_h_scalar(table, cells, L, mask, c, t);
     return corners_sum_h(t, c);
 }
 
@@ -357,7 +382,7 @@ __device__ __forceinline__ void levels_features_h(const __half2* table, const En
     for (int j = 0; j < LB; ++j) {
         const LevelDev L = enc.lv[l0 + j];
         cc[j] = cell_of(p, L.res);
-        level_corners_h(table, L, enc.hash_mask, cc[j], t + 8 * j);
+        level_corners_h(table, enc.cells, L, enc.hash_mask, cc[j], t + 8 * j);
     }
 #pragma unroll
     for (int j = 0; j < LB; ++j) {
@@ -436,6 +461,24 @@ __device__ __forceinline__ void glue16_aux(const FactorParams& fp, const float* 
     for (int k = 10; k < 16; ++k) x1[k] = 0.f;
 }
 
+// the reference network's glue (train.cu:41-112): [bc(max(L,0)) x3, bc(max(L^2,0)) x3, bc(thp) x3,
+// warped roughness, bc(ref_mean), 1, 0 x4] from its 6 outputs
+__device__ __forceinline__ void glue16_ref_aux(const float* y, const VertexAux& x, float* x1) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        x1[c] = box_cox(fmaxf(y[c], 0.f));
+        x1[3 + c] = box_cox(fmaxf(y[3 + c], 0.f));
+        x1[6 + c] = box_cox(x.thp[c]);
+    }
+    x1[9] = warp_rough(x.rough);
+    x1[10] = box_cox(x.ref);
+    x1[11] = 1.0f;
+#pragma unroll
+    for (int k = 12; k < 16; ++k) x1[k] = 0.f;
+}
+
+// REF: the reference network's StatNet outputs L itself (no log statistic)
+template <bool REF = false>
 __device__ __forceinline__ float rrs_factor_aux(const FactorParams& fp, const float* y, float raw,
                                                 const VertexAux& x) {
     float rrs;
@@ -444,7 +487,7 @@ __device__ __forceinline__ float rrs_factor_aux(const FactorParams& fp, const fl
         float acc = 0.f;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            float L = expf(fminf(y[c], 20.0f)) - fp.stat_eps;
+            float L = REF ? y[c] : expf(fminf(y[c], 20.0f)) - fp.stat_eps;
             L = L < 1e-4f ? 1e-4f : (L > 1e4f ? 1e4f : L);
             acc += L * x.thp[c] / ref;
         }
@@ -486,6 +529,49 @@ __device__ __forceinline__ float rrs_factor(const FactorParams& fp, const float*
     }
     rrs = rrs < fp.clamp_min ? fp.clamp_min : (rrs > fp.clamp_max ? fp.clamp_max : rrs);
     return rrs;
+}
+
+// ---- the reference's shipped network (NRRS_NET_REFERENCE): 32-wide LeakyReLU MLPs, a 32-lane
+//      StatNet input (8 hash levels, one-blob of the lat-long direction and of the warped
+//      roughness) and 6 outputs (L, L^2). Only this network is 32 wide, so kernels templated on
+//      the width select it by W == 32. ----
+constexpr int kRefStatIn = 32;
+constexpr int kRefStatOut = 6;
+constexpr int kRefLevels = 8;
+constexpr int kRefRrsLanes = 12;   // live RRSNet input lanes of the reference glue
+
+__host__ __device__ constexpr int stat_in_of(int w) { return w == 32 ? kRefStatIn : kStatIn; }
+__host__ __device__ constexpr int stat_out_of(int w) { return w == 32 ? kRefStatOut : kStatOut; }
+
+__device__ __forceinline__ float leaky(float x) { return x > 0.f ? x : 0.01f * x; }
+
+// CDF of the quartic (biweight) kernel of radius 1/bins at offset t: 15/16 (u - 2u^3/3 + u^5/5)
+// + 1/2 at u = t bins, clamped to [-1, 1]
+__device__ __forceinline__ float quartic_cdf(float t, int bins) {
+    float u = t * (float)bins;
+    u = u < -1.f ? -1.f : (u > 1.f ? 1.f : u);
+    const float u2 = u * u;
+    return 15.f / 16.f * u * (1.f - 2.f / 3.f * u2 + u2 * u2 / 5.f) + 0.5f;
+}
+// one-blob encoding of x in [0,1] into `bins` lanes: the kernel mass in each bin
+template <int BINS>
+__device__ __forceinline__ void one_blob(float x, float* out) {
+#pragma unroll
+    for (int k = 0; k < BINS; ++k)
+        out[k] = quartic_cdf((float)(k + 1) / (float)BINS - x, BINS) -
+                 quartic_cdf((float)k / (float)BINS - x, BINS);
+}
+// the 16 non-hash StatNet lanes of the reference network: one-blob (4 bins) of the lat-long u
+// and v of wi, u = atan2(y, x) / 2pi + 1/2, v = acos(z) / pi, and one-blob (8 bins) of the warped
+// roughness
+__device__ __forceinline__ void ref_blob_lanes(const VertexPtrs& v, uint32_t i, float* o /*16*/) {
+    const size_t i3 = 3 * (size_t)i;
+    const float z = fminf(fmaxf(v.wi[i3 + 2], -1.f), 1.f);
+    const float u = atan2f(v.wi[i3 + 1], v.wi[i3]) * 0.15915494309189535f + 0.5f;
+    const float w = acosf(z) * 0.3183098861837907f;
+    one_blob<4>(u, o);
+    one_blob<4>(w, o + 4);
+    one_blob<8>(1.0f - expf(-v.rough[i]), o + 8);
 }
 
 // ---- per-sample weights of the two losses (nrrs_train_step_batch) ----

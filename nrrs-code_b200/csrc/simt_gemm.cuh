@@ -3,8 +3,9 @@
 //
 // A CTA of 128 threads holds the activations of 64 samples in one shared-memory tile, K-major
 // ([k][64 samples + 4 pad]). A layer out[n][m] = epi(sum_k B[k][n] in[k][m]) is computed in place
-// on that tile: each thread owns an 8 x (W/16) block of outputs (8 samples x 8 or 4 neurons)
-// and, per k, reads 8 activations and 8 (or 4) B values as float4 and issues 64 (or 32) FMAs.
+// on that tile: each thread owns an 8 x (W/16) block of outputs (8 samples x 8, 4 or 2 neurons)
+// and, per k, reads 8 activations and 8, 4 or 2 B values (float4 / float2) and issues 64, 32 or
+// 16 FMAs.
 // B ([k_rows][W] in global memory: a layer's transposed weights for a forward step, its row-major
 // weights for a backward step) comes from L2 in 32-row chunks, double-buffered with cp.async.
 // Every output is accumulated as fmaf(B[k][n], in[k][m], acc) over k ascending, the order of the
@@ -46,8 +47,9 @@ __device__ __forceinline__ void load_chunk(float* dst, const float* __restrict__
 template <int W, class Epi>
 __device__ __forceinline__ void tile_gemm(const float* __restrict__ B, int k_rows, int k_eff,
                                           const float* act, float* wch, int tid, Epi&& epi) {
-    static_assert(W == 64 || W == 128, "tile widths");
-    constexpr int C = W / 16;                 // neurons per thread: 8 (W = 128) or 4 (W = 64)
+    static_assert(W == 32 || W == 64 || W == 128, "tile widths");
+    constexpr int C = W / 16;                 // neurons per thread: 8, 4 or 2 (W = 128, 64, 32)
+    constexpr int CW = C < 4 ? C : 4;         // consecutive neurons of a thread's group
     const int lane = tid & 31, warp = tid >> 5;
     const int tx = lane & 15, ty = warp * 2 + (lane >> 4);   // ty 0..7: samples ty*8 .. +7
     float acc[8][C];
@@ -68,7 +70,7 @@ __device__ __forceinline__ void tile_gemm(const float* __restrict__ B, int k_row
         cp_async_commit();
         cp_async_wait1();   // every group but the newest: chunk c has landed
         __syncthreads();
-        const float* Bc = wch + (c & 1) * kKC * W + tx * 4;
+        const float* Bc = wch + (c & 1) * kKC * W + tx * CW;
         const float* A = act + (size_t)(c * kKC) * kLd + ty * 8;
         const int kn = k_eff - c * kKC < kKC ? k_eff - c * kKC : kKC;
 #pragma unroll 4
@@ -77,8 +79,13 @@ __device__ __forceinline__ void tile_gemm(const float* __restrict__ B, int k_row
             const float4 a1 = *reinterpret_cast<const float4*>(A + kk * kLd + 4);
             const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
             float bv[C];
-            const float4 b0 = *reinterpret_cast<const float4*>(Bc + kk * W);
-            bv[0] = b0.x; bv[1] = b0.y; bv[2] = b0.z; bv[3] = b0.w;
+            if constexpr (C == 2) {
+                const float2 b0 = *reinterpret_cast<const float2*>(Bc + kk * W);
+                bv[0] = b0.x; bv[1] = b0.y;
+            } else {
+                const float4 b0 = *reinterpret_cast<const float4*>(Bc + kk * W);
+                bv[0] = b0.x; bv[1] = b0.y; bv[2] = b0.z; bv[3] = b0.w;
+            }
             if constexpr (C == 8) {
                 const float4 b1 = *reinterpret_cast<const float4*>(Bc + kk * W + 64);
                 bv[4] = b1.x; bv[5] = b1.y; bv[6] = b1.z; bv[7] = b1.w;
@@ -92,7 +99,7 @@ __device__ __forceinline__ void tile_gemm(const float* __restrict__ B, int k_row
     }
 #pragma unroll
     for (int j = 0; j < C; ++j) {
-        const int n = (j < 4 ? 0 : 64) + tx * 4 + (j & 3);
+        const int n = (j < 4 ? 0 : 64) + tx * CW + (j & 3);
         const float v[8] = {acc[0][j], acc[1][j], acc[2][j], acc[3][j],
                             acc[4][j], acc[5][j], acc[6][j], acc[7][j]};
         epi(n, ty * 8, v);

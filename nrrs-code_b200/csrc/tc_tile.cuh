@@ -173,5 +173,55 @@ __device__ __forceinline__ void epilogue_relu(uint32_t trow, uint8_t* sOut, int 
     }
 }
 
+// epilogue with the network's activation: ReLU, or LeakyReLU with slope 0.01 (the reference
+// network)
+template <int N, bool BF, bool LEAKY>
+__device__ __forceinline__ void epilogue_act(uint32_t trow, uint8_t* sOut, int m) {
+    if constexpr (!LEAKY) {
+        epilogue_relu<N, BF>(trow, sOut, m);
+    } else {
+#pragma unroll
+        for (int c0 = 0; c0 < N; c0 += 32) {
+            float v[32];
+            tc::tmem_ld16(trow + c0, v);
+            tc::tmem_ld16(trow + c0 + 16, v + 16);
+            tc::tmem_wait_ld();
+#pragma unroll
+            for (int j = 0; j < 32; ++j) v[j] = v[j] > 0.f ? v[j] : 0.01f * v[j];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) store_chunk(sOut, m, c0 / 8 + j, N, pack8<BF>(v + 8 * j));
+        }
+    }
+}
+
+// hidden-layer epilogue into TMEM: the TMEM row of D (N FP32 columns at trow) -> activation ->
+// FP16/BF16 pairs -> the next layer's A operand (N / 2 columns at trow_a); the caller waits for
+// the stores (tcgen05.wait::st) before the next MMA is issued
+template <int N, bool BF, bool LEAKY>
+__device__ __forceinline__ void epilogue_act_tmem(uint32_t trow, uint32_t trow_a) {
+#pragma unroll
+    for (int c0 = 0; c0 < N; c0 += 32) {
+        float v[32];
+        tc::tmem_ld16(trow + c0, v);
+        tc::tmem_ld16(trow + c0 + 16, v + 16);
+        tc::tmem_wait_ld();
+        uint32_t pk[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            float x0 = v[2 * j], x1 = v[2 * j + 1];
+            if constexpr (LEAKY) {
+                x0 = x0 > 0.f ? x0 : 0.01f * x0;
+                x1 = x1 > 0.f ? x1 : 0.01f * x1;
+            } else {
+                x0 = fmaxf(x0, 0.f);
+                x1 = fmaxf(x1, 0.f);
+            }
+            pk[j] = pack2<BF>(x0, x1);
+        }
+        tc::tmem_st16(trow_a + c0 / 2, pk);
+    }
+    tc::tmem_wait_st();
+}
+
 }  // namespace tile
 }  // namespace nrrs

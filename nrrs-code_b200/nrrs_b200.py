@@ -51,7 +51,7 @@ class Config(C.Structure):
         ("loss_clamp_max", C.c_float), ("cost_offset", C.c_float),
         ("normalize_pos", C.c_int32), ("aabb_min", C.c_float * 3), ("aabb_max", C.c_float * 3),
         ("max_queue", C.c_uint32), ("max_train", C.c_uint32), ("step", C.c_int32),
-        ("network", C.c_int32),
+        ("network", C.c_int32), ("ema_decay", C.c_float),
     ]
 
 
@@ -183,6 +183,7 @@ _SIGS = {
                                     C.POINTER(C.c_uint64)]),
     "nrrs_get_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     "nrrs_set_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
+    "nrrs_get_inference_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     "nrrs_get_grads": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     "nrrs_get_adam_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
                                       C.POINTER(C.c_uint64)]),
@@ -233,6 +234,8 @@ _SIGS = {
     "nrrs_get_launch_shape": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "nrrs_set_infer_split": (C.c_int, [C.c_void_p, C.c_int32]),
     "nrrs_get_infer_split": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "nrrs_set_cell_image": (C.c_int, [C.c_void_p, C.c_int32]),
+    "nrrs_get_cell_image": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "nrrs_set_train_split": (C.c_int, [C.c_void_p, C.c_int32]),
     "nrrs_get_train_split": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "nrrs_graph_capture_batched": (C.c_int, [C.c_void_p, C.POINTER(VertexSoA), C.c_void_p,
@@ -329,7 +332,7 @@ _SIGS = {
 
 KERNEL_KINDS = ("infer_fp32", "infer_tc", "sum", "decide", "pack_weights", "table_half",
                 "train_statnet", "train_rrsnet", "train_wgrad", "train_reduce", "adam", "encode",
-                "train_scatter", "train_encode", "infer_rrs")
+                "train_scatter", "train_encode", "infer_rrs", "cell_image")
 
 
 def lib():
@@ -1101,6 +1104,13 @@ class NRRSNetwork:
         self._check(lib().nrrs_get_params(self._h, a.ctypes.data, a.size))
         return a
 
+    def get_inference_params(self):
+        """the weights inference uses (the debiased moving average when ema_decay > 0)"""
+        import numpy as np
+        a = np.empty(self.param_count(), np.float32)
+        self._check(lib().nrrs_get_inference_params(self._h, a.ctypes.data, a.size))
+        return a
+
     def set_params(self, a):
         import numpy as np
         a = np.ascontiguousarray(a, dtype=np.float32)
@@ -1139,7 +1149,8 @@ class NRRSNetwork:
 
     def set_infer_split(self, split: int):
         """0 = fused inference, 1 = level-major encoding kernel + MLP kernel (large tables),
-        2 = encoding kernel + StatNet kernel + RRSNet kernel."""
+        2 = encoding kernel + StatNet kernel + RRSNet kernel, 3 = as 2 with the hidden
+        activations in TMEM."""
         self._check(lib().nrrs_set_infer_split(self._h, int(split)))
 
     def set_train_split(self, split: bool):
@@ -1155,6 +1166,16 @@ class NRRSNetwork:
         v = C.c_int32()
         self._check(lib().nrrs_get_infer_split(self._h, C.byref(v)))
         return int(v.value)
+
+    def set_cell_image(self, enable: bool):
+        """gathers of the dense levels from the cell image (one 32-byte load per cell) or from
+        the table rows; bit-identical results"""
+        self._check(lib().nrrs_set_cell_image(self._h, int(bool(enable))))
+
+    def cell_image(self) -> bool:
+        v = C.c_int32()
+        self._check(lib().nrrs_get_cell_image(self._h, C.byref(v)))
+        return bool(v.value)
 
     def launch_shape(self) -> tuple[int, int]:
         c, w = C.c_int32(), C.c_int32()

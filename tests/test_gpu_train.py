@@ -7,7 +7,7 @@ import pytest
 
 import nrrs_b200 as nb
 import oracle as O
-from gpu_util import host, make_net, random_params, soa, stream, torch_cuda, upload
+from gpu_util import empty, host, make_net, random_params, soa, stream, torch_cuda, upload
 
 pytestmark = pytest.mark.gpu
 
@@ -249,25 +249,36 @@ def test_train_step_batch_weighted_losses_vs_fp64_oracle(prec):
 
 @pytest.mark.parametrize("prec", [nb.PREC_FP32, nb.PREC_FP16], ids=["fp32", "fp16"])
 def test_train_step_batch_defaults_equal_train_step(prec):
-    """with no side arrays and the default loss parameters the batch step is nrrs_train_step"""
+    """with no side arrays and the default loss parameters the batch step is nrrs_train_step,
+    and so is everything after it: the factors inferred with the updated weights (the weight
+    images are rebuilt after the step) and the losses of a second step"""
     torch = torch_cuda()
     n = 5000
     v = nb.synth(44, n)
+    dp = nb.default_decide()
     out = []
     for batch_form in (False, True):
         net = make_net(precision=prec, max_train=1 << 13, step=3, log2_hashmap_size=15)
         random_params(net, 45, table_scale=0.5, mlp_scale=0.15)
         b = _batch_dev(v, {})
-        loss = torch.zeros(2, dtype=torch.float64, device="cuda")
-        if batch_form:
-            net.trainStepBatch(nb.train_batch(**b), n, None, None, nb.default_loss_params(),
-                               loss, stream())
-        else:
-            net.train(soa(b), b["target"], n, loss, stream())
+        losses = []
+        for _ in range(2):
+            loss = torch.zeros(2, dtype=torch.float64, device="cuda")
+            if batch_form:
+                net.trainStepBatch(nb.train_batch(**b), n, None, None,
+                                   nb.default_loss_params(), loss, stream())
+            else:
+                net.train(soa(b), b["target"], n, loss, stream())
+            losses.append(loss)
+            if len(losses) == 1:
+                st, rr = empty(3 * n), empty(n)
+                net.inference(soa(b), n, dp, st, rr, stream())
         torch.cuda.synchronize()
-        out.append((loss.cpu().numpy(), net.get_grads().astype(np.float64), net.get_params()))
+        out.append((np.stack([l.cpu().numpy() for l in losses]),
+                    net.get_grads().astype(np.float64), net.get_params(), host(rr)[:n].copy()))
         net.close()
-    (la, ga, pa), (lb, gb, pb) = out
+    (la, ga, pa, ra), (lb, gb, pb, rb) = out
     assert np.allclose(la, lb, rtol=1e-6, atol=0)
     assert rel_err(gb, ga) < 1e-6
     assert np.allclose(pa, pb, rtol=1e-5, atol=1e-7)
+    assert np.allclose(ra, rb, rtol=1e-5, atol=1e-7)

@@ -104,9 +104,10 @@ SPLIT_SHAPES = {
 @pytest.mark.parametrize("factor", [nb.FACTOR_RRSNET, nb.FACTOR_ADRRS], ids=["rrsnet", "adrrs"])
 @pytest.mark.parametrize("shape", list(SPLIT_SHAPES))
 def test_split_inference_equals_fused(shape, factor):
-    """both split modes (encoding kernel + one MLP kernel; encoding + StatNet + RRSNet kernels)
-    give the fused kernel's outputs bit for bit, for every warpgroup count that fits, on a ragged
-    multi-segment launch, with RRSNet and ADRRS factors"""
+    """every split mode (encoding kernel + one MLP kernel; encoding + StatNet + RRSNet kernels;
+    the same with the hidden activations in TMEM) gives the fused kernel's outputs bit for bit,
+    for every warpgroup count that fits, on a ragged multi-segment launch, with RRSNet and
+    ADRRS factors"""
     torch = torch_cuda()
     prec, kw = SPLIT_SHAPES[shape]
     net = make_net(precision=prec, **kw)
@@ -136,7 +137,7 @@ def test_split_inference_equals_fused(shape, factor):
     net.set_launch_shape(0, 1)
     ref = run()
     tried = 0
-    for mode in (1, 2):
+    for mode in (1, 2, 3):
         net.set_infer_split(mode)
         assert net.infer_split() == mode
         for w in (1, 2, 4):
