@@ -344,6 +344,9 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
 // 2^T x 8 bytes), which stays in L2, instead of the whole table. dxs: the per-sample hash-lane
 // gradients that k_ttc_stat wrote, [16][n] float pairs; the 1/n of the batch mean is applied
 // here. Levels [level_begin, level_end) of the launch.
+// FP32 table-gradient bytes per scatter launch of the split step (a fraction of L2)
+constexpr uint64_t kScatterGroupBytes = 40ull << 20;
+
 struct ScatterLvArgs {
     EncodeParams enc;
     const float* pos;
@@ -818,7 +821,11 @@ int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint3
         (reinterpret_cast<uintptr_t>(partial + chunks_max * mlp) + 15u) & ~uintptr_t(15));
     const bool train_rrs = c.step >= 3;
     const bool split = ctx->train_split != 0;
-    cudaError_t e = cudaMemsetAsync(ctx->grads, 0, sizeof(float) * ctx->n_params, s);
+    // the split step zeroes the table gradient level group by level group right before that
+    // group's scatter (below); here only what the other kernels accumulate into
+    const uint64_t zero_from = split ? ctx->n_table : 0;
+    cudaError_t e = cudaMemsetAsync(ctx->grads + zero_from, 0,
+                                    sizeof(float) * (ctx->n_params - zero_from), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(part, 0, sizeof(double) * 4 * part_rows, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(partial, 0, sizeof(float) * chunks * mlp, s);
     if (e != cudaSuccess) {
@@ -880,6 +887,11 @@ int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint3
     if (W == 64) e = H == 2 ? launch_ttc<64, 2>(ctx, a, s, train_rrs) : launch_ttc<64, 3>(ctx, a, s, train_rrs);
     else e = H == 2 ? launch_ttc<128, 2>(ctx, a, s, train_rrs) : launch_ttc<128, 3>(ctx, a, s, train_rrs);
     if (e == cudaSuccess && split) {
+        // Level groups of at most kScatterGroupBytes of FP32 gradient, each zeroed right before
+        // its scatter: the zeroing writes whole sectors into L2, so the reductions that follow
+        // hit there. Zeroed at the start of the step, the slices were evicted by the kernels in
+        // between, and every first reduction into a sector read its zeros back from HBM as a
+        // random 32-byte access.
         ScatterLvArgs sa{};
         sa.enc = ctx->enc;
         sa.pos = v.pos;
@@ -887,14 +899,35 @@ int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint3
         sa.table_grad = ctx->grads;
         sa.n = n;
         sa.inv_n = a.inv_n;
-        sa.level_begin = 0;
-        sa.level_end = kMaxLevels;
-        const uint32_t items = kMaxLevels * ((n + 127) / 128);
-        uint32_t g = (uint32_t)(ctx->sm_count * resident_ctas((const void*)k_scatter_levels, 128, 0, 16));
-        if (g > items) g = items;
-        ProfScope ps(ctx, NRRS_KERNEL_TRAIN_SCATTER, s);
-        if (g) k_scatter_levels<<<g, 128, 0, s>>>(sa);
-        e = cudaGetLastError();
+        const uint32_t tiles = (n + 127) / 128;
+        const uint32_t g_max =
+            (uint32_t)(ctx->sm_count * resident_ctas((const void*)k_scatter_levels, 128, 0, 16));
+        const int nl = c.n_levels;
+        auto level_rows = [&](int l) -> uint64_t {
+            const LevelDev& lv = ctx->enc.lv[l];
+            const uint64_t r = (uint64_t)lv.res + 1;
+            return lv.dense ? r * r * r : (uint64_t)ctx->enc.hash_mask + 1;
+        };
+        for (int l0 = 0; l0 < nl && e == cudaSuccess;) {
+            const uint64_t row0 = ctx->enc.lv[l0].offset;
+            uint64_t row1 = row0 + level_rows(l0);
+            int l1 = l0 + 1;
+            while (l1 < nl && (ctx->enc.lv[l1].offset + level_rows(l1) - row0) * 8u <=
+                                  kScatterGroupBytes) {
+                row1 = ctx->enc.lv[l1].offset + level_rows(l1);
+                ++l1;
+            }
+            e = cudaMemsetAsync(ctx->grads + 2 * row0, 0, sizeof(float) * 2 * (row1 - row0), s);
+            if (e != cudaSuccess) break;
+            sa.level_begin = (uint32_t)l0;
+            sa.level_end = (uint32_t)l1;
+            const uint32_t items = (uint32_t)(l1 - l0) * tiles;
+            const uint32_t g = g_max < items ? g_max : items;
+            ProfScope ps(ctx, NRRS_KERNEL_TRAIN_SCATTER, s);
+            if (g) k_scatter_levels<<<g, 128, 0, s>>>(sa);
+            e = cudaGetLastError();
+            l0 = l1;
+        }
     }
     if (e != cudaSuccess) {
         ctx->last_error = std::string("tensor-core train launch: ") + cudaGetErrorString(e);
