@@ -73,7 +73,11 @@ struct TcShape {
         PRE && PART != 2 && 1024 + kAOff + WGS * (kABytes + kSepBytes) + 64 > 232448u;
     static constexpr uint32_t kHBytes = PRE && PART != 2 && !kShare ? kSepBytes : 0u;
     static constexpr uint32_t kHOff = kAOff + WGS * kABytes;
-    static constexpr uint32_t kBarOff = kHOff + WGS * kHBytes;
+    // PART 2: per warpgroup the RRSNet input tile, apart from the activation tile so that the
+    // next tile's can be fetched while this one's chain runs
+    static constexpr uint32_t kXBytes = PART == 2 ? kX1TileBytes : 0u;
+    static constexpr uint32_t kXOff = kHOff + WGS * kHBytes;
+    static constexpr uint32_t kBarOff = kXOff + WGS * kXBytes;
     static constexpr size_t kSmem = 1024 + kBarOff + 96;
     static_assert(!kShare || kABytes >= kSepBytes, "feature blocks inside the activation tile");
 };
@@ -156,6 +160,46 @@ __device__ __forceinline__ void sh_misc_row_tc(const InferArgs& a, uint32_t i, u
     store_chunk(sS, m, 1, 32, pack8<BF>(sh + 8));
     float misc[16];
     misc_lanes(a.v, i, misc);
+    store_chunk(sS, m, 2, 32, pack8<BF>(misc));
+    store_chunk(sS, m, 3, 32, make_uint4(0u, 0u, 0u, 0u));
+}
+
+// The SH and misc inputs of one vertex (wi, normal, albedo, roughness), loaded during the
+// previous tile's MLP chain so that their memory latency is not on the tile's critical path.
+struct ShMiscIn {
+    float wi[3], nrm[3], alb[3], rough;
+};
+
+__device__ __forceinline__ ShMiscIn load_sh_misc(const InferArgs& a, uint32_t i) {
+    ShMiscIn s;
+    const size_t i3 = 3 * (size_t)i;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        s.wi[c] = a.v.wi[i3 + c];
+        s.nrm[c] = a.v.normal[i3 + c];
+        s.alb[c] = a.v.albedo[i3 + c];
+    }
+    s.rough = a.v.rough[i];
+    return s;
+}
+
+// the lanes of sh_misc_row_tc from inputs already in registers (the same arithmetic)
+template <bool BF>
+__device__ __forceinline__ void sh_misc_row_from(const ShMiscIn& in, uint8_t* sS, int m) {
+    float sh[16];
+    sh16(in.wi[0], in.wi[1], in.wi[2], sh);
+    store_chunk(sS, m, 0, 32, pack8<BF>(sh));
+    store_chunk(sS, m, 1, 32, pack8<BF>(sh + 8));
+    float misc[16];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        misc[c] = in.nrm[c];
+        misc[3 + c] = in.alb[c];
+    }
+    misc[6] = warp_rough(in.rough);
+    misc[7] = 1.0f;
+#pragma unroll
+    for (int k = 8; k < 16; ++k) misc[k] = 0.f;
     store_chunk(sS, m, 2, 32, pack8<BF>(misc));
     store_chunk(sS, m, 3, 32, make_uint4(0u, 0u, 0u, 0u));
 }
@@ -256,6 +300,7 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64 && !TA) ? 3 :
     uint8_t* sA = base + S::kAOff + wg * S::kABytes;
     uint8_t* sH = S::kShare ? sA : base + S::kHOff + wg * S::kHBytes;  // split mode only
     uint8_t* sS = sH + kEncTileBytes;
+    uint8_t* sX = base + S::kXOff + wg * S::kXBytes;   // PART 2 only
 
     if (tid == 0) {
         for (int k = 0; k < 1 + 2 * WGS; ++k) tc::mbar_init(&bars[k], 1);
@@ -311,9 +356,27 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64 && !TA) ? 3 :
         }
         h_pending = true;
     };
+    auto fetch_x1 = [&](uint32_t tt) {
+        if (ltid == 0) {
+            tc::mbar_arrive_expect_tx(hbar, kX1TileBytes);
+            tc::bulk_g2s(sX, a.x1_tiles + (size_t)tt * kX1TileBytes, kX1TileBytes, hbar);
+        }
+        h_pending = true;
+    };
     const SegmentTable& ST = seg_table(a.segs);
     const uint32_t total_tiles = ST.total_tiles;
-    if (PRE && kStat && !S::kShare && t0 < total_tiles && !flags) fetch_features(t0);
+    // PART 1 requests every tile's feature block and SH/misc inputs one tile ahead: the first
+    // here, the next ones during the previous tile's chain; PART 2 its RRSNet input tiles
+    ShMiscIn shin{};
+    if (t0 < total_tiles && !flags) {
+        if (PRE && kStat && (!S::kShare || PART == 1)) fetch_features(t0);
+        if constexpr (PART == 1) {
+            const Segment& g0 = ST.s[find_segment(ST, t0)];
+            const uint32_t i0 = g0.offset + (t0 - g0.tile_start) * kTile + ltid;
+            if (i0 < g0.offset + g0.count) shin = load_sh_misc(a, i0);
+        }
+        if constexpr (PART == 2) fetch_x1(t0);
+    }
 
     for (uint32_t t = t0; t < total_tiles && !flags; t += tstride) {
         const int si = find_segment(ST, t);
@@ -331,13 +394,16 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64 && !TA) ? 3 :
             for (int k = 0; k < 16; ++k) y[k] = 0.f;  // not used by the RRSNet factor
         }
         if constexpr (kStat) {
-            // the previous tile's RRSNet-input store (PART 1) has finished reading the A tile
-            if (PART == 1 && ltid == 0) tc::bulk_wait_read();
-            // shared layout: the previous tile's chain has finished with the activation tile
-            if (PRE && S::kShare) fetch_features(t);
+            // shared layout (PART 0): the previous tile's chain has finished with the activation
+            // tile
+            if (PRE && S::kShare && PART != 1) fetch_features(t);
             if constexpr (PRE) {
-                if (valid) sh_misc_row_tc<BF>(a, i, sS, ltid);
-                else zero_row(sS, ltid, 32);
+                if constexpr (PART == 1) {
+                    if (valid) sh_misc_row_from<BF>(shin, sS, ltid);
+                } else {
+                    if (valid) sh_misc_row_tc<BF>(a, i, sS, ltid);
+                }
+                if (!valid) zero_row(sS, ltid, 32);
                 ok = tc::mbar_wait(hbar, hphase, kSpin);
                 hphase ^= 1u;
                 h_pending = false;
@@ -381,6 +447,17 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64 && !TA) ? 3 :
                 }
                 ok &= tc_layer<WS, 16, BF>(sA, wSo, tmem, mbar, phase, ltid);
             }
+            if constexpr (PART == 1) {
+                // every read of the tile is done: request the next tile's inputs, which land
+                // while this tile's glue and stores run
+                const uint32_t tn = t + tstride;
+                if (tn < total_tiles && ok) {
+                    if (S::kShare) fetch_features(tn);
+                    const Segment& gn = ST.s[find_segment(ST, tn)];
+                    const uint32_t in_ = gn.offset + (tn - gn.tile_start) * kTile + ltid;
+                    if (in_ < gn.offset + gn.count) shin = load_sh_misc(a, in_);
+                }
+            }
             tc::tmem_ld16(trow, y);
             tc::tmem_wait_ld();
 
@@ -393,31 +470,37 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64 && !TA) ? 3 :
 #pragma unroll
                 for (int k = 0; k < 16; ++k) x1[k] = 0.f;
             }
-            store_chunk(sA, ltid, 0, 16, pack8<BF>(x1));
-            store_chunk(sA, ltid, 1, 16, pack8<BF>(x1 + 8));
-            wg_sync_for_mma(wg);
-            if (PART == 1 && ltid == 0) {
-                tc::bulk_s2g(a.x1_tiles + (size_t)t * kX1TileBytes, sA, kX1TileBytes);
-                tc::bulk_commit();
+            if constexpr (PART == 1) {
+                // straight from registers into the tile's K-major core-matrix layout in HBM
+                uint8_t* dst = a.x1_tiles + (size_t)t * kX1TileBytes;
+                *reinterpret_cast<uint4*>(dst + chunk_offset(ltid, 0, 16)) = pack8<BF>(x1);
+                *reinterpret_cast<uint4*>(dst + chunk_offset(ltid, 1, 16)) = pack8<BF>(x1 + 8);
+            } else {
+                store_chunk(sA, ltid, 0, 16, pack8<BF>(x1));
+                store_chunk(sA, ltid, 1, 16, pack8<BF>(x1 + 8));
+                wg_sync_for_mma(wg);
             }
         } else {
-            // PART 2: this tile's RRSNet input from the StatNet kernel
-            if (ltid == 0) {
-                tc::mbar_arrive_expect_tx(hbar, kX1TileBytes);
-                tc::bulk_g2s(sA, a.x1_tiles + (size_t)t * kX1TileBytes, kX1TileBytes, hbar);
-            }
+            // PART 2: this tile's RRSNet input from the StatNet kernel, requested one tile ahead
             ok = tc::mbar_wait(hbar, hphase, kSpin);
             hphase ^= 1u;
+            h_pending = false;
             tc::fence_after_sync();
         }
 
         float r[16];
         if constexpr (kRrs) {
             // ---- RRSNet ----
-            ok &= tc_layer<kRrsIn, WR, BF>(sA, wR0, tmem, mbar, phase, ltid);
+            ok &= tc_layer<kRrsIn, WR, BF>(PART == 2 ? sX : sA, wR0, tmem, mbar, phase, ltid);
+            // PART 2: the first layer has read the input tile, and after the barrier below every
+            // thread of the warpgroup has seen this tile's copy land (a copy requested before
+            // that could complete the barrier's next phase under a thread still waiting for
+            // this one, which would then wait forever): bring in the next tile's
+            const bool next_x1 = PART == 2 && ok && t + tstride < total_tiles;
             if constexpr (TA) {
                 epilogue_act_tmem<WR, BF, REF>(trow, trow_a);
                 wg_sync_tmem(wg);
+                if (next_x1) fetch_x1(t + tstride);
 #pragma unroll 1
                 for (int h = 1; h < HR; ++h) {
                     ok &= tc_layer_ts<WR, WR, BF>(tmem_a, wRh + (h - 1) * WR * WR * 2, tmem, mbar,
@@ -429,6 +512,7 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64 && !TA) ? 3 :
             } else {
                 epilogue_act<WR, BF, REF>(trow, sA, ltid);
                 wg_sync_for_mma(wg);
+                if (next_x1) fetch_x1(t + tstride);
 #pragma unroll 1
                 for (int h = 1; h < HR; ++h) {
                     ok &= tc_layer<WR, WR, BF>(sA, wRh + (h - 1) * WR * WR * 2, tmem, mbar, phase,
@@ -474,10 +558,8 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64 && !TA) ? 3 :
         if (s_abort[wg]) flags |= NRRS_DEV_TIMEOUT;
     }
 
-    // a copy still in flight (the loop ended early) lands before the CTA leaves; the RRSNet
-    // input stores are complete
+    // a copy still in flight (the loop ended early) lands before the CTA leaves
     if (h_pending && ltid == 0 && !tc::mbar_wait(hbar, hphase, kSpin)) flags |= NRRS_DEV_TIMEOUT;
-    if (PART == 1 && ltid == 0) tc::bulk_wait_all();
     if (flags && a.scr) atomicOr(&a.scr->status, flags);
     tc::fence_before_sync();
     __syncthreads();

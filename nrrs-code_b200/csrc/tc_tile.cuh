@@ -26,6 +26,18 @@ __device__ __forceinline__ uint32_t pack2(float a, float b) {
     }
 }
 
+// ReLU and the conversion in one instruction (cvt with .relu: negative results become 0);
+// x0 goes to the low half like pack2
+template <bool BF>
+__device__ __forceinline__ uint32_t pack2_relu(float x0, float x1) {
+    uint32_t d;
+    if constexpr (BF)
+        asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(x1), "f"(x0));
+    else
+        asm("cvt.rn.relu.f16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(x1), "f"(x0));
+    return d;
+}
+
 template <bool BF>
 __device__ __forceinline__ float2 unpack2(uint32_t u) {
     if constexpr (BF) {
@@ -157,7 +169,8 @@ __device__ __forceinline__ void epilogue_mask_bits(uint32_t trow, const uint32_t
     }
 }
 
-// hidden-layer epilogue: TMEM row -> ReLU -> tile (K = N)
+// hidden-layer epilogue: TMEM row -> ReLU -> tile (K = N); ReLU and conversion are one cvt
+// per pair of columns
 template <int N, bool BF>
 __device__ __forceinline__ void epilogue_relu(uint32_t trow, uint8_t* sOut, int m) {
 #pragma unroll
@@ -167,9 +180,12 @@ __device__ __forceinline__ void epilogue_relu(uint32_t trow, uint8_t* sOut, int 
         tc::tmem_ld16(trow + c0 + 16, v + 16);
         tc::tmem_wait_ld();
 #pragma unroll
-        for (int j = 0; j < 32; ++j) v[j] = fmaxf(v[j], 0.f);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) store_chunk(sOut, m, c0 / 8 + j, N, pack8<BF>(v + 8 * j));
+        for (int j = 0; j < 4; ++j) {
+            const float* w = v + 8 * j;
+            store_chunk(sOut, m, c0 / 8 + j, N,
+                        make_uint4(pack2_relu<BF>(w[0], w[1]), pack2_relu<BF>(w[2], w[3]),
+                                   pack2_relu<BF>(w[4], w[5]), pack2_relu<BF>(w[6], w[7])));
+        }
     }
 }
 
@@ -212,11 +228,10 @@ __device__ __forceinline__ void epilogue_act_tmem(uint32_t trow, uint32_t trow_a
             if constexpr (LEAKY) {
                 x0 = x0 > 0.f ? x0 : 0.01f * x0;
                 x1 = x1 > 0.f ? x1 : 0.01f * x1;
+                pk[j] = pack2<BF>(x0, x1);
             } else {
-                x0 = fmaxf(x0, 0.f);
-                x1 = fmaxf(x1, 0.f);
+                pk[j] = pack2_relu<BF>(x0, x1);
             }
-            pk[j] = pack2<BF>(x0, x1);
         }
         tc::tmem_st16(trow_a + c0 / 2, pk);
     }

@@ -155,6 +155,41 @@ def test_split_inference_equals_fused(shape, factor):
     net.close()
 
 
+def test_split_modes_with_many_tiles_per_warpgroup():
+    """one CTA per SM, so every warpgroup walks about 27 tiles and requests each next tile's
+    inputs during the current one: no wait runs out (device status clean) and the outputs
+    equal the fused kernel's, in every split mode and warpgroup count"""
+    torch = torch_cuda()
+    prec, kw = SPLIT_SHAPES["w128h3_bf16"]
+    net = make_net(precision=prec, **kw)
+    random_params(net, 57, table_scale=0.5, mlp_scale=0.1)
+    n = 2_000_000
+    v = nb.synth(58, n)
+    d = upload(v)
+    dp = nb.default_decide()
+
+    def run():
+        st, rr = empty(3 * n), empty(n)
+        net.inference(soa(d), n, dp, st, rr, stream())
+        torch.cuda.synchronize()
+        return st, rr
+
+    net.set_infer_split(0)
+    net.set_launch_shape(0, 1)
+    ref = run()
+    for mode in (1, 2, 3):
+        net.set_infer_split(mode)
+        for w in (1, 2, 4):
+            try:
+                net.set_launch_shape(1, w)
+            except nb.NRRSError:
+                continue
+            out = run()
+            assert net.device_status(stream()) == (nb.OK, 0), (mode, w)
+            assert torch.equal(out[0], ref[0]) and torch.equal(out[1], ref[1]), (mode, w)
+    net.close()
+
+
 def test_split_mode_graph_equals_fused_direct():
     torch = torch_cuda()
     net = make_net(precision=nb.PREC_FP16)
