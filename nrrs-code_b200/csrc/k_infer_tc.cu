@@ -447,15 +447,17 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64 && !TA) ? 3 :
                 }
                 ok &= tc_layer<WS, 16, BF>(sA, wSo, tmem, mbar, phase, ltid);
             }
+            // PART 1: every read of the tile is done: request the next tile's feature block,
+            // which lands while this tile's glue and stores run; its SH/misc inputs are loaded
+            // after the glue (issued before it, the loads measured slower)
+            uint32_t next_i = 0xffffffffu;
             if constexpr (PART == 1) {
-                // every read of the tile is done: request the next tile's inputs, which land
-                // while this tile's glue and stores run
                 const uint32_t tn = t + tstride;
                 if (tn < total_tiles && ok) {
                     if (S::kShare) fetch_features(tn);
                     const Segment& gn = ST.s[find_segment(ST, tn)];
                     const uint32_t in_ = gn.offset + (tn - gn.tile_start) * kTile + ltid;
-                    if (in_ < gn.offset + gn.count) shin = load_sh_misc(a, in_);
+                    if (in_ < gn.offset + gn.count) next_i = in_;
                 }
             }
             tc::tmem_ld16(trow, y);
@@ -471,7 +473,9 @@ __global__ void __launch_bounds__(128 * WGS, (WGS == 2 && WS <= 64 && !TA) ? 3 :
                 for (int k = 0; k < 16; ++k) x1[k] = 0.f;
             }
             if constexpr (PART == 1) {
-                // straight from registers into the tile's K-major core-matrix layout in HBM
+                if (next_i != 0xffffffffu) shin = load_sh_misc(a, next_i);
+                // the RRSNet input straight from registers into the tile's K-major core-matrix
+                // layout in HBM
                 uint8_t* dst = a.x1_tiles + (size_t)t * kX1TileBytes;
                 *reinterpret_cast<uint4*>(dst + chunk_offset(ltid, 0, 16)) = pack8<BF>(x1);
                 *reinterpret_cast<uint4*>(dst + chunk_offset(ltid, 1, 16)) = pack8<BF>(x1 + 8);
