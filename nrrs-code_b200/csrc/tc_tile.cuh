@@ -169,8 +169,10 @@ __device__ __forceinline__ void epilogue_mask_bits(uint32_t trow, const uint32_t
     }
 }
 
-// hidden-layer epilogue: TMEM row -> ReLU -> tile (K = N); ReLU and conversion are one cvt
-// per pair of columns
+// hidden-layer epilogue: TMEM row -> ReLU -> tile (K = N). At N = 128 ReLU and conversion are
+// one cvt per pair of columns (fewer instructions in the 4K kernels' epilogues); the 64-wide
+// kernels keep max + convert, which the compiler schedules into fewer registers (their
+// 3-CTA launch bounds leave 80)
 template <int N, bool BF>
 __device__ __forceinline__ void epilogue_relu(uint32_t trow, uint8_t* sOut, int m) {
 #pragma unroll
@@ -179,12 +181,19 @@ __device__ __forceinline__ void epilogue_relu(uint32_t trow, uint8_t* sOut, int 
         tc::tmem_ld16(trow + c0, v);
         tc::tmem_ld16(trow + c0 + 16, v + 16);
         tc::tmem_wait_ld();
+        if constexpr (N >= 128) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const float* w = v + 8 * j;
-            store_chunk(sOut, m, c0 / 8 + j, N,
-                        make_uint4(pack2_relu<BF>(w[0], w[1]), pack2_relu<BF>(w[2], w[3]),
-                                   pack2_relu<BF>(w[4], w[5]), pack2_relu<BF>(w[6], w[7])));
+            for (int j = 0; j < 4; ++j) {
+                const float* w = v + 8 * j;
+                store_chunk(sOut, m, c0 / 8 + j, N,
+                            make_uint4(pack2_relu<BF>(w[0], w[1]), pack2_relu<BF>(w[2], w[3]),
+                                       pack2_relu<BF>(w[4], w[5]), pack2_relu<BF>(w[6], w[7])));
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) v[j] = fmaxf(v[j], 0.f);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) store_chunk(sOut, m, c0 / 8 + j, N, pack8<BF>(v + 8 * j));
         }
     }
 }
