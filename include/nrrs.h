@@ -118,6 +118,10 @@ typedef struct {
      * and the inference entry points use e / (1 - d^t), t the number of steps since; training
      * keeps using w. 0 (the default) = off: inference uses w. */
     float ema_decay;
+    /* Adam learning rate of the RRSNet parameters; 0 (the default) = lr. The reference trains
+     * its two networks with separate optimizers (2net-simple.json level0 lr 5e-3 for the
+     * encoding and StatNet, level1 lr 5e-4 for RRSNet). */
+    float lr_rrsnet;
 } nrrs_config;
 
 /* The two network families.
@@ -177,8 +181,9 @@ typedef struct nrrs_ctx nrrs_ctx;
 /* ---- lifetime ---- */
 void nrrs_config_default(nrrs_config* cfg);
 /* the reference's shipped network (NRRS_NET_REFERENCE) with its grid, widths and optimizer
- * settings (2net-simple.json: HashGrid 8 x 2, 2^19, base 16, scale 2.0; 32 x 3; Adam lr 5e-3,
- * beta 0.9 / 0.99, eps 1e-15, l2 3e-6); the other fields keep nrrs_config_default's values */
+ * settings (2net-simple.json: HashGrid 8 x 2, 2^19, base 16, scale 2.0; 32 x 3; Adam lr 5e-3
+ * (RRSNet 5e-4), beta 0.9 / 0.99, eps 1e-15, l2 3e-6, moving average 0.95); the other fields
+ * keep nrrs_config_default's values */
 void nrrs_config_reference_network(nrrs_config* cfg);
 /* NRRSNetwork::NRRSNetwork + reset + resize (network.cpp:443-576, 351-441). */
 int nrrs_create(const nrrs_config* cfg, nrrs_ctx** out);

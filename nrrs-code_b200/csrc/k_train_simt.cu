@@ -592,17 +592,20 @@ struct AdamArgs {
     __half* table_h;       // FP16 copy of [0, n_table) refreshed in the same pass (may be null)
     uint64_t n_table;
     uint64_t first, count;
-    float lr, b1, b2, eps, l2, inv_c1, inv_c2;
+    uint64_t rrs_first;    // parameters from here on (the RRSNet) use lr_rrs
+    float lr, lr_rrs, b1, b2, eps, l2, inv_c1, inv_c2;
 };
 
 // Adam on one parameter. The bias corrections are multiplications by 1/c1 and 1/c2 computed on
 // the host, and the step is one fast division: IEEE divisions made this streaming kernel
 // instruction-bound (69 % issue-active at 50 % of HBM bandwidth).
-__device__ __forceinline__ float adam_one(const AdamArgs& a, float w, float g0, float& m, float& v) {
+__device__ __forceinline__ float adam_one(const AdamArgs& a, uint64_t k, float w, float g0,
+                                          float& m, float& v) {
     const float g = g0 * a.gscale + a.l2 * w;
     m = a.b1 * m + (1.0f - a.b1) * g;
     v = a.b2 * v + (1.0f - a.b2) * g * g;
-    return w - __fdividef(a.lr * (m * a.inv_c1), sqrtf(v * a.inv_c2) + a.eps);
+    const float lr = k < a.rrs_first ? a.lr : a.lr_rrs;
+    return w - __fdividef(lr * (m * a.inv_c1), sqrtf(v * a.inv_c2) + a.eps);
 }
 
 // HBM-bound (30 B per parameter): four parameters per thread with 16-byte loads and stores of
@@ -618,10 +621,10 @@ __global__ void k_adam(const __grid_constant__ AdamArgs a) {
         float4 m = *reinterpret_cast<const float4*>(a.m + k);
         float4 v = *reinterpret_cast<const float4*>(a.v + k);
         float4 nw;
-        nw.x = adam_one(a, w.x, g.x, m.x, v.x);
-        nw.y = adam_one(a, w.y, g.y, m.y, v.y);
-        nw.z = adam_one(a, w.z, g.z, m.z, v.z);
-        nw.w = adam_one(a, w.w, g.w, m.w, v.w);
+        nw.x = adam_one(a, k, w.x, g.x, m.x, v.x);
+        nw.y = adam_one(a, k + 1, w.y, g.y, m.y, v.y);
+        nw.z = adam_one(a, k + 2, w.z, g.z, m.z, v.z);
+        nw.w = adam_one(a, k + 3, w.w, g.w, m.w, v.w);
         *reinterpret_cast<float4*>(a.m + k) = m;
         *reinterpret_cast<float4*>(a.v + k) = v;
         *reinterpret_cast<float4*>(a.p + k) = nw;
@@ -640,7 +643,7 @@ __global__ void k_adam(const __grid_constant__ AdamArgs a) {
     for (uint64_t k = a.first + 4 * quads + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
          k < a.first + a.count; k += (uint64_t)gridDim.x * blockDim.x) {
         float m = a.m[k], v = a.v[k];
-        const float nw = adam_one(a, a.p[k], a.g[k], m, v);
+        const float nw = adam_one(a, k, a.p[k], a.g[k], m, v);
         a.m[k] = m;
         a.v[k] = v;
         a.p[k] = nw;
@@ -740,6 +743,8 @@ cudaError_t launch_adam_step(nrrs_ctx* ctx, bool train_rrs, cudaStream_t s, floa
     ad.first = 0;
     ad.count = ctx->n_table + ctx->n_stat + (train_rrs ? ctx->n_rrs : 0);
     ad.lr = c.lr;
+    ad.rrs_first = ctx->n_table + ctx->n_stat;
+    ad.lr_rrs = c.lr_rrsnet > 0.f ? c.lr_rrsnet : c.lr;
     ad.b1 = c.beta1;
     ad.b2 = c.beta2;
     ad.eps = c.eps;

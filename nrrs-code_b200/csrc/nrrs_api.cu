@@ -430,6 +430,7 @@ void nrrs_config_reference_network(nrrs_config* c) {
     c->eps = 1e-15f;
     c->l2_reg = 3e-6f;
     c->ema_decay = 0.95f;   // "otype": "Ema", "decay": 0.95
+    c->lr_rrsnet = 5e-4f;   // level1 (RRSNet) Adam
 }
 
 void nrrs_decide_params_default(nrrs_decide_params* p) {
@@ -508,6 +509,8 @@ int nrrs_create(const nrrs_config* cfg, nrrs_ctx** out) {
         return fail(nullptr, NRRS_ERR_INVALID_ARG, "max_queue and max_train must be > 0");
     if (!(c.ema_decay >= 0.f && c.ema_decay < 1.f))
         return fail(nullptr, NRRS_ERR_INVALID_ARG, "ema_decay must be in [0, 1)");
+    if (!(c.lr_rrsnet >= 0.f) || !std::isfinite(c.lr_rrsnet))
+        return fail(nullptr, NRRS_ERR_INVALID_ARG, "lr_rrsnet must be finite and >= 0");
     if (!nrrs_device_available())
         return fail(nullptr, NRRS_ERR_NO_DEVICE, "no sm_100 CUDA device (this library has no CPU path)");
 

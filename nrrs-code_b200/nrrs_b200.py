@@ -51,7 +51,7 @@ class Config(C.Structure):
         ("loss_clamp_max", C.c_float), ("cost_offset", C.c_float),
         ("normalize_pos", C.c_int32), ("aabb_min", C.c_float * 3), ("aabb_max", C.c_float * 3),
         ("max_queue", C.c_uint32), ("max_train", C.c_uint32), ("step", C.c_int32),
-        ("network", C.c_int32), ("ema_decay", C.c_float),
+        ("network", C.c_int32), ("ema_decay", C.c_float), ("lr_rrsnet", C.c_float),
     ]
 
 

@@ -393,17 +393,22 @@ static uint64_t decide_core(const float* rrs, const float* rnd, const uint32_t* 
 }
 
 /* Adam (Kingma & Ba 2015) in FP32 with an optional L2 term added to the gradient */
+/* The RRSNet parameters use lr_rrsnet when it is set (the reference's level1 optimizer). */
 void oracle_adam_f32(const nrrs_config* cfg, float* params, const float* grads, float* m,
                      float* v, uint64_t first, uint64_t count, uint64_t t) {
     const float b1 = cfg->beta1, b2 = cfg->beta2;
     const float c1 = 1.0f - powf(b1, (float)t), c2 = 1.0f - powf(b2, (float)t);
+    uint64_t n_table = 0, n_stat = 0;
+    oracle_param_count(cfg, &n_table, &n_stat, NULL);
+    const int64_t rrs_first = (int64_t)(n_table + n_stat);
+    const float lr_rrs = cfg->lr_rrsnet > 0.f ? cfg->lr_rrsnet : cfg->lr;
 #pragma omp parallel for schedule(static)
     for (int64_t k = (int64_t)first; k < (int64_t)(first + count); ++k) {
         const float g = grads[k] + cfg->l2_reg * params[k];
         m[k] = b1 * m[k] + (1.0f - b1) * g;
         v[k] = b2 * v[k] + (1.0f - b2) * g * g;
         const float mh = m[k] / c1, vh = v[k] / c2;
-        params[k] -= cfg->lr * mh / (sqrtf(vh) + cfg->eps);
+        params[k] -= (k < rrs_first ? cfg->lr : lr_rrs) * mh / (sqrtf(vh) + cfg->eps);
     }
 }
 

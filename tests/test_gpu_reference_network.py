@@ -163,3 +163,35 @@ def test_mixed_context_trains_on_the_fp32_kernels():
     assert loss.cpu().numpy() == pytest.approx(l64, rel=1e-4)
     assert np.linalg.norm(g - g64) / np.linalg.norm(g64) < 5e-4
     net.close()
+
+
+def test_adam_step_uses_the_per_network_learning_rates():
+    """the shipped settings train the encoding and StatNet with lr 5e-3 and RRSNet with 5e-4
+    (2net-simple.json level0 / level1): one step of the GPU equals the oracle's Adam on the
+    GPU's own gradients, and the first step moves each parameter by its network's lr"""
+    torch = torch_cuda()
+    net = ref_net(precision=nb.PREC_FP32, max_train=1 << 14, log2_hashmap_size=16)
+    cfg = net.config
+    assert cfg.lr == pytest.approx(5e-3) and cfg.lr_rrsnet == pytest.approx(5e-4)
+    p0 = ref_params(net, 90)
+    n = 5000
+    v = nb.synth(91, n)
+    d = upload(v)
+    loss = torch.zeros(2, dtype=torch.float64, device="cuda")
+    net.train(soa(d), d["target"], n, loss, stream())
+    torch.cuda.synchronize()
+    g = net.get_grads()
+    p1 = net.get_params()
+    pe = p0.copy()
+    m = np.zeros_like(pe)
+    vv = np.zeros_like(pe)
+    O.adam(cfg, pe, g, m, vv, 1)
+    assert np.allclose(p1, pe, rtol=1e-5, atol=1e-7)
+    ntab, nst, nrr = net.param_layout()
+    moved = np.abs(p1 - p0)
+    big = np.abs(g) > 1e-6     # away from the eps and l2 corners of the first step
+    st = slice(ntab, ntab + nst)
+    rr = slice(ntab + nst, ntab + nst + nrr)
+    assert np.allclose(moved[st][big[st]], 5e-3, rtol=2e-2)
+    assert np.allclose(moved[rr][big[rr]], 5e-4, rtol=2e-2)
+    net.close()

@@ -315,6 +315,24 @@ def test_adam_matches_textbook():
     assert np.allclose(p0 - p, 1e-2 * np.sign(g) + 1e-2 * mh / np.sqrt(vh), rtol=1e-5)
 
 
+def test_adam_rrsnet_learning_rate():
+    """lr_rrsnet applies from the first RRSNet parameter on; lr to the table and StatNet"""
+    cfg = O.reference_config(max_train=1 << 12, log2_hashmap_size=12)
+    npar, ntab, nst, nrr = O.param_count(cfg)
+    rng = np.random.default_rng(9)
+    p = rng.standard_normal(npar).astype(np.float32)
+    g = rng.standard_normal(npar).astype(np.float32)
+    m = np.zeros_like(p)
+    v = np.zeros_like(p)
+    p0 = p.copy()
+    O.adam(cfg, p, g, m, v, 1)
+    step = np.abs(p0 - p)
+    # first step: lr x (g + l2 w) / |g + l2 w|, i.e. lr up to eps (and up to the float32
+    # rounding of p0 - p for parameters of size ~1)
+    assert np.allclose(step[:ntab + nst], 5e-3, rtol=1e-3)
+    assert np.allclose(step[ntab + nst:], 5e-4, rtol=1e-3)
+
+
 def test_oracle_defaults_and_generator_agree_with_library():
     """The CPU baseline builds its configuration and inputs from oracle/ alone; they must be the
     library's own defaults and generator output."""
