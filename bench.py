@@ -199,15 +199,17 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def config_fields(precision: str, wl: dict, max_queue: int, max_train: int) -> dict:
+def config_fields(precision: str, wl: dict, max_queue: int, max_train: int,
+                  sum_shards: int = 0) -> dict:
     return dict(precision=PREC[precision], max_queue=max_queue, max_train=max_train,
                 statnet_width=wl["width"], statnet_hidden=wl["hidden"],
                 rrsnet_width=wl["width"], rrsnet_hidden=wl["hidden"],
-                log2_hashmap_size=wl["log2_table"])
+                log2_hashmap_size=wl["log2_table"], sum_shards=sum_shards)
 
 
-def make_config(precision: str, wl: dict, max_queue: int, max_train: int):
-    return load_product().default_config(**config_fields(precision, wl, max_queue, max_train))
+def make_config(precision: str, wl: dict, max_queue: int, max_train: int, sum_shards: int = 0):
+    return load_product().default_config(**config_fields(precision, wl, max_queue, max_train,
+                                                         sum_shards))
 
 
 def do_train_of(args, wl):
@@ -451,7 +453,8 @@ class FrameArm:
         self.B, self.N = wl["bounces"], wl["n_vert"]
         self.precision = precision
         self.dev_b, self.td, self.train = dev_b, td, train
-        self.net = nb.NRRSNetwork(make_config(precision, wl, self.N, wl["train_batch"]))
+        self.net = nb.NRRSNetwork(make_config(precision, wl, self.N, wl["train_batch"],
+                                              world if sharded else 0))
         if not cell_image and self.net.cell_image():
             self.net.set_cell_image(False)
         self.tune = None

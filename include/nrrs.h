@@ -122,6 +122,11 @@ typedef struct {
      * its two networks with separate optimizers (2net-simple.json level0 lr 5e-3 for the
      * encoding and StatNet, level1 lr 5e-4 for RRSNet). */
     float lr_rrsnet;
+    /* Contexts whose exact normalisation sums are added together (sharded queues:
+     * nrrs_infer_accumulate on every rank, then an integer all-reduce). The fixed-point shift
+     * leaves room for sum_shards x max_queue terms, so the added sum cannot overflow; give
+     * every rank the same value. 0 or 1 = one context. */
+    uint32_t sum_shards;
 } nrrs_config;
 
 /* The two network families.
@@ -294,8 +299,9 @@ int nrrs_step_batched_dev(nrrs_ctx* ctx, const nrrs_vertex_soa* v, const float* 
  *      single GPU processing the concatenated queue:
  *        *sum = 0; nrrs_infer_accumulate(shard, sum); allreduce_sum_int64(sum);
  *        nrrs_decide_emit_with_sum(shard, global budget, global n_specular, sum)
- *      sum_acc_dev is a caller-owned int64 on the device; the shift is fixed by max_queue, so all
- *      ranks must use the same max_queue and decision parameters. ---- */
+ *      sum_acc_dev is a caller-owned int64 on the device; the shift is fixed by max_queue and
+ *      sum_shards, so all ranks must use the same max_queue, sum_shards (at least the number of
+ *      ranks) and decision parameters. ---- */
 int nrrs_infer_accumulate(nrrs_ctx* ctx, const nrrs_vertex_soa* v, uint32_t n,
                           const nrrs_decide_params* p, float* stats, float* rrs,
                           int64_t* sum_acc_dev, void* stream);

@@ -54,8 +54,12 @@ __device__ __forceinline__ unsigned split_count(float r, float rnd, unsigned* fl
     return (unsigned)s;
 }
 
+// queue entries of one chunk staged in shared memory (E[s] is about 1: 2,048 per chunk)
+constexpr unsigned kDecStage = 4096;
+
 __global__ void __launch_bounds__(kDecThreads) k_decide(const __grid_constant__ DecideArgs a) {
     __shared__ unsigned s_chunk, s_epoch, s_prefix;
+    __shared__ uint32_t s_stage[kDecStage];
     __shared__ unsigned s_warp[kDecThreads / 32];
     const int tid = threadIdx.x;
     if (tid == 0) {
@@ -237,14 +241,32 @@ __global__ void __launch_bounds__(kDecThreads) k_decide(const __grid_constant__ 
         }
         __syncthreads();
 
-        // emission: s copies of stid, vertex order, capacity-guarded
-        unsigned pos = s_prefix + thread_excl;
-        uint32_t* q = a.queue + sg.queue_offset;
+        // emission: s copies of stid, vertex order, capacity-guarded. The chunk's entries are
+        // one contiguous range of the queue; staged in shared memory, they go out in coalesced
+        // stores (written straight from each thread's runs, a warp's stores touched a sector per
+        // entry). A chunk with more entries than the stage holds writes them directly.
+        // room: queue slots left from the chunk's first entry (0 when the prefix is past the
+        // capacity, including a saturated prefix)
+        uint32_t* q = a.queue + sg.queue_offset + s_prefix;
+        const unsigned room = s_prefix < sg.queue_capacity ? sg.queue_capacity - s_prefix : 0u;
+        if (chunk_total <= kDecStage) {
+            unsigned pos = thread_excl;
 #pragma unroll
-        for (int j = 0; j < kDecVPT; ++j) {
-            for (unsigned k = 0; k < sv[j]; ++k, ++pos) {
-                if (pos < sg.queue_capacity) q[pos] = st[j];
+            for (int j = 0; j < kDecVPT; ++j)
+                for (unsigned k = 0; k < sv[j]; ++k, ++pos) s_stage[pos] = st[j];
+            __syncthreads();
+            for (unsigned e = tid; e < chunk_total; e += kDecThreads) {
+                if (e < room) q[e] = s_stage[e];
                 else flags |= NRRS_DEV_OVERFLOW;
+            }
+        } else {
+            unsigned pos = thread_excl;
+#pragma unroll
+            for (int j = 0; j < kDecVPT; ++j) {
+                for (unsigned k = 0; k < sv[j]; ++k, ++pos) {
+                    if (pos < room) q[pos] = st[j];
+                    else flags |= NRRS_DEV_OVERFLOW;
+                }
             }
         }
     }

@@ -79,8 +79,13 @@ uint64_t mlp_params(int in, int w, int h, int out) {
 
 // The shift depends only on the context capacity and the clamp, so a depth gives the same
 // decisions whether it runs alone, batched, or sharded.
+// the terms an exact sum can hold: max_queue per context, times the contexts added together
+uint64_t sum_capacity(const nrrs_ctx* ctx) {
+    return (uint64_t)ctx->cfg.max_queue * (ctx->cfg.sum_shards > 1 ? ctx->cfg.sum_shards : 1u);
+}
+
 FactorParams factor_params(const nrrs_ctx* ctx, const nrrs_decide_params* p) {
-    const uint64_t n = ctx->cfg.max_queue;
+    const uint64_t n = sum_capacity(ctx);
     FactorParams f{};
     f.clamp_min = p->clamp_min;
     f.clamp_max = p->clamp_max;
@@ -102,7 +107,7 @@ int check_decide_params(nrrs_ctx* ctx, const nrrs_decide_params* p, uint64_t n_t
     if (p->factor_source != NRRS_FACTOR_ADRRS && p->factor_source != NRRS_FACTOR_RRSNET)
         return fail(ctx, NRRS_ERR_INVALID_ARG, "factor_source must be 2 (ADRRS) or 3 (RRSNet)");
     (void)n_total;
-    if (sum_shift(ctx->cfg.max_queue, p->use_ceil ? ceilf(p->clamp_max) : p->clamp_max) < 16)
+    if (sum_shift(sum_capacity(ctx), p->use_ceil ? ceilf(p->clamp_max) : p->clamp_max) < 16)
         return fail(ctx, NRRS_ERR_UNSUPPORTED, "n * clamp_max too large for the exact sum");
     return NRRS_OK;
 }

@@ -52,6 +52,7 @@ class Config(C.Structure):
         ("normalize_pos", C.c_int32), ("aabb_min", C.c_float * 3), ("aabb_max", C.c_float * 3),
         ("max_queue", C.c_uint32), ("max_train", C.c_uint32), ("step", C.c_int32),
         ("network", C.c_int32), ("ema_decay", C.c_float), ("lr_rrsnet", C.c_float),
+        ("sum_shards", C.c_uint32),
     ]
 
 

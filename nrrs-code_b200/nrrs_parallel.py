@@ -9,6 +9,9 @@ union of the per-rank queues is bit-identical to what one GPU emits for the whol
 keeps its own next-bounce queue (the next bounce is sharded the same way); `queue_offsets` gives
 the global position of each rank's queue when a caller wants one concatenated queue.
 
+Every rank's context is created with the same max_queue and with sum_shards at least the world
+size, so that the fixed-point shift leaves room for the terms of all shards.
+
 Training is data-parallel: per-rank gradients (nrrs_train_grads), an all-reduce of the
 gradient vector, and Adam on the mean (nrrs_adam_apply with scale 1/world).
 
@@ -27,6 +30,11 @@ class ShardedNRRS:
         self.group = group
         self.rank = dist.get_rank(group) if dist.is_initialized() else 0
         self.world = dist.get_world_size(group) if dist.is_initialized() else 1
+        # the all-reduced exact sum holds world x max_queue terms: the contexts must leave room
+        cfg = getattr(backend, "config", None)
+        if cfg is not None and self.world > 1 and max(int(cfg.sum_shards), 1) < self.world:
+            raise ValueError(f"create the contexts with sum_shards >= {self.world} (the world "
+                             f"size): the all-reduced exact sum adds that many shards")
 
     def _allreduce(self, t):
         if self.world > 1:

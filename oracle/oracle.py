@@ -190,7 +190,7 @@ _CONFIG_DEFAULTS = dict(
     rrsnet_hidden=2, precision=0, seed=0, table_init_scale=1e-4, lr=1e-2, beta1=0.9, beta2=0.99,
     eps=1e-15, l2_reg=0.0, stat_eps=0.01, ref_eps=0.01, loss_clamp_max=10.0, cost_offset=1.0,
     normalize_pos=0, aabb_min=(0.0, 0.0, 0.0), aabb_max=(1.0, 1.0, 1.0), max_queue=1 << 20,
-    max_train=1 << 18, step=3, network=0, ema_decay=0.0, lr_rrsnet=0.0)
+    max_train=1 << 18, step=3, network=0, ema_decay=0.0, lr_rrsnet=0.0, sum_shards=0)
 _DECIDE_DEFAULTS = dict(clamp_min=0.05, clamp_max=8.0, normalize_rate=0.85, use_ceil=1,
                         scale_up=0, use_weight_window=0, weight_window_size=5.0,
                         factor_source=nb.FACTOR_RRSNET)

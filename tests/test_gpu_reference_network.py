@@ -195,3 +195,52 @@ def test_adam_step_uses_the_per_network_learning_rates():
     assert np.allclose(moved[st][big[st]], 5e-3, rtol=2e-2)
     assert np.allclose(moved[rr][big[rr]], 5e-4, rtol=2e-2)
     net.close()
+
+
+def test_weighted_training_step_batch_vs_fp64_oracle():
+    """nrrs_train_step_batch on the shipped network with every per-sample side array, the error
+    sum and the shipped gammas: losses and gradients against the FP64 oracle's weighted losses
+    (FP32 kernels, the reference network's relative L2 StatNet loss)"""
+    torch = torch_cuda()
+    net = ref_net(precision=nb.PREC_FP32, max_train=1 << 14, log2_hashmap_size=16)
+    p0 = ref_params(net, 92)
+    n = 6000
+    v = nb.synth(93, n)
+    rng = np.random.default_rng(94)
+    rt = rng.uniform(0.1, 3.0, n).astype(np.float32)
+    rt[rng.random(n) < 0.25] = -1.0
+    extra = {"rrs_target": rt, "error": rng.uniform(0.0, 4.0, n).astype(np.float32),
+             "error_for_avg": rng.uniform(0.0, 6.0, n).astype(np.float32),
+             "number_samples": rng.integers(0, 9, n).astype(np.float32)}
+    sw = rng.uniform(0.1, 1.0, n).astype(np.float32)
+    d = upload(v)
+    b = {k: d[k] for k in ("pos", "wi", "normal", "roughness", "albedo", "thp", "depth",
+                           "ref_mean", "target")}
+    for k, a in extra.items():
+        b[k] = torch.from_numpy(a).cuda()
+    n_pix = 1500
+    esum = 2.5 * n_pix
+    d_esum = torch.tensor([esum], dtype=torch.float32, device="cuda")
+    lp = nb.default_loss_params(gamma1=0.01, gamma2=0.05, gamma3=0.0, gamma4=0.01, clamp_on=1,
+                                clamp_max=10.0, n_pixels=n_pix)
+    loss = torch.zeros(2, dtype=torch.float64, device="cuda")
+    net.trainStepBatch(nb.train_batch(**b), n, torch.from_numpy(sw).cuda(), d_esum, lp, loss,
+                       stream())
+    torch.cuda.synchronize()
+    g = net.get_grads().astype(np.float64)
+    ov = dict(v)
+    ov.update(extra)
+    ov["sample_weight"] = sw
+    w, _ = O.loss_weights(ov, gammas=(0.01, 0.05, 0.0, 0.01), clamp_on=1, clamp_max=10.0,
+                          error_mean=esum / n_pix)
+    g64, l64 = O.train_grads(net.config, p0, v, v["target"], "f64", weights=w)
+    lo = loss.cpu().numpy()
+    assert lo[0] == pytest.approx(l64[0], rel=1e-4)
+    assert lo[1] == pytest.approx(l64[1], rel=1e-4)
+    ntab, nst, nrr = net.param_layout()
+    for name, sl in (("table", slice(0, ntab)), ("statnet", slice(ntab, ntab + nst)),
+                     ("rrsnet", slice(ntab + nst, ntab + nst + nrr))):
+        e = np.linalg.norm(g[sl] - g64[sl]) / max(np.linalg.norm(g64[sl]), 1e-30)
+        assert e < 5e-4, (name, e)
+    assert net.device_status(stream()) == (nb.OK, 0)
+    net.close()

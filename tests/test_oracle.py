@@ -376,9 +376,11 @@ def test_weighted_losses_default_equal_plain_losses():
                        rtol=1e-13)
 
 
-def test_weighted_losses_fd_gradients_fp64():
-    """central finite differences (h = 1e-3, FP64) of the weighted losses on 256 parameters"""
-    cfg = small_cfg(step=3)
+@pytest.mark.parametrize("family", ["workload", "reference"])
+def test_weighted_losses_fd_gradients_fp64(family):
+    """central finite differences (h = 1e-3, FP64) of the weighted losses on 256 parameters, for
+    both network families"""
+    cfg = small_cfg(step=3) if family == "workload" else ref_cfg(step=3)
     n = 96
     v = nb.synth(6, n)
     tgt = v["target"]
