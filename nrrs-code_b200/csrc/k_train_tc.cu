@@ -91,66 +91,96 @@ __device__ __forceinline__ double block_sum_d(double v, double* red) {
     __syncthreads();
     double t = 0.0;
     if (threadIdx.x == 0)
-        for (int k = 0; k < 4; ++k) t += red[k];
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += red[k];
     return t;
+}
+
+// named barrier of one warpgroup (id 0 is __syncthreads)
+__device__ __forceinline__ void wg_bar(int wg) {
+    asm volatile("bar.sync %0, 128;" ::"r"(1 + wg) : "memory");
+}
+// sync_for_mma for the 128 threads of one warpgroup
+__device__ __forceinline__ void sync_for_mma_wg(int wg) {
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    wg_bar(wg);
 }
 
 // ---------------------------------------------------------------------------------------------
 // Shared-memory plan of the StatNet kernel: the forward weight images (the backward reads them
-// as MN-major operands, i.e. transposed), two [128 x W] tiles that take turns as the input tile,
-// activations and deltas, and the two 16-wide tiles. The ReLU masks live in registers: row m of
-// every tile is produced and consumed by thread m.
-template <int W, int H>
+// as MN-major operands, i.e. transposed), then per warpgroup two [128 x W] tiles that take turns
+// as the input tile, activations and deltas, and the two 16-wide tiles. The ReLU masks live in
+// registers: row m of every tile is produced and consumed by thread m of the warpgroup.
+//
+// WGS warpgroups share one copy of the weights, each running its own 128-sample tiles with its
+// own tiles, TMEM columns, mbarriers and named barrier, so that one warpgroup's MMAs run while
+// another waits on its epilogue or its stores. With two warpgroups of the 128-wide networks the
+// 16-wide tiles live in the first 8 KB of tile buffer (H + 1) % 2 (which then holds h[H-2],
+// already stored), so the plan fits one SM.
+template <int W, int H, int WGS>
 struct StatSmem {
+    static constexpr bool kAlias = WGS > 1;
     static constexpr uint32_t kFwd = 2u * (W * kStatIn + (H - 1) * W * W + 16 * W);
     static constexpr uint32_t kW = (kFwd + 1023u) / 1024u * 1024u;
     static constexpr uint32_t kTileW = 128u * W * 2u;   // one [128 x W] tile
-    static constexpr uint32_t kB0 = kW;
-    static constexpr uint32_t kB1 = kB0 + kTileW;
-    static constexpr uint32_t kDY = kB1 + kTileW;
-    static constexpr uint32_t kX1 = kDY + 128u * 16u * 2u;
-    static constexpr uint32_t kBar = kX1 + 128u * 16u * 2u;
-    static constexpr size_t kSmem = 1024 + kBar + 64;
+    static constexpr uint32_t kT16 = 128u * 16u * 2u;   // one [128 x 16] tile
+    static constexpr uint32_t kPerWg = 2u * kTileW + (kAlias ? 0u : 2u * kT16);
+    static constexpr uint32_t kBar = kW + WGS * kPerWg;
+    static constexpr uint32_t kNumBars = 1 + 2 * WGS;  // weights, then (mma, x0 tile) per warpgroup
+    static constexpr size_t kSmem = 1024 + kBar + 8 * kNumBars + 16;
+    static_assert(kSmem <= 232448u, "StatNet training plan exceeds shared memory");
+    __device__ static uint8_t* buf(uint8_t* base, int wg, int b) {
+        return base + kW + (uint32_t)wg * kPerWg + (uint32_t)b * kTileW;
+    }
+    __device__ static uint8_t* dy(uint8_t* base, int wg) {
+        return kAlias ? buf(base, wg, (H + 1) % 2) : buf(base, wg, 2);
+    }
+    __device__ static uint8_t* x1(uint8_t* base, int wg) { return dy(base, wg) + kT16; }
 };
 
 // Layer h's activations go to buffer (h + 1) % 2 (buffer 0 first holds the input tile), its
-// deltas to buffer h % 2. Before an epilogue overwrites a buffer, thread 0 waits until the bulk
-// store that last read it has finished: the counts below are the bulk groups committed since.
-template <int W, int H>
-__global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcTrainArgs a) {
+// deltas to buffer h % 2. Before an epilogue overwrites a buffer, thread 0 of the warpgroup
+// waits until the bulk store that last read it has finished: the counts below are the bulk
+// groups it committed since (bulk groups are per thread, so the warpgroups do not see each
+// other's).
+template <int W, int H, int WGS>
+__global__ void __launch_bounds__(128 * WGS, 1) k_ttc_stat(const __grid_constant__ TcTrainArgs a) {
     static_assert((W == 64 || W == 128) && (H == 2 || H == 3), "tensor-core training shapes");
-    using S = StatSmem<W, H>;
+    static_assert(WGS == 1 || WGS == 2, "one or two warpgroups");
+    using S = StatSmem<W, H, WGS>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023u) &
                                                ~uintptr_t(1023));
+    const int wg = (int)(threadIdx.x >> 7);
+    const int tid = (int)(threadIdx.x & 127), warp = tid >> 5;  // row and lane quarter in the warpgroup
     uint8_t* sW = base;
-    uint8_t* sB[2] = {base + S::kB0, base + S::kB1};
-    uint8_t* sDY = base + S::kDY;
-    uint8_t* sX1 = base + S::kX1;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(base + S::kBar);  // weights, mma, x0 tile
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 3);
-    __shared__ int s_abort;
-    __shared__ double red[4];
-    const int tid = threadIdx.x, warp = tid >> 5;
+    uint8_t* sB[2] = {S::buf(base, wg, 0), S::buf(base, wg, 1)};
+    uint8_t* sDY = S::dy(base, wg);
+    uint8_t* sX1 = S::x1(base, wg);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(base + S::kBar);
+    uint64_t* bar_mma = &bars[1 + 2 * wg];
+    uint64_t* bar_x0 = &bars[2 + 2 * wg];
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + S::kNumBars);
+    __shared__ int s_abort[WGS];
+    __shared__ double red[4 * WGS];
 
-    if (tid == 0) {
-        tc::mbar_init(&bars[0], 1);
-        tc::mbar_init(&bars[1], 1);
-        tc::mbar_init(&bars[2], 1);
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < (int)S::kNumBars; ++k) tc::mbar_init(&bars[k], 1);
         tc::fence_mbar_init();
-        s_abort = 0;
+        for (int k = 0; k < WGS; ++k) s_abort[k] = 0;
     }
-    if (warp == 0) {
-        tc::tmem_alloc(tslot, W);
+    if (threadIdx.x < 32) {
+        tc::tmem_alloc(tslot, W * WGS);
         tc::tmem_relinquish();
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    const uint32_t tmem = *tslot;
-    if (!load_weights(sW, a.tpack, S::kFwd, &bars[0], tid)) s_abort = 1;
+    const uint32_t tmem = *tslot + (uint32_t)(wg * W);
+    if (!load_weights(sW, a.tpack, S::kFwd, &bars[0], threadIdx.x))
+        for (int k = 0; k < WGS; ++k) s_abort[k] = 1;
     __syncthreads();
-    unsigned flags = s_abort ? NRRS_DEV_TIMEOUT : 0u;
+    unsigned flags = s_abort[wg] ? NRRS_DEV_TIMEOUT : 0u;
     uint32_t phase = 0, xphase = 0;
     const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
 
@@ -164,9 +194,9 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
     double lossS = 0.0;
     const __half2* table = reinterpret_cast<const __half2*>(a.table_h);
     const uint32_t tiles = (a.n + 127) / 128;
-    for (uint32_t t = blockIdx.x; t < tiles && !flags; t += gridDim.x) {
+    for (uint32_t t = blockIdx.x * WGS + wg; t < tiles && !flags; t += gridDim.x * WGS) {
         if (tid == 0) tc::bulk_wait_read();  // the previous tile's stores have left smem
-        __syncthreads();
+        wg_bar(wg);
         const uint32_t i = t * 128 + tid;
         const bool valid = i < a.n;
         float p[3] = {0.f, 0.f, 0.f};
@@ -174,8 +204,8 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
         if (a.pre) {
             // hash columns from k_encode_levels: bring the tile in, add the SH and misc lanes
             if (tid == 0) {
-                tc::mbar_arrive_expect_tx(&bars[2], 128u * 64u * 2u);
-                tc::bulk_g2s(sB[0], tile_ptr(a.act, a.x0, t), 128u * 64u * 2u, &bars[2]);
+                tc::mbar_arrive_expect_tx(bar_x0, 128u * 64u * 2u);
+                tc::bulk_g2s(sB[0], tile_ptr(a.act, a.x0, t), 128u * 64u * 2u, bar_x0);
             }
             float sh[16], misc[16];
             if (valid) {
@@ -184,7 +214,7 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
                 misc_lanes(a.v, i, misc);
                 if (!a.dxs) norm_pos(a.enc, a.v.pos, i, p);  // for the in-kernel scatter
             }
-            ok = tc::mbar_wait(&bars[2], xphase, kSpin);
+            ok = tc::mbar_wait(bar_x0, xphase, kSpin);
             xphase ^= 1u;
             if (valid) {
                 store_chunk(sB[0], tid, 4, 64, pack8<false>(sh));
@@ -224,25 +254,25 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
         } else {
             zero_row(sB[0], tid, 64);
         }
-        sync_for_mma();
+        sync_for_mma_wg(wg);
         if (tid == 0) store_tile(tile_ptr(a.act, a.x0, t), sB[0], 128u * 64u * 2u);
 
         // ---- StatNet forward ----
         uint32_t mk[H][W / 32];
-        ok &= mma_layer<kStatIn, W, false>(sB[0], wF[0], tmem, &bars[1], phase, tid);
+        ok &= mma_layer<kStatIn, W, false>(sB[0], wF[0], tmem, bar_mma, phase, tid);
         epilogue_relu_bits<W, false>(trow, sB[1], tid, mk[0]);
-        sync_for_mma();
+        sync_for_mma_wg(wg);
         if (tid == 0) store_tile(tile_ptr(a.act, a.hs[0], t), sB[1], S::kTileW);
 #pragma unroll
         for (int h = 1; h < H; ++h) {
-            ok &= mma_layer<W, W, false>(sB[h % 2], wF[h], tmem, &bars[1], phase, tid);
+            ok &= mma_layer<W, W, false>(sB[h % 2], wF[h], tmem, bar_mma, phase, tid);
             if (tid == 0) tc::bulk_wait_read_n<1>();
-            __syncthreads();
+            wg_bar(wg);
             epilogue_relu_bits<W, false>(trow, sB[(h + 1) % 2], tid, mk[h]);
-            sync_for_mma();
+            sync_for_mma_wg(wg);
             if (tid == 0) store_tile(tile_ptr(a.act, a.hs[h], t), sB[(h + 1) % 2], S::kTileW);
         }
-        ok &= mma_layer<W, 16, false>(sB[H % 2], wF[H], tmem, &bars[1], phase, tid);
+        ok &= mma_layer<W, 16, false>(sB[H % 2], wF[H], tmem, bar_mma, phase, tid);
         float y[16];
         tc::tmem_ld16(trow, y);
         tc::tmem_wait_ld();
@@ -267,43 +297,54 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
             }
             glue16(a.fp, y, a.v, i, x1);
         }
+        if constexpr (S::kAlias) {
+            // the 16-wide tiles overwrite buffer (H + 1) % 2, whose h[H-2] store is the second
+            // most recent bulk group
+            if (tid == 0) tc::bulk_wait_read_n<1>();
+            wg_bar(wg);
+        }
         store_chunk(sDY, tid, 0, 16, pack8<false>(dyv));
         store_chunk(sDY, tid, 1, 16, pack8<false>(dyv + 8));
         store_chunk(sX1, tid, 0, 16, pack8<true>(x1));  // RRSNet input: BF16
         store_chunk(sX1, tid, 1, 16, pack8<true>(x1 + 8));
-        sync_for_mma();
+        sync_for_mma_wg(wg);
         if (tid == 0) {
             store_tile(tile_ptr(a.act, a.dy, t), sDY, 128u * 16u * 2u);
             store_tile(tile_ptr(a.act, a.x1, t), sX1, 128u * 16u * 2u);
         }
 
         // ---- backward: delta of layer h -> buffer h % 2 ----
-        ok &= mma_layer_t<16, W, W, false>(sDY, wF[H], tmem, &bars[1], phase, tid);
-        if (tid == 0) tc::bulk_wait_read_n<3>();  // since: h[H-1], dy, x1
-        __syncthreads();
+        ok &= mma_layer_t<16, W, W, false>(sDY, wF[H], tmem, bar_mma, phase, tid);
+        if (tid == 0) {
+            // the first delta goes to buffer (H - 1) % 2: with the 16-wide tiles inside it, the
+            // dy and x1 stores must have left it as well
+            if constexpr (S::kAlias) tc::bulk_wait_read();
+            else tc::bulk_wait_read_n<3>();  // since: h[H-1], dy, x1
+        }
+        wg_bar(wg);
         epilogue_mask_bits<W, false>(trow, mk[H - 1], sB[(H - 1) % 2], tid);
-        sync_for_mma();
+        sync_for_mma_wg(wg);
         if (tid == 0) store_tile(tile_ptr(a.act, a.dhs[H - 1], t), sB[(H - 1) % 2], S::kTileW);
 #pragma unroll
         for (int h = H - 1; h >= 1; --h) {
-            ok &= mma_layer_t<W, W, W, false>(sB[h % 2], wF[h], tmem, &bars[1], phase, tid);
+            ok &= mma_layer_t<W, W, W, false>(sB[h % 2], wF[h], tmem, bar_mma, phase, tid);
             if (tid == 0) {
                 if (h == H - 1) tc::bulk_wait_read_n<3>();  // since: dy, x1, d[H-1]
                 else tc::bulk_wait_read_n<1>();             // since: d[h]
             }
-            __syncthreads();
+            wg_bar(wg);
             epilogue_mask_bits<W, false>(trow, mk[h - 1], sB[(h - 1) % 2], tid);
-            sync_for_mma();
+            sync_for_mma_wg(wg);
             if (tid == 0) store_tile(tile_ptr(a.act, a.dhs[h - 1], t), sB[(h - 1) % 2], S::kTileW);
         }
         // input gradient of the 32 hash lanes (per sample; 1/n applied below)
-        ok &= mma_layer_t<W, 32, kStatIn, false>(sB[0], wF[0], tmem, &bars[1], phase, tid);
+        ok &= mma_layer_t<W, 32, kStatIn, false>(sB[0], wF[0], tmem, bar_mma, phase, tid);
         float dx[32];
         tc::tmem_ld16(trow, dx);
         tc::tmem_ld16(trow + 16, dx + 16);
         tc::tmem_wait_ld();
         tc::fence_before_sync();
-        __syncthreads();  // TMEM free for the next tile
+        wg_bar(wg);  // TMEM free for the next tile
         if (valid && a.dxs) {
             // the level-major scatter kernel applies them; stored level-major ([16][n] pairs),
             // so that kernel reads each level's gradients coalesced
@@ -320,20 +361,18 @@ __global__ void __launch_bounds__(128, 1) k_ttc_stat(const __grid_constant__ TcT
                                    dx[2 * l + 1] * a.inv_n, lanes);
             }
         }
-        if (!ok) s_abort = 1;
-        __syncthreads();
-        if (s_abort) flags |= NRRS_DEV_TIMEOUT;
+        if (!ok) s_abort[wg] = 1;
+        wg_bar(wg);
+        if (s_abort[wg]) flags |= NRRS_DEV_TIMEOUT;
     }
     const double s0 = block_sum_d(lossS, red);
-    if (tid == 0) {
-        a.part[4 * blockIdx.x + 0] = s0;
-        tc::bulk_wait_all();
-    }
+    if (threadIdx.x == 0) a.part[4 * blockIdx.x + 0] = s0;
+    if (tid == 0) tc::bulk_wait_all();
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) {
+    if (threadIdx.x < 32) {
         tc::fence_after_sync();
-        tc::tmem_dealloc(tmem, W);
+        tc::tmem_dealloc(*tslot, W * WGS);
     }
     (void)flags;
 }
@@ -377,19 +416,25 @@ __global__ void __launch_bounds__(128) k_scatter_levels(const __grid_constant__ 
 }
 
 // ---------------------------------------------------------------------------------------------
-// RRSNet: forward images, the BF16 input tile, two [128 x W] tiles (activations of layer h in
-// buffer h % 2, deltas of layer h in buffer (h + 1) % 2) and the output-delta tile.
-template <int W, int H>
+// RRSNet: forward images, then per warpgroup the BF16 input tile, two [128 x W] tiles
+// (activations of layer h in buffer h % 2, deltas of layer h in buffer (h + 1) % 2) and the
+// output-delta tile. WGS warpgroups share the weights as in the StatNet kernel.
+template <int W, int H, int WGS>
 struct RrsSmem {
     static constexpr uint32_t kFwd = 2u * (W * kRrsIn + (H - 1) * W * W + 16 * W);
     static constexpr uint32_t kW = (kFwd + 1023u) / 1024u * 1024u;
     static constexpr uint32_t kTileW = 128u * W * 2u;
-    static constexpr uint32_t kX1 = kW;
-    static constexpr uint32_t kB0 = kX1 + 128u * 16u * 2u;
-    static constexpr uint32_t kB1 = kB0 + kTileW;
-    static constexpr uint32_t kDR = kB1 + kTileW;
-    static constexpr uint32_t kBar = kDR + 128u * 16u * 2u;
-    static constexpr size_t kSmem = 1024 + kBar + 64;
+    static constexpr uint32_t kT16 = 128u * 16u * 2u;
+    static constexpr uint32_t kPerWg = kT16 + 2u * kTileW + kT16;  // x1, b0, b1, draw
+    static constexpr uint32_t kBar = kW + WGS * kPerWg;
+    static constexpr uint32_t kNumBars = 1 + 2 * WGS;  // weights, then (mma, x1 tile) per warpgroup
+    static constexpr size_t kSmem = 1024 + kBar + 8 * kNumBars + 16;
+    static_assert(kSmem <= 232448u, "RRSNet training plan exceeds shared memory");
+    __device__ static uint8_t* x1(uint8_t* base, int wg) { return base + kW + (uint32_t)wg * kPerWg; }
+    __device__ static uint8_t* buf(uint8_t* base, int wg, int b) {
+        return x1(base, wg) + kT16 + (uint32_t)b * kTileW;
+    }
+    __device__ static uint8_t* dr(uint8_t* base, int wg) { return buf(base, wg, 2); }
 };
 
 __device__ __forceinline__ float rel_contrib_tc(const TcTrainArgs& a, uint32_t i) {
@@ -402,36 +447,38 @@ __device__ __forceinline__ float rel_contrib_tc(const TcTrainArgs& a, uint32_t i
     return r < a.loss_clamp ? r : a.loss_clamp;
 }
 
-template <int W, int H, bool BACKWARD>
-__global__ void __launch_bounds__(128, 1) k_ttc_rrs(const __grid_constant__ TcTrainArgs a) {
+template <int W, int H, int WGS, bool BACKWARD>
+__global__ void __launch_bounds__(128 * WGS, 1) k_ttc_rrs(const __grid_constant__ TcTrainArgs a) {
     static_assert((W == 64 || W == 128) && (H == 2 || H == 3), "tensor-core training shapes");
-    using S = RrsSmem<W, H>;
+    static_assert(WGS == 1 || WGS == 2, "one or two warpgroups");
+    using S = RrsSmem<W, H, WGS>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023u) &
                                                ~uintptr_t(1023));
+    const int wg = (int)(threadIdx.x >> 7);
+    const int tid = (int)(threadIdx.x & 127), warp = tid >> 5;  // row and lane quarter in the warpgroup
     uint8_t* sW = base;
-    uint8_t* sX1 = base + S::kX1;
-    uint8_t* sB[2] = {base + S::kB0, base + S::kB1};
-    uint8_t* sDR = base + S::kDR;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(base + S::kBar);  // weights, mma, x1 load
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 3);
-    __shared__ int s_abort;
-    __shared__ double red[4];
+    uint8_t* sX1 = S::x1(base, wg);
+    uint8_t* sB[2] = {S::buf(base, wg, 0), S::buf(base, wg, 1)};
+    uint8_t* sDR = S::dr(base, wg);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(base + S::kBar);
+    uint64_t* bar_mma = &bars[1 + 2 * wg];
+    uint64_t* bar_x1 = &bars[2 + 2 * wg];
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + S::kNumBars);
+    __shared__ int s_abort[WGS];
+    __shared__ double red[4 * WGS];
     __shared__ double s_tot[4];
-    const int tid = threadIdx.x, warp = tid >> 5;
 
-    if (tid == 0) {
-        tc::mbar_init(&bars[0], 1);
-        tc::mbar_init(&bars[1], 1);
-        tc::mbar_init(&bars[2], 1);
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < (int)S::kNumBars; ++k) tc::mbar_init(&bars[k], 1);
         tc::fence_mbar_init();
-        s_abort = 0;
+        for (int k = 0; k < WGS; ++k) s_abort[k] = 0;
     }
     if (BACKWARD) {
         // batch sums of the loss partials (rows written by the StatNet and forward launches),
         // in a fixed order, so every CTA holds the same V and C
         double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
-        for (uint32_t b = tid; b < a.part_used; b += 128) {
+        for (uint32_t b = threadIdx.x; b < a.part_used; b += blockDim.x) {
             t0 += a.part[4 * b + 0];
             t1 += a.part[4 * b + 1];
             t2 += a.part[4 * b + 2];
@@ -441,9 +488,9 @@ __global__ void __launch_bounds__(128, 1) k_ttc_rrs(const __grid_constant__ TcTr
         t1 = block_sum_d(t1, red);
         t2 = block_sum_d(t2, red);
         t3 = block_sum_d(t3, red);
-        if (tid == 0) s_tot[0] = t0, s_tot[1] = t1, s_tot[2] = t2, s_tot[3] = t3;
+        if (threadIdx.x == 0) s_tot[0] = t0, s_tot[1] = t1, s_tot[2] = t2, s_tot[3] = t3;
         __syncthreads();
-        if (blockIdx.x == 0 && tid == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
             const double Vm = s_tot[1] / (double)a.n, Cm = s_tot[2] / (double)a.n;
             a.loss_out[0] = s_tot[0] / (3.0 * (double)a.n);
             a.loss_out[1] = a.train_rrs ? (a.lw.active ? Vm * Cm + s_tot[3] / (double)a.n : Vm * Cm)
@@ -451,22 +498,23 @@ __global__ void __launch_bounds__(128, 1) k_ttc_rrs(const __grid_constant__ TcTr
         }
         if (!a.train_rrs) return;  // StatNet-only steps: losses are all this launch writes
     }
-    if (warp == 0) {
-        tc::tmem_alloc(tslot, W);
+    if (threadIdx.x < 32) {
+        tc::tmem_alloc(tslot, W * WGS);
         tc::tmem_relinquish();
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    const uint32_t tmem = *tslot;
+    const uint32_t tmem = *tslot + (uint32_t)(wg * W);
     float Vf = 0.f, Cf = 0.f;
     if (BACKWARD) {
         Vf = (float)(s_tot[1] / (double)a.n);
         Cf = (float)(s_tot[2] / (double)a.n);
     }
-    if (!load_weights(sW, a.tpack + a.r_off, S::kFwd, &bars[0], tid)) s_abort = 1;
+    if (!load_weights(sW, a.tpack + a.r_off, S::kFwd, &bars[0], threadIdx.x))
+        for (int k = 0; k < WGS; ++k) s_abort[k] = 1;
     __syncthreads();
-    unsigned flags = s_abort ? NRRS_DEV_TIMEOUT : 0u;
+    unsigned flags = s_abort[wg] ? NRRS_DEV_TIMEOUT : 0u;
     uint32_t phase = 0, xphase = 0;
     const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
     // forward images: [W x 16], (H - 1) x [W x W], [16 x W]
@@ -478,35 +526,35 @@ __global__ void __launch_bounds__(128, 1) k_ttc_rrs(const __grid_constant__ TcTr
 
     double sumV = 0.0, sumC = 0.0, sumR = 0.0;
     const uint32_t tiles = (a.n + 127) / 128;
-    for (uint32_t t = blockIdx.x; t < tiles && !flags; t += gridDim.x) {
+    for (uint32_t t = blockIdx.x * WGS + wg; t < tiles && !flags; t += gridDim.x * WGS) {
         if (tid == 0) {
             tc::bulk_wait_read();
-            tc::mbar_arrive_expect_tx(&bars[2], 128u * 16u * 2u);
-            tc::bulk_g2s(sX1, tile_ptr(a.act, a.x1, t), 128u * 16u * 2u, &bars[2]);
+            tc::mbar_arrive_expect_tx(bar_x1, 128u * 16u * 2u);
+            tc::bulk_g2s(sX1, tile_ptr(a.act, a.x1, t), 128u * 16u * 2u, bar_x1);
         }
-        bool ok = tc::mbar_wait(&bars[2], xphase, kSpin);
+        bool ok = tc::mbar_wait(bar_x1, xphase, kSpin);
         xphase ^= 1u;
-        __syncthreads();
+        wg_bar(wg);
         const uint32_t i = t * 128 + tid;
         const bool valid = i < a.n;
 
         uint32_t mk[H][W / 32];
-        ok &= mma_layer<kRrsIn, W, true>(sX1, wF[0], tmem, &bars[1], phase, tid);
+        ok &= mma_layer<kRrsIn, W, true>(sX1, wF[0], tmem, bar_mma, phase, tid);
         epilogue_relu_bits<W, true>(trow, sB[0], tid, mk[0]);
-        sync_for_mma();
+        sync_for_mma_wg(wg);
         if (BACKWARD && tid == 0) store_tile(tile_ptr(a.act, a.hr[0], t), sB[0], S::kTileW);
 #pragma unroll
         for (int h = 1; h < H; ++h) {
-            ok &= mma_layer<W, W, true>(sB[(h - 1) % 2], wF[h], tmem, &bars[1], phase, tid);
+            ok &= mma_layer<W, W, true>(sB[(h - 1) % 2], wF[h], tmem, bar_mma, phase, tid);
             if (BACKWARD) {
                 if (tid == 0) tc::bulk_wait_read_n<1>();  // since: h[h-1]
-                __syncthreads();
+                wg_bar(wg);
             }
             epilogue_relu_bits<W, true>(trow, sB[h % 2], tid, mk[h]);
-            sync_for_mma();
+            sync_for_mma_wg(wg);
             if (BACKWARD && tid == 0) store_tile(tile_ptr(a.act, a.hr[h], t), sB[h % 2], S::kTileW);
         }
-        ok &= mma_layer<W, 16, true>(sB[(H - 1) % 2], wF[H], tmem, &bars[1], phase, tid);
+        ok &= mma_layer<W, 16, true>(sB[(H - 1) % 2], wF[H], tmem, bar_mma, phase, tid);
         float r16[16];
         tc::tmem_ld16(trow, r16);
         tc::tmem_wait_ld();
@@ -531,7 +579,7 @@ __global__ void __launch_bounds__(128, 1) k_ttc_rrs(const __grid_constant__ TcTr
                 }
             }
             tc::fence_before_sync();
-            __syncthreads();
+            wg_bar(wg);
         } else {
             float dr[16];
 #pragma unroll
@@ -545,38 +593,38 @@ __global__ void __launch_bounds__(128, 1) k_ttc_rrs(const __grid_constant__ TcTr
             }
             store_chunk(sDR, tid, 0, 16, pack8<true>(dr));
             store_chunk(sDR, tid, 1, 16, pack8<true>(dr + 8));
-            sync_for_mma();
+            sync_for_mma_wg(wg);
             if (tid == 0) store_tile(tile_ptr(a.act, a.draw, t), sDR, 128u * 16u * 2u);
-            ok &= mma_layer_t<16, W, W, true>(sDR, wF[H], tmem, &bars[1], phase, tid);
+            ok &= mma_layer_t<16, W, W, true>(sDR, wF[H], tmem, bar_mma, phase, tid);
             if (tid == 0) tc::bulk_wait_read_n<2>();  // since: h[H-1], draw
-            __syncthreads();
+            wg_bar(wg);
             epilogue_mask_bits<W, true>(trow, mk[H - 1], sB[H % 2], tid);
-            sync_for_mma();
+            sync_for_mma_wg(wg);
             if (tid == 0) store_tile(tile_ptr(a.act, a.dhr[H - 1], t), sB[H % 2], S::kTileW);
 #pragma unroll
             for (int h = H - 1; h >= 1; --h) {
-                ok &= mma_layer_t<W, W, W, true>(sB[(h + 1) % 2], wF[h], tmem, &bars[1], phase, tid);
+                ok &= mma_layer_t<W, W, W, true>(sB[(h + 1) % 2], wF[h], tmem, bar_mma, phase, tid);
                 if (tid == 0) {
                     if (h == H - 1) tc::bulk_wait_read_n<2>();  // since: draw, d[H-1]
                     else tc::bulk_wait_read_n<1>();             // since: d[h]
                 }
-                __syncthreads();
+                wg_bar(wg);
                 epilogue_mask_bits<W, true>(trow, mk[h - 1], sB[h % 2], tid);
-                sync_for_mma();
+                sync_for_mma_wg(wg);
                 if (tid == 0) store_tile(tile_ptr(a.act, a.dhr[h - 1], t), sB[h % 2], S::kTileW);
             }
             tc::fence_before_sync();
-            __syncthreads();
+            wg_bar(wg);
         }
-        if (!ok) s_abort = 1;
-        __syncthreads();
-        if (s_abort) flags |= NRRS_DEV_TIMEOUT;
+        if (!ok) s_abort[wg] = 1;
+        wg_bar(wg);
+        if (s_abort[wg]) flags |= NRRS_DEV_TIMEOUT;
     }
     if (!BACKWARD) {
         const double v = block_sum_d(sumV, red);
         const double c = block_sum_d(sumC, red);
         const double rr = block_sum_d(sumR, red);
-        if (tid == 0) {
+        if (threadIdx.x == 0) {
             a.part[4 * blockIdx.x + 1] = v;
             a.part[4 * blockIdx.x + 2] = c;
             a.part[4 * blockIdx.x + 3] = rr;
@@ -585,9 +633,9 @@ __global__ void __launch_bounds__(128, 1) k_ttc_rrs(const __grid_constant__ TcTr
     if (tid == 0) tc::bulk_wait_all();
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) {
+    if (threadIdx.x < 32) {
         tc::fence_after_sync();
-        tc::tmem_dealloc(tmem, W);
+        tc::tmem_dealloc(*tslot, W * WGS);
     }
     (void)flags;
 }
@@ -745,21 +793,26 @@ TcLayout tc_layout(const nrrs_config& c, uint32_t max_n) {
 
 template <int W, int H>
 cudaError_t launch_ttc(nrrs_ctx* ctx, TcTrainArgs& a, cudaStream_t s, bool train_rrs) {
-    using SS = StatSmem<W, H>;
-    using RS = RrsSmem<W, H>;
-    auto ks = k_ttc_stat<W, H>;
-    auto kr0 = k_ttc_rrs<W, H, false>;
-    auto kr1 = k_ttc_rrs<W, H, true>;
+    // the 128-wide networks run two warpgroups per CTA over one weight copy (one CTA per SM);
+    // the 64-wide ones fit three single-warpgroup CTAs per SM
+    constexpr int WGS = W == 128 ? 2 : 1;
+    constexpr int kThreads = 128 * WGS;
+    using SS = StatSmem<W, H, WGS>;
+    using RS = RrsSmem<W, H, WGS>;
+    auto ks = k_ttc_stat<W, H, WGS>;
+    auto kr0 = k_ttc_rrs<W, H, WGS, false>;
+    auto kr1 = k_ttc_rrs<W, H, WGS, true>;
     cudaError_t e = cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SS::kSmem);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(kr0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RS::kSmem);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(kr1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RS::kSmem);
     if (e != cudaSuccess) return e;
-    const uint32_t tiles = (a.n + 127) / 128;
+    // CTAs needed to give every warpgroup at least one tile
+    const uint32_t ctas = ((a.n + 127) / 128 + WGS - 1) / WGS;
     auto grid_of = [&](const void* k, size_t smem) {
-        uint32_t g = (uint32_t)(ctx->sm_count * resident_ctas(k, 128, smem, 8));
-        return g > tiles ? tiles : g;
+        uint32_t g = (uint32_t)(ctx->sm_count * resident_ctas(k, kThreads, smem, 8));
+        return g > ctas ? ctas : g;
     };
     const uint32_t gs = grid_of((const void*)ks, SS::kSmem);
     const uint32_t g = grid_of((const void*)kr0, RS::kSmem);
@@ -767,18 +820,18 @@ cudaError_t launch_ttc(nrrs_ctx* ctx, TcTrainArgs& a, cudaStream_t s, bool train
     if (a.part_used > a.part_rows) return cudaErrorInvalidConfiguration;
     {
         ProfScope ps(ctx, NRRS_KERNEL_TRAIN_STAT, s);
-        ks<<<gs, 128, SS::kSmem, s>>>(a);
+        ks<<<gs, kThreads, SS::kSmem, s>>>(a);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (train_rrs) {
         ProfScope ps(ctx, NRRS_KERNEL_TRAIN_RRS, s);
-        kr0<<<g, 128, RS::kSmem, s>>>(a);
+        kr0<<<g, kThreads, RS::kSmem, s>>>(a);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        kr1<<<g, 128, RS::kSmem, s>>>(a);
+        kr1<<<g, kThreads, RS::kSmem, s>>>(a);
     } else {
         // losses without the RRSNet: only the StatNet sum is present
         ProfScope ps(ctx, NRRS_KERNEL_TRAIN_RRS, s);
-        kr1<<<1, 128, RS::kSmem, s>>>(a);
+        kr1<<<1, kThreads, RS::kSmem, s>>>(a);
     }
     return cudaGetLastError();
 }
