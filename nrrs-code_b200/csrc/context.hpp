@@ -60,6 +60,8 @@ struct nrrs_ctx {
     nrrs::DecideScratch* scr = nullptr;
     unsigned long long* states = nullptr;
     uint32_t max_chunks = 0;
+    // split counts of the two-pass decision when the caller passes no split array
+    uint8_t* split_tmp = nullptr;
     // segment tables resolved on the device from device-resident queue sizes: [0] in inference
     // tiles, [1] in decision chunks (the *_dev entry points)
     nrrs::SegmentTable* segs_dev = nullptr;

@@ -42,6 +42,7 @@ struct DecideArgs {
     int32_t scale_up;
     double inv_fixed_scale;
     uint32_t spin_limit;
+    int32_t split_chunked;        // two-pass decision: split is scratch with one block per chunk
 };
 
 struct SumArgs {
@@ -92,6 +93,9 @@ extern thread_local int g_last_grid;
 
 // decision + emission (single pass, decoupled look-back)
 cudaError_t launch_decide(const DecideArgs& a, cudaStream_t s);
+// the same decision and queue in two passes without a look-back (count + prefix scan, emission);
+// needs a.split (the caller's array or context scratch of one byte per vertex)
+cudaError_t launch_decide_two_pass(const DecideArgs& a, cudaStream_t s);
 // device-side segment tables of device-resident queue sizes (counts_dev[host_max.n]), in units
 // of kTile (tiles_dev) and kDecChunk (chunks_dev); counts above the host maxima are clamped and
 // flag NRRS_DEV_OVERFLOW in *status

@@ -5,9 +5,10 @@
 // allocation through its own arena (the way the reference's integrator gets its queues from
 // KiRaRay's allocator) and forbids a plugin to allocate; a frame loop with a device-memory
 // budget fixed at start-up; code where cudaMalloc's implicit device synchronisation would stall
-// the pipeline. This entry point serves them: it runs the same exact-sum and decide/emit
-// kernels as nrrs_decide_emit, with their scratch in a file-scope device array instead of
-// context memory.
+// the pipeline. This entry point serves them: it runs the same exact-sum kernel as
+// nrrs_decide_emit and the single-pass decision kernel (whose look-back state is a few bytes per
+// 2,048 vertices; the context path's two-pass decision keeps a byte per vertex), with their
+// scratch in a file-scope device array instead of context memory. The results are the same bits.
 //
 // The array holds NRRS_NOALLOC_MAX_N vertices' worth of look-back state (about 66 KB) and stays
 // resident on every GPU that loads the library until the process exits. In host code its name

@@ -322,7 +322,9 @@ int run_decide(nrrs_ctx* ctx, const float* rrs, const float* rnd, const uint32_t
     d.rnd = rnd;
     d.sidx = sidx;
     d.rrs_norm = rrs_norm;
-    d.split = split;
+    // the two-pass decision reads the split counts back: the caller's array, or scratch
+    d.split = split ? split : ctx->split_tmp;
+    d.split_chunked = split ? 0 : 1;
     d.queue = queue;
     d.next_size = next_size;
     d.n_spec_dev = n_spec_dev;
@@ -346,7 +348,7 @@ int run_decide(nrrs_ctx* ctx, const float* rrs, const float* rnd, const uint32_t
     cudaError_t e;
     {
         ProfScope ps(ctx, NRRS_KERNEL_DECIDE, s);
-        e = launch_decide(d, s);
+        e = launch_decide_two_pass(d, s);
     }
     if (e != cudaSuccess) {
         cudaMemsetAsync(ctx->scr, 0, offsetof(DecideScratch, epoch), s);
@@ -587,6 +589,7 @@ int nrrs_create(const nrrs_config* cfg, nrrs_ctx** out) {
     const size_t scr_bytes = sizeof(DecideScratch) + sizeof(unsigned long long) * ctx->max_chunks;
     NRRS_ALLOC(ctx->scr, scr_bytes);
     ctx->states = reinterpret_cast<unsigned long long*>(ctx->scr + 1);
+    NRRS_ALLOC(ctx->split_tmp, (size_t)ctx->max_chunks * kDecChunk);
     NRRS_ALLOC(ctx->loss_dev, sizeof(double) * 2);
     NRRS_ALLOC(ctx->segs_dev, sizeof(SegmentTable) * 2);
     NRRS_ALLOC(ctx->loss_sums, sizeof(double) * 4);
@@ -656,6 +659,7 @@ void nrrs_destroy(nrrs_ctx* ctx) {
     cudaFree(ctx->enc_tiles);
     cudaFree(ctx->x1_tiles);
     cudaFree(ctx->scr);
+    cudaFree(ctx->split_tmp);
     cudaFree(ctx->loss_dev);
     cudaFree(ctx->segs_dev);
     cudaFree(ctx->loss_sums);
