@@ -427,8 +427,16 @@ __global__ void __launch_bounds__(kDecThreads) k_decide_count(const __grid_const
         const unsigned per = (nch + kDecThreads - 1) / kDecThreads;
         const unsigned lo = sg.tile_start + min(nch, tid * per);
         const unsigned hi = sg.tile_start + min(nch, (tid + 1) * per);
+        // the totals come in batches of independent L2 loads (the other CTAs' stores are visible
+        // after their fences and the done counter)
         unsigned long long mine = 0;
-        for (unsigned q = lo; q < hi; ++q) mine += (unsigned)load_state(&a.states[q]);
+        for (unsigned q0 = lo; q0 < hi; q0 += 8) {
+            unsigned t8[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) t8[j] = q0 + j < hi ? (unsigned)__ldcg(&a.states[q0 + j]) : 0u;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) mine += t8[j];
+        }
         s_scan[tid] = mine;
         __syncthreads();
 #pragma unroll 1
@@ -439,10 +447,15 @@ __global__ void __launch_bounds__(kDecThreads) k_decide_count(const __grid_const
             __syncthreads();
         }
         unsigned long long run = tid ? s_scan[tid - 1] : 0ull;
-        for (unsigned q = lo; q < hi; ++q) {
-            const unsigned t = (unsigned)load_state(&a.states[q]);
-            store_state(&a.states[q], run > 0xffffffffull ? 0xffffffffull : run);
-            run += t;
+        for (unsigned q0 = lo; q0 < hi; q0 += 8) {
+            unsigned t8[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) t8[j] = q0 + j < hi ? (unsigned)__ldcg(&a.states[q0 + j]) : 0u;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                if (q0 + j < hi) __stcg(&a.states[q0 + j], run > 0xffffffffull ? 0xffffffffull : run);
+                run += t8[j];
+            }
         }
         if (tid == kDecThreads - 1) {
             const unsigned long long tot = s_scan[tid];
