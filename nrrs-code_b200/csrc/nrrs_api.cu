@@ -349,6 +349,7 @@ int run_decide(nrrs_ctx* ctx, const float* rrs, const float* rnd, const uint32_t
     {
         ProfScope ps(ctx, NRRS_KERNEL_DECIDE, s);
         e = launch_decide_two_pass(d, s);
+        ++ctx->prof.total_launches;  // the scope counts one of its two kernels
     }
     if (e != cudaSuccess) {
         cudaMemsetAsync(ctx->scr, 0, offsetof(DecideScratch, epoch), s);
