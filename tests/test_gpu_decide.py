@@ -141,3 +141,23 @@ def test_device_n_specular(net):
                    n_specular_dev=d_spec, stream=stream())
     assert int(host(d_sz, np.uint32)[0]) == o["total"]
     assert np.array_equal(host(d_split), o["split"])
+
+
+@pytest.mark.parametrize("n", [2049, 300001])
+def test_without_split_and_norm_arrays(net, n):
+    """split and rrs_norm are optional outputs: without them the decision keeps the split counts
+    in its own scratch, and the queue and its size are still the oracle's"""
+    torch = torch_cuda()
+    rng = np.random.default_rng(n)
+    rrs = np.clip(rng.lognormal(-0.2, 1.1, n), 0.05, 8).astype(np.float32)
+    rnd = rng.random(n, dtype=np.float32)
+    dp = nb.default_decide()
+    o = O.decide_emit(rrs, rnd, n, n // 40, dp, shift_n=MAXQ)
+    cap = 9 * n
+    d_q, d_sz = empty(cap, "int32"), empty(1, "int32")
+    net.decideEmit(torch.from_numpy(rrs).cuda(), torch.from_numpy(rnd).cuda(), n, n, n // 40, dp,
+                   None, None, d_q, cap, d_sz, stream=stream())
+    tot = int(host(d_sz, np.uint32)[0])
+    assert tot == o["total"]
+    assert np.array_equal(host(d_q, np.uint32)[:tot], o["queue"])
+    assert net.device_status(stream()) == (nb.OK, 0)

@@ -268,3 +268,35 @@ def test_full_size_4k_bounce():
     rc, flags = net.device_status(stream())
     assert rc == nb.OK and flags == 0
     net.close()
+
+
+def test_batched_gapped_segments_without_split_array(fp32_net):
+    """segments at caller-chosen offsets with gaps between them, one empty, and no split
+    array: the same sizes, queue and normalised factors as the call that passes one"""
+    random_params(fp32_net, 5)
+    counts = [5000, 0, 3001, 2048]
+    offs = [0, 7000, 7000, 12345]
+    N = offs[-1] + counts[-1]
+    v = nb.synth(10, N)
+    d = upload(v)
+    dp = nb.default_decide()
+    caps = [9 * c for c in counts]
+    qoffs = np.concatenate([[0], np.cumsum(caps)]).astype(np.int64)
+    segs = [nb.Segment(offs[k], counts[k], max(counts[k], 1), 0, int(qoffs[k]), caps[k])
+            for k in range(len(counts))]
+    out = []
+    for with_split in (True, False):
+        o = dict(stats=empty(3 * N), rrs=empty(N), norm=empty(N),
+                 split=empty(N, "uint8") if with_split else None,
+                 q=empty(int(qoffs[-1]), "int32"), sz=empty(len(counts), "int32"))
+        fp32_net.generateRRSNumberBatched(soa(d), d["rnd"], segs, dp, o["stats"], o["rrs"],
+                                          o["norm"], o["split"], o["q"], o["sz"], stream())
+        out.append((host(o["sz"], np.uint32).copy(), host(o["q"], np.uint32).copy(),
+                    host(o["norm"]).view(np.uint32).copy()))
+    (sz_a, q_a, n_a), (sz_b, q_b, n_b) = out
+    assert np.array_equal(sz_a, sz_b) and sz_a[1] == 0 and sz_a[0] > 0
+    for k, c in enumerate(counts):
+        q0 = int(qoffs[k])
+        assert np.array_equal(q_a[q0:q0 + sz_a[k]], q_b[q0:q0 + sz_b[k]]), k
+        assert np.array_equal(n_a[offs[k]:offs[k] + c], n_b[offs[k]:offs[k] + c]), k
+    assert fp32_net.device_status(stream()) == (nb.OK, 0)
