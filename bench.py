@@ -508,27 +508,49 @@ class FrameArm:
             post("train")
 
     def measure(self, timer, steps, warmup, clocks=None):
-        """ms per step, per-kernel profile and our kernel launches in the timed region"""
+        """ms per step, per-kernel profile, our kernel launches in the timed region and the
+        device time of the training phase (events around each frame's training steps: its
+        kernels overlap across streams, so their summed times would overstate it)"""
+        import torch
         net = self.net
         for _ in range(warmup):
             self.step()
         timer.sync()
+        spans = []
+
+        def pre(tag):
+            if tag == "train":
+                e = torch.cuda.Event(enable_timing=True)
+                e.record()
+                spans.append([e, None])
+
+        def post(tag):
+            if tag == "train":
+                e = torch.cuda.Event(enable_timing=True)
+                e.record()
+                spans[-1][1] = e
+
         l0 = net.launch_count()
         net.profile(True)
         net.profile_read()
-        ms = timer(self.step, steps, 0, clocks)
+        ms = timer(lambda: self.step(pre, post), steps, 0, clocks)
         launches = net.launch_count() - l0
         prof = net.profile_read()
         net.profile(False)
+        torch.cuda.synchronize()
+        self.train_ms = sum(a.elapsed_time(b) for a, b in spans if b is not None) if spans else None
         return ms, prof, launches
 
     def close(self):
         self.net.close()
 
 
-def train_rate(prof, wl, steps):
-    t_train = sum(t for k, (n, t) in prof.items() if k.startswith("train") or k == "adam"
-                  or k in ("pack_weights", "table_half"))
+def train_rate(prof, wl, steps, train_ms=None):
+    """training samples per second from the device time of the timed frames' training phases
+    (or, without it, the summed times of the training kernels)"""
+    t_train = train_ms if train_ms else sum(
+        t for k, (n, t) in prof.items() if k.startswith("train") or k == "adam"
+        or k in ("pack_weights", "table_half"))
     return wl["train_steps"] * wl["train_batch"] * steps / (t_train * 1e-3) if t_train else None
 
 
@@ -683,7 +705,7 @@ def run_frame_pair(args, torch, dev, stream, timer, name, steps, warmup, fp32_st
     ms, prof, launches = mixed.measure(timer, steps, warmup, clk)
     out.update(ms=ms, prof=prof, launches=launches, clocks=clk.summary() if clk else None)
     out["value"] = wl["bounces"] * wl["n_vert"] * world / (ms * 1e-3)
-    out["train_rate"] = train_rate(prof, wl, steps) if train else None
+    out["train_rate"] = train_rate(prof, wl, steps, mixed.train_ms) if train else None
     out["status"] = mixed.net.device_status(stream)
     if world == 1 and fp32_steps > 0 and prec != "fp32":
         fp = FrameArm(torch, dev, stream, wl, "fp32", dev_b, td, train, 1,
@@ -691,7 +713,8 @@ def run_frame_pair(args, torch, dev, stream, timer, name, steps, warmup, fp32_st
         clk32 = ClockSampler(env_int("LOCAL_RANK", 0)) if headline else None
         ms32, prof32, _ = fp.measure(timer, fp32_steps, 1, clk32)
         out["fp32"] = {"value": wl["bounces"] * wl["n_vert"] / (ms32 * 1e-3), "ms_per_step": ms32,
-                       "train_samples_per_s": train_rate(prof32, wl, fp32_steps) if train else None,
+                       "train_samples_per_s": train_rate(prof32, wl, fp32_steps, fp.train_ms)
+                       if train else None,
                        "steps": fp32_steps, "warmup": 1,
                        "clocks": clk32.summary() if clk32 else None,
                        "kernels": {k: {"launches": n, "ms_total": t} for k, (n, t) in prof32.items()}}

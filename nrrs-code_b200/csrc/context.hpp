@@ -62,6 +62,10 @@ struct nrrs_ctx {
     uint32_t max_chunks = 0;
     // split counts of the two-pass decision when the caller passes no split array
     uint8_t* split_tmp = nullptr;
+    // the split training step runs the table-gradient scatter on this stream, forked from and
+    // joined back into the caller's stream with the two events
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     // segment tables resolved on the device from device-resident queue sizes: [0] in inference
     // tiles, [1] in decision chunks (the *_dev entry points)
     nrrs::SegmentTable* segs_dev = nullptr;

@@ -791,8 +791,11 @@ TcLayout tc_layout(const nrrs_config& c, uint32_t max_n) {
     return L;
 }
 
-template <int W, int H>
-cudaError_t launch_ttc(nrrs_ctx* ctx, TcTrainArgs& a, cudaStream_t s, bool train_rrs) {
+// after_stat() is called once the StatNet kernel is launched (the split step forks the
+// table-gradient scatter there)
+template <int W, int H, class AfterStat>
+cudaError_t launch_ttc(nrrs_ctx* ctx, TcTrainArgs& a, cudaStream_t s, bool train_rrs,
+                       AfterStat after_stat) {
     // the 128-wide networks run two warpgroups per CTA over one weight copy (one CTA per SM);
     // the 64-wide ones fit three single-warpgroup CTAs per SM
     constexpr int WGS = W == 128 ? 2 : 1;
@@ -823,6 +826,7 @@ cudaError_t launch_ttc(nrrs_ctx* ctx, TcTrainArgs& a, cudaStream_t s, bool train
         ks<<<gs, kThreads, SS::kSmem, s>>>(a);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = after_stat()) != cudaSuccess) return e;
     if (train_rrs) {
         ProfScope ps(ctx, NRRS_KERNEL_TRAIN_RRS, s);
         kr0<<<g, kThreads, RS::kSmem, s>>>(a);
@@ -937,14 +941,16 @@ int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint3
         a.pre = 1;
         a.dxs = dxs;
     }
-    if (W == 64) e = H == 2 ? launch_ttc<64, 2>(ctx, a, s, train_rrs) : launch_ttc<64, 3>(ctx, a, s, train_rrs);
-    else e = H == 2 ? launch_ttc<128, 2>(ctx, a, s, train_rrs) : launch_ttc<128, 3>(ctx, a, s, train_rrs);
-    if (e == cudaSuccess && split) {
-        // Level groups of at most kScatterGroupBytes of FP32 gradient, each zeroed right before
-        // its scatter: the zeroing writes whole sectors into L2, so the reductions that follow
-        // hit there. Zeroed at the start of the step, the slices were evicted by the kernels in
-        // between, and every first reduction into a sector read its zeros back from HBM as a
-        // random 32-byte access.
+    // Split step: the table-gradient scatter needs only the StatNet kernel's lane gradients,
+    // and nothing before Adam reads the table gradient, so it runs on the context's side
+    // stream, forked after the StatNet launch, while the RRSNet kernels and the weight
+    // gradients run here; the step joins it before Adam (or before returning the gradients).
+    // Level groups of at most kScatterGroupBytes of FP32 gradient, each zeroed right before its
+    // scatter: the zeroing writes whole sectors into L2, so the reductions that follow hit
+    // there. Zeroed at the start of the step, the slices were evicted by the kernels in between,
+    // and every first reduction into a sector read its zeros back from HBM as a random 32-byte
+    // access.
+    auto scatter_table = [&](cudaStream_t ss) -> cudaError_t {
         ScatterLvArgs sa{};
         sa.enc = ctx->enc;
         sa.pos = v.pos;
@@ -961,7 +967,8 @@ int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint3
             const uint64_t r = (uint64_t)lv.res + 1;
             return lv.dense ? r * r * r : (uint64_t)ctx->enc.hash_mask + 1;
         };
-        for (int l0 = 0; l0 < nl && e == cudaSuccess;) {
+        cudaError_t es = cudaSuccess;
+        for (int l0 = 0; l0 < nl && es == cudaSuccess;) {
             const uint64_t row0 = ctx->enc.lv[l0].offset;
             uint64_t row1 = row0 + level_rows(l0);
             int l1 = l0 + 1;
@@ -970,19 +977,42 @@ int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint3
                 row1 = ctx->enc.lv[l1].offset + level_rows(l1);
                 ++l1;
             }
-            e = cudaMemsetAsync(ctx->grads + 2 * row0, 0, sizeof(float) * 2 * (row1 - row0), s);
-            if (e != cudaSuccess) break;
+            es = cudaMemsetAsync(ctx->grads + 2 * row0, 0, sizeof(float) * 2 * (row1 - row0), ss);
+            if (es != cudaSuccess) break;
             sa.level_begin = (uint32_t)l0;
             sa.level_end = (uint32_t)l1;
             const uint32_t items = (uint32_t)(l1 - l0) * tiles;
             const uint32_t g = g_max < items ? g_max : items;
-            ProfScope ps(ctx, NRRS_KERNEL_TRAIN_SCATTER, s);
-            if (g) k_scatter_levels<<<g, 128, 0, s>>>(sa);
-            e = cudaGetLastError();
+            ProfScope ps(ctx, NRRS_KERNEL_TRAIN_SCATTER, ss);
+            if (g) k_scatter_levels<<<g, 128, 0, ss>>>(sa);
+            es = cudaGetLastError();
             l0 = l1;
         }
-    }
+        return es;
+    };
+    bool forked = false;
+    auto after_stat = [&]() -> cudaError_t {
+        if (!split) return cudaSuccess;
+        cudaError_t ef = cudaEventRecord(ctx->ev_fork, s);
+        if (ef == cudaSuccess) ef = cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0);
+        if (ef != cudaSuccess) return ef;
+        forked = true;
+        ef = scatter_table(ctx->side);
+        const cudaError_t ej = cudaEventRecord(ctx->ev_join, ctx->side);
+        return ef != cudaSuccess ? ef : ej;
+    };
+    auto join = [&]() {
+        if (forked) cudaStreamWaitEvent(s, ctx->ev_join, 0);
+        forked = false;
+    };
+    if (W == 64)
+        e = H == 2 ? launch_ttc<64, 2>(ctx, a, s, train_rrs, after_stat)
+                   : launch_ttc<64, 3>(ctx, a, s, train_rrs, after_stat);
+    else
+        e = H == 2 ? launch_ttc<128, 2>(ctx, a, s, train_rrs, after_stat)
+                   : launch_ttc<128, 3>(ctx, a, s, train_rrs, after_stat);
     if (e != cudaSuccess) {
+        join();
         ctx->last_error = std::string("tensor-core train launch: ") + cudaGetErrorString(e);
         return NRRS_ERR_CUDA;
     }
@@ -1027,6 +1057,7 @@ int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint3
         e = launch_wreduce(partial, (uint32_t)chunks, (uint32_t)mlp, ctx->grads + ctx->n_table,
                            1.0f / (float)n, s);
     }
+    join();  // the table gradient is complete on s from here
     if (e != cudaSuccess) {
         ctx->last_error = std::string("tensor-core wgrad launch: ") + cudaGetErrorString(e);
         return NRRS_ERR_CUDA;

@@ -620,6 +620,9 @@ int nrrs_create(const nrrs_config* cfg, nrrs_ctx** out) {
         e = cudaMemcpy(&ctx->scr->epoch, &one, sizeof(one), cudaMemcpyHostToDevice);
     }
     if (e == cudaSuccess) e = cudaMemset(ctx->loss_dev, 0, sizeof(double) * 2);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         nrrs_destroy(ctx);
         return fail(nullptr, NRRS_ERR_CUDA, std::string("init: ") + cudaGetErrorString(e));
@@ -642,6 +645,12 @@ int nrrs_create(const nrrs_config* cfg, nrrs_ctx** out) {
 void nrrs_destroy(nrrs_ctx* ctx) {
     if (!ctx) return;
     for (cudaEvent_t ev : ctx->prof.pool) cudaEventDestroy(ev);
+    if (ctx->side) {
+        cudaStreamSynchronize(ctx->side);
+        cudaStreamDestroy(ctx->side);
+    }
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
     cudaFree(ctx->params);
     cudaFree(ctx->grads);
     cudaFree(ctx->adam_m);
