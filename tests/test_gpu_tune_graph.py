@@ -216,7 +216,7 @@ def test_split_mode_graph_equals_fused_direct():
     l0 = net.launch_count()
     g = net.captureBatched(soa(d), d["rnd"], segs, dp, b["st"], b["rrs"], b["norm"], b["split"],
                            b["q"], b["sz"])
-    assert net.launch_count() - l0 == 3      # encode, MLP, decide
+    assert net.launch_count() - l0 == 4      # encode, MLP, decision count and emit
     g.launch(stream())
     torch.cuda.synchronize()
     for k in a:
