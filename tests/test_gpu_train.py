@@ -134,6 +134,16 @@ def test_mixed_training_vs_fp64_oracle(prec, step, shape):
             continue
         e = rel_err(g[sl].astype(np.float64), g64[sl])
         assert e < bars[name], (name, e)
+    # Adam (t = 1) on the step's own gradients: the table part runs level group by level group
+    # on the side stream, the MLP part after the join
+    p1 = net.get_params()
+    pe = p0.copy()
+    m = np.zeros_like(pe); vv = np.zeros_like(pe)
+    count = ntab + nst + (nrr if step >= 3 else 0)
+    O.adam(net.config, pe, g, m, vv, 1, 0, count)
+    assert np.allclose(p1, pe, rtol=1e-5, atol=1e-7)
+    m1, _, t = net.get_adam_state()
+    assert t == 1 and np.allclose(m1[:count], 0.1 * g[:count], rtol=1e-5, atol=1e-12)
     rc, flags = net.device_status(stream())
     assert rc == nb.OK and flags == 0
     net.close()
