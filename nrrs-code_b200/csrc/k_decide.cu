@@ -61,6 +61,19 @@ __device__ __forceinline__ unsigned split_count(float r, float rnd, unsigned* fl
 // queue entries of one chunk staged in shared memory (E[s] is about 1: 2,048 per chunk)
 constexpr unsigned kDecStage = 4096;
 
+// normalisation scale of segment si (FP32 sequence of integrator.cpp:1376-1397)
+__device__ __forceinline__ float decide_scale(const DecideArgs& a, const Segment& sg, int si) {
+    const long long acc = a.ext_sum ? *(const volatile long long*)a.ext_sum
+                                    : (long long)*(volatile unsigned long long*)&a.scr->sum_acc[si];
+    const float sumf = (float)((double)acc * a.inv_fixed_scale);
+    const float rcp = __fdiv_rn(1.0f, sumf);
+    const unsigned nspec = (a.n_spec_dev && si == 0) ? *a.n_spec_dev : sg.n_specular;
+    const float bud = (float)(unsigned)(sg.budget - nspec);
+    float nf = __fmul_rn(bud, rcp);
+    nf = __fmul_rn(nf, a.use_ceil ? 1.0f : a.normalize_rate);
+    return a.scale_up ? nf : (nf < 1.0f ? nf : 1.0f);
+}
+
 __global__ void __launch_bounds__(kDecThreads) k_decide(const __grid_constant__ DecideArgs a) {
     __shared__ unsigned s_chunk, s_epoch, s_prefix;
     __shared__ uint32_t s_stage[kDecStage];
@@ -83,16 +96,7 @@ __global__ void __launch_bounds__(kDecThreads) k_decide(const __grid_constant__ 
         const unsigned base = sg.offset + lc * kDecChunk;
         const unsigned end = sg.offset + min(sg.count, (lc + 1) * kDecChunk);
 
-        // normalisation factor, FP32 sequence of integrator.cpp:1376-1397
-        const long long acc = a.ext_sum ? *(const volatile long long*)a.ext_sum
-                                        : (long long)*(volatile unsigned long long*)&a.scr->sum_acc[si];
-        const float sumf = (float)((double)acc * a.inv_fixed_scale);
-        const float rcp = __fdiv_rn(1.0f, sumf);
-        const unsigned nspec = (a.n_spec_dev && si == 0) ? *a.n_spec_dev : sg.n_specular;
-        const float bud = (float)(unsigned)(sg.budget - nspec);
-        float nf = __fmul_rn(bud, rcp);
-        nf = __fmul_rn(nf, a.use_ceil ? 1.0f : a.normalize_rate);
-        const float scale = a.scale_up ? nf : (nf < 1.0f ? nf : 1.0f);
+        const float scale = decide_scale(a, sg, si);
 
         unsigned sv[kDecVPT];
         unsigned st[kDecVPT];
@@ -302,19 +306,6 @@ __global__ void __launch_bounds__(kDecThreads) k_decide(const __grid_constant__ 
 // counts back (1 byte per vertex) and writes its queue entries at its prefix. Same decisions and
 // the same queue as the single-pass kernel, bit for bit; each CTA runs without waiting on any
 // other, which the single-pass kernel's per-chunk look-back and block barriers did.
-
-// normalisation scale of segment si (FP32 sequence of integrator.cpp:1376-1397)
-__device__ __forceinline__ float decide_scale(const DecideArgs& a, const Segment& sg, int si) {
-    const long long acc = a.ext_sum ? *(const volatile long long*)a.ext_sum
-                                    : (long long)*(volatile unsigned long long*)&a.scr->sum_acc[si];
-    const float sumf = (float)((double)acc * a.inv_fixed_scale);
-    const float rcp = __fdiv_rn(1.0f, sumf);
-    const unsigned nspec = (a.n_spec_dev && si == 0) ? *a.n_spec_dev : sg.n_specular;
-    const float bud = (float)(unsigned)(sg.budget - nspec);
-    float nf = __fmul_rn(bud, rcp);
-    nf = __fmul_rn(nf, a.use_ceil ? 1.0f : a.normalize_rate);
-    return a.scale_up ? nf : (nf < 1.0f ? nf : 1.0f);
-}
 
 __device__ __forceinline__ unsigned block_sum_u(unsigned v, unsigned* s_red) {
 #pragma unroll

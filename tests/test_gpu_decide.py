@@ -161,3 +161,20 @@ def test_without_split_and_norm_arrays(net, n):
     assert tot == o["total"]
     assert np.array_equal(host(d_q, np.uint32)[:tot], o["queue"])
     assert net.device_status(stream()) == (nb.OK, 0)
+
+
+def test_chunks_beyond_the_shared_memory_stage(net):
+    """scale_up with a few large factors: chunks whose queue entries exceed the emission's
+    shared-memory stage (4,096 entries for 2,048 vertices) write them directly"""
+    rng = np.random.default_rng(11)
+    n = 100_000
+    rrs = np.full(n, 0.05, np.float32)
+    rrs[:3000] = 8.0
+    rrs[50_000:50_500] = rng.uniform(4.0, 8.0, 500).astype(np.float32)
+    rnd = rng.random(n, dtype=np.float32)
+    dp = nb.default_decide(use_ceil=0, scale_up=1, normalize_rate=1.0)
+    o = O.decide_emit(rrs, rnd, n, 0, dp, shift_n=MAXQ)
+    assert o["split"][:2048].sum() > 4096
+    g = run_decide(net, rrs, rnd, n, 0, dp, capacity=o["total"] + 16)
+    compare(g, o)
+    assert g["rc"] == nb.OK
