@@ -654,6 +654,7 @@ struct TcJob {
 struct TcWGradArgs {
     const uint8_t* act;
     uint32_t n, chunks, total;
+    uint32_t chunk;             // samples per chunk (a multiple of 64, at least kTcChunk)
     float* partial;
     int32_t njobs;
     TcJob job[8];
@@ -688,8 +689,8 @@ __global__ void __launch_bounds__(128, 1) k_wgrad_tc(const __grid_constant__ TcW
     const int tid = threadIdx.x, warp = tid >> 5;
     const TcJob& j = a.job[blockIdx.y];
     const uint32_t c = blockIdx.x;
-    const uint32_t s0 = c * kTcChunk;
-    const uint32_t s1 = min(a.n, s0 + kTcChunk);
+    const uint32_t s0 = c * a.chunk;
+    const uint32_t s1 = min(a.n, s0 + a.chunk);
     const uint32_t stages = (s1 - s0 + 63) / 64;
 
     if (tid == 0) {
@@ -866,7 +867,19 @@ int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint3
                   double* loss_dev, cudaStream_t s, bool apply, const LossWeights* lw) {
     const nrrs_config& c = ctx->cfg;
     const TcLayout L = tc_layout(c, c.max_train);
-    const uint64_t chunks = (n + kTcChunk - 1) / kTcChunk;
+    const bool train_rrs = c.step >= 3;
+    // Weight-gradient chunks: as many as fill one wave of the weight-gradient grid (one CTA per
+    // chunk and layer), each at least kTcChunk samples so that the partials fit the scratch
+    // sized by kTcChunk. 262,144 samples and 8 layers on 444 CTA slots: 55 chunks of 4,800
+    // (64 chunks of 4,096 were 1.15 waves).
+    const size_t wsm = 1024 + 4 * kWgBuf + 64;
+    const uint32_t njobs = (uint32_t)(c.statnet_hidden + 1) * (train_rrs ? 2u : 1u);
+    const uint32_t slots =
+        (uint32_t)ctx->sm_count * (uint32_t)resident_ctas((const void*)k_wgrad_tc, 128, wsm, 4);
+    const uint32_t per_wave = slots / njobs > 0 ? slots / njobs : 1u;
+    uint32_t chunk_len = ((n + per_wave - 1) / per_wave + 63u) / 64u * 64u;
+    if (chunk_len < kTcChunk) chunk_len = kTcChunk;
+    const uint64_t chunks = (n + chunk_len - 1) / chunk_len;
     const uint64_t mlp = ctx->n_stat + ctx->n_rrs;
     uint8_t* act = reinterpret_cast<uint8_t*>(ctx->train_scratch);
     double* part = reinterpret_cast<double*>(act + L.act_bytes);
@@ -876,7 +889,6 @@ int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint3
     const uint64_t chunks_max = (c.max_train + kTcChunk - 1) / kTcChunk;
     float* dxs = reinterpret_cast<float*>(
         (reinterpret_cast<uintptr_t>(partial + chunks_max * mlp) + 15u) & ~uintptr_t(15));
-    const bool train_rrs = c.step >= 3;
     const bool split = ctx->train_split != 0;
     // the split step zeroes the table gradient level group by level group right before that
     // group's scatter (below); here only what the other kernels accumulate into
@@ -1021,6 +1033,7 @@ int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint3
     w.act = act;
     w.n = n;
     w.chunks = (uint32_t)chunks;
+    w.chunk = chunk_len;
     w.total = (uint32_t)mlp;
     w.partial = partial;
     int nj = 0;
@@ -1045,7 +1058,6 @@ int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint3
         w.job[nj++] = TcJob{1, 0, L.draw.off, 16, 1, (uint32_t)W, (uint32_t)W, L.hr[H - 1].off, off, (uint32_t)W};
     }
     w.njobs = nj;
-    const size_t wsm = 1024 + 4 * kWgBuf + 64;
     e = cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
     if (e == cudaSuccess) {
         ProfScope ps(ctx, NRRS_KERNEL_TRAIN_WGRAD, s);
