@@ -58,6 +58,7 @@ struct TcTrainArgs {
     uint32_t part_used;     // rows the StatNet and RRSNet-forward grids write
     double* loss_out;
     LossWeights lw;         // per-sample loss weights (inactive: plain means)
+    unsigned* status;       // the context's NRRS_DEV_* word: wait timeouts are reported there
 };
 
 __device__ __forceinline__ uint8_t* tile_ptr(uint8_t* act, const Arr& r, uint32_t t) {
@@ -374,7 +375,7 @@ __global__ void __launch_bounds__(128 * WGS, 1) k_ttc_stat(const __grid_constant
         tc::fence_after_sync();
         tc::tmem_dealloc(*tslot, W * WGS);
     }
-    (void)flags;
+    if (flags && tid == 0) atomicOr(a.status, flags);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -637,7 +638,7 @@ __global__ void __launch_bounds__(128 * WGS, 1) k_ttc_rrs(const __grid_constant_
         tc::fence_after_sync();
         tc::tmem_dealloc(*tslot, W * WGS);
     }
-    (void)flags;
+    if (flags && tid == 0) atomicOr(a.status, flags);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -658,6 +659,7 @@ struct TcWGradArgs {
     float* partial;
     int32_t njobs;
     TcJob job[8];
+    unsigned* status;           // the context's NRRS_DEV_* word
 };
 
 constexpr uint32_t kWgBuf = 16384;  // bytes per operand stage (64 samples x up to 128 features)
@@ -756,6 +758,7 @@ __global__ void __launch_bounds__(128, 1) k_wgrad_tc(const __grid_constant__ TcW
         else if (j.Fa == 16) wgrad_epilogue<16>(trow, j, out, m);
         else wgrad_epilogue<128>(trow, j, out, m);
     }
+    if (tid == 0 && (s_fail || !done)) atomicOr(a.status, NRRS_DEV_TIMEOUT);
     tc::fence_before_sync();
     __syncthreads();
     if (warp == 0) {
@@ -927,6 +930,7 @@ int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint3
     a.part = part;
     a.part_rows = part_rows;
     a.loss_out = loss_dev ? loss_dev : ctx->loss_dev;
+    a.status = &ctx->scr->status;
     if (lw) a.lw = *lw;
     if (split) {
         // hash columns of the x0 tiles, level-major (FP16, the StatNet training precision)
@@ -1034,6 +1038,7 @@ int train_step_tc(nrrs_ctx* ctx, const VertexPtrs& v, const float* target, uint3
     w.n = n;
     w.chunks = (uint32_t)chunks;
     w.chunk = chunk_len;
+    w.status = &ctx->scr->status;
     w.total = (uint32_t)mlp;
     w.partial = partial;
     int nj = 0;
